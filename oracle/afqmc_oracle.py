@@ -1,0 +1,632 @@
+"""ORACLE (test infrastructure only) -- FP64 CPU restatement of SAFIRE's AFQMC hot path.
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import this
+module, and only as the checker / the timed CPU baseline; the product path (safire_b200)
+never calls it.
+
+It restates, function by function, the reference's CLOSED-shell, single-determinant,
+dense-real-Cholesky path (paths relative to the SAFIRE source tree):
+
+  log_determinant_from_getrf    src/numerics/operations/determinants_impl.hpp:33-75
+  log_determinant_from_geqrf    src/numerics/operations/determinants_impl.hpp:78-108
+  log_overlap_impl              src/AFQMC/SlaterDeterminantOperations/density_matrix.hpp:120-156
+  getri_or_zero                 src/numerics/nda_functions.hpp:422-438
+  inverse_logdet                src/AFQMC/SlaterDeterminantOperations/density_matrix.hpp:42-76
+  MixedDensityMatrix            src/AFQMC/SlaterDeterminantOperations/density_matrix.hpp:544-601
+  Log_Overlap                   src/AFQMC/SlaterDeterminantOperations/density_matrix.hpp:437-447
+  NOMSD::Log_Overlap (CLOSED x2) src/AFQMC/Wavefunctions/NOMSD.cpp:280-300
+  NOMSD::DensityMatrix          src/AFQMC/Wavefunctions/NOMSD.hpp:293-343
+  Real3IndexFactorization       src/AFQMC/HamiltonianOperations/Real3IndexFactorization.hpp
+      vHS :282-326, vbias :328-428, energy :138-174, energy_impl :476-590,
+      getOneBodyPropagatorMatrix :99-124
+  add_one_body_shifts           src/AFQMC/HamiltonianOperations/detail/one_body.hpp:65-85
+  half rotation, v0             src/AFQMC/Hamiltonians/RealDenseHamiltonian.cpp:138-180
+  NOMSD::vMF                    src/AFQMC/Wavefunctions/NOMSD.cpp:437-466
+  generateP1 / exp_hermitian    src/AFQMC/Propagators/AFQMCBasePropagator.cpp:43-214;
+                                src/numerics/operations/exp.hpp:28-60
+  assemble_X / construct_X      src/AFQMC/Propagators/AFQMCBasePropagator.cpp:687-733;
+                                src/AFQMC/Propagators/construct_X_kernel.hpp:34-87
+  probit (Acklam)               src/AFQMC/Utilities/probit.h:58-136
+  Propagate (step 1..7)         src/AFQMC/Propagators/AFQMCBasePropagator.cpp:290-392
+  apply_expM / propagate_impl   src/AFQMC/SlaterDeterminantOperations/propagate.hpp:45-70,247-298
+  walker_update / bounds        src/AFQMC/Propagators/WalkerSetUpdate.hpp:46-218
+  orthogonalize                 src/AFQMC/SlaterDeterminantOperations/orthogonalize.hpp:135-169
+  comb / swap_walkers_async     src/AFQMC/Walkers/population_control.hpp:34-65,143-255
+  averagePseudoEnergy / averageEnergy   src/AFQMC/Drivers/average_energy.hpp:33-76
+  EnergyEstimator::measure      src/AFQMC/Estimators/EnergyEstimator.h:51-100
+  run_afqmc step loop           src/AFQMC/Drivers/run_afqmc.cpp:69-113
+
+LAPACK arithmetic at the boundary (the reference reaches it through TRIQS/nda @5046352):
+zgetrf / zgetri / zgeqrf / zungqr from scipy's OpenBLAS, and numpy's eigh (zheevd).
+
+Auxiliary fields come from ``oracle.philox`` (Philox-4x32-10, stream 1); the comb draws from
+stream 0.  The reference uses mt19937 here (src/utilities/Random.hpp:37-51); the injection
+point ``sampleUniformFields`` is the same.
+"""
+import math
+
+import numpy as np
+import scipy.linalg.lapack as lapack
+
+from . import philox
+
+SMALL = np.finfo(np.float64).tiny  # numeric_limits<double>::min(), determinants_impl.hpp:40
+
+
+# --------------------------------------------------------------------------------------------
+# log det, LU, inverse (determinants_impl.hpp:33-75; nda_functions.hpp:422-438)
+# --------------------------------------------------------------------------------------------
+def log_det_from_getrf(lu, piv, res=0j):
+    """Sum_i log(+-U_ii + tiny), pivot sign per row swap, imag folded into [-pi, pi].
+
+    ``piv`` is LAPACK's 0-based pivot vector (scipy), so "no swap" is piv[i] == i; the
+    reference compares the 1-based ipiv to i+1 (determinants_impl.hpp:46-50).  ``res``
+    accumulates, as in the reference.
+    """
+    n = lu.shape[0]
+    for i in range(n):
+        d = complex(lu[i, i])
+        if piv[i] == i:
+            res += np.log(d + SMALL)
+        else:
+            res += np.log(-d + SMALL)
+    im = res.imag
+    if im > math.pi:
+        while im > math.pi:
+            im -= 2 * math.pi
+    elif im < -math.pi:
+        while im < -math.pi:
+            im += 2 * math.pi
+    return complex(res.real, im)
+
+
+def lu_logdet_inverse(T, res=0j, invert=True):
+    """getrf + log det + getri_or_zero for one N x N complex matrix."""
+    lu, piv, info = lapack.zgetrf(np.asarray(T, dtype=np.complex128))
+    ld = log_det_from_getrf(lu, piv, res)
+    if not invert:
+        return ld, None
+    inv, info2 = lapack.zgetri(lu, piv)
+    if info2 != 0:
+        inv = np.zeros_like(inv)
+    return ld, inv
+
+
+def inverse_logdet(A):
+    """density_matrix.hpp:82-108 -- batched (nbatch, N, N): returns (inverse, logdet)."""
+    A = np.asarray(A, dtype=np.complex128)
+    inv = np.empty_like(A)
+    ld = np.zeros(A.shape[0], dtype=np.complex128)
+    for b in range(A.shape[0]):
+        ld[b], inv[b] = lu_logdet_inverse(A[b])
+    return inv, ld
+
+
+# --------------------------------------------------------------------------------------------
+# Overlaps and mixed density matrix (density_matrix.hpp:120-156,437-447,544-601)
+# --------------------------------------------------------------------------------------------
+def mixed_density_matrix(A, B, compact=True, ovlp=None):
+    """A = PsiT (N x M, herm=true form), B = walkers (W, M, N).
+
+    Returns (G, ovlp) with G (W, N, M) when compact (G = T(T^-1) * T(B)), or (W, M, M)
+    otherwise (G = conj-free A^T * T^-T * B^T, density_matrix.hpp:580-585).
+    ``ovlp`` accumulates (log_determinant_from_getrf adds to res).
+    """
+    A = np.asarray(A, dtype=np.complex128)
+    B = np.asarray(B, dtype=np.complex128)
+    W, M, N = B.shape
+    if ovlp is None:
+        ovlp = np.zeros(W, dtype=np.complex128)
+    else:
+        ovlp = np.array(ovlp, dtype=np.complex128)
+    if N == 0:
+        return np.zeros((W, 0, M) if compact else (W, M, M), np.complex128), ovlp
+    T = A @ B                                   # (W, N, N)   math::product(A,B,TNN)
+    Tinv = np.empty_like(T)
+    for w in range(W):
+        ovlp[w], Tinv[w] = lu_logdet_inverse(T[w], ovlp[w])
+    # C = T(TNN) * T(B)  -> C[w] = Tinv[w]^T @ B[w]^T
+    Gc = np.transpose(Tinv, (0, 2, 1)) @ np.transpose(B, (0, 2, 1))   # (W, N, M)
+    if compact:
+        return Gc, ovlp
+    # herm: C = T(A) * T2 with T2 = T(TNN) * T(B)
+    return A.T[None, :, :] @ Gc, ovlp
+
+
+def log_overlap(A, B, ovlp=None):
+    """det_ops::Log_Overlap (density_matrix.hpp:437-447): accumulating, no inverse."""
+    A = np.asarray(A, dtype=np.complex128)
+    B = np.asarray(B, dtype=np.complex128)
+    W = B.shape[0]
+    ovlp = np.zeros(W, np.complex128) if ovlp is None else np.array(ovlp, np.complex128)
+    if B.shape[2] == 0:
+        return ovlp
+    T = A @ B
+    for w in range(W):
+        ovlp[w], _ = lu_logdet_inverse(T[w], ovlp[w], invert=False)
+    return ovlp
+
+
+def log_overlap_closed(PsiT, Wk):
+    """NOMSD::Log_Overlap, ndet = 1, CLOSED: 2 * Log_Overlap + log(conj(ci0)), ci0 = 1."""
+    return 2.0 * log_overlap(PsiT, Wk) + np.log(np.conj(1.0 + 0j))
+
+
+# --------------------------------------------------------------------------------------------
+# Hamiltonian setup (RealDenseHamiltonian.cpp:138-180; one_body.hpp:65-153)
+# --------------------------------------------------------------------------------------------
+class Hamiltonian:
+    """Dense real Cholesky Hamiltonian + single-determinant CLOSED trial.
+
+    hcore (M, M) real symmetric; Likn (M, M, Nc) real, L[i, k, n]; PsiT (N, M) complex.
+    """
+
+    def __init__(self, hcore, Likn, PsiT, E0=0.0):
+        self.hcore = np.asarray(hcore, dtype=np.float64)
+        self.Likn = np.ascontiguousarray(Likn, dtype=np.float64)
+        self.PsiT = np.asarray(PsiT, dtype=np.complex128)
+        self.E0 = float(E0)
+        self.M = self.hcore.shape[0]
+        self.N = self.PsiT.shape[0]
+        self.Nc = self.Likn.shape[2]
+        M, N, Nc = self.M, self.N, self.Nc
+        # haj = PsiT * hcore (one_body.hpp:124-153)
+        self.haj = self.PsiT @ self.hcore.astype(np.complex128)
+        # Lnak[n, a, k] = sum_i PsiT[a, i] L[i, k, n]  (RealDenseHamiltonian.cpp:141-161)
+        L2 = self.Likn.reshape(M, M * Nc)
+        Lak_n = (self.PsiT.real @ L2 + 1j * (self.PsiT.imag @ L2)).reshape(N, M, Nc)
+        self.Lnak = np.ascontiguousarray(np.transpose(Lak_n, (2, 0, 1)))
+        # v0[i, l] = -0.5 sum_{j,n} L[i, j, n] L[l, j, n]  (RealDenseHamiltonian.cpp:165-180)
+        Lf = self.Likn.reshape(M, M * Nc)
+        self.v0 = -0.5 * (Lf @ Lf.T)
+
+    # Real3IndexFactorization::vbias, CLOSED, ndet = 1 (:328-428): a = 2 sqrt(dt)
+    def vbias(self, G, dt):
+        W = G.shape[0]
+        a = 2.0 * math.sqrt(dt)
+        G2 = G.reshape(W, self.N * self.M)
+        L2 = self.Lnak.reshape(self.Nc, self.N * self.M)
+        return a * (G2 @ L2.T)
+
+    # Real3IndexFactorization::vHS (:282-326): v[w, i, k] = sqrt(dt) sum_n L[i, k, n] X[w, n]
+    def vHS(self, X, dt):
+        W = X.shape[0]
+        a = math.sqrt(dt)
+        L2 = self.Likn.reshape(self.M * self.M, self.Nc)
+        Xr = np.ascontiguousarray(X.real.T)
+        Xi = np.ascontiguousarray(X.imag.T)
+        v = (L2 @ Xr) + 1j * (L2 @ Xi)            # (M*M, W)
+        return a * np.ascontiguousarray(v.T).reshape(W, self.M, self.M)
+
+    # Real3IndexFactorization::energy / energy_impl, CLOSED (:138-174, :476-590)
+    def energy(self, G, addH1=True, addEJ=True, addEXX=True, chunk=None):
+        W = G.shape[0]
+        N, M, Nc = self.N, self.M, self.Nc
+        scl = 2.0
+        E = np.zeros((W, 3), dtype=np.complex128)
+        if addH1:
+            E[:, 0] = self.E0
+            E[:, 0] += scl * np.einsum('waj,aj->w', G, self.haj)
+        Kl = np.zeros((W, Nc), dtype=np.complex128)
+        if addEXX:
+            if chunk is None:
+                chunk = max(1, min(Nc, int(2e8 // max(1, W * N * N))))
+            L3 = self.Lnak
+            for n0 in range(0, Nc, chunk):
+                n1 = min(Nc, n0 + chunk)
+                Lc = L3[n0:n1].reshape((n1 - n0) * N, M)          # rows (n, a)
+                T = (G.reshape(W * N, M) @ Lc.T).reshape(W, N, n1 - n0, N)  # T[w,b,n,a]
+                # E1 += -0.5 scl sum_abn T[w,a,n,b] T[w,b,n,a]
+                E[:, 1] += -0.5 * scl * np.einsum('wanb,wbna->w', T, T)
+                if addEJ:
+                    Kl[:, n0:n1] += np.einsum('wana->wn', T)
+        if addEJ:
+            E[:, 2] += 0.5 * 4.0 * np.einsum('wn,wn->w', Kl, Kl)
+        return E
+
+    # Real3IndexFactorization::getOneBodyPropagatorMatrix (:99-124) + add_one_body_shifts
+    def one_body_propagator_matrix(self, dt, vMF):
+        shift = self.vHS(np.asarray(vMF, np.complex128)[None, :], dt)[0]
+        return dt * self.hcore + dt * self.v0 + shift
+
+
+def trial_density(ham):
+    """G of the trial against itself (NOMSD::vMF: MixedDensityMatrix(PsiT, PsiT^H))."""
+    B = np.conj(ham.PsiT.T)[None, :, :]
+    G, _ = mixed_density_matrix(ham.PsiT, B, compact=True)
+    return G
+
+
+def vMF(ham, dt):
+    """NOMSD::vMF (NOMSD.cpp:437-466) with zero_imag (AFQMCBasePropagator.cpp:107)."""
+    v = ham.vbias(trial_density(ham), dt)[0]
+    return v.real.astype(np.complex128)
+
+
+def hermitize(H):
+    """math::hermitize (numerics/operations/tensor.hpp:75-93)."""
+    H = np.array(H, dtype=np.complex128)
+    n = H.shape[0]
+    for i in range(n):
+        H[i, i] = H[i, i].real
+        for j in range(i + 1, n):
+            H[i, j] = 0.5 * H[i, j] + 0.5 * np.conj(H[j, i])
+            H[j, i] = np.conj(H[i, j])
+    return H
+
+
+def exp_hermitian(A):
+    """math::exp_hermitian (exp.hpp:28-60): M sqrt(exp(V)) (M sqrt(exp(V)))^H."""
+    V, Mv = np.linalg.eigh(np.asarray(A, dtype=np.complex128))
+    Ms = Mv * np.sqrt(np.exp(V))[None, :]
+    return Ms @ np.conj(Ms.T)
+
+
+def build_P1(ham, vmf, dt, dense=False, drop=1e-8):
+    """generateP1 (AFQMCBasePropagator.cpp:43-214): P1 = exp(-1/2 herm(H1)).
+
+    With ``dense=False`` entries with |P1_ij| < drop are zeroed, which is what the CSR
+    conversion ``to_csr(P1d, 1e-8)`` keeps (AFQMCBasePropagator.cpp:165-172).
+    """
+    H1 = ham.one_body_propagator_matrix(dt, vmf)
+    H1 = hermitize(H1) * (-0.5)
+    P = exp_hermitian(H1)
+    if not dense:
+        P = np.where(np.abs(P) < drop, 0.0, P)
+    return P
+
+
+# --------------------------------------------------------------------------------------------
+# Fields (construct_X_kernel.hpp:34-87; probit.h:58-136; AFQMCBasePropagator.cpp:324-336)
+# --------------------------------------------------------------------------------------------
+_PA = (-3.969683028665376e+01, 2.209460984245205e+02, -2.759285104469687e+02,
+       1.383577518672690e+02, -3.066479806614716e+01, 2.506628277459239e+00)
+_PB = (-5.447609879822406e+01, 1.615858368580409e+02, -1.556989798598866e+02,
+       6.680131188771972e+01, -1.328068155288572e+01)
+_PC = (-7.784894002430293e-03, -3.223964580411365e-01, -2.400758277161838e+00,
+       -2.549732539343734e+00, 4.374664141464968e+00, 2.938163982698783e+00)
+_PD = (7.784695709041462e-03, 3.224671290700398e-01, 2.445134137142996e+00,
+       3.754408661907416e+00)
+
+
+def probit(p):
+    """Acklam's rational approximation of the inverse normal CDF (published coefficients)."""
+    p = np.asarray(p, dtype=np.float64)
+    out = np.zeros_like(p)
+    lo = (p > 0) & (p < 0.02425)
+    hi = (p > 0.97575) & (p < 1)
+    mid = (p >= 0.02425) & (p <= 0.97575)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        q = np.sqrt(-2 * np.log(np.where(lo, p, 0.5)))
+        vlo = ((((((_PC[0] * q + _PC[1]) * q + _PC[2]) * q + _PC[3]) * q + _PC[4]) * q + _PC[5]) /
+               ((((_PD[0] * q + _PD[1]) * q + _PD[2]) * q + _PD[3]) * q + 1))
+        q = np.sqrt(-2 * np.log(1 - np.where(hi, p, 0.5)))
+        vhi = -((((((_PC[0] * q + _PC[1]) * q + _PC[2]) * q + _PC[3]) * q + _PC[4]) * q + _PC[5]) /
+                ((((_PD[0] * q + _PD[1]) * q + _PD[2]) * q + _PD[3]) * q + 1))
+        q = p - 0.5
+        r = q * q
+        vmid = ((((((_PA[0] * r + _PA[1]) * r + _PA[2]) * r + _PA[3]) * r + _PA[4]) * r + _PA[5]) * q /
+                (((((_PB[0] * r + _PB[1]) * r + _PB[2]) * r + _PB[3]) * r + _PB[4]) * r + 1))
+    out = np.where(lo, vlo, out)
+    out = np.where(hi, vhi, out)
+    out = np.where(mid, vmid, out)
+    out = np.where(p == 0, -np.inf, out)
+    out = np.where(p == 1, np.inf, out)
+    return out
+
+
+def _clamp_c(z, bound):
+    a = np.abs(z)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        return np.where(a > bound, z / a * bound, z)
+
+
+def assemble_X(vb, vmf, u, vbias_bound=50.0, free_projection=False):
+    """construct_X_impl for continuous charge fields; returns (X, HW).
+
+    HW is accumulated sequentially over m, as the host loop does
+    (AFQMCBasePropagator.cpp:726-731).
+    """
+    vmf_t = _clamp_c(np.asarray(vmf, np.complex128), vbias_bound)[None, :]
+    vb_t = _clamp_c(np.asarray(vb, np.complex128), vbias_bound)
+    if free_projection:
+        vdiff = np.zeros_like(vb_t)
+    else:
+        vdiff = 1j * (vb_t - vmf_t)
+    X = probit(u) + vdiff
+    terms = -vdiff * (X - 0.5 * vdiff)
+    HW = np.zeros(X.shape[0], dtype=np.complex128)
+    for m in range(X.shape[1]):
+        HW += terms[:, m]
+    return X, HW
+
+
+def meanfield_factor(X, vmf):
+    """AFQMCBasePropagator.cpp:335-336: -1/2 Re(vMF.vMF) + i X.vMF."""
+    vmf = np.asarray(vmf, np.complex128)
+    return -0.5 * np.dot(vmf, vmf).real + 1j * (X @ vmf)
+
+
+# --------------------------------------------------------------------------------------------
+# Propagation (propagate.hpp:45-70,247-298)
+# --------------------------------------------------------------------------------------------
+def apply_expM(V, S, order=6):
+    S = S.copy()
+    T1 = S.copy()
+    for n in range(1, order + 1):
+        T2 = (1j / n) * (V @ T1)
+        S += T2
+        T1 = T2
+    return S
+
+
+def propagate(Wk, P1, V, order=6):
+    TMN = P1[None, :, :] @ Wk
+    TMN = apply_expM(V, TMN, order)
+    return P1[None, :, :] @ TMN
+
+
+# --------------------------------------------------------------------------------------------
+# Walker update and weight bound (WalkerSetUpdate.hpp:46-218)
+# --------------------------------------------------------------------------------------------
+class Walkers:
+    """SoA view of WalkerSetBase for CLOSED walkers (WalkerSetBase.cpp:44-124)."""
+
+    def __init__(self, SM, weight=None):
+        self.SM = np.array(SM, dtype=np.complex128)        # (W, M, N)
+        W = self.SM.shape[0]
+        self.weight = np.ones(W, np.complex128) if weight is None else np.array(weight, np.complex128)
+        self.phase = np.ones(W, np.complex128)
+        self.pseudo_eloc = np.zeros(W, np.complex128)
+        self.e1 = np.zeros(W, np.complex128)
+        self.exx = np.zeros(W, np.complex128)
+        self.ej = np.zeros(W, np.complex128)
+        self.ovlp = np.zeros(W, np.complex128)
+        self.theta = np.zeros(W, np.complex128)
+
+    FIELDS = ('SM', 'weight', 'phase', 'pseudo_eloc', 'e1', 'exx', 'ej', 'ovlp', 'theta')
+
+    def size(self):
+        return self.SM.shape[0]
+
+    def copy(self):
+        c = Walkers(self.SM)
+        for f in self.FIELDS:
+            setattr(c, f, getattr(self, f).copy())
+        return c
+
+    def copy_walker(self, src, dst):
+        for f in self.FIELDS:
+            getattr(self, f)[dst] = getattr(self, f)[src]
+
+
+def walker_update(wset, dt, Eshift, energy_offset, new_ovlp, mf, hw,
+                  lower_cutoff_scale=1.0, upper_cutoff_scale=10.0,
+                  hybrid=True, free_projection=False, use_cp_constraint=False,
+                  new_energies=None):
+    nw = wset.size()
+    hi = Eshift + upper_cutoff_scale * math.sqrt(2.0 / dt)
+    lo = Eshift - lower_cutoff_scale * math.sqrt(2.0 / dt)
+    for i in range(nw):
+        old_ovlp = complex(wset.ovlp[i])
+        old_eloc = complex(wset.pseudo_eloc[i])
+        scale = 1.0
+        dtheta = 0.0
+        if not free_projection:
+            dtheta = new_ovlp[i].imag - old_ovlp.imag - mf[i].imag
+            if use_cp_constraint:
+                scale = 1.0 if math.cos(dtheta) > 0.0 else 0.0
+            else:
+                scale = max(0.0, math.cos(dtheta))
+        wset.theta[i] = dtheta
+        if hybrid:
+            eloc = (mf[i] - hw[i] - (new_ovlp[i] - old_ovlp)) / dt + energy_offset
+        else:
+            eloc = new_energies[i, 0] + new_energies[i, 1] + new_energies[i, 2]
+        eloc = complex(eloc)
+        if not math.isfinite(eloc.real):
+            wset.weight[i] = 0.0
+            wset.phase[i] = 0.0
+            eloc = old_eloc
+        else:
+            if not free_projection:
+                eloc = complex(min(max(eloc.real, lo), hi), eloc.imag)
+            eloc_eff = eloc if hybrid else 0.5 * (eloc + old_eloc)
+            w = np.exp(-dt * (eloc_eff - Eshift))
+            wset.weight[i] *= (scale * w) if free_projection else (scale * abs(w))
+            wset.phase[i] *= w / abs(w)
+        wset.pseudo_eloc[i] = eloc
+        wset.ovlp[i] = new_ovlp[i]
+    if not hybrid:
+        wset.e1[:] = new_energies[:, 0]
+        wset.exx[:] = new_energies[:, 1]
+        wset.ej[:] = new_energies[:, 2]
+
+
+def bound_walker_weights(wset, target_population, floor=100.0, fraction=0.1):
+    max_w = max(floor, fraction * target_population)
+    for i in range(wset.size()):
+        a = abs(wset.weight[i])
+        if a > max_w:
+            wset.weight[i] *= max_w / a
+
+
+# --------------------------------------------------------------------------------------------
+# Orthogonalization (orthogonalize.hpp:135-169; determinants_impl.hpp:78-108)
+# --------------------------------------------------------------------------------------------
+def orthogonalize(Wk):
+    """Householder QR of each walker (zgeqrf + zungqr on the transposed layout), then Q's
+    columns scaled by sign(Re R_ii); returns (Q, log det R) with log det R accumulated the
+    way log_determinant_from_geqrf does."""
+    Wk = np.array(Wk, dtype=np.complex128)
+    nw, M, N = Wk.shape
+    ldet = np.zeros(nw, np.complex128)
+    for w in range(nw):
+        qr, tau, work, info = lapack.zgeqrf(Wk[w])
+        scl = np.where(qr.diagonal()[:N].real < 0, -1.0, 1.0)
+        for i in range(N):
+            ldet[w] += np.log(complex(scl[i] * qr[i, i]) + SMALL)
+        q, work, info = lapack.zungqr(qr[:, :N], tau)
+        Wk[w] = q * scl[None, :]
+    return Wk, ldet
+
+
+# --------------------------------------------------------------------------------------------
+# Population control (population_control.hpp:34-65,143-255), single rank
+# --------------------------------------------------------------------------------------------
+def comb(weights, r, num_target):
+    weights = np.asarray(weights, dtype=np.float64)
+    cum = np.empty_like(weights)
+    acc = 0.0
+    for i, w in enumerate(weights):       # std::partial_sum, sequential
+        acc = acc + w
+        cum[i] = acc
+    total = cum[-1]
+    if not total > 1e-6:
+        raise RuntimeError(f"The total walker weight collapsed to {total}.")
+    last = len(weights) - 1
+    while weights[last] <= 0.0:
+        last -= 1
+    off = np.zeros(len(weights), dtype=np.int64)
+    iw = 0
+    ic = 0
+    while ic < num_target:
+        c = (ic + r) * total / num_target
+        if c < cum[iw] or iw == last:
+            off[iw] += 1
+            ic += 1
+        else:
+            iw += 1
+    return off
+
+
+def copy_plan(offspring):
+    """The (src, dst) walker copies swap_walkers_async performs on a single rank."""
+    keep = list(int(k) for k in offspring)
+    free = [i for i, k in enumerate(keep) if k == 0]
+    plan = []
+    nxt = 0
+    for i, k in enumerate(keep):
+        for _ in range(1, k):
+            plan.append((i, free[nxt]))
+            nxt += 1
+    assert nxt == len(free)
+    return plan
+
+
+def population_control(wset, r):
+    weights = np.abs(wset.weight)
+    off = comb(weights, r, wset.size())
+    for src, dst in copy_plan(off):
+        wset.copy_walker(src, dst)
+    wset.weight = wset.weight / np.abs(wset.weight)
+    return off
+
+
+# --------------------------------------------------------------------------------------------
+# Propagator + driver (AFQMCBasePropagator.cpp:290-392,736-741; run_afqmc.cpp:69-113)
+# --------------------------------------------------------------------------------------------
+class Propagator:
+    def __init__(self, ham, dt, seed=0, taylor_order=6, vbias_bound=50.0,
+                 lower_cutoff_scale=1.0, upper_cutoff_scale=10.0,
+                 weight_bound_floor=100.0, weight_bound_fraction=0.1,
+                 subtractMF=True, denseP1=False):
+        self.ham = ham
+        self.dt = dt
+        self.seed = seed
+        self.order = taylor_order
+        self.vbias_bound = vbias_bound
+        self.lower = lower_cutoff_scale
+        self.upper = upper_cutoff_scale
+        self.wfloor = weight_bound_floor
+        self.wfrac = weight_bound_fraction
+        self.vmf = vMF(ham, dt) if subtractMF else np.zeros(ham.Nc, np.complex128)
+        self.P1 = build_P1(ham, self.vmf, dt, dense=denseP1)
+
+    def propagate(self, wset, Eshift, step, target_population=None, uniforms=None):
+        ham = self.ham
+        W = wset.size()
+        G, _ = mixed_density_matrix(ham.PsiT, wset.SM, compact=True)
+        vb = ham.vbias(G, self.dt)
+        if uniforms is None:
+            uniforms = philox.uniforms(self.seed, philox.STREAM_FIELDS, step, W, ham.Nc)
+        X, HW = assemble_X(vb, self.vmf, uniforms, self.vbias_bound)
+        mf = meanfield_factor(X, self.vmf)
+        V = ham.vHS(X, self.dt)
+        wset.SM = propagate(wset.SM, self.P1, V, self.order)
+        new_ov = log_overlap_closed(ham.PsiT, wset.SM)
+        walker_update(wset, self.dt, Eshift, ham.E0, new_ov, mf, HW, self.lower, self.upper)
+        tp = W if target_population is None else target_population
+        bound_walker_weights(wset, tp, self.wfloor, self.wfrac)
+        return dict(G=G, vbias=vb, X=X, HW=HW, mf=mf, vHS=V, new_ovlp=new_ov)
+
+    def orthogonalize(self, wset):
+        wset.SM, _ = orthogonalize(wset.SM)
+        wset.ovlp = log_overlap_closed(self.ham.PsiT, wset.SM)
+
+
+def wfn_energy(ham, wset):
+    """NOMSD::Energy(wset) (NOMSD.cpp:159-217 / :64-75): writes E1_, EXX_, EJ_, OVLP."""
+    G, ov = mixed_density_matrix(ham.PsiT, wset.SM, compact=True)
+    ov = 2.0 * ov
+    E = ham.energy(G)
+    wset.ovlp = ov
+    wset.e1, wset.exx, wset.ej = E[:, 0].copy(), E[:, 1].copy(), E[:, 2].copy()
+    return E, ov
+
+
+def average_pseudo_energy(wset, dt):
+    e = np.exp(dt * wset.pseudo_eloc)
+    avg = np.sum(wset.weight * e) / np.sum(wset.weight)
+    return math.log(avg.real) / dt
+
+
+def average_energy(wset):
+    return (np.sum(wset.weight * (wset.e1 + wset.exx + wset.ej)) / np.sum(wset.weight)).real
+
+
+def measure_energy(ham, wset):
+    """EnergyEstimator::measure: sum_w w E_w / sum_w w, plus the three components."""
+    E, ov = wfn_energy_noupdate(ham, wset)
+    wsum = np.sum(wset.weight)
+    avg = (wset.weight @ E) / wsum
+    return dict(Energy=complex(np.sum(avg)), OnebodyEnergy=complex(avg[0]),
+                ExchangeEnergy=complex(avg[1]), CoulombEnergy=complex(avg[2]),
+                TotalWeight=complex(wsum))
+
+
+def wfn_energy_noupdate(ham, wset):
+    G, ov = mixed_density_matrix(ham.PsiT, wset.SM, compact=True)
+    return ham.energy(G), 2.0 * ov
+
+
+def init_walkers(ham, wset):
+    """execute.cpp:172-184: Energy(wset), seedPseudoEnergy, Eshift = averageEnergy."""
+    wfn_energy(ham, wset)
+    wset.pseudo_eloc = wset.e1 + wset.exx + wset.ej
+    return average_energy(wset)
+
+
+def run(ham, wset, prop, steps, Eshift, ortho_interval=10, pop_interval=10,
+        equilibration_steps=100, measure_interval=10, relax=None, step0=0, record=None):
+    """run_afqmc (run_afqmc.cpp:69-113). Returns (Eshift, list of measurements)."""
+    if relax is None:
+        relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
+    meas = []
+    pop_calls = 0
+    for step in range(step0, step0 + steps):
+        prop.propagate(wset, Eshift, step)
+        if step % ortho_interval == 0:
+            prop.orthogonalize(wset)
+        if step % pop_interval == 0:
+            population_control(wset, philox.comb_uniform(prop.seed, step))
+            pop_calls += 1
+        if step >= equilibration_steps:
+            if step % measure_interval == 0:
+                meas.append((step, measure_energy(ham, wset)))
+        else:
+            Eshift += relax * (average_pseudo_energy(wset, prop.dt) - Eshift)
+        if record is not None:
+            record.append(dict(step=step, Eshift=Eshift, weight=wset.weight.copy(),
+                               ovlp=wset.ovlp.copy(), pseudo_eloc=wset.pseudo_eloc.copy()))
+    return Eshift, meas
