@@ -1,0 +1,233 @@
+/*
+ * SAFIRE-B200: C ABI for the AFQMC walker-propagation / local-energy path on one B200.
+ *
+ * The reference exposes this path as C++ templates (nda arrays parameterised by MEMORY_SPACE);
+ * every entry point below replaces one of those calls for MEMORY_SPACE = DEVICE_MEMORY,
+ * CLOSED walkers, a single-determinant trial and a dense real Cholesky Hamiltonian
+ * (Real3IndexFactorization).  Reference paths are relative to the SAFIRE source tree.
+ *
+ * Conventions
+ *  - complex numbers are interleaved (re, im) doubles, the layout of std::complex<double>;
+ *  - arrays are C-ordered (row-major) exactly as the reference stores them;
+ *  - "device" pointers are CUDA device addresses on the current device; `stream` is a
+ *    cudaStream_t (NULL = legacy default stream);
+ *  - functions return 0 (SFQ_OK) or an SFQ_ERR_* code and never throw; sfq_last_error()
+ *    returns a description of the last failure on the calling thread.
+ *  - workspace-taking functions need `ws_bytes >= sfq_workspace_size(...)` of device memory.
+ */
+#ifndef SAFIRE_B200_H
+#define SAFIRE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SFQ_OK 0
+#define SFQ_ERR_SHAPE 1           /* utils::check size mismatch (src/utilities/check.hpp:36-46) */
+#define SFQ_ERR_ARG 2             /* invalid argument / null pointer */
+#define SFQ_ERR_UNSUPPORTED 3     /* size or combination this build does not implement */
+#define SFQ_ERR_CUDA 4            /* CUDA runtime error (cuda_check, src/arch/cuda_init.cpp:60-70) */
+#define SFQ_ERR_OOM 5             /* device allocation failed */
+#define SFQ_ERR_WEIGHT_COLLAPSE 6 /* comb: total weight <= 1e-6 (population_control.hpp:39) */
+#define SFQ_ERR_NONFINITE 7       /* non-finite input where one is not allowed */
+#define SFQ_ERR_TIMEOUT 8         /* bounded device wait expired */
+#define SFQ_ERR_WORKSPACE 9       /* workspace smaller than sfq_workspace_size() */
+#define SFQ_ERR_INTERNAL 10       /* internal consistency check failed */
+#define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
+
+/* version of this ABI */
+int sfq_abi_version(void);
+const char* sfq_last_error(void);
+/* cudaMemcpyAsync + stream synchronize (kind: 1 H2D, 2 D2H, 3 D2D), for callers without a CUDA runtime */
+int sfq_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * det_ops (src/AFQMC/SlaterDeterminantOperations/)
+ * --------------------------------------------------------------------------------------- */
+enum sfq_op {
+  SFQ_OP_MIXED_DENSITY_MATRIX = 1,
+  SFQ_OP_LOG_OVERLAP = 2,
+  SFQ_OP_PROPAGATE = 3,
+  SFQ_OP_ORTHOGONALIZE = 4,
+  SFQ_OP_ENERGY = 5,
+  SFQ_OP_INVERSE_LOGDET = 6
+};
+/* device bytes of scratch the op needs for these sizes */
+size_t sfq_workspace_size(int op, int nwalk, int nmo, int nel, int nchol);
+
+/* det_ops::MixedDensityMatrix(A, B, C, ovlp, compact, herm=true)
+ *   density_matrix.hpp:544-601 (log_overlap_impl :120-156, getri_or_zero nda_functions.hpp:422-438)
+ * A: trial PsiT (nel x nmo), complex if a_complex else real;  B: walkers (nwalk, nmo, nel) complex;
+ * C: compact ? (nwalk, nel, nmo) : (nwalk, nmo, nmo) complex;  ovlp: (nwalk) complex, accumulated
+ * (log det folded to [-pi, pi]).  A singular overlap gives a zero inverse, as in the reference. */
+int sfq_mixed_density_matrix(const void* A, int a_complex, const void* B, void* C, void* ovlp, int nwalk, int nmo,
+                             int nel, int compact, void* ws, size_t ws_bytes, void* stream);
+
+/* det_ops::Log_Overlap(A, B, ovlp, herm=true)   density_matrix.hpp:437-447 (accumulates into ovlp) */
+int sfq_log_overlap(const void* A, int a_complex, const void* B, void* ovlp, int nwalk, int nmo, int nel, void* ws,
+                    size_t ws_bytes, void* stream);
+
+/* det_ops::detail::inverse_logdet(A, ovlp, TNN)   density_matrix.hpp:82-108
+ * A (nbatch, n, n) complex (read only), Ainv (nbatch, n, n) complex out, logdet (nbatch) accumulated */
+int sfq_inverse_logdet(const void* A, void* Ainv, void* logdet, int nbatch, int n, void* stream);
+
+/* det_ops::Propagate<DEVICE,'N'>(wset, P1, V, order) for CLOSED walkers   propagate.hpp:247-298,391-408
+ * SM (nwalk, nmo, nel) complex updated in place:  SM <- P1 * sum_k (i V)^k/k! * P1 * SM;
+ * P1 (nmo, nmo) complex if p1_complex else real;  V (nwalk, nmo, nmo) complex */
+int sfq_propagate(void* SM, const void* P1, int p1_complex, const void* V, int nwalk, int nmo, int nel, int order,
+                  void* ws, size_t ws_bytes, void* stream);
+
+/* det_ops::orthogonalize(A, log_detR)   orthogonalize.hpp:135-169
+ * SM (nwalk, nmo, nel) complex replaced by Q with a positive real R diagonal (CholeskyQR2);
+ * log_detR (nwalk) complex accumulated with sum_i log R_ii, may be NULL. */
+int sfq_orthogonalize(void* SM, void* log_detR, int nwalk, int nmo, int nel, void* ws, size_t ws_bytes,
+                      void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * HamiltonianOperations -> Real3IndexFactorization (src/AFQMC/HamiltonianOperations/)
+ * --------------------------------------------------------------------------------------- */
+
+/* vbias(G, v, dt)   Real3IndexFactorization.hpp:328-428 (ndet = 1, compact G)
+ * v[w,n] = a * sum_{a,k} G[w,a,k] Lnak[n,a,k];  a = sqrt(dt) * (closed ? 2 : 1)
+ * G (nwalk, nel*nmo) complex; Lnak (nchol, nel, nmo) complex if lnak_complex else real; v (nwalk, nchol) */
+int sfq_vbias(const void* G, const void* Lnak, int lnak_complex, void* v, int nwalk, int nel, int nmo, int nchol,
+              double dt, int closed, void* stream);
+
+/* vHS(X, dt)   Real3IndexFactorization.hpp:282-326
+ * vHS[w,i,k] = sqrt(dt) * sum_n Likn[i,k,n] X[w,n];  Likn (nmo, nmo, nchol) real; X (nwalk, nchol) complex;
+ * vHS (nwalk, nmo, nmo) complex */
+int sfq_vhs(const double* Likn, const void* X, void* vHS, int nwalk, int nmo, int nchol, double dt, void* stream);
+
+/* energy(E, G, idet=0, addH1, addEJ, addEXX)   Real3IndexFactorization.hpp:138-174, energy_impl :476-590
+ * E (nwalk, 3) complex out [E1, EXX, EJ]; G (nwalk, nel*nmo); haj (nel, nmo) complex; Lnak as in vbias;
+ * CLOSED scaling (scl = 2, EJ factor 2). */
+int sfq_energy(void* E, const void* G, const void* haj, const void* Lnak, int lnak_complex, double E0, int nwalk,
+               int nel, int nmo, int nchol, int addH1, int addEJ, int addEXX, void* ws, size_t ws_bytes,
+               void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * AFQMCBasePropagator pieces (src/AFQMC/Propagators/)
+ * --------------------------------------------------------------------------------------- */
+
+/* assemble_X + construct_X_impl + meanfield_factor   AFQMCBasePropagator.cpp:687-733,335-336;
+ * construct_X_kernel.hpp:34-87.  X (nwalk, nchol) complex: in = vbias, out = fields;
+ * vmf (nchol) real; hw, mf (nwalk) complex out.  uniforms (nwalk, nchol) doubles in (0,1) replace
+ * sampleUniformFields when not NULL; otherwise Philox(seed, step) is drawn in-kernel. */
+int sfq_assemble_x(void* X, const double* vmf, void* hw, void* mf, const double* uniforms, unsigned long long seed,
+                   unsigned long long step, int nwalk, int nchol, double vbias_bound, int free_projection,
+                   void* stream);
+
+/* comb(rng, weights, num_target)   population_control.hpp:34-65
+ * weights (nwalk) doubles (|w|), device;  offspring (nwalk) ints, device;  r: the comb's uniform.
+ * Returns SFQ_ERR_WEIGHT_COLLAPSE when the total weight is <= 1e-6. */
+int sfq_comb(const double* weights, double r, int nwalk, int* offspring, void* stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Resident engine: HamiltonianOperations + NOMSD trial + WalkerSet + AFQMCBasePropagator
+ * kept in device memory on one GPU (the drop-in for execute_simulation's objects).
+ * --------------------------------------------------------------------------------------- */
+typedef struct sfq_engine_s* sfq_engine_t;
+
+typedef struct {
+  int nmo, nel, nchol, nwalk;
+  double dt;
+  double E0;                     /* energy_offset() */
+  int taylor_order;              /* PropagatorParameters::taylor_n (6) */
+  double vbias_bound;            /* 50 */
+  double lower_cutoff_scale;     /* 1 */
+  double upper_cutoff_scale;     /* 10 */
+  double weight_bound_floor;     /* 100 */
+  double weight_bound_fraction;  /* 0.1 */
+  int subtractMF;                /* 1 */
+  int denseP1;                   /* 0: entries |P1| < 1e-8 dropped, as the CSR P1 does */
+  int free_projection;           /* 0 */
+  int target_population;         /* global target population (0 -> nwalk) */
+  unsigned long long seed;       /* Philox key for fields and comb */
+  int device;                    /* CUDA device ordinal */
+} sfq_engine_params_t;
+
+/* fill *p with the reference's defaults (parameters.hpp:103-131, parameter_defaults.cpp:274-285) */
+void sfq_engine_params_default(sfq_engine_params_t* p);
+
+/* RealDenseHamiltonian::getHamiltonianOperations (RealDenseHamiltonian.cpp:53-185) + NOMSD ctor +
+ * AFQMCBasePropagator ctor / generateP1 (AFQMCBasePropagator.cpp:43-214), from HOST arrays:
+ * hcore (nmo, nmo) real; Likn (nmo, nmo, nchol) real; PsiT (nel, nmo) complex.
+ * Walkers start as copies of the trial (PsiT^H) with unit weight. */
+int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
+                      const void* PsiT);
+int sfq_engine_destroy(sfq_engine_t e);
+int sfq_engine_synchronize(sfq_engine_t e);
+/* the stream the engine enqueues on (cudaStream_t) */
+void* sfq_engine_stream(sfq_engine_t e);
+
+/* walker set I/O (WalkerSetBase.h:320-481): SM (nwalk, nmo, nel) complex; props (8, nwalk) complex in the
+ * order WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, THETA.  Host pointers; NULL skips. */
+int sfq_engine_set_walkers(sfq_engine_t e, const void* SM, const void* props);
+int sfq_engine_get_walkers(sfq_engine_t e, void* SM, void* props);
+/* the reference's walker_buffer rows (nwalk, nmo*nel + 11): SM, WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_,
+ * EJ_, OVLP, LOGSCL_UP, LOGSCL_DN, IS_UNITARY, THETA (WalkerSetBase.cpp:44-124). Host pointer. */
+int sfq_engine_export_walker_buffer(sfq_engine_t e, void* rows);
+
+/* NOMSD::Energy(wset) (NOMSD.cpp:64-75,159-217): E1_/EXX_/EJ_/OVLP of every walker; with
+ * seed_pseudo != 0 also seedPseudoEnergy (execute.cpp:46-53).  E3 (nwalk, 3) host out, may be NULL. */
+int sfq_engine_energy(sfq_engine_t e, int seed_pseudo, void* E3);
+
+/* AFQMCBasePropagator::Propagate(wset, Eshift) (AFQMCBasePropagator.cpp:290-392), hybrid, one step;
+ * fields from Philox(seed, step) or, when uniforms_dev != NULL, from that (nwalk, nchol) device buffer. */
+int sfq_engine_propagate(sfq_engine_t e, double Eshift, unsigned long long step, const double* uniforms_dev);
+/* same step with HOST inputs and outputs: the field uniforms are copied in from uniforms_host (may be
+ * NULL -> Philox) and the (8, nwalk) properties are copied back into props_host (may be NULL). */
+int sfq_engine_propagate_host(sfq_engine_t e, double Eshift, unsigned long long step, const double* uniforms_host,
+                              void* props_host);
+/* AFQMCBasePropagator::Orthogonalize (AFQMCBasePropagator.cpp:736-741) */
+int sfq_engine_orthogonalize(sfq_engine_t e);
+/* population_control (population_control.hpp:219-255), single rank; the comb draws Philox(seed, call) */
+int sfq_engine_population_control(sfq_engine_t e, unsigned long long call);
+/* averagePseudoEnergy / averageEnergy / total weight (average_energy.hpp:33-76); host scalars out */
+int sfq_engine_averages(sfq_engine_t e, double* pseudo_energy, double* energy, double* total_weight);
+/* EnergyEstimator::measure (EnergyEstimator.h:51-100): out[0..9] = Energy(re,im), Onebody(re,im),
+ * Exchange(re,im), Coulomb(re,im), TotalWeight(re,im); walkers are not modified. */
+int sfq_engine_measure(sfq_engine_t e, double* out10);
+
+typedef struct {
+  int steps;
+  int walker_ortho_interval;        /* 10 */
+  int population_control_interval;  /* 10 */
+  int equilibration_steps;          /* 100 */
+  int measure_interval;             /* 10 */
+  double Eshift_relaxation_factor;  /* <= 0 -> 1 - exp(-10/equilibration_steps) */
+  unsigned long long step0;
+} sfq_run_params_t;
+/* run_afqmc's step loop (run_afqmc.cpp:69-113). *Eshift in/out.  Measurements (10 doubles each, see
+ * sfq_engine_measure) are written to meas (capacity max_meas); *nmeas receives the count. */
+int sfq_engine_run(sfq_engine_t e, const sfq_run_params_t* rp, double* Eshift, double* meas, int max_meas,
+                   int* nmeas);
+
+/* device addresses of the engine's resident arrays, for tests and zero-copy callers */
+typedef struct {
+  void* SM;           /* (nwalk, nmo, nel) complex */
+  void* props;        /* (8, nwalk) complex */
+  void* PsiT;         /* (nel, nmo) complex */
+  void* Lnak;         /* (nchol, nel, nmo), real if lnak_complex == 0 */
+  int lnak_complex;
+  void* Likn;         /* (nmo, nmo, nchol) real */
+  void* haj;          /* (nel, nmo) complex */
+  void* v0;           /* (nmo, nmo) real */
+  void* vmf;          /* (nchol) real */
+  void* P1;           /* (nmo, nmo) real */
+  void* G;            /* (nwalk, nel, nmo) complex, last mixed density matrix */
+  void* X;            /* (nwalk, nchol) complex, last fields */
+  void* vHS;          /* (nwalk, nmo, nmo) complex, last vHS */
+  void* hw;           /* (nwalk) complex */
+  void* mf;           /* (nwalk) complex */
+  void* new_ovlp;     /* (nwalk) complex */
+  unsigned long long bound_stats[5]; /* eloc total/upper/lower, weight total/upper */
+} sfq_engine_info_t;
+int sfq_engine_info(sfq_engine_t e, sfq_engine_info_t* info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SAFIRE_B200_H */

@@ -1,0 +1,154 @@
+// SAFIRE-B200 C++ interface: the reference's AFQMC class and function names, on top of the C ABI.
+//
+// Reference counterparts (SAFIRE source tree):
+//   sfqmc::afqmc::det_ops::{MixedDensityMatrix, Log_Overlap, Propagate, orthogonalize}
+//       src/AFQMC/SlaterDeterminantOperations/{density_matrix,propagate,orthogonalize}.hpp
+//   sfqmc::afqmc::HamiltonianOperations / Real3IndexFactorization
+//       src/AFQMC/HamiltonianOperations/HamiltonianOperations.h:34-103, Real3IndexFactorization.hpp
+//   sfqmc::afqmc::WalkerSet (WalkerSetBase.h:51-572), AFQMCBasePropagator (AFQMCBasePropagator.h:51-172)
+//
+// Arrays are device pointers in the reference's C layouts; errors become safire_b200::Error,
+// matching utils::check's throw-on-failure semantics (src/utilities/check.hpp:36-46).
+#pragma once
+
+#include <complex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "safire_b200.h"
+
+namespace safire_b200 {
+
+using ComplexType = std::complex<double>;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+inline void check(int rc) {
+  if (rc != SFQ_OK) throw Error(rc, sfq_last_error());
+}
+
+// walker_data columns kept by the engine (WalkerConfig.hpp:28-48 names)
+enum walker_data { WEIGHT = 0, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, THETA };
+
+namespace det_ops {
+
+// MixedDensityMatrix(A, B, C, ovlp, compact, herm = true)
+inline void MixedDensityMatrix(const ComplexType* A, const ComplexType* B, ComplexType* C, ComplexType* ovlp,
+                               int nwalk, int nmo, int nel, bool compact, void* ws, size_t ws_bytes,
+                               void* stream = nullptr) {
+  check(sfq_mixed_density_matrix(A, 1, B, C, ovlp, nwalk, nmo, nel, compact ? 1 : 0, ws, ws_bytes, stream));
+}
+inline void Log_Overlap(const ComplexType* A, const ComplexType* B, ComplexType* ovlp, int nwalk, int nmo, int nel,
+                        void* ws, size_t ws_bytes, void* stream = nullptr) {
+  check(sfq_log_overlap(A, 1, B, ovlp, nwalk, nmo, nel, ws, ws_bytes, stream));
+}
+// Propagate<DEVICE,'N'>(wset, P1, V, order) on the Slater matrices of CLOSED walkers
+inline void Propagate(ComplexType* SM, const ComplexType* P1, const ComplexType* V, int nwalk, int nmo, int nel,
+                      int order, void* ws, size_t ws_bytes, void* stream = nullptr) {
+  check(sfq_propagate(SM, P1, 1, V, nwalk, nmo, nel, order, ws, ws_bytes, stream));
+}
+inline void orthogonalize(ComplexType* SM, ComplexType* log_detR, int nwalk, int nmo, int nel, void* ws,
+                          size_t ws_bytes, void* stream = nullptr) {
+  check(sfq_orthogonalize(SM, log_detR, nwalk, nmo, nel, ws, ws_bytes, stream));
+}
+inline size_t workspace_size(int op, int nwalk, int nmo, int nel, int nchol = 0) {
+  return sfq_workspace_size(op, nwalk, nmo, nel, nchol);
+}
+
+}  // namespace det_ops
+
+// Real3IndexFactorization over caller-owned device tensors (CLOSED, ndet = 1)
+class HamiltonianOperations {
+ public:
+  HamiltonianOperations(int nmo, int nel, int nchol, const double* Likn, const void* Lnak, bool lnak_complex,
+                        const ComplexType* haj, double E0)
+      : nmo_(nmo), nel_(nel), nchol_(nchol), Likn_(Likn), Lnak_(Lnak), lnak_complex_(lnak_complex), haj_(haj),
+        E0_(E0) {}
+
+  int number_of_cholesky_vectors() const { return nchol_; }
+  double energy_offset() const { return E0_; }
+
+  // vbias(G, v, dt): v[W, nchol] = 2 sqrt(dt) G Lnak^T
+  void vbias(const ComplexType* G, ComplexType* v, int nwalk, double dt, void* stream = nullptr) const {
+    check(sfq_vbias(G, Lnak_, lnak_complex_ ? 1 : 0, v, nwalk, nel_, nmo_, nchol_, dt, 1, stream));
+  }
+  // vHS(X, dt): vHS[W, nmo, nmo] = sqrt(dt) sum_n L_n X_n
+  void vHS(const ComplexType* X, ComplexType* vHS, int nwalk, double dt, void* stream = nullptr) const {
+    check(sfq_vhs(Likn_, X, vHS, nwalk, nmo_, nchol_, dt, stream));
+  }
+  // energy(E, G, 0, addH1, addEJ, addEXX): E[W, 3] = (E1, EXX, EJ)
+  void energy(ComplexType* E, const ComplexType* G, int nwalk, void* ws, size_t ws_bytes, bool addH1 = true,
+              bool addEJ = true, bool addEXX = true, void* stream = nullptr) const {
+    check(sfq_energy(E, G, haj_, Lnak_, lnak_complex_ ? 1 : 0, E0_, nwalk, nel_, nmo_, nchol_, addH1, addEJ, addEXX,
+                     ws, ws_bytes, stream));
+  }
+
+ private:
+  int nmo_, nel_, nchol_;
+  const double* Likn_;
+  const void* Lnak_;
+  bool lnak_complex_;
+  const ComplexType* haj_;
+  double E0_;
+};
+
+// The resident system: HamOps + NOMSD trial + WalkerSet + AFQMCBasePropagator on one GPU.
+class Engine {
+ public:
+  Engine(const sfq_engine_params_t& p, const double* hcore, const double* Likn, const ComplexType* PsiT) {
+    check(sfq_engine_create(&h_, &p, hcore, Likn, PsiT));
+    p_ = p;
+  }
+  ~Engine() { sfq_engine_destroy(h_); }
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+  sfq_engine_t handle() const { return h_; }
+  const sfq_engine_params_t& params() const { return p_; }
+
+ private:
+  sfq_engine_t h_ = nullptr;
+  sfq_engine_params_t p_{};
+};
+
+// WalkerSet view of an engine (WalkerSetBase.h): size, properties, Slater matrices
+class WalkerSet {
+ public:
+  explicit WalkerSet(Engine& e) : e_(e) {}
+  int size() const { return e_.params().nwalk; }
+  std::vector<ComplexType> getProperty(walker_data id) const {
+    std::vector<ComplexType> props(size_t(8) * size());
+    check(sfq_engine_get_walkers(e_.handle(), nullptr, props.data()));
+    return std::vector<ComplexType>(props.begin() + size_t(id) * size(), props.begin() + size_t(id + 1) * size());
+  }
+  std::vector<ComplexType> SlaterMatrices() const {
+    const auto& p = e_.params();
+    std::vector<ComplexType> sm(size_t(p.nwalk) * p.nmo * p.nel);
+    check(sfq_engine_get_walkers(e_.handle(), sm.data(), nullptr));
+    return sm;
+  }
+  Engine& engine() { return e_; }
+
+ private:
+  Engine& e_;
+};
+
+// AFQMCBasePropagator: Propagate(wset, Eshift) / Orthogonalize(wset)
+class AFQMCBasePropagator {
+ public:
+  explicit AFQMCBasePropagator(Engine& e) : e_(e) {}
+  void Propagate(WalkerSet& wset, double Eshift) {
+    check(sfq_engine_propagate(wset.engine().handle(), Eshift, step_++, nullptr));
+  }
+  void Orthogonalize(WalkerSet& wset) { check(sfq_engine_orthogonalize(wset.engine().handle())); }
+  bool stores_local_energy() const { return false; }  // hybrid propagation
+
+ private:
+  Engine& e_;
+  unsigned long long step_ = 0;
+};
+
+}  // namespace safire_b200

@@ -1,0 +1,278 @@
+"""Python mirror of the reference's AFQMC interfaces, backed by the sm_100a library.
+
+* ``det_ops``-style functions (MixedDensityMatrix, Log_Overlap, Propagate, orthogonalize) and
+  ``Real3IndexFactorization`` operations (vbias, vHS, energy) take CUDA tensors (torch) in the
+  reference's layouts and call the C ABI on the current torch stream;
+* ``AfqmcEngine`` owns one resident system (HamOps + trial + WalkerSet + propagator) and exposes
+  Propagate / Orthogonalize / population control / Energy / the run_afqmc loop.
+
+torch is used only for device memory and streams; all arithmetic runs in the library.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import capi
+from .capi import check, lib, ptr
+
+try:
+    import torch
+except ImportError:  # pragma: no cover - torch is part of the image
+    torch = None
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ws(op, nwalk, nmo, nel, nchol=0):
+    n = lib().sfq_workspace_size(op, nwalk, nmo, nel, nchol)
+    return torch.empty(max(int(n), 1), dtype=torch.uint8, device="cuda")
+
+
+def _is_cplx(t):
+    return t.dtype == torch.complex128
+
+
+def _need(t, name, dtypes):
+    if not t.is_cuda or not t.is_contiguous() or t.dtype not in dtypes:
+        raise ValueError(f"{name}: expected a contiguous CUDA tensor of {dtypes}, got {t.dtype} {t.device}")
+
+
+C128 = (torch.complex128,) if torch else ()
+F64 = (torch.float64,) if torch else ()
+
+
+# ------------------------------------------------------------------------------------------
+# det_ops (density_matrix.hpp, propagate.hpp, orthogonalize.hpp)
+# ------------------------------------------------------------------------------------------
+def MixedDensityMatrix(A, B, compact=True, ovlp=None):
+    """det_ops::MixedDensityMatrix(A, B, C, ovlp, compact, herm=true); ovlp accumulates."""
+    _need(A, "A", C128 + F64)
+    _need(B, "B", C128)
+    W, M, N = B.shape
+    C = torch.empty((W, N, M) if compact else (W, M, M), dtype=torch.complex128, device="cuda")
+    ov = torch.zeros(W, dtype=torch.complex128, device="cuda") if ovlp is None else ovlp
+    ws = _ws(capi.OP_MIXED_DENSITY_MATRIX, W, M, N)
+    check(lib().sfq_mixed_density_matrix(ptr(A), int(_is_cplx(A)), ptr(B), ptr(C), ptr(ov), W, M, N,
+                                         int(compact), ptr(ws), ws.numel(), _stream()))
+    return C, ov
+
+
+def Log_Overlap(A, B, ovlp=None):
+    _need(A, "A", C128 + F64)
+    _need(B, "B", C128)
+    W, M, N = B.shape
+    ov = torch.zeros(W, dtype=torch.complex128, device="cuda") if ovlp is None else ovlp
+    ws = _ws(capi.OP_LOG_OVERLAP, W, M, N)
+    check(lib().sfq_log_overlap(ptr(A), int(_is_cplx(A)), ptr(B), ptr(ov), W, M, N, ptr(ws), ws.numel(),
+                                _stream()))
+    return ov
+
+
+def inverse_logdet(A, logdet=None):
+    _need(A, "A", C128)
+    nb, n, _ = A.shape
+    Ainv = torch.empty_like(A)
+    ld = torch.zeros(nb, dtype=torch.complex128, device="cuda") if logdet is None else logdet
+    check(lib().sfq_inverse_logdet(ptr(A), ptr(Ainv), ptr(ld), nb, n, _stream()))
+    return Ainv, ld
+
+
+def Propagate(SM, P1, V, order=6):
+    """det_ops::Propagate<'N'> on CLOSED walkers, in place."""
+    _need(SM, "SM", C128)
+    _need(P1, "P1", C128 + F64)
+    _need(V, "V", C128)
+    W, M, N = SM.shape
+    ws = _ws(capi.OP_PROPAGATE, W, M, N)
+    check(lib().sfq_propagate(ptr(SM), ptr(P1), int(_is_cplx(P1)), ptr(V), W, M, N, order, ptr(ws), ws.numel(),
+                              _stream()))
+    return SM
+
+
+def orthogonalize(SM):
+    _need(SM, "SM", C128)
+    W, M, N = SM.shape
+    ws = _ws(capi.OP_ORTHOGONALIZE, W, M, N)
+    check(lib().sfq_orthogonalize(ptr(SM), None, W, M, N, ptr(ws), ws.numel(), _stream()))
+    return SM
+
+
+# ------------------------------------------------------------------------------------------
+# Real3IndexFactorization (vbias, vHS, energy)
+# ------------------------------------------------------------------------------------------
+def vbias(G, Lnak, dt, closed=True):
+    _need(G, "G", C128)
+    _need(Lnak, "Lnak", C128 + F64)
+    W = G.shape[0]
+    Nc, N, M = Lnak.shape
+    v = torch.empty((W, Nc), dtype=torch.complex128, device="cuda")
+    check(lib().sfq_vbias(ptr(G), ptr(Lnak), int(_is_cplx(Lnak)), ptr(v), W, N, M, Nc, dt, int(closed), _stream()))
+    return v
+
+
+def vHS(Likn, X, dt):
+    _need(Likn, "Likn", F64)
+    _need(X, "X", C128)
+    M, _, Nc = Likn.shape
+    W = X.shape[0]
+    V = torch.empty((W, M, M), dtype=torch.complex128, device="cuda")
+    check(lib().sfq_vhs(ptr(Likn), ptr(X), ptr(V), W, M, Nc, dt, _stream()))
+    return V
+
+
+def energy(G, haj, Lnak, E0=0.0, addH1=True, addEJ=True, addEXX=True):
+    _need(G, "G", C128)
+    _need(haj, "haj", C128)
+    _need(Lnak, "Lnak", C128 + F64)
+    W = G.shape[0]
+    Nc, N, M = Lnak.shape
+    E = torch.empty((W, 3), dtype=torch.complex128, device="cuda")
+    ws = _ws(capi.OP_ENERGY, W, M, N, Nc)
+    check(lib().sfq_energy(ptr(E), ptr(G), ptr(haj), ptr(Lnak), int(_is_cplx(Lnak)), E0, W, N, M, Nc, int(addH1),
+                           int(addEJ), int(addEXX), ptr(ws), ws.numel(), _stream()))
+    return E
+
+
+def assemble_X(vb, vmf, uniforms=None, seed=0, step=0, vbias_bound=50.0, free_projection=False):
+    """X, HW, meanfield_factor from vbias; vb is overwritten with X."""
+    _need(vb, "vbias", C128)
+    _need(vmf, "vmf", F64)
+    W, Nc = vb.shape
+    hw = torch.empty(W, dtype=torch.complex128, device="cuda")
+    mf = torch.empty(W, dtype=torch.complex128, device="cuda")
+    if uniforms is not None:
+        _need(uniforms, "uniforms", F64)
+    check(lib().sfq_assemble_x(ptr(vb), ptr(vmf), ptr(hw), ptr(mf), ptr(uniforms), seed, step, W, Nc, vbias_bound,
+                               int(free_projection), _stream()))
+    return vb, hw, mf
+
+
+def comb(weights, r):
+    _need(weights, "weights", F64)
+    n = weights.shape[0]
+    off = torch.empty(n, dtype=torch.int32, device="cuda")
+    check(lib().sfq_comb(ptr(weights), float(r), n, ptr(off), _stream()))
+    return off
+
+
+# ------------------------------------------------------------------------------------------
+# Resident engine
+# ------------------------------------------------------------------------------------------
+class AfqmcEngine:
+    """One system resident on one GPU: the drop-in for the objects execute_simulation builds."""
+
+    def __init__(self, system, nwalk, dt=0.005, seed=0, device=0, **params):
+        self.M, self.N, self.Nc, self.W = system.M, system.N, system.Nc, nwalk
+        self.dt = dt
+        p = capi.default_params(nmo=system.M, nel=system.N, nchol=system.Nc, nwalk=nwalk, dt=dt,
+                                E0=float(system.E0), seed=seed, device=device)
+        for k, v in params.items():
+            setattr(p, k, v)
+        self.params = p
+        h = np.ascontiguousarray(system.hcore, dtype=np.float64)
+        L = np.ascontiguousarray(system.Likn, dtype=np.float64)
+        P = np.ascontiguousarray(system.PsiT, dtype=np.complex128)
+        handle = ctypes.c_void_p()
+        check(lib().sfq_engine_create(ctypes.byref(handle), ctypes.byref(p), h.ctypes.data, L.ctypes.data,
+                                      P.ctypes.data))
+        self.h = handle
+
+    def close(self):
+        if self.h:
+            lib().sfq_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return lib().sfq_engine_stream(self.h)
+
+    def synchronize(self):
+        check(lib().sfq_engine_synchronize(self.h))
+
+    # WalkerSet
+    def walkers(self):
+        SM = np.empty((self.W, self.M, self.N), np.complex128)
+        pr = np.empty((len(capi.PROPS), self.W), np.complex128)
+        check(lib().sfq_engine_get_walkers(self.h, SM.ctypes.data, pr.ctypes.data))
+        return SM, {k: pr[i].copy() for i, k in enumerate(capi.PROPS)}
+
+    def set_walkers(self, SM=None, props=None):
+        sm = None if SM is None else np.ascontiguousarray(SM, np.complex128)
+        pr = None
+        if props is not None:
+            pr = np.stack([np.asarray(props[k], np.complex128) for k in capi.PROPS])
+        check(lib().sfq_engine_set_walkers(self.h, None if sm is None else sm.ctypes.data,
+                                           None if pr is None else pr.ctypes.data))
+
+    def walker_buffer(self):
+        rows = np.empty((self.W, self.M * self.N + 11), np.complex128)
+        check(lib().sfq_engine_export_walker_buffer(self.h, rows.ctypes.data))
+        return rows
+
+    # Wavefunction / Propagator
+    def energy(self, seed_pseudo=False):
+        E = np.empty((self.W, 3), np.complex128)
+        check(lib().sfq_engine_energy(self.h, int(seed_pseudo), E.ctypes.data))
+        return E
+
+    def init(self):
+        """execute.cpp:172-184: Energy, seedPseudoEnergy, Eshift = averageEnergy."""
+        self.energy(seed_pseudo=True)
+        return self.averages()[1]
+
+    def propagate(self, Eshift, step, uniforms=None):
+        check(lib().sfq_engine_propagate(self.h, float(Eshift), int(step), None if uniforms is None else
+                                         ctypes.c_void_p(ptr(uniforms))))
+
+    def propagate_host(self, Eshift, step, uniforms_host=None, props_out=None):
+        check(lib().sfq_engine_propagate_host(self.h, float(Eshift), int(step),
+                                              None if uniforms_host is None else ctypes.c_void_p(ptr(uniforms_host)),
+                                              None if props_out is None else ctypes.c_void_p(ptr(props_out))))
+
+    def orthogonalize(self):
+        check(lib().sfq_engine_orthogonalize(self.h))
+
+    def population_control(self, call):
+        check(lib().sfq_engine_population_control(self.h, int(call)))
+
+    def averages(self):
+        pe, e, tw = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(lib().sfq_engine_averages(self.h, ctypes.byref(pe), ctypes.byref(e), ctypes.byref(tw)))
+        return pe.value, e.value, tw.value
+
+    def measure(self):
+        o = np.empty(10, np.float64)
+        check(lib().sfq_engine_measure(self.h, o.ctypes.data))
+        keys = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "TotalWeight")
+        return {k: complex(o[2 * i], o[2 * i + 1]) for i, k in enumerate(keys)}
+
+    def run(self, steps, Eshift, ortho_interval=10, pop_interval=10, equilibration_steps=100, measure_interval=10,
+            relax=0.0, step0=0, max_meas=4096):
+        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0)
+        es = ctypes.c_double(Eshift)
+        meas = np.zeros((max_meas, 10), np.float64)
+        nm = ctypes.c_int()
+        check(lib().sfq_engine_run(self.h, ctypes.byref(rp), ctypes.byref(es), meas.ctypes.data, max_meas,
+                                   ctypes.byref(nm)))
+        return es.value, meas[:nm.value]
+
+    def info(self):
+        inf = capi.EngineInfo()
+        check(lib().sfq_engine_info(self.h, ctypes.byref(inf)))
+        return inf
+
+    def fetch(self, name, shape, dtype):
+        """Copy one of the engine's resident device arrays (by EngineInfo field) to the host."""
+        inf = self.info()
+        out = np.empty(shape, dtype)
+        check(lib().sfq_memcpy(out.ctypes.data, getattr(inf, name), out.nbytes, 2, None))
+        return out

@@ -1,0 +1,132 @@
+"""ctypes binding of the C ABI declared in include/safire_b200.h.
+
+Loading fails loudly when the sm_100a library has not been built: there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libsafire_b200.so")
+
+SFQ_OK = 0
+ERRORS = {1: "SHAPE", 2: "ARG", 3: "UNSUPPORTED", 4: "CUDA", 5: "OOM", 6: "WEIGHT_COLLAPSE", 7: "NONFINITE",
+          8: "TIMEOUT", 9: "WORKSPACE", 10: "INTERNAL", 11: "RANK"}
+OP_MIXED_DENSITY_MATRIX, OP_LOG_OVERLAP, OP_PROPAGATE, OP_ORTHOGONALIZE, OP_ENERGY, OP_INVERSE_LOGDET = 1, 2, 3, 4, 5, 6
+
+# walker property columns, in the order the engine stores them (WalkerConfig.hpp:28-48 names)
+PROPS = ("WEIGHT", "PHASE", "PSEUDO_ELOC_", "E1_", "EXX_", "EJ_", "OVLP", "THETA")
+
+
+class SafireError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"SFQ_ERR_{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class EngineParams(ctypes.Structure):
+    _fields_ = [("nmo", ctypes.c_int), ("nel", ctypes.c_int), ("nchol", ctypes.c_int), ("nwalk", ctypes.c_int),
+                ("dt", ctypes.c_double), ("E0", ctypes.c_double), ("taylor_order", ctypes.c_int),
+                ("vbias_bound", ctypes.c_double), ("lower_cutoff_scale", ctypes.c_double),
+                ("upper_cutoff_scale", ctypes.c_double), ("weight_bound_floor", ctypes.c_double),
+                ("weight_bound_fraction", ctypes.c_double), ("subtractMF", ctypes.c_int),
+                ("denseP1", ctypes.c_int), ("free_projection", ctypes.c_int),
+                ("target_population", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("device", ctypes.c_int)]
+
+
+class RunParams(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int), ("walker_ortho_interval", ctypes.c_int),
+                ("population_control_interval", ctypes.c_int), ("equilibration_steps", ctypes.c_int),
+                ("measure_interval", ctypes.c_int), ("Eshift_relaxation_factor", ctypes.c_double),
+                ("step0", ctypes.c_ulonglong)]
+
+
+class EngineInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("SM", "props", "PsiT", "Lnak")] + \
+               [("lnak_complex", ctypes.c_int)] + \
+               [(n, ctypes.c_void_p) for n in ("Likn", "haj", "v0", "vmf", "P1", "G", "X", "vHS", "hw", "mf",
+                                               "new_ovlp")] + \
+               [("bound_stats", ctypes.c_ulonglong * 5)]
+
+
+_lib = None
+
+_VP, _I, _D, _SZ, _U64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t, ctypes.c_ulonglong
+_SIGS = {
+    "sfq_abi_version": ([], _I),
+    "sfq_last_error": ([], ctypes.c_char_p),
+    "sfq_memcpy": ([_VP, _VP, _SZ, _I, _VP], _I),
+    "sfq_workspace_size": ([_I, _I, _I, _I, _I], _SZ),
+    "sfq_mixed_density_matrix": ([_VP, _I, _VP, _VP, _VP, _I, _I, _I, _I, _VP, _SZ, _VP], _I),
+    "sfq_log_overlap": ([_VP, _I, _VP, _VP, _I, _I, _I, _VP, _SZ, _VP], _I),
+    "sfq_inverse_logdet": ([_VP, _VP, _VP, _I, _I, _VP], _I),
+    "sfq_propagate": ([_VP, _VP, _I, _VP, _I, _I, _I, _I, _VP, _SZ, _VP], _I),
+    "sfq_orthogonalize": ([_VP, _VP, _I, _I, _I, _VP, _SZ, _VP], _I),
+    "sfq_vbias": ([_VP, _VP, _I, _VP, _I, _I, _I, _I, _D, _I, _VP], _I),
+    "sfq_vhs": ([_VP, _VP, _VP, _I, _I, _I, _D, _VP], _I),
+    "sfq_energy": ([_VP, _VP, _VP, _VP, _I, _D, _I, _I, _I, _I, _I, _I, _I, _VP, _SZ, _VP], _I),
+    "sfq_assemble_x": ([_VP, _VP, _VP, _VP, _VP, _U64, _U64, _I, _I, _D, _I, _VP], _I),
+    "sfq_comb": ([_VP, _D, _I, _VP, _VP], _I),
+    "sfq_engine_params_default": ([ctypes.POINTER(EngineParams)], None),
+    "sfq_engine_create": ([ctypes.POINTER(_VP), ctypes.POINTER(EngineParams), _VP, _VP, _VP], _I),
+    "sfq_engine_destroy": ([_VP], _I),
+    "sfq_engine_synchronize": ([_VP], _I),
+    "sfq_engine_stream": ([_VP], _VP),
+    "sfq_engine_set_walkers": ([_VP, _VP, _VP], _I),
+    "sfq_engine_get_walkers": ([_VP, _VP, _VP], _I),
+    "sfq_engine_export_walker_buffer": ([_VP, _VP], _I),
+    "sfq_engine_energy": ([_VP, _I, _VP], _I),
+    "sfq_engine_propagate": ([_VP, _D, _U64, _VP], _I),
+    "sfq_engine_propagate_host": ([_VP, _D, _U64, _VP, _VP], _I),
+    "sfq_engine_orthogonalize": ([_VP], _I),
+    "sfq_engine_population_control": ([_VP, _U64], _I),
+    "sfq_engine_averages": ([_VP, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)], _I),
+    "sfq_engine_measure": ([_VP, _VP], _I),
+    "sfq_engine_run": ([_VP, ctypes.POINTER(RunParams), ctypes.POINTER(_D), _VP, _I, ctypes.POINTER(_I)], _I),
+    "sfq_engine_info": ([_VP, ctypes.POINTER(EngineInfo)], _I),
+}
+
+
+def exported_symbols():
+    return sorted(_SIGS)
+
+
+def lib():
+    """The loaded library; raises if it was not built (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m safire_b200.build` "
+                               "(the AFQMC path has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != SFQ_OK:
+        raise SafireError(rc, lib().sfq_last_error().decode())
+    return rc
+
+
+def ptr(x):
+    """Device/host address of a torch tensor or numpy array (None -> NULL)."""
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    return x.data_ptr()
+
+
+def default_params(**kw):
+    p = EngineParams()
+    lib().sfq_engine_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p

@@ -1,0 +1,253 @@
+// Per-walker small dense factorizations, one CTA per N x N matrix held in shared memory.
+//
+//  * lu_logdet_kernel: partial-pivot LU (pivot = first max of |re|+|im|, LAPACK izamax
+//    semantics), log det = sum_i log(+-U_ii + tiny) folded to [-pi, pi]
+//    (src/numerics/operations/determinants_impl.hpp:33-75), and optionally the inverse computed
+//    the way zgetri does it (inv(U), then inv(A) L = inv(U), then column swaps), zeroed when
+//    any U_ii == 0 (getri_or_zero, src/numerics/nda_functions.hpp:422-438).
+//  * chol_rinv_kernel: S = R^H R (Cholesky, real positive diagonal) and R^-1, the small step
+//    of CholeskyQR2; Q = W R^-1 has the positive-real-diagonal R that the reference produces
+//    with geqrf + sign(Re R_ii) column scaling (orthogonalize.hpp:135-169).
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace sfq {
+
+namespace {
+
+constexpr int LU_THREADS = 256;
+
+__device__ __forceinline__ double cabs1(cplx a) { return fabs(a.x) + fabs(a.y); }
+
+template <bool INVERT>
+__global__ void __launch_bounds__(LU_THREADS) lu_logdet_kernel(cplx* T, long sT, int N, cplx* ovlp, int accumulate,
+                                                               double post_scale) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  cplx* A = reinterpret_cast<cplx*>(sm_raw);
+  cplx* work = A + N * N;
+  int* piv = reinterpret_cast<int*>(work + N);
+  __shared__ int s_p;
+  __shared__ int s_info;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tx = lane, ty = warp, NY = LU_THREADS / 32;
+  const long b = blockIdx.x;
+  cplx* Tb = T + b * sT;
+
+  for (int e = tid; e < N * N; e += LU_THREADS) A[e] = Tb[e];
+  if (tid == 0) s_info = 0;
+  __syncthreads();
+
+  for (int j = 0; j < N; ++j) {
+    if (warp == 0) {
+      double best = -1.0;
+      int bi = j;
+      for (int i = j + lane; i < N; i += 32) {
+        double v = cabs1(A[i * N + j]);
+        if (v > best) { best = v; bi = i; }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        double ob = __shfl_down_sync(0xffffffffu, best, off);
+        int oi = __shfl_down_sync(0xffffffffu, bi, off);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) {
+        piv[j] = bi;
+        s_p = bi;
+        cplx d = A[bi * N + j];
+        if (d.x == 0.0 && d.y == 0.0 && s_info == 0) s_info = j + 1;
+      }
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p != j) {
+      for (int k = tid; k < N; k += LU_THREADS) {
+        cplx t = A[j * N + k];
+        A[j * N + k] = A[p * N + k];
+        A[p * N + k] = t;
+      }
+      __syncthreads();
+    }
+    const cplx d = A[j * N + j];
+    if (d.x != 0.0 || d.y != 0.0) {
+      const cplx r = cdiv(mk(1.0, 0.0), d);
+      for (int i = j + 1 + tid; i < N; i += LU_THREADS) A[i * N + j] = cmul(A[i * N + j], r);
+    }
+    __syncthreads();
+    for (int i = j + 1 + ty; i < N; i += NY) {
+      const cplx l = A[i * N + j];
+      for (int k = j + 1 + tx; k < N; k += 32) A[i * N + k] = csub(A[i * N + k], cmul(l, A[j * N + k]));
+    }
+    __syncthreads();
+  }
+
+  if (tid == 0) {
+    cplx res = accumulate ? ovlp[b] : mk(0.0, 0.0);
+    const double tiny = 2.2250738585072014e-308;
+    for (int i = 0; i < N; ++i) {
+      cplx dgl = A[i * N + i];
+      cplx v = (piv[i] == i) ? dgl : mk(-dgl.x, -dgl.y);
+      v.x += tiny;
+      res = cadd(res, clog_(v));
+    }
+    const double pi = 3.141592653589793238462643383279502884;
+    // bring the imaginary part to [-pi, pi]; |Im| <= N*pi, so the loops are bounded by N
+    if (res.y > pi) {
+      for (int it = 0; res.y > pi && it < 4 * N + 8; ++it) res.y -= 2 * pi;
+    } else if (res.y < -pi) {
+      for (int it = 0; res.y < -pi && it < 4 * N + 8; ++it) res.y += 2 * pi;
+    }
+    ovlp[b] = mk(res.x * post_scale, res.y * post_scale);
+  }
+  if (!INVERT) return;
+
+  // singular (some U_ii == 0): getri reports info > 0 and the inverse is zeroed
+  bool singular = false;
+  for (int i = 0; i < N; ++i) {
+    cplx dgl = A[i * N + i];
+    if (dgl.x == 0.0 && dgl.y == 0.0) { singular = true; break; }
+  }
+  if (singular) {
+    for (int e = tid; e < N * N; e += LU_THREADS) Tb[e] = mk(0.0, 0.0);
+    return;
+  }
+  // inv(U) in place (ztrti2, upper, non-unit)
+  for (int j = 0; j < N; ++j) {
+    for (int i = tid; i < j; i += LU_THREADS) work[i] = A[i * N + j];
+    __syncthreads();
+    const cplx ujj = cdiv(mk(1.0, 0.0), A[j * N + j]);
+    const cplx ajj = mk(-ujj.x, -ujj.y);
+    for (int i = tid; i < j; i += LU_THREADS) {
+      cplx s = mk(0.0, 0.0);
+      for (int k = i; k < j; ++k) s = cadd(s, cmul(A[i * N + k], work[k]));
+      A[i * N + j] = cmul(ajj, s);
+    }
+    __syncthreads();
+    if (tid == 0) A[j * N + j] = ujj;
+    __syncthreads();
+  }
+  // solve inv(A) * L = inv(U) (zgetri, unblocked)
+  for (int j = N - 1; j >= 0; --j) {
+    for (int i = j + 1 + tid; i < N; i += LU_THREADS) {
+      work[i] = A[i * N + j];
+      A[i * N + j] = mk(0.0, 0.0);
+    }
+    __syncthreads();
+    if (j < N - 1) {
+      for (int i = tid; i < N; i += LU_THREADS) {
+        cplx s = mk(0.0, 0.0);
+        for (int k = j + 1; k < N; ++k) s = cadd(s, cmul(A[i * N + k], work[k]));
+        A[i * N + j] = csub(A[i * N + j], s);
+      }
+    }
+    __syncthreads();
+  }
+  // column interchanges in reverse order
+  for (int j = N - 2; j >= 0; --j) {
+    const int jp = piv[j];
+    if (jp != j) {
+      for (int i = tid; i < N; i += LU_THREADS) {
+        cplx t = A[i * N + j];
+        A[i * N + j] = A[i * N + jp];
+        A[i * N + jp] = t;
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < N * N; e += LU_THREADS) Tb[e] = A[e];
+}
+
+// Cholesky of the Hermitian positive definite S (N x N, upper storage used) into R (upper,
+// S = R^H R), then R^-1 (upper) written over S.  status[b] = 0, or j+1 when the pivot j is not
+// positive (the walker matrix lost rank).
+__global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS, int N, int* status) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  cplx* A = reinterpret_cast<cplx*>(sm_raw);
+  cplx* work = A + N * N;
+  __shared__ int s_bad;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long b = blockIdx.x;
+  cplx* Sb = S + b * sS;
+  for (int e = tid; e < N * N; e += LU_THREADS) A[e] = Sb[e];
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  // right-looking upper Cholesky: for j: r_jj = sqrt(a_jj); row j /= r_jj; trailing -= r_j^H r_j
+  for (int j = 0; j < N; ++j) {
+    const double ajj = A[j * N + j].x;
+    if (!(ajj > 0.0)) {
+      if (tid == 0 && s_bad == 0) s_bad = j + 1;
+      break;
+    }
+    const double rjj = sqrt(ajj);
+    const double inv = 1.0 / rjj;
+    __syncthreads();
+    for (int k = j + tid; k < N; k += LU_THREADS) {
+      A[j * N + k] = (k == j) ? mk(rjj, 0.0) : cscale(A[j * N + k], inv);
+    }
+    __syncthreads();
+    // A[i][k] -= conj(R[j][i]) * R[j][k] for j < i <= k
+    for (int i = j + 1 + warp; i < N; i += LU_THREADS / 32) {
+      const cplx ci = cconj(A[j * N + i]);
+      for (int k = i + lane; k < N; k += 32) A[i * N + k] = csub(A[i * N + k], cmul(ci, A[j * N + k]));
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (s_bad) {
+    if (tid == 0) status[b] = s_bad;
+    return;
+  }
+  // R^-1 in place (upper, non-unit), as in the LU inverse
+  for (int j = 0; j < N; ++j) {
+    for (int i = tid; i < j; i += LU_THREADS) work[i] = A[i * N + j];
+    __syncthreads();
+    const double ujj = 1.0 / A[j * N + j].x;
+    for (int i = tid; i < j; i += LU_THREADS) {
+      cplx s = mk(0.0, 0.0);
+      for (int k = i; k < j; ++k) s = cadd(s, cmul(A[i * N + k], work[k]));
+      A[i * N + j] = cscale(s, -ujj);
+    }
+    __syncthreads();
+    if (tid == 0) A[j * N + j] = mk(ujj, 0.0);
+    __syncthreads();
+  }
+  // zero the strictly lower part (the GEMM W R^-1 reads the full square)
+  for (int e = tid; e < N * N; e += LU_THREADS) {
+    int i = e / N, k = e % N;
+    Sb[e] = (i > k) ? mk(0.0, 0.0) : A[e];
+  }
+  if (tid == 0) status[b] = 0;
+}
+
+}  // namespace
+
+size_t lu_smem_bytes(int N) { return size_t(N) * N * sizeof(cplx) + size_t(N) * sizeof(cplx) + size_t(N) * sizeof(int) + 16; }
+
+int lu_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, double post_scale, bool invert,
+              cudaStream_t st) {
+  if (nbatch <= 0) return SFQ_OK;
+  if (N <= 0) return SFQ_OK;
+  if (N > kMaxSmallN) return record_error(SFQ_ERR_UNSUPPORTED, "lu_logdet: N=%d exceeds %d", N, kMaxSmallN);
+  const size_t sm = lu_smem_bytes(N);
+  if (invert) {
+    SFQ_CUDA_TRY(cudaFuncSetAttribute(lu_logdet_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    lu_logdet_kernel<true><<<nbatch, LU_THREADS, sm, st>>>(T, sT, N, ovlp, accumulate ? 1 : 0, post_scale);
+  } else {
+    SFQ_CUDA_TRY(cudaFuncSetAttribute(lu_logdet_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    lu_logdet_kernel<false><<<nbatch, LU_THREADS, sm, st>>>(T, sT, N, ovlp, accumulate ? 1 : 0, post_scale);
+  }
+  SFQ_CUDA_TRY(cudaGetLastError());
+  return SFQ_OK;
+}
+
+int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, cudaStream_t st) {
+  if (nbatch <= 0 || N <= 0) return SFQ_OK;
+  if (N > kMaxSmallN) return record_error(SFQ_ERR_UNSUPPORTED, "chol_rinv: N=%d exceeds %d", N, kMaxSmallN);
+  const size_t sm = lu_smem_bytes(N);
+  SFQ_CUDA_TRY(cudaFuncSetAttribute(chol_rinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+  chol_rinv_kernel<<<nbatch, LU_THREADS, sm, st>>>(S, sS, N, status);
+  SFQ_CUDA_TRY(cudaGetLastError());
+  return SFQ_OK;
+}
+
+}  // namespace sfq

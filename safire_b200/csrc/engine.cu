@@ -1,0 +1,650 @@
+// The resident AFQMC engine: one system's Hamiltonian tensors, trial, walker set, propagator
+// state and scratch, all in device memory on one GPU, driven on one CUDA stream.
+//
+// It plays the role of the objects execute_simulation builds (src/AFQMC/execute.cpp:107-206):
+// Real3IndexFactorization (HamOps), NOMSD with ndet = 1 (trial), WalkerSet and
+// AFQMCBasePropagator, for CLOSED walkers.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ops.cuh"
+
+struct sfq_engine_s;
+
+namespace sfq {
+
+namespace {
+
+constexpr int kNumProps = 8;  // WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, THETA
+enum { P_WEIGHT = 0, P_PHASE, P_PSEUDO, P_E1, P_EXX, P_EJ, P_OVLP, P_THETA };
+constexpr long kEnergyChunkElems = 1L << 27;
+
+// weighted sums for the averages: out[0..1] = sum w e^{dt eloc}, out[2..3] = sum w,
+// out[4..9] = sum w*E1, w*EXX, w*EJ (from E3 if given, else from the walker columns)
+__global__ void averages_kernel(const cplx* props, int nwalk, double dt, const cplx* E3, double* out) {
+  __shared__ double red[10][32];
+  double acc[10];
+  for (int i = 0; i < 10; ++i) acc[i] = 0.0;
+  const cplx* w = props + (long)P_WEIGHT * nwalk;
+  const cplx* el = props + (long)P_PSEUDO * nwalk;
+  for (int i = threadIdx.x; i < nwalk; i += blockDim.x) {
+    cplx wi = w[i];
+    cplx ex = cexp_(cscale(el[i], dt));
+    cplx a = cmul(wi, ex);
+    acc[0] += a.x; acc[1] += a.y;
+    acc[2] += wi.x; acc[3] += wi.y;
+    cplx e1, e2, e3;
+    if (E3) {
+      e1 = E3[3 * i]; e2 = E3[3 * i + 1]; e3 = E3[3 * i + 2];
+    } else {
+      e1 = props[(long)P_E1 * nwalk + i]; e2 = props[(long)P_EXX * nwalk + i]; e3 = props[(long)P_EJ * nwalk + i];
+    }
+    cplx b1 = cmul(wi, e1), b2 = cmul(wi, e2), b3 = cmul(wi, e3);
+    acc[4] += b1.x; acc[5] += b1.y; acc[6] += b2.x; acc[7] += b2.y; acc[8] += b3.x; acc[9] += b3.y;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < 10; ++k) {
+    double v = acc[k];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) red[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 10; ++k) {
+      double s = 0.0;
+      for (int i = 0; i < (int)(blockDim.x / 32); ++i) s += red[k][i];
+      out[k] = s;
+    }
+  }
+}
+
+__global__ void seed_pseudo_kernel(cplx* props, const cplx* E3, const cplx* ov, int nwalk, int update_props) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwalk) return;
+  if (update_props) {
+    props[(long)P_E1 * nwalk + i] = E3[3 * i];
+    props[(long)P_EXX * nwalk + i] = E3[3 * i + 1];
+    props[(long)P_EJ * nwalk + i] = E3[3 * i + 2];
+    props[(long)P_OVLP * nwalk + i] = ov[i];
+  }
+  if (update_props == 2) props[(long)P_PSEUDO * nwalk + i] = cadd(cadd(E3[3 * i], E3[3 * i + 1]), E3[3 * i + 2]);
+}
+
+size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+struct Engine {
+  sfq_engine_params_t p{};
+  int M = 0, N = 0, Nc = 0, W = 0;
+  bool trial_real = true;
+  cudaStream_t st = nullptr;
+  // arena
+  unsigned char* arena = nullptr;
+  size_t arena_bytes = 0;
+  // Hamiltonian / trial
+  double* hcore = nullptr;
+  double* Likn = nullptr;
+  cplx* PsiT = nullptr;
+  double* PsiTr = nullptr;
+  void* Lnak = nullptr;
+  cplx* haj = nullptr;
+  double* v0 = nullptr;
+  double* vmf = nullptr;
+  double* P1 = nullptr;
+  // walkers
+  cplx* SM = nullptr;
+  cplx* props = nullptr;
+  // scratch
+  cplx *SM2 = nullptr, *T = nullptr, *G = nullptr, *X = nullptr, *V = nullptr;
+  cplx *TMN = nullptr, *T1 = nullptr, *T2 = nullptr;
+  cplx *hw = nullptr, *mf = nullptr, *newov = nullptr, *E3 = nullptr, *ovtmp = nullptr;
+  cplx *Tchunk = nullptr, *exxn = nullptr, *kl = nullptr;
+  long tchunk_elems = 0;
+  int* status = nullptr;
+  double* red = nullptr;       // 16 doubles
+  double* uni = nullptr;       // (W, Nc) staging for injected uniforms
+  unsigned long long* stats = nullptr;  // 5 counters
+  PopWork pw{};
+  double* h_pinned = nullptr;  // pinned host staging for e2e calls
+  size_t h_pinned_bytes = 0;
+
+  WalkerProps wprops() const {
+    WalkerProps w;
+    w.weight = props + (long)P_WEIGHT * W;
+    w.phase = props + (long)P_PHASE * W;
+    w.pseudo_eloc = props + (long)P_PSEUDO * W;
+    w.e1 = props + (long)P_E1 * W;
+    w.exx = props + (long)P_EXX * W;
+    w.ej = props + (long)P_EJ * W;
+    w.ovlp = props + (long)P_OVLP * W;
+    w.theta = props + (long)P_THETA * W;
+    return w;
+  }
+  const void* lnak_ptr() const { return Lnak; }
+  double target_pop() const { return p.target_population > 0 ? p.target_population : W; }
+
+  int allocate() {
+    const size_t c = sizeof(cplx), d = sizeof(double);
+    const long MN = (long)M * N, NN = (long)N * N, MM = (long)M * M;
+    tchunk_elems = (long)W * N * ops::energy_chunk(W, N, Nc, kEnergyChunkElems) * N;
+    struct Item { void** ptr; size_t bytes; };
+    std::vector<Item> items = {
+        {(void**)&hcore, d * MM},
+        {(void**)&Likn, d * MM * Nc},
+        {(void**)&PsiT, c * N * M},
+        {(void**)&PsiTr, d * N * M},
+        {(void**)&Lnak, (trial_real ? d : c) * (size_t)Nc * N * M},
+        {(void**)&haj, c * N * M},
+        {(void**)&v0, d * MM},
+        {(void**)&vmf, d * Nc},
+        {(void**)&P1, d * MM},
+        {(void**)&SM, c * W * MN},
+        {(void**)&props, c * kNumProps * W},
+        {(void**)&SM2, c * W * MN},
+        {(void**)&T, c * W * NN},
+        {(void**)&G, c * W * MN},
+        {(void**)&X, c * (size_t)W * Nc},
+        {(void**)&V, c * W * MM},
+        {(void**)&TMN, c * W * MN},
+        {(void**)&T1, c * W * MN},
+        {(void**)&T2, c * W * MN},
+        {(void**)&hw, c * W},
+        {(void**)&mf, c * W},
+        {(void**)&newov, c * W},
+        {(void**)&E3, c * 3 * W},
+        {(void**)&ovtmp, c * W},
+        {(void**)&Tchunk, c * tchunk_elems},
+        {(void**)&exxn, c * (size_t)W * Nc},
+        {(void**)&kl, c * (size_t)W * Nc},
+        {(void**)&status, sizeof(int) * W},
+        {(void**)&red, d * 16},
+        {(void**)&uni, d * (size_t)W * Nc},
+        {(void**)&stats, sizeof(unsigned long long) * 8},
+        {(void**)&pw.offspring, sizeof(int) * W},
+        {(void**)&pw.pairs, sizeof(int) * 2 * W},
+        {(void**)&pw.npairs, sizeof(int) * 4},
+        {(void**)&pw.cum, d * W},
+        {(void**)&pw.flag, sizeof(int) * 4},
+    };
+    size_t total = 0;
+    for (auto& it : items) total += a256(it.bytes);
+    SFQ_CUDA_TRY(cudaMalloc(&arena, total));
+    arena_bytes = total;
+    size_t off = 0;
+    for (auto& it : items) {
+      *it.ptr = arena + off;
+      off += a256(it.bytes);
+    }
+    SFQ_CUDA_TRY(cudaMemsetAsync(arena, 0, total, st));
+    return SFQ_OK;
+  }
+
+  // --- setup: RealDenseHamiltonian::getHamiltonianOperations + NOMSD::vMF + generateP1 --------
+  int setup(const double* h_hcore, const double* h_Likn, const cplx* h_PsiT) {
+    int rc;
+    const long MM = (long)M * M;
+    SFQ_CUDA_TRY(cudaMemcpyAsync(hcore, h_hcore, sizeof(double) * MM, cudaMemcpyHostToDevice, st));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(Likn, h_Likn, sizeof(double) * MM * Nc, cudaMemcpyHostToDevice, st));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiT, h_PsiT, sizeof(cplx) * N * M, cudaMemcpyHostToDevice, st));
+    std::vector<double> pr(size_t(N) * M);
+    for (size_t i = 0; i < pr.size(); ++i) pr[i] = h_PsiT[i].x;
+    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiTr, pr.data(), sizeof(double) * N * M, cudaMemcpyHostToDevice, st));
+    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+
+    // Lnak[n][a][k] = sum_i PsiT[a][i] L[i][k][n]  via tmp[a][(k,n)] then a permute
+    {
+      void* tmp = nullptr;
+      const size_t esz = trial_real ? sizeof(double) : sizeof(cplx);
+      SFQ_CUDA_TRY(cudaMallocAsync(&tmp, esz * (size_t)N * M * Nc, st));
+      GemmDesc d;
+      d.M = N; d.N = int((long)M * Nc); d.K = M;
+      d.A = trial_real ? (const void*)PsiTr : (const void*)PsiT; d.sAm = M; d.sAk = 1; d.a_cplx = !trial_real;
+      d.B = Likn; d.sBk = (long)M * Nc; d.sBn = 1; d.b_cplx = false;
+      d.C = tmp; d.sCm = (long)M * Nc; d.sCn = 1;
+      if ((rc = gemm_f64(d, st))) return rc;
+      if ((rc = permute_lnak(tmp, Lnak, N, M, Nc, int(esz), st))) return rc;
+      SFQ_CUDA_TRY(cudaFreeAsync(tmp, st));
+    }
+    // haj = PsiT * hcore  (one_body.hpp:124-153)
+    {
+      GemmDesc d;
+      d.M = N; d.N = M; d.K = M;
+      d.A = PsiT; d.sAm = M; d.sAk = 1; d.a_cplx = true;
+      d.B = hcore; d.sBk = M; d.sBn = 1; d.b_cplx = false;
+      d.C = haj; d.sCm = M; d.sCn = 1;
+      if ((rc = gemm_f64(d, st))) return rc;
+    }
+    // v0 = -1/2 L L^T over (j, n)   (RealDenseHamiltonian.cpp:165-180)
+    {
+      GemmDesc d;
+      const long K = (long)M * Nc;
+      d.M = M; d.N = M; d.K = int(K);
+      d.A = Likn; d.sAm = K; d.sAk = 1;
+      d.B = Likn; d.sBk = 1; d.sBn = K;
+      d.C = v0; d.sCm = M; d.sCn = 1;
+      d.alpha = mk(-0.5, 0.0);
+      if ((rc = gemm_f64(d, st))) return rc;
+    }
+    // vMF = Re vbias(G_trial)  (NOMSD.cpp:437-466; AFQMCBasePropagator.cpp:107 zero_imag)
+    if (p.subtractMF) {
+      std::vector<cplx> psi(size_t(M) * N);  // PsiT^H  (M x N)
+      for (int a = 0; a < N; ++a)
+        for (int i = 0; i < M; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * M + i]);
+      SFQ_CUDA_TRY(cudaMemcpyAsync(SM2, psi.data(), sizeof(cplx) * M * N, cudaMemcpyHostToDevice, st));
+      if ((rc = ops::overlap_matrix(PsiT, true, SM2, T, 1, M, N, st))) return rc;
+      if ((rc = lu_logdet(T, (long)N * N, 1, N, ovtmp, false, 1.0, true, st))) return rc;
+      if ((rc = ops::green_compact(T, SM2, G, 1, M, N, st))) return rc;
+      if ((rc = ops::vbias(G, Lnak, !trial_real, X, 1, N, M, Nc, 2.0 * std::sqrt(p.dt), st))) return rc;
+      if ((rc = real_of(X, vmf, Nc, st))) return rc;
+      SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    } else {
+      SFQ_CUDA_TRY(cudaMemsetAsync(vmf, 0, sizeof(double) * Nc, st));
+    }
+    // H1 = -1/2 herm(dt h + dt v0 + vHS(vMF)); P1 = exp(H1)  (generateP1, one_body.hpp:65-85)
+    {
+      // X <- vMF as a complex row
+      std::vector<double> hv(Nc);
+      SFQ_CUDA_TRY(cudaMemcpyAsync(hv.data(), vmf, sizeof(double) * Nc, cudaMemcpyDeviceToHost, st));
+      SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+      std::vector<cplx> xv(Nc);
+      for (int n = 0; n < Nc; ++n) xv[n] = mk(hv[n], 0.0);
+      SFQ_CUDA_TRY(cudaMemcpyAsync(X, xv.data(), sizeof(cplx) * Nc, cudaMemcpyHostToDevice, st));
+      if ((rc = ops::vhs(Likn, X, V, 1, M, Nc, std::sqrt(p.dt), st))) return rc;
+      double* scr = nullptr;
+      SFQ_CUDA_TRY(cudaMallocAsync((void**)&scr, sizeof(double) * 5 * MM, st));
+      double* H = scr;
+      double* Pa = H + MM;
+      double* Pb = H + 2 * MM;
+      double* term_a = H + 3 * MM;
+      double* term_b = H + 4 * MM;
+      if ((rc = build_h1(hcore, v0, V, p.dt, H, M, st))) return rc;
+      std::vector<double> hh(MM);
+      SFQ_CUDA_TRY(cudaMemcpyAsync(hh.data(), H, sizeof(double) * MM, cudaMemcpyDeviceToHost, st));
+      SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+      double norm1 = 0.0;
+      for (int k = 0; k < M; ++k) {
+        double s = 0.0;
+        for (int i = 0; i < M; ++i) s += std::fabs(hh[size_t(i) * M + k]);
+        norm1 = std::fmax(norm1, s);
+      }
+      // scaling and squaring: exp(H) = exp(H / 2^s)^(2^s), ||H / 2^s||_1 <= 1/4, Taylor to order 18
+      int sq = 0;
+      while (norm1 / std::ldexp(1.0, sq) > 0.25) ++sq;
+      const double scale = std::ldexp(1.0, -sq);
+      SFQ_CUDA_TRY(cudaMemsetAsync(Pa, 0, sizeof(double) * MM, st));
+      SFQ_CUDA_TRY(cudaMemsetAsync(term_a, 0, sizeof(double) * MM, st));
+      if ((rc = add_identity(Pa, M, 1.0, st))) return rc;
+      if ((rc = add_identity(term_a, M, 1.0, st))) return rc;
+      for (int k = 1; k <= 18; ++k) {
+        GemmDesc d;  // term_b = (scale/k) H term_a; Pa += term_b
+        d.M = M; d.N = M; d.K = M;
+        d.A = H; d.sAm = M; d.sAk = 1;
+        d.B = term_a; d.sBk = M; d.sBn = 1;
+        d.C = term_b; d.sCm = M; d.sCn = 1;
+        d.S = Pa;
+        d.alpha = mk(scale / double(k), 0.0);
+        if ((rc = gemm_f64(d, st))) return rc;
+        std::swap(term_a, term_b);
+      }
+      double* cur = Pa;
+      double* nxt = Pb;
+      for (int s = 0; s < sq; ++s) {
+        GemmDesc d;
+        d.M = M; d.N = M; d.K = M;
+        d.A = cur; d.sAm = M; d.sAk = 1;
+        d.B = cur; d.sBk = M; d.sBn = 1;
+        d.C = nxt; d.sCm = M; d.sCn = 1;
+        if ((rc = gemm_f64(d, st))) return rc;
+        std::swap(cur, nxt);
+      }
+      SFQ_CUDA_TRY(cudaMemcpyAsync(P1, cur, sizeof(double) * MM, cudaMemcpyDeviceToDevice, st));
+      SFQ_CUDA_TRY(cudaFreeAsync(scr, st));
+      if (!p.denseP1) {
+        if ((rc = threshold_real(P1, MM, 1e-8, st))) return rc;
+      }
+    }
+    // walkers: copies of the trial, unit weight and phase
+    {
+      std::vector<cplx> psi(size_t(M) * N);
+      for (int a = 0; a < N; ++a)
+        for (int i = 0; i < M; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * M + i]);
+      for (int w = 0; w < W; ++w)
+        SFQ_CUDA_TRY(cudaMemcpyAsync(SM + (size_t)w * M * N, psi.data(), sizeof(cplx) * M * N,
+                                     cudaMemcpyHostToDevice, st));
+      SFQ_CUDA_TRY(cudaMemsetAsync(props, 0, sizeof(cplx) * kNumProps * W, st));
+      if ((rc = fill_cplx(props + (long)P_WEIGHT * W, W, mk(1.0, 0.0), st))) return rc;
+      if ((rc = fill_cplx(props + (long)P_PHASE * W, W, mk(1.0, 0.0), st))) return rc;
+    }
+    SFQ_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * 8, st));
+    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    return SFQ_OK;
+  }
+
+  // --- NOMSD::MixedDensityMatrix (compact, CLOSED: Ov x 2) into G, ov (W) -------------------
+  int density(cplx* ov) {
+    int rc;
+    const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
+    if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, M, N, st))) return rc;
+    if ((rc = lu_logdet(T, (long)N * N, W, N, ov, false, 2.0, true, st))) return rc;
+    return ops::green_compact(T, SM, G, W, M, N, st);
+  }
+
+  int log_overlap(cplx* ov) {
+    int rc;
+    const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
+    if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, M, N, st))) return rc;
+    return lu_logdet(T, (long)N * N, W, N, ov, false, 2.0, false, st);
+  }
+
+  // --- AFQMCBasePropagator::Propagate (hybrid) ----------------------------------------------
+  int propagate(double Eshift, unsigned long long step, const double* uniforms) {
+    int rc;
+    if ((rc = density(ovtmp))) return rc;                                            // 1. G
+    if ((rc = ops::vbias(G, Lnak, !trial_real, X, W, N, M, Nc, 2.0 * std::sqrt(p.dt), st))) return rc;
+    FieldParams fp;                                                                   // 2. X
+    fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
+    fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms;
+    if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
+    if ((rc = ops::vhs(Likn, X, V, W, M, Nc, std::sqrt(p.dt), st))) return rc;       // 3. vHS
+    if ((rc = ops::propagate(SM, P1, false, V, W, M, N, p.taylor_order, TMN, T1, T2, st))) return rc;  // 4.
+    if ((rc = log_overlap(newov))) return rc;                                         // 5.
+    UpdateParams up;                                                                  // 6.+7.
+    up.nwalk = W; up.dt = p.dt; up.Eshift = Eshift; up.E0 = p.E0;
+    up.lower_cutoff = p.lower_cutoff_scale; up.upper_cutoff = p.upper_cutoff_scale;
+    up.max_weight = std::fmax(p.weight_bound_floor, p.weight_bound_fraction * target_pop());
+    up.hybrid = 1; up.free_projection = p.free_projection; up.use_cp_constraint = 0;
+    return walker_update(wprops(), newov, mf, hw, E3, up, stats, st);
+  }
+
+  int orthogonalize() {
+    int rc;
+    if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, M, N, st))) return rc;
+    return log_overlap(props + (long)P_OVLP * W);  // wfn->Log_Overlap(wset)
+  }
+
+  int population_control(unsigned long long call) {
+    int rc;
+    if ((rc = sfq::population_control(SM, (long)M * N, wprops(), W, 0.0, p.seed, call, 1, pw, st))) return rc;
+    int flag = 0;
+    SFQ_CUDA_TRY(cudaMemcpyAsync(&flag, pw.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    if (flag == SFQ_ERR_WEIGHT_COLLAPSE) return record_error(flag, "The total walker weight collapsed.");
+    if (flag) return record_error(flag, "population control: inconsistent copy plan");
+    return SFQ_OK;
+  }
+
+  // NOMSD::Energy(wset, E, Ov): E3 and ovtmp
+  int energy_only() {
+    int rc;
+    if ((rc = density(ovtmp))) return rc;
+    return ops::energy(E3, G, haj, Lnak, !trial_real, p.E0, W, N, M, Nc, 1, 1, 1, Tchunk, tchunk_elems, exxn, kl,
+                       st);
+  }
+
+  int averages(const cplx* E, double* out10) {
+    averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, E, red);
+    SFQ_CUDA_TRY(cudaGetLastError());
+    SFQ_CUDA_TRY(cudaMemcpyAsync(out10, red, sizeof(double) * 10, cudaMemcpyDeviceToHost, st));
+    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    return SFQ_OK;
+  }
+};
+
+}  // namespace sfq
+
+struct sfq_engine_s {
+  sfq::Engine e;
+};
+
+using namespace sfq;
+
+extern "C" {
+
+void sfq_engine_params_default(sfq_engine_params_t* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->dt = 0.005;
+  p->taylor_order = 6;
+  p->vbias_bound = 50.0;
+  p->lower_cutoff_scale = 1.0;
+  p->upper_cutoff_scale = 10.0;
+  p->weight_bound_floor = 100.0;
+  p->weight_bound_fraction = 0.1;
+  p->subtractMF = 1;
+  p->denseP1 = 0;
+  p->free_projection = 0;
+}
+
+int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
+                      const void* PsiT) {
+  if (!out || !p || !hcore || !Likn || !PsiT) return record_error(SFQ_ERR_ARG, "null pointer");
+  *out = nullptr;
+  if (p->nmo <= 0 || p->nel <= 0 || p->nchol <= 0 || p->nwalk <= 0 || p->nel > p->nmo)
+    return record_error(SFQ_ERR_SHAPE, "engine: invalid sizes nmo=%d nel=%d nchol=%d nwalk=%d", p->nmo, p->nel,
+                        p->nchol, p->nwalk);
+  if (p->nel > kMaxSmallN) return record_error(SFQ_ERR_UNSUPPORTED, "engine: nel=%d exceeds %d", p->nel, kMaxSmallN);
+  if (!(p->dt > 0.0)) return record_error(SFQ_ERR_ARG, "engine: dt must be positive");
+  SFQ_CUDA_TRY(cudaSetDevice(p->device));
+  auto* h = new sfq_engine_s();
+  Engine& e = h->e;
+  e.p = *p;
+  e.M = p->nmo; e.N = p->nel; e.Nc = p->nchol; e.W = p->nwalk;
+  const cplx* ps = reinterpret_cast<const cplx*>(PsiT);
+  e.trial_real = true;
+  for (long i = 0; i < (long)e.N * e.M; ++i)
+    if (ps[i].y != 0.0) { e.trial_real = false; break; }
+  int rc;
+  cudaError_t ce = cudaStreamCreateWithFlags(&e.st, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) { delete h; return record_cuda(ce, "cudaStreamCreate", __FILE__, __LINE__); }
+  if ((rc = e.allocate()) || (rc = e.setup(hcore, Likn, ps))) {
+    sfq_engine_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return SFQ_OK;
+}
+
+int sfq_engine_destroy(sfq_engine_t h) {
+  if (!h) return SFQ_OK;
+  Engine& e = h->e;
+  if (e.st) cudaStreamSynchronize(e.st);
+  if (e.arena) cudaFree(e.arena);
+  if (e.h_pinned) cudaFreeHost(e.h_pinned);
+  if (e.st) cudaStreamDestroy(e.st);
+  delete h;
+  return SFQ_OK;
+}
+
+int sfq_engine_synchronize(sfq_engine_t h) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  SFQ_CUDA_TRY(cudaStreamSynchronize(h->e.st));
+  return SFQ_OK;
+}
+
+void* sfq_engine_stream(sfq_engine_t h) { return h ? (void*)h->e.st : nullptr; }
+
+int sfq_engine_set_walkers(sfq_engine_t h, const void* SM, const void* props) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  if (SM) SFQ_CUDA_TRY(cudaMemcpyAsync(e.SM, SM, sizeof(cplx) * e.W * e.M * e.N, cudaMemcpyHostToDevice, e.st));
+  if (props) SFQ_CUDA_TRY(cudaMemcpyAsync(e.props, props, sizeof(cplx) * kNumProps * e.W, cudaMemcpyHostToDevice, e.st));
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+int sfq_engine_get_walkers(sfq_engine_t h, void* SM, void* props) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  if (SM) SFQ_CUDA_TRY(cudaMemcpyAsync(SM, e.SM, sizeof(cplx) * e.W * e.M * e.N, cudaMemcpyDeviceToHost, e.st));
+  if (props) SFQ_CUDA_TRY(cudaMemcpyAsync(props, e.props, sizeof(cplx) * kNumProps * e.W, cudaMemcpyDeviceToHost, e.st));
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+int sfq_engine_export_walker_buffer(sfq_engine_t h, void* rows) {
+  if (!h || !rows) return record_error(SFQ_ERR_ARG, "null pointer");
+  Engine& e = h->e;
+  const long mn = (long)e.M * e.N, rl = mn + 11;
+  std::vector<cplx> sm(size_t(e.W) * mn), pr(size_t(kNumProps) * e.W);
+  int rc;
+  if ((rc = sfq_engine_get_walkers(h, sm.data(), pr.data()))) return rc;
+  cplx* out = reinterpret_cast<cplx*>(rows);
+  for (int w = 0; w < e.W; ++w) {
+    cplx* r = out + (size_t)w * rl;
+    std::memcpy(r, sm.data() + (size_t)w * mn, sizeof(cplx) * mn);
+    // WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, LOGSCL_UP, LOGSCL_DN, IS_UNITARY, THETA
+    for (int k = 0; k < 7; ++k) r[mn + k] = pr[(size_t)k * e.W + w];
+    r[mn + 7] = mk(0.0, 0.0);
+    r[mn + 8] = mk(0.0, 0.0);
+    r[mn + 9] = mk(0.0, 0.0);
+    r[mn + 10] = pr[(size_t)P_THETA * e.W + w];
+  }
+  return SFQ_OK;
+}
+
+int sfq_engine_energy(sfq_engine_t h, int seed_pseudo, void* E3host) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  int rc;
+  if ((rc = e.energy_only())) return rc;
+  seed_pseudo_kernel<<<(e.W + 127) / 128, 128, 0, e.st>>>(e.props, e.E3, e.ovtmp, e.W, seed_pseudo ? 2 : 1);
+  SFQ_CUDA_TRY(cudaGetLastError());
+  if (E3host) SFQ_CUDA_TRY(cudaMemcpyAsync(E3host, e.E3, sizeof(cplx) * 3 * e.W, cudaMemcpyDeviceToHost, e.st));
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+int sfq_engine_propagate(sfq_engine_t h, double Eshift, unsigned long long step, const double* uniforms_dev) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.propagate(Eshift, step, uniforms_dev);
+}
+
+int sfq_engine_propagate_host(sfq_engine_t h, double Eshift, unsigned long long step, const double* uniforms_host,
+                              void* props_host) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  int rc;
+  const double* ud = nullptr;
+  if (uniforms_host) {
+    SFQ_CUDA_TRY(cudaMemcpyAsync(e.uni, uniforms_host, sizeof(double) * e.W * e.Nc, cudaMemcpyHostToDevice, e.st));
+    ud = e.uni;
+  }
+  if ((rc = e.propagate(Eshift, step, ud))) return rc;
+  if (props_host)
+    SFQ_CUDA_TRY(cudaMemcpyAsync(props_host, e.props, sizeof(cplx) * kNumProps * e.W, cudaMemcpyDeviceToHost, e.st));
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+int sfq_engine_orthogonalize(sfq_engine_t h) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.orthogonalize();
+}
+
+int sfq_engine_population_control(sfq_engine_t h, unsigned long long call) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.population_control(call);
+}
+
+int sfq_engine_averages(sfq_engine_t h, double* pseudo_energy, double* energy, double* total_weight) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  double o[10];
+  int rc;
+  if ((rc = h->e.averages(nullptr, o))) return rc;
+  cplx num = mk(o[0], o[1]), den = mk(o[2], o[3]);
+  // log(Re(sum w e^{dt eloc} / sum w)) / dt
+  double re = (num.x * den.x + num.y * den.y) / (den.x * den.x + den.y * den.y);
+  if (pseudo_energy) *pseudo_energy = std::log(re) / h->e.p.dt;
+  if (energy) {
+    cplx s = mk(o[4] + o[6] + o[8], o[5] + o[7] + o[9]);
+    *energy = (s.x * den.x + s.y * den.y) / (den.x * den.x + den.y * den.y);
+  }
+  if (total_weight) *total_weight = den.x;
+  return SFQ_OK;
+}
+
+int sfq_engine_measure(sfq_engine_t h, double* out10) {
+  if (!h || !out10) return record_error(SFQ_ERR_ARG, "null pointer");
+  Engine& e = h->e;
+  int rc;
+  if ((rc = e.energy_only())) return rc;
+  double o[10];
+  if ((rc = e.averages(e.E3, o))) return rc;
+  // MeasurementOutput divides by sum_w (Measurements.hpp:101,120)
+  auto div = [](double ar, double ai, double br, double bi, double* r) {
+    double d = br * br + bi * bi;
+    r[0] = (ar * br + ai * bi) / d;
+    r[1] = (ai * br - ar * bi) / d;
+  };
+  double E1[2], EX[2], EJ[2];
+  div(o[4], o[5], o[2], o[3], E1);
+  div(o[6], o[7], o[2], o[3], EX);
+  div(o[8], o[9], o[2], o[3], EJ);
+  out10[0] = E1[0] + EX[0] + EJ[0];
+  out10[1] = E1[1] + EX[1] + EJ[1];
+  out10[2] = E1[0]; out10[3] = E1[1];
+  out10[4] = EX[0]; out10[5] = EX[1];
+  out10[6] = EJ[0]; out10[7] = EJ[1];
+  out10[8] = o[2]; out10[9] = o[3];
+  return SFQ_OK;
+}
+
+int sfq_engine_run(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, double* meas, int max_meas,
+                   int* nmeas) {
+  if (!h || !rp || !Eshift) return record_error(SFQ_ERR_ARG, "null pointer");
+  Engine& e = h->e;
+  int rc;
+  double relax = rp->Eshift_relaxation_factor;
+  if (!(relax > 0.0)) relax = rp->equilibration_steps > 1 ? 1.0 - std::exp(-10.0 / rp->equilibration_steps) : 1.0;
+  int nm = 0;
+  for (unsigned long long step = rp->step0; step < rp->step0 + (unsigned long long)rp->steps; ++step) {
+    if ((rc = e.propagate(*Eshift, step, nullptr))) return rc;
+    if (rp->walker_ortho_interval > 0 && step % rp->walker_ortho_interval == 0)
+      if ((rc = e.orthogonalize())) return rc;
+    if (rp->population_control_interval > 0 && step % rp->population_control_interval == 0)
+      if ((rc = e.population_control(step))) return rc;
+    if ((long long)step >= rp->equilibration_steps) {
+      if (rp->measure_interval > 0 && step % rp->measure_interval == 0) {
+        double o[10];
+        if ((rc = sfq_engine_measure(h, o))) return rc;
+        if (meas && nm < max_meas) std::memcpy(meas + 10 * nm, o, sizeof(o));
+        ++nm;
+      }
+    } else {
+      double pe;
+      if ((rc = sfq_engine_averages(h, &pe, nullptr, nullptr))) return rc;
+      *Eshift += relax * (pe - *Eshift);
+    }
+  }
+  if (nmeas) *nmeas = nm;
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+int sfq_engine_info(sfq_engine_t h, sfq_engine_info_t* info) {
+  if (!h || !info) return record_error(SFQ_ERR_ARG, "null pointer");
+  Engine& e = h->e;
+  info->SM = e.SM;
+  info->props = e.props;
+  info->PsiT = e.PsiT;
+  info->Lnak = e.Lnak;
+  info->lnak_complex = e.trial_real ? 0 : 1;
+  info->Likn = e.Likn;
+  info->haj = e.haj;
+  info->v0 = e.v0;
+  info->vmf = e.vmf;
+  info->P1 = e.P1;
+  info->G = e.G;
+  info->X = e.X;
+  info->vHS = e.V;
+  info->hw = e.hw;
+  info->mf = e.mf;
+  info->new_ovlp = e.newov;
+  SFQ_CUDA_TRY(cudaMemcpyAsync(info->bound_stats, e.stats, sizeof(unsigned long long) * 5, cudaMemcpyDeviceToHost, e.st));
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+// Host dispatch for the FP64 DMMA GEMM: picks the instantiation from operand kinds/contiguity
+// and the tile shape from the problem shape.
+#include "gemm_f64.cuh"
+
+namespace sfq {
+using namespace gemm_detail;
+
+namespace {
+
+template <bool AC, bool BC, bool CONJA, bool AK, bool BK, int BM, int BN, int WM, int WN, int STAGES>
+int launch(const GemmDesc& d, cudaStream_t st) {
+  using C_ = Cfg<AC, BC, CONJA, AK, BK, BM, BN, WM, WN, STAGES>;
+  auto k = gemm_f64_kernel<AC, BC, CONJA, AK, BK, BM, BN, WM, WN, STAGES>;
+  static bool attr_set = false;  // one opt-in per instantiation (per process, device-agnostic)
+  if (!attr_set) {
+    SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, C_::SMEM));
+    attr_set = true;
+  }
+  dim3 grid((d.N + BN - 1) / BN, (d.M + BM - 1) / BM, d.batch);
+  if (grid.y > 65535u || grid.z > 65535u)
+    return record_error(SFQ_ERR_SHAPE, "gemm_f64: grid (%u,%u,%u) too large", grid.x, grid.y, grid.z);
+  k<<<grid, C_::THREADS, C_::SMEM, st>>>(d);
+  SFQ_CUDA_TRY(cudaGetLastError());
+  return SFQ_OK;
+}
+
+template <bool AC, bool BC, bool CONJA, bool AK, bool BK>
+int pick_tile(const GemmDesc& d, cudaStream_t st) {
+  if constexpr (AC || BC) {
+    if (d.N <= 32) return launch<AC, BC, CONJA, AK, BK, 128, 32, 4, 1, 3>(d, st);
+    return launch<AC, BC, CONJA, AK, BK, 64, 64, 2, 2, 3>(d, st);
+  } else {
+    return launch<AC, BC, CONJA, AK, BK, 128, 64, 4, 2, 3>(d, st);
+  }
+}
+
+}  // namespace
+
+int gemm_f64(const GemmDesc& d, cudaStream_t st) {
+  if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return SFQ_OK;
+  if (d.K <= 0) {
+    if (d.beta.x != 0.0 || d.beta.y != 0.0)
+      return record_error(SFQ_ERR_SHAPE, "gemm_f64: K=0 with beta != 0 is not supported");
+  }
+  const bool AK = d.sAk == 1, BK = d.sBk == 1;
+  if (!AK && d.sAm != 1) return record_error(SFQ_ERR_SHAPE, "gemm_f64: A must be contiguous along K or M");
+  if (!BK && d.sBn != 1) return record_error(SFQ_ERR_SHAPE, "gemm_f64: B must be contiguous along K or N");
+  const bool AC = d.a_cplx, BC = d.b_cplx, CJ = d.conj_a && d.a_cplx;
+  // instantiations used by the AFQMC path
+  if (!AC && BC && !CJ && AK && !BK) return pick_tile<false, true, false, true, false>(d, st);
+  if (AC && BC && !CJ && AK && !BK) return pick_tile<true, true, false, true, false>(d, st);
+  if (AC && BC && !CJ && !AK && BK) return pick_tile<true, true, false, false, true>(d, st);
+  if (AC && !BC && !CJ && AK && BK) return pick_tile<true, false, false, true, true>(d, st);
+  if (AC && BC && !CJ && AK && BK) return pick_tile<true, true, false, true, true>(d, st);
+  if (AC && BC && CJ && !AK && !BK) return pick_tile<true, true, true, false, false>(d, st);
+  if (!AC && !BC && !CJ && AK && !BK) return pick_tile<false, false, false, true, false>(d, st);
+  if (AC && !BC && !CJ && AK && !BK) return pick_tile<true, false, false, true, false>(d, st);
+  if (!AC && !BC && !CJ && AK && BK) return pick_tile<false, false, false, true, true>(d, st);
+  if (AC && BC && !CJ && !AK && !BK) return pick_tile<true, true, false, false, false>(d, st);
+  if (!AC && BC && !CJ && !AK && !BK) return pick_tile<false, true, false, false, false>(d, st);
+  return record_error(SFQ_ERR_UNSUPPORTED, "gemm_f64: operand combination (ac=%d bc=%d conj=%d ak=%d bk=%d) not built",
+                      int(AC), int(BC), int(CJ), int(AK), int(BK));
+}
+
+}  // namespace sfq

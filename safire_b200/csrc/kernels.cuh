@@ -1,0 +1,76 @@
+// Internal kernel launchers shared by the C ABI and the resident engine.
+#pragma once
+#include "common.cuh"
+
+namespace sfq {
+
+constexpr int kMaxSmallN = 118;  // N x N complex + work (+ static) fits in 227 KB of shared memory
+
+size_t lu_smem_bytes(int N);
+// T: nbatch matrices N x N (row-major, batch stride sT); ovlp[b] = post_scale * fold(acc + logdet)
+int lu_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, double post_scale, bool invert,
+              cudaStream_t st);
+int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, cudaStream_t st);
+
+struct FieldParams {
+  int nwalk = 0, nchol = 0;
+  double vbias_bound = 50.0;
+  int free_projection = 0;
+  unsigned long long seed = 0, step = 0;
+  const double* uniforms = nullptr;  // optional injected (nwalk, nchol) buffer, else Philox
+};
+// X: in = vbias (nwalk, nchol) complex, out = fields; vmf (nchol) real; hw, mf (nwalk) complex
+int assemble_x(cplx* X, const double* vmf, cplx* hw, cplx* mf, const FieldParams& p, cudaStream_t st);
+
+struct UpdateParams {
+  int nwalk = 0;
+  double dt = 0.0, Eshift = 0.0, E0 = 0.0;
+  double lower_cutoff = 1.0, upper_cutoff = 10.0;
+  double max_weight = 100.0;  // max(floor, fraction * target population)
+  int hybrid = 1, free_projection = 0, use_cp_constraint = 0;
+};
+struct WalkerProps {  // columns of the walker set (SoA), each nwalk complex
+  cplx *weight, *phase, *pseudo_eloc, *e1, *exx, *ej, *ovlp, *theta;
+};
+// stats: 5 counters (eloc total, eloc upper, eloc lower, weight total, weight upper)
+int walker_update(const WalkerProps& w, const cplx* new_ovlp, const cplx* mf, const cplx* hw, const cplx* E3,
+                  const UpdateParams& p, unsigned long long* stats, cudaStream_t st);
+
+// population control: comb on |weight| with one Philox draw, then copy walkers into the
+// slots left free, in the order swap_walkers_async fills them; weights -> w/|w|.
+struct PopWork {
+  int* offspring;   // nwalk
+  int* pairs;       // 2 * nwalk (src, dst)
+  int* npairs;      // 1
+  double* cum;      // nwalk
+  int* flag;        // 1: 0 ok, SFQ_ERR_WEIGHT_COLLAPSE
+};
+int population_control(cplx* SM, long walker_elems, const WalkerProps& w, int nwalk, double r_uniform,
+                       unsigned long long seed, unsigned long long call, int use_philox, const PopWork& pw,
+                       cudaStream_t st);
+
+int comb_weights(const double* wts, int nwalk, double r, int* offspring, double* cum, int* flag, cudaStream_t st);
+
+// energy pieces
+int energy_e1(const cplx* G, const cplx* haj, cplx* E3, int nwalk, int nel, int nmo, double E0, double scl,
+              int addH1, cudaStream_t st);
+// T chunk (nwalk, nel, nv, nel): exxn[w, n0+n] = sum_ab T[a,n,b]T[b,n,a]; kl[w, n0+n] = sum_a T[a,n,a]
+int energy_exx_reduce(const cplx* T, int nwalk, int nel, int nv, int n0, int nchol, cplx* exxn, cplx* kl,
+                      cudaStream_t st);
+// E3[:,1] += -0.5*scl*sum_n exxn; E3[:,2] += (CLOSED ? 2 : 0.5) * sum_n kl^2
+int energy_finish(const cplx* exxn, const cplx* kl, cplx* E3, int nwalk, int nchol, double scl, int addEXX,
+                  int addEJ, cudaStream_t st);
+
+// misc
+// [a][k][n] -> [n][a][k], complex or real (elements of esz bytes: 8 or 16)
+int permute_lnak(const void* tmp, void* Lnak, int nel, int nmo, int nchol, int esz, cudaStream_t st);
+// H[i][k] = -0.5 * herm(dt*h + dt*v0 + Re vhs)  (real symmetric one-body matrix of P1)
+int build_h1(const double* h, const double* v0, const cplx* vhs, double dt, double* H, int nmo, cudaStream_t st);
+int add_identity(double* P, int nmo, double v, cudaStream_t st);
+int threshold_real(double* P, long n, double drop, cudaStream_t st);
+int real_of(const cplx* z, double* r, long n, cudaStream_t st);
+int fill_cplx(cplx* p, long n, cplx v, cudaStream_t st);
+int copy_walkers_prop(cplx* dst, const cplx* src, long n, cudaStream_t st);
+int scale_cplx(cplx* p, long n, cplx s, cudaStream_t st);
+
+}  // namespace sfq

@@ -1,0 +1,362 @@
+// Composite device operations and the det_ops / HamOps C entry points.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "ops.cuh"
+
+namespace sfq {
+
+// ---- error plumbing ------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+int record_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int record_cuda(cudaError_t e, const char* what, const char* file, int line) {
+  if (e == cudaErrorMemoryAllocation)
+    return record_error(SFQ_ERR_OOM, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  return record_error(SFQ_ERR_CUDA, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+}
+
+namespace ops {
+
+int overlap_matrix(const void* A, bool a_cplx, const cplx* B, cplx* T, int W, int M, int N, cudaStream_t st) {
+  GemmDesc d;
+  d.M = N; d.N = N; d.K = M; d.batch = W;
+  d.A = A; d.sAm = M; d.sAk = 1; d.sAb = 0; d.a_cplx = a_cplx;
+  d.B = B; d.sBk = N; d.sBn = 1; d.sBb = (long)M * N; d.b_cplx = true;
+  d.C = T; d.sCm = N; d.sCn = 1; d.sCb = (long)N * N;
+  return gemm_f64(d, st);
+}
+
+int green_compact(const cplx* Tinv, const cplx* B, cplx* G, int W, int M, int N, cudaStream_t st) {
+  GemmDesc d;
+  d.M = N; d.N = M; d.K = N; d.batch = W;
+  d.A = Tinv; d.sAm = 1; d.sAk = N; d.sAb = (long)N * N; d.a_cplx = true;
+  d.B = B; d.sBk = 1; d.sBn = N; d.sBb = (long)M * N; d.b_cplx = true;
+  d.C = G; d.sCm = M; d.sCn = 1; d.sCb = (long)N * M;
+  return gemm_f64(d, st);
+}
+
+int green_full(const void* A, bool a_cplx, const cplx* Gc, cplx* C, int W, int M, int N, cudaStream_t st) {
+  GemmDesc d;
+  d.M = M; d.N = M; d.K = N; d.batch = W;
+  d.A = A; d.sAm = 1; d.sAk = M; d.sAb = 0; d.a_cplx = a_cplx;
+  d.B = Gc; d.sBk = M; d.sBn = 1; d.sBb = (long)N * M; d.b_cplx = true;
+  d.C = C; d.sCm = M; d.sCn = 1; d.sCb = (long)M * M;
+  return gemm_f64(d, st);
+}
+
+int vbias(const cplx* G, const void* Lnak, bool l_cplx, cplx* v, int W, int N, int M, int Nc, double a,
+          cudaStream_t st) {
+  GemmDesc d;
+  const long K = (long)N * M;
+  d.M = W; d.N = Nc; d.K = int(K); d.batch = 1;
+  d.A = G; d.sAm = K; d.sAk = 1; d.a_cplx = true;
+  d.B = Lnak; d.sBk = 1; d.sBn = K; d.b_cplx = l_cplx;
+  d.C = v; d.sCm = Nc; d.sCn = 1;
+  d.alpha = mk(a, 0.0);
+  return gemm_f64(d, st);
+}
+
+int vhs(const double* Likn, const cplx* X, cplx* V, int W, int M, int Nc, double a, cudaStream_t st) {
+  GemmDesc d;
+  const long M2 = (long)M * M;
+  d.M = W; d.N = int(M2); d.K = Nc; d.batch = 1;
+  d.A = X; d.sAm = Nc; d.sAk = 1; d.a_cplx = true;
+  d.B = Likn; d.sBk = 1; d.sBn = Nc; d.b_cplx = false;
+  d.C = V; d.sCm = M2; d.sCn = 1;
+  d.alpha = mk(a, 0.0);
+  return gemm_f64(d, st);
+}
+
+static int p1_apply(const void* P1, bool p_cplx, const cplx* in, cplx* out, int W, int M, int N, cudaStream_t st) {
+  GemmDesc d;
+  d.M = M; d.N = N; d.K = M; d.batch = W;
+  d.A = P1; d.sAm = M; d.sAk = 1; d.sAb = 0; d.a_cplx = p_cplx;
+  d.B = in; d.sBk = N; d.sBn = 1; d.sBb = (long)M * N; d.b_cplx = true;
+  d.C = out; d.sCm = N; d.sCn = 1; d.sCb = (long)M * N;
+  return gemm_f64(d, st);
+}
+
+int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M, int N, int order, cplx* TMN,
+              cplx* T1, cplx* T2, cudaStream_t st) {
+  int rc;
+  const long n = (long)W * M * N;
+  // TMN = P1 * SM   (propagate.hpp:260)
+  if ((rc = p1_apply(P1, p_cplx, SM, TMN, W, M, N, st))) return rc;
+  // apply_expM (propagate.hpp:45-70): T1 = S; T2 = (i/n) V T1; S += T2; swap
+  SFQ_CUDA_TRY(cudaMemcpyAsync(T1, TMN, n * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+  cplx* a = T1;
+  cplx* b = T2;
+  for (int k = 1; k <= order; ++k) {
+    GemmDesc d;
+    d.M = M; d.N = N; d.K = M; d.batch = W;
+    d.A = V; d.sAm = M; d.sAk = 1; d.sAb = (long)M * M; d.a_cplx = true;
+    d.B = a; d.sBk = N; d.sBn = 1; d.sBb = (long)M * N; d.b_cplx = true;
+    d.C = b; d.sCm = N; d.sCn = 1; d.sCb = (long)M * N;
+    d.S = TMN;
+    d.alpha = mk(0.0, 1.0 / double(k));
+    if ((rc = gemm_f64(d, st))) return rc;
+    cplx* t = a; a = b; b = t;
+  }
+  // SM = P1 * TMN   (propagate.hpp:297)
+  return p1_apply(P1, p_cplx, TMN, SM, W, M, N, st);
+}
+
+int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int W, int M, int N, cudaStream_t st) {
+  int rc;
+  for (int pass = 0; pass < 2; ++pass) {
+    GemmDesc d;  // S = SM^H SM
+    d.M = N; d.N = N; d.K = M; d.batch = W;
+    d.A = SM; d.sAm = 1; d.sAk = N; d.sAb = (long)M * N; d.a_cplx = true; d.conj_a = true;
+    d.B = SM; d.sBk = N; d.sBn = 1; d.sBb = (long)M * N; d.b_cplx = true;
+    d.C = S; d.sCm = N; d.sCn = 1; d.sCb = (long)N * N;
+    if ((rc = gemm_f64(d, st))) return rc;
+    if ((rc = chol_rinv(S, (long)N * N, W, N, status, st))) return rc;
+    GemmDesc q;  // SM2 = SM R^-1
+    q.M = M; q.N = N; q.K = N; q.batch = W;
+    q.A = SM; q.sAm = N; q.sAk = 1; q.sAb = (long)M * N; q.a_cplx = true;
+    q.B = S; q.sBk = N; q.sBn = 1; q.sBb = (long)N * N; q.b_cplx = true;
+    q.C = SM2; q.sCm = N; q.sCn = 1; q.sCb = (long)M * N;
+    if ((rc = gemm_f64(q, st))) return rc;
+    SFQ_CUDA_TRY(cudaMemcpyAsync(SM, SM2, (long)W * M * N * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+  }
+  (void)log_detR;
+  return SFQ_OK;
+}
+
+int energy_chunk(int W, int N, int Nc, long max_elems) {
+  long per = (long)W * N * N;
+  long nv = per > 0 ? max_elems / per : Nc;
+  if (nv < 1) nv = 1;
+  if (nv > Nc) nv = Nc;
+  return int(nv);
+}
+
+int energy(cplx* E3, const cplx* G, const cplx* haj, const void* Lnak, bool l_cplx, double E0, int W, int N, int M,
+           int Nc, int addH1, int addEJ, int addEXX, cplx* Tchunk, long tchunk_elems, cplx* exxn, cplx* kl,
+           cudaStream_t st) {
+  int rc;
+  const double scl = 2.0;
+  if ((rc = energy_e1(G, haj, E3, W, N, M, E0, scl, addH1, st))) return rc;
+  if (!addEXX && !addEJ) return SFQ_OK;
+  const int nv_max = energy_chunk(W, N, Nc, tchunk_elems);
+  const size_t esz = l_cplx ? sizeof(cplx) : sizeof(double);
+  for (int n0 = 0; n0 < Nc; n0 += nv_max) {
+    const int nv = (Nc - n0) < nv_max ? (Nc - n0) : nv_max;
+    GemmDesc d;  // T[(w,b)][(n,a)] = sum_k G[w,b,k] Lnak[n0+n, a, k]
+    d.M = W * N; d.N = nv * N; d.K = M; d.batch = 1;
+    d.A = G; d.sAm = M; d.sAk = 1; d.a_cplx = true;
+    d.B = (const unsigned char*)Lnak + (size_t)n0 * N * M * esz; d.sBk = 1; d.sBn = M; d.b_cplx = l_cplx;
+    d.C = Tchunk; d.sCm = (long)nv * N; d.sCn = 1;
+    if ((rc = gemm_f64(d, st))) return rc;
+    if ((rc = energy_exx_reduce(Tchunk, W, N, nv, n0, Nc, exxn, kl, st))) return rc;
+  }
+  return energy_finish(exxn, kl, E3, W, Nc, scl, addEXX, addEJ, st);
+}
+
+}  // namespace ops
+}  // namespace sfq
+
+// ============================================================================================
+// C entry points: det_ops / HamiltonianOperations / propagator pieces
+// ============================================================================================
+using namespace sfq;
+
+namespace {
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+inline cudaStream_t S(void* p) { return reinterpret_cast<cudaStream_t>(p); }
+constexpr long kEnergyChunkElems = 1L << 27;  // 2 GiB of complex T per chunk at most
+}  // namespace
+
+extern "C" {
+
+int sfq_abi_version(void) { return 1; }
+
+const char* sfq_last_error(void) { return g_last_error.c_str(); }
+
+int sfq_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream) {
+  if (bytes == 0) return SFQ_OK;
+  if (!dst || !src) return record_error(SFQ_ERR_ARG, "null pointer");
+  cudaMemcpyKind k = kind == 1 ? cudaMemcpyHostToDevice : kind == 2 ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  SFQ_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, k, S(stream)));
+  SFQ_CUDA_TRY(cudaStreamSynchronize(S(stream)));
+  return SFQ_OK;
+}
+
+size_t sfq_workspace_size(int op, int nwalk, int nmo, int nel, int nchol) {
+  const size_t c = sizeof(cplx);
+  switch (op) {
+    case SFQ_OP_MIXED_DENSITY_MATRIX:
+      return align256(c * nwalk * nel * nel) + align256(c * nwalk * nel * nmo);
+    case SFQ_OP_LOG_OVERLAP:
+      return align256(c * nwalk * nel * nel);
+    case SFQ_OP_PROPAGATE:
+      return 3 * align256(c * (size_t)nwalk * nmo * nel);
+    case SFQ_OP_ORTHOGONALIZE:
+      return align256(c * (size_t)nwalk * nmo * nel) + align256(c * nwalk * nel * nel) + align256(sizeof(int) * nwalk);
+    case SFQ_OP_ENERGY: {
+      long nv = ops::energy_chunk(nwalk, nel, nchol, kEnergyChunkElems);
+      return align256(c * (size_t)nwalk * nel * nv * nel) + 2 * align256(c * (size_t)nwalk * nchol);
+    }
+    case SFQ_OP_INVERSE_LOGDET:
+      return 0;
+    default:
+      return 0;
+  }
+}
+
+int sfq_mixed_density_matrix(const void* A, int a_complex, const void* B, void* C, void* ovlp, int nwalk, int nmo,
+                             int nel, int compact, void* ws, size_t ws_bytes, void* stream) {
+  if (nwalk < 0 || nmo < 0 || nel < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0) return SFQ_OK;
+  if (nel == 0) {  // empty sector: overlap factor 1, G = 0 (density_matrix.hpp:563-566)
+    if (!compact && nmo > 0)
+      SFQ_CUDA_TRY(cudaMemsetAsync(C, 0, sizeof(cplx) * (size_t)nwalk * nmo * nmo, S(stream)));
+    return SFQ_OK;
+  }
+  if (!A || !B || !C || !ovlp) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (ws_bytes < sfq_workspace_size(SFQ_OP_MIXED_DENSITY_MATRIX, nwalk, nmo, nel, 0))
+    return record_error(SFQ_ERR_WORKSPACE, "mixed_density_matrix: workspace too small");
+  cplx* T = (cplx*)ws;
+  cplx* Gc = (cplx*)((char*)ws + align256(sizeof(cplx) * nwalk * nel * nel));
+  int rc;
+  if ((rc = ops::overlap_matrix(A, a_complex != 0, (const cplx*)B, T, nwalk, nmo, nel, S(stream)))) return rc;
+  if ((rc = lu_logdet(T, (long)nel * nel, nwalk, nel, (cplx*)ovlp, true, 1.0, true, S(stream)))) return rc;
+  if (compact) return ops::green_compact(T, (const cplx*)B, (cplx*)C, nwalk, nmo, nel, S(stream));
+  if ((rc = ops::green_compact(T, (const cplx*)B, Gc, nwalk, nmo, nel, S(stream)))) return rc;
+  return ops::green_full(A, a_complex != 0, Gc, (cplx*)C, nwalk, nmo, nel, S(stream));
+}
+
+int sfq_log_overlap(const void* A, int a_complex, const void* B, void* ovlp, int nwalk, int nmo, int nel, void* ws,
+                    size_t ws_bytes, void* stream) {
+  if (nwalk < 0 || nmo < 0 || nel < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0 || nel == 0) return SFQ_OK;
+  if (!A || !B || !ovlp) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (ws_bytes < sfq_workspace_size(SFQ_OP_LOG_OVERLAP, nwalk, nmo, nel, 0))
+    return record_error(SFQ_ERR_WORKSPACE, "log_overlap: workspace too small");
+  cplx* T = (cplx*)ws;
+  int rc;
+  if ((rc = ops::overlap_matrix(A, a_complex != 0, (const cplx*)B, T, nwalk, nmo, nel, S(stream)))) return rc;
+  return lu_logdet(T, (long)nel * nel, nwalk, nel, (cplx*)ovlp, true, 1.0, false, S(stream));
+}
+
+int sfq_inverse_logdet(const void* A, void* Ainv, void* logdet, int nbatch, int n, void* stream) {
+  if (nbatch < 0 || n < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nbatch == 0 || n == 0) return SFQ_OK;
+  if (!A || !Ainv || !logdet) return record_error(SFQ_ERR_ARG, "null pointer");
+  SFQ_CUDA_TRY(cudaMemcpyAsync(Ainv, A, sizeof(cplx) * (size_t)nbatch * n * n, cudaMemcpyDeviceToDevice, S(stream)));
+  return lu_logdet((cplx*)Ainv, (long)n * n, nbatch, n, (cplx*)logdet, true, 1.0, true, S(stream));
+}
+
+int sfq_propagate(void* SM, const void* P1, int p1_complex, const void* V, int nwalk, int nmo, int nel, int order,
+                  void* ws, size_t ws_bytes, void* stream) {
+  if (nwalk < 0 || nmo < 0 || nel < 0 || order < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0 || nel == 0 || nmo == 0) return SFQ_OK;
+  if (!SM || !P1 || !V) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (ws_bytes < sfq_workspace_size(SFQ_OP_PROPAGATE, nwalk, nmo, nel, 0))
+    return record_error(SFQ_ERR_WORKSPACE, "propagate: workspace too small");
+  const size_t blk = align256(sizeof(cplx) * (size_t)nwalk * nmo * nel);
+  cplx* TMN = (cplx*)ws;
+  cplx* T1 = (cplx*)((char*)ws + blk);
+  cplx* T2 = (cplx*)((char*)ws + 2 * blk);
+  return ops::propagate((cplx*)SM, P1, p1_complex != 0, (const cplx*)V, nwalk, nmo, nel, order, TMN, T1, T2,
+                        S(stream));
+}
+
+int sfq_orthogonalize(void* SM, void* log_detR, int nwalk, int nmo, int nel, void* ws, size_t ws_bytes,
+                      void* stream) {
+  if (nwalk < 0 || nmo < 0 || nel < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0 || nel == 0) return SFQ_OK;
+  if (nel > nmo) return record_error(SFQ_ERR_SHAPE, "orthogonalize: nel > nmo");
+  if (!SM) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (ws_bytes < sfq_workspace_size(SFQ_OP_ORTHOGONALIZE, nwalk, nmo, nel, 0))
+    return record_error(SFQ_ERR_WORKSPACE, "orthogonalize: workspace too small");
+  const size_t b1 = align256(sizeof(cplx) * (size_t)nwalk * nmo * nel);
+  const size_t b2 = align256(sizeof(cplx) * (size_t)nwalk * nel * nel);
+  cplx* SM2 = (cplx*)ws;
+  cplx* Sb = (cplx*)((char*)ws + b1);
+  int* status = (int*)((char*)ws + b1 + b2);
+  return ops::orthogonalize((cplx*)SM, SM2, Sb, status, (cplx*)log_detR, nwalk, nmo, nel, S(stream));
+}
+
+int sfq_vbias(const void* G, const void* Lnak, int lnak_complex, void* v, int nwalk, int nel, int nmo, int nchol,
+              double dt, int closed, void* stream) {
+  if (nwalk < 0 || nel < 0 || nmo < 0 || nchol < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0 || nchol == 0) return SFQ_OK;
+  if (!G || !Lnak || !v) return record_error(SFQ_ERR_ARG, "null pointer");
+  const double a = std::sqrt(dt) * (closed ? 2.0 : 1.0);
+  return ops::vbias((const cplx*)G, Lnak, lnak_complex != 0, (cplx*)v, nwalk, nel, nmo, nchol, a, S(stream));
+}
+
+int sfq_vhs(const double* Likn, const void* X, void* vHS, int nwalk, int nmo, int nchol, double dt, void* stream) {
+  if (nwalk < 0 || nmo < 0 || nchol < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0 || nmo == 0) return SFQ_OK;
+  if (!Likn || !X || !vHS) return record_error(SFQ_ERR_ARG, "null pointer");
+  return ops::vhs(Likn, (const cplx*)X, (cplx*)vHS, nwalk, nmo, nchol, std::sqrt(dt), S(stream));
+}
+
+int sfq_energy(void* E, const void* G, const void* haj, const void* Lnak, int lnak_complex, double E0, int nwalk,
+               int nel, int nmo, int nchol, int addH1, int addEJ, int addEXX, void* ws, size_t ws_bytes,
+               void* stream) {
+  if (nwalk < 0 || nel < 0 || nmo < 0 || nchol < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0) return SFQ_OK;
+  if (!E || !G || !haj || !Lnak) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (addEJ && !addEXX) return record_error(SFQ_ERR_UNSUPPORTED, "addEJ and not addEXX not yet implemented");
+  if (ws_bytes < sfq_workspace_size(SFQ_OP_ENERGY, nwalk, nmo, nel, nchol))
+    return record_error(SFQ_ERR_WORKSPACE, "energy: workspace too small");
+  long nv = ops::energy_chunk(nwalk, nel, nchol, kEnergyChunkElems);
+  const size_t bt = align256(sizeof(cplx) * (size_t)nwalk * nel * nv * nel);
+  const size_t bk = align256(sizeof(cplx) * (size_t)nwalk * nchol);
+  cplx* Tc = (cplx*)ws;
+  cplx* exxn = (cplx*)((char*)ws + bt);
+  cplx* kl = (cplx*)((char*)ws + bt + bk);
+  return ops::energy((cplx*)E, (const cplx*)G, (const cplx*)haj, Lnak, lnak_complex != 0, E0, nwalk, nel, nmo, nchol,
+                     addH1, addEJ, addEXX, Tc, (long)nwalk * nel * nv * nel, exxn, kl, S(stream));
+}
+
+int sfq_assemble_x(void* X, const double* vmf, void* hw, void* mf, const double* uniforms, unsigned long long seed,
+                   unsigned long long step, int nwalk, int nchol, double vbias_bound, int free_projection,
+                   void* stream) {
+  if (nwalk < 0 || nchol < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0) return SFQ_OK;
+  if (!X || !vmf || !hw || !mf) return record_error(SFQ_ERR_ARG, "null pointer");
+  FieldParams p;
+  p.nwalk = nwalk; p.nchol = nchol; p.vbias_bound = vbias_bound; p.free_projection = free_projection;
+  p.seed = seed; p.step = step; p.uniforms = uniforms;
+  return assemble_x((cplx*)X, vmf, (cplx*)hw, (cplx*)mf, p, S(stream));
+}
+
+int sfq_comb(const double* weights, double r, int nwalk, int* offspring, void* stream) {
+  if (nwalk < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0) return SFQ_OK;
+  if (!weights || !offspring) return record_error(SFQ_ERR_ARG, "null pointer");
+  double* cum = nullptr;
+  int* flag = nullptr;
+  SFQ_CUDA_TRY(cudaMallocAsync((void**)&cum, sizeof(double) * nwalk + 256, S(stream)));
+  flag = (int*)((char*)cum + ((sizeof(double) * nwalk + 15) & ~size_t(15)));
+  int rc = comb_weights(weights, nwalk, r, offspring, cum, flag, S(stream));
+  int h = 0;
+  if (!rc) {
+    cudaError_t e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, S(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S(stream));
+    if (e != cudaSuccess) rc = record_cuda(e, "sfq_comb", __FILE__, __LINE__);
+  }
+  cudaFreeAsync(cum, S(stream));
+  if (rc) return rc;
+  if (h == SFQ_ERR_WEIGHT_COLLAPSE) return record_error(h, "The total walker weight collapsed.");
+  return h;
+}
+
+}  // extern "C"

@@ -1,0 +1,31 @@
+// Composite operations on device arrays (the bodies of the det_ops / HamOps entry points).
+#pragma once
+#include "common.cuh"
+#include "gemm_f64.cuh"
+#include "kernels.cuh"
+
+namespace sfq {
+namespace ops {
+
+// T[w] = A * B[w]  (A: nel x nmo shared, real or complex; B: (W, nmo, nel) complex) -> (W, nel, nel)
+int overlap_matrix(const void* A, bool a_cplx, const cplx* B, cplx* T, int W, int M, int N, cudaStream_t st);
+// G[w] = Tinv[w]^T * B[w]^T -> (W, nel, nmo)
+int green_compact(const cplx* Tinv, const cplx* B, cplx* G, int W, int M, int N, cudaStream_t st);
+// C[w] = A^T * Gc[w] -> (W, nmo, nmo)   (non-compact, herm = true)
+int green_full(const void* A, bool a_cplx, const cplx* Gc, cplx* C, int W, int M, int N, cudaStream_t st);
+int vbias(const cplx* G, const void* Lnak, bool l_cplx, cplx* v, int W, int N, int M, int Nc, double a,
+          cudaStream_t st);
+int vhs(const double* Likn, const cplx* X, cplx* V, int W, int M, int Nc, double a, cudaStream_t st);
+// SM <- P1 * Taylor(iV) * P1 * SM with scratch TMN, T1, T2 (each W*M*N complex)
+int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M, int N, int order, cplx* TMN,
+              cplx* T1, cplx* T2, cudaStream_t st);
+// CholeskyQR2; SM2 (W*M*N), S (W*N*N) scratch, status (W) ints.  log_detR (W) accumulated if not null
+int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int W, int M, int N, cudaStream_t st);
+// energy with chunked T; ws: T chunk (W*N*nv*N) + exxn (W*Nc) + kl (W*Nc)
+int energy(cplx* E3, const cplx* G, const cplx* haj, const void* Lnak, bool l_cplx, double E0, int W, int N, int M,
+           int Nc, int addH1, int addEJ, int addEXX, cplx* Tchunk, long tchunk_elems, cplx* exxn, cplx* kl,
+           cudaStream_t st);
+int energy_chunk(int W, int N, int Nc, long max_elems);
+
+}  // namespace ops
+}  // namespace sfq

@@ -1,0 +1,84 @@
+"""CPU checks of the drop-in boundary: the sm_100a library loads and exports every symbol that
+include/safire_b200.h declares, and the Python binding covers them.  No compute call is made."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "safire_b200.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|size_t|const char\*|void\*)\s+(sfq_\w+)\s*\(", text, re.M)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from safire_b200 import build
+    path = build.build()
+    return ctypes.CDLL(path)
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert len(names) >= 25
+    for n in ("sfq_mixed_density_matrix", "sfq_log_overlap", "sfq_propagate", "sfq_orthogonalize", "sfq_vbias",
+              "sfq_vhs", "sfq_energy", "sfq_assemble_x", "sfq_comb", "sfq_engine_create", "sfq_engine_propagate",
+              "sfq_engine_run"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_header():
+    from safire_b200 import capi
+    assert set(declared()) <= set(capi.exported_symbols())
+
+
+def test_last_error_and_version(lib):
+    from safire_b200 import capi
+    L = capi.lib()
+    assert L.sfq_abi_version() == 1
+    assert isinstance(L.sfq_last_error(), bytes)
+
+
+def test_argument_errors_without_gpu():
+    """Shape / null checks return codes before any device work."""
+    from safire_b200 import capi
+    L = capi.lib()
+    assert L.sfq_mixed_density_matrix(None, 0, None, None, None, -1, 4, 2, 1, None, 0, None) == 1
+    assert L.sfq_mixed_density_matrix(None, 0, None, None, None, 3, 4, 2, 1, None, 0, None) == 2
+    assert L.sfq_vbias(None, None, 0, None, 2, 2, 4, 0, 0.01, 1, None) == 0  # empty: no-op
+    p = capi.default_params(nmo=4, nel=8, nchol=3, nwalk=2)
+    h = ctypes.c_void_p()
+    import numpy as np
+    z = np.zeros(64)
+    rc = L.sfq_engine_create(ctypes.byref(h), ctypes.byref(p), z.ctypes.data, z.ctypes.data, z.ctypes.data)
+    assert rc == 1  # nel > nmo: SFQ_ERR_SHAPE
+
+
+def test_workspace_sizes_monotone():
+    from safire_b200 import capi
+    L = capi.lib()
+    a = L.sfq_workspace_size(capi.OP_MIXED_DENSITY_MATRIX, 8, 40, 10, 0)
+    b = L.sfq_workspace_size(capi.OP_MIXED_DENSITY_MATRIX, 16, 40, 10, 0)
+    assert 0 < a < b
+    assert L.sfq_workspace_size(capi.OP_ENERGY, 8, 40, 10, 100) > 0
+
+
+def test_cpp_header_compiles():
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    hpp = os.path.join(ROOT, "include", "safire_b200.hpp")
+    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-x", "c++", hpp],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
