@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Walker-steps/s of the AFQMC propagation path on B200 (one JSON line on rank 0).
+
+A "step" is one iteration of run_afqmc's loop in its equilibration phase: Propagate of every
+walker (force bias, fields, vHS, P1 + order-6 Taylor exp, overlap, walker update, weight bound),
+orthogonalization every 5 steps and comb population control every 20 steps amortised into the
+steps they fall on, and the Eshift relaxation from the growth estimator.  Workload (default): synthetic dense-Cholesky
+system M=400, N=100+100 (closed shell), Nchol=2400, 256 walkers, dt=0.005, Philox fields.
+
+  value       device time (CUDA events on the engine stream), inputs resident in HBM
+  e2e         the same steps through sfq_engine_propagate_host: the step's field uniforms are
+              copied from pinned host memory and the walker properties read back every step
+  roofline    the dominant kernel (the vHS GEMM) timed with CUDA events inside this run
+  cpu_baseline the FP64 oracle (numpy + LAPACK/BLAS) on a bounded walker sample, on host cores
+
+--impl reference times the CPU restatement of the reference's path (the oracle) on the same
+configuration, with all host threads.  Under torchrun every rank runs an independent walker
+population of the same system (replicas; weak scaling); timings are max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# dt: the small system uses the configured 0.005.  With the same tensor distributions, M=128 and
+# M=400 give |vHS| ~ 1.1 and ~ 2 per step at dt = 0.005 and the phaseless constraint zeroes every
+# walker within a few steps (the oracle shows it; the reference's comb then aborts), so those
+# systems run at the dt where |vHS| ~ 0.5-0.7 per step.  The work per step does not depend on dt.
+CONFIGS = {
+    "large": dict(spec="CFG_LARGE", nwalk=256, cpu_walkers=32, dt=0.0005),
+    "medium": dict(spec="CFG_MEDIUM", nwalk=1024, cpu_walkers=64, dt=0.002),
+    "small": dict(spec="CFG_SMALL", nwalk=32, cpu_walkers=32, dt=0.005),
+}
+ORTHO_EVERY = 5
+POP_EVERY = 20
+EQUIL_STEPS = 100  # run_afqmc relaxes Eshift every step for the first equilibration_steps
+RELAX = 1.0 - math.exp(-10.0 / EQUIL_STEPS)
+
+
+def step_flops(M, N, Nc):
+    """Algorithmic flops per walker-step (complex multiply-add = 8 real flops)."""
+    return 8 * N * M * Nc + 4 * M * M * Nc + 64 * M * M * N + 24 * N * N * M + (32 / 3) * N ** 3
+
+
+def vhs_flops(M, Nc, W):
+    """Algorithmic flops of one vHS launch: real L (M^2 x Nc) times complex X (Nc x W)."""
+    return 4.0 * M * M * Nc * W
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.proc = None
+        self.lines = []
+        self.dev = device_index
+
+    def start(self):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            sel = ["-i", uuid if uuid.startswith("GPU-") else "GPU-" + uuid]
+        except Exception:
+            sel = []
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200"] + sel, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+                power.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def fp64_gemm_peak_tflops(dev):
+    """cuBLAS DGEMM throughput on this GPU (FP64 has no driver-measured peak)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = 1e30
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_baseline(cfg, steps=2, warm=1):
+    """The FP64 oracle on a bounded walker sample of the same system, on this host's cores."""
+    from oracle import afqmc_oracle as O
+    from safire_b200 import synthetic
+    spec = getattr(synthetic, cfg["spec"])
+    s = synthetic.make_system(spec)
+    Ws = cfg["cpu_walkers"]
+    ham = O.Hamiltonian(s.hcore, s.Likn, s.PsiT)
+    dt = cfg["dt"]
+    prop = O.Propagator(ham, dt, seed=0)
+    wo = O.Walkers(s.initial_walkers(Ws))
+    Esh = O.init_walkers(ham, wo)
+    for st in range(warm):
+        prop.propagate(wo, Esh, st)
+    t0 = time.perf_counter()
+    for st in range(warm, warm + steps):
+        prop.propagate(wo, Esh, st)
+        if st % ORTHO_EVERY == 0:
+            prop.orthogonalize(wo)
+        Esh += RELAX * (O.average_pseudo_energy(wo, dt) - Esh)
+    t = time.perf_counter() - t0
+    return dict(value=Ws * steps / t, unit="walker-steps/s", cores=os.cpu_count(), kind="port",
+                sample=f"{Ws} walkers x {steps} steps of {spec.name} (after {warm} warm-up), FP64 numpy/OpenBLAS")
+
+
+def run_reference(args, cfg):
+    """--impl reference: the oracle (CPU restatement of the reference path), all host threads."""
+    from oracle import afqmc_oracle as O
+    from oracle import philox
+    from safire_b200 import synthetic
+    spec = getattr(synthetic, cfg["spec"])
+    s = synthetic.make_system(spec)
+    Ws = cfg["cpu_walkers"]
+    ham = O.Hamiltonian(s.hcore, s.Likn, s.PsiT)
+    dt = cfg["dt"]
+    prop = O.Propagator(ham, dt, seed=0)
+    wo = O.Walkers(s.initial_walkers(Ws))
+    state = {"Esh": O.init_walkers(ham, wo)}
+
+    def one(st):
+        prop.propagate(wo, state["Esh"], st)
+        if st % ORTHO_EVERY == 0:
+            prop.orthogonalize(wo)
+        if st % POP_EVERY == 0:
+            O.population_control(wo, philox.comb_uniform(0, st))
+        state["Esh"] += RELAX * (O.average_pseudo_energy(wo, dt) - state["Esh"])
+
+    for st in range(args.warmup):
+        one(st)
+    t0 = time.perf_counter()
+    for st in range(args.warmup, args.warmup + args.steps):
+        one(st)
+    t = time.perf_counter() - t0
+    value = Ws * args.steps / t
+    unit = "walker-steps/s"
+    line = {"impl": "reference", "metric": "walker-steps/s", "value": value, "unit": unit, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"AFQMC propagation {spec.name} (dense real Cholesky, closed shell, "
+                                   f"{cfg['nwalk']} walkers; CPU sample {Ws} walkers per step)",
+                       "M": spec.M, "N": spec.N, "Nchol": spec.Nc, "walkers": cfg["nwalk"], "dt": dt,
+                       "ortho_every": ORTHO_EVERY, "popcontrol_every": POP_EVERY},
+            "cpu_baseline": {"value": value, "unit": unit, "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{Ws} walkers per step, {args.steps} timed steps after {args.warmup} warm-up; "
+                                       "oracle = FP64 numpy/LAPACK restatement of the reference path"},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="large", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    cfg = CONFIGS[args.config]
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, cfg)
+        return
+
+    import torch
+    from safire_b200 import afqmc, capi, synthetic
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    spec = getattr(synthetic, cfg["spec"])
+    W = cfg["nwalk"]
+    DT = cfg["dt"]
+    s = synthetic.make_system(spec)
+    eng = afqmc.AfqmcEngine(s, W, dt=DT, seed=1000 + rank, device=local)
+    state = {"Esh": eng.init()}
+    ext = torch.cuda.ExternalStream(eng.stream)
+    L = capi.lib()
+
+    def step(st, host=False, ubuf=None, pbuf=None):
+        """One run_afqmc iteration in the equilibration phase (run_afqmc.cpp:69-93)."""
+        if host:
+            eng.propagate_host(state["Esh"], st, ubuf, pbuf)
+        else:
+            eng.propagate(state["Esh"], st)
+        if st % ORTHO_EVERY == 0:
+            eng.orthogonalize()
+        if st % POP_EVERY == 0:
+            eng.population_control(st)
+        pe = eng.averages()[0]
+        state["Esh"] += RELAX * (pe - state["Esh"])
+
+    for st in range(args.warmup):
+        step(st)
+    eng.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    # ---- timed region: device events on the engine stream ---------------------------------
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    n0 = L.sfq_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for st in range(args.warmup, args.warmup + args.steps):
+        step(st)
+    e1.record(ext)
+    e1.synchronize()
+    launches = int(L.sfq_launch_count() - n0)
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = W * args.steps * world / (ms * 1e-3)
+
+    # ---- per-phase profile pass (not part of the headline) --------------------------------
+    s1 = args.warmup + args.steps
+    eng.profile(True)
+    for st in range(s1, s1 + args.steps):
+        step(st)
+    ph = eng.phase_times()
+    eng.profile(False)
+    s1 += args.steps
+
+    # ---- e2e through the host-buffer C ABI call -------------------------------------------
+    e2e = None
+    if not args.no_e2e:
+        ubytes = W * spec.Nc * 8
+        pbytes = 8 * W * 16
+        ubuf = torch.empty((args.steps, W, spec.Nc), dtype=torch.float64).pin_memory()
+        pbuf = torch.empty((args.steps, 8, W), dtype=torch.complex128).pin_memory()
+        tmp = torch.empty((W, spec.Nc), dtype=torch.float64, device="cuda")
+        for i in range(args.steps):
+            capi.check(L.sfq_field_uniforms(tmp.data_ptr(), 1000 + rank, s1 + i, W, spec.Nc, None))
+            ubuf[i].copy_(tmp.cpu())
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        tw = time.perf_counter()
+        f0.record(ext)
+        for i in range(args.steps):
+            step(s1 + i, host=True, ubuf=ubuf[i], pbuf=pbuf[i])
+        f1.record(ext)
+        f1.synchronize()
+        wall = time.perf_counter() - tw
+        ems = max(f0.elapsed_time(f1), wall * 1e3)
+        if dist:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": W * args.steps * world / (ems * 1e-3), "unit": "walker-steps/s",
+               "h2d_bytes_per_step": ubytes, "d2h_bytes_per_step": pbytes,
+               "path": "sfq_engine_propagate_host (pinned host uniforms in, walker properties out)"}
+
+    # ---- roofline of the dominant kernel --------------------------------------------------
+    vhs_ms, vhs_n = ph["vHS"]
+    vhs_launch_ms = vhs_ms / max(vhs_n, 1)
+    achieved = vhs_flops(spec.M, spec.Nc, W) / (vhs_launch_ms * 1e-3) / 1e12
+    peaks = measured_peaks()
+    peak = fp64_gemm_peak_tflops(local)
+    roofline = {"bound": "tensor", "kernel": "gemm_f64 (vHS: real Likn x complex X, DMMA m8n8k4)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (the driver's peaks file has no FP64 entry)",
+                "algorithmic_flops_per_launch": vhs_flops(spec.M, spec.Nc, W), "launch_ms": vhs_launch_ms,
+                "traffic": None}
+    tot_ph = sum(v[0] for v in ph.values())
+    phases = {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / tot_ph if tot_ph else None}
+              for k, v in ph.items() if v[1] > 0}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(cfg)
+
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"AFQMC propagation {spec.name}: dense real Cholesky, closed shell, "
+                                   f"{W} walkers per GPU, FP64 drop-in",
+                       "M": spec.M, "N": spec.N, "Nchol": spec.Nc, "walkers_per_gpu": W, "dt": DT,
+                       "eshift": "relaxed every step (equilibration phase of run_afqmc)",
+                       "taylor_order": 6, "ortho_every": ORTHO_EVERY, "popcontrol_every": POP_EVERY,
+                       "l2": "inputs larger than L2 (Likn alone is %.2f GB)" % (spec.M ** 2 * spec.Nc * 8 / 1e9),
+                       "parallelism": f"replicas x{world}"},
+            "algorithmic_tflops": step_flops(spec.M, spec.N, spec.Nc) * W * args.steps * world / (ms * 1e-3) / 1e12,
+            "gpu_launches": launches, "clocks": clocks, "e2e": e2e, "roofline": roofline, "phases": phases,
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

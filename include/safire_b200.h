@@ -40,6 +40,8 @@ extern "C" {
 /* version of this ABI */
 int sfq_abi_version(void);
 const char* sfq_last_error(void);
+/* kernels this library has launched in this process (all threads, all devices) */
+unsigned long long sfq_launch_count(void);
 /* cudaMemcpyAsync + stream synchronize (kind: 1 H2D, 2 D2H, 3 D2D), for callers without a CUDA runtime */
 int sfq_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream);
 
@@ -118,6 +120,11 @@ int sfq_energy(void* E, const void* G, const void* haj, const void* Lnak, int ln
 int sfq_assemble_x(void* X, const double* vmf, void* hw, void* mf, const double* uniforms, unsigned long long seed,
                    unsigned long long step, int nwalk, int nchol, double vbias_bound, int free_projection,
                    void* stream);
+
+/* RandomGenerator_t::sampleUniformFields for one step (Random.hpp:37-83, replaced by Philox-4x32-10):
+ * out (nwalk, nchol) doubles in (0,1), device; the same draws the engine makes in-kernel for (seed, step). */
+int sfq_field_uniforms(double* out, unsigned long long seed, unsigned long long step, int nwalk, int nchol,
+                       void* stream);
 
 /* comb(rng, weights, num_target)   population_control.hpp:34-65
  * weights (nwalk) doubles (|w|), device;  offspring (nwalk) ints, device;  r: the comb's uniform.
@@ -204,6 +211,24 @@ typedef struct {
  * sfq_engine_measure) are written to meas (capacity max_meas); *nmeas receives the count. */
 int sfq_engine_run(sfq_engine_t e, const sfq_run_params_t* rp, double* Eshift, double* meas, int max_meas,
                    int* nmeas);
+
+/* per-phase CUDA-event timing on the engine stream (AFQMCTimers analogue, AFQMCTimer.h:25-63) */
+enum sfq_phase {
+  SFQ_PH_DENSITY = 0,     /* overlap matrix + LU + mixed density matrix */
+  SFQ_PH_VBIAS = 1,       /* force bias GEMM */
+  SFQ_PH_FIELDS = 2,      /* assemble_X + meanfield factor */
+  SFQ_PH_VHS = 3,         /* vHS GEMM */
+  SFQ_PH_PROPAGATE = 4,   /* P1, Taylor exp, P1 */
+  SFQ_PH_OVERLAP = 5,     /* post-propagation log overlap */
+  SFQ_PH_UPDATE = 6,      /* walker_update + weight bound */
+  SFQ_PH_ORTHO = 7,       /* orthogonalize + overlap refresh */
+  SFQ_PH_POPCONTROL = 8,  /* comb + walker copies */
+  SFQ_PH_ENERGY = 9,      /* local energy */
+  SFQ_NUM_PHASES = 10
+};
+int sfq_engine_profile(sfq_engine_t e, int enable);
+/* synchronizes; ms[ph] = summed device time since the last call, counts[ph] = intervals (either may be NULL) */
+int sfq_engine_phase_times(sfq_engine_t e, double* ms, int* counts, int nphase);
 
 /* device addresses of the engine's resident arrays, for tests and zero-copy callers */
 typedef struct {

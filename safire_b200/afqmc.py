@@ -265,6 +265,15 @@ class AfqmcEngine:
                                    ctypes.byref(nm)))
         return es.value, meas[:nm.value]
 
+    def profile(self, enable=True):
+        check(lib().sfq_engine_profile(self.h, int(enable)))
+
+    def phase_times(self):
+        ms = np.zeros(len(capi.PHASES), np.float64)
+        cnt = np.zeros(len(capi.PHASES), np.int32)
+        check(lib().sfq_engine_phase_times(self.h, ms.ctypes.data, cnt.ctypes.data, len(capi.PHASES)))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(capi.PHASES)}
+
     def info(self):
         inf = capi.EngineInfo()
         check(lib().sfq_engine_info(self.h, ctypes.byref(inf)))

@@ -16,6 +16,7 @@ OP_MIXED_DENSITY_MATRIX, OP_LOG_OVERLAP, OP_PROPAGATE, OP_ORTHOGONALIZE, OP_ENER
 
 # walker property columns, in the order the engine stores them (WalkerConfig.hpp:28-48 names)
 PROPS = ("WEIGHT", "PHASE", "PSEUDO_ELOC_", "E1_", "EXX_", "EJ_", "OVLP", "THETA")
+PHASES = ("density", "vbias", "fields", "vHS", "propagate", "overlap", "update", "ortho", "popcontrol", "energy")
 
 
 class SafireError(RuntimeError):
@@ -84,6 +85,10 @@ _SIGS = {
     "sfq_engine_measure": ([_VP, _VP], _I),
     "sfq_engine_run": ([_VP, ctypes.POINTER(RunParams), ctypes.POINTER(_D), _VP, _I, ctypes.POINTER(_I)], _I),
     "sfq_engine_info": ([_VP, ctypes.POINTER(EngineInfo)], _I),
+    "sfq_engine_profile": ([_VP, _I], _I),
+    "sfq_engine_phase_times": ([_VP, _VP, _VP, _I], _I),
+    "sfq_launch_count": ([], ctypes.c_ulonglong),
+    "sfq_field_uniforms": ([_VP, _U64, _U64, _I, _I, _VP], _I),
 }
 
 

@@ -49,6 +49,14 @@ __device__ __forceinline__ cplx cexp_(cplx a) {
   } while (0)
 
 int record_cuda(cudaError_t e, const char* what, const char* file, int line);
+void count_launch();
+
+// after every kernel launch: count it and surface launch-configuration errors
+#define SFQ_LAUNCHED()                        \
+  do {                                        \
+    ::sfq::count_launch();                    \
+    SFQ_CUDA_TRY(cudaGetLastError());         \
+  } while (0)
 int record_error(int code, const char* fmt, ...);
 
 inline int ceil_div(long a, long b) { return int((a + b - 1) / b); }

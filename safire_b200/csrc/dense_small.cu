@@ -236,7 +236,7 @@ int lu_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, 
     SFQ_CUDA_TRY(cudaFuncSetAttribute(lu_logdet_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     lu_logdet_kernel<false><<<nbatch, LU_THREADS, sm, st>>>(T, sT, N, ovlp, accumulate ? 1 : 0, post_scale);
   }
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
@@ -246,7 +246,7 @@ int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, cudaStream_t st)
   const size_t sm = lu_smem_bytes(N);
   SFQ_CUDA_TRY(cudaFuncSetAttribute(chol_rinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
   chol_rinv_kernel<<<nbatch, LU_THREADS, sm, st>>>(S, sS, N, status);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 

@@ -110,6 +110,62 @@ struct Engine {
   double* h_pinned = nullptr;  // pinned host staging for e2e calls
   size_t h_pinned_bytes = 0;
 
+  // optional per-phase CUDA-event timing on the engine stream
+  static constexpr int NPH = SFQ_NUM_PHASES;
+  bool profile = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[NPH];
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t open_ev[NPH] = {};
+  cudaEvent_t take_event() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void ph_begin(int ph) {
+    if (!profile) return;
+    open_ev[ph] = take_event();
+    cudaEventRecord(open_ev[ph], st);
+  }
+  void ph_end(int ph) {
+    if (!profile || !open_ev[ph]) return;
+    cudaEvent_t e = take_event();
+    cudaEventRecord(e, st);
+    ev[ph].push_back({open_ev[ph], e});
+    open_ev[ph] = nullptr;
+  }
+  int phase_times(double* ms, int* counts, int n) {
+    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int ph = 0; ph < NPH; ++ph) {
+      double acc = 0.0;
+      for (auto& pr : ev[ph]) {
+        float t = 0.f;
+        SFQ_CUDA_TRY(cudaEventElapsedTime(&t, pr.first, pr.second));
+        acc += t;
+        pool.push_back(pr.first);
+        pool.push_back(pr.second);
+      }
+      if (ph < n) {
+        if (ms) ms[ph] = acc;
+        if (counts) counts[ph] = int(ev[ph].size());
+      }
+      ev[ph].clear();
+    }
+    return SFQ_OK;
+  }
+  void release_events() {
+    for (int ph = 0; ph < NPH; ++ph) {
+      for (auto& pr : ev[ph]) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+      ev[ph].clear();
+    }
+    for (auto e : pool) cudaEventDestroy(e);
+    pool.clear();
+  }
+
   WalkerProps wprops() const {
     WalkerProps w;
     w.weight = props + (long)P_WEIGHT * W;
@@ -341,32 +397,52 @@ struct Engine {
   // --- AFQMCBasePropagator::Propagate (hybrid) ----------------------------------------------
   int propagate(double Eshift, unsigned long long step, const double* uniforms) {
     int rc;
+    ph_begin(SFQ_PH_DENSITY);
     if ((rc = density(ovtmp))) return rc;                                            // 1. G
+    ph_end(SFQ_PH_DENSITY);
+    ph_begin(SFQ_PH_VBIAS);
     if ((rc = ops::vbias(G, Lnak, !trial_real, X, W, N, M, Nc, 2.0 * std::sqrt(p.dt), st))) return rc;
+    ph_end(SFQ_PH_VBIAS);
+    ph_begin(SFQ_PH_FIELDS);
     FieldParams fp;                                                                   // 2. X
     fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
     fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms;
     if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
+    ph_end(SFQ_PH_FIELDS);
+    ph_begin(SFQ_PH_VHS);
     if ((rc = ops::vhs(Likn, X, V, W, M, Nc, std::sqrt(p.dt), st))) return rc;       // 3. vHS
+    ph_end(SFQ_PH_VHS);
+    ph_begin(SFQ_PH_PROPAGATE);
     if ((rc = ops::propagate(SM, P1, false, V, W, M, N, p.taylor_order, TMN, T1, T2, st))) return rc;  // 4.
+    ph_end(SFQ_PH_PROPAGATE);
+    ph_begin(SFQ_PH_OVERLAP);
     if ((rc = log_overlap(newov))) return rc;                                         // 5.
+    ph_end(SFQ_PH_OVERLAP);
+    ph_begin(SFQ_PH_UPDATE);
     UpdateParams up;                                                                  // 6.+7.
     up.nwalk = W; up.dt = p.dt; up.Eshift = Eshift; up.E0 = p.E0;
     up.lower_cutoff = p.lower_cutoff_scale; up.upper_cutoff = p.upper_cutoff_scale;
     up.max_weight = std::fmax(p.weight_bound_floor, p.weight_bound_fraction * target_pop());
     up.hybrid = 1; up.free_projection = p.free_projection; up.use_cp_constraint = 0;
-    return walker_update(wprops(), newov, mf, hw, E3, up, stats, st);
+    if ((rc = walker_update(wprops(), newov, mf, hw, E3, up, stats, st))) return rc;
+    ph_end(SFQ_PH_UPDATE);
+    return SFQ_OK;
   }
 
   int orthogonalize() {
     int rc;
+    ph_begin(SFQ_PH_ORTHO);
     if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, M, N, st))) return rc;
-    return log_overlap(props + (long)P_OVLP * W);  // wfn->Log_Overlap(wset)
+    if ((rc = log_overlap(props + (long)P_OVLP * W))) return rc;  // wfn->Log_Overlap(wset)
+    ph_end(SFQ_PH_ORTHO);
+    return SFQ_OK;
   }
 
   int population_control(unsigned long long call) {
     int rc;
+    ph_begin(SFQ_PH_POPCONTROL);
     if ((rc = sfq::population_control(SM, (long)M * N, wprops(), W, 0.0, p.seed, call, 1, pw, st))) return rc;
+    ph_end(SFQ_PH_POPCONTROL);
     int flag = 0;
     SFQ_CUDA_TRY(cudaMemcpyAsync(&flag, pw.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
     SFQ_CUDA_TRY(cudaStreamSynchronize(st));
@@ -378,14 +454,18 @@ struct Engine {
   // NOMSD::Energy(wset, E, Ov): E3 and ovtmp
   int energy_only() {
     int rc;
+    ph_begin(SFQ_PH_ENERGY);
     if ((rc = density(ovtmp))) return rc;
-    return ops::energy(E3, G, haj, Lnak, !trial_real, p.E0, W, N, M, Nc, 1, 1, 1, Tchunk, tchunk_elems, exxn, kl,
-                       st);
+    if ((rc = ops::energy(E3, G, haj, Lnak, !trial_real, p.E0, W, N, M, Nc, 1, 1, 1, Tchunk, tchunk_elems, exxn, kl,
+                          st)))
+      return rc;
+    ph_end(SFQ_PH_ENERGY);
+    return SFQ_OK;
   }
 
   int averages(const cplx* E, double* out10) {
     averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, E, red);
-    SFQ_CUDA_TRY(cudaGetLastError());
+    SFQ_LAUNCHED();
     SFQ_CUDA_TRY(cudaMemcpyAsync(out10, red, sizeof(double) * 10, cudaMemcpyDeviceToHost, st));
     SFQ_CUDA_TRY(cudaStreamSynchronize(st));
     return SFQ_OK;
@@ -450,6 +530,7 @@ int sfq_engine_destroy(sfq_engine_t h) {
   if (!h) return SFQ_OK;
   Engine& e = h->e;
   if (e.st) cudaStreamSynchronize(e.st);
+  e.release_events();
   if (e.arena) cudaFree(e.arena);
   if (e.h_pinned) cudaFreeHost(e.h_pinned);
   if (e.st) cudaStreamDestroy(e.st);
@@ -510,7 +591,7 @@ int sfq_engine_energy(sfq_engine_t h, int seed_pseudo, void* E3host) {
   int rc;
   if ((rc = e.energy_only())) return rc;
   seed_pseudo_kernel<<<(e.W + 127) / 128, 128, 0, e.st>>>(e.props, e.E3, e.ovtmp, e.W, seed_pseudo ? 2 : 1);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   if (E3host) SFQ_CUDA_TRY(cudaMemcpyAsync(E3host, e.E3, sizeof(cplx) * 3 * e.W, cudaMemcpyDeviceToHost, e.st));
   SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
   return SFQ_OK;
@@ -621,6 +702,17 @@ int sfq_engine_run(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, d
   if (nmeas) *nmeas = nm;
   SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
   return SFQ_OK;
+}
+
+int sfq_engine_profile(sfq_engine_t h, int enable) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  h->e.profile = enable != 0;
+  return SFQ_OK;
+}
+
+int sfq_engine_phase_times(sfq_engine_t h, double* ms, int* counts, int nphase) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.phase_times(ms, counts, nphase);
 }
 
 int sfq_engine_info(sfq_engine_t h, sfq_engine_info_t* info) {

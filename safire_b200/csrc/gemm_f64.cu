@@ -20,7 +20,7 @@ int launch(const GemmDesc& d, cudaStream_t st) {
   if (grid.y > 65535u || grid.z > 65535u)
     return record_error(SFQ_ERR_SHAPE, "gemm_f64: grid (%u,%u,%u) too large", grid.x, grid.y, grid.z);
   k<<<grid, C_::THREADS, C_::SMEM, st>>>(d);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 

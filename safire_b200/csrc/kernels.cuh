@@ -19,6 +19,8 @@ struct FieldParams {
   unsigned long long seed = 0, step = 0;
   const double* uniforms = nullptr;  // optional injected (nwalk, nchol) buffer, else Philox
 };
+int field_uniforms(double* out, unsigned long long seed, unsigned long long step, int nwalk, int nchol,
+                   cudaStream_t st);
 // X: in = vbias (nwalk, nchol) complex, out = fields; vmf (nchol) real; hw, mf (nwalk) complex
 int assemble_x(cplx* X, const double* vmf, cplx* hw, cplx* mf, const FieldParams& p, cudaStream_t st);
 

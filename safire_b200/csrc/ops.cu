@@ -1,4 +1,5 @@
 // Composite device operations and the det_ops / HamOps C entry points.
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -11,6 +12,9 @@ namespace sfq {
 
 // ---- error plumbing ------------------------------------------------------------------------
 static thread_local std::string g_last_error;
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int record_error(int code, const char* fmt, ...) {
   char buf[512];
@@ -183,6 +187,16 @@ constexpr long kEnergyChunkElems = 1L << 27;  // 2 GiB of complex T per chunk at
 extern "C" {
 
 int sfq_abi_version(void) { return 1; }
+
+unsigned long long sfq_launch_count(void) { return g_launches.load(); }
+
+int sfq_field_uniforms(double* out, unsigned long long seed, unsigned long long step, int nwalk, int nchol,
+                       void* stream) {
+  if (nwalk < 0 || nchol < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (nwalk == 0 || nchol == 0) return SFQ_OK;
+  if (!out) return record_error(SFQ_ERR_ARG, "null pointer");
+  return field_uniforms(out, seed, step, nwalk, nchol, S(stream));
+}
 
 const char* sfq_last_error(void) { return g_last_error.c_str(); }
 

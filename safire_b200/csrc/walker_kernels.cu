@@ -372,6 +372,19 @@ __global__ void copy_kernel(cplx* d, const cplx* s, long n) {
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) d[e] = s[e];
 }
 
+__global__ void field_uniforms_kernel(double* out, unsigned long long seed, unsigned long long step, int nwalk,
+                                      int nchol) {
+  const int npair = (nchol + 1) / 2;
+  const long total = (long)nwalk * npair;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int w = int(e / npair), j = int(e % npair);
+    double u0, u1;
+    field_uniform_pair(seed, step, (uint32_t)w, (uint32_t)j, u0, u1);
+    out[(long)w * nchol + 2 * j] = u0;
+    if (2 * j + 1 < nchol) out[(long)w * nchol + 2 * j + 1] = u1;
+  }
+}
+
 inline int grid_for(long n) {
   long g = (n + 255) / 256;
   if (g > 148L * 32) g = 148L * 32;
@@ -381,10 +394,17 @@ inline int grid_for(long n) {
 
 }  // namespace
 
+int field_uniforms(double* out, unsigned long long seed, unsigned long long step, int nwalk, int nchol,
+                   cudaStream_t st) {
+  field_uniforms_kernel<<<grid_for((long)nwalk * ((nchol + 1) / 2)), 256, 0, st>>>(out, seed, step, nwalk, nchol);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
 int assemble_x(cplx* X, const double* vmf, cplx* hw, cplx* mf, const FieldParams& p, cudaStream_t st) {
   if (p.nwalk <= 0) return SFQ_OK;
   assemble_x_kernel<<<p.nwalk, RT, 0, st>>>(X, vmf, hw, mf, p);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
@@ -392,7 +412,7 @@ int walker_update(const WalkerProps& w, const cplx* new_ovlp, const cplx* mf, co
                   const UpdateParams& p, unsigned long long* stats, cudaStream_t st) {
   if (p.nwalk <= 0) return SFQ_OK;
   walker_update_kernel<<<(p.nwalk + 127) / 128, 128, 0, st>>>(w, new_ovlp, mf, hw, E3, p, stats);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
@@ -401,13 +421,13 @@ int population_control(cplx* SM, long walker_elems, const WalkerProps& w, int nw
                        cudaStream_t st) {
   if (nwalk <= 0) return SFQ_OK;
   comb_kernel<<<1, PT, 0, st>>>(w, nwalk, r_uniform, seed, call, use_philox, pw);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   int gx = int((walker_elems + 255) / 256);
   if (gx > 8) gx = 8;
   if (nwalk > 1) {
     dim3 grid(gx, nwalk - 1);
     copy_walkers_kernel<<<grid, 256, 0, st>>>(SM, walker_elems, w, pw.pairs, pw.npairs);
-    SFQ_CUDA_TRY(cudaGetLastError());
+    SFQ_LAUNCHED();
   }
   return SFQ_OK;
 }
@@ -415,7 +435,7 @@ int population_control(cplx* SM, long walker_elems, const WalkerProps& w, int nw
 int comb_weights(const double* wts, int nwalk, double r, int* offspring, double* cum, int* flag, cudaStream_t st) {
   if (nwalk <= 0) return SFQ_OK;
   comb_weights_kernel<<<1, PT, 0, st>>>(wts, nwalk, r, offspring, cum, flag);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
@@ -423,7 +443,7 @@ int energy_e1(const cplx* G, const cplx* haj, cplx* E3, int nwalk, int nel, int 
               int addH1, cudaStream_t st) {
   if (nwalk <= 0) return SFQ_OK;
   energy_e1_kernel<<<nwalk, RT, 0, st>>>(G, haj, E3, nel, nmo, E0, scl, addH1);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
@@ -432,7 +452,7 @@ int energy_exx_reduce(const cplx* T, int nwalk, int nel, int nv, int n0, int nch
   if (nwalk <= 0 || nv <= 0) return SFQ_OK;
   dim3 grid(nv, nwalk);
   energy_exx_kernel<<<grid, RT, 0, st>>>(T, nel, nv, n0, nchol, exxn, kl);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
@@ -440,7 +460,7 @@ int energy_finish(const cplx* exxn, const cplx* kl, cplx* E3, int nwalk, int nch
                   int addEJ, cudaStream_t st) {
   if (nwalk <= 0) return SFQ_OK;
   energy_finish_kernel<<<nwalk, RT, 0, st>>>(exxn, kl, E3, nchol, scl, addEXX, addEJ);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
@@ -450,52 +470,52 @@ int permute_lnak(const void* tmp, void* Lnak, int nel, int nmo, int nchol, int e
     permute_lnak_kernel<cplx><<<g, 256, 0, st>>>((const cplx*)tmp, (cplx*)Lnak, nel, nmo, nchol);
   else
     permute_lnak_kernel<double><<<g, 256, 0, st>>>((const double*)tmp, (double*)Lnak, nel, nmo, nchol);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
 int build_h1(const double* h, const double* v0, const cplx* vhs, double dt, double* H, int nmo, cudaStream_t st) {
   build_h1_kernel<<<grid_for((long)nmo * nmo), 256, 0, st>>>(h, v0, vhs, dt, H, nmo);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
 int add_identity(double* P, int nmo, double v, cudaStream_t st) {
   add_identity_kernel<<<(nmo + 255) / 256, 256, 0, st>>>(P, nmo, v);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
 int threshold_real(double* P, long n, double drop, cudaStream_t st) {
   threshold_kernel<<<grid_for(n), 256, 0, st>>>(P, n, drop);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
 int real_of(const cplx* z, double* r, long n, cudaStream_t st) {
   real_of_kernel<<<grid_for(n), 256, 0, st>>>(z, r, n);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
 int fill_cplx(cplx* p, long n, cplx v, cudaStream_t st) {
   if (n <= 0) return SFQ_OK;
   fill_kernel<<<grid_for(n), 256, 0, st>>>(p, n, v);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
 int scale_cplx(cplx* p, long n, cplx s, cudaStream_t st) {
   if (n <= 0) return SFQ_OK;
   scale_kernel<<<grid_for(n), 256, 0, st>>>(p, n, s);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
 int copy_walkers_prop(cplx* dst, const cplx* src, long n, cudaStream_t st) {
   if (n <= 0) return SFQ_OK;
   copy_kernel<<<grid_for(n), 256, 0, st>>>(dst, src, n);
-  SFQ_CUDA_TRY(cudaGetLastError());
+  SFQ_LAUNCHED();
   return SFQ_OK;
 }
 

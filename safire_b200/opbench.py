@@ -1,0 +1,92 @@
+"""Time one AFQMC operation in isolation (CUDA events), e.g. for profiling a single kernel.
+
+  python -m safire_b200.opbench --op vhs --M 400 --N 100 --Nc 2400 --W 64 --reps 3
+
+Operands are random with the shapes of the path; prints one JSON line per op with the
+average device time per call and the algorithmic TFLOP/s.
+"""
+import argparse
+import json
+
+import numpy as np
+import torch
+
+from . import afqmc
+
+
+def _flops(op, M, N, Nc, W):
+    return {
+        "vhs": 4.0 * M * M * Nc * W,
+        "vbias": 8.0 * N * M * Nc * W,
+        "propagate": 64.0 * M * M * N * W,
+        "density": (8.0 * N * N * M + 8.0 * N * N * M + 8.0 * N ** 3) * W,
+        "energy": 8.0 * N * N * M * Nc * W,
+        "orthogonalize": 2 * (8.0 * N * N * M * 2) * W,
+    }[op]
+
+
+def run(op, M, N, Nc, W, reps, warm=2, real_lnak=True):
+    g = torch.Generator(device="cuda").manual_seed(0)
+
+    def crand(*shape):
+        return torch.complex(torch.randn(*shape, generator=g, device="cuda", dtype=torch.float64),
+                             torch.randn(*shape, generator=g, device="cuda", dtype=torch.float64))
+
+    if op == "vhs":
+        L = torch.randn(M, M, Nc, generator=g, device="cuda", dtype=torch.float64)
+        X = crand(W, Nc)
+        fn = lambda: afqmc.vHS(L, X, 0.005)  # noqa: E731
+    elif op == "vbias":
+        G = crand(W, N, M)
+        Ln = torch.randn(Nc, N, M, generator=g, device="cuda", dtype=torch.float64) if real_lnak else crand(Nc, N, M)
+        fn = lambda: afqmc.vbias(G, Ln, 0.005)  # noqa: E731
+    elif op == "propagate":
+        SM = crand(W, M, N)
+        P1 = torch.eye(M, device="cuda", dtype=torch.float64)
+        V = crand(W, M, M) * 1e-3
+        fn = lambda: afqmc.Propagate(SM, P1, V, 6)  # noqa: E731
+    elif op == "density":
+        A = torch.randn(N, M, generator=g, device="cuda", dtype=torch.float64)
+        B = crand(W, M, N)
+        fn = lambda: afqmc.MixedDensityMatrix(A, B)  # noqa: E731
+    elif op == "energy":
+        G = crand(W, N, M) * 0.01
+        haj = crand(N, M)
+        Ln = torch.randn(Nc, N, M, generator=g, device="cuda", dtype=torch.float64)
+        fn = lambda: afqmc.energy(G, haj, Ln)  # noqa: E731
+    elif op == "orthogonalize":
+        SM = crand(W, M, N)
+        fn = lambda: afqmc.orthogonalize(SM)  # noqa: E731
+    else:
+        raise ValueError(op)
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    fl = _flops(op, M, N, Nc, W)
+    return {"op": op, "M": M, "N": N, "Nc": Nc, "W": W, "ms": ms, "tflops": fl / (ms * 1e-3) / 1e12}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--op", default="vhs")
+    ap.add_argument("--M", type=int, default=400)
+    ap.add_argument("--N", type=int, default=100)
+    ap.add_argument("--Nc", type=int, default=2400)
+    ap.add_argument("--W", type=int, default=64)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--warm", type=int, default=2)
+    a = ap.parse_args()
+    for op in a.op.split(","):
+        print(json.dumps(run(op, a.M, a.N, a.Nc, a.W, a.reps, a.warm)), flush=True)
+
+
+if __name__ == "__main__":
+    main()
