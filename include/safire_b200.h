@@ -67,6 +67,19 @@ size_t sfq_workspace_size(int op, int nwalk, int nmo, int nel, int nchol);
 int sfq_mixed_density_matrix(const void* A, int a_complex, const void* B, void* C, void* ovlp, int nwalk, int nmo,
                              int nel, int compact, void* ws, size_t ws_bytes, void* stream);
 
+/* Compact mixed density matrix with no allocation at all (no counterpart in the reference).
+ * Same arguments and results as sfq_mixed_density_matrix(..., compact = 1, ...) but without a
+ * workspace: for callers that cannot allocate device memory (a host program whose allocator owns
+ * all of it, an FFI binding without a CUDA runtime, a loop that cannot afford cudaMalloc's
+ * device-wide synchronisation).  Scratch is a fixed array of sfq_noalloc_scratch_bytes() (16 MiB)
+ * compiled into the library and held on every GPU that loads it until the process exits; calls
+ * with nwalk * nel * nel * 16 bytes above that return SFQ_ERR_WORKSPACE.  All calls on a device
+ * share the array, so calls that overlap on the GPU race; the first call on each device looks up
+ * the array's address and should come before any stream capture. */
+int sfq_mixed_density_matrix_noalloc(const void* A, int a_complex, const void* B, void* C, void* ovlp, int nwalk,
+                                     int nmo, int nel, void* stream);
+size_t sfq_noalloc_scratch_bytes(void);
+
 /* det_ops::Log_Overlap(A, B, ovlp, herm=true)   density_matrix.hpp:437-447 (accumulates into ovlp) */
 int sfq_log_overlap(const void* A, int a_complex, const void* B, void* ovlp, int nwalk, int nmo, int nel, void* ws,
                     size_t ws_bytes, void* stream);

@@ -60,6 +60,8 @@ _SIGS = {
     "sfq_workspace_size": ([_I, _I, _I, _I, _I], _SZ),
     "sfq_mixed_density_matrix": ([_VP, _I, _VP, _VP, _VP, _I, _I, _I, _I, _VP, _SZ, _VP], _I),
     "sfq_log_overlap": ([_VP, _I, _VP, _VP, _I, _I, _I, _VP, _SZ, _VP], _I),
+    "sfq_mixed_density_matrix_noalloc": ([_VP, _I, _VP, _VP, _VP, _I, _I, _I, _VP], _I),
+    "sfq_noalloc_scratch_bytes": ([], _SZ),
     "sfq_inverse_logdet": ([_VP, _VP, _VP, _I, _I, _VP], _I),
     "sfq_propagate": ([_VP, _VP, _I, _VP, _I, _I, _I, _I, _VP, _SZ, _VP], _I),
     "sfq_orthogonalize": ([_VP, _VP, _I, _I, _I, _VP, _SZ, _VP], _I),
