@@ -223,6 +223,7 @@ def main():
     ap.add_argument("--config", default="large", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -251,7 +252,8 @@ def main():
     W = cfg["nwalk"]
     DT = cfg["dt"]
     s = synthetic.make_system(spec)
-    eng = afqmc.AfqmcEngine(s, W, dt=DT, seed=1000 + rank, device=local)
+    prec = capi.PRECISION_MIXED if args.precision == "mixed" else capi.PRECISION_FP64
+    eng = afqmc.AfqmcEngine(s, W, dt=DT, seed=1000 + rank, device=local, precision=prec)
     state = {"Esh": eng.init()}
     ext = torch.cuda.ExternalStream(eng.stream)
     L = capi.lib()

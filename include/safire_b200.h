@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void);
+int sfq_abi_version(void); /* 2 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -144,6 +144,22 @@ int sfq_field_uniforms(double* out, unsigned long long seed, unsigned long long 
  * Returns SFQ_ERR_WEIGHT_COLLAPSE when the total weight is <= 1e-6. */
 int sfq_comb(const double* weights, double r, int nwalk, int* offspring, void* stream);
 
+/* Mixed-precision tensor-core GEMM (tcgen05, split BF16, FP32 accumulation), no reference
+ * counterpart: C[b] (M x N, fp32) = sum over terms A[b] (M x K) * B[b] (N x K)^T with A, B fp64 on the
+ * device (K contiguous), split into bf16 hi/lo planes; nterms 3 = hi*hi + hi*lo + lo*hi, 1 = hi*hi.
+ * a_batched / b_batched: 0 = one matrix shared by all batches.  tile_n: 0 auto, 64, 128 or 256.
+ * K must be a multiple of 8. */
+int sfq_gemm_split_bf16(const double* A, const double* B, float* C, int M, int N, int K, int batch, int a_batched,
+                        int b_batched, int nterms, int tile_n, void* stream);
+
+/* the same product on operands already held as bf16 planes (rows x K, K contiguous, 16-byte aligned,
+ * K a multiple of 8); batch strides in elements (0 = shared); C = alpha * A B^T + beta * C (fp32). */
+int sfq_gemm_bf16_planes(const void* A_hi, const void* A_lo, const void* B_hi, const void* B_lo, float* C, int M,
+                         int N, int K, int batch, long a_batch_stride, long b_batch_stride, float alpha, float beta,
+                         int nterms, int tile_n, void* stream);
+/* x = hi + lo with hi = bf16(x), lo = bf16(x - hi), elementwise over n doubles (lo may be NULL) */
+int sfq_split_bf16(const double* src, long n, void* hi, void* lo, void* stream);
+
 /* ---------------------------------------------------------------------------------------
  * Resident engine: HamiltonianOperations + NOMSD trial + WalkerSet + AFQMCBasePropagator
  * kept in device memory on one GPU (the drop-in for execute_simulation's objects).
@@ -166,7 +182,15 @@ typedef struct {
   int target_population;         /* global target population (0 -> nwalk) */
   unsigned long long seed;       /* Philox key for fields and comb */
   int device;                    /* CUDA device ordinal */
+  int precision;                 /* SFQ_PRECISION_FP64 (drop-in) or SFQ_PRECISION_MIXED */
 } sfq_engine_params_t;
+
+/* SFQ_PRECISION_MIXED: vbias, vHS, the P1 products and the Taylor terms run on the tcgen05 tensor
+ * cores as split-BF16 products (hi*hi + hi*lo + lo*hi) with FP32 accumulation; the mixed density
+ * matrix, LU / log det / phase, fields, overlaps, orthogonalization, walker update, population
+ * control and energies stay FP64.  Needs a real trial and nmo, nchol multiples of 8. */
+#define SFQ_PRECISION_FP64 0
+#define SFQ_PRECISION_MIXED 1
 
 /* fill *p with the reference's defaults (parameters.hpp:103-131, parameter_defaults.cpp:274-285) */
 void sfq_engine_params_default(sfq_engine_params_t* p);

@@ -32,7 +32,10 @@ class EngineParams(ctypes.Structure):
                 ("upper_cutoff_scale", ctypes.c_double), ("weight_bound_floor", ctypes.c_double),
                 ("weight_bound_fraction", ctypes.c_double), ("subtractMF", ctypes.c_int),
                 ("denseP1", ctypes.c_int), ("free_projection", ctypes.c_int),
-                ("target_population", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("device", ctypes.c_int)]
+                ("target_population", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("device", ctypes.c_int),
+                ("precision", ctypes.c_int)]
+
+PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 
 class RunParams(ctypes.Structure):
@@ -70,6 +73,10 @@ _SIGS = {
     "sfq_energy": ([_VP, _VP, _VP, _VP, _I, _D, _I, _I, _I, _I, _I, _I, _I, _VP, _SZ, _VP], _I),
     "sfq_assemble_x": ([_VP, _VP, _VP, _VP, _VP, _U64, _U64, _I, _I, _D, _I, _VP], _I),
     "sfq_comb": ([_VP, _D, _I, _VP, _VP], _I),
+    "sfq_gemm_split_bf16": ([_VP, _VP, _VP, _I, _I, _I, _I, _I, _I, _I, _I, _VP], _I),
+    "sfq_gemm_bf16_planes": ([_VP, _VP, _VP, _VP, _VP, _I, _I, _I, _I, ctypes.c_long, ctypes.c_long,
+                              ctypes.c_float, ctypes.c_float, _I, _I, _VP], _I),
+    "sfq_split_bf16": ([_VP, ctypes.c_long, _VP, _VP, _VP], _I),
     "sfq_engine_params_default": ([ctypes.POINTER(EngineParams)], None),
     "sfq_engine_create": ([ctypes.POINTER(_VP), ctypes.POINTER(EngineParams), _VP, _VP, _VP], _I),
     "sfq_engine_destroy": ([_VP], _I),

@@ -228,6 +228,8 @@ int lu_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, 
   if (nbatch <= 0) return SFQ_OK;
   if (N <= 0) return SFQ_OK;
   if (N > kMaxSmallN) return record_error(SFQ_ERR_UNSUPPORTED, "lu_logdet: N=%d exceeds %d", N, kMaxSmallN);
+  // register-resident Gauss-Jordan for the sizes it covers; shared-memory LU + getri above that
+  if (N <= kGjMaxLarge) return gj_logdet(T, sT, nbatch, N, ovlp, accumulate, post_scale, invert, st);
   const size_t sm = lu_smem_bytes(N);
   if (invert) {
     SFQ_CUDA_TRY(cudaFuncSetAttribute(lu_logdet_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));

@@ -8,7 +8,9 @@
 #include <cstring>
 #include <vector>
 
+#include "mixed.cuh"
 #include "ops.cuh"
+#include "umma_gemm.cuh"
 
 struct sfq_engine_s;
 
@@ -107,6 +109,13 @@ struct Engine {
   double* uni = nullptr;       // (W, Nc) staging for injected uniforms
   unsigned long long* stats = nullptr;  // 5 counters
   PopWork pw{};
+  // mixed precision: split-BF16 planes and fp32 accumulators
+  bool mixed = false;
+  void *LiknH = nullptr, *LiknL = nullptr, *LnakH = nullptr, *LnakL = nullptr, *P1H = nullptr, *P1L = nullptr;
+  void *GsH = nullptr, *GsL = nullptr, *XsH = nullptr, *XsL = nullptr, *VbH = nullptr, *VbL = nullptr;
+  void *WtH = nullptr, *WtL = nullptr;
+  float *Cvb = nullptr, *Cv = nullptr, *Sacc = nullptr, *Ck = nullptr;
+  int* gemm_err = nullptr;
   double* h_pinned = nullptr;  // pinned host staging for e2e calls
   size_t h_pinned_bytes = 0;
 
@@ -224,6 +233,25 @@ struct Engine {
         {(void**)&pw.cum, d * W},
         {(void**)&pw.flag, sizeof(int) * 4},
     };
+    if (mixed) {
+      const size_t b = 2;  // bf16
+      const long MN2 = 2L * M * N;
+      std::vector<Item> mx = {
+          {&LiknH, b * MM * Nc}, {&LiknL, b * MM * Nc},
+          {&LnakH, b * (size_t)Nc * N * M}, {&LnakL, b * (size_t)Nc * N * M},
+          {&P1H, b * MM}, {&P1L, b * MM},
+          {&GsH, b * 2 * W * MN}, {&GsL, b * 2 * W * MN},
+          {&XsH, b * 2 * (size_t)W * Nc}, {&XsL, b * 2 * (size_t)W * Nc},
+          {&VbH, b * 4 * W * MM}, {&VbL, b * 4 * W * MM},
+          {&WtH, b * W * MN2}, {&WtL, b * W * MN2},
+          {(void**)&Cvb, sizeof(float) * 2 * (size_t)W * Nc},
+          {(void**)&Cv, sizeof(float) * 2 * W * MM},
+          {(void**)&Sacc, sizeof(float) * W * MN2},
+          {(void**)&Ck, sizeof(float) * W * MN2},
+          {(void**)&gemm_err, sizeof(int) * 4},
+      };
+      items.insert(items.end(), mx.begin(), mx.end());
+    }
     size_t total = 0;
     for (auto& it : items) total += a256(it.bytes);
     SFQ_CUDA_TRY(cudaMalloc(&arena, total));
@@ -361,6 +389,13 @@ struct Engine {
         if ((rc = threshold_real(P1, MM, 1e-8, st))) return rc;
       }
     }
+    // mixed precision: bf16 hi/lo planes of the resident real tensors
+    if (mixed) {
+      if ((rc = split_bf16_f64(Likn, MM * Nc, LiknH, LiknL, st))) return rc;
+      if ((rc = split_bf16_f64((const double*)Lnak, (long)Nc * N * M, LnakH, LnakL, st))) return rc;
+      if ((rc = split_bf16_f64(P1, MM, P1H, P1L, st))) return rc;
+      SFQ_CUDA_TRY(cudaMemsetAsync(gemm_err, 0, sizeof(int) * 4, st));
+    }
     // walkers: copies of the trial, unit weight and phase
     {
       std::vector<cplx> psi(size_t(M) * N);
@@ -396,6 +431,7 @@ struct Engine {
 
   // --- AFQMCBasePropagator::Propagate (hybrid) ----------------------------------------------
   int propagate(double Eshift, unsigned long long step, const double* uniforms) {
+    if (mixed) return propagate_mixed(Eshift, step, uniforms);
     int rc;
     ph_begin(SFQ_PH_DENSITY);
     if ((rc = density(ovtmp))) return rc;                                            // 1. G
@@ -420,6 +456,76 @@ struct Engine {
     ph_end(SFQ_PH_OVERLAP);
     ph_begin(SFQ_PH_UPDATE);
     UpdateParams up;                                                                  // 6.+7.
+    up.nwalk = W; up.dt = p.dt; up.Eshift = Eshift; up.E0 = p.E0;
+    up.lower_cutoff = p.lower_cutoff_scale; up.upper_cutoff = p.upper_cutoff_scale;
+    up.max_weight = std::fmax(p.weight_bound_floor, p.weight_bound_fraction * target_pop());
+    up.hybrid = 1; up.free_projection = p.free_projection; up.use_cp_constraint = 0;
+    if ((rc = walker_update(wprops(), newov, mf, hw, E3, up, stats, st))) return rc;
+    ph_end(SFQ_PH_UPDATE);
+    return SFQ_OK;
+  }
+
+  // C = alpha * A B^T on split planes (A: rows x K, B: cols x K, both K-major)
+  int tc_gemm(const void* Ah, const void* Al, long a_rows, long a_bs, const void* Bh, const void* Bl, long b_rows,
+              long b_bs, int K, int batch, float* C, long ldc, long sCb, float alpha, int bn = 0) {
+    UmmaGemmDesc d;
+    d.M = int(a_rows); d.N = int(b_rows); d.K = K; d.batch = batch;
+    d.A.hi = Ah; d.A.lo = Al; d.A.rows = a_rows; d.A.ld = K; d.A.batch_stride = a_bs;
+    d.B.hi = Bh; d.B.lo = Bl; d.B.rows = b_rows; d.B.ld = K; d.B.batch_stride = b_bs;
+    d.C = C; d.ldc = ldc; d.sCb = sCb; d.alpha = alpha; d.nterms = 3; d.bn = bn; d.err = gemm_err;
+    return umma_gemm(d, st);
+  }
+
+  // AFQMCBasePropagator::Propagate with the bulk products on the tensor cores (split BF16, FP32
+  // accumulation); G, LU/log det, fields, overlaps and the walker update stay FP64.
+  int propagate_mixed(double Eshift, unsigned long long step, const double* uniforms) {
+    int rc;
+    const long MM = (long)M * M, NM = (long)N * M, M2 = 2L * M;
+    const double sdt = std::sqrt(p.dt);
+    ph_begin(SFQ_PH_DENSITY);
+    if ((rc = density(ovtmp))) return rc;
+    ph_end(SFQ_PH_DENSITY);
+    ph_begin(SFQ_PH_VBIAS);
+    if ((rc = mixed_split_planar(G, W, NM, GsH, GsL, st))) return rc;
+    if ((rc = tc_gemm(GsH, GsL, 2L * W, 0, LnakH, LnakL, Nc, 0, int(NM), 1, Cvb, Nc, 0, float(2.0 * sdt),
+                      Nc <= 4096 ? 64 : 0)))
+      return rc;
+    if ((rc = mixed_planar_to_cplx(Cvb, W, Nc, 1.0, X, st))) return rc;
+    ph_end(SFQ_PH_VBIAS);
+    ph_begin(SFQ_PH_FIELDS);
+    FieldParams fp;
+    fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
+    fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms;
+    if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
+    ph_end(SFQ_PH_FIELDS);
+    ph_begin(SFQ_PH_VHS);
+    if ((rc = mixed_split_planar(X, W, Nc, XsH, XsL, st))) return rc;
+    if ((rc = tc_gemm(XsH, XsL, 2L * W, 0, LiknH, LiknL, MM, 0, Nc, 1, Cv, MM, 0, float(sdt)))) return rc;
+    if ((rc = mixed_build_vblk(Cv, W, M, VbH, VbL, st))) return rc;
+    ph_end(SFQ_PH_VHS);
+    ph_begin(SFQ_PH_PROPAGATE);
+    const long rows = 2L * W * N;  // (w, a, c) rows of the walker operand
+    if ((rc = mixed_walkers_to_wt(SM, W, M, N, WtH, WtL, st))) return rc;
+    if ((rc = tc_gemm(WtH, WtL, rows, 0, P1H, P1L, M, 0, M, 1, Sacc, M, 0, 1.f))) return rc;  // S = P1 W
+    if ((rc = mixed_split_f32(Sacc, rows * M, WtH, WtL, st))) return rc;                      // T1 = S
+    for (int k = 1; k <= p.taylor_order; ++k) {
+      // C[w] (N x 2M) = T_k[w] (N x 2M) VB[w]^T;  T_{k+1} = (i/k) C;  S += T_{k+1}
+      if ((rc = tc_gemm(WtH, WtL, N, long(N) * M2, VbH, VbL, M2, M2 * M2, int(M2), W, Ck, M2, long(N) * M2, 1.f)))
+        return rc;
+      const bool last = k == p.taylor_order;
+      if ((rc = mixed_taylor_update(Ck, (long)W * N, M, 1.f / float(k), Sacc, last ? nullptr : WtH,
+                                    last ? nullptr : WtL, st)))
+        return rc;
+    }
+    if ((rc = mixed_split_f32(Sacc, rows * M, WtH, WtL, st))) return rc;
+    if ((rc = tc_gemm(WtH, WtL, rows, 0, P1H, P1L, M, 0, M, 1, Ck, M, 0, 1.f))) return rc;    // P1 S
+    if ((rc = mixed_wt_to_walkers(Ck, W, M, N, SM, st))) return rc;
+    ph_end(SFQ_PH_PROPAGATE);
+    ph_begin(SFQ_PH_OVERLAP);
+    if ((rc = log_overlap(newov))) return rc;
+    ph_end(SFQ_PH_OVERLAP);
+    ph_begin(SFQ_PH_UPDATE);
+    UpdateParams up;
     up.nwalk = W; up.dt = p.dt; up.Eshift = Eshift; up.E0 = p.E0;
     up.lower_cutoff = p.lower_cutoff_scale; up.upper_cutoff = p.upper_cutoff_scale;
     up.max_weight = std::fmax(p.weight_bound_floor, p.weight_bound_fraction * target_pop());
@@ -495,6 +601,7 @@ void sfq_engine_params_default(sfq_engine_params_t* p) {
   p->subtractMF = 1;
   p->denseP1 = 0;
   p->free_projection = 0;
+  p->precision = SFQ_PRECISION_FP64;
 }
 
 int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
@@ -515,6 +622,17 @@ int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const dou
   e.trial_real = true;
   for (long i = 0; i < (long)e.N * e.M; ++i)
     if (ps[i].y != 0.0) { e.trial_real = false; break; }
+  e.mixed = p->precision == SFQ_PRECISION_MIXED;
+  if (p->precision != SFQ_PRECISION_FP64 && p->precision != SFQ_PRECISION_MIXED) {
+    delete h;
+    return record_error(SFQ_ERR_ARG, "engine: unknown precision %d", p->precision);
+  }
+  if (e.mixed && (!e.trial_real || e.M % 8 || e.Nc % 8)) {
+    delete h;
+    return record_error(SFQ_ERR_UNSUPPORTED,
+                        "engine: mixed precision needs a real trial and nmo, nchol multiples of 8 (nmo=%d nchol=%d)",
+                        e.M, e.Nc);
+  }
   int rc;
   cudaError_t ce = cudaStreamCreateWithFlags(&e.st, cudaStreamNonBlocking);
   if (ce != cudaSuccess) { delete h; return record_cuda(ce, "cudaStreamCreate", __FILE__, __LINE__); }

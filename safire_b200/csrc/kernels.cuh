@@ -7,6 +7,9 @@ namespace sfq {
 constexpr int kMaxSmallN = 118;  // N x N complex + work (+ static) fits in 227 KB of shared memory
 
 size_t lu_smem_bytes(int N);
+constexpr int kGjMaxLarge = 100;  // register-resident Gauss-Jordan up to this N
+int gj_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, double post_scale, bool invert,
+              cudaStream_t st);
 // T: nbatch matrices N x N (row-major, batch stride sT); ovlp[b] = post_scale * fold(acc + logdet)
 int lu_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, double post_scale, bool invert,
               cudaStream_t st);

@@ -1,0 +1,189 @@
+// Layout conversions of the mixed-precision propagation step.
+//
+// Working layouts (per walker w, orbitals i,k < M, electrons a < N, c = 0 real / 1 imaginary):
+//   planar rows      P[c*W + w][e]               (split operands of the vbias / vHS GEMMs)
+//   walker rows      WT[w][a][c][i]              (K = (c,i) contiguous: Taylor / P1 A operand)
+//   vHS blocks       VB[w][(c,i)][(c',k)] = [[Vr, -Vi], [Vi, Vr]]   (Taylor B operand)
+// so that the complex products become real K-major GEMMs on the tensor cores:
+//   (V T)^T[a][(c,i)] = sum_(c',k) WT[a][(c',k)] VB[(c,i)][(c',k)],
+//   (P1 W)^T[(a,c)][j] = sum_i WT[(a,c)][i] P1[j][i].
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "mixed.cuh"
+
+namespace sfq {
+namespace {
+
+__device__ __forceinline__ void split_store(float x, __nv_bfloat16* hi, __nv_bfloat16* lo, long idx) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  hi[idx] = h;
+  lo[idx] = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+__device__ __forceinline__ void split_store_d(double x, __nv_bfloat16* hi, __nv_bfloat16* lo, long idx) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(float(x));
+  hi[idx] = h;
+  lo[idx] = __float2bfloat16_rn(float(x - double(__bfloat162float(h))));
+}
+
+inline int grid_for(long n) {
+  long g = (n + 255) / 256;
+  if (g > 148L * 32) g = 148L * 32;
+  return int(g < 1 ? 1 : g);
+}
+
+// complex (W, E) -> planar split rows c*W + w
+__global__ void split_planar_kernel(const cplx* src, int W, long E, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  const long total = (long)W * E;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long w = t / E, e = t % E;
+    const cplx z = src[t];
+    split_store_d(z.x, hi, lo, w * E + e);
+    split_store_d(z.y, hi, lo, ((long)W + w) * E + e);
+  }
+}
+
+// planar fp32 rows (c*W + w) -> complex fp64 (W, E), times alpha
+__global__ void planar_to_cplx_kernel(const float* C, int W, long E, double alpha, cplx* out) {
+  const long total = (long)W * E;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long w = t / E, e = t % E;
+    out[t] = mk(alpha * double(C[w * E + e]), alpha * double(C[((long)W + w) * E + e]));
+  }
+}
+
+// planar vHS (rows c*W + w, columns i*M + k) -> VB[w] = [[Vr, -Vi], [Vi, Vr]] split
+__global__ void build_vblk_kernel(const float* Cv, int W, int M, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  const long MM = (long)M * M;
+  const long total = (long)W * MM;
+  const long M2 = 2L * M;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long w = t / MM, r = t % MM;
+    const long i = r / M, k = r % M;
+    const float vr = Cv[w * MM + r];
+    const float vi = Cv[((long)W + w) * MM + r];
+    const long base = w * M2 * M2;
+    split_store(vr, hi, lo, base + i * M2 + k);             // (0,i),(0,k):  Vr
+    split_store(-vi, hi, lo, base + i * M2 + M + k);        // (0,i),(1,k): -Vi
+    split_store(vi, hi, lo, base + (M + i) * M2 + k);       // (1,i),(0,k):  Vi
+    split_store(vr, hi, lo, base + (M + i) * M2 + M + k);   // (1,i),(1,k):  Vr
+  }
+}
+
+// SM (W, M, N) complex fp64 -> WT[w][a][c][i] split, 32x32 tiles through shared memory
+__global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  __shared__ cplx tile[32][33];
+  const int w = blockIdx.z;
+  const int i0 = blockIdx.y * 32, a0 = blockIdx.x * 32;
+  const cplx* S = SM + (long)w * M * N;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, a = a0 + threadIdx.x;
+    if (i < M && a < N) tile[r][threadIdx.x] = S[(long)i * N + a];
+  }
+  __syncthreads();
+  const long base = (long)w * N * 2 * M;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int a = a0 + r, i = i0 + threadIdx.x;
+    if (i < M && a < N) {
+      const cplx z = tile[threadIdx.x][r];
+      split_store_d(z.x, hi, lo, base + ((long)a * 2 + 0) * M + i);
+      split_store_d(z.y, hi, lo, base + ((long)a * 2 + 1) * M + i);
+    }
+  }
+}
+
+// C2[w][a][c][j] fp32 -> SM (W, M, N) complex fp64
+__global__ void wt_to_walkers_kernel(const float* C2, int M, int N, cplx* SM) {
+  __shared__ float2 tile[32][33];
+  const int w = blockIdx.z;
+  const int j0 = blockIdx.y * 32, a0 = blockIdx.x * 32;
+  const long base = (long)w * N * 2 * M;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int a = a0 + r, j = j0 + threadIdx.x;
+    if (j < M && a < N) {
+      tile[r][threadIdx.x] = make_float2(C2[base + ((long)a * 2 + 0) * M + j], C2[base + ((long)a * 2 + 1) * M + j]);
+    }
+  }
+  __syncthreads();
+  cplx* S = SM + (long)w * M * N;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = j0 + r, a = a0 + threadIdx.x;
+    if (j < M && a < N) {
+      const float2 v = tile[threadIdx.x][r];
+      S[(long)j * N + a] = mk(double(v.x), double(v.y));
+    }
+  }
+}
+
+// T_{k+1} = (i/k) C: T[a][(0,i)] = -C[a][(1,i)]/k, T[a][(1,i)] = C[a][(0,i)]/k; S += T; split T
+__global__ void taylor_update_kernel(const float* C, long rows, int M, float inv_k, float* S, __nv_bfloat16* hi,
+                                     __nv_bfloat16* lo) {
+  const long total = rows * M;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long row = t / M, i = t % M;
+    const long o0 = row * 2 * M + i, o1 = o0 + M;
+    const float cr = C[o0], ci = C[o1];
+    const float tr = -ci * inv_k, ti = cr * inv_k;
+    S[o0] += tr;
+    S[o1] += ti;
+    if (hi) {
+      split_store(tr, hi, lo, o0);
+      split_store(ti, hi, lo, o1);
+    }
+  }
+}
+
+__global__ void split_f32_kernel(const float* src, long n, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+    split_store(src[e], hi, lo, e);
+}
+
+}  // namespace
+
+int mixed_split_planar(const cplx* src, int W, long E, void* hi, void* lo, cudaStream_t st) {
+  split_planar_kernel<<<grid_for((long)W * E), 256, 0, st>>>(src, W, E, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int mixed_planar_to_cplx(const float* C, int W, long E, double alpha, cplx* out, cudaStream_t st) {
+  planar_to_cplx_kernel<<<grid_for((long)W * E), 256, 0, st>>>(C, W, E, alpha, out);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int mixed_build_vblk(const float* Cv, int W, int M, void* hi, void* lo, cudaStream_t st) {
+  build_vblk_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Cv, W, M, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* hi, void* lo, cudaStream_t st) {
+  dim3 grid((N + 31) / 32, (M + 31) / 32, W), block(32, 8);
+  walkers_to_wt_kernel<<<grid, block, 0, st>>>(SM, M, N, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int mixed_wt_to_walkers(const float* C2, int W, int M, int N, cplx* SM, cudaStream_t st) {
+  dim3 grid((N + 31) / 32, (M + 31) / 32, W), block(32, 8);
+  wt_to_walkers_kernel<<<grid, block, 0, st>>>(C2, M, N, SM);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int mixed_taylor_update(const float* C, long rows, int M, float inv_k, float* S, void* hi, void* lo,
+                        cudaStream_t st) {
+  taylor_update_kernel<<<grid_for(rows * M), 256, 0, st>>>(C, rows, M, inv_k, S, (__nv_bfloat16*)hi,
+                                                           (__nv_bfloat16*)lo);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int mixed_split_f32(const float* src, long n, void* hi, void* lo, cudaStream_t st) {
+  split_f32_kernel<<<grid_for(n), 256, 0, st>>>(src, n, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+}  // namespace sfq

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "ops.cuh"
+#include "umma_gemm.cuh"
 
 namespace sfq {
 
@@ -186,7 +187,7 @@ constexpr long kEnergyChunkElems = 1L << 27;  // 2 GiB of complex T per chunk at
 
 extern "C" {
 
-int sfq_abi_version(void) { return 1; }
+int sfq_abi_version(void) { return 2; }
 
 unsigned long long sfq_launch_count(void) { return g_launches.load(); }
 
@@ -350,6 +351,37 @@ int sfq_assemble_x(void* X, const double* vmf, void* hw, void* mf, const double*
   p.nwalk = nwalk; p.nchol = nchol; p.vbias_bound = vbias_bound; p.free_projection = free_projection;
   p.seed = seed; p.step = step; p.uniforms = uniforms;
   return assemble_x((cplx*)X, vmf, (cplx*)hw, (cplx*)mf, p, S(stream));
+}
+
+int sfq_gemm_split_bf16(const double* A, const double* B, float* C, int M, int N, int K, int batch, int a_batched,
+                        int b_batched, int nterms, int tile_n, void* stream) {
+  if (M < 0 || N < 0 || K < 0 || batch < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (!M || !N || !batch) return SFQ_OK;
+  if (!A || !B || !C) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (K % 8) return record_error(SFQ_ERR_SHAPE, "sfq_gemm_split_bf16: K must be a multiple of 8");
+  return gemm_split_bf16_f64(A, B, C, M, N, K, batch, a_batched, b_batched, nterms, tile_n, S(stream));
+}
+
+int sfq_split_bf16(const double* src, long n, void* hi, void* lo, void* stream) {
+  if (n < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (n == 0) return SFQ_OK;
+  if (!src || !hi) return record_error(SFQ_ERR_ARG, "null pointer");
+  return split_bf16_f64(src, n, hi, lo, S(stream));
+}
+
+int sfq_gemm_bf16_planes(const void* A_hi, const void* A_lo, const void* B_hi, const void* B_lo, float* C, int M,
+                         int N, int K, int batch, long a_batch_stride, long b_batch_stride, float alpha, float beta,
+                         int nterms, int tile_n, void* stream) {
+  if (M < 0 || N < 0 || K < 0 || batch < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
+  if (!M || !N || !batch) return SFQ_OK;
+  if (!A_hi || !B_hi || !C) return record_error(SFQ_ERR_ARG, "null pointer");
+  UmmaGemmDesc d;
+  d.M = M; d.N = N; d.K = K; d.batch = batch;
+  d.A.hi = A_hi; d.A.lo = A_lo; d.A.rows = M; d.A.ld = K; d.A.batch_stride = a_batch_stride;
+  d.B.hi = B_hi; d.B.lo = B_lo; d.B.rows = N; d.B.ld = K; d.B.batch_stride = b_batch_stride;
+  d.C = C; d.ldc = N; d.sCb = (long)M * N;
+  d.alpha = alpha; d.beta = beta; d.nterms = nterms; d.bn = tile_n;
+  return umma_gemm(d, S(stream));
 }
 
 int sfq_comb(const double* weights, double r, int nwalk, int* offspring, void* stream) {

@@ -22,6 +22,8 @@ def _flops(op, M, N, Nc, W):
         "density": (8.0 * N * N * M + 8.0 * N * N * M + 8.0 * N ** 3) * W,
         "energy": 8.0 * N * N * M * Nc * W,
         "orthogonalize": 2 * (8.0 * N * N * M * 2) * W,
+        "umma_vhs": 2.0 * (2 * W) * M * M * Nc,   # one real product of the split GEMM
+        "umma_planes": 2.0 * (2 * W) * M * M * Nc,
     }[op]
 
 
@@ -54,6 +56,32 @@ def run(op, M, N, Nc, W, reps, warm=2, real_lnak=True):
         haj = crand(N, M)
         Ln = torch.randn(Nc, N, M, generator=g, device="cuda", dtype=torch.float64)
         fn = lambda: afqmc.energy(G, haj, Ln)  # noqa: E731
+    elif op == "umma_vhs":
+        # the vHS-shaped split-BF16 tensor-core GEMM: (2W x Nc) x (M^2 x Nc)^T, 3 products
+        import ctypes
+        from . import capi
+        A = torch.randn(2 * W, Nc, generator=g, device="cuda", dtype=torch.float64)
+        B = torch.randn(M * M, Nc, generator=g, device="cuda", dtype=torch.float64)
+        C = torch.empty(2 * W, M * M, device="cuda", dtype=torch.float32)
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        fn = lambda: capi.check(capi.lib().sfq_gemm_split_bf16(A.data_ptr(), B.data_ptr(), C.data_ptr(), 2 * W,  # noqa
+                                                               M * M, Nc, 1, 0, 0, 3, 0, st))
+    elif op == "umma_planes":
+        # the same GEMM on pre-split planes: tensor-core time only
+        import ctypes
+        from . import capi
+        L = capi.lib()
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        A = torch.randn(2 * W, Nc, generator=g, device="cuda", dtype=torch.float64)
+        B = torch.randn(M * M, Nc, generator=g, device="cuda", dtype=torch.float64)
+        planes = [torch.empty(x.numel(), dtype=torch.bfloat16, device="cuda") for x in (A, A, B, B)]
+        capi.check(L.sfq_split_bf16(A.data_ptr(), A.numel(), planes[0].data_ptr(), planes[1].data_ptr(), st))
+        capi.check(L.sfq_split_bf16(B.data_ptr(), B.numel(), planes[2].data_ptr(), planes[3].data_ptr(), st))
+        del B
+        C = torch.empty(2 * W, M * M, device="cuda", dtype=torch.float32)
+        tn = int(__import__("os").environ.get("SFQ_TILE_N", "0"))
+        fn = lambda: capi.check(L.sfq_gemm_bf16_planes(*[p.data_ptr() for p in planes], C.data_ptr(), 2 * W,  # noqa
+                                                       M * M, Nc, 1, 0, 0, 1.0, 0.0, 3, tn, st))
     elif op == "orthogonalize":
         SM = crand(W, M, N)
         fn = lambda: afqmc.orthogonalize(SM)  # noqa: E731
