@@ -214,49 +214,17 @@ def run_reference(args, cfg):
     print(json.dumps(line), flush=True)
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="large", choices=sorted(CONFIGS))
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    args = ap.parse_args()
-    if args.warmup < 3:
-        ap.error("--warmup must be >= 3")
-    cfg = CONFIGS[args.config]
+def run_engine(args, cfg, spec, s, W, DT, prec, rank, local, profile_pass=True, e2e=True):
+    """Warm up, time args.steps steps on the device, optionally a profile pass and the e2e pass.
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-
-    if args.impl == "reference":
-        if rank == 0:
-            run_reference(args, cfg)
-        return
-
+    Returns (engine, dict of measurements); the engine is left open for the caller.
+    """
     import torch
-    from safire_b200 import afqmc, capi, synthetic
-
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    spec = getattr(synthetic, cfg["spec"])
-    W = cfg["nwalk"]
-    DT = cfg["dt"]
-    s = synthetic.make_system(spec)
-    prec = capi.PRECISION_MIXED if args.precision == "mixed" else capi.PRECISION_FP64
+    from safire_b200 import afqmc, capi
+    L = capi.lib()
     eng = afqmc.AfqmcEngine(s, W, dt=DT, seed=1000 + rank, device=local, precision=prec)
     state = {"Esh": eng.init()}
     ext = torch.cuda.ExternalStream(eng.stream)
-    L = capi.lib()
 
     def step(st, host=False, ubuf=None, pbuf=None):
         """One run_afqmc iteration in the equilibration phase (run_afqmc.cpp:69-93)."""
@@ -274,11 +242,8 @@ def main():
     for st in range(args.warmup):
         step(st)
     eng.synchronize()
-    if dist:
-        dist.barrier()
     torch.cuda.synchronize()
-
-    # ---- timed region: device events on the engine stream ---------------------------------
+    out = {}
     clk = ClockSampler(local)
     clk.start()
     time.sleep(0.3)
@@ -290,27 +255,21 @@ def main():
         step(st)
     e1.record(ext)
     e1.synchronize()
-    launches = int(L.sfq_launch_count() - n0)
-    clocks = clk.stop()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = W * args.steps * world / (ms * 1e-3)
-
-    # ---- per-phase profile pass (not part of the headline) --------------------------------
+    out["launches"] = int(L.sfq_launch_count() - n0)
+    out["clocks"] = clk.stop()
+    out["ms"] = e0.elapsed_time(e1)
+    # energy at the end of the timed block (EnergyEstimator::measure), outside the timed region
+    meas = eng.measure()
+    out["energy"] = meas["Energy"].real
     s1 = args.warmup + args.steps
-    eng.profile(True)
-    for st in range(s1, s1 + args.steps):
-        step(st)
-    ph = eng.phase_times()
-    eng.profile(False)
-    s1 += args.steps
-
-    # ---- e2e through the host-buffer C ABI call -------------------------------------------
-    e2e = None
-    if not args.no_e2e:
+    if profile_pass:
+        eng.profile(True)
+        for st in range(s1, s1 + args.steps):
+            step(st)
+        out["phases"] = eng.phase_times()
+        eng.profile(False)
+        s1 += args.steps
+    if e2e:
         ubytes = W * spec.Nc * 8
         pbytes = 8 * W * 16
         ubuf = torch.empty((args.steps, W, spec.Nc), dtype=torch.float64).pin_memory()
@@ -320,8 +279,6 @@ def main():
             capi.check(L.sfq_field_uniforms(tmp.data_ptr(), 1000 + rank, s1 + i, W, spec.Nc, None))
             ubuf[i].copy_(tmp.cpu())
         torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
         tw = time.perf_counter()
@@ -331,53 +288,140 @@ def main():
         f1.record(ext)
         f1.synchronize()
         wall = time.perf_counter() - tw
-        ems = max(f0.elapsed_time(f1), wall * 1e3)
-        if dist:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        out["e2e_ms"] = max(f0.elapsed_time(f1), wall * 1e3)
+        out["e2e_bytes"] = (ubytes, pbytes)
+    return eng, out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="large", choices=sorted(CONFIGS))
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed-fp32"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 drop-in comparison run")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    cfg = CONFIGS[args.config]
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, cfg)
+        return
+
+    import torch
+    from safire_b200 import capi, synthetic
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    spec = getattr(synthetic, cfg["spec"])
+    W = cfg["nwalk"]
+    DT = cfg["dt"]
+    s = synthetic.make_system(spec)
+    prec = {"fp64": capi.PRECISION_FP64, "mixed": capi.PRECISION_MIXED,
+            "mixed-fp32": capi.PRECISION_MIXED_FP32}[args.precision]
+    if dist:
+        dist.barrier()
+    eng, m = run_engine(args, cfg, spec, s, W, DT, prec, rank, local, e2e=not args.no_e2e)
+    eng.close()
+    del eng
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms = max_over_ranks(m["ms"])
+    value = W * args.steps * world / (ms * 1e-3)
+    e2e = None
+    if "e2e_ms" in m:
+        ems = max_over_ranks(m["e2e_ms"])
         e2e = {"value": W * args.steps * world / (ems * 1e-3), "unit": "walker-steps/s",
-               "h2d_bytes_per_step": ubytes, "d2h_bytes_per_step": pbytes,
+               "h2d_bytes_per_step": m["e2e_bytes"][0], "d2h_bytes_per_step": m["e2e_bytes"][1],
                "path": "sfq_engine_propagate_host (pinned host uniforms in, walker properties out)"}
 
-    # ---- roofline of the dominant kernel --------------------------------------------------
-    vhs_ms, vhs_n = ph["vHS"]
-    vhs_launch_ms = vhs_ms / max(vhs_n, 1)
-    achieved = vhs_flops(spec.M, spec.Nc, W) / (vhs_launch_ms * 1e-3) / 1e12
+    # the FP64 drop-in on the same system, seeds and schedule: speed ratio and block-energy difference
+    compare = None
+    if prec != capi.PRECISION_FP64 and not args.no_compare:
+        eng64, m64 = run_engine(args, cfg, spec, s, W, DT, capi.PRECISION_FP64, rank, local, profile_pass=False,
+                                e2e=False)
+        eng64.close()
+        del eng64
+        ms64 = max_over_ranks(m64["ms"])
+        v64 = W * args.steps * world / (ms64 * 1e-3)
+        compare = {"fp64_value": v64, "fp64_ms_per_step": ms64 / args.steps, "speedup_vs_fp64": value / v64,
+                   "block_energy_mixed": m["energy"], "block_energy_fp64": m64["energy"],
+                   "block_energy_delta_mHa": 1e3 * (m["energy"] - m64["energy"]),
+                   "block_energy_delta_rel": (m["energy"] - m64["energy"]) / abs(m64["energy"]),
+                   "block": f"energy measured after the {args.warmup}+{args.steps} steps of each timed run"}
+
+    # ---- roofline of the dominant kernel: the vHS product ---------------------------------
+    ph = m["phases"]
+    g_ms, g_n = ph["vHS_gemm"]
+    launch_ms = g_ms / max(g_n, 1)
+    alg = vhs_flops(spec.M, spec.Nc, W)
+    achieved = alg / (launch_ms * 1e-3) / 1e12
     peaks = measured_peaks()
-    peak = fp64_gemm_peak_tflops(local)
-    roofline = {"bound": "tensor", "kernel": "gemm_f64 (vHS: real Likn x complex X, DMMA m8n8k4)",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (the driver's peaks file has no FP64 entry)",
-                "algorithmic_flops_per_launch": vhs_flops(spec.M, spec.Nc, W), "launch_ms": vhs_launch_ms,
-                "traffic": None}
-    tot_ph = sum(v[0] for v in ph.values())
-    phases = {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / tot_ph if tot_ph else None}
-              for k, v in ph.items() if v[1] > 0}
+    if prec == capi.PRECISION_FP64:
+        peak = fp64_gemm_peak_tflops(local)
+        roofline = {"bound": "tensor", "kernel": "gemm_f64_kernel (vHS: complex X x real Likn, DMMA m8n8k4)",
+                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in the peaks file)"}
+    else:
+        nprod = 3 if prec == capi.PRECISION_MIXED else 6
+        peak = peaks.get("bf16_tflops_sustained") or 1400.0
+        src = "MEASURED_PEAKS.json bf16_tflops_sustained (kernel timed inside a long step)" \
+            if peaks.get("bf16_tflops_sustained") else "fallback 1.4 PFLOP/s sustained"
+        roofline = {"bound": "tensor",
+                    "kernel": f"umma_gemm_kernel (vHS: split-BF16 tcgen05, {nprod} tensor-core products per real product)",
+                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "executed_tflops": achieved * nprod, "executed_frac": achieved * nprod / peak,
+                    "peak_source": src}
+    roofline.update({"algorithmic_flops_per_launch": alg, "launch_ms": launch_ms, "traffic": None})
+    tot = sum(v[0] for k, v in ph.items() if k != "vHS_gemm")
+    phases = {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / tot if tot else None}
+              for k, v in ph.items() if v[1] > 0 and k != "vHS_gemm"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(cfg)
 
-    eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return
+    dtype = {"fp64": "f64", "mixed": "bf16x3 split (fp32 accumulate) + f64", "mixed-fp32":
+             "bf16x6 split (fp32 accumulate) + f64"}[args.precision]
     line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
             "config": {"workload": f"AFQMC propagation {spec.name}: dense real Cholesky, closed shell, "
-                                   f"{W} walkers per GPU, FP64 drop-in",
+                                   f"{W} walkers per GPU, precision {args.precision}",
                        "M": spec.M, "N": spec.N, "Nchol": spec.Nc, "walkers_per_gpu": W, "dt": DT,
                        "eshift": "relaxed every step (equilibration phase of run_afqmc)",
                        "taylor_order": 6, "ortho_every": ORTHO_EVERY, "popcontrol_every": POP_EVERY,
                        "l2": "inputs larger than L2 (Likn alone is %.2f GB)" % (spec.M ** 2 * spec.Nc * 8 / 1e9),
                        "parallelism": f"replicas x{world}"},
             "algorithmic_tflops": step_flops(spec.M, spec.N, spec.Nc) * W * args.steps * world / (ms * 1e-3) / 1e12,
-            "gpu_launches": launches, "clocks": clocks, "e2e": e2e, "roofline": roofline, "phases": phases,
-            "cpu_baseline": cpu}
+            "gpu_launches": m["launches"], "clocks": m["clocks"], "e2e": e2e, "roofline": roofline,
+            "fp64_comparison": compare, "phases": phases, "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
 
 

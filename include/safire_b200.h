@@ -145,20 +145,22 @@ int sfq_field_uniforms(double* out, unsigned long long seed, unsigned long long 
 int sfq_comb(const double* weights, double r, int nwalk, int* offspring, void* stream);
 
 /* Mixed-precision tensor-core GEMM (tcgen05, split BF16, FP32 accumulation), no reference
- * counterpart: C[b] (M x N, fp32) = sum over terms A[b] (M x K) * B[b] (N x K)^T with A, B fp64 on the
- * device (K contiguous), split into bf16 hi/lo planes; nterms 3 = hi*hi + hi*lo + lo*hi, 1 = hi*hi.
- * a_batched / b_batched: 0 = one matrix shared by all batches.  tile_n: 0 auto, 64, 128 or 256.
- * K must be a multiple of 8. */
+ * counterpart: C[b] (M x N, fp32) = A[b] (M x K) * B[b] (N x K)^T with A, B fp64 on the device
+ * (K contiguous), each split into nplanes bf16 planes x ~ p0 + p1 + p2 (p0 = bf16(x), p1 = bf16(x-p0),
+ * ...); the product keeps the plane pairs of combined order < nplanes: 1 plane -> 1 tensor-core
+ * product (8 bits), 2 -> 3 products (~16 bits), 3 -> 6 products (~24 bits, FP32 class).
+ * a_batched / b_batched: 0 = one matrix shared by all batches.  tile_n: 0 auto, 64, 128 or 256 (256 only
+ * with nplanes <= 2).  K must be a multiple of 8. */
 int sfq_gemm_split_bf16(const double* A, const double* B, float* C, int M, int N, int K, int batch, int a_batched,
-                        int b_batched, int nterms, int tile_n, void* stream);
+                        int b_batched, int nplanes, int tile_n, void* stream);
 
 /* the same product on operands already held as bf16 planes (rows x K, K contiguous, 16-byte aligned,
  * K a multiple of 8); batch strides in elements (0 = shared); C = alpha * A B^T + beta * C (fp32). */
-int sfq_gemm_bf16_planes(const void* A_hi, const void* A_lo, const void* B_hi, const void* B_lo, float* C, int M,
-                         int N, int K, int batch, long a_batch_stride, long b_batch_stride, float alpha, float beta,
-                         int nterms, int tile_n, void* stream);
-/* x = hi + lo with hi = bf16(x), lo = bf16(x - hi), elementwise over n doubles (lo may be NULL) */
-int sfq_split_bf16(const double* src, long n, void* hi, void* lo, void* stream);
+int sfq_gemm_bf16_planes(const void* const* A, const void* const* B, int nplanes, float* C, int M, int N, int K,
+                         int batch, long a_batch_stride, long b_batch_stride, float alpha, float beta, int tile_n,
+                         void* stream);
+/* the planes of n doubles: p0 = bf16(x), p1 = bf16(x - p0), p2 = bf16(x - p0 - p1); p1, p2 may be NULL */
+int sfq_split_bf16(const double* src, long n, void* p0, void* p1, void* p2, void* stream);
 
 /* ---------------------------------------------------------------------------------------
  * Resident engine: HamiltonianOperations + NOMSD trial + WalkerSet + AFQMCBasePropagator
@@ -185,12 +187,13 @@ typedef struct {
   int precision;                 /* SFQ_PRECISION_FP64 (drop-in) or SFQ_PRECISION_MIXED */
 } sfq_engine_params_t;
 
-/* SFQ_PRECISION_MIXED: vbias, vHS, the P1 products and the Taylor terms run on the tcgen05 tensor
- * cores as split-BF16 products (hi*hi + hi*lo + lo*hi) with FP32 accumulation; the mixed density
+/* SFQ_PRECISION_MIXED / _MIXED_FP32: vbias, vHS, the P1 products and the Taylor terms run on the tcgen05 tensor
+ * cores as split-BF16 products (see sfq_gemm_split_bf16) with FP32 accumulation; the mixed density
  * matrix, LU / log det / phase, fields, overlaps, orthogonalization, walker update, population
  * control and energies stay FP64.  Needs a real trial and nmo, nchol multiples of 8. */
 #define SFQ_PRECISION_FP64 0
-#define SFQ_PRECISION_MIXED 1
+#define SFQ_PRECISION_MIXED 1      /* 2 bf16 planes per operand: ~16-bit operands, 3 tensor-core products */
+#define SFQ_PRECISION_MIXED_FP32 2 /* 3 bf16 planes per operand: ~24-bit operands, 6 tensor-core products */
 
 /* fill *p with the reference's defaults (parameters.hpp:103-131, parameter_defaults.cpp:274-285) */
 void sfq_engine_params_default(sfq_engine_params_t* p);
@@ -261,7 +264,8 @@ enum sfq_phase {
   SFQ_PH_ORTHO = 7,       /* orthogonalize + overlap refresh */
   SFQ_PH_POPCONTROL = 8,  /* comb + walker copies */
   SFQ_PH_ENERGY = 9,      /* local energy */
-  SFQ_NUM_PHASES = 10
+  SFQ_PH_VHS_GEMM = 10,   /* the vHS matrix product alone (inside SFQ_PH_VHS) */
+  SFQ_NUM_PHASES = 11
 };
 int sfq_engine_profile(sfq_engine_t e, int enable);
 /* synchronizes; ms[ph] = summed device time since the last call, counts[ph] = intervals (either may be NULL) */

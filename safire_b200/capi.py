@@ -16,7 +16,8 @@ OP_MIXED_DENSITY_MATRIX, OP_LOG_OVERLAP, OP_PROPAGATE, OP_ORTHOGONALIZE, OP_ENER
 
 # walker property columns, in the order the engine stores them (WalkerConfig.hpp:28-48 names)
 PROPS = ("WEIGHT", "PHASE", "PSEUDO_ELOC_", "E1_", "EXX_", "EJ_", "OVLP", "THETA")
-PHASES = ("density", "vbias", "fields", "vHS", "propagate", "overlap", "update", "ortho", "popcontrol", "energy")
+PHASES = ("density", "vbias", "fields", "vHS", "propagate", "overlap", "update", "ortho", "popcontrol", "energy",
+          "vHS_gemm")
 
 
 class SafireError(RuntimeError):
@@ -35,7 +36,7 @@ class EngineParams(ctypes.Structure):
                 ("target_population", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("device", ctypes.c_int),
                 ("precision", ctypes.c_int)]
 
-PRECISION_FP64, PRECISION_MIXED = 0, 1
+PRECISION_FP64, PRECISION_MIXED, PRECISION_MIXED_FP32 = 0, 1, 2
 
 
 class RunParams(ctypes.Structure):
@@ -74,9 +75,9 @@ _SIGS = {
     "sfq_assemble_x": ([_VP, _VP, _VP, _VP, _VP, _U64, _U64, _I, _I, _D, _I, _VP], _I),
     "sfq_comb": ([_VP, _D, _I, _VP, _VP], _I),
     "sfq_gemm_split_bf16": ([_VP, _VP, _VP, _I, _I, _I, _I, _I, _I, _I, _I, _VP], _I),
-    "sfq_gemm_bf16_planes": ([_VP, _VP, _VP, _VP, _VP, _I, _I, _I, _I, ctypes.c_long, ctypes.c_long,
-                              ctypes.c_float, ctypes.c_float, _I, _I, _VP], _I),
-    "sfq_split_bf16": ([_VP, ctypes.c_long, _VP, _VP, _VP], _I),
+    "sfq_gemm_bf16_planes": ([ctypes.POINTER(_VP), ctypes.POINTER(_VP), _I, _VP, _I, _I, _I, _I, ctypes.c_long,
+                              ctypes.c_long, ctypes.c_float, ctypes.c_float, _I, _VP], _I),
+    "sfq_split_bf16": ([_VP, ctypes.c_long, _VP, _VP, _VP, _VP], _I),
     "sfq_engine_params_default": ([ctypes.POINTER(EngineParams)], None),
     "sfq_engine_create": ([ctypes.POINTER(_VP), ctypes.POINTER(EngineParams), _VP, _VP, _VP], _I),
     "sfq_engine_destroy": ([_VP], _I),

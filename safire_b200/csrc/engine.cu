@@ -111,9 +111,14 @@ struct Engine {
   PopWork pw{};
   // mixed precision: split-BF16 planes and fp32 accumulators
   bool mixed = false;
-  void *LiknH = nullptr, *LiknL = nullptr, *LnakH = nullptr, *LnakL = nullptr, *P1H = nullptr, *P1L = nullptr;
-  void *GsH = nullptr, *GsL = nullptr, *XsH = nullptr, *XsL = nullptr, *VbH = nullptr, *VbL = nullptr;
-  void *WtH = nullptr, *WtL = nullptr;
+  int nplanes = 3;  // bf16 planes per operand (2: ~16-bit products, 3: FP32-class)
+  void* Likn_p[3] = {};
+  void* Lnak_p[3] = {};
+  void* P1_p[3] = {};
+  void* Gs_p[3] = {};
+  void* Xs_p[3] = {};
+  void* Vb_p[3] = {};
+  void* Wt_p[3] = {};
   float *Cvb = nullptr, *Cv = nullptr, *Sacc = nullptr, *Ck = nullptr;
   int* gemm_err = nullptr;
   double* h_pinned = nullptr;  // pinned host staging for e2e calls
@@ -236,14 +241,17 @@ struct Engine {
     if (mixed) {
       const size_t b = 2;  // bf16
       const long MN2 = 2L * M * N;
-      std::vector<Item> mx = {
-          {&LiknH, b * MM * Nc}, {&LiknL, b * MM * Nc},
-          {&LnakH, b * (size_t)Nc * N * M}, {&LnakL, b * (size_t)Nc * N * M},
-          {&P1H, b * MM}, {&P1L, b * MM},
-          {&GsH, b * 2 * W * MN}, {&GsL, b * 2 * W * MN},
-          {&XsH, b * 2 * (size_t)W * Nc}, {&XsL, b * 2 * (size_t)W * Nc},
-          {&VbH, b * 4 * W * MM}, {&VbL, b * 4 * W * MM},
-          {&WtH, b * W * MN2}, {&WtL, b * W * MN2},
+      std::vector<Item> mx;
+      for (int q = 0; q < nplanes; ++q) {
+        mx.push_back({&Likn_p[q], b * MM * Nc});
+        mx.push_back({&Lnak_p[q], b * (size_t)Nc * N * M});
+        mx.push_back({&P1_p[q], b * MM});
+        mx.push_back({&Gs_p[q], b * 2 * W * MN});
+        mx.push_back({&Xs_p[q], b * 2 * (size_t)W * Nc});
+        mx.push_back({&Vb_p[q], b * 4 * W * MM});
+        mx.push_back({&Wt_p[q], b * W * MN2});
+      }
+      std::vector<Item> mx2 = {
           {(void**)&Cvb, sizeof(float) * 2 * (size_t)W * Nc},
           {(void**)&Cv, sizeof(float) * 2 * W * MM},
           {(void**)&Sacc, sizeof(float) * W * MN2},
@@ -251,6 +259,7 @@ struct Engine {
           {(void**)&gemm_err, sizeof(int) * 4},
       };
       items.insert(items.end(), mx.begin(), mx.end());
+      items.insert(items.end(), mx2.begin(), mx2.end());
     }
     size_t total = 0;
     for (auto& it : items) total += a256(it.bytes);
@@ -391,9 +400,9 @@ struct Engine {
     }
     // mixed precision: bf16 hi/lo planes of the resident real tensors
     if (mixed) {
-      if ((rc = split_bf16_f64(Likn, MM * Nc, LiknH, LiknL, st))) return rc;
-      if ((rc = split_bf16_f64((const double*)Lnak, (long)Nc * N * M, LnakH, LnakL, st))) return rc;
-      if ((rc = split_bf16_f64(P1, MM, P1H, P1L, st))) return rc;
+      if ((rc = split_bf16_f64(Likn, MM * Nc, Likn_p[0], Likn_p[1], Likn_p[2], st))) return rc;
+      if ((rc = split_bf16_f64((const double*)Lnak, (long)Nc * N * M, Lnak_p[0], Lnak_p[1], Lnak_p[2], st))) return rc;
+      if ((rc = split_bf16_f64(P1, MM, P1_p[0], P1_p[1], P1_p[2], st))) return rc;
       SFQ_CUDA_TRY(cudaMemsetAsync(gemm_err, 0, sizeof(int) * 4, st));
     }
     // walkers: copies of the trial, unit weight and phase
@@ -446,7 +455,9 @@ struct Engine {
     if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
     ph_end(SFQ_PH_FIELDS);
     ph_begin(SFQ_PH_VHS);
+    ph_begin(SFQ_PH_VHS_GEMM);
     if ((rc = ops::vhs(Likn, X, V, W, M, Nc, std::sqrt(p.dt), st))) return rc;       // 3. vHS
+    ph_end(SFQ_PH_VHS_GEMM);
     ph_end(SFQ_PH_VHS);
     ph_begin(SFQ_PH_PROPAGATE);
     if ((rc = ops::propagate(SM, P1, false, V, W, M, N, p.taylor_order, TMN, T1, T2, st))) return rc;  // 4.
@@ -466,13 +477,17 @@ struct Engine {
   }
 
   // C = alpha * A B^T on split planes (A: rows x K, B: cols x K, both K-major)
-  int tc_gemm(const void* Ah, const void* Al, long a_rows, long a_bs, const void* Bh, const void* Bl, long b_rows,
-              long b_bs, int K, int batch, float* C, long ldc, long sCb, float alpha, int bn = 0) {
+  int tc_gemm(void* const* A, long a_rows, long a_bs, void* const* B, long b_rows, long b_bs, int K, int batch,
+              float* C, long ldc, long sCb, float alpha, int bn = 0) {
     UmmaGemmDesc d;
     d.M = int(a_rows); d.N = int(b_rows); d.K = K; d.batch = batch;
-    d.A.hi = Ah; d.A.lo = Al; d.A.rows = a_rows; d.A.ld = K; d.A.batch_stride = a_bs;
-    d.B.hi = Bh; d.B.lo = Bl; d.B.rows = b_rows; d.B.ld = K; d.B.batch_stride = b_bs;
-    d.C = C; d.ldc = ldc; d.sCb = sCb; d.alpha = alpha; d.nterms = 3; d.bn = bn; d.err = gemm_err;
+    for (int q = 0; q < 3; ++q) {
+      d.A.p[q] = A[q];
+      d.B.p[q] = B[q];
+    }
+    d.A.rows = a_rows; d.A.ld = K; d.A.batch_stride = a_bs;
+    d.B.rows = b_rows; d.B.ld = K; d.B.batch_stride = b_bs;
+    d.C = C; d.ldc = ldc; d.sCb = sCb; d.alpha = alpha; d.nplanes = nplanes; d.bn = bn; d.err = gemm_err;
     return umma_gemm(d, st);
   }
 
@@ -486,9 +501,8 @@ struct Engine {
     if ((rc = density(ovtmp))) return rc;
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
-    if ((rc = mixed_split_planar(G, W, NM, GsH, GsL, st))) return rc;
-    if ((rc = tc_gemm(GsH, GsL, 2L * W, 0, LnakH, LnakL, Nc, 0, int(NM), 1, Cvb, Nc, 0, float(2.0 * sdt),
-                      Nc <= 4096 ? 64 : 0)))
+    if ((rc = mixed_split_planar(G, W, NM, Gs_p, st))) return rc;
+    if ((rc = tc_gemm(Gs_p, 2L * W, 0, Lnak_p, Nc, 0, int(NM), 1, Cvb, Nc, 0, float(2.0 * sdt), Nc <= 4096 ? 64 : 0)))
       return rc;
     if ((rc = mixed_planar_to_cplx(Cvb, W, Nc, 1.0, X, st))) return rc;
     ph_end(SFQ_PH_VBIAS);
@@ -499,26 +513,25 @@ struct Engine {
     if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
     ph_end(SFQ_PH_FIELDS);
     ph_begin(SFQ_PH_VHS);
-    if ((rc = mixed_split_planar(X, W, Nc, XsH, XsL, st))) return rc;
-    if ((rc = tc_gemm(XsH, XsL, 2L * W, 0, LiknH, LiknL, MM, 0, Nc, 1, Cv, MM, 0, float(sdt)))) return rc;
-    if ((rc = mixed_build_vblk(Cv, W, M, VbH, VbL, st))) return rc;
+    if ((rc = mixed_split_planar(X, W, Nc, Xs_p, st))) return rc;
+    ph_begin(SFQ_PH_VHS_GEMM);
+    if ((rc = tc_gemm(Xs_p, 2L * W, 0, Likn_p, MM, 0, Nc, 1, Cv, MM, 0, float(sdt)))) return rc;
+    ph_end(SFQ_PH_VHS_GEMM);
+    if ((rc = mixed_build_vblk(Cv, W, M, Vb_p, st))) return rc;
     ph_end(SFQ_PH_VHS);
     ph_begin(SFQ_PH_PROPAGATE);
     const long rows = 2L * W * N;  // (w, a, c) rows of the walker operand
-    if ((rc = mixed_walkers_to_wt(SM, W, M, N, WtH, WtL, st))) return rc;
-    if ((rc = tc_gemm(WtH, WtL, rows, 0, P1H, P1L, M, 0, M, 1, Sacc, M, 0, 1.f))) return rc;  // S = P1 W
-    if ((rc = mixed_split_f32(Sacc, rows * M, WtH, WtL, st))) return rc;                      // T1 = S
+    if ((rc = mixed_walkers_to_wt(SM, W, M, N, Wt_p, st))) return rc;
+    if ((rc = tc_gemm(Wt_p, rows, 0, P1_p, M, 0, M, 1, Sacc, M, 0, 1.f))) return rc;  // S = P1 W
+    if ((rc = mixed_split_f32(Sacc, rows * M, Wt_p, st))) return rc;                  // T1 = S
     for (int k = 1; k <= p.taylor_order; ++k) {
       // C[w] (N x 2M) = T_k[w] (N x 2M) VB[w]^T;  T_{k+1} = (i/k) C;  S += T_{k+1}
-      if ((rc = tc_gemm(WtH, WtL, N, long(N) * M2, VbH, VbL, M2, M2 * M2, int(M2), W, Ck, M2, long(N) * M2, 1.f)))
-        return rc;
+      if ((rc = tc_gemm(Wt_p, N, long(N) * M2, Vb_p, M2, M2 * M2, int(M2), W, Ck, M2, long(N) * M2, 1.f))) return rc;
       const bool last = k == p.taylor_order;
-      if ((rc = mixed_taylor_update(Ck, (long)W * N, M, 1.f / float(k), Sacc, last ? nullptr : WtH,
-                                    last ? nullptr : WtL, st)))
-        return rc;
+      if ((rc = mixed_taylor_update(Ck, (long)W * N, M, 1.f / float(k), Sacc, last ? nullptr : Wt_p, st))) return rc;
     }
-    if ((rc = mixed_split_f32(Sacc, rows * M, WtH, WtL, st))) return rc;
-    if ((rc = tc_gemm(WtH, WtL, rows, 0, P1H, P1L, M, 0, M, 1, Ck, M, 0, 1.f))) return rc;    // P1 S
+    if ((rc = mixed_split_f32(Sacc, rows * M, Wt_p, st))) return rc;
+    if ((rc = tc_gemm(Wt_p, rows, 0, P1_p, M, 0, M, 1, Ck, M, 0, 1.f))) return rc;    // P1 S
     if ((rc = mixed_wt_to_walkers(Ck, W, M, N, SM, st))) return rc;
     ph_end(SFQ_PH_PROPAGATE);
     ph_begin(SFQ_PH_OVERLAP);
@@ -622,8 +635,9 @@ int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const dou
   e.trial_real = true;
   for (long i = 0; i < (long)e.N * e.M; ++i)
     if (ps[i].y != 0.0) { e.trial_real = false; break; }
-  e.mixed = p->precision == SFQ_PRECISION_MIXED;
-  if (p->precision != SFQ_PRECISION_FP64 && p->precision != SFQ_PRECISION_MIXED) {
+  e.mixed = p->precision == SFQ_PRECISION_MIXED || p->precision == SFQ_PRECISION_MIXED_FP32;
+  e.nplanes = p->precision == SFQ_PRECISION_MIXED_FP32 ? 3 : 2;
+  if (p->precision != SFQ_PRECISION_FP64 && !e.mixed) {
     delete h;
     return record_error(SFQ_ERR_ARG, "engine: unknown precision %d", p->precision);
   }

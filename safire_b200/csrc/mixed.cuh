@@ -5,13 +5,14 @@
 
 namespace sfq {
 
-int mixed_split_planar(const cplx* src, int W, long E, void* hi, void* lo, cudaStream_t st);
+// `pl` points at 3 plane pointers (p0, p1, p2); unused planes are null
+int mixed_split_planar(const cplx* src, int W, long E, void* const* pl, cudaStream_t st);
 int mixed_planar_to_cplx(const float* C, int W, long E, double alpha, cplx* out, cudaStream_t st);
-int mixed_build_vblk(const float* Cv, int W, int M, void* hi, void* lo, cudaStream_t st);
-int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* hi, void* lo, cudaStream_t st);
+int mixed_build_vblk(const float* Cv, int W, int M, void* const* pl, cudaStream_t st);
+int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* const* pl, cudaStream_t st);
 int mixed_wt_to_walkers(const float* C2, int W, int M, int N, cplx* SM, cudaStream_t st);
-int mixed_taylor_update(const float* C, long rows, int M, float inv_k, float* S, void* hi, void* lo,
-                        cudaStream_t st);
-int mixed_split_f32(const float* src, long n, void* hi, void* lo, cudaStream_t st);
+// pl == null: only accumulate into S (last Taylor term)
+int mixed_taylor_update(const float* C, long rows, int M, float inv_k, float* S, void* const* pl, cudaStream_t st);
+int mixed_split_f32(const float* src, long n, void* const* pl, cudaStream_t st);
 
 }  // namespace sfq

@@ -15,15 +15,38 @@
 namespace sfq {
 namespace {
 
-__device__ __forceinline__ void split_store(float x, __nv_bfloat16* hi, __nv_bfloat16* lo, long idx) {
-  const __nv_bfloat16 h = __float2bfloat16_rn(x);
-  hi[idx] = h;
-  lo[idx] = __float2bfloat16_rn(x - __bfloat162float(h));
+// operand planes: p0 = bf16(x), p1 = bf16(x - p0), p2 = bf16(x - p0 - p1) (null planes skipped)
+struct Planes {
+  __nv_bfloat16 *p0, *p1, *p2;
+};
+
+__device__ __forceinline__ void split_store(float x, const Planes& P, long idx) {
+  const __nv_bfloat16 h0 = __float2bfloat16_rn(x);
+  P.p0[idx] = h0;
+  if (P.p1) {
+    const float r1 = x - __bfloat162float(h0);
+    const __nv_bfloat16 h1 = __float2bfloat16_rn(r1);
+    P.p1[idx] = h1;
+    if (P.p2) P.p2[idx] = __float2bfloat16_rn(r1 - __bfloat162float(h1));
+  }
 }
-__device__ __forceinline__ void split_store_d(double x, __nv_bfloat16* hi, __nv_bfloat16* lo, long idx) {
-  const __nv_bfloat16 h = __float2bfloat16_rn(float(x));
-  hi[idx] = h;
-  lo[idx] = __float2bfloat16_rn(float(x - double(__bfloat162float(h))));
+__device__ __forceinline__ void split_store_d(double x, const Planes& P, long idx) {
+  const __nv_bfloat16 h0 = __float2bfloat16_rn(float(x));
+  P.p0[idx] = h0;
+  if (P.p1) {
+    const double r1 = x - double(__bfloat162float(h0));
+    const __nv_bfloat16 h1 = __float2bfloat16_rn(float(r1));
+    P.p1[idx] = h1;
+    if (P.p2) P.p2[idx] = __float2bfloat16_rn(float(r1 - double(__bfloat162float(h1))));
+  }
+}
+
+Planes planes(void* const* pl) {
+  Planes P;
+  P.p0 = (__nv_bfloat16*)pl[0];
+  P.p1 = (__nv_bfloat16*)pl[1];
+  P.p2 = (__nv_bfloat16*)pl[2];
+  return P;
 }
 
 inline int grid_for(long n) {
@@ -33,13 +56,13 @@ inline int grid_for(long n) {
 }
 
 // complex (W, E) -> planar split rows c*W + w
-__global__ void split_planar_kernel(const cplx* src, int W, long E, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+__global__ void split_planar_kernel(const cplx* src, int W, long E, Planes P) {
   const long total = (long)W * E;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
     const long w = t / E, e = t % E;
     const cplx z = src[t];
-    split_store_d(z.x, hi, lo, w * E + e);
-    split_store_d(z.y, hi, lo, ((long)W + w) * E + e);
+    split_store_d(z.x, P, w * E + e);
+    split_store_d(z.y, P, ((long)W + w) * E + e);
   }
 }
 
@@ -53,7 +76,7 @@ __global__ void planar_to_cplx_kernel(const float* C, int W, long E, double alph
 }
 
 // planar vHS (rows c*W + w, columns i*M + k) -> VB[w] = [[Vr, -Vi], [Vi, Vr]] split
-__global__ void build_vblk_kernel(const float* Cv, int W, int M, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+__global__ void build_vblk_kernel(const float* Cv, int W, int M, Planes P) {
   const long MM = (long)M * M;
   const long total = (long)W * MM;
   const long M2 = 2L * M;
@@ -63,15 +86,15 @@ __global__ void build_vblk_kernel(const float* Cv, int W, int M, __nv_bfloat16* 
     const float vr = Cv[w * MM + r];
     const float vi = Cv[((long)W + w) * MM + r];
     const long base = w * M2 * M2;
-    split_store(vr, hi, lo, base + i * M2 + k);             // (0,i),(0,k):  Vr
-    split_store(-vi, hi, lo, base + i * M2 + M + k);        // (0,i),(1,k): -Vi
-    split_store(vi, hi, lo, base + (M + i) * M2 + k);       // (1,i),(0,k):  Vi
-    split_store(vr, hi, lo, base + (M + i) * M2 + M + k);   // (1,i),(1,k):  Vr
+    split_store(vr, P, base + i * M2 + k);             // (0,i),(0,k):  Vr
+    split_store(-vi, P, base + i * M2 + M + k);        // (0,i),(1,k): -Vi
+    split_store(vi, P, base + (M + i) * M2 + k);       // (1,i),(0,k):  Vi
+    split_store(vr, P, base + (M + i) * M2 + M + k);   // (1,i),(1,k):  Vr
   }
 }
 
 // SM (W, M, N) complex fp64 -> WT[w][a][c][i] split, 32x32 tiles through shared memory
-__global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+__global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, Planes P) {
   __shared__ cplx tile[32][33];
   const int w = blockIdx.z;
   const int i0 = blockIdx.y * 32, a0 = blockIdx.x * 32;
@@ -86,8 +109,8 @@ __global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, __nv_bfloat16
     const int a = a0 + r, i = i0 + threadIdx.x;
     if (i < M && a < N) {
       const cplx z = tile[threadIdx.x][r];
-      split_store_d(z.x, hi, lo, base + ((long)a * 2 + 0) * M + i);
-      split_store_d(z.y, hi, lo, base + ((long)a * 2 + 1) * M + i);
+      split_store_d(z.x, P, base + ((long)a * 2 + 0) * M + i);
+      split_store_d(z.y, P, base + ((long)a * 2 + 1) * M + i);
     }
   }
 }
@@ -116,8 +139,7 @@ __global__ void wt_to_walkers_kernel(const float* C2, int M, int N, cplx* SM) {
 }
 
 // T_{k+1} = (i/k) C: T[a][(0,i)] = -C[a][(1,i)]/k, T[a][(1,i)] = C[a][(0,i)]/k; S += T; split T
-__global__ void taylor_update_kernel(const float* C, long rows, int M, float inv_k, float* S, __nv_bfloat16* hi,
-                                     __nv_bfloat16* lo) {
+__global__ void taylor_update_kernel(const float* C, long rows, int M, float inv_k, float* S, Planes P) {
   const long total = rows * M;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
     const long row = t / M, i = t % M;
@@ -126,22 +148,22 @@ __global__ void taylor_update_kernel(const float* C, long rows, int M, float inv
     const float tr = -ci * inv_k, ti = cr * inv_k;
     S[o0] += tr;
     S[o1] += ti;
-    if (hi) {
-      split_store(tr, hi, lo, o0);
-      split_store(ti, hi, lo, o1);
+    if (P.p0) {
+      split_store(tr, P, o0);
+      split_store(ti, P, o1);
     }
   }
 }
 
-__global__ void split_f32_kernel(const float* src, long n, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+__global__ void split_f32_kernel(const float* src, long n, Planes P) {
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
-    split_store(src[e], hi, lo, e);
+    split_store(src[e], P, e);
 }
 
 }  // namespace
 
-int mixed_split_planar(const cplx* src, int W, long E, void* hi, void* lo, cudaStream_t st) {
-  split_planar_kernel<<<grid_for((long)W * E), 256, 0, st>>>(src, W, E, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+int mixed_split_planar(const cplx* src, int W, long E, void* const* pl, cudaStream_t st) {
+  split_planar_kernel<<<grid_for((long)W * E), 256, 0, st>>>(src, W, E, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
@@ -152,15 +174,15 @@ int mixed_planar_to_cplx(const float* C, int W, long E, double alpha, cplx* out,
   return SFQ_OK;
 }
 
-int mixed_build_vblk(const float* Cv, int W, int M, void* hi, void* lo, cudaStream_t st) {
-  build_vblk_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Cv, W, M, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+int mixed_build_vblk(const float* Cv, int W, int M, void* const* pl, cudaStream_t st) {
+  build_vblk_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Cv, W, M, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
-int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* hi, void* lo, cudaStream_t st) {
+int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* const* pl, cudaStream_t st) {
   dim3 grid((N + 31) / 32, (M + 31) / 32, W), block(32, 8);
-  walkers_to_wt_kernel<<<grid, block, 0, st>>>(SM, M, N, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+  walkers_to_wt_kernel<<<grid, block, 0, st>>>(SM, M, N, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
@@ -172,16 +194,15 @@ int mixed_wt_to_walkers(const float* C2, int W, int M, int N, cplx* SM, cudaStre
   return SFQ_OK;
 }
 
-int mixed_taylor_update(const float* C, long rows, int M, float inv_k, float* S, void* hi, void* lo,
-                        cudaStream_t st) {
-  taylor_update_kernel<<<grid_for(rows * M), 256, 0, st>>>(C, rows, M, inv_k, S, (__nv_bfloat16*)hi,
-                                                           (__nv_bfloat16*)lo);
+int mixed_taylor_update(const float* C, long rows, int M, float inv_k, float* S, void* const* pl, cudaStream_t st) {
+  Planes P = pl ? planes(pl) : Planes{nullptr, nullptr, nullptr};
+  taylor_update_kernel<<<grid_for(rows * M), 256, 0, st>>>(C, rows, M, inv_k, S, P);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
-int mixed_split_f32(const float* src, long n, void* hi, void* lo, cudaStream_t st) {
-  split_f32_kernel<<<grid_for(n), 256, 0, st>>>(src, n, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+int mixed_split_f32(const float* src, long n, void* const* pl, cudaStream_t st) {
+  split_f32_kernel<<<grid_for(n), 256, 0, st>>>(src, n, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

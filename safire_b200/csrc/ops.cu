@@ -354,33 +354,39 @@ int sfq_assemble_x(void* X, const double* vmf, void* hw, void* mf, const double*
 }
 
 int sfq_gemm_split_bf16(const double* A, const double* B, float* C, int M, int N, int K, int batch, int a_batched,
-                        int b_batched, int nterms, int tile_n, void* stream) {
+                        int b_batched, int nplanes, int tile_n, void* stream) {
   if (M < 0 || N < 0 || K < 0 || batch < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
   if (!M || !N || !batch) return SFQ_OK;
   if (!A || !B || !C) return record_error(SFQ_ERR_ARG, "null pointer");
   if (K % 8) return record_error(SFQ_ERR_SHAPE, "sfq_gemm_split_bf16: K must be a multiple of 8");
-  return gemm_split_bf16_f64(A, B, C, M, N, K, batch, a_batched, b_batched, nterms, tile_n, S(stream));
+  return gemm_split_bf16_f64(A, B, C, M, N, K, batch, a_batched, b_batched, nplanes, tile_n, S(stream));
 }
 
-int sfq_split_bf16(const double* src, long n, void* hi, void* lo, void* stream) {
+int sfq_split_bf16(const double* src, long n, void* p0, void* p1, void* p2, void* stream) {
   if (n < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
   if (n == 0) return SFQ_OK;
-  if (!src || !hi) return record_error(SFQ_ERR_ARG, "null pointer");
-  return split_bf16_f64(src, n, hi, lo, S(stream));
+  if (!src || !p0) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (p2 && !p1) return record_error(SFQ_ERR_ARG, "plane 2 needs plane 1");
+  return split_bf16_f64(src, n, p0, p1, p2, S(stream));
 }
 
-int sfq_gemm_bf16_planes(const void* A_hi, const void* A_lo, const void* B_hi, const void* B_lo, float* C, int M,
-                         int N, int K, int batch, long a_batch_stride, long b_batch_stride, float alpha, float beta,
-                         int nterms, int tile_n, void* stream) {
+int sfq_gemm_bf16_planes(const void* const* A, const void* const* B, int nplanes, float* C, int M, int N, int K,
+                         int batch, long a_batch_stride, long b_batch_stride, float alpha, float beta, int tile_n,
+                         void* stream) {
   if (M < 0 || N < 0 || K < 0 || batch < 0) return record_error(SFQ_ERR_SHAPE, "negative size");
   if (!M || !N || !batch) return SFQ_OK;
-  if (!A_hi || !B_hi || !C) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (!A || !B || !C) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (nplanes < 1 || nplanes > 3) return record_error(SFQ_ERR_ARG, "nplanes must be 1, 2 or 3");
   UmmaGemmDesc d;
   d.M = M; d.N = N; d.K = K; d.batch = batch;
-  d.A.hi = A_hi; d.A.lo = A_lo; d.A.rows = M; d.A.ld = K; d.A.batch_stride = a_batch_stride;
-  d.B.hi = B_hi; d.B.lo = B_lo; d.B.rows = N; d.B.ld = K; d.B.batch_stride = b_batch_stride;
+  for (int q = 0; q < nplanes; ++q) {
+    d.A.p[q] = A[q];
+    d.B.p[q] = B[q];
+  }
+  d.A.rows = M; d.A.ld = K; d.A.batch_stride = a_batch_stride;
+  d.B.rows = N; d.B.ld = K; d.B.batch_stride = b_batch_stride;
   d.C = C; d.ldc = N; d.sCb = (long)M * N;
-  d.alpha = alpha; d.beta = beta; d.nterms = nterms; d.bn = tile_n;
+  d.alpha = alpha; d.beta = beta; d.nplanes = nplanes; d.bn = tile_n;
   return umma_gemm(d, S(stream));
 }
 

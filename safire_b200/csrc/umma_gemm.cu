@@ -21,9 +21,14 @@ struct KParams {
   float* C;
   long ldc, sCb;
   float alpha, beta;
-  int nterms;
   int* err;
 };
+
+// products (plane of A, plane of B) kept for NP planes: the pairs of combined order < NP, listed
+// so that NP = 1, 2, 3 use the first 1, 3, 6 entries
+__host__ __device__ constexpr int n_terms(int np) { return np == 1 ? 1 : np == 2 ? 3 : 6; }
+__host__ __device__ constexpr int term_a(int t) { return t < 2 ? 0 : t == 2 ? 1 : t == 3 ? 0 : t == 4 ? 1 : 2; }
+__host__ __device__ constexpr int term_b(int t) { return t == 0 ? 0 : t == 1 ? 1 : t == 2 ? 0 : t == 3 ? 2 : t == 4 ? 1 : 0; }
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -119,21 +124,23 @@ __host__ __device__ constexpr uint32_t tmem_cols() {
   return BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int NP>
 struct Smem {
   static constexpr int A_BYTES = BM * BK * 2;
   static constexpr int B_BYTES = BN * BK * 2;
-  static constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int STAGE = NP * (A_BYTES + B_BYTES);
   static constexpr int BAR_OFF = STAGES * STAGE;
   static constexpr int TOTAL = BAR_OFF + (2 * STAGES + 1) * 8 + 16 + 1024;  // + alignment slack
   static_assert(A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "tiles must keep 1024-byte alignment");
 };
 
-template <int BN, int STAGES>
-__global__ void __launch_bounds__(kThreads, 1)
-    umma_gemm_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
-                     const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, KParams p) {
-  using L = Smem<BN, STAGES>;
+struct Maps {
+  CUtensorMap a[3], b[3];
+};
+
+template <int BN, int STAGES, int NP>
+__global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_constant__ Maps maps, KParams p) {
+  using L = Smem<BN, STAGES, NP>;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
@@ -145,8 +152,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN, bz = blockIdx.z;
   const int KT = (p.K + BK - 1) / BK;
-  const bool three = p.nterms == 3;
-  const uint32_t stage_tx = three ? uint32_t(2 * L::A_BYTES + 2 * L::B_BYTES) : uint32_t(L::A_BYTES + L::B_BYTES);
+  const uint32_t stage_tx = uint32_t(L::STAGE);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -183,11 +189,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_expect_tx(&full[s], stage_tx);
         const int k0 = kt * BK;
         const int ab = p.a_batched ? bz : 0, bb = p.b_batched ? bz : 0;
-        tma_load_3d(st, &tAh, &full[s], k0, m0, ab);
-        tma_load_3d(st + 2 * L::A_BYTES, &tBh, &full[s], k0, n0, bb);
-        if (three) {
-          tma_load_3d(st + L::A_BYTES, &tAl, &full[s], k0, m0, ab);
-          tma_load_3d(st + 2 * L::A_BYTES + L::B_BYTES, &tBl, &full[s], k0, n0, bb);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+          tma_load_3d(st + q * L::A_BYTES, &maps.a[q], &full[s], k0, m0, ab);
+          tma_load_3d(st + NP * L::A_BYTES + q * L::B_BYTES, &maps.b[q], &full[s], k0, n0, bb);
         }
         issued = kt + 1;
       }
@@ -207,16 +212,18 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         fence_after();
         unsigned char* st = smem + s * L::STAGE;
-        const uint64_t ah = smem_desc(st), al = smem_desc(st + L::A_BYTES);
-        const uint64_t bh = smem_desc(st + 2 * L::A_BYTES), bl = smem_desc(st + 2 * L::A_BYTES + L::B_BYTES);
+        uint64_t ad[NP], bd[NP];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+          ad[q] = smem_desc(st + q * L::A_BYTES);
+          bd[q] = smem_desc(st + NP * L::A_BYTES + q * L::B_BYTES);
+        }
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk) {
           const uint64_t off = uint64_t(kk * 32) >> 4;  // 16 bf16 = 32 bytes along the swizzled row
-          umma_bf16(tmem, ah + off, bh + off, idesc, (kt | kk) ? 1u : 0u);
-          if (three) {
-            umma_bf16(tmem, ah + off, bl + off, idesc, 1u);
-            umma_bf16(tmem, al + off, bh + off, idesc, 1u);
-          }
+#pragma unroll
+          for (int tt = 0; tt < n_terms(NP); ++tt)
+            umma_bf16(tmem, ad[term_a(tt)] + off, bd[term_b(tt)] + off, idesc, (kt | kk | tt) ? 1u : 0u);
         }
         umma_commit(&empty[s]);
       }
@@ -300,41 +307,46 @@ int make_map(CUtensorMap* m, const void* base, long rows, long K, long ld, long 
   return SFQ_OK;
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int NP>
 int launch(const UmmaGemmDesc& d, cudaStream_t st) {
-  using L = Smem<BN, STAGES>;
-  CUtensorMap ah, al, bh, bl;
+  using L = Smem<BN, STAGES, NP>;
+  static_assert(L::TOTAL <= 232448, "shared memory budget");
+  Maps maps;
   int rc;
   const long ab = d.A.batch_stride ? d.batch : 1, bb = d.B.batch_stride ? d.batch : 1;
-  if ((rc = make_map(&ah, d.A.hi, d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
-  if ((rc = make_map(&bh, d.B.hi, d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, BN))) return rc;
-  if (d.nterms == 3) {
-    if ((rc = make_map(&al, d.A.lo, d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
-    if ((rc = make_map(&bl, d.B.lo, d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, BN))) return rc;
-  } else {
-    al = ah;
-    bl = bh;
+  for (int q = 0; q < NP; ++q) {
+    if (!d.A.p[q] || !d.B.p[q]) return record_error(SFQ_ERR_ARG, "umma_gemm: plane %d missing", q);
+    if ((rc = make_map(&maps.a[q], d.A.p[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
+    if ((rc = make_map(&maps.b[q], d.B.p[q], d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, BN))) return rc;
+  }
+  for (int q = NP; q < 3; ++q) {
+    maps.a[q] = maps.a[0];
+    maps.b[q] = maps.b[0];
   }
   KParams kp;
   kp.M = d.M; kp.N = d.N; kp.K = d.K;
   kp.a_batched = d.A.batch_stride != 0; kp.b_batched = d.B.batch_stride != 0;
   kp.C = d.C; kp.ldc = d.ldc; kp.sCb = d.sCb; kp.alpha = d.alpha; kp.beta = d.beta;
-  kp.nterms = d.nterms; kp.err = d.err;
-  auto k = umma_gemm_kernel<BN, STAGES>;
+  kp.err = d.err;
+  auto k = umma_gemm_kernel<BN, STAGES, NP>;
   SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
   dim3 grid((d.M + BM - 1) / BM, (d.N + BN - 1) / BN, d.batch);
   if (grid.y > 65535u || grid.z > 65535u) return record_error(SFQ_ERR_SHAPE, "umma_gemm: grid too large");
-  k<<<grid, kThreads, L::TOTAL, st>>>(ah, al, bh, bl, kp);
+  k<<<grid, kThreads, L::TOTAL, st>>>(maps, kp);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
-__global__ void split_f64_kernel(const double* src, long n, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+__global__ void split_f64_kernel(const double* src, long n, __nv_bfloat16* p0, __nv_bfloat16* p1,
+                                 __nv_bfloat16* p2) {
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
     const double x = src[e];
-    const __nv_bfloat16 h = __float2bfloat16_rn(float(x));
-    hi[e] = h;
-    if (lo) lo[e] = __float2bfloat16_rn(float(x - double(__bfloat162float(h))));
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(float(x));
+    p0[e] = h0;
+    const double r1 = x - double(__bfloat162float(h0));
+    const __nv_bfloat16 h1 = __float2bfloat16_rn(float(r1));
+    if (p1) p1[e] = h1;
+    if (p2) p2[e] = __float2bfloat16_rn(float(r1 - double(__bfloat162float(h1))));
   }
 }
 
@@ -343,50 +355,59 @@ __global__ void split_f64_kernel(const double* src, long n, __nv_bfloat16* hi, _
 int umma_gemm(const UmmaGemmDesc& d, cudaStream_t st) {
   if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return SFQ_OK;
   if (d.K <= 0) return record_error(SFQ_ERR_SHAPE, "umma_gemm: K must be positive");
-  if (d.nterms != 1 && d.nterms != 3) return record_error(SFQ_ERR_ARG, "umma_gemm: nterms must be 1 or 3");
-  if (d.nterms == 3 && (!d.A.lo || !d.B.lo)) return record_error(SFQ_ERR_ARG, "umma_gemm: lo planes missing");
   const int bn = d.bn ? d.bn : (d.N <= 64 ? 64 : 128);
-  switch (bn) {
-    case 64: return umma::launch<64, 4>(d, st);
-    case 128: return umma::launch<128, 3>(d, st);
-    case 256: return umma::launch<256, 2>(d, st);
-    default: return record_error(SFQ_ERR_ARG, "umma_gemm: tile width %d not built (64, 128, 256)", bn);
+  switch (d.nplanes * 1000 + bn) {
+    case 1064: return umma::launch<64, 6, 1>(d, st);
+    case 1128: return umma::launch<128, 6, 1>(d, st);
+    case 1256: return umma::launch<256, 4, 1>(d, st);
+    case 2064: return umma::launch<64, 4, 2>(d, st);
+    case 2128: return umma::launch<128, 3, 2>(d, st);
+    case 2256: return umma::launch<256, 2, 2>(d, st);
+    case 3064: return umma::launch<64, 3, 3>(d, st);
+    case 3128: return umma::launch<128, 2, 3>(d, st);
+    default:
+      return record_error(SFQ_ERR_ARG, "umma_gemm: %d planes with tile width %d not built", d.nplanes, bn);
   }
 }
 
 // C ABI test/benchmark entry: fp64 operands split on the fly
 int gemm_split_bf16_f64(const double* A, const double* B, float* C, int M, int N, int K, int batch, int a_batched,
-                        int b_batched, int nterms, int bn, cudaStream_t st) {
+                        int b_batched, int nplanes, int bn, cudaStream_t st) {
+  if (nplanes < 1 || nplanes > 3) return record_error(SFQ_ERR_ARG, "nplanes must be 1, 2 or 3");
   const long na = (long)M * K * (a_batched ? batch : 1), nb = (long)N * K * (b_batched ? batch : 1);
-  void* buf = nullptr;
-  const size_t bytes = size_t(2) * 2 * (na + nb) + 1024;
-  SFQ_CUDA_TRY(cudaMallocAsync(&buf, bytes, st));
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t pa = al(2 * na), pb = al(2 * nb);
+  void* buf = nullptr;
+  SFQ_CUDA_TRY(cudaMallocAsync(&buf, nplanes * (pa + pb) + 256, st));
   char* base = (char*)buf;
-  void* ah = base;
-  void* alo = base + al(2 * na);
-  void* bh = base + 2 * al(2 * na);
-  void* blo = base + 2 * al(2 * na) + al(2 * nb);
-  int rc = split_bf16_f64(A, na, ah, alo, st);
-  if (!rc) rc = split_bf16_f64(B, nb, bh, blo, st);
+  UmmaGemmDesc d;
+  for (int q = 0; q < nplanes; ++q) {
+    d.A.p[q] = base + q * pa;
+    d.B.p[q] = base + nplanes * pa + q * pb;
+  }
+  int rc = split_bf16_f64(A, na, (void*)d.A.p[0], nplanes > 1 ? (void*)d.A.p[1] : nullptr,
+                          nplanes > 2 ? (void*)d.A.p[2] : nullptr, st);
+  if (!rc)
+    rc = split_bf16_f64(B, nb, (void*)d.B.p[0], nplanes > 1 ? (void*)d.B.p[1] : nullptr,
+                        nplanes > 2 ? (void*)d.B.p[2] : nullptr, st);
   if (!rc) {
-    UmmaGemmDesc d;
     d.M = M; d.N = N; d.K = K; d.batch = batch;
-    d.A.hi = ah; d.A.lo = alo; d.A.rows = M; d.A.ld = K; d.A.batch_stride = a_batched ? (long)M * K : 0;
-    d.B.hi = bh; d.B.lo = blo; d.B.rows = N; d.B.ld = K; d.B.batch_stride = b_batched ? (long)N * K : 0;
+    d.A.rows = M; d.A.ld = K; d.A.batch_stride = a_batched ? (long)M * K : 0;
+    d.B.rows = N; d.B.ld = K; d.B.batch_stride = b_batched ? (long)N * K : 0;
     d.C = C; d.ldc = N; d.sCb = (long)M * N;
-    d.nterms = nterms; d.bn = bn;
+    d.nplanes = nplanes; d.bn = bn;
     rc = umma_gemm(d, st);
   }
   cudaFreeAsync(buf, st);
   return rc;
 }
 
-int split_bf16_f64(const double* src, long n, void* hi, void* lo, cudaStream_t st) {
+int split_bf16_f64(const double* src, long n, void* p0, void* p1, void* p2, cudaStream_t st) {
   if (n <= 0) return SFQ_OK;
   long g = (n + 255) / 256;
   if (g > 148 * 16) g = 148 * 16;
-  umma::split_f64_kernel<<<int(g), 256, 0, st>>>(src, n, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo);
+  umma::split_f64_kernel<<<int(g), 256, 0, st>>>(src, n, (__nv_bfloat16*)p0, (__nv_bfloat16*)p1,
+                                                 (__nv_bfloat16*)p2);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

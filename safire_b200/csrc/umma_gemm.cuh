@@ -2,10 +2,13 @@
 //
 //   C[b] (M x N, fp32) = alpha * sum_t A_t[b] (M x K) * B_t[b] (N x K)^T  (+ beta * C[b])
 //
-// Every operand is held as two BF16 planes, x ~= hi + lo with hi = bf16(x), lo = bf16(x - hi),
-// and the product is taken as hi*hi + hi*lo + lo*hi with FP32 accumulation in tensor memory:
-// about 16 significant bits per operand, the "complex FP32 from split-BF16" arithmetic of the
-// mixed-precision propagation.  nterms = 1 keeps hi*hi only.
+// Every operand is held as BF16 planes, x ~= p0 + p1 (+ p2) with p0 = bf16(x), p1 = bf16(x - p0),
+// p2 = bf16(x - p0 - p1), and the product keeps the terms of combined order <= nplanes - 1:
+//   1 plane : p0 q0                                   ( 8 significant bits)
+//   2 planes: p0 q0 + p0 q1 + p1 q0                   (~16 bits, 3 tensor-core products)
+//   3 planes: + p0 q2 + p1 q1 + p2 q0                 (~24 bits = FP32 class, 6 products)
+// all accumulated in FP32 in tensor memory: the "complex FP32 from split-BF16" arithmetic of the
+// mixed-precision propagation.
 //
 // Operands are K-major (K contiguous), loaded by TMA as 64-element (128-byte) K slices with the
 // 128-byte swizzle; one elected thread issues tcgen05.mma (M = 128, N = BN, K = 16) on the smem
@@ -20,8 +23,7 @@
 namespace sfq {
 
 struct UmmaOperand {
-  const void* hi = nullptr;  // bf16 (rows, K) per batch, K contiguous
-  const void* lo = nullptr;  // same layout; may be null when nterms == 1
+  const void* p[3] = {nullptr, nullptr, nullptr};  // bf16 planes (rows, K) per batch, K contiguous
   long rows = 0;             // rows per batch
   long ld = 0;               // elements between rows (>= K, multiple of 8)
   long batch_stride = 0;     // elements between batches (0: shared)
@@ -33,17 +35,17 @@ struct UmmaGemmDesc {
   float* C = nullptr;
   long ldc = 0, sCb = 0;  // fp32 row-major output
   float alpha = 1.f, beta = 0.f;
-  int nterms = 3;
-  int bn = 0;             // tile width: 0 = automatic, else 64, 128 or 256
+  int nplanes = 2;        // 1, 2 or 3 (see above)
+  int bn = 0;             // tile width: 0 = automatic, else 64, 128 or 256 (256: nplanes <= 2)
   int* err = nullptr;     // device flag, SFQ_ERR_TIMEOUT on an expired wait (may be null)
 };
 
 int umma_gemm(const UmmaGemmDesc& d, cudaStream_t st);
 
 int gemm_split_bf16_f64(const double* A, const double* B, float* C, int M, int N, int K, int batch, int a_batched,
-                        int b_batched, int nterms, int bn, cudaStream_t st);
+                        int b_batched, int nplanes, int bn, cudaStream_t st);
 
-// bf16 hi/lo planes of a strided fp64 / fp32 / complex source (elementwise helpers)
-int split_bf16_f64(const double* src, long n, void* hi, void* lo, cudaStream_t st);
+// bf16 planes of an fp64 array: p0 = bf16(x), p1 = bf16(x - p0), p2 = bf16(x - p0 - p1); null planes skipped
+int split_bf16_f64(const double* src, long n, void* p0, void* p1, void* p2, cudaStream_t st);
 
 }  // namespace sfq

@@ -74,14 +74,20 @@ def run(op, M, N, Nc, W, reps, warm=2, real_lnak=True):
         st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         A = torch.randn(2 * W, Nc, generator=g, device="cuda", dtype=torch.float64)
         B = torch.randn(M * M, Nc, generator=g, device="cuda", dtype=torch.float64)
-        planes = [torch.empty(x.numel(), dtype=torch.bfloat16, device="cuda") for x in (A, A, B, B)]
-        capi.check(L.sfq_split_bf16(A.data_ptr(), A.numel(), planes[0].data_ptr(), planes[1].data_ptr(), st))
-        capi.check(L.sfq_split_bf16(B.data_ptr(), B.numel(), planes[2].data_ptr(), planes[3].data_ptr(), st))
+        env = __import__("os").environ
+        npl = int(env.get("SFQ_PLANES", "2"))
+        tn = int(env.get("SFQ_TILE_N", "0"))
+        pa = [torch.empty(A.numel(), dtype=torch.bfloat16, device="cuda") for _ in range(npl)]
+        pb = [torch.empty(B.numel(), dtype=torch.bfloat16, device="cuda") for _ in range(npl)]
+        ptr3 = lambda ps: [ps[q].data_ptr() if q < len(ps) else None for q in range(3)]  # noqa: E731
+        capi.check(L.sfq_split_bf16(A.data_ptr(), A.numel(), *ptr3(pa), st))
+        capi.check(L.sfq_split_bf16(B.data_ptr(), B.numel(), *ptr3(pb), st))
         del B
         C = torch.empty(2 * W, M * M, device="cuda", dtype=torch.float32)
-        tn = int(__import__("os").environ.get("SFQ_TILE_N", "0"))
-        fn = lambda: capi.check(L.sfq_gemm_bf16_planes(*[p.data_ptr() for p in planes], C.data_ptr(), 2 * W,  # noqa
-                                                       M * M, Nc, 1, 0, 0, 1.0, 0.0, 3, tn, st))
+        VP3 = ctypes.c_void_p * 3
+        Aarr, Barr = VP3(*ptr3(pa)), VP3(*ptr3(pb))
+        fn = lambda: capi.check(L.sfq_gemm_bf16_planes(Aarr, Barr, npl, C.data_ptr(), 2 * W, M * M, Nc, 1,  # noqa
+                                                       0, 0, 1.0, 0.0, tn, st))
     elif op == "orthogonalize":
         SM = crand(W, M, N)
         fn = lambda: afqmc.orthogonalize(SM)  # noqa: E731
