@@ -111,6 +111,12 @@ struct Engine {
   PopWork pw{};
   // mixed precision: split-BF16 planes and fp32 accumulators
   bool mixed = false;
+  // T holds the inverse overlap matrices (PsiT W)^-1 of the current walkers and inv_ov their log
+  // overlaps whenever inv_cached is set: the log overlap taken after a propagation or an
+  // orthogonalization factors exactly the matrix the next Green's function needs, so that step
+  // reuses it (same GEMM, same pivots, bit-identical G).  Every change to SM clears the flag.
+  bool inv_cached = false;
+  const cplx* inv_ov = nullptr;
   int nplanes = 3;  // bf16 planes per operand (2: ~16-bit products, 3: FP32-class)
   void* Likn_p[3] = {};
   void* Lnak_p[3] = {};
@@ -422,20 +428,32 @@ struct Engine {
     return SFQ_OK;
   }
 
-  // --- NOMSD::MixedDensityMatrix (compact, CLOSED: Ov x 2) into G, ov (W) -------------------
+  // --- NOMSD::MixedDensityMatrix (compact, CLOSED: Ov x 2) into G, ov (W; may be null) ------
   int density(cplx* ov) {
     int rc;
-    const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
-    if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, M, N, st))) return rc;
-    if ((rc = lu_logdet(T, (long)N * N, W, N, ov, false, 2.0, true, st))) return rc;
+    if (!inv_cached) {
+      const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
+      cplx* out = ov ? ov : ovtmp;
+      if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, M, N, st))) return rc;
+      if ((rc = lu_logdet(T, (long)N * N, W, N, out, false, 2.0, true, st))) return rc;
+      inv_cached = true;
+      inv_ov = out;
+    } else if (ov && ov != inv_ov) {
+      SFQ_CUDA_TRY(cudaMemcpyAsync(ov, inv_ov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
+    }
     return ops::green_compact(T, SM, G, W, M, N, st);
   }
 
+  // NOMSD::Overlap of the current walkers into ov; keeps their inverse overlap matrices in T
   int log_overlap(cplx* ov) {
     int rc;
     const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
+    inv_cached = false;
     if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, M, N, st))) return rc;
-    return lu_logdet(T, (long)N * N, W, N, ov, false, 2.0, false, st);
+    if ((rc = lu_logdet(T, (long)N * N, W, N, ov, false, 2.0, true, st))) return rc;
+    inv_cached = true;
+    inv_ov = ov;
+    return SFQ_OK;
   }
 
   // --- AFQMCBasePropagator::Propagate (hybrid) ----------------------------------------------
@@ -443,7 +461,7 @@ struct Engine {
     if (mixed) return propagate_mixed(Eshift, step, uniforms);
     int rc;
     ph_begin(SFQ_PH_DENSITY);
-    if ((rc = density(ovtmp))) return rc;                                            // 1. G
+    if ((rc = density(nullptr))) return rc;                                          // 1. G
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
     if ((rc = ops::vbias(G, Lnak, !trial_real, X, W, N, M, Nc, 2.0 * std::sqrt(p.dt), st))) return rc;
@@ -460,6 +478,7 @@ struct Engine {
     ph_end(SFQ_PH_VHS_GEMM);
     ph_end(SFQ_PH_VHS);
     ph_begin(SFQ_PH_PROPAGATE);
+    inv_cached = false;
     if ((rc = ops::propagate(SM, P1, false, V, W, M, N, p.taylor_order, TMN, T1, T2, st))) return rc;  // 4.
     ph_end(SFQ_PH_PROPAGATE);
     ph_begin(SFQ_PH_OVERLAP);
@@ -498,7 +517,7 @@ struct Engine {
     const long MM = (long)M * M, NM = (long)N * M, M2 = 2L * M;
     const double sdt = std::sqrt(p.dt);
     ph_begin(SFQ_PH_DENSITY);
-    if ((rc = density(ovtmp))) return rc;
+    if ((rc = density(nullptr))) return rc;
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
     if ((rc = mixed_split_planar(G, W, NM, Gs_p, st))) return rc;
@@ -521,6 +540,7 @@ struct Engine {
     ph_end(SFQ_PH_VHS);
     ph_begin(SFQ_PH_PROPAGATE);
     const long rows = 2L * W * N;  // (w, a, c) rows of the walker operand
+    inv_cached = false;
     if ((rc = mixed_walkers_to_wt(SM, W, M, N, Wt_p, st))) return rc;
     if ((rc = tc_gemm(Wt_p, rows, 0, P1_p, M, 0, M, 1, Sacc, M, 0, 1.f))) return rc;  // S = P1 W
     if ((rc = mixed_split_f32(Sacc, rows * M, Wt_p, st))) return rc;                  // T1 = S
@@ -551,8 +571,10 @@ struct Engine {
   int orthogonalize() {
     int rc;
     ph_begin(SFQ_PH_ORTHO);
+    inv_cached = false;
     if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, M, N, st))) return rc;
-    if ((rc = log_overlap(props + (long)P_OVLP * W))) return rc;  // wfn->Log_Overlap(wset)
+    if ((rc = log_overlap(newov))) return rc;  // wfn->Log_Overlap(wset)
+    SFQ_CUDA_TRY(cudaMemcpyAsync(props + (long)P_OVLP * W, newov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
     ph_end(SFQ_PH_ORTHO);
     return SFQ_OK;
   }
@@ -560,6 +582,7 @@ struct Engine {
   int population_control(unsigned long long call) {
     int rc;
     ph_begin(SFQ_PH_POPCONTROL);
+    inv_cached = false;
     if ((rc = sfq::population_control(SM, (long)M * N, wprops(), W, 0.0, p.seed, call, 1, pw, st))) return rc;
     ph_end(SFQ_PH_POPCONTROL);
     int flag = 0;
@@ -681,6 +704,7 @@ void* sfq_engine_stream(sfq_engine_t h) { return h ? (void*)h->e.st : nullptr; }
 int sfq_engine_set_walkers(sfq_engine_t h, const void* SM, const void* props) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
   Engine& e = h->e;
+  e.inv_cached = false;  // also the way to announce writes made through sfq_engine_info's SM pointer
   if (SM) SFQ_CUDA_TRY(cudaMemcpyAsync(e.SM, SM, sizeof(cplx) * e.W * e.M * e.N, cudaMemcpyHostToDevice, e.st));
   if (props) SFQ_CUDA_TRY(cudaMemcpyAsync(e.props, props, sizeof(cplx) * kNumProps * e.W, cudaMemcpyHostToDevice, e.st));
   SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));

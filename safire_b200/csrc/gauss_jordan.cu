@@ -2,8 +2,11 @@
 //
 // One CTA per matrix, 4*N threads.  Thread t owns column j = t / 4 and rows i = (t % 4) + 4 r,
 // r < R: the matrix lives in registers, the four owners of a column are four adjacent lanes of one
-// warp (the pivot search is a shuffle reduction), and an elimination step moves only the pivot row
-// and pivot column through shared memory (double-buffered, two barriers per step).
+// warp (the pivot search is a shuffle reduction).  One block barrier per step: the pivot column
+// and pivot go through shared memory (double-buffered), the pivot row by warp shuffles (each
+// element is needed only by the owners of its column).  The warp that holds column k+1 starts its
+// pivot search as soon as its own step-k elimination is done.  A step costs each thread one shared
+// load and four FMAs per row it owns.
 //
 // Pivoting reproduces LAPACK's partial pivoting (zgetrf): the pivot of column k is the first
 // maximum of |re| + |im| over the rows not yet pivoted, "first" in the row order LAPACK has after
@@ -11,9 +14,9 @@
 // diagonal of LAPACK's LU, and the log determinant follows log_determinant_from_getrf
 // (src/numerics/operations/determinants_impl.hpp:33-75): sum over k of log(+-U_kk + tiny), negated
 // when the pivot came from another position, imaginary part folded into [-pi, pi].
-// With INVERT the sweep is Gauss-Jordan in place and ends with A^-1[a][p_k] = B[p_a][k]
-// (p_k: pivot row of step k), scattered straight to the output; without it only the trailing
-// block is updated (an LU).  A zero pivot marks the matrix singular: the step is skipped and the
+// The sweep is Gauss-Jordan in place with the pivot rows left unscaled until the end, where
+// A^-1[a][p_k] = B[p_a][k] / U_aa (p_k: pivot row of step k) is scattered straight to the output
+// with INVERT; without it only the log det is written.  A zero pivot marks the matrix singular: the step is skipped and the
 // inverse is written as zeros (getri_or_zero, src/numerics/nda_functions.hpp:422-438).
 #include "common.cuh"
 #include "kernels.cuh"
@@ -25,11 +28,56 @@ constexpr int kGjMaxN = 128;
 
 __device__ __forceinline__ double cabs1(cplx a) { return fabs(a.x) + fabs(a.y); }
 
+// |re| + |im| of the rows still unpivoted (bit r of `pivoted` set: row g + 4r is done), else -1
+__device__ __forceinline__ double cand_abs(cplx z, bool cand) { return cand ? cabs1(z) : -1.0; }
+
+// the largest candidate of one owner, its smallest index, and whether it occurs twice: NQ
+// interleaved running maxima, each with the bit mask of the indices that attain it, so that the
+// dependent depth is about R/NQ rather than R and no candidate has to stay live (three chains
+// for R = 25, whose 100 registers of matrix leave no room for a fourth)
+template <int R>
+__device__ __forceinline__ void owner_max(const cplx (&a)[R], int g, int N, unsigned pivoted, double& best, int& idx,
+                                          bool& tie) {
+  constexpr int NQ = R > 16 ? 3 : 4;
+  double m[4] = {-1.0, -1.0, -1.0, -1.0};
+  unsigned msk[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const double v = cand_abs(a[r], g + 4 * r < N && !((pivoted >> r) & 1u));
+    const int q = r % NQ;
+    if (v > m[q]) {
+      m[q] = v;
+      msk[q] = 1u << r;
+    } else if (v == m[q]) {
+      msk[q] |= 1u << r;
+    }
+  }
+  best = fmax(fmax(m[0], m[1]), fmax(m[2], m[3]));
+  unsigned mask = 0;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) mask |= (m[q] == best) ? msk[q] : 0u;
+  idx = __ffs(mask) - 1;
+  tie = best >= 0.0 && __popc(mask) > 1;
+}
+
+// dst = v when r == sel: a compare and a predicated shared store, so that a thread can hand out
+// the register of a run-time row without a chain of selects over its whole array
+__device__ __forceinline__ void st_shared_if(cplx* dst, cplx v, int r, int sel) {
+  const unsigned addr = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile(
+      "{\n\t.reg .pred q;\n\t"
+      "setp.eq.s32 q, %0, %1;\n\t"
+      "@q st.shared.v2.f64 [%2], {%3, %4};\n\t}" ::"r"(r),
+      "r"(sel), "r"(addr), "d"(v.x), "d"(v.y)
+      : "memory");
+}
+
 template <int R, bool INVERT>
-__global__ void __launch_bounds__(4 * 4 * R + 32)
+__global__ void __launch_bounds__(((16 * R + 31) / 32) * 32)
     gj_kernel(cplx* T, long sT, int N, cplx* ovlp, int accumulate, double post_scale) {
   __shared__ cplx prow[2][kGjMaxN];
   __shared__ cplx pcol[2][kGjMaxN];
+  __shared__ cplx pinv_of[kGjMaxN];     // 1 / U_kk, for the deferred row scaling
   __shared__ cplx diag[kGjMaxN];        // U_kk, for the log det
   __shared__ unsigned char flip[kGjMaxN];
   __shared__ int pos_of[kGjMaxN];       // LAPACK position of each physical row
@@ -38,6 +86,7 @@ __global__ void __launch_bounds__(4 * 4 * R + 32)
   __shared__ int piv_row[kGjMaxN];      // pivot row of each step
   __shared__ int s_p[2];
   __shared__ cplx s_pinv[2];
+  __shared__ cplx s_bz;
   __shared__ int s_singular;
 
   const int t = threadIdx.x;
@@ -57,6 +106,11 @@ __global__ void __launch_bounds__(4 * 4 * R + 32)
     pos_of[i] = i;
     row_at[i] = i;
   }
+  // rows N .. 4R-1 of the pivot column stay zero, so the padding rows stay zero without a test
+  for (int i = N + t; i < 4 * R; i += blockDim.x) {
+    pcol[0][i] = mk(0.0, 0.0);
+    pcol[1][i] = mk(0.0, 0.0);
+  }
   if (t == 0) s_singular = 0;
   __syncthreads();
 
@@ -65,46 +119,72 @@ __global__ void __launch_bounds__(4 * 4 * R + 32)
     // (a) the warp holding column k: candidate per lane, shuffle reduction, winner bookkeeping
     if ((k >> 3) == (t >> 5)) {  // column k lives in lanes 4*(k%8) .. +3 of warp k/8
       const bool mine = (j == k);
-      double best = -1.0;
-      int brow = 1 << 30;
-      cplx bz = mk(0.0, 0.0);
       if (mine) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int i = g + 4 * r;
-          if (i < N) {
-            pcol[buf][i] = a[r];
-            if (!((pivoted >> r) & 1u)) {
-              const double v = cabs1(a[r]);
-              if (v > best) {
-                best = v;
-                brow = i;
-                bz = a[r];
-              } else if (v == best && pos_of[i] < pos_of[brow]) {
-                brow = i;
-                bz = a[r];
-              }
-            }
-          }
-        }
+        for (int r = 0; r < R; ++r)
+          if (g + 4 * r < N) pcol[buf][g + 4 * r] = a[r];
       }
+      double best = -1.0;
+      int br = 0;
+      bool tie = false;
+      if (mine) owner_max<R>(a, g, N, pivoted, best, br, tie);
+      int brow = (best >= 0.0) ? g + 4 * br : (1 << 30);
       // reduce over the 4 owners (adjacent lanes, aligned to 4)
 #pragma unroll
       for (int off = 1; off < 4; off <<= 1) {
         const double ob = __shfl_xor_sync(0xffffffffu, best, off);
         const int orow = __shfl_xor_sync(0xffffffffu, brow, off);
-        const double ozx = __shfl_xor_sync(0xffffffffu, bz.x, off);
-        const double ozy = __shfl_xor_sync(0xffffffffu, bz.y, off);
-        bool take = ob > best;
-        if (!take && ob == best && ob >= 0.0 && orow < N && brow < N) take = pos_of[orow] < pos_of[brow];
-        if (take) {
+        const int otie = __shfl_xor_sync(0xffffffffu, int(tie), off);
+        if (ob > best) {
           best = ob;
           brow = orow;
-          bz = mk(ozx, ozy);
+          tie = otie != 0;
+        } else if (ob == best && ob >= 0.0) {
+          tie = true;
         }
       }
+      // only the four lanes of column k can see a tie: decide warp-uniformly, since the shuffles
+      // below need every lane
+      if (__any_sync(0xffffffffu, tie)) {
+        // exact zgetrf rule among the tied maxima: the lowest LAPACK position
+        int bpos = 1 << 30, prow_ = 1 << 30;
+        if (mine && tie) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int i = g + 4 * r;
+            if (i < N && cand_abs(a[r], !((pivoted >> r) & 1u)) == best) {
+              const int ps = pos_of[i];
+              if (ps < bpos) {
+                bpos = ps;
+                prow_ = i;
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int off = 1; off < 4; off <<= 1) {
+          const int opos = __shfl_xor_sync(0xffffffffu, bpos, off);
+          const int orow = __shfl_xor_sync(0xffffffffu, prow_, off);
+          if (opos < bpos) {
+            bpos = opos;
+            prow_ = orow;
+          }
+        }
+        if (tie) brow = prow_;
+      }
+      // the pivot value itself: its owner (one of the four lanes) leaves it in shared memory
+      {
+        const int rsel = (mine && brow < N && (brow & 3) == g) ? (brow >> 2) : -1;
+#pragma unroll
+        for (int r = 0; r < R; ++r) st_shared_if(&s_bz, a[r], r, rsel);
+      }
+      __syncwarp();  // the column's stores to pcol[buf] and s_bz come before their use below
       if (mine && g == 0) {
-        const int p = brow;
+        // no candidate compares (a column of NaNs): take the row at position k; bz = 0 makes the
+        // step singular
+        const cplx bz = brow < N ? s_bz : mk(0.0, 0.0);
+        const int p = brow < N ? brow : row_at[k];
+        pcol[buf][p] = mk(0.0, 0.0);  // the pivot row itself is left as it is (scaled at the end)
         const int ps = pos_of[p];
         flip[k] = ps != k ? 1 : 0;  // ipiv[k] != k: zgetrf swapped rows
         const int other = row_at[k];
@@ -119,11 +199,18 @@ __global__ void __launch_bounds__(4 * 4 * R + 32)
         const double d = bz.x * bz.x + bz.y * bz.y;
         if (d == 0.0) {
           s_pinv[buf] = mk(0.0, 0.0);
+          pinv_of[k] = mk(0.0, 0.0);
           s_singular = 1;
         } else {
-          const double inv = 1.0 / d;
+          const double inv = __drcp_rn(d);
           s_pinv[buf] = mk(bz.x * inv, -bz.y * inv);
+          pinv_of[k] = s_pinv[buf];
         }
+      }
+      // column k is now in pcol: its owners clear it, so that the sweep below leaves -a_ik / a_pk
+      if (mine) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[r] = mk(0.0, 0.0);
       }
     }
     __syncthreads();
@@ -132,31 +219,28 @@ __global__ void __launch_bounds__(4 * 4 * R + 32)
     const bool skip = (pinv.x == 0.0 && pinv.y == 0.0);
     const int gp = p & 3, rp = p >> 2;
     if (g == gp) pivoted |= 1u << rp;
-    // (b) the pivot row, normalised; column k carries the reciprocal pivot (in-place inverse)
-    if (active && g == gp) {
-      cplx v = mk(0.0, 0.0);
+    // (b) the pivot row element of column j, normalised (column k: the reciprocal pivot); the
+    // owner of row p in column j hands it to the other three owners through shared memory
+    const int rsel = (g == gp) ? rp : -1;
+    if (active) {
 #pragma unroll
-      for (int r = 0; r < R; ++r)
-        if (r == rp) v = a[r];
-      prow[buf][j] = (j == k) ? pinv : cmul(v, pinv);
+      for (int r = 0; r < R; ++r) st_shared_if(&prow[buf][j], a[r], r, rsel);
     }
-    __syncthreads();
-    // (c) eliminate column k (Gauss-Jordan: every other row; LU: the trailing block only)
-    if (active && !skip && (INVERT || j > k)) {
-      const cplx pr = prow[buf][j];
-      const bool colk = (j == k);
+    __syncwarp();
+    // (c) eliminate column k from every other row: a_ij -= a_ik pr_j.  Column k was cleared, so it
+    // becomes -a_ik / a_pk; row p, whose pivot-column entry reads as 0, keeps its values:
+    // pivot rows are normalised only when the result is written (times 1 / a_pk, and + 1 at
+    // column k, where the clearing left 0 instead of a_pk / a_pk).  The LU variant runs the same
+    // sweep: its trailing block, pivots and log det are the same numbers.
+    if (active && !skip) {
+      const cplx pr = (j == k) ? pinv : cmul(prow[buf][j], pinv);
       const cplx* pc = pcol[buf];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int i = g + 4 * r;
-        const bool live = INVERT ? true : !((pivoted >> r) & 1u);
-        if (i < N && live) {
-          const cplx f = pc[i];
-          const cplx base = colk ? mk(0.0, 0.0) : a[r];
-          const cplx upd = csub(base, cmul(f, pr));
-          a[r] = (i == p) ? pr : upd;
-        }
-        if ((r & 3) == 3) asm volatile("" ::: "memory");
+        const cplx f = pc[g + 4 * r];
+        a[r].x = fma(-f.x, pr.x, fma(f.y, pr.y, a[r].x));
+        a[r].y = fma(-f.x, pr.y, fma(-f.y, pr.x, a[r].y));
+        if ((r & 3) == 3) asm volatile("" ::: "memory");  // bounds the loads in flight (registers)
       }
     }
   }
@@ -183,13 +267,19 @@ __global__ void __launch_bounds__(4 * 4 * R + 32)
   }
   if (!INVERT) return;
   const bool singular = s_singular != 0;
-  // A^-1[step_of[i]][piv_row[j]] = B[i][j]
+  // A^-1[step_of[i]][piv_row[j]] = (B[i][j] + [j == step_of[i]]) / a_(i, step_of[i])
   if (active) {
     const int col = piv_row[j];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int i = g + 4 * r;
-      if (i < N) Tb[(long)step_of[i] * N + col] = singular ? mk(0.0, 0.0) : a[r];
+      if (i < N) {
+        const int si = step_of[i];
+        cplx v = a[r];
+        if (si == j) v.x += 1.0;
+        Tb[(long)si * N + col] = singular ? mk(0.0, 0.0) : cmul(v, pinv_of[si]);
+      }
+      if ((r & 3) == 3) asm volatile("" ::: "memory");
     }
   }
 }
