@@ -51,9 +51,11 @@ def step_flops(M, N, Nc):
     return 8 * N * M * Nc + 4 * M * M * Nc + 64 * M * M * N + 24 * N * N * M + (32 / 3) * N ** 3
 
 
-def vhs_flops(M, Nc, W):
-    """Algorithmic flops of one vHS launch: real L (M^2 x Nc) times complex X (Nc x W)."""
-    return 4.0 * M * M * Nc * W
+def vhs_flops(M, Nc, W, packed):
+    """Algorithmic flops of one vHS launch: real L (M^2 x Nc, or its M(M+1)/2 packed upper-triangle
+    rows when the Cholesky vectors are symmetric) times complex X (Nc x W)."""
+    rows = M * (M + 1) // 2 if packed else M * M
+    return 4.0 * rows * Nc * W
 
 
 class ClockSampler:
@@ -290,6 +292,7 @@ def run_engine(args, cfg, spec, s, W, DT, prec, rank, local, profile_pass=True, 
         wall = time.perf_counter() - tw
         out["e2e_ms"] = max(f0.elapsed_time(f1), wall * 1e3)
         out["e2e_bytes"] = (ubytes, pbytes)
+    out["vhs_packed"] = bool(eng.info().vhs_packed)
     return eng, out
 
 
@@ -375,7 +378,7 @@ def main():
     ph = m["phases"]
     g_ms, g_n = ph["vHS_gemm"]
     launch_ms = g_ms / max(g_n, 1)
-    alg = vhs_flops(spec.M, spec.Nc, W)
+    alg = vhs_flops(spec.M, spec.Nc, W, m["vhs_packed"])
     achieved = alg / (launch_ms * 1e-3) / 1e12
     peaks = measured_peaks()
     if prec == capi.PRECISION_FP64:
@@ -393,7 +396,8 @@ def main():
                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                     "executed_tflops": achieved * nprod, "executed_frac": achieved * nprod / peak,
                     "peak_source": src}
-    roofline.update({"algorithmic_flops_per_launch": alg, "launch_ms": launch_ms, "traffic": None})
+    roofline.update({"algorithmic_flops_per_launch": alg, "launch_ms": launch_ms, "traffic": None,
+                     "vhs_columns": "packed upper triangle M(M+1)/2" if m["vhs_packed"] else "full M*M"})
     tot = sum(v[0] for k, v in ph.items() if k != "vHS_gemm")
     phases = {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / tot if tot else None}
               for k, v in ph.items() if v[1] > 0 and k != "vHS_gemm"}

@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 2 */
+int sfq_abi_version(void); /* 3 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -290,6 +290,7 @@ typedef struct {
   void* mf;           /* (nwalk) complex */
   void* new_ovlp;     /* (nwalk) complex */
   unsigned long long bound_stats[5]; /* eloc total/upper/lower, weight total/upper */
+  int vhs_packed;     /* 1: the Cholesky vectors are symmetric and vHS comes from their upper triangle */
 } sfq_engine_info_t;
 int sfq_engine_info(sfq_engine_t e, sfq_engine_info_t* info);
 

@@ -51,7 +51,7 @@ class EngineInfo(ctypes.Structure):
                [("lnak_complex", ctypes.c_int)] + \
                [(n, ctypes.c_void_p) for n in ("Likn", "haj", "v0", "vmf", "P1", "G", "X", "vHS", "hw", "mf",
                                                "new_ovlp")] + \
-               [("bound_stats", ctypes.c_ulonglong * 5)]
+               [("bound_stats", ctypes.c_ulonglong * 5), ("vhs_packed", ctypes.c_int)]
 
 
 _lib = None

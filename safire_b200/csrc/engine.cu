@@ -111,6 +111,12 @@ struct Engine {
   PopWork pw{};
   // mixed precision: split-BF16 planes and fp32 accumulators
   bool mixed = false;
+  // symmetric Cholesky vectors (checked bit for bit at setup): vHS comes from the packed upper
+  // triangle, P = M(M+1)/2 columns instead of M*M, and is mirrored afterwards
+  bool sym = false;
+  long P = 0;
+  double* Lp = nullptr;  // (P, Nc), FP64 engines
+  cplx* Vp = nullptr;    // (W, P), FP64 engines
   // T holds the inverse overlap matrices (PsiT W)^-1 of the current walkers and inv_ov their log
   // overlaps whenever inv_cached is set: the log overlap taken after a propagation or an
   // orthogonalization factors exactly the matrix the next Green's function needs, so that step
@@ -290,6 +296,21 @@ struct Engine {
     std::vector<double> pr(size_t(N) * M);
     for (size_t i = 0; i < pr.size(); ++i) pr[i] = h_PsiT[i].x;
     SFQ_CUDA_TRY(cudaMemcpyAsync(PsiTr, pr.data(), sizeof(double) * N * M, cudaMemcpyHostToDevice, st));
+    {
+      int asym = 1;
+      SFQ_CUDA_TRY(cudaMemsetAsync(pw.flag, 0, sizeof(int), st));
+      if ((rc = check_symmetric(Likn, M, Nc, pw.flag, st))) return rc;
+      SFQ_CUDA_TRY(cudaMemcpyAsync(&asym, pw.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+      SFQ_CUDA_TRY(cudaMemsetAsync(pw.flag, 0, sizeof(int), st));
+      SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+      sym = asym == 0;
+      P = (long)M * (M + 1) / 2;
+      if (sym && !mixed) {
+        SFQ_CUDA_TRY(cudaMalloc(&Lp, sizeof(double) * P * Nc));
+        SFQ_CUDA_TRY(cudaMalloc(&Vp, sizeof(cplx) * P * W));
+        if ((rc = pack_upper(Likn, M, Nc, Lp, st))) return rc;
+      }
+    }
     SFQ_CUDA_TRY(cudaStreamSynchronize(st));
 
     // Lnak[n][a][k] = sum_i PsiT[a][i] L[i][k][n]  via tmp[a][(k,n)] then a permute
@@ -406,7 +427,15 @@ struct Engine {
     }
     // mixed precision: bf16 hi/lo planes of the resident real tensors
     if (mixed) {
-      if ((rc = split_bf16_f64(Likn, MM * Nc, Likn_p[0], Likn_p[1], Likn_p[2], st))) return rc;
+      if (sym) {
+        double* packed = nullptr;
+        SFQ_CUDA_TRY(cudaMallocAsync(&packed, sizeof(double) * P * Nc, st));
+        if ((rc = pack_upper(Likn, M, Nc, packed, st))) return rc;
+        if ((rc = split_bf16_f64(packed, P * Nc, Likn_p[0], Likn_p[1], Likn_p[2], st))) return rc;
+        SFQ_CUDA_TRY(cudaFreeAsync(packed, st));
+      } else {
+        if ((rc = split_bf16_f64(Likn, MM * Nc, Likn_p[0], Likn_p[1], Likn_p[2], st))) return rc;
+      }
       if ((rc = split_bf16_f64((const double*)Lnak, (long)Nc * N * M, Lnak_p[0], Lnak_p[1], Lnak_p[2], st))) return rc;
       if ((rc = split_bf16_f64(P1, MM, P1_p[0], P1_p[1], P1_p[2], st))) return rc;
       SFQ_CUDA_TRY(cudaMemsetAsync(gemm_err, 0, sizeof(int) * 4, st));
@@ -474,8 +503,13 @@ struct Engine {
     ph_end(SFQ_PH_FIELDS);
     ph_begin(SFQ_PH_VHS);
     ph_begin(SFQ_PH_VHS_GEMM);
-    if ((rc = ops::vhs(Likn, X, V, W, M, Nc, std::sqrt(p.dt), st))) return rc;       // 3. vHS
+    if (sym) {                                                                        // 3. vHS
+      if ((rc = ops::vhs_rows(Lp, P, X, Vp, W, Nc, std::sqrt(p.dt), st))) return rc;
+    } else {
+      if ((rc = ops::vhs(Likn, X, V, W, M, Nc, std::sqrt(p.dt), st))) return rc;
+    }
     ph_end(SFQ_PH_VHS_GEMM);
+    if (sym && (rc = unpack_symmetric(Vp, W, M, V, st))) return rc;
     ph_end(SFQ_PH_VHS);
     ph_begin(SFQ_PH_PROPAGATE);
     inv_cached = false;
@@ -534,9 +568,10 @@ struct Engine {
     ph_begin(SFQ_PH_VHS);
     if ((rc = mixed_split_planar(X, W, Nc, Xs_p, st))) return rc;
     ph_begin(SFQ_PH_VHS_GEMM);
-    if ((rc = tc_gemm(Xs_p, 2L * W, 0, Likn_p, MM, 0, Nc, 1, Cv, MM, 0, float(sdt)))) return rc;
+    const long vcols = sym ? P : MM;
+    if ((rc = tc_gemm(Xs_p, 2L * W, 0, Likn_p, vcols, 0, Nc, 1, Cv, vcols, 0, float(sdt)))) return rc;
     ph_end(SFQ_PH_VHS_GEMM);
-    if ((rc = mixed_build_vblk(Cv, W, M, Vb_p, st))) return rc;
+    if ((rc = mixed_build_vblk(Cv, W, M, sym, Vb_p, st))) return rc;
     ph_end(SFQ_PH_VHS);
     ph_begin(SFQ_PH_PROPAGATE);
     const long rows = 2L * W * N;  // (w, a, c) rows of the walker operand
@@ -687,6 +722,8 @@ int sfq_engine_destroy(sfq_engine_t h) {
   if (e.st) cudaStreamSynchronize(e.st);
   e.release_events();
   if (e.arena) cudaFree(e.arena);
+  if (e.Lp) cudaFree(e.Lp);
+  if (e.Vp) cudaFree(e.Vp);
   if (e.h_pinned) cudaFreeHost(e.h_pinned);
   if (e.st) cudaStreamDestroy(e.st);
   delete h;
@@ -890,6 +927,7 @@ int sfq_engine_info(sfq_engine_t h, sfq_engine_info_t* info) {
   info->hw = e.hw;
   info->mf = e.mf;
   info->new_ovlp = e.newov;
+  info->vhs_packed = e.sym ? 1 : 0;
   SFQ_CUDA_TRY(cudaMemcpyAsync(info->bound_stats, e.stats, sizeof(unsigned long long) * 5, cudaMemcpyDeviceToHost, e.st));
   SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
   return SFQ_OK;

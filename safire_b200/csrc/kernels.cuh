@@ -78,4 +78,14 @@ int fill_cplx(cplx* p, long n, cplx v, cudaStream_t st);
 int copy_walkers_prop(cplx* dst, const cplx* src, long n, cudaStream_t st);
 int scale_cplx(cplx* p, long n, cplx s, cudaStream_t st);
 
+// Symmetric Cholesky vectors, L[i][k][n] == L[k][i][n]: the upper triangle i <= k, row-major,
+// holds everything, and vHS = sum_n X_n L_n is symmetric too.
+__host__ __device__ inline long upper_index(long i, long k, long M) { return i * M - i * (i - 1) / 2 + (k - i); }
+// flag |= 1 when some L[i][k][n] and L[k][i][n] differ in any bit
+int check_symmetric(const double* L, int M, int Nc, int* flag, cudaStream_t st);
+// Lp[upper_index(i, k)][n] = L[i][k][n], i <= k
+int pack_upper(const double* L, int M, int Nc, double* Lp, cudaStream_t st);
+// V[w][i][k] = V[w][k][i] = Vp[w][upper_index(min, max)]
+int unpack_symmetric(const cplx* Vp, int W, int M, cplx* V, cudaStream_t st);
+
 }  // namespace sfq

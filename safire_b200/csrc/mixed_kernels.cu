@@ -10,6 +10,7 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "kernels.cuh"
 #include "mixed.cuh"
 
 namespace sfq {
@@ -75,16 +76,19 @@ __global__ void planar_to_cplx_kernel(const float* C, int W, long E, double alph
   }
 }
 
-// planar vHS (rows c*W + w, columns i*M + k) -> VB[w] = [[Vr, -Vi], [Vi, Vr]] split
-__global__ void build_vblk_kernel(const float* Cv, int W, int M, Planes P) {
+// planar vHS (rows c*W + w, columns i*M + k, or the packed upper triangle when packed) ->
+// VB[w] = [[Vr, -Vi], [Vi, Vr]] split
+__global__ void build_vblk_kernel(const float* Cv, int W, int M, int packed, Planes P) {
   const long MM = (long)M * M;
+  const long ld = packed ? (long)M * (M + 1) / 2 : MM;  // columns of Cv
   const long total = (long)W * MM;
   const long M2 = 2L * M;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
     const long w = t / MM, r = t % MM;
     const long i = r / M, k = r % M;
-    const float vr = Cv[w * MM + r];
-    const float vi = Cv[((long)W + w) * MM + r];
+    const long col = packed ? (i <= k ? upper_index(i, k, M) : upper_index(k, i, M)) : r;
+    const float vr = Cv[w * ld + col];
+    const float vi = Cv[((long)W + w) * ld + col];
     const long base = w * M2 * M2;
     split_store(vr, P, base + i * M2 + k);             // (0,i),(0,k):  Vr
     split_store(-vi, P, base + i * M2 + M + k);        // (0,i),(1,k): -Vi
@@ -174,8 +178,8 @@ int mixed_planar_to_cplx(const float* C, int W, long E, double alpha, cplx* out,
   return SFQ_OK;
 }
 
-int mixed_build_vblk(const float* Cv, int W, int M, void* const* pl, cudaStream_t st) {
-  build_vblk_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Cv, W, M, planes(pl));
+int mixed_build_vblk(const float* Cv, int W, int M, bool packed, void* const* pl, cudaStream_t st) {
+  build_vblk_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Cv, W, M, packed ? 1 : 0, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

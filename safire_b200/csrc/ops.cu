@@ -74,15 +74,18 @@ int vbias(const cplx* G, const void* Lnak, bool l_cplx, cplx* v, int W, int N, i
   return gemm_f64(d, st);
 }
 
-int vhs(const double* Likn, const cplx* X, cplx* V, int W, int M, int Nc, double a, cudaStream_t st) {
+int vhs_rows(const double* L, long rows, const cplx* X, cplx* V, int W, int Nc, double a, cudaStream_t st) {
   GemmDesc d;
-  const long M2 = (long)M * M;
-  d.M = W; d.N = int(M2); d.K = Nc; d.batch = 1;
+  d.M = W; d.N = int(rows); d.K = Nc; d.batch = 1;
   d.A = X; d.sAm = Nc; d.sAk = 1; d.a_cplx = true;
-  d.B = Likn; d.sBk = 1; d.sBn = Nc; d.b_cplx = false;
-  d.C = V; d.sCm = M2; d.sCn = 1;
+  d.B = L; d.sBk = 1; d.sBn = Nc; d.b_cplx = false;
+  d.C = V; d.sCm = rows; d.sCn = 1;
   d.alpha = mk(a, 0.0);
   return gemm_f64(d, st);
+}
+
+int vhs(const double* Likn, const cplx* X, cplx* V, int W, int M, int Nc, double a, cudaStream_t st) {
+  return vhs_rows(Likn, (long)M * M, X, V, W, Nc, a, st);
 }
 
 static int p1_apply(const void* P1, bool p_cplx, const cplx* in, cplx* out, int W, int M, int N, cudaStream_t st) {
@@ -187,7 +190,7 @@ constexpr long kEnergyChunkElems = 1L << 27;  // 2 GiB of complex T per chunk at
 
 extern "C" {
 
-int sfq_abi_version(void) { return 2; }
+int sfq_abi_version(void) { return 3; }
 
 unsigned long long sfq_launch_count(void) { return g_launches.load(); }
 

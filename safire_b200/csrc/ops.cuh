@@ -16,6 +16,8 @@ int green_full(const void* A, bool a_cplx, const cplx* Gc, cplx* C, int W, int M
 int vbias(const cplx* G, const void* Lnak, bool l_cplx, cplx* v, int W, int N, int M, int Nc, double a,
           cudaStream_t st);
 int vhs(const double* Likn, const cplx* X, cplx* V, int W, int M, int Nc, double a, cudaStream_t st);
+// V (W, rows) = a X L^T for L (rows, Nc): rows = M*M, or the packed upper triangle of symmetric L
+int vhs_rows(const double* L, long rows, const cplx* X, cplx* V, int W, int Nc, double a, cudaStream_t st);
 // SM <- P1 * Taylor(iV) * P1 * SM with scratch TMN, T1, T2 (each W*M*N complex)
 int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M, int N, int order, cplx* TMN,
               cplx* T1, cplx* T2, cudaStream_t st);

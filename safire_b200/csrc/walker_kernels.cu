@@ -464,6 +464,60 @@ int energy_finish(const cplx* exxn, const cplx* kl, cplx* E3, int nwalk, int nch
   return SFQ_OK;
 }
 
+namespace {
+__global__ void check_symmetric_kernel(const double* L, int M, int Nc, int* flag) {
+  const long total = (long)M * M * Nc;
+  int bad = 0;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long row = t / Nc, n = t % Nc;
+    const long i = row / M, k = row % M;
+    if (i < k) {
+      const long long a = __double_as_longlong(L[t]);
+      const long long b = __double_as_longlong(L[(k * M + i) * Nc + n]);
+      bad |= (a != b);
+    }
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+__global__ void pack_upper_kernel(const double* L, int M, int Nc, double* Lp) {
+  const long total = (long)M * M * Nc;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long row = t / Nc, n = t % Nc;
+    const long i = row / M, k = row % M;
+    if (i <= k) Lp[upper_index(i, k, M) * Nc + n] = L[t];
+  }
+}
+
+__global__ void unpack_symmetric_kernel(const cplx* Vp, int W, int M, cplx* V) {
+  const long MM = (long)M * M, P = (long)M * (M + 1) / 2;
+  const long total = (long)W * MM;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long w = t / MM, r = t % MM;
+    const long i = r / M, k = r % M;
+    V[t] = Vp[w * P + (i <= k ? upper_index(i, k, M) : upper_index(k, i, M))];
+  }
+}
+}  // namespace
+
+int check_symmetric(const double* L, int M, int Nc, int* flag, cudaStream_t st) {
+  check_symmetric_kernel<<<grid_for((long)M * M * Nc), 256, 0, st>>>(L, M, Nc, flag);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int pack_upper(const double* L, int M, int Nc, double* Lp, cudaStream_t st) {
+  pack_upper_kernel<<<grid_for((long)M * M * Nc), 256, 0, st>>>(L, M, Nc, Lp);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int unpack_symmetric(const cplx* Vp, int W, int M, cplx* V, cudaStream_t st) {
+  unpack_symmetric_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Vp, W, M, V);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
 int permute_lnak(const void* tmp, void* Lnak, int nel, int nmo, int nchol, int esz, cudaStream_t st) {
   const int g = grid_for((long)nel * nmo * nchol);
   if (esz == 16)

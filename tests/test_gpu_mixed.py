@@ -109,3 +109,23 @@ def test_mixed_engine_rejects_unsupported_shapes():
     s = synthetic.make_system(synthetic.SystemSpec(M=20, N=5, Nc=40, decay=20.0))
     with pytest.raises(capi.SafireError, match="UNSUPPORTED"):
         afqmc.AfqmcEngine(s, 4, precision=capi.PRECISION_MIXED)
+
+
+def test_mixed_engine_full_vhs_path_for_asymmetric_vectors():
+    """Asymmetric Cholesky vectors: the mixed engine falls back to the full M*M vHS product."""
+    s = synthetic.make_system(synthetic.CFG_SMALL)
+    s.Likn = s.Likn.copy()
+    s.Likn[2, 0, :] -= 2e-3
+    W = 8
+    eng = afqmc.AfqmcEngine(s, W, dt=0.005, seed=4, precision=capi.PRECISION_MIXED)
+    assert eng.info().vhs_packed == 0
+    ham = O.Hamiltonian(s.hcore, s.Likn, s.PsiT)
+    prop = O.Propagator(ham, 0.005, seed=4)
+    wo = O.Walkers(s.initial_walkers(W))
+    Esh_o = O.init_walkers(ham, wo)
+    Esh = eng.init()
+    prop.propagate(wo, Esh_o, 0)
+    eng.propagate(Esh, 0)
+    SM, pr = eng.walkers()
+    assert _rel(SM, wo.SM) < STEP_TOL[capi.PRECISION_MIXED]
+    eng.close()

@@ -331,3 +331,28 @@ def test_engine_medium_steps():
     Eo, _ = O.wfn_energy_noupdate(ham, wo)
     assert rel(E, Eo) < REL
     eng.close()
+
+
+@pytest.mark.parametrize("symmetric", [True, False])
+def test_engine_vhs_packed_and_full_paths(symmetric):
+    """Symmetric Cholesky vectors take the packed upper-triangle vHS; any asymmetry the full one.
+    Both give the oracle's vHS and step."""
+    s = synthetic.make_system(synthetic.CFG_SMALL)
+    if not symmetric:
+        s.Likn = s.Likn.copy()
+        s.Likn[0, 1, :] += 1e-3  # L_n no longer symmetric in (i, k)
+    ham = O.Hamiltonian(s.hcore, s.Likn, s.PsiT)
+    W = 8
+    eng = A.AfqmcEngine(s, W, dt=0.005, seed=2)
+    prop = O.Propagator(ham, 0.005, seed=2)
+    wo = O.Walkers(s.initial_walkers(W))
+    assert eng.info().vhs_packed == (1 if symmetric else 0)
+    Esh_o = O.init_walkers(ham, wo)
+    Esh = eng.init()
+    dbg = prop.propagate(wo, Esh_o, 0)
+    eng.propagate(Esh, 0)
+    assert rel(eng.fetch("vHS", (W, s.M, s.M), np.complex128), dbg["vHS"]) < REL
+    SM, pr = eng.walkers()
+    assert rel(SM, wo.SM) < REL
+    assert rel(pr["WEIGHT"], wo.weight) < REL
+    eng.close()
