@@ -28,48 +28,42 @@ constexpr int kGjMaxN = 128;
 
 __device__ __forceinline__ double cabs1(cplx a) { return fabs(a.x) + fabs(a.y); }
 
-// |re| + |im| of the rows still unpivoted (bit r of `pivoted` set: row g + 4r is done), else -1
-__device__ __forceinline__ double cand_abs(cplx z, bool cand) { return cand ? cabs1(z) : -1.0; }
-
-// the largest candidate of one owner, its smallest index, and whether it occurs twice: NQ
-// interleaved running maxima, each with the bit mask of the indices that attain it, so that the
-// dependent depth is about R/NQ rather than R and no candidate has to stay live (three chains
-// for R = 25, whose 100 registers of matrix leave no room for a fourth)
-template <int R>
-__device__ __forceinline__ void owner_max(const cplx (&a)[R], int g, int N, unsigned pivoted, double& best, int& idx,
-                                          bool& tie) {
-  constexpr int NQ = R > 16 ? 3 : 4;
-  double m[4] = {-1.0, -1.0, -1.0, -1.0};
-  unsigned msk[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const double v = cand_abs(a[r], g + 4 * r < N && !((pivoted >> r) & 1u));
-    const int q = r % NQ;
-    if (v > m[q]) {
-      m[q] = v;
-      msk[q] = 1u << r;
-    } else if (v == m[q]) {
-      msk[q] |= 1u << r;
-    }
-  }
-  best = fmax(fmax(m[0], m[1]), fmax(m[2], m[3]));
-  unsigned mask = 0;
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) mask |= (m[q] == best) ? msk[q] : 0u;
-  idx = __ffs(mask) - 1;
-  tie = best >= 0.0 && __popc(mask) > 1;
+// Pivot candidates as integer keys: |re| + |im| of an unpivoted row as its bit pattern (a
+// non-negative double orders like its bits, and integer compares are short and branch-free), -1
+// for pivoted rows and NaN (never chosen, as no comparison with NaN succeeds).
+__device__ __forceinline__ long long cand_key(cplx z, bool cand) {
+  const long long bits = __double_as_longlong(fabs(z.x) + fabs(z.y));
+  return (cand && bits <= 0x7ff0000000000000LL) ? bits : -1LL;
 }
 
-// dst = v when r == sel: a compare and a predicated shared store, so that a thread can hand out
-// the register of a run-time row without a chain of selects over its whole array
-__device__ __forceinline__ void st_shared_if(cplx* dst, cplx v, int r, int sel) {
-  const unsigned addr = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  asm volatile(
-      "{\n\t.reg .pred q;\n\t"
-      "setp.eq.s32 q, %0, %1;\n\t"
-      "@q st.shared.v2.f64 [%2], {%3, %4};\n\t}" ::"r"(r),
-      "r"(sel), "r"(addr), "d"(v.x), "d"(v.y)
-      : "memory");
+// the largest key of one owner and the bit mask of its rows that attain it, in one pass of NQ
+// interleaved running maxima (dependent depth about R/NQ), with selects only: no branch, and no
+// key kept beyond its own step (three chains at R = 25, whose matrix leaves few registers)
+template <int R>
+__device__ __forceinline__ void owner_max(const cplx (&a)[R], int g, int N, unsigned pivoted, long long& best,
+                                          unsigned& mask) {
+  constexpr int NQ = R > 16 ? 3 : 4;
+  long long m[NQ];
+  unsigned mk_[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    m[q] = -1LL;
+    mk_[q] = 0u;
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int q = r % NQ;
+    const long long key = cand_key(a[r], g + 4 * r < N && !((pivoted >> r) & 1u));
+    const bool gt = key > m[q], eq = key == m[q];
+    mk_[q] = gt ? (1u << r) : (eq ? (mk_[q] | (1u << r)) : mk_[q]);
+    m[q] = gt ? key : m[q];
+  }
+  best = m[0];
+#pragma unroll
+  for (int q = 1; q < NQ; ++q) best = m[q] > best ? m[q] : best;
+  mask = 0u;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) mask |= (m[q] == best) ? mk_[q] : 0u;
 }
 
 template <int R, bool INVERT>
@@ -86,7 +80,6 @@ __global__ void __launch_bounds__(((16 * R + 31) / 32) * 32)
   __shared__ int piv_row[kGjMaxN];      // pivot row of each step
   __shared__ int s_p[2];
   __shared__ cplx s_pinv[2];
-  __shared__ cplx s_bz;
   __shared__ int s_singular;
 
   const int t = threadIdx.x;
@@ -124,22 +117,22 @@ __global__ void __launch_bounds__(((16 * R + 31) / 32) * 32)
         for (int r = 0; r < R; ++r)
           if (g + 4 * r < N) pcol[buf][g + 4 * r] = a[r];
       }
-      double best = -1.0;
-      int br = 0;
-      bool tie = false;
-      if (mine) owner_max<R>(a, g, N, pivoted, best, br, tie);
-      int brow = (best >= 0.0) ? g + 4 * br : (1 << 30);
+      long long best = -1LL;
+      unsigned mask = 0u;
+      if (mine) owner_max<R>(a, g, N, pivoted, best, mask);
+      int brow = (best >= 0) ? g + 4 * (__ffs(mask) - 1) : (1 << 30);
+      bool tie = best >= 0 && __popc(mask) > 1;
       // reduce over the 4 owners (adjacent lanes, aligned to 4)
 #pragma unroll
       for (int off = 1; off < 4; off <<= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const long long ob = __shfl_xor_sync(0xffffffffu, best, off);
         const int orow = __shfl_xor_sync(0xffffffffu, brow, off);
         const int otie = __shfl_xor_sync(0xffffffffu, int(tie), off);
         if (ob > best) {
           best = ob;
           brow = orow;
           tie = otie != 0;
-        } else if (ob == best && ob >= 0.0) {
+        } else if (ob == best && ob >= 0) {
           tie = true;
         }
       }
@@ -152,7 +145,7 @@ __global__ void __launch_bounds__(((16 * R + 31) / 32) * 32)
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const int i = g + 4 * r;
-            if (i < N && cand_abs(a[r], !((pivoted >> r) & 1u)) == best) {
+            if (i < N && cand_key(a[r], !((pivoted >> r) & 1u)) == best) {
               const int ps = pos_of[i];
               if (ps < bpos) {
                 bpos = ps;
@@ -172,17 +165,11 @@ __global__ void __launch_bounds__(((16 * R + 31) / 32) * 32)
         }
         if (tie) brow = prow_;
       }
-      // the pivot value itself: its owner (one of the four lanes) leaves it in shared memory
-      {
-        const int rsel = (mine && brow < N && (brow & 3) == g) ? (brow >> 2) : -1;
-#pragma unroll
-        for (int r = 0; r < R; ++r) st_shared_if(&s_bz, a[r], r, rsel);
-      }
-      __syncwarp();  // the column's stores to pcol[buf] and s_bz come before their use below
+      __syncwarp();  // the column's stores to pcol[buf] come before their use below
       if (mine && g == 0) {
         // no candidate compares (a column of NaNs): take the row at position k; bz = 0 makes the
         // step singular
-        const cplx bz = brow < N ? s_bz : mk(0.0, 0.0);
+        const cplx bz = brow < N ? pcol[buf][brow] : mk(0.0, 0.0);
         const int p = brow < N ? brow : row_at[k];
         pcol[buf][p] = mk(0.0, 0.0);  // the pivot row itself is left as it is (scaled at the end)
         const int ps = pos_of[p];
@@ -221,11 +208,10 @@ __global__ void __launch_bounds__(((16 * R + 31) / 32) * 32)
     if (g == gp) pivoted |= 1u << rp;
     // (b) the pivot row element of column j, normalised (column k: the reciprocal pivot); the
     // owner of row p in column j hands it to the other three owners through shared memory
-    const int rsel = (g == gp) ? rp : -1;
-    if (active) {
+    const int rsel = (active && g == gp) ? rp : -1;
 #pragma unroll
-      for (int r = 0; r < R; ++r) st_shared_if(&prow[buf][j], a[r], r, rsel);
-    }
+    for (int r = 0; r < R; ++r)
+      if (r == rsel) prow[buf][j] = a[r];
     __syncwarp();
     // (c) eliminate column k from every other row: a_ij -= a_ik pr_j.  Column k was cleared, so it
     // becomes -a_ik / a_pk; row p, whose pivot-column entry reads as 0, keeps its values:
