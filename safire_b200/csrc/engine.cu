@@ -131,7 +131,11 @@ struct Engine {
   void* Xs_p[3] = {};
   void* Vb_p[3] = {};
   void* Wt_p[3] = {};
-  float *Cvb = nullptr, *Cv = nullptr, *Sacc = nullptr, *Ck = nullptr;
+  void* Wt2_p[3] = {};  // second walker-operand buffer: a product's epilogue writes the next A here
+  float *Cvb = nullptr, *Cv = nullptr, *Sacc = nullptr;
+  int vb_ks = 1;        // K splits of the vbias product (partial sums, reduced in a fixed order)
+  int tay_half = 0;     // orbitals per Taylor tile (tile width 2 * tay_half, re and im halves)
+  long vb_rows = 0;     // rows of one walker's vHS block operand: ceil(M / tay_half) * 2 * tay_half
   int* gemm_err = nullptr;
   double* h_pinned = nullptr;  // pinned host staging for e2e calls
   size_t h_pinned_bytes = 0;
@@ -253,6 +257,7 @@ struct Engine {
     if (mixed) {
       const size_t b = 2;  // bf16
       const long MN2 = 2L * M * N;
+      plan_mixed();
       std::vector<Item> mx;
       for (int q = 0; q < nplanes; ++q) {
         mx.push_back({&Likn_p[q], b * MM * Nc});
@@ -260,14 +265,14 @@ struct Engine {
         mx.push_back({&P1_p[q], b * MM});
         mx.push_back({&Gs_p[q], b * 2 * W * MN});
         mx.push_back({&Xs_p[q], b * 2 * (size_t)W * Nc});
-        mx.push_back({&Vb_p[q], b * 4 * W * MM});
+        mx.push_back({&Vb_p[q], b * W * vb_rows * 2 * M});
         mx.push_back({&Wt_p[q], b * W * MN2});
+        mx.push_back({&Wt2_p[q], b * W * MN2});
       }
       std::vector<Item> mx2 = {
-          {(void**)&Cvb, sizeof(float) * 2 * (size_t)W * Nc},
+          {(void**)&Cvb, sizeof(float) * vb_ks * 2 * (size_t)W * Nc},
           {(void**)&Cv, sizeof(float) * 2 * W * MM},
           {(void**)&Sacc, sizeof(float) * W * MN2},
-          {(void**)&Ck, sizeof(float) * W * MN2},
           {(void**)&gemm_err, sizeof(int) * 4},
       };
       items.insert(items.end(), mx.begin(), mx.end());
@@ -529,9 +534,48 @@ struct Engine {
     return SFQ_OK;
   }
 
+  // tile shapes of the mixed products, fixed by the sizes
+  void plan_mixed() {
+    // Taylor tiles: `tay_half` orbitals, re and im halves side by side (tile width 2 * half, a
+    // tile width the GEMM is built with); the least padding of M, then the widest tile
+    int best = 0;
+    long best_pad = 1L << 40;
+    for (int h : {16, 32, 64, 80, 128}) {
+      if (h == 128 && nplanes > 2) continue;
+      const long pad = (long)((M + h - 1) / h) * h;
+      if (pad < best_pad || (pad == best_pad && h > best)) {
+        best = h;
+        best_pad = pad;
+      }
+    }
+    tay_half = best;
+    vb_rows = 2 * best_pad;
+    // vbias: 128-wide tiles over (2W, Nc), K = N*M split so that the work units fill whole waves
+    // of SMs (K splits write partial sums, reduced in a fixed order)
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device);
+    const long tiles = (long)((2 * W + 127) / 128) * ((Nc + 127) / 128);
+    const long kt = ((long)N * M + 63) / 64;
+    double best_eff = 0.0;
+    vb_ks = 1;
+    for (int ks = 1; ks <= 64 && ks * 8 <= kt; ++ks) {
+      const double units = double(tiles) * ks;
+      const double eff = units / (std::ceil(units / sms) * sms);
+      if (eff > best_eff + 1e-9) {
+        best_eff = eff;
+        vb_ks = ks;
+      }
+      if (eff > 0.999) break;
+    }
+  }
+
+  // tile width of the P1 products (M columns): little padding, and a tile width built for the planes
+  int p1_tile() const { return M <= 128 ? 128 : (nplanes > 2 ? 160 : 208); }
+
   // C = alpha * A B^T on split planes (A: rows x K, B: cols x K, both K-major)
   int tc_gemm(void* const* A, long a_rows, long a_bs, void* const* B, long b_rows, long b_bs, int K, int batch,
-              float* C, long ldc, long sCb, float alpha, int bn = 0) {
+              float* C, long ldc, long sCb, float alpha, int bn = 0, const UmmaEpilogue* epi = nullptr,
+              int ksplit = 1, long sCk = 0) {
     UmmaGemmDesc d;
     d.M = int(a_rows); d.N = int(b_rows); d.K = K; d.batch = batch;
     for (int q = 0; q < 3; ++q) {
@@ -541,6 +585,8 @@ struct Engine {
     d.A.rows = a_rows; d.A.ld = K; d.A.batch_stride = a_bs;
     d.B.rows = b_rows; d.B.ld = K; d.B.batch_stride = b_bs;
     d.C = C; d.ldc = ldc; d.sCb = sCb; d.alpha = alpha; d.nplanes = nplanes; d.bn = bn; d.err = gemm_err;
+    d.ksplit = ksplit; d.sCk = sCk;
+    if (epi) d.epi = *epi;
     return umma_gemm(d, st);
   }
 
@@ -555,9 +601,10 @@ struct Engine {
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
     if ((rc = mixed_split_planar(G, W, NM, Gs_p, st))) return rc;
-    if ((rc = tc_gemm(Gs_p, 2L * W, 0, Lnak_p, Nc, 0, int(NM), 1, Cvb, Nc, 0, float(2.0 * sdt), Nc <= 4096 ? 64 : 0)))
+    const long part = 2L * W * Nc;  // one K split's partial sums
+    if ((rc = tc_gemm(Gs_p, 2L * W, 0, Lnak_p, Nc, 0, int(NM), 1, Cvb, Nc, 0, 1.f, 128, nullptr, vb_ks, part)))
       return rc;
-    if ((rc = mixed_planar_to_cplx(Cvb, W, Nc, 1.0, X, st))) return rc;
+    if ((rc = mixed_reduce_planar_to_cplx(Cvb, vb_ks, part, W, Nc, 2.0 * sdt, X, st))) return rc;
     ph_end(SFQ_PH_VBIAS);
     ph_begin(SFQ_PH_FIELDS);
     FieldParams fp;
@@ -571,23 +618,39 @@ struct Engine {
     const long vcols = sym ? P : MM;
     if ((rc = tc_gemm(Xs_p, 2L * W, 0, Likn_p, vcols, 0, Nc, 1, Cv, vcols, 0, float(sdt)))) return rc;
     ph_end(SFQ_PH_VHS_GEMM);
-    if ((rc = mixed_build_vblk(Cv, W, M, sym, Vb_p, st))) return rc;
+    if ((rc = mixed_build_vblk(Cv, W, M, sym, tay_half, vb_rows, Vb_p, st))) return rc;
     ph_end(SFQ_PH_VHS);
     ph_begin(SFQ_PH_PROPAGATE);
-    const long rows = 2L * W * N;  // (w, a, c) rows of the walker operand
     inv_cached = false;
+    // S = P1 W (fp32) and its planes T1 = S; then T_{k+1} = (i/k) VB T_k, S += T_{k+1} in the
+    // Taylor products' epilogues, the operand planes alternating between the two buffers; the
+    // last one leaves the planes of S for SM = P1 S, written straight back to the walkers
+    const long rows = 2L * W * N;  // (w, a, c) rows of the walker operand
     if ((rc = mixed_walkers_to_wt(SM, W, M, N, Wt_p, st))) return rc;
-    if ((rc = tc_gemm(Wt_p, rows, 0, P1_p, M, 0, M, 1, Sacc, M, 0, 1.f))) return rc;  // S = P1 W
-    if ((rc = mixed_split_f32(Sacc, rows * M, Wt_p, st))) return rc;                  // T1 = S
+    UmmaEpilogue e1;
+    e1.kind = UMMA_EPI_STORE_SPLIT;
+    for (int q = 0; q < 3; ++q) e1.out[q] = Wt2_p[q];
+    e1.out_planes = nplanes;
+    if ((rc = tc_gemm(Wt_p, rows, 0, P1_p, M, 0, M, 1, Sacc, M, 0, 1.f, p1_tile(), &e1))) return rc;
+    void** cur = Wt2_p;
+    void** nxt = Wt_p;
     for (int k = 1; k <= p.taylor_order; ++k) {
-      // C[w] (N x 2M) = T_k[w] (N x 2M) VB[w]^T;  T_{k+1} = (i/k) C;  S += T_{k+1}
-      if ((rc = tc_gemm(Wt_p, N, long(N) * M2, Vb_p, M2, M2 * M2, int(M2), W, Ck, M2, long(N) * M2, 1.f))) return rc;
-      const bool last = k == p.taylor_order;
-      if ((rc = mixed_taylor_update(Ck, (long)W * N, M, 1.f / float(k), Sacc, last ? nullptr : Wt_p, st))) return rc;
+      UmmaEpilogue et;
+      et.kind = UMMA_EPI_TAYLOR;
+      et.S = Sacc; et.nmo = M; et.half = tay_half; et.inv_k = 1.f / float(k);
+      et.write = k < p.taylor_order ? 1 : 2;
+      for (int q = 0; q < 3; ++q) et.out[q] = nxt[q];
+      et.out_planes = nplanes;
+      if ((rc = tc_gemm(cur, N, long(N) * M2, Vb_p, vb_rows, vb_rows * M2, int(M2), W, nullptr, 0, 0, 1.f,
+                        2 * tay_half, &et)))
+        return rc;
+      std::swap(cur, nxt);
     }
-    if ((rc = mixed_split_f32(Sacc, rows * M, Wt_p, st))) return rc;
-    if ((rc = tc_gemm(Wt_p, rows, 0, P1_p, M, 0, M, 1, Ck, M, 0, 1.f))) return rc;    // P1 S
-    if ((rc = mixed_wt_to_walkers(Ck, W, M, N, SM, st))) return rc;
+    UmmaEpilogue ew;
+    ew.kind = UMMA_EPI_TO_WALKERS;
+    ew.SM = reinterpret_cast<double*>(SM);
+    ew.nel = N;
+    if ((rc = tc_gemm(cur, rows, 0, P1_p, M, 0, M, 1, nullptr, 0, 0, 1.f, p1_tile(), &ew))) return rc;
     ph_end(SFQ_PH_PROPAGATE);
     ph_begin(SFQ_PH_OVERLAP);
     if ((rc = log_overlap(newov))) return rc;

@@ -7,13 +7,13 @@ namespace sfq {
 
 // `pl` points at 3 plane pointers (p0, p1, p2); unused planes are null
 int mixed_split_planar(const cplx* src, int W, long E, void* const* pl, cudaStream_t st);
-int mixed_planar_to_cplx(const float* C, int W, long E, double alpha, cplx* out, cudaStream_t st);
-// Cv: (2W, M*M) planar, or (2W, M(M+1)/2) with packed (upper triangle of a symmetric vHS)
-int mixed_build_vblk(const float* Cv, int W, int M, bool packed, void* const* pl, cudaStream_t st);
+// out[w][e] = alpha * (sum_s C_s[w][e], sum_s C_s[W + w][e]), the KS partial sums C_s = C + s * sk
+int mixed_reduce_planar_to_cplx(const float* C, int KS, long sk, int W, long E, double alpha, cplx* out,
+                                cudaStream_t st);
+// Cv: (2W, M*M) planar, or (2W, M(M+1)/2) with packed (upper triangle of a symmetric vHS); the
+// blocks get `rows` rows per walker, grouped by `half` orbitals (see mixed_kernels.cu)
+int mixed_build_vblk(const float* Cv, int W, int M, bool packed, int half, long rows, void* const* pl,
+                     cudaStream_t st);
 int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* const* pl, cudaStream_t st);
-int mixed_wt_to_walkers(const float* C2, int W, int M, int N, cplx* SM, cudaStream_t st);
-// pl == null: only accumulate into S (last Taylor term)
-int mixed_taylor_update(const float* C, long rows, int M, float inv_k, float* S, void* const* pl, cudaStream_t st);
-int mixed_split_f32(const float* src, long n, void* const* pl, cudaStream_t st);
 
 }  // namespace sfq

@@ -3,9 +3,11 @@
 // Working layouts (per walker w, orbitals i,k < M, electrons a < N, c = 0 real / 1 imaginary):
 //   planar rows      P[c*W + w][e]               (split operands of the vbias / vHS GEMMs)
 //   walker rows      WT[w][a][c][i]              (K = (c,i) contiguous: Taylor / P1 A operand)
-//   vHS blocks       VB[w][(c,i)][(c',k)] = [[Vr, -Vi], [Vi, Vr]]   (Taylor B operand)
+//   vHS blocks       VB[w][row(c,i)][(c',k)] = [[Vr, -Vi], [Vi, Vr]]   (Taylor B operand), its rows
+//                    grouped by `half` orbitals: row(c, i) = (i / half) 2 half + c half + i % half,
+//                    so that one Taylor output tile holds the re and im parts of the same orbitals
 // so that the complex products become real K-major GEMMs on the tensor cores:
-//   (V T)^T[a][(c,i)] = sum_(c',k) WT[a][(c',k)] VB[(c,i)][(c',k)],
+//   (V T)^T[a][(c,i)] = sum_(c',k) WT[a][(c',k)] VB[row(c,i)][(c',k)],
 //   (P1 W)^T[(a,c)][j] = sum_i WT[(a,c)][i] P1[j][i].
 #include <cuda_bf16.h>
 
@@ -67,18 +69,25 @@ __global__ void split_planar_kernel(const cplx* src, int W, long E, Planes P) {
   }
 }
 
-// planar fp32 rows (c*W + w) -> complex fp64 (W, E), times alpha
-__global__ void planar_to_cplx_kernel(const float* C, int W, long E, double alpha, cplx* out) {
+// KS partial sums of planar fp32 rows (c*W + w), split s at C + s * sk -> complex fp64 (W, E),
+// times alpha; the splits are added in order, in double precision
+__global__ void reduce_planar_to_cplx_kernel(const float* C, int KS, long sk, int W, long E, double alpha,
+                                             cplx* out) {
   const long total = (long)W * E;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
     const long w = t / E, e = t % E;
-    out[t] = mk(alpha * double(C[w * E + e]), alpha * double(C[((long)W + w) * E + e]));
+    double re = 0.0, im = 0.0;
+    for (int s = 0; s < KS; ++s) {
+      re += double(C[s * sk + w * E + e]);
+      im += double(C[s * sk + ((long)W + w) * E + e]);
+    }
+    out[t] = mk(alpha * re, alpha * im);
   }
 }
 
 // planar vHS (rows c*W + w, columns i*M + k, or the packed upper triangle when packed) ->
 // VB[w] = [[Vr, -Vi], [Vi, Vr]] split
-__global__ void build_vblk_kernel(const float* Cv, int W, int M, int packed, Planes P) {
+__global__ void build_vblk_kernel(const float* Cv, int W, int M, int packed, int half, long rows, Planes P) {
   const long MM = (long)M * M;
   const long ld = packed ? (long)M * (M + 1) / 2 : MM;  // columns of Cv
   const long total = (long)W * MM;
@@ -89,11 +98,13 @@ __global__ void build_vblk_kernel(const float* Cv, int W, int M, int packed, Pla
     const long col = packed ? (i <= k ? upper_index(i, k, M) : upper_index(k, i, M)) : r;
     const float vr = Cv[w * ld + col];
     const float vi = Cv[((long)W + w) * ld + col];
-    const long base = w * M2 * M2;
-    split_store(vr, P, base + i * M2 + k);             // (0,i),(0,k):  Vr
-    split_store(-vi, P, base + i * M2 + M + k);        // (0,i),(1,k): -Vi
-    split_store(vi, P, base + (M + i) * M2 + k);       // (1,i),(0,k):  Vi
-    split_store(vr, P, base + (M + i) * M2 + M + k);   // (1,i),(1,k):  Vr
+    const long base = w * rows * M2;
+    const long r0 = (i / half) * 2 * half + i % half;  // row (0, i); row (1, i) is half further
+    const long r1 = r0 + half;
+    split_store(vr, P, base + r0 * M2 + k);         // (0,i),(0,k):  Vr
+    split_store(-vi, P, base + r0 * M2 + M + k);    // (0,i),(1,k): -Vi
+    split_store(vi, P, base + r1 * M2 + k);         // (1,i),(0,k):  Vi
+    split_store(vr, P, base + r1 * M2 + M + k);     // (1,i),(1,k):  Vr
   }
 }
 
@@ -119,51 +130,6 @@ __global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, Planes P) {
   }
 }
 
-// C2[w][a][c][j] fp32 -> SM (W, M, N) complex fp64
-__global__ void wt_to_walkers_kernel(const float* C2, int M, int N, cplx* SM) {
-  __shared__ float2 tile[32][33];
-  const int w = blockIdx.z;
-  const int j0 = blockIdx.y * 32, a0 = blockIdx.x * 32;
-  const long base = (long)w * N * 2 * M;
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int a = a0 + r, j = j0 + threadIdx.x;
-    if (j < M && a < N) {
-      tile[r][threadIdx.x] = make_float2(C2[base + ((long)a * 2 + 0) * M + j], C2[base + ((long)a * 2 + 1) * M + j]);
-    }
-  }
-  __syncthreads();
-  cplx* S = SM + (long)w * M * N;
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int j = j0 + r, a = a0 + threadIdx.x;
-    if (j < M && a < N) {
-      const float2 v = tile[threadIdx.x][r];
-      S[(long)j * N + a] = mk(double(v.x), double(v.y));
-    }
-  }
-}
-
-// T_{k+1} = (i/k) C: T[a][(0,i)] = -C[a][(1,i)]/k, T[a][(1,i)] = C[a][(0,i)]/k; S += T; split T
-__global__ void taylor_update_kernel(const float* C, long rows, int M, float inv_k, float* S, Planes P) {
-  const long total = rows * M;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const long row = t / M, i = t % M;
-    const long o0 = row * 2 * M + i, o1 = o0 + M;
-    const float cr = C[o0], ci = C[o1];
-    const float tr = -ci * inv_k, ti = cr * inv_k;
-    S[o0] += tr;
-    S[o1] += ti;
-    if (P.p0) {
-      split_store(tr, P, o0);
-      split_store(ti, P, o1);
-    }
-  }
-}
-
-__global__ void split_f32_kernel(const float* src, long n, Planes P) {
-  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
-    split_store(src[e], P, e);
-}
-
 }  // namespace
 
 int mixed_split_planar(const cplx* src, int W, long E, void* const* pl, cudaStream_t st) {
@@ -172,14 +138,16 @@ int mixed_split_planar(const cplx* src, int W, long E, void* const* pl, cudaStre
   return SFQ_OK;
 }
 
-int mixed_planar_to_cplx(const float* C, int W, long E, double alpha, cplx* out, cudaStream_t st) {
-  planar_to_cplx_kernel<<<grid_for((long)W * E), 256, 0, st>>>(C, W, E, alpha, out);
+int mixed_reduce_planar_to_cplx(const float* C, int KS, long sk, int W, long E, double alpha, cplx* out,
+                                cudaStream_t st) {
+  reduce_planar_to_cplx_kernel<<<grid_for((long)W * E), 256, 0, st>>>(C, KS, sk, W, E, alpha, out);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
 
-int mixed_build_vblk(const float* Cv, int W, int M, bool packed, void* const* pl, cudaStream_t st) {
-  build_vblk_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Cv, W, M, packed ? 1 : 0, planes(pl));
+int mixed_build_vblk(const float* Cv, int W, int M, bool packed, int half, long rows, void* const* pl,
+                     cudaStream_t st) {
+  build_vblk_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Cv, W, M, packed ? 1 : 0, half, rows, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
@@ -187,26 +155,6 @@ int mixed_build_vblk(const float* Cv, int W, int M, bool packed, void* const* pl
 int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* const* pl, cudaStream_t st) {
   dim3 grid((N + 31) / 32, (M + 31) / 32, W), block(32, 8);
   walkers_to_wt_kernel<<<grid, block, 0, st>>>(SM, M, N, planes(pl));
-  SFQ_LAUNCHED();
-  return SFQ_OK;
-}
-
-int mixed_wt_to_walkers(const float* C2, int W, int M, int N, cplx* SM, cudaStream_t st) {
-  dim3 grid((N + 31) / 32, (M + 31) / 32, W), block(32, 8);
-  wt_to_walkers_kernel<<<grid, block, 0, st>>>(C2, M, N, SM);
-  SFQ_LAUNCHED();
-  return SFQ_OK;
-}
-
-int mixed_taylor_update(const float* C, long rows, int M, float inv_k, float* S, void* const* pl, cudaStream_t st) {
-  Planes P = pl ? planes(pl) : Planes{nullptr, nullptr, nullptr};
-  taylor_update_kernel<<<grid_for(rows * M), 256, 0, st>>>(C, rows, M, inv_k, S, P);
-  SFQ_LAUNCHED();
-  return SFQ_OK;
-}
-
-int mixed_split_f32(const float* src, long n, void* const* pl, cudaStream_t st) {
-  split_f32_kernel<<<grid_for(n), 256, 0, st>>>(src, n, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

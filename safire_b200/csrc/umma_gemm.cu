@@ -18,9 +18,12 @@ constexpr unsigned long long kWaitNs = 2000000000ull;  // bounded waits: 2 s
 struct KParams {
   int M, N, K;
   int a_batched, b_batched;
+  int MT, NT, KS;  // tiles along M, N; K splits
+  long tiles;
   float* C;
-  long ldc, sCb;
+  long ldc, sCb, sCk;  // sCk: elements between the partial outputs of the K splits
   float alpha, beta;
+  UmmaEpilogue e;
   int* err;
 };
 
@@ -37,6 +40,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
@@ -130,7 +136,8 @@ struct Smem {
   static constexpr int B_BYTES = BN * BK * 2;
   static constexpr int STAGE = NP * (A_BYTES + B_BYTES);
   static constexpr int BAR_OFF = STAGES * STAGE;
-  static constexpr int TOTAL = BAR_OFF + (2 * STAGES + 1) * 8 + 16 + 1024;  // + alignment slack
+  static constexpr int NBAR = 2 * STAGES + 5;  // full, empty, acc_full[2], acc_empty[2], done
+  static constexpr int TOTAL = BAR_OFF + NBAR * 8 + 16 + 1024;  // + alignment slack
   static_assert(A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "tiles must keep 1024-byte alignment");
 };
 
@@ -138,19 +145,180 @@ struct Maps {
   CUtensorMap a[3], b[3];
 };
 
+// tile t -> (M tile, N tile, batch, K split), M fastest, K split slowest
+__device__ __forceinline__ void decode(const KParams& p, long t, int& mt, int& nt, int& bz, int& ks) {
+  mt = int(t % p.MT);
+  long r = t / p.MT;
+  nt = int(r % p.NT);
+  r /= p.NT;
+  const long nb = p.tiles / ((long)p.MT * p.NT * p.KS);
+  bz = int(r % nb);
+  ks = int(r / nb);
+}
+// first K block of split s of KS over KT blocks (whole blocks, as even as they come)
+__device__ __forceinline__ int k_begin(int KT, int KS, int s) { return int((long)KT * s / KS); }
+
+// ---- epilogue helpers --------------------------------------------------------------------
+// planes of x: p0 = bf16(x), p1 = bf16(x - p0), p2 = bf16(x - p0 - p1)
+__device__ __forceinline__ void split3(float x, __nv_bfloat16& h0, __nv_bfloat16& h1, __nv_bfloat16& h2) {
+  h0 = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(h0);
+  h1 = __float2bfloat16_rn(r1);
+  h2 = __float2bfloat16_rn(r1 - __bfloat162float(h1));
+}
+
+// 16 consecutive values -> np planes at idx (vector stores when aligned: idx % 8 == 0)
+__device__ __forceinline__ void put_planes16(const float* v, void* const* out, int np, long idx, bool vec, int valid) {
+  __nv_bfloat16 h[3][16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) split3(v[j], h[0][j], h[1][j], h[2][j]);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    if (q >= np) break;
+    __nv_bfloat16* dst = static_cast<__nv_bfloat16*>(out[q]) + idx;
+    if (vec) {
+      uint4 w0, w1;
+      memcpy(&w0, &h[q][0], 16);
+      memcpy(&w1, &h[q][8], 16);
+      reinterpret_cast<uint4*>(dst)[0] = w0;
+      reinterpret_cast<uint4*>(dst)[1] = w1;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (j < valid) dst[j] = h[q][j];
+    }
+  }
+}
+
+__device__ __forceinline__ void ld16f(const float* src, float* v, bool vec, int valid) {
+  if (vec) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float4 x = reinterpret_cast<const float4*>(src)[j];
+      v[4 * j] = x.x; v[4 * j + 1] = x.y; v[4 * j + 2] = x.z; v[4 * j + 3] = x.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = j < valid ? src[j] : 0.f;
+  }
+}
+__device__ __forceinline__ void st16f(float* dst, const float* v, bool vec, int valid) {
+  if (vec) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      reinterpret_cast<float4*>(dst)[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (j < valid) dst[j] = v[j];
+  }
+}
+
+// the accumulator row `row` (TMEM lane) of one tile, at column base taddr, through the epilogue
+template <int BN>
+__device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, int row, int mt, int nt, int bz,
+                                              int ks) {
+  const int gm = mt * BM + row;  // row within the batch
+  const bool live = gm < p.M;
+  const UmmaEpilogue& e = p.e;
+  if (e.kind == UMMA_EPI_TAYLOR) {
+    const int h = e.half, nmo = e.nmo;
+    const long srow = ((long)bz * p.M + gm) * (2L * nmo);
+#pragma unroll 1
+    for (int c = 0; c < h; c += 16) {
+      float re[16], im[16];
+      __syncwarp();
+      tmem_ld16(taddr + uint32_t(c), re);
+      tmem_ld16(taddr + uint32_t(h + c), im);
+      const int i0 = nt * h + c;
+      if (live && i0 < nmo) {
+      const int valid = nmo - i0 < 16 ? nmo - i0 : 16;
+      const bool vec = valid == 16 && (nmo % 8) == 0;
+      float tr[16], ti[16], s0[16], s1[16];
+      float* S0 = e.S + srow + i0;
+      float* S1 = S0 + nmo;
+      ld16f(S0, s0, vec, valid);
+      ld16f(S1, s1, vec, valid);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        tr[j] = -im[j] * e.inv_k;
+        ti[j] = re[j] * e.inv_k;
+        s0[j] += tr[j];
+        s1[j] += ti[j];
+      }
+      st16f(S0, s0, vec, valid);
+      st16f(S1, s1, vec, valid);
+      if (e.write == 1) {
+        put_planes16(tr, e.out, e.out_planes, srow + i0, vec, valid);
+        put_planes16(ti, e.out, e.out_planes, srow + nmo + i0, vec, valid);
+      } else if (e.write == 2) {
+        put_planes16(s0, e.out, e.out_planes, srow + i0, vec, valid);
+        put_planes16(s1, e.out, e.out_planes, srow + nmo + i0, vec, valid);
+      }
+      }
+    }
+    return;
+  }
+  if (e.kind == UMMA_EPI_TO_WALKERS) {
+    // rows (w, a, c) of the walker operand, columns j
+    const int w = gm / (2 * e.nel), a = (gm >> 1) % e.nel, cp = gm & 1;
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 16) {
+      float v[16];
+      __syncwarp();
+      tmem_ld16(taddr + uint32_t(c), v);
+      if (live) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int gn = nt * BN + c + j;
+          if (gn < p.N) e.SM[(((long)w * p.N + gn) * e.nel + a) * 2 + cp] = double(p.alpha * v[j]);
+        }
+      }
+    }
+    return;
+  }
+  // STORE / STORE_SPLIT
+  const long rbase = (long)ks * p.sCk + (long)bz * p.sCb + (long)gm * p.ldc;
+  float* crow = p.C + rbase;
+#pragma unroll 1
+  for (int c = 0; c < BN; c += 16) {
+    float v[16];
+    __syncwarp();
+    tmem_ld16(taddr + uint32_t(c), v);
+    const int n0 = nt * BN + c;
+    if (!live || n0 >= p.N) continue;
+    const int valid = p.N - n0 < 16 ? p.N - n0 : 16;
+    const bool vec4 = valid == 16 && ((rbase + n0) % 4) == 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] *= p.alpha;
+    if (p.beta != 0.f) {
+      float o[16];
+      ld16f(crow + n0, o, vec4, valid);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[j] += p.beta * o[j];
+    }
+    st16f(crow + n0, v, vec4, valid);
+    if (e.kind == UMMA_EPI_STORE_SPLIT)
+      put_planes16(v, e.out, e.out_planes, rbase + n0, valid == 16 && ((rbase + n0) % 8) == 0, valid);
+  }
+}
+
 template <int BN, int STAGES, int NP>
-__global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_constant__ Maps maps, KParams p) {
+__global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_constant__ Maps maps,
+                                                                const __grid_constant__ KParams p) {
   using L = Smem<BN, STAGES, NP>;
+  constexpr uint32_t COLS = tmem_cols<BN>();  // one accumulator buffer; two are allocated
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
   uint64_t* empty = full + STAGES;
-  uint64_t* accum = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum + 1);
+  uint64_t* acc_full = empty + STAGES;  // [2]
+  uint64_t* acc_empty = acc_full + 2;   // [2]
+  uint64_t* done = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile int* s_abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN, bz = blockIdx.z;
   const int KT = (p.K + BK - 1) / BK;
   const uint32_t stage_tx = uint32_t(L::STAGE);
 
@@ -159,13 +327,17 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accum, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 128);
+    }
+    mbar_init(done, 1);
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
-                 "r"(tmem_cols<BN>()));
+                 "r"(2 * COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   fence_before();
@@ -176,86 +348,105 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
 
   if (warp == 0) {
     if (lane == 0) {  // TMA producer
-      int issued = 0;
-      for (int kt = 0; kt < KT; ++kt) {
-        const int s = kt % STAGES;
-        const uint32_t ph = (kt / STAGES) & 1;
-        if (!mbar_wait(&empty[s], ph ^ 1, deadline)) {
-          *s_abort = 1;
-          break;
-        }
-        if (*s_abort) break;
-        unsigned char* st = smem + s * L::STAGE;
-        mbar_expect_tx(&full[s], stage_tx);
-        const int k0 = kt * BK;
+      uint32_t it = 0;
+      bool stop = false;
+      for (long t = blockIdx.x; t < p.tiles && !stop; t += gridDim.x) {
+        int mt, nt, bz, ks;
+        decode(p, t, mt, nt, bz, ks);
+        const int m0 = mt * BM, n0 = nt * BN;
         const int ab = p.a_batched ? bz : 0, bb = p.b_batched ? bz : 0;
+        const int kb = k_begin(KT, p.KS, ks), ke = k_begin(KT, p.KS, ks + 1);
+        for (int kt = kb; kt < ke; ++kt, ++it) {
+          const int s = int(it % STAGES);
+          const uint32_t ph = (it / STAGES) & 1;
+          if (!mbar_wait(&empty[s], ph ^ 1, deadline) || *s_abort) {
+            *s_abort = 1;
+            stop = true;
+            break;
+          }
+          unsigned char* st = smem + s * L::STAGE;
+          mbar_expect_tx(&full[s], stage_tx);
+          const int k0 = kt * BK;
 #pragma unroll
-        for (int q = 0; q < NP; ++q) {
-          tma_load_3d(st + q * L::A_BYTES, &maps.a[q], &full[s], k0, m0, ab);
-          tma_load_3d(st + NP * L::A_BYTES + q * L::B_BYTES, &maps.b[q], &full[s], k0, n0, bb);
+          for (int q = 0; q < NP; ++q) {
+            tma_load_3d(st + q * L::A_BYTES, &maps.a[q], &full[s], k0, m0, ab);
+            tma_load_3d(st + NP * L::A_BYTES + q * L::B_BYTES, &maps.b[q], &full[s], k0, n0, bb);
+          }
         }
-        issued = kt + 1;
       }
       // drain: every issued stage must have landed before the CTA may exit
-      for (int kt = (issued > STAGES ? issued - STAGES : 0); kt < issued; ++kt)
-        mbar_wait(&full[kt % STAGES], (kt / STAGES) & 1, gtimer() + kWaitNs);
+      for (uint32_t j = (it > uint32_t(STAGES) ? it - STAGES : 0u); j < it; ++j)
+        mbar_wait(&full[j % STAGES], (j / STAGES) & 1, gtimer() + kWaitNs);
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
       constexpr uint32_t idesc = instr_desc<BN>();
-      for (int kt = 0; kt < KT; ++kt) {
-        const int s = kt % STAGES;
-        const uint32_t ph = (kt / STAGES) & 1;
-        if (*s_abort || !mbar_wait(&full[s], ph, deadline)) {
+      uint32_t it = 0;
+      int lt = 0;
+      bool stop = false;
+      for (long t = blockIdx.x; t < p.tiles && !stop; t += gridDim.x, ++lt) {
+        const int b = lt & 1;
+        const uint32_t aph = (uint32_t(lt) >> 1) & 1;
+        if (*s_abort || !mbar_wait(&acc_empty[b], aph ^ 1, deadline)) {
           *s_abort = 1;
           break;
         }
         fence_after();
-        unsigned char* st = smem + s * L::STAGE;
-        uint64_t ad[NP], bd[NP];
+        const uint32_t d_tmem = tmem + uint32_t(b) * COLS;
+        int mt, nt, bz, ks;
+        decode(p, t, mt, nt, bz, ks);
+        const int kb = k_begin(KT, p.KS, ks), ke = k_begin(KT, p.KS, ks + 1);
+        for (int kt = kb; kt < ke; ++kt, ++it) {
+          const int s = int(it % STAGES);
+          const uint32_t ph = (it / STAGES) & 1;
+          if (*s_abort || !mbar_wait(&full[s], ph, deadline)) {
+            *s_abort = 1;
+            stop = true;
+            break;
+          }
+          fence_after();
+          unsigned char* st = smem + s * L::STAGE;
+          uint64_t ad[NP], bd[NP];
 #pragma unroll
-        for (int q = 0; q < NP; ++q) {
-          ad[q] = smem_desc(st + q * L::A_BYTES);
-          bd[q] = smem_desc(st + NP * L::A_BYTES + q * L::B_BYTES);
+          for (int q = 0; q < NP; ++q) {
+            ad[q] = smem_desc(st + q * L::A_BYTES);
+            bd[q] = smem_desc(st + NP * L::A_BYTES + q * L::B_BYTES);
+          }
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            const uint64_t off = uint64_t(kk * 32) >> 4;  // 16 bf16 = 32 bytes along the swizzled row
+#pragma unroll
+            for (int tt = 0; tt < n_terms(NP); ++tt)
+              umma_bf16(d_tmem, ad[term_a(tt)] + off, bd[term_b(tt)] + off, idesc, ((kt - kb) | kk | tt) ? 1u : 0u);
+          }
+          umma_commit(&empty[s]);
         }
-#pragma unroll
-        for (int kk = 0; kk < BK / 16; ++kk) {
-          const uint64_t off = uint64_t(kk * 32) >> 4;  // 16 bf16 = 32 bytes along the swizzled row
-#pragma unroll
-          for (int tt = 0; tt < n_terms(NP); ++tt)
-            umma_bf16(tmem, ad[term_a(tt)] + off, bd[term_b(tt)] + off, idesc, (kt | kk | tt) ? 1u : 0u);
-        }
-        umma_commit(&empty[s]);
+        if (!stop) umma_commit(&acc_full[b]);
       }
-      umma_commit(accum);
+      // every MMA issued has completed before the tensor memory may be released
+      umma_commit(done);
+      mbar_wait(done, 0, gtimer() + kWaitNs);
     }
   } else {  // epilogue warps 2..5 -> TMEM lane quarters 2,3,0,1
     const int q = warp & 3;
     const int row = q * 32 + lane;
-    const bool ok = mbar_wait(accum, 0, deadline);
-    fence_after();
-    if (ok && !*s_abort) {
-      const int gm = m0 + row;
-      float* Cb = p.C + (long)bz * p.sCb;
-#pragma unroll 1
-      for (int c = 0; c < BN; c += 16) {
-        float v[16];
-        tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c), v);
-        if (gm < p.M) {
-          float* crow = Cb + (long)gm * p.ldc;
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int gn = n0 + c + j;
-            if (gn < p.N) {
-              float out = p.alpha * v[j];
-              if (p.beta != 0.f) out += p.beta * crow[gn];
-              crow[gn] = out;
-            }
-          }
-        }
+    int lt = 0;
+    for (long t = blockIdx.x; t < p.tiles; t += gridDim.x, ++lt) {
+      const int b = lt & 1;
+      const uint32_t aph = (uint32_t(lt) >> 1) & 1;
+      const bool ok = mbar_wait(&acc_full[b], aph, deadline);
+      // tcgen05.ld is warp-collective: the whole warp goes on, or stops, together
+      const bool go = __all_sync(0xffffffffu, ok) && !__any_sync(0xffffffffu, *s_abort != 0);
+      if (!go) {
+        *s_abort = 1;
+        break;
       }
-    } else if (!ok) {
-      *s_abort = 1;
+      fence_after();
+      int mt, nt, bz, ks;
+      decode(p, t, mt, nt, bz, ks);
+      epilogue_tile<BN>(p, tmem + (uint32_t(q * 32) << 16) + uint32_t(b) * COLS, row, mt, nt, bz, ks);
+      fence_before();
+      mbar_arrive(&acc_empty[b]);
     }
   }
   fence_before();
@@ -263,7 +454,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
   if (threadIdx.x == 0 && *s_abort && p.err) atomicExch(p.err, SFQ_ERR_TIMEOUT);
   if (warp == 1) {
     fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols<BN>()));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * COLS));
   }
 }
 
@@ -307,10 +498,23 @@ int make_map(CUtensorMap* m, const void* base, long rows, long K, long ld, long 
   return SFQ_OK;
 }
 
+int sm_count() {
+  static int counts[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!counts[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    counts[dev] = n;
+  }
+  return counts[dev];
+}
+
 template <int BN, int STAGES, int NP>
 int launch(const UmmaGemmDesc& d, cudaStream_t st) {
   using L = Smem<BN, STAGES, NP>;
   static_assert(L::TOTAL <= 232448, "shared memory budget");
+  static_assert(2 * tmem_cols<BN>() <= 512, "two accumulators must fit in tensor memory");
   Maps maps;
   int rc;
   const long ab = d.A.batch_stride ? d.batch : 1, bb = d.B.batch_stride ? d.batch : 1;
@@ -323,16 +527,38 @@ int launch(const UmmaGemmDesc& d, cudaStream_t st) {
     maps.a[q] = maps.a[0];
     maps.b[q] = maps.b[0];
   }
+  const UmmaEpilogue& e = d.epi;
+  if (e.kind == UMMA_EPI_STORE_SPLIT || (e.kind == UMMA_EPI_TAYLOR && e.write)) {
+    if (e.out_planes < 1 || e.out_planes > 3) return record_error(SFQ_ERR_ARG, "umma_gemm: output planes");
+    for (int q = 0; q < e.out_planes; ++q)
+      if (!e.out[q]) return record_error(SFQ_ERR_ARG, "umma_gemm: output plane %d missing", q);
+  }
+  if (e.kind == UMMA_EPI_TAYLOR) {
+    const bool tile_ok = (BN % 32) == 0 && e.half * 2 == BN;  // two halves of whole 16-column chunks
+    if (!tile_ok || !e.S || e.nmo <= 0)
+      return record_error(SFQ_ERR_ARG, "umma_gemm: Taylor epilogue needs S and tile width 2 * half, half %% 16 == 0");
+  }
+  if (e.kind == UMMA_EPI_TO_WALKERS && (!e.SM || e.nel <= 0 || d.batch != 1 || d.M % (2 * e.nel)))
+    return record_error(SFQ_ERR_ARG, "umma_gemm: walker epilogue needs rows (w, a, c) and one batch");
+  if ((e.kind == UMMA_EPI_STORE || e.kind == UMMA_EPI_STORE_SPLIT) && !d.C)
+    return record_error(SFQ_ERR_ARG, "umma_gemm: output missing");
   KParams kp;
   kp.M = d.M; kp.N = d.N; kp.K = d.K;
   kp.a_batched = d.A.batch_stride != 0; kp.b_batched = d.B.batch_stride != 0;
-  kp.C = d.C; kp.ldc = d.ldc; kp.sCb = d.sCb; kp.alpha = d.alpha; kp.beta = d.beta;
+  kp.MT = (d.M + BM - 1) / BM;
+  kp.NT = (d.N + BN - 1) / BN;
+  const int KT = (d.K + BK - 1) / BK;
+  kp.KS = d.ksplit < 1 ? 1 : (d.ksplit > KT ? KT : d.ksplit);
+  if (kp.KS > 1 && (e.kind != UMMA_EPI_STORE || d.beta != 0.f || d.sCk <= 0))
+    return record_error(SFQ_ERR_ARG, "umma_gemm: K splits write partial sums (plain store, beta = 0, sCk > 0)");
+  kp.tiles = (long)kp.MT * kp.NT * d.batch * kp.KS;
+  kp.C = d.C; kp.ldc = d.ldc; kp.sCb = d.sCb; kp.sCk = d.sCk; kp.alpha = d.alpha; kp.beta = d.beta;
+  kp.e = e;
   kp.err = d.err;
   auto k = umma_gemm_kernel<BN, STAGES, NP>;
   SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
-  dim3 grid((d.M + BM - 1) / BM, (d.N + BN - 1) / BN, d.batch);
-  if (grid.y > 65535u || grid.z > 65535u) return record_error(SFQ_ERR_SHAPE, "umma_gemm: grid too large");
-  k<<<grid, kThreads, L::TOTAL, st>>>(maps, kp);
+  const long grid = kp.tiles < sm_count() ? kp.tiles : sm_count();
+  k<<<unsigned(grid), kThreads, L::TOTAL, st>>>(maps, kp);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
@@ -357,14 +583,22 @@ int umma_gemm(const UmmaGemmDesc& d, cudaStream_t st) {
   if (d.K <= 0) return record_error(SFQ_ERR_SHAPE, "umma_gemm: K must be positive");
   const int bn = d.bn ? d.bn : (d.N <= 64 ? 64 : 128);
   switch (d.nplanes * 1000 + bn) {
-    case 1064: return umma::launch<64, 6, 1>(d, st);
+    case 1032: return umma::launch<32, 8, 1>(d, st);
+    case 1064: return umma::launch<64, 8, 1>(d, st);
     case 1128: return umma::launch<128, 6, 1>(d, st);
+    case 1160: return umma::launch<160, 6, 1>(d, st);
+    case 1208: return umma::launch<208, 4, 1>(d, st);
     case 1256: return umma::launch<256, 4, 1>(d, st);
+    case 2032: return umma::launch<32, 5, 2>(d, st);
     case 2064: return umma::launch<64, 4, 2>(d, st);
     case 2128: return umma::launch<128, 3, 2>(d, st);
+    case 2160: return umma::launch<160, 3, 2>(d, st);
+    case 2208: return umma::launch<208, 2, 2>(d, st);
     case 2256: return umma::launch<256, 2, 2>(d, st);
+    case 3032: return umma::launch<32, 3, 3>(d, st);
     case 3064: return umma::launch<64, 3, 3>(d, st);
     case 3128: return umma::launch<128, 2, 3>(d, st);
+    case 3160: return umma::launch<160, 2, 3>(d, st);
     default:
       return record_error(SFQ_ERR_ARG, "umma_gemm: %d planes with tile width %d not built", d.nplanes, bn);
   }

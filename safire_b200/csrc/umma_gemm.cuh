@@ -10,11 +10,26 @@
 // all accumulated in FP32 in tensor memory: the "complex FP32 from split-BF16" arithmetic of the
 // mixed-precision propagation.
 //
-// Operands are K-major (K contiguous), loaded by TMA as 64-element (128-byte) K slices with the
-// 128-byte swizzle; one elected thread issues tcgen05.mma (M = 128, N = BN, K = 16) on the smem
-// descriptors; tcgen05.commit releases each stage to the TMA producer; four epilogue warps read
-// the accumulator with tcgen05.ld.  Every mbarrier wait is bounded: on expiry the kernel records
-// SFQ_ERR_TIMEOUT in *err, drains its own TMA loads, frees its tensor memory and returns.
+// Persistent kernel, one CTA per SM walking a static list of 128 x BN output tiles (M fastest, so
+// the CTAs that share a B tile run together; optionally also split along K, each split writing
+// its own partial C, for products with few output tiles and a long K).  Operands are K-major
+// (K contiguous), loaded by TMA as 64-element (128-byte) K slices with the 128-byte swizzle into
+// a ring of stages; one elected
+// thread issues tcgen05.mma (M = 128, N = BN, K = 16) on the smem descriptors and commits each
+// stage back to the TMA producer; the accumulator is double-buffered in tensor memory, so four
+// epilogue warps drain tile i (tcgen05.ld) while the tensor core computes tile i + 1.  Every
+// mbarrier wait is bounded: on expiry the kernel records SFQ_ERR_TIMEOUT in *err, waits for its
+// own TMA loads and MMAs, frees its tensor memory and returns.
+//
+// The epilogue is selectable, so that the elementwise work around the products of the mixed
+// propagation happens while the tile is still on chip:
+//   STORE        C = alpha acc + beta C
+//   STORE_SPLIT  C = alpha acc, and the BF16 planes of C (same layout) for a following product
+//   TAYLOR       the tile's columns are [re | im] halves over `half` orbitals i (B rows ordered so);
+//                T = (i / k) C, i.e. T_re = -C_im / k, T_im = C_re / k; S += T; planes of T (the
+//                next term's A operand) or of the updated S (the final P1 product's A operand).
+//                S and the planes use the walker layout [b][row][c * nmo + i].
+//   TO_WALKERS   rows (w, a, c), columns j: SM[w][j][a].c = alpha acc (complex fp64 walkers)
 #pragma once
 #include <cuda.h>
 
@@ -29,6 +44,23 @@ struct UmmaOperand {
   long batch_stride = 0;     // elements between batches (0: shared)
 };
 
+enum UmmaEpiKind { UMMA_EPI_STORE = 0, UMMA_EPI_STORE_SPLIT = 1, UMMA_EPI_TAYLOR = 2, UMMA_EPI_TO_WALKERS = 3 };
+
+struct UmmaEpilogue {
+  int kind = UMMA_EPI_STORE;
+  void* out[3] = {nullptr, nullptr, nullptr};  // bf16 planes written by STORE_SPLIT and TAYLOR
+  int out_planes = 0;                          // how many of them (1..3)
+  // TAYLOR
+  float* S = nullptr;     // [batch][M rows][2 * nmo]
+  int nmo = 0;            // orbitals per half
+  int half = 0;           // orbitals per tile (BN = 2 * half, a multiple of 16)
+  float inv_k = 0.f;      // 1 / k for T_{k+1} = (i / k) C
+  int write = 0;          // 1: planes of T_{k+1}; 2: planes of the updated S; 0: none
+  // TO_WALKERS
+  double* SM = nullptr;   // (nwalk, nmo, nel) complex
+  int nel = 0;
+};
+
 struct UmmaGemmDesc {
   int M = 0, N = 0, K = 0, batch = 1;
   UmmaOperand A, B;
@@ -36,7 +68,10 @@ struct UmmaGemmDesc {
   long ldc = 0, sCb = 0;  // fp32 row-major output
   float alpha = 1.f, beta = 0.f;
   int nplanes = 2;        // 1, 2 or 3 (see above)
-  int bn = 0;             // tile width: 0 = automatic, else 64, 128 or 256 (256: nplanes <= 2)
+  int bn = 0;             // tile width: 0 = automatic, else 32, 64, 128, 160, 208 or 256
+  int ksplit = 1;         // K split into this many ranges, each writing its partial C at C + s * sCk
+  long sCk = 0;
+  UmmaEpilogue epi;
   int* err = nullptr;     // device flag, SFQ_ERR_TIMEOUT on an expired wait (may be null)
 };
 
