@@ -3,7 +3,9 @@
   python -m safire_b200.opbench --op vhs --M 400 --N 100 --Nc 2400 --W 64 --reps 3
 
 Operands are random with the shapes of the path; prints one JSON line per op with the
-average device time per call and the algorithmic TFLOP/s.
+average device time per call and the algorithmic TFLOP/s.  `mixed_step` runs whole propagation
+steps of a resident mixed-precision engine on a synthetic system of the given sizes (the Taylor
+and P1 products do not depend on Nc, so a small Nc profiles them in a small footprint).
 """
 import argparse
 import json
@@ -24,10 +26,40 @@ def _flops(op, M, N, Nc, W):
         "orthogonalize": 2 * (8.0 * N * N * M * 2) * W,
         "umma_vhs": 2.0 * (2 * W) * M * M * Nc,   # one real product of the split GEMM
         "umma_planes": 2.0 * (2 * W) * M * M * Nc,
+        "mixed_step": (8.0 * N * M * Nc + 4.0 * M * M * Nc + 64.0 * M * M * N + 24.0 * N * N * M
+                       + (32.0 / 3.0) * N ** 3) * W,
     }[op]
 
 
+def _mixed_step(M, N, Nc, W, reps, warm):
+    from . import capi, synthetic
+    s = synthetic.make_system(synthetic.SystemSpec(M=M, N=N, Nc=Nc, decay=max(Nc / 6.0, 1.0), seed=0))
+    eng = afqmc.AfqmcEngine(s, W, dt=0.0005, seed=1, precision=capi.PRECISION_MIXED)
+    Esh = eng.init()
+    ext = torch.cuda.ExternalStream(eng.stream)
+    step = 0
+    for _ in range(warm):
+        eng.propagate(Esh, step)
+        step += 1
+    eng.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(ext)
+    for _ in range(reps):
+        eng.propagate(Esh, step)
+        step += 1
+    e1.record(ext)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    eng.close()
+    return ms
+
+
 def run(op, M, N, Nc, W, reps, warm=2, real_lnak=True):
+    if op == "mixed_step":
+        ms = _mixed_step(M, N, Nc, W, reps, warm)
+        fl = _flops(op, M, N, Nc, W)
+        return {"op": op, "M": M, "N": N, "Nc": Nc, "W": W, "ms": ms, "tflops": fl / (ms * 1e-3) / 1e12}
     g = torch.Generator(device="cuda").manual_seed(0)
 
     def crand(*shape):
