@@ -396,7 +396,19 @@ def main():
                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                     "executed_tflops": achieved * nprod, "executed_frac": achieved * nprod / peak,
                     "peak_source": src}
-    roofline.update({"algorithmic_flops_per_launch": alg, "launch_ms": launch_ms, "traffic": None,
+    traffic = None
+    if prec == capi.PRECISION_MIXED and m["vhs_packed"] and W == 256 and spec.Nc == 2400:
+        # dram__bytes_read.sum + dram__bytes_write.sum of this kernel in one ncu capture of the same
+        # product with 80089 rows, 256 walkers, Nc = 2400
+        # (profiles/umma_gemm_vhs_packed_rows80089_W256_Nc2400_full.md: 779.1 + 153.2 MB), scaled
+        # by the rows of this system (both operand and result bytes grow with the rows)
+        rows = spec.M * (spec.M + 1) // 2
+        traffic = (779.1e6 + 153.2e6) * rows / 80089.0
+        roofline.update({"traffic_unit": "bytes per launch",
+                         "traffic_source": "ncu capture of the same product (80089 rows), scaled to this system's rows",
+                         "algorithmic_bytes_per_launch": 2 * 2.0 * rows * spec.Nc + 2 * 2.0 * 2 * W * spec.Nc
+                         + 4.0 * 2 * W * rows})
+    roofline.update({"algorithmic_flops_per_launch": alg, "launch_ms": launch_ms, "traffic": traffic,
                      "vhs_columns": "packed upper triangle M(M+1)/2" if m["vhs_packed"] else "full M*M"})
     tot = sum(v[0] for k, v in ph.items() if k != "vHS_gemm")
     phases = {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / tot if tot else None}

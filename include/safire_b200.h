@@ -205,12 +205,15 @@ void sfq_engine_params_default(sfq_engine_params_t* p);
 int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
                       const void* PsiT);
 int sfq_engine_destroy(sfq_engine_t e);
+/* waits for the engine stream; SFQ_ERR_TIMEOUT if a tensor-core product's bounded wait expired */
 int sfq_engine_synchronize(sfq_engine_t e);
 /* the stream the engine enqueues on (cudaStream_t) */
 void* sfq_engine_stream(sfq_engine_t e);
 
 /* walker set I/O (WalkerSetBase.h:320-481): SM (nwalk, nmo, nel) complex; props (8, nwalk) complex in the
- * order WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, THETA.  Host pointers; NULL skips. */
+ * order WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, THETA.  Host pointers; NULL skips.
+ * set_walkers also drops the inverse overlap matrices the engine keeps for the next step: call it
+ * with both NULL after writing the walkers through sfq_engine_info's device pointer. */
 int sfq_engine_set_walkers(sfq_engine_t e, const void* SM, const void* props);
 int sfq_engine_get_walkers(sfq_engine_t e, void* SM, void* props);
 /* the reference's walker_buffer rows (nwalk, nmo*nel + 11): SM, WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_,
@@ -271,7 +274,8 @@ int sfq_engine_profile(sfq_engine_t e, int enable);
 /* synchronizes; ms[ph] = summed device time since the last call, counts[ph] = intervals (either may be NULL) */
 int sfq_engine_phase_times(sfq_engine_t e, double* ms, int* counts, int nphase);
 
-/* device addresses of the engine's resident arrays, for tests and zero-copy callers */
+/* device addresses of the engine's resident arrays, for tests and zero-copy callers (writes to SM
+ * through this pointer are announced with sfq_engine_set_walkers(e, NULL, NULL)) */
 typedef struct {
   void* SM;           /* (nwalk, nmo, nel) complex */
   void* props;        /* (8, nwalk) complex */

@@ -685,7 +685,7 @@ struct Engine {
     ph_end(SFQ_PH_POPCONTROL);
     int flag = 0;
     SFQ_CUDA_TRY(cudaMemcpyAsync(&flag, pw.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    if ((rc = sync_checked())) return rc;
     if (flag == SFQ_ERR_WEIGHT_COLLAPSE) return record_error(flag, "The total walker weight collapsed.");
     if (flag) return record_error(flag, "population control: inconsistent copy plan");
     return SFQ_OK;
@@ -707,7 +707,20 @@ struct Engine {
     averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, E, red);
     SFQ_LAUNCHED();
     SFQ_CUDA_TRY(cudaMemcpyAsync(out10, red, sizeof(double) * 10, cudaMemcpyDeviceToHost, st));
+    return sync_checked();
+  }
+
+  // Synchronise the engine stream, then report a bounded wait of the tensor-core product that
+  // expired since the last check (SFQ_ERR_TIMEOUT: the steps since then are invalid).
+  int sync_checked() {
+    int gflag = 0;
+    if (mixed) SFQ_CUDA_TRY(cudaMemcpyAsync(&gflag, gemm_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    if (gflag) {
+      cudaMemsetAsync(gemm_err, 0, sizeof(int), st);
+      return record_error(SFQ_ERR_TIMEOUT, "tensor-core product: a bounded wait expired; the steps since the "
+                                           "last check are invalid");
+    }
     return SFQ_OK;
   }
 };
@@ -795,8 +808,7 @@ int sfq_engine_destroy(sfq_engine_t h) {
 
 int sfq_engine_synchronize(sfq_engine_t h) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
-  SFQ_CUDA_TRY(cudaStreamSynchronize(h->e.st));
-  return SFQ_OK;
+  return h->e.sync_checked();
 }
 
 void* sfq_engine_stream(sfq_engine_t h) { return h ? (void*)h->e.st : nullptr; }
@@ -871,8 +883,7 @@ int sfq_engine_propagate_host(sfq_engine_t h, double Eshift, unsigned long long 
   if ((rc = e.propagate(Eshift, step, ud))) return rc;
   if (props_host)
     SFQ_CUDA_TRY(cudaMemcpyAsync(props_host, e.props, sizeof(cplx) * kNumProps * e.W, cudaMemcpyDeviceToHost, e.st));
-  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
-  return SFQ_OK;
+  return e.sync_checked();
 }
 
 int sfq_engine_orthogonalize(sfq_engine_t h) {
@@ -956,8 +967,7 @@ int sfq_engine_run(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, d
     }
   }
   if (nmeas) *nmeas = nm;
-  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
-  return SFQ_OK;
+  return e.sync_checked();
 }
 
 int sfq_engine_profile(sfq_engine_t h, int enable) {
