@@ -159,14 +159,50 @@ __global__ void __launch_bounds__(LU_THREADS) lu_logdet_kernel(cplx* T, long sT,
 
 // Cholesky of the Hermitian positive definite S (N x N, upper storage used) into R (upper,
 // S = R^H R), then R^-1 (upper) written over S.  status[b] = 0, or j+1 when the pivot j is not
-// positive (the walker matrix lost rank).
-__global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS, int N, int* status) {
+// positive (the walker matrix lost rank).  again[b] = 1 when an upper bound of the condition
+// number of R, sqrt(|R|_1 |R|_inf |R^-1|_1 |R^-1|_inf) with |z| <= |re| + |im|, exceeds
+// kappa_max (one CholeskyQR pass leaves Q^H Q - I of order eps kappa^2: such walkers take a
+// second pass).  Walkers with active[b] == 0 are skipped (active may be null).
+// max over the block of v (all threads call it; red holds >= 32 doubles)
+__device__ __forceinline__ double block_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  for (int w = 0; w < int(blockDim.x >> 5); ++w) r = fmax(r, red[w]);
+  return r;
+}
+
+// |A|_1 * |A|_inf of the upper triangle of A (N x N row-major), |z| as |re| + |im|
+__device__ double norm1_inf_upper(const cplx* A, int N, double* red) {
+  double rmax = 0.0, cmax = 0.0;
+  for (int t = threadIdx.x; t < N; t += blockDim.x) {
+    double rs = 0.0, cs = 0.0;
+    for (int k = t; k < N; ++k) rs += fabs(A[t * N + k].x) + fabs(A[t * N + k].y);
+    for (int i = 0; i <= t; ++i) cs += fabs(A[i * N + t].x) + fabs(A[i * N + t].y);
+    rmax = fmax(rmax, rs);
+    cmax = fmax(cmax, cs);
+  }
+  const double r = block_max(rmax, red);
+  const double c = block_max(cmax, red);
+  return r * c;
+}
+
+__global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS, int N, int* status, int* again,
+                                                               const int* active, double kappa_max) {
+  const long b = blockIdx.x;
+  if (active && !active[b]) return;  // the whole CTA
   extern __shared__ __align__(16) unsigned char sm_raw[];
   cplx* A = reinterpret_cast<cplx*>(sm_raw);
   cplx* work = A + N * N;
+  __shared__ double diag[kMaxSmallN];
+  __shared__ double red[32];
   __shared__ int s_bad;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long b = blockIdx.x;
+  constexpr int NW = LU_THREADS / 32;
   cplx* Sb = S + b * sS;
   for (int e = tid; e < N * N; e += LU_THREADS) A[e] = Sb[e];
   if (tid == 0) s_bad = 0;
@@ -186,7 +222,7 @@ __global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS,
     }
     __syncthreads();
     // A[i][k] -= conj(R[j][i]) * R[j][k] for j < i <= k
-    for (int i = j + 1 + warp; i < N; i += LU_THREADS / 32) {
+    for (int i = j + 1 + warp; i < N; i += NW) {
       const cplx ci = cconj(A[j * N + i]);
       for (int k = i + lane; k < N; k += 32) A[i * N + k] = csub(A[i * N + k], cmul(ci, A[j * N + k]));
     }
@@ -194,29 +230,47 @@ __global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS,
   }
   __syncthreads();
   if (s_bad) {
-    if (tid == 0) status[b] = s_bad;
+    if (tid == 0) {
+      status[b] = s_bad;
+      if (again) again[b] = 0;
+    }
     return;
   }
-  // R^-1 in place (upper, non-unit), as in the LU inverse
-  for (int j = 0; j < N; ++j) {
-    for (int i = tid; i < j; i += LU_THREADS) work[i] = A[i * N + j];
+  const double nR = norm1_inf_upper(A, N, red);
+  // R^-1 by back substitution on all columns at once, right-looking and in place: going up
+  // the rows, row k of R^-1 is the pending row k over r_kk, and its product with column k of R
+  // leaves the rows above at once (one rank-1 update per row, parallel over the block).  The
+  // diagonal of R moves to diag[] and the in-place diagonal becomes the identity's.
+  for (int i = tid; i < N; i += LU_THREADS) {
+    diag[i] = A[i * N + i].x;
+    A[i * N + i] = mk(1.0, 0.0);
+  }
+  __syncthreads();
+  for (int k = N - 1; k >= 0; --k) {
+    const double xkk = 1.0 / diag[k];
+    for (int i = tid; i < k; i += LU_THREADS) work[i] = A[i * N + k];  // column k of R, read once
+    for (int jj = k + tid; jj < N; jj += LU_THREADS) A[k * N + jj] = cscale(A[k * N + jj], xkk);  // row k of R^-1
     __syncthreads();
-    const double ujj = 1.0 / A[j * N + j].x;
-    for (int i = tid; i < j; i += LU_THREADS) {
-      cplx s = mk(0.0, 0.0);
-      for (int k = i; k < j; ++k) s = cadd(s, cmul(A[i * N + k], work[k]));
-      A[i * N + j] = cscale(s, -ujj);
+    // pending rows above: P[i][j] -= R[i][k] X[k][j], where P[i][k] starts at 0 (the identity)
+    for (int i = warp; i < k; i += NW) {
+      const cplx rik = work[i];
+      for (int jj = k + lane; jj < N; jj += 32) {
+        const cplx base = (jj == k) ? mk(0.0, 0.0) : A[i * N + jj];
+        A[i * N + jj] = csub(base, cmul(rik, A[k * N + jj]));
+      }
     }
     __syncthreads();
-    if (tid == 0) A[j * N + j] = mk(ujj, 0.0);
-    __syncthreads();
   }
+  const double nX = norm1_inf_upper(A, N, red);
   // zero the strictly lower part (the GEMM W R^-1 reads the full square)
   for (int e = tid; e < N * N; e += LU_THREADS) {
     int i = e / N, k = e % N;
     Sb[e] = (i > k) ? mk(0.0, 0.0) : A[e];
   }
-  if (tid == 0) status[b] = 0;
+  if (tid == 0) {
+    status[b] = 0;
+    if (again) again[b] = (sqrt(nR * nX) > kappa_max) ? 1 : 0;
+  }
 }
 
 }  // namespace
@@ -242,12 +296,13 @@ int lu_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, 
   return SFQ_OK;
 }
 
-int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, cudaStream_t st) {
+int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, int* again, const int* active, double kappa_max,
+              cudaStream_t st) {
   if (nbatch <= 0 || N <= 0) return SFQ_OK;
   if (N > kMaxSmallN) return record_error(SFQ_ERR_UNSUPPORTED, "chol_rinv: N=%d exceeds %d", N, kMaxSmallN);
   const size_t sm = lu_smem_bytes(N);
   SFQ_CUDA_TRY(cudaFuncSetAttribute(chol_rinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-  chol_rinv_kernel<<<nbatch, LU_THREADS, sm, st>>>(S, sS, N, status);
+  chol_rinv_kernel<<<nbatch, LU_THREADS, sm, st>>>(S, sS, N, status, again, active, kappa_max);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

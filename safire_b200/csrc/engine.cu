@@ -244,7 +244,7 @@ struct Engine {
         {(void**)&Tchunk, c * tchunk_elems},
         {(void**)&exxn, c * (size_t)W * Nc},
         {(void**)&kl, c * (size_t)W * Nc},
-        {(void**)&status, sizeof(int) * W},
+        {(void**)&status, sizeof(int) * 2 * W},
         {(void**)&red, d * 16},
         {(void**)&uni, d * (size_t)W * Nc},
         {(void**)&stats, sizeof(unsigned long long) * 8},

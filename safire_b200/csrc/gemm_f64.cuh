@@ -29,6 +29,7 @@ struct GemmDesc {
   bool a_cplx = false, b_cplx = false, conj_a = false;
   cplx alpha = {1.0, 0.0};
   cplx beta = {0.0, 0.0};
+  const int* mask = nullptr;  // optional: batch b is computed only where mask[b] != 0
 };
 
 int gemm_f64(const GemmDesc& d, cudaStream_t stream);
@@ -92,6 +93,7 @@ __global__ void __launch_bounds__(WM* WN * 32)
   const int wm = warp / WN, wn = warp % WN;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   const long bz = blockIdx.z;
+  if (d.mask && !d.mask[bz]) return;  // the whole CTA: batches left out by the mask
 
   const unsigned char* Ab = (const unsigned char*)d.A + bz * d.sAb * C_::A_ESZ;
   const unsigned char* Bb = (const unsigned char*)d.B + bz * d.sBb * C_::B_ESZ;

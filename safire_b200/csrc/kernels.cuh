@@ -13,7 +13,10 @@ int gj_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, 
 // T: nbatch matrices N x N (row-major, batch stride sT); ovlp[b] = post_scale * fold(acc + logdet)
 int lu_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, double post_scale, bool invert,
               cudaStream_t st);
-int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, cudaStream_t st);
+// S = R^H R and R^-1 over S; again[b] = 1 when R's condition bound exceeds kappa_max (may be
+// null); batches with active[b] == 0 are left alone (active may be null)
+int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, int* again, const int* active, double kappa_max,
+              cudaStream_t st);
 
 struct FieldParams {
   int nwalk = 0, nchol = 0;
@@ -76,6 +79,10 @@ int threshold_real(double* P, long n, double drop, cudaStream_t st);
 int real_of(const cplx* z, double* r, long n, cudaStream_t st);
 int fill_cplx(cplx* p, long n, cplx v, cudaStream_t st);
 int copy_walkers_prop(cplx* dst, const cplx* src, long n, cudaStream_t st);
+// dst walker w = src walker w (n elements each) where (mask[w] != 0) == want
+int copy_walkers_where(cplx* dst, const cplx* src, const int* mask, int want, int W, long n, cudaStream_t st);
+// condition bound below which one CholeskyQR pass is kept
+constexpr double kCholQrKappa = 100.0;
 int scale_cplx(cplx* p, long n, cplx s, cudaStream_t st);
 
 // Symmetric Cholesky vectors, L[i][k][n] == L[k][i][n]: the upper triangle i <= k, row-major,

@@ -122,24 +122,37 @@ int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M
   return p1_apply(P1, p_cplx, TMN, SM, W, M, N, st);
 }
 
+// One CholeskyQR pass over the walkers selected by mask (all when null): S = Win^H Win = R^H R,
+// Wout = Win R^-1; again[b] set from R's condition bound when again is not null.
+static int cholqr_pass(const cplx* Win, cplx* Wout, cplx* S, int* status, int* again, const int* mask, int W, int M,
+                       int N, cudaStream_t st) {
+  int rc;
+  GemmDesc d;  // S = Win^H Win
+  d.M = N; d.N = N; d.K = M; d.batch = W;
+  d.A = Win; d.sAm = 1; d.sAk = N; d.sAb = (long)M * N; d.a_cplx = true; d.conj_a = true;
+  d.B = Win; d.sBk = N; d.sBn = 1; d.sBb = (long)M * N; d.b_cplx = true;
+  d.C = S; d.sCm = N; d.sCn = 1; d.sCb = (long)N * N;
+  d.mask = mask;
+  if ((rc = gemm_f64(d, st))) return rc;
+  if ((rc = chol_rinv(S, (long)N * N, W, N, status, again, mask, kCholQrKappa, st))) return rc;
+  GemmDesc q;  // Wout = Win R^-1
+  q.M = M; q.N = N; q.K = N; q.batch = W;
+  q.A = Win; q.sAm = N; q.sAk = 1; q.sAb = (long)M * N; q.a_cplx = true;
+  q.B = S; q.sBk = N; q.sBn = 1; q.sBb = (long)N * N; q.b_cplx = true;
+  q.C = Wout; q.sCm = N; q.sCn = 1; q.sCb = (long)M * N;
+  q.mask = mask;
+  return gemm_f64(q, st);
+}
+
+// CholeskyQR2, with the second pass only where the first one's R was not well conditioned
+// (kappa bound > kCholQrKappa: Q^H Q - I of one pass is of order eps kappa^2, <= 1e-12 below
+// it).  status holds 2 W ints: the Cholesky status per walker, then the second-pass flags.
 int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int W, int M, int N, cudaStream_t st) {
   int rc;
-  for (int pass = 0; pass < 2; ++pass) {
-    GemmDesc d;  // S = SM^H SM
-    d.M = N; d.N = N; d.K = M; d.batch = W;
-    d.A = SM; d.sAm = 1; d.sAk = N; d.sAb = (long)M * N; d.a_cplx = true; d.conj_a = true;
-    d.B = SM; d.sBk = N; d.sBn = 1; d.sBb = (long)M * N; d.b_cplx = true;
-    d.C = S; d.sCm = N; d.sCn = 1; d.sCb = (long)N * N;
-    if ((rc = gemm_f64(d, st))) return rc;
-    if ((rc = chol_rinv(S, (long)N * N, W, N, status, st))) return rc;
-    GemmDesc q;  // SM2 = SM R^-1
-    q.M = M; q.N = N; q.K = N; q.batch = W;
-    q.A = SM; q.sAm = N; q.sAk = 1; q.sAb = (long)M * N; q.a_cplx = true;
-    q.B = S; q.sBk = N; q.sBn = 1; q.sBb = (long)N * N; q.b_cplx = true;
-    q.C = SM2; q.sCm = N; q.sCn = 1; q.sCb = (long)M * N;
-    if ((rc = gemm_f64(q, st))) return rc;
-    SFQ_CUDA_TRY(cudaMemcpyAsync(SM, SM2, (long)W * M * N * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-  }
+  int* again = status + W;
+  if ((rc = cholqr_pass(SM, SM2, S, status, again, nullptr, W, M, N, st))) return rc;
+  if ((rc = cholqr_pass(SM2, SM, S, status, nullptr, again, W, M, N, st))) return rc;
+  if ((rc = copy_walkers_where(SM, SM2, again, 0, W, (long)M * N, st))) return rc;  // one-pass walkers
   (void)log_detR;
   return SFQ_OK;
 }
@@ -223,7 +236,7 @@ size_t sfq_workspace_size(int op, int nwalk, int nmo, int nel, int nchol) {
     case SFQ_OP_PROPAGATE:
       return 3 * align256(c * (size_t)nwalk * nmo * nel);
     case SFQ_OP_ORTHOGONALIZE:
-      return align256(c * (size_t)nwalk * nmo * nel) + align256(c * nwalk * nel * nel) + align256(sizeof(int) * nwalk);
+      return align256(c * (size_t)nwalk * nmo * nel) + align256(c * nwalk * nel * nel) + align256(2 * sizeof(int) * nwalk);
     case SFQ_OP_ENERGY: {
       long nv = ops::energy_chunk(nwalk, nel, nchol, kEnergyChunkElems);
       return align256(c * (size_t)nwalk * nel * nv * nel) + 2 * align256(c * (size_t)nwalk * nchol);

@@ -22,6 +22,7 @@ int vhs_rows(const double* L, long rows, const cplx* X, cplx* V, int W, int Nc, 
 int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M, int N, int order, cplx* TMN,
               cplx* T1, cplx* T2, cudaStream_t st);
 // CholeskyQR2; SM2 (W*M*N), S (W*N*N) scratch, status (W) ints.  log_detR (W) accumulated if not null
+// CholeskyQR2 in place on SM (SM2, S: scratch; status: 2 W ints)
 int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int W, int M, int N, cudaStream_t st);
 // energy with chunked T; ws: T chunk (W*N*nv*N) + exxn (W*Nc) + kl (W*Nc)
 int energy(cplx* E3, const cplx* G, const cplx* haj, const void* Lnak, bool l_cplx, double E0, int W, int N, int M,

@@ -465,6 +465,13 @@ int energy_finish(const cplx* exxn, const cplx* kl, cplx* E3, int nwalk, int nch
 }
 
 namespace {
+__global__ void copy_where_kernel(cplx* dst, const cplx* src, const int* mask, int want, long n) {
+  const long w = blockIdx.y;
+  if ((mask[w] != 0) != (want != 0)) return;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+    dst[w * n + e] = src[w * n + e];
+}
+
 __global__ void check_symmetric_kernel(const double* L, int M, int Nc, int* flag) {
   const long total = (long)M * M * Nc;
   int bad = 0;
@@ -499,6 +506,13 @@ __global__ void unpack_symmetric_kernel(const cplx* Vp, int W, int M, cplx* V) {
   }
 }
 }  // namespace
+
+int copy_walkers_where(cplx* dst, const cplx* src, const int* mask, int want, int W, long n, cudaStream_t st) {
+  dim3 grid(unsigned((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024), unsigned(W));
+  copy_where_kernel<<<grid, 256, 0, st>>>(dst, src, mask, want, n);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
 
 int check_symmetric(const double* L, int M, int Nc, int* flag, cudaStream_t st) {
   check_symmetric_kernel<<<grid_for((long)M * M * Nc), 256, 0, st>>>(L, M, Nc, flag);
