@@ -132,6 +132,7 @@ struct Engine {
   void* Vb_p[3] = {};
   void* Wt_p[3] = {};
   void* Wt2_p[3] = {};  // second walker-operand buffer: a product's epilogue writes the next A here
+  void* Tb_p[3] = {};   // block operand [[Tr, -Ti], [Ti, Tr]] of the inverse overlaps, (W, 2N, 2N)
   float *Cvb = nullptr, *Cv = nullptr, *Sacc = nullptr;
   int vb_ks = 1;        // K splits of the vbias product (partial sums, reduced in a fixed order)
   int tay_half = 0;     // orbitals per Taylor tile (tile width 2 * tay_half, re and im halves)
@@ -268,6 +269,7 @@ struct Engine {
         mx.push_back({&Vb_p[q], b * W * vb_rows * 2 * M});
         mx.push_back({&Wt_p[q], b * W * MN2});
         mx.push_back({&Wt2_p[q], b * W * MN2});
+        mx.push_back({&Tb_p[q], b * W * 4 * NN});
       }
       std::vector<Item> mx2 = {
           {(void**)&Cvb, sizeof(float) * vb_ks * 2 * (size_t)W * Nc},
@@ -462,8 +464,9 @@ struct Engine {
     return SFQ_OK;
   }
 
-  // --- NOMSD::MixedDensityMatrix (compact, CLOSED: Ov x 2) into G, ov (W; may be null) ------
-  int density(cplx* ov) {
+  // the inverse overlap matrices (PsiT W)^-1 of the current walkers in T, their log overlaps in
+  // ov (W; may be null)
+  int ensure_inverse(cplx* ov) {
     int rc;
     if (!inv_cached) {
       const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
@@ -475,7 +478,39 @@ struct Engine {
     } else if (ov && ov != inv_ov) {
       SFQ_CUDA_TRY(cudaMemcpyAsync(ov, inv_ov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
     }
+    return SFQ_OK;
+  }
+
+  // --- NOMSD::MixedDensityMatrix (compact, CLOSED: Ov x 2) into G, ov (W; may be null) ------
+  int density(cplx* ov) {
+    int rc;
+    if ((rc = ensure_inverse(ov))) return rc;
     return ops::green_compact(T, SM, G, W, M, N, st);
+  }
+
+  // G for the force bias in the mixed mode: G[w][a][k] = sum_b Tinv[b][a] SM[k][b] as split-BF16
+  // products, rows (c, a) of the block [[Tr, -Ti], [Ti, Tr]] against SM read as reals (K = (b, c')
+  // interleaved), written straight into the planar planes of the vbias operand.  The FP64 G of
+  // density() serves the energy; the force bias only ever saw G through these planes.
+  bool mixed_green() const { return (N % 4) == 0; }
+  int density_mixed() {
+    int rc;
+    if ((rc = ensure_inverse(nullptr))) return rc;
+    if (!mixed_green()) {
+      if ((rc = ops::green_compact(T, SM, G, W, M, N, st))) return rc;
+      return mixed_split_planar(G, W, (long)N * M, Gs_p, st);
+    }
+    if ((rc = mixed_build_tblk(T, W, N, Tb_p, st))) return rc;
+    if ((rc = split_bf16_f64(reinterpret_cast<const double*>(SM), 2L * W * M * N, Wt_p[0], Wt_p[1],
+                             nplanes > 2 ? Wt_p[2] : nullptr, st)))
+      return rc;
+    UmmaEpilogue eg;
+    eg.kind = UMMA_EPI_PLANAR_SPLIT;
+    eg.nel = N;
+    eg.nmo = M;
+    for (int q = 0; q < 3; ++q) eg.out[q] = Gs_p[q];
+    eg.out_planes = nplanes;
+    return tc_gemm(Tb_p, 2L * N, 4L * N * N, Wt_p, M, 2L * M * N, 2 * N, W, nullptr, 0, 0, 1.f, p1_tile(), &eg);
   }
 
   // NOMSD::Overlap of the current walkers into ov; keeps their inverse overlap matrices in T
@@ -597,10 +632,9 @@ struct Engine {
     const long MM = (long)M * M, NM = (long)N * M, M2 = 2L * M;
     const double sdt = std::sqrt(p.dt);
     ph_begin(SFQ_PH_DENSITY);
-    if ((rc = density(nullptr))) return rc;
+    if ((rc = density_mixed())) return rc;
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
-    if ((rc = mixed_split_planar(G, W, NM, Gs_p, st))) return rc;
     const long part = 2L * W * Nc;  // one K split's partial sums
     if ((rc = tc_gemm(Gs_p, 2L * W, 0, Lnak_p, Nc, 0, int(NM), 1, Cvb, Nc, 0, 1.f, 128, nullptr, vb_ks, part)))
       return rc;

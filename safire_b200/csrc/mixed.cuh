@@ -14,6 +14,8 @@ int mixed_reduce_planar_to_cplx(const float* C, int KS, long sk, int W, long E, 
 // blocks get `rows` rows per walker, grouped by `half` orbitals (see mixed_kernels.cu)
 int mixed_build_vblk(const float* Cv, int W, int M, bool packed, int half, long rows, void* const* pl,
                      cudaStream_t st);
+// Tinv (W, N, N) -> split planes of the block operand [[Tr, -Ti], [Ti, Tr]] (rows (c, a), columns (b, c'))
+int mixed_build_tblk(const cplx* Tinv, int W, int N, void* const* pl, cudaStream_t st);
 int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* const* pl, cudaStream_t st);
 
 }  // namespace sfq

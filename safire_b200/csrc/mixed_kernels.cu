@@ -108,6 +108,20 @@ __global__ void build_vblk_kernel(const float* Cv, int W, int M, int packed, int
   }
 }
 
+// inverse overlaps Tinv (W, N, N) complex -> the real block operand of G = (W Tinv)^T, rows
+// (c, a), columns (b, c'): [[Tr, -Ti], [Ti, Tr]] at (Tinv[b][a]), split
+__global__ void build_tblk_kernel(const cplx* Tinv, int W, int N, Planes P) {
+  const long N2 = 2L * N;
+  const long total = (long)W * N2 * N2;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long w = t / (N2 * N2), r = (t / N2) % N2, q = t % N2;
+    const int c = int(r / N), a = int(r % N), b = int(q >> 1), cp = int(q & 1);
+    const cplx z = Tinv[(w * N + b) * N + a];
+    const double v = (c == cp) ? z.x : (c == 0 ? -z.y : z.y);
+    split_store_d(v, P, t);
+  }
+}
+
 // SM (W, M, N) complex fp64 -> WT[w][a][c][i] split, 32x32 tiles through shared memory
 __global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, Planes P) {
   __shared__ cplx tile[32][33];
@@ -148,6 +162,12 @@ int mixed_reduce_planar_to_cplx(const float* C, int KS, long sk, int W, long E, 
 int mixed_build_vblk(const float* Cv, int W, int M, bool packed, int half, long rows, void* const* pl,
                      cudaStream_t st) {
   build_vblk_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Cv, W, M, packed ? 1 : 0, half, rows, planes(pl));
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int mixed_build_tblk(const cplx* Tinv, int W, int N, void* const* pl, cudaStream_t st) {
+  build_tblk_kernel<<<grid_for((long)W * 4 * N * N), 256, 0, st>>>(Tinv, W, N, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

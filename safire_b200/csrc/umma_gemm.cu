@@ -19,6 +19,7 @@ struct KParams {
   int M, N, K;
   int a_batched, b_batched;
   int MT, NT, KS;  // tiles along M, N; K splits
+  int batch;
   long tiles;
   float* C;
   long ldc, sCb, sCk;  // sCk: elements between the partial outputs of the K splits
@@ -255,6 +256,25 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
         put_planes16(s0, e.out, e.out_planes, srow + i0, vec, valid);
         put_planes16(s1, e.out, e.out_planes, srow + nmo + i0, vec, valid);
       }
+      }
+    }
+    return;
+  }
+  if (e.kind == UMMA_EPI_PLANAR_SPLIT) {
+    const int c = gm / e.nel, a = gm - c * e.nel;
+    const long orow = ((long)c * p.batch + bz) * e.nel + a;
+#pragma unroll 1
+    for (int cc = 0; cc < BN; cc += 16) {
+      float v[16];
+      __syncwarp();
+      tmem_ld16(taddr + uint32_t(cc), v);
+      const int n0 = nt * BN + cc;
+      if (live && n0 < p.N) {
+        const int valid = p.N - n0 < 16 ? p.N - n0 : 16;
+        const long idx = orow * e.nmo + n0;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] *= p.alpha;
+        put_planes16(v, e.out, e.out_planes, idx, valid == 16 && (idx % 8) == 0, valid);
       }
     }
     return;
@@ -528,7 +548,9 @@ int launch(const UmmaGemmDesc& d, cudaStream_t st) {
     maps.b[q] = maps.b[0];
   }
   const UmmaEpilogue& e = d.epi;
-  if (e.kind == UMMA_EPI_STORE_SPLIT || (e.kind == UMMA_EPI_TAYLOR && e.write)) {
+  if (e.kind == UMMA_EPI_PLANAR_SPLIT && (e.nel <= 0 || d.M != 2 * e.nel || e.nmo < d.N))
+    return record_error(SFQ_ERR_ARG, "umma_gemm: planar epilogue needs rows (c, a), 2 * nel of them");
+  if (e.kind == UMMA_EPI_STORE_SPLIT || e.kind == UMMA_EPI_PLANAR_SPLIT || (e.kind == UMMA_EPI_TAYLOR && e.write)) {
     if (e.out_planes < 1 || e.out_planes > 3) return record_error(SFQ_ERR_ARG, "umma_gemm: output planes");
     for (int q = 0; q < e.out_planes; ++q)
       if (!e.out[q]) return record_error(SFQ_ERR_ARG, "umma_gemm: output plane %d missing", q);
@@ -552,6 +574,7 @@ int launch(const UmmaGemmDesc& d, cudaStream_t st) {
   if (kp.KS > 1 && (e.kind != UMMA_EPI_STORE || d.beta != 0.f || d.sCk <= 0))
     return record_error(SFQ_ERR_ARG, "umma_gemm: K splits write partial sums (plain store, beta = 0, sCk > 0)");
   kp.tiles = (long)kp.MT * kp.NT * d.batch * kp.KS;
+  kp.batch = d.batch;
   kp.C = d.C; kp.ldc = d.ldc; kp.sCb = d.sCb; kp.sCk = d.sCk; kp.alpha = d.alpha; kp.beta = d.beta;
   kp.e = e;
   kp.err = d.err;

@@ -30,6 +30,9 @@
 //                next term's A operand) or of the updated S (the final P1 product's A operand).
 //                S and the planes use the walker layout [b][row][c * nmo + i].
 //   TO_WALKERS   rows (w, a, c), columns j: SM[w][j][a].c = alpha acc (complex fp64 walkers)
+//   PLANAR_SPLIT rows (c, a) of batch b (c < 2, a < nel), columns n: the BF16 planes of
+//                alpha acc at row (c * batch + b) * nel + a, column n of an nmo-wide matrix (the
+//                planar operand of a following product)
 #pragma once
 #include <cuda.h>
 
@@ -44,7 +47,13 @@ struct UmmaOperand {
   long batch_stride = 0;     // elements between batches (0: shared)
 };
 
-enum UmmaEpiKind { UMMA_EPI_STORE = 0, UMMA_EPI_STORE_SPLIT = 1, UMMA_EPI_TAYLOR = 2, UMMA_EPI_TO_WALKERS = 3 };
+enum UmmaEpiKind {
+  UMMA_EPI_STORE = 0,
+  UMMA_EPI_STORE_SPLIT = 1,
+  UMMA_EPI_TAYLOR = 2,
+  UMMA_EPI_TO_WALKERS = 3,
+  UMMA_EPI_PLANAR_SPLIT = 4
+};
 
 struct UmmaEpilogue {
   int kind = UMMA_EPI_STORE;

@@ -94,14 +94,16 @@ def test_mixed_engine_one_step_vs_oracle(prec, spec):
     dbg = prop.propagate(wo, Esh_o, 0)
     eng.propagate(Esh, 0)
     tol = STEP_TOL[prec]
-    G = eng.fetch("G", (W, s.N, s.M), np.complex128)
-    assert _rel(G, dbg["G"]) < 1e-10  # the mixed density matrix stays FP64
     X = eng.fetch("X", (W, s.Nc), np.complex128)
     assert _rel(X, dbg["X"]) < tol  # fields carry the force bias from the split vbias product
     SM, pr = eng.walkers()
     assert _rel(SM, wo.SM) < tol
     assert _rel(pr["OVLP"], wo.ovlp) < 10 * tol
     assert _rel(pr["WEIGHT"], wo.weight) < 10 * tol
+    # the local energy stays FP64: of these walkers it matches the oracle's on the same walkers
+    E = eng.energy()
+    Eo, _ = O.wfn_energy_noupdate(ham, O.Walkers(SM))
+    assert _rel(E, Eo) < 1e-10
     eng.close()
 
 
