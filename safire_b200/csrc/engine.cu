@@ -133,10 +133,12 @@ struct Engine {
   void* Wt_p[3] = {};
   void* Wt2_p[3] = {};  // second walker-operand buffer: a product's epilogue writes the next A here
   void* Tb_p[3] = {};   // block operand [[Tr, -Ti], [Ti, Tr]] of the inverse overlaps, (W, 2N, 2N)
+  void* Ws_p[3] = {};   // the walkers read as reals, (W, M, 2N): the other operand of G
   float *Cvb = nullptr, *Cv = nullptr, *Sacc = nullptr;
   int vb_ks = 1;        // K splits of the vbias product (partial sums, reduced in a fixed order)
   int tay_half = 0;     // orbitals per Taylor tile (tile width 2 * tay_half, re and im halves)
-  long vb_rows = 0;     // rows of one walker's vHS block operand: ceil(M / tay_half) * 2 * tay_half
+  long vb_rows = 0;     // output columns of a Taylor product: ceil(M / tay_half) * 2 * tay_half
+  int ldh = 0;          // padded half of the walker operand rows (re, im): M rounded up to 64
   int* gemm_err = nullptr;
   double* h_pinned = nullptr;  // pinned host staging for e2e calls
   size_t h_pinned_bytes = 0;
@@ -266,10 +268,11 @@ struct Engine {
         mx.push_back({&P1_p[q], b * MM});
         mx.push_back({&Gs_p[q], b * 2 * W * MN});
         mx.push_back({&Xs_p[q], b * 2 * (size_t)W * Nc});
-        mx.push_back({&Vb_p[q], b * W * vb_rows * 2 * M});
-        mx.push_back({&Wt_p[q], b * W * MN2});
-        mx.push_back({&Wt2_p[q], b * W * MN2});
+        mx.push_back({&Vb_p[q], b * W * 2 * MM});
+        mx.push_back({&Wt_p[q], b * W * 2L * N * ldh});
+        mx.push_back({&Wt2_p[q], b * W * 2L * N * ldh});
         mx.push_back({&Tb_p[q], b * W * 4 * NN});
+        mx.push_back({&Ws_p[q], b * W * 2 * MN});
       }
       std::vector<Item> mx2 = {
           {(void**)&Cvb, sizeof(float) * vb_ks * 2 * (size_t)W * Nc},
@@ -501,8 +504,8 @@ struct Engine {
       return mixed_split_planar(G, W, (long)N * M, Gs_p, st);
     }
     if ((rc = mixed_build_tblk(T, W, N, Tb_p, st))) return rc;
-    if ((rc = split_bf16_f64(reinterpret_cast<const double*>(SM), 2L * W * M * N, Wt_p[0], Wt_p[1],
-                             nplanes > 2 ? Wt_p[2] : nullptr, st)))
+    if ((rc = split_bf16_f64(reinterpret_cast<const double*>(SM), 2L * W * M * N, Ws_p[0], Ws_p[1],
+                             nplanes > 2 ? Ws_p[2] : nullptr, st)))
       return rc;
     UmmaEpilogue eg;
     eg.kind = UMMA_EPI_PLANAR_SPLIT;
@@ -510,7 +513,7 @@ struct Engine {
     eg.nmo = M;
     for (int q = 0; q < 3; ++q) eg.out[q] = Gs_p[q];
     eg.out_planes = nplanes;
-    return tc_gemm(Tb_p, 2L * N, 4L * N * N, Wt_p, M, 2L * M * N, 2 * N, W, nullptr, 0, 0, 1.f, p1_tile(), &eg);
+    return tc_gemm(Tb_p, 2L * N, 4L * N * N, Ws_p, M, 2L * M * N, 2 * N, W, nullptr, 0, 0, 1.f, p1_tile(), &eg);
   }
 
   // NOMSD::Overlap of the current walkers into ov; keeps their inverse overlap matrices in T
@@ -585,6 +588,7 @@ struct Engine {
     }
     tay_half = best;
     vb_rows = 2 * best_pad;
+    ldh = (M + 63) / 64 * 64;
     // vbias: 128-wide tiles over (2W, Nc), K = N*M split so that the work units fill whole waves
     // of SMs (K splits write partial sums, reduced in a fixed order)
     int sms = 148;
@@ -607,17 +611,18 @@ struct Engine {
   // tile width of the P1 products (M columns): little padding, and a tile width built for the planes
   int p1_tile() const { return M <= 128 ? 128 : (nplanes > 2 ? 160 : 208); }
 
-  // C = alpha * A B^T on split planes (A: rows x K, B: cols x K, both K-major)
+  // C = alpha * A B^T on split planes (A: rows x K, B: cols x K, both K-major; rows a_ld apart,
+  // K when 0)
   int tc_gemm(void* const* A, long a_rows, long a_bs, void* const* B, long b_rows, long b_bs, int K, int batch,
               float* C, long ldc, long sCb, float alpha, int bn = 0, const UmmaEpilogue* epi = nullptr,
-              int ksplit = 1, long sCk = 0) {
+              int ksplit = 1, long sCk = 0, long a_ld = 0) {
     UmmaGemmDesc d;
     d.M = int(a_rows); d.N = int(b_rows); d.K = K; d.batch = batch;
     for (int q = 0; q < 3; ++q) {
       d.A.p[q] = A[q];
       d.B.p[q] = B[q];
     }
-    d.A.rows = a_rows; d.A.ld = K; d.A.batch_stride = a_bs;
+    d.A.rows = a_rows; d.A.ld = a_ld ? a_ld : K; d.A.batch_stride = a_bs;
     d.B.rows = b_rows; d.B.ld = K; d.B.batch_stride = b_bs;
     d.C = C; d.ldc = ldc; d.sCb = sCb; d.alpha = alpha; d.nplanes = nplanes; d.bn = bn; d.err = gemm_err;
     d.ksplit = ksplit; d.sCk = sCk;
@@ -652,7 +657,7 @@ struct Engine {
     const long vcols = sym ? P : MM;
     if ((rc = tc_gemm(Xs_p, 2L * W, 0, Likn_p, vcols, 0, Nc, 1, Cv, vcols, 0, float(sdt)))) return rc;
     ph_end(SFQ_PH_VHS_GEMM);
-    if ((rc = mixed_build_vblk(Cv, W, M, sym, tay_half, vb_rows, Vb_p, st))) return rc;
+    if ((rc = mixed_build_v(Cv, W, M, sym, Vb_p, st))) return rc;
     ph_end(SFQ_PH_VHS);
     ph_begin(SFQ_PH_PROPAGATE);
     inv_cached = false;
@@ -660,31 +665,41 @@ struct Engine {
     // Taylor products' epilogues, the operand planes alternating between the two buffers; the
     // last one leaves the planes of S for SM = P1 S, written straight back to the walkers
     const long rows = 2L * W * N;  // (w, a, c) rows of the walker operand
-    if ((rc = mixed_walkers_to_wt(SM, W, M, N, Wt_p, st))) return rc;
+    if ((rc = mixed_walkers_to_wt(SM, W, M, N, ldh, Wt_p, st))) return rc;
     UmmaEpilogue e1;
     e1.kind = UMMA_EPI_STORE_SPLIT;
     for (int q = 0; q < 3; ++q) e1.out[q] = Wt2_p[q];
     e1.out_planes = nplanes;
-    if ((rc = tc_gemm(Wt_p, rows, 0, P1_p, M, 0, M, 1, Sacc, M, 0, 1.f, p1_tile(), &e1))) return rc;
+    e1.ldh = ldh;
+    if ((rc = tc_gemm(Wt_p, rows, 0, P1_p, M, 0, M, 1, Sacc, M, 0, 1.f, p1_tile(), &e1, 1, 0, ldh))) return rc;
     void** cur = Wt2_p;
     void** nxt = Wt_p;
+    const long L2h = 2L * ldh;  // walker-operand row: [re | pad | im | pad]
     for (int k = 1; k <= p.taylor_order; ++k) {
-      UmmaEpilogue et;
+      UmmaGemmDesc d;
+      d.M = N; d.N = int(vb_rows); d.K = int(L2h); d.batch = W;
+      for (int q = 0; q < 3; ++q) {
+        d.A.p[q] = cur[q];
+        d.B.p[q] = Vb_p[q];
+      }
+      d.A.rows = N; d.A.ld = L2h; d.A.batch_stride = long(N) * L2h;
+      d.B.rows = M2; d.B.ld = M; d.B.batch_stride = M2 * M;
+      d.cplx_half = tay_half; d.cplx_nmo = M; d.cplx_ldh = ldh;
+      d.nplanes = nplanes; d.bn = 2 * tay_half; d.err = gemm_err;
+      UmmaEpilogue& et = d.epi;
       et.kind = UMMA_EPI_TAYLOR;
-      et.S = Sacc; et.nmo = M; et.half = tay_half; et.inv_k = 1.f / float(k);
+      et.S = Sacc; et.nmo = M; et.ldh = ldh; et.half = tay_half; et.inv_k = 1.f / float(k);
       et.write = k < p.taylor_order ? 1 : 2;
       for (int q = 0; q < 3; ++q) et.out[q] = nxt[q];
       et.out_planes = nplanes;
-      if ((rc = tc_gemm(cur, N, long(N) * M2, Vb_p, vb_rows, vb_rows * M2, int(M2), W, nullptr, 0, 0, 1.f,
-                        2 * tay_half, &et)))
-        return rc;
+      if ((rc = umma_gemm(d, st))) return rc;
       std::swap(cur, nxt);
     }
     UmmaEpilogue ew;
     ew.kind = UMMA_EPI_TO_WALKERS;
     ew.SM = reinterpret_cast<double*>(SM);
     ew.nel = N;
-    if ((rc = tc_gemm(cur, rows, 0, P1_p, M, 0, M, 1, nullptr, 0, 0, 1.f, p1_tile(), &ew))) return rc;
+    if ((rc = tc_gemm(cur, rows, 0, P1_p, M, 0, M, 1, nullptr, 0, 0, 1.f, p1_tile(), &ew, 1, 0, ldh))) return rc;
     ph_end(SFQ_PH_PROPAGATE);
     ph_begin(SFQ_PH_OVERLAP);
     if ((rc = log_overlap(newov))) return rc;

@@ -10,12 +10,12 @@ int mixed_split_planar(const cplx* src, int W, long E, void* const* pl, cudaStre
 // out[w][e] = alpha * (sum_s C_s[w][e], sum_s C_s[W + w][e]), the KS partial sums C_s = C + s * sk
 int mixed_reduce_planar_to_cplx(const float* C, int KS, long sk, int W, long E, double alpha, cplx* out,
                                 cudaStream_t st);
-// Cv: (2W, M*M) planar, or (2W, M(M+1)/2) with packed (upper triangle of a symmetric vHS); the
-// blocks get `rows` rows per walker, grouped by `half` orbitals (see mixed_kernels.cu)
-int mixed_build_vblk(const float* Cv, int W, int M, bool packed, int half, long rows, void* const* pl,
-                     cudaStream_t st);
+// Cv: (2W, M*M) planar, or (2W, M(M+1)/2) with packed (upper triangle of a symmetric vHS) ->
+// split planes V[w][c][i][k] (Vr, Vi)
+int mixed_build_v(const float* Cv, int W, int M, bool packed, void* const* pl, cudaStream_t st);
 // Tinv (W, N, N) -> split planes of the block operand [[Tr, -Ti], [Ti, Tr]] (rows (c, a), columns (b, c'))
 int mixed_build_tblk(const cplx* Tinv, int W, int N, void* const* pl, cudaStream_t st);
-int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* const* pl, cudaStream_t st);
+// SM (W, M, N) -> walker-operand planes WT[w][a][c * ldh + i]
+int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, int ldh, void* const* pl, cudaStream_t st);
 
 }  // namespace sfq

@@ -2,12 +2,12 @@
 //
 // Working layouts (per walker w, orbitals i,k < M, electrons a < N, c = 0 real / 1 imaginary):
 //   planar rows      P[c*W + w][e]               (split operands of the vbias / vHS GEMMs)
-//   walker rows      WT[w][a][c][i]              (K = (c,i) contiguous: Taylor / P1 A operand)
-//   vHS blocks       VB[w][row(c,i)][(c',k)] = [[Vr, -Vi], [Vi, Vr]]   (Taylor B operand), its rows
-//                    grouped by `half` orbitals: row(c, i) = (i / half) 2 half + c half + i % half,
-//                    so that one Taylor output tile holds the re and im parts of the same orbitals
+//   walker rows      WT[w][a][c*ldh + i]         (K = (c,i), each half padded to ldh, a multiple
+//                                                 of 64, with zeros: Taylor / P1 A operand)
+//   vHS planes       V[w][c][i][k] = Vr / Vi     (Taylor B operand; the tensor-core product forms
+//                                                 [[Vr, -Vi], [Vi, Vr]] from them, negating Vi)
 // so that the complex products become real K-major GEMMs on the tensor cores:
-//   (V T)^T[a][(c,i)] = sum_(c',k) WT[a][(c',k)] VB[row(c,i)][(c',k)],
+//   (V T)^T[a][(c,i)] = sum_(c',k) WT[a][(c',k)] [[Vr, -Vi], [Vi, Vr]][(c,i)][(c',k)],
 //   (P1 W)^T[(a,c)][j] = sum_i WT[(a,c)][i] P1[j][i].
 #include <cuda_bf16.h>
 
@@ -86,25 +86,41 @@ __global__ void reduce_planar_to_cplx_kernel(const float* C, int KS, long sk, in
 }
 
 // planar vHS (rows c*W + w, columns i*M + k, or the packed upper triangle when packed) ->
-// VB[w] = [[Vr, -Vi], [Vi, Vr]] split
-__global__ void build_vblk_kernel(const float* Cv, int W, int M, int packed, int half, long rows, Planes P) {
+// V[w][c][i][k] split.  One 32 x 32 tile per block through shared memory: packed rows are read
+// along k and V is written along its rows; for the packed triangle a block reads the tile
+// i-block <= k-block once and writes it and its mirror.
+__global__ void build_v_kernel(const float* Cv, int W, int M, int packed, Planes P) {
+  __shared__ float tile[32][33];
+  const int wc = blockIdx.z;  // c * W + w
+  const int c = wc / W, w = wc - c * W;
+  const int ib = blockIdx.y, kb = blockIdx.x;
   const long MM = (long)M * M;
-  const long ld = packed ? (long)M * (M + 1) / 2 : MM;  // columns of Cv
-  const long total = (long)W * MM;
-  const long M2 = 2L * M;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const long w = t / MM, r = t % MM;
-    const long i = r / M, k = r % M;
-    const long col = packed ? (i <= k ? upper_index(i, k, M) : upper_index(k, i, M)) : r;
-    const float vr = Cv[w * ld + col];
-    const float vi = Cv[((long)W + w) * ld + col];
-    const long base = w * rows * M2;
-    const long r0 = (i / half) * 2 * half + i % half;  // row (0, i); row (1, i) is half further
-    const long r1 = r0 + half;
-    split_store(vr, P, base + r0 * M2 + k);         // (0,i),(0,k):  Vr
-    split_store(-vi, P, base + r0 * M2 + M + k);    // (0,i),(1,k): -Vi
-    split_store(vi, P, base + r1 * M2 + k);         // (1,i),(0,k):  Vi
-    split_store(vr, P, base + r1 * M2 + M + k);     // (1,i),(1,k):  Vr
+  const long ld = packed ? (long)M * (M + 1) / 2 : MM;
+  const float* src = Cv + (long)wc * ld;
+  const long vbase = ((long)w * 2 + c) * MM;
+  const int tx = threadIdx.x;
+  if (!packed) {
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int i = ib * 32 + r, k = kb * 32 + tx;
+      if (i < M && k < M) split_store(src[(long)i * M + k], P, vbase + (long)i * M + k);
+    }
+    return;
+  }
+  if (ib > kb) return;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = ib * 32 + r, k = kb * 32 + tx;
+    if (i < M && k < M && i <= k) tile[r][tx] = src[upper_index(i, k, M)];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = ib * 32 + r, k = kb * 32 + tx;
+    if (i < M && k < M) split_store(i <= k ? tile[r][tx] : tile[tx][r], P, vbase + (long)i * M + k);
+  }
+  if (ib < kb) {
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int k = kb * 32 + r, i = ib * 32 + tx;
+      if (k < M && i < M) split_store(tile[tx][r], P, vbase + (long)k * M + i);
+    }
   }
 }
 
@@ -123,7 +139,7 @@ __global__ void build_tblk_kernel(const cplx* Tinv, int W, int N, Planes P) {
 }
 
 // SM (W, M, N) complex fp64 -> WT[w][a][c][i] split, 32x32 tiles through shared memory
-__global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, Planes P) {
+__global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, int ldh, Planes P) {
   __shared__ cplx tile[32][33];
   const int w = blockIdx.z;
   const int i0 = blockIdx.y * 32, a0 = blockIdx.x * 32;
@@ -133,13 +149,13 @@ __global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, Planes P) {
     if (i < M && a < N) tile[r][threadIdx.x] = S[(long)i * N + a];
   }
   __syncthreads();
-  const long base = (long)w * N * 2 * M;
+  const long base = (long)w * N * 2 * ldh;
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int a = a0 + r, i = i0 + threadIdx.x;
     if (i < M && a < N) {
       const cplx z = tile[threadIdx.x][r];
-      split_store_d(z.x, P, base + ((long)a * 2 + 0) * M + i);
-      split_store_d(z.y, P, base + ((long)a * 2 + 1) * M + i);
+      split_store_d(z.x, P, base + ((long)a * 2 + 0) * ldh + i);
+      split_store_d(z.y, P, base + ((long)a * 2 + 1) * ldh + i);
     }
   }
 }
@@ -159,9 +175,11 @@ int mixed_reduce_planar_to_cplx(const float* C, int KS, long sk, int W, long E, 
   return SFQ_OK;
 }
 
-int mixed_build_vblk(const float* Cv, int W, int M, bool packed, int half, long rows, void* const* pl,
-                     cudaStream_t st) {
-  build_vblk_kernel<<<grid_for((long)W * M * M), 256, 0, st>>>(Cv, W, M, packed ? 1 : 0, half, rows, planes(pl));
+int mixed_build_v(const float* Cv, int W, int M, bool packed, void* const* pl, cudaStream_t st) {
+  const unsigned t = unsigned((M + 31) / 32);
+  if (2L * W > 65535) return record_error(SFQ_ERR_SHAPE, "build_v: too many walkers for one launch");
+  dim3 grid(t, t, unsigned(2 * W)), block(32, 8);
+  build_v_kernel<<<grid, block, 0, st>>>(Cv, W, M, packed ? 1 : 0, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
@@ -172,9 +190,9 @@ int mixed_build_tblk(const cplx* Tinv, int W, int N, void* const* pl, cudaStream
   return SFQ_OK;
 }
 
-int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, void* const* pl, cudaStream_t st) {
+int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, int ldh, void* const* pl, cudaStream_t st) {
   dim3 grid((N + 31) / 32, (M + 31) / 32, W), block(32, 8);
-  walkers_to_wt_kernel<<<grid, block, 0, st>>>(SM, M, N, planes(pl));
+  walkers_to_wt_kernel<<<grid, block, 0, st>>>(SM, M, N, ldh, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

@@ -20,6 +20,7 @@ struct KParams {
   int a_batched, b_batched;
   int MT, NT, KS;  // tiles along M, N; K splits
   int batch;
+  int cb_half, cb_nmo, cb_kth, cb_ldh;  // complex B (cb_half > 0): see UmmaGemmDesc
   long tiles;
   float* C;
   long ldc, sCb, sCk;  // sCk: elements between the partial outputs of the K splits
@@ -96,6 +97,9 @@ template <int BN>
 __host__ __device__ constexpr uint32_t instr_desc() {
   // kind::f16: D = F32, A = B = BF16, both K-major, N = BN, M = 128
   return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(BN >> 3) << 17) | (uint32_t(BM >> 4) << 24);
+}
+__host__ __device__ inline uint32_t instr_desc_n(uint32_t n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | (uint32_t(BM >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -223,8 +227,9 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
   const bool live = gm < p.M;
   const UmmaEpilogue& e = p.e;
   if (e.kind == UMMA_EPI_TAYLOR) {
-    const int h = e.half, nmo = e.nmo;
+    const int h = e.half, nmo = e.nmo, ldh = e.ldh ? e.ldh : e.nmo;
     const long srow = ((long)bz * p.M + gm) * (2L * nmo);
+    const long prow = ((long)bz * p.M + gm) * (2L * ldh);
 #pragma unroll 1
     for (int c = 0; c < h; c += 16) {
       float re[16], im[16];
@@ -249,12 +254,13 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
       }
       st16f(S0, s0, vec, valid);
       st16f(S1, s1, vec, valid);
+      const bool pvec = valid == 16 && (ldh % 8) == 0;
       if (e.write == 1) {
-        put_planes16(tr, e.out, e.out_planes, srow + i0, vec, valid);
-        put_planes16(ti, e.out, e.out_planes, srow + nmo + i0, vec, valid);
+        put_planes16(tr, e.out, e.out_planes, prow + i0, pvec, valid);
+        put_planes16(ti, e.out, e.out_planes, prow + ldh + i0, pvec, valid);
       } else if (e.write == 2) {
-        put_planes16(s0, e.out, e.out_planes, srow + i0, vec, valid);
-        put_planes16(s1, e.out, e.out_planes, srow + nmo + i0, vec, valid);
+        put_planes16(s0, e.out, e.out_planes, prow + i0, pvec, valid);
+        put_planes16(s1, e.out, e.out_planes, prow + ldh + i0, pvec, valid);
       }
       }
     }
@@ -318,8 +324,10 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
       for (int j = 0; j < 16; ++j) v[j] += p.beta * o[j];
     }
     st16f(crow + n0, v, vec4, valid);
-    if (e.kind == UMMA_EPI_STORE_SPLIT)
-      put_planes16(v, e.out, e.out_planes, rbase + n0, valid == 16 && ((rbase + n0) % 8) == 0, valid);
+    if (e.kind == UMMA_EPI_STORE_SPLIT) {
+      const long pidx = (long)ks * p.sCk + (long)bz * p.sCb + (long)gm * (e.ldh ? e.ldh : p.ldc) + n0;
+      put_planes16(v, e.out, e.out_planes, pidx, valid == 16 && (pidx % 8) == 0, valid);
+    }
   }
 }
 
@@ -386,11 +394,26 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
           }
           unsigned char* st = smem + s * L::STAGE;
           mbar_expect_tx(&full[s], stage_tx);
-          const int k0 = kt * BK;
+          if (p.cb_half) {
+            // K slice kt = (c', k0): A at c' * ldh + k0; B: the Vr and Vi rows of the tile's orbitals,
+            // [Vr; Vi] for c' = 0 and [Vi; Vr] for c' = 1 (each box half the tile)
+            const int cp = kt / p.cb_kth, k0 = (kt - cp * p.cb_kth) * BK;
+            const int i0 = nt * p.cb_half;
+            const int r1 = (cp ? p.cb_nmo : 0) + i0, r2 = (cp ? 0 : p.cb_nmo) + i0;
 #pragma unroll
-          for (int q = 0; q < NP; ++q) {
-            tma_load_3d(st + q * L::A_BYTES, &maps.a[q], &full[s], k0, m0, ab);
-            tma_load_3d(st + NP * L::A_BYTES + q * L::B_BYTES, &maps.b[q], &full[s], k0, n0, bb);
+            for (int q = 0; q < NP; ++q) {
+              unsigned char* bt = st + NP * L::A_BYTES + q * L::B_BYTES;
+              tma_load_3d(st + q * L::A_BYTES, &maps.a[q], &full[s], cp * p.cb_ldh + k0, m0, ab);
+              tma_load_3d(bt, &maps.b[q], &full[s], k0, r1, bb);
+              tma_load_3d(bt + p.cb_half * (BK * 2), &maps.b[q], &full[s], k0, r2, bb);
+            }
+          } else {
+            const int k0 = kt * BK;
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+              tma_load_3d(st + q * L::A_BYTES, &maps.a[q], &full[s], k0, m0, ab);
+              tma_load_3d(st + NP * L::A_BYTES + q * L::B_BYTES, &maps.b[q], &full[s], k0, n0, bb);
+            }
           }
         }
       }
@@ -432,12 +455,31 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
             ad[q] = smem_desc(st + q * L::A_BYTES);
             bd[q] = smem_desc(st + NP * L::A_BYTES + q * L::B_BYTES);
           }
+          if (p.cb_half) {
+            // two N = half products per slice: re half with Vr (c' = 0) or -Vi (c' = 1), im half with
+            // Vi or Vr, the second B box starting half * 128 bytes into the tile
+            const uint32_t h = uint32_t(p.cb_half);
+            const uint32_t id_h = instr_desc_n(h), id_hneg = id_h | (1u << 14);  // bit 14: negate B
+            const uint32_t id_re = (kt >= p.cb_kth) ? id_hneg : id_h;
+            const uint64_t boff = uint64_t(h * (BK * 2)) >> 4;
 #pragma unroll
-          for (int kk = 0; kk < BK / 16; ++kk) {
-            const uint64_t off = uint64_t(kk * 32) >> 4;  // 16 bf16 = 32 bytes along the swizzled row
+            for (int kk = 0; kk < BK / 16; ++kk) {
+              const uint64_t off = uint64_t(kk * 32) >> 4;
 #pragma unroll
-            for (int tt = 0; tt < n_terms(NP); ++tt)
-              umma_bf16(d_tmem, ad[term_a(tt)] + off, bd[term_b(tt)] + off, idesc, ((kt - kb) | kk | tt) ? 1u : 0u);
+              for (int tt = 0; tt < n_terms(NP); ++tt) {
+                const uint32_t acc = ((kt - kb) | kk | tt) ? 1u : 0u;
+                umma_bf16(d_tmem, ad[term_a(tt)] + off, bd[term_b(tt)] + off, id_re, acc);
+                umma_bf16(d_tmem + h, ad[term_a(tt)] + off, bd[term_b(tt)] + boff + off, id_h, acc);
+              }
+            }
+          } else {
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+              const uint64_t off = uint64_t(kk * 32) >> 4;  // 16 bf16 = 32 bytes along the swizzled row
+#pragma unroll
+              for (int tt = 0; tt < n_terms(NP); ++tt)
+                umma_bf16(d_tmem, ad[term_a(tt)] + off, bd[term_b(tt)] + off, idesc, ((kt - kb) | kk | tt) ? 1u : 0u);
+            }
           }
           umma_commit(&empty[s]);
         }
@@ -538,10 +580,19 @@ int launch(const UmmaGemmDesc& d, cudaStream_t st) {
   Maps maps;
   int rc;
   const long ab = d.A.batch_stride ? d.batch : 1, bb = d.B.batch_stride ? d.batch : 1;
+  const bool cb = d.cplx_half > 0;
+  if (cb && (d.cplx_half * 2 != BN || d.cplx_half % 16 || d.cplx_ldh % BK || d.cplx_ldh < d.cplx_nmo ||
+             d.K != 2 * d.cplx_ldh || d.B.rows != 2L * d.cplx_nmo))
+    return record_error(SFQ_ERR_ARG, "umma_gemm: complex B needs BN = 2 half, K = 2 ldh, B rows = 2 nmo");
   for (int q = 0; q < NP; ++q) {
     if (!d.A.p[q] || !d.B.p[q]) return record_error(SFQ_ERR_ARG, "umma_gemm: plane %d missing", q);
     if ((rc = make_map(&maps.a[q], d.A.p[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
-    if ((rc = make_map(&maps.b[q], d.B.p[q], d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, BN))) return rc;
+    if (cb) {
+      if ((rc = make_map(&maps.b[q], d.B.p[q], d.B.rows, d.cplx_nmo, d.B.ld, bb, d.B.batch_stride, d.cplx_half)))
+        return rc;
+    } else if ((rc = make_map(&maps.b[q], d.B.p[q], d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, BN))) {
+      return rc;
+    }
   }
   for (int q = NP; q < 3; ++q) {
     maps.a[q] = maps.a[0];
@@ -575,6 +626,11 @@ int launch(const UmmaGemmDesc& d, cudaStream_t st) {
     return record_error(SFQ_ERR_ARG, "umma_gemm: K splits write partial sums (plain store, beta = 0, sCk > 0)");
   kp.tiles = (long)kp.MT * kp.NT * d.batch * kp.KS;
   kp.batch = d.batch;
+  kp.cb_half = cb ? d.cplx_half : 0;
+  kp.cb_nmo = d.cplx_nmo;
+  kp.cb_ldh = d.cplx_ldh;
+  kp.cb_kth = cb ? d.cplx_ldh / BK : 0;
+  if (cb && kp.KS != 1) return record_error(SFQ_ERR_ARG, "umma_gemm: complex B takes no K split");
   kp.C = d.C; kp.ldc = d.ldc; kp.sCb = d.sCb; kp.sCk = d.sCk; kp.alpha = d.alpha; kp.beta = d.beta;
   kp.e = e;
   kp.err = d.err;

@@ -28,7 +28,7 @@
 //   TAYLOR       the tile's columns are [re | im] halves over `half` orbitals i (B rows ordered so);
 //                T = (i / k) C, i.e. T_re = -C_im / k, T_im = C_re / k; S += T; planes of T (the
 //                next term's A operand) or of the updated S (the final P1 product's A operand).
-//                S and the planes use the walker layout [b][row][c * nmo + i].
+//                S uses [b][row][c * nmo + i], the planes [b][row][c * ldh + i].
 //   TO_WALKERS   rows (w, a, c), columns j: SM[w][j][a].c = alpha acc (complex fp64 walkers)
 //   PLANAR_SPLIT rows (c, a) of batch b (c < 2, a < nel), columns n: the BF16 planes of
 //                alpha acc at row (c * batch + b) * nel + a, column n of an nmo-wide matrix (the
@@ -62,6 +62,7 @@ struct UmmaEpilogue {
   // TAYLOR
   float* S = nullptr;     // [batch][M rows][2 * nmo]
   int nmo = 0;            // orbitals per half
+  int ldh = 0;            // planes: [batch][M rows][2 * ldh], half c at c * ldh (0: ldh = nmo); STORE_SPLIT: row stride of the planes (0: ldc)
   int half = 0;           // orbitals per tile (BN = 2 * half, a multiple of 16)
   float inv_k = 0.f;      // 1 / k for T_{k+1} = (i / k) C
   int write = 0;          // 1: planes of T_{k+1}; 2: planes of the updated S; 0: none
@@ -80,6 +81,13 @@ struct UmmaGemmDesc {
   int bn = 0;             // tile width: 0 = automatic, else 32, 64, 128, 160, 208 or 256
   int ksplit = 1;         // K split into this many ranges, each writing its partial C at C + s * sCk
   long sCk = 0;
+  // Complex B (cplx_half > 0): B holds only Vr and Vi, rows (c, i) of 2 * cplx_nmo per batch, K = k
+  // (cplx_nmo); A's K is (c', k) with each half padded to cplx_ldh (a multiple of 64).  Output
+  // tile t has columns [re | im] over orbitals t * half .. + half, computed as
+  //   re += A_re Vr^T - A_im Vi^T,   im += A_re Vi^T + A_im Vr^T
+  // by two N = half MMAs per K slice (the -Vi through the instruction's negate-B bit): the
+  // product with [[Vr, -Vi], [Vi, Vr]] without storing that block.  BN = 2 * half.
+  int cplx_half = 0, cplx_nmo = 0, cplx_ldh = 0;
   UmmaEpilogue epi;
   int* err = nullptr;     // device flag, SFQ_ERR_TIMEOUT on an expired wait (may be null)
 };
