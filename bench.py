@@ -216,6 +216,31 @@ def run_reference(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+def step_errors(eng, eng64, W, spec, Eshift, step):
+    """One step of both engines from the FP64 engine's walkers with the same seeded fields: the
+    relative error (max |mixed - fp64| / max |fp64|) of each quantity of the step."""
+    import numpy as np
+
+    def rel(a, b):
+        a, b = np.asarray(a), np.asarray(b)
+        return float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300))
+
+    SM, pr = eng64.walkers()
+    eng.set_walkers(SM, pr)
+    eng.propagate(Eshift, step)
+    eng64.propagate(Eshift, step)
+    X = eng.fetch("X", (W, spec.Nc), np.complex128)
+    X64 = eng64.fetch("X", (W, spec.Nc), np.complex128)
+    S, p = eng.walkers()
+    S64, p64 = eng64.walkers()
+    E, E64 = eng.energy(), eng64.energy()
+    return {"fields_from_vbias": rel(X.imag, X64.imag), "propagated_walkers": rel(S, S64),
+            "log_overlap": rel(p["OVLP"], p64["OVLP"]), "weights": rel(p["WEIGHT"], p64["WEIGHT"]),
+            "local_energy_E1": rel(E[:, 0], E64[:, 0]), "local_energy_EXX": rel(E[:, 1], E64[:, 1]),
+            "local_energy_EJ": rel(E[:, 2], E64[:, 2]), "local_energy": rel(E.sum(1), E64.sum(1)),
+            "how": "one step of both engines from identical walkers and seeded fields; max |mixed - fp64| / max |fp64|"}
+
+
 def run_engine(args, cfg, spec, s, W, DT, prec, rank, local, profile_pass=True, e2e=True):
     """Warm up, time args.steps steps on the device, optionally a profile pass and the e2e pass.
 
@@ -340,8 +365,6 @@ def main():
     if dist:
         dist.barrier()
     eng, m = run_engine(args, cfg, spec, s, W, DT, prec, rank, local, e2e=not args.no_e2e)
-    eng.close()
-    del eng
 
     def max_over_ranks(x):
         if not dist:
@@ -364,6 +387,7 @@ def main():
     if prec != capi.PRECISION_FP64 and not args.no_compare:
         eng64, m64 = run_engine(args, cfg, spec, s, W, DT, capi.PRECISION_FP64, rank, local, profile_pass=False,
                                 e2e=False)
+        errors = step_errors(eng, eng64, W, spec, m64["energy"], args.warmup + args.steps + 1000)
         eng64.close()
         del eng64
         ms64 = max_over_ranks(m64["ms"])
@@ -372,7 +396,10 @@ def main():
                    "block_energy_mixed": m["energy"], "block_energy_fp64": m64["energy"],
                    "block_energy_delta_mHa": 1e3 * (m["energy"] - m64["energy"]),
                    "block_energy_delta_rel": (m["energy"] - m64["energy"]) / abs(m64["energy"]),
-                   "block": f"energy measured after the {args.warmup}+{args.steps} steps of each timed run"}
+                   "block": f"energy measured after the {args.warmup}+{args.steps} steps of each timed run",
+                   "step_errors": errors}
+    eng.close()
+    del eng
 
     # ---- roofline of the dominant kernel: the vHS product ---------------------------------
     ph = m["phases"]

@@ -255,6 +255,21 @@ typedef struct {
 int sfq_engine_run(sfq_engine_t e, const sfq_run_params_t* rp, double* Eshift, double* meas, int max_meas,
                    int* nmeas);
 
+/* The same loop as one device-resident block: Eshift, the step counter and the measurements live in
+ * device memory, every step's work (propagation, orthogonalization, population control, Eshift
+ * relaxation, measurements at their cadence) is enqueued with no host round trip, and the block is
+ * replayed from a CUDA graph captured the first time its schedule is seen.  At most 64
+ * measurements per block.  sfq_engine_block runs it and waits; the _async form enqueues it on the
+ * engine's stream, _query returns 1 once it has finished (0 while it runs, minus an SFQ_ERR_* code
+ * on a CUDA error), _result waits for it
+ * and returns its final Eshift and measurements (and its errors: SFQ_ERR_WEIGHT_COLLAPSE,
+ * SFQ_ERR_TIMEOUT).  No counterpart in the reference, whose loop returns to the host every step. */
+int sfq_engine_block(sfq_engine_t e, const sfq_run_params_t* rp, double* Eshift, double* meas, int max_meas,
+                     int* nmeas);
+int sfq_engine_block_async(sfq_engine_t e, const sfq_run_params_t* rp, double Eshift);
+int sfq_engine_block_query(sfq_engine_t e);
+int sfq_engine_block_result(sfq_engine_t e, double* Eshift, double* meas, int max_meas, int* nmeas);
+
 /* per-phase CUDA-event timing on the engine stream (AFQMCTimers analogue, AFQMCTimer.h:25-63) */
 enum sfq_phase {
   SFQ_PH_DENSITY = 0,     /* overlap matrix + LU + mixed density matrix */

@@ -265,6 +265,35 @@ class AfqmcEngine:
                                    ctypes.byref(nm)))
         return es.value, meas[:nm.value]
 
+    def run_block(self, steps, Eshift, ortho_interval=10, pop_interval=10, equilibration_steps=100,
+                  measure_interval=10, relax=0.0, step0=0):
+        """The same loop as run(), device-resident and replayed from a CUDA graph (sfq_engine_block)."""
+        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0)
+        es = ctypes.c_double(Eshift)
+        meas = np.zeros((64, 10), np.float64)
+        nm = ctypes.c_int()
+        check(lib().sfq_engine_block(self.h, ctypes.byref(rp), ctypes.byref(es), meas.ctypes.data, 64,
+                                     ctypes.byref(nm)))
+        return es.value, meas[:nm.value]
+
+    def block_async(self, steps, Eshift, ortho_interval=10, pop_interval=10, equilibration_steps=100,
+                    measure_interval=10, relax=0.0, step0=0):
+        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0)
+        check(lib().sfq_engine_block_async(self.h, ctypes.byref(rp), float(Eshift)))
+
+    def block_query(self):
+        rc = lib().sfq_engine_block_query(self.h)
+        if rc < 0:
+            check(-rc)
+        return rc == 1
+
+    def block_result(self):
+        es = ctypes.c_double()
+        meas = np.zeros((64, 10), np.float64)
+        nm = ctypes.c_int()
+        check(lib().sfq_engine_block_result(self.h, ctypes.byref(es), meas.ctypes.data, 64, ctypes.byref(nm)))
+        return es.value, meas[:nm.value]
+
     def profile(self, enable=True):
         check(lib().sfq_engine_profile(self.h, int(enable)))
 

@@ -94,6 +94,10 @@ _SIGS = {
     "sfq_engine_averages": ([_VP, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)], _I),
     "sfq_engine_measure": ([_VP, _VP], _I),
     "sfq_engine_run": ([_VP, ctypes.POINTER(RunParams), ctypes.POINTER(_D), _VP, _I, ctypes.POINTER(_I)], _I),
+    "sfq_engine_block": ([_VP, ctypes.POINTER(RunParams), ctypes.POINTER(_D), _VP, _I, ctypes.POINTER(_I)], _I),
+    "sfq_engine_block_async": ([_VP, ctypes.POINTER(RunParams), _D], _I),
+    "sfq_engine_block_query": ([_VP], _I),
+    "sfq_engine_block_result": ([_VP, ctypes.POINTER(_D), _VP, _I, ctypes.POINTER(_I)], _I),
     "sfq_engine_info": ([_VP, ctypes.POINTER(EngineInfo)], _I),
     "sfq_engine_profile": ([_VP, _I], _I),
     "sfq_engine_phase_times": ([_VP, _VP, _VP, _I], _I),

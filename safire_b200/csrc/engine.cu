@@ -6,6 +6,8 @@
 // AFQMCBasePropagator, for CLOSED walkers.
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "mixed.cuh"
@@ -75,6 +77,36 @@ __global__ void seed_pseudo_kernel(cplx* props, const cplx* E3, const cplx* ov, 
 
 size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// ---- the device-resident block driver's small kernels ------------------------------------
+// Eshift += relax (log(Re(sum w e^{dt eloc} / sum w)) / dt - Eshift), from averages_kernel's sums
+// (average_energy.hpp:37-48 and run_afqmc.cpp:91, on the device)
+__global__ void eshift_relax_kernel(const double* red, double dt, double relax, double* eshift) {
+  const double nr = red[0], ni = red[1], dr = red[2], di = red[3];
+  const double re = (nr * dr + ni * di) / (dr * dr + di * di);
+  const double pe = log(re) / dt;
+  *eshift += relax * (pe - *eshift);
+}
+// MeasurementOutput (Measurements.hpp:96-142): the 10 numbers of sfq_engine_measure
+__global__ void measure_kernel(const double* o, double* out) {
+  const double d = o[2] * o[2] + o[3] * o[3];
+  double r[6];
+  for (int q = 0; q < 3; ++q) {
+    const double ar = o[4 + 2 * q], ai = o[5 + 2 * q];
+    r[2 * q] = (ar * o[2] + ai * o[3]) / d;
+    r[2 * q + 1] = (ai * o[2] - ar * o[3]) / d;
+  }
+  out[0] = r[0] + r[2] + r[4];
+  out[1] = r[1] + r[3] + r[5];
+  for (int q = 0; q < 6; ++q) out[2 + q] = r[q];
+  out[8] = o[2];
+  out[9] = o[3];
+}
+__global__ void step_add_kernel(unsigned long long* step) { *step += 1ull; }
+__global__ void set_block_state_kernel(unsigned long long* step, unsigned long long s0, double* eshift, double e0) {
+  *step = s0;
+  *eshift = e0;
+}
+
 }  // namespace
 
 struct Engine {
@@ -142,6 +174,24 @@ struct Engine {
   int* gemm_err = nullptr;
   double* h_pinned = nullptr;  // pinned host staging for e2e calls
   size_t h_pinned_bytes = 0;
+  // device-resident block driver: Eshift, the step counter and the block's measurements in device
+  // memory; one CUDA graph per block schedule, replayed
+  static constexpr int kMeasCap = 64;
+  bool dev_mode = false;  // steps read the step and Eshift from d_step / d_eshift
+  double* d_eshift = nullptr;
+  unsigned long long* d_step = nullptr;
+  double* d_meas = nullptr;  // kMeasCap x 10
+  struct BlockGraph {
+    cudaGraphExec_t exec = nullptr;
+    bool inv_after = false;
+    const cplx* inv_ov_after = nullptr;
+    int nmeas = 0;
+  };
+  std::map<std::string, BlockGraph> graphs;
+  // results of the last block, staged in pinned memory: Eshift, status flags, measurements
+  double* blk_host = nullptr;  // 4 + 10 kMeasCap doubles
+  cudaEvent_t blk_done = nullptr;
+  int blk_nmeas = 0;
 
   // optional per-phase CUDA-event timing on the engine stream
   static constexpr int NPH = SFQ_NUM_PHASES;
@@ -256,6 +306,9 @@ struct Engine {
         {(void**)&pw.npairs, sizeof(int) * 4},
         {(void**)&pw.cum, d * W},
         {(void**)&pw.flag, sizeof(int) * 4},
+        {(void**)&d_eshift, sizeof(double) * 2},
+        {(void**)&d_step, sizeof(unsigned long long) * 2},
+        {(void**)&d_meas, sizeof(double) * 10 * kMeasCap},
     };
     if (mixed) {
       const size_t b = 2;  // bf16
@@ -541,7 +594,7 @@ struct Engine {
     ph_begin(SFQ_PH_FIELDS);
     FieldParams fp;                                                                   // 2. X
     fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
-    fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms;
+    fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms; fp.step_dev = dev_mode ? d_step : nullptr;
     if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
     ph_end(SFQ_PH_FIELDS);
     ph_begin(SFQ_PH_VHS);
@@ -567,6 +620,7 @@ struct Engine {
     up.lower_cutoff = p.lower_cutoff_scale; up.upper_cutoff = p.upper_cutoff_scale;
     up.max_weight = std::fmax(p.weight_bound_floor, p.weight_bound_fraction * target_pop());
     up.hybrid = 1; up.free_projection = p.free_projection; up.use_cp_constraint = 0;
+    up.Eshift_dev = dev_mode ? d_eshift : nullptr;
     if ((rc = walker_update(wprops(), newov, mf, hw, E3, up, stats, st))) return rc;
     ph_end(SFQ_PH_UPDATE);
     return SFQ_OK;
@@ -648,7 +702,7 @@ struct Engine {
     ph_begin(SFQ_PH_FIELDS);
     FieldParams fp;
     fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
-    fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms;
+    fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms; fp.step_dev = dev_mode ? d_step : nullptr;
     if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
     ph_end(SFQ_PH_FIELDS);
     ph_begin(SFQ_PH_VHS);
@@ -710,6 +764,7 @@ struct Engine {
     up.lower_cutoff = p.lower_cutoff_scale; up.upper_cutoff = p.upper_cutoff_scale;
     up.max_weight = std::fmax(p.weight_bound_floor, p.weight_bound_fraction * target_pop());
     up.hybrid = 1; up.free_projection = p.free_projection; up.use_cp_constraint = 0;
+    up.Eshift_dev = dev_mode ? d_eshift : nullptr;
     if ((rc = walker_update(wprops(), newov, mf, hw, E3, up, stats, st))) return rc;
     ph_end(SFQ_PH_UPDATE);
     return SFQ_OK;
@@ -730,8 +785,11 @@ struct Engine {
     int rc;
     ph_begin(SFQ_PH_POPCONTROL);
     inv_cached = false;
-    if ((rc = sfq::population_control(SM, (long)M * N, wprops(), W, 0.0, p.seed, call, 1, pw, st))) return rc;
+    if ((rc = sfq::population_control(SM, (long)M * N, wprops(), W, 0.0, p.seed, call, 1, pw, st,
+                                      dev_mode ? d_step : nullptr)))
+      return rc;
     ph_end(SFQ_PH_POPCONTROL);
+    if (dev_mode) return SFQ_OK;  // the collapse flag stays on the device until the block ends
     int flag = 0;
     SFQ_CUDA_TRY(cudaMemcpyAsync(&flag, pw.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
     if ((rc = sync_checked())) return rc;
@@ -757,6 +815,136 @@ struct Engine {
     SFQ_LAUNCHED();
     SFQ_CUDA_TRY(cudaMemcpyAsync(out10, red, sizeof(double) * 10, cudaMemcpyDeviceToHost, st));
     return sync_checked();
+  }
+
+  // run_afqmc's loop (run_afqmc.cpp:69-113) over steps step0 .. step0+steps-1 as a string of
+  // per-step codes: bit 0 orthogonalize, bit 1 population control, bit 2 Eshift relaxation,
+  // bit 3 measurement; the schedule a block graph is captured for
+  static std::string block_schedule(const sfq_run_params_t& rp) {
+    std::string key;
+    for (unsigned long long step = rp.step0; step < rp.step0 + (unsigned long long)rp.steps; ++step) {
+      int c = 0;
+      if (rp.walker_ortho_interval > 0 && step % rp.walker_ortho_interval == 0) c |= 1;
+      if (rp.population_control_interval > 0 && step % rp.population_control_interval == 0) c |= 2;
+      if ((long long)step < rp.equilibration_steps) c |= 4;
+      else if (rp.measure_interval > 0 && step % rp.measure_interval == 0) c |= 8;
+      key.push_back(char('a' + c));
+    }
+    return key;
+  }
+
+  // the block's work on the stream, in device mode (no host reads; captured into a graph)
+  int record_block(const std::string& sched, double relax, int* nmeas) {
+    int rc;
+    inv_cached = false;  // the block starts from whatever walkers it is given
+    int slot = 0;
+    for (char ch : sched) {
+      const int c = ch - 'a';
+      if ((rc = propagate(0.0, 0, nullptr))) return rc;  // step and Eshift come from the device
+      if ((c & 1) && (rc = orthogonalize())) return rc;
+      if ((c & 2) && (rc = population_control(0))) return rc;
+      if (c & 4) {
+        averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, nullptr, red);
+        SFQ_LAUNCHED();
+        eshift_relax_kernel<<<1, 1, 0, st>>>(red, p.dt, relax, d_eshift);
+        SFQ_LAUNCHED();
+      } else if (c & 8) {
+        if (slot >= kMeasCap) return record_error(SFQ_ERR_ARG, "block: more than %d measurements", kMeasCap);
+        if ((rc = energy_only())) return rc;
+        averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, E3, red);
+        SFQ_LAUNCHED();
+        measure_kernel<<<1, 1, 0, st>>>(red, d_meas + 10 * slot);
+        SFQ_LAUNCHED();
+        ++slot;
+      }
+      step_add_kernel<<<1, 1, 0, st>>>(d_step);
+      SFQ_LAUNCHED();
+    }
+    *nmeas = slot;
+    return SFQ_OK;
+  }
+
+  // enqueue one block: its graph (captured on first use of its schedule), then the copies of
+  // its results into pinned memory and an event; block_result() waits for them
+  int block_async(const sfq_run_params_t& rp, double Eshift) {
+    int rc;
+    if (rp.steps <= 0) return record_error(SFQ_ERR_ARG, "block: steps must be positive");
+    double relax = rp.Eshift_relaxation_factor;
+    if (!(relax > 0.0)) relax = rp.equilibration_steps > 1 ? 1.0 - std::exp(-10.0 / rp.equilibration_steps) : 1.0;
+    std::string key = block_schedule(rp);
+    char tail[64];
+    std::snprintf(tail, sizeof(tail), "|%.17g", relax);
+    key += tail;
+    auto it = graphs.find(key);
+    if (it == graphs.end()) {
+      BlockGraph bg;
+      const bool prof = profile;
+      profile = false;
+      dev_mode = true;
+      SFQ_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+      int nm = 0;
+      rc = record_block(key.substr(0, rp.steps), relax, &nm);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(st, &g);
+      dev_mode = false;
+      profile = prof;
+      if (rc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return rc ? rc : record_cuda(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+      }
+      const cudaError_t ie = cudaGraphInstantiate(&bg.exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) return record_cuda(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+      bg.inv_after = inv_cached;
+      bg.inv_ov_after = inv_ov;
+      bg.nmeas = nm;
+      it = graphs.emplace(key, bg).first;
+    }
+    if (!blk_host) {
+      SFQ_CUDA_TRY(cudaMallocHost(&blk_host, sizeof(double) * (4 + 10 * kMeasCap)));
+      SFQ_CUDA_TRY(cudaEventCreateWithFlags(&blk_done, cudaEventDisableTiming));
+    }
+    const BlockGraph& bg = it->second;
+    set_block_state_kernel<<<1, 1, 0, st>>>(d_step, rp.step0, d_eshift, Eshift);
+    SFQ_LAUNCHED();
+    SFQ_CUDA_TRY(cudaGraphLaunch(bg.exec, st));
+    inv_cached = bg.inv_after;
+    inv_ov = bg.inv_ov_after;
+    SFQ_CUDA_TRY(cudaMemcpyAsync(blk_host, d_eshift, sizeof(double), cudaMemcpyDeviceToHost, st));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(blk_host + 1, pw.flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (mixed) SFQ_CUDA_TRY(cudaMemcpyAsync(blk_host + 2, gemm_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (bg.nmeas)
+      SFQ_CUDA_TRY(cudaMemcpyAsync(blk_host + 4, d_meas, sizeof(double) * 10 * bg.nmeas, cudaMemcpyDeviceToHost, st));
+    SFQ_CUDA_TRY(cudaEventRecord(blk_done, st));
+    blk_nmeas = bg.nmeas;
+    return SFQ_OK;
+  }
+
+  int block_query() {
+    if (!blk_done) return 1;
+    const cudaError_t q = cudaEventQuery(blk_done);
+    if (q == cudaSuccess) return 1;
+    if (q == cudaErrorNotReady) return 0;
+    return -record_cuda(q, "cudaEventQuery", __FILE__, __LINE__);
+  }
+
+  int block_result(double* Eshift, double* meas, int max_meas, int* nmeas) {
+    if (!blk_done) return record_error(SFQ_ERR_ARG, "block: no block was run");
+    SFQ_CUDA_TRY(cudaEventSynchronize(blk_done));
+    int flag = 0, gflag = 0;
+    std::memcpy(&flag, blk_host + 1, sizeof(int));
+    if (mixed) std::memcpy(&gflag, blk_host + 2, sizeof(int));
+    if (gflag) {
+      cudaMemsetAsync(gemm_err, 0, sizeof(int), st);
+      return record_error(SFQ_ERR_TIMEOUT, "tensor-core product: a bounded wait expired in the block");
+    }
+    if (flag == SFQ_ERR_WEIGHT_COLLAPSE) return record_error(flag, "The total walker weight collapsed.");
+    if (flag) return record_error(flag, "population control: inconsistent copy plan");
+    if (Eshift) *Eshift = blk_host[0];
+    const int n = blk_nmeas < max_meas ? blk_nmeas : max_meas;
+    if (meas && n > 0) std::memcpy(meas, blk_host + 4, sizeof(double) * 10 * n);
+    if (nmeas) *nmeas = blk_nmeas;
+    return SFQ_OK;
   }
 
   // Synchronise the engine stream, then report a bounded wait of the tensor-core product that
@@ -846,6 +1034,10 @@ int sfq_engine_destroy(sfq_engine_t h) {
   Engine& e = h->e;
   if (e.st) cudaStreamSynchronize(e.st);
   e.release_events();
+  for (auto& kv : e.graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  if (e.blk_done) cudaEventDestroy(e.blk_done);
+  if (e.blk_host) cudaFreeHost(e.blk_host);
   if (e.arena) cudaFree(e.arena);
   if (e.Lp) cudaFree(e.Lp);
   if (e.Vp) cudaFree(e.Vp);
@@ -1017,6 +1209,29 @@ int sfq_engine_run(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, d
   }
   if (nmeas) *nmeas = nm;
   return e.sync_checked();
+}
+
+int sfq_engine_block(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, double* meas, int max_meas,
+                     int* nmeas) {
+  if (!h || !rp || !Eshift) return record_error(SFQ_ERR_ARG, "null pointer");
+  int rc;
+  if ((rc = h->e.block_async(*rp, *Eshift))) return rc;
+  return h->e.block_result(Eshift, meas, max_meas, nmeas);
+}
+
+int sfq_engine_block_async(sfq_engine_t h, const sfq_run_params_t* rp, double Eshift) {
+  if (!h || !rp) return record_error(SFQ_ERR_ARG, "null pointer");
+  return h->e.block_async(*rp, Eshift);
+}
+
+int sfq_engine_block_query(sfq_engine_t h) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.block_query();
+}
+
+int sfq_engine_block_result(sfq_engine_t h, double* Eshift, double* meas, int max_meas, int* nmeas) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.block_result(Eshift, meas, max_meas, nmeas);
 }
 
 int sfq_engine_profile(sfq_engine_t h, int enable) {

@@ -24,6 +24,7 @@ struct FieldParams {
   int free_projection = 0;
   unsigned long long seed = 0, step = 0;
   const double* uniforms = nullptr;  // optional injected (nwalk, nchol) buffer, else Philox
+  const unsigned long long* step_dev = nullptr;  // when set, the step is read from device memory
 };
 int field_uniforms(double* out, unsigned long long seed, unsigned long long step, int nwalk, int nchol,
                    cudaStream_t st);
@@ -36,6 +37,7 @@ struct UpdateParams {
   double lower_cutoff = 1.0, upper_cutoff = 10.0;
   double max_weight = 100.0;  // max(floor, fraction * target population)
   int hybrid = 1, free_projection = 0, use_cp_constraint = 0;
+  const double* Eshift_dev = nullptr;  // when set, Eshift is read from device memory
 };
 struct WalkerProps {  // columns of the walker set (SoA), each nwalk complex
   cplx *weight, *phase, *pseudo_eloc, *e1, *exx, *ej, *ovlp, *theta;
@@ -53,9 +55,10 @@ struct PopWork {
   double* cum;      // nwalk
   int* flag;        // 1: 0 ok, SFQ_ERR_WEIGHT_COLLAPSE
 };
+// call_dev: when set, the comb's call index is read from device memory
 int population_control(cplx* SM, long walker_elems, const WalkerProps& w, int nwalk, double r_uniform,
                        unsigned long long seed, unsigned long long call, int use_philox, const PopWork& pw,
-                       cudaStream_t st);
+                       cudaStream_t st, const unsigned long long* call_dev = nullptr);
 
 int comb_weights(const double* wts, int nwalk, double r, int* offspring, double* cum, int* flag, cudaStream_t st);
 

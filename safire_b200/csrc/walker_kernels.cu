@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(RT) assemble_x_kernel(cplx* X, const double* v
       u[0] = p.uniforms[(long)w * Nc + 2 * j];
       u[1] = (2 * j + 1 < Nc) ? p.uniforms[(long)w * Nc + 2 * j + 1] : 0.5;
     } else {
-      field_uniform_pair(p.seed, p.step, (uint32_t)w, (uint32_t)j, u[0], u[1]);
+      field_uniform_pair(p.seed, p.step_dev ? *p.step_dev : p.step, (uint32_t)w, (uint32_t)j, u[0], u[1]);
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(RT) assemble_x_kernel(cplx* X, const double* v
 // walker_update + bound_local_energy + bound_walker_weights (WalkerSetUpdate.hpp:46-218)
 __global__ void walker_update_kernel(WalkerProps wp, const cplx* new_ovlp, const cplx* mf, const cplx* hw,
                                      const cplx* E3, UpdateParams p, unsigned long long* stats) {
+  const double Eshift = p.Eshift_dev ? *p.Eshift_dev : p.Eshift;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.nwalk) return;
   const cplx old_ovlp = wp.ovlp[i];
@@ -110,8 +111,8 @@ __global__ void walker_update_kernel(WalkerProps wp, const cplx* new_ovlp, const
     eloc = old_eloc;
   } else {
     if (!p.free_projection) {
-      const double hi = p.Eshift + p.upper_cutoff * sqrt(2.0 / p.dt);
-      const double lo = p.Eshift - p.lower_cutoff * sqrt(2.0 / p.dt);
+      const double hi = Eshift + p.upper_cutoff * sqrt(2.0 / p.dt);
+      const double lo = Eshift - p.lower_cutoff * sqrt(2.0 / p.dt);
       if (stats) {
         atomicAdd(&stats[0], 1ull);
         if (eloc.x > hi) atomicAdd(&stats[1], 1ull);
@@ -120,7 +121,7 @@ __global__ void walker_update_kernel(WalkerProps wp, const cplx* new_ovlp, const
       eloc.x = fmin(fmax(eloc.x, lo), hi);
     }
     cplx eff = p.hybrid ? eloc : cscale(cadd(eloc, old_eloc), 0.5);
-    cplx z = mk(-p.dt * (eff.x - p.Eshift), -p.dt * eff.y);
+    cplx z = mk(-p.dt * (eff.x - Eshift), -p.dt * eff.y);
     cplx wf = cexp_(z);
     double aw = hypot(wf.x, wf.y);
     if (p.free_projection) weight = cmul(weight, cscale(wf, scale));
@@ -151,7 +152,8 @@ __global__ void walker_update_kernel(WalkerProps wp, const cplx* new_ovlp, const
 // sequential walk), and the copy plan is integer-only.
 constexpr int PT = 1024;
 __global__ void __launch_bounds__(PT) comb_kernel(WalkerProps wp, int nwalk, double r_in, unsigned long long seed,
-                                                  unsigned long long call, int use_philox, PopWork pw) {
+                                                  unsigned long long call, int use_philox, PopWork pw,
+                                                  const unsigned long long* call_dev) {
   __shared__ double s_total;
   __shared__ int s_last;
   __shared__ int s_ok;
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(PT) comb_kernel(WalkerProps wp, int nwalk, dou
     int last = nwalk - 1;
     while (last > 0 && !(hypot(wp.weight[last].x, wp.weight[last].y) > 0.0)) --last;
     s_last = last;
-    s_r = use_philox ? comb_uniform(seed, call) : r_in;
+    s_r = use_philox ? comb_uniform(seed, call_dev ? *call_dev : call) : r_in;
     *pw.flag = s_ok ? 0 : SFQ_ERR_WEIGHT_COLLAPSE;
   }
   __syncthreads();
@@ -418,9 +420,9 @@ int walker_update(const WalkerProps& w, const cplx* new_ovlp, const cplx* mf, co
 
 int population_control(cplx* SM, long walker_elems, const WalkerProps& w, int nwalk, double r_uniform,
                        unsigned long long seed, unsigned long long call, int use_philox, const PopWork& pw,
-                       cudaStream_t st) {
+                       cudaStream_t st, const unsigned long long* call_dev) {
   if (nwalk <= 0) return SFQ_OK;
-  comb_kernel<<<1, PT, 0, st>>>(w, nwalk, r_uniform, seed, call, use_philox, pw);
+  comb_kernel<<<1, PT, 0, st>>>(w, nwalk, r_uniform, seed, call, use_philox, pw, call_dev);
   SFQ_LAUNCHED();
   int gx = int((walker_elems + 255) / 256);
   if (gx > 8) gx = 8;
