@@ -269,6 +269,46 @@ int sfq_engine_block(sfq_engine_t e, const sfq_run_params_t* rp, double* Eshift,
 int sfq_engine_block_async(sfq_engine_t e, const sfq_run_params_t* rp, double Eshift);
 int sfq_engine_block_query(sfq_engine_t e);
 int sfq_engine_block_result(sfq_engine_t e, double* Eshift, double* meas, int max_meas, int* nmeas);
+/* bytes of device memory the engine holds (its arena and packed tensors) */
+int sfq_engine_footprint(sfq_engine_t e, size_t* bytes);
+
+/* ---- serving loop: continuous batching of propagation blocks over resident systems -----------
+ * Systems are registered with their inputs (kept on the host); their engines are built on the
+ * device when a request needs them and stay resident between blocks, under an HBM budget (the
+ * least recently used idle systems are evicted, their walkers saved on the host and restored
+ * when they are built again).  A request is one block (sfq_engine_block semantics; the server
+ * continues each system's step count and Eshift).  sfq_server_progress retires finished blocks and
+ * admits queued requests in arrival order as slots (max_inflight blocks on the GPU at once, one
+ * per system) and memory free up; blocks of different systems run concurrently on their own
+ * streams.  Times are seconds on sfq_server_clock.  No counterpart in the reference. */
+typedef struct sfq_server_s* sfq_server_t;
+typedef struct {
+  size_t hbm_budget; /* bytes the resident engines may hold */
+  int max_inflight;  /* blocks running at once */
+  int device;
+} sfq_server_params_t;
+typedef struct {
+  int status;        /* 1 queued, 2 running, 0 done, or an SFQ_ERR_* code */
+  int system;
+  double t_submit, t_start, t_finish;
+  double Eshift;     /* after the block */
+  int nmeas;
+  unsigned long long step0; /* the system's step index the block started at */
+} sfq_request_info_t;
+int sfq_server_create(sfq_server_t* out, const sfq_server_params_t* p);
+int sfq_server_destroy(sfq_server_t s);
+int sfq_server_add_system(sfq_server_t s, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
+                          const void* PsiT, int* id);
+/* build a system's engine now (e.g. before timing), evicting idle systems if the budget needs it */
+int sfq_server_warm(sfq_server_t s, int system);
+int sfq_server_submit(sfq_server_t s, int system, const sfq_run_params_t* rp, long long* request);
+/* retire finished blocks and admit queued ones; *completed (may be NULL) = requests finished by this call */
+int sfq_server_progress(sfq_server_t s, int* completed);
+/* state and results of a request (meas: up to max_meas measurements of 10 doubles) */
+int sfq_server_request(sfq_server_t s, long long request, sfq_request_info_t* info, double* meas, int max_meas);
+/* resident bytes, resident systems, running and queued requests (any may be NULL) */
+int sfq_server_stats(sfq_server_t s, size_t* used_bytes, int* resident, int* running, int* queued);
+double sfq_server_clock(sfq_server_t s);
 
 /* per-phase CUDA-event timing on the engine stream (AFQMCTimers analogue, AFQMCTimer.h:25-63) */
 enum sfq_phase {

@@ -54,6 +54,16 @@ class EngineInfo(ctypes.Structure):
                [("bound_stats", ctypes.c_ulonglong * 5), ("vhs_packed", ctypes.c_int)]
 
 
+class ServerParams(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_inflight", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("system", ctypes.c_int), ("t_submit", ctypes.c_double),
+                ("t_start", ctypes.c_double), ("t_finish", ctypes.c_double), ("Eshift", ctypes.c_double),
+                ("nmeas", ctypes.c_int), ("step0", ctypes.c_ulonglong)]
+
+
 _lib = None
 
 _VP, _I, _D, _SZ, _U64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t, ctypes.c_ulonglong
@@ -98,6 +108,16 @@ _SIGS = {
     "sfq_engine_block_async": ([_VP, ctypes.POINTER(RunParams), _D], _I),
     "sfq_engine_block_query": ([_VP], _I),
     "sfq_engine_block_result": ([_VP, ctypes.POINTER(_D), _VP, _I, ctypes.POINTER(_I)], _I),
+    "sfq_engine_footprint": ([_VP, ctypes.POINTER(_SZ)], _I),
+    "sfq_server_create": ([ctypes.POINTER(_VP), ctypes.POINTER(ServerParams)], _I),
+    "sfq_server_destroy": ([_VP], _I),
+    "sfq_server_add_system": ([_VP, ctypes.POINTER(EngineParams), _VP, _VP, _VP, ctypes.POINTER(_I)], _I),
+    "sfq_server_warm": ([_VP, _I], _I),
+    "sfq_server_submit": ([_VP, _I, ctypes.POINTER(RunParams), ctypes.POINTER(ctypes.c_longlong)], _I),
+    "sfq_server_progress": ([_VP, ctypes.POINTER(_I)], _I),
+    "sfq_server_request": ([_VP, ctypes.c_longlong, ctypes.POINTER(RequestInfo), _VP, _I], _I),
+    "sfq_server_stats": ([_VP, ctypes.POINTER(_SZ), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
+    "sfq_server_clock": ([_VP], _D),
     "sfq_engine_info": ([_VP, ctypes.POINTER(EngineInfo)], _I),
     "sfq_engine_profile": ([_VP, _I], _I),
     "sfq_engine_phase_times": ([_VP, _VP, _VP, _I], _I),

@@ -1234,6 +1234,13 @@ int sfq_engine_block_result(sfq_engine_t h, double* Eshift, double* meas, int ma
   return h->e.block_result(Eshift, meas, max_meas, nmeas);
 }
 
+int sfq_engine_footprint(sfq_engine_t h, size_t* bytes) {
+  if (!h || !bytes) return record_error(SFQ_ERR_ARG, "null pointer");
+  const Engine& e = h->e;
+  *bytes = e.arena_bytes + (e.Lp ? sizeof(double) * e.P * e.Nc : 0) + (e.Vp ? sizeof(cplx) * e.P * e.W : 0);
+  return SFQ_OK;
+}
+
 int sfq_engine_profile(sfq_engine_t h, int enable) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
   h->e.profile = enable != 0;

@@ -1,0 +1,186 @@
+"""The serving loop (sfq_server_*): resident systems, requests that are propagation blocks,
+continuous batching on the GPU; and its benchmark.
+
+    python -m safire_b200.serve            # 40 systems, Poisson arrivals, p50/p99 block latency
+
+The benchmark builds 40 synthetic systems (M uniform in [32, 400] on a multiple of 16, N = M/4,
+Nchol = 6M, 128 walkers each, mixed precision), measures batch-mode capacity (blocks of all systems
+submitted at once, repeatedly), then drives Poisson arrivals at fractions of that capacity, each
+request a block of 20 steps plus one local-energy measurement for a uniformly chosen system, and
+prints one JSON line with p50/p99 block latency and walker-steps/s per arrival rate.
+"""
+import argparse
+import ctypes
+import json
+import time
+
+import numpy as np
+
+from . import capi, synthetic
+from .capi import check, lib
+
+BLOCK = dict(ortho_interval=5, pop_interval=20, equilibration_steps=0, measure_interval=20)
+
+
+class Server:
+    def __init__(self, hbm_budget_gb=150.0, max_inflight=8, device=0):
+        p = capi.ServerParams(int(hbm_budget_gb * 1e9), int(max_inflight), int(device))
+        h = ctypes.c_void_p()
+        check(lib().sfq_server_create(ctypes.byref(h), ctypes.byref(p)))
+        self.h = h
+        self.walkers = {}
+
+    def close(self):
+        if self.h:
+            lib().sfq_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_system(self, system, nwalk, dt=0.005, seed=0, **params):
+        p = capi.default_params(nmo=system.M, nel=system.N, nchol=system.Nc, nwalk=nwalk, dt=dt,
+                                E0=float(system.E0), seed=seed)
+        for k, v in params.items():
+            setattr(p, k, v)
+        h = np.ascontiguousarray(system.hcore, dtype=np.float64)
+        L = np.ascontiguousarray(system.Likn, dtype=np.float64)
+        P = np.ascontiguousarray(system.PsiT, dtype=np.complex128)
+        sid = ctypes.c_int()
+        check(lib().sfq_server_add_system(self.h, ctypes.byref(p), h.ctypes.data, L.ctypes.data, P.ctypes.data,
+                                          ctypes.byref(sid)))
+        self.walkers[sid.value] = nwalk
+        return sid.value
+
+    def warm(self, sid):
+        check(lib().sfq_server_warm(self.h, int(sid)))
+
+    def submit(self, sid, steps=20, ortho_interval=5, pop_interval=20, equilibration_steps=0, measure_interval=20,
+               relax=0.0):
+        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, 0)
+        rid = ctypes.c_longlong()
+        check(lib().sfq_server_submit(self.h, int(sid), ctypes.byref(rp), ctypes.byref(rid)))
+        return rid.value
+
+    def progress(self):
+        n = ctypes.c_int()
+        check(lib().sfq_server_progress(self.h, ctypes.byref(n)))
+        return n.value
+
+    def request(self, rid):
+        inf = capi.RequestInfo()
+        meas = np.zeros((64, 10), np.float64)
+        check(lib().sfq_server_request(self.h, int(rid), ctypes.byref(inf), meas.ctypes.data, 64))
+        return {"status": inf.status, "system": inf.system, "t_submit": inf.t_submit, "t_start": inf.t_start,
+                "t_finish": inf.t_finish, "Eshift": inf.Eshift, "step0": inf.step0, "meas": meas[:inf.nmeas].copy()}
+
+    def stats(self):
+        b, r, run, q = ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().sfq_server_stats(self.h, ctypes.byref(b), ctypes.byref(r), ctypes.byref(run), ctypes.byref(q)))
+        return {"used_bytes": b.value, "resident": r.value, "running": run.value, "queued": q.value}
+
+    def clock(self):
+        return lib().sfq_server_clock(self.h)
+
+    def drain(self, rids, timeout=600.0, poll=0.0002):
+        """progress() until every request in rids has left the queue and the GPU."""
+        t0 = time.time()
+        left = set(rids)
+        while left:
+            self.progress()
+            left = {r for r in left if self.request(r)["status"] in (1, 2)}
+            if time.time() - t0 > timeout:
+                raise TimeoutError(f"{len(left)} requests still open")
+            if left:
+                time.sleep(poll)
+
+
+def _systems(count, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        M = int(rng.uniform(32, 400)) // 16 * 16
+        M = max(M, 32)
+        N = M // 4
+        spec = synthetic.SystemSpec(M=M, N=N, Nc=6 * M, decay=float(M), seed=100 + i)
+        out.append(synthetic.make_system(spec))
+    return out
+
+
+def _percentile(x, q):
+    return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--systems", type=int, default=40)
+    ap.add_argument("--walkers", type=int, default=128)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--inflight", type=int, default=8)
+    ap.add_argument("--rates", default="0.1,0.3,0.5,0.7,0.9,1.0,1.2")
+    ap.add_argument("--seconds", type=float, default=8.0, help="arrival window per rate")
+    ap.add_argument("--batch-rounds", type=int, default=3)
+    ap.add_argument("--dt", type=float, default=0.0005)
+    a = ap.parse_args()
+    systems = _systems(a.systems, 7)
+    srv = Server(a.budget_gb, a.inflight)
+    ids = [srv.add_system(s, a.walkers, dt=a.dt, seed=1000 + i, precision=capi.PRECISION_MIXED)
+           for i, s in enumerate(systems)]
+    t0 = time.time()
+    for sid in ids:
+        srv.warm(sid)
+    build_s = time.time() - t0
+    blk = dict(BLOCK, steps=a.steps)
+    # one warm block per system (graph capture), then batch mode: every system at once, repeatedly
+    srv.drain([srv.submit(sid, **blk) for sid in ids])
+    t0 = srv.clock()
+    for _ in range(a.batch_rounds):
+        srv.drain([srv.submit(sid, **blk) for sid in ids])
+    batch_s = srv.clock() - t0
+    nblocks = a.batch_rounds * len(ids)
+    ws_block = a.walkers * a.steps
+    batch_ws = nblocks * ws_block / batch_s
+    cap_rps = nblocks / batch_s  # blocks per second at capacity
+    rng = np.random.default_rng(11)
+    rows = []
+    for f in [float(x) for x in a.rates.split(",")]:
+        lam = f * cap_rps
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, size=int(lam * a.seconds * 1.5) + 4))
+        arrivals = arrivals[arrivals < a.seconds]
+        picks = rng.integers(0, len(ids), size=len(arrivals))
+        rids = []
+        base = srv.clock()
+        k = 0
+        while k < len(arrivals) or any(srv.request(r)["status"] in (1, 2) for r in rids[-64:]):
+            now = srv.clock() - base
+            while k < len(arrivals) and arrivals[k] <= now:
+                rids.append(srv.submit(ids[picks[k]], **blk))
+                k += 1
+            srv.progress()
+            time.sleep(0.0002)
+            if srv.clock() - base > a.seconds * 20:
+                break
+        srv.drain(rids)
+        info = [srv.request(r) for r in rids]
+        lat = [i["t_finish"] - i["t_submit"] for i in info if i["status"] == 0]
+        span = max(i["t_finish"] for i in info) - base if info else 1.0
+        rows.append({"load": f, "requests": len(info), "p50_ms": 1e3 * _percentile(lat, 50),
+                     "p99_ms": 1e3 * _percentile(lat, 99), "walker_steps_per_s": len(lat) * ws_block / span,
+                     "fraction_of_batch": len(lat) * ws_block / span / batch_ws,
+                     "failed": sum(1 for i in info if i["status"] != 0)})
+    st = srv.stats()
+    srv.close()
+    print(json.dumps({
+        "metric": "serving block latency", "unit": "ms", "systems": len(ids), "walkers_per_system": a.walkers,
+        "block": f"{a.steps} steps + 1 local-energy measurement", "precision": "mixed (2 BF16 planes)",
+        "dt": a.dt, "max_inflight": a.inflight, "hbm_budget_gb": a.budget_gb, "resident_bytes": st["used_bytes"],
+        "build_seconds": build_s, "batch_walker_steps_per_s": batch_ws, "batch_blocks_per_s": cap_rps,
+        "rates": rows, "data": "synthetic (M uniform in [32, 400] on multiples of 16, N = M/4, Nchol = 6M)"}))
+
+
+if __name__ == "__main__":
+    main()
