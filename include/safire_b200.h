@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 3 */
+int sfq_abi_version(void); /* 4 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -249,6 +249,8 @@ typedef struct {
   int measure_interval;             /* 10 */
   double Eshift_relaxation_factor;  /* <= 0 -> 1 - exp(-10/equilibration_steps) */
   unsigned long long step0;
+  int steer_eshift;  /* 1: Eshift keeps relaxing every step after equilibration too (measurements are taken
+                        at their cadence, then Eshift relaxes); 0: run_afqmc's fixed Eshift */
 } sfq_run_params_t;
 /* run_afqmc's step loop (run_afqmc.cpp:69-113). *Eshift in/out.  Measurements (10 doubles each, see
  * sfq_engine_measure) are written to meas (capacity max_meas); *nmeas receives the count. */
@@ -294,6 +296,7 @@ typedef struct {
   double Eshift;     /* after the block */
   int nmeas;
   unsigned long long step0; /* the system's step index the block started at */
+  char message[128];  /* the error of a failed request */
 } sfq_request_info_t;
 int sfq_server_create(sfq_server_t* out, const sfq_server_params_t* p);
 int sfq_server_destroy(sfq_server_t s);

@@ -256,8 +256,9 @@ class AfqmcEngine:
         return {k: complex(o[2 * i], o[2 * i + 1]) for i, k in enumerate(keys)}
 
     def run(self, steps, Eshift, ortho_interval=10, pop_interval=10, equilibration_steps=100, measure_interval=10,
-            relax=0.0, step0=0, max_meas=4096):
-        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0)
+            relax=0.0, step0=0, max_meas=4096, steer=False):
+        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0,
+                            int(steer))
         es = ctypes.c_double(Eshift)
         meas = np.zeros((max_meas, 10), np.float64)
         nm = ctypes.c_int()
@@ -266,9 +267,10 @@ class AfqmcEngine:
         return es.value, meas[:nm.value]
 
     def run_block(self, steps, Eshift, ortho_interval=10, pop_interval=10, equilibration_steps=100,
-                  measure_interval=10, relax=0.0, step0=0):
+                  measure_interval=10, relax=0.0, step0=0, steer=False):
         """The same loop as run(), device-resident and replayed from a CUDA graph (sfq_engine_block)."""
-        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0)
+        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0,
+                            int(steer))
         es = ctypes.c_double(Eshift)
         meas = np.zeros((64, 10), np.float64)
         nm = ctypes.c_int()
@@ -277,8 +279,9 @@ class AfqmcEngine:
         return es.value, meas[:nm.value]
 
     def block_async(self, steps, Eshift, ortho_interval=10, pop_interval=10, equilibration_steps=100,
-                    measure_interval=10, relax=0.0, step0=0):
-        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0)
+                    measure_interval=10, relax=0.0, step0=0, steer=False):
+        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0,
+                            int(steer))
         check(lib().sfq_engine_block_async(self.h, ctypes.byref(rp), float(Eshift)))
 
     def block_query(self):

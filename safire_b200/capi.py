@@ -43,7 +43,7 @@ class RunParams(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_int), ("walker_ortho_interval", ctypes.c_int),
                 ("population_control_interval", ctypes.c_int), ("equilibration_steps", ctypes.c_int),
                 ("measure_interval", ctypes.c_int), ("Eshift_relaxation_factor", ctypes.c_double),
-                ("step0", ctypes.c_ulonglong)]
+                ("step0", ctypes.c_ulonglong), ("steer_eshift", ctypes.c_int)]
 
 
 class EngineInfo(ctypes.Structure):
@@ -61,7 +61,7 @@ class ServerParams(ctypes.Structure):
 class RequestInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("system", ctypes.c_int), ("t_submit", ctypes.c_double),
                 ("t_start", ctypes.c_double), ("t_finish", ctypes.c_double), ("Eshift", ctypes.c_double),
-                ("nmeas", ctypes.c_int), ("step0", ctypes.c_ulonglong)]
+                ("nmeas", ctypes.c_int), ("step0", ctypes.c_ulonglong), ("message", ctypes.c_char * 128)]
 
 
 _lib = None

@@ -801,11 +801,42 @@ struct Engine {
   // NOMSD::Energy(wset, E, Ov): E3 and ovtmp
   int energy_only() {
     int rc;
+    if (mixed) return energy_mixed();
     ph_begin(SFQ_PH_ENERGY);
     if ((rc = density(ovtmp))) return rc;
     if ((rc = ops::energy(E3, G, haj, Lnak, !trial_real, p.E0, W, N, M, Nc, 1, 1, 1, Tchunk, tchunk_elems, exxn, kl,
                           st)))
       return rc;
+    ph_end(SFQ_PH_ENERGY);
+    return SFQ_OK;
+  }
+
+  // the same in the mixed mode: E1 from the FP64 G, the exchange tensor T[(c,w,b)][(n,a)] =
+  // sum_k G_c[w,b,k] Lnak[n,a,k] as split-BF16 tcgen05 products into FP32 (in chunks of Cholesky
+  // vectors), its contractions summed in FP64
+  int energy_mixed() {
+    int rc;
+    ph_begin(SFQ_PH_ENERGY);
+    if ((rc = density(ovtmp))) return rc;
+    const double scl = 2.0;
+    if ((rc = energy_e1(G, haj, E3, W, N, M, p.E0, scl, 1, st))) return rc;
+    if ((rc = mixed_split_planar(G, W, (long)N * M, Gs_p, st))) return rc;
+    // FP32 chunk of T in the FP64 chunk buffer: twice the elements
+    const long per_n = 2L * W * N * N;  // FP32 values of T per Cholesky vector
+    long nv_max = (2L * tchunk_elems) / per_n;
+    if (nv_max < 1) nv_max = 1;
+    if (nv_max > Nc) nv_max = Nc;
+    float* Tf = reinterpret_cast<float*>(Tchunk);
+    for (int n0 = 0; n0 < Nc; n0 += int(nv_max)) {
+      const int nv = (Nc - n0) < nv_max ? (Nc - n0) : int(nv_max);
+      void* Lc[3];
+      for (int q = 0; q < 3; ++q)
+        Lc[q] = Lnak_p[q] ? static_cast<void*>(static_cast<char*>(Lnak_p[q]) + 2L * n0 * N * M) : nullptr;
+      const long ldc = (long)nv * N;
+      if ((rc = tc_gemm(Gs_p, 2L * W * N, 0, Lc, ldc, 0, M, 1, Tf, ldc, 0, 1.f))) return rc;
+      if ((rc = energy_exx_reduce_f32(Tf, W, N, nv, n0, Nc, ldc, exxn, kl, st))) return rc;
+    }
+    if ((rc = energy_finish(exxn, kl, E3, W, Nc, scl, 1, 1, st))) return rc;
     ph_end(SFQ_PH_ENERGY);
     return SFQ_OK;
   }
@@ -826,8 +857,9 @@ struct Engine {
       int c = 0;
       if (rp.walker_ortho_interval > 0 && step % rp.walker_ortho_interval == 0) c |= 1;
       if (rp.population_control_interval > 0 && step % rp.population_control_interval == 0) c |= 2;
-      if ((long long)step < rp.equilibration_steps) c |= 4;
-      else if (rp.measure_interval > 0 && step % rp.measure_interval == 0) c |= 8;
+      const bool equil = (long long)step < rp.equilibration_steps;
+      if (equil || rp.steer_eshift) c |= 4;
+      if (!equil && rp.measure_interval > 0 && step % rp.measure_interval == 0) c |= 8;
       key.push_back(char('a' + c));
     }
     return key;
@@ -843,12 +875,7 @@ struct Engine {
       if ((rc = propagate(0.0, 0, nullptr))) return rc;  // step and Eshift come from the device
       if ((c & 1) && (rc = orthogonalize())) return rc;
       if ((c & 2) && (rc = population_control(0))) return rc;
-      if (c & 4) {
-        averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, nullptr, red);
-        SFQ_LAUNCHED();
-        eshift_relax_kernel<<<1, 1, 0, st>>>(red, p.dt, relax, d_eshift);
-        SFQ_LAUNCHED();
-      } else if (c & 8) {
+      if (c & 8) {
         if (slot >= kMeasCap) return record_error(SFQ_ERR_ARG, "block: more than %d measurements", kMeasCap);
         if ((rc = energy_only())) return rc;
         averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, E3, red);
@@ -856,6 +883,12 @@ struct Engine {
         measure_kernel<<<1, 1, 0, st>>>(red, d_meas + 10 * slot);
         SFQ_LAUNCHED();
         ++slot;
+      }
+      if (c & 4) {
+        averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, nullptr, red);
+        SFQ_LAUNCHED();
+        eshift_relax_kernel<<<1, 1, 0, st>>>(red, p.dt, relax, d_eshift);
+        SFQ_LAUNCHED();
       }
       step_add_kernel<<<1, 1, 0, st>>>(d_step);
       SFQ_LAUNCHED();
@@ -1194,14 +1227,14 @@ int sfq_engine_run(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, d
       if ((rc = e.orthogonalize())) return rc;
     if (rp->population_control_interval > 0 && step % rp->population_control_interval == 0)
       if ((rc = e.population_control(step))) return rc;
-    if ((long long)step >= rp->equilibration_steps) {
-      if (rp->measure_interval > 0 && step % rp->measure_interval == 0) {
-        double o[10];
-        if ((rc = sfq_engine_measure(h, o))) return rc;
-        if (meas && nm < max_meas) std::memcpy(meas + 10 * nm, o, sizeof(o));
-        ++nm;
-      }
-    } else {
+    const bool equil = (long long)step < rp->equilibration_steps;
+    if (!equil && rp->measure_interval > 0 && step % rp->measure_interval == 0) {
+      double o[10];
+      if ((rc = sfq_engine_measure(h, o))) return rc;
+      if (meas && nm < max_meas) std::memcpy(meas + 10 * nm, o, sizeof(o));
+      ++nm;
+    }
+    if (equil || rp->steer_eshift) {
       double pe;
       if ((rc = sfq_engine_averages(h, &pe, nullptr, nullptr))) return rc;
       *Eshift += relax * (pe - *Eshift);

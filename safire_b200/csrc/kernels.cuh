@@ -68,6 +68,9 @@ int energy_e1(const cplx* G, const cplx* haj, cplx* E3, int nwalk, int nel, int 
 // T chunk (nwalk, nel, nv, nel): exxn[w, n0+n] = sum_ab T[a,n,b]T[b,n,a]; kl[w, n0+n] = sum_a T[a,n,a]
 int energy_exx_reduce(const cplx* T, int nwalk, int nel, int nv, int n0, int nchol, cplx* exxn, cplx* kl,
                       cudaStream_t st);
+// the same from FP32 planar T of the split-BF16 product: rows (c*W + w)*nel + a, columns n*nel + b
+int energy_exx_reduce_f32(const float* C, int nwalk, int nel, int nv, int n0, int nchol, long ldc, cplx* exxn,
+                          cplx* kl, cudaStream_t st);
 // E3[:,1] += -0.5*scl*sum_n exxn; E3[:,2] += (CLOSED ? 2 : 0.5) * sum_n kl^2
 int energy_finish(const cplx* exxn, const cplx* kl, cplx* E3, int nwalk, int nchol, double scl, int addEXX,
                   int addEJ, cudaStream_t st);

@@ -9,7 +9,9 @@
 // would be exceeded, idle engines are evicted least recently used first, their walkers and
 // properties copied to the host and restored when the system is built again.
 #include <chrono>
+#include <cstring>
 #include <deque>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -41,6 +43,7 @@ struct Request {
   double Eshift = 0.0;
   std::vector<double> meas;
   int nmeas = 0;
+  std::string message;
 };
 
 }  // namespace
@@ -198,6 +201,7 @@ int sfq_server_progress(sfq_server_t s, int* completed) {
     int rc = st < 0 ? -st : sfq_engine_block_result(r.eng, &q.Eshift, q.meas.data(), 64, &q.nmeas);
     q.t_finish = s->now();
     q.status = rc;
+    if (rc) q.message = sfq_last_error();
     q.meas.resize(size_t(10) * (q.nmeas < 64 ? q.nmeas : 64));
     if (!rc) {
       r.Eshift = q.Eshift;
@@ -226,6 +230,7 @@ int sfq_server_progress(sfq_server_t s, int* completed) {
     }
     if (rc) {
       q.status = rc;
+      q.message = sfq_last_error();
       q.t_finish = s->now();
       ++done;
     } else {
@@ -253,6 +258,8 @@ int sfq_server_request(sfq_server_t s, long long request, sfq_request_info_t* in
   info->Eshift = q.Eshift;
   info->nmeas = q.nmeas;
   info->step0 = q.step0;
+  std::strncpy(info->message, q.message.c_str(), sizeof(info->message) - 1);
+  info->message[sizeof(info->message) - 1] = 0;
   if (meas && q.status == 0) {
     const int n = q.nmeas < max_meas ? q.nmeas : max_meas;
     for (int k = 0; k < 10 * n; ++k) meas[k] = q.meas[k];

@@ -303,6 +303,31 @@ __global__ void __launch_bounds__(RT) energy_exx_kernel(const cplx* T, int nel, 
   }
 }
 
+// the same from the split-BF16 product: T planar in FP32, T[a][n][b] = (C[w*nel + a][n*nel + b],
+// C[(W + w)*nel + a][n*nel + b]), sums in FP64
+__global__ void __launch_bounds__(RT) energy_exx_f32_kernel(const float* C, int W, int nel, int nv, int n0, int nchol,
+                                                            long ldc, cplx* exxn, cplx* kl) {
+  __shared__ cplx red[RT / 32];
+  const int n = blockIdx.x, w = blockIdx.y;
+  const float* Cr = C + (long)w * nel * ldc + (long)n * nel;
+  const float* Ci = Cr + (long)W * nel * ldc;
+  cplx acc = mk(0.0, 0.0), tr = mk(0.0, 0.0);
+  const int nn = nel * nel;
+  for (int e = threadIdx.x; e < nn; e += RT) {
+    const int a = e / nel, b = e % nel;
+    const cplx tab = mk(Cr[(long)a * ldc + b], Ci[(long)a * ldc + b]);
+    const cplx tba = mk(Cr[(long)b * ldc + a], Ci[(long)b * ldc + a]);
+    acc = cadd(acc, cmul(tab, tba));
+    if (a == b) tr = cadd(tr, tab);
+  }
+  cplx s = block_sum<RT>(acc, red);
+  cplx t = block_sum<RT>(tr, red);
+  if (threadIdx.x == 0) {
+    exxn[(long)w * nchol + n0 + n] = s;
+    kl[(long)w * nchol + n0 + n] = t;
+  }
+}
+
 __global__ void __launch_bounds__(RT) energy_finish_kernel(const cplx* exxn, const cplx* kl, cplx* E3, int nchol,
                                                            double scl, int addEXX, int addEJ) {
   __shared__ cplx red[RT / 32];
@@ -454,6 +479,15 @@ int energy_exx_reduce(const cplx* T, int nwalk, int nel, int nv, int n0, int nch
   if (nwalk <= 0 || nv <= 0) return SFQ_OK;
   dim3 grid(nv, nwalk);
   energy_exx_kernel<<<grid, RT, 0, st>>>(T, nel, nv, n0, nchol, exxn, kl);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int energy_exx_reduce_f32(const float* C, int nwalk, int nel, int nv, int n0, int nchol, long ldc, cplx* exxn,
+                          cplx* kl, cudaStream_t st) {
+  if (nwalk <= 0 || nv <= 0) return SFQ_OK;
+  dim3 grid(nv, nwalk);
+  energy_exx_f32_kernel<<<grid, RT, 0, st>>>(C, nwalk, nel, nv, n0, nchol, ldc, exxn, kl);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

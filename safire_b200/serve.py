@@ -19,7 +19,10 @@ import numpy as np
 from . import capi, synthetic
 from .capi import check, lib
 
-BLOCK = dict(ortho_interval=5, pop_interval=20, equilibration_steps=0, measure_interval=20)
+# a block: 20 steps (orthogonalization every 5, population control every 20) and one measurement;
+# Eshift is steered every step (the systems keep running block after block)
+BLOCK = dict(ortho_interval=5, pop_interval=20, equilibration_steps=0, measure_interval=20, steer=True,
+             relax=0.09516258196404048)  # 1 - exp(-10/100), run_afqmc's factor for 100 equilibration steps
 
 
 class Server:
@@ -59,8 +62,9 @@ class Server:
         check(lib().sfq_server_warm(self.h, int(sid)))
 
     def submit(self, sid, steps=20, ortho_interval=5, pop_interval=20, equilibration_steps=0, measure_interval=20,
-               relax=0.0):
-        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, 0)
+               relax=0.0, steer=False):
+        rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, 0,
+                            int(steer))
         rid = ctypes.c_longlong()
         check(lib().sfq_server_submit(self.h, int(sid), ctypes.byref(rp), ctypes.byref(rid)))
         return rid.value
@@ -75,7 +79,8 @@ class Server:
         meas = np.zeros((64, 10), np.float64)
         check(lib().sfq_server_request(self.h, int(rid), ctypes.byref(inf), meas.ctypes.data, 64))
         return {"status": inf.status, "system": inf.system, "t_submit": inf.t_submit, "t_start": inf.t_start,
-                "t_finish": inf.t_finish, "Eshift": inf.Eshift, "step0": inf.step0, "meas": meas[:inf.nmeas].copy()}
+                "t_finish": inf.t_finish, "Eshift": inf.Eshift, "step0": inf.step0, "meas": meas[:inf.nmeas].copy(),
+                "message": inf.message.decode(errors="replace")}
 
     def stats(self):
         b, r, run, q = ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
@@ -85,17 +90,17 @@ class Server:
     def clock(self):
         return lib().sfq_server_clock(self.h)
 
-    def drain(self, rids, timeout=600.0, poll=0.0002):
-        """progress() until every request in rids has left the queue and the GPU."""
+    def drain(self, rids=None, timeout=600.0, poll=0.0001):
+        """progress() until nothing is queued or running."""
         t0 = time.time()
-        left = set(rids)
-        while left:
+        while True:
             self.progress()
-            left = {r for r in left if self.request(r)["status"] in (1, 2)}
+            st = self.stats()
+            if st["running"] == 0 and st["queued"] == 0:
+                return
             if time.time() - t0 > timeout:
-                raise TimeoutError(f"{len(left)} requests still open")
-            if left:
-                time.sleep(poll)
+                raise TimeoutError(f"{st['running']} running, {st['queued']} queued")
+            time.sleep(poll)
 
 
 def _systems(count, seed):
@@ -108,6 +113,14 @@ def _systems(count, seed):
         spec = synthetic.SystemSpec(M=M, N=N, Nc=6 * M, decay=float(M), seed=100 + i)
         out.append(synthetic.make_system(spec))
     return out
+
+
+def system_dt(M):
+    """Timestep of a serving system: these synthetic systems' force bias grows as the walkers move
+    away from the (poor) trial, and the walkers of the larger ones die out after a few hundred steps
+    at dt = 5e-4 (in FP64 as in mixed precision); dt ~ 1/M keeps every system alive for the whole
+    run.  The work per step does not depend on dt."""
+    return float(min(max(1e-4 * 256.0 / M, 5e-5), 1e-3))
 
 
 def _percentile(x, q):
@@ -124,11 +137,10 @@ def main():
     ap.add_argument("--rates", default="0.1,0.3,0.5,0.7,0.9,1.0,1.2")
     ap.add_argument("--seconds", type=float, default=8.0, help="arrival window per rate")
     ap.add_argument("--batch-rounds", type=int, default=3)
-    ap.add_argument("--dt", type=float, default=0.0005)
     a = ap.parse_args()
     systems = _systems(a.systems, 7)
     srv = Server(a.budget_gb, a.inflight)
-    ids = [srv.add_system(s, a.walkers, dt=a.dt, seed=1000 + i, precision=capi.PRECISION_MIXED)
+    ids = [srv.add_system(s, a.walkers, dt=system_dt(s.M), seed=1000 + i, precision=capi.PRECISION_MIXED)
            for i, s in enumerate(systems)]
     t0 = time.time()
     for sid in ids:
@@ -155,29 +167,28 @@ def main():
         rids = []
         base = srv.clock()
         k = 0
-        while k < len(arrivals) or any(srv.request(r)["status"] in (1, 2) for r in rids[-64:]):
+        while k < len(arrivals):
             now = srv.clock() - base
             while k < len(arrivals) and arrivals[k] <= now:
                 rids.append(srv.submit(ids[picks[k]], **blk))
                 k += 1
             srv.progress()
-            time.sleep(0.0002)
-            if srv.clock() - base > a.seconds * 20:
-                break
-        srv.drain(rids)
+            time.sleep(0.0001)
+        srv.drain()
         info = [srv.request(r) for r in rids]
         lat = [i["t_finish"] - i["t_submit"] for i in info if i["status"] == 0]
         span = max(i["t_finish"] for i in info) - base if info else 1.0
         rows.append({"load": f, "requests": len(info), "p50_ms": 1e3 * _percentile(lat, 50),
                      "p99_ms": 1e3 * _percentile(lat, 99), "walker_steps_per_s": len(lat) * ws_block / span,
                      "fraction_of_batch": len(lat) * ws_block / span / batch_ws,
-                     "failed": sum(1 for i in info if i["status"] != 0)})
+                     "failed": sum(1 for i in info if i["status"] != 0),
+                     "errors": sorted({i["message"][:100] for i in info if i["status"] != 0})[:3]})
     st = srv.stats()
     srv.close()
     print(json.dumps({
         "metric": "serving block latency", "unit": "ms", "systems": len(ids), "walkers_per_system": a.walkers,
         "block": f"{a.steps} steps + 1 local-energy measurement", "precision": "mixed (2 BF16 planes)",
-        "dt": a.dt, "max_inflight": a.inflight, "hbm_budget_gb": a.budget_gb, "resident_bytes": st["used_bytes"],
+        "dt": "1e-4 * 256 / M, clipped to [5e-5, 1e-3]", "max_inflight": a.inflight, "hbm_budget_gb": a.budget_gb, "resident_bytes": st["used_bytes"],
         "build_seconds": build_s, "batch_walker_steps_per_s": batch_ws, "batch_blocks_per_s": cap_rps,
         "rates": rows, "data": "synthetic (M uniform in [32, 400] on multiples of 16, N = M/4, Nchol = 6M)"}))
 

@@ -93,3 +93,19 @@ def test_mixed_block_matches_host_loop():
     assert _rel(S2, S1) < 1e-12
     host.close()
     dev.close()
+
+
+def test_steered_block_matches_host_loop():
+    """steer_eshift: Eshift keeps relaxing after equilibration, measurements continue."""
+    host, dev = _pair(seed=13)
+    E0 = host.init()
+    dev.init()
+    sched = dict(ortho_interval=5, pop_interval=20, equilibration_steps=10, measure_interval=10, relax=0.1,
+                 steer=True)
+    Eh, mh = host.run(40, E0, **sched)
+    Ed, md = dev.run_block(40, E0, **sched)
+    assert len(md) == len(mh) == 3
+    assert abs(Ed - Eh) < 1e-10 * abs(Eh)
+    assert _rel(md, mh) < 1e-9
+    host.close()
+    dev.close()
