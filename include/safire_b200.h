@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 4 */
+int sfq_abi_version(void); /* 5 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -273,6 +273,51 @@ int sfq_engine_block_query(sfq_engine_t e);
 int sfq_engine_block_result(sfq_engine_t e, double* Eshift, double* meas, int max_meas, int* nmeas);
 /* bytes of device memory the engine holds (its arena and packed tensors) */
 int sfq_engine_footprint(sfq_engine_t e, size_t* bytes);
+
+/* ---- tile autotuner (mixed precision only) ----------------------------------------------------
+ * The tensor-core products are tiled in output tiles of 128 rows by a width the kernel is built
+ * for (64, 128, 160 with any plane count; 208, 256 with at most 2 planes).  sfq_engine_autotune
+ * times every built width of each product on the engine's own operands (the current walkers; only
+ * scratch buffers are written) and keeps the fastest: the G product, the force-bias product (its
+ * K split follows from its width), the vHS product, the Taylor terms (taylor_half orbitals per
+ * tile: 16, 32, 64, 80, or 128 with at most 2 planes) and the two P1 products.  The widths change
+ * how the output is tiled and, for the force bias, how many partial sums are reduced, so two
+ * engines given the same tiles (sfq_engine_set_tiles; 0 = the built-in choice) produce identical
+ * results.  Setting tiles drops the engine's captured block graphs.  us_builtin / us_tuned: median
+ * time of each product (G, force bias, vHS, one Taylor term, both P1 products) with the built-in
+ * and the chosen tiles (0 when a product was not timed).  No counterpart in the reference. */
+typedef struct {
+  int g_bn, vbias_bn, vhs_bn, taylor_half, p1_bn;
+  int vbias_ksplit; /* out */
+  double us_builtin[5];
+  double us_tuned[5];
+} sfq_tiles_t;
+int sfq_engine_autotune(sfq_engine_t e, int repeats, sfq_tiles_t* out);
+int sfq_engine_set_tiles(sfq_engine_t e, const sfq_tiles_t* tiles);
+int sfq_engine_tiles(sfq_engine_t e, sfq_tiles_t* tiles);
+
+/* ---- several systems advanced together --------------------------------------------------------
+ * A group of engines (systems of any M, N, Nchol, walker counts and precisions on one device)
+ * advances by one block of every member per call: the members' blocks (sfq_engine_block
+ * semantics, each with its own run parameters rps[i] and Eshift[i]) are captured, the first time a
+ * combination of schedules is seen, as the branches of ONE CUDA graph, so that one graph launch
+ * advances all systems and their kernels share the SMs.  sfq_group_set_lanes sets the schedule:
+ * `lanes` chains of members run side by side, the members of a chain one after another (members
+ * assigned longest first to the least loaded chain by their flops per block); 0 (the default)
+ * gives every member its own chain, 1 runs them all in turn.  Results per member: Eshift[i] (in/out),
+ * status[i] (0, SFQ_ERR_WEIGHT_COLLAPSE, SFQ_ERR_TIMEOUT), nmeas[i] measurements of 10 doubles at
+ * meas + 10 * max_meas * i.  The call returns the first member error.  The engines stay usable on
+ * their own between group blocks; one block of a group runs at a time (_async, then _result).
+ * No counterpart in the reference, which runs one system per process. */
+typedef struct sfq_group_s* sfq_group_t;
+int sfq_group_create(sfq_group_t* g, const sfq_engine_t* engines, int n);
+int sfq_group_destroy(sfq_group_t g);
+int sfq_group_block(sfq_group_t g, const sfq_run_params_t* rps, double* Eshift, int* status, double* meas,
+                    int max_meas, int* nmeas);
+int sfq_group_block_async(sfq_group_t g, const sfq_run_params_t* rps, const double* Eshift);
+int sfq_group_block_query(sfq_group_t g);
+int sfq_group_set_lanes(sfq_group_t g, int lanes);
+int sfq_group_block_result(sfq_group_t g, double* Eshift, int* status, double* meas, int max_meas, int* nmeas);
 
 /* ---- serving loop: continuous batching of propagation blocks over resident systems -----------
  * Systems are registered with their inputs (kept on the host); their engines are built on the

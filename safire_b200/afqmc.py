@@ -9,6 +9,7 @@
 torch is used only for device memory and streams; all arithmetic runs in the library.
 """
 import ctypes
+import time
 import math
 
 import numpy as np
@@ -297,6 +298,27 @@ class AfqmcEngine:
         check(lib().sfq_engine_block_result(self.h, ctypes.byref(es), meas.ctypes.data, 64, ctypes.byref(nm)))
         return es.value, meas[:nm.value]
 
+    def autotune(self, repeats=9):
+        """Time every built tile width of each mixed product on this engine and keep the fastest
+        (sfq_engine_autotune); returns the Tiles record (choice and per-product times)."""
+        t = capi.Tiles()
+        check(lib().sfq_engine_autotune(self.h, int(repeats), ctypes.byref(t)))
+        return t
+
+    def tiles(self):
+        t = capi.Tiles()
+        check(lib().sfq_engine_tiles(self.h, ctypes.byref(t)))
+        return t.choice()
+
+    def set_tiles(self, g_bn=0, vbias_bn=0, vhs_bn=0, taylor_half=0, p1_bn=0, **_):
+        t = capi.Tiles(g_bn, vbias_bn, vhs_bn, taylor_half, p1_bn)
+        check(lib().sfq_engine_set_tiles(self.h, ctypes.byref(t)))
+
+    def footprint(self):
+        b = ctypes.c_size_t()
+        check(lib().sfq_engine_footprint(self.h, ctypes.byref(b)))
+        return b.value
+
     def profile(self, enable=True):
         check(lib().sfq_engine_profile(self.h, int(enable)))
 
@@ -317,3 +339,93 @@ class AfqmcEngine:
         out = np.empty(shape, dtype)
         check(lib().sfq_memcpy(out.ctypes.data, getattr(inf, name), out.nbytes, 2, None))
         return out
+
+
+class EngineGroup:
+    """Several resident engines (systems of any sizes) advanced together: one block of every member
+    per call, all members' blocks captured as branches of one CUDA graph (sfq_group_*)."""
+
+    MAX_MEAS = 64
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        arr = (ctypes.c_void_p * len(self.engines))(*[e.h for e in self.engines])
+        h = ctypes.c_void_p()
+        check(lib().sfq_group_create(ctypes.byref(h), arr, len(self.engines)))
+        self.h = h
+        self.lanes = 0
+
+    def close(self):
+        if self.h:
+            lib().sfq_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _params(self, steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0,
+                steer):
+        n = len(self.engines)
+        step0 = np.broadcast_to(np.asarray(step0, np.uint64), (n,))
+        relax = np.broadcast_to(np.asarray(relax, np.float64), (n,))
+        rps = (capi.RunParams * n)()
+        for i in range(n):
+            rps[i] = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval,
+                                    float(relax[i]), int(step0[i]), int(steer))
+        return rps
+
+    def block_async(self, steps, Eshift, ortho_interval=10, pop_interval=10, equilibration_steps=100,
+                    measure_interval=10, relax=0.0, step0=0, steer=False):
+        rps = self._params(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0,
+                           steer)
+        es = np.ascontiguousarray(np.broadcast_to(np.asarray(Eshift, np.float64), (len(self.engines),)))
+        check(lib().sfq_group_block_async(self.h, rps, es.ctypes.data))
+
+    def block_query(self):
+        rc = lib().sfq_group_block_query(self.h)
+        if rc < 0:
+            check(-rc)
+        return rc == 1
+
+    def block_result(self, raise_errors=True):
+        """(Eshift per member, status per member, list of measurement arrays per member)"""
+        n = len(self.engines)
+        es = np.zeros(n, np.float64)
+        status = np.zeros(n, np.int32)
+        meas = np.zeros((n, self.MAX_MEAS, 10), np.float64)
+        nm = np.zeros(n, np.int32)
+        rc = lib().sfq_group_block_result(self.h, es.ctypes.data, status.ctypes.data, meas.ctypes.data,
+                                          self.MAX_MEAS, nm.ctypes.data)
+        if raise_errors:
+            check(rc)
+        return es, status, [meas[i, :nm[i]] for i in range(n)]
+
+    def run_block(self, steps, Eshift, **kw):
+        self.block_async(steps, Eshift, **kw)
+        return self.block_result()
+
+    def set_lanes(self, lanes):
+        """Schedule: `lanes` chains run side by side, members of a chain in turn (0: one per member)."""
+        check(lib().sfq_group_set_lanes(self.h, int(lanes)))
+        self.lanes = int(lanes)
+
+    def tune_lanes(self, steps, Eshift, step0=0, candidates=(1, 2, 3, 4, 6, 8, 0), **kw):
+        """Schedule autotuner: run real blocks with each lane count (one to capture its graph, one
+        timed) and keep the fastest.  Returns (Eshift, next step0, {lanes: seconds per block})."""
+        times = {}
+        es = Eshift
+        for L in candidates:
+            if L > len(self.engines):
+                continue
+            self.set_lanes(L)
+            es, _st, _m = self.run_block(steps, es, step0=step0, **kw)
+            step0 += steps
+            t0 = time.perf_counter()
+            es, _st, _m = self.run_block(steps, es, step0=step0, **kw)
+            times[L] = time.perf_counter() - t0
+            step0 += steps
+        self.set_lanes(min(times, key=times.get))
+        return es, step0, times

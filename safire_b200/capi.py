@@ -54,6 +54,17 @@ class EngineInfo(ctypes.Structure):
                [("bound_stats", ctypes.c_ulonglong * 5), ("vhs_packed", ctypes.c_int)]
 
 
+class Tiles(ctypes.Structure):
+    _fields_ = [("g_bn", ctypes.c_int), ("vbias_bn", ctypes.c_int), ("vhs_bn", ctypes.c_int),
+                ("taylor_half", ctypes.c_int), ("p1_bn", ctypes.c_int), ("vbias_ksplit", ctypes.c_int),
+                ("us_builtin", ctypes.c_double * 5), ("us_tuned", ctypes.c_double * 5)]
+
+    PRODUCTS = ("G", "vbias", "vHS", "taylor_term", "P1")
+
+    def choice(self):
+        return {k: getattr(self, k) for k in ("g_bn", "vbias_bn", "vhs_bn", "taylor_half", "p1_bn", "vbias_ksplit")}
+
+
 class ServerParams(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_inflight", ctypes.c_int), ("device", ctypes.c_int)]
 
@@ -109,6 +120,16 @@ _SIGS = {
     "sfq_engine_block_query": ([_VP], _I),
     "sfq_engine_block_result": ([_VP, ctypes.POINTER(_D), _VP, _I, ctypes.POINTER(_I)], _I),
     "sfq_engine_footprint": ([_VP, ctypes.POINTER(_SZ)], _I),
+    "sfq_engine_autotune": ([_VP, _I, ctypes.POINTER(Tiles)], _I),
+    "sfq_engine_set_tiles": ([_VP, ctypes.POINTER(Tiles)], _I),
+    "sfq_engine_tiles": ([_VP, ctypes.POINTER(Tiles)], _I),
+    "sfq_group_create": ([ctypes.POINTER(_VP), ctypes.POINTER(_VP), _I], _I),
+    "sfq_group_destroy": ([_VP], _I),
+    "sfq_group_block": ([_VP, ctypes.POINTER(RunParams), _VP, _VP, _VP, _I, _VP], _I),
+    "sfq_group_block_async": ([_VP, ctypes.POINTER(RunParams), _VP], _I),
+    "sfq_group_block_query": ([_VP], _I),
+    "sfq_group_set_lanes": ([_VP, _I], _I),
+    "sfq_group_block_result": ([_VP, _VP, _VP, _VP, _I, _VP], _I),
     "sfq_server_create": ([ctypes.POINTER(_VP), ctypes.POINTER(ServerParams)], _I),
     "sfq_server_destroy": ([_VP], _I),
     "sfq_server_add_system": ([_VP, ctypes.POINTER(EngineParams), _VP, _VP, _VP, ctypes.POINTER(_I)], _I),

@@ -4,6 +4,7 @@
 // It plays the role of the objects execute_simulation builds (src/AFQMC/execute.cpp:107-206):
 // Real3IndexFactorization (HamOps), NOMSD with ndet = 1 (trial), WalkerSet and
 // AFQMCBasePropagator, for CLOSED walkers.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -106,6 +107,23 @@ __global__ void set_block_state_kernel(unsigned long long* step, unsigned long l
   *step = s0;
   *eshift = e0;
 }
+// a group member's block state from the group's input row: {step0, Eshift bits}
+__global__ void load_block_state_kernel(const unsigned long long* in, unsigned long long* step, double* eshift) {
+  *step = in[0];
+  *eshift = __longlong_as_double((long long)in[1]);
+}
+// a group member's results into its output row: Eshift, population-control flag, product-timeout
+// flag, then nm measurements of 10
+__global__ void store_block_result_kernel(const double* eshift, const int* flag, const int* gerr, const double* meas,
+                                          int nm, double* out) {
+  if (threadIdx.x == 0) {
+    out[0] = *eshift;
+    out[1] = double(*flag);
+    out[2] = gerr ? double(*gerr) : 0.0;
+    out[3] = 0.0;
+  }
+  for (int i = threadIdx.x; i < 10 * nm; i += blockDim.x) out[4 + i] = meas[i];
+}
 
 }  // namespace
 
@@ -168,7 +186,11 @@ struct Engine {
   void* Ws_p[3] = {};   // the walkers read as reals, (W, M, 2N): the other operand of G
   float *Cvb = nullptr, *Cv = nullptr, *Sacc = nullptr;
   int vb_ks = 1;        // K splits of the vbias product (partial sums, reduced in a fixed order)
+  int vb_ks_max = 1;    // the most any vbias tile width can take (the partial-sum buffer's size)
+  // tile widths of the products (0: the built-in choice), set by autotune() or set_tiles()
+  int vb_bn = 128, vhs_bn = 0, p1_bn = 0, g_bn = 0;
   int tay_half = 0;     // orbitals per Taylor tile (tile width 2 * tay_half, re and im halves)
+  int tay_req = 0;      // a Taylor tile asked for (0: the least padding)
   long vb_rows = 0;     // output columns of a Taylor product: ceil(M / tay_half) * 2 * tay_half
   int ldh = 0;          // padded half of the walker operand rows (re, im): M rounded up to 64
   int* gemm_err = nullptr;
@@ -328,7 +350,7 @@ struct Engine {
         mx.push_back({&Ws_p[q], b * W * 2 * MN});
       }
       std::vector<Item> mx2 = {
-          {(void**)&Cvb, sizeof(float) * vb_ks * 2 * (size_t)W * Nc},
+          {(void**)&Cvb, sizeof(float) * vb_ks_max * 2 * (size_t)W * Nc},
           {(void**)&Cv, sizeof(float) * 2 * W * MM},
           {(void**)&Sacc, sizeof(float) * W * MN2},
           {(void**)&gemm_err, sizeof(int) * 4},
@@ -566,7 +588,7 @@ struct Engine {
     eg.nmo = M;
     for (int q = 0; q < 3; ++q) eg.out[q] = Gs_p[q];
     eg.out_planes = nplanes;
-    return tc_gemm(Tb_p, 2L * N, 4L * N * N, Ws_p, M, 2L * M * N, 2 * N, W, nullptr, 0, 0, 1.f, p1_tile(), &eg);
+    return tc_gemm(Tb_p, 2L * N, 4L * N * N, Ws_p, M, 2L * M * N, 2 * N, W, nullptr, 0, 0, 1.f, g_tile(), &eg);
   }
 
   // NOMSD::Overlap of the current walkers into ov; keeps their inverse overlap matrices in T
@@ -634,6 +656,7 @@ struct Engine {
     long best_pad = 1L << 40;
     for (int h : {16, 32, 64, 80, 128}) {
       if (h == 128 && nplanes > 2) continue;
+      if (tay_req && h != tay_req) continue;
       const long pad = (long)((M + h - 1) / h) * h;
       if (pad < best_pad || (pad == best_pad && h > best)) {
         best = h;
@@ -643,27 +666,35 @@ struct Engine {
     tay_half = best;
     vb_rows = 2 * best_pad;
     ldh = (M + 63) / 64 * 64;
-    // vbias: 128-wide tiles over (2W, Nc), K = N*M split so that the work units fill whole waves
-    // of SMs (K splits write partial sums, reduced in a fixed order)
+    vb_ks = plan_ks(vb_bn);
+    vb_ks_max = 1;
+    for (int bn : {32, 64, 128, 160, 208, 256}) vb_ks_max = std::max(vb_ks_max, plan_ks(bn));  // every width set_tiles takes
+  }
+
+  // vbias: tiles of width bn over (2W, Nc), K = N*M split so that the work units fill whole waves
+  // of SMs (K splits write partial sums, reduced in a fixed order)
+  int plan_ks(int bn) const {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device);
-    const long tiles = (long)((2 * W + 127) / 128) * ((Nc + 127) / 128);
+    const long tiles = (long)((2 * W + 127) / 128) * ((Nc + bn - 1) / bn);
     const long kt = ((long)N * M + 63) / 64;
     double best_eff = 0.0;
-    vb_ks = 1;
+    int best = 1;
     for (int ks = 1; ks <= 64 && ks * 8 <= kt; ++ks) {
       const double units = double(tiles) * ks;
       const double eff = units / (std::ceil(units / sms) * sms);
       if (eff > best_eff + 1e-9) {
         best_eff = eff;
-        vb_ks = ks;
+        best = ks;
       }
       if (eff > 0.999) break;
     }
+    return best;
   }
 
   // tile width of the P1 products (M columns): little padding, and a tile width built for the planes
-  int p1_tile() const { return M <= 128 ? 128 : (nplanes > 2 ? 160 : 208); }
+  int p1_tile() const { return p1_bn ? p1_bn : (M <= 128 ? 128 : (nplanes > 2 ? 160 : 208)); }
+  int g_tile() const { return g_bn ? g_bn : p1_tile(); }
 
   // C = alpha * A B^T on split planes (A: rows x K, B: cols x K, both K-major; rows a_ld apart,
   // K when 0)
@@ -684,6 +715,210 @@ struct Engine {
     return umma_gemm(d, st);
   }
 
+  // ---- autotuner: the tile widths of the mixed products, timed on the engine's own operands ----
+  // Product index: 0 G (density), 1 vbias (with its K-split reduction), 2 vHS, 3 one Taylor term,
+  // 4 the two P1 products.  The choice changes only how the output is tiled, and for vbias in how
+  // many K ranges the sum is split, so results of two engines with the same tiles are identical.
+  static constexpr int kTunedProducts = 5;
+
+  bool tile_built(int bn) const {
+    if (bn == 32 || bn == 64 || bn == 128 || bn == 160) return true;
+    return (bn == 208 || bn == 256) && nplanes <= 2;
+  }
+  bool half_ok(int h) const { return h == 16 || h == 32 || h == 64 || h == 80 || (h == 128 && nplanes <= 2); }
+
+  // set the tiles (0: the built-in choice); the captured block graphs are dropped
+  int set_tiles(int gbn, int vbbn, int vhsbn, int half, int p1bn) {
+    if (!mixed) return record_error(SFQ_ERR_UNSUPPORTED, "tiles: only the mixed-precision products are tiled");
+    for (int bn : {gbn, vbbn, vhsbn, p1bn})
+      if (bn && !tile_built(bn))
+        return record_error(SFQ_ERR_ARG, "tiles: width %d is not built for %d planes", bn, nplanes);
+    if (half && !half_ok(half)) return record_error(SFQ_ERR_ARG, "tiles: Taylor half %d not built", half);
+    g_bn = gbn;
+    vb_bn = vbbn ? vbbn : 128;
+    vhs_bn = vhsbn;
+    p1_bn = p1bn;
+    tay_req = half;
+    plan_mixed();
+    drop_graphs();
+    return SFQ_OK;
+  }
+
+  void drop_graphs() {
+    if (st) cudaStreamSynchronize(st);
+    for (auto& kv : graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+  }
+
+  void get_tiles(sfq_tiles_t* t) const {
+    t->g_bn = g_tile();
+    t->vbias_bn = vb_bn;
+    t->vhs_bn = vhs_bn ? vhs_bn : 128;
+    t->taylor_half = tay_half;
+    t->p1_bn = p1_tile();
+    t->vbias_ksplit = vb_ks;
+  }
+
+  // median over `reps` launches of f (us), after two warm-up launches, by events on the engine stream
+  template <class F>
+  int time_median(F&& f, int reps, double* us) {
+    int rc;
+    for (int i = 0; i < 2; ++i)
+      if ((rc = f())) return rc;
+    std::vector<cudaEvent_t> ev(reps + 1, nullptr);
+    cudaError_t ce = cudaSuccess;
+    for (auto& x : ev)
+      if (ce == cudaSuccess) ce = cudaEventCreate(&x);
+    rc = ce == cudaSuccess ? SFQ_OK : record_cuda(ce, "cudaEventCreate", __FILE__, __LINE__);
+    if (!rc) ce = cudaEventRecord(ev[0], st);
+    for (int i = 0; i < reps && !rc && ce == cudaSuccess; ++i) {
+      rc = f();
+      if (!rc) ce = cudaEventRecord(ev[i + 1], st);
+    }
+    if (!rc && ce == cudaSuccess) ce = cudaEventSynchronize(ev[reps]);
+    if (!rc && ce != cudaSuccess) rc = record_cuda(ce, "autotune events", __FILE__, __LINE__);
+    std::vector<double> t(reps, 0.0);
+    for (int i = 0; i < reps && !rc; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+      t[i] = 1e3 * ms;
+    }
+    for (auto& x : ev)
+      if (x) cudaEventDestroy(x);
+    if (rc) return rc;
+    std::sort(t.begin(), t.end());
+    *us = t[reps / 2];
+    return SFQ_OK;
+  }
+
+  // the products with tile width bn (Taylor: half) on the operands the scratch buffers hold
+  int tune_product(int which, int bn) {
+    int rc;
+    const long NM = (long)N * M, L2h = 2L * ldh, rows = 2L * W * N;
+    switch (which) {
+      case 0: {
+        UmmaEpilogue eg;
+        eg.kind = UMMA_EPI_PLANAR_SPLIT;
+        eg.nel = N;
+        eg.nmo = M;
+        for (int q = 0; q < 3; ++q) eg.out[q] = Gs_p[q];
+        eg.out_planes = nplanes;
+        return tc_gemm(Tb_p, 2L * N, 4L * N * N, Ws_p, M, 2L * M * N, 2 * N, W, nullptr, 0, 0, 1.f, bn, &eg);
+      }
+      case 1: {
+        const int ks = plan_ks(bn);
+        const long part = 2L * W * Nc;
+        if ((rc = tc_gemm(Gs_p, 2L * W, 0, Lnak_p, Nc, 0, int(NM), 1, Cvb, Nc, 0, 1.f, bn, nullptr, ks, part)))
+          return rc;
+        return mixed_reduce_planar_to_cplx(Cvb, ks, part, W, Nc, 2.0 * std::sqrt(p.dt), X, st);
+      }
+      case 2: {
+        const long vcols = sym ? P : (long)M * M;
+        return tc_gemm(Xs_p, 2L * W, 0, Likn_p, vcols, 0, Nc, 1, Cv, vcols, 0, float(std::sqrt(p.dt)), bn);
+      }
+      case 3: {
+        UmmaGemmDesc d;
+        d.M = N; d.N = int(2L * ((M + bn - 1) / bn) * bn); d.K = int(L2h); d.batch = W;
+        for (int q = 0; q < 3; ++q) {
+          d.A.p[q] = Wt2_p[q];
+          d.B.p[q] = Vb_p[q];
+        }
+        d.A.rows = N; d.A.ld = L2h; d.A.batch_stride = long(N) * L2h;
+        d.B.rows = 2L * M; d.B.ld = M; d.B.batch_stride = 2L * M * M;
+        d.cplx_half = bn; d.cplx_nmo = M; d.cplx_ldh = ldh;
+        d.nplanes = nplanes; d.bn = 2 * bn; d.err = gemm_err;
+        UmmaEpilogue& et = d.epi;
+        et.kind = UMMA_EPI_TAYLOR;
+        et.S = Sacc; et.nmo = M; et.ldh = ldh; et.half = bn; et.inv_k = 1.f;
+        et.write = 1;
+        for (int q = 0; q < 3; ++q) et.out[q] = Wt_p[q];
+        et.out_planes = nplanes;
+        return umma_gemm(d, st);
+      }
+      default: {
+        UmmaEpilogue e1;
+        e1.kind = UMMA_EPI_STORE_SPLIT;
+        for (int q = 0; q < 3; ++q) e1.out[q] = Wt2_p[q];
+        e1.out_planes = nplanes;
+        e1.ldh = ldh;
+        if ((rc = tc_gemm(Wt_p, rows, 0, P1_p, M, 0, M, 1, Sacc, M, 0, 1.f, bn, &e1, 1, 0, ldh))) return rc;
+        UmmaEpilogue ew;  // into the scratch walker buffer: the walkers are not touched
+        ew.kind = UMMA_EPI_TO_WALKERS;
+        ew.SM = reinterpret_cast<double*>(SM2);
+        ew.nel = N;
+        return tc_gemm(Wt2_p, rows, 0, P1_p, M, 0, M, 1, nullptr, 0, 0, 1.f, bn, &ew, 1, 0, ldh);
+      }
+    }
+  }
+
+  // time every built tile width of each product on this engine's sizes and keep the fastest; the
+  // walkers, their weights and overlaps are not modified (only scratch buffers are written)
+  int autotune(int reps, sfq_tiles_t* out) {
+    if (!mixed) return record_error(SFQ_ERR_UNSUPPORTED, "autotune: only the mixed-precision products are tiled");
+    const bool prof = profile;
+    profile = false;
+    const int rc = autotune_run(reps < 1 ? 9 : reps, out);
+    profile = prof;
+    return rc;
+  }
+
+  int autotune_run(int reps, sfq_tiles_t* out) {
+    int rc;
+    // real operands in the scratch buffers: G planes, force bias, its planes, vHS and V, walker planes
+    const double sdt = std::sqrt(p.dt);
+    const long part = 2L * W * Nc;
+    const long vcols = sym ? P : (long)M * M;
+    if ((rc = density_mixed())) return rc;
+    if ((rc = tc_gemm(Gs_p, 2L * W, 0, Lnak_p, Nc, 0, int((long)N * M), 1, Cvb, Nc, 0, 1.f, vb_bn, nullptr,
+                      vb_ks, part)))
+      return rc;
+    if ((rc = mixed_reduce_planar_to_cplx(Cvb, vb_ks, part, W, Nc, 2.0 * sdt, X, st))) return rc;
+    if ((rc = mixed_split_planar(X, W, Nc, Xs_p, st))) return rc;
+    if ((rc = tc_gemm(Xs_p, 2L * W, 0, Likn_p, vcols, 0, Nc, 1, Cv, vcols, 0, float(sdt), vhs_bn))) return rc;
+    if ((rc = mixed_build_v(Cv, W, M, sym, Vb_p, st))) return rc;
+    if ((rc = mixed_walkers_to_wt(SM, W, M, N, ldh, Wt_p, st))) return rc;
+    if ((rc = tune_product(4, p1_tile()))) return rc;
+    sfq_tiles_t cur{};
+    get_tiles(&cur);
+    const int current[kTunedProducts] = {cur.g_bn, cur.vbias_bn, cur.vhs_bn, cur.taylor_half, cur.p1_bn};
+    int chosen[kTunedProducts];
+    double t_cur[kTunedProducts] = {}, t_best[kTunedProducts] = {};
+    for (int which = 0; which < kTunedProducts; ++which) {
+      std::vector<int> cand;
+      if (which == 3) {
+        for (int h : {16, 32, 64, 80, 128})
+          if (half_ok(h)) cand.push_back(h);
+      } else {
+        for (int bn : {64, 128, 160, 208, 256})
+          if (tile_built(bn)) cand.push_back(bn);
+      }
+      chosen[which] = current[which];
+      if (which == 0 && !mixed_green()) continue;  // G comes from the FP64 density
+      double best = 1e300;
+      for (int bn : cand) {
+        double us = 0.0;
+        if ((rc = time_median([&] { return tune_product(which, bn); }, reps, &us))) return rc;
+        if (bn == current[which]) t_cur[which] = us;
+        if (us < best) {
+          best = us;
+          chosen[which] = bn;
+        }
+      }
+      t_best[which] = best;
+    }
+    if ((rc = sync_checked())) return rc;
+    if ((rc = set_tiles(chosen[0], chosen[1], chosen[2], chosen[3], chosen[4]))) return rc;
+    if (out) {
+      get_tiles(out);
+      for (int i = 0; i < kTunedProducts; ++i) {
+        out->us_builtin[i] = t_cur[i];
+        out->us_tuned[i] = t_best[i];
+      }
+    }
+    return SFQ_OK;
+  }
+
   // AFQMCBasePropagator::Propagate with the bulk products on the tensor cores (split BF16, FP32
   // accumulation); G, LU/log det, fields, overlaps and the walker update stay FP64.
   int propagate_mixed(double Eshift, unsigned long long step, const double* uniforms) {
@@ -695,7 +930,7 @@ struct Engine {
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
     const long part = 2L * W * Nc;  // one K split's partial sums
-    if ((rc = tc_gemm(Gs_p, 2L * W, 0, Lnak_p, Nc, 0, int(NM), 1, Cvb, Nc, 0, 1.f, 128, nullptr, vb_ks, part)))
+    if ((rc = tc_gemm(Gs_p, 2L * W, 0, Lnak_p, Nc, 0, int(NM), 1, Cvb, Nc, 0, 1.f, vb_bn, nullptr, vb_ks, part)))
       return rc;
     if ((rc = mixed_reduce_planar_to_cplx(Cvb, vb_ks, part, W, Nc, 2.0 * sdt, X, st))) return rc;
     ph_end(SFQ_PH_VBIAS);
@@ -709,7 +944,7 @@ struct Engine {
     if ((rc = mixed_split_planar(X, W, Nc, Xs_p, st))) return rc;
     ph_begin(SFQ_PH_VHS_GEMM);
     const long vcols = sym ? P : MM;
-    if ((rc = tc_gemm(Xs_p, 2L * W, 0, Likn_p, vcols, 0, Nc, 1, Cv, vcols, 0, float(sdt)))) return rc;
+    if ((rc = tc_gemm(Xs_p, 2L * W, 0, Likn_p, vcols, 0, Nc, 1, Cv, vcols, 0, float(sdt), vhs_bn))) return rc;
     ph_end(SFQ_PH_VHS_GEMM);
     if ((rc = mixed_build_v(Cv, W, M, sym, Vb_p, st))) return rc;
     ph_end(SFQ_PH_VHS);
@@ -897,17 +1132,53 @@ struct Engine {
     return SFQ_OK;
   }
 
+  // run_afqmc's Eshift relaxation factor (run_afqmc.cpp:58-60) unless one is given
+  static double block_relax(const sfq_run_params_t& rp) {
+    double relax = rp.Eshift_relaxation_factor;
+    if (!(relax > 0.0)) relax = rp.equilibration_steps > 1 ? 1.0 - std::exp(-10.0 / rp.equilibration_steps) : 1.0;
+    return relax;
+  }
+  static std::string block_key(const sfq_run_params_t& rp) {
+    char tail[64];
+    std::snprintf(tail, sizeof(tail), "|%.17g", block_relax(rp));
+    return block_schedule(rp) + tail;
+  }
+
+  // relative cost of one step, for balancing group lanes: the algorithmic flops of the products,
+  // weighted by how much slower the FP64 path runs them
+  double step_cost() const {
+    const double f = double(W) * (8.0 * N * M * Nc + 4.0 * M * double(M) * Nc + 64.0 * M * double(M) * N);
+    return mixed ? f : 6.0 * f;
+  }
+
+  // one member's part of a group block, recorded on the engine stream inside the group's capture:
+  // the step counter and Eshift from the group's input row, the block, then the results into the
+  // group's output row (4 + 10 kMeasCap doubles)
+  int record_group_part(const sfq_run_params_t& rp, const unsigned long long* in, double* out, int* nmeas) {
+    int rc;
+    const bool prof = profile;
+    profile = false;
+    dev_mode = true;
+    load_block_state_kernel<<<1, 1, 0, st>>>(in, d_step, d_eshift);
+    SFQ_LAUNCHED();
+    rc = record_block(block_schedule(rp), block_relax(rp), nmeas);
+    if (!rc) {
+      store_block_result_kernel<<<1, 128, 0, st>>>(d_eshift, pw.flag, mixed ? gemm_err : nullptr, d_meas, *nmeas,
+                                                   out);
+      SFQ_LAUNCHED();
+    }
+    dev_mode = false;
+    profile = prof;
+    return rc;
+  }
+
   // enqueue one block: its graph (captured on first use of its schedule), then the copies of
   // its results into pinned memory and an event; block_result() waits for them
   int block_async(const sfq_run_params_t& rp, double Eshift) {
     int rc;
     if (rp.steps <= 0) return record_error(SFQ_ERR_ARG, "block: steps must be positive");
-    double relax = rp.Eshift_relaxation_factor;
-    if (!(relax > 0.0)) relax = rp.equilibration_steps > 1 ? 1.0 - std::exp(-10.0 / rp.equilibration_steps) : 1.0;
-    std::string key = block_schedule(rp);
-    char tail[64];
-    std::snprintf(tail, sizeof(tail), "|%.17g", relax);
-    key += tail;
+    const double relax = block_relax(rp);
+    const std::string key = block_key(rp);
     auto it = graphs.find(key);
     if (it == graphs.end()) {
       BlockGraph bg;
@@ -995,10 +1266,218 @@ struct Engine {
   }
 };
 
+// ---- several systems advanced together ---------------------------------------------------------
+// One block of every member as ONE CUDA graph: the members' block recordings (each on its own
+// engine stream) form `lanes` branches forked from and joined back to the group stream; within a
+// lane the members run one after another, the lanes side by side on the SMs.  Members go to lanes
+// longest first, each to the lane with the least work so far (by step_cost x steps).  Per launch
+// the group copies each member's {step0, Eshift} to the device once and reads all results back
+// in one copy.
+struct Group {
+  static constexpr int kOut = 4 + 10 * Engine::kMeasCap;  // doubles per member's output row
+  std::vector<Engine*> es;
+  cudaStream_t gst = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_done = nullptr;
+  std::vector<cudaEvent_t> ev_join, ev_pre;
+  unsigned long long* d_in = nullptr;
+  double* d_out = nullptr;
+  unsigned long long* h_in = nullptr;
+  double* h_out = nullptr;
+  struct Captured {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<char> inv_after;
+    std::vector<const cplx*> inv_ov_after;
+    std::vector<int> nmeas;
+  };
+  std::map<std::string, Captured> graphs;
+  const Captured* pending = nullptr;
+  int lanes = 0;  // 0: one lane per member
+
+  // lane of each member, and the members of each lane in order
+  std::vector<std::vector<int>> plan_lanes(const sfq_run_params_t* rps) const {
+    const int n = int(es.size());
+    const int L = (lanes <= 0 || lanes > n) ? n : lanes;
+    std::vector<int> order(n);
+    std::vector<double> cost(n);
+    for (int i = 0; i < n; ++i) {
+      order[i] = i;
+      cost[i] = es[i]->step_cost() * rps[i].steps;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<std::vector<int>> out(L);
+    std::vector<double> load(L, 0.0);
+    for (int i : order) {
+      int best = 0;
+      for (int l = 1; l < L; ++l)
+        if (load[l] < load[best]) best = l;
+      out[best].push_back(i);
+      load[best] += cost[i];
+    }
+    return out;
+  }
+
+  int init(const std::vector<Engine*>& members) {
+    es = members;
+    const size_t n = es.size();
+    SFQ_CUDA_TRY(cudaSetDevice(es[0]->p.device));
+    SFQ_CUDA_TRY(cudaStreamCreateWithFlags(&gst, cudaStreamNonBlocking));
+    SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+    ev_join.assign(n, nullptr);
+    ev_pre.assign(n, nullptr);
+    for (size_t i = 0; i < n; ++i) {
+      SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_join[i], cudaEventDisableTiming));
+      SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_pre[i], cudaEventDisableTiming));
+    }
+    SFQ_CUDA_TRY(cudaMalloc(&d_in, sizeof(unsigned long long) * 2 * n));
+    SFQ_CUDA_TRY(cudaMalloc(&d_out, sizeof(double) * kOut * n));
+    SFQ_CUDA_TRY(cudaMallocHost(&h_in, sizeof(unsigned long long) * 2 * n));
+    SFQ_CUDA_TRY(cudaMallocHost(&h_out, sizeof(double) * kOut * n));
+    return SFQ_OK;
+  }
+
+  void release() {
+    if (gst) cudaStreamSynchronize(gst);
+    for (auto& kv : graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+    for (auto* v : {&ev_join, &ev_pre})
+      for (auto& x : *v)
+        if (x) cudaEventDestroy(x);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_done) cudaEventDestroy(ev_done);
+    if (d_in) cudaFree(d_in);
+    if (d_out) cudaFree(d_out);
+    if (h_in) cudaFreeHost(h_in);
+    if (h_out) cudaFreeHost(h_out);
+    if (gst) cudaStreamDestroy(gst);
+  }
+
+  // capture the members' blocks as the lanes of one graph
+  int capture(const sfq_run_params_t* rps, Captured* c) {
+    const size_t n = es.size();
+    c->nmeas.assign(n, 0);
+    c->inv_after.assign(n, 0);
+    c->inv_ov_after.assign(n, nullptr);
+    const std::vector<std::vector<int>> plan = plan_lanes(rps);
+    SFQ_CUDA_TRY(cudaStreamBeginCapture(gst, cudaStreamCaptureModeRelaxed));
+    int rc = SFQ_OK;
+    cudaError_t ce = cudaEventRecord(ev_fork, gst);
+    for (const auto& lane : plan) {
+      cudaEvent_t after = ev_fork;  // a member starts after the fork or after its lane predecessor
+      for (int i : lane) {
+        Engine& e = *es[i];
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e.st, after, 0);
+        if (ce != cudaSuccess) break;
+        if (!rc) rc = e.record_group_part(rps[i], d_in + 2 * i, d_out + (size_t)kOut * i, &c->nmeas[i]);
+        c->inv_after[i] = e.inv_cached ? 1 : 0;
+        c->inv_ov_after[i] = e.inv_ov;
+        ce = cudaEventRecord(ev_join[i], e.st);  // close every forked branch, also after an error
+        after = ev_join[i];
+      }
+      if (ce != cudaSuccess) break;
+      ce = cudaStreamWaitEvent(gst, after, 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(gst, &g);
+    if (rc || ce != cudaSuccess || ee != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      if (rc) return rc;
+      return record_cuda(ce != cudaSuccess ? ce : ee, "group capture", __FILE__, __LINE__);
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&c->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return record_cuda(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+    return SFQ_OK;
+  }
+
+  int block_async(const sfq_run_params_t* rps, const double* Eshift) {
+    const size_t n = es.size();
+    if (pending) return record_error(SFQ_ERR_ARG, "group: the previous block's results were not taken");
+    std::string key = std::to_string(lanes) + "#";
+    for (size_t i = 0; i < n; ++i) {
+      if (rps[i].steps <= 0) return record_error(SFQ_ERR_ARG, "group: steps must be positive");
+      key += Engine::block_key(rps[i]);
+      key += ';';
+    }
+    auto it = graphs.find(key);
+    if (it == graphs.end()) {
+      Captured c;
+      int rc = capture(rps, &c);
+      if (rc) return rc;
+      it = graphs.emplace(key, std::move(c)).first;
+    }
+    for (size_t i = 0; i < n; ++i) {
+      h_in[2 * i] = rps[i].step0;
+      std::memcpy(&h_in[2 * i + 1], &Eshift[i], sizeof(double));
+    }
+    // after every member's earlier work, one input copy, the graph, one output copy
+    for (size_t i = 0; i < n; ++i) {
+      SFQ_CUDA_TRY(cudaEventRecord(ev_pre[i], es[i]->st));
+      SFQ_CUDA_TRY(cudaStreamWaitEvent(gst, ev_pre[i], 0));
+    }
+    SFQ_CUDA_TRY(cudaMemcpyAsync(d_in, h_in, sizeof(unsigned long long) * 2 * n, cudaMemcpyHostToDevice, gst));
+    SFQ_CUDA_TRY(cudaGraphLaunch(it->second.exec, gst));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(h_out, d_out, sizeof(double) * kOut * n, cudaMemcpyDeviceToHost, gst));
+    SFQ_CUDA_TRY(cudaEventRecord(ev_done, gst));
+    for (size_t i = 0; i < n; ++i) {
+      SFQ_CUDA_TRY(cudaStreamWaitEvent(es[i]->st, ev_done, 0));
+      es[i]->inv_cached = it->second.inv_after[i] != 0;
+      es[i]->inv_ov = it->second.inv_ov_after[i];
+    }
+    pending = &it->second;
+    return SFQ_OK;
+  }
+
+  int block_query() {
+    if (!pending) return 1;
+    const cudaError_t q = cudaEventQuery(ev_done);
+    if (q == cudaSuccess) return 1;
+    if (q == cudaErrorNotReady) return 0;
+    return -record_cuda(q, "cudaEventQuery", __FILE__, __LINE__);
+  }
+
+  // per member: Eshift, status (0, SFQ_ERR_WEIGHT_COLLAPSE, SFQ_ERR_TIMEOUT, ...), measurements
+  int block_result(double* Eshift, int* status, double* meas, int max_meas, int* nmeas) {
+    if (!pending) return record_error(SFQ_ERR_ARG, "group: no block was run");
+    SFQ_CUDA_TRY(cudaEventSynchronize(ev_done));
+    const Captured& c = *pending;
+    pending = nullptr;
+    int first = SFQ_OK;
+    for (size_t i = 0; i < es.size(); ++i) {
+      const double* o = h_out + (size_t)kOut * i;
+      int s = SFQ_OK;
+      if (o[2] != 0.0) {
+        cudaMemsetAsync(es[i]->gemm_err, 0, sizeof(int), es[i]->st);
+        s = SFQ_ERR_TIMEOUT;
+      } else if (o[1] == double(SFQ_ERR_WEIGHT_COLLAPSE)) {
+        s = SFQ_ERR_WEIGHT_COLLAPSE;
+      } else if (o[1] != 0.0) {
+        s = SFQ_ERR_INTERNAL;
+      }
+      if (status) status[i] = s;
+      if (s && !first) first = s;
+      if (Eshift) Eshift[i] = o[0];
+      const int nm = c.nmeas[i] < max_meas ? c.nmeas[i] : max_meas;
+      if (meas && nm > 0) std::memcpy(meas + (size_t)10 * max_meas * i, o + 4, sizeof(double) * 10 * nm);
+      if (nmeas) nmeas[i] = c.nmeas[i];
+    }
+    if (first == SFQ_ERR_TIMEOUT)
+      return record_error(first, "group: a tensor-core product's bounded wait expired in the block");
+    if (first == SFQ_ERR_WEIGHT_COLLAPSE) return record_error(first, "group: a member's total walker weight collapsed.");
+    if (first) return record_error(first, "group: population control: inconsistent copy plan");
+    return SFQ_OK;
+  }
+};
+
 }  // namespace sfq
 
 struct sfq_engine_s {
   sfq::Engine e;
+};
+
+struct sfq_group_s {
+  sfq::Group g;
 };
 
 using namespace sfq;
@@ -1067,8 +1546,7 @@ int sfq_engine_destroy(sfq_engine_t h) {
   Engine& e = h->e;
   if (e.st) cudaStreamSynchronize(e.st);
   e.release_events();
-  for (auto& kv : e.graphs)
-    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  e.drop_graphs();
   if (e.blk_done) cudaEventDestroy(e.blk_done);
   if (e.blk_host) cudaFreeHost(e.blk_host);
   if (e.arena) cudaFree(e.arena);
@@ -1265,6 +1743,84 @@ int sfq_engine_block_query(sfq_engine_t h) {
 int sfq_engine_block_result(sfq_engine_t h, double* Eshift, double* meas, int max_meas, int* nmeas) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
   return h->e.block_result(Eshift, meas, max_meas, nmeas);
+}
+
+int sfq_group_create(sfq_group_t* out, const sfq_engine_t* engines, int n) {
+  if (!out || !engines || n <= 0) return record_error(SFQ_ERR_ARG, "group: no members");
+  *out = nullptr;
+  std::vector<Engine*> es;
+  for (int i = 0; i < n; ++i) {
+    if (!engines[i]) return record_error(SFQ_ERR_ARG, "group: null member %d", i);
+    if (engines[i]->e.p.device != engines[0]->e.p.device)
+      return record_error(SFQ_ERR_ARG, "group: members on different devices");
+    for (int j = 0; j < i; ++j)
+      if (engines[j] == engines[i]) return record_error(SFQ_ERR_ARG, "group: member %d repeated", i);
+    es.push_back(&engines[i]->e);
+  }
+  sfq_group_t h = new sfq_group_s;
+  const int rc = h->g.init(es);
+  if (rc) {
+    h->g.release();
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return SFQ_OK;
+}
+
+int sfq_group_destroy(sfq_group_t h) {
+  if (!h) return SFQ_OK;
+  h->g.release();
+  delete h;
+  return SFQ_OK;
+}
+
+int sfq_group_block_async(sfq_group_t h, const sfq_run_params_t* rps, const double* Eshift) {
+  if (!h || !rps || !Eshift) return record_error(SFQ_ERR_ARG, "null pointer");
+  return h->g.block_async(rps, Eshift);
+}
+
+int sfq_group_set_lanes(sfq_group_t h, int lanes) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null group");
+  if (lanes < 0) return record_error(SFQ_ERR_ARG, "group: lanes must be >= 0");
+  if (h->g.pending) return record_error(SFQ_ERR_ARG, "group: a block is running");
+  h->g.lanes = lanes;
+  return SFQ_OK;
+}
+
+int sfq_group_block_query(sfq_group_t h) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null group");
+  return h->g.block_query();
+}
+
+int sfq_group_block_result(sfq_group_t h, double* Eshift, int* status, double* meas, int max_meas, int* nmeas) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null group");
+  return h->g.block_result(Eshift, status, meas, max_meas, nmeas);
+}
+
+int sfq_group_block(sfq_group_t h, const sfq_run_params_t* rps, double* Eshift, int* status, double* meas,
+                    int max_meas, int* nmeas) {
+  int rc;
+  if ((rc = sfq_group_block_async(h, rps, Eshift))) return rc;
+  return h->g.block_result(Eshift, status, meas, max_meas, nmeas);
+}
+
+int sfq_engine_autotune(sfq_engine_t h, int repeats, sfq_tiles_t* out) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.autotune(repeats, out);
+}
+
+int sfq_engine_set_tiles(sfq_engine_t h, const sfq_tiles_t* t) {
+  if (!h || !t) return record_error(SFQ_ERR_ARG, "null pointer");
+  return h->e.set_tiles(t->g_bn, t->vbias_bn, t->vhs_bn, t->taylor_half, t->p1_bn);
+}
+
+int sfq_engine_tiles(sfq_engine_t h, sfq_tiles_t* t) {
+  if (!h || !t) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (!h->e.mixed) return record_error(SFQ_ERR_UNSUPPORTED, "tiles: only the mixed-precision products are tiled");
+  std::memset(t, 0, sizeof(*t));
+  h->e.get_tiles(t);
+  return SFQ_OK;
 }
 
 int sfq_engine_footprint(sfq_engine_t h, size_t* bytes) {

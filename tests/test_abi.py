@@ -44,7 +44,7 @@ def test_binding_covers_header():
 def test_last_error_and_version(lib):
     from safire_b200 import capi
     L = capi.lib()
-    assert L.sfq_abi_version() == 4
+    assert L.sfq_abi_version() == 5
     assert isinstance(L.sfq_last_error(), bytes)
 
 
@@ -82,3 +82,25 @@ def test_cpp_header_compiles():
     r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-x", "c++", hpp],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_group_and_tiles_argument_errors_without_gpu():
+    from safire_b200 import capi
+    L = capi.lib()
+    g = ctypes.c_void_p()
+    assert L.sfq_group_create(ctypes.byref(g), None, 0) == 2
+    arr = (ctypes.c_void_p * 2)(None, None)
+    assert L.sfq_group_create(ctypes.byref(g), arr, 2) == 2
+    assert L.sfq_group_destroy(None) == 0
+    assert L.sfq_group_block_query(None) == 2
+    assert L.sfq_engine_autotune(None, 3, None) == 2
+    assert L.sfq_engine_set_tiles(None, None) == 2
+
+
+def test_uneven_systems_layout():
+    """24 systems: M = 48..320 in steps of 16, cycled; N = M/4; Nchol = 5M; walkers in [64, 512]."""
+    from safire_b200 import batched
+    specs, walkers = batched.uneven_specs(24)
+    assert [s.M for s in specs] == [48 + 16 * (i % 18) for i in range(24)]
+    assert all(s.N * 4 == s.M and s.Nc == 5 * s.M for s in specs)
+    assert all(64 <= w <= 512 for w in walkers) and len(set(walkers)) > 12
