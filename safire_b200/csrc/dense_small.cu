@@ -192,7 +192,7 @@ __device__ double norm1_inf_upper(const cplx* A, int N, double* red) {
 }
 
 __global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS, int N, int* status, int* again,
-                                                               const int* active, double kappa_max) {
+                                                               const int* active, double kappa_max, cplx* Rout) {
   const long b = blockIdx.x;
   if (active && !active[b]) return;  // the whole CTA
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -237,6 +237,14 @@ __global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS,
     return;
   }
   const double nR = norm1_inf_upper(A, N, red);
+  if (Rout) {
+    cplx* Rb = Rout + b * sS;
+    for (int e = tid; e < N * N; e += LU_THREADS) {
+      const int i = e / N, k = e % N;
+      Rb[e] = (i > k) ? mk(0.0, 0.0) : A[e];
+    }
+    __syncthreads();  // every r_ii read before the diagonal below is replaced
+  }
   // R^-1 by back substitution on all columns at once, right-looking and in place: going up
   // the rows, row k of R^-1 is the pending row k over r_kk, and its product with column k of R
   // leaves the rows above at once (one rank-1 update per row, parallel over the block).  The
@@ -297,12 +305,12 @@ int lu_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, 
 }
 
 int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, int* again, const int* active, double kappa_max,
-              cudaStream_t st) {
+              cudaStream_t st, cplx* Rout) {
   if (nbatch <= 0 || N <= 0) return SFQ_OK;
   if (N > kMaxSmallN) return record_error(SFQ_ERR_UNSUPPORTED, "chol_rinv: N=%d exceeds %d", N, kMaxSmallN);
   const size_t sm = lu_smem_bytes(N);
   SFQ_CUDA_TRY(cudaFuncSetAttribute(chol_rinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-  chol_rinv_kernel<<<nbatch, LU_THREADS, sm, st>>>(S, sS, N, status, again, active, kappa_max);
+  chol_rinv_kernel<<<nbatch, LU_THREADS, sm, st>>>(S, sS, N, status, again, active, kappa_max, Rout);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

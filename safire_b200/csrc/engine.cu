@@ -1008,9 +1008,20 @@ struct Engine {
   int orthogonalize() {
     int rc;
     ph_begin(SFQ_PH_ORTHO);
-    inv_cached = false;
-    if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, M, N, st))) return rc;
-    if ((rc = log_overlap(newov))) return rc;  // wfn->Log_Overlap(wset)
+    const long NN = (long)N * N;
+    if (inv_cached && tchunk_elems >= 2L * W * NN) {
+      // the cached inverse overlaps and log overlaps of the walkers ride through the QR, which
+      // gives wfn->Log_Overlap(wset) of the orthogonalized walkers without a new factorization
+      if (inv_ov != newov)
+        SFQ_CUDA_TRY(cudaMemcpyAsync(newov, inv_ov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
+      if ((rc = ops::orthogonalize_carry(SM, SM2, Tchunk, Tchunk + W * NN, G, status, T, newov, 2.0, W, M, N, st)))
+        return rc;
+      inv_ov = newov;
+    } else {
+      inv_cached = false;
+      if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, M, N, st))) return rc;
+      if ((rc = log_overlap(newov))) return rc;  // wfn->Log_Overlap(wset)
+    }
     SFQ_CUDA_TRY(cudaMemcpyAsync(props + (long)P_OVLP * W, newov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
     ph_end(SFQ_PH_ORTHO);
     return SFQ_OK;

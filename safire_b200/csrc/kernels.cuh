@@ -14,9 +14,10 @@ int gj_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, 
 int lu_logdet(cplx* T, long sT, int nbatch, int N, cplx* ovlp, bool accumulate, double post_scale, bool invert,
               cudaStream_t st);
 // S = R^H R and R^-1 over S; again[b] = 1 when R's condition bound exceeds kappa_max (may be
-// null); batches with active[b] == 0 are left alone (active may be null)
+// null); batches with active[b] == 0 are left alone (active may be null); R itself (upper, zeros
+// below) into Rout when it is not null
 int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, int* again, const int* active, double kappa_max,
-              cudaStream_t st);
+              cudaStream_t st, cplx* Rout = nullptr);
 
 struct FieldParams {
   int nwalk = 0, nchol = 0;

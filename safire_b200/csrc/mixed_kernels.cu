@@ -86,41 +86,98 @@ __global__ void reduce_planar_to_cplx_kernel(const float* C, int KS, long sk, in
 }
 
 // planar vHS (rows c*W + w, columns i*M + k, or the packed upper triangle when packed) ->
-// V[w][c][i][k] split.  One 32 x 32 tile per block through shared memory: packed rows are read
-// along k and V is written along its rows; for the packed triangle a block reads the tile
-// i-block <= k-block once and writes it and its mirror.
-__global__ void build_v_kernel(const float* Cv, int W, int M, int packed, Planes P) {
-  __shared__ float tile[32][33];
-  const int wc = blockIdx.z;  // c * W + w
-  const int c = wc / W, w = wc - c * W;
-  const int ib = blockIdx.y, kb = blockIdx.x;
+// V[w][c][i][k] split.  Each thread converts 4 consecutive elements of a row and stores each
+// plane's 4 BF16 values as one 8-byte word (M is a multiple of 8, so a group never straddles the
+// row end and is 8-byte aligned).
+__device__ __forceinline__ void split_store4(const float (&x)[4], const Planes& P, long idx) {
+  union U {
+    __nv_bfloat162 h[2];
+    uint2 u;
+  };
+  U q0;
+  q0.h[0] = __floats2bfloat162_rn(x[0], x[1]);
+  q0.h[1] = __floats2bfloat162_rn(x[2], x[3]);
+  *reinterpret_cast<uint2*>(P.p0 + idx) = q0.u;
+  if (!P.p1) return;
+  float r[4];
+  r[0] = x[0] - __low2float(q0.h[0]);
+  r[1] = x[1] - __high2float(q0.h[0]);
+  r[2] = x[2] - __low2float(q0.h[1]);
+  r[3] = x[3] - __high2float(q0.h[1]);
+  U q1;
+  q1.h[0] = __floats2bfloat162_rn(r[0], r[1]);
+  q1.h[1] = __floats2bfloat162_rn(r[2], r[3]);
+  *reinterpret_cast<uint2*>(P.p1 + idx) = q1.u;
+  if (!P.p2) return;
+  U q2;
+  q2.h[0] = __floats2bfloat162_rn(r[0] - __low2float(q1.h[0]), r[1] - __high2float(q1.h[0]));
+  q2.h[1] = __floats2bfloat162_rn(r[2] - __low2float(q1.h[1]), r[3] - __high2float(q1.h[1]));
+  *reinterpret_cast<uint2*>(P.p2 + idx) = q2.u;
+}
+
+// full M x M rows: float4 loads, 8-byte plane stores
+__global__ void build_v_full_kernel(const float* Cv, int W, int M, Planes P) {
   const long MM = (long)M * M;
-  const long ld = packed ? (long)M * (M + 1) / 2 : MM;
-  const float* src = Cv + (long)wc * ld;
-  const long vbase = ((long)w * 2 + c) * MM;
-  const int tx = threadIdx.x;
-  if (!packed) {
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-      const int i = ib * 32 + r, k = kb * 32 + tx;
-      if (i < M && k < M) split_store(src[(long)i * M + k], P, vbase + (long)i * M + k);
-    }
-    return;
+  const long groups = 2L * W * MM / 4;
+  for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < groups; g += (long)gridDim.x * blockDim.x) {
+    const long e = 4 * g;                 // element of the planar rows (c * W + w, i * M + k)
+    const long wc = e / MM, ik = e - wc * MM;
+    const long c = wc / W, w = wc - c * W;
+    const float4 v = *reinterpret_cast<const float4*>(Cv + e);
+    const float x[4] = {v.x, v.y, v.z, v.w};
+    split_store4(x, P, (w * 2 + c) * MM + ik);
   }
-  if (ib > kb) return;
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int i = ib * 32 + r, k = kb * 32 + tx;
-    if (i < M && k < M && i <= k) tile[r][tx] = src[upper_index(i, k, M)];
+}
+
+// packed upper triangle: one block per 64 x 64 tile pair (ib <= kb) of one planar row; the tile is
+// read once along the packed rows and written as V[i][k] and, off the diagonal, as its mirror
+// V[k][i]
+constexpr int kVT = 64;
+__global__ void __launch_bounds__(256) build_v_packed_kernel(const float* Cv, int W, int M, int T, Planes P) {
+  __shared__ float tile[kVT][kVT + 1];
+  __shared__ long rowbase[kVT];
+  const int wc = blockIdx.y;  // c * W + w
+  const int c = wc / W, w = wc - c * W;
+  int t = blockIdx.x, ib = 0;  // tile pair from the linear index: row ib holds kb = ib .. T-1
+  while (ib < T && t >= T - ib) {
+    t -= T - ib;
+    ++ib;
+  }
+  const int kb = ib + t;
+  const int i0 = ib * kVT, k0 = kb * kVT;
+  const long MM = (long)M * M;
+  const float* src = Cv + (long)wc * ((long)M * (M + 1) / 2);
+  const long vbase = ((long)w * 2 + c) * MM;
+  const int tid = threadIdx.x;
+  if (tid < kVT) {
+    const long i = i0 + tid;
+    rowbase[tid] = i * M - i * (i + 1) / 2;  // packed index of (i, k) = rowbase + k, k >= i
   }
   __syncthreads();
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int i = ib * 32 + r, k = kb * 32 + tx;
-    if (i < M && k < M) split_store(i <= k ? tile[r][tx] : tile[tx][r], P, vbase + (long)i * M + k);
+  for (int e = tid; e < kVT * kVT; e += 256) {
+    const int r = e / kVT, q = e % kVT;
+    const int i = i0 + r, k = k0 + q;
+    if (i < M && k < M && i <= k) tile[r][q] = src[rowbase[r] + k];
   }
-  if (ib < kb) {
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-      const int k = kb * 32 + r, i = ib * 32 + tx;
-      if (k < M && i < M) split_store(tile[tx][r], P, vbase + (long)k * M + i);
-    }
+  __syncthreads();
+  for (int e = tid; e < kVT * kVT / 4; e += 256) {
+    const int r = e / (kVT / 4), g = 4 * (e % (kVT / 4));
+    const int i = i0 + r, k = k0 + g;
+    if (i >= M || k >= M) continue;
+    float x[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[j] = (i <= k + j) ? tile[r][g + j] : tile[g + j][r];  // the diagonal tile's lower half mirrored
+    split_store4(x, P, vbase + (long)i * M + k);
+  }
+  if (ib == kb) return;
+  for (int e = tid; e < kVT * kVT / 4; e += 256) {
+    const int r = e / (kVT / 4), g = 4 * (e % (kVT / 4));
+    const int k = k0 + r, i = i0 + g;
+    if (k >= M || i >= M) continue;
+    float x[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[j] = tile[g + j][r];
+    split_store4(x, P, vbase + (long)k * M + i);
   }
 }
 
@@ -176,10 +233,16 @@ int mixed_reduce_planar_to_cplx(const float* C, int KS, long sk, int W, long E, 
 }
 
 int mixed_build_v(const float* Cv, int W, int M, bool packed, void* const* pl, cudaStream_t st) {
-  const unsigned t = unsigned((M + 31) / 32);
+  if (M % 8) return record_error(SFQ_ERR_SHAPE, "build_v: M=%d is not a multiple of 8", M);
+  if (!packed) {
+    build_v_full_kernel<<<grid_for(2L * W * M * M / 4), 256, 0, st>>>(Cv, W, M, planes(pl));
+    SFQ_LAUNCHED();
+    return SFQ_OK;
+  }
   if (2L * W > 65535) return record_error(SFQ_ERR_SHAPE, "build_v: too many walkers for one launch");
-  dim3 grid(t, t, unsigned(2 * W)), block(32, 8);
-  build_v_kernel<<<grid, block, 0, st>>>(Cv, W, M, packed ? 1 : 0, planes(pl));
+  const int T = (M + kVT - 1) / kVT;
+  dim3 grid(unsigned(T * (T + 1) / 2), unsigned(2 * W));
+  build_v_packed_kernel<<<grid, 256, 0, st>>>(Cv, W, M, T, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

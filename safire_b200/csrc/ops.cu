@@ -125,7 +125,7 @@ int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M
 // One CholeskyQR pass over the walkers selected by mask (all when null): S = Win^H Win = R^H R,
 // Wout = Win R^-1; again[b] set from R's condition bound when again is not null.
 static int cholqr_pass(const cplx* Win, cplx* Wout, cplx* S, int* status, int* again, const int* mask, int W, int M,
-                       int N, cudaStream_t st) {
+                       int N, cudaStream_t st, cplx* R = nullptr) {
   int rc;
   GemmDesc d;  // S = Win^H Win
   d.M = N; d.N = N; d.K = M; d.batch = W;
@@ -134,7 +134,7 @@ static int cholqr_pass(const cplx* Win, cplx* Wout, cplx* S, int* status, int* a
   d.C = S; d.sCm = N; d.sCn = 1; d.sCb = (long)N * N;
   d.mask = mask;
   if ((rc = gemm_f64(d, st))) return rc;
-  if ((rc = chol_rinv(S, (long)N * N, W, N, status, again, mask, kCholQrKappa, st))) return rc;
+  if ((rc = chol_rinv(S, (long)N * N, W, N, status, again, mask, kCholQrKappa, st, R))) return rc;
   GemmDesc q;  // Wout = Win R^-1
   q.M = M; q.N = N; q.K = N; q.batch = W;
   q.A = Win; q.sAm = N; q.sAk = 1; q.sAb = (long)M * N; q.a_cplx = true;
@@ -155,6 +155,56 @@ int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int
   if ((rc = copy_walkers_where(SM, SM2, again, 0, W, (long)M * N, st))) return rc;  // one-pass walkers
   (void)log_detR;
   return SFQ_OK;
+}
+
+namespace {
+// ov[w] -= scale * sum_i log r_ii over R[w] (real positive diagonal), one warp per walker, the sum
+// in a fixed order; walkers with mask[w] == 0 are left alone (mask may be null)
+__global__ void sub_logdiag_kernel(const cplx* R, int N, const int* mask, cplx* ov, double scale, int W) {
+  const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= W || (mask && !mask[w])) return;
+  const cplx* Rw = R + (long)w * N * N;
+  double s = 0.0;
+  for (int i = lane; i < N; i += 32) s += log(Rw[(long)i * N + i].x);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) ov[w].x -= scale * s;
+}
+
+// C[w] = R[w] Tin[w] (N x N complex, batch W; walkers with mask[w] == 0 skipped)
+int rmul(const cplx* R, const cplx* Tin, cplx* C, const int* mask, int W, int N, cudaStream_t st) {
+  GemmDesc d;
+  d.M = N; d.N = N; d.K = N; d.batch = W;
+  d.A = R; d.sAm = N; d.sAk = 1; d.sAb = (long)N * N; d.a_cplx = true;
+  d.B = Tin; d.sBk = N; d.sBn = 1; d.sBb = (long)N * N; d.b_cplx = true;
+  d.C = C; d.sCm = N; d.sCn = 1; d.sCb = (long)N * N;
+  d.mask = mask;
+  return gemm_f64(d, st);
+}
+}  // namespace
+
+// orthogonalize() carrying the walkers' inverse overlap matrices and log overlaps through the
+// QR instead of factoring the new overlaps again: with W' = W R^-1 (R = R2 R1 over the passes),
+// (PsiT W')^-1 = R (PsiT W)^-1 and log det(PsiT W') = log det(PsiT W) - sum_i log r_ii, the r_ii
+// real and positive (the phase is unchanged).  Tinv (W, N, N) and ov (W) in/out, scale = the
+// number of identical determinants (2 for CLOSED walkers); S, R, Tw: (W, N, N) scratch.
+int orthogonalize_carry(cplx* SM, cplx* SM2, cplx* S, cplx* R, cplx* Tw, int* status, cplx* Tinv, cplx* ov,
+                        double scale, int W, int M, int N, cudaStream_t st) {
+  int rc;
+  int* again = status + W;
+  const long NN = (long)N * N;
+  if ((rc = cholqr_pass(SM, SM2, S, status, again, nullptr, W, M, N, st, R))) return rc;
+  if ((rc = rmul(R, Tinv, Tw, nullptr, W, N, st))) return rc;
+  const int wpb = 8;
+  sub_logdiag_kernel<<<(W + wpb - 1) / wpb, 32 * wpb, 0, st>>>(R, N, nullptr, ov, scale, W);
+  SFQ_LAUNCHED();
+  if ((rc = cholqr_pass(SM2, SM, S, status, nullptr, again, W, M, N, st, R))) return rc;
+  if ((rc = rmul(R, Tw, Tinv, again, W, N, st))) return rc;
+  sub_logdiag_kernel<<<(W + wpb - 1) / wpb, 32 * wpb, 0, st>>>(R, N, again, ov, scale, W);
+  SFQ_LAUNCHED();
+  if ((rc = copy_walkers_where(SM, SM2, again, 0, W, (long)M * N, st))) return rc;  // one-pass walkers
+  return copy_walkers_where(Tinv, Tw, again, 0, W, NN, st);
 }
 
 int energy_chunk(int W, int N, int Nc, long max_elems) {

@@ -24,6 +24,11 @@ int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M
 // CholeskyQR2; SM2 (W*M*N), S (W*N*N) scratch, status (W) ints.  log_detR (W) accumulated if not null
 // CholeskyQR2 in place on SM (SM2, S: scratch; status: 2 W ints)
 int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int W, int M, int N, cudaStream_t st);
+// the same, carrying the inverse overlap matrices Tinv (W, N, N) and log overlaps ov (W) of the
+// walkers through the QR ((PsiT W R^-1)^-1 = R (PsiT W)^-1, log det drops by scale * sum log r_ii);
+// S, R, Tw: (W, N, N) scratch
+int orthogonalize_carry(cplx* SM, cplx* SM2, cplx* S, cplx* R, cplx* Tw, int* status, cplx* Tinv, cplx* ov,
+                        double scale, int W, int M, int N, cudaStream_t st);
 // energy with chunked T; ws: T chunk (W*N*nv*N) + exxn (W*Nc) + kl (W*Nc)
 int energy(cplx* E3, const cplx* G, const cplx* haj, const void* Lnak, bool l_cplx, double E0, int W, int N, int M,
            int Nc, int addH1, int addEJ, int addEXX, cplx* Tchunk, long tchunk_elems, cplx* exxn, cplx* kl,
