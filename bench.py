@@ -252,6 +252,9 @@ def run_engine(args, cfg, spec, s, W, DT, prec, rank, local, profile_pass=True, 
     eng = afqmc.AfqmcEngine(s, W, dt=DT, seed=1000 + rank, device=local, precision=prec)
     state = {"Esh": eng.init()}
     ext = torch.cuda.ExternalStream(eng.stream)
+    out = {}
+    if prec != capi.PRECISION_FP64 and not getattr(args, "no_autotune", False):
+        out["tiles"] = eng.autotune().choice()  # tile widths from timing the products on this engine
 
     def step(st, host=False, ubuf=None, pbuf=None):
         """One run_afqmc iteration in the equilibration phase (run_afqmc.cpp:69-93)."""
@@ -270,7 +273,6 @@ def run_engine(args, cfg, spec, s, W, DT, prec, rank, local, profile_pass=True, 
         step(st)
     eng.synchronize()
     torch.cuda.synchronize()
-    out = {}
     clk = ClockSampler(local)
     clk.start()
     time.sleep(0.3)
@@ -332,6 +334,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 drop-in comparison run")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the built-in tile widths")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -461,7 +464,7 @@ def main():
                        "eshift": "relaxed every step (equilibration phase of run_afqmc)",
                        "taylor_order": 6, "ortho_every": ORTHO_EVERY, "popcontrol_every": POP_EVERY,
                        "l2": "inputs larger than L2 (Likn alone is %.2f GB)" % (spec.M ** 2 * spec.Nc * 8 / 1e9),
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", "tiles": m.get("tiles")},
             "algorithmic_tflops": step_flops(spec.M, spec.N, spec.Nc) * W * args.steps * world / (ms * 1e-3) / 1e12,
             "gpu_launches": m["launches"], "clocks": m["clocks"], "e2e": e2e, "roofline": roofline,
             "fp64_comparison": compare, "phases": phases, "cpu_baseline": cpu}

@@ -455,12 +455,22 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
             ad[q] = smem_desc(st + q * L::A_BYTES);
             bd[q] = smem_desc(st + NP * L::A_BYTES + q * L::B_BYTES);
           }
-          if (p.cb_half) {
-            // two N = half products per slice: re half with Vr (c' = 0) or -Vi (c' = 1), im half with
-            // Vi or Vr, the second B box starting half * 128 bytes into the tile
+          if (p.cb_half && kt < p.cb_kth) {
+            // c' = 0: the boxes [Vr; Vi] lie in shared memory exactly as one 2 * half = BN row tile
+            // (half is a multiple of 8, the swizzle atom), so [re | im] += A_re [Vr; Vi]^T is one
+            // N = BN product
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+              const uint64_t off = uint64_t(kk * 32) >> 4;
+#pragma unroll
+              for (int tt = 0; tt < n_terms(NP); ++tt)
+                umma_bf16(d_tmem, ad[term_a(tt)] + off, bd[term_b(tt)] + off, idesc, ((kt - kb) | kk | tt) ? 1u : 0u);
+            }
+          } else if (p.cb_half) {
+            // c' = 1: two N = half products per slice, re half with -Vi (the instruction's negate-B
+            // bit), im half with Vr, the second B box starting half * 128 bytes into the tile
             const uint32_t h = uint32_t(p.cb_half);
             const uint32_t id_h = instr_desc_n(h), id_hneg = id_h | (1u << 14);  // bit 14: negate B
-            const uint32_t id_re = (kt >= p.cb_kth) ? id_hneg : id_h;
             const uint64_t boff = uint64_t(h * (BK * 2)) >> 4;
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk) {
@@ -468,7 +478,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
 #pragma unroll
               for (int tt = 0; tt < n_terms(NP); ++tt) {
                 const uint32_t acc = ((kt - kb) | kk | tt) ? 1u : 0u;
-                umma_bf16(d_tmem, ad[term_a(tt)] + off, bd[term_b(tt)] + off, id_re, acc);
+                umma_bf16(d_tmem, ad[term_a(tt)] + off, bd[term_b(tt)] + off, id_hneg, acc);
                 umma_bf16(d_tmem + h, ad[term_a(tt)] + off, bd[term_b(tt)] + boff + off, id_h, acc);
               }
             }
