@@ -181,17 +181,62 @@ __global__ void __launch_bounds__(256) build_v_packed_kernel(const float* Cv, in
   }
 }
 
+// split_store_d for 4 consecutive elements (residuals in double), each plane's 4 values as one
+// 8-byte word (idx a multiple of 4)
+__device__ __forceinline__ void split_store4_d(const double (&x)[4], const Planes& P, long idx) {
+  union U {
+    __nv_bfloat162 h[2];
+    uint2 u;
+  };
+  U q0;
+  q0.h[0] = __floats2bfloat162_rn(float(x[0]), float(x[1]));
+  q0.h[1] = __floats2bfloat162_rn(float(x[2]), float(x[3]));
+  *reinterpret_cast<uint2*>(P.p0 + idx) = q0.u;
+  if (!P.p1) return;
+  double r[4];
+  r[0] = x[0] - double(__low2float(q0.h[0]));
+  r[1] = x[1] - double(__high2float(q0.h[0]));
+  r[2] = x[2] - double(__low2float(q0.h[1]));
+  r[3] = x[3] - double(__high2float(q0.h[1]));
+  U q1;
+  q1.h[0] = __floats2bfloat162_rn(float(r[0]), float(r[1]));
+  q1.h[1] = __floats2bfloat162_rn(float(r[2]), float(r[3]));
+  *reinterpret_cast<uint2*>(P.p1 + idx) = q1.u;
+  if (!P.p2) return;
+  U q2;
+  q2.h[0] = __floats2bfloat162_rn(float(r[0] - double(__low2float(q1.h[0]))), float(r[1] - double(__high2float(q1.h[0]))));
+  q2.h[1] = __floats2bfloat162_rn(float(r[2] - double(__low2float(q1.h[1]))), float(r[3] - double(__high2float(q1.h[1]))));
+  *reinterpret_cast<uint2*>(P.p2 + idx) = q2.u;
+}
+
 // inverse overlaps Tinv (W, N, N) complex -> the real block operand of G = (W Tinv)^T, rows
-// (c, a), columns (b, c'): [[Tr, -Ti], [Ti, Tr]] at (Tinv[b][a]), split
+// (c, a), columns (b, c'): [[Tr, -Ti], [Ti, Tr]] at (Tinv[b][a]), split.  A 32 x 32 tile of Tinv
+// goes through shared memory (read along a, written along b); each thread writes 4 consecutive
+// columns (two b, both c') of one row as one 8-byte word per plane.  N is a multiple of 4.
 __global__ void build_tblk_kernel(const cplx* Tinv, int W, int N, Planes P) {
+  __shared__ cplx tile[32][33];
+  const int w = blockIdx.z, b0 = blockIdx.y * 32, a0 = blockIdx.x * 32;
+  const cplx* Tw = Tinv + (long)w * N * N;
+  for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
+    const int bb = e / 32, aa = e % 32;
+    const int b = b0 + bb, a = a0 + aa;
+    if (b < N && a < N) tile[bb][aa] = Tw[(long)b * N + a];
+  }
+  __syncthreads();
   const long N2 = 2L * N;
-  const long total = (long)W * N2 * N2;
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const long w = t / (N2 * N2), r = (t / N2) % N2, q = t % N2;
-    const int c = int(r / N), a = int(r % N), b = int(q >> 1), cp = int(q & 1);
-    const cplx z = Tinv[(w * N + b) * N + a];
-    const double v = (c == cp) ? z.x : (c == 0 ? -z.y : z.y);
-    split_store_d(v, P, t);
+  for (int e = threadIdx.x; e < 2 * 32 * 16; e += blockDim.x) {
+    const int c = e / (32 * 16), rem = e % (32 * 16);
+    const int aa = rem / 16, bb = 2 * (rem % 16);
+    const int a = a0 + aa, b = b0 + bb;
+    if (a >= N || b >= N) continue;  // b even and N a multiple of 4: b + 1 < N too
+    const cplx z0 = tile[bb][aa], z1 = tile[bb + 1][aa];
+    double x[4];
+    if (c == 0) {
+      x[0] = z0.x; x[1] = -z0.y; x[2] = z1.x; x[3] = -z1.y;
+    } else {
+      x[0] = z0.y; x[1] = z0.x; x[2] = z1.y; x[3] = z1.x;
+    }
+    split_store4_d(x, P, ((long)w * N2 + (long)c * N + a) * N2 + 2L * b);
   }
 }
 
@@ -248,7 +293,10 @@ int mixed_build_v(const float* Cv, int W, int M, bool packed, void* const* pl, c
 }
 
 int mixed_build_tblk(const cplx* Tinv, int W, int N, void* const* pl, cudaStream_t st) {
-  build_tblk_kernel<<<grid_for((long)W * 4 * N * N), 256, 0, st>>>(Tinv, W, N, planes(pl));
+  if (N % 4) return record_error(SFQ_ERR_SHAPE, "build_tblk: N=%d is not a multiple of 4", N);
+  if (W > 65535) return record_error(SFQ_ERR_SHAPE, "build_tblk: too many walkers for one launch");
+  dim3 grid(unsigned((N + 31) / 32), unsigned((N + 31) / 32), unsigned(W));
+  build_tblk_kernel<<<grid, 256, 0, st>>>(Tinv, W, N, planes(pl));
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
