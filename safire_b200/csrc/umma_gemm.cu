@@ -135,11 +135,14 @@ __host__ __device__ constexpr uint32_t tmem_cols() {
   return BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
 }
 
-template <int BN, int STAGES, int NP>
+// JOINT: complex-B products whose stage holds both halves of A (re and im parts of the walker
+// operand at the same k) against one load of the tile's [Vr; Vi] rows
+template <int BN, int STAGES, int NP, bool JOINT = false>
 struct Smem {
   static constexpr int A_BYTES = BM * BK * 2;
   static constexpr int B_BYTES = BN * BK * 2;
-  static constexpr int STAGE = NP * (A_BYTES + B_BYTES);
+  static constexpr int A_SLOTS = JOINT ? 2 : 1;
+  static constexpr int STAGE = NP * (A_SLOTS * A_BYTES + B_BYTES);
   static constexpr int BAR_OFF = STAGES * STAGE;
   static constexpr int NBAR = 2 * STAGES + 5;  // full, empty, acc_full[2], acc_empty[2], done
   static constexpr int TOTAL = BAR_OFF + NBAR * 8 + 16 + 1024;  // + alignment slack
@@ -331,10 +334,10 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
   }
 }
 
-template <int BN, int STAGES, int NP>
+template <int BN, int STAGES, int NP, bool JOINT>
 __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_constant__ Maps maps,
                                                                 const __grid_constant__ KParams p) {
-  using L = Smem<BN, STAGES, NP>;
+  using L = Smem<BN, STAGES, NP, JOINT>;
   constexpr uint32_t COLS = tmem_cols<BN>();  // one accumulator buffer; two are allocated
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
   volatile int* s_abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int KT = (p.K + BK - 1) / BK;
+  const int KT = JOINT ? p.cb_kth : (p.K + BK - 1) / BK;  // JOINT: one stage per k slice of both halves
   const uint32_t stage_tx = uint32_t(L::STAGE);
 
   if (threadIdx.x == 0) {
@@ -394,7 +397,19 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
           }
           unsigned char* st = smem + s * L::STAGE;
           mbar_expect_tx(&full[s], stage_tx);
-          if (p.cb_half) {
+          if constexpr (JOINT) {
+            // k slice kt of both halves: A at k0 (re) and ldh + k0 (im), B the tile's [Vr; Vi] rows once
+            const int k0 = kt * BK, i0 = nt * p.cb_half;
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+              unsigned char* aq = st + q * 2 * L::A_BYTES;
+              unsigned char* bt = st + NP * 2 * L::A_BYTES + q * L::B_BYTES;
+              tma_load_3d(aq, &maps.a[q], &full[s], k0, m0, ab);
+              tma_load_3d(aq + L::A_BYTES, &maps.a[q], &full[s], p.cb_ldh + k0, m0, ab);
+              tma_load_3d(bt, &maps.b[q], &full[s], k0, i0, bb);
+              tma_load_3d(bt + p.cb_half * (BK * 2), &maps.b[q], &full[s], k0, p.cb_nmo + i0, bb);
+            }
+          } else if (p.cb_half) {
             // K slice kt = (c', k0): A at c' * ldh + k0; B: the Vr and Vi rows of the tile's orbitals,
             // [Vr; Vi] for c' = 0 and [Vi; Vr] for c' = 1 (each box half the tile)
             const int cp = kt / p.cb_kth, k0 = (kt - cp * p.cb_kth) * BK;
@@ -452,10 +467,27 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
           uint64_t ad[NP], bd[NP];
 #pragma unroll
           for (int q = 0; q < NP; ++q) {
-            ad[q] = smem_desc(st + q * L::A_BYTES);
-            bd[q] = smem_desc(st + NP * L::A_BYTES + q * L::B_BYTES);
+            ad[q] = smem_desc(st + q * L::A_SLOTS * L::A_BYTES);
+            bd[q] = smem_desc(st + NP * L::A_SLOTS * L::A_BYTES + q * L::B_BYTES);
           }
-          if (p.cb_half && kt < p.cb_kth) {
+          if constexpr (JOINT) {
+            // [re | im] += A_re [Vr; Vi]^T (one N = BN product), re -= A_im Vi^T, im += A_im Vr^T
+            const uint32_t h = uint32_t(p.cb_half);
+            const uint32_t id_h = instr_desc_n(h), id_hneg = id_h | (1u << 14);  // bit 14: negate B
+            const uint64_t boff = uint64_t(h * (BK * 2)) >> 4;
+            const uint64_t aim = uint64_t(L::A_BYTES) >> 4;  // the im half, one A tile further
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+              const uint64_t off = uint64_t(kk * 32) >> 4;
+#pragma unroll
+              for (int tt = 0; tt < n_terms(NP); ++tt) {
+                const uint64_t are = ad[term_a(tt)] + off, aimd = ad[term_a(tt)] + aim + off;
+                umma_bf16(d_tmem, are, bd[term_b(tt)] + off, idesc, ((kt - kb) | kk | tt) ? 1u : 0u);
+                umma_bf16(d_tmem, aimd, bd[term_b(tt)] + boff + off, id_hneg, 1u);
+                umma_bf16(d_tmem + h, aimd, bd[term_b(tt)] + off, id_h, 1u);
+              }
+            }
+          } else if (p.cb_half && kt < p.cb_kth) {
             // c' = 0: the boxes [Vr; Vi] lie in shared memory exactly as one 2 * half = BN row tile
             // (half is a multiple of 8, the swizzle atom), so [re | im] += A_re [Vr; Vi]^T is one
             // N = BN product
@@ -582,9 +614,9 @@ int sm_count() {
   return counts[dev];
 }
 
-template <int BN, int STAGES, int NP>
+template <int BN, int STAGES, int NP, bool JOINT = false>
 int launch(const UmmaGemmDesc& d, cudaStream_t st) {
-  using L = Smem<BN, STAGES, NP>;
+  using L = Smem<BN, STAGES, NP, JOINT>;
   static_assert(L::TOTAL <= 232448, "shared memory budget");
   static_assert(2 * tmem_cols<BN>() <= 512, "two accumulators must fit in tensor memory");
   Maps maps;
@@ -644,7 +676,8 @@ int launch(const UmmaGemmDesc& d, cudaStream_t st) {
   kp.C = d.C; kp.ldc = d.ldc; kp.sCb = d.sCb; kp.sCk = d.sCk; kp.alpha = d.alpha; kp.beta = d.beta;
   kp.e = e;
   kp.err = d.err;
-  auto k = umma_gemm_kernel<BN, STAGES, NP>;
+  if (JOINT && !cb) return record_error(SFQ_ERR_ARG, "umma_gemm: the joint layout is for complex B only");
+  auto k = umma_gemm_kernel<BN, STAGES, NP, JOINT>;
   SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
   const long grid = kp.tiles < sm_count() ? kp.tiles : sm_count();
   k<<<unsigned(grid), kThreads, L::TOTAL, st>>>(maps, kp);
@@ -671,6 +704,21 @@ int umma_gemm(const UmmaGemmDesc& d, cudaStream_t st) {
   if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return SFQ_OK;
   if (d.K <= 0) return record_error(SFQ_ERR_SHAPE, "umma_gemm: K must be positive");
   const int bn = d.bn ? d.bn : (d.N <= 64 ? 64 : 128);
+  // complex B with at most 2 planes and tiles up to 160 wide: the joint stage layout (both halves of
+  // A against one load of [Vr; Vi]); two stages of it fit where three of the split layout did
+  if (d.cplx_half > 0 && d.nplanes <= 2 && bn <= 160) {
+    switch (d.nplanes * 1000 + bn) {
+      case 1032: return umma::launch<32, 6, 1, true>(d, st);
+      case 1064: return umma::launch<64, 5, 1, true>(d, st);
+      case 1128: return umma::launch<128, 4, 1, true>(d, st);
+      case 1160: return umma::launch<160, 4, 1, true>(d, st);
+      case 2032: return umma::launch<32, 3, 2, true>(d, st);
+      case 2064: return umma::launch<64, 2, 2, true>(d, st);
+      case 2128: return umma::launch<128, 2, 2, true>(d, st);
+      case 2160: return umma::launch<160, 2, 2, true>(d, st);
+      default: break;
+    }
+  }
   switch (d.nplanes * 1000 + bn) {
     case 1032: return umma::launch<32, 8, 1>(d, st);
     case 1064: return umma::launch<64, 8, 1>(d, st);
