@@ -132,6 +132,10 @@ struct Engine {
   int M = 0, N = 0, Nc = 0, W = 0;
   bool trial_real = true;
   cudaStream_t st = nullptr;
+  // host-buffer steps: the field uniforms go in on a copy stream while the step's density and force
+  // bias run; the fields kernel waits for uni_wait (cleared once waited on)
+  cudaStream_t cst = nullptr;
+  cudaEvent_t uni_ready = nullptr, uni_free = nullptr, uni_wait = nullptr;
   // arena
   unsigned char* arena = nullptr;
   size_t arena_bytes = 0;
@@ -579,9 +583,9 @@ struct Engine {
       return mixed_split_planar(G, W, (long)N * M, Gs_p, st);
     }
     if ((rc = mixed_build_tblk(T, W, N, Tb_p, st))) return rc;
-    if ((rc = split_bf16_f64(reinterpret_cast<const double*>(SM), 2L * W * M * N, Ws_p[0], Ws_p[1],
-                             nplanes > 2 ? Ws_p[2] : nullptr, st)))
-      return rc;
+    // the walkers' planes for this product and, in the same pass, the walker rows of the P1
+    // product later in the step (the walkers do not change in between)
+    if ((rc = mixed_walkers_split_both(SM, W, M, N, ldh, Ws_p, Wt_p, st))) return rc;
     UmmaEpilogue eg;
     eg.kind = UMMA_EPI_PLANAR_SPLIT;
     eg.nel = N;
@@ -617,6 +621,10 @@ struct Engine {
     FieldParams fp;                                                                   // 2. X
     fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
     fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms; fp.step_dev = dev_mode ? d_step : nullptr;
+    if (uni_wait) {
+      SFQ_CUDA_TRY(cudaStreamWaitEvent(st, uni_wait, 0));
+      uni_wait = nullptr;
+    }
     if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
     ph_end(SFQ_PH_FIELDS);
     ph_begin(SFQ_PH_VHS);
@@ -938,6 +946,10 @@ struct Engine {
     FieldParams fp;
     fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
     fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms; fp.step_dev = dev_mode ? d_step : nullptr;
+    if (uni_wait) {
+      SFQ_CUDA_TRY(cudaStreamWaitEvent(st, uni_wait, 0));
+      uni_wait = nullptr;
+    }
     if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
     ph_end(SFQ_PH_FIELDS);
     ph_begin(SFQ_PH_VHS);
@@ -954,7 +966,7 @@ struct Engine {
     // Taylor products' epilogues, the operand planes alternating between the two buffers; the
     // last one leaves the planes of S for SM = P1 S, written straight back to the walkers
     const long rows = 2L * W * N;  // (w, a, c) rows of the walker operand
-    if ((rc = mixed_walkers_to_wt(SM, W, M, N, ldh, Wt_p, st))) return rc;
+    if (!mixed_green() && (rc = mixed_walkers_to_wt(SM, W, M, N, ldh, Wt_p, st))) return rc;  // else done with G
     UmmaEpilogue e1;
     e1.kind = UMMA_EPI_STORE_SPLIT;
     for (int q = 0; q < 3; ++q) e1.out[q] = Wt2_p[q];
@@ -1558,6 +1570,10 @@ int sfq_engine_destroy(sfq_engine_t h) {
   if (e.st) cudaStreamSynchronize(e.st);
   e.release_events();
   e.drop_graphs();
+  if (e.cst) cudaStreamSynchronize(e.cst);
+  if (e.uni_ready) cudaEventDestroy(e.uni_ready);
+  if (e.uni_free) cudaEventDestroy(e.uni_free);
+  if (e.cst) cudaStreamDestroy(e.cst);
   if (e.blk_done) cudaEventDestroy(e.blk_done);
   if (e.blk_host) cudaFreeHost(e.blk_host);
   if (e.arena) cudaFree(e.arena);
@@ -1640,10 +1656,26 @@ int sfq_engine_propagate_host(sfq_engine_t h, double Eshift, unsigned long long 
   int rc;
   const double* ud = nullptr;
   if (uniforms_host) {
-    SFQ_CUDA_TRY(cudaMemcpyAsync(e.uni, uniforms_host, sizeof(double) * e.W * e.Nc, cudaMemcpyHostToDevice, e.st));
+    // the copy overlaps the step's density and force bias; it starts once earlier work on the
+    // engine stream (a previous step's fields, which read the same buffer) is done
+    if (!e.cst) {
+      SFQ_CUDA_TRY(cudaStreamCreateWithFlags(&e.cst, cudaStreamNonBlocking));
+      SFQ_CUDA_TRY(cudaEventCreateWithFlags(&e.uni_ready, cudaEventDisableTiming));
+      SFQ_CUDA_TRY(cudaEventCreateWithFlags(&e.uni_free, cudaEventDisableTiming));
+    }
+    SFQ_CUDA_TRY(cudaEventRecord(e.uni_free, e.st));
+    SFQ_CUDA_TRY(cudaStreamWaitEvent(e.cst, e.uni_free, 0));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(e.uni, uniforms_host, sizeof(double) * e.W * e.Nc, cudaMemcpyHostToDevice, e.cst));
+    SFQ_CUDA_TRY(cudaEventRecord(e.uni_ready, e.cst));
+    e.uni_wait = e.uni_ready;
     ud = e.uni;
   }
-  if ((rc = e.propagate(Eshift, step, ud))) return rc;
+  rc = e.propagate(Eshift, step, ud);
+  if (e.uni_wait) {  // not consumed (an error before the fields): keep the stream order anyway
+    cudaStreamWaitEvent(e.st, e.uni_wait, 0);
+    e.uni_wait = nullptr;
+  }
+  if (rc) return rc;
   if (props_host)
     SFQ_CUDA_TRY(cudaMemcpyAsync(props_host, e.props, sizeof(cplx) * kNumProps * e.W, cudaMemcpyDeviceToHost, e.st));
   return e.sync_checked();

@@ -17,5 +17,9 @@ int mixed_build_v(const float* Cv, int W, int M, bool packed, void* const* pl, c
 int mixed_build_tblk(const cplx* Tinv, int W, int N, void* const* pl, cudaStream_t st);
 // SM (W, M, N) -> walker-operand planes WT[w][a][c * ldh + i]
 int mixed_walkers_to_wt(const cplx* SM, int W, int M, int N, int ldh, void* const* pl, cudaStream_t st);
+// one pass over SM: the planes of SM read as reals (ps, same layout) and the walker rows of
+// mixed_walkers_to_wt (pt)
+int mixed_walkers_split_both(const cplx* SM, int W, int M, int N, int ldh, void* const* ps, void* const* pt,
+                             cudaStream_t st);
 
 }  // namespace sfq

@@ -262,7 +262,45 @@ __global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, int ldh, Plan
   }
 }
 
+// the two operand layouts of the walkers in one pass over SM: the planes of SM read as reals (the G
+// product's B operand, same layout) and WT[w][a][c * ldh + i] (the P1 product's A operand)
+__global__ void walkers_split_both_kernel(const cplx* SM, int M, int N, int ldh, Planes PS, Planes PT) {
+  __shared__ cplx tile[32][33];
+  const int w = blockIdx.z;
+  const int i0 = blockIdx.y * 32, a0 = blockIdx.x * 32;
+  const cplx* S = SM + (long)w * M * N;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = i0 + r, a = a0 + threadIdx.x;
+    if (i < M && a < N) {
+      const cplx z = S[(long)i * N + a];
+      tile[r][threadIdx.x] = z;
+      const long e = 2 * (((long)w * M + i) * N + a);
+      split_store_d(z.x, PS, e);
+      split_store_d(z.y, PS, e + 1);
+    }
+  }
+  __syncthreads();
+  const long base = (long)w * N * 2 * ldh;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int a = a0 + r, i = i0 + threadIdx.x;
+    if (i < M && a < N) {
+      const cplx z = tile[threadIdx.x][r];
+      split_store_d(z.x, PT, base + ((long)a * 2 + 0) * ldh + i);
+      split_store_d(z.y, PT, base + ((long)a * 2 + 1) * ldh + i);
+    }
+  }
+}
+
 }  // namespace
+
+int mixed_walkers_split_both(const cplx* SM, int W, int M, int N, int ldh, void* const* ps, void* const* pt,
+                             cudaStream_t st) {
+  if (W > 65535) return record_error(SFQ_ERR_SHAPE, "walker split: too many walkers for one launch");
+  dim3 grid((N + 31) / 32, (M + 31) / 32, W), block(32, 8);
+  walkers_split_both_kernel<<<grid, block, 0, st>>>(SM, M, N, ldh, planes(ps), planes(pt));
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
 
 int mixed_split_planar(const cplx* src, int W, long E, void* const* pl, cudaStream_t st) {
   split_planar_kernel<<<grid_for((long)W * E), 256, 0, st>>>(src, W, E, planes(pl));

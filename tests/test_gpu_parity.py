@@ -300,14 +300,15 @@ def test_engine_host_step_matches_device_step():
     e2 = A.AfqmcEngine(s, 8, seed=3)
     Esh = e1.init()
     e2.init()
-    u = philox.uniforms(3, philox.STREAM_FIELDS, 0, 8, s.Nc)
     props = np.empty((8, 8), np.complex128)
-    e1.propagate_host(Esh, 0, u, props)
-    e2.propagate(Esh, 0)
-    SM1, p1 = e1.walkers()
-    SM2, p2 = e2.walkers()
-    assert np.array_equal(SM1, SM2)
-    assert np.array_equal(props[0], p2["WEIGHT"])
+    for step in range(3):  # consecutive host steps: each one's uniforms copied while the last is read
+        u = philox.uniforms(3, philox.STREAM_FIELDS, step, 8, s.Nc)
+        e1.propagate_host(Esh, step, u, props)
+        e2.propagate(Esh, step)
+        SM1, p1 = e1.walkers()
+        SM2, p2 = e2.walkers()
+        assert np.array_equal(SM1, SM2)
+        assert np.array_equal(props[0], p2["WEIGHT"])
     e1.close()
     e2.close()
 
