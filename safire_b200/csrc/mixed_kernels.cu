@@ -154,10 +154,17 @@ __global__ void __launch_bounds__(256) build_v_packed_kernel(const float* Cv, in
     rowbase[tid] = i * M - i * (i + 1) / 2;  // packed index of (i, k) = rowbase + k, k >= i
   }
   __syncthreads();
-  for (int e = tid; e < kVT * kVT; e += 256) {
-    const int r = e / kVT, q = e % kVT;
-    const int i = i0 + r, k = k0 + q;
-    if (i < M && k < M && i <= k) tile[r][q] = src[rowbase[r] + k];
+  {
+    // thread: column q of rows r0 + 4 s; all 16 loads issued before the first shared store
+    const int q = tid % kVT, r0 = tid / kVT;
+    float v[kVT / 4];
+#pragma unroll
+    for (int s = 0; s < kVT / 4; ++s) {
+      const int r = r0 + 4 * s, i = i0 + r, k = k0 + q;
+      v[s] = (i < M && k < M && i <= k) ? src[rowbase[r] + k] : 0.f;
+    }
+#pragma unroll
+    for (int s = 0; s < kVT / 4; ++s) tile[r0 + 4 * s][q] = v[s];
   }
   __syncthreads();
   for (int e = tid; e < kVT * kVT / 4; e += 256) {
