@@ -76,10 +76,26 @@ __global__ void reduce_planar_to_cplx_kernel(const float* C, int KS, long sk, in
   const long total = (long)W * E;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
     const long w = t / E, e = t % E;
+    const float* cr = C + w * E + e;
+    const float* ci = C + ((long)W + w) * E + e;
     double re = 0.0, im = 0.0;
-    for (int s = 0; s < KS; ++s) {
-      re += double(C[s * sk + w * E + e]);
-      im += double(C[s * sk + ((long)W + w) * E + e]);
+    int s = 0;
+    for (; s + 4 <= KS; s += 4) {  // four splits' loads in flight, added in the same order
+      float r[4], q[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        r[u] = cr[(s + u) * sk];
+        q[u] = ci[(s + u) * sk];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        re += double(r[u]);
+        im += double(q[u]);
+      }
+    }
+    for (; s < KS; ++s) {
+      re += double(cr[s * sk]);
+      im += double(ci[s * sk]);
     }
     out[t] = mk(alpha * re, alpha * im);
   }
@@ -270,31 +286,39 @@ __global__ void walkers_to_wt_kernel(const cplx* SM, int M, int N, int ldh, Plan
 }
 
 // the two operand layouts of the walkers in one pass over SM: the planes of SM read as reals (the G
-// product's B operand, same layout) and WT[w][a][c * ldh + i] (the P1 product's A operand)
+// product's B operand, same layout) and WT[w][a][c * ldh + i] (the P1 product's A operand).  A
+// 32 x 32 tile of SM goes through shared memory; every thread writes 4 consecutive values per plane
+// as one 8-byte word (N is a multiple of 4, M of 8).
 __global__ void walkers_split_both_kernel(const cplx* SM, int M, int N, int ldh, Planes PS, Planes PT) {
   __shared__ cplx tile[32][33];
   const int w = blockIdx.z;
   const int i0 = blockIdx.y * 32, a0 = blockIdx.x * 32;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
   const cplx* S = SM + (long)w * M * N;
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int i = i0 + r, a = a0 + threadIdx.x;
-    if (i < M && a < N) {
-      const cplx z = S[(long)i * N + a];
-      tile[r][threadIdx.x] = z;
-      const long e = 2 * (((long)w * M + i) * N + a);
-      split_store_d(z.x, PS, e);
-      split_store_d(z.y, PS, e + 1);
-    }
+    if (i < M && a < N) tile[r][threadIdx.x] = S[(long)i * N + a];
   }
   __syncthreads();
+  // SM as reals: row i, electrons a, a + 1 -> 4 consecutive doubles
+  for (int e = tid; e < 32 * 16; e += 256) {
+    const int r = e / 16, aa = 2 * (e % 16);
+    const int i = i0 + r, a = a0 + aa;
+    if (i >= M || a >= N) continue;  // a even and N a multiple of 4: a + 1 < N too
+    const cplx z0 = tile[r][aa], z1 = tile[r][aa + 1];
+    const double x[4] = {z0.x, z0.y, z1.x, z1.y};
+    split_store4_d(x, PS, 2 * (((long)w * M + i) * N + a));
+  }
+  // walker rows: electron a, part c, orbitals i .. i + 3
   const long base = (long)w * N * 2 * ldh;
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const int a = a0 + r, i = i0 + threadIdx.x;
-    if (i < M && a < N) {
-      const cplx z = tile[threadIdx.x][r];
-      split_store_d(z.x, PT, base + ((long)a * 2 + 0) * ldh + i);
-      split_store_d(z.y, PT, base + ((long)a * 2 + 1) * ldh + i);
-    }
+  for (int e = tid; e < 32 * 2 * 8; e += 256) {
+    const int aa = e / 16, c = (e / 8) % 2, ii = 4 * (e % 8);
+    const int a = a0 + aa, i = i0 + ii;
+    if (a >= N || i >= M) continue;  // i a multiple of 4 and M of 8: i + 3 < M too
+    double x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) x[u] = c ? tile[ii + u][aa].y : tile[ii + u][aa].x;
+    split_store4_d(x, PT, base + ((long)a * 2 + c) * ldh + i);
   }
 }
 
