@@ -177,12 +177,16 @@ __device__ __forceinline__ double block_max(double v, double* red) {
 }
 
 // |A|_1 * |A|_inf of the upper triangle of A (N x N row-major), |z| as |re| + |im|
+// position of (i, k), i <= k, in the packed upper triangle (rows of N - i entries)
+__device__ __forceinline__ int pku(int i, int k, int N) { return i * N - ((i * (i - 1)) >> 1) + (k - i); }
+
+// ||R||_1 * ||R||_inf of the packed upper-triangular R
 __device__ double norm1_inf_upper(const cplx* A, int N, double* red) {
   double rmax = 0.0, cmax = 0.0;
   for (int t = threadIdx.x; t < N; t += blockDim.x) {
     double rs = 0.0, cs = 0.0;
-    for (int k = t; k < N; ++k) rs += fabs(A[t * N + k].x) + fabs(A[t * N + k].y);
-    for (int i = 0; i <= t; ++i) cs += fabs(A[i * N + t].x) + fabs(A[i * N + t].y);
+    for (int k = t; k < N; ++k) rs += fabs(A[pku(t, k, N)].x) + fabs(A[pku(t, k, N)].y);
+    for (int i = 0; i <= t; ++i) cs += fabs(A[pku(i, t, N)].x) + fabs(A[pku(i, t, N)].y);
     rmax = fmax(rmax, rs);
     cmax = fmax(cmax, cs);
   }
@@ -191,25 +195,31 @@ __device__ double norm1_inf_upper(const cplx* A, int N, double* red) {
   return r * c;
 }
 
+// S = R^H R (right-looking upper Cholesky) and R^-1 for one Hermitian S per CTA, both on the packed
+// upper triangle in shared memory (N(N+1)/2 entries: two CTAs share an SM at N = 100, where the
+// barrier-bound sweeps of one CTA leave it mostly idle)
 __global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS, int N, int* status, int* again,
                                                                const int* active, double kappa_max, cplx* Rout) {
   const long b = blockIdx.x;
   if (active && !active[b]) return;  // the whole CTA
   extern __shared__ __align__(16) unsigned char sm_raw[];
   cplx* A = reinterpret_cast<cplx*>(sm_raw);
-  cplx* work = A + N * N;
+  cplx* work = A + N * (N + 1) / 2;
   __shared__ double diag[kMaxSmallN];
   __shared__ double red[32];
   __shared__ int s_bad;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = LU_THREADS / 32;
   cplx* Sb = S + b * sS;
-  for (int e = tid; e < N * N; e += LU_THREADS) A[e] = Sb[e];
+  for (int e = tid; e < N * N; e += LU_THREADS) {
+    const int i = e / N, k = e % N;
+    if (i <= k) A[pku(i, k, N)] = Sb[e];
+  }
   if (tid == 0) s_bad = 0;
   __syncthreads();
   // right-looking upper Cholesky: for j: r_jj = sqrt(a_jj); row j /= r_jj; trailing -= r_j^H r_j
   for (int j = 0; j < N; ++j) {
-    const double ajj = A[j * N + j].x;
+    const double ajj = A[pku(j, j, N)].x;
     if (!(ajj > 0.0)) {
       if (tid == 0 && s_bad == 0) s_bad = j + 1;
       break;
@@ -217,14 +227,16 @@ __global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS,
     const double rjj = sqrt(ajj);
     const double inv = 1.0 / rjj;
     __syncthreads();
+    const int rj = pku(j, j, N);  // row j, column k at rj + (k - j)
     for (int k = j + tid; k < N; k += LU_THREADS) {
-      A[j * N + k] = (k == j) ? mk(rjj, 0.0) : cscale(A[j * N + k], inv);
+      A[rj + (k - j)] = (k == j) ? mk(rjj, 0.0) : cscale(A[rj + (k - j)], inv);
     }
     __syncthreads();
     // A[i][k] -= conj(R[j][i]) * R[j][k] for j < i <= k
     for (int i = j + 1 + warp; i < N; i += NW) {
-      const cplx ci = cconj(A[j * N + i]);
-      for (int k = i + lane; k < N; k += 32) A[i * N + k] = csub(A[i * N + k], cmul(ci, A[j * N + k]));
+      const cplx ci = cconj(A[rj + (i - j)]);
+      const int ri = pku(i, i, N);
+      for (int k = i + lane; k < N; k += 32) A[ri + (k - i)] = csub(A[ri + (k - i)], cmul(ci, A[rj + (k - j)]));
     }
     __syncthreads();
   }
@@ -241,7 +253,7 @@ __global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS,
     cplx* Rb = Rout + b * sS;
     for (int e = tid; e < N * N; e += LU_THREADS) {
       const int i = e / N, k = e % N;
-      Rb[e] = (i > k) ? mk(0.0, 0.0) : A[e];
+      Rb[e] = (i > k) ? mk(0.0, 0.0) : A[pku(i, k, N)];
     }
     __syncthreads();  // every r_ii read before the diagonal below is replaced
   }
@@ -250,21 +262,23 @@ __global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS,
   // leaves the rows above at once (one rank-1 update per row, parallel over the block).  The
   // diagonal of R moves to diag[] and the in-place diagonal becomes the identity's.
   for (int i = tid; i < N; i += LU_THREADS) {
-    diag[i] = A[i * N + i].x;
-    A[i * N + i] = mk(1.0, 0.0);
+    diag[i] = A[pku(i, i, N)].x;
+    A[pku(i, i, N)] = mk(1.0, 0.0);
   }
   __syncthreads();
   for (int k = N - 1; k >= 0; --k) {
     const double xkk = 1.0 / diag[k];
-    for (int i = tid; i < k; i += LU_THREADS) work[i] = A[i * N + k];  // column k of R, read once
-    for (int jj = k + tid; jj < N; jj += LU_THREADS) A[k * N + jj] = cscale(A[k * N + jj], xkk);  // row k of R^-1
+    for (int i = tid; i < k; i += LU_THREADS) work[i] = A[pku(i, k, N)];  // column k of R, read once
+    const int rk = pku(k, k, N);
+    for (int jj = k + tid; jj < N; jj += LU_THREADS) A[rk + (jj - k)] = cscale(A[rk + (jj - k)], xkk);  // row k of R^-1
     __syncthreads();
     // pending rows above: P[i][j] -= R[i][k] X[k][j], where P[i][k] starts at 0 (the identity)
     for (int i = warp; i < k; i += NW) {
       const cplx rik = work[i];
+      const int ri = pku(i, i, N);
       for (int jj = k + lane; jj < N; jj += 32) {
-        const cplx base = (jj == k) ? mk(0.0, 0.0) : A[i * N + jj];
-        A[i * N + jj] = csub(base, cmul(rik, A[k * N + jj]));
+        const cplx base = (jj == k) ? mk(0.0, 0.0) : A[ri + (jj - i)];
+        A[ri + (jj - i)] = csub(base, cmul(rik, A[rk + (jj - k)]));
       }
     }
     __syncthreads();
@@ -272,8 +286,8 @@ __global__ void __launch_bounds__(LU_THREADS) chol_rinv_kernel(cplx* S, long sS,
   const double nX = norm1_inf_upper(A, N, red);
   // zero the strictly lower part (the GEMM W R^-1 reads the full square)
   for (int e = tid; e < N * N; e += LU_THREADS) {
-    int i = e / N, k = e % N;
-    Sb[e] = (i > k) ? mk(0.0, 0.0) : A[e];
+    const int i = e / N, k = e % N;
+    Sb[e] = (i > k) ? mk(0.0, 0.0) : A[pku(i, k, N)];
   }
   if (tid == 0) {
     status[b] = 0;
@@ -308,7 +322,7 @@ int chol_rinv(cplx* S, long sS, int nbatch, int N, int* status, int* again, cons
               cudaStream_t st, cplx* Rout) {
   if (nbatch <= 0 || N <= 0) return SFQ_OK;
   if (N > kMaxSmallN) return record_error(SFQ_ERR_UNSUPPORTED, "chol_rinv: N=%d exceeds %d", N, kMaxSmallN);
-  const size_t sm = lu_smem_bytes(N);
+  const size_t sm = size_t(N) * (N + 1) / 2 * sizeof(cplx) + size_t(N) * sizeof(cplx);  // packed R + work
   SFQ_CUDA_TRY(cudaFuncSetAttribute(chol_rinv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
   chol_rinv_kernel<<<nbatch, LU_THREADS, sm, st>>>(S, sS, N, status, again, active, kappa_max, Rout);
   SFQ_LAUNCHED();
