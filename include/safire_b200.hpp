@@ -109,9 +109,88 @@ class Engine {
   sfq_engine_t handle() const { return h_; }
   const sfq_engine_params_t& params() const { return p_; }
 
+  // run_afqmc's loop as one device-resident block replayed from a CUDA graph (sfq_engine_block);
+  // returns the measurements (10 doubles each), Eshift in/out
+  std::vector<double> run_block(const sfq_run_params_t& rp, double& Eshift) {
+    std::vector<double> meas(size_t(10) * 64);
+    int n = 0;
+    check(sfq_engine_block(h_, &rp, &Eshift, meas.data(), 64, &n));
+    meas.resize(size_t(10) * (n < 64 ? n : 64));
+    return meas;
+  }
+  // tile widths of the mixed-precision products: timed on this engine and kept, or set
+  sfq_tiles_t autotune(int repeats = 9) {
+    sfq_tiles_t t{};
+    check(sfq_engine_autotune(h_, repeats, &t));
+    return t;
+  }
+  void set_tiles(const sfq_tiles_t& t) { check(sfq_engine_set_tiles(h_, &t)); }
+
  private:
   sfq_engine_t h_ = nullptr;
   sfq_engine_params_t p_{};
+};
+
+// Several engines advanced together: one block of every member per CUDA graph launch
+class EngineGroup {
+ public:
+  explicit EngineGroup(const std::vector<Engine*>& members) {
+    std::vector<sfq_engine_t> hs;
+    for (Engine* e : members) hs.push_back(e->handle());
+    check(sfq_group_create(&g_, hs.data(), int(hs.size())));
+    n_ = int(hs.size());
+  }
+  ~EngineGroup() { sfq_group_destroy(g_); }
+  EngineGroup(const EngineGroup&) = delete;
+  EngineGroup& operator=(const EngineGroup&) = delete;
+  void set_lanes(int lanes) { check(sfq_group_set_lanes(g_, lanes)); }
+  // rps and Eshift per member (Eshift in/out); status per member; measurements at 10 * 64 * i
+  std::vector<double> run_block(const std::vector<sfq_run_params_t>& rps, std::vector<double>& Eshift,
+                                std::vector<int>& status, std::vector<int>& nmeas) {
+    std::vector<double> meas(size_t(10) * 64 * n_);
+    status.assign(n_, 0);
+    nmeas.assign(n_, 0);
+    check(sfq_group_block(g_, rps.data(), Eshift.data(), status.data(), meas.data(), 64, nmeas.data()));
+    return meas;
+  }
+
+ private:
+  sfq_group_t g_ = nullptr;
+  int n_ = 0;
+};
+
+// The request loop over resident systems (sfq_server_*)
+class Server {
+ public:
+  explicit Server(const sfq_server_params_t& p) { check(sfq_server_create(&s_, &p)); }
+  ~Server() { sfq_server_destroy(s_); }
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
+  int add_system(const sfq_engine_params_t& p, const double* hcore, const double* Likn, const ComplexType* PsiT) {
+    int id = -1;
+    check(sfq_server_add_system(s_, &p, hcore, Likn, PsiT, &id));
+    return id;
+  }
+  long long submit(int system, const sfq_run_params_t& rp) {
+    long long rid = -1;
+    check(sfq_server_submit(s_, system, &rp, &rid));
+    return rid;
+  }
+  int progress() {
+    int n = 0;
+    check(sfq_server_progress(s_, &n));
+    return n;
+  }
+  sfq_request_info_t request(long long rid, std::vector<double>* meas = nullptr) {
+    sfq_request_info_t info{};
+    std::vector<double> m(size_t(10) * 64);
+    check(sfq_server_request(s_, rid, &info, m.data(), 64));
+    if (meas) *meas = m;
+    return info;
+  }
+
+ private:
+  sfq_server_t s_ = nullptr;
 };
 
 // WalkerSet view of an engine (WalkerSetBase.h): size, properties, Slater matrices
