@@ -279,7 +279,8 @@ int sfq_engine_footprint(sfq_engine_t e, size_t* bytes);
  * for (64, 128, 160 with any plane count; 208, 256 with at most 2 planes).  sfq_engine_autotune
  * times every built width of each product on the engine's own operands (the current walkers; only
  * scratch buffers are written) and keeps the fastest: the G product, the force-bias product (its
- * K split follows from its width), the vHS product, the Taylor terms (taylor_half orbitals per
+ * width, and its K split: the one that fills whole waves of SMs or the smallest within 6 % of it,
+ * fewer partial sums to add), the vHS product, the Taylor terms (taylor_half orbitals per
  * tile: 16, 32, 64, 80, or 128 with at most 2 planes) and the two P1 products.  The widths change
  * how the output is tiled and, for the force bias, how many partial sums are reduced, so two
  * engines given the same tiles (sfq_engine_set_tiles; 0 = the built-in choice) produce identical
@@ -288,7 +289,7 @@ int sfq_engine_footprint(sfq_engine_t e, size_t* bytes);
  * and the chosen tiles (0 when a product was not timed).  No counterpart in the reference. */
 typedef struct {
   int g_bn, vbias_bn, vhs_bn, taylor_half, p1_bn;
-  int vbias_ksplit; /* out */
+  int vbias_ksplit; /* force-bias K split; set_tiles: 0 = planned from vbias_bn */
   double us_builtin[5];
   double us_tuned[5];
 } sfq_tiles_t;

@@ -310,8 +310,8 @@ class AfqmcEngine:
         check(lib().sfq_engine_tiles(self.h, ctypes.byref(t)))
         return t.choice()
 
-    def set_tiles(self, g_bn=0, vbias_bn=0, vhs_bn=0, taylor_half=0, p1_bn=0, **_):
-        t = capi.Tiles(g_bn, vbias_bn, vhs_bn, taylor_half, p1_bn)
+    def set_tiles(self, g_bn=0, vbias_bn=0, vhs_bn=0, taylor_half=0, p1_bn=0, vbias_ksplit=0):
+        t = capi.Tiles(g_bn, vbias_bn, vhs_bn, taylor_half, p1_bn, vbias_ksplit)
         check(lib().sfq_engine_set_tiles(self.h, ctypes.byref(t)))
 
     def footprint(self):

@@ -193,6 +193,7 @@ struct Engine {
   int vb_ks_max = 1;    // the most any vbias tile width can take (the partial-sum buffer's size)
   // tile widths of the products (0: the built-in choice), set by autotune() or set_tiles()
   int vb_bn = 128, vhs_bn = 0, p1_bn = 0, g_bn = 0;
+  int vb_ks_req = 0;  // a force-bias K split asked for (0: planned from the tile width)
   int tay_half = 0;     // orbitals per Taylor tile (tile width 2 * tay_half, re and im halves)
   int tay_req = 0;      // a Taylor tile asked for (0: the least padding)
   long vb_rows = 0;     // output columns of a Taylor product: ceil(M / tay_half) * 2 * tay_half
@@ -674,14 +675,16 @@ struct Engine {
     tay_half = best;
     vb_rows = 2 * best_pad;
     ldh = (M + 63) / 64 * 64;
-    vb_ks = plan_ks(vb_bn);
+    vb_ks = vb_ks_req ? vb_ks_req : plan_ks(vb_bn);
     vb_ks_max = 1;
     for (int bn : {32, 64, 128, 160, 208, 256}) vb_ks_max = std::max(vb_ks_max, plan_ks(bn));  // every width set_tiles takes
   }
 
   // vbias: tiles of width bn over (2W, Nc), K = N*M split so that the work units fill whole waves
   // of SMs (K splits write partial sums, reduced in a fixed order)
-  int plan_ks(int bn) const {
+  // (the smallest split reaching min_eff of whole waves when min_eff < 1: fewer partial sums to write
+  // and add, a little wave quantization traded for it)
+  int plan_ks(int bn, double min_eff = 0.999) const {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device);
     const long tiles = (long)((2 * W + 127) / 128) * ((Nc + bn - 1) / bn);
@@ -695,7 +698,7 @@ struct Engine {
         best_eff = eff;
         best = ks;
       }
-      if (eff > 0.999) break;
+      if (eff > min_eff) break;
     }
     return best;
   }
@@ -736,12 +739,17 @@ struct Engine {
   bool half_ok(int h) const { return h == 16 || h == 32 || h == 64 || h == 80 || (h == 128 && nplanes <= 2); }
 
   // set the tiles (0: the built-in choice); the captured block graphs are dropped
-  int set_tiles(int gbn, int vbbn, int vhsbn, int half, int p1bn) {
+  int set_tiles(int gbn, int vbbn, int vhsbn, int half, int p1bn, int vbks = 0) {
     if (!mixed) return record_error(SFQ_ERR_UNSUPPORTED, "tiles: only the mixed-precision products are tiled");
     for (int bn : {gbn, vbbn, vhsbn, p1bn})
       if (bn && !tile_built(bn))
         return record_error(SFQ_ERR_ARG, "tiles: width %d is not built for %d planes", bn, nplanes);
     if (half && !half_ok(half)) return record_error(SFQ_ERR_ARG, "tiles: Taylor half %d not built", half);
+    const long kt = ((long)N * M + 63) / 64;
+    if (vbks < 0 || vbks > vb_ks_max || vbks > kt)
+      return record_error(SFQ_ERR_ARG, "tiles: force-bias K split %d outside 0..%d", vbks,
+                          int(vb_ks_max < kt ? vb_ks_max : kt));
+    vb_ks_req = vbks;
     g_bn = gbn;
     vb_bn = vbbn ? vbbn : 128;
     vhs_bn = vhsbn;
@@ -801,7 +809,7 @@ struct Engine {
   }
 
   // the products with tile width bn (Taylor: half) on the operands the scratch buffers hold
-  int tune_product(int which, int bn) {
+  int tune_product(int which, int bn, int vbks = 0) {
     int rc;
     const long NM = (long)N * M, L2h = 2L * ldh, rows = 2L * W * N;
     switch (which) {
@@ -815,7 +823,7 @@ struct Engine {
         return tc_gemm(Tb_p, 2L * N, 4L * N * N, Ws_p, M, 2L * M * N, 2 * N, W, nullptr, 0, 0, 1.f, bn, &eg);
       }
       case 1: {
-        const int ks = plan_ks(bn);
+        const int ks = vbks ? vbks : plan_ks(bn);
         const long part = 2L * W * Nc;
         if ((rc = tc_gemm(Gs_p, 2L * W, 0, Lnak_p, Nc, 0, int(NM), 1, Cvb, Nc, 0, 1.f, bn, nullptr, ks, part)))
           return rc;
@@ -891,32 +899,44 @@ struct Engine {
     get_tiles(&cur);
     const int current[kTunedProducts] = {cur.g_bn, cur.vbias_bn, cur.vhs_bn, cur.taylor_half, cur.p1_bn};
     int chosen[kTunedProducts];
+    int chosen_ks = cur.vbias_ksplit;
     double t_cur[kTunedProducts] = {}, t_best[kTunedProducts] = {};
     for (int which = 0; which < kTunedProducts; ++which) {
-      std::vector<int> cand;
+      // candidates (width, force-bias K split; 0 elsewhere)
+      std::vector<std::pair<int, int>> cand;
       if (which == 3) {
         for (int h : {16, 32, 64, 80, 128})
-          if (half_ok(h)) cand.push_back(h);
+          if (half_ok(h)) cand.push_back({h, 0});
       } else {
-        for (int bn : {64, 128, 160, 208, 256})
-          if (tile_built(bn)) cand.push_back(bn);
+        for (int bn : {64, 128, 160, 208, 256}) {
+          if (!tile_built(bn)) continue;
+          if (which != 1) {
+            cand.push_back({bn, 0});
+            continue;
+          }
+          // the split that fills whole waves, and the smallest one within 6 % of it
+          const int k1 = plan_ks(bn), k2 = plan_ks(bn, 0.94);
+          cand.push_back({bn, k1});
+          if (k2 != k1) cand.push_back({bn, k2});
+        }
       }
       chosen[which] = current[which];
       if (which == 0 && !mixed_green()) continue;  // G comes from the FP64 density
       double best = 1e300;
-      for (int bn : cand) {
+      for (const auto& c : cand) {
         double us = 0.0;
-        if ((rc = time_median([&] { return tune_product(which, bn); }, reps, &us))) return rc;
-        if (bn == current[which]) t_cur[which] = us;
+        if ((rc = time_median([&] { return tune_product(which, c.first, c.second); }, reps, &us))) return rc;
+        if (c.first == current[which] && (which != 1 || c.second == cur.vbias_ksplit)) t_cur[which] = us;
         if (us < best) {
           best = us;
-          chosen[which] = bn;
+          chosen[which] = c.first;
+          if (which == 1) chosen_ks = c.second;
         }
       }
       t_best[which] = best;
     }
     if ((rc = sync_checked())) return rc;
-    if ((rc = set_tiles(chosen[0], chosen[1], chosen[2], chosen[3], chosen[4]))) return rc;
+    if ((rc = set_tiles(chosen[0], chosen[1], chosen[2], chosen[3], chosen[4], chosen_ks))) return rc;
     if (out) {
       get_tiles(out);
       for (int i = 0; i < kTunedProducts; ++i) {
@@ -1855,7 +1875,7 @@ int sfq_engine_autotune(sfq_engine_t h, int repeats, sfq_tiles_t* out) {
 
 int sfq_engine_set_tiles(sfq_engine_t h, const sfq_tiles_t* t) {
   if (!h || !t) return record_error(SFQ_ERR_ARG, "null pointer");
-  return h->e.set_tiles(t->g_bn, t->vbias_bn, t->vhs_bn, t->taylor_half, t->p1_bn);
+  return h->e.set_tiles(t->g_bn, t->vbias_bn, t->vhs_bn, t->taylor_half, t->p1_bn, t->vbias_ksplit);
 }
 
 int sfq_engine_tiles(sfq_engine_t h, sfq_tiles_t* t) {
