@@ -280,7 +280,9 @@ int sfq_engine_footprint(sfq_engine_t e, size_t* bytes);
  * times every built width of each product on the engine's own operands (the current walkers; only
  * scratch buffers are written) and keeps the fastest: the G product, the force-bias product (its
  * width, and its K split: the one that fills whole waves of SMs or the smallest within 6 % of it,
- * fewer partial sums to add), the vHS product, the Taylor terms (taylor_half orbitals per
+ * fewer partial sums to add; longer K ranges accumulate more FP32 rounding in the force bias, about
+ * as sqrt(K per range), so a caller that wants the tighter force bias sets the larger split), the
+ * vHS product, the Taylor terms (taylor_half orbitals per
  * tile: 16, 32, 64, 80, or 128 with at most 2 planes) and the two P1 products.  The widths change
  * how the output is tiled and, for the force bias, how many partial sums are reduced, so two
  * engines given the same tiles (sfq_engine_set_tiles; 0 = the built-in choice) produce identical
