@@ -30,6 +30,8 @@ struct GemmDesc {
   cplx alpha = {1.0, 0.0};
   cplx beta = {0.0, 0.0};
   const int* mask = nullptr;  // optional: batch b is computed only where mask[b] != 0
+  bool upper_only = false;    // C is needed on and above the diagonal only: tiles wholly below it are skipped
+  bool b_upper = false;       // B is upper triangular: column n of C needs K <= n only
 };
 
 int gemm_f64(const GemmDesc& d, cudaStream_t stream);
@@ -94,11 +96,13 @@ __global__ void __launch_bounds__(WM* WN * 32)
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   const long bz = blockIdx.z;
   if (d.mask && !d.mask[bz]) return;  // the whole CTA: batches left out by the mask
+  if (d.upper_only && m0 >= n0 + BN) return;  // every row of the tile is below every column
 
   const unsigned char* Ab = (const unsigned char*)d.A + bz * d.sAb * C_::A_ESZ;
   const unsigned char* Bb = (const unsigned char*)d.B + bz * d.sBb * C_::B_ESZ;
 
-  const int KT = (d.K + BKT - 1) / BKT;
+  const int Keff = d.b_upper && n0 + BN < d.K ? n0 + BN : d.K;  // B[k][n] = 0 for k > n
+  const int KT = (Keff + BKT - 1) / BKT;
 
   auto load_stage = [&](int stage, int kt) {
     unsigned char* As = smem + stage * C_::STAGE_BYTES;

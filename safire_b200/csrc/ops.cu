@@ -133,6 +133,7 @@ static int cholqr_pass(const cplx* Win, cplx* Wout, cplx* S, int* status, int* a
   d.B = Win; d.sBk = N; d.sBn = 1; d.sBb = (long)M * N; d.b_cplx = true;
   d.C = S; d.sCm = N; d.sCn = 1; d.sCb = (long)N * N;
   d.mask = mask;
+  d.upper_only = true;  // Hermitian: the Cholesky below reads the upper triangle only
   if ((rc = gemm_f64(d, st))) return rc;
   if ((rc = chol_rinv(S, (long)N * N, W, N, status, again, mask, kCholQrKappa, st, R))) return rc;
   GemmDesc q;  // Wout = Win R^-1
@@ -141,6 +142,7 @@ static int cholqr_pass(const cplx* Win, cplx* Wout, cplx* S, int* status, int* a
   q.B = S; q.sBk = N; q.sBn = 1; q.sBb = (long)N * N; q.b_cplx = true;
   q.C = Wout; q.sCm = N; q.sCn = 1; q.sCb = (long)M * N;
   q.mask = mask;
+  q.b_upper = true;  // R^-1 is upper triangular (its lower part stored as zeros)
   return gemm_f64(q, st);
 }
 
