@@ -249,7 +249,8 @@ def run_engine(args, cfg, spec, s, W, DT, prec, rank, local, profile_pass=True, 
     import torch
     from safire_b200 import afqmc, capi
     L = capi.lib()
-    eng = afqmc.AfqmcEngine(s, W, dt=DT, seed=1000 + rank, device=local, precision=prec)
+    from safire_b200 import replicas
+    eng = afqmc.AfqmcEngine(s, W, dt=DT, seed=replicas.seed_for(rank), device=local, precision=prec)
     state = {"Esh": eng.init()}
     ext = torch.cuda.ExternalStream(eng.stream)
     out = {}
@@ -305,7 +306,7 @@ def run_engine(args, cfg, spec, s, W, DT, prec, rank, local, profile_pass=True, 
         pbuf = torch.empty((args.steps, 8, W), dtype=torch.complex128).pin_memory()
         tmp = torch.empty((W, spec.Nc), dtype=torch.float64, device="cuda")
         for i in range(args.steps):
-            capi.check(L.sfq_field_uniforms(tmp.data_ptr(), 1000 + rank, s1 + i, W, spec.Nc, None))
+            capi.check(L.sfq_field_uniforms(tmp.data_ptr(), replicas.seed_for(rank), s1 + i, W, spec.Nc, None))
             ubuf[i].copy_(tmp.cpu())
         torch.cuda.synchronize()
         f0 = torch.cuda.Event(enable_timing=True)
@@ -350,14 +351,10 @@ def main():
         return
 
     import torch
-    from safire_b200 import capi, synthetic
+    from safire_b200 import capi, replicas, synthetic
 
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist = replicas.init(world, "nccl", timeout_s=300)
 
     spec = getattr(synthetic, cfg["spec"])
     W = cfg["nwalk"]
@@ -370,18 +367,14 @@ def main():
     eng, m = run_engine(args, cfg, spec, s, W, DT, prec, rank, local, e2e=not args.no_e2e)
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, device="cuda")
 
     ms = max_over_ranks(m["ms"])
-    value = W * args.steps * world / (ms * 1e-3)
+    value = replicas.job_rate(W * args.steps, world, ms)
     e2e = None
     if "e2e_ms" in m:
         ems = max_over_ranks(m["e2e_ms"])
-        e2e = {"value": W * args.steps * world / (ems * 1e-3), "unit": "walker-steps/s",
+        e2e = {"value": replicas.job_rate(W * args.steps, world, ems), "unit": "walker-steps/s",
                "h2d_bytes_per_step": m["e2e_bytes"][0], "d2h_bytes_per_step": m["e2e_bytes"][1],
                "path": "sfq_engine_propagate_host (pinned host uniforms in, walker properties out)"}
 
@@ -394,7 +387,7 @@ def main():
         eng64.close()
         del eng64
         ms64 = max_over_ranks(m64["ms"])
-        v64 = W * args.steps * world / (ms64 * 1e-3)
+        v64 = replicas.job_rate(W * args.steps, world, ms64)
         compare = {"fp64_value": v64, "fp64_ms_per_step": ms64 / args.steps, "speedup_vs_fp64": value / v64,
                    "block_energy_mixed": m["energy"], "block_energy_fp64": m64["energy"],
                    "block_energy_delta_mHa": 1e3 * (m["energy"] - m64["energy"]),
