@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 5 */
+int sfq_abi_version(void); /* 6 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -235,6 +235,10 @@ int sfq_engine_propagate_host(sfq_engine_t e, double Eshift, unsigned long long 
 int sfq_engine_orthogonalize(sfq_engine_t e);
 /* population_control (population_control.hpp:219-255), single rank; the comb draws Philox(seed, call) */
 int sfq_engine_population_control(sfq_engine_t e, unsigned long long call);
+/* the same with the comb's uniform r in [0, 1) from the caller: the draw comb takes from the walker set's
+ * generator (population_control.hpp:41-42, HostRandomGenerator::sampleUniformFields), so a caller that
+ * owns the reference's stream replays its population control exactly */
+int sfq_engine_population_control_uniform(sfq_engine_t e, double r);
 /* averagePseudoEnergy / averageEnergy / total weight (average_energy.hpp:33-76); host scalars out */
 int sfq_engine_averages(sfq_engine_t e, double* pseudo_energy, double* energy, double* total_weight);
 /* EnergyEstimator::measure (EnergyEstimator.h:51-100): out[0..9] = Energy(re,im), Onebody(re,im),

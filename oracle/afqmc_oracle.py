@@ -630,3 +630,72 @@ def run(ham, wset, prop, steps, Eshift, ortho_interval=10, pop_interval=10,
             record.append(dict(step=step, Eshift=Eshift, weight=wset.weight.copy(),
                                ovlp=wset.ovlp.copy(), pseudo_eloc=wset.pseudo_eloc.copy()))
     return Eshift, meas
+
+
+# --------------------------------------------------------------------------------------------
+# Seeded replay of one stage on the reference's own random streams (execute.cpp:117-190,
+# run_afqmc.cpp:69-104, EnergyEstimator.h:51-100, Measurements.hpp:96-147), one rank
+# --------------------------------------------------------------------------------------------
+def measure_step(ham, wset, step, dt):
+    """One bin of every observable EnergyEstimator::measure records at this step."""
+    E, ov = wfn_energy_noupdate(ham, wset)
+    w = wset.weight
+    den = np.sum(w)                                 # MeasurementOutput's denominator
+    avg = (w @ E) / den                             # gemv(transpose(E), weights)
+    aw = np.abs(w)
+    return {"Energy": complex(np.sum(avg)), "OnebodyEnergy": complex(avg[0]),
+            "ExchangeEnergy": complex(avg[1]), "CoulombEnergy": complex(avg[2]),
+            "Overlap": complex(np.sum(np.exp(ov) * w) / den),
+            "ProjectionTime": (step + 1) * dt,
+            "EffectiveNumWalkers": float(np.sum(aw) ** 2 / np.sum(aw * aw)),
+            "Phase": complex(np.sum(w) / np.sum(aw)), "TotalWeight": complex(np.sum(w))}
+
+
+def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, measure_interval=10,
+               equilibration_steps=0, relax=None, rank=0, **prop_args):
+    """execute_simulation + run_afqmc for one stage with HostRandomGenerator streams: walkers from
+    the trial (NOMSD::initial_guess), Energy + seedPseudoEnergy, Eshift = averageEnergy, then the
+    step loop.  Fields come from stream 1 (nwalk x nchol uniforms per step), the comb from stream 0.
+    Returns (initial Eshift, final Eshift, {observable: list of bins})."""
+    from .mt19937 import HostRandomGenerator, split_seed
+    walker_rng = HostRandomGenerator(split_seed(seed, rank, 0))
+    field_rng = HostRandomGenerator(split_seed(seed, rank, 1))
+    psi = np.conj(ham.PsiT.T)
+    wset = Walkers(np.broadcast_to(psi, (nwalk,) + psi.shape))
+    Eshift = init_walkers(ham, wset)
+    E_init = Eshift
+    prop = Propagator(ham, dt, **prop_args)
+    if relax is None:
+        relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
+    series = {}
+    for step in range(steps):
+        u = field_rng.uniforms(nwalk * ham.Nc).reshape(nwalk, ham.Nc)
+        prop.propagate(wset, Eshift, step, uniforms=u)
+        if step % ortho_interval == 0:
+            prop.orthogonalize(wset)
+        if step % pop_interval == 0:
+            population_control(wset, float(walker_rng.uniforms(1)[0]))
+        if step >= equilibration_steps:
+            if step % measure_interval == 0:
+                for k, v in measure_step(ham, wset, step, dt).items():
+                    series.setdefault(k, []).append(v)
+        else:
+            Eshift += relax * (average_pseudo_energy(wset, dt) - Eshift)
+    return E_init, Eshift, series
+
+
+def rebinned_average(series, rebinsize):
+    """safiretools Results.average with a given rebin size (python/safiretools/results/stats.py:55-100,
+    results.py:196-240): the series cut to whole bins, the mean of the bin means, and the standard
+    error std(bins, ddof=1) / sqrt(bins) of real and imaginary parts separately."""
+    s = np.asarray(series)
+    nb = s.shape[0] // rebinsize
+    if nb < 2:
+        raise ValueError("fewer than two bins")
+    bins = s[:nb * rebinsize].reshape(nb, rebinsize, *s.shape[1:]).mean(axis=1)
+    mean = bins.mean(axis=0)
+    if np.iscomplexobj(bins):
+        err = (np.std(bins.real, axis=0, ddof=1) + 1j * np.std(bins.imag, axis=0, ddof=1)) / math.sqrt(nb)
+    else:
+        err = np.std(bins, axis=0, ddof=1) / math.sqrt(nb)
+    return mean, err

@@ -242,8 +242,12 @@ class AfqmcEngine:
     def orthogonalize(self):
         check(lib().sfq_engine_orthogonalize(self.h))
 
-    def population_control(self, call):
-        check(lib().sfq_engine_population_control(self.h, int(call)))
+    def population_control(self, call=0, uniform=None):
+        """population_control: the comb draws Philox(seed, call), or takes `uniform` in [0, 1)."""
+        if uniform is None:
+            check(lib().sfq_engine_population_control(self.h, int(call)))
+        else:
+            check(lib().sfq_engine_population_control_uniform(self.h, float(uniform)))
 
     def averages(self):
         pe, e, tw = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()

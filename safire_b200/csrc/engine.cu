@@ -1059,12 +1059,14 @@ struct Engine {
     return SFQ_OK;
   }
 
-  int population_control(unsigned long long call) {
+  // the comb's uniform: Philox(seed, call), or r itself when r >= 0 (a caller's generator)
+  int population_control(unsigned long long call, double r = -1.0) {
     int rc;
     ph_begin(SFQ_PH_POPCONTROL);
     inv_cached = false;
-    if ((rc = sfq::population_control(SM, (long)M * N, wprops(), W, 0.0, p.seed, call, 1, pw, st,
-                                      dev_mode ? d_step : nullptr)))
+    const bool own = r >= 0.0;
+    if ((rc = sfq::population_control(SM, (long)M * N, wprops(), W, own ? r : 0.0, p.seed, call, own ? 0 : 1, pw, st,
+                                      dev_mode && !own ? d_step : nullptr)))
       return rc;
     ph_end(SFQ_PH_POPCONTROL);
     if (dev_mode) return SFQ_OK;  // the collapse flag stays on the device until the block ends
@@ -1704,6 +1706,12 @@ int sfq_engine_propagate_host(sfq_engine_t h, double Eshift, unsigned long long 
 int sfq_engine_orthogonalize(sfq_engine_t h) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
   return h->e.orthogonalize();
+}
+
+int sfq_engine_population_control_uniform(sfq_engine_t h, double r) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  if (!(r >= 0.0 && r < 1.0)) return record_error(SFQ_ERR_ARG, "comb uniform %g outside [0, 1)", r);
+  return h->e.population_control(0, r);
 }
 
 int sfq_engine_population_control(sfq_engine_t h, unsigned long long call) {

@@ -1,0 +1,56 @@
+"""Extract the BH seeded snapshot case of the reference's functional tests into bh_rhf_closed_snapshot.npz.
+
+    python tests/golden/make_bh_snapshot.py [SAFIRE source tree]
+
+The case (tests/functional/run_functional.py:195-245 with --snapshot; functional_cases.py:101-134):
+Hamiltonian afqmc_inputs/BH/afqmc_H_rhf_closed.h5 (dense Cholesky), trial afqmc_inputs/BH/afqmc_rhf_nomsd.h5
+(RHF, NOMSD, one determinant), CLOSED walkers, seed 42, 50 walkers, timestep 0.01, 20 steps, population
+control and measurement every step, orthogonalization every 10 steps, no equilibration, one rank.  The
+recorded results are snapshot_references/BH/dense_rhf_basis_closed/rhf_nomsd/closed/results.h5: for each
+observable the mean and error of its rebinned series (safiretools Results.average).
+
+Stored: the Hamiltonian and trial as the engine takes them (read by safire_b200.inputs), the run
+settings, and the recorded mean / error of every observable of the energy estimator.  The
+back-propagated and mixed RDM estimators the case also recorded are outside the path and not stored.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from safire_b200.h5read import H5File  # noqa: E402
+from safire_b200.inputs import load_dense_hamiltonian, load_nomsd_trial  # noqa: E402
+
+OBSERVABLES = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "Overlap", "ProjectionTime",
+               "EffectiveNumWalkers", "Phase", "TotalWeight")
+
+
+def main():
+    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    fn = os.path.join(src, "tests", "functional")
+    wfn = load_nomsd_trial(os.path.join(fn, "afqmc_inputs", "BH", "afqmc_rhf_nomsd.h5"))
+    ham = load_dense_hamiltonian(os.path.join(fn, "afqmc_inputs", "BH", "afqmc_H_rhf_closed.h5"), wfn["nup"])
+    res = H5File(os.path.join(fn, "snapshot_references", "BH", "dense_rhf_basis_closed", "rhf_nomsd", "closed",
+                              "results.h5"))
+    inp = json.loads(res["input_file"])
+    ex = inp["execute"]
+    settings = dict(seed=inp["seed"], nwalk=ex["num_walkers"], dt=ex["timestep"], steps=ex["steps"],
+                    ortho_interval=ex["walker_ortho_interval"], pop_interval=ex["population_control_interval"],
+                    measure_interval=ex["measure_interval"], equilibration_steps=ex["equilibration_steps"],
+                    num_ranks=int(res["num_ranks"]), walker_type=ex["walker_set"]["walker_type"])
+    out = dict(hcore=ham["hcore"], Likn=ham["Likn"], PsiT=wfn["PsiT"], E0=np.float64(ham["E0"]),
+               settings=json.dumps(settings))
+    for k in OBSERVABLES:
+        out[f"mean_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/mean"])
+        out[f"error_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/error"])
+    path = os.path.join(HERE, "bh_rhf_closed_snapshot.npz")
+    np.savez_compressed(path, **out)
+    print(path, settings)
+
+
+if __name__ == "__main__":
+    main()

@@ -22,3 +22,28 @@ def sdet_kats():
         else:
             out[key] = v
     return out
+
+
+SNAPSHOT_OBSERVABLES = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "Overlap", "ProjectionTime",
+                        "EffectiveNumWalkers", "Phase", "TotalWeight")
+
+
+def bh_snapshot():
+    """The BH seeded snapshot case (make_bh_snapshot.py): inputs, settings and recorded (mean, error)."""
+    z = np.load(os.path.join(HERE, "bh_rhf_closed_snapshot.npz"))
+    rec = {k: (z[f"mean_{k}"][()], z[f"error_{k}"][()]) for k in SNAPSHOT_OBSERVABLES}
+    return dict(hcore=z["hcore"], Likn=z["Likn"], PsiT=z["PsiT"], E0=float(z["E0"]),
+                settings=json.loads(str(z["settings"])), recorded=rec)
+
+
+def snapshot_match(series, recorded, rebinned_average, tol=1e-9):
+    """The rebin size at which the series reproduces the recorded mean and error the way the
+    reference's snapshot comparison does (np.allclose, rtol = atol = 1e-9), or None.  The recorded
+    numbers came from safiretools' own choice of rebin size; every size with at least two bins is
+    tried."""
+    m_ref, e_ref = recorded
+    for B in range(1, len(series) // 2 + 1):
+        m, e = rebinned_average(series, B)
+        if np.allclose(m, m_ref, rtol=tol, atol=tol) and np.allclose(e, e_ref, rtol=tol, atol=tol):
+            return B
+    return None

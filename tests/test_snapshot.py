@@ -1,0 +1,93 @@
+"""The reference's seeded snapshot of a real molecule, replayed on its own random streams.
+
+The BH case of the reference's functional tests (dense Cholesky Hamiltonian, RHF NOMSD trial,
+CLOSED walkers, seed 42, 50 walkers, 20 steps, one rank) recorded every energy-estimator
+observable; the reference's runner requires a rerun to reproduce them to 1e-9.  These tests pin:
+
+  * the host random streams (std::mt19937 via split_seed, uniform_real_distribution) against the
+    C++ standard's known answer and numpy's independent MT19937;
+  * the oracle's whole stage -- vbias, fields, vHS, P1 * Taylor * P1, overlaps, walker update,
+    orthogonalization, comb, energies and the estimator -- against the recorded snapshot;
+  * the HDF5 reader and the input loaders against the reference's own files, where those are
+    present (they are only read when the fixture is regenerated).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import afqmc_oracle as O
+from oracle.mt19937 import MT19937, HostRandomGenerator, split_seed
+from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, snapshot_match
+
+REF = "/root/reference/tests/functional"
+
+
+def test_mt19937_known_answers():
+    # C++ [rand.predef]: the 10000th consecutive invocation of a default-constructed mt19937 produces 4123659995
+    assert MT19937().raw(10000)[-1] == 4123659995
+    for seed in (0, 42, split_seed(42, 0, 1)):
+        a = MT19937(seed).raw(1500).astype(np.uint64)
+        b = np.random.RandomState(seed & 0xFFFFFFFF).randint(0, 2**32, size=1500, dtype=np.uint64)
+        assert np.array_equal(a, b)
+
+
+def test_uniforms_from_two_draws():
+    g, h = HostRandomGenerator(7), MT19937(7)
+    u = g.uniforms(1000)
+    r = h.raw(2000).astype(np.float64).reshape(-1, 2)
+    assert np.array_equal(u, (r[:, 0] + r[:, 1] * 2.0**32) / 2.0**64)
+    assert np.all((u >= 0.0) & (u < 1.0))
+
+
+def test_split_seed_streams_distinct():
+    seeds = {split_seed(42, rank, stream) for rank in range(64) for stream in range(4)}
+    assert len(seeds) == 256
+    assert all(0 <= s < 2**64 for s in seeds)
+
+
+def test_oracle_reproduces_reference_snapshot():
+    snap = bh_snapshot()
+    st = snap["settings"]
+    assert st["num_ranks"] == 1 and st["walker_type"] == "CLOSED"
+    ham = O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
+    _, _, series = O.run_seeded(ham, st["nwalk"], st["dt"], st["steps"], st["seed"],
+                                ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
+                                measure_interval=st["measure_interval"],
+                                equilibration_steps=st["equilibration_steps"])
+    for k in SNAPSHOT_OBSERVABLES:
+        assert len(series[k]) == st["steps"]
+        B = snapshot_match(series[k], snap["recorded"][k], O.rebinned_average)
+        assert B is not None, (k, snap["recorded"][k])
+
+
+def test_snapshot_detects_a_planted_mistake():
+    """A field stream off by one draw, or one other seed, no longer reproduces the snapshot."""
+    snap = bh_snapshot()
+    st = snap["settings"]
+    ham = O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
+    _, _, series = O.run_seeded(ham, st["nwalk"], st["dt"], st["steps"], st["seed"] + 1,
+                                ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
+                                measure_interval=st["measure_interval"])
+    assert snapshot_match(series["Energy"], snap["recorded"]["Energy"], O.rebinned_average) is None
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="the reference's input files are not on this machine")
+def test_loaders_read_reference_files():
+    from safire_b200.h5read import H5File
+    from safire_b200.inputs import InputError, load_dense_hamiltonian, load_nomsd_trial
+    snap = bh_snapshot()
+    wfn = load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_rhf_nomsd.h5")
+    ham = load_dense_hamiltonian(f"{REF}/afqmc_inputs/BH/afqmc_H_rhf_closed.h5", wfn["nup"])
+    assert np.array_equal(ham["hcore"], snap["hcore"]) and np.array_equal(ham["Likn"], snap["Likn"])
+    assert np.array_equal(wfn["PsiT"], snap["PsiT"]) and ham["E0"] == snap["E0"]
+    f = H5File(f"{REF}/afqmc_inputs/BH/afqmc_H_rhf_closed.h5")
+    assert f.keys("Hamiltonian") == ["DenseFactorized", "X", "hcore"]
+    assert f.shape("Hamiltonian/DenseFactorized/L") == (1, 1, 19, 1, 19, 78)
+    # what the CLOSED single-determinant dense path does not take is refused with the reason
+    with pytest.raises(InputError):
+        load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_uhf_nomsd.h5")       # collinear trial
+    with pytest.raises(InputError):
+        load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_casci_rhf_nomsd.h5")  # several determinants
+    with pytest.raises(InputError):
+        load_dense_hamiltonian(f"{REF}/afqmc_inputs/BH/afqmc_H_rhf_noncollinear.h5", 3)
