@@ -41,7 +41,9 @@ zgetrf / zgetri / zgeqrf / zungqr from scipy's OpenBLAS, and numpy's eigh (zheev
 
 Auxiliary fields come from ``oracle.philox`` (Philox-4x32-10, stream 1); the comb draws from
 stream 0.  The reference uses mt19937 here (src/utilities/Random.hpp:37-51); the injection
-point ``sampleUniformFields`` is the same.
+point ``sampleUniformFields`` is the same.  ``run_seeded`` replays a whole stage on the reference's
+own streams (``oracle.mt19937``) and reproduces the reference's recorded seeded BH run
+(tests/functional/snapshot_references/BH/dense_rhf_basis_closed/rhf_nomsd/closed) to ~1e-14.
 """
 import math
 

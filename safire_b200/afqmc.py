@@ -260,6 +260,40 @@ class AfqmcEngine:
         keys = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "TotalWeight")
         return {k: complex(o[2 * i], o[2 * i + 1]) for i, k in enumerate(keys)}
 
+    def run_with_streams(self, steps, Eshift, field_uniforms, comb_uniform, ortho_interval=10, pop_interval=10,
+                         equilibration_steps=100, measure_interval=10, relax=None, step0=0):
+        """run_afqmc's step loop (run_afqmc.cpp:69-104) with the caller's random streams at the
+        reference's two injection points: field_uniforms(n) returns the n = nwalk * nchol uniforms
+        of a step (walker-major, assemble_X's sampleUniformFields) and comb_uniform() the comb's
+        uniform (population_control.hpp:41-42).  Given the reference's own generators it replays
+        a reference run.  Every measurement records EnergyEstimator::measure's observables
+        (EnergyEstimator.h:51-100).  Returns (Eshift, {observable: list of bins})."""
+        if relax is None:
+            relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
+        series = {}
+        for step in range(step0, step0 + steps):
+            u = np.ascontiguousarray(np.asarray(field_uniforms(self.W * self.Nc), np.float64).reshape(self.W, self.Nc))
+            self.propagate_host(Eshift, step, uniforms_host=u)
+            if step % ortho_interval == 0:
+                self.orthogonalize()
+            if step % pop_interval == 0:
+                self.population_control(uniform=float(comb_uniform()))
+            if step >= equilibration_steps:
+                if step % measure_interval == 0:
+                    m = self.measure()
+                    _, pr = self.walkers()
+                    w, ov = pr["WEIGHT"], pr["OVLP"]
+                    aw = np.abs(w)
+                    m["Overlap"] = complex(np.sum(np.exp(ov) * w) / np.sum(w))
+                    m["ProjectionTime"] = (step + 1) * self.dt
+                    m["EffectiveNumWalkers"] = float(np.sum(aw) ** 2 / np.sum(aw * aw))
+                    m["Phase"] = complex(np.sum(w) / np.sum(aw))
+                    for k, v in m.items():
+                        series.setdefault(k, []).append(v)
+            else:
+                Eshift += relax * (self.averages()[0] - Eshift)
+        return Eshift, series
+
     def run(self, steps, Eshift, ortho_interval=10, pop_interval=10, equilibration_steps=100, measure_interval=10,
             relax=0.0, step0=0, max_meas=4096, steer=False):
         rp = capi.RunParams(steps, ortho_interval, pop_interval, equilibration_steps, measure_interval, relax, step0,

@@ -1,4 +1,5 @@
-"""Extract the BH seeded snapshot case of the reference's functional tests into bh_rhf_closed_snapshot.npz.
+"""Extract the BH case of the reference's functional tests: the seeded snapshot into
+bh_rhf_closed_snapshot.npz, the statistical reference into bh_rhf_closed_statistical.json.
 
     python tests/golden/make_bh_snapshot.py [SAFIRE source tree]
 
@@ -12,6 +13,10 @@ observable the mean and error of its rebinned series (safiretools Results.averag
 Stored: the Hamiltonian and trial as the engine takes them (read by safire_b200.inputs), the run
 settings, and the recorded mean / error of every observable of the energy estimator.  The
 back-propagated and mixed RDM estimators the case also recorded are outside the path and not stored.
+
+The statistical reference (statistical_references/BH/dense_rhf_basis_closed/rhf_nomsd/closed/results.h5)
+is the same case run long: its settings (walkers per rank x ranks, steps, equilibration, intervals) and
+the mean / error of the energy observables after equilibration.
 """
 import json
 import os
@@ -50,6 +55,24 @@ def main():
     path = os.path.join(HERE, "bh_rhf_closed_snapshot.npz")
     np.savez_compressed(path, **out)
     print(path, settings)
+
+    res = H5File(os.path.join(fn, "statistical_references", "BH", "dense_rhf_basis_closed", "rhf_nomsd", "closed",
+                              "results.h5"))
+    inp = json.loads(res["input_file"])
+    ex = inp["execute"]
+    ranks = int(res["num_ranks"])
+    nwalk = ex["num_walkers"] if "num_walkers" in ex else ex["n_walkers_per_mpi_task"] * ranks
+    stat = dict(seed=inp["seed"], nwalk=nwalk, num_ranks=ranks, dt=ex["timestep"], steps=ex["steps"],
+                ortho_interval=ex["walker_ortho_interval"], pop_interval=ex["population_control_interval"],
+                measure_interval=ex["measure_interval"], equilibration_steps=ex["equilibration_steps"],
+                walker_type=ex["walker_set"]["walker_type"], recorded={})
+    for k in ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy"):
+        m, e = complex(res[f"measurements/Stage0/{k}/mean"]), complex(res[f"measurements/Stage0/{k}/error"])
+        stat["recorded"][k] = dict(mean=[m.real, m.imag], error=[e.real, e.imag])
+    path = os.path.join(HERE, "bh_rhf_closed_statistical.json")
+    with open(path, "w") as f:
+        json.dump(stat, f, indent=1)
+    print(path, {k: v for k, v in stat.items() if k != "recorded"})
 
 
 if __name__ == "__main__":

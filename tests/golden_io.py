@@ -47,3 +47,21 @@ def snapshot_match(series, recorded, rebinned_average, tol=1e-9):
         if np.allclose(m, m_ref, rtol=tol, atol=tol) and np.allclose(e, e_ref, rtol=tol, atol=tol):
             return B
     return None
+
+
+def bh_statistical():
+    """The BH statistical reference (make_bh_snapshot.py): settings and recorded mean / error."""
+    with open(os.path.join(HERE, "bh_rhf_closed_statistical.json")) as f:
+        s = json.load(f)
+    s["recorded"] = {k: (complex(*v["mean"]), complex(*v["error"])) for k, v in s["recorded"].items()}
+    return s
+
+
+def statistically_equal(a, a_err, b, b_err, significance=0.001, components=1):
+    """The reference's statistical comparison (run_functional.py:384-412): |a - b| within
+    z * sqrt(|a_err|^2 + |b_err|^2), z the two-sided normal quantile at the Bonferroni-adjusted
+    significance, or within 1e-9 * (1 + |b|)."""
+    from scipy.stats import norm
+    z = norm.ppf(1 - significance / (2 * components))
+    tol = max(z * float(np.hypot(abs(a_err), abs(b_err))), 1e-9 * (1 + abs(b)))
+    return abs(a - b) <= tol, abs(a - b), tol

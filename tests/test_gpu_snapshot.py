@@ -24,31 +24,16 @@ def _engine_series(snap):
     Nc = snap["Likn"].shape[2]
     system = synthetic.System(synthetic.SystemSpec(M=M, N=N, Nc=Nc, decay=0.0), snap["hcore"], snap["Likn"],
                               snap["PsiT"], snap["E0"])
-    W, dt = st["nwalk"], st["dt"]
-    eng = A.AfqmcEngine(system, W, dt=dt, seed=0, precision=capi.PRECISION_FP64)
+    eng = A.AfqmcEngine(system, st["nwalk"], dt=st["dt"], seed=0, precision=capi.PRECISION_FP64)
     walker_rng = HostRandomGenerator(split_seed(st["seed"], 0, 0))
     field_rng = HostRandomGenerator(split_seed(st["seed"], 0, 1))
-    Eshift = eng.init()
-    series = {k: [] for k in SNAPSHOT_OBSERVABLES}
-    for step in range(st["steps"]):
-        u = np.ascontiguousarray(field_rng.uniforms(W * Nc).reshape(W, Nc))
-        eng.propagate_host(Eshift, step, uniforms_host=u)
-        if step % st["ortho_interval"] == 0:
-            eng.orthogonalize()
-        if step % st["pop_interval"] == 0:
-            eng.population_control(uniform=float(walker_rng.uniforms(1)[0]))
-        m = eng.measure()
-        _, pr = eng.walkers()
-        w, ov = pr["WEIGHT"], pr["OVLP"]
-        aw = np.abs(w)
-        for k in ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "TotalWeight"):
-            series[k].append(m[k])
-        series["Overlap"].append(complex(np.sum(np.exp(ov) * w) / np.sum(w)))
-        series["ProjectionTime"].append((step + 1) * dt)
-        series["EffectiveNumWalkers"].append(float(np.sum(aw) ** 2 / np.sum(aw * aw)))
-        series["Phase"].append(complex(np.sum(w) / np.sum(aw)))
+    E_init = eng.init()
+    _, series = eng.run_with_streams(st["steps"], E_init, field_rng.uniforms, lambda: walker_rng.uniforms(1)[0],
+                                     ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
+                                     equilibration_steps=st["equilibration_steps"],
+                                     measure_interval=st["measure_interval"])
     eng.close()
-    return Eshift, series
+    return E_init, series
 
 
 def test_engine_reproduces_reference_snapshot():
