@@ -231,12 +231,110 @@ class Hamiltonian:
         shift = self.vHS(np.asarray(vMF, np.complex128)[None, :], dt)[0]
         return dt * self.hcore + dt * self.v0 + shift
 
+    # the walker type's view of the NOMSD trial (NOMSD.hpp:293-343, NOMSD.cpp:280-300): CLOSED walkers
+    # are one (M, N) Slater matrix, the overlap counts it twice
+    def green(self, SM):
+        G, ov = mixed_density_matrix(self.PsiT, SM, compact=True)
+        return G, 2.0 * ov
+
+    def log_overlap(self, SM):
+        return log_overlap_closed(self.PsiT, SM)
+
+    def trial_walker(self):
+        return np.conj(self.PsiT.T)
+
+    def orthogonalize(self, SM):
+        return orthogonalize(SM)[0]
+
+
+class CollinearHamiltonian(Hamiltonian):
+    """The same dense Hamiltonian for COLLINEAR walkers and a single-determinant NOMSD trial with
+    PsiT_up (nup, M) and PsiT_dn (ndn, M).  A walker is one (M, nup + ndn) matrix, the up columns
+    first (the reference keeps the two blocks one after the other, WalkerSetBase.h:256-264).
+
+      half rotation   haj = [PsiT_up; PsiT_dn] hcore, Lnak per spin (RealDenseHamiltonian.cpp:141-161)
+      G, overlap      MixedDensityMatrix per spin into the rows of one compact G, the overlaps
+                      accumulated (NOMSD.hpp:293-343); + log(conj(ci)) (NOMSD.cpp:174-177)
+      vbias           a = sqrt(dt), the two spins' G Lnak^T summed (Real3IndexFactorization.hpp:328-390)
+      energy          E1 and exchange per spin with scl = 1, Coulomb 0.5 (Kl_up + Kl_dn)^2 (:138-174, :476-590)
+      P1, vHS         one for both spins: the Hamiltonian is spin-independent (AFQMCBasePropagator.cpp:128-160)
+      orthogonalize   each spin block on its own (orthogonalize.hpp:135-169)
+    """
+
+    def __init__(self, hcore, Likn, PsiT_up, PsiT_dn, E0=0.0, ci=1.0):
+        super().__init__(hcore, Likn, PsiT_up, E0)
+        self.PsiT_up = np.asarray(PsiT_up, dtype=np.complex128)
+        self.PsiT_dn = np.asarray(PsiT_dn, dtype=np.complex128)
+        self.nup, self.ndn = self.PsiT_up.shape[0], self.PsiT_dn.shape[0]
+        self.ci = complex(ci)
+        M, Nc = self.M, self.Nc
+        self.N = self.nup + self.ndn
+        self.haj = np.concatenate([self.PsiT_up, self.PsiT_dn]) @ self.hcore.astype(np.complex128)
+        L2 = self.Likn.reshape(M, M * Nc)
+        self.Lnak_s = []
+        for P in (self.PsiT_up, self.PsiT_dn):
+            Lak_n = (P.real @ L2 + 1j * (P.imag @ L2)).reshape(P.shape[0], M, Nc)
+            self.Lnak_s.append(np.ascontiguousarray(np.transpose(Lak_n, (2, 0, 1))))
+        self.Lnak = np.concatenate(self.Lnak_s, axis=1)   # (Nc, nup + ndn, M)
+
+    def _lci(self):
+        return np.log(1e-12 if abs(self.ci) < 1e-12 else np.conj(self.ci))
+
+    def green(self, SM):
+        G_up, ov = mixed_density_matrix(self.PsiT_up, SM[:, :, :self.nup], compact=True)
+        G_dn, ov = mixed_density_matrix(self.PsiT_dn, SM[:, :, self.nup:], compact=True, ovlp=ov)
+        return np.concatenate([G_up, G_dn], axis=1), ov + self._lci()
+
+    def log_overlap(self, SM):
+        ov = log_overlap(self.PsiT_up, SM[:, :, :self.nup])
+        return log_overlap(self.PsiT_dn, SM[:, :, self.nup:], ovlp=ov) + self._lci()
+
+    def trial_walker(self):
+        return np.concatenate([np.conj(self.PsiT_up.T), np.conj(self.PsiT_dn.T)], axis=1)
+
+    def orthogonalize(self, SM):
+        up = orthogonalize(SM[:, :, :self.nup])[0]
+        dn = orthogonalize(SM[:, :, self.nup:])[0] if self.ndn else SM[:, :, self.nup:]
+        return np.concatenate([up, dn], axis=2)
+
+    def vbias(self, G, dt):
+        W = G.shape[0]
+        a = math.sqrt(dt)
+        v = np.zeros((W, self.Nc), np.complex128)
+        rows = ((0, self.nup), (self.nup, self.N))
+        for s, (r0, r1) in enumerate(rows):
+            if r1 > r0:
+                v += G[:, r0:r1, :].reshape(W, -1) @ self.Lnak_s[s].reshape(self.Nc, -1).T
+        return a * v
+
+    def energy(self, G, addH1=True, addEJ=True, addEXX=True, chunk=None):
+        W = G.shape[0]
+        M, Nc = self.M, self.Nc
+        E = np.zeros((W, 3), dtype=np.complex128)
+        Kl = np.zeros((W, Nc), dtype=np.complex128)
+        if addH1:
+            E[:, 0] = self.E0
+        for s, (r0, r1) in enumerate(((0, self.nup), (self.nup, self.N))):
+            n = r1 - r0
+            if n == 0:
+                continue
+            Gs = G[:, r0:r1, :]
+            if addH1:
+                E[:, 0] += np.einsum('waj,aj->w', Gs, self.haj[r0:r1])
+            if addEXX:
+                Lc = self.Lnak_s[s].reshape(Nc * n, M)
+                T = (Gs.reshape(W * n, M) @ Lc.T).reshape(W, n, Nc, n)   # T[w,b,n,a]
+                E[:, 1] += -0.5 * np.einsum('wanb,wbna->w', T, T)
+                if addEJ:
+                    Kl += np.einsum('wana->wn', T)
+        if addEJ:
+            E[:, 2] += 0.5 * np.einsum('wn,wn->w', Kl, Kl)
+        return E
+
 
 def trial_density(ham):
-    """G of the trial against itself (NOMSD::vMF: MixedDensityMatrix(PsiT, PsiT^H))."""
-    B = np.conj(ham.PsiT.T)[None, :, :]
-    G, _ = mixed_density_matrix(ham.PsiT, B, compact=True)
-    return G
+    """G of the trial against itself (NOMSD::vMF: MixedDensityMatrix(PsiT, PsiT^H), NOMSD.cpp:437-466)."""
+    return ham.green(ham.trial_walker()[None])[0]
 
 
 def vMF(ham, dt):
@@ -548,7 +646,7 @@ class Propagator:
     def propagate(self, wset, Eshift, step, target_population=None, uniforms=None):
         ham = self.ham
         W = wset.size()
-        G, _ = mixed_density_matrix(ham.PsiT, wset.SM, compact=True)
+        G, _ = ham.green(wset.SM)
         vb = ham.vbias(G, self.dt)
         if uniforms is None:
             uniforms = philox.uniforms(self.seed, philox.STREAM_FIELDS, step, W, ham.Nc)
@@ -556,21 +654,20 @@ class Propagator:
         mf = meanfield_factor(X, self.vmf)
         V = ham.vHS(X, self.dt)
         wset.SM = propagate(wset.SM, self.P1, V, self.order)
-        new_ov = log_overlap_closed(ham.PsiT, wset.SM)
+        new_ov = ham.log_overlap(wset.SM)
         walker_update(wset, self.dt, Eshift, ham.E0, new_ov, mf, HW, self.lower, self.upper)
         tp = W if target_population is None else target_population
         bound_walker_weights(wset, tp, self.wfloor, self.wfrac)
         return dict(G=G, vbias=vb, X=X, HW=HW, mf=mf, vHS=V, new_ovlp=new_ov)
 
     def orthogonalize(self, wset):
-        wset.SM, _ = orthogonalize(wset.SM)
-        wset.ovlp = log_overlap_closed(self.ham.PsiT, wset.SM)
+        wset.SM = self.ham.orthogonalize(wset.SM)
+        wset.ovlp = self.ham.log_overlap(wset.SM)
 
 
 def wfn_energy(ham, wset):
     """NOMSD::Energy(wset) (NOMSD.cpp:159-217 / :64-75): writes E1_, EXX_, EJ_, OVLP."""
-    G, ov = mixed_density_matrix(ham.PsiT, wset.SM, compact=True)
-    ov = 2.0 * ov
+    G, ov = ham.green(wset.SM)
     E = ham.energy(G)
     wset.ovlp = ov
     wset.e1, wset.exx, wset.ej = E[:, 0].copy(), E[:, 1].copy(), E[:, 2].copy()
@@ -598,8 +695,8 @@ def measure_energy(ham, wset):
 
 
 def wfn_energy_noupdate(ham, wset):
-    G, ov = mixed_density_matrix(ham.PsiT, wset.SM, compact=True)
-    return ham.energy(G), 2.0 * ov
+    G, ov = ham.green(wset.SM)
+    return ham.energy(G), ov
 
 
 def init_walkers(ham, wset):
@@ -662,7 +759,7 @@ def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, 
     from .mt19937 import HostRandomGenerator, split_seed
     walker_rng = HostRandomGenerator(split_seed(seed, rank, 0))
     field_rng = HostRandomGenerator(split_seed(seed, rank, 1))
-    psi = np.conj(ham.PsiT.T)
+    psi = ham.trial_walker()
     wset = Walkers(np.broadcast_to(psi, (nwalk,) + psi.shape))
     Eshift = init_walkers(ham, wset)
     E_init = Eshift

@@ -1,17 +1,20 @@
-"""Extract the BH case of the reference's functional tests: the seeded snapshot into
-bh_rhf_closed_snapshot.npz, the statistical reference into bh_rhf_closed_statistical.json.
+"""Extract the dense-Cholesky NOMSD cases of the reference's functional tests: the seeded snapshots
+of BH with CLOSED walkers (bh_rhf_closed_snapshot.npz), BH with a UHF trial and COLLINEAR walkers
+(bh_uhf_collinear_snapshot.npz) and Li with a polarized ROHF trial and COLLINEAR walkers
+(li_rohf_collinear_snapshot.npz), and the statistical reference of the first (bh_rhf_closed_statistical.json).
 
     python tests/golden/make_bh_snapshot.py [SAFIRE source tree]
 
-The case (tests/functional/run_functional.py:195-245 with --snapshot; functional_cases.py:101-134):
+The BH closed case (tests/functional/run_functional.py:195-245 with --snapshot; functional_cases.py:101-134):
 Hamiltonian afqmc_inputs/BH/afqmc_H_rhf_closed.h5 (dense Cholesky), trial afqmc_inputs/BH/afqmc_rhf_nomsd.h5
 (RHF, NOMSD, one determinant), CLOSED walkers, seed 42, 50 walkers, timestep 0.01, 20 steps, population
 control and measurement every step, orthogonalization every 10 steps, no equilibration, one rank.  The
 recorded results are snapshot_references/BH/dense_rhf_basis_closed/rhf_nomsd/closed/results.h5: for each
 observable the mean and error of its rebinned series (safiretools Results.average).
 
-Stored: the Hamiltonian and trial as the engine takes them (read by safire_b200.inputs), the run
-settings, and the recorded mean / error of every observable of the energy estimator.  The
+The collinear cases have the same settings (functional_cases.py:101-143).  Stored per case: the
+Hamiltonian and trial as the engine takes them (read by safire_b200.inputs), the run settings, and the
+recorded mean / error of every observable of the energy estimator.  The
 back-propagated and mixed RDM estimators the case also recorded are outside the path and not stored.
 
 The statistical reference (statistical_references/BH/dense_rhf_basis_closed/rhf_nomsd/closed/results.h5)
@@ -34,27 +37,42 @@ OBSERVABLES = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "Ov
                "EffectiveNumWalkers", "Phase", "TotalWeight")
 
 
-def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    fn = os.path.join(src, "tests", "functional")
-    wfn = load_nomsd_trial(os.path.join(fn, "afqmc_inputs", "BH", "afqmc_rhf_nomsd.h5"))
-    ham = load_dense_hamiltonian(os.path.join(fn, "afqmc_inputs", "BH", "afqmc_H_rhf_closed.h5"), wfn["nup"])
-    res = H5File(os.path.join(fn, "snapshot_references", "BH", "dense_rhf_basis_closed", "rhf_nomsd", "closed",
-                              "results.h5"))
+def snapshot_case(fn, system, ham_file, wfn_file, case, walker_type, out_name, with_hamiltonian=True):
+    """One seeded snapshot case: inputs as the engine takes them, settings, recorded mean / error."""
+    wfn = load_nomsd_trial(os.path.join(fn, "afqmc_inputs", system, wfn_file), walker_type)
+    ham = load_dense_hamiltonian(os.path.join(fn, "afqmc_inputs", system, ham_file), wfn["nup"])
+    res = H5File(os.path.join(fn, "snapshot_references", system, *case.split("/"), "results.h5"))
     inp = json.loads(res["input_file"])
     ex = inp["execute"]
     settings = dict(seed=inp["seed"], nwalk=ex["num_walkers"], dt=ex["timestep"], steps=ex["steps"],
                     ortho_interval=ex["walker_ortho_interval"], pop_interval=ex["population_control_interval"],
                     measure_interval=ex["measure_interval"], equilibration_steps=ex["equilibration_steps"],
                     num_ranks=int(res["num_ranks"]), walker_type=ex["walker_set"]["walker_type"])
-    out = dict(hcore=ham["hcore"], Likn=ham["Likn"], PsiT=wfn["PsiT"], E0=np.float64(ham["E0"]),
-               settings=json.dumps(settings))
+    assert settings["walker_type"] == walker_type
+    out = dict(PsiT=wfn["PsiT"], E0=np.float64(ham["E0"]), ci=np.complex128(wfn["ci"]), settings=json.dumps(settings))
+    if walker_type == "COLLINEAR":
+        out.update(PsiT_up=wfn["PsiT_up"], PsiT_dn=wfn["PsiT_dn"])
+    if with_hamiltonian:
+        out.update(hcore=ham["hcore"], Likn=ham["Likn"])
     for k in OBSERVABLES:
         out[f"mean_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/mean"])
         out[f"error_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/error"])
-    path = os.path.join(HERE, "bh_rhf_closed_snapshot.npz")
+    path = os.path.join(HERE, out_name)
     np.savez_compressed(path, **out)
     print(path, settings)
+
+
+def main():
+    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    fn = os.path.join(src, "tests", "functional")
+    snapshot_case(fn, "BH", "afqmc_H_rhf_closed.h5", "afqmc_rhf_nomsd.h5", "dense_rhf_basis_closed/rhf_nomsd/closed",
+                  "CLOSED", "bh_rhf_closed_snapshot.npz")
+    # the same Hamiltonian with a UHF trial (the Hamiltonian tensors are those of the file above)
+    snapshot_case(fn, "BH", "afqmc_H_rhf_closed.h5", "afqmc_uhf_nomsd.h5",
+                  "dense_rhf_basis_closed/uhf_nomsd/collinear", "COLLINEAR", "bh_uhf_collinear_snapshot.npz",
+                  with_hamiltonian=False)
+    snapshot_case(fn, "Li", "hamil_closed.h5", "rohf_nomsd_polarized.h5",
+                  "hamil_closed/rohf_wfn_polarized/collinear", "COLLINEAR", "li_rohf_collinear_snapshot.npz")
 
     res = H5File(os.path.join(fn, "statistical_references", "BH", "dense_rhf_basis_closed", "rhf_nomsd", "closed",
                               "results.h5"))

@@ -28,12 +28,23 @@ SNAPSHOT_OBSERVABLES = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEne
                         "EffectiveNumWalkers", "Phase", "TotalWeight")
 
 
-def bh_snapshot():
-    """The BH seeded snapshot case (make_bh_snapshot.py): inputs, settings and recorded (mean, error)."""
-    z = np.load(os.path.join(HERE, "bh_rhf_closed_snapshot.npz"))
+def snapshot(name):
+    """A seeded snapshot case (make_bh_snapshot.py): inputs, settings and recorded (mean, error).
+    The BH collinear case shares the BH Hamiltonian tensors of the closed case's file."""
+    z = np.load(os.path.join(HERE, f"{name}_snapshot.npz"))
     rec = {k: (z[f"mean_{k}"][()], z[f"error_{k}"][()]) for k in SNAPSHOT_OBSERVABLES}
-    return dict(hcore=z["hcore"], Likn=z["Likn"], PsiT=z["PsiT"], E0=float(z["E0"]),
-                settings=json.loads(str(z["settings"])), recorded=rec)
+    out = dict(PsiT=z["PsiT"], E0=float(z["E0"]), ci=complex(z["ci"]), settings=json.loads(str(z["settings"])),
+               recorded=rec)
+    if "PsiT_up" in z:
+        out.update(PsiT_up=z["PsiT_up"], PsiT_dn=z["PsiT_dn"])
+    h = z if "hcore" in z else np.load(os.path.join(HERE, "bh_rhf_closed_snapshot.npz"))
+    out.update(hcore=h["hcore"], Likn=h["Likn"])
+    return out
+
+
+def bh_snapshot():
+    """The BH CLOSED case."""
+    return snapshot("bh_rhf_closed")
 
 
 def snapshot_match(series, recorded, rebinned_average, tol=1e-9):

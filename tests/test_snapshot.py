@@ -1,8 +1,9 @@
 """The reference's seeded snapshot of a real molecule, replayed on its own random streams.
 
-The BH case of the reference's functional tests (dense Cholesky Hamiltonian, RHF NOMSD trial,
-CLOSED walkers, seed 42, 50 walkers, 20 steps, one rank) recorded every energy-estimator
-observable; the reference's runner requires a rerun to reproduce them to 1e-9.  These tests pin:
+The dense-Cholesky NOMSD cases of the reference's functional tests (BH with an RHF trial and CLOSED
+walkers, BH with a UHF trial and Li with a polarized ROHF trial and COLLINEAR walkers; seed 42,
+50 walkers, 20 steps, one rank) recorded every energy-estimator observable; the reference's runner
+requires a rerun to reproduce them to 1e-9.  These tests pin:
 
   * the host random streams (std::mt19937 via split_seed, uniform_real_distribution) against the
     C++ standard's known answer and numpy's independent MT19937;
@@ -18,7 +19,7 @@ import pytest
 
 from oracle import afqmc_oracle as O
 from oracle.mt19937 import MT19937, HostRandomGenerator, split_seed
-from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, snapshot_match
+from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, snapshot, snapshot_match
 
 REF = "/root/reference/tests/functional"
 
@@ -46,11 +47,21 @@ def test_split_seed_streams_distinct():
     assert all(0 <= s < 2**64 for s in seeds)
 
 
-def test_oracle_reproduces_reference_snapshot():
-    snap = bh_snapshot()
+def _oracle_hamiltonian(snap):
+    if snap["settings"]["walker_type"] == "COLLINEAR":
+        return O.CollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_up"], snap["PsiT_dn"], snap["E0"],
+                                      snap["ci"])
+    return O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
+
+
+@pytest.mark.parametrize("case", ["bh_rhf_closed", "bh_uhf_collinear", "li_rohf_collinear"])
+def test_oracle_reproduces_reference_snapshot(case):
+    """BH with an RHF trial and CLOSED walkers, BH with a UHF trial and COLLINEAR walkers, Li with a
+    fully polarized ROHF trial (no down electrons) and COLLINEAR walkers."""
+    snap = snapshot(case)
     st = snap["settings"]
-    assert st["num_ranks"] == 1 and st["walker_type"] == "CLOSED"
-    ham = O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
+    assert st["num_ranks"] == 1
+    ham = _oracle_hamiltonian(snap)
     _, _, series = O.run_seeded(ham, st["nwalk"], st["dt"], st["steps"], st["seed"],
                                 ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
                                 measure_interval=st["measure_interval"],
@@ -86,7 +97,12 @@ def test_loaders_read_reference_files():
     assert f.shape("Hamiltonian/DenseFactorized/L") == (1, 1, 19, 1, 19, 78)
     # what the CLOSED single-determinant dense path does not take is refused with the reason
     with pytest.raises(InputError):
-        load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_uhf_nomsd.h5")       # collinear trial
+        load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_uhf_nomsd.h5")       # collinear trial, CLOSED walkers
+    coll = load_nomsd_trial(f"{REF}/afqmc_inputs/Li/rohf_nomsd_polarized.h5", "COLLINEAR")
+    li = snapshot("li_rohf_collinear")
+    assert coll["ndn"] == 0 and np.array_equal(coll["PsiT_up"], li["PsiT_up"])
+    with pytest.raises(InputError):
+        load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_rhf_nomsd.h5", "COLLINEAR")  # closed trial
     with pytest.raises(InputError):
         load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_casci_rhf_nomsd.h5")  # several determinants
     with pytest.raises(InputError):
