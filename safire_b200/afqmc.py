@@ -168,8 +168,7 @@ class AfqmcEngine:
     def __init__(self, system, nwalk, dt=0.005, seed=0, device=0, **params):
         self.M, self.N, self.Nc, self.W = system.M, system.N, system.Nc, nwalk
         self.dt = dt
-        p = capi.default_params(nmo=system.M, nel=system.N, nchol=system.Nc, nwalk=nwalk, dt=dt,
-                                E0=float(system.E0), seed=seed, device=device)
+        p = capi.system_params(system, nwalk=nwalk, dt=dt, E0=float(system.E0), seed=seed, device=device)
         for k, v in params.items():
             setattr(p, k, v)
         self.params = p

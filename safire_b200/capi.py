@@ -34,9 +34,10 @@ class EngineParams(ctypes.Structure):
                 ("weight_bound_fraction", ctypes.c_double), ("subtractMF", ctypes.c_int),
                 ("denseP1", ctypes.c_int), ("free_projection", ctypes.c_int),
                 ("target_population", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("device", ctypes.c_int),
-                ("precision", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("walker_type", ctypes.c_int), ("nel_dn", ctypes.c_int)]
 
 PRECISION_FP64, PRECISION_MIXED, PRECISION_MIXED_FP32 = 0, 1, 2
+WALKER_CLOSED, WALKER_COLLINEAR = 1, 2
 
 
 class RunParams(ctypes.Structure):
@@ -181,6 +182,17 @@ def ptr(x):
     if isinstance(x, np.ndarray):
         return x.ctypes.data
     return x.data_ptr()
+
+
+def system_params(system, **kw):
+    """default_params for a System: CLOSED, or COLLINEAR when the system has nel_dn >= 0 down
+    electrons (its PsiT then stacks the up rows over the down rows)."""
+    nel_dn = getattr(system, "nel_dn", -1)
+    coll = nel_dn is not None and nel_dn >= 0
+    p = default_params(nmo=system.M, nel=system.N - (nel_dn if coll else 0), nchol=system.Nc, **kw)
+    if coll:
+        p.walker_type, p.nel_dn = WALKER_COLLINEAR, nel_dn
+    return p
 
 
 def default_params(**kw):

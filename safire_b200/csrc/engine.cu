@@ -3,7 +3,14 @@
 //
 // It plays the role of the objects execute_simulation builds (src/AFQMC/execute.cpp:107-206):
 // Real3IndexFactorization (HamOps), NOMSD with ndet = 1 (trial), WalkerSet and
-// AFQMCBasePropagator, for CLOSED walkers.
+// AFQMCBasePropagator, for CLOSED walkers, and in FP64 for COLLINEAR walkers.
+//
+// A COLLINEAR walker is kept as one (M, nup + ndn) matrix, the up columns first, against the
+// stacked trial [PsiT_up; PsiT_dn]: propagation, vHS, P1 and the half-rotated Lnak / haj are those
+// of one N = nup + ndn matrix (the Hamiltonian is spin-independent), vbias sums both spins' rows.
+// What is per spin -- the overlap matrix and its inverse and log det, the CholeskyQR Gram matrix,
+// the exchange pairs -- keeps only the two diagonal spin blocks, which gives exactly the per-spin
+// factorizations (with the pivots LAPACK would choose per spin) and the sum of the two log dets.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -131,6 +138,12 @@ struct Engine {
   sfq_engine_params_t p{};
   int M = 0, N = 0, Nc = 0, W = 0;
   bool trial_real = true;
+  // COLLINEAR walkers: N = nup + ndn columns, up first (CLOSED: collinear false, N = nup)
+  bool collinear = false;
+  int nup = 0;
+  int spin_split() const { return collinear ? nup : -1; }
+  double ov_scale() const { return collinear ? 1.0 : 2.0; }  // NOMSD.cpp:285-290: CLOSED counts its determinant twice
+  double vb_scale() const { return (collinear ? 1.0 : 2.0) * std::sqrt(p.dt); }  // Real3IndexFactorization.hpp:349
   cudaStream_t st = nullptr;
   // host-buffer steps: the field uniforms go in on a copy stream while the step's density and force
   // bias run; the fields kernel waits for uni_wait (cleared once waited on)
@@ -444,9 +457,10 @@ struct Engine {
         for (int i = 0; i < M; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * M + i]);
       SFQ_CUDA_TRY(cudaMemcpyAsync(SM2, psi.data(), sizeof(cplx) * M * N, cudaMemcpyHostToDevice, st));
       if ((rc = ops::overlap_matrix(PsiT, true, SM2, T, 1, M, N, st))) return rc;
+      if ((rc = ops::mask_cross_spin(T, 1, N, spin_split(), st))) return rc;
       if ((rc = lu_logdet(T, (long)N * N, 1, N, ovtmp, false, 1.0, true, st))) return rc;
       if ((rc = ops::green_compact(T, SM2, G, 1, M, N, st))) return rc;
-      if ((rc = ops::vbias(G, Lnak, !trial_real, X, 1, N, M, Nc, 2.0 * std::sqrt(p.dt), st))) return rc;
+      if ((rc = ops::vbias(G, Lnak, !trial_real, X, 1, N, M, Nc, vb_scale(), st))) return rc;
       if ((rc = real_of(X, vmf, Nc, st))) return rc;
       SFQ_CUDA_TRY(cudaStreamSynchronize(st));
     } else {
@@ -555,7 +569,8 @@ struct Engine {
       const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
       cplx* out = ov ? ov : ovtmp;
       if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, M, N, st))) return rc;
-      if ((rc = lu_logdet(T, (long)N * N, W, N, out, false, 2.0, true, st))) return rc;
+      if ((rc = ops::mask_cross_spin(T, W, N, spin_split(), st))) return rc;
+      if ((rc = lu_logdet(T, (long)N * N, W, N, out, false, ov_scale(), true, st))) return rc;
       inv_cached = true;
       inv_ov = out;
     } else if (ov && ov != inv_ov) {
@@ -602,7 +617,8 @@ struct Engine {
     const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
     inv_cached = false;
     if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, M, N, st))) return rc;
-    if ((rc = lu_logdet(T, (long)N * N, W, N, ov, false, 2.0, true, st))) return rc;
+    if ((rc = ops::mask_cross_spin(T, W, N, spin_split(), st))) return rc;
+    if ((rc = lu_logdet(T, (long)N * N, W, N, ov, false, ov_scale(), true, st))) return rc;
     inv_cached = true;
     inv_ov = ov;
     return SFQ_OK;
@@ -616,7 +632,7 @@ struct Engine {
     if ((rc = density(nullptr))) return rc;                                          // 1. G
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
-    if ((rc = ops::vbias(G, Lnak, !trial_real, X, W, N, M, Nc, 2.0 * std::sqrt(p.dt), st))) return rc;
+    if ((rc = ops::vbias(G, Lnak, !trial_real, X, W, N, M, Nc, vb_scale(), st))) return rc;
     ph_end(SFQ_PH_VBIAS);
     ph_begin(SFQ_PH_FIELDS);
     FieldParams fp;                                                                   // 2. X
@@ -1046,12 +1062,13 @@ struct Engine {
       // gives wfn->Log_Overlap(wset) of the orthogonalized walkers without a new factorization
       if (inv_ov != newov)
         SFQ_CUDA_TRY(cudaMemcpyAsync(newov, inv_ov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
-      if ((rc = ops::orthogonalize_carry(SM, SM2, Tchunk, Tchunk + W * NN, G, status, T, newov, 2.0, W, M, N, st)))
+      if ((rc = ops::orthogonalize_carry(SM, SM2, Tchunk, Tchunk + W * NN, G, status, T, newov, ov_scale(), W, M, N,
+                                         st, spin_split())))
         return rc;
       inv_ov = newov;
     } else {
       inv_cached = false;
-      if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, M, N, st))) return rc;
+      if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, M, N, st, spin_split()))) return rc;
       if ((rc = log_overlap(newov))) return rc;  // wfn->Log_Overlap(wset)
     }
     SFQ_CUDA_TRY(cudaMemcpyAsync(props + (long)P_OVLP * W, newov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
@@ -1085,7 +1102,7 @@ struct Engine {
     ph_begin(SFQ_PH_ENERGY);
     if ((rc = density(ovtmp))) return rc;
     if ((rc = ops::energy(E3, G, haj, Lnak, !trial_real, p.E0, W, N, M, Nc, 1, 1, 1, Tchunk, tchunk_elems, exxn, kl,
-                          st)))
+                          st, spin_split())))
       return rc;
     ph_end(SFQ_PH_ENERGY);
     return SFQ_OK;
@@ -1543,22 +1560,34 @@ void sfq_engine_params_default(sfq_engine_params_t* p) {
   p->denseP1 = 0;
   p->free_projection = 0;
   p->precision = SFQ_PRECISION_FP64;
+  p->walker_type = SFQ_WALKER_CLOSED;
+  p->nel_dn = 0;
 }
 
 int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
                       const void* PsiT) {
   if (!out || !p || !hcore || !Likn || !PsiT) return record_error(SFQ_ERR_ARG, "null pointer");
   *out = nullptr;
-  if (p->nmo <= 0 || p->nel <= 0 || p->nchol <= 0 || p->nwalk <= 0 || p->nel > p->nmo)
-    return record_error(SFQ_ERR_SHAPE, "engine: invalid sizes nmo=%d nel=%d nchol=%d nwalk=%d", p->nmo, p->nel,
-                        p->nchol, p->nwalk);
-  if (p->nel > kMaxSmallN) return record_error(SFQ_ERR_UNSUPPORTED, "engine: nel=%d exceeds %d", p->nel, kMaxSmallN);
+  const int wt = p->walker_type == 0 ? SFQ_WALKER_CLOSED : p->walker_type;
+  if (wt != SFQ_WALKER_CLOSED && wt != SFQ_WALKER_COLLINEAR)
+    return record_error(SFQ_ERR_UNSUPPORTED, "engine: walker type %d (CLOSED = 1 and COLLINEAR = 2 are built)",
+                        p->walker_type);
+  const bool coll = wt == SFQ_WALKER_COLLINEAR;
+  if (p->nmo <= 0 || p->nel <= 0 || p->nchol <= 0 || p->nwalk <= 0 || p->nel > p->nmo ||
+      (coll && (p->nel_dn < 0 || p->nel_dn > p->nmo)))
+    return record_error(SFQ_ERR_SHAPE, "engine: invalid sizes nmo=%d nel=%d nel_dn=%d nchol=%d nwalk=%d", p->nmo,
+                        p->nel, p->nel_dn, p->nchol, p->nwalk);
+  const int ntot = p->nel + (coll ? p->nel_dn : 0);
+  if (ntot > kMaxSmallN)
+    return record_error(SFQ_ERR_UNSUPPORTED, "engine: %d electrons per walker exceed %d", ntot, kMaxSmallN);
   if (!(p->dt > 0.0)) return record_error(SFQ_ERR_ARG, "engine: dt must be positive");
   SFQ_CUDA_TRY(cudaSetDevice(p->device));
   auto* h = new sfq_engine_s();
   Engine& e = h->e;
   e.p = *p;
-  e.M = p->nmo; e.N = p->nel; e.Nc = p->nchol; e.W = p->nwalk;
+  e.M = p->nmo; e.N = ntot; e.Nc = p->nchol; e.W = p->nwalk;
+  e.collinear = coll;
+  e.nup = p->nel;
   const cplx* ps = reinterpret_cast<const cplx*>(PsiT);
   e.trial_real = true;
   for (long i = 0; i < (long)e.N * e.M; ++i)
@@ -1568,6 +1597,10 @@ int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const dou
   if (p->precision != SFQ_PRECISION_FP64 && !e.mixed) {
     delete h;
     return record_error(SFQ_ERR_ARG, "engine: unknown precision %d", p->precision);
+  }
+  if (e.mixed && coll) {
+    delete h;
+    return record_error(SFQ_ERR_UNSUPPORTED, "engine: COLLINEAR walkers run in FP64 (SFQ_PRECISION_FP64)");
   }
   if (e.mixed && (!e.trial_real || e.M % 8 || e.Nc % 8)) {
     delete h;
@@ -1641,9 +1674,17 @@ int sfq_engine_export_walker_buffer(sfq_engine_t h, void* rows) {
   int rc;
   if ((rc = sfq_engine_get_walkers(h, sm.data(), pr.data()))) return rc;
   cplx* out = reinterpret_cast<cplx*>(rows);
+  const int nu = e.collinear ? e.nup : e.N, nd = e.N - nu;
   for (int w = 0; w < e.W; ++w) {
     cplx* r = out + (size_t)w * rl;
-    std::memcpy(r, sm.data() + (size_t)w * mn, sizeof(cplx) * mn);
+    const cplx* s = sm.data() + (size_t)w * mn;
+    if (nd == 0) {
+      std::memcpy(r, s, sizeof(cplx) * mn);
+    } else {  // the up block (M x nup) then the down block (M x ndn), WalkerSetBase.h:256-264
+      for (int i = 0; i < e.M; ++i)
+        for (int a = 0; a < e.N; ++a)
+          r[a < nu ? (size_t)i * nu + a : (size_t)e.M * nu + (size_t)i * nd + (a - nu)] = s[(size_t)i * e.N + a];
+    }
     // WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, LOGSCL_UP, LOGSCL_DN, IS_UNITARY, THETA
     for (int k = 0; k < 7; ++k) r[mn + k] = pr[(size_t)k * e.W + w];
     r[mn + 7] = mk(0.0, 0.0);

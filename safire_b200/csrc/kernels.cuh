@@ -67,8 +67,9 @@ int comb_weights(const double* wts, int nwalk, double r, int* offspring, double*
 int energy_e1(const cplx* G, const cplx* haj, cplx* E3, int nwalk, int nel, int nmo, double E0, double scl,
               int addH1, cudaStream_t st);
 // T chunk (nwalk, nel, nv, nel): exxn[w, n0+n] = sum_ab T[a,n,b]T[b,n,a]; kl[w, n0+n] = sum_a T[a,n,a]
+// nup >= 0: COLLINEAR walkers, the exchange pairs orbitals of one spin only ([0, nup) and [nup, nel))
 int energy_exx_reduce(const cplx* T, int nwalk, int nel, int nv, int n0, int nchol, cplx* exxn, cplx* kl,
-                      cudaStream_t st);
+                      cudaStream_t st, int nup = -1);
 // the same from FP32 planar T of the split-BF16 product: rows (c*W + w)*nel + a, columns n*nel + b
 int energy_exx_reduce_f32(const float* C, int nwalk, int nel, int nv, int n0, int nchol, long ldc, cplx* exxn,
                           cplx* kl, cudaStream_t st);

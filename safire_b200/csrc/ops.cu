@@ -122,10 +122,35 @@ int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M
   return p1_apply(P1, p_cplx, TMN, SM, W, M, N, st);
 }
 
+namespace {
+// A[w][a][b] = 0 where a and b belong to different spins (a < nup <= b or b < nup <= a)
+__global__ void mask_cross_spin_kernel(cplx* A, int N, int nup) {
+  cplx* Aw = A + (long)blockIdx.x * N * N;
+  const int ndn = N - nup;
+  for (int e = threadIdx.x; e < nup * ndn; e += blockDim.x) {
+    const int a = e / ndn, b = nup + e % ndn;
+    Aw[(long)a * N + b] = mk(0.0, 0.0);
+    Aw[(long)b * N + a] = mk(0.0, 0.0);
+  }
+}
+}  // namespace
+
+// COLLINEAR walkers (columns [0, nup) up, [nup, N) down): the per-walker N x N matrices keep only
+// their two spin blocks; nothing to do unless both spins are occupied
+int mask_cross_spin(cplx* A, int W, int N, int nup, cudaStream_t st) {
+  if (nup <= 0 || nup >= N || W <= 0) return SFQ_OK;
+  mask_cross_spin_kernel<<<W, 128, 0, st>>>(A, N, nup);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
 // One CholeskyQR pass over the walkers selected by mask (all when null): S = Win^H Win = R^H R,
 // Wout = Win R^-1; again[b] set from R's condition bound when again is not null.
+// nup in (0, N): COLLINEAR walkers, columns [0, nup) up and [nup, N) down; the Gram matrix's
+// cross-spin blocks are zeroed, so R, R^-1 and the new walkers are those of each spin on its own
+// (orthogonalize.hpp:135-169 runs per spin).
 static int cholqr_pass(const cplx* Win, cplx* Wout, cplx* S, int* status, int* again, const int* mask, int W, int M,
-                       int N, cudaStream_t st, cplx* R = nullptr) {
+                       int N, cudaStream_t st, cplx* R = nullptr, int nup = -1) {
   int rc;
   GemmDesc d;  // S = Win^H Win
   d.M = N; d.N = N; d.K = M; d.batch = W;
@@ -135,6 +160,7 @@ static int cholqr_pass(const cplx* Win, cplx* Wout, cplx* S, int* status, int* a
   d.mask = mask;
   d.upper_only = true;  // Hermitian: the Cholesky below reads the upper triangle only
   if ((rc = gemm_f64(d, st))) return rc;
+  if ((rc = mask_cross_spin(S, W, N, nup, st))) return rc;
   if ((rc = chol_rinv(S, (long)N * N, W, N, status, again, mask, kCholQrKappa, st, R))) return rc;
   GemmDesc q;  // Wout = Win R^-1
   q.M = M; q.N = N; q.K = N; q.batch = W;
@@ -149,11 +175,12 @@ static int cholqr_pass(const cplx* Win, cplx* Wout, cplx* S, int* status, int* a
 // CholeskyQR2, with the second pass only where the first one's R was not well conditioned
 // (kappa bound > kCholQrKappa: Q^H Q - I of one pass is of order eps kappa^2, <= 1e-12 below
 // it).  status holds 2 W ints: the Cholesky status per walker, then the second-pass flags.
-int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int W, int M, int N, cudaStream_t st) {
+int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int W, int M, int N, cudaStream_t st,
+                  int nup) {
   int rc;
   int* again = status + W;
-  if ((rc = cholqr_pass(SM, SM2, S, status, again, nullptr, W, M, N, st))) return rc;
-  if ((rc = cholqr_pass(SM2, SM, S, status, nullptr, again, W, M, N, st))) return rc;
+  if ((rc = cholqr_pass(SM, SM2, S, status, again, nullptr, W, M, N, st, nullptr, nup))) return rc;
+  if ((rc = cholqr_pass(SM2, SM, S, status, nullptr, again, W, M, N, st, nullptr, nup))) return rc;
   if ((rc = copy_walkers_where(SM, SM2, again, 0, W, (long)M * N, st))) return rc;  // one-pass walkers
   (void)log_detR;
   return SFQ_OK;
@@ -192,16 +219,16 @@ int rmul(const cplx* R, const cplx* Tin, cplx* C, const int* mask, int W, int N,
 // real and positive (the phase is unchanged).  Tinv (W, N, N) and ov (W) in/out, scale = the
 // number of identical determinants (2 for CLOSED walkers); S, R, Tw: (W, N, N) scratch.
 int orthogonalize_carry(cplx* SM, cplx* SM2, cplx* S, cplx* R, cplx* Tw, int* status, cplx* Tinv, cplx* ov,
-                        double scale, int W, int M, int N, cudaStream_t st) {
+                        double scale, int W, int M, int N, cudaStream_t st, int nup) {
   int rc;
   int* again = status + W;
   const long NN = (long)N * N;
-  if ((rc = cholqr_pass(SM, SM2, S, status, again, nullptr, W, M, N, st, R))) return rc;
+  if ((rc = cholqr_pass(SM, SM2, S, status, again, nullptr, W, M, N, st, R, nup))) return rc;
   if ((rc = rmul(R, Tinv, Tw, nullptr, W, N, st))) return rc;
   const int wpb = 8;
   sub_logdiag_kernel<<<(W + wpb - 1) / wpb, 32 * wpb, 0, st>>>(R, N, nullptr, ov, scale, W);
   SFQ_LAUNCHED();
-  if ((rc = cholqr_pass(SM2, SM, S, status, nullptr, again, W, M, N, st, R))) return rc;
+  if ((rc = cholqr_pass(SM2, SM, S, status, nullptr, again, W, M, N, st, R, nup))) return rc;
   if ((rc = rmul(R, Tw, Tinv, again, W, N, st))) return rc;
   sub_logdiag_kernel<<<(W + wpb - 1) / wpb, 32 * wpb, 0, st>>>(R, N, again, ov, scale, W);
   SFQ_LAUNCHED();
@@ -219,9 +246,9 @@ int energy_chunk(int W, int N, int Nc, long max_elems) {
 
 int energy(cplx* E3, const cplx* G, const cplx* haj, const void* Lnak, bool l_cplx, double E0, int W, int N, int M,
            int Nc, int addH1, int addEJ, int addEXX, cplx* Tchunk, long tchunk_elems, cplx* exxn, cplx* kl,
-           cudaStream_t st) {
+           cudaStream_t st, int nup) {
   int rc;
-  const double scl = 2.0;
+  const double scl = nup < 0 ? 2.0 : 1.0;  // CLOSED counts each orbital twice (energy, :148-173)
   if ((rc = energy_e1(G, haj, E3, W, N, M, E0, scl, addH1, st))) return rc;
   if (!addEXX && !addEJ) return SFQ_OK;
   const int nv_max = energy_chunk(W, N, Nc, tchunk_elems);
@@ -234,7 +261,7 @@ int energy(cplx* E3, const cplx* G, const cplx* haj, const void* Lnak, bool l_cp
     d.B = (const unsigned char*)Lnak + (size_t)n0 * N * M * esz; d.sBk = 1; d.sBn = M; d.b_cplx = l_cplx;
     d.C = Tchunk; d.sCm = (long)nv * N; d.sCn = 1;
     if ((rc = gemm_f64(d, st))) return rc;
-    if ((rc = energy_exx_reduce(Tchunk, W, N, nv, n0, Nc, exxn, kl, st))) return rc;
+    if ((rc = energy_exx_reduce(Tchunk, W, N, nv, n0, Nc, exxn, kl, st, nup))) return rc;
   }
   return energy_finish(exxn, kl, E3, W, Nc, scl, addEXX, addEJ, st);
 }

@@ -23,16 +23,23 @@ int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M
               cplx* T1, cplx* T2, cudaStream_t st);
 // CholeskyQR2; SM2 (W*M*N), S (W*N*N) scratch, status (W) ints.  log_detR (W) accumulated if not null
 // CholeskyQR2 in place on SM (SM2, S: scratch; status: 2 W ints)
-int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int W, int M, int N, cudaStream_t st);
+// nup in (0, N) (here and below): COLLINEAR walkers, columns [0, nup) up and [nup, N) down, each spin
+// on its own; -1: CLOSED
+int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int W, int M, int N, cudaStream_t st,
+                  int nup = -1);
 // the same, carrying the inverse overlap matrices Tinv (W, N, N) and log overlaps ov (W) of the
 // walkers through the QR ((PsiT W R^-1)^-1 = R (PsiT W)^-1, log det drops by scale * sum log r_ii);
 // S, R, Tw: (W, N, N) scratch
 int orthogonalize_carry(cplx* SM, cplx* SM2, cplx* S, cplx* R, cplx* Tw, int* status, cplx* Tinv, cplx* ov,
-                        double scale, int W, int M, int N, cudaStream_t st);
+                        double scale, int W, int M, int N, cudaStream_t st, int nup = -1);
+// zero the cross-spin blocks of W per-walker N x N matrices (a no-op unless 0 < nup < N)
+int mask_cross_spin(cplx* A, int W, int N, int nup, cudaStream_t st);
 // energy with chunked T; ws: T chunk (W*N*nv*N) + exxn (W*Nc) + kl (W*Nc)
+// nup >= 0: COLLINEAR (scale 1, exchange within each spin, Coulomb 0.5 (sum of both spins' traces)^2);
+// -1: CLOSED (scale 2)
 int energy(cplx* E3, const cplx* G, const cplx* haj, const void* Lnak, bool l_cplx, double E0, int W, int N, int M,
            int Nc, int addH1, int addEJ, int addEXX, cplx* Tchunk, long tchunk_elems, cplx* exxn, cplx* kl,
-           cudaStream_t st);
+           cudaStream_t st, int nup = -1);
 int energy_chunk(int W, int N, int Nc, long max_elems);
 
 }  // namespace ops

@@ -18,6 +18,10 @@
 
 namespace sfq {
 namespace {
+// electrons per walker: the rows of PsiT and the columns of a walker (COLLINEAR: up and down)
+int electrons(const sfq_engine_params_t& p) {
+  return p.nel + (p.walker_type == SFQ_WALKER_COLLINEAR ? p.nel_dn : 0);
+}
 
 constexpr int kProps = 8;  // property columns of sfq_engine_get_walkers
 
@@ -76,7 +80,7 @@ int evict(sfq_server_s& s, int keep, size_t need) {
     }
     if (victim < 0) return SFQ_ERR_OOM;  // everything resident is running: wait
     SystemRec& v = s.sys[victim];
-    const size_t mn = size_t(v.p.nmo) * v.p.nel * v.p.nwalk;
+    const size_t mn = size_t(v.p.nmo) * electrons(v.p) * v.p.nwalk;
     v.saved_SM.resize(2 * mn);
     v.saved_props.resize(2 * size_t(kProps) * v.p.nwalk);
     int rc = sfq_engine_get_walkers(v.eng, v.saved_SM.data(), v.saved_props.data());
@@ -158,7 +162,7 @@ int sfq_server_add_system(sfq_server_t s, const sfq_engine_params_t* p, const do
   r.hcore.assign(hcore, hcore + MM);
   r.Likn.assign(Likn, Likn + MM * p->nchol);
   const double* ps = static_cast<const double*>(PsiT);
-  r.PsiT.assign(ps, ps + 2 * size_t(p->nel) * p->nmo);
+  r.PsiT.assign(ps, ps + 2 * size_t(electrons(*p)) * p->nmo);
   s->sys.push_back(std::move(r));
   *id = int(s->sys.size()) - 1;
   return SFQ_OK;

@@ -280,8 +280,10 @@ __global__ void __launch_bounds__(RT) energy_e1_kernel(const cplx* G, const cplx
 }
 
 // one CTA per (n, w): exx[w, n0+n] = sum_ab T[w,a,n,b] T[w,b,n,a]; kl[w, n0+n] = sum_a T[w,a,n,a]
+// nup < nel: COLLINEAR walkers, orbitals [0, nup) up and [nup, nel) down; the exchange pairs only
+// orbitals of one spin (energy_impl runs per spin, Real3IndexFactorization.hpp:476-560)
 __global__ void __launch_bounds__(RT) energy_exx_kernel(const cplx* T, int nel, int nv, int n0, int nchol,
-                                                        cplx* exxn, cplx* kl) {
+                                                        cplx* exxn, cplx* kl, int nup) {
   __shared__ cplx red[RT / 32];
   const int n = blockIdx.x, w = blockIdx.y;
   const long rowstride = (long)nv * nel;  // T[(w*nel + a)][(n*nel + b)]
@@ -291,9 +293,10 @@ __global__ void __launch_bounds__(RT) energy_exx_kernel(const cplx* T, int nel, 
   for (int e = threadIdx.x; e < nn; e += RT) {
     const int a = e / nel, b = e % nel;
     const cplx tab = Tw[(long)a * rowstride + b];
+    if (a == b) tr = cadd(tr, tab);
+    if ((a < nup) != (b < nup)) continue;
     const cplx tba = Tw[(long)b * rowstride + a];
     acc = cadd(acc, cmul(tab, tba));
-    if (a == b) tr = cadd(tr, tab);
   }
   cplx s = block_sum<RT>(acc, red);
   cplx t = block_sum<RT>(tr, red);
@@ -475,10 +478,10 @@ int energy_e1(const cplx* G, const cplx* haj, cplx* E3, int nwalk, int nel, int 
 }
 
 int energy_exx_reduce(const cplx* T, int nwalk, int nel, int nv, int n0, int nchol, cplx* exxn, cplx* kl,
-                      cudaStream_t st) {
+                      cudaStream_t st, int nup) {
   if (nwalk <= 0 || nv <= 0) return SFQ_OK;
   dim3 grid(nv, nwalk);
-  energy_exx_kernel<<<grid, RT, 0, st>>>(T, nel, nv, n0, nchol, exxn, kl);
+  energy_exx_kernel<<<grid, RT, 0, st>>>(T, nel, nv, n0, nchol, exxn, kl, nup < 0 ? nel : nup);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

@@ -142,11 +142,16 @@ def load_nomsd_trial(path, walker_type="CLOSED"):
     return out
 
 
-def load_system(hamiltonian_path, wavefunction_path):
-    """The engine's System (hcore, Likn, PsiT, E0 and sizes) from a Hamiltonian and a trial file."""
+def load_system(hamiltonian_path, wavefunction_path, walker_type="CLOSED"):
+    """The engine's System (hcore, Likn, PsiT, E0 and sizes) from a Hamiltonian and a trial file; for
+    COLLINEAR walkers PsiT stacks the up rows over the down rows and nel_dn counts the latter."""
     from .synthetic import System, SystemSpec
-    wfn = load_nomsd_trial(wavefunction_path)
+    wfn = load_nomsd_trial(wavefunction_path, walker_type)
     ham = load_dense_hamiltonian(hamiltonian_path, wfn["nup"])
     _check(wfn["nmo"] == ham["nmo"], f"trial has {wfn['nmo']} orbitals, Hamiltonian {ham['nmo']}")
+    if walker_type.upper() == "COLLINEAR":
+        PsiT = np.concatenate([wfn["PsiT_up"], wfn["PsiT_dn"]])
+        spec = SystemSpec(M=ham["nmo"], N=PsiT.shape[0], Nc=ham["nchol"], decay=0.0)
+        return System(spec, ham["hcore"], ham["Likn"], PsiT, ham["E0"], nel_dn=wfn["ndn"])
     spec = SystemSpec(M=ham["nmo"], N=wfn["nup"], Nc=ham["nchol"], decay=0.0)
     return System(spec, ham["hcore"], ham["Likn"], wfn["PsiT"], ham["E0"])

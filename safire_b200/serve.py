@@ -45,8 +45,7 @@ class Server:
             pass
 
     def add_system(self, system, nwalk, dt=0.005, seed=0, **params):
-        p = capi.default_params(nmo=system.M, nel=system.N, nchol=system.Nc, nwalk=nwalk, dt=dt,
-                                E0=float(system.E0), seed=seed)
+        p = capi.system_params(system, nwalk=nwalk, dt=dt, E0=float(system.E0), seed=seed)
         for k, v in params.items():
             setattr(p, k, v)
         h = np.ascontiguousarray(system.hcore, dtype=np.float64)

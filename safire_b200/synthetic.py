@@ -45,8 +45,9 @@ class System:
     spec: SystemSpec
     hcore: np.ndarray      # (M, M) float64
     Likn: np.ndarray       # (M, M, Nc) float64
-    PsiT: np.ndarray       # (N, M) complex128
+    PsiT: np.ndarray       # (N, M) complex128; COLLINEAR: the up rows over the down rows
     E0: float = 0.0
+    nel_dn: int = -1       # COLLINEAR walkers: the last nel_dn rows of PsiT are the down spin; -1: CLOSED
 
     @property
     def M(self):

@@ -1,10 +1,11 @@
-"""The FP64 engine replays the reference's seeded BH snapshot through the C ABI.
+"""The FP64 engine replays the reference's seeded snapshots through the C ABI.
 
 The engine takes the reference's own random streams at its two injection points: the field
 uniforms of every step (sfq_engine_propagate_host, the nwalk x nchol draw of assemble_X) and the
 comb's uniform (sfq_engine_population_control_uniform).  Driven in run_afqmc's order it must
 reproduce, step by step, the oracle's energy-estimator series, and through it the snapshot the
-reference recorded, to the reference's own 1e-9.
+reference recorded, to the reference's own 1e-9: BH with an RHF trial and CLOSED walkers, BH with
+a UHF trial and Li with a polarized ROHF trial (no down electrons) and COLLINEAR walkers.
 """
 import numpy as np
 import pytest
@@ -13,18 +14,35 @@ from oracle import afqmc_oracle as O
 from oracle.mt19937 import HostRandomGenerator, split_seed
 from safire_b200 import afqmc as A
 from safire_b200 import capi, synthetic
-from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, snapshot_match
+from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, snapshot, snapshot_match
 
 pytestmark = pytest.mark.gpu
 
+CASES = ["bh_rhf_closed", "bh_uhf_collinear", "li_rohf_collinear"]
 
-def _engine_series(snap):
+
+def _system(snap):
+    """The engine's System of a case: COLLINEAR stacks PsiT_up over PsiT_dn."""
+    M, Nc = snap["hcore"].shape[0], snap["Likn"].shape[2]
+    if snap["settings"]["walker_type"] == "COLLINEAR":
+        PsiT = np.concatenate([snap["PsiT_up"], snap["PsiT_dn"]])
+        spec = synthetic.SystemSpec(M=M, N=PsiT.shape[0], Nc=Nc, decay=0.0)
+        return synthetic.System(spec, snap["hcore"], snap["Likn"], PsiT, snap["E0"],
+                                nel_dn=snap["PsiT_dn"].shape[0])
+    spec = synthetic.SystemSpec(M=M, N=snap["PsiT"].shape[0], Nc=Nc, decay=0.0)
+    return synthetic.System(spec, snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
+
+
+def _oracle_hamiltonian(snap):
+    if snap["settings"]["walker_type"] == "COLLINEAR":
+        return O.CollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_up"], snap["PsiT_dn"], snap["E0"],
+                                      snap["ci"])
+    return O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
+
+
+def _engine_series(snap, system=None):
     st = snap["settings"]
-    M, N = snap["PsiT"].shape[1], snap["PsiT"].shape[0]
-    Nc = snap["Likn"].shape[2]
-    system = synthetic.System(synthetic.SystemSpec(M=M, N=N, Nc=Nc, decay=0.0), snap["hcore"], snap["Likn"],
-                              snap["PsiT"], snap["E0"])
-    eng = A.AfqmcEngine(system, st["nwalk"], dt=st["dt"], seed=0, precision=capi.PRECISION_FP64)
+    eng = A.AfqmcEngine(system or _system(snap), st["nwalk"], dt=st["dt"], seed=0, precision=capi.PRECISION_FP64)
     walker_rng = HostRandomGenerator(split_seed(st["seed"], 0, 0))
     field_rng = HostRandomGenerator(split_seed(st["seed"], 0, 1))
     E_init = eng.init()
@@ -32,23 +50,52 @@ def _engine_series(snap):
                                      ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
                                      equilibration_steps=st["equilibration_steps"],
                                      measure_interval=st["measure_interval"])
+    rows = eng.walker_buffer()
+    SM, _ = eng.walkers()
     eng.close()
-    return E_init, series
+    return E_init, series, rows, SM
 
 
-def test_engine_reproduces_reference_snapshot():
-    snap = bh_snapshot()
+@pytest.mark.parametrize("case", CASES)
+def test_engine_reproduces_reference_snapshot(case):
+    snap = snapshot(case)
     st = snap["settings"]
-    Eshift, series = _engine_series(snap)
-    ham = O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
-    E_init, _, oracle_series = O.run_seeded(ham, st["nwalk"], st["dt"], st["steps"], st["seed"],
-                                            ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
-                                            measure_interval=st["measure_interval"])
+    Eshift, series, rows, SM = _engine_series(snap)
+    E_init, _, oracle_series = O.run_seeded(_oracle_hamiltonian(snap), st["nwalk"], st["dt"], st["steps"],
+                                            st["seed"], ortho_interval=st["ortho_interval"],
+                                            pop_interval=st["pop_interval"], measure_interval=st["measure_interval"])
     assert abs(Eshift - E_init) < 1e-12 * abs(E_init)
     for k in SNAPSHOT_OBSERVABLES:
         a, b = np.asarray(series[k]), np.asarray(oracle_series[k])
         assert np.max(np.abs(a - b)) <= 1e-11 * max(1.0, float(np.max(np.abs(b)))), k
         assert snapshot_match(series[k], snap["recorded"][k], O.rebinned_average) is not None, k
+    if st["walker_type"] == "COLLINEAR":
+        # the reference's walker rows: the up block (M x nup), then the down block (M x ndn)
+        nup = snap["PsiT_up"].shape[0]
+        W, M, N = SM.shape
+        assert np.array_equal(rows[:, :M * nup].reshape(W, M, nup), SM[:, :, :nup])
+        assert np.array_equal(rows[:, M * nup:M * N].reshape(W, M, N - nup), SM[:, :, nup:])
+
+
+def test_collinear_with_identical_spins_is_closed():
+    """COLLINEAR walkers with the RHF orbitals for both spins follow the CLOSED walk on the GPU too."""
+    snap = bh_snapshot()
+    spec = synthetic.SystemSpec(M=snap["hcore"].shape[0], N=2 * snap["PsiT"].shape[0], Nc=snap["Likn"].shape[2],
+                                decay=0.0)
+    coll = synthetic.System(spec, snap["hcore"], snap["Likn"], np.concatenate([snap["PsiT"], snap["PsiT"]]),
+                            snap["E0"], nel_dn=snap["PsiT"].shape[0])
+    _, closed_series, _, _ = _engine_series(snap)
+    _, coll_series, _, _ = _engine_series(snap, coll)
+    for k in ("Energy", "ExchangeEnergy", "CoulombEnergy", "Overlap"):
+        a, b = np.asarray(closed_series[k]), np.asarray(coll_series[k])
+        assert np.max(np.abs(a - b)) < 1e-10 * np.max(np.abs(a)), k
+
+
+def test_collinear_rejected_in_mixed_precision():
+    snap = snapshot("bh_uhf_collinear")
+    with pytest.raises(capi.SafireError) as ex:
+        A.AfqmcEngine(_system(snap), 8, dt=0.01, precision=capi.PRECISION_MIXED)
+    assert ex.value.code == 3  # SFQ_ERR_UNSUPPORTED
 
 
 def test_comb_uniform_rejected_outside_unit_interval():

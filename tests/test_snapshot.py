@@ -107,3 +107,17 @@ def test_loaders_read_reference_files():
         load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_casci_rhf_nomsd.h5")  # several determinants
     with pytest.raises(InputError):
         load_dense_hamiltonian(f"{REF}/afqmc_inputs/BH/afqmc_H_rhf_noncollinear.h5", 3)
+
+
+def test_collinear_with_identical_spins_is_closed():
+    """COLLINEAR walkers whose up and down trials are the same RHF orbitals follow the CLOSED walk:
+    same fields, overlaps (two equal determinants) and energies."""
+    snap = bh_snapshot()
+    closed = O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
+    coll = O.CollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["PsiT"], snap["E0"])
+    runs = [O.run_seeded(h, 16, 0.01, 12, 7, ortho_interval=5, pop_interval=3, measure_interval=1)
+            for h in (closed, coll)]
+    assert abs(runs[0][0] - runs[1][0]) < 1e-12 * abs(runs[0][0])
+    for k in ("Energy", "ExchangeEnergy", "CoulombEnergy", "Overlap"):
+        a, b = np.asarray(runs[0][2][k]), np.asarray(runs[1][2][k])
+        assert np.max(np.abs(a - b)) < 1e-10 * np.max(np.abs(a)), k
