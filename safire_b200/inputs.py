@@ -117,8 +117,9 @@ def read_csr(f, group):
 
 def load_nomsd_trial(path, walker_type="CLOSED"):
     """A single-determinant NOMSD trial: for CLOSED walkers PsiT (nel, nmo) complex; for COLLINEAR
-    walkers also PsiT_up (nup, nmo) and PsiT_dn (ndn, nmo), ndn possibly 0 (read_wavefunction_info,
-    readWfn.cpp:86-119)."""
+    walkers also PsiT_up (nup, nmo) and PsiT_dn (ndn, nmo), ndn possibly 0, from a collinear file or,
+    upgraded, from a closed one (both spins the same orbitals) (read_wavefunction_info,
+    readWfn.cpp:86-119; read_nomsd_wavefunction, readWfn.h:90-139)."""
     walker_type = walker_type.upper()
     _check(walker_type in ("CLOSED", "COLLINEAR"), f"walker type {walker_type}: the path takes CLOSED or COLLINEAR")
     f = H5File(path)
@@ -127,14 +128,17 @@ def load_nomsd_trial(path, walker_type="CLOSED"):
     spin = at.get("spin_type")
     if spin is not None:
         spin = str(spin).lower()
-        _check(spin == walker_type.lower(),
-               f"wavefunction spin_type is '{spin}': {walker_type} walkers take a {walker_type.lower()} trial here")
+        ok = spin == walker_type.lower() or (spin == "closed" and walker_type == "COLLINEAR")
+        _check(ok, f"wavefunction spin_type is '{spin}': {walker_type} walkers take a "
+                   f"{'closed or collinear' if walker_type == 'COLLINEAR' else 'closed'} trial here")
     ci = np.atleast_1d(_complex_last(f["Wavefunction/NOMSD/ci_coeffs"], 1))
     _check(ci.size == 1, f"{ci.size} determinants: the path takes a single-determinant trial")
     _check("Wavefunction/NOMSD/PsiT_0" in f, "Wavefunction/NOMSD/PsiT_0 missing")
     PsiT = read_csr(f, "Wavefunction/NOMSD/PsiT_0")
     out = dict(PsiT=PsiT, ci=complex(ci[0]), nup=PsiT.shape[0], nmo=PsiT.shape[1], spin_type=spin)
-    if walker_type == "COLLINEAR":
+    if walker_type == "COLLINEAR" and spin == "closed":
+        out.update(PsiT_up=PsiT, PsiT_dn=PsiT.copy(), ndn=PsiT.shape[0])  # readWfn.h:130-139
+    elif walker_type == "COLLINEAR":
         _check("Wavefunction/NOMSD/PsiT_1" in f, "Wavefunction/NOMSD/PsiT_1 missing for a collinear trial")
         dn = read_csr(f, "Wavefunction/NOMSD/PsiT_1")
         _check(dn.shape[1] == PsiT.shape[1], f"PsiT_1 has {dn.shape[1]} columns, PsiT_0 {PsiT.shape[1]}")

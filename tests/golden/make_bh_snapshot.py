@@ -1,6 +1,7 @@
 """Extract the dense-Cholesky NOMSD cases of the reference's functional tests: the seeded snapshots
 of BH with CLOSED walkers (bh_rhf_closed_snapshot.npz), BH with a UHF trial and COLLINEAR walkers
-(bh_uhf_collinear_snapshot.npz) and Li with a polarized ROHF trial and COLLINEAR walkers
+(bh_uhf_collinear_snapshot.npz), BH with the RHF trial and COLLINEAR walkers
+(bh_rhf_collinear_snapshot.npz), Li with a polarized ROHF trial and COLLINEAR walkers
 (li_rohf_collinear_snapshot.npz), and the statistical reference of the first (bh_rhf_closed_statistical.json).
 
     python tests/golden/make_bh_snapshot.py [SAFIRE source tree]
@@ -70,6 +71,10 @@ def main():
     # the same Hamiltonian with a UHF trial (the Hamiltonian tensors are those of the file above)
     snapshot_case(fn, "BH", "afqmc_H_rhf_closed.h5", "afqmc_uhf_nomsd.h5",
                   "dense_rhf_basis_closed/uhf_nomsd/collinear", "COLLINEAR", "bh_uhf_collinear_snapshot.npz",
+                  with_hamiltonian=False)
+    # the RHF trial upgraded to COLLINEAR walkers (both spins the same orbitals)
+    snapshot_case(fn, "BH", "afqmc_H_rhf_closed.h5", "afqmc_rhf_nomsd.h5",
+                  "dense_rhf_basis_closed/rhf_nomsd/collinear", "COLLINEAR", "bh_rhf_collinear_snapshot.npz",
                   with_hamiltonian=False)
     snapshot_case(fn, "Li", "hamil_closed.h5", "rohf_nomsd_polarized.h5",
                   "hamil_closed/rohf_wfn_polarized/collinear", "COLLINEAR", "li_rohf_collinear_snapshot.npz")

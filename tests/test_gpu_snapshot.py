@@ -18,7 +18,7 @@ from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, snapshot, snapsho
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["bh_rhf_closed", "bh_uhf_collinear", "li_rohf_collinear"]
+CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_rhf_collinear", "li_rohf_collinear"]
 
 
 def _system(snap):

@@ -54,7 +54,7 @@ def _oracle_hamiltonian(snap):
     return O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
 
 
-@pytest.mark.parametrize("case", ["bh_rhf_closed", "bh_uhf_collinear", "li_rohf_collinear"])
+@pytest.mark.parametrize("case", ["bh_rhf_closed", "bh_uhf_collinear", "bh_rhf_collinear", "li_rohf_collinear"])
 def test_oracle_reproduces_reference_snapshot(case):
     """BH with an RHF trial and CLOSED walkers, BH with a UHF trial and COLLINEAR walkers, Li with a
     fully polarized ROHF trial (no down electrons) and COLLINEAR walkers."""
@@ -101,8 +101,8 @@ def test_loaders_read_reference_files():
     coll = load_nomsd_trial(f"{REF}/afqmc_inputs/Li/rohf_nomsd_polarized.h5", "COLLINEAR")
     li = snapshot("li_rohf_collinear")
     assert coll["ndn"] == 0 and np.array_equal(coll["PsiT_up"], li["PsiT_up"])
-    with pytest.raises(InputError):
-        load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_rhf_nomsd.h5", "COLLINEAR")  # closed trial
+    up = load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_rhf_nomsd.h5", "COLLINEAR")  # closed trial, upgraded
+    assert np.array_equal(up["PsiT_up"], up["PsiT_dn"]) and np.array_equal(up["PsiT_up"], snap["PsiT"])
     with pytest.raises(InputError):
         load_nomsd_trial(f"{REF}/afqmc_inputs/BH/afqmc_casci_rhf_nomsd.h5")  # several determinants
     with pytest.raises(InputError):
