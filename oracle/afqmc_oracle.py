@@ -246,6 +246,9 @@ class Hamiltonian:
     def orthogonalize(self, SM):
         return orthogonalize(SM)[0]
 
+    def propagate(self, SM, P1, V, order):
+        return propagate(SM, P1, V, order)
+
 
 class CollinearHamiltonian(Hamiltonian):
     """The same dense Hamiltonian for COLLINEAR walkers and a single-determinant NOMSD trial with
@@ -329,6 +332,74 @@ class CollinearHamiltonian(Hamiltonian):
                     Kl += np.einsum('wana->wn', T)
         if addEJ:
             E[:, 2] += 0.5 * np.einsum('wn,wn->w', Kl, Kl)
+        return E
+
+
+class NoncollinearHamiltonian(Hamiltonian):
+    """The same dense, spin-independent Hamiltonian for NONCOLLINEAR walkers: a walker is one
+    (2M, N) spinor matrix (the two components' rows one after the other), the trial PsiT (N, 2M).
+
+      half rotation   haj = PsiT blockdiag(hcore, hcore); Lnak[n, a, p M + k] = sum_i PsiT[a, p M + i]
+                      L[i, k, n] (RealDenseHamiltonian.cpp:141-161 with npol = 2)
+      G, overlap      one determinant of the 2M x N matrix, counted once (NOMSD.hpp:293-343)
+      vbias           a = sqrt(dt), G Lnak^T over (a, p, k) (Real3IndexFactorization.hpp:328-390)
+      energy          scale 1, the exchange tensor summed over both components (:476-560)
+      P1, vHS         polarization independent: the M x M propagators act on each component
+                      (getOneBodyPropagatorMatrix :99-124, propagate_impl propagate.hpp:247-298)
+    """
+
+    def __init__(self, hcore, Likn, PsiT, E0=0.0, ci=1.0):
+        PsiT = np.asarray(PsiT, dtype=np.complex128)
+        M = np.asarray(hcore).shape[0]
+        assert PsiT.shape[1] == 2 * M
+        super().__init__(hcore, Likn, PsiT[:, :M], E0)
+        self.PsiT = PsiT
+        self.ci = complex(ci)
+        self.N = PsiT.shape[0]
+        Nc = self.Nc
+        h = self.hcore.astype(np.complex128)
+        self.haj = np.concatenate([PsiT[:, :M] @ h, PsiT[:, M:] @ h], axis=1)
+        L2 = self.Likn.reshape(M, M * Nc)
+        parts = []
+        for q in (PsiT[:, :M], PsiT[:, M:]):
+            parts.append((q.real @ L2 + 1j * (q.imag @ L2)).reshape(self.N, M, Nc))
+        self.Lnak = np.ascontiguousarray(np.transpose(np.concatenate(parts, axis=1), (2, 0, 1)))  # (Nc, N, 2M)
+
+    def _lci(self):
+        return np.log(1e-12 if abs(self.ci) < 1e-12 else np.conj(self.ci))
+
+    def green(self, SM):
+        G, ov = mixed_density_matrix(self.PsiT, SM, compact=True)
+        return G, ov + self._lci()
+
+    def log_overlap(self, SM):
+        return log_overlap(self.PsiT, SM) + self._lci()
+
+    def trial_walker(self):
+        return np.conj(self.PsiT.T)
+
+    def propagate(self, SM, P1, V, order):
+        W, M2, N = SM.shape
+        M = M2 // 2
+        halves = np.ascontiguousarray(SM).reshape(2 * W, M, N)
+        return propagate(halves, P1, np.repeat(V, 2, axis=0), order).reshape(W, M2, N)
+
+    def vbias(self, G, dt):
+        W = G.shape[0]
+        return math.sqrt(dt) * (G.reshape(W, -1) @ self.Lnak.reshape(self.Nc, -1).T)
+
+    def energy(self, G, addH1=True, addEJ=True, addEXX=True, chunk=None):
+        W, N, M2 = G.shape
+        Nc = self.Nc
+        E = np.zeros((W, 3), dtype=np.complex128)
+        if addH1:
+            E[:, 0] = self.E0 + np.einsum('waj,aj->w', G, self.haj)
+        if addEXX:
+            T = (G.reshape(W * N, M2) @ self.Lnak.reshape(Nc * N, M2).T).reshape(W, N, Nc, N)  # T[w,b,n,a]
+            E[:, 1] = -0.5 * np.einsum('wanb,wbna->w', T, T)
+            if addEJ:
+                Kl = np.einsum('wana->wn', T)
+                E[:, 2] = 0.5 * np.einsum('wn,wn->w', Kl, Kl)
         return E
 
 
@@ -653,7 +724,7 @@ class Propagator:
         X, HW = assemble_X(vb, self.vmf, uniforms, self.vbias_bound)
         mf = meanfield_factor(X, self.vmf)
         V = ham.vHS(X, self.dt)
-        wset.SM = propagate(wset.SM, self.P1, V, self.order)
+        wset.SM = ham.propagate(wset.SM, self.P1, V, self.order)
         new_ov = ham.log_overlap(wset.SM)
         walker_update(wset, self.dt, Eshift, ham.E0, new_ov, mf, HW, self.lower, self.upper)
         tp = W if target_population is None else target_population

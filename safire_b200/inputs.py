@@ -44,7 +44,8 @@ def _complex_last(a, rank):
 
 
 def energy_offset(f, nup, ndn=0, closed=True):
-    """read_energy_offset (hdf5_helpers.hpp:84-106): nuclear + frozen core - madelung * nelec."""
+    """read_energy_offset (hdf5_helpers.hpp:84-106): nuclear + frozen core - madelung * nelec, nelec
+    2 nup for CLOSED walkers, nup + ndn otherwise (NONCOLLINEAR: nup is every electron, ndn 0)."""
     at = f.attrs("Hamiltonian")
     nuc = float(at.get("nuclear_energy", 0.0))
     fzc = float(at.get("frozen_core_energy", 0.0))
@@ -55,9 +56,9 @@ def energy_offset(f, nup, ndn=0, closed=True):
     return nuc + fzc + mad
 
 
-def load_dense_hamiltonian(path, nup):
-    """hcore (nmo, nmo) real, Likn (nmo, nmo, nchol) real and E0 of a dense Cholesky Hamiltonian
-    for CLOSED walkers with nup electrons per spin."""
+def load_dense_hamiltonian(path, nup, ndn=None):
+    """hcore (nmo, nmo) real, Likn (nmo, nmo, nchol) real and E0 of a dense Cholesky Hamiltonian;
+    ndn None: CLOSED walkers with nup electrons per spin, else nup up and ndn down electrons."""
     f = H5File(path)
     _check("Hamiltonian" in f, f"{path}: no Hamiltonian group")
     _check("Hamiltonian/DenseFactorized/L" in f, f"{path}: not a dense factorized Hamiltonian "
@@ -79,7 +80,7 @@ def load_dense_hamiltonian(path, nup):
     _check(not np.iscomplexobj(L), "DenseFactorized/L must be real")
     Likn = np.ascontiguousarray(L[0, 0, :, 0, :, :], dtype=np.float64)
     return dict(hcore=np.ascontiguousarray(hc, dtype=np.float64), Likn=Likn,
-                E0=energy_offset(f, nup), nmo=nmo, nchol=Likn.shape[2])
+                E0=energy_offset(f, nup, ndn or 0, closed=ndn is None), nmo=nmo, nchol=Likn.shape[2])
 
 
 def read_csr(f, group):
@@ -121,22 +122,35 @@ def load_nomsd_trial(path, walker_type="CLOSED"):
     upgraded, from a closed one (both spins the same orbitals) (read_wavefunction_info,
     readWfn.cpp:86-119; read_nomsd_wavefunction, readWfn.h:90-139)."""
     walker_type = walker_type.upper()
-    _check(walker_type in ("CLOSED", "COLLINEAR"), f"walker type {walker_type}: the path takes CLOSED or COLLINEAR")
+    _check(walker_type in ("CLOSED", "COLLINEAR", "NONCOLLINEAR"), f"unknown walker type {walker_type}")
     f = H5File(path)
     _check("Wavefunction/NOMSD" in f, f"{path}: no Wavefunction/NOMSD group")
     at = f.attrs("Wavefunction/NOMSD")
     spin = at.get("spin_type")
     if spin is not None:
         spin = str(spin).lower()
-        ok = spin == walker_type.lower() or (spin == "closed" and walker_type == "COLLINEAR")
-        _check(ok, f"wavefunction spin_type is '{spin}': {walker_type} walkers take a "
-                   f"{'closed or collinear' if walker_type == 'COLLINEAR' else 'closed'} trial here")
+        order = ("closed", "collinear", "noncollinear")  # walkerTypeIsConvertible: upgrades only
+        _check(spin in order and order.index(spin) <= order.index(walker_type.lower()),
+               f"wavefunction spin_type is '{spin}': {walker_type} walkers cannot take it")
     ci = np.atleast_1d(_complex_last(f["Wavefunction/NOMSD/ci_coeffs"], 1))
     _check(ci.size == 1, f"{ci.size} determinants: the path takes a single-determinant trial")
     _check("Wavefunction/NOMSD/PsiT_0" in f, "Wavefunction/NOMSD/PsiT_0 missing")
     PsiT = read_csr(f, "Wavefunction/NOMSD/PsiT_0")
     out = dict(PsiT=PsiT, ci=complex(ci[0]), nup=PsiT.shape[0], nmo=PsiT.shape[1], spin_type=spin)
-    if walker_type == "COLLINEAR" and spin == "closed":
+    if walker_type == "NONCOLLINEAR":
+        # one (nel, 2 nmo) spinor matrix: native, or the up rows over the down rows shifted by nmo
+        # (combine_csr, readWfn.h:116-153)
+        if spin == "noncollinear":
+            _check(PsiT.shape[1] % 2 == 0, f"noncollinear PsiT_0 has {PsiT.shape[1]} columns, not 2 nmo")
+            sp = PsiT
+        else:
+            dn = read_csr(f, "Wavefunction/NOMSD/PsiT_1") if spin == "collinear" else PsiT
+            M = PsiT.shape[1]
+            sp = np.zeros((PsiT.shape[0] + dn.shape[0], 2 * M), np.complex128)
+            sp[:PsiT.shape[0], :M] = PsiT
+            sp[PsiT.shape[0]:, M:] = dn
+        out.update(PsiT=sp, nup=sp.shape[0], nmo=sp.shape[1] // 2)
+    elif walker_type == "COLLINEAR" and spin == "closed":
         out.update(PsiT_up=PsiT, PsiT_dn=PsiT.copy(), ndn=PsiT.shape[0])  # readWfn.h:130-139
     elif walker_type == "COLLINEAR":
         _check("Wavefunction/NOMSD/PsiT_1" in f, "Wavefunction/NOMSD/PsiT_1 missing for a collinear trial")
@@ -150,12 +164,16 @@ def load_system(hamiltonian_path, wavefunction_path, walker_type="CLOSED"):
     """The engine's System (hcore, Likn, PsiT, E0 and sizes) from a Hamiltonian and a trial file; for
     COLLINEAR walkers PsiT stacks the up rows over the down rows and nel_dn counts the latter."""
     from .synthetic import System, SystemSpec
-    wfn = load_nomsd_trial(wavefunction_path, walker_type)
-    ham = load_dense_hamiltonian(hamiltonian_path, wfn["nup"])
-    _check(wfn["nmo"] == ham["nmo"], f"trial has {wfn['nmo']} orbitals, Hamiltonian {ham['nmo']}")
-    if walker_type.upper() == "COLLINEAR":
+    wt = walker_type.upper()
+    _check(wt in ("CLOSED", "COLLINEAR"), f"the engine runs CLOSED and COLLINEAR walkers, not {wt}")
+    wfn = load_nomsd_trial(wavefunction_path, wt)
+    if wt == "COLLINEAR":
+        ham = load_dense_hamiltonian(hamiltonian_path, wfn["nup"], wfn["ndn"])
+        _check(wfn["nmo"] == ham["nmo"], f"trial has {wfn['nmo']} orbitals, Hamiltonian {ham['nmo']}")
         PsiT = np.concatenate([wfn["PsiT_up"], wfn["PsiT_dn"]])
         spec = SystemSpec(M=ham["nmo"], N=PsiT.shape[0], Nc=ham["nchol"], decay=0.0)
         return System(spec, ham["hcore"], ham["Likn"], PsiT, ham["E0"], nel_dn=wfn["ndn"])
+    ham = load_dense_hamiltonian(hamiltonian_path, wfn["nup"])
+    _check(wfn["nmo"] == ham["nmo"], f"trial has {wfn['nmo']} orbitals, Hamiltonian {ham['nmo']}")
     spec = SystemSpec(M=ham["nmo"], N=wfn["nup"], Nc=ham["nchol"], decay=0.0)
     return System(spec, ham["hcore"], ham["Likn"], wfn["PsiT"], ham["E0"])

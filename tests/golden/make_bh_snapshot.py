@@ -1,7 +1,8 @@
 """Extract the dense-Cholesky NOMSD cases of the reference's functional tests: the seeded snapshots
 of BH with CLOSED walkers (bh_rhf_closed_snapshot.npz), BH with a UHF trial and COLLINEAR walkers
 (bh_uhf_collinear_snapshot.npz), BH with the RHF trial and COLLINEAR walkers
-(bh_rhf_collinear_snapshot.npz), Li with a polarized ROHF trial and COLLINEAR walkers
+(bh_rhf_collinear_snapshot.npz), BH with NONCOLLINEAR walkers and the RHF, UHF and GHF trials
+(bh_{rhf,uhf,ghf}_noncollinear_snapshot.npz), Li with a polarized ROHF trial and COLLINEAR walkers
 (li_rohf_collinear_snapshot.npz), and the statistical reference of the first (bh_rhf_closed_statistical.json).
 
     python tests/golden/make_bh_snapshot.py [SAFIRE source tree]
@@ -41,7 +42,8 @@ OBSERVABLES = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "Ov
 def snapshot_case(fn, system, ham_file, wfn_file, case, walker_type, out_name, with_hamiltonian=True):
     """One seeded snapshot case: inputs as the engine takes them, settings, recorded mean / error."""
     wfn = load_nomsd_trial(os.path.join(fn, "afqmc_inputs", system, wfn_file), walker_type)
-    ham = load_dense_hamiltonian(os.path.join(fn, "afqmc_inputs", system, ham_file), wfn["nup"])
+    ndn = None if walker_type == "CLOSED" else (wfn.get("ndn", 0))
+    ham = load_dense_hamiltonian(os.path.join(fn, "afqmc_inputs", system, ham_file), wfn["nup"], ndn)
     res = H5File(os.path.join(fn, "snapshot_references", system, *case.split("/"), "results.h5"))
     inp = json.loads(res["input_file"])
     ex = inp["execute"]
@@ -76,6 +78,10 @@ def main():
     snapshot_case(fn, "BH", "afqmc_H_rhf_closed.h5", "afqmc_rhf_nomsd.h5",
                   "dense_rhf_basis_closed/rhf_nomsd/collinear", "COLLINEAR", "bh_rhf_collinear_snapshot.npz",
                   with_hamiltonian=False)
+    # NONCOLLINEAR walkers: the RHF and UHF trials upgraded to spinors, and a GHF trial
+    for wfn, name in (("afqmc_rhf_nomsd.h5", "rhf"), ("afqmc_uhf_nomsd.h5", "uhf"), ("afqmc_ghf_nomsd.h5", "ghf")):
+        snapshot_case(fn, "BH", "afqmc_H_rhf_closed.h5", wfn, f"dense_rhf_basis_closed/{name}_nomsd/noncollinear",
+                      "NONCOLLINEAR", f"bh_{name}_noncollinear_snapshot.npz", with_hamiltonian=False)
     snapshot_case(fn, "Li", "hamil_closed.h5", "rohf_nomsd_polarized.h5",
                   "hamil_closed/rohf_wfn_polarized/collinear", "COLLINEAR", "li_rohf_collinear_snapshot.npz")
 

@@ -1,9 +1,9 @@
 """The reference's seeded snapshot of a real molecule, replayed on its own random streams.
 
-The dense-Cholesky NOMSD cases of the reference's functional tests (BH with an RHF trial and CLOSED
-walkers, BH with a UHF trial and Li with a polarized ROHF trial and COLLINEAR walkers; seed 42,
-50 walkers, 20 steps, one rank) recorded every energy-estimator observable; the reference's runner
-requires a rerun to reproduce them to 1e-9.  These tests pin:
+The dense-Cholesky single-determinant NOMSD cases of the reference's functional tests (BH and Li;
+CLOSED, COLLINEAR and NONCOLLINEAR walkers; seed 42, 50 walkers, 20 steps, one rank) recorded every
+energy-estimator observable; the reference's runner requires a rerun to reproduce them to 1e-9.
+These tests pin:
 
   * the host random streams (std::mt19937 via split_seed, uniform_real_distribution) against the
     C++ standard's known answer and numpy's independent MT19937;
@@ -48,16 +48,23 @@ def test_split_seed_streams_distinct():
 
 
 def _oracle_hamiltonian(snap):
+    if snap["settings"]["walker_type"] == "NONCOLLINEAR":
+        return O.NoncollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"], snap["ci"])
     if snap["settings"]["walker_type"] == "COLLINEAR":
         return O.CollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_up"], snap["PsiT_dn"], snap["E0"],
                                       snap["ci"])
     return O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
 
 
-@pytest.mark.parametrize("case", ["bh_rhf_closed", "bh_uhf_collinear", "bh_rhf_collinear", "li_rohf_collinear"])
+SNAPSHOT_CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_rhf_collinear", "li_rohf_collinear",
+                  "bh_rhf_noncollinear", "bh_uhf_noncollinear", "bh_ghf_noncollinear"]
+
+
+@pytest.mark.parametrize("case", SNAPSHOT_CASES)
 def test_oracle_reproduces_reference_snapshot(case):
-    """BH with an RHF trial and CLOSED walkers, BH with a UHF trial and COLLINEAR walkers, Li with a
-    fully polarized ROHF trial (no down electrons) and COLLINEAR walkers."""
+    """BH with an RHF trial and CLOSED walkers; COLLINEAR walkers with BH's UHF and RHF trials and Li's
+    fully polarized ROHF trial (no down electrons); NONCOLLINEAR walkers with BH's RHF and UHF trials
+    upgraded to spinors and a GHF trial."""
     snap = snapshot(case)
     st = snap["settings"]
     assert st["num_ranks"] == 1
