@@ -185,7 +185,7 @@ typedef struct {
   unsigned long long seed;       /* Philox key for fields and comb */
   int device;                    /* CUDA device ordinal */
   int precision;                 /* SFQ_PRECISION_FP64 (drop-in) or SFQ_PRECISION_MIXED */
-  int walker_type;               /* SFQ_WALKER_CLOSED (0 reads as CLOSED) or SFQ_WALKER_COLLINEAR */
+  int walker_type;               /* SFQ_WALKER_CLOSED (0 reads as CLOSED), _COLLINEAR or _NONCOLLINEAR */
   int nel_dn;                    /* COLLINEAR: down electrons, may be 0 (nel = up electrons) */
 } sfq_engine_params_t;
 
@@ -194,9 +194,13 @@ typedef struct {
  * both spins.  Engine arrays then hold nel + nel_dn electrons per walker: PsiT is passed as the
  * stacked (nel + nel_dn, nmo) matrix [PsiT_up; PsiT_dn], a walker's SM is (nmo, nel + nel_dn) with
  * the up columns first, and sfq_engine_export_walker_buffer writes the reference's rows (the up
- * block nmo x nel, then the down block nmo x nel_dn).  COLLINEAR runs in SFQ_PRECISION_FP64. */
+ * block nmo x nel, then the down block nmo x nel_dn).  NONCOLLINEAR walkers are (2 nmo, nel) spinor
+ * matrices (the two components' rows one after the other) against PsiT (nel, 2 nmo), nel every
+ * electron and nel_dn unused; the Hamiltonian acts on each component.  COLLINEAR and NONCOLLINEAR
+ * run in SFQ_PRECISION_FP64. */
 #define SFQ_WALKER_CLOSED 1
 #define SFQ_WALKER_COLLINEAR 2
+#define SFQ_WALKER_NONCOLLINEAR 3
 
 /* SFQ_PRECISION_MIXED / _MIXED_FP32: vbias, vHS, the P1 products and the Taylor terms run on the tcgen05 tensor
  * cores as split-BF16 products (see sfq_gemm_split_bf16) with FP32 accumulation; the mixed density

@@ -167,6 +167,7 @@ class AfqmcEngine:
 
     def __init__(self, system, nwalk, dt=0.005, seed=0, device=0, **params):
         self.M, self.N, self.Nc, self.W = system.M, system.N, system.Nc, nwalk
+        self.Mr = getattr(system, "npol", 1) * system.M  # rows of a walker (NONCOLLINEAR spinors: 2M)
         self.dt = dt
         p = capi.system_params(system, nwalk=nwalk, dt=dt, E0=float(system.E0), seed=seed, device=device)
         for k, v in params.items():
@@ -200,7 +201,7 @@ class AfqmcEngine:
 
     # WalkerSet
     def walkers(self):
-        SM = np.empty((self.W, self.M, self.N), np.complex128)
+        SM = np.empty((self.W, self.Mr, self.N), np.complex128)
         pr = np.empty((len(capi.PROPS), self.W), np.complex128)
         check(lib().sfq_engine_get_walkers(self.h, SM.ctypes.data, pr.ctypes.data))
         return SM, {k: pr[i].copy() for i, k in enumerate(capi.PROPS)}
@@ -214,7 +215,7 @@ class AfqmcEngine:
                                            None if pr is None else pr.ctypes.data))
 
     def walker_buffer(self):
-        rows = np.empty((self.W, self.M * self.N + 11), np.complex128)
+        rows = np.empty((self.W, self.Mr * self.N + 11), np.complex128)
         check(lib().sfq_engine_export_walker_buffer(self.h, rows.ctypes.data))
         return rows
 

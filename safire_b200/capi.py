@@ -37,7 +37,7 @@ class EngineParams(ctypes.Structure):
                 ("precision", ctypes.c_int), ("walker_type", ctypes.c_int), ("nel_dn", ctypes.c_int)]
 
 PRECISION_FP64, PRECISION_MIXED, PRECISION_MIXED_FP32 = 0, 1, 2
-WALKER_CLOSED, WALKER_COLLINEAR = 1, 2
+WALKER_CLOSED, WALKER_COLLINEAR, WALKER_NONCOLLINEAR = 1, 2, 3
 
 
 class RunParams(ctypes.Structure):
@@ -185,13 +185,16 @@ def ptr(x):
 
 
 def system_params(system, **kw):
-    """default_params for a System: CLOSED, or COLLINEAR when the system has nel_dn >= 0 down
-    electrons (its PsiT then stacks the up rows over the down rows)."""
+    """default_params for a System: CLOSED; COLLINEAR when the system has nel_dn >= 0 down electrons
+    (its PsiT then stacks the up rows over the down rows); NONCOLLINEAR when it has npol = 2 (PsiT
+    (N, 2M) spinor orbitals)."""
     nel_dn = getattr(system, "nel_dn", -1)
     coll = nel_dn is not None and nel_dn >= 0
     p = default_params(nmo=system.M, nel=system.N - (nel_dn if coll else 0), nchol=system.Nc, **kw)
     if coll:
         p.walker_type, p.nel_dn = WALKER_COLLINEAR, nel_dn
+    elif getattr(system, "npol", 1) == 2:
+        p.walker_type = WALKER_NONCOLLINEAR
     return p
 
 

@@ -11,6 +11,11 @@
 // What is per spin -- the overlap matrix and its inverse and log det, the CholeskyQR Gram matrix,
 // the exchange pairs -- keeps only the two diagonal spin blocks, which gives exactly the per-spin
 // factorizations (with the pivots LAPACK would choose per spin) and the sum of the two log dets.
+//
+// A NONCOLLINEAR walker is one (2M, N) spinor matrix, the reference's layout, against PsiT (N, 2M):
+// overlaps, G, vbias, the energy and the QR are those of a walker with Mr = 2M rows; P1 and vHS act
+// on each component (the Hamiltonian is polarization-independent), and Lnak / haj are half-rotated
+// per component.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -138,12 +143,16 @@ struct Engine {
   sfq_engine_params_t p{};
   int M = 0, N = 0, Nc = 0, W = 0;
   bool trial_real = true;
-  // COLLINEAR walkers: N = nup + ndn columns, up first (CLOSED: collinear false, N = nup)
+  // COLLINEAR walkers: N = nup + ndn columns, up first (CLOSED: collinear false, N = nup);
+  // NONCOLLINEAR walkers: npol = 2, Mr = 2M rows (CLOSED, COLLINEAR: npol = 1, Mr = M)
   bool collinear = false;
   int nup = 0;
-  int spin_split() const { return collinear ? nup : -1; }
-  double ov_scale() const { return collinear ? 1.0 : 2.0; }  // NOMSD.cpp:285-290: CLOSED counts its determinant twice
-  double vb_scale() const { return (collinear ? 1.0 : 2.0) * std::sqrt(p.dt); }  // Real3IndexFactorization.hpp:349
+  int npol = 1, Mr = 0;
+  bool closed() const { return !collinear && npol == 1; }
+  // the exchange's spin split (and the CLOSED marker -1); a NONCOLLINEAR walker is one sector
+  int spin_split() const { return collinear ? nup : (npol == 2 ? N : -1); }
+  double ov_scale() const { return closed() ? 2.0 : 1.0; }  // NOMSD.cpp:285-290: CLOSED counts its determinant twice
+  double vb_scale() const { return (closed() ? 2.0 : 1.0) * std::sqrt(p.dt); }  // Real3IndexFactorization.hpp:349
   cudaStream_t st = nullptr;
   // host-buffer steps: the field uniforms go in on a copy stream while the step's density and force
   // bias run; the fields kernel waits for uni_wait (cleared once waited on)
@@ -307,28 +316,29 @@ struct Engine {
   int allocate() {
     const size_t c = sizeof(cplx), d = sizeof(double);
     const long MN = (long)M * N, NN = (long)N * N, MM = (long)M * M;
+    const long RN = (long)Mr * N;  // a walker's elements
     tchunk_elems = (long)W * N * ops::energy_chunk(W, N, Nc, kEnergyChunkElems) * N;
     struct Item { void** ptr; size_t bytes; };
     std::vector<Item> items = {
         {(void**)&hcore, d * MM},
         {(void**)&Likn, d * MM * Nc},
-        {(void**)&PsiT, c * N * M},
-        {(void**)&PsiTr, d * N * M},
-        {(void**)&Lnak, (trial_real ? d : c) * (size_t)Nc * N * M},
-        {(void**)&haj, c * N * M},
+        {(void**)&PsiT, c * RN},
+        {(void**)&PsiTr, d * RN},
+        {(void**)&Lnak, (trial_real ? d : c) * (size_t)Nc * RN},
+        {(void**)&haj, c * RN},
         {(void**)&v0, d * MM},
         {(void**)&vmf, d * Nc},
         {(void**)&P1, d * MM},
-        {(void**)&SM, c * W * MN},
+        {(void**)&SM, c * W * RN},
         {(void**)&props, c * kNumProps * W},
-        {(void**)&SM2, c * W * MN},
+        {(void**)&SM2, c * W * RN},
         {(void**)&T, c * W * NN},
-        {(void**)&G, c * W * MN},
+        {(void**)&G, c * W * RN},
         {(void**)&X, c * (size_t)W * Nc},
         {(void**)&V, c * W * MM},
-        {(void**)&TMN, c * W * MN},
-        {(void**)&T1, c * W * MN},
-        {(void**)&T2, c * W * MN},
+        {(void**)&TMN, c * W * RN},
+        {(void**)&T1, c * W * RN},
+        {(void**)&T2, c * W * RN},
         {(void**)&hw, c * W},
         {(void**)&mf, c * W},
         {(void**)&newov, c * W},
@@ -395,10 +405,10 @@ struct Engine {
     const long MM = (long)M * M;
     SFQ_CUDA_TRY(cudaMemcpyAsync(hcore, h_hcore, sizeof(double) * MM, cudaMemcpyHostToDevice, st));
     SFQ_CUDA_TRY(cudaMemcpyAsync(Likn, h_Likn, sizeof(double) * MM * Nc, cudaMemcpyHostToDevice, st));
-    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiT, h_PsiT, sizeof(cplx) * N * M, cudaMemcpyHostToDevice, st));
-    std::vector<double> pr(size_t(N) * M);
+    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiT, h_PsiT, sizeof(cplx) * N * Mr, cudaMemcpyHostToDevice, st));
+    std::vector<double> pr(size_t(N) * Mr);
     for (size_t i = 0; i < pr.size(); ++i) pr[i] = h_PsiT[i].x;
-    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiTr, pr.data(), sizeof(double) * N * M, cudaMemcpyHostToDevice, st));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiTr, pr.data(), sizeof(double) * N * Mr, cudaMemcpyHostToDevice, st));
     {
       int asym = 1;
       SFQ_CUDA_TRY(cudaMemsetAsync(pw.flag, 0, sizeof(int), st));
@@ -416,27 +426,40 @@ struct Engine {
     }
     SFQ_CUDA_TRY(cudaStreamSynchronize(st));
 
-    // Lnak[n][a][k] = sum_i PsiT[a][i] L[i][k][n]  via tmp[a][(k,n)] then a permute
+    // Lnak[n][a][k] = sum_i PsiT[a][i] L[i][k][n]  via tmp[a][(k,n)] then a permute; NONCOLLINEAR:
+    // Lnak[n][a][q M + k] from PsiT's component q (RealDenseHamiltonian.cpp:141-161 with npol = 2)
     {
       void* tmp = nullptr;
+      void* lq = nullptr;
       const size_t esz = trial_real ? sizeof(double) : sizeof(cplx);
       SFQ_CUDA_TRY(cudaMallocAsync(&tmp, esz * (size_t)N * M * Nc, st));
-      GemmDesc d;
-      d.M = N; d.N = int((long)M * Nc); d.K = M;
-      d.A = trial_real ? (const void*)PsiTr : (const void*)PsiT; d.sAm = M; d.sAk = 1; d.a_cplx = !trial_real;
-      d.B = Likn; d.sBk = (long)M * Nc; d.sBn = 1; d.b_cplx = false;
-      d.C = tmp; d.sCm = (long)M * Nc; d.sCn = 1;
-      if ((rc = gemm_f64(d, st))) return rc;
-      if ((rc = permute_lnak(tmp, Lnak, N, M, Nc, int(esz), st))) return rc;
+      if (npol > 1) SFQ_CUDA_TRY(cudaMallocAsync(&lq, esz * (size_t)N * M * Nc, st));
+      for (int q = 0; q < npol; ++q) {
+        GemmDesc d;
+        d.M = N; d.N = int((long)M * Nc); d.K = M;
+        d.A = trial_real ? (const void*)(PsiTr + (long)q * M) : (const void*)(PsiT + (long)q * M);
+        d.sAm = Mr; d.sAk = 1; d.a_cplx = !trial_real;
+        d.B = Likn; d.sBk = (long)M * Nc; d.sBn = 1; d.b_cplx = false;
+        d.C = tmp; d.sCm = (long)M * Nc; d.sCn = 1;
+        if ((rc = gemm_f64(d, st))) return rc;
+        if (npol == 1) {
+          if ((rc = permute_lnak(tmp, Lnak, N, M, Nc, int(esz), st))) return rc;
+        } else {
+          if ((rc = permute_lnak(tmp, lq, N, M, Nc, int(esz), st))) return rc;
+          SFQ_CUDA_TRY(cudaMemcpy2DAsync(static_cast<char*>(Lnak) + (size_t)q * M * esz, Mr * esz, lq, M * esz,
+                                         M * esz, (size_t)Nc * N, cudaMemcpyDeviceToDevice, st));
+        }
+      }
       SFQ_CUDA_TRY(cudaFreeAsync(tmp, st));
+      if (lq) SFQ_CUDA_TRY(cudaFreeAsync(lq, st));
     }
-    // haj = PsiT * hcore  (one_body.hpp:124-153)
-    {
+    // haj = PsiT * hcore  (one_body.hpp:124-153); NONCOLLINEAR: PsiT * blockdiag(hcore, hcore)
+    for (int q = 0; q < npol; ++q) {
       GemmDesc d;
       d.M = N; d.N = M; d.K = M;
-      d.A = PsiT; d.sAm = M; d.sAk = 1; d.a_cplx = true;
+      d.A = PsiT + (long)q * M; d.sAm = Mr; d.sAk = 1; d.a_cplx = true;
       d.B = hcore; d.sBk = M; d.sBn = 1; d.b_cplx = false;
-      d.C = haj; d.sCm = M; d.sCn = 1;
+      d.C = haj + (long)q * M; d.sCm = Mr; d.sCn = 1;
       if ((rc = gemm_f64(d, st))) return rc;
     }
     // v0 = -1/2 L L^T over (j, n)   (RealDenseHamiltonian.cpp:165-180)
@@ -452,15 +475,15 @@ struct Engine {
     }
     // vMF = Re vbias(G_trial)  (NOMSD.cpp:437-466; AFQMCBasePropagator.cpp:107 zero_imag)
     if (p.subtractMF) {
-      std::vector<cplx> psi(size_t(M) * N);  // PsiT^H  (M x N)
+      std::vector<cplx> psi(size_t(Mr) * N);  // PsiT^H  (Mr x N)
       for (int a = 0; a < N; ++a)
-        for (int i = 0; i < M; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * M + i]);
-      SFQ_CUDA_TRY(cudaMemcpyAsync(SM2, psi.data(), sizeof(cplx) * M * N, cudaMemcpyHostToDevice, st));
-      if ((rc = ops::overlap_matrix(PsiT, true, SM2, T, 1, M, N, st))) return rc;
+        for (int i = 0; i < Mr; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * Mr + i]);
+      SFQ_CUDA_TRY(cudaMemcpyAsync(SM2, psi.data(), sizeof(cplx) * Mr * N, cudaMemcpyHostToDevice, st));
+      if ((rc = ops::overlap_matrix(PsiT, true, SM2, T, 1, Mr, N, st))) return rc;
       if ((rc = ops::mask_cross_spin(T, 1, N, spin_split(), st))) return rc;
       if ((rc = lu_logdet(T, (long)N * N, 1, N, ovtmp, false, 1.0, true, st))) return rc;
-      if ((rc = ops::green_compact(T, SM2, G, 1, M, N, st))) return rc;
-      if ((rc = ops::vbias(G, Lnak, !trial_real, X, 1, N, M, Nc, vb_scale(), st))) return rc;
+      if ((rc = ops::green_compact(T, SM2, G, 1, Mr, N, st))) return rc;
+      if ((rc = ops::vbias(G, Lnak, !trial_real, X, 1, N, Mr, Nc, vb_scale(), st))) return rc;
       if ((rc = real_of(X, vmf, Nc, st))) return rc;
       SFQ_CUDA_TRY(cudaStreamSynchronize(st));
     } else {
@@ -546,11 +569,11 @@ struct Engine {
     }
     // walkers: copies of the trial, unit weight and phase
     {
-      std::vector<cplx> psi(size_t(M) * N);
+      std::vector<cplx> psi(size_t(Mr) * N);
       for (int a = 0; a < N; ++a)
-        for (int i = 0; i < M; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * M + i]);
+        for (int i = 0; i < Mr; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * Mr + i]);
       for (int w = 0; w < W; ++w)
-        SFQ_CUDA_TRY(cudaMemcpyAsync(SM + (size_t)w * M * N, psi.data(), sizeof(cplx) * M * N,
+        SFQ_CUDA_TRY(cudaMemcpyAsync(SM + (size_t)w * Mr * N, psi.data(), sizeof(cplx) * Mr * N,
                                      cudaMemcpyHostToDevice, st));
       SFQ_CUDA_TRY(cudaMemsetAsync(props, 0, sizeof(cplx) * kNumProps * W, st));
       if ((rc = fill_cplx(props + (long)P_WEIGHT * W, W, mk(1.0, 0.0), st))) return rc;
@@ -568,7 +591,7 @@ struct Engine {
     if (!inv_cached) {
       const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
       cplx* out = ov ? ov : ovtmp;
-      if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, M, N, st))) return rc;
+      if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, Mr, N, st))) return rc;
       if ((rc = ops::mask_cross_spin(T, W, N, spin_split(), st))) return rc;
       if ((rc = lu_logdet(T, (long)N * N, W, N, out, false, ov_scale(), true, st))) return rc;
       inv_cached = true;
@@ -583,7 +606,7 @@ struct Engine {
   int density(cplx* ov) {
     int rc;
     if ((rc = ensure_inverse(ov))) return rc;
-    return ops::green_compact(T, SM, G, W, M, N, st);
+    return ops::green_compact(T, SM, G, W, Mr, N, st);
   }
 
   // G for the force bias in the mixed mode: G[w][a][k] = sum_b Tinv[b][a] SM[k][b] as split-BF16
@@ -616,7 +639,7 @@ struct Engine {
     int rc;
     const void* A = trial_real ? (const void*)PsiTr : (const void*)PsiT;
     inv_cached = false;
-    if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, M, N, st))) return rc;
+    if ((rc = ops::overlap_matrix(A, !trial_real, SM, T, W, Mr, N, st))) return rc;
     if ((rc = ops::mask_cross_spin(T, W, N, spin_split(), st))) return rc;
     if ((rc = lu_logdet(T, (long)N * N, W, N, ov, false, ov_scale(), true, st))) return rc;
     inv_cached = true;
@@ -632,7 +655,7 @@ struct Engine {
     if ((rc = density(nullptr))) return rc;                                          // 1. G
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
-    if ((rc = ops::vbias(G, Lnak, !trial_real, X, W, N, M, Nc, vb_scale(), st))) return rc;
+    if ((rc = ops::vbias(G, Lnak, !trial_real, X, W, N, Mr, Nc, vb_scale(), st))) return rc;
     ph_end(SFQ_PH_VBIAS);
     ph_begin(SFQ_PH_FIELDS);
     FieldParams fp;                                                                   // 2. X
@@ -656,7 +679,7 @@ struct Engine {
     ph_end(SFQ_PH_VHS);
     ph_begin(SFQ_PH_PROPAGATE);
     inv_cached = false;
-    if ((rc = ops::propagate(SM, P1, false, V, W, M, N, p.taylor_order, TMN, T1, T2, st))) return rc;  // 4.
+    if ((rc = ops::propagate(SM, P1, false, V, W, M, N, p.taylor_order, TMN, T1, T2, st, npol))) return rc;  // 4.
     ph_end(SFQ_PH_PROPAGATE);
     ph_begin(SFQ_PH_OVERLAP);
     if ((rc = log_overlap(newov))) return rc;                                         // 5.
@@ -1062,13 +1085,13 @@ struct Engine {
       // gives wfn->Log_Overlap(wset) of the orthogonalized walkers without a new factorization
       if (inv_ov != newov)
         SFQ_CUDA_TRY(cudaMemcpyAsync(newov, inv_ov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
-      if ((rc = ops::orthogonalize_carry(SM, SM2, Tchunk, Tchunk + W * NN, G, status, T, newov, ov_scale(), W, M, N,
+      if ((rc = ops::orthogonalize_carry(SM, SM2, Tchunk, Tchunk + W * NN, G, status, T, newov, ov_scale(), W, Mr, N,
                                          st, spin_split())))
         return rc;
       inv_ov = newov;
     } else {
       inv_cached = false;
-      if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, M, N, st, spin_split()))) return rc;
+      if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, Mr, N, st, spin_split()))) return rc;
       if ((rc = log_overlap(newov))) return rc;  // wfn->Log_Overlap(wset)
     }
     SFQ_CUDA_TRY(cudaMemcpyAsync(props + (long)P_OVLP * W, newov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
@@ -1082,7 +1105,7 @@ struct Engine {
     ph_begin(SFQ_PH_POPCONTROL);
     inv_cached = false;
     const bool own = r >= 0.0;
-    if ((rc = sfq::population_control(SM, (long)M * N, wprops(), W, own ? r : 0.0, p.seed, call, own ? 0 : 1, pw, st,
+    if ((rc = sfq::population_control(SM, (long)Mr * N, wprops(), W, own ? r : 0.0, p.seed, call, own ? 0 : 1, pw, st,
                                       dev_mode && !own ? d_step : nullptr)))
       return rc;
     ph_end(SFQ_PH_POPCONTROL);
@@ -1101,7 +1124,7 @@ struct Engine {
     if (mixed) return energy_mixed();
     ph_begin(SFQ_PH_ENERGY);
     if ((rc = density(ovtmp))) return rc;
-    if ((rc = ops::energy(E3, G, haj, Lnak, !trial_real, p.E0, W, N, M, Nc, 1, 1, 1, Tchunk, tchunk_elems, exxn, kl,
+    if ((rc = ops::energy(E3, G, haj, Lnak, !trial_real, p.E0, W, N, Mr, Nc, 1, 1, 1, Tchunk, tchunk_elems, exxn, kl,
                           st, spin_split())))
       return rc;
     ph_end(SFQ_PH_ENERGY);
@@ -1569,11 +1592,11 @@ int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const dou
   if (!out || !p || !hcore || !Likn || !PsiT) return record_error(SFQ_ERR_ARG, "null pointer");
   *out = nullptr;
   const int wt = p->walker_type == 0 ? SFQ_WALKER_CLOSED : p->walker_type;
-  if (wt != SFQ_WALKER_CLOSED && wt != SFQ_WALKER_COLLINEAR)
-    return record_error(SFQ_ERR_UNSUPPORTED, "engine: walker type %d (CLOSED = 1 and COLLINEAR = 2 are built)",
-                        p->walker_type);
+  if (wt != SFQ_WALKER_CLOSED && wt != SFQ_WALKER_COLLINEAR && wt != SFQ_WALKER_NONCOLLINEAR)
+    return record_error(SFQ_ERR_UNSUPPORTED, "engine: unknown walker type %d", p->walker_type);
   const bool coll = wt == SFQ_WALKER_COLLINEAR;
-  if (p->nmo <= 0 || p->nel <= 0 || p->nchol <= 0 || p->nwalk <= 0 || p->nel > p->nmo ||
+  const int npol = wt == SFQ_WALKER_NONCOLLINEAR ? 2 : 1;
+  if (p->nmo <= 0 || p->nel <= 0 || p->nchol <= 0 || p->nwalk <= 0 || p->nel > npol * p->nmo ||
       (coll && (p->nel_dn < 0 || p->nel_dn > p->nmo)))
     return record_error(SFQ_ERR_SHAPE, "engine: invalid sizes nmo=%d nel=%d nel_dn=%d nchol=%d nwalk=%d", p->nmo,
                         p->nel, p->nel_dn, p->nchol, p->nwalk);
@@ -1588,9 +1611,11 @@ int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const dou
   e.M = p->nmo; e.N = ntot; e.Nc = p->nchol; e.W = p->nwalk;
   e.collinear = coll;
   e.nup = p->nel;
+  e.npol = npol;
+  e.Mr = npol * p->nmo;
   const cplx* ps = reinterpret_cast<const cplx*>(PsiT);
   e.trial_real = true;
-  for (long i = 0; i < (long)e.N * e.M; ++i)
+  for (long i = 0; i < (long)e.N * e.Mr; ++i)
     if (ps[i].y != 0.0) { e.trial_real = false; break; }
   e.mixed = p->precision == SFQ_PRECISION_MIXED || p->precision == SFQ_PRECISION_MIXED_FP32;
   e.nplanes = p->precision == SFQ_PRECISION_MIXED_FP32 ? 3 : 2;
@@ -1598,9 +1623,9 @@ int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const dou
     delete h;
     return record_error(SFQ_ERR_ARG, "engine: unknown precision %d", p->precision);
   }
-  if (e.mixed && coll) {
+  if (e.mixed && (coll || npol > 1)) {
     delete h;
-    return record_error(SFQ_ERR_UNSUPPORTED, "engine: COLLINEAR walkers run in FP64 (SFQ_PRECISION_FP64)");
+    return record_error(SFQ_ERR_UNSUPPORTED, "engine: COLLINEAR and NONCOLLINEAR walkers run in FP64 (SFQ_PRECISION_FP64)");
   }
   if (e.mixed && (!e.trial_real || e.M % 8 || e.Nc % 8)) {
     delete h;
@@ -1651,7 +1676,7 @@ int sfq_engine_set_walkers(sfq_engine_t h, const void* SM, const void* props) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
   Engine& e = h->e;
   e.inv_cached = false;  // also the way to announce writes made through sfq_engine_info's SM pointer
-  if (SM) SFQ_CUDA_TRY(cudaMemcpyAsync(e.SM, SM, sizeof(cplx) * e.W * e.M * e.N, cudaMemcpyHostToDevice, e.st));
+  if (SM) SFQ_CUDA_TRY(cudaMemcpyAsync(e.SM, SM, sizeof(cplx) * e.W * e.Mr * e.N, cudaMemcpyHostToDevice, e.st));
   if (props) SFQ_CUDA_TRY(cudaMemcpyAsync(e.props, props, sizeof(cplx) * kNumProps * e.W, cudaMemcpyHostToDevice, e.st));
   SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
   return SFQ_OK;
@@ -1660,7 +1685,7 @@ int sfq_engine_set_walkers(sfq_engine_t h, const void* SM, const void* props) {
 int sfq_engine_get_walkers(sfq_engine_t h, void* SM, void* props) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
   Engine& e = h->e;
-  if (SM) SFQ_CUDA_TRY(cudaMemcpyAsync(SM, e.SM, sizeof(cplx) * e.W * e.M * e.N, cudaMemcpyDeviceToHost, e.st));
+  if (SM) SFQ_CUDA_TRY(cudaMemcpyAsync(SM, e.SM, sizeof(cplx) * e.W * e.Mr * e.N, cudaMemcpyDeviceToHost, e.st));
   if (props) SFQ_CUDA_TRY(cudaMemcpyAsync(props, e.props, sizeof(cplx) * kNumProps * e.W, cudaMemcpyDeviceToHost, e.st));
   SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
   return SFQ_OK;
@@ -1669,7 +1694,7 @@ int sfq_engine_get_walkers(sfq_engine_t h, void* SM, void* props) {
 int sfq_engine_export_walker_buffer(sfq_engine_t h, void* rows) {
   if (!h || !rows) return record_error(SFQ_ERR_ARG, "null pointer");
   Engine& e = h->e;
-  const long mn = (long)e.M * e.N, rl = mn + 11;
+  const long mn = (long)e.Mr * e.N, rl = mn + 11;
   std::vector<cplx> sm(size_t(e.W) * mn), pr(size_t(kNumProps) * e.W);
   int rc;
   if ((rc = sfq_engine_get_walkers(h, sm.data(), pr.data()))) return rc;

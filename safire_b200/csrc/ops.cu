@@ -98,28 +98,33 @@ static int p1_apply(const void* P1, bool p_cplx, const cplx* in, cplx* out, int 
 }
 
 int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M, int N, int order, cplx* TMN,
-              cplx* T1, cplx* T2, cudaStream_t st) {
+              cplx* T1, cplx* T2, cudaStream_t st, int npol) {
   int rc;
-  const long n = (long)W * M * N;
+  // npol = 2: spinor walkers (2M, N), the two components' M x N blocks one after the other; P1 and
+  // V act on each component (propagate.hpp:247-298, polarization-independent vHS)
+  const long n = (long)W * npol * M * N;
   // TMN = P1 * SM   (propagate.hpp:260)
-  if ((rc = p1_apply(P1, p_cplx, SM, TMN, W, M, N, st))) return rc;
+  if ((rc = p1_apply(P1, p_cplx, SM, TMN, W * npol, M, N, st))) return rc;
   // apply_expM (propagate.hpp:45-70): T1 = S; T2 = (i/n) V T1; S += T2; swap
   SFQ_CUDA_TRY(cudaMemcpyAsync(T1, TMN, n * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
   cplx* a = T1;
   cplx* b = T2;
+  const long MN = (long)M * N;
   for (int k = 1; k <= order; ++k) {
-    GemmDesc d;
-    d.M = M; d.N = N; d.K = M; d.batch = W;
-    d.A = V; d.sAm = M; d.sAk = 1; d.sAb = (long)M * M; d.a_cplx = true;
-    d.B = a; d.sBk = N; d.sBn = 1; d.sBb = (long)M * N; d.b_cplx = true;
-    d.C = b; d.sCm = N; d.sCn = 1; d.sCb = (long)M * N;
-    d.S = TMN;
-    d.alpha = mk(0.0, 1.0 / double(k));
-    if ((rc = gemm_f64(d, st))) return rc;
+    for (int q = 0; q < npol; ++q) {
+      GemmDesc d;
+      d.M = M; d.N = N; d.K = M; d.batch = W;
+      d.A = V; d.sAm = M; d.sAk = 1; d.sAb = (long)M * M; d.a_cplx = true;
+      d.B = a + q * MN; d.sBk = N; d.sBn = 1; d.sBb = npol * MN; d.b_cplx = true;
+      d.C = b + q * MN; d.sCm = N; d.sCn = 1; d.sCb = npol * MN;
+      d.S = TMN + q * MN;
+      d.alpha = mk(0.0, 1.0 / double(k));
+      if ((rc = gemm_f64(d, st))) return rc;
+    }
     cplx* t = a; a = b; b = t;
   }
   // SM = P1 * TMN   (propagate.hpp:297)
-  return p1_apply(P1, p_cplx, TMN, SM, W, M, N, st);
+  return p1_apply(P1, p_cplx, TMN, SM, W * npol, M, N, st);
 }
 
 namespace {

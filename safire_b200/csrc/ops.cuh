@@ -20,7 +20,7 @@ int vhs(const double* Likn, const cplx* X, cplx* V, int W, int M, int Nc, double
 int vhs_rows(const double* L, long rows, const cplx* X, cplx* V, int W, int Nc, double a, cudaStream_t st);
 // SM <- P1 * Taylor(iV) * P1 * SM with scratch TMN, T1, T2 (each W*M*N complex)
 int propagate(cplx* SM, const void* P1, bool p_cplx, const cplx* V, int W, int M, int N, int order, cplx* TMN,
-              cplx* T1, cplx* T2, cudaStream_t st);
+              cplx* T1, cplx* T2, cudaStream_t st, int npol = 1);
 // CholeskyQR2; SM2 (W*M*N), S (W*N*N) scratch, status (W) ints.  log_detR (W) accumulated if not null
 // CholeskyQR2 in place on SM (SM2, S: scratch; status: 2 W ints)
 // nup in (0, N) (here and below): COLLINEAR walkers, columns [0, nup) up and [nup, N) down, each spin

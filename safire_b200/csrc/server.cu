@@ -22,6 +22,8 @@ namespace {
 int electrons(const sfq_engine_params_t& p) {
   return p.nel + (p.walker_type == SFQ_WALKER_COLLINEAR ? p.nel_dn : 0);
 }
+// rows of a walker and columns of PsiT: nmo, or 2 nmo for NONCOLLINEAR spinors
+int walker_rows(const sfq_engine_params_t& p) { return (p.walker_type == SFQ_WALKER_NONCOLLINEAR ? 2 : 1) * p.nmo; }
 
 constexpr int kProps = 8;  // property columns of sfq_engine_get_walkers
 
@@ -80,7 +82,7 @@ int evict(sfq_server_s& s, int keep, size_t need) {
     }
     if (victim < 0) return SFQ_ERR_OOM;  // everything resident is running: wait
     SystemRec& v = s.sys[victim];
-    const size_t mn = size_t(v.p.nmo) * electrons(v.p) * v.p.nwalk;
+    const size_t mn = size_t(walker_rows(v.p)) * electrons(v.p) * v.p.nwalk;
     v.saved_SM.resize(2 * mn);
     v.saved_props.resize(2 * size_t(kProps) * v.p.nwalk);
     int rc = sfq_engine_get_walkers(v.eng, v.saved_SM.data(), v.saved_props.data());
@@ -162,7 +164,7 @@ int sfq_server_add_system(sfq_server_t s, const sfq_engine_params_t* p, const do
   r.hcore.assign(hcore, hcore + MM);
   r.Likn.assign(Likn, Likn + MM * p->nchol);
   const double* ps = static_cast<const double*>(PsiT);
-  r.PsiT.assign(ps, ps + 2 * size_t(electrons(*p)) * p->nmo);
+  r.PsiT.assign(ps, ps + 2 * size_t(electrons(*p)) * walker_rows(*p));
   s->sys.push_back(std::move(r));
   *id = int(s->sys.size()) - 1;
   return SFQ_OK;

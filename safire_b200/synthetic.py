@@ -48,6 +48,7 @@ class System:
     PsiT: np.ndarray       # (N, M) complex128; COLLINEAR: the up rows over the down rows
     E0: float = 0.0
     nel_dn: int = -1       # COLLINEAR walkers: the last nel_dn rows of PsiT are the down spin; -1: CLOSED
+    npol: int = 1          # 2: NONCOLLINEAR walkers, PsiT (N, 2M) spinor orbitals
 
     @property
     def M(self):

@@ -4,8 +4,9 @@ The engine takes the reference's own random streams at its two injection points:
 uniforms of every step (sfq_engine_propagate_host, the nwalk x nchol draw of assemble_X) and the
 comb's uniform (sfq_engine_population_control_uniform).  Driven in run_afqmc's order it must
 reproduce, step by step, the oracle's energy-estimator series, and through it the snapshot the
-reference recorded, to the reference's own 1e-9: BH with an RHF trial and CLOSED walkers, BH with
-a UHF trial and Li with a polarized ROHF trial (no down electrons) and COLLINEAR walkers.
+reference recorded, to the reference's own 1e-9: BH with an RHF trial and CLOSED walkers;
+COLLINEAR walkers with BH's UHF and RHF trials and Li's polarized ROHF trial (no down electrons);
+NONCOLLINEAR walkers with BH's RHF and UHF trials upgraded to spinors and a GHF trial.
 """
 import numpy as np
 import pytest
@@ -18,12 +19,17 @@ from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, snapshot, snapsho
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_rhf_collinear", "li_rohf_collinear"]
+CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_rhf_collinear", "li_rohf_collinear",
+         "bh_rhf_noncollinear", "bh_uhf_noncollinear", "bh_ghf_noncollinear"]
 
 
 def _system(snap):
-    """The engine's System of a case: COLLINEAR stacks PsiT_up over PsiT_dn."""
+    """The engine's System of a case: COLLINEAR stacks PsiT_up over PsiT_dn; NONCOLLINEAR takes the
+    (N, 2M) spinor trial."""
     M, Nc = snap["hcore"].shape[0], snap["Likn"].shape[2]
+    if snap["settings"]["walker_type"] == "NONCOLLINEAR":
+        spec = synthetic.SystemSpec(M=M, N=snap["PsiT"].shape[0], Nc=Nc, decay=0.0)
+        return synthetic.System(spec, snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"], npol=2)
     if snap["settings"]["walker_type"] == "COLLINEAR":
         PsiT = np.concatenate([snap["PsiT_up"], snap["PsiT_dn"]])
         spec = synthetic.SystemSpec(M=M, N=PsiT.shape[0], Nc=Nc, decay=0.0)
@@ -34,6 +40,8 @@ def _system(snap):
 
 
 def _oracle_hamiltonian(snap):
+    if snap["settings"]["walker_type"] == "NONCOLLINEAR":
+        return O.NoncollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"], snap["ci"])
     if snap["settings"]["walker_type"] == "COLLINEAR":
         return O.CollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_up"], snap["PsiT_dn"], snap["E0"],
                                       snap["ci"])
@@ -91,10 +99,10 @@ def test_collinear_with_identical_spins_is_closed():
         assert np.max(np.abs(a - b)) < 1e-10 * np.max(np.abs(a)), k
 
 
-def test_collinear_rejected_in_mixed_precision():
-    snap = snapshot("bh_uhf_collinear")
+@pytest.mark.parametrize("case", ["bh_uhf_collinear", "bh_ghf_noncollinear"])
+def test_spin_walkers_rejected_in_mixed_precision(case):
     with pytest.raises(capi.SafireError) as ex:
-        A.AfqmcEngine(_system(snap), 8, dt=0.01, precision=capi.PRECISION_MIXED)
+        A.AfqmcEngine(_system(snapshot(case)), 8, dt=0.01, precision=capi.PRECISION_MIXED)
     assert ex.value.code == 3  # SFQ_ERR_UNSUPPORTED
 
 
