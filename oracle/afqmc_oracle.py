@@ -249,6 +249,37 @@ class Hamiltonian:
     def propagate(self, SM, P1, V, order):
         return propagate(SM, P1, V, order)
 
+    def local_energy(self, SM):
+        """NOMSD::Energy(wset, E, Ov), ndet = 1: (E (W, 3), log overlaps)."""
+        G, ov = self.green(SM)
+        return self.energy(G), ov
+
+    def mean_field(self, dt):
+        """NOMSD::vMF, ndet = 1 (NOMSD.cpp:437-456): vbias of the trial's own G, real part kept."""
+        return self.vbias(self.green(self.trial_walker()[None])[0], dt)[0].real.astype(np.complex128)
+
+    # the pieces a multi-determinant trial combines (NOMSD.cpp:184-216,238-278,300-331)
+    nspin_blocks = 1           # full-G blocks: CLOSED 1, COLLINEAR 2 spins
+    vbias_scale = 2.0          # CLOSED: 2 sqrt(dt)
+    ov_factor = 2.0            # DensityMatrix / Log_Overlap count a CLOSED determinant twice
+
+    def det_log_overlap(self, SM):
+        """The determinant's log overlap without the ci term (CLOSED: twice one spin's)."""
+        return 2.0 * log_overlap(self.PsiT, SM)
+
+    def full_green(self, SM):
+        """det_ops::MixedDensityMatrix(compact = false) per spin: (W, nspin_blocks, Mr, Mr) and the
+        accumulated log overlap as det_ops returns it (CLOSED: one spin's, not doubled)."""
+        G, ov = mixed_density_matrix(self.PsiT, SM, compact=False)
+        return G[:, None], ov
+
+    def full_green_vbias(self, Gf, dt):
+        """Real3IndexFactorization::vbias on a full G (:392-426): sum_s sum_ik L[i,k,n] G[w,s,i,k]."""
+        W = Gf.shape[0]
+        L2 = self.Likn.reshape(self.M * self.M, self.Nc)
+        g = Gf.sum(axis=1).reshape(W, self.M * self.M)
+        return self.vbias_scale * math.sqrt(dt) * (g @ L2)
+
 
 class CollinearHamiltonian(Hamiltonian):
     """The same dense Hamiltonian for COLLINEAR walkers and a single-determinant NOMSD trial with
@@ -294,6 +325,19 @@ class CollinearHamiltonian(Hamiltonian):
 
     def trial_walker(self):
         return np.concatenate([np.conj(self.PsiT_up.T), np.conj(self.PsiT_dn.T)], axis=1)
+
+    nspin_blocks = 2
+    vbias_scale = 1.0
+    ov_factor = 1.0
+
+    def det_log_overlap(self, SM):
+        ov = log_overlap(self.PsiT_up, SM[:, :, :self.nup])
+        return log_overlap(self.PsiT_dn, SM[:, :, self.nup:], ovlp=ov)
+
+    def full_green(self, SM):
+        G_up, ov = mixed_density_matrix(self.PsiT_up, SM[:, :, :self.nup], compact=False)
+        G_dn, ov = mixed_density_matrix(self.PsiT_dn, SM[:, :, self.nup:], compact=False, ovlp=ov)
+        return np.stack([G_up, G_dn], axis=1), ov
 
     def orthogonalize(self, SM):
         up = orthogonalize(SM[:, :, :self.nup])[0]
@@ -378,6 +422,22 @@ class NoncollinearHamiltonian(Hamiltonian):
     def trial_walker(self):
         return np.conj(self.PsiT.T)
 
+    vbias_scale = 1.0
+    ov_factor = 1.0
+
+    def det_log_overlap(self, SM):
+        return log_overlap(self.PsiT, SM)
+
+    def full_green(self, SM):
+        G, ov = mixed_density_matrix(self.PsiT, SM, compact=False)
+        return G[:, None], ov
+
+    def full_green_vbias(self, Gf, dt):
+        """npol = 2: the diagonal polarization blocks, sum_p sum_ik L[i,k,n] G[w, pM+i, pM+k]."""
+        W, M = Gf.shape[0], self.M
+        g = Gf[:, 0, :M, :M] + Gf[:, 0, M:, M:]
+        return math.sqrt(dt) * (g.reshape(W, M * M) @ self.Likn.reshape(M * M, self.Nc))
+
     def propagate(self, SM, P1, V, order):
         W, M2, N = SM.shape
         M = M2 // 2
@@ -403,6 +463,110 @@ class NoncollinearHamiltonian(Hamiltonian):
         return E
 
 
+class MultiDetHamiltonian:
+    """NOMSD with ndet > 1 determinants of one walker type (NOMSD.cpp:159-217,238-331,466-520).
+
+    dets: one single-determinant Hamiltonian per determinant (Hamiltonian, CollinearHamiltonian or
+    NoncollinearHamiltonian, each half-rotated with its own orbitals and built with ci = 1); ci: the
+    coefficients.  The propagator (P1, vHS, propagation, orthogonalization) is that of the walker type.
+
+      log overlap   a_d = log det_d + log(conj(ci_d)); log_m + log sum_d exp(a_d - log_m), log_m the
+                    a_d of largest real part (Log_Overlap :301-331)
+      force bias    the full G mixed over the determinants with weights conj(ci_d) exp(Ot_d - log_m),
+                    log_m the walker's log overlap, then vbias on the full G with L itself (:238-278;
+                    Real3IndexFactorization.hpp:392-426)
+      energy        per determinant with its own haj / Lnak, mixed with conj(ci_d) exp(ov_d - log_m),
+                    log_m the ov_d of largest real part (Energy :184-216)
+      vMF           pairs p <= q of the trial's own determinants: G of PsiT_q against PsiT_p^H weighted
+                    by Re(conj(ci_q) ci_p exp(log det)), normalised by the weights' sum (vMF :466-512)
+      walkers       start as the determinant of largest |ci| (initial_guess :132-153)
+    """
+
+    def __init__(self, dets, ci):
+        self.dets = list(dets)
+        self.ci = np.asarray(ci, dtype=np.complex128)
+        d0 = self.dets[0]
+        self.M, self.Nc, self.E0, self.N = d0.M, d0.Nc, d0.E0, d0.N
+        self.Likn, self.hcore = d0.Likn, d0.hcore
+
+    def _lci(self, d):
+        c = self.ci[d]
+        return np.log(1e-12 if abs(c) < 1e-12 else np.conj(c))
+
+    # the walker type's propagator
+    def vHS(self, X, dt):
+        return self.dets[0].vHS(X, dt)
+
+    def one_body_propagator_matrix(self, dt, vMF):
+        return self.dets[0].one_body_propagator_matrix(dt, vMF)
+
+    def propagate(self, SM, P1, V, order):
+        return self.dets[0].propagate(SM, P1, V, order)
+
+    def orthogonalize(self, SM):
+        return self.dets[0].orthogonalize(SM)
+
+    def trial_walker(self):
+        return self.dets[int(np.argmax(np.abs(self.ci)))].trial_walker()
+
+    @staticmethod
+    def _log_sum(a):
+        """log sum_d exp(a[d, w]) per walker, about the a of largest real part."""
+        out = np.empty(a.shape[1], np.complex128)
+        for w in range(a.shape[1]):
+            lm = a[int(np.argmax(a[:, w].real)), w]
+            out[w] = lm + np.log(np.sum(np.exp(a[:, w] - lm)))
+        return out
+
+    def log_overlap(self, SM):
+        a = np.stack([d.det_log_overlap(SM) + self._lci(i) for i, d in enumerate(self.dets)])
+        return self._log_sum(a)
+
+    def green(self, SM):
+        log_m = self.log_overlap(SM)
+        G = 0.0
+        wsum = 0.0
+        for i, d in enumerate(self.dets):
+            Gd, ot = d.full_green(SM)
+            wgt = np.conj(self.ci[i]) * np.exp(d.ov_factor * ot - log_m)
+            wsum = wsum + wgt
+            G = G + Gd * wgt[:, None, None, None]
+        return G / wsum[:, None, None, None], log_m
+
+    def vbias(self, G, dt):
+        return self.dets[0].full_green_vbias(G, dt)
+
+    def local_energy(self, SM):
+        Es, ovs = [], []
+        for d in self.dets:
+            E, ov = d.local_energy(SM)
+            Es.append(E)
+            ovs.append(ov)
+        Es, ovs = np.stack(Es), np.stack(ovs)
+        W = SM.shape[0]
+        E = np.empty((W, 3), np.complex128)
+        Ov = np.empty(W, np.complex128)
+        for w in range(W):
+            lm = ovs[int(np.argmax(ovs[:, w].real)), w]
+            e = np.exp(ovs[:, w] - lm) * np.conj(self.ci)
+            deno = np.sum(e)
+            E[w] = np.sum(e[:, None] * Es[:, w, :], axis=0) / deno
+            Ov[w] = np.log(deno) + lm
+        return E, Ov
+
+    def mean_field(self, dt):
+        Gsum = 0.0
+        Osum = 0.0
+        for p_, dp in enumerate(self.dets):
+            B = dp.trial_walker()[None]
+            for q_ in range(p_, len(self.dets)):
+                Gq, ov = self.dets[q_].full_green(B)
+                scl = (np.conj(self.ci[q_]) * self.ci[p_] * np.exp(ov[0])).real
+                Osum += scl
+                Gsum = Gsum + scl * Gq
+        return self.vbias(Gsum / Osum, dt)[0].real.astype(np.complex128)
+
+
 def trial_density(ham):
     """G of the trial against itself (NOMSD::vMF: MixedDensityMatrix(PsiT, PsiT^H), NOMSD.cpp:437-466)."""
     return ham.green(ham.trial_walker()[None])[0]
@@ -410,8 +574,7 @@ def trial_density(ham):
 
 def vMF(ham, dt):
     """NOMSD::vMF (NOMSD.cpp:437-466) with zero_imag (AFQMCBasePropagator.cpp:107)."""
-    v = ham.vbias(trial_density(ham), dt)[0]
-    return v.real.astype(np.complex128)
+    return ham.mean_field(dt)
 
 
 def hermitize(H):
@@ -738,8 +901,7 @@ class Propagator:
 
 def wfn_energy(ham, wset):
     """NOMSD::Energy(wset) (NOMSD.cpp:159-217 / :64-75): writes E1_, EXX_, EJ_, OVLP."""
-    G, ov = ham.green(wset.SM)
-    E = ham.energy(G)
+    E, ov = ham.local_energy(wset.SM)
     wset.ovlp = ov
     wset.e1, wset.exx, wset.ej = E[:, 0].copy(), E[:, 1].copy(), E[:, 2].copy()
     return E, ov
@@ -766,8 +928,7 @@ def measure_energy(ham, wset):
 
 
 def wfn_energy_noupdate(ham, wset):
-    G, ov = ham.green(wset.SM)
-    return ham.energy(G), ov
+    return ham.local_energy(wset.SM)
 
 
 def init_walkers(ham, wset):

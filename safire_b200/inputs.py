@@ -116,47 +116,62 @@ def read_csr(f, group):
     return A
 
 
-def load_nomsd_trial(path, walker_type="CLOSED"):
-    """A single-determinant NOMSD trial: for CLOSED walkers PsiT (nel, nmo) complex; for COLLINEAR
-    walkers also PsiT_up (nup, nmo) and PsiT_dn (ndn, nmo), ndn possibly 0, from a collinear file or,
-    upgraded, from a closed one (both spins the same orbitals) (read_wavefunction_info,
-    readWfn.cpp:86-119; read_nomsd_wavefunction, readWfn.h:90-139)."""
+def _spinors(up, dn):
+    """combine_csr (csr_utils.hpp:70-110): the up rows over the down rows, the latter shifted by nmo."""
+    M = up.shape[1]
+    sp = np.zeros((up.shape[0] + dn.shape[0], 2 * M), np.complex128)
+    sp[:up.shape[0], :M] = up
+    sp[up.shape[0]:, M:] = dn
+    return sp
+
+
+def load_nomsd_determinants(path, walker_type="CLOSED"):
+    """Every determinant of a NOMSD trial for the given walker type, upgraded as
+    read_nomsd_wavefunction does (readWfn.h:90-153): a list of dicts (PsiT; COLLINEAR also PsiT_up,
+    PsiT_dn) and the coefficients ci.  A closed file gives COLLINEAR walkers the same orbitals for
+    both spins and NONCOLLINEAR walkers the spinor matrix of both; a collinear file gives
+    NONCOLLINEAR walkers its up and down rows as spinors."""
     walker_type = walker_type.upper()
     _check(walker_type in ("CLOSED", "COLLINEAR", "NONCOLLINEAR"), f"unknown walker type {walker_type}")
     f = H5File(path)
     _check("Wavefunction/NOMSD" in f, f"{path}: no Wavefunction/NOMSD group")
-    at = f.attrs("Wavefunction/NOMSD")
-    spin = at.get("spin_type")
-    if spin is not None:
-        spin = str(spin).lower()
-        order = ("closed", "collinear", "noncollinear")  # walkerTypeIsConvertible: upgrades only
-        _check(spin in order and order.index(spin) <= order.index(walker_type.lower()),
-               f"wavefunction spin_type is '{spin}': {walker_type} walkers cannot take it")
+    spin = f.attrs("Wavefunction/NOMSD").get("spin_type")
+    spin = str(spin).lower() if spin is not None else walker_type.lower()
+    order = ("closed", "collinear", "noncollinear")  # walkerTypeIsConvertible: upgrades only
+    _check(spin in order and order.index(spin) <= order.index(walker_type.lower()),
+           f"wavefunction spin_type is '{spin}': {walker_type} walkers cannot take it")
     ci = np.atleast_1d(_complex_last(f["Wavefunction/NOMSD/ci_coeffs"], 1))
-    _check(ci.size == 1, f"{ci.size} determinants: the path takes a single-determinant trial")
-    _check("Wavefunction/NOMSD/PsiT_0" in f, "Wavefunction/NOMSD/PsiT_0 missing")
-    PsiT = read_csr(f, "Wavefunction/NOMSD/PsiT_0")
-    out = dict(PsiT=PsiT, ci=complex(ci[0]), nup=PsiT.shape[0], nmo=PsiT.shape[1], spin_type=spin)
-    if walker_type == "NONCOLLINEAR":
-        # one (nel, 2 nmo) spinor matrix: native, or the up rows over the down rows shifted by nmo
-        # (combine_csr, readWfn.h:116-153)
-        if spin == "noncollinear":
-            _check(PsiT.shape[1] % 2 == 0, f"noncollinear PsiT_0 has {PsiT.shape[1]} columns, not 2 nmo")
-            sp = PsiT
+    per = 2 if spin == "collinear" else 1
+    dets = []
+    for d in range(ci.size):
+        g = f"Wavefunction/NOMSD/PsiT_{per * d}"
+        _check(g in f, f"{g} missing")
+        P = read_csr(f, g)
+        dn = read_csr(f, f"Wavefunction/NOMSD/PsiT_{per * d + 1}") if spin == "collinear" else None
+        if walker_type == "NONCOLLINEAR":
+            if spin == "noncollinear":
+                _check(P.shape[1] % 2 == 0, f"noncollinear {g} has {P.shape[1]} columns, not 2 nmo")
+                dets.append(dict(PsiT=P, nup=P.shape[0], nmo=P.shape[1] // 2))
+            else:
+                sp = _spinors(P, dn if dn is not None else P)
+                dets.append(dict(PsiT=sp, nup=sp.shape[0], nmo=P.shape[1]))
+        elif walker_type == "COLLINEAR":
+            dn = P if dn is None else dn
+            _check(dn.shape[1] == P.shape[1], f"{g}: up and down orbitals differ in nmo")
+            dets.append(dict(PsiT=P, PsiT_up=P, PsiT_dn=dn, nup=P.shape[0], ndn=dn.shape[0], nmo=P.shape[1]))
         else:
-            dn = read_csr(f, "Wavefunction/NOMSD/PsiT_1") if spin == "collinear" else PsiT
-            M = PsiT.shape[1]
-            sp = np.zeros((PsiT.shape[0] + dn.shape[0], 2 * M), np.complex128)
-            sp[:PsiT.shape[0], :M] = PsiT
-            sp[PsiT.shape[0]:, M:] = dn
-        out.update(PsiT=sp, nup=sp.shape[0], nmo=sp.shape[1] // 2)
-    elif walker_type == "COLLINEAR" and spin == "closed":
-        out.update(PsiT_up=PsiT, PsiT_dn=PsiT.copy(), ndn=PsiT.shape[0])  # readWfn.h:130-139
-    elif walker_type == "COLLINEAR":
-        _check("Wavefunction/NOMSD/PsiT_1" in f, "Wavefunction/NOMSD/PsiT_1 missing for a collinear trial")
-        dn = read_csr(f, "Wavefunction/NOMSD/PsiT_1")
-        _check(dn.shape[1] == PsiT.shape[1], f"PsiT_1 has {dn.shape[1]} columns, PsiT_0 {PsiT.shape[1]}")
-        out.update(PsiT_up=PsiT, PsiT_dn=dn, ndn=dn.shape[0])
+            dets.append(dict(PsiT=P, nup=P.shape[0], nmo=P.shape[1]))
+    return dets, ci.astype(np.complex128), spin
+
+
+def load_nomsd_trial(path, walker_type="CLOSED"):
+    """A single-determinant NOMSD trial: for CLOSED walkers PsiT (nel, nmo) complex; for COLLINEAR
+    walkers also PsiT_up (nup, nmo) and PsiT_dn (ndn, nmo), ndn possibly 0; for NONCOLLINEAR walkers
+    PsiT (nel, 2 nmo) spinors.  Trials are upgraded as load_nomsd_determinants says."""
+    dets, ci, spin = load_nomsd_determinants(path, walker_type)
+    _check(ci.size == 1, f"{ci.size} determinants: the path takes a single-determinant trial")
+    out = dict(dets[0])
+    out.update(ci=complex(ci[0]), spin_type=spin)
     return out
 
 

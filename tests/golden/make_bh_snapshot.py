@@ -2,7 +2,8 @@
 of BH with CLOSED walkers (bh_rhf_closed_snapshot.npz), BH with a UHF trial and COLLINEAR walkers
 (bh_uhf_collinear_snapshot.npz), BH with the RHF trial and COLLINEAR walkers
 (bh_rhf_collinear_snapshot.npz), BH with NONCOLLINEAR walkers and the RHF, UHF and GHF trials
-(bh_{rhf,uhf,ghf}_noncollinear_snapshot.npz), Li with a polarized ROHF trial and COLLINEAR walkers
+(bh_{rhf,uhf,ghf}_noncollinear_snapshot.npz), BH with multi-determinant CASCI trials
+(bh_rcasci_*_snapshot.npz), Li with a polarized ROHF trial and COLLINEAR walkers
 (li_rohf_collinear_snapshot.npz), and the statistical reference of the first (bh_rhf_closed_statistical.json).
 
     python tests/golden/make_bh_snapshot.py [SAFIRE source tree]
@@ -33,7 +34,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from safire_b200.h5read import H5File  # noqa: E402
-from safire_b200.inputs import load_dense_hamiltonian, load_nomsd_trial  # noqa: E402
+from safire_b200.inputs import load_dense_hamiltonian, load_nomsd_determinants, load_nomsd_trial  # noqa: E402
 
 OBSERVABLES = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "Overlap", "ProjectionTime",
                "EffectiveNumWalkers", "Phase", "TotalWeight")
@@ -65,6 +66,30 @@ def snapshot_case(fn, system, ham_file, wfn_file, case, walker_type, out_name, w
     print(path, settings)
 
 
+def multidet_case(fn, system, ham_file, wfn_file, case, walker_type, out_name):
+    """A seeded snapshot case with a multi-determinant trial: every determinant (upgraded to the
+    walker type) and the coefficients; the Hamiltonian tensors are those of the BH closed file."""
+    dets, ci, _ = load_nomsd_determinants(os.path.join(fn, "afqmc_inputs", system, wfn_file), walker_type)
+    res = H5File(os.path.join(fn, "snapshot_references", system, *case.split("/"), "results.h5"))
+    inp = json.loads(res["input_file"])
+    ex = inp["execute"]
+    settings = dict(seed=inp["seed"], nwalk=ex["num_walkers"], dt=ex["timestep"], steps=ex["steps"],
+                    ortho_interval=ex["walker_ortho_interval"], pop_interval=ex["population_control_interval"],
+                    measure_interval=ex["measure_interval"], equilibration_steps=ex["equilibration_steps"],
+                    num_ranks=int(res["num_ranks"]), walker_type=ex["walker_set"]["walker_type"])
+    assert settings["walker_type"] == walker_type
+    out = dict(ci_dets=ci, PsiT_dets=np.stack([d["PsiT"] for d in dets]), settings=json.dumps(settings))
+    if walker_type == "COLLINEAR":
+        out.update(PsiT_up_dets=np.stack([d["PsiT_up"] for d in dets]),
+                   PsiT_dn_dets=np.stack([d["PsiT_dn"] for d in dets]))
+    for k in OBSERVABLES:
+        out[f"mean_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/mean"])
+        out[f"error_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/error"])
+    path = os.path.join(HERE, out_name)
+    np.savez_compressed(path, **out)
+    print(path, len(dets), "determinants", settings)
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     fn = os.path.join(src, "tests", "functional")
@@ -82,6 +107,13 @@ def main():
     for wfn, name in (("afqmc_rhf_nomsd.h5", "rhf"), ("afqmc_uhf_nomsd.h5", "uhf"), ("afqmc_ghf_nomsd.h5", "ghf")):
         snapshot_case(fn, "BH", "afqmc_H_rhf_closed.h5", wfn, f"dense_rhf_basis_closed/{name}_nomsd/noncollinear",
                       "NONCOLLINEAR", f"bh_{name}_noncollinear_snapshot.npz", with_hamiltonian=False)
+    # multi-determinant (CASCI) trials: RHF-based for every walker type, UHF-based, GHF-based
+    for wfn, name, wts in (("afqmc_casci_rhf_nomsd.h5", "rcasci_rhf", ("closed", "collinear", "noncollinear")),
+                           ("afqmc_casci_uhf_nomsd.h5", "rcasci_uhf", ("collinear", "noncollinear")),
+                           ("afqmc_casci_ghf_nomsd.h5", "rcasci_ghf", ("noncollinear",))):
+        for wt in wts:
+            multidet_case(fn, "BH", "afqmc_H_rhf_closed.h5", wfn, f"dense_rhf_basis_closed/{name}_nomsd/{wt}",
+                          wt.upper(), f"bh_{name}_{wt}_snapshot.npz")
     snapshot_case(fn, "Li", "hamil_closed.h5", "rohf_nomsd_polarized.h5",
                   "hamil_closed/rohf_wfn_polarized/collinear", "COLLINEAR", "li_rohf_collinear_snapshot.npz")
 

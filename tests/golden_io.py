@@ -33,12 +33,17 @@ def snapshot(name):
     The BH collinear case shares the BH Hamiltonian tensors of the closed case's file."""
     z = np.load(os.path.join(HERE, f"{name}_snapshot.npz"))
     rec = {k: (z[f"mean_{k}"][()], z[f"error_{k}"][()]) for k in SNAPSHOT_OBSERVABLES}
-    out = dict(PsiT=z["PsiT"], E0=float(z["E0"]), ci=complex(z["ci"]), settings=json.loads(str(z["settings"])),
-               recorded=rec)
-    if "PsiT_up" in z:
-        out.update(PsiT_up=z["PsiT_up"], PsiT_dn=z["PsiT_dn"])
+    out = dict(settings=json.loads(str(z["settings"])), recorded=rec)
+    if "ci_dets" in z:  # multi-determinant trial: per-determinant orbitals and coefficients
+        out.update(ci_dets=z["ci_dets"], PsiT_dets=z["PsiT_dets"])
+        if "PsiT_up_dets" in z:
+            out.update(PsiT_up_dets=z["PsiT_up_dets"], PsiT_dn_dets=z["PsiT_dn_dets"])
+    else:
+        out.update(PsiT=z["PsiT"], ci=complex(z["ci"]))
+        if "PsiT_up" in z:
+            out.update(PsiT_up=z["PsiT_up"], PsiT_dn=z["PsiT_dn"])
     h = z if "hcore" in z else np.load(os.path.join(HERE, "bh_rhf_closed_snapshot.npz"))
-    out.update(hcore=h["hcore"], Likn=h["Likn"])
+    out.update(hcore=h["hcore"], Likn=h["Likn"], E0=float(z["E0"]) if "E0" in z else float(h["E0"]))
     return out
 
 

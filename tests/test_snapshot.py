@@ -1,8 +1,9 @@
 """The reference's seeded snapshot of a real molecule, replayed on its own random streams.
 
-The dense-Cholesky single-determinant NOMSD cases of the reference's functional tests (BH and Li;
-CLOSED, COLLINEAR and NONCOLLINEAR walkers; seed 42, 50 walkers, 20 steps, one rank) recorded every
-energy-estimator observable; the reference's runner requires a rerun to reproduce them to 1e-9.
+The dense-Cholesky NOMSD cases of the reference's functional tests (BH and Li; CLOSED, COLLINEAR and
+NONCOLLINEAR walkers; single-determinant and 34-determinant CASCI trials; seed 42, 50 walkers,
+20 steps, one rank) recorded every energy-estimator observable; the reference's runner requires a
+rerun to reproduce them to 1e-9.
 These tests pin:
 
   * the host random streams (std::mt19937 via split_seed, uniform_real_distribution) against the
@@ -48,6 +49,8 @@ def test_split_seed_streams_distinct():
 
 
 def _oracle_hamiltonian(snap):
+    if "ci_dets" in snap:
+        return _oracle_multidet(snap)
     if snap["settings"]["walker_type"] == "NONCOLLINEAR":
         return O.NoncollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"], snap["ci"])
     if snap["settings"]["walker_type"] == "COLLINEAR":
@@ -56,15 +59,32 @@ def _oracle_hamiltonian(snap):
     return O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
 
 
+def _oracle_multidet(snap):
+    wt = snap["settings"]["walker_type"]
+    dets = []
+    for d in range(len(snap["ci_dets"])):
+        if wt == "CLOSED":
+            dets.append(O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_dets"][d], snap["E0"]))
+        elif wt == "COLLINEAR":
+            dets.append(O.CollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_up_dets"][d],
+                                               snap["PsiT_dn_dets"][d], snap["E0"]))
+        else:
+            dets.append(O.NoncollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_dets"][d], snap["E0"]))
+    return O.MultiDetHamiltonian(dets, snap["ci_dets"])
+
+
 SNAPSHOT_CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_rhf_collinear", "li_rohf_collinear",
                   "bh_rhf_noncollinear", "bh_uhf_noncollinear", "bh_ghf_noncollinear"]
+# CASCI trials of 34 determinants
+MULTIDET_CASES = ["bh_rcasci_rhf_closed", "bh_rcasci_rhf_collinear", "bh_rcasci_rhf_noncollinear",
+                  "bh_rcasci_uhf_collinear", "bh_rcasci_uhf_noncollinear", "bh_rcasci_ghf_noncollinear"]
 
 
-@pytest.mark.parametrize("case", SNAPSHOT_CASES)
+@pytest.mark.parametrize("case", SNAPSHOT_CASES + MULTIDET_CASES)
 def test_oracle_reproduces_reference_snapshot(case):
     """BH with an RHF trial and CLOSED walkers; COLLINEAR walkers with BH's UHF and RHF trials and Li's
     fully polarized ROHF trial (no down electrons); NONCOLLINEAR walkers with BH's RHF and UHF trials
-    upgraded to spinors and a GHF trial."""
+    upgraded to spinors and a GHF trial; and 34-determinant CASCI trials with each walker type."""
     snap = snapshot(case)
     st = snap["settings"]
     assert st["num_ranks"] == 1
