@@ -219,6 +219,13 @@ void sfq_engine_params_default(sfq_engine_params_t* p);
  * Walkers start as copies of the trial (PsiT^H) with unit weight. */
 int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
                       const void* PsiT);
+/* the same with a multi-determinant NOMSD trial (NOMSD.cpp:159-331,466-512, ndet > 1): PsiT holds ndet
+ * matrices of the walker type's shape one after the other, ci (ndet) complex the coefficients.  The
+ * force bias comes from the ci-weighted full Green's function, overlaps and energies from the
+ * determinants' own, the mean field from the trial's determinant pairs; walkers start as the
+ * determinant of largest |ci|.  FP64 only; ndet = 1 is sfq_engine_create. */
+int sfq_engine_create_nomsd(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
+                            int ndet, const void* PsiT, const void* ci);
 int sfq_engine_destroy(sfq_engine_t e);
 /* waits for the engine stream; SFQ_ERR_TIMEOUT if a tensor-core product's bounded wait expired */
 int sfq_engine_synchronize(sfq_engine_t e);

@@ -177,8 +177,14 @@ class AfqmcEngine:
         L = np.ascontiguousarray(system.Likn, dtype=np.float64)
         P = np.ascontiguousarray(system.PsiT, dtype=np.complex128)
         handle = ctypes.c_void_p()
-        check(lib().sfq_engine_create(ctypes.byref(handle), ctypes.byref(p), h.ctypes.data, L.ctypes.data,
-                                      P.ctypes.data))
+        ci = getattr(system, "ci", None)
+        if ci is not None and np.size(ci) > 1:  # multi-determinant trial: PsiT (ndet, rows, cols)
+            c = np.ascontiguousarray(ci, dtype=np.complex128)
+            check(lib().sfq_engine_create_nomsd(ctypes.byref(handle), ctypes.byref(p), h.ctypes.data, L.ctypes.data,
+                                                int(c.size), P.ctypes.data, c.ctypes.data))
+        else:
+            check(lib().sfq_engine_create(ctypes.byref(handle), ctypes.byref(p), h.ctypes.data, L.ctypes.data,
+                                          P.ctypes.data))
         self.h = handle
 
     def close(self):

@@ -102,6 +102,7 @@ _SIGS = {
     "sfq_split_bf16": ([_VP, ctypes.c_long, _VP, _VP, _VP, _VP], _I),
     "sfq_engine_params_default": ([ctypes.POINTER(EngineParams)], None),
     "sfq_engine_create": ([ctypes.POINTER(_VP), ctypes.POINTER(EngineParams), _VP, _VP, _VP], _I),
+    "sfq_engine_create_nomsd": ([ctypes.POINTER(_VP), ctypes.POINTER(EngineParams), _VP, _VP, _I, _VP, _VP], _I),
     "sfq_engine_destroy": ([_VP], _I),
     "sfq_engine_synchronize": ([_VP], _I),
     "sfq_engine_stream": ([_VP], _VP),

@@ -137,6 +137,79 @@ __global__ void store_block_result_kernel(const double* eshift, const int* flag,
   for (int i = threadIdx.x; i < 10 * nm; i += blockDim.x) out[4 + i] = meas[i];
 }
 
+// ---- multi-determinant NOMSD (NOMSD.cpp:184-216,238-331,466-512) ----------------------------
+// Racc[w] (+)= wgt R[w], wsum[w] (+)= wgt with wgt = conj(ci) exp(ov[w] - lm[w]) (MixedDensityMatrix,
+// ndet > 1: lm the walker's log overlap, which cancels in the ratio)
+__global__ void md_accumulate_kernel(const cplx* R, const cplx* ov, const cplx* lm, cplx ci, cplx* Racc, cplx* wsum,
+                                     long n, int first) {
+  const long w = blockIdx.y;
+  const cplx wg = cmul(cconj(ci), cexp_(csub(ov[w], lm[w])));
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const cplx v = cmul(wg, R[w * n + e]);
+    Racc[w * n + e] = first ? v : cadd(Racc[w * n + e], v);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) wsum[w] = first ? wg : cadd(wsum[w], wg);
+}
+// the trial's own pair (q >= p): Racc += scl R, wsum += scl, scl = Re(conj(ci_q) ci_p exp(ov)) (vMF)
+__global__ void md_pair_kernel(const cplx* R, const cplx* ov, cplx ciq, cplx cip, cplx* Racc, cplx* wsum, long n,
+                               int first) {
+  const double scl = cmul(cmul(cconj(ciq), cip), cexp_(ov[0])).x;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const cplx v = cscale(R[e], scl);
+    Racc[e] = first ? v : cadd(Racc[e], v);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) wsum[0] = first ? mk(scl, 0.0) : cadd(wsum[0], mk(scl, 0.0));
+}
+__global__ void md_normalize_kernel(cplx* Racc, const cplx* wsum, long n) {
+  const long w = blockIdx.y;
+  const cplx s = wsum[w];
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+    Racc[w * n + e] = cdiv(Racc[w * n + e], s);
+}
+// the position of the largest real part in a[d * W + w] over d, the first one on ties (max_element)
+__device__ __forceinline__ int md_argmax(const cplx* a, int ndet, int W, int w) {
+  int best = 0;
+  for (int d = 1; d < ndet; ++d)
+    if (a[(long)d * W + w].x > a[(long)best * W + w].x) best = d;
+  return best;
+}
+// Log_Overlap, ndet > 1 (NOMSD.cpp:301-331): a_d = ov_d + log(conj ci_d); out = a_m + log sum exp(a_d - a_m)
+__global__ void md_logsum_kernel(const cplx* ov, const cplx* lci, int ndet, int W, cplx* out) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  int m = 0;
+  double best = 0.0;
+  for (int d = 0; d < ndet; ++d) {
+    const double r = ov[(long)d * W + w].x + lci[d].x;
+    if (d == 0 || r > best) { best = r; m = d; }
+  }
+  const cplx am = cadd(ov[(long)m * W + w], lci[m]);
+  cplx s = mk(0.0, 0.0);
+  for (int d = 0; d < ndet; ++d) s = cadd(s, cexp_(csub(cadd(ov[(long)d * W + w], lci[d]), am)));
+  out[w] = cadd(am, clog_(s));
+}
+// Energy, ndet > 1 (NOMSD.cpp:184-215): E = sum conj(ci_d) E_d exp(ov_d - ov_m) / deno, Ov = log deno + ov_m
+__global__ void md_energy_kernel(const cplx* ov, const cplx* Ed, const cplx* cic, int ndet, int W, cplx* E3,
+                                 cplx* Ov) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  const int m = md_argmax(ov, ndet, W, w);
+  const cplx om = ov[(long)m * W + w];
+  cplx deno = mk(0.0, 0.0), s0 = mk(0.0, 0.0), s1 = mk(0.0, 0.0), s2 = mk(0.0, 0.0);
+  for (int d = 0; d < ndet; ++d) {
+    const cplx e = cmul(cic[d], cexp_(csub(ov[(long)d * W + w], om)));
+    const cplx* E = Ed + ((long)d * W + w) * 3;
+    s0 = cadd(s0, cmul(e, E[0]));
+    s1 = cadd(s1, cmul(e, E[1]));
+    s2 = cadd(s2, cmul(e, E[2]));
+    deno = cadd(deno, e);
+  }
+  E3[3 * w] = cdiv(s0, deno);
+  E3[3 * w + 1] = cdiv(s1, deno);
+  E3[3 * w + 2] = cdiv(s2, deno);
+  Ov[w] = cadd(clog_(deno), om);
+}
+
 }  // namespace
 
 struct Engine {
@@ -149,6 +222,19 @@ struct Engine {
   int nup = 0;
   int npol = 1, Mr = 0;
   bool closed() const { return !collinear && npol == 1; }
+  // multi-determinant NOMSD trial (ndet > 1, FP64): PsiT, PsiTr, Lnak and haj hold the ndet
+  // determinants one after the other (the names point at determinant 0); ci on the host
+  int ndet = 1;
+  std::vector<cplx> ci_h;
+  cplx* md_ov = nullptr;   // (ndet, W) per-determinant log overlaps, without the ci terms
+  cplx* md_E = nullptr;    // (ndet, W, 3) per-determinant local energies
+  cplx* md_lci = nullptr;  // (ndet) log(conj ci), 1e-12 for a vanishing ci (NOMSD.cpp:312)
+  cplx* md_cic = nullptr;  // (ndet) conj ci
+  cplx* Rd = nullptr;      // (W, M, M) one determinant's full G summed over the spin / polarization blocks
+  cplx* Racc = nullptr;    // (W, M, M) their ci-weighted mixture
+  cplx* wsum = nullptr;    // (W) the mixture's weights
+  long det_elems() const { return (long)N * Mr; }
+  size_t lnak_esz() const { return trial_real ? sizeof(double) : sizeof(cplx); }
   // the exchange's spin split (and the CLOSED marker -1); a NONCOLLINEAR walker is one sector
   int spin_split() const { return collinear ? nup : (npol == 2 ? N : -1); }
   double ov_scale() const { return closed() ? 2.0 : 1.0; }  // NOMSD.cpp:285-290: CLOSED counts its determinant twice
@@ -322,10 +408,10 @@ struct Engine {
     std::vector<Item> items = {
         {(void**)&hcore, d * MM},
         {(void**)&Likn, d * MM * Nc},
-        {(void**)&PsiT, c * RN},
-        {(void**)&PsiTr, d * RN},
-        {(void**)&Lnak, (trial_real ? d : c) * (size_t)Nc * RN},
-        {(void**)&haj, c * RN},
+        {(void**)&PsiT, c * ndet * RN},
+        {(void**)&PsiTr, d * ndet * RN},
+        {(void**)&Lnak, (trial_real ? d : c) * (size_t)ndet * Nc * RN},
+        {(void**)&haj, c * ndet * RN},
         {(void**)&v0, d * MM},
         {(void**)&vmf, d * Nc},
         {(void**)&P1, d * MM},
@@ -360,6 +446,14 @@ struct Engine {
         {(void**)&d_step, sizeof(unsigned long long) * 2},
         {(void**)&d_meas, sizeof(double) * 10 * kMeasCap},
     };
+    if (ndet > 1) {
+      std::vector<Item> md = {
+          {(void**)&md_ov, c * ndet * W}, {(void**)&md_E, c * ndet * W * 3}, {(void**)&md_lci, c * ndet},
+          {(void**)&md_cic, c * ndet},    {(void**)&Rd, c * W * MM},          {(void**)&Racc, c * W * MM},
+          {(void**)&wsum, c * W},
+      };
+      items.insert(items.end(), md.begin(), md.end());
+    }
     if (mixed) {
       const size_t b = 2;  // bf16
       const long MN2 = 2L * M * N;
@@ -405,10 +499,23 @@ struct Engine {
     const long MM = (long)M * M;
     SFQ_CUDA_TRY(cudaMemcpyAsync(hcore, h_hcore, sizeof(double) * MM, cudaMemcpyHostToDevice, st));
     SFQ_CUDA_TRY(cudaMemcpyAsync(Likn, h_Likn, sizeof(double) * MM * Nc, cudaMemcpyHostToDevice, st));
-    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiT, h_PsiT, sizeof(cplx) * N * Mr, cudaMemcpyHostToDevice, st));
-    std::vector<double> pr(size_t(N) * Mr);
+    const long RN = det_elems();
+    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiT, h_PsiT, sizeof(cplx) * ndet * RN, cudaMemcpyHostToDevice, st));
+    std::vector<double> pr(size_t(ndet) * RN);
     for (size_t i = 0; i < pr.size(); ++i) pr[i] = h_PsiT[i].x;
-    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiTr, pr.data(), sizeof(double) * N * Mr, cudaMemcpyHostToDevice, st));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(PsiTr, pr.data(), sizeof(double) * ndet * RN, cudaMemcpyHostToDevice, st));
+    if (ndet > 1) {
+      std::vector<cplx> lci(ndet), cic(ndet);
+      for (int k = 0; k < ndet; ++k) {
+        const cplx c = ci_h[k];
+        cic[k] = cconj(c);
+        const double a = std::hypot(c.x, c.y);
+        lci[k] = a < 1e-12 ? mk(std::log(1e-12), 0.0) : mk(std::log(a), std::atan2(-c.y, c.x));
+      }
+      SFQ_CUDA_TRY(cudaMemcpyAsync(md_lci, lci.data(), sizeof(cplx) * ndet, cudaMemcpyHostToDevice, st));
+      SFQ_CUDA_TRY(cudaMemcpyAsync(md_cic, cic.data(), sizeof(cplx) * ndet, cudaMemcpyHostToDevice, st));
+      SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    }
     {
       int asym = 1;
       SFQ_CUDA_TRY(cudaMemsetAsync(pw.flag, 0, sizeof(int), st));
@@ -434,32 +541,36 @@ struct Engine {
       const size_t esz = trial_real ? sizeof(double) : sizeof(cplx);
       SFQ_CUDA_TRY(cudaMallocAsync(&tmp, esz * (size_t)N * M * Nc, st));
       if (npol > 1) SFQ_CUDA_TRY(cudaMallocAsync(&lq, esz * (size_t)N * M * Nc, st));
+      for (int det = 0; det < ndet; ++det)
       for (int q = 0; q < npol; ++q) {
         GemmDesc d;
+        const long a0 = det * RN + (long)q * M;
+        char* ldst = static_cast<char*>(Lnak) + (size_t)det * Nc * RN * esz;
         d.M = N; d.N = int((long)M * Nc); d.K = M;
-        d.A = trial_real ? (const void*)(PsiTr + (long)q * M) : (const void*)(PsiT + (long)q * M);
+        d.A = trial_real ? (const void*)(PsiTr + a0) : (const void*)(PsiT + a0);
         d.sAm = Mr; d.sAk = 1; d.a_cplx = !trial_real;
         d.B = Likn; d.sBk = (long)M * Nc; d.sBn = 1; d.b_cplx = false;
         d.C = tmp; d.sCm = (long)M * Nc; d.sCn = 1;
         if ((rc = gemm_f64(d, st))) return rc;
         if (npol == 1) {
-          if ((rc = permute_lnak(tmp, Lnak, N, M, Nc, int(esz), st))) return rc;
+          if ((rc = permute_lnak(tmp, ldst, N, M, Nc, int(esz), st))) return rc;
         } else {
           if ((rc = permute_lnak(tmp, lq, N, M, Nc, int(esz), st))) return rc;
-          SFQ_CUDA_TRY(cudaMemcpy2DAsync(static_cast<char*>(Lnak) + (size_t)q * M * esz, Mr * esz, lq, M * esz,
-                                         M * esz, (size_t)Nc * N, cudaMemcpyDeviceToDevice, st));
+          SFQ_CUDA_TRY(cudaMemcpy2DAsync(ldst + (size_t)q * M * esz, Mr * esz, lq, M * esz, M * esz, (size_t)Nc * N,
+                                         cudaMemcpyDeviceToDevice, st));
         }
       }
       SFQ_CUDA_TRY(cudaFreeAsync(tmp, st));
       if (lq) SFQ_CUDA_TRY(cudaFreeAsync(lq, st));
     }
     // haj = PsiT * hcore  (one_body.hpp:124-153); NONCOLLINEAR: PsiT * blockdiag(hcore, hcore)
+    for (int det = 0; det < ndet; ++det)
     for (int q = 0; q < npol; ++q) {
       GemmDesc d;
       d.M = N; d.N = M; d.K = M;
-      d.A = PsiT + (long)q * M; d.sAm = Mr; d.sAk = 1; d.a_cplx = true;
+      d.A = PsiT + det * RN + (long)q * M; d.sAm = Mr; d.sAk = 1; d.a_cplx = true;
       d.B = hcore; d.sBk = M; d.sBn = 1; d.b_cplx = false;
-      d.C = haj + (long)q * M; d.sCm = Mr; d.sCn = 1;
+      d.C = haj + det * RN + (long)q * M; d.sCm = Mr; d.sCn = 1;
       if ((rc = gemm_f64(d, st))) return rc;
     }
     // v0 = -1/2 L L^T over (j, n)   (RealDenseHamiltonian.cpp:165-180)
@@ -474,7 +585,9 @@ struct Engine {
       if ((rc = gemm_f64(d, st))) return rc;
     }
     // vMF = Re vbias(G_trial)  (NOMSD.cpp:437-466; AFQMCBasePropagator.cpp:107 zero_imag)
-    if (p.subtractMF) {
+    if (p.subtractMF && ndet > 1) {
+      if ((rc = mean_field_md(h_PsiT))) return rc;
+    } else if (p.subtractMF) {
       std::vector<cplx> psi(size_t(Mr) * N);  // PsiT^H  (Mr x N)
       for (int a = 0; a < N; ++a)
         for (int i = 0; i < Mr; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * Mr + i]);
@@ -569,9 +682,14 @@ struct Engine {
     }
     // walkers: copies of the trial, unit weight and phase
     {
+      // NOMSD::initial_guess (NOMSD.cpp:132-153): the determinant of largest |ci|
+      int d0 = 0;
+      for (int k = 1; k < ndet; ++k)
+        if (std::hypot(ci_h[k].x, ci_h[k].y) > std::hypot(ci_h[d0].x, ci_h[d0].y)) d0 = k;
+      const cplx* ps = h_PsiT + (size_t)d0 * RN;
       std::vector<cplx> psi(size_t(Mr) * N);
       for (int a = 0; a < N; ++a)
-        for (int i = 0; i < Mr; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * Mr + i]);
+        for (int i = 0; i < Mr; ++i) psi[size_t(i) * N + a] = cconj(ps[size_t(a) * Mr + i]);
       for (int w = 0; w < W; ++w)
         SFQ_CUDA_TRY(cudaMemcpyAsync(SM + (size_t)w * Mr * N, psi.data(), sizeof(cplx) * Mr * N,
                                      cudaMemcpyHostToDevice, st));
@@ -599,6 +717,118 @@ struct Engine {
     } else if (ov && ov != inv_ov) {
       SFQ_CUDA_TRY(cudaMemcpyAsync(ov, inv_ov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
     }
+    return SFQ_OK;
+  }
+
+  // --- multi-determinant NOMSD (ndet > 1) -----------------------------------------------------
+  // determinant d against the walkers B (nb of them): overlap matrices, their inverses in T and log
+  // overlaps (times post, without the ci term) in ov
+  int md_factor(int d, const cplx* B, int nb, cplx* ov, bool invert, double post) {
+    int rc;
+    const long o = d * det_elems();
+    const void* A = trial_real ? (const void*)(PsiTr + o) : (const void*)(PsiT + o);
+    if ((rc = ops::overlap_matrix(A, !trial_real, B, T, nb, Mr, N, st))) return rc;
+    if ((rc = ops::mask_cross_spin(T, nb, N, spin_split(), st))) return rc;
+    return lu_logdet(T, (long)N * N, nb, N, ov, false, post, invert, st);
+  }
+  // R[w][i][k] = sum_q sum_a PsiT_d[a][qM + i] Gc[w][a][qM + k]: determinant d's full G
+  // (PsiT_d^T Gc, density_matrix.hpp:580-585) summed over the spin (rows of both spins) and
+  // polarization (the diagonal component blocks) blocks, what vbias contracts with L
+  int md_reduced_green(int d, const cplx* Gc, int nb, cplx* R) {
+    int rc;
+    for (int q = 0; q < npol; ++q) {
+      GemmDesc g;
+      g.M = M; g.N = M; g.K = N; g.batch = nb;
+      g.A = PsiT + d * det_elems() + (long)q * M; g.sAm = 1; g.sAk = Mr; g.sAb = 0; g.a_cplx = true;
+      g.B = Gc + (long)q * M; g.sBk = Mr; g.sBn = 1; g.sBb = det_elems(); g.b_cplx = true;
+      g.C = R; g.sCm = M; g.sCn = 1; g.sCb = (long)M * M;
+      if (q > 0) g.beta = mk(1.0, 0.0);
+      if ((rc = gemm_f64(g, st))) return rc;
+    }
+    return SFQ_OK;
+  }
+  // vbias from a full G: out[w][n] = a sum_ik L[i][k][n] R[w][i][k] (Real3IndexFactorization.hpp:392-426)
+  int vbias_full(const cplx* R, int nb, cplx* out) {
+    GemmDesc g;
+    g.M = nb; g.N = Nc; g.K = M * M; g.batch = 1;
+    g.A = R; g.sAm = (long)M * M; g.sAk = 1; g.a_cplx = true;
+    g.B = Likn; g.sBk = Nc; g.sBn = 1; g.b_cplx = false;
+    g.C = out; g.sCm = Nc; g.sCn = 1;
+    g.alpha = mk(vb_scale(), 0.0);
+    return gemm_f64(g, st);
+  }
+  int md_grid(long n) const { return int(std::min<long>((n + 255) / 256, 64)); }
+  // NOMSD::vMF, ndet > 1 (NOMSD.cpp:466-512): the pairs q >= p of the trial's own determinants
+  int mean_field_md(const cplx* h_PsiT) {
+    int rc;
+    const long MM = (long)M * M;
+    bool first = true;
+    std::vector<cplx> psi(size_t(Mr) * N);
+    for (int pd = 0; pd < ndet; ++pd) {
+      const cplx* ps = h_PsiT + (size_t)pd * det_elems();
+      for (int a = 0; a < N; ++a)
+        for (int i = 0; i < Mr; ++i) psi[size_t(i) * N + a] = cconj(ps[size_t(a) * Mr + i]);
+      SFQ_CUDA_TRY(cudaMemcpyAsync(SM2, psi.data(), sizeof(cplx) * Mr * N, cudaMemcpyHostToDevice, st));
+      for (int qd = pd; qd < ndet; ++qd) {
+        // det_ops::MixedDensityMatrix as called there: the overlap not doubled for CLOSED
+        if ((rc = md_factor(qd, SM2, 1, ovtmp, true, 1.0))) return rc;
+        if ((rc = ops::green_compact(T, SM2, G, 1, Mr, N, st))) return rc;
+        if ((rc = md_reduced_green(qd, G, 1, Rd))) return rc;
+        md_pair_kernel<<<md_grid(MM), 256, 0, st>>>(Rd, ovtmp, ci_h[qd], ci_h[pd], Racc, wsum, MM, first ? 1 : 0);
+        SFQ_LAUNCHED();
+        first = false;
+      }
+      SFQ_CUDA_TRY(cudaStreamSynchronize(st));  // psi is refilled for the next p
+    }
+    md_normalize_kernel<<<dim3(md_grid(MM), 1), 256, 0, st>>>(Racc, wsum, MM);
+    SFQ_LAUNCHED();
+    if ((rc = vbias_full(Racc, 1, X))) return rc;
+    if ((rc = real_of(X, vmf, Nc, st))) return rc;
+    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    return SFQ_OK;
+  }
+  // NOMSD::vbias with ndet > 1 (NOMSD.cpp:39-61,238-278): the ci-weighted full G, then vbias on it
+  int vbias_md(cplx* out) {
+    int rc;
+    const long MM = (long)M * M;
+    const cplx* lm = props + (long)P_OVLP * W;
+    for (int d = 0; d < ndet; ++d) {
+      if ((rc = md_factor(d, SM, W, md_ov + (long)d * W, true, ov_scale()))) return rc;
+      if ((rc = ops::green_compact(T, SM, G, W, Mr, N, st))) return rc;
+      if ((rc = md_reduced_green(d, G, W, Rd))) return rc;
+      md_accumulate_kernel<<<dim3(md_grid(MM), W), 256, 0, st>>>(Rd, md_ov + (long)d * W, lm, ci_h[d], Racc, wsum,
+                                                                 MM, d == 0 ? 1 : 0);
+      SFQ_LAUNCHED();
+    }
+    md_normalize_kernel<<<dim3(md_grid(MM), W), 256, 0, st>>>(Racc, wsum, MM);
+    SFQ_LAUNCHED();
+    return vbias_full(Racc, W, out);
+  }
+  // NOMSD::Log_Overlap with ndet > 1 into ov (W)
+  int log_overlap_md(cplx* ov) {
+    int rc;
+    inv_cached = false;
+    for (int d = 0; d < ndet; ++d)
+      if ((rc = md_factor(d, SM, W, md_ov + (long)d * W, false, ov_scale()))) return rc;
+    md_logsum_kernel<<<(W + 127) / 128, 128, 0, st>>>(md_ov, md_lci, ndet, W, ov);
+    SFQ_LAUNCHED();
+    return SFQ_OK;
+  }
+  // NOMSD::Energy with ndet > 1: E3 and ovtmp
+  int energy_md() {
+    int rc;
+    inv_cached = false;
+    const long o = det_elems();
+    for (int d = 0; d < ndet; ++d) {
+      if ((rc = md_factor(d, SM, W, md_ov + (long)d * W, true, ov_scale()))) return rc;
+      if ((rc = ops::green_compact(T, SM, G, W, Mr, N, st))) return rc;
+      const void* Ld = static_cast<const char*>(Lnak) + (size_t)d * Nc * o * lnak_esz();
+      if ((rc = ops::energy(md_E + (long)d * W * 3, G, haj + d * o, Ld, !trial_real, p.E0, W, N, Mr, Nc, 1, 1, 1,
+                            Tchunk, tchunk_elems, exxn, kl, st, spin_split())))
+        return rc;
+    }
+    md_energy_kernel<<<(W + 127) / 128, 128, 0, st>>>(md_ov, md_E, md_cic, ndet, W, E3, ovtmp);
+    SFQ_LAUNCHED();
     return SFQ_OK;
   }
 
@@ -651,12 +881,18 @@ struct Engine {
   int propagate(double Eshift, unsigned long long step, const double* uniforms) {
     if (mixed) return propagate_mixed(Eshift, step, uniforms);
     int rc;
-    ph_begin(SFQ_PH_DENSITY);
-    if ((rc = density(nullptr))) return rc;                                          // 1. G
-    ph_end(SFQ_PH_DENSITY);
-    ph_begin(SFQ_PH_VBIAS);
-    if ((rc = ops::vbias(G, Lnak, !trial_real, X, W, N, Mr, Nc, vb_scale(), st))) return rc;
-    ph_end(SFQ_PH_VBIAS);
+    if (ndet > 1) {
+      ph_begin(SFQ_PH_VBIAS);
+      if ((rc = vbias_md(X))) return rc;                                              // 1. G, vbias
+      ph_end(SFQ_PH_VBIAS);
+    } else {
+      ph_begin(SFQ_PH_DENSITY);
+      if ((rc = density(nullptr))) return rc;                                        // 1. G
+      ph_end(SFQ_PH_DENSITY);
+      ph_begin(SFQ_PH_VBIAS);
+      if ((rc = ops::vbias(G, Lnak, !trial_real, X, W, N, Mr, Nc, vb_scale(), st))) return rc;
+      ph_end(SFQ_PH_VBIAS);
+    }
     ph_begin(SFQ_PH_FIELDS);
     FieldParams fp;                                                                   // 2. X
     fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
@@ -682,7 +918,7 @@ struct Engine {
     if ((rc = ops::propagate(SM, P1, false, V, W, M, N, p.taylor_order, TMN, T1, T2, st, npol))) return rc;  // 4.
     ph_end(SFQ_PH_PROPAGATE);
     ph_begin(SFQ_PH_OVERLAP);
-    if ((rc = log_overlap(newov))) return rc;                                         // 5.
+    if ((rc = ndet > 1 ? log_overlap_md(newov) : log_overlap(newov))) return rc;      // 5.
     ph_end(SFQ_PH_OVERLAP);
     ph_begin(SFQ_PH_UPDATE);
     UpdateParams up;                                                                  // 6.+7.
@@ -1080,7 +1316,7 @@ struct Engine {
     int rc;
     ph_begin(SFQ_PH_ORTHO);
     const long NN = (long)N * N;
-    if (inv_cached && tchunk_elems >= 2L * W * NN) {
+    if (ndet == 1 && inv_cached && tchunk_elems >= 2L * W * NN) {
       // the cached inverse overlaps and log overlaps of the walkers ride through the QR, which
       // gives wfn->Log_Overlap(wset) of the orthogonalized walkers without a new factorization
       if (inv_ov != newov)
@@ -1092,7 +1328,7 @@ struct Engine {
     } else {
       inv_cached = false;
       if ((rc = ops::orthogonalize(SM, SM2, T, status, nullptr, W, Mr, N, st, spin_split()))) return rc;
-      if ((rc = log_overlap(newov))) return rc;  // wfn->Log_Overlap(wset)
+      if ((rc = ndet > 1 ? log_overlap_md(newov) : log_overlap(newov))) return rc;  // wfn->Log_Overlap(wset)
     }
     SFQ_CUDA_TRY(cudaMemcpyAsync(props + (long)P_OVLP * W, newov, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
     ph_end(SFQ_PH_ORTHO);
@@ -1123,6 +1359,11 @@ struct Engine {
     int rc;
     if (mixed) return energy_mixed();
     ph_begin(SFQ_PH_ENERGY);
+    if (ndet > 1) {
+      if ((rc = energy_md())) return rc;
+      ph_end(SFQ_PH_ENERGY);
+      return SFQ_OK;
+    }
     if ((rc = density(ovtmp))) return rc;
     if ((rc = ops::energy(E3, G, haj, Lnak, !trial_real, p.E0, W, N, Mr, Nc, 1, 1, 1, Tchunk, tchunk_elems, exxn, kl,
                           st, spin_split())))
@@ -1587,9 +1828,10 @@ void sfq_engine_params_default(sfq_engine_params_t* p) {
   p->nel_dn = 0;
 }
 
-int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
-                      const void* PsiT) {
-  if (!out || !p || !hcore || !Likn || !PsiT) return record_error(SFQ_ERR_ARG, "null pointer");
+int sfq_engine_create_nomsd(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
+                            int ndet, const void* PsiT, const void* ci) {
+  if (!out || !p || !hcore || !Likn || !PsiT || (ndet > 1 && !ci)) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (ndet < 1) return record_error(SFQ_ERR_SHAPE, "engine: ndet=%d", ndet);
   *out = nullptr;
   const int wt = p->walker_type == 0 ? SFQ_WALKER_CLOSED : p->walker_type;
   if (wt != SFQ_WALKER_CLOSED && wt != SFQ_WALKER_COLLINEAR && wt != SFQ_WALKER_NONCOLLINEAR)
@@ -1613,9 +1855,14 @@ int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const dou
   e.nup = p->nel;
   e.npol = npol;
   e.Mr = npol * p->nmo;
+  e.ndet = ndet;
+  if (ndet > 1) {
+    const cplx* c = reinterpret_cast<const cplx*>(ci);
+    e.ci_h.assign(c, c + ndet);
+  }
   const cplx* ps = reinterpret_cast<const cplx*>(PsiT);
   e.trial_real = true;
-  for (long i = 0; i < (long)e.N * e.Mr; ++i)
+  for (long i = 0; i < (long)ndet * e.N * e.Mr; ++i)
     if (ps[i].y != 0.0) { e.trial_real = false; break; }
   e.mixed = p->precision == SFQ_PRECISION_MIXED || p->precision == SFQ_PRECISION_MIXED_FP32;
   e.nplanes = p->precision == SFQ_PRECISION_MIXED_FP32 ? 3 : 2;
@@ -1623,9 +1870,10 @@ int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const dou
     delete h;
     return record_error(SFQ_ERR_ARG, "engine: unknown precision %d", p->precision);
   }
-  if (e.mixed && (coll || npol > 1)) {
+  if (e.mixed && (coll || npol > 1 || ndet > 1)) {
     delete h;
-    return record_error(SFQ_ERR_UNSUPPORTED, "engine: COLLINEAR and NONCOLLINEAR walkers run in FP64 (SFQ_PRECISION_FP64)");
+    return record_error(SFQ_ERR_UNSUPPORTED,
+                        "engine: COLLINEAR and NONCOLLINEAR walkers and multi-determinant trials run in FP64");
   }
   if (e.mixed && (!e.trial_real || e.M % 8 || e.Nc % 8)) {
     delete h;
@@ -1642,6 +1890,11 @@ int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const dou
   }
   *out = h;
   return SFQ_OK;
+}
+
+int sfq_engine_create(sfq_engine_t* out, const sfq_engine_params_t* p, const double* hcore, const double* Likn,
+                      const void* PsiT) {
+  return sfq_engine_create_nomsd(out, p, hcore, Likn, 1, PsiT, nullptr);
 }
 
 int sfq_engine_destroy(sfq_engine_t h) {

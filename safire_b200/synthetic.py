@@ -49,6 +49,7 @@ class System:
     E0: float = 0.0
     nel_dn: int = -1       # COLLINEAR walkers: the last nel_dn rows of PsiT are the down spin; -1: CLOSED
     npol: int = 1          # 2: NONCOLLINEAR walkers, PsiT (N, 2M) spinor orbitals
+    ci: np.ndarray = None  # multi-determinant trial: the coefficients, PsiT then (ndet, N, M or 2M)
 
     @property
     def M(self):

@@ -81,3 +81,54 @@ def statistically_equal(a, a_err, b, b_err, significance=0.001, components=1):
     z = norm.ppf(1 - significance / (2 * components))
     tol = max(z * float(np.hypot(abs(a_err), abs(b_err))), 1e-9 * (1 + abs(b)))
     return abs(a - b) <= tol, abs(a - b), tol
+
+
+def oracle_hamiltonian(snap):
+    """The oracle's Hamiltonian for a snapshot case: the walker type's class, or their
+    multi-determinant combination."""
+    from oracle import afqmc_oracle as O
+    wt = snap["settings"]["walker_type"]
+
+    def one(PsiT=None, up=None, dn=None, ci=1.0):
+        if wt == "NONCOLLINEAR":
+            return O.NoncollinearHamiltonian(snap["hcore"], snap["Likn"], PsiT, snap["E0"], ci)
+        if wt == "COLLINEAR":
+            return O.CollinearHamiltonian(snap["hcore"], snap["Likn"], up, dn, snap["E0"], ci)
+        return O.Hamiltonian(snap["hcore"], snap["Likn"], PsiT, snap["E0"])
+
+    if "ci_dets" in snap:
+        n = len(snap["ci_dets"])
+        if wt == "COLLINEAR":
+            dets = [one(up=snap["PsiT_up_dets"][d], dn=snap["PsiT_dn_dets"][d]) for d in range(n)]
+        else:
+            dets = [one(PsiT=snap["PsiT_dets"][d]) for d in range(n)]
+        return O.MultiDetHamiltonian(dets, snap["ci_dets"])
+    return one(PsiT=snap["PsiT"], up=snap.get("PsiT_up"), dn=snap.get("PsiT_dn"), ci=snap["ci"])
+
+
+def engine_system(snap):
+    """The engine's System for a snapshot case: COLLINEAR stacks the up rows over the down rows,
+    NONCOLLINEAR takes the (N, 2M) spinor trial, a multi-determinant trial stacks its determinants."""
+    from safire_b200 import synthetic
+    wt = snap["settings"]["walker_type"]
+    M, Nc = snap["hcore"].shape[0], snap["Likn"].shape[2]
+    kw = {}
+    if "ci_dets" in snap:
+        if wt == "COLLINEAR":
+            PsiT = np.concatenate([snap["PsiT_up_dets"], snap["PsiT_dn_dets"]], axis=1)
+            kw["nel_dn"] = snap["PsiT_dn_dets"].shape[1]
+        else:
+            PsiT = snap["PsiT_dets"]
+        kw["ci"] = snap["ci_dets"]
+        N = PsiT.shape[1]
+    elif wt == "COLLINEAR":
+        PsiT = np.concatenate([snap["PsiT_up"], snap["PsiT_dn"]])
+        kw["nel_dn"] = snap["PsiT_dn"].shape[0]
+        N = PsiT.shape[0]
+    else:
+        PsiT = snap["PsiT"]
+        N = PsiT.shape[0]
+    if wt == "NONCOLLINEAR":
+        kw["npol"] = 2
+    spec = synthetic.SystemSpec(M=M, N=N, Nc=Nc, decay=0.0)
+    return synthetic.System(spec, snap["hcore"], snap["Likn"], PsiT, snap["E0"], **kw)

@@ -6,7 +6,8 @@ comb's uniform (sfq_engine_population_control_uniform).  Driven in run_afqmc's o
 reproduce, step by step, the oracle's energy-estimator series, and through it the snapshot the
 reference recorded, to the reference's own 1e-9: BH with an RHF trial and CLOSED walkers;
 COLLINEAR walkers with BH's UHF and RHF trials and Li's polarized ROHF trial (no down electrons);
-NONCOLLINEAR walkers with BH's RHF and UHF trials upgraded to spinors and a GHF trial.
+NONCOLLINEAR walkers with BH's RHF and UHF trials upgraded to spinors and a GHF trial; and the
+34-determinant CASCI trials with each walker type.
 """
 import numpy as np
 import pytest
@@ -15,37 +16,24 @@ from oracle import afqmc_oracle as O
 from oracle.mt19937 import HostRandomGenerator, split_seed
 from safire_b200 import afqmc as A
 from safire_b200 import capi, synthetic
-from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, snapshot, snapshot_match
+from tests.golden_io import (SNAPSHOT_OBSERVABLES, bh_snapshot, engine_system, oracle_hamiltonian, snapshot,
+                             snapshot_match)
 
 pytestmark = pytest.mark.gpu
 
 CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_rhf_collinear", "li_rohf_collinear",
-         "bh_rhf_noncollinear", "bh_uhf_noncollinear", "bh_ghf_noncollinear"]
+         "bh_rhf_noncollinear", "bh_uhf_noncollinear", "bh_ghf_noncollinear",
+         # 34-determinant CASCI trials
+         "bh_rcasci_rhf_closed", "bh_rcasci_rhf_collinear", "bh_rcasci_rhf_noncollinear",
+         "bh_rcasci_uhf_collinear", "bh_rcasci_uhf_noncollinear", "bh_rcasci_ghf_noncollinear"]
 
 
 def _system(snap):
-    """The engine's System of a case: COLLINEAR stacks PsiT_up over PsiT_dn; NONCOLLINEAR takes the
-    (N, 2M) spinor trial."""
-    M, Nc = snap["hcore"].shape[0], snap["Likn"].shape[2]
-    if snap["settings"]["walker_type"] == "NONCOLLINEAR":
-        spec = synthetic.SystemSpec(M=M, N=snap["PsiT"].shape[0], Nc=Nc, decay=0.0)
-        return synthetic.System(spec, snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"], npol=2)
-    if snap["settings"]["walker_type"] == "COLLINEAR":
-        PsiT = np.concatenate([snap["PsiT_up"], snap["PsiT_dn"]])
-        spec = synthetic.SystemSpec(M=M, N=PsiT.shape[0], Nc=Nc, decay=0.0)
-        return synthetic.System(spec, snap["hcore"], snap["Likn"], PsiT, snap["E0"],
-                                nel_dn=snap["PsiT_dn"].shape[0])
-    spec = synthetic.SystemSpec(M=M, N=snap["PsiT"].shape[0], Nc=Nc, decay=0.0)
-    return synthetic.System(spec, snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
+    return engine_system(snap)
 
 
 def _oracle_hamiltonian(snap):
-    if snap["settings"]["walker_type"] == "NONCOLLINEAR":
-        return O.NoncollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"], snap["ci"])
-    if snap["settings"]["walker_type"] == "COLLINEAR":
-        return O.CollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_up"], snap["PsiT_dn"], snap["E0"],
-                                      snap["ci"])
-    return O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
+    return oracle_hamiltonian(snap)
 
 
 def _engine_series(snap, system=None):
@@ -79,7 +67,7 @@ def test_engine_reproduces_reference_snapshot(case):
         assert snapshot_match(series[k], snap["recorded"][k], O.rebinned_average) is not None, k
     if st["walker_type"] == "COLLINEAR":
         # the reference's walker rows: the up block (M x nup), then the down block (M x ndn)
-        nup = snap["PsiT_up"].shape[0]
+        nup = (snap["PsiT_up_dets"][0] if "ci_dets" in snap else snap["PsiT_up"]).shape[0]
         W, M, N = SM.shape
         assert np.array_equal(rows[:, :M * nup].reshape(W, M, nup), SM[:, :, :nup])
         assert np.array_equal(rows[:, M * nup:M * N].reshape(W, M, N - nup), SM[:, :, nup:])
@@ -99,7 +87,7 @@ def test_collinear_with_identical_spins_is_closed():
         assert np.max(np.abs(a - b)) < 1e-10 * np.max(np.abs(a)), k
 
 
-@pytest.mark.parametrize("case", ["bh_uhf_collinear", "bh_ghf_noncollinear"])
+@pytest.mark.parametrize("case", ["bh_uhf_collinear", "bh_ghf_noncollinear", "bh_rcasci_rhf_closed"])
 def test_spin_walkers_rejected_in_mixed_precision(case):
     with pytest.raises(capi.SafireError) as ex:
         A.AfqmcEngine(_system(snapshot(case)), 8, dt=0.01, precision=capi.PRECISION_MIXED)

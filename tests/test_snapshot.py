@@ -20,7 +20,7 @@ import pytest
 
 from oracle import afqmc_oracle as O
 from oracle.mt19937 import MT19937, HostRandomGenerator, split_seed
-from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, snapshot, snapshot_match
+from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, oracle_hamiltonian, snapshot, snapshot_match
 
 REF = "/root/reference/tests/functional"
 
@@ -49,28 +49,7 @@ def test_split_seed_streams_distinct():
 
 
 def _oracle_hamiltonian(snap):
-    if "ci_dets" in snap:
-        return _oracle_multidet(snap)
-    if snap["settings"]["walker_type"] == "NONCOLLINEAR":
-        return O.NoncollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"], snap["ci"])
-    if snap["settings"]["walker_type"] == "COLLINEAR":
-        return O.CollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_up"], snap["PsiT_dn"], snap["E0"],
-                                      snap["ci"])
-    return O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT"], snap["E0"])
-
-
-def _oracle_multidet(snap):
-    wt = snap["settings"]["walker_type"]
-    dets = []
-    for d in range(len(snap["ci_dets"])):
-        if wt == "CLOSED":
-            dets.append(O.Hamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_dets"][d], snap["E0"]))
-        elif wt == "COLLINEAR":
-            dets.append(O.CollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_up_dets"][d],
-                                               snap["PsiT_dn_dets"][d], snap["E0"]))
-        else:
-            dets.append(O.NoncollinearHamiltonian(snap["hcore"], snap["Likn"], snap["PsiT_dets"][d], snap["E0"]))
-    return O.MultiDetHamiltonian(dets, snap["ci_dets"])
+    return oracle_hamiltonian(snap)
 
 
 SNAPSHOT_CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_rhf_collinear", "li_rohf_collinear",
