@@ -982,11 +982,69 @@ def measure_step(ham, wset, step, dt):
             "Phase": complex(np.sum(w) / np.sum(aw)), "TotalWeight": complex(np.sum(w))}
 
 
+def _references(ham):
+    """(determinant Hamiltonians, coefficients) of a trial: NOMSD::getReferences (NOMSD.cpp:104-129)."""
+    if isinstance(ham, MultiDetHamiltonian):
+        return ham.dets, ham.ci
+    return [ham], np.array([getattr(ham, "ci", 1.0)], np.complex128)
+
+
+def measure_mixed_rdms(ham, wset):
+    """MixedEstimator::measure with the OneRDM and DiagonalTwoRDM observables (MixedEstimator.hpp:37-147,
+    Observables/onerdm.hpp:42-75, Observables/diagonal_twordm.hpp:36-140), one rank.
+
+    Per reference determinant d the full mixed G_d (W, nspin, Mr, Mr) and its log overlap (one
+    determinant per spin, not doubled for CLOSED) give refCoeff_d = conj(c_d) exp(ov_d - OVLP) /
+    sum_d' conj(c_d') exp(ov_d' - OVLP); with weightedCoeff = weight * refCoeff_d,
+      OneRDM[s,i,j]  += sum_w weightedCoeff[w] G_d[w,s,i,j]
+      2RDM (aaaa)_s  += sum_w wc G[w,s,i,i] G[w,s,j,j] - wc G[w,s,i,j] G[w,s,j,i]
+      2RDM (aabb)    += sum_w wc G[w,0,i,i] G[w,dn,j,j]   (CLOSED, COLLINEAR; dn = 0 for CLOSED)
+    each divided by sum_w weight, the 2RDM folded over i <-> j (compress, :104-140)."""
+    dets, ci = _references(ham)
+    w = wset.weight
+    shift = wset.ovlp
+    parts = [d.full_green(wset.SM) for d in dets]
+    e = [np.conj(ci[k]) * np.exp(ov - shift) for k, (_, ov) in enumerate(parts)]
+    tot = np.sum(e, axis=0)
+    wt = "NONCOLLINEAR" if isinstance(dets[0], NoncollinearHamiltonian) else (
+        "COLLINEAR" if isinstance(dets[0], CollinearHamiltonian) else "CLOSED")
+    G0 = parts[0][0]
+    nspin, Mr = G0.shape[1], G0.shape[2]
+    nblk = {"COLLINEAR": 3, "CLOSED": 2}.get(wt, 1)
+    one = np.zeros((nspin, Mr, Mr), np.complex128)
+    avg = np.zeros((nblk, Mr, Mr), np.complex128)
+    for k, (G, _) in enumerate(parts):
+        wc = w * e[k] / tot
+        one += np.einsum('w,wsij->sij', wc, G)
+        dg = np.einsum('wsii->wsi', G)
+        for sp in range(nspin):
+            avg[2 * sp] += np.einsum('w,wi,wj->ij', wc, dg[:, sp], dg[:, sp])
+            avg[2 * sp] -= np.einsum('w,wij,wji->ij', wc, G[:, sp], G[:, sp])
+        if wt != "NONCOLLINEAR":
+            avg[1] += np.einsum('w,wi,wj->ij', wc, dg[:, 0], dg[:, 1 if wt == "COLLINEAR" else 0])
+    den = np.sum(w)
+    one, avg = one / den, avg / den
+    M = ham.M
+    out = []
+    if wt != "NONCOLLINEAR":
+        for i in range(M):
+            out += [(avg[0, i, j] + avg[0, j, i]) / 2 for j in range(i + 1, M)]
+            out += [avg[1, i, j] for j in range(M)]
+        if wt == "COLLINEAR":
+            for i in range(M):
+                out += [(avg[2, i, j] + avg[2, j, i]) / 2 for j in range(i + 1, M)]
+    else:
+        for i in range(2 * M):
+            out += [(avg[0, i, j] + avg[0, j, i]) / 2 for j in range(i + 1, 2 * M)]
+    return {"MixedEstimator/OneRDM": one, "MixedEstimator/DiagonalTwoRDM": np.array(out, np.complex128)}
+
+
 def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, measure_interval=10,
-               equilibration_steps=0, relax=None, rank=0, **prop_args):
+               equilibration_steps=0, relax=None, rank=0, mixed_interval=None, **prop_args):
     """execute_simulation + run_afqmc for one stage with HostRandomGenerator streams: walkers from
     the trial (NOMSD::initial_guess), Energy + seedPseudoEnergy, Eshift = averageEnergy, then the
     step loop.  Fields come from stream 1 (nwalk x nchol uniforms per step), the comb from stream 0.
+    With mixed_interval the mixed estimator's one-body and diagonal two-body RDMs are measured too.
     Returns (initial Eshift, final Eshift, {observable: list of bins})."""
     from .mt19937 import HostRandomGenerator, split_seed
     walker_rng = HostRandomGenerator(split_seed(seed, rank, 0))
@@ -1009,6 +1067,9 @@ def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, 
         if step >= equilibration_steps:
             if step % measure_interval == 0:
                 for k, v in measure_step(ham, wset, step, dt).items():
+                    series.setdefault(k, []).append(v)
+            if mixed_interval and step % mixed_interval == 0:
+                for k, v in measure_mixed_rdms(ham, wset).items():
                     series.setdefault(k, []).append(v)
         else:
             Eshift += relax * (average_pseudo_energy(wset, dt) - Eshift)

@@ -38,6 +38,20 @@ from safire_b200.inputs import load_dense_hamiltonian, load_nomsd_determinants, 
 
 OBSERVABLES = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "Overlap", "ProjectionTime",
                "EffectiveNumWalkers", "Phase", "TotalWeight")
+# the RDM estimators of the back-propagation cases: their mixed and back-propagated observables
+RDM_OBSERVABLES = ("MixedEstimator/OneRDM", "MixedEstimator/DiagonalTwoRDM")
+
+
+def rdm_records(res, ex, out):
+    """The mixed estimator's recorded RDMs and its measure interval, where the case has them."""
+    est = ex.get("estimators")
+    if not est or "mixed" not in est:
+        return
+    out["mixed_interval"] = np.int64(est["mixed"]["measure_interval"])
+    for k in RDM_OBSERVABLES:
+        key = k.replace("/", "_")
+        out[f"mean_{key}"] = np.asarray(res[f"measurements/Stage0/{k}/mean"])
+        out[f"error_{key}"] = np.asarray(res[f"measurements/Stage0/{k}/error"])
 
 
 def snapshot_case(fn, system, ham_file, wfn_file, case, walker_type, out_name, with_hamiltonian=True):
@@ -61,6 +75,7 @@ def snapshot_case(fn, system, ham_file, wfn_file, case, walker_type, out_name, w
     for k in OBSERVABLES:
         out[f"mean_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/mean"])
         out[f"error_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/error"])
+    rdm_records(res, ex, out)
     path = os.path.join(HERE, out_name)
     np.savez_compressed(path, **out)
     print(path, settings)
@@ -85,6 +100,7 @@ def multidet_case(fn, system, ham_file, wfn_file, case, walker_type, out_name):
     for k in OBSERVABLES:
         out[f"mean_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/mean"])
         out[f"error_{k}"] = np.asarray(res[f"measurements/Stage0/{k}/error"])
+    rdm_records(res, ex, out)
     path = os.path.join(HERE, out_name)
     np.savez_compressed(path, **out)
     print(path, len(dets), "determinants", settings)

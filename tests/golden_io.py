@@ -33,7 +33,12 @@ def snapshot(name):
     The BH collinear case shares the BH Hamiltonian tensors of the closed case's file."""
     z = np.load(os.path.join(HERE, f"{name}_snapshot.npz"))
     rec = {k: (z[f"mean_{k}"][()], z[f"error_{k}"][()]) for k in SNAPSHOT_OBSERVABLES}
-    out = dict(settings=json.loads(str(z["settings"])), recorded=rec)
+    for k in ("MixedEstimator/OneRDM", "MixedEstimator/DiagonalTwoRDM"):
+        key = k.replace("/", "_")
+        if f"mean_{key}" in z:
+            rec[k] = (z[f"mean_{key}"], z[f"error_{key}"])
+    out = dict(settings=json.loads(str(z["settings"])), recorded=rec,
+               mixed_interval=int(z["mixed_interval"]) if "mixed_interval" in z else None)
     if "ci_dets" in z:  # multi-determinant trial: per-determinant orbitals and coefficients
         out.update(ci_dets=z["ci_dets"], PsiT_dets=z["PsiT_dets"])
         if "PsiT_up_dets" in z:

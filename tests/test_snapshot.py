@@ -127,3 +127,22 @@ def test_collinear_with_identical_spins_is_closed():
     for k in ("Energy", "ExchangeEnergy", "CoulombEnergy", "Overlap"):
         a, b = np.asarray(runs[0][2][k]), np.asarray(runs[1][2][k])
         assert np.max(np.abs(a - b)) < 1e-10 * np.max(np.abs(a)), k
+
+
+RDM_CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_uhf_noncollinear", "bh_rcasci_uhf_collinear",
+             "bh_rcasci_uhf_noncollinear", "li_rohf_collinear"]
+
+
+@pytest.mark.parametrize("case", RDM_CASES)
+def test_oracle_reproduces_recorded_mixed_rdms(case):
+    """The mixed estimator's one-body and diagonal two-body RDMs the reference recorded with the
+    back-propagation cases (every 2 steps): CLOSED, COLLINEAR, NONCOLLINEAR, a 34-determinant trial."""
+    snap = snapshot(case)
+    st = snap["settings"]
+    _, _, series = O.run_seeded(oracle_hamiltonian(snap), st["nwalk"], st["dt"], st["steps"], st["seed"],
+                                ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
+                                measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"])
+    for k in ("MixedEstimator/OneRDM", "MixedEstimator/DiagonalTwoRDM"):
+        assert len(series[k]) == st["steps"] // snap["mixed_interval"]
+        assert np.asarray(series[k]).shape[1:] == snap["recorded"][k][0].shape
+        assert snapshot_match(series[k], snap["recorded"][k], O.rebinned_average) is not None, k
