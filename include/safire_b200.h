@@ -257,6 +257,12 @@ int sfq_engine_propagate_host(sfq_engine_t e, double Eshift, unsigned long long 
 int sfq_engine_orthogonalize(sfq_engine_t e);
 /* population_control (population_control.hpp:219-255), single rank; the comb draws Philox(seed, call) */
 int sfq_engine_population_control(sfq_engine_t e, unsigned long long call);
+/* MixedEstimator::measure with the OneRDM and DiagonalTwoRDM observables (MixedEstimator.hpp:37-147,
+ * Observables/onerdm.hpp, diagonal_twordm.hpp), FP64 engines: one_rdm (nspin, R, R) complex with
+ * nspin 2 for COLLINEAR walkers, else 1, and R = 2 nmo for NONCOLLINEAR, else nmo; diag_two_rdm the
+ * folded diagonal two-body RDM, nmo (2 nmo - 1) complex values (CLOSED: nmo (2 nmo - 1) - nmo (nmo - 1) / 2).
+ * Both divided by the total weight, as recorded per measurement; host pointers, either may be NULL. */
+int sfq_engine_measure_rdm(sfq_engine_t e, void* one_rdm, void* diag_two_rdm);
 /* the same with the comb's uniform r in [0, 1) from the caller: the draw comb takes from the walker set's
  * generator (population_control.hpp:41-42, HostRandomGenerator::sampleUniformFields), so a caller that
  * owns the reference's stream replays its population control exactly */

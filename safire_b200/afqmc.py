@@ -266,14 +266,28 @@ class AfqmcEngine:
         keys = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "TotalWeight")
         return {k: complex(o[2 * i], o[2 * i + 1]) for i, k in enumerate(keys)}
 
+    def measure_mixed_rdms(self):
+        """MixedEstimator's OneRDM and DiagonalTwoRDM of the current walkers (sfq_engine_measure_rdm)."""
+        nspin = 2 if self.params.walker_type == capi.WALKER_COLLINEAR else 1
+        M = self.M
+        if self.params.walker_type == capi.WALKER_CLOSED:
+            n2 = M * (2 * M - 1) - M * (M - 1) // 2
+        else:
+            n2 = M * (2 * M - 1)
+        one = np.empty((nspin, self.Mr, self.Mr), np.complex128)
+        two = np.empty(n2, np.complex128)
+        check(lib().sfq_engine_measure_rdm(self.h, one.ctypes.data, two.ctypes.data))
+        return {"MixedEstimator/OneRDM": one, "MixedEstimator/DiagonalTwoRDM": two}
+
     def run_with_streams(self, steps, Eshift, field_uniforms, comb_uniform, ortho_interval=10, pop_interval=10,
-                         equilibration_steps=100, measure_interval=10, relax=None, step0=0):
+                         equilibration_steps=100, measure_interval=10, relax=None, step0=0, mixed_interval=None):
         """run_afqmc's step loop (run_afqmc.cpp:69-104) with the caller's random streams at the
         reference's two injection points: field_uniforms(n) returns the n = nwalk * nchol uniforms
         of a step (walker-major, assemble_X's sampleUniformFields) and comb_uniform() the comb's
         uniform (population_control.hpp:41-42).  Given the reference's own generators it replays
         a reference run.  Every measurement records EnergyEstimator::measure's observables
-        (EnergyEstimator.h:51-100).  Returns (Eshift, {observable: list of bins})."""
+        (EnergyEstimator.h:51-100), and every mixed_interval steps the mixed estimator's RDMs.
+        Returns (Eshift, {observable: list of bins})."""
         if relax is None:
             relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
         series = {}
@@ -295,6 +309,9 @@ class AfqmcEngine:
                     m["EffectiveNumWalkers"] = float(np.sum(aw) ** 2 / np.sum(aw * aw))
                     m["Phase"] = complex(np.sum(w) / np.sum(aw))
                     for k, v in m.items():
+                        series.setdefault(k, []).append(v)
+                if mixed_interval and step % mixed_interval == 0:
+                    for k, v in self.measure_mixed_rdms().items():
                         series.setdefault(k, []).append(v)
             else:
                 Eshift += relax * (self.averages()[0] - Eshift)

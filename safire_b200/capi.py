@@ -115,6 +115,7 @@ _SIGS = {
     "sfq_engine_orthogonalize": ([_VP], _I),
     "sfq_engine_population_control": ([_VP, _U64], _I),
     "sfq_engine_population_control_uniform": ([_VP, ctypes.c_double], _I),
+    "sfq_engine_measure_rdm": ([_VP, _VP, _VP], _I),
     "sfq_engine_averages": ([_VP, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)], _I),
     "sfq_engine_measure": ([_VP, _VP], _I),
     "sfq_engine_run": ([_VP, ctypes.POINTER(RunParams), ctypes.POINTER(_D), _VP, _I, ctypes.POINTER(_I)], _I),

@@ -210,6 +210,48 @@ __global__ void md_energy_kernel(const cplx* ov, const cplx* Ed, const cplx* cic
   Ov[w] = cadd(clog_(deno), om);
 }
 
+// ---- the mixed estimator's RDMs (MixedEstimator.hpp:37-147) ---------------------------------
+// tot[w] = sum_d conj(ci_d) exp(ov_d[w] - shift[w]) over the reference determinants
+__global__ void rdm_tot_kernel(const cplx* ov, const cplx* cic, const cplx* shift, int ndet, int W, cplx* tot) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  cplx s = mk(0.0, 0.0);
+  for (int d = 0; d < ndet; ++d) s = cadd(s, cmul(cic[d], cexp_(csub(ov[(long)d * W + w], shift[w]))));
+  tot[w] = s;
+}
+// wc[w] = weight[w] conj(ci_d) exp(ov_d[w] - shift[w]) / tot[w]
+__global__ void rdm_coeff_kernel(const cplx* ov, cplx cic, const cplx* shift, const cplx* tot, const cplx* weight,
+                                 int W, cplx* wc) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  wc[w] = cmul(weight[w], cdiv(cmul(cic, cexp_(csub(ov[w], shift[w]))), tot[w]));
+}
+// diagonal two-body RDM blocks (Observables/diagonal_twordm.hpp:60-80), avg[b][i][j] += sum_w wc[w] (...):
+// b = 2 s: G[s,i,i] G[s,j,j] - G[s,i,j] G[s,j,i] for each spin s; b = 1 (CLOSED, COLLINEAR):
+// G[0,i,i] G[dn,j,j], dn the down block (CLOSED: the same)
+__global__ void rdm_two_kernel(const cplx* Gf, const cplx* wc, int W, int nspin, int Mr, int nblk, cplx* avg) {
+  const long MM = (long)Mr * Mr;
+  const long total = nblk * MM;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const int b = int(e / MM);
+    const int i = int((e % MM) / Mr), j = int(e % Mr);
+    cplx acc = mk(0.0, 0.0);
+    for (int w = 0; w < W; ++w) {
+      const cplx* Gw = Gf + (long)w * nspin * MM;
+      cplx v;
+      if (b == 1 && nblk > 1) {
+        const cplx* Gd = Gw + (nspin == 2 ? MM : 0);
+        v = cmul(Gw[(long)i * Mr + i], Gd[(long)j * Mr + j]);
+      } else {
+        const cplx* Gs = Gw + (long)(b / 2) * MM;
+        v = csub(cmul(Gs[(long)i * Mr + i], Gs[(long)j * Mr + j]), cmul(Gs[(long)i * Mr + j], Gs[(long)j * Mr + i]));
+      }
+      acc = cadd(acc, cmul(wc[w], v));
+    }
+    avg[e] = cadd(avg[e], acc);
+  }
+}
+
 }  // namespace
 
 struct Engine {
@@ -829,6 +871,91 @@ struct Engine {
     }
     md_energy_kernel<<<(W + 127) / 128, 128, 0, st>>>(md_ov, md_E, md_cic, ndet, W, E3, ovtmp);
     SFQ_LAUNCHED();
+    return SFQ_OK;
+  }
+
+  // --- MixedEstimator with the OneRDM and DiagonalTwoRDM observables -------------------------
+  cplx* rdm_buf = nullptr;  // Gf (W, nspin, Mr, Mr), one (nspin Mr Mr), two (nblk Mr Mr), wc, tot (W), ov (ndet W)
+  int rdm_nspin() const { return collinear ? 2 : 1; }
+  int rdm_nblk() const { return collinear ? 3 : (npol == 2 ? 1 : 2); }
+  // one (rdm_nspin, Mr, Mr) and the diagonal two-body RDM before folding (rdm_nblk, Mr, Mr), both divided
+  // by the total weight, on the host (MixedEstimator.hpp:37-147)
+  int measure_rdm(std::vector<cplx>& one, std::vector<cplx>& two) {
+    int rc;
+    if (mixed) return record_error(SFQ_ERR_UNSUPPORTED, "the mixed estimator's RDMs are measured in FP64 engines");
+    const int ns = rdm_nspin(), nb = rdm_nblk();
+    const long MM = (long)Mr * Mr;
+    const size_t elems = (size_t)W * ns * MM + ns * MM + nb * MM + 2 * (size_t)W + (size_t)ndet * W;
+    if (!rdm_buf) SFQ_CUDA_TRY(cudaMalloc(&rdm_buf, sizeof(cplx) * elems));
+    cplx* Gf = rdm_buf;
+    cplx* o1 = Gf + (size_t)W * ns * MM;
+    cplx* o2 = o1 + ns * MM;
+    cplx* wc = o2 + nb * MM;
+    cplx* tot = wc + W;
+    cplx* ovd = tot + W;
+    SFQ_CUDA_TRY(cudaMemsetAsync(o1, 0, sizeof(cplx) * (ns + nb) * MM, st));
+    const cplx* shift = props + (long)P_OVLP * W;
+    const cplx* weight = props + (long)P_WEIGHT * W;
+    std::vector<cplx> cic(ndet, mk(1.0, 0.0));
+    for (int d = 0; d < ndet && ndet > 1; ++d) cic[d] = cconj(ci_h[d]);
+    // the reference determinants' log overlaps, one determinant per spin (not doubled for CLOSED)
+    inv_cached = false;
+    for (int d = 0; d < ndet; ++d)
+      if ((rc = md_factor(d, SM, W, ovd + (long)d * W, false, 1.0))) return rc;
+    {
+      std::vector<cplx> tmp(cic);
+      cplx* dcic = nullptr;
+      SFQ_CUDA_TRY(cudaMallocAsync((void**)&dcic, sizeof(cplx) * ndet, st));
+      SFQ_CUDA_TRY(cudaMemcpyAsync(dcic, tmp.data(), sizeof(cplx) * ndet, cudaMemcpyHostToDevice, st));
+      rdm_tot_kernel<<<(W + 127) / 128, 128, 0, st>>>(ovd, dcic, shift, ndet, W, tot);
+      SFQ_LAUNCHED();
+      SFQ_CUDA_TRY(cudaFreeAsync(dcic, st));
+      SFQ_CUDA_TRY(cudaStreamSynchronize(st));  // tmp lives until the copy is done
+    }
+    for (int d = 0; d < ndet; ++d) {
+      if ((rc = md_factor(d, SM, W, ovd + (long)d * W, true, 1.0))) return rc;
+      if ((rc = ops::green_compact(T, SM, G, W, Mr, N, st))) return rc;
+      // the full G of each spin block: Gf[w][s] = PsiT_d[rows s]^T Gc[w][rows s] (density_matrix.hpp:580-600)
+      for (int s = 0; s < ns; ++s) {
+        const int r0 = collinear ? (s == 0 ? 0 : nup) : 0, r1 = collinear ? (s == 0 ? nup : N) : N;
+        if (r1 == r0) {  // an empty spin sector has a zero G
+          SFQ_CUDA_TRY(cudaMemset2DAsync(Gf + s * MM, sizeof(cplx) * ns * MM, 0, sizeof(cplx) * MM, W, st));
+          continue;
+        }
+        GemmDesc g;
+        g.M = Mr; g.N = Mr; g.K = r1 - r0; g.batch = W;
+        g.A = PsiT + d * det_elems() + (long)r0 * Mr; g.sAm = 1; g.sAk = Mr; g.sAb = 0; g.a_cplx = true;
+        g.B = G + (long)r0 * Mr; g.sBk = Mr; g.sBn = 1; g.sBb = det_elems(); g.b_cplx = true;
+        g.C = Gf + s * MM; g.sCm = Mr; g.sCn = 1; g.sCb = ns * MM;
+        if ((rc = gemm_f64(g, st))) return rc;
+      }
+      rdm_coeff_kernel<<<(W + 127) / 128, 128, 0, st>>>(ovd + (long)d * W, cic[d], shift, tot, weight, W, wc);
+      SFQ_LAUNCHED();
+      GemmDesc g;  // one[s,i,j] += sum_w wc[w] Gf[w,s,i,j] (onerdm.hpp:56-61)
+      g.M = 1; g.N = int(ns * MM); g.K = W; g.batch = 1;
+      g.A = wc; g.sAm = W; g.sAk = 1; g.a_cplx = true;
+      g.B = Gf; g.sBk = ns * MM; g.sBn = 1; g.b_cplx = true;
+      g.C = o1; g.sCm = ns * MM; g.sCn = 1; g.beta = mk(1.0, 0.0);
+      if ((rc = gemm_f64(g, st))) return rc;
+      const long tot2 = nb * MM;
+      rdm_two_kernel<<<int(std::min<long>((tot2 + 127) / 128, 1184)), 128, 0, st>>>(Gf, wc, W, ns, Mr, nb, o2);
+      SFQ_LAUNCHED();
+    }
+    one.resize(ns * MM);
+    two.resize(nb * MM);
+    std::vector<cplx> pw(W);
+    SFQ_CUDA_TRY(cudaMemcpyAsync(one.data(), o1, sizeof(cplx) * ns * MM, cudaMemcpyDeviceToHost, st));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(two.data(), o2, sizeof(cplx) * nb * MM, cudaMemcpyDeviceToHost, st));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(pw.data(), weight, sizeof(cplx) * W, cudaMemcpyDeviceToHost, st));
+    if ((rc = sync_checked())) return rc;
+    cplx den = mk(0.0, 0.0);
+    for (int w = 0; w < W; ++w) den = mk(den.x + pw[w].x, den.y + pw[w].y);  // MeasurementOutput's denominator
+    const double dd = den.x * den.x + den.y * den.y;
+    auto divide = [&](std::vector<cplx>& v) {
+      for (auto& z : v) z = mk((z.x * den.x + z.y * den.y) / dd, (z.y * den.x - z.x * den.y) / dd);
+    };
+    divide(one);
+    divide(two);
     return SFQ_OK;
   }
 
@@ -1913,6 +2040,7 @@ int sfq_engine_destroy(sfq_engine_t h) {
   if (e.Lp) cudaFree(e.Lp);
   if (e.Vp) cudaFree(e.Vp);
   if (e.h_pinned) cudaFreeHost(e.h_pinned);
+  if (e.rdm_buf) cudaFree(e.rdm_buf);
   if (e.st) cudaStreamDestroy(e.st);
   delete h;
   return SFQ_OK;
@@ -2025,6 +2153,35 @@ int sfq_engine_propagate_host(sfq_engine_t h, double Eshift, unsigned long long 
 int sfq_engine_orthogonalize(sfq_engine_t h) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
   return h->e.orthogonalize();
+}
+
+int sfq_engine_measure_rdm(sfq_engine_t h, void* one_rdm, void* diag_two_rdm) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  std::vector<cplx> one, two;
+  int rc;
+  if ((rc = e.measure_rdm(one, two))) return rc;
+  if (one_rdm) std::memcpy(one_rdm, one.data(), sizeof(cplx) * one.size());
+  if (!diag_two_rdm) return SFQ_OK;
+  // fold the i <-> j symmetry (Observables/diagonal_twordm.hpp:104-140)
+  cplx* out = static_cast<cplx*>(diag_two_rdm);
+  const int M = e.M, R = e.Mr;
+  auto at = [&](int b, int i, int j) { return two[((size_t)b * R + i) * R + j]; };
+  auto half = [](cplx a, cplx b) { return mk(0.5 * (a.x + b.x), 0.5 * (a.y + b.y)); };
+  long idx = 0;
+  if (e.npol == 1) {
+    for (int i = 0; i < M; ++i) {
+      for (int j = i + 1; j < M; ++j) out[idx++] = half(at(0, i, j), at(0, j, i));
+      for (int j = 0; j < M; ++j) out[idx++] = at(1, i, j);
+    }
+    if (e.collinear)
+      for (int i = 0; i < M; ++i)
+        for (int j = i + 1; j < M; ++j) out[idx++] = half(at(2, i, j), at(2, j, i));
+  } else {
+    for (int i = 0; i < 2 * M; ++i)
+      for (int j = i + 1; j < 2 * M; ++j) out[idx++] = half(at(0, i, j), at(0, j, i));
+  }
+  return SFQ_OK;
 }
 
 int sfq_engine_population_control_uniform(sfq_engine_t h, double r) {

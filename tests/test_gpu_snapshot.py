@@ -103,3 +103,31 @@ def test_comb_uniform_rejected_outside_unit_interval():
             eng.population_control(uniform=r)
         assert ex.value.code == 2
     eng.close()
+
+
+RDM_CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_uhf_noncollinear", "bh_rcasci_uhf_collinear",
+             "bh_rcasci_uhf_noncollinear", "li_rohf_collinear"]
+
+
+@pytest.mark.parametrize("case", RDM_CASES)
+def test_engine_reproduces_recorded_mixed_rdms(case):
+    """sfq_engine_measure_rdm every 2 steps of the replay: the mixed estimator's one-body and folded
+    diagonal two-body RDMs against the oracle's per measurement and the recorded means / errors."""
+    snap = snapshot(case)
+    st = snap["settings"]
+    eng = A.AfqmcEngine(_system(snap), st["nwalk"], dt=st["dt"], seed=0, precision=capi.PRECISION_FP64)
+    walker_rng = HostRandomGenerator(split_seed(st["seed"], 0, 0))
+    field_rng = HostRandomGenerator(split_seed(st["seed"], 0, 1))
+    _, series = eng.run_with_streams(st["steps"], eng.init(), field_rng.uniforms, lambda: walker_rng.uniforms(1)[0],
+                                     ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
+                                     equilibration_steps=st["equilibration_steps"],
+                                     measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"])
+    eng.close()
+    _, _, oracle_series = O.run_seeded(_oracle_hamiltonian(snap), st["nwalk"], st["dt"], st["steps"], st["seed"],
+                                       ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
+                                       measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"])
+    for k in ("MixedEstimator/OneRDM", "MixedEstimator/DiagonalTwoRDM"):
+        a, b = np.asarray(series[k]), np.asarray(oracle_series[k])
+        assert a.shape == b.shape
+        assert np.max(np.abs(a - b)) <= 1e-11 * max(1.0, float(np.max(np.abs(b)))), k
+        assert snapshot_match(series[k], snap["recorded"][k], O.rebinned_average) is not None, k
