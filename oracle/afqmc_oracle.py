@@ -249,6 +249,16 @@ class Hamiltonian:
     def propagate(self, SM, P1, V, order):
         return propagate(SM, P1, V, order)
 
+    def orthogonalize_ldet(self, SM):
+        """det_ops::orthogonalize(wset, ldet): the walkers' QR and the log det of R."""
+        return orthogonalize(SM)
+
+    def bp_full_green(self, A, SM):
+        """Full G (W, nspin, Mr, Mr) and log overlap between per-walker references A (W, n, Mr) in
+        the herm form and the walkers (the batched det_ops with T = Refs^H B, density_matrix.hpp:158-195)."""
+        G, ov = _batched_full_green(A, SM)
+        return G[:, None], ov
+
     def local_energy(self, SM):
         """NOMSD::Energy(wset, E, Ov), ndet = 1: (E (W, 3), log overlaps)."""
         G, ov = self.green(SM)
@@ -338,6 +348,20 @@ class CollinearHamiltonian(Hamiltonian):
         G_up, ov = mixed_density_matrix(self.PsiT_up, SM[:, :, :self.nup], compact=False)
         G_dn, ov = mixed_density_matrix(self.PsiT_dn, SM[:, :, self.nup:], compact=False, ovlp=ov)
         return np.stack([G_up, G_dn], axis=1), ov
+
+    def orthogonalize_ldet(self, SM):
+        up, ld = orthogonalize(SM[:, :, :self.nup])
+        if self.ndn:
+            dn, l2 = orthogonalize(SM[:, :, self.nup:])
+            ld = ld + l2
+        else:
+            dn = SM[:, :, self.nup:]
+        return np.concatenate([up, dn], axis=2), ld
+
+    def bp_full_green(self, A, SM):
+        Gu, ov = _batched_full_green(A[:, :self.nup], SM[:, :, :self.nup])
+        Gd, o2 = _batched_full_green(A[:, self.nup:], SM[:, :, self.nup:])
+        return np.stack([Gu, Gd], axis=1), ov + o2
 
     def orthogonalize(self, SM):
         up = orthogonalize(SM[:, :, :self.nup])[0]
@@ -729,9 +753,21 @@ class Walkers:
             setattr(c, f, getattr(self, f).copy())
         return c
 
+    # back propagation (WalkerSetBase::resize_bp, WalkerSetBase.cpp:331-385): the anchored walkers,
+    # the field ring and the weight-factor history travel with each walker
+    BP_FIELDS = ('SMN', 'fields', 'wfac')
+    nbp = 0
+
     def copy_walker(self, src, dst):
-        for f in self.FIELDS:
+        for f in self.FIELDS + (self.BP_FIELDS if self.nbp else ()):
             getattr(self, f)[dst] = getattr(self, f)[src]
+
+    def enable_back_propagation(self, nbp, nchol):
+        W = self.size()
+        self.nbp, self.nhist, self.hist_pos = nbp, 3 * nbp, 0
+        self.SMN = self.SM.copy()
+        self.fields = np.zeros((W, nbp, nchol), np.complex128)
+        self.wfac = np.ones((W, 3 * nbp), np.complex128)
 
 
 def walker_update(wset, dt, Eshift, energy_offset, new_ovlp, mf, hw,
@@ -741,6 +777,7 @@ def walker_update(wset, dt, Eshift, energy_offset, new_ovlp, mf, hw,
     nw = wset.size()
     hi = Eshift + upper_cutoff_scale * math.sqrt(2.0 / dt)
     lo = Eshift - lower_cutoff_scale * math.sqrt(2.0 / dt)
+    wfac = np.zeros(nw, np.complex128)  # the step's phase over the projection (WalkerSetUpdate.hpp:141-147)
     for i in range(nw):
         old_ovlp = complex(wset.ovlp[i])
         old_eloc = complex(wset.pseudo_eloc[i])
@@ -767,10 +804,13 @@ def walker_update(wset, dt, Eshift, energy_offset, new_ovlp, mf, hw,
                 eloc = complex(min(max(eloc.real, lo), hi), eloc.imag)
             eloc_eff = eloc if hybrid else 0.5 * (eloc + old_eloc)
             w = np.exp(-dt * (eloc_eff - Eshift))
+            wfac[i] = (w / abs(w) / scale) if abs(scale) > np.finfo(np.float64).tiny else 0.0
             wset.weight[i] *= (scale * w) if free_projection else (scale * abs(w))
             wset.phase[i] *= w / abs(w)
         wset.pseudo_eloc[i] = eloc
         wset.ovlp[i] = new_ovlp[i]
+    if wset.nbp:
+        wset.wfac[:, wset.hist_pos] = wfac
     if not hybrid:
         wset.e1[:] = new_energies[:, 0]
         wset.exx[:] = new_energies[:, 1]
@@ -886,12 +926,16 @@ class Propagator:
             uniforms = philox.uniforms(self.seed, philox.STREAM_FIELDS, step, W, ham.Nc)
         X, HW = assemble_X(vb, self.vmf, uniforms, self.vbias_bound)
         mf = meanfield_factor(X, self.vmf)
+        if wset.nbp:
+            wset.fields[:, wset.hist_pos % wset.nbp] = X  # storeFields (AFQMCBasePropagator.cpp:342-344)
         V = ham.vHS(X, self.dt)
         wset.SM = ham.propagate(wset.SM, self.P1, V, self.order)
         new_ov = ham.log_overlap(wset.SM)
         walker_update(wset, self.dt, Eshift, ham.E0, new_ov, mf, HW, self.lower, self.upper)
         tp = W if target_population is None else target_population
         bound_walker_weights(wset, tp, self.wfloor, self.wfrac)
+        if wset.nbp:
+            wset.hist_pos = (wset.hist_pos + 1) % wset.nhist
         return dict(G=G, vbias=vb, X=X, HW=HW, mf=mf, vHS=V, new_ovlp=new_ov)
 
     def orthogonalize(self, wset):
@@ -989,32 +1033,36 @@ def _references(ham):
     return [ham], np.array([getattr(ham, "ci", 1.0)], np.complex128)
 
 
-def measure_mixed_rdms(ham, wset):
-    """MixedEstimator::measure with the OneRDM and DiagonalTwoRDM observables (MixedEstimator.hpp:37-147,
-    Observables/onerdm.hpp:42-75, Observables/diagonal_twordm.hpp:36-140), one rank.
+def _batched_full_green(A, B):
+    """Per walker: T = A B (A (W, n, Mr) in the herm form), log det, and the full G = A^T T^-T B^T;
+    an empty sector gives G = 0 and log det 0."""
+    W, Mr, n = B.shape
+    if n == 0:
+        return np.zeros((W, Mr, Mr), np.complex128), np.zeros(W, np.complex128)
+    T = A @ B
+    ov = np.zeros(W, np.complex128)
+    Tinv = np.empty_like(T)
+    for w in range(W):
+        ov[w], Tinv[w] = lu_logdet_inverse(T[w])
+    Gc = np.transpose(Tinv, (0, 2, 1)) @ np.transpose(B, (0, 2, 1))
+    return np.transpose(A, (0, 2, 1)) @ Gc, ov
 
-    Per reference determinant d the full mixed G_d (W, nspin, Mr, Mr) and its log overlap (one
-    determinant per spin, not doubled for CLOSED) give refCoeff_d = conj(c_d) exp(ov_d - OVLP) /
-    sum_d' conj(c_d') exp(ov_d' - OVLP); with weightedCoeff = weight * refCoeff_d,
-      OneRDM[s,i,j]  += sum_w weightedCoeff[w] G_d[w,s,i,j]
-      2RDM (aaaa)_s  += sum_w wc G[w,s,i,i] G[w,s,j,j] - wc G[w,s,i,j] G[w,s,j,i]
-      2RDM (aabb)    += sum_w wc G[w,0,i,i] G[w,dn,j,j]   (CLOSED, COLLINEAR; dn = 0 for CLOSED)
-    each divided by sum_w weight, the 2RDM folded over i <-> j (compress, :104-140)."""
-    dets, ci = _references(ham)
-    w = wset.weight
-    shift = wset.ovlp
-    parts = [d.full_green(wset.SM) for d in dets]
-    e = [np.conj(ci[k]) * np.exp(ov - shift) for k, (_, ov) in enumerate(parts)]
-    tot = np.sum(e, axis=0)
-    wt = "NONCOLLINEAR" if isinstance(dets[0], NoncollinearHamiltonian) else (
-        "COLLINEAR" if isinstance(dets[0], CollinearHamiltonian) else "CLOSED")
-    G0 = parts[0][0]
-    nspin, Mr = G0.shape[1], G0.shape[2]
+
+def _walker_kind(det):
+    if isinstance(det, NoncollinearHamiltonian):
+        return "NONCOLLINEAR"
+    return "COLLINEAR" if isinstance(det, CollinearHamiltonian) else "CLOSED"
+
+
+def _rdm_reduce(parts, coeffs, w, wt, M):
+    """OneRDM and the folded DiagonalTwoRDM (Observables/onerdm.hpp:42-75, diagonal_twordm.hpp:36-140)
+    from per-reference full G's and walker coefficients, divided by sum_w w."""
+    nspin, Mr = parts[0].shape[1], parts[0].shape[2]
     nblk = {"COLLINEAR": 3, "CLOSED": 2}.get(wt, 1)
     one = np.zeros((nspin, Mr, Mr), np.complex128)
     avg = np.zeros((nblk, Mr, Mr), np.complex128)
-    for k, (G, _) in enumerate(parts):
-        wc = w * e[k] / tot
+    for G, c in zip(parts, coeffs):
+        wc = w * c
         one += np.einsum('w,wsij->sij', wc, G)
         dg = np.einsum('wsii->wsi', G)
         for sp in range(nspin):
@@ -1024,7 +1072,6 @@ def measure_mixed_rdms(ham, wset):
             avg[1] += np.einsum('w,wi,wj->ij', wc, dg[:, 0], dg[:, 1 if wt == "COLLINEAR" else 0])
     den = np.sum(w)
     one, avg = one / den, avg / den
-    M = ham.M
     out = []
     if wt != "NONCOLLINEAR":
         for i in range(M):
@@ -1036,15 +1083,103 @@ def measure_mixed_rdms(ham, wset):
     else:
         for i in range(2 * M):
             out += [(avg[0, i, j] + avg[0, j, i]) / 2 for j in range(i + 1, 2 * M)]
-    return {"MixedEstimator/OneRDM": one, "MixedEstimator/DiagonalTwoRDM": np.array(out, np.complex128)}
+    return one, np.array(out, np.complex128)
+
+
+class BackPropEstimator:
+    """BackPropEstimator with the OneRDM and DiagonalTwoRDM observables (BackPropEstimator.hpp:36-275,
+    AFQMCBasePropagator::BackPropagate :404-526), one rank.
+
+    The walker set keeps, per walker, the anchored Slater matrices (SMN), a ring of the last nbp
+    steps' fields and the history of the steps' weight factors (phase over projection).  When
+    `bp` = step - anchor is one of the propagation lengths, every walker's copy of the trial's
+    references is propagated backwards through the stored fields with the adjoint propagator
+    (P1^H, exp(-i V^H), propagate.hpp:41-75 with TA = 'H'), orthogonalized every ortho_interval
+    steps and at the end (the QR log dets summed in logdetR, shifted by their mean over references);
+    the walker weights are restored by the last bp weight factors, and the RDMs are measured between
+    the propagated references and the anchored walkers with coefficients conj(c_d) exp(ov_d +
+    conj(logdetR_d)) / sum (CLOSED: both doubled).  The anchor moves to the current step once bp
+    reaches the longest length."""
+
+    def __init__(self, ham, prop, wset, steps=(2,), ortho_interval=10, path_restoration=True):
+        self.ham, self.prop = ham, prop
+        self.steps = sorted(int(k) for k in steps)
+        self.ortho = int(ortho_interval)
+        self.path_restoration = path_restoration
+        wset.enable_back_propagation(self.steps[-1], ham.Nc)
+        self.anchor(wset, -1)
+
+    def anchor(self, wset, step):
+        wset.SMN = wset.SM.copy()
+        self.bp_pos = step
+
+    def measure(self, wset, step):
+        bp = step - self.bp_pos
+        out = self.back_propagate(wset, bp) if bp in self.steps else {}
+        if bp >= self.steps[-1]:
+            self.anchor(wset, step)
+        return out
+
+    def back_propagate(self, wset, nb):
+        ham, prop = self.ham, self.prop
+        dets, ci = _references(ham)
+        W = wset.size()
+        refs = [np.ascontiguousarray(np.broadcast_to(d.trial_walker(), (W,) + d.trial_walker().shape))
+                for d in dets]
+        logdetR = np.zeros((W, len(dets)), np.complex128)
+        P1h = np.conj(prop.P1.T)
+        slot = wset.hist_pos % wset.nbp
+        for ni in range(nb - 1, -1, -1):
+            slot = wset.nbp - 1 if slot == 0 else slot - 1
+            V = ham.vHS(wset.fields[:, slot], prop.dt)
+            Vadj = -np.conj(np.transpose(V, (0, 2, 1)))  # exp(i Vadj) = exp(-i V^H)
+            for r in range(len(dets)):
+                S = ham.propagate(refs[r], P1h, Vadj, prop.order)
+                if ni == 0 or ni % self.ortho == 0:
+                    S, ld = dets[0].orthogonalize_ldet(S)
+                    logdetR[:, r] += ld
+                refs[r] = S
+        logdetR -= (logdetR.sum(axis=1) / len(dets))[:, None]
+        weights = wset.weight.copy()
+        if self.path_restoration:
+            hpos = wset.hist_pos
+            for _ in range(nb):
+                hpos = wset.nhist - 1 if hpos == 0 else hpos - 1
+                weights = weights * wset.wfac[:, hpos]
+        f = dets[0].ov_factor
+        parts, es = [], []
+        for d, det in enumerate(dets):
+            A = np.conj(np.transpose(refs[d], (0, 2, 1)))  # T = Refs^H SMN
+            G, ov = det.bp_full_green(A, wset.SMN)
+            parts.append(G)
+            es.append(np.conj(ci[d]) * np.exp(f * ov + np.conj(f * logdetR[:, d])))
+        tot = np.sum(es, axis=0)
+        one, two = _rdm_reduce(parts, [e / tot for e in es], weights, _walker_kind(dets[0]), ham.M)
+        pre = f"BackPropEstimator/Steps={nb}"
+        return {f"{pre}/OneRDM": one, f"{pre}/DiagonalTwoRDM": two}
+
+
+def measure_mixed_rdms(ham, wset):
+    """MixedEstimator::measure with the OneRDM and DiagonalTwoRDM observables (MixedEstimator.hpp:37-147),
+    one rank: per reference determinant d the full mixed G_d and its log overlap (one determinant per
+    spin, not doubled for CLOSED) give refCoeff_d = conj(c_d) exp(ov_d - OVLP) / sum_d' (...); the
+    RDMs are the walker averages with weight * refCoeff_d (_rdm_reduce)."""
+    dets, ci = _references(ham)
+    parts = [d.full_green(wset.SM) for d in dets]
+    e = [np.conj(ci[k]) * np.exp(ov - wset.ovlp) for k, (_, ov) in enumerate(parts)]
+    tot = np.sum(e, axis=0)
+    one, two = _rdm_reduce([G for G, _ in parts], [x / tot for x in e], wset.weight, _walker_kind(dets[0]), ham.M)
+    return {"MixedEstimator/OneRDM": one, "MixedEstimator/DiagonalTwoRDM": two}
 
 
 def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, measure_interval=10,
-               equilibration_steps=0, relax=None, rank=0, mixed_interval=None, **prop_args):
+               equilibration_steps=0, relax=None, rank=0, mixed_interval=None, bp_steps=None, bp_ortho_interval=None,
+               **prop_args):
     """execute_simulation + run_afqmc for one stage with HostRandomGenerator streams: walkers from
     the trial (NOMSD::initial_guess), Energy + seedPseudoEnergy, Eshift = averageEnergy, then the
     step loop.  Fields come from stream 1 (nwalk x nchol uniforms per step), the comb from stream 0.
-    With mixed_interval the mixed estimator's one-body and diagonal two-body RDMs are measured too.
+    With mixed_interval the mixed estimator's one-body and diagonal two-body RDMs are measured too,
+    with bp_steps (back propagation lengths) the back-propagated ones.
     Returns (initial Eshift, final Eshift, {observable: list of bins})."""
     from .mt19937 import HostRandomGenerator, split_seed
     walker_rng = HostRandomGenerator(split_seed(seed, rank, 0))
@@ -1054,6 +1189,7 @@ def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, 
     Eshift = init_walkers(ham, wset)
     E_init = Eshift
     prop = Propagator(ham, dt, **prop_args)
+    bp = BackPropEstimator(ham, prop, wset, bp_steps, bp_ortho_interval or ortho_interval) if bp_steps else None
     if relax is None:
         relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
     series = {}
@@ -1070,6 +1206,9 @@ def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, 
                     series.setdefault(k, []).append(v)
             if mixed_interval and step % mixed_interval == 0:
                 for k, v in measure_mixed_rdms(ham, wset).items():
+                    series.setdefault(k, []).append(v)
+            if bp is not None:
+                for k, v in bp.measure(wset, step).items():
                     series.setdefault(k, []).append(v)
         else:
             Eshift += relax * (average_pseudo_energy(wset, dt) - Eshift)

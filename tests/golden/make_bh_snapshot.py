@@ -48,8 +48,16 @@ def rdm_records(res, ex, out):
     if not est or "mixed" not in est:
         return
     out["mixed_interval"] = np.int64(est["mixed"]["measure_interval"])
-    for k in RDM_OBSERVABLES:
-        key = k.replace("/", "_")
+    obs = list(RDM_OBSERVABLES)
+    bp = est.get("backprop")
+    if bp:
+        steps = [int(k) for k in bp["propagation_steps"]]
+        out["bp_steps"] = np.asarray(steps, np.int64)
+        out["bp_ortho_interval"] = np.int64(bp.get("walker_ortho_interval", ex["walker_ortho_interval"]))
+        out["bp_path_restoration"] = np.int64(bool(bp.get("path_restoration", True)))
+        obs += [f"BackPropEstimator/Steps={k}/{o}" for k in steps for o in ("OneRDM", "DiagonalTwoRDM")]
+    for k in obs:
+        key = k.replace("/", "_").replace("=", "")
         out[f"mean_{key}"] = np.asarray(res[f"measurements/Stage0/{k}/mean"])
         out[f"error_{key}"] = np.asarray(res[f"measurements/Stage0/{k}/error"])
 

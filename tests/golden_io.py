@@ -33,12 +33,17 @@ def snapshot(name):
     The BH collinear case shares the BH Hamiltonian tensors of the closed case's file."""
     z = np.load(os.path.join(HERE, f"{name}_snapshot.npz"))
     rec = {k: (z[f"mean_{k}"][()], z[f"error_{k}"][()]) for k in SNAPSHOT_OBSERVABLES}
-    for k in ("MixedEstimator/OneRDM", "MixedEstimator/DiagonalTwoRDM"):
-        key = k.replace("/", "_")
+    rdm = ["MixedEstimator/OneRDM", "MixedEstimator/DiagonalTwoRDM"]
+    bp_steps = [int(k) for k in z["bp_steps"]] if "bp_steps" in z else []
+    rdm += [f"BackPropEstimator/Steps={k}/{o}" for k in bp_steps for o in ("OneRDM", "DiagonalTwoRDM")]
+    for k in rdm:
+        key = k.replace("/", "_").replace("=", "")
         if f"mean_{key}" in z:
             rec[k] = (z[f"mean_{key}"], z[f"error_{key}"])
     out = dict(settings=json.loads(str(z["settings"])), recorded=rec,
-               mixed_interval=int(z["mixed_interval"]) if "mixed_interval" in z else None)
+               mixed_interval=int(z["mixed_interval"]) if "mixed_interval" in z else None,
+               bp_steps=bp_steps or None,
+               bp_ortho_interval=int(z["bp_ortho_interval"]) if "bp_ortho_interval" in z else None)
     if "ci_dets" in z:  # multi-determinant trial: per-determinant orbitals and coefficients
         out.update(ci_dets=z["ci_dets"], PsiT_dets=z["PsiT_dets"])
         if "PsiT_up_dets" in z:

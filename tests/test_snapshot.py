@@ -134,15 +134,19 @@ RDM_CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_uhf_noncollinear", "bh_rca
 
 
 @pytest.mark.parametrize("case", RDM_CASES)
-def test_oracle_reproduces_recorded_mixed_rdms(case):
-    """The mixed estimator's one-body and diagonal two-body RDMs the reference recorded with the
-    back-propagation cases (every 2 steps): CLOSED, COLLINEAR, NONCOLLINEAR, a 34-determinant trial."""
+def test_oracle_reproduces_recorded_rdms(case):
+    """The mixed (every 2 steps) and back-propagated (2 steps, path restoration) one-body and diagonal
+    two-body RDMs the reference recorded with its back-propagation cases: CLOSED, COLLINEAR,
+    NONCOLLINEAR, a 34-determinant trial, Li."""
     snap = snapshot(case)
     st = snap["settings"]
     _, _, series = O.run_seeded(oracle_hamiltonian(snap), st["nwalk"], st["dt"], st["steps"], st["seed"],
                                 ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
-                                measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"])
-    for k in ("MixedEstimator/OneRDM", "MixedEstimator/DiagonalTwoRDM"):
-        assert len(series[k]) == st["steps"] // snap["mixed_interval"]
+                                measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"],
+                                bp_steps=snap["bp_steps"], bp_ortho_interval=snap["bp_ortho_interval"])
+    rdms = [k for k in snap["recorded"] if k.startswith(("MixedEstimator", "BackPropEstimator"))]
+    assert len(rdms) == 4
+    for k in rdms:
+        assert len(series[k]) == st["steps"] // 2
         assert np.asarray(series[k]).shape[1:] == snap["recorded"][k][0].shape
         assert snapshot_match(series[k], snap["recorded"][k], O.rebinned_average) is not None, k
