@@ -263,6 +263,21 @@ int sfq_engine_population_control(sfq_engine_t e, unsigned long long call);
  * folded diagonal two-body RDM, nmo (2 nmo - 1) complex values (CLOSED: nmo (2 nmo - 1) - nmo (nmo - 1) / 2).
  * Both divided by the total weight, as recorded per measurement; host pointers, either may be NULL. */
 int sfq_engine_measure_rdm(sfq_engine_t e, void* one_rdm, void* diag_two_rdm);
+
+/* Back propagation (BackPropEstimator.hpp, AFQMCBasePropagator.cpp:404-526), FP64 engines.
+ * enable: every later step keeps, per walker, its fields in a ring of nbp slots and its weight factor
+ * (the step's phase over its projection, WalkerSetUpdate.hpp:141-147) in a history of 3 nbp slots,
+ * copied with the walkers by population control (resize_bp); the anchored walkers start as the current
+ * ones.  anchor: the anchored walkers become the current ones (setAnchor).  measure_bp_rdm: the trial's
+ * references propagated backwards over the last nsteps <= nbp steps (adjoint propagator, QR every
+ * ortho_interval steps and at the end), the weights restored by the last nsteps weight factors when
+ * path_restoration, and the OneRDM / DiagonalTwoRDM between the references and the anchored walkers,
+ * shaped as sfq_engine_measure_rdm's.  The caller keeps the estimator's schedule (measure at anchor +
+ * nsteps, then re-anchor).  Device-resident blocks and groups refuse an engine with back propagation. */
+int sfq_engine_enable_back_propagation(sfq_engine_t e, int nbp);
+int sfq_engine_bp_anchor(sfq_engine_t e);
+int sfq_engine_measure_bp_rdm(sfq_engine_t e, int nsteps, int ortho_interval, int path_restoration, void* one_rdm,
+                              void* diag_two_rdm);
 /* the same with the comb's uniform r in [0, 1) from the caller: the draw comb takes from the walker set's
  * generator (population_control.hpp:41-42, HostRandomGenerator::sampleUniformFields), so a caller that
  * owns the reference's stream replays its population control exactly */

@@ -266,31 +266,51 @@ class AfqmcEngine:
         keys = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy", "TotalWeight")
         return {k: complex(o[2 * i], o[2 * i + 1]) for i, k in enumerate(keys)}
 
-    def measure_mixed_rdms(self):
-        """MixedEstimator's OneRDM and DiagonalTwoRDM of the current walkers (sfq_engine_measure_rdm)."""
+    def _rdm_buffers(self):
         nspin = 2 if self.params.walker_type == capi.WALKER_COLLINEAR else 1
         M = self.M
-        if self.params.walker_type == capi.WALKER_CLOSED:
-            n2 = M * (2 * M - 1) - M * (M - 1) // 2
-        else:
-            n2 = M * (2 * M - 1)
-        one = np.empty((nspin, self.Mr, self.Mr), np.complex128)
-        two = np.empty(n2, np.complex128)
+        n2 = M * (2 * M - 1) - (M * (M - 1) // 2 if self.params.walker_type == capi.WALKER_CLOSED else 0)
+        return np.empty((nspin, self.Mr, self.Mr), np.complex128), np.empty(n2, np.complex128)
+
+    def measure_mixed_rdms(self):
+        """MixedEstimator's OneRDM and DiagonalTwoRDM of the current walkers (sfq_engine_measure_rdm)."""
+        one, two = self._rdm_buffers()
         check(lib().sfq_engine_measure_rdm(self.h, one.ctypes.data, two.ctypes.data))
         return {"MixedEstimator/OneRDM": one, "MixedEstimator/DiagonalTwoRDM": two}
 
+    def enable_back_propagation(self, nbp):
+        """Keep the fields and weight factors of the last nbp steps per walker (resize_bp)."""
+        check(lib().sfq_engine_enable_back_propagation(self.h, int(nbp)))
+
+    def bp_anchor(self):
+        check(lib().sfq_engine_bp_anchor(self.h))
+
+    def measure_bp_rdms(self, nsteps, ortho_interval=10, path_restoration=True):
+        """BackPropEstimator's OneRDM and DiagonalTwoRDM over the last nsteps (sfq_engine_measure_bp_rdm)."""
+        one, two = self._rdm_buffers()
+        check(lib().sfq_engine_measure_bp_rdm(self.h, int(nsteps), int(ortho_interval), int(bool(path_restoration)),
+                                              one.ctypes.data, two.ctypes.data))
+        pre = f"BackPropEstimator/Steps={int(nsteps)}"
+        return {f"{pre}/OneRDM": one, f"{pre}/DiagonalTwoRDM": two}
+
     def run_with_streams(self, steps, Eshift, field_uniforms, comb_uniform, ortho_interval=10, pop_interval=10,
-                         equilibration_steps=100, measure_interval=10, relax=None, step0=0, mixed_interval=None):
+                         equilibration_steps=100, measure_interval=10, relax=None, step0=0, mixed_interval=None,
+                         bp_steps=None, bp_ortho_interval=None, path_restoration=True):
         """run_afqmc's step loop (run_afqmc.cpp:69-104) with the caller's random streams at the
         reference's two injection points: field_uniforms(n) returns the n = nwalk * nchol uniforms
         of a step (walker-major, assemble_X's sampleUniformFields) and comb_uniform() the comb's
         uniform (population_control.hpp:41-42).  Given the reference's own generators it replays
         a reference run.  Every measurement records EnergyEstimator::measure's observables
-        (EnergyEstimator.h:51-100), and every mixed_interval steps the mixed estimator's RDMs.
+        (EnergyEstimator.h:51-100), every mixed_interval steps the mixed estimator's RDMs, and with
+        bp_steps the back-propagated ones.
         Returns (Eshift, {observable: list of bins})."""
         if relax is None:
             relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
         series = {}
+        if bp_steps:  # BackPropEstimator's schedule (BackPropEstimator.hpp:150-168): anchored at step0 - 1
+            bp_steps = sorted(int(k) for k in bp_steps)
+            self.enable_back_propagation(bp_steps[-1])
+            bp_pos = step0 - 1
         for step in range(step0, step0 + steps):
             u = np.ascontiguousarray(np.asarray(field_uniforms(self.W * self.Nc), np.float64).reshape(self.W, self.Nc))
             self.propagate_host(Eshift, step, uniforms_host=u)
@@ -313,6 +333,14 @@ class AfqmcEngine:
                 if mixed_interval and step % mixed_interval == 0:
                     for k, v in self.measure_mixed_rdms().items():
                         series.setdefault(k, []).append(v)
+                if bp_steps:
+                    if step - bp_pos in bp_steps:
+                        for k, v in self.measure_bp_rdms(step - bp_pos, bp_ortho_interval or ortho_interval,
+                                                         path_restoration).items():
+                            series.setdefault(k, []).append(v)
+                    if step - bp_pos >= bp_steps[-1]:
+                        self.bp_anchor()
+                        bp_pos = step
             else:
                 Eshift += relax * (self.averages()[0] - Eshift)
         return Eshift, series

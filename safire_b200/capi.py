@@ -116,6 +116,9 @@ _SIGS = {
     "sfq_engine_population_control": ([_VP, _U64], _I),
     "sfq_engine_population_control_uniform": ([_VP, ctypes.c_double], _I),
     "sfq_engine_measure_rdm": ([_VP, _VP, _VP], _I),
+    "sfq_engine_enable_back_propagation": ([_VP, _I], _I),
+    "sfq_engine_bp_anchor": ([_VP], _I),
+    "sfq_engine_measure_bp_rdm": ([_VP, _I, _I, _I, _VP, _VP], _I),
     "sfq_engine_averages": ([_VP, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)], _I),
     "sfq_engine_measure": ([_VP, _VP], _I),
     "sfq_engine_run": ([_VP, ctypes.POINTER(RunParams), ctypes.POINTER(_D), _VP, _I, ctypes.POINTER(_I)], _I),

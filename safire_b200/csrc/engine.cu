@@ -210,13 +210,58 @@ __global__ void md_energy_kernel(const cplx* ov, const cplx* Ed, const cplx* cic
   Ov[w] = cadd(clog_(deno), om);
 }
 
+// ---- back propagation (AFQMCBasePropagator.cpp:404-526, BackPropEstimator.hpp:170-230) -----
+// refs[d][w] = PsiT_d^H for every walker (the references BackPropagate starts from)
+__global__ void bp_init_refs_kernel(const cplx* PsiT, int ndet, int W, int Mr, int N, cplx* refs) {
+  const long per = (long)Mr * N, total = (long)ndet * W * per;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+    const long d = e / (W * per), r = e % per;
+    const long i = r / N, a = r % N;
+    refs[e] = cconj(PsiT[d * per + a * Mr + i]);
+  }
+}
+// V[w] <- -V[w]^H in place: exp(i (-V^H)) = exp(-i V^H), the adjoint Taylor propagator (propagate.hpp:56-57)
+__global__ void neg_adjoint_kernel(cplx* V, int M) {
+  cplx* Vw = V + (long)blockIdx.y * M * M;
+  const long npairs = (long)M * (M + 1) / 2;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < npairs; e += (long)gridDim.x * blockDim.x) {
+    int i = int((sqrt(8.0 * e + 1.0) - 1.0) / 2.0);
+    while ((long)i * (i + 1) / 2 > e) --i;
+    while ((long)(i + 1) * (i + 2) / 2 <= e) ++i;
+    const int j = int(e - (long)i * (i + 1) / 2);  // j <= i
+    const cplx a = Vw[(long)i * M + j], b = Vw[(long)j * M + i];
+    Vw[(long)i * M + j] = mk(-b.x, b.y);
+    Vw[(long)j * M + i] = mk(-a.x, a.y);
+  }
+}
+// logdetR[d][w] -= mean over d (BackPropEstimator.hpp:183-186)
+__global__ void bp_shift_kernel(cplx* ld, int ndet, int W) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= W) return;
+  cplx s = mk(0.0, 0.0);
+  for (int d = 0; d < ndet; ++d) s = cadd(s, ld[(long)d * W + w]);
+  s = cscale(s, 1.0 / ndet);
+  for (int d = 0; d < ndet; ++d) ld[(long)d * W + w] = csub(ld[(long)d * W + w], s);
+}
+// wt[w] *= wfac[w * stride]: one step of path restoration (BackPropEstimator.hpp:192-206)
+__global__ void bp_restore_kernel(cplx* wt, const cplx* wfac, long stride, int W) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < W) wt[w] = cmul(wt[w], wfac[(long)w * stride]);
+}
+// ov[w] = f ov[w] + conj(f ld[w]) (constructBPMeasurementInputs: CLOSED doubles both)
+__global__ void bp_ov_kernel(cplx* ov, const cplx* ld, double f, int W) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < W) ov[w] = cadd(cscale(ov[w], f), cconj(cscale(ld[w], f)));
+}
+
 // ---- the mixed estimator's RDMs (MixedEstimator.hpp:37-147) ---------------------------------
 // tot[w] = sum_d conj(ci_d) exp(ov_d[w] - shift[w]) over the reference determinants
 __global__ void rdm_tot_kernel(const cplx* ov, const cplx* cic, const cplx* shift, int ndet, int W, cplx* tot) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= W) return;
   cplx s = mk(0.0, 0.0);
-  for (int d = 0; d < ndet; ++d) s = cadd(s, cmul(cic[d], cexp_(csub(ov[(long)d * W + w], shift[w]))));
+  const cplx sh = shift ? shift[w] : mk(0.0, 0.0);
+  for (int d = 0; d < ndet; ++d) s = cadd(s, cmul(cic[d], cexp_(csub(ov[(long)d * W + w], sh))));
   tot[w] = s;
 }
 // wc[w] = weight[w] conj(ci_d) exp(ov_d[w] - shift[w]) / tot[w]
@@ -224,7 +269,8 @@ __global__ void rdm_coeff_kernel(const cplx* ov, cplx cic, const cplx* shift, co
                                  int W, cplx* wc) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= W) return;
-  wc[w] = cmul(weight[w], cdiv(cmul(cic, cexp_(csub(ov[w], shift[w]))), tot[w]));
+  const cplx sh = shift ? shift[w] : mk(0.0, 0.0);
+  wc[w] = cmul(weight[w], cdiv(cmul(cic, cexp_(csub(ov[w], sh))), tot[w]));
 }
 // diagonal two-body RDM blocks (Observables/diagonal_twordm.hpp:60-80), avg[b][i][j] += sum_w wc[w] (...):
 // b = 2 s: G[s,i,i] G[s,j,j] - G[s,i,j] G[s,j,i] for each spin s; b = 1 (CLOSED, COLLINEAR):
@@ -874,6 +920,84 @@ struct Engine {
     return SFQ_OK;
   }
 
+  // --- back propagation (WalkerSetBase::resize_bp, BackPropEstimator) ---------------------------
+  // per walker: the anchored walkers, a ring of the last nbp steps' fields (slot hist_pos % nbp),
+  // the weight factors of the last 3 nbp steps (slot hist_pos); all travel with population control
+  int nbp = 0, nhist = 0, hist_pos = 0;
+  cplx *bp_SMN = nullptr, *bp_fields = nullptr, *bp_wfac = nullptr;
+  cplx *bp_refs = nullptr, *bp_ldet = nullptr, *bp_wt = nullptr;
+  int enable_bp(int n) {
+    if (mixed) return record_error(SFQ_ERR_UNSUPPORTED, "back propagation runs in FP64 engines");
+    if (n <= 0) return record_error(SFQ_ERR_ARG, "back propagation needs nbp > 0");
+    if (nbp) return record_error(SFQ_ERR_ARG, "back propagation is already enabled (nbp = %d)", nbp);
+    nbp = n;
+    nhist = 3 * n;
+    hist_pos = 0;
+    const long RN = det_elems();
+    SFQ_CUDA_TRY(cudaMalloc(&bp_SMN, sizeof(cplx) * W * RN));
+    SFQ_CUDA_TRY(cudaMalloc(&bp_fields, sizeof(cplx) * (size_t)W * nbp * Nc));
+    SFQ_CUDA_TRY(cudaMalloc(&bp_wfac, sizeof(cplx) * (size_t)W * nhist));
+    SFQ_CUDA_TRY(cudaMalloc(&bp_refs, sizeof(cplx) * (size_t)ndet * W * RN));
+    SFQ_CUDA_TRY(cudaMalloc(&bp_ldet, sizeof(cplx) * (size_t)ndet * W));
+    SFQ_CUDA_TRY(cudaMalloc(&bp_wt, sizeof(cplx) * W));
+    SFQ_CUDA_TRY(cudaMemsetAsync(bp_fields, 0, sizeof(cplx) * (size_t)W * nbp * Nc, st));
+    int rc;
+    if ((rc = fill_cplx(bp_wfac, (long)W * nhist, mk(1.0, 0.0), st))) return rc;
+    return bp_anchor();
+  }
+  int bp_anchor() {
+    if (!nbp) return record_error(SFQ_ERR_ARG, "back propagation is not enabled");
+    SFQ_CUDA_TRY(cudaMemcpyAsync(bp_SMN, SM, sizeof(cplx) * W * det_elems(), cudaMemcpyDeviceToDevice, st));
+    return sync_checked();
+  }
+  // BackPropagate over the last nb steps and the BackPropEstimator's RDMs (one (nspin, Mr, Mr), two
+  // before folding (nblk, Mr, Mr)), divided by the sum of the restored weights
+  int measure_bp(int nb, int ortho, bool restore, std::vector<cplx>& one, std::vector<cplx>& two) {
+    int rc;
+    if (!nbp) return record_error(SFQ_ERR_ARG, "back propagation is not enabled");
+    if (nb <= 0 || nb > nbp || ortho <= 0) return record_error(SFQ_ERR_ARG, "back propagation over %d steps (ring %d)", nb, nbp);
+    const long RN = det_elems(), MM = (long)M * M;
+    inv_cached = false;
+    bp_init_refs_kernel<<<1184, 256, 0, st>>>(PsiT, ndet, W, Mr, N, bp_refs);
+    SFQ_LAUNCHED();
+    SFQ_CUDA_TRY(cudaMemsetAsync(bp_ldet, 0, sizeof(cplx) * (size_t)ndet * W, st));
+    int slot = hist_pos % nbp;
+    for (int ni = nb - 1; ni >= 0; --ni) {
+      slot = slot == 0 ? nbp - 1 : slot - 1;
+      SFQ_CUDA_TRY(cudaMemcpy2DAsync(X, sizeof(cplx) * Nc, bp_fields + (long)slot * Nc, sizeof(cplx) * nbp * Nc,
+                                     sizeof(cplx) * Nc, W, cudaMemcpyDeviceToDevice, st));
+      if (sym) {
+        if ((rc = ops::vhs_rows(Lp, P, X, Vp, W, Nc, std::sqrt(p.dt), st))) return rc;
+        if ((rc = unpack_symmetric(Vp, W, M, V, st))) return rc;
+      } else if ((rc = ops::vhs(Likn, X, V, W, M, Nc, std::sqrt(p.dt), st))) {
+        return rc;
+      }
+      neg_adjoint_kernel<<<dim3(md_grid(MM / 2 + M), W), 256, 0, st>>>(V, M);
+      SFQ_LAUNCHED();
+      for (int d = 0; d < ndet; ++d) {
+        cplx* S = bp_refs + (long)d * W * RN;
+        // P1 is real symmetric: P1^H = P1 (propagate.hpp:258-297 with TA = 'H')
+        if ((rc = ops::propagate(S, P1, false, V, W, M, N, p.taylor_order, TMN, T1, T2, st, npol))) return rc;
+        if (ni == 0 || ni % ortho == 0)
+          if ((rc = ops::orthogonalize_logdet(S, SM2, T, Tchunk, status, bp_ldet + (long)d * W, W, Mr, N, st,
+                                              spin_split())))
+            return rc;
+      }
+    }
+    bp_shift_kernel<<<(W + 127) / 128, 128, 0, st>>>(bp_ldet, ndet, W);
+    SFQ_LAUNCHED();
+    SFQ_CUDA_TRY(cudaMemcpyAsync(bp_wt, props + (long)P_WEIGHT * W, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
+    if (restore) {
+      int h = hist_pos;
+      for (int k = 0; k < nb; ++k) {
+        h = h == 0 ? nhist - 1 : h - 1;
+        bp_restore_kernel<<<(W + 127) / 128, 128, 0, st>>>(bp_wt, bp_wfac + h, nhist, W);
+        SFQ_LAUNCHED();
+      }
+    }
+    return rdm_measure(bp_wt, true, one, two);
+  }
+
   // --- MixedEstimator with the OneRDM and DiagonalTwoRDM observables -------------------------
   cplx* rdm_buf = nullptr;  // Gf (W, nspin, Mr, Mr), one (nspin Mr Mr), two (nblk Mr Mr), wc, tot (W), ov (ndet W)
   int rdm_nspin() const { return collinear ? 2 : 1; }
@@ -881,10 +1005,18 @@ struct Engine {
   // one (rdm_nspin, Mr, Mr) and the diagonal two-body RDM before folding (rdm_nblk, Mr, Mr), both divided
   // by the total weight, on the host (MixedEstimator.hpp:37-147)
   int measure_rdm(std::vector<cplx>& one, std::vector<cplx>& two) {
-    int rc;
     if (mixed) return record_error(SFQ_ERR_UNSUPPORTED, "the mixed estimator's RDMs are measured in FP64 engines");
+    inv_cached = false;
+    return rdm_measure(props + (long)P_WEIGHT * W, false, one, two);
+  }
+  // the RDM reduction shared by the mixed estimator (bp false: the trial's references against the
+  // walkers, coefficients relative to the walkers' log overlaps) and the back-propagated one (bp true:
+  // each walker's propagated references against its anchored matrix, the overlaps with conj of the
+  // references' QR log dets, constructBPMeasurementInputs, BackPropEstimator.hpp:36-110)
+  int rdm_measure(const cplx* weight, bool bp, std::vector<cplx>& one, std::vector<cplx>& two) {
+    int rc;
     const int ns = rdm_nspin(), nb = rdm_nblk();
-    const long MM = (long)Mr * Mr;
+    const long MM = (long)Mr * Mr, RN = det_elems();
     const size_t elems = (size_t)W * ns * MM + ns * MM + nb * MM + 2 * (size_t)W + (size_t)ndet * W;
     if (!rdm_buf) SFQ_CUDA_TRY(cudaMalloc(&rdm_buf, sizeof(cplx) * elems));
     cplx* Gf = rdm_buf;
@@ -894,28 +1026,42 @@ struct Engine {
     cplx* tot = wc + W;
     cplx* ovd = tot + W;
     SFQ_CUDA_TRY(cudaMemsetAsync(o1, 0, sizeof(cplx) * (ns + nb) * MM, st));
-    const cplx* shift = props + (long)P_OVLP * W;
-    const cplx* weight = props + (long)P_WEIGHT * W;
+    const cplx* shift = bp ? nullptr : props + (long)P_OVLP * W;
+    const cplx* B = bp ? bp_SMN : SM;
     std::vector<cplx> cic(ndet, mk(1.0, 0.0));
     for (int d = 0; d < ndet && ndet > 1; ++d) cic[d] = cconj(ci_h[d]);
-    // the reference determinants' log overlaps, one determinant per spin (not doubled for CLOSED)
-    inv_cached = false;
+    // determinant d's overlap matrices (one determinant per spin, not doubled), inverses in T
+    auto factor = [&](int d, bool invert) -> int {
+      if (!bp) return md_factor(d, SM, W, ovd + (long)d * W, invert, 1.0);
+      GemmDesc g;  // T = Refs^H SMN, per walker (density_matrix.hpp:158-195)
+      g.M = N; g.N = N; g.K = Mr; g.batch = W;
+      g.A = bp_refs + (long)d * W * RN; g.sAm = 1; g.sAk = N; g.sAb = RN; g.a_cplx = true; g.conj_a = true;
+      g.B = bp_SMN; g.sBk = N; g.sBn = 1; g.sBb = RN; g.b_cplx = true;
+      g.C = T; g.sCm = N; g.sCn = 1; g.sCb = (long)N * N;
+      int r;
+      if ((r = gemm_f64(g, st))) return r;
+      if ((r = ops::mask_cross_spin(T, W, N, spin_split(), st))) return r;
+      if ((r = lu_logdet(T, (long)N * N, W, N, ovd + (long)d * W, false, 1.0, invert, st))) return r;
+      bp_ov_kernel<<<(W + 127) / 128, 128, 0, st>>>(ovd + (long)d * W, bp_ldet + (long)d * W, ov_scale(), W);
+      SFQ_LAUNCHED();
+      return SFQ_OK;
+    };
     for (int d = 0; d < ndet; ++d)
-      if ((rc = md_factor(d, SM, W, ovd + (long)d * W, false, 1.0))) return rc;
+      if ((rc = factor(d, false))) return rc;
     {
-      std::vector<cplx> tmp(cic);
       cplx* dcic = nullptr;
       SFQ_CUDA_TRY(cudaMallocAsync((void**)&dcic, sizeof(cplx) * ndet, st));
-      SFQ_CUDA_TRY(cudaMemcpyAsync(dcic, tmp.data(), sizeof(cplx) * ndet, cudaMemcpyHostToDevice, st));
+      SFQ_CUDA_TRY(cudaMemcpyAsync(dcic, cic.data(), sizeof(cplx) * ndet, cudaMemcpyHostToDevice, st));
       rdm_tot_kernel<<<(W + 127) / 128, 128, 0, st>>>(ovd, dcic, shift, ndet, W, tot);
       SFQ_LAUNCHED();
       SFQ_CUDA_TRY(cudaFreeAsync(dcic, st));
-      SFQ_CUDA_TRY(cudaStreamSynchronize(st));  // tmp lives until the copy is done
+      SFQ_CUDA_TRY(cudaStreamSynchronize(st));  // cic lives until the copy is done
     }
     for (int d = 0; d < ndet; ++d) {
-      if ((rc = md_factor(d, SM, W, ovd + (long)d * W, true, 1.0))) return rc;
-      if ((rc = ops::green_compact(T, SM, G, W, Mr, N, st))) return rc;
-      // the full G of each spin block: Gf[w][s] = PsiT_d[rows s]^T Gc[w][rows s] (density_matrix.hpp:580-600)
+      if ((rc = factor(d, true))) return rc;
+      if ((rc = ops::green_compact(T, B, G, W, Mr, N, st))) return rc;
+      // the full G of each spin block: Gf[w][s] = Aeff[rows s]^T Gc[w][rows s] (density_matrix.hpp:580-600),
+      // Aeff = PsiT_d (shared) or the walker's conj(Refs^T)
       for (int s = 0; s < ns; ++s) {
         const int r0 = collinear ? (s == 0 ? 0 : nup) : 0, r1 = collinear ? (s == 0 ? nup : N) : N;
         if (r1 == r0) {  // an empty spin sector has a zero G
@@ -924,8 +1070,13 @@ struct Engine {
         }
         GemmDesc g;
         g.M = Mr; g.N = Mr; g.K = r1 - r0; g.batch = W;
-        g.A = PsiT + d * det_elems() + (long)r0 * Mr; g.sAm = 1; g.sAk = Mr; g.sAb = 0; g.a_cplx = true;
-        g.B = G + (long)r0 * Mr; g.sBk = Mr; g.sBn = 1; g.sBb = det_elems(); g.b_cplx = true;
+        if (bp) {
+          g.A = bp_refs + (long)d * W * RN + r0; g.sAm = N; g.sAk = 1; g.sAb = RN; g.conj_a = true;
+        } else {
+          g.A = PsiT + d * RN + (long)r0 * Mr; g.sAm = 1; g.sAk = Mr; g.sAb = 0;
+        }
+        g.a_cplx = true;
+        g.B = G + (long)r0 * Mr; g.sBk = Mr; g.sBn = 1; g.sBb = RN; g.b_cplx = true;
         g.C = Gf + s * MM; g.sCm = Mr; g.sCn = 1; g.sCb = ns * MM;
         if ((rc = gemm_f64(g, st))) return rc;
       }
@@ -1029,6 +1180,9 @@ struct Engine {
       uni_wait = nullptr;
     }
     if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
+    if (nbp)  // storeFields (AFQMCBasePropagator.cpp:342-344): the fields into the ring slot
+      SFQ_CUDA_TRY(cudaMemcpy2DAsync(bp_fields + (long)(hist_pos % nbp) * Nc, sizeof(cplx) * nbp * Nc, X,
+                                     sizeof(cplx) * Nc, sizeof(cplx) * Nc, W, cudaMemcpyDeviceToDevice, st));
     ph_end(SFQ_PH_FIELDS);
     ph_begin(SFQ_PH_VHS);
     ph_begin(SFQ_PH_VHS_GEMM);
@@ -1054,7 +1208,12 @@ struct Engine {
     up.max_weight = std::fmax(p.weight_bound_floor, p.weight_bound_fraction * target_pop());
     up.hybrid = 1; up.free_projection = p.free_projection; up.use_cp_constraint = 0;
     up.Eshift_dev = dev_mode ? d_eshift : nullptr;
+    if (nbp) {  // the step's weight factors into the history slot (WalkerSetUpdate.hpp:184-188)
+      up.wfac = bp_wfac + hist_pos;
+      up.wfac_stride = nhist;
+    }
     if ((rc = walker_update(wprops(), newov, mf, hw, E3, up, stats, st))) return rc;
+    if (nbp) hist_pos = (hist_pos + 1) % nhist;  // advanceHistoryPos
     ph_end(SFQ_PH_UPDATE);
     return SFQ_OK;
   }
@@ -1471,6 +1630,11 @@ struct Engine {
     if ((rc = sfq::population_control(SM, (long)Mr * N, wprops(), W, own ? r : 0.0, p.seed, call, own ? 0 : 1, pw, st,
                                       dev_mode && !own ? d_step : nullptr)))
       return rc;
+    if (nbp) {  // copy_walker copies the back-propagation buffers too (WalkerSetBase.h:375-415)
+      if ((rc = copy_walker_rows(bp_SMN, (long)Mr * N, pw, W, st))) return rc;
+      if ((rc = copy_walker_rows(bp_fields, (long)nbp * Nc, pw, W, st))) return rc;
+      if ((rc = copy_walker_rows(bp_wfac, nhist, pw, W, st))) return rc;
+    }
     ph_end(SFQ_PH_POPCONTROL);
     if (dev_mode) return SFQ_OK;  // the collapse flag stays on the device until the block ends
     int flag = 0;
@@ -2041,6 +2205,9 @@ int sfq_engine_destroy(sfq_engine_t h) {
   if (e.Vp) cudaFree(e.Vp);
   if (e.h_pinned) cudaFreeHost(e.h_pinned);
   if (e.rdm_buf) cudaFree(e.rdm_buf);
+  for (void* q : {(void*)e.bp_SMN, (void*)e.bp_fields, (void*)e.bp_wfac, (void*)e.bp_refs, (void*)e.bp_ldet,
+                  (void*)e.bp_wt})
+    if (q) cudaFree(q);
   if (e.st) cudaStreamDestroy(e.st);
   delete h;
   return SFQ_OK;
@@ -2155,12 +2322,40 @@ int sfq_engine_orthogonalize(sfq_engine_t h) {
   return h->e.orthogonalize();
 }
 
+int sfq_engine_enable_back_propagation(sfq_engine_t h, int nbp) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.enable_bp(nbp);
+}
+
+int sfq_engine_bp_anchor(sfq_engine_t h) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.bp_anchor();
+}
+
+static int fold_rdms(Engine& e, const std::vector<cplx>& one, const std::vector<cplx>& two, void* one_rdm,
+                     void* diag_two_rdm);
+
+int sfq_engine_measure_bp_rdm(sfq_engine_t h, int nsteps, int ortho_interval, int path_restoration, void* one_rdm,
+                              void* diag_two_rdm) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  std::vector<cplx> one, two;
+  int rc;
+  if ((rc = e.measure_bp(nsteps, ortho_interval, path_restoration != 0, one, two))) return rc;
+  return fold_rdms(e, one, two, one_rdm, diag_two_rdm);
+}
+
 int sfq_engine_measure_rdm(sfq_engine_t h, void* one_rdm, void* diag_two_rdm) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
   Engine& e = h->e;
   std::vector<cplx> one, two;
   int rc;
   if ((rc = e.measure_rdm(one, two))) return rc;
+  return fold_rdms(e, one, two, one_rdm, diag_two_rdm);
+}
+
+static int fold_rdms(Engine& e, const std::vector<cplx>& one, const std::vector<cplx>& two, void* one_rdm,
+                     void* diag_two_rdm) {
   if (one_rdm) std::memcpy(one_rdm, one.data(), sizeof(cplx) * one.size());
   if (!diag_two_rdm) return SFQ_OK;
   // fold the i <-> j symmetry (Observables/diagonal_twordm.hpp:104-140)
@@ -2272,6 +2467,8 @@ int sfq_engine_run(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, d
 int sfq_engine_block(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, double* meas, int max_meas,
                      int* nmeas) {
   if (!h || !rp || !Eshift) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (h->e.nbp)
+    return record_error(SFQ_ERR_UNSUPPORTED, "device-resident blocks do not keep the back-propagation history");
   int rc;
   if ((rc = h->e.block_async(*rp, *Eshift))) return rc;
   return h->e.block_result(Eshift, meas, max_meas, nmeas);
@@ -2279,6 +2476,8 @@ int sfq_engine_block(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift,
 
 int sfq_engine_block_async(sfq_engine_t h, const sfq_run_params_t* rp, double Eshift) {
   if (!h || !rp) return record_error(SFQ_ERR_ARG, "null pointer");
+  if (h->e.nbp)
+    return record_error(SFQ_ERR_UNSUPPORTED, "device-resident blocks do not keep the back-propagation history");
   return h->e.block_async(*rp, Eshift);
 }
 
@@ -2302,6 +2501,7 @@ int sfq_group_create(sfq_group_t* out, const sfq_engine_t* engines, int n) {
       return record_error(SFQ_ERR_ARG, "group: members on different devices");
     for (int j = 0; j < i; ++j)
       if (engines[j] == engines[i]) return record_error(SFQ_ERR_ARG, "group: member %d repeated", i);
+    if (engines[i]->e.nbp) return record_error(SFQ_ERR_UNSUPPORTED, "group: member %d keeps back propagation", i);
     es.push_back(&engines[i]->e);
   }
   sfq_group_t h = new sfq_group_s;

@@ -56,6 +56,8 @@ int gemm_f64(const GemmDesc& d, cudaStream_t st) {
   if (AC && !BC && !CJ && AK && BK) return pick_tile<true, false, false, true, true>(d, st);
   if (AC && BC && !CJ && AK && BK) return pick_tile<true, true, false, true, true>(d, st);
   if (AC && BC && CJ && !AK && !BK) return pick_tile<true, true, true, false, false>(d, st);
+  // conj(A) contiguous along K: the back-propagated references' full Green's function
+  if (AC && BC && CJ && AK && !BK) return pick_tile<true, true, true, true, false>(d, st);
   if (!AC && !BC && !CJ && AK && !BK) return pick_tile<false, false, false, true, false>(d, st);
   if (AC && !BC && !CJ && AK && !BK) return pick_tile<true, false, false, true, false>(d, st);
   if (!AC && !BC && !CJ && AK && BK) return pick_tile<false, false, false, true, true>(d, st);

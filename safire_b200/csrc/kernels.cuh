@@ -39,6 +39,10 @@ struct UpdateParams {
   double max_weight = 100.0;  // max(floor, fraction * target population)
   int hybrid = 1, free_projection = 0, use_cp_constraint = 0;
   const double* Eshift_dev = nullptr;  // when set, Eshift is read from device memory
+  // back propagation: the step's weight factor (phase over projection, WalkerSetUpdate.hpp:141-147)
+  // of walker i goes to wfac[i * wfac_stride] when wfac is set
+  cplx* wfac = nullptr;
+  long wfac_stride = 1;
 };
 struct WalkerProps {  // columns of the walker set (SoA), each nwalk complex
   cplx *weight, *phase, *pseudo_eloc, *e1, *exx, *ej, *ovlp, *theta;
@@ -56,6 +60,8 @@ struct PopWork {
   double* cum;      // nwalk
   int* flag;        // 1: 0 ok, SFQ_ERR_WEIGHT_COLLAPSE
 };
+// the rows of A (elems per walker) copied along the population-control plan pw (after population_control)
+int copy_walker_rows(cplx* A, long elems, const PopWork& pw, int nwalk, cudaStream_t st);
 // call_dev: when set, the comb's call index is read from device memory
 int population_control(cplx* SM, long walker_elems, const WalkerProps& w, int nwalk, double r_uniform,
                        unsigned long long seed, unsigned long long call, int use_philox, const PopWork& pw,

@@ -241,6 +241,23 @@ int orthogonalize_carry(cplx* SM, cplx* SM2, cplx* S, cplx* R, cplx* Tw, int* st
   return copy_walkers_where(Tinv, Tw, again, 0, W, NN, st);
 }
 
+// orthogonalize() that also accumulates log det R = sum_i log r_ii of both passes into ldet (W):
+// det_ops::orthogonalize(wset, ldet) with log_determinant_from_geqrf (orthogonalize.hpp:444-469;
+// CholeskyQR's r_ii are real and positive, as Householder's after the sign fix)
+int orthogonalize_logdet(cplx* SM, cplx* SM2, cplx* S, cplx* R, int* status, cplx* ldet, int W, int M, int N,
+                         cudaStream_t st, int nup) {
+  int rc;
+  int* again = status + W;
+  const int wpb = 8;
+  if ((rc = cholqr_pass(SM, SM2, S, status, again, nullptr, W, M, N, st, R, nup))) return rc;
+  sub_logdiag_kernel<<<(W + wpb - 1) / wpb, 32 * wpb, 0, st>>>(R, N, nullptr, ldet, -1.0, W);
+  SFQ_LAUNCHED();
+  if ((rc = cholqr_pass(SM2, SM, S, status, nullptr, again, W, M, N, st, R, nup))) return rc;
+  sub_logdiag_kernel<<<(W + wpb - 1) / wpb, 32 * wpb, 0, st>>>(R, N, again, ldet, -1.0, W);
+  SFQ_LAUNCHED();
+  return copy_walkers_where(SM, SM2, again, 0, W, (long)M * N, st);  // one-pass walkers
+}
+
 int energy_chunk(int W, int N, int Nc, long max_elems) {
   long per = (long)W * N * N;
   long nv = per > 0 ? max_elems / per : Nc;

@@ -32,6 +32,9 @@ int orthogonalize(cplx* SM, cplx* SM2, cplx* S, int* status, cplx* log_detR, int
 // S, R, Tw: (W, N, N) scratch
 int orthogonalize_carry(cplx* SM, cplx* SM2, cplx* S, cplx* R, cplx* Tw, int* status, cplx* Tinv, cplx* ov,
                         double scale, int W, int M, int N, cudaStream_t st, int nup = -1);
+// the same QR accumulating log det R into ldet (W); S, R: (W, N, N) scratch
+int orthogonalize_logdet(cplx* SM, cplx* SM2, cplx* S, cplx* R, int* status, cplx* ldet, int W, int M, int N,
+                         cudaStream_t st, int nup = -1);
 // zero the cross-spin blocks of W per-walker N x N matrices (a no-op unless 0 < nup < N)
 int mask_cross_spin(cplx* A, int W, int N, int nup, cudaStream_t st);
 // energy with chunked T; ws: T chunk (W*N*nv*N) + exxn (W*Nc) + kl (W*Nc)

@@ -105,6 +105,7 @@ __global__ void walker_update_kernel(WalkerProps wp, const cplx* new_ovlp, const
     eloc = cadd(cadd(E3[3 * i + 0], E3[3 * i + 1]), E3[3 * i + 2]);
   }
   cplx weight = wp.weight[i], phase = wp.phase[i];
+  cplx wfac = mk(0.0, 0.0);
   if (!isfinite(eloc.x)) {
     weight = mk(0.0, 0.0);
     phase = mk(0.0, 0.0);
@@ -127,7 +128,9 @@ __global__ void walker_update_kernel(WalkerProps wp, const cplx* new_ovlp, const
     if (p.free_projection) weight = cmul(weight, cscale(wf, scale));
     else weight = cscale(weight, scale * aw);
     phase = cmul(phase, mk(wf.x / aw, wf.y / aw));
+    if (fabs(scale) > 2.2250738585072014e-308) wfac = mk(wf.x / aw / scale, wf.y / aw / scale);
   }
+  if (p.wfac) p.wfac[(long)i * p.wfac_stride] = wfac;
   // bound_walker_weights
   const double a = hypot(weight.x, weight.y);
   if (stats) atomicAdd(&stats[3], 1ull);
@@ -442,6 +445,25 @@ int walker_update(const WalkerProps& w, const cplx* new_ovlp, const cplx* mf, co
                   const UpdateParams& p, unsigned long long* stats, cudaStream_t st) {
   if (p.nwalk <= 0) return SFQ_OK;
   walker_update_kernel<<<(p.nwalk + 127) / 128, 128, 0, st>>>(w, new_ovlp, mf, hw, E3, p, stats);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+namespace {
+__global__ void copy_rows_kernel(cplx* A, long elems, const int* pairs, const int* npairs) {
+  const int pidx = blockIdx.y;
+  if (pidx >= *npairs) return;
+  const cplx* s = A + (long)pairs[2 * pidx] * elems;
+  cplx* d = A + (long)pairs[2 * pidx + 1] * elems;
+  for (long e = blockIdx.x * blockDim.x + threadIdx.x; e < elems; e += (long)gridDim.x * blockDim.x) d[e] = s[e];
+}
+}  // namespace
+
+int copy_walker_rows(cplx* A, long elems, const PopWork& pw, int nwalk, cudaStream_t st) {
+  if (nwalk <= 1 || elems <= 0) return SFQ_OK;
+  int gx = int((elems + 255) / 256);
+  if (gx > 8) gx = 8;
+  copy_rows_kernel<<<dim3(gx, nwalk - 1), 256, 0, st>>>(A, elems, pw.pairs, pw.npairs);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

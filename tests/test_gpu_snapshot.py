@@ -87,6 +87,20 @@ def test_collinear_with_identical_spins_is_closed():
         assert np.max(np.abs(a - b)) < 1e-10 * np.max(np.abs(a)), k
 
 
+def test_back_propagation_refused_by_blocks():
+    snap = bh_snapshot()
+    eng = A.AfqmcEngine(_system(snap), 8, dt=0.01, precision=capi.PRECISION_FP64)
+    E0 = eng.init()
+    eng.enable_back_propagation(2)
+    with pytest.raises(capi.SafireError) as ex:
+        eng.run_block(4, E0, ortho_interval=2, pop_interval=2, equilibration_steps=0, measure_interval=2)
+    assert ex.value.code == 3
+    with pytest.raises(capi.SafireError) as ex:
+        eng.measure_bp_rdms(3)  # longer than the ring
+    assert ex.value.code == 2
+    eng.close()
+
+
 @pytest.mark.parametrize("case", ["bh_uhf_collinear", "bh_ghf_noncollinear", "bh_rcasci_rhf_closed"])
 def test_spin_walkers_rejected_in_mixed_precision(case):
     with pytest.raises(capi.SafireError) as ex:
@@ -110,9 +124,10 @@ RDM_CASES = ["bh_rhf_closed", "bh_uhf_collinear", "bh_uhf_noncollinear", "bh_rca
 
 
 @pytest.mark.parametrize("case", RDM_CASES)
-def test_engine_reproduces_recorded_mixed_rdms(case):
-    """sfq_engine_measure_rdm every 2 steps of the replay: the mixed estimator's one-body and folded
-    diagonal two-body RDMs against the oracle's per measurement and the recorded means / errors."""
+def test_engine_reproduces_recorded_rdms(case):
+    """sfq_engine_measure_rdm every 2 steps and sfq_engine_measure_bp_rdm over 2 steps (with path
+    restoration) in the replay: the mixed and back-propagated one-body and folded diagonal two-body
+    RDMs against the oracle's per measurement and the recorded means / errors."""
     snap = snapshot(case)
     st = snap["settings"]
     eng = A.AfqmcEngine(_system(snap), st["nwalk"], dt=st["dt"], seed=0, precision=capi.PRECISION_FP64)
@@ -121,12 +136,16 @@ def test_engine_reproduces_recorded_mixed_rdms(case):
     _, series = eng.run_with_streams(st["steps"], eng.init(), field_rng.uniforms, lambda: walker_rng.uniforms(1)[0],
                                      ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
                                      equilibration_steps=st["equilibration_steps"],
-                                     measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"])
+                                     measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"],
+                                     bp_steps=snap["bp_steps"], bp_ortho_interval=snap["bp_ortho_interval"])
     eng.close()
     _, _, oracle_series = O.run_seeded(_oracle_hamiltonian(snap), st["nwalk"], st["dt"], st["steps"], st["seed"],
                                        ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
-                                       measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"])
-    for k in ("MixedEstimator/OneRDM", "MixedEstimator/DiagonalTwoRDM"):
+                                       measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"],
+                                       bp_steps=snap["bp_steps"], bp_ortho_interval=snap["bp_ortho_interval"])
+    rdms = [k for k in snap["recorded"] if k.startswith(("MixedEstimator", "BackPropEstimator"))]
+    assert len(rdms) == 4
+    for k in rdms:
         a, b = np.asarray(series[k]), np.asarray(oracle_series[k])
         assert a.shape == b.shape
         assert np.max(np.abs(a - b)) <= 1e-11 * max(1.0, float(np.max(np.abs(b)))), k
