@@ -103,6 +103,12 @@ class Engine {
     check(sfq_engine_create(&h_, &p, hcore, Likn, PsiT));
     p_ = p;
   }
+  // a multi-determinant NOMSD trial: ndet matrices of the walker type's shape, coefficients ci
+  Engine(const sfq_engine_params_t& p, const double* hcore, const double* Likn, int ndet, const ComplexType* PsiT,
+         const ComplexType* ci) {
+    check(sfq_engine_create_nomsd(&h_, &p, hcore, Likn, ndet, PsiT, ci));
+    p_ = p;
+  }
   ~Engine() { sfq_engine_destroy(h_); }
   Engine(const Engine&) = delete;
   Engine& operator=(const Engine&) = delete;
@@ -126,7 +132,29 @@ class Engine {
   }
   void set_tiles(const sfq_tiles_t& t) { check(sfq_engine_set_tiles(h_, &t)); }
 
+  // MixedEstimator's OneRDM (nspin, R, R) and folded DiagonalTwoRDM (see sfq_engine_measure_rdm)
+  void measure_rdm(std::vector<ComplexType>& one_rdm, std::vector<ComplexType>& diag_two_rdm) {
+    resize_rdms(one_rdm, diag_two_rdm);
+    check(sfq_engine_measure_rdm(h_, one_rdm.data(), diag_two_rdm.data()));
+  }
+  // BackPropEstimator: the walker set's resize_bp, setAnchor and one back-propagated measurement
+  void enable_back_propagation(int nbp) { check(sfq_engine_enable_back_propagation(h_, nbp)); }
+  void bp_anchor() { check(sfq_engine_bp_anchor(h_)); }
+  void measure_bp_rdm(int nsteps, int ortho_interval, bool path_restoration, std::vector<ComplexType>& one_rdm,
+                      std::vector<ComplexType>& diag_two_rdm) {
+    resize_rdms(one_rdm, diag_two_rdm);
+    check(sfq_engine_measure_bp_rdm(h_, nsteps, ortho_interval, path_restoration ? 1 : 0, one_rdm.data(),
+                                    diag_two_rdm.data()));
+  }
+
  private:
+  void resize_rdms(std::vector<ComplexType>& one, std::vector<ComplexType>& two) const {
+    const long M = p_.nmo;
+    const bool coll = p_.walker_type == SFQ_WALKER_COLLINEAR, ncol = p_.walker_type == SFQ_WALKER_NONCOLLINEAR;
+    const long R = (ncol ? 2 : 1) * M;
+    one.resize(size_t((coll ? 2 : 1) * R * R));
+    two.resize(size_t(M * (2 * M - 1) - ((coll || ncol) ? 0 : M * (M - 1) / 2)));
+  }
   sfq_engine_t h_ = nullptr;
   sfq_engine_params_t p_{};
 };

@@ -104,3 +104,17 @@ def test_uneven_systems_layout():
     assert [s.M for s in specs] == [48 + 16 * (i % 18) for i in range(24)]
     assert all(s.N * 4 == s.M and s.Nc == 5 * s.M for s in specs)
     assert all(64 <= w <= 512 for w in walkers) and len(set(walkers)) > 12
+
+
+def test_cpp_header_compiles():
+    """include/safire_b200.hpp (the reference-named C++ view) is valid C++17 against the C header."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    src = '#include "safire_b200.hpp"\nint main() { return 0; }\n'
+    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", inc, "-x", "c++", "-"], input=src,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
