@@ -141,8 +141,14 @@ def main():
     snapshot_case(fn, "Li", "hamil_closed.h5", "rohf_nomsd_polarized.h5",
                   "hamil_closed/rohf_wfn_polarized/collinear", "COLLINEAR", "li_rohf_collinear_snapshot.npz")
 
-    res = H5File(os.path.join(fn, "statistical_references", "BH", "dense_rhf_basis_closed", "rhf_nomsd", "closed",
-                              "results.h5"))
+    statistical_case(fn, "BH/dense_rhf_basis_closed/rhf_nomsd/closed", "bh_rhf_closed_statistical.json")
+    statistical_case(fn, "Li/hamil_closed/rohf_wfn_polarized/collinear", "li_rohf_collinear_statistical.json")
+
+
+def statistical_case(fn, case, out_name):
+    """A statistical reference: its settings (walkers per rank x ranks, steps, equilibration,
+    intervals) and the mean / error of the energy observables after equilibration."""
+    res = H5File(os.path.join(fn, "statistical_references", *case.split("/"), "results.h5"))
     inp = json.loads(res["input_file"])
     ex = inp["execute"]
     ranks = int(res["num_ranks"])
@@ -154,7 +160,7 @@ def main():
     for k in ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy"):
         m, e = complex(res[f"measurements/Stage0/{k}/mean"]), complex(res[f"measurements/Stage0/{k}/error"])
         stat["recorded"][k] = dict(mean=[m.real, m.imag], error=[e.real, e.imag])
-    path = os.path.join(HERE, "bh_rhf_closed_statistical.json")
+    path = os.path.join(HERE, out_name)
     with open(path, "w") as f:
         json.dump(stat, f, indent=1)
     print(path, {k: v for k, v in stat.items() if k != "recorded"})

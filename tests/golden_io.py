@@ -75,9 +75,9 @@ def snapshot_match(series, recorded, rebinned_average, tol=1e-9):
     return None
 
 
-def bh_statistical():
-    """The BH statistical reference (make_bh_snapshot.py): settings and recorded mean / error."""
-    with open(os.path.join(HERE, "bh_rhf_closed_statistical.json")) as f:
+def bh_statistical(name="bh_rhf_closed"):
+    """A statistical reference (make_bh_snapshot.py): settings and recorded mean / error."""
+    with open(os.path.join(HERE, f"{name}_statistical.json")) as f:
         s = json.load(f)
     s["recorded"] = {k: (complex(*v["mean"]), complex(*v["error"])) for k, v in s["recorded"].items()}
     return s

@@ -1,30 +1,30 @@
-"""The FP64 engine's own run of BH agrees with the reference's statistical reference.
+"""The FP64 engine's own runs agree with the reference's statistical references.
 
-The reference's long BH run (dense Cholesky, RHF trial, CLOSED walkers: 96 ranks x 16 walkers, 48000
-steps of 0.01, 3000 of them equilibration with a relaxing Eshift, population control, orthogonalization
-and a measurement every 10 steps) recorded the mean and error of each energy.  The engine runs the same
-schedule on one GPU for the same 1536 walkers, with its own Philox fields and comb, as device-resident
-blocks; its means must agree with the recorded ones under the reference's own statistical comparison.
+The reference's long runs of BH (RHF trial, CLOSED walkers) and Li (polarized ROHF trial, COLLINEAR
+walkers) -- dense Cholesky, 96 ranks x 16 walkers, 48000 steps of 0.01, 3000 of them equilibration
+with a relaxing Eshift, population control, orthogonalization and a measurement every 10 steps --
+recorded the mean and error of each energy.  The engine runs the same schedule on one GPU for the same
+1536 walkers, with its own Philox fields and comb, as device-resident blocks; its means must agree
+with the recorded ones under the reference's own statistical comparison.
 """
 import numpy as np
 import pytest
 
 from oracle import afqmc_oracle as O
 from safire_b200 import afqmc as A
-from safire_b200 import capi, synthetic
-from tests.golden_io import bh_snapshot, bh_statistical, statistically_equal
+from safire_b200 import capi
+from tests.golden_io import bh_statistical, engine_system, snapshot, statistically_equal
 
 pytestmark = pytest.mark.gpu
 
 KEYS = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy")
 
 
-def test_engine_agrees_with_reference_statistics():
-    snap, stat = bh_snapshot(), bh_statistical()
-    M, N, Nc = snap["PsiT"].shape[1], snap["PsiT"].shape[0], snap["Likn"].shape[2]
-    system = synthetic.System(synthetic.SystemSpec(M=M, N=N, Nc=Nc, decay=0.0), snap["hcore"], snap["Likn"],
-                              snap["PsiT"], snap["E0"])
-    eng = A.AfqmcEngine(system, stat["nwalk"], dt=stat["dt"], seed=2024, precision=capi.PRECISION_FP64)
+@pytest.mark.parametrize("case", ["bh_rhf_closed", "li_rohf_collinear"])
+def test_engine_agrees_with_reference_statistics(case):
+    snap, stat = snapshot(case), bh_statistical(case)
+    assert snap["settings"]["walker_type"] == stat["walker_type"]
+    eng = A.AfqmcEngine(engine_system(snap), stat["nwalk"], dt=stat["dt"], seed=2024, precision=capi.PRECISION_FP64)
     Eshift = eng.init()
     block = 50 * stat["measure_interval"]  # 50 measurements per device-resident block
     assert stat["steps"] % block == 0
@@ -44,6 +44,6 @@ def test_engine_agrees_with_reference_statistics():
         mean, err = O.rebinned_average(series, 50)  # bins of 500 steps, longer than the correlation time
         ok, d, tol = statistically_equal(mean, err, *stat["recorded"][k])
         rm, re_ = stat["recorded"][k]
-        print(f"{k}: {mean.real:.6f} +- {abs(err):.6f} vs recorded {rm.real:.6f} +- {abs(re_):.6f}, "
+        print(f"{case} {k}: {mean.real:.6f} +- {abs(err):.6f} vs recorded {rm.real:.6f} +- {abs(re_):.6f}, "
               f"|d| = {d:.2e} <= {tol:.2e}")
         assert ok, (k, mean, err, stat["recorded"][k], d, tol)
