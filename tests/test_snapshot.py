@@ -150,3 +150,38 @@ def test_oracle_reproduces_recorded_rdms(case):
         assert len(series[k]) == st["steps"] // 2
         assert np.asarray(series[k]).shape[1:] == snap["recorded"][k][0].shape
         assert snapshot_match(series[k], snap["recorded"][k], O.rebinned_average) is not None, k
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="the reference's files are not on this machine")
+def test_h5read_reads_every_reference_file_and_chunked_data():
+    """The reader parses every HDF5 file of the reference tree (groups, datasets, attributes), and its
+    chunked, deflate-compressed datasets decode to consistent data: in a recorded results file the
+    back-propagated one-body RDM has the electron count as its trace in every bin."""
+    import glob
+    from safire_b200.h5read import H5File
+    root = os.path.dirname(os.path.dirname(REF))
+    files = sorted(glob.glob(os.path.join(root, "**", "*.h5"), recursive=True))
+    assert len(files) > 100
+    ndata = 0
+    for p in files:
+        f = H5File(p)
+        stack = ["/"]
+        while stack:
+            q = stack.pop()
+            for k in f.keys(q):
+                path = q.rstrip("/") + "/" + k
+                if f.is_group(path):
+                    f.attrs(path)
+                    stack.append(path)
+                else:
+                    f[path]
+                    ndata += 1
+    assert ndata > 1000
+    res = os.path.join(root, "docs", "examples", "solids", "02_C_diamond_pyscf_interface", "data", "afqmc.results.h5")
+    if os.path.exists(res):
+        f = H5File(res)
+        R = f["/Measurements/Stage0/BackPropEstimator/Steps=100/OneRDM/bins"]
+        tr = np.einsum("bsii->b", R[..., 0] + 1j * R[..., 1])
+        assert np.allclose(tr, np.round(tr.real[0]), atol=1e-8)
+        E = f["/Measurements/Stage0/Energy/bins"]
+        assert np.all(np.isfinite(E)) and np.all(E[:, 0] != 0.0)
