@@ -146,16 +146,17 @@ def population_control(dist, SM, props, r, group=None):
         dist.broadcast(off, 0, group=group)
     offspring = off.numpy()
     _, sends, recvs, copies = local_moves(offspring, counts, rank)
+    sm_elems = int(np.prod(SM.shape[1:]))  # a rank may hold no walkers
     row = lambda i: torch.from_numpy(np.concatenate([SM[i].reshape(-1), props[:, i]]).view(np.float64))
     # a rank either sends or receives; both ends post in plan order (MPI's non-overtaking rule there)
     for walker, dst in sends:
         dist.send(row(walker).contiguous(), dst, group=group)
     for slot, src in recvs:
-        t = torch.empty(2 * (SM[0].size + props.shape[0]), dtype=torch.float64)
+        t = torch.empty(2 * (sm_elems + props.shape[0]), dtype=torch.float64)
         dist.recv(t, src, group=group)
         v = t.numpy().view(np.complex128)
-        SM[slot] = v[:SM[0].size].reshape(SM.shape[1:])
-        props[:, slot] = v[SM[0].size:]
+        SM[slot] = v[:sm_elems].reshape(SM.shape[1:])
+        props[:, slot] = v[sm_elems:]
     for src, dst in copies:
         SM[dst] = SM[src]
         props[:, dst] = props[:, src]

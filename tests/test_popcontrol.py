@@ -82,7 +82,7 @@ def _rank(rank, world, port, counts, q):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("counts", [[9, 9], [6, 11]])
+@pytest.mark.parametrize("counts", [[9, 9], [6, 11], [0, 12]])
 def test_two_ranks_equal_one_rank_holding_everything(counts):
     """The walkers two gloo ranks end with are, together, the population one rank ends with, and each
     rank keeps its own count; the weights become unit-modulus."""
