@@ -36,6 +36,16 @@ dense-real-Cholesky path (paths relative to the SAFIRE source tree):
   EnergyEstimator::measure      src/AFQMC/Estimators/EnergyEstimator.h:51-100
   run_afqmc step loop           src/AFQMC/Drivers/run_afqmc.cpp:69-113
 
+Beyond the CLOSED single-determinant path, restated the same way and pinned the same way (below):
+  CollinearHamiltonian          the COLLINEAR branches of NOMSD / Real3IndexFactorization (per spin)
+  NoncollinearHamiltonian       the npol = 2 branches (spinor walkers, polarization-independent H)
+  MultiDetHamiltonian           NOMSD with ndet > 1 (NOMSD.cpp:159-331,466-512)
+  measure_mixed_rdms            MixedEstimator + OneRDM / DiagonalTwoRDM (MixedEstimator.hpp:37-147)
+  BackPropEstimator             BackPropEstimator + BackPropagate (BackPropEstimator.hpp:36-275,
+                                AFQMCBasePropagator.cpp:404-526)
+  run_seeded, rebinned_average  execute_simulation + run_afqmc on the reference's host streams
+                                (oracle.mt19937); safiretools' Results.average
+
 LAPACK arithmetic at the boundary (the reference reaches it through TRIQS/nda @5046352):
 zgetrf / zgetri / zgeqrf / zungqr from scipy's OpenBLAS, and numpy's eigh (zheevd).
 
