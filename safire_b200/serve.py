@@ -45,6 +45,10 @@ class Server:
             pass
 
     def add_system(self, system, nwalk, dt=0.005, seed=0, **params):
+        ci = getattr(system, "ci", None)
+        if ci is not None and np.size(ci) > 1:
+            raise capi.SafireError(3, "the serving loop takes single-determinant systems; use AfqmcEngine "
+                                      "(sfq_engine_create_nomsd) for a multi-determinant trial")
         p = capi.system_params(system, nwalk=nwalk, dt=dt, E0=float(system.E0), seed=seed)
         for k, v in params.items():
             setattr(p, k, v)

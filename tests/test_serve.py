@@ -41,3 +41,18 @@ def test_server_argument_errors():
     with pytest.raises(capi.SafireError):
         srv.request(99)
     srv.close()
+
+
+def test_server_refuses_multideterminant_systems():
+    """The serving loop builds single-determinant engines; a multi-determinant system is refused
+    before any library call (no GPU needed)."""
+    import numpy as np
+    from safire_b200 import capi, synthetic
+    from safire_b200.serve import Server
+    s = synthetic.System(synthetic.SystemSpec(M=4, N=1, Nc=4, decay=1.0), np.eye(4), np.zeros((4, 4, 4)),
+                         np.zeros((2, 1, 4), np.complex128), 0.0, ci=np.array([1.0, 0.5], np.complex128))
+    srv = Server.__new__(Server)  # the check precedes the server handle
+    srv.walkers = {}
+    with pytest.raises(capi.SafireError) as ex:
+        Server.add_system(srv, s, 8)
+    assert ex.value.code == 3
