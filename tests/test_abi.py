@@ -44,7 +44,7 @@ def test_binding_covers_header():
 def test_last_error_and_version(lib):
     from safire_b200 import capi
     L = capi.lib()
-    assert L.sfq_abi_version() == 6
+    assert L.sfq_abi_version() == 7
     assert isinstance(L.sfq_last_error(), bytes)
 
 
