@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 7 */
+int sfq_abi_version(void); /* 8 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -143,6 +143,33 @@ int sfq_field_uniforms(double* out, unsigned long long seed, unsigned long long 
  * weights (nwalk) doubles (|w|), device;  offspring (nwalk) ints, device;  r: the comb's uniform.
  * Returns SFQ_ERR_WEIGHT_COLLAPSE when the total weight is <= 1e-6. */
 int sfq_comb(const double* weights, double r, int nwalk, int* offspring, void* stream);
+
+/* Population control over walkers sharded across ranks: host-only planning, no device needed
+ * (population_control.hpp:34-255).  The global population is rank-major: rank r holds counts[r]
+ * walkers, and its walker i is entry counts[0] + ... + counts[r-1] + i of weights / offspring.
+ *
+ * comb(rng, weights, num_target) on the root over the gathered |w| (host memory):
+ * offspring (nwalk) receives the copies of each walker; SFQ_ERR_WEIGHT_COLLAPSE when the total
+ * weight is <= 1e-6.  Same comparisons, in the same order, as sfq_comb. */
+int sfq_comb_host(const double* weights, double r, int nwalk, int num_target, int* offspring);
+
+/* plan_walker_exchange (population_control.hpp:73-133): the transfers realising offspring, as
+ * (src rank, local walker on src, dst rank, copies dst ends with) quadruples in plan order.  Ranks
+ * with excess export their walkers with the most copies first (ties in index order), filling the
+ * ranks with a deficit in rank order.  Deterministic: every rank computes the same plan.
+ * *ntransfers is set to the plan's length; SFQ_ERR_WORKSPACE when it exceeds capacity (at most
+ * sum(counts) + nranks transfers).  SFQ_ERR_ARG when offspring does not preserve the population. */
+int sfq_plan_walker_exchange(const int* offspring, const int* counts, int nranks, int* transfers, int capacity,
+                             int* ntransfers);
+
+/* rank's part of swap_walkers_async (population_control.hpp:143-209), all as (int, int) pairs:
+ *   sends   (local walker, dst rank), in plan order          room for counts[rank] + nranks pairs
+ *   recvs   (slot, src rank), in plan order                   room for counts[rank] pairs
+ *   copies  (src slot, dst slot), made after the receives     room for counts[rank] pairs
+ * A walker received into a slot replaces the walker that left it; local copies fill the remaining
+ * free slots, the kept walkers' extra copies (in index order) first, then the received walkers'. */
+int sfq_walker_moves(const int* offspring, const int* counts, int nranks, int rank, int* sends, int* nsends,
+                     int* recvs, int* nrecvs, int* copies, int* ncopies);
 
 /* Mixed-precision tensor-core GEMM (tcgen05, split BF16, FP32 accumulation), no reference
  * counterpart: C[b] (M x N, fp32) = A[b] (M x K) * B[b] (N x K)^T with A, B fp64 on the device

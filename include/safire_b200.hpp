@@ -61,6 +61,34 @@ inline size_t workspace_size(int op, int nwalk, int nmo, int nel, int nchol = 0)
 
 }  // namespace det_ops
 
+// population control planning on the host (population_control.hpp:34-209); no device needed
+struct walker_transfer {
+  int src;     // sending rank
+  int walker;  // local index of the walker on src
+  int dst;     // receiving rank
+  int copies;  // copies of the walker that dst ends up with
+};
+// comb over |w| (host memory) with the uniform r: the copies of each walker
+inline std::vector<int> comb(const std::vector<double>& weights, double r, int num_target) {
+  std::vector<int> offspring(weights.size());
+  check(sfq_comb_host(weights.data(), r, int(weights.size()), num_target, offspring.data()));
+  return offspring;
+}
+inline std::vector<walker_transfer> plan_walker_exchange(const std::vector<int>& offspring,
+                                                         const std::vector<int>& counts) {
+  long ntot = 0;
+  for (int c : counts) ntot += c;
+  if (long(offspring.size()) != ntot)
+    throw Error(SFQ_ERR_ARG, "plan_walker_exchange: offspring does not match the ranks' walkers");
+  static_assert(sizeof(walker_transfer) == 4 * sizeof(int), "walker_transfer is the ABI's int quadruple");
+  std::vector<walker_transfer> plan(size_t(ntot) + counts.size());
+  int n = 0;
+  check(sfq_plan_walker_exchange(offspring.data(), counts.data(), int(counts.size()),
+                                 reinterpret_cast<int*>(plan.data()), int(plan.size()), &n));
+  plan.resize(n);
+  return plan;
+}
+
 // Real3IndexFactorization over caller-owned device tensors (CLOSED, ndet = 1)
 class HamiltonianOperations {
  public:

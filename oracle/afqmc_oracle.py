@@ -32,6 +32,7 @@ dense-real-Cholesky path (paths relative to the SAFIRE source tree):
   walker_update / bounds        src/AFQMC/Propagators/WalkerSetUpdate.hpp:46-218
   orthogonalize                 src/AFQMC/SlaterDeterminantOperations/orthogonalize.hpp:135-169
   comb / swap_walkers_async     src/AFQMC/Walkers/population_control.hpp:34-65,143-255
+  plan_walker_exchange / moves  src/AFQMC/Walkers/population_control.hpp:73-209 (sharded walkers)
   averagePseudoEnergy / averageEnergy   src/AFQMC/Drivers/average_energy.hpp:33-76
   EnergyEstimator::measure      src/AFQMC/Estimators/EnergyEstimator.h:51-100
   run_afqmc step loop           src/AFQMC/Drivers/run_afqmc.cpp:69-113
@@ -896,6 +897,65 @@ def copy_plan(offspring):
             nxt += 1
     assert nxt == len(free)
     return plan
+
+
+def plan_walker_exchange(offspring, counts):
+    """plan_walker_exchange (population_control.hpp:73-133): (src rank, local walker, dst rank,
+    copies) transfers for a rank-major population, rank r holding counts[r] walkers."""
+    offspring = [int(k) for k in offspring]
+    counts = [int(c) for c in counts]
+    assert len(offspring) == sum(counts) and sum(offspring) == sum(counts)
+    exports, deficits, first = [], [], 0
+    for r, nw in enumerate(counts):
+        local = offspring[first:first + nw]
+        excess = sum(local) - nw
+        if excess < 0:
+            deficits.append([r, -excess])
+        order = sorted(range(nw), key=lambda i: -local[i])  # std::stable_sort on copies, descending
+        k = 0
+        while excess > 0:
+            m = min(local[order[k]], excess)
+            exports.append([r, order[k], m])
+            excess -= m
+            k += 1
+        first += nw
+    plan, d = [], 0
+    for src, walker, copies in exports:
+        while copies > 0:
+            n = min(copies, deficits[d][1])
+            plan.append((src, walker, deficits[d][0], n))
+            copies -= n
+            deficits[d][1] -= n
+            if deficits[d][1] == 0:
+                d += 1
+    return plan
+
+
+def walker_moves(offspring, counts, rank):
+    """rank's part of swap_walkers_async (population_control.hpp:143-209): sends (walker, dst) and
+    receives (slot, src) in plan order, then the local copies (src slot, dst slot), the kept walkers'
+    extra copies in index order before the received walkers'."""
+    plan = plan_walker_exchange(offspring, counts)
+    first = sum(counts[:rank])
+    keep = [int(k) for k in offspring[first:first + counts[rank]]]
+    for src, walker, dst, n in plan:
+        if src == rank:
+            keep[walker] -= n
+    free = [i for i, k in enumerate(keep) if k == 0]
+    nxt, sends, recvs, arrivals, copies = 0, [], [], [], []
+    for src, walker, dst, n in plan:
+        if src == rank:
+            sends.append((walker, dst))
+        elif dst == rank:
+            recvs.append((free[nxt], src))
+            arrivals.append((free[nxt], n))
+            nxt += 1
+    for slot, n in list(enumerate(keep)) + arrivals:
+        for _ in range(1, n):
+            copies.append((slot, free[nxt]))
+            nxt += 1
+    assert nxt == len(free)
+    return sends, recvs, copies
 
 
 def population_control(wset, r):

@@ -10,107 +10,81 @@ AfqmcEngine.walkers() returns and set_walkers() takes.
 
     offspring = comb(weights, r, ntot)                # the root's comb (population_control.hpp:34-65)
     plan = plan_walker_exchange(offspring, counts)    # population_control.hpp:73-133
+    sends, recvs, copies = local_moves(offspring, counts, rank)   # population_control.hpp:143-209
     SM, props = population_control(dist, SM, props, r, group)   # collective; r used on the root
 
-Within one rank the copies fill the slots of walkers that leave, in the order swap_walkers_async
-fills them (population_control.hpp:143-209), so one rank reproduces the single-rank comb exactly.
+The comb, the plan and each rank's moves are native host code behind the C ABI (sfq_comb_host,
+sfq_plan_walker_exchange, sfq_walker_moves), which needs no device; the data movement runs over
+torch.distributed.  Within one rank the copies fill the slots of walkers that leave, in the order
+swap_walkers_async fills them (population_control.hpp:143-209), so one rank reproduces the
+single-rank comb exactly.
 """
 import numpy as np
+
+from . import capi
 
 WEIGHT = 0  # property column of the weights
 
 
+def _i32(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.int32))
+
+
+def _cell():
+    """A one-int output of the C ABI."""
+    return np.zeros(1, dtype=np.int32)
+
+
+def _population(offspring, counts):
+    """offspring and counts as int32 arrays, checked against each other (the C ABI cannot see the
+    length of offspring, which must be sum(counts))."""
+    off, cnt = _i32(offspring).ravel(), _i32(counts).ravel()
+    if cnt.size == 0 or off.size != int(cnt.sum()):
+        raise capi.SafireError(2, f"{off.size} offspring entries for ranks holding {cnt.tolist()} walkers")
+    return off, cnt
+
+
 def comb(weights, r, num_target):
-    """The comb over |w| with the uniform r (population_control.hpp:34-65): offspring per walker."""
-    w = np.asarray(weights, dtype=np.float64)
-    cum = np.cumsum(w)  # std::partial_sum, sequential
-    total = float(cum[-1])
-    if not total > 1e-6:
-        raise RuntimeError(f"The total walker weight collapsed to {total}.")
-    last = len(w) - 1
-    while w[last] <= 0.0:
-        last -= 1
-    off = np.zeros(len(w), dtype=np.int64)
-    iw = ic = 0
-    while ic < num_target:
-        if (ic + r) * total / num_target < cum[iw] or iw == last:
-            off[iw] += 1
-            ic += 1
-        else:
-            iw += 1
-    return off
+    """The comb over |w| with the uniform r (population_control.hpp:34-65): offspring per walker.
+    Native host code (sfq_comb_host); raises SafireError WEIGHT_COLLAPSE when the total weight
+    collapses."""
+    w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+    off = np.zeros(w.size, dtype=np.int32)
+    capi.check(capi.lib().sfq_comb_host(capi.ptr(w), float(r), w.size, int(num_target), capi.ptr(off)))
+    return off.astype(np.int64)
 
 
 def plan_walker_exchange(offspring, counts):
     """(src rank, local walker, dst rank, copies) transfers realising offspring (rank-major over the
     global population, rank r holding counts[r] walkers): ranks with excess export their walkers with
-    the most copies first, filling the ranks with a deficit in rank order (population_control.hpp:73-133)."""
-    offspring = np.asarray(offspring, dtype=np.int64)
-    counts = [int(c) for c in counts]
-    if offspring.size != sum(counts) or int(offspring.sum()) != sum(counts):
-        raise ValueError("plan_walker_exchange: offspring does not match or preserve the population")
-    exports, deficits = [], []
-    first = 0
-    for r, nw in enumerate(counts):
-        local = offspring[first:first + nw]
-        excess = int(local.sum()) - nw
-        if excess < 0:
-            deficits.append([r, -excess])
-        if excess > 0:
-            order = sorted(range(nw), key=lambda i: -int(local[i]))  # stable: ties keep index order
-            k = 0
-            while excess > 0:
-                m = min(int(local[order[k]]), excess)
-                exports.append([r, order[k], m])
-                excess -= m
-                k += 1
-        first += nw
-    plan, d = [], 0
-    for src, walker, copies in exports:
-        while copies > 0:
-            n = min(copies, deficits[d][1])
-            plan.append((src, walker, deficits[d][0], n))
-            copies -= n
-            deficits[d][1] -= n
-            if deficits[d][1] == 0:
-                d += 1
-    return plan
+    the most copies first, filling the ranks with a deficit in rank order (population_control.hpp:73-133).
+    Native host code (sfq_plan_walker_exchange)."""
+    off, cnt = _population(offspring, counts)
+    cap = int(cnt.sum()) + cnt.size
+    out = np.zeros((cap, 4), dtype=np.int32)
+    n = _cell()
+    capi.check(capi.lib().sfq_plan_walker_exchange(capi.ptr(off), capi.ptr(cnt), cnt.size, capi.ptr(out), cap,
+                                                   capi.ptr(n)))
+    return [tuple(int(v) for v in row) for row in out[:int(n[0])]]
 
 
 def local_moves(offspring, counts, rank):
-    """This rank's part of swap_walkers_async (population_control.hpp:143-209): the plan, the sends
-    (local walker, dst), the receives (slot, src, copies) in plan order, and the local copies
-    (src slot, dst slot) to make after the receives, in the order the reference makes them."""
-    plan = plan_walker_exchange(offspring, counts)
-    nw = counts[rank]
-    first = sum(counts[:rank])
-    keep = [int(k) for k in np.asarray(offspring)[first:first + nw]]
-    for src, walker, dst, n in plan:
-        if src == rank:
-            keep[walker] -= n
-    free = [i for i in range(nw) if keep[i] == 0]
-    nxt = 0
-    sends, recvs, arrivals = [], [], []
-    for src, walker, dst, n in plan:
-        if src == rank:
-            sends.append((walker, dst))
-        elif dst == rank:
-            slot = free[nxt]
-            nxt += 1
-            recvs.append((slot, src))
-            arrivals.append((slot, n))
-    copies = []
-    for i in range(nw):
-        for _ in range(1, keep[i]):
-            copies.append((i, free[nxt]))
-            nxt += 1
-    for slot, n in arrivals:
-        for _ in range(1, n):
-            copies.append((slot, free[nxt]))
-            nxt += 1
-    if nxt != len(free):
-        raise RuntimeError(f"swap_walkers_async: {len(free) - nxt} slots left unfilled")
-    return plan, sends, recvs, copies
+    """This rank's part of swap_walkers_async (population_control.hpp:143-209): the sends (local
+    walker, dst) and receives (slot, src) in plan order, and the local copies (src slot, dst slot) to
+    make after the receives, in the order the reference makes them.  Native host code (sfq_walker_moves)."""
+    off, cnt = _population(offspring, counts)
+    if not 0 <= rank < cnt.size:
+        raise capi.SafireError(2, f"rank {rank} of {cnt.size}")
+    nw = int(cnt[rank])
+    sends = np.zeros((nw + cnt.size, 2), dtype=np.int32)
+    recvs = np.zeros((max(nw, 1), 2), dtype=np.int32)
+    copies = np.zeros((max(nw, 1), 2), dtype=np.int32)
+    ns, nr, nc = _cell(), _cell(), _cell()
+    capi.check(capi.lib().sfq_walker_moves(capi.ptr(off), capi.ptr(cnt), cnt.size, int(rank), capi.ptr(sends),
+                                           capi.ptr(ns), capi.ptr(recvs), capi.ptr(nr), capi.ptr(copies),
+                                           capi.ptr(nc)))
+    pairs = lambda a, n: [(int(x), int(y)) for x, y in a[:int(n[0])]]
+    return pairs(sends, ns), pairs(recvs, nr), pairs(copies, nc)
 
 
 def population_control(dist, SM, props, r, group=None):
@@ -145,7 +119,7 @@ def population_control(dist, SM, props, r, group=None):
     if dist:
         dist.broadcast(off, 0, group=group)
     offspring = off.numpy()
-    _, sends, recvs, copies = local_moves(offspring, counts, rank)
+    sends, recvs, copies = local_moves(offspring, counts, rank)
     sm_elems = int(np.prod(SM.shape[1:]))  # a rank may hold no walkers
     row = lambda i: torch.from_numpy(np.concatenate([SM[i].reshape(-1), props[:, i]]).view(np.float64))
     # a rank either sends or receives; both ends post in plan order (MPI's non-overtaking rule there)

@@ -44,7 +44,7 @@ def test_binding_covers_header():
 def test_last_error_and_version(lib):
     from safire_b200 import capi
     L = capi.lib()
-    assert L.sfq_abi_version() == 7
+    assert L.sfq_abi_version() == 8
     assert isinstance(L.sfq_last_error(), bytes)
 
 
@@ -70,18 +70,6 @@ def test_workspace_sizes_monotone():
     b = L.sfq_workspace_size(capi.OP_MIXED_DENSITY_MATRIX, 16, 40, 10, 0)
     assert 0 < a < b
     assert L.sfq_workspace_size(capi.OP_ENERGY, 8, 40, 10, 100) > 0
-
-
-def test_cpp_header_compiles():
-    import shutil
-    import subprocess
-    gxx = shutil.which("g++")
-    if gxx is None:
-        pytest.skip("no g++")
-    hpp = os.path.join(ROOT, "include", "safire_b200.hpp")
-    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-x", "c++", hpp],
-                       capture_output=True, text=True)
-    assert r.returncode == 0, r.stderr
 
 
 def test_group_and_tiles_argument_errors_without_gpu():
@@ -118,3 +106,49 @@ def test_cpp_header_compiles():
     r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", inc, "-x", "c++", "-"], input=src,
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_cpp_population_planning_runs_on_the_host(tmp_path):
+    """A C++ program using the reference-named comb and plan_walker_exchange of safire_b200.hpp,
+    linked against the library, runs on the CPU (host-only entry points) and agrees with the oracle."""
+    import shutil
+    import subprocess
+    import numpy as np
+    from oracle import afqmc_oracle as O
+    from safire_b200 import build
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    lib = build.build()
+    src = r'''
+#include <cstdio>
+#include "safire_b200.hpp"
+int main() {
+  std::vector<double> w;
+  for (int i = 0; i < 24; ++i) w.push_back((i % 5 == 0) ? 0.0 : 0.25 * ((i * 7) % 11 + 1));
+  std::vector<int> off = safire_b200::comb(w, 0.3125, 24);
+  for (int k : off) std::printf("%d ", k);
+  std::printf("\n");
+  for (auto t : safire_b200::plan_walker_exchange(off, {5, 9, 0, 10})) std::printf("%d %d %d %d\n", t.src, t.walker, t.dst, t.copies);
+  try {
+    safire_b200::plan_walker_exchange(off, {5, 9});
+  } catch (const safire_b200::Error& e) {
+    std::printf("error %d\n", e.code);
+  }
+  return 0;
+}
+'''
+    exe = str(tmp_path / "plan")
+    r = subprocess.run([gxx, "-std=c++17", "-I", os.path.join(ROOT, "include"), "-x", "c++", "-", "-x", "none", lib,
+                        "-o", exe, "-Wl,-rpath," + os.path.dirname(lib)], input=src, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, out.stderr
+    lines = out.stdout.strip().splitlines()
+    w = np.array([0.0 if i % 5 == 0 else 0.25 * ((i * 7) % 11 + 1) for i in range(24)])
+    off = O.comb(w, 0.3125, 24)
+    assert [int(v) for v in lines[0].split()] == off.tolist()
+    plan = [tuple(int(v) for v in ln.split()) for ln in lines[1:-1]]
+    assert plan == O.plan_walker_exchange(off, [5, 9, 0, 10]) and plan
+    assert lines[-1] == "error 2"

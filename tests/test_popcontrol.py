@@ -1,6 +1,7 @@
-"""Population control over walkers sharded across ranks (safire_b200.popcontrol): the exchange plan,
-one rank against the oracle's single-rank comb, and two gloo ranks on the CPU against one rank
-holding the whole population."""
+"""Population control over walkers sharded across ranks (safire_b200.popcontrol): the native host
+comb, exchange plan and per-rank moves (sfq_comb_host, sfq_plan_walker_exchange, sfq_walker_moves)
+against the oracle's restatement, one rank against the oracle's single-rank comb, and two gloo ranks
+on the CPU against one rank holding the whole population."""
 import os
 import socket
 
@@ -9,7 +10,14 @@ import pytest
 import torch.multiprocessing as mp
 
 from oracle import afqmc_oracle as O
+from safire_b200 import capi
 from safire_b200 import popcontrol as P
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    from safire_b200 import build
+    build.build()
 
 
 def _table(nw, seed, rows=5, cols=2):
@@ -25,10 +33,51 @@ def _table(nw, seed, rows=5, cols=2):
 
 def test_comb_matches_the_oracle():
     rng = np.random.default_rng(1)
-    for _ in range(20):
-        w = np.abs(rng.standard_normal(37)) ** 3
-        r = rng.uniform()
-        assert np.array_equal(P.comb(w, r, 37), O.comb(w, r, 37))
+    for n in (1, 2, 37, 500):
+        for _ in range(20):
+            w = np.abs(rng.standard_normal(n)) ** 3
+            w[rng.random(n) < 0.2] = 0.0
+            if not w.sum() > 1e-6:
+                w[-1] = 1.0
+            r = rng.uniform()
+            for target in (n, max(1, n // 2), 2 * n):
+                assert np.array_equal(P.comb(w, r, target), O.comb(w, r, target))
+
+
+def test_comb_trailing_dead_walkers_and_collapse():
+    """Teeth past the last live walker land on it (the iw == last clause), and a collapsed total
+    weight is an error, not a division by zero."""
+    w = np.array([0.5, 2.0, 0.0, 0.0])
+    assert np.array_equal(P.comb(w, 0.999999, 4), O.comb(w, 0.999999, 4))
+    assert P.comb(w, 0.999999, 4)[2:].sum() == 0
+    with pytest.raises(capi.SafireError, match="WEIGHT_COLLAPSE"):
+        P.comb(np.full(5, 1e-8), 0.5, 5)
+    with pytest.raises(capi.SafireError, match="ARG"):
+        P.comb(w, 1.0, 4)
+
+
+def test_plan_and_moves_match_the_oracle():
+    rng = np.random.default_rng(11)
+    for _ in range(200):
+        nranks = int(rng.integers(1, 7))
+        counts = [int(c) for c in rng.integers(0, 9, nranks)]
+        if sum(counts) == 0:
+            counts[0] = 3
+        ntot = sum(counts)
+        w = np.abs(rng.standard_normal(ntot)) ** int(rng.integers(1, 5))
+        off = O.comb(w, rng.uniform(), ntot)
+        assert P.plan_walker_exchange(off, counts) == O.plan_walker_exchange(off, counts)
+        for r in range(nranks):
+            assert P.local_moves(off, counts, r) == O.walker_moves(off, counts, r)
+
+
+def test_plan_rejects_a_population_that_changes():
+    with pytest.raises(capi.SafireError, match="ARG"):
+        P.plan_walker_exchange([2, 2, 1], [2, 2])       # 3 entries for 4 walkers
+    with pytest.raises(capi.SafireError, match="ARG"):
+        P.plan_walker_exchange([2, 0, 0, 1], [2, 2])    # 3 copies of 4 walkers
+    with pytest.raises(capi.SafireError, match="ARG"):
+        P.local_moves([1, 1, 1, 1], [2, 2], 2)          # no rank 2
 
 
 @pytest.mark.parametrize("counts", [[6, 6], [5, 7, 4], [1, 9], [8, 0, 8]])
