@@ -196,6 +196,9 @@ def test_comb_bit_exact():
         r = float(rng.uniform())
         off = host(A.comb(cu(w), r))
         assert np.array_equal(off, O.comb(w, r, n))
+        # the host comb a sharded run's root uses draws the same offspring
+        from safire_b200 import popcontrol
+        assert np.array_equal(popcontrol.comb(w, r, n), off)
 
 
 def test_comb_weight_collapse():
