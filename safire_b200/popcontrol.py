@@ -87,6 +87,15 @@ def local_moves(offspring, counts, rank):
     return pairs(sends, ns), pairs(recvs, nr), pairs(copies, nc)
 
 
+def comm_device(dist, group=None):
+    """The device a collective of this group takes its tensors on: the current CUDA device for
+    NCCL (which moves only device memory), the host otherwise (gloo)."""
+    import torch
+    if dist is not None and dist.get_backend(group) == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
 def population_control(dist, SM, props, r, group=None):
     """The collective population control on this rank's walker table (SM (nw, rows, cols) complex,
     props (8, nw) complex); r is the root's comb uniform (ignored elsewhere).  Returns the new table:
@@ -97,9 +106,10 @@ def population_control(dist, SM, props, r, group=None):
     nw = SM.shape[0]
     rank = dist.get_rank(group) if dist else 0
     size = dist.get_world_size(group) if dist else 1
+    dev = comm_device(dist, group)
     if dist:
-        cnt = [torch.zeros(1, dtype=torch.int64) for _ in range(size)]
-        dist.all_gather(cnt, torch.tensor([nw], dtype=torch.int64), group=group)
+        cnt = [torch.zeros(1, dtype=torch.int64, device=dev) for _ in range(size)]
+        dist.all_gather(cnt, torch.tensor([nw], dtype=torch.int64, device=dev), group=group)
         counts = [int(c.item()) for c in cnt]
     else:
         counts = [nw]
@@ -108,27 +118,28 @@ def population_control(dist, SM, props, r, group=None):
         mx = max(counts)
         buf = torch.zeros(mx, dtype=torch.float64)
         buf[:nw] = torch.from_numpy(w)
-        allw = [torch.zeros(mx, dtype=torch.float64) for _ in range(size)]
-        dist.all_gather(allw, buf, group=group)
-        weights = np.concatenate([a.numpy()[:c] for a, c in zip(allw, counts)])
+        allw = [torch.zeros(mx, dtype=torch.float64, device=dev) for _ in range(size)]
+        dist.all_gather(allw, buf.to(dev), group=group)
+        weights = np.concatenate([a.cpu().numpy()[:c] for a, c in zip(allw, counts)])
     else:
         weights = w
     off = torch.zeros(sum(counts), dtype=torch.int64)
     if rank == 0:
         off = torch.from_numpy(comb(weights, r, sum(counts)))
     if dist:
+        off = off.to(dev)
         dist.broadcast(off, 0, group=group)
-    offspring = off.numpy()
+    offspring = off.cpu().numpy()
     sends, recvs, copies = local_moves(offspring, counts, rank)
     sm_elems = int(np.prod(SM.shape[1:]))  # a rank may hold no walkers
-    row = lambda i: torch.from_numpy(np.concatenate([SM[i].reshape(-1), props[:, i]]).view(np.float64))
+    row = lambda i: torch.from_numpy(np.concatenate([SM[i].reshape(-1), props[:, i]]).view(np.float64)).to(dev)
     # a rank either sends or receives; both ends post in plan order (MPI's non-overtaking rule there)
     for walker, dst in sends:
         dist.send(row(walker).contiguous(), dst, group=group)
     for slot, src in recvs:
-        t = torch.empty(2 * (sm_elems + props.shape[0]), dtype=torch.float64)
+        t = torch.empty(2 * (sm_elems + props.shape[0]), dtype=torch.float64, device=dev)
         dist.recv(t, src, group=group)
-        v = t.numpy().view(np.complex128)
+        v = t.cpu().numpy().view(np.complex128)
         SM[slot] = v[:sm_elems].reshape(SM.shape[1:])
         props[:, slot] = v[sm_elems:]
     for src, dst in copies:

@@ -16,7 +16,7 @@ import math
 
 import numpy as np
 
-from .popcontrol import engine_population_control
+from .popcontrol import comm_device, engine_population_control
 
 
 def _allreduce(dist, values, group=None):
@@ -25,9 +25,9 @@ def _allreduce(dist, values, group=None):
     if dist is None:
         return v
     import torch
-    t = torch.from_numpy(v.view(np.float64).copy())
+    t = torch.from_numpy(v.view(np.float64).copy()).to(comm_device(dist, group))
     dist.all_reduce(t, group=group)
-    return t.numpy().view(np.complex128)
+    return t.cpu().numpy().view(np.complex128)
 
 
 def global_pseudo_energy(dist, engine, group=None):
