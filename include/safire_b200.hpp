@@ -14,6 +14,7 @@
 #include <complex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "safire_b200.h"
@@ -87,6 +88,31 @@ inline std::vector<walker_transfer> plan_walker_exchange(const std::vector<int>&
                                  reinterpret_cast<int*>(plan.data()), int(plan.size()), &n));
   plan.resize(n);
   return plan;
+}
+// rank's part of swap_walkers_async: sends (walker, dst) and receives (slot, src) in plan order,
+// then local copies (src slot, dst slot)
+struct walker_moves_t {
+  std::vector<std::pair<int, int>> sends, recvs, copies;
+};
+inline walker_moves_t walker_moves(const std::vector<int>& offspring, const std::vector<int>& counts, int rank) {
+  long ntot = 0;
+  for (int c : counts) ntot += c;
+  if (long(offspring.size()) != ntot || rank < 0 || rank >= int(counts.size()))
+    throw Error(SFQ_ERR_ARG, "walker_moves: offspring or rank does not match the ranks' walkers");
+  static_assert(sizeof(std::pair<int, int>) == 2 * sizeof(int), "moves are the ABI's int pairs");
+  int nw = counts[rank];
+  walker_moves_t m;
+  m.sends.resize(size_t(nw) + counts.size());
+  m.recvs.resize(size_t(nw) + 1);
+  m.copies.resize(size_t(nw) + 1);
+  int ns = 0, nr = 0, nc = 0;
+  check(sfq_walker_moves(offspring.data(), counts.data(), int(counts.size()), rank,
+                         reinterpret_cast<int*>(m.sends.data()), &ns, reinterpret_cast<int*>(m.recvs.data()), &nr,
+                         reinterpret_cast<int*>(m.copies.data()), &nc));
+  m.sends.resize(ns);
+  m.recvs.resize(nr);
+  m.copies.resize(nc);
+  return m;
 }
 
 // Real3IndexFactorization over caller-owned device tensors (CLOSED, ndet = 1)

@@ -130,6 +130,15 @@ int main() {
   for (int k : off) std::printf("%d ", k);
   std::printf("\n");
   for (auto t : safire_b200::plan_walker_exchange(off, {5, 9, 0, 10})) std::printf("%d %d %d %d\n", t.src, t.walker, t.dst, t.copies);
+  for (int r = 0; r < 4; ++r) {
+    auto m = safire_b200::walker_moves(off, {5, 9, 0, 10}, r);
+    std::printf("moves %d", r);
+    for (auto* v : {&m.sends, &m.recvs, &m.copies}) {
+      std::printf(" |");
+      for (auto p : *v) std::printf(" %d %d", p.first, p.second);
+    }
+    std::printf("\n");
+  }
   try {
     safire_b200::plan_walker_exchange(off, {5, 9});
   } catch (const safire_b200::Error& e) {
@@ -149,6 +158,11 @@ int main() {
     w = np.array([0.0 if i % 5 == 0 else 0.25 * ((i * 7) % 11 + 1) for i in range(24)])
     off = O.comb(w, 0.3125, 24)
     assert [int(v) for v in lines[0].split()] == off.tolist()
-    plan = [tuple(int(v) for v in ln.split()) for ln in lines[1:-1]]
+    moves = [ln for ln in lines if ln.startswith("moves")]
+    plan = [tuple(int(v) for v in ln.split()) for ln in lines[1:-1] if not ln.startswith("moves")]
     assert plan == O.plan_walker_exchange(off, [5, 9, 0, 10]) and plan
-    assert lines[-1] == "error 2"
+    for r, ln in enumerate(moves):
+        parts = ln.split("|")[1:]
+        got = [list(zip(*[iter(int(v) for v in p.split())] * 2)) for p in parts]
+        assert got == [list(x) for x in O.walker_moves(off, [5, 9, 0, 10], r)]
+    assert len(moves) == 4 and lines[-1] == "error 2"
