@@ -131,14 +131,15 @@ def _rank(rank, world, port, counts, q):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("counts", [[9, 9], [6, 11], [0, 12]])
-def test_two_ranks_equal_one_rank_holding_everything(counts):
-    """The walkers two gloo ranks end with are, together, the population one rank ends with, and each
-    rank keeps its own count; the weights become unit-modulus."""
+@pytest.mark.parametrize("counts", [[9, 9], [6, 11], [0, 12], [3, 10, 5], [7, 0, 9]])
+def test_ranks_equal_one_rank_holding_everything(counts):
+    """The walkers two or three gloo ranks end with are, together, the population one rank ends with,
+    and each rank keeps its own count; the weights become unit-modulus."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, counts, q)) for r in range(2)]
+    world = len(counts)
+    procs = [ctx.Process(target=_rank, args=(r, world, port, counts, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = sorted((q.get(timeout=120) for _ in procs), key=lambda t: t[0])
