@@ -166,3 +166,49 @@ int main() {
         got = [list(zip(*[iter(int(v) for v in p.split())] * 2)) for p in parts]
         assert got == [list(x) for x in O.walker_moves(off, [5, 9, 0, 10], r)]
     assert len(moves) == 4 and lines[-1] == "error 2"
+
+
+def test_c_program_links_and_calls_the_host_entry_points(tmp_path):
+    """include/safire_b200.h is valid C99 (-pedantic), and a C program linked against the library
+    calls the host-only entry points (what a cgo or plain-C binding does) and agrees with the oracle."""
+    import shutil
+    import subprocess
+    import numpy as np
+    from oracle import afqmc_oracle as O
+    from safire_b200 import build
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no gcc")
+    lib = build.build()
+    src = r'''
+#include <stdio.h>
+#include "safire_b200.h"
+int main(void) {
+  double w[12];
+  int off[12], counts[3] = {4, 5, 3}, plan[4 * 15], n = 0, i;
+  for (i = 0; i < 12; ++i) w[i] = (i == 2 || i == 9) ? 0.0 : 0.5 + 0.375 * ((i * 5) % 7);
+  if (sfq_abi_version() != 8) return 3;
+  if (sfq_comb_host(w, 0.71, 12, 12, off) != SFQ_OK) return 4;
+  for (i = 0; i < 12; ++i) printf("%d ", off[i]);
+  printf("\n");
+  if (sfq_plan_walker_exchange(off, counts, 3, plan, 15, &n) != SFQ_OK) return 5;
+  for (i = 0; i < n; ++i) printf("%d %d %d %d\n", plan[4 * i], plan[4 * i + 1], plan[4 * i + 2], plan[4 * i + 3]);
+  if (sfq_plan_walker_exchange(off, counts, 3, plan, 0, &n) != SFQ_ERR_WORKSPACE || n == 0) return 6;
+  printf("%s\n", sfq_last_error());
+  return 0;
+}
+'''
+    exe = str(tmp_path / "cplan")
+    r = subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        "-x", "c", "-", "-x", "none", lib, "-o", exe, "-Wl,-rpath," + os.path.dirname(lib)],
+                       input=src, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
+    lines = out.stdout.strip().splitlines()
+    w = np.array([0.0 if i in (2, 9) else 0.5 + 0.375 * ((i * 5) % 7) for i in range(12)])
+    off = O.comb(w, 0.71, 12)
+    assert [int(v) for v in lines[0].split()] == off.tolist()
+    plan = [tuple(int(v) for v in ln.split()) for ln in lines[1:-1]]
+    assert plan == O.plan_walker_exchange(off, [4, 5, 3]) and plan
+    assert "room for 0" in lines[-1]
