@@ -18,7 +18,7 @@ from safire_b200 import capi
 from safire_b200 import sharded as S
 from tests.golden_io import bh_snapshot
 
-NW = 16  # global walkers
+NW = 24  # global walkers (divisible by 2 and 3 ranks)
 FIELDS = dict(zip(capi.PROPS, ("weight", "phase", "pseudo_eloc", "e1", "exx", "ej", "ovlp", "theta")))
 
 
@@ -88,11 +88,11 @@ def _rank(rank, world, port, pop_interval, q):
     dist.destroy_process_group()
 
 
-def _two_ranks(pop_interval):
+def _ranks(world, pop_interval):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, pop_interval, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, pop_interval, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = sorted((q.get(timeout=300) for _ in procs), key=lambda t: t[0])
@@ -102,8 +102,9 @@ def _two_ranks(pop_interval):
     return out
 
 
-def test_two_ranks_without_exchange_equal_one_rank():
-    out = _two_ranks(pop_interval=1000)
+@pytest.mark.parametrize("world", [2, 3])
+def test_ranks_without_exchange_equal_one_rank(world):
+    out = _ranks(world, pop_interval=1000)
     E1, m1, _ = _run(0, 1, 1000)
     for _, Eshift, meas, _ in out:
         assert abs(Eshift - E1) < 1e-10 * abs(E1)
@@ -113,10 +114,12 @@ def test_two_ranks_without_exchange_equal_one_rank():
                 assert abs(a[k] - b[k]) < 1e-10 * max(1.0, abs(b[k])), k
 
 
-def test_two_ranks_with_exchange_agree_and_keep_their_counts():
-    out = _two_ranks(pop_interval=2)
-    (_, E_a, m_a, w_a), (_, E_b, m_b, w_b) = out
-    assert w_a == w_b == NW // 2
-    assert E_a == E_b and m_a == m_b                   # every rank sees the global reductions
+@pytest.mark.parametrize("world", [2, 3])
+def test_ranks_with_exchange_agree_and_keep_their_counts(world):
+    out = _ranks(world, pop_interval=2)
+    (_, E_a, m_a, w_a) = out[0]
+    for _, E_b, m_b, w_b in out:
+        assert w_b == NW // world
+        assert E_a == E_b and m_a == m_b               # every rank sees the global reductions
     assert all(np.isfinite(m["Energy"].real) for _, m in m_a)
     assert all(abs(m["TotalWeight"].real - NW) < 1e-9 for s, m in m_a if (s % 2) == 0)  # after a comb
