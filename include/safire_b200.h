@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 8 */
+int sfq_abi_version(void); /* 9 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -163,13 +163,16 @@ int sfq_plan_walker_exchange(const int* offspring, const int* counts, int nranks
                              int* ntransfers);
 
 /* rank's part of swap_walkers_async (population_control.hpp:143-209), all as (int, int) pairs:
- *   sends   (local walker, dst rank), in plan order          room for counts[rank] + nranks pairs
- *   recvs   (slot, src rank), in plan order                   room for counts[rank] pairs
- *   copies  (src slot, dst slot), made after the receives     room for counts[rank] pairs
+ *   sends   (local walker, dst rank), in plan order          at most counts[rank] + nranks pairs
+ *   recvs   (slot, src rank), in plan order                   at most counts[rank] pairs
+ *   copies  (src slot, dst slot), made after the receives     at most counts[rank] pairs
+ * max_sends, max_recvs and max_copies are the pairs each array has room for.  When one is too
+ * small nothing is written, the three counts are set to the lengths needed and SFQ_ERR_WORKSPACE
+ * is returned (a walker exported to several deficit ranks makes more sends than walkers).
  * A walker received into a slot replaces the walker that left it; local copies fill the remaining
  * free slots, the kept walkers' extra copies (in index order) first, then the received walkers'. */
-int sfq_walker_moves(const int* offspring, const int* counts, int nranks, int rank, int* sends, int* nsends,
-                     int* recvs, int* nrecvs, int* copies, int* ncopies);
+int sfq_walker_moves(const int* offspring, const int* counts, int nranks, int rank, int* sends, int max_sends,
+                     int* nsends, int* recvs, int max_recvs, int* nrecvs, int* copies, int max_copies, int* ncopies);
 
 /* Mixed-precision tensor-core GEMM (tcgen05, split BF16, FP32 accumulation), no reference
  * counterpart: C[b] (M x N, fp32) = A[b] (M x K) * B[b] (N x K)^T with A, B fp64 on the device

@@ -107,8 +107,9 @@ inline walker_moves_t walker_moves(const std::vector<int>& offspring, const std:
   m.copies.resize(size_t(nw) + 1);
   int ns = 0, nr = 0, nc = 0;
   check(sfq_walker_moves(offspring.data(), counts.data(), int(counts.size()), rank,
-                         reinterpret_cast<int*>(m.sends.data()), &ns, reinterpret_cast<int*>(m.recvs.data()), &nr,
-                         reinterpret_cast<int*>(m.copies.data()), &nc));
+                         reinterpret_cast<int*>(m.sends.data()), int(m.sends.size()), &ns,
+                         reinterpret_cast<int*>(m.recvs.data()), int(m.recvs.size()), &nr,
+                         reinterpret_cast<int*>(m.copies.data()), int(m.copies.size()), &nc));
   m.sends.resize(ns);
   m.recvs.resize(nr);
   m.copies.resize(nc);

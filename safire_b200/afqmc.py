@@ -186,6 +186,7 @@ class AfqmcEngine:
             check(lib().sfq_engine_create(ctypes.byref(handle), ctypes.byref(p), h.ctypes.data, L.ctypes.data,
                                           P.ctypes.data))
         self.h = handle
+        self.nbp = 0  # back-propagation ring length (enable_back_propagation)
 
     def close(self):
         if self.h:
@@ -281,6 +282,7 @@ class AfqmcEngine:
     def enable_back_propagation(self, nbp):
         """Keep the fields and weight factors of the last nbp steps per walker (resize_bp)."""
         check(lib().sfq_engine_enable_back_propagation(self.h, int(nbp)))
+        self.nbp = int(nbp)
 
     def bp_anchor(self):
         check(lib().sfq_engine_bp_anchor(self.h))

@@ -98,7 +98,7 @@ _SIGS = {
     "sfq_comb": ([_VP, _D, _I, _VP, _VP], _I),
     "sfq_comb_host": ([_VP, _D, _I, _I, _VP], _I),
     "sfq_plan_walker_exchange": ([_VP, _VP, _I, _VP, _I, _VP], _I),
-    "sfq_walker_moves": ([_VP, _VP, _I, _I, _VP, _VP, _VP, _VP, _VP, _VP], _I),
+    "sfq_walker_moves": ([_VP, _VP, _I, _I, _VP, _I, _VP, _VP, _I, _VP, _VP, _I, _VP], _I),
     "sfq_gemm_split_bf16": ([_VP, _VP, _VP, _I, _I, _I, _I, _I, _I, _I, _I, _VP], _I),
     "sfq_gemm_bf16_planes": ([ctypes.POINTER(_VP), ctypes.POINTER(_VP), _I, _VP, _I, _I, _I, _I, ctypes.c_long,
                               ctypes.c_long, ctypes.c_float, ctypes.c_float, _I, _VP], _I),

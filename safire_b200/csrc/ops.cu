@@ -304,7 +304,7 @@ constexpr long kEnergyChunkElems = 1L << 27;  // 2 GiB of complex T per chunk at
 
 extern "C" {
 
-int sfq_abi_version(void) { return 8; }
+int sfq_abi_version(void) { return 9; }
 
 unsigned long long sfq_launch_count(void) { return g_launches.load(); }
 

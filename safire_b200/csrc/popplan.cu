@@ -126,14 +126,15 @@ int sfq_plan_walker_exchange(const int* offspring, const int* counts, int nranks
   return SFQ_OK;
 }
 
-int sfq_walker_moves(const int* offspring, const int* counts, int nranks, int rank, int* sends, int* nsends,
-                     int* recvs, int* nrecvs, int* copies, int* ncopies) {
+int sfq_walker_moves(const int* offspring, const int* counts, int nranks, int rank, int* sends, int max_sends,
+                     int* nsends, int* recvs, int max_recvs, int* nrecvs, int* copies, int max_copies, int* ncopies) {
   long ntot = 0;
   if (int rc = check_population(offspring, counts, nranks, &ntot)) return rc;
   if (rank < 0 || rank >= nranks) return record_error(SFQ_ERR_ARG, "walker_moves: rank %d of %d", rank, nranks);
   if (!nsends || !nrecvs || !ncopies) return record_error(SFQ_ERR_ARG, "walker_moves: null pointer");
+  if ((max_sends > 0 && !sends) || (max_recvs > 0 && !recvs) || (max_copies > 0 && !copies))
+    return record_error(SFQ_ERR_ARG, "walker_moves: null pointer");
   int nw = counts[rank];
-  if (nw > 0 && (!sends || !recvs || !copies)) return record_error(SFQ_ERR_ARG, "walker_moves: null pointer");
   long first = 0;
   for (int r = 0; r < rank; ++r) first += counts[r];
   std::vector<Transfer> p = plan(offspring, counts, nranks);
@@ -146,6 +147,23 @@ int sfq_walker_moves(const int* offspring, const int* counts, int nranks, int ra
     if (keep[i] == 0) freed.push_back(i);
   size_t next = 0;
   int ns = 0, nr = 0, nc = 0;
+  *nsends = *nrecvs = *ncopies = 0;
+  // the lists' lengths are counted first, so an undersized array is reported before anything is written
+  {
+    int need_s = 0, need_r = 0;
+    for (const Transfer& t : p) {
+      if (t.src == rank) ++need_s;
+      else if (t.dst == rank) ++need_r;
+    }
+    const int need_c = int(freed.size()) - need_r;  // every freed slot not taken by a receive is a copy
+    if (need_s > max_sends || need_r > max_recvs || need_c > max_copies) {
+      *nsends = need_s;
+      *nrecvs = need_r;
+      *ncopies = need_c < 0 ? 0 : need_c;
+      return record_error(SFQ_ERR_WORKSPACE, "walker_moves: %d sends, %d receives, %d copies; room for %d, %d, %d",
+                          need_s, need_r, need_c, max_sends, max_recvs, max_copies);
+    }
+  }
   std::vector<std::pair<int, int>> arrivals;  // (slot, copies) of the walkers received
   // the sends and receives in plan order: both ends post them in the same order
   for (const Transfer& t : p) {

@@ -81,8 +81,8 @@ def local_moves(offspring, counts, rank):
     copies = np.zeros((max(nw, 1), 2), dtype=np.int32)
     ns, nr, nc = _cell(), _cell(), _cell()
     capi.check(capi.lib().sfq_walker_moves(capi.ptr(off), capi.ptr(cnt), cnt.size, int(rank), capi.ptr(sends),
-                                           capi.ptr(ns), capi.ptr(recvs), capi.ptr(nr), capi.ptr(copies),
-                                           capi.ptr(nc)))
+                                           len(sends), capi.ptr(ns), capi.ptr(recvs), len(recvs), capi.ptr(nr),
+                                           capi.ptr(copies), len(copies), capi.ptr(nc)))
     pairs = lambda a, n: [(int(x), int(y)) for x, y in a[:int(n[0])]]
     return pairs(sends, ns), pairs(recvs, nr), pairs(copies, nc)
 
@@ -152,9 +152,17 @@ def population_control(dist, SM, props, r, group=None):
 
 def engine_population_control(dist, engine, r, group=None):
     """population_control for an AfqmcEngine whose walkers are this rank's share of the population:
-    the engine's walker table goes through the collective comb and exchange and back (set_walkers)."""
+    the engine's walker table goes through the collective comb and exchange and back (set_walkers).
+
+    Only the Slater matrices and the property columns travel.  An engine that keeps back-propagation
+    history (enable_back_propagation) also holds per-walker field rings, weight factors and anchored
+    walkers, which the reference moves with the walker (copy_walker, population_control.hpp:243-247);
+    those would stay behind here and pair each walker with another walker's history, so such an
+    engine is refused."""
+    if getattr(engine, "nbp", 0) > 0:
+        raise capi.SafireError(3, "sharded population control does not move back-propagation history; "
+                                  "run back propagation on one rank (engine.population_control)")
     SM, pr = engine.walkers()
-    from . import capi
     props = np.stack([pr[k] for k in capi.PROPS])
     SM, props = population_control(dist, SM, props, r, group)
     engine.set_walkers(SM, {k: props[i] for i, k in enumerate(capi.PROPS)})

@@ -115,7 +115,9 @@ def multidet_case(fn, system, ham_file, wfn_file, case, walker_type, out_name):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SAFIRE_REFERENCE_ROOT", "")
+    if not src or not os.path.isdir(src):
+        sys.exit("usage: make_bh_snapshot.py <SAFIRE source tree> (or set SAFIRE_REFERENCE_ROOT)")
     fn = os.path.join(src, "tests", "functional")
     snapshot_case(fn, "BH", "afqmc_H_rhf_closed.h5", "afqmc_rhf_nomsd.h5", "dense_rhf_basis_closed/rhf_nomsd/closed",
                   "CLOSED", "bh_rhf_closed_snapshot.npz")

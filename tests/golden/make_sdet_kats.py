@@ -16,7 +16,9 @@ import os
 import re
 import sys
 
-SRC_DEFAULT = "/root/reference/tests/test_sdet_ops.cpp"
+# tests/test_sdet_ops.cpp under the SAFIRE source tree named by SAFIRE_REFERENCE_ROOT
+SRC_DEFAULT = (os.path.join(os.environ["SAFIRE_REFERENCE_ROOT"], "tests", "test_sdet_ops.cpp")
+               if os.environ.get("SAFIRE_REFERENCE_ROOT") else "")
 NUM = r"[-+]?\s*\d+(?:\.\d*)?(?:[eE][-+]?\d+)?"
 CPLX = re.compile(rf"({NUM})\s*([-+])\s*(\d+(?:\.\d*)?(?:[eE][-+]?\d+)?)i")
 
@@ -50,6 +52,8 @@ def _scalar_type(text, name):
 
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else SRC_DEFAULT
+    if not src or not os.path.isfile(src):
+        sys.exit("usage: make_sdet_kats.py <path/to/test_sdet_ops.cpp> (or set SAFIRE_REFERENCE_ROOT)")
     text = open(src).read()
     kats = {
         "source": "tests/test_sdet_ops.cpp (SAFIRE)",

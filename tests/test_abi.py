@@ -44,7 +44,7 @@ def test_binding_covers_header():
 def test_last_error_and_version(lib):
     from safire_b200 import capi
     L = capi.lib()
-    assert L.sfq_abi_version() == 8
+    assert L.sfq_abi_version() == 9
     assert isinstance(L.sfq_last_error(), bytes)
 
 
@@ -187,7 +187,7 @@ int main(void) {
   double w[12];
   int off[12], counts[3] = {4, 5, 3}, plan[4 * 15], n = 0, i;
   for (i = 0; i < 12; ++i) w[i] = (i == 2 || i == 9) ? 0.0 : 0.5 + 0.375 * ((i * 5) % 7);
-  if (sfq_abi_version() != 8) return 3;
+  if (sfq_abi_version() != 9) return 3;
   if (sfq_comb_host(w, 0.71, 12, 12, off) != SFQ_OK) return 4;
   for (i = 0; i < 12; ++i) printf("%d ", off[i]);
   printf("\n");
@@ -195,6 +195,20 @@ int main(void) {
   for (i = 0; i < n; ++i) printf("%d %d %d %d\n", plan[4 * i], plan[4 * i + 1], plan[4 * i + 2], plan[4 * i + 3]);
   if (sfq_plan_walker_exchange(off, counts, 3, plan, 0, &n) != SFQ_ERR_WORKSPACE || n == 0) return 6;
   printf("%s\n", sfq_last_error());
+  {
+    /* a rank's moves: exact room succeeds, one pair short reports the lengths and writes nothing */
+    int sends[2 * 8], recvs[2 * 8], copies[2 * 8], ns = -1, nr = -1, nc = -1, r, ns2, nr2, nc2;
+    for (r = 0; r < 3; ++r) {
+      if (sfq_walker_moves(off, counts, 3, r, sends, 8, &ns, recvs, 8, &nr, copies, 8, &nc) != SFQ_OK) return 7;
+      printf("moves %d %d %d %d\n", r, ns, nr, nc);
+      if (ns > 0) {
+        sends[0] = -7;
+        if (sfq_walker_moves(off, counts, 3, r, sends, ns - 1, &ns2, recvs, 8, &nr2, copies, 8, &nc2) !=
+                SFQ_ERR_WORKSPACE || ns2 != ns || nr2 != nr || nc2 != nc || sends[0] != -7)
+          return 8;
+      }
+    }
+  }
   return 0;
 }
 '''
@@ -209,6 +223,12 @@ int main(void) {
     w = np.array([0.0 if i in (2, 9) else 0.5 + 0.375 * ((i * 5) % 7) for i in range(12)])
     off = O.comb(w, 0.71, 12)
     assert [int(v) for v in lines[0].split()] == off.tolist()
+    moves = [ln for ln in lines if ln.startswith("moves")]
+    lines = [ln for ln in lines if not ln.startswith("moves")]
     plan = [tuple(int(v) for v in ln.split()) for ln in lines[1:-1]]
     assert plan == O.plan_walker_exchange(off, [4, 5, 3]) and plan
     assert "room for 0" in lines[-1]
+    assert len(moves) == 3
+    for r, ln in enumerate(moves):
+        s_, rv, cp = O.walker_moves(off, [4, 5, 3], r)
+        assert [int(v) for v in ln.split()[1:]] == [r, len(s_), len(rv), len(cp)]

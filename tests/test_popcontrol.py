@@ -154,3 +154,18 @@ def test_ranks_equal_one_rank_holding_everything(counts):
     key = lambda S, pr: sorted(tuple(np.round(np.concatenate([S[i].ravel(), pr[:, i]]), 12)) for i in range(S.shape[0]))
     both = key(np.concatenate([o[1] for o in out]), np.concatenate([o[2] for o in out], axis=1))
     assert both == key(SM1, pr1)
+
+
+def test_engine_with_back_propagation_is_refused():
+    """Sharded population control moves only the Slater matrices and properties: an engine that keeps
+    back-propagation history (fields, weight factors, anchors per walker) is refused before any
+    walker is read or any message is sent."""
+    class FakeEngine:
+        nbp = 4
+
+        def walkers(self):
+            raise AssertionError("the walkers must not be read")
+
+    with pytest.raises(capi.SafireError) as ei:
+        P.engine_population_control(None, FakeEngine(), 0.5)
+    assert ei.value.code == 3

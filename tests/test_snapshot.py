@@ -22,7 +22,9 @@ from oracle import afqmc_oracle as O
 from oracle.mt19937 import MT19937, HostRandomGenerator, split_seed
 from tests.golden_io import SNAPSHOT_OBSERVABLES, bh_snapshot, oracle_hamiltonian, snapshot, snapshot_match
 
-REF = "/root/reference/tests/functional"
+# the SAFIRE source tree, when present on this machine (only then are its own input files read)
+REF_ROOT = os.environ.get("SAFIRE_REFERENCE_ROOT", "")
+REF = os.path.join(REF_ROOT, "tests", "functional") if REF_ROOT else ""
 
 
 def test_mt19937_known_answers():
@@ -89,7 +91,8 @@ def test_snapshot_detects_a_planted_mistake():
     assert snapshot_match(series["Energy"], snap["recorded"]["Energy"], O.rebinned_average) is None
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="the reference's input files are not on this machine")
+@pytest.mark.skipif(not (REF and os.path.isdir(REF)),
+                    reason="SAFIRE_REFERENCE_ROOT does not name the reference tree on this machine")
 def test_loaders_read_reference_files():
     from safire_b200.h5read import H5File
     from safire_b200.inputs import InputError, load_dense_hamiltonian, load_nomsd_trial
@@ -152,7 +155,8 @@ def test_oracle_reproduces_recorded_rdms(case):
         assert snapshot_match(series[k], snap["recorded"][k], O.rebinned_average) is not None, k
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="the reference's files are not on this machine")
+@pytest.mark.skipif(not (REF and os.path.isdir(REF)),
+                    reason="SAFIRE_REFERENCE_ROOT does not name the reference tree on this machine")
 def test_h5read_reads_every_reference_file_and_chunked_data():
     """The reader parses every HDF5 file of the reference tree (groups, datasets, attributes), and its
     chunked, deflate-compressed datasets decode to consistent data: in a recorded results file the
