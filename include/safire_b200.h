@@ -192,6 +192,21 @@ int sfq_gemm_bf16_planes(const void* const* A, const void* const* B, int nplanes
 /* the planes of n doubles: p0 = bf16(x), p1 = bf16(x - p0), p2 = bf16(x - p0 - p1); p1, p2 may be NULL */
 int sfq_split_bf16(const double* src, long n, void* p0, void* p1, void* p2, void* stream);
 
+/* Exact-accumulation tensor-core products from int8 fixed-point slices (tcgen05 kind::i8), no
+ * reference counterpart (the reference's products are FP64 BLAS calls): every row r of A (M x K)
+ * and of B (N x K), device doubles, is held as 2^e_r (q1 + 2^-8 q2 + 2^-16 q3) with int8 slices
+ * q, rounded to nearest from the row's largest entry (|q1| <= 127); the slice pairs of combined
+ * order < nslices are multiplied and summed exactly in int32, combined exactly in FP64 and rounded
+ * once: C = A B^T (FP32, M x N).  ksplit > 1 writes the partial products of ksplit K ranges at
+ * C + s * M * N.  tile_n: 64, 128 or 160 (0: automatic). */
+int sfq_gemm_int8_slices(const double* A, const double* B, float* C, int M, int N, int K, int nslices, int tile_n,
+                         int ksplit, void* stream);
+/* the Taylor term's product in the same arithmetic: C[c][w][a][j] = part c of sum_i A[w][a][i] V[w][j][i]
+ * (A (W, N, M), V (W, M, M) complex doubles, taken through FP32 as the engine holds them; C planar
+ * FP32 (2, W, N, M)); half: 32, 64 or 80 orbitals per tile. */
+int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, int N, int nslices, int half,
+                         void* stream);
+
 /* ---------------------------------------------------------------------------------------
  * Resident engine: HamiltonianOperations + NOMSD trial + WalkerSet + AFQMCBasePropagator
  * kept in device memory on one GPU (the drop-in for execute_simulation's objects).
@@ -239,6 +254,16 @@ typedef struct {
 #define SFQ_PRECISION_FP64 0
 #define SFQ_PRECISION_MIXED 1      /* 2 bf16 planes per operand: ~16-bit operands, 3 tensor-core products */
 #define SFQ_PRECISION_MIXED_FP32 2 /* 3 bf16 planes per operand: ~24-bit operands, 6 tensor-core products */
+/* SFQ_PRECISION_INT8X3 / _INT8X2: the same products from int8 fixed-point slices of every operand row
+ * (x = 2^e (q1 + 2^-8 q2 + 2^-16 q3)), multiplied on the tensor cores (tcgen05 kind::i8) with exact
+ * int32 accumulation and one round-to-nearest when the slice groups are combined.  The split-BF16
+ * products above lose their low bits toward zero in the tensor cores' FP32 accumulation, which
+ * biases every product by the same relative shrink; these carry no such bias.  The force bias, the
+ * fields, vHS, the P1 products and Taylor terms, and the exchange tensor of the energy run this way;
+ * the Green's function, LU / log det, overlaps, orthogonalization, walker update and all sums stay
+ * FP64.  Needs a real trial; any nmo and nchol. */
+#define SFQ_PRECISION_INT8X3 3     /* 3 slices: 2^-24 of each row's largest entry, 6 int8 products */
+#define SFQ_PRECISION_INT8X2 4     /* 2 slices: 2^-16 of each row's largest entry, 3 int8 products */
 
 /* fill *p with the reference's defaults (parameters.hpp:103-131, parameter_defaults.cpp:274-285) */
 void sfq_engine_params_default(sfq_engine_params_t* p);

@@ -36,7 +36,7 @@ class EngineParams(ctypes.Structure):
                 ("target_population", ctypes.c_int), ("seed", ctypes.c_ulonglong), ("device", ctypes.c_int),
                 ("precision", ctypes.c_int), ("walker_type", ctypes.c_int), ("nel_dn", ctypes.c_int)]
 
-PRECISION_FP64, PRECISION_MIXED, PRECISION_MIXED_FP32 = 0, 1, 2
+PRECISION_FP64, PRECISION_MIXED, PRECISION_MIXED_FP32, PRECISION_INT8X3, PRECISION_INT8X2 = 0, 1, 2, 3, 4
 WALKER_CLOSED, WALKER_COLLINEAR, WALKER_NONCOLLINEAR = 1, 2, 3
 
 
@@ -103,6 +103,8 @@ _SIGS = {
     "sfq_gemm_bf16_planes": ([ctypes.POINTER(_VP), ctypes.POINTER(_VP), _I, _VP, _I, _I, _I, _I, ctypes.c_long,
                               ctypes.c_long, ctypes.c_float, ctypes.c_float, _I, _VP], _I),
     "sfq_split_bf16": ([_VP, ctypes.c_long, _VP, _VP, _VP, _VP], _I),
+    "sfq_gemm_int8_slices": ([_VP, _VP, _VP, _I, _I, _I, _I, _I, _I, _VP], _I),
+    "sfq_gemm_int8_cplx_b": ([_VP, _VP, _VP, _I, _I, _I, _I, _I, _VP], _I),
     "sfq_engine_params_default": ([ctypes.POINTER(EngineParams)], None),
     "sfq_engine_create": ([ctypes.POINTER(_VP), ctypes.POINTER(EngineParams), _VP, _VP, _VP], _I),
     "sfq_engine_create_nomsd": ([ctypes.POINTER(_VP), ctypes.POINTER(EngineParams), _VP, _VP, _I, _VP, _VP], _I),

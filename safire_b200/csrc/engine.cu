@@ -26,6 +26,7 @@
 #include "mixed.cuh"
 #include "ops.cuh"
 #include "umma_gemm.cuh"
+#include "islice.cuh"
 
 struct sfq_engine_s;
 
@@ -395,6 +396,24 @@ struct Engine {
   long vb_rows = 0;     // output columns of a Taylor product: ceil(M / tay_half) * 2 * tay_half
   int ldh = 0;          // padded half of the walker operand rows (re, im): M rounded up to 64
   int* gemm_err = nullptr;
+  // exact-accumulation mode (nslices > 0): int8 fixed-point slices of every tensor-core operand, one
+  // exponent per row (islice.cuh); rows of the walker-shaped arrays are r = w * N + a
+  int nslices = 0;
+  long ld_m = 0, ld_nm = 0, ld_nc = 0;  // slice row strides (bytes): M, N*M, Nc rounded up to 16
+  int8_t* Lv_q[3] = {};  int* Lv_e = nullptr;   // Lnak, rows n over (a, k): the force bias's B
+  int8_t* Le_q[3] = {};  int* Le_e = nullptr;   // Lnak, rows (n, a) over k: the exchange tensor's B
+  int8_t* Lh_q[3] = {};  int* Lh_e = nullptr;   // L, rows (i, k) (packed pairs when symmetric) over n: vHS's B
+  int8_t* P1_q[3] = {};  int* P1_e = nullptr;   // P1, rows j over i
+  int8_t* Gv_q[3] = {};  int* Gv_e = nullptr;   // G, planar rows (c, w) over (a, k)
+  int8_t* Ge_q[3] = {};  int* Ge_e = nullptr;   // G, planar rows (c, w, a) over k
+  int8_t* Xq_q[3] = {};  int* Xq_e = nullptr;   // fields, planar rows (c, w) over n
+  int8_t* V_q[3] = {};   int* V_e = nullptr;  int* V_emax = nullptr;  // V[w][c][i][k], exponent per (w, i)
+  int8_t* A_q[2][3] = {};  int8_t* A_n[2][3] = {};  int* A_e[2] = {};  // walker operand: rows (c, r); -im rows r
+  int8_t* Tb_q[3] = {};  int* Tb_e = nullptr;   // [[Tr, -Ti], [Ti, Tr]] of the inverse overlaps, rows (w, c, a)
+  int8_t* Ws_q[3] = {};  int* Ws_e = nullptr;   // the walkers read as reals, rows (w, k) over (b, c')
+  long ld_2n = 0;
+  float* Cp = nullptr;  // FP32 output of the walker-shaped products, planar (2 W N, M)
+  int i8_vb_bn = 160, i8_vb_ks = 1, i8_bn = 160, i8_half = 80;
   double* h_pinned = nullptr;  // pinned host staging for e2e calls
   size_t h_pinned_bytes = 0;
   // device-resident block driver: Eshift, the step counter and the block's measurements in device
@@ -542,7 +561,42 @@ struct Engine {
       };
       items.insert(items.end(), md.begin(), md.end());
     }
-    if (mixed) {
+    if (mixed && nslices) {
+      plan_i8();
+      const long R = (long)W * N, vrows = sym ? P : MM;
+      std::vector<Item> mx;
+      for (int q = 0; q < nslices; ++q) {
+        mx.push_back({(void**)&Lv_q[q], (size_t)Nc * ld_nm});
+        mx.push_back({(void**)&Le_q[q], (size_t)Nc * N * ld_m});
+        mx.push_back({(void**)&Lh_q[q], (size_t)vrows * ld_nc});
+        mx.push_back({(void**)&P1_q[q], (size_t)M * ld_m});
+        mx.push_back({(void**)&Gv_q[q], (size_t)2 * W * ld_nm});
+        mx.push_back({(void**)&Ge_q[q], (size_t)2 * R * ld_m});
+        mx.push_back({(void**)&Xq_q[q], (size_t)2 * W * ld_nc});
+        mx.push_back({(void**)&V_q[q], (size_t)W * 2 * M * ld_m});
+        for (int b = 0; b < 2; ++b) {
+          mx.push_back({(void**)&A_q[b][q], (size_t)2 * R * ld_m});
+          mx.push_back({(void**)&A_n[b][q], (size_t)R * ld_m});
+        }
+        mx.push_back({(void**)&Tb_q[q], (size_t)W * 2 * N * ld_2n});
+        mx.push_back({(void**)&Ws_q[q], (size_t)W * M * ld_2n});
+      }
+      const size_t ie = sizeof(int);
+      std::vector<Item> mx2 = {
+          {(void**)&Lv_e, ie * Nc}, {(void**)&Le_e, ie * Nc * N}, {(void**)&Lh_e, ie * vrows},
+          {(void**)&P1_e, ie * M}, {(void**)&Gv_e, ie * 2 * W}, {(void**)&Ge_e, ie * 2 * R},
+          {(void**)&Xq_e, ie * 2 * W}, {(void**)&V_e, ie * W * M}, {(void**)&V_emax, ie * W * M},
+          {(void**)&A_e[0], ie * R}, {(void**)&A_e[1], ie * R},
+          {(void**)&Tb_e, ie * 2 * R}, {(void**)&Ws_e, ie * W * M},
+          {(void**)&Cvb, sizeof(float) * i8_vb_ks * 2 * (size_t)W * Nc},
+          {(void**)&Cv, sizeof(float) * 2 * W * vrows},
+          {(void**)&Sacc, sizeof(float) * 2 * R * M},
+          {(void**)&Cp, sizeof(float) * 2 * R * M},
+          {(void**)&gemm_err, sizeof(int) * 4},
+      };
+      items.insert(items.end(), mx.begin(), mx.end());
+      items.insert(items.end(), mx2.begin(), mx2.end());
+    } else if (mixed) {
       const size_t b = 2;  // bf16
       const long MN2 = 2L * M * N;
       plan_mixed();
@@ -753,8 +807,31 @@ struct Engine {
         if ((rc = threshold_real(P1, MM, 1e-8, st))) return rc;
       }
     }
-    // mixed precision: bf16 hi/lo planes of the resident real tensors
-    if (mixed) {
+    // exact-accumulation mode: int8 slices of the resident real tensors
+    if (mixed && nslices) {
+      const long NM = (long)N * M;
+      const double* Ln = (const double*)Lnak;
+      if ((rc = islice_rows_real(Ln, Nc, NM, NM, nslices, Lv_q, ld_nm, Lv_e, st))) return rc;
+      if ((rc = islice_rows_real(Ln, (long)Nc * N, M, M, nslices, Le_q, ld_m, Le_e, st))) return rc;
+      if (sym) {
+        double* packed = nullptr;
+        SFQ_CUDA_TRY(cudaMallocAsync(&packed, sizeof(double) * P * Nc, st));
+        if ((rc = pack_upper(Likn, M, Nc, packed, st))) return rc;
+        if ((rc = islice_rows_real(packed, P, Nc, Nc, nslices, Lh_q, ld_nc, Lh_e, st))) return rc;
+        SFQ_CUDA_TRY(cudaFreeAsync(packed, st));
+      } else {
+        if ((rc = islice_rows_real(Likn, MM, Nc, Nc, nslices, Lh_q, ld_nc, Lh_e, st))) return rc;
+      }
+      // P1 = I + Q with Q of order dt: the slices hold Q (each row's entries at their own scale, not
+      // at the diagonal's), and the identity part is added exactly where the products are used
+      double* q1 = nullptr;
+      SFQ_CUDA_TRY(cudaMallocAsync((void**)&q1, sizeof(double) * MM, st));
+      SFQ_CUDA_TRY(cudaMemcpyAsync(q1, P1, sizeof(double) * MM, cudaMemcpyDeviceToDevice, st));
+      if ((rc = add_identity(q1, M, -1.0, st))) return rc;
+      if ((rc = islice_rows_real(q1, M, M, M, nslices, P1_q, ld_m, P1_e, st))) return rc;
+      SFQ_CUDA_TRY(cudaFreeAsync(q1, st));
+      SFQ_CUDA_TRY(cudaMemsetAsync(gemm_err, 0, sizeof(int) * 4, st));
+    } else if (mixed) {  // mixed precision: bf16 hi/lo planes of the resident real tensors
       if (sym) {
         double* packed = nullptr;
         SFQ_CUDA_TRY(cudaMallocAsync(&packed, sizeof(double) * P * Nc, st));
@@ -1302,6 +1379,7 @@ struct Engine {
   // set the tiles (0: the built-in choice); the captured block graphs are dropped
   int set_tiles(int gbn, int vbbn, int vhsbn, int half, int p1bn, int vbks = 0) {
     if (!mixed) return record_error(SFQ_ERR_UNSUPPORTED, "tiles: only the mixed-precision products are tiled");
+    if (nslices) return record_error(SFQ_ERR_UNSUPPORTED, "tiles: the int8-slice products keep their planned tiles");
     for (int bn : {gbn, vbbn, vhsbn, p1bn})
       if (bn && !tile_built(bn))
         return record_error(SFQ_ERR_ARG, "tiles: width %d is not built for %d planes", bn, nplanes);
@@ -1433,6 +1511,10 @@ struct Engine {
   // walkers, their weights and overlaps are not modified (only scratch buffers are written)
   int autotune(int reps, sfq_tiles_t* out) {
     if (!mixed) return record_error(SFQ_ERR_UNSUPPORTED, "autotune: only the mixed-precision products are tiled");
+    if (nslices) {  // the int8-slice products keep their planned tiles
+      if (out) get_tiles(out);
+      return SFQ_OK;
+    }
     const bool prof = profile;
     profile = false;
     const int rc = autotune_run(reps < 1 ? 9 : reps, out);
@@ -1508,9 +1590,224 @@ struct Engine {
     return SFQ_OK;
   }
 
+  // ---- exact-accumulation mode (int8 slices) ------------------------------------------------
+  static long round16(long x) { return (x + 15) / 16 * 16; }
+  // tile shapes of the int8-slice products: Taylor tiles of `half` orbitals (the least padding of
+  // M, then the widest), the force bias split along K to fill whole waves of SMs
+  void plan_i8() {
+    ld_m = round16(M);
+    ld_nm = round16((long)N * M);
+    ld_nc = round16(Nc);
+    ld_2n = round16(2L * N);
+    int best = 0;
+    long best_pad = 1L << 40;
+    for (int h : {32, 64, 80}) {
+      const long pad = (long)((M + h - 1) / h) * h;
+      if (pad < best_pad || (pad == best_pad && h > best)) {
+        best = h;
+        best_pad = pad;
+      }
+    }
+    i8_half = best;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device);
+    const long tiles = (long)((2 * W + 127) / 128) * ((Nc + i8_vb_bn - 1) / i8_vb_bn);
+    const long kt = ((long)N * M + 127) / 128;
+    double best_eff = 0.0;
+    i8_vb_ks = 1;
+    for (int ks = 1; ks <= 64 && ks * 4 <= kt; ++ks) {
+      const double units = double(tiles) * ks;
+      const double eff = units / (std::ceil(units / sms) * sms);
+      if (eff > best_eff + 1e-9) {
+        best_eff = eff;
+        i8_vb_ks = ks;
+      }
+      if (eff > 0.999) break;
+    }
+  }
+  IsliceOperand i8_operand(int8_t* const* q, long rows, long ld, const int* e, long bstride = 0, long e_bs = 0,
+                           long e_mod = 0) const {
+    IsliceOperand o;
+    for (int s2 = 0; s2 < 3; ++s2) o.q[s2] = q[s2];
+    o.rows = rows; o.ld = ld; o.batch_stride = bstride; o.e = e; o.e_bs = e_bs; o.e_mod = e_mod;
+    return o;
+  }
+  IsliceGemmDesc i8_desc() const {
+    IsliceGemmDesc d;
+    d.nslices = nslices;
+    d.err = gemm_err;
+    return d;
+  }
+  // C (2R, M) planar (+)= A (rows (c, r), one exponent per r) times (P1 - I)^T: the two P1 products,
+  // whose identity part the caller adds
+  int i8_p1(int buf, float* C, bool accumulate) {
+    const long R = (long)W * N;
+    IsliceGemmDesc d = i8_desc();
+    d.M = int(2 * R); d.N = M; d.K = M;
+    d.A = i8_operand(A_q[buf], 2 * R, ld_m, A_e[buf], 0, 0, R);
+    d.B = i8_operand(P1_q, M, ld_m, P1_e);
+    d.bn = i8_bn;
+    d.C = C; d.ldc = M; d.accumulate = accumulate;
+    return islice_gemm(d, st);
+  }
+  // one Taylor product of every walker: Cp = A [[Vr, -Vi], [Vi, Vr]]^T, planar [c][w][a][j]
+  int i8_taylor(int buf) {
+    const long R = (long)W * N;
+    IsliceGemmDesc d = i8_desc();
+    d.M = N; d.N = M; d.K = M; d.batch = W;
+    d.A = i8_operand(A_q[buf], N, ld_m, A_e[buf], (long)N * ld_m, N);
+    for (int s2 = 0; s2 < 3; ++s2) {
+      d.a_im[s2] = A_q[buf][s2] ? A_q[buf][s2] + R * ld_m : nullptr;
+      d.a_nim[s2] = A_n[buf][s2];
+    }
+    d.B = i8_operand(V_q, 2L * M, ld_m, V_e, 2L * M * ld_m, M);
+    d.cplx_half = i8_half;
+    d.C = Cp; d.ldc = M; d.sCc = R * M;
+    return islice_gemm(d, st);
+  }
+
+  // the force bias's G = (W Tinv)^T from int8 slices: rows (c, a) of [[Tr, -Ti], [Ti, Tr]] of the
+  // (cached FP64) inverse overlaps against each walker read as reals (K = (b, c')), written planar
+  // (c, w, a, k) in FP32 and sliced as the force bias's rows (c, w) over (a, k)
+  int density_i8() {
+    int rc;
+    if ((rc = ensure_inverse(nullptr))) return rc;
+    if ((rc = islice_tblk(T, W, N, nslices, Tb_q, ld_2n, Tb_e, st))) return rc;
+    if ((rc = islice_rows_real(reinterpret_cast<const double*>(SM), (long)W * M, 2L * N, 2L * N, nslices, Ws_q,
+                               ld_2n, Ws_e, st)))
+      return rc;
+    IsliceGemmDesc d = i8_desc();
+    d.M = 2 * N; d.N = M; d.K = 2 * N; d.batch = W;
+    d.A = i8_operand(Tb_q, 2L * N, ld_2n, Tb_e, 2L * N * ld_2n, 2L * N);
+    d.B = i8_operand(Ws_q, M, ld_2n, Ws_e, (long)M * ld_2n, M);
+    d.bn = i8_bn;
+    d.C = Cp; d.ldc = M; d.sCb = (long)N * M; d.row_split = N; d.sCc = (long)W * N * M;
+    if ((rc = islice_gemm(d, st))) return rc;
+    return islice_rows_real_f32(Cp, 2L * W, (long)N * M, (long)N * M, nslices, Gv_q, ld_nm, Gv_e, st);
+  }
+
+  // AFQMCBasePropagator::Propagate with the products from int8 slices (exact accumulation): G,
+  // force bias, vHS, P1 and the Taylor terms on the tensor cores; the elementwise steps between them
+  // (T = (i/k) C, S += T, slicing) round to nearest; LU / overlaps / walker update in FP64.
+  int propagate_i8(double Eshift, unsigned long long step, const double* uniforms) {
+    int rc;
+    const long R = (long)W * N;
+    const double sdt = std::sqrt(p.dt);
+    ph_begin(SFQ_PH_DENSITY);
+    if ((rc = density_i8())) return rc;
+    ph_end(SFQ_PH_DENSITY);
+    ph_begin(SFQ_PH_VBIAS);
+    const long part = 2L * W * Nc;
+    {
+      IsliceGemmDesc d = i8_desc();
+      d.M = 2 * W; d.N = Nc; d.K = int((long)N * M);
+      d.A = i8_operand(Gv_q, 2L * W, ld_nm, Gv_e);
+      d.B = i8_operand(Lv_q, Nc, ld_nm, Lv_e);
+      d.bn = i8_vb_bn; d.ksplit = i8_vb_ks; d.sCk = part;
+      d.C = Cvb; d.ldc = Nc;
+      if ((rc = islice_gemm(d, st))) return rc;
+    }
+    if ((rc = mixed_reduce_planar_to_cplx(Cvb, i8_vb_ks, part, W, Nc, 2.0 * sdt, X, st))) return rc;
+    ph_end(SFQ_PH_VBIAS);
+    ph_begin(SFQ_PH_FIELDS);
+    FieldParams fp;
+    fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
+    fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms; fp.step_dev = dev_mode ? d_step : nullptr;
+    if (uni_wait) {
+      SFQ_CUDA_TRY(cudaStreamWaitEvent(st, uni_wait, 0));
+      uni_wait = nullptr;
+    }
+    if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
+    ph_end(SFQ_PH_FIELDS);
+    ph_begin(SFQ_PH_VHS);
+    if ((rc = islice_rows_planar(X, W, Nc, nslices, Xq_q, ld_nc, Xq_e, st))) return rc;
+    ph_begin(SFQ_PH_VHS_GEMM);
+    const long vcols = sym ? P : (long)M * M;
+    {
+      IsliceGemmDesc d = i8_desc();
+      d.M = 2 * W; d.N = int(vcols); d.K = Nc;
+      d.A = i8_operand(Xq_q, 2L * W, ld_nc, Xq_e);
+      d.B = i8_operand(Lh_q, vcols, ld_nc, Lh_e);
+      d.bn = i8_bn;
+      d.C = Cv; d.ldc = vcols; d.alpha = sdt;
+      if ((rc = islice_gemm(d, st))) return rc;
+    }
+    ph_end(SFQ_PH_VHS_GEMM);
+    if ((rc = islice_build_v(Cv, W, M, sym, nslices, V_q, ld_m, V_e, V_emax, st))) return rc;
+    ph_end(SFQ_PH_VHS);
+    ph_begin(SFQ_PH_PROPAGATE);
+    inv_cached = false;
+    // S = P1 W = W + (P1 - I) W; then T_k = (i/k) V T_{k-1}, S += T_k for k = 1..order; SM = S + (P1 - I) S
+    if ((rc = islice_walkers(SM, W, M, N, nslices, A_q[0], ld_m, A_e[0], Sacc, st))) return rc;
+    if ((rc = i8_p1(0, Sacc, true))) return rc;
+    if ((rc = islice_taylor_update(nullptr, Sacc, R, M, 0, true, nslices, A_q[1], A_n[1], ld_m, A_e[1], st)))
+      return rc;
+    int cur = 1;
+    for (int k = 1; k <= p.taylor_order; ++k) {
+      if ((rc = i8_taylor(cur))) return rc;
+      const bool last = k == p.taylor_order;
+      if ((rc = islice_taylor_update(Cp, Sacc, R, M, k, last, nslices, A_q[1 - cur], last ? nullptr : A_n[1 - cur],
+                                     ld_m, A_e[1 - cur], st)))
+        return rc;
+      cur = 1 - cur;
+    }
+    if ((rc = i8_p1(cur, Cp, false))) return rc;
+    if ((rc = islice_to_walkers(Cp, Sacc, W, M, N, SM, st))) return rc;
+    ph_end(SFQ_PH_PROPAGATE);
+    ph_begin(SFQ_PH_OVERLAP);
+    if ((rc = log_overlap(newov))) return rc;
+    ph_end(SFQ_PH_OVERLAP);
+    ph_begin(SFQ_PH_UPDATE);
+    UpdateParams up;
+    up.nwalk = W; up.dt = p.dt; up.Eshift = Eshift; up.E0 = p.E0;
+    up.lower_cutoff = p.lower_cutoff_scale; up.upper_cutoff = p.upper_cutoff_scale;
+    up.max_weight = std::fmax(p.weight_bound_floor, p.weight_bound_fraction * target_pop());
+    up.hybrid = 1; up.free_projection = p.free_projection; up.use_cp_constraint = 0;
+    up.Eshift_dev = dev_mode ? d_eshift : nullptr;
+    if ((rc = walker_update(wprops(), newov, mf, hw, E3, up, stats, st))) return rc;
+    ph_end(SFQ_PH_UPDATE);
+    return SFQ_OK;
+  }
+
+  // NOMSD::Energy in the exact-accumulation mode: E1 from the FP64 G; the exchange tensor
+  // T[(c,w,b)][(n,a)] = sum_k G_c[w,b,k] Lnak[n,a,k] from int8 slices in chunks of Cholesky vectors
+  // (FP32, one rounding), its contractions summed in FP64
+  int energy_i8() {
+    int rc;
+    ph_begin(SFQ_PH_ENERGY);
+    if ((rc = density(ovtmp))) return rc;
+    const double scl = 2.0;
+    if ((rc = energy_e1(G, haj, E3, W, N, M, p.E0, scl, 1, st))) return rc;
+    const long R = (long)W * N;
+    if ((rc = islice_rows_planar(G, R, M, nslices, Ge_q, ld_m, Ge_e, st))) return rc;
+    const long per_n = 2L * W * N * N;
+    long nv_max = (2L * tchunk_elems) / per_n;
+    if (nv_max < 1) nv_max = 1;
+    if (nv_max > Nc) nv_max = Nc;
+    float* Tf = reinterpret_cast<float*>(Tchunk);
+    for (int n0 = 0; n0 < Nc; n0 += int(nv_max)) {
+      const int nv = (Nc - n0) < nv_max ? (Nc - n0) : int(nv_max);
+      const long ldc = (long)nv * N;
+      int8_t* Lc[3];
+      for (int q = 0; q < 3; ++q) Lc[q] = Le_q[q] ? Le_q[q] + (long)n0 * N * ld_m : nullptr;
+      IsliceGemmDesc d = i8_desc();
+      d.M = int(2 * R); d.N = int(ldc); d.K = M;
+      d.A = i8_operand(Ge_q, 2 * R, ld_m, Ge_e);
+      d.B = i8_operand(Lc, ldc, ld_m, Le_e + (long)n0 * N);
+      d.bn = i8_bn;
+      d.C = Tf; d.ldc = ldc;
+      if ((rc = islice_gemm(d, st))) return rc;
+      if ((rc = energy_exx_reduce_f32(Tf, W, N, nv, n0, Nc, ldc, exxn, kl, st))) return rc;
+    }
+    if ((rc = energy_finish(exxn, kl, E3, W, Nc, scl, 1, 1, st))) return rc;
+    ph_end(SFQ_PH_ENERGY);
+    return SFQ_OK;
+  }
+
   // AFQMCBasePropagator::Propagate with the bulk products on the tensor cores (split BF16, FP32
   // accumulation); G, LU/log det, fields, overlaps and the walker update stay FP64.
   int propagate_mixed(double Eshift, unsigned long long step, const double* uniforms) {
+    if (nslices) return propagate_i8(Eshift, step, uniforms);
     int rc;
     const long MM = (long)M * M, NM = (long)N * M, M2 = 2L * M;
     const double sdt = std::sqrt(p.dt);
@@ -1667,6 +1964,7 @@ struct Engine {
   // sum_k G_c[w,b,k] Lnak[n,a,k] as split-BF16 tcgen05 products into FP32 (in chunks of Cholesky
   // vectors), its contractions summed in FP64
   int energy_mixed() {
+    if (nslices) return energy_i8();
     int rc;
     ph_begin(SFQ_PH_ENERGY);
     if ((rc = density(ovtmp))) return rc;
@@ -2155,7 +2453,8 @@ int sfq_engine_create_nomsd(sfq_engine_t* out, const sfq_engine_params_t* p, con
   e.trial_real = true;
   for (long i = 0; i < (long)ndet * e.N * e.Mr; ++i)
     if (ps[i].y != 0.0) { e.trial_real = false; break; }
-  e.mixed = p->precision == SFQ_PRECISION_MIXED || p->precision == SFQ_PRECISION_MIXED_FP32;
+  e.nslices = p->precision == SFQ_PRECISION_INT8X3 ? 3 : p->precision == SFQ_PRECISION_INT8X2 ? 2 : 0;
+  e.mixed = p->precision == SFQ_PRECISION_MIXED || p->precision == SFQ_PRECISION_MIXED_FP32 || e.nslices > 0;
   e.nplanes = p->precision == SFQ_PRECISION_MIXED_FP32 ? 3 : 2;
   if (p->precision != SFQ_PRECISION_FP64 && !e.mixed) {
     delete h;
@@ -2166,7 +2465,11 @@ int sfq_engine_create_nomsd(sfq_engine_t* out, const sfq_engine_params_t* p, con
     return record_error(SFQ_ERR_UNSUPPORTED,
                         "engine: COLLINEAR and NONCOLLINEAR walkers and multi-determinant trials run in FP64");
   }
-  if (e.mixed && (!e.trial_real || e.M % 8 || e.Nc % 8)) {
+  if (e.nslices && !e.trial_real) {
+    delete h;
+    return record_error(SFQ_ERR_UNSUPPORTED, "engine: the int8-slice products need a real trial");
+  }
+  if (e.mixed && !e.nslices && (!e.trial_real || e.M % 8 || e.Nc % 8)) {
     delete h;
     return record_error(SFQ_ERR_UNSUPPORTED,
                         "engine: mixed precision needs a real trial and nmo, nchol multiples of 8 (nmo=%d nchol=%d)",

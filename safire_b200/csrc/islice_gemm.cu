@@ -1,0 +1,588 @@
+// Exact-accumulation int8-slice products on the tensor cores (see islice.cuh).
+#include <cstring>
+
+#include "islice.cuh"
+#include "tc_common.cuh"
+
+namespace sfq {
+namespace islice {
+using namespace tc;
+
+constexpr int BM = 128;                  // MMA M: accumulator rows = TMEM lanes
+constexpr int BK = 128;                  // int8 elements per K slice = one 128-byte swizzle row
+constexpr int KSTEP = 32;                // K of one kind::i8 MMA
+constexpr int kWarps = 6;                // 0: TMA producer, 1: TMEM owner + MMA issuer, 2-5: epilogue
+constexpr int kThreads = kWarps * 32;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // limit of one wait: 2 s without progress
+
+// slice pairs kept for NS slices, listed by group: g0 (0,0) | g1 (0,1) (1,0) | g2 (0,2) (1,1) (2,0)
+__host__ __device__ constexpr int n_pairs(int ns) { return ns == 2 ? 3 : 6; }
+__host__ __device__ constexpr int pair_a(int t) { return t == 0 ? 0 : t == 1 ? 0 : t == 2 ? 1 : t == 3 ? 0 : t == 4 ? 1 : 2; }
+__host__ __device__ constexpr int pair_b(int t) { return t == 0 ? 0 : t == 1 ? 1 : t == 2 ? 0 : t == 3 ? 2 : t == 4 ? 1 : 0; }
+__host__ __device__ constexpr int pair_g(int t) { return t == 0 ? 0 : t <= 2 ? 1 : 2; }
+__host__ __device__ constexpr bool pair_first(int t) { return t == 0 || t == 1 || t == 3; }
+
+// kind::i8: D = S32 (bits 4-5 = 2), A = B = signed 8-bit (bits 7-9, 10-12 = 1), both K-major, N, M = 128
+__host__ __device__ constexpr uint32_t idesc_i8(uint32_t n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | (uint32_t(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2),
+        "r"(mask3));
+}
+
+__host__ __device__ constexpr uint32_t pow2_ceil(uint32_t x) {
+  return x <= 32 ? 32 : x <= 64 ? 64 : x <= 128 ? 128 : x <= 256 ? 256 : 512;
+}
+
+template <int BN, int STAGES, int NS>
+struct Smem {
+  static constexpr int A_BYTES = BM * BK;
+  static constexpr int B_BYTES = BN * BK;
+  static constexpr int STAGE = NS * (A_BYTES + B_BYTES);
+  static constexpr int BAR_OFF = STAGES * STAGE;
+  static constexpr int NBAR = 2 * STAGES + 5;  // full, empty, acc_full[2], acc_empty[2], done
+  static constexpr int TOTAL = BAR_OFF + NBAR * 8 + 16 + 1024;
+  static_assert(A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "tiles must keep 1024-byte alignment");
+};
+
+struct Maps {
+  CUtensorMap a[3], b[3], aim[3], anim[3];
+};
+
+struct KParams {
+  int M, N, K, batch;
+  int a_batched, b_batched;
+  int MT, NT, KS, KT;  // tiles along M, N; K splits; K slices (complex B: 3 per 128 orbitals)
+  long tiles;
+  int half;            // complex B: orbitals per tile (0: plain product)
+  const int* ea; long ea_bs, ea_mod;
+  const int* eb; long eb_bs, eb_mod;
+  float* C;
+  long ldc, sCb, sCc, sCk;
+  int row_split;
+  double alpha;
+  int accumulate;      // C += the product (one FP32 round to nearest) instead of C = the product
+  int* err;
+  unsigned long long wait_ns;
+  const int* hold;
+};
+
+__device__ __forceinline__ void decode(const KParams& p, long t, int& mt, int& nt, int& bz, int& ks) {
+  mt = int(t % p.MT);
+  long r = t / p.MT;
+  nt = int(r % p.NT);
+  r /= p.NT;
+  bz = int(r % p.batch);
+  ks = int(r / p.batch);
+}
+__device__ __forceinline__ int k_begin(int KT, int KS, int s) { return int((long)KT * s / KS); }
+
+__device__ __forceinline__ double pow2(int e) {
+  e = e < -1022 ? -1022 : (e > 1023 ? 1023 : e);
+  return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+// one tile's accumulator groups at taddr (group g at column g * BN) -> FP32 output, row `row`
+template <int BN, int NS>
+__device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, int row, int mt, int nt, int bz,
+                                              int ks) {
+  const int gm = mt * BM + row;
+  const bool live = gm < p.M;
+  const int ea = live ? p.ea[(long)bz * p.ea_bs + (p.ea_mod ? gm % p.ea_mod : gm)] : 0;
+#pragma unroll 1
+  for (int c = 0; c < BN; c += 16) {
+    uint32_t acc[3][16];
+    __syncwarp();
+#pragma unroll
+    for (int g = 0; g < NS; ++g) tmem_ld16_u32(taddr + uint32_t(g * BN + c), acc[g]);
+    if (!live) continue;
+    long obase;
+    int col0, valid;
+    if (p.half) {  // complex B: [re | im] halves of `half` orbitals
+      const int part = c >= p.half ? 1 : 0;
+      col0 = nt * p.half + (c - part * p.half);
+      if (col0 >= p.N) continue;
+      valid = p.N - col0 < 16 ? p.N - col0 : 16;
+      obase = (long)part * p.sCc + ((long)bz * p.M + gm) * p.ldc + col0;
+    } else {
+      col0 = nt * BN + c;
+      if (col0 >= p.N) continue;
+      valid = p.N - col0 < 16 ? p.N - col0 : 16;
+      const long orow = p.row_split ? (long)(gm / p.row_split) * p.sCc + (long)(gm % p.row_split) * p.ldc
+                                    : (long)gm * p.ldc;
+      obase = (long)ks * p.sCk + (long)bz * p.sCb + orow + col0;
+    }
+    float v[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int col = col0 + j < p.N ? col0 + j : p.N - 1;
+      const int eb = p.eb[(long)bz * p.eb_bs + (p.eb_mod ? col % p.eb_mod : col)];
+      // acc0 2^16 + acc1 2^8 + acc2: exact in int64 (< 2^48) and in its conversion to FP64 (< 2^53)
+      long long s = (long long)int(acc[0][j]) << (8 * (NS - 1));
+      if (NS > 1) s += (long long)int(acc[1][j]) << (8 * (NS - 2));
+      if (NS > 2) s += (long long)int(acc[2][j]);
+      v[j] = __double2float_rn(double(s) * pow2(ea + eb - 8 * (NS - 1)) * p.alpha);
+    }
+    float* out = p.C + obase;
+    const bool vec = valid == 16 && (obase % 4) == 0;
+    if (p.accumulate) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (j < valid) v[j] = __fadd_rn(v[j], out[j]);
+    }
+    if (vec) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        reinterpret_cast<float4*>(out)[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (j < valid) out[j] = v[j];
+    }
+  }
+}
+
+template <int BN, int STAGES, int NS, int BUFS>
+__global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_constant__ Maps maps,
+                                                                  const __grid_constant__ KParams p) {
+  using L = Smem<BN, STAGES, NS>;
+  constexpr uint32_t GCOLS = uint32_t(NS * BN);               // columns of one tile's groups
+  constexpr uint32_t ALLOC = pow2_ceil(GCOLS * BUFS);
+  constexpr int NP = n_pairs(NS);
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::BAR_OFF);
+  uint64_t* empty = full + STAGES;
+  uint64_t* acc_full = empty + STAGES;  // [2]
+  uint64_t* acc_empty = acc_full + 2;   // [2]
+  uint64_t* done = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* s_abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool cb = p.half > 0;
+  const int Kv = cb ? p.N : p.K;  // valid K elements (complex B: the orbitals)
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 128);
+    }
+    mbar_init(done, 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
+                 "r"(ALLOC));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const unsigned long long wait_ns = p.wait_ns;
+
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer
+      uint32_t it = 0;
+      bool stop = false;
+      if (p.hold) {  // start only once *hold is set (bounded like every wait)
+        const unsigned long long t0 = gtimer();
+        while (*reinterpret_cast<const volatile int*>(p.hold) == 0) {
+          if (gtimer() - t0 > wait_ns) {
+            *s_abort = 1;
+            stop = true;
+            break;
+          }
+        }
+      }
+      for (long t = blockIdx.x; t < p.tiles && !stop; t += gridDim.x) {
+        int mt, nt, bz, ks;
+        decode(p, t, mt, nt, bz, ks);
+        const int m0 = mt * BM;
+        const int ab = p.a_batched ? bz : 0, bb = p.b_batched ? bz : 0;
+        const int kb = k_begin(p.KT, p.KS, ks), ke = k_begin(p.KT, p.KS, ks + 1);
+        for (int kt = kb; kt < ke; ++kt, ++it) {
+          const int s = int(it % STAGES);
+          const uint32_t ph = (it / STAGES) & 1;
+          if (!mbar_wait_for(&empty[s], ph ^ 1, wait_ns) || *s_abort) {
+            *s_abort = 1;
+            stop = true;
+            break;
+          }
+          unsigned char* stg = smem + s * L::STAGE;
+          if (cb) {
+            const int part = kt % 3, k0 = (kt / 3) * BK, i0 = nt * p.half;
+            const uint32_t bbytes = uint32_t((part == 0 ? 2 : 1) * p.half * BK);
+            mbar_expect_tx(&full[s], uint32_t(NS) * (uint32_t(L::A_BYTES) + bbytes));
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+              unsigned char* at = stg + q * L::A_BYTES;
+              unsigned char* bt = stg + NS * L::A_BYTES + q * L::B_BYTES;
+              const CUtensorMap* am = part == 0 ? &maps.a[q] : part == 1 ? &maps.anim[q] : &maps.aim[q];
+              tma_load_3d(at, am, &full[s], k0, m0, ab);
+              if (part == 0) {  // [Vr; Vi] rows of the tile's orbitals
+                tma_load_3d(bt, &maps.b[q], &full[s], k0, i0, bb);
+                tma_load_3d(bt + p.half * BK, &maps.b[q], &full[s], k0, p.N + i0, bb);
+              } else {          // Vi (for -A_im) or Vr (for A_im)
+                tma_load_3d(bt, &maps.b[q], &full[s], k0, (part == 1 ? p.N : 0) + i0, bb);
+              }
+            }
+          } else {
+            const int k0 = kt * BK, n0 = nt * BN;
+            mbar_expect_tx(&full[s], uint32_t(L::STAGE));
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+              tma_load_3d(stg + q * L::A_BYTES, &maps.a[q], &full[s], k0, m0, ab);
+              tma_load_3d(stg + NS * L::A_BYTES + q * L::B_BYTES, &maps.b[q], &full[s], k0, n0, bb);
+            }
+          }
+        }
+      }
+      // every issued stage must have landed before the CTA may exit
+      for (uint32_t j = (it > uint32_t(STAGES) ? it - STAGES : 0u); j < it; ++j)
+        mbar_wait_for(&full[j % STAGES], (j / STAGES) & 1, kWaitNs);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      uint32_t it = 0;
+      int lt = 0;
+      bool stop = false;
+      for (long t = blockIdx.x; t < p.tiles && !stop; t += gridDim.x, ++lt) {
+        const int b = BUFS == 2 ? (lt & 1) : 0;
+        const uint32_t aph = BUFS == 2 ? ((uint32_t(lt) >> 1) & 1) : (uint32_t(lt) & 1);
+        if (*s_abort || !mbar_wait_for(&acc_empty[b], aph ^ 1, wait_ns)) {
+          *s_abort = 1;
+          break;
+        }
+        fence_after();
+        const uint32_t d_tmem = tmem + uint32_t(b) * GCOLS;
+        int mt, nt, bz, ks;
+        decode(p, t, mt, nt, bz, ks);
+        const int kb = k_begin(p.KT, p.KS, ks), ke = k_begin(p.KT, p.KS, ks + 1);
+        for (int kt = kb; kt < ke; ++kt, ++it) {
+          const int s = int(it % STAGES);
+          const uint32_t ph = (it / STAGES) & 1;
+          if (*s_abort || !mbar_wait_for(&full[s], ph, wait_ns)) {
+            *s_abort = 1;
+            stop = true;
+            break;
+          }
+          fence_after();
+          unsigned char* stg = smem + s * L::STAGE;
+          uint64_t ad[NS], bd[NS];
+#pragma unroll
+          for (int q = 0; q < NS; ++q) {
+            ad[q] = smem_desc(stg + q * L::A_BYTES);
+            bd[q] = smem_desc(stg + NS * L::A_BYTES + q * L::B_BYTES);
+          }
+          const int part = cb ? kt % 3 : 0;
+          const int k0 = cb ? (kt / 3) * BK : kt * BK;
+          const int rem = Kv - k0;
+          const int nk = rem >= BK ? BK / KSTEP : (rem + KSTEP - 1) / KSTEP;  // K tail: skip all-zero steps
+          uint32_t idesc, coff;
+          if (!cb || part == 0) {
+            idesc = idesc_i8(uint32_t(BN));
+            coff = 0;
+          } else {
+            idesc = idesc_i8(uint32_t(p.half));
+            coff = part == 1 ? 0u : uint32_t(p.half);  // -A_im Vi^T into re, A_im Vr^T into im
+          }
+          const bool first_slice = kt == kb;  // complex B: part 0 of the first K block initialises
+          for (int kk = 0; kk < nk; ++kk) {
+            const uint64_t off = uint64_t(kk * KSTEP) >> 4;  // 32 bytes along the swizzled row
+#pragma unroll
+            for (int t2 = 0; t2 < NP; ++t2) {
+              const uint32_t accum = (first_slice && kk == 0 && pair_first(t2)) ? 0u : 1u;
+              umma_i8(d_tmem + uint32_t(pair_g(t2) * BN) + coff, ad[pair_a(t2)] + off, bd[pair_b(t2)] + off, idesc,
+                      accum);
+            }
+          }
+          umma_commit(&empty[s]);
+        }
+        if (!stop) umma_commit(&acc_full[b]);
+      }
+      // every MMA issued has completed before the tensor memory may be released
+      umma_commit(done);
+      mbar_wait_for(done, 0, kWaitNs);
+    }
+  } else {  // epilogue warps 2..5 -> TMEM lane quarters 2,3,0,1
+    const int q = warp & 3;
+    const int row = q * 32 + lane;
+    int lt = 0;
+    for (long t = blockIdx.x; t < p.tiles; t += gridDim.x, ++lt) {
+      const int b = BUFS == 2 ? (lt & 1) : 0;
+      const uint32_t aph = BUFS == 2 ? ((uint32_t(lt) >> 1) & 1) : (uint32_t(lt) & 1);
+      const bool ok = mbar_wait_for(&acc_full[b], aph, wait_ns);
+      const bool go = __all_sync(0xffffffffu, ok) && !__any_sync(0xffffffffu, *s_abort != 0);
+      if (!go) {
+        *s_abort = 1;
+        break;
+      }
+      fence_after();
+      int mt, nt, bz, ks;
+      decode(p, t, mt, nt, bz, ks);
+      epilogue_tile<BN, NS>(p, tmem + (uint32_t(q * 32) << 16) + uint32_t(b) * GCOLS, row, mt, nt, bz, ks);
+      fence_before();
+      mbar_arrive(&acc_empty[b]);
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0 && *s_abort && p.err) atomicExch(p.err, SFQ_ERR_TIMEOUT);
+  if (warp == 1) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ALLOC));
+  }
+}
+
+// ---- host side -------------------------------------------------------------------------------
+int make_map_i8(CUtensorMap* m, const void* base, long rows, long K, long ld, long batch, long bstride, int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return record_error(SFQ_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld % 16) || ld < K)
+    return record_error(SFQ_ERR_SHAPE, "islice_gemm: slices need 16-byte alignment and a row stride >= K, a multiple of 16");
+  if (batch <= 1) {
+    batch = 1;
+    bstride = (rows * ld + 15) / 16 * 16;
+  } else if (bstride % 16) {
+    return record_error(SFQ_ERR_SHAPE, "islice_gemm: batch stride must be a multiple of 16 bytes");
+  }
+  cuuint64_t dims[3] = {cuuint64_t(K), cuuint64_t(rows), cuuint64_t(batch)};
+  cuuint64_t strides[2] = {cuuint64_t(ld), cuuint64_t(bstride)};
+  cuuint32_t box[3] = {cuuint32_t(BK), cuuint32_t(box_rows), 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return record_error(SFQ_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
+  return SFQ_OK;
+}
+
+template <int BN, int STAGES, int NS>
+int launch(const IsliceGemmDesc& d, cudaStream_t st) {
+  using L = Smem<BN, STAGES, NS>;
+  constexpr int BUFS = (2 * NS * BN <= 512) ? 2 : 1;
+  static_assert(L::TOTAL <= 232448, "shared memory budget");
+  static_assert(NS * BN * BUFS <= 512, "accumulator groups must fit in tensor memory");
+  const bool cb = d.cplx_half > 0;
+  Maps maps;
+  int rc;
+  const long ab = d.A.batch_stride ? d.batch : 1, bb = d.B.batch_stride ? d.batch : 1;
+  for (int q = 0; q < NS; ++q) {
+    if (!d.A.q[q] || !d.B.q[q]) return record_error(SFQ_ERR_ARG, "islice_gemm: slice %d missing", q);
+    if ((rc = make_map_i8(&maps.a[q], d.A.q[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
+    if ((rc = make_map_i8(&maps.b[q], d.B.q[q], d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, cb ? d.cplx_half : BN)))
+      return rc;
+    if (cb) {
+      if (!d.a_im[q] || !d.a_nim[q]) return record_error(SFQ_ERR_ARG, "islice_gemm: complex B needs a_im and a_nim");
+      if ((rc = make_map_i8(&maps.aim[q], d.a_im[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
+      if ((rc = make_map_i8(&maps.anim[q], d.a_nim[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
+    } else {
+      maps.aim[q] = maps.a[q];
+      maps.anim[q] = maps.a[q];
+    }
+  }
+  for (int q = NS; q < 3; ++q) {
+    maps.a[q] = maps.a[0];
+    maps.b[q] = maps.b[0];
+    maps.aim[q] = maps.aim[0];
+    maps.anim[q] = maps.anim[0];
+  }
+  if (!d.A.e || !d.B.e || !d.C) return record_error(SFQ_ERR_ARG, "islice_gemm: exponents and output required");
+  KParams kp;
+  kp.M = d.M; kp.N = d.N; kp.K = d.K; kp.batch = d.batch;
+  kp.a_batched = d.A.batch_stride != 0; kp.b_batched = d.B.batch_stride != 0;
+  kp.MT = (d.M + BM - 1) / BM;
+  if (cb) {
+    if (d.cplx_half * 2 != BN || d.cplx_half % 16 || d.K != d.N || d.B.rows != 2L * d.N || d.ksplit > 1)
+      return record_error(SFQ_ERR_ARG, "islice_gemm: complex B needs BN = 2 half, half %% 16 == 0, K = N = nmo, "
+                                       "B rows = 2 nmo and no K split");
+    kp.NT = (d.N + d.cplx_half - 1) / d.cplx_half;
+    kp.KT = 3 * ((d.K + BK - 1) / BK);
+    kp.KS = 1;
+  } else {
+    kp.NT = (d.N + BN - 1) / BN;
+    kp.KT = (d.K + BK - 1) / BK;
+    kp.KS = d.ksplit < 1 ? 1 : (d.ksplit > kp.KT ? kp.KT : d.ksplit);
+    if (kp.KS > 1 && d.sCk <= 0) return record_error(SFQ_ERR_ARG, "islice_gemm: K splits need a partial-sum stride");
+  }
+  // int32 exactness: a group sums at most 3 pairs of |q| <= 128 products over one K range (complex
+  // B: each output sums both halves, 2 nmo terms)
+  const long krange = cb ? 2L * d.K : (long)((kp.KT + kp.KS - 1) / kp.KS) * BK;
+  if (krange > 43000)
+    return record_error(SFQ_ERR_SHAPE, "islice_gemm: K range of %ld too long for exact int32 accumulation", krange);
+  kp.tiles = (long)kp.MT * kp.NT * d.batch * kp.KS;
+  kp.half = cb ? d.cplx_half : 0;
+  kp.ea = d.A.e; kp.ea_bs = d.A.e_bs; kp.ea_mod = d.A.e_mod;
+  kp.eb = d.B.e; kp.eb_bs = d.B.e_bs; kp.eb_mod = cb ? 0 : d.B.e_mod;  // complex B: indexed by orbital
+  kp.C = d.C; kp.ldc = d.ldc; kp.sCb = d.sCb; kp.sCc = d.sCc; kp.sCk = d.sCk;
+  kp.row_split = cb ? 0 : d.row_split;
+  kp.alpha = d.alpha;
+  kp.accumulate = d.accumulate ? 1 : 0;
+  kp.err = d.err;
+  kp.wait_ns = d.wait_ns ? d.wait_ns : kWaitNs;
+  kp.hold = d.hold;
+  auto k = islice_gemm_kernel<BN, STAGES, NS, BUFS>;
+  SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
+  const long grid = kp.tiles < sm_count() ? kp.tiles : sm_count();
+  k<<<unsigned(grid), kThreads, L::TOTAL, st>>>(maps, kp);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+}  // namespace islice
+
+int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st) {
+  if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return SFQ_OK;
+  if (d.K <= 0) return record_error(SFQ_ERR_SHAPE, "islice_gemm: K must be positive");
+  const int bn = d.cplx_half > 0 ? 2 * d.cplx_half : (d.bn ? d.bn : (d.N <= 64 ? 64 : 128));
+  switch (d.nslices * 1000 + bn) {
+    case 2064: return islice::launch<64, 4, 2>(d, st);
+    case 2128: return islice::launch<128, 3, 2>(d, st);
+    case 2160: return islice::launch<160, 3, 2>(d, st);
+    case 3064: return islice::launch<64, 3, 3>(d, st);
+    case 3128: return islice::launch<128, 2, 3>(d, st);
+    case 3160: return islice::launch<160, 2, 3>(d, st);
+    default:
+      return record_error(SFQ_ERR_ARG, "islice_gemm: %d slices with tile width %d not built", d.nslices, bn);
+  }
+}
+
+}  // namespace sfq
+
+// ---- C ABI: the int8-slice products on caller operands (tests and benchmarks) ---------------
+namespace sfq {
+namespace {
+__global__ void cplx_to_planar_f32_kernel(const cplx* src, long n, float* re, float* im) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    re[t] = float(src[t].x);
+    im[t] = float(src[t].y);
+  }
+}
+}  // namespace
+}  // namespace sfq
+
+extern "C" {
+
+int sfq_gemm_int8_slices(const double* A, const double* B, float* C, int M, int N, int K, int nslices, int tile_n,
+                         int ksplit, void* stream) {
+  using namespace sfq;
+  if (nslices < 2 || nslices > 3) return record_error(SFQ_ERR_ARG, "nslices must be 2 or 3");
+  if (M <= 0 || N <= 0 || K <= 0) return record_error(SFQ_ERR_SHAPE, "gemm_int8_slices: empty product");
+  if (tile_n != 0 && tile_n != 64 && tile_n != 128 && tile_n != 160)
+    return record_error(SFQ_ERR_ARG, "gemm_int8_slices: tile width %d not built", tile_n);
+  if (!A || !B || !C) return record_error(SFQ_ERR_ARG, "gemm_int8_slices: null operand");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long ld = (K + 15) / 16 * 16;
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t qa = al((size_t)M * ld), qb = al((size_t)N * ld), ea = al(sizeof(int) * M), eb = al(sizeof(int) * N);
+  const int ks = ksplit < 1 ? 1 : ksplit;
+  const size_t cpart = al(sizeof(float) * (size_t)M * N);
+  char* buf = nullptr;
+  SFQ_CUDA_TRY(cudaMallocAsync((void**)&buf, nslices * (qa + qb) + ea + eb + (ks > 1 ? ks * cpart : 0), st));
+  int8_t *aq[3] = {}, *bq[3] = {};
+  for (int s = 0; s < nslices; ++s) {
+    aq[s] = reinterpret_cast<int8_t*>(buf + s * qa);
+    bq[s] = reinterpret_cast<int8_t*>(buf + nslices * qa + s * qb);
+  }
+  int* eA = reinterpret_cast<int*>(buf + nslices * (qa + qb));
+  int* eB = reinterpret_cast<int*>(buf + nslices * (qa + qb) + ea);
+  float* part = ks > 1 ? reinterpret_cast<float*>(buf + nslices * (qa + qb) + ea + eb) : nullptr;
+  int rc = islice_rows_real(A, M, K, K, nslices, aq, ld, eA, st);
+  if (!rc) rc = islice_rows_real(B, N, K, K, nslices, bq, ld, eB, st);
+  if (!rc) {
+    IsliceGemmDesc d;
+    d.M = M; d.N = N; d.K = K; d.nslices = nslices; d.bn = tile_n; d.ksplit = ks;
+    for (int s = 0; s < 3; ++s) {
+      d.A.q[s] = aq[s];
+      d.B.q[s] = bq[s];
+    }
+    d.A.rows = M; d.A.ld = ld; d.A.e = eA;
+    d.B.rows = N; d.B.ld = ld; d.B.e = eB;
+    d.C = ks > 1 ? part : C; d.ldc = N; d.sCk = (long)cpart / sizeof(float);
+    rc = islice_gemm(d, st);
+  }
+  if (!rc && ks > 1) {  // the K ranges' partial products, written at C + s * M * N
+    for (int s = 0; s < ks && !rc; ++s) {
+      const cudaError_t ce = cudaMemcpyAsync(C + (size_t)s * M * N, reinterpret_cast<char*>(part) + s * cpart,
+                                             sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToDevice, st);
+      if (ce != cudaSuccess) rc = record_cuda(ce, "cudaMemcpyAsync", __FILE__, __LINE__);
+    }
+  }
+  cudaFreeAsync(buf, st);
+  return rc;
+}
+
+int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, int N, int nslices, int half,
+                         void* stream) {
+  using namespace sfq;
+  if (nslices < 2 || nslices > 3) return record_error(SFQ_ERR_ARG, "nslices must be 2 or 3");
+  if (W <= 0 || M <= 0 || N <= 0) return record_error(SFQ_ERR_SHAPE, "gemm_int8_cplx_b: empty product");
+  if (half != 32 && half != 64 && half != 80)
+    return record_error(SFQ_ERR_ARG, "gemm_int8_cplx_b: %d orbitals per tile not built", half);
+  if (!A || !V || !C) return record_error(SFQ_ERR_ARG, "gemm_int8_cplx_b: null operand");
+  if (32L * 32 < M) return record_error(SFQ_ERR_SHAPE, "gemm_int8_cplx_b: M=%d too large", M);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long ld = (M + 15) / 16 * 16, R = (long)W * N, MM = (long)M * M;
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t sa = al(sizeof(float) * 2 * R * M), sv = al(sizeof(float) * 2 * W * MM);
+  const size_t qa = al((size_t)2 * R * ld), qn = al((size_t)R * ld), qv = al((size_t)W * 2 * M * ld);
+  const size_t ea = al(sizeof(int) * R), ev = al(sizeof(int) * W * M);
+  char* buf = nullptr;
+  SFQ_CUDA_TRY(cudaMallocAsync((void**)&buf, sa + sv + nslices * (qa + qn + qv) + ea + 2 * ev, st));
+  char* o = buf;
+  float* S = reinterpret_cast<float*>(o); o += sa;
+  float* Cv = reinterpret_cast<float*>(o); o += sv;
+  int8_t *aq[3] = {}, *an[3] = {}, *vq[3] = {};
+  for (int s = 0; s < nslices; ++s) {
+    aq[s] = reinterpret_cast<int8_t*>(o); o += qa;
+    an[s] = reinterpret_cast<int8_t*>(o); o += qn;
+    vq[s] = reinterpret_cast<int8_t*>(o); o += qv;
+  }
+  int* eA = reinterpret_cast<int*>(o); o += ea;
+  int* eV = reinterpret_cast<int*>(o); o += ev;
+  int* eVmax = reinterpret_cast<int*>(o);
+  // A as FP32 planar rows (c, w, a); V[w][j][i] as the planar rows (c * W + w, j * M + i) of a full vHS
+  cplx_to_planar_f32_kernel<<<148 * 8, 256, 0, st>>>(static_cast<const cplx*>(A), R * M, S, S + R * M);
+  SFQ_LAUNCHED();
+  for (int w = 0; w < W; ++w) {
+    cplx_to_planar_f32_kernel<<<148, 256, 0, st>>>(static_cast<const cplx*>(V) + w * MM, MM, Cv + w * MM,
+                                                   Cv + (W + w) * MM);
+    SFQ_LAUNCHED();
+  }
+  int rc = islice_taylor_update(nullptr, S, R, M, 0, true, nslices, aq, an, ld, eA, st);
+  if (!rc) rc = islice_build_v(Cv, W, M, false, nslices, vq, ld, eV, eVmax, st);
+  if (!rc) {
+    IsliceGemmDesc d;
+    d.M = N; d.N = M; d.K = M; d.batch = W; d.nslices = nslices;
+    for (int s = 0; s < 3; ++s) {
+      d.A.q[s] = aq[s];
+      d.a_im[s] = aq[s] ? aq[s] + R * ld : nullptr;
+      d.a_nim[s] = an[s];
+      d.B.q[s] = vq[s];
+    }
+    d.A.rows = N; d.A.ld = ld; d.A.batch_stride = (long)N * ld; d.A.e = eA; d.A.e_bs = N;
+    d.B.rows = 2L * M; d.B.ld = ld; d.B.batch_stride = 2L * M * ld; d.B.e = eV; d.B.e_bs = M;
+    d.cplx_half = half;
+    d.C = C; d.ldc = M; d.sCc = R * M;
+    rc = islice_gemm(d, st);
+  }
+  cudaFreeAsync(buf, st);
+  return rc;
+}
+
+}  // extern "C"

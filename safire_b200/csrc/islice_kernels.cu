@@ -1,0 +1,685 @@
+// Fixed-point int8 slices of the operands of the exact-accumulation products (see islice.cuh), and
+// the elementwise steps between those products in the propagation.
+//
+// Row exponent: for a row whose largest |x| is m, e = floor(log2 m) - 6, plus one when 2^-e m > 126,
+// so that y = 2^-e x has |y| <= 126.  Slices of y, each round to nearest (ties to even):
+//   q1 = rint(y),  r = 256 (y - q1),  q2 = rint(r),  q3 = rint(256 (r - q2))   (|r| <= 128)
+// then a q3 of +128 is carried into q2 and a q2 of +128 or more into q1, so every slice is int8
+// (|q1| <= 127).  Every step is exact in FP64, so the slices are a function of x and e alone.
+#include <cstdint>
+
+#include "common.cuh"
+#include "islice.cuh"
+
+namespace sfq {
+namespace {
+
+__device__ __forceinline__ double pow2d(int e) {
+  e = e < -1022 ? -1022 : (e > 1023 ? 1023 : e);
+  return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+__device__ __forceinline__ int row_exponent(double m) {
+  if (!(m > 0.0)) return 0;
+  int ex = 0;
+  frexp(m, &ex);  // m = f 2^ex, f in [0.5, 1)
+  int e = ex - 7;  // 2^-e m in [64, 128)
+  if (m * pow2d(-e) > 126.0) e += 1;
+  return e;
+}
+
+// slices of x at scale 2^-e (passed as s = 2^-e)
+__device__ __forceinline__ void slice_value(double x, double s, int ns, int& q1, int& q2, int& q3) {
+  const double y = x * s;
+  const double a = rint(y);
+  const double r = (y - a) * 256.0;
+  const double b = rint(r);
+  int i1 = int(a), i2 = int(b), i3 = 0;
+  if (ns > 2) {
+    i3 = int(rint((r - b) * 256.0));
+    if (i3 == 128) {
+      i3 = -128;
+      i2 += 1;
+    }
+  }
+  if (i2 >= 128) {
+    i2 -= 256;
+    i1 += 1;
+  }
+  q1 = i1;
+  q2 = i2;
+  q3 = i3;
+}
+
+struct Q {
+  int8_t* p[3];
+};
+Q qptrs(int8_t* const* q) {
+  Q r;
+  for (int s = 0; s < 3; ++s) r.p[s] = q[s];
+  return r;
+}
+
+__device__ __forceinline__ void put(const Q& q, int ns, long idx, double x, double s) {
+  int a, b, c;
+  slice_value(x, s, ns, a, b, c);
+  q.p[0][idx] = int8_t(a);
+  if (ns > 1) q.p[1][idx] = int8_t(b);
+  if (ns > 2) q.p[2][idx] = int8_t(c);
+}
+
+// the same slices for an FP32 value, in FP32 arithmetic: every step is exact for FP32 inputs (y has
+// 24 significant bits and |y| <= 126, so y - q1, 256 r and r - q2 are representable), so these are
+// the slices slice_value gives for the same value
+__device__ __forceinline__ void slice_value_f(float x, float s, int ns, int& q1, int& q2, int& q3) {
+  const float y = x * s;
+  const float a = rintf(y);
+  const float r = (y - a) * 256.f;
+  const float b = rintf(r);
+  int i1 = int(a), i2 = int(b), i3 = 0;
+  if (ns > 2) {
+    i3 = int(rintf((r - b) * 256.f));
+    if (i3 == 128) {
+      i3 = -128;
+      i2 += 1;
+    }
+  }
+  if (i2 >= 128) {
+    i2 -= 256;
+    i1 += 1;
+  }
+  q1 = i1;
+  q2 = i2;
+  q3 = i3;
+}
+// 2^-e as a float (e within the float exponent range; rows of FP32 values always are)
+__device__ __forceinline__ float pow2f(int e) {
+  e = e < -126 ? -126 : (e > 127 ? 127 : e);
+  return __int_as_float((e + 127) << 23);
+}
+// four consecutive FP32 values -> one 4-byte word per slice at idx (a multiple of 4)
+__device__ __forceinline__ void put4f(const Q& q, int ns, long idx, const float (&x)[4], float s) {
+  int a[4], b[4], c[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) slice_value_f(x[u], s, ns, a[u], b[u], c[u]);
+  *reinterpret_cast<char4*>(q.p[0] + idx) = make_char4(char(a[0]), char(a[1]), char(a[2]), char(a[3]));
+  if (ns > 1) *reinterpret_cast<char4*>(q.p[1] + idx) = make_char4(char(b[0]), char(b[1]), char(b[2]), char(b[3]));
+  if (ns > 2) *reinterpret_cast<char4*>(q.p[2] + idx) = make_char4(char(c[0]), char(c[1]), char(c[2]), char(c[3]));
+}
+
+// scalar store of one FP32 value's slices
+__device__ __forceinline__ void put1f(const Q& q, int ns, long idx, float x, float s) {
+  int a, b, c;
+  slice_value_f(x, s, ns, a, b, c);
+  q.p[0][idx] = int8_t(a);
+  if (ns > 1) q.p[1][idx] = int8_t(b);
+  if (ns > 2) q.p[2][idx] = int8_t(c);
+}
+
+__device__ __forceinline__ double block_max(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double u = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) u = fmax(u, __shfl_xor_sync(0xffffffffu, u, o));
+    if (threadIdx.x == 0) sh[0] = u;
+  }
+  __syncthreads();
+  return sh[0];
+}
+
+// one block per row
+__global__ void rows_real_kernel(const double* src, long K, long lds, int ns, Q q, long ld, int* e) {
+  __shared__ double sh[32];
+  const long r = blockIdx.x;
+  const double* x = src + r * lds;
+  double m = 0.0;
+  for (long k = threadIdx.x; k < K; k += blockDim.x) m = fmax(m, fabs(x[k]));
+  m = block_max(m, sh);
+  const int ex = row_exponent(m);
+  if (threadIdx.x == 0) e[r] = ex;
+  const double s = pow2d(-ex);
+  for (long k = threadIdx.x; k < ld; k += blockDim.x) put(q, ns, r * ld + k, k < K ? x[k] : 0.0, s);
+}
+
+// one block per complex row r: planar rows r (re) and R + r (im)
+__global__ void rows_planar_kernel(const cplx* src, long R, long K, int ns, Q q, long ld, int* e) {
+  __shared__ double sh[32];
+  const long r = blockIdx.x;
+  const cplx* x = src + r * K;
+  double mr = 0.0, mi = 0.0;
+  for (long k = threadIdx.x; k < K; k += blockDim.x) {
+    const cplx z = x[k];
+    mr = fmax(mr, fabs(z.x));
+    mi = fmax(mi, fabs(z.y));
+  }
+  mr = block_max(mr, sh);
+  mi = block_max(mi, sh);
+  const int er = row_exponent(mr), ei = row_exponent(mi);
+  if (threadIdx.x == 0) {
+    e[r] = er;
+    e[R + r] = ei;
+  }
+  const double sr = pow2d(-er), si = pow2d(-ei);
+  for (long k = threadIdx.x; k < ld; k += blockDim.x) {
+    const cplx z = k < K ? x[k] : mk(0.0, 0.0);
+    put(q, ns, r * ld + k, z.x, sr);
+    put(q, ns, (R + r) * ld + k, z.y, si);
+  }
+}
+
+// FP32 rows (four values per thread when K is a multiple of 4): one block per row
+template <bool VEC>
+__global__ void rows_real_f32_kernel(const float* src, long K, long lds, int ns, Q q, long ld, int* e) {
+  __shared__ double sh[32];
+  const long r = blockIdx.x;
+  const float* x = src + r * lds;
+  float m = 0.f;
+  if (VEC) {
+    for (long k = 4 * threadIdx.x; k < K; k += 4 * blockDim.x) {
+      const float4 v = *reinterpret_cast<const float4*>(x + k);
+      m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+    }
+  } else {
+    for (long k = threadIdx.x; k < K; k += blockDim.x) m = fmaxf(m, fabsf(x[k]));
+  }
+  const int ex = row_exponent(block_max(double(m), sh));
+  if (threadIdx.x == 0) e[r] = ex;
+  const float sc = pow2f(-ex);
+  if (VEC) {
+    for (long k = 4 * threadIdx.x; k < ld; k += 4 * blockDim.x) {
+      float v[4] = {0.f, 0.f, 0.f, 0.f};
+      if (k < K) {
+        const float4 u = *reinterpret_cast<const float4*>(x + k);
+        v[0] = u.x; v[1] = u.y; v[2] = u.z; v[3] = u.w;
+      }
+      put4f(q, ns, r * ld + k, v, sc);
+    }
+  } else {
+    for (long k = threadIdx.x; k < ld; k += blockDim.x) put1f(q, ns, r * ld + k, k < K ? x[k] : 0.f, sc);
+  }
+}
+
+// inverse overlaps Tinv (W, N, N) complex -> the rows (w, c, a) over (b, c') of the real block
+// [[Tr, -Ti], [Ti, Tr]] at Tinv[b][a] (the A operand of G = (W Tinv)^T), one exponent per (w, a)
+// shared by both rows; one block per (w, a), thread b
+__global__ void tblk_slices_kernel(const cplx* Tinv, int N, int ns, Q q, long ld, int* e) {
+  __shared__ double sh[32];
+  const int w = blockIdx.y, a = blockIdx.x;
+  const cplx* T = Tinv + (long)w * N * N;
+  double m = 0.0;
+  for (int b = threadIdx.x; b < N; b += blockDim.x) {
+    const cplx z = T[(long)b * N + a];
+    m = fmax(m, fmax(fabs(z.x), fabs(z.y)));
+  }
+  const int ex = row_exponent(block_max(m, sh));
+  const long r0 = ((long)w * 2) * N + a, r1 = r0 + N;  // rows (w, 0, a) and (w, 1, a)
+  if (threadIdx.x == 0) {
+    e[r0] = ex;
+    e[r1] = ex;
+  }
+  const double sc = pow2d(-ex);
+  for (int b = threadIdx.x; 2 * b < ld; b += blockDim.x) {
+    const cplx z = b < N ? T[(long)b * N + a] : mk(0.0, 0.0);
+    if (2 * b + 1 < ld) {
+      put(q, ns, r0 * ld + 2 * b, z.x, sc);
+      put(q, ns, r0 * ld + 2 * b + 1, -z.y, sc);
+      put(q, ns, r1 * ld + 2 * b, z.y, sc);
+      put(q, ns, r1 * ld + 2 * b + 1, z.x, sc);
+    }
+  }
+}
+
+// walkers: the largest |re|, |im| of each (w, a) over the orbitals (threads along a: coalesced)
+__global__ void walkers_max_kernel(const cplx* SM, int M, int N, int* e) {
+  __shared__ double sh[8][33];
+  const int w = blockIdx.y, a = blockIdx.x * 32 + threadIdx.x;
+  double m = 0.0;
+  if (a < N)
+    for (int j = threadIdx.y; j < M; j += blockDim.y) {
+      const cplx z = SM[((long)w * M + j) * N + a];
+      m = fmax(m, fmax(fabs(z.x), fabs(z.y)));
+    }
+  sh[threadIdx.y][threadIdx.x] = m;
+  __syncthreads();
+  if (threadIdx.y == 0 && a < N) {
+    for (int y = 1; y < blockDim.y; ++y) m = fmax(m, sh[y][threadIdx.x]);
+    e[(long)w * N + a] = row_exponent(m);
+  }
+}
+
+// walkers -> rows (c, w, a) over j, 32 x 32 tiles through shared memory
+__global__ void walkers_slice_kernel(const cplx* SM, int W, int M, int N, int ns, Q q, long ld, const int* e,
+                                     float* planar) {
+  __shared__ cplx tile[32][33];
+  const int w = blockIdx.z, j0 = blockIdx.y * 32, a0 = blockIdx.x * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = j0 + r, a = a0 + threadIdx.x;
+    tile[r][threadIdx.x] = (j < M && a < N) ? SM[((long)w * M + j) * N + a] : mk(0.0, 0.0);
+  }
+  __syncthreads();
+  const long R = (long)W * N;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int a = a0 + r, j = j0 + threadIdx.x;
+    if (a >= N || j >= ld) continue;
+    const long row = (long)w * N + a;
+    const double s = pow2d(-e[row]);
+    const cplx z = tile[threadIdx.x][r];
+    put(q, ns, row * ld + j, z.x, s);
+    put(q, ns, (R + row) * ld + j, z.y, s);
+    if (planar && j < M) {
+      planar[row * M + j] = float(z.x);
+      planar[(R + row) * M + j] = float(z.y);
+    }
+  }
+}
+
+// Taylor update, one warp per row r; each lane keeps its <= kMaxPerLane values per part in registers
+constexpr int kMaxPerLane = 32;
+__global__ void taylor_update_kernel(const float* C, float* S, long R, int M, int k, int slice_sum, int ns, Q q,
+                                     Q qn, long ld, int* e) {
+  const long r = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= R) return;
+  float v[2][kMaxPerLane];
+  double m = 0.0;
+  const float fk = float(k);
+#pragma unroll
+  for (int t = 0; t < kMaxPerLane; ++t) {
+    const int j = lane + 32 * t;
+    if (j >= M) break;
+    const long i0 = r * M + j, i1 = (R + r) * M + j;
+    float sr = S[i0], si = S[i1];
+    if (k > 0) {
+      const float tr = -C[i1] / fk, ti = C[i0] / fk;  // T_{k} = (i / k) C
+      sr += tr;
+      si += ti;
+      S[i0] = sr;
+      S[i1] = si;
+      v[0][t] = slice_sum ? sr : tr;
+      v[1][t] = slice_sum ? si : ti;
+    } else {
+      v[0][t] = sr;
+      v[1][t] = si;
+    }
+    m = fmax(m, fmax(fabs(double(v[0][t])), fabs(double(v[1][t]))));
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  const int ex = row_exponent(m);
+  if (lane == 0) e[r] = ex;
+  const double s = pow2d(-ex);
+#pragma unroll
+  for (int t = 0; t < kMaxPerLane; ++t) {
+    const int j = lane + 32 * t;
+    if (j >= ld) break;
+    const double xr = j < M ? double(v[0][t]) : 0.0, xi = j < M ? double(v[1][t]) : 0.0;
+    put(q, ns, r * ld + j, xr, s);
+    put(q, ns, (R + r) * ld + j, xi, s);
+    if (qn.p[0]) put(qn, ns, r * ld + j, -xi, s);
+  }
+}
+
+// the same, four consecutive orbitals per lane (M a multiple of 4: 16-byte rows of C and S)
+constexpr int kMaxQuadsPerLane = 8;  // M <= 1024
+__global__ void taylor_update4_kernel(const float* C, float* S, long R, int M, int k, int slice_sum, int ns, Q q,
+                                      Q qn, long ld, int* e) {
+  const long r = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= R) return;
+  const int M4 = M >> 2;
+  float v[2][kMaxQuadsPerLane][4];
+  float m = 0.f;
+  const float fk = float(k);
+#pragma unroll
+  for (int t = 0; t < kMaxQuadsPerLane; ++t) {
+    const int g = lane + 32 * t;
+    if (g >= M4) break;
+    const long i0 = r * M + 4 * g, i1 = (R + r) * M + 4 * g;
+    float4 sr = *reinterpret_cast<const float4*>(S + i0), si = *reinterpret_cast<const float4*>(S + i1);
+    float xr[4] = {sr.x, sr.y, sr.z, sr.w}, xi[4] = {si.x, si.y, si.z, si.w};
+    if (k > 0) {
+      const float4 cr = *reinterpret_cast<const float4*>(C + i0), ci = *reinterpret_cast<const float4*>(C + i1);
+      const float c0[4] = {cr.x, cr.y, cr.z, cr.w}, c1[4] = {ci.x, ci.y, ci.z, ci.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const float tr = -c1[u] / fk, ti = c0[u] / fk;  // T_k = (i / k) C
+        const float nr = xr[u] + tr, ni = xi[u] + ti;
+        v[0][t][u] = slice_sum ? nr : tr;
+        v[1][t][u] = slice_sum ? ni : ti;
+        xr[u] = nr;
+        xi[u] = ni;
+      }
+      *reinterpret_cast<float4*>(S + i0) = make_float4(xr[0], xr[1], xr[2], xr[3]);
+      *reinterpret_cast<float4*>(S + i1) = make_float4(xi[0], xi[1], xi[2], xi[3]);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        v[0][t][u] = xr[u];
+        v[1][t][u] = xi[u];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) m = fmaxf(m, fmaxf(fabsf(v[0][t][u]), fabsf(v[1][t][u])));
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  const int ex = row_exponent(double(m));
+  if (lane == 0) e[r] = ex;
+  const float sc = pow2f(-ex);
+#pragma unroll
+  for (int t = 0; t < kMaxQuadsPerLane; ++t) {
+    const int g = lane + 32 * t;
+    if (4 * g >= ld) break;
+    float xr[4], xi[4], xn[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool in = g < M4;
+      xr[u] = in ? v[0][t][u] : 0.f;
+      xi[u] = in ? v[1][t][u] : 0.f;
+      xn[u] = -xi[u];
+    }
+    put4f(q, ns, r * ld + 4 * g, xr, sc);
+    put4f(q, ns, (R + r) * ld + 4 * g, xi, sc);
+    if (qn.p[0]) put4f(qn, ns, r * ld + 4 * g, xn, sc);
+  }
+}
+
+// vHS row maxima over k and both parts, per (w, i), as float bits (non-negative floats order as ints)
+constexpr int kVT = 64;
+__global__ void __launch_bounds__(256) v_max_packed_kernel(const float* Cv, int W, int M, int T, int* emax) {
+  __shared__ float tile[kVT][kVT + 1];
+  const int wc = blockIdx.y, w = wc % W;
+  int t = blockIdx.x, ib = 0;
+  while (ib < T && t >= T - ib) {
+    t -= T - ib;
+    ++ib;
+  }
+  const int kb = ib + t;
+  const int i0 = ib * kVT, k0 = kb * kVT;
+  const float* src = Cv + (long)wc * ((long)M * (M + 1) / 2);
+  const int tid = threadIdx.x;
+  {
+    const int qc = tid % kVT, r0 = tid / kVT;
+#pragma unroll
+    for (int s = 0; s < kVT / 4; ++s) {
+      const int r = r0 + 4 * s;
+      const long i = i0 + r, k = k0 + qc;
+      tile[r][qc] = (i < M && k < M && i <= k) ? fabsf(src[i * M - i * (i + 1) / 2 + k]) : 0.f;
+    }
+  }
+  __syncthreads();
+  if (tid < kVT) {  // row i0 + tid: V[i][k] over the tile's k
+    float m = 0.f;
+    for (int c = 0; c < kVT; ++c) m = fmaxf(m, tile[tid][c]);
+    if (i0 + tid < M) atomicMax(emax + (long)w * M + i0 + tid, __float_as_int(m));
+  } else if (tid < 2 * kVT && ib != kb) {  // row k0 + c: the mirrored V[k][i] over the tile's i
+    const int c = tid - kVT;
+    float m = 0.f;
+    for (int r = 0; r < kVT; ++r) m = fmaxf(m, tile[r][c]);
+    if (k0 + c < M) atomicMax(emax + (long)w * M + k0 + c, __float_as_int(m));
+  } else if (tid < 2 * kVT) {  // diagonal tile: the lower half mirrored into row k0 + c
+    const int c = tid - kVT;
+    float m = 0.f;
+    for (int r = 0; r < c; ++r) m = fmaxf(m, tile[r][c]);
+    if (k0 + c < M) atomicMax(emax + (long)w * M + k0 + c, __float_as_int(m));
+  }
+}
+
+__global__ void v_max_full_kernel(const float* Cv, int W, int M, int* emax) {
+  const long row = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);  // (c * W + w) * M + i
+  const int lane = threadIdx.x & 31;
+  if (row >= 2L * W * M) return;
+  const float* x = Cv + row * M;
+  float m = 0.f;
+  for (int k = lane; k < M; k += 32) m = fmaxf(m, fabsf(x[k]));
+#pragma unroll
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  const long wc = row / M, i = row % M, w = wc % W;
+  if (lane == 0) atomicMax(emax + w * M + i, __float_as_int(m));
+}
+
+__global__ void v_exponent_kernel(const int* emax, long n, int* e) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
+    e[t] = row_exponent(double(__int_as_float(emax[t])));
+}
+
+// V slices: one block per 64 x 64 tile pair of one planar row, V[w][c][i][k] and its mirror
+template <bool VEC>
+__global__ void __launch_bounds__(256) v_slice_packed_kernel(const float* Cv, int W, int M, int T, int ns, Q q,
+                                                               long ld, const int* e) {
+  __shared__ float tile[kVT][kVT + 1];
+  const int wc = blockIdx.y;
+  const int c = wc / W, w = wc - c * W;
+  int t = blockIdx.x, ib = 0;
+  while (ib < T && t >= T - ib) {
+    t -= T - ib;
+    ++ib;
+  }
+  const int kb = ib + t;
+  const int i0 = ib * kVT, k0 = kb * kVT;
+  const float* src = Cv + (long)wc * ((long)M * (M + 1) / 2);
+  const long vbase = ((long)w * 2 + c) * M * ld;
+  const int* ew = e + (long)w * M;
+  const int tid = threadIdx.x;
+  {
+    const int qc = tid % kVT, r0 = tid / kVT;
+#pragma unroll
+    for (int s = 0; s < kVT / 4; ++s) {
+      const int r = r0 + 4 * s;
+      const long i = i0 + r, k = k0 + qc;
+      tile[r][qc] = (i < M && k < M && i <= k) ? src[i * M - i * (i + 1) / 2 + k] : 0.f;
+    }
+  }
+  __syncthreads();
+  if (!VEC) {  // M not a multiple of 4: one value at a time
+    for (int el = tid; el < kVT * kVT; el += 256) {
+      const int r = el / kVT, g = el % kVT;
+      const int i = i0 + r, k = k0 + g;
+      if (i >= M || k >= ld) continue;
+      put1f(q, ns, vbase + (long)i * ld + k, k >= M ? 0.f : (i <= k ? tile[r][g] : tile[g][r]), pow2f(-ew[i]));
+    }
+    if (ib == kb) return;
+    for (int el = tid; el < kVT * kVT; el += 256) {
+      const int r = el / kVT, g = el % kVT;
+      const int k = k0 + r, i = i0 + g;
+      if (k >= M || i >= M) continue;
+      put1f(q, ns, vbase + (long)k * ld + i, tile[g][r], pow2f(-ew[k]));
+    }
+    return;
+  }
+  // four consecutive columns per thread (ld is a multiple of 16 and k0 of 64: a group lies inside
+  // the row's [0, ld) or wholly past it)
+  for (int el = tid; el < kVT * kVT / 4; el += 256) {
+    const int r = el / (kVT / 4), g = 4 * (el % (kVT / 4));
+    const int i = i0 + r, k = k0 + g;
+    if (i >= M || k >= ld) continue;
+    float x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)  // the diagonal tile's lower half mirrored; zeros past M
+      x[u] = k + u >= M ? 0.f : (i <= k + u ? tile[r][g + u] : tile[g + u][r]);
+    put4f(q, ns, vbase + (long)i * ld + k, x, pow2f(-ew[i]));
+  }
+  if (ib == kb) return;
+  for (int el = tid; el < kVT * kVT / 4; el += 256) {
+    const int r = el / (kVT / 4), g = 4 * (el % (kVT / 4));
+    const int k = k0 + r, i = i0 + g;
+    if (k >= M || i >= M) continue;  // i < M and M a multiple of 4 (else the full path): i + 3 < M
+    float x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) x[u] = tile[g + u][r];
+    put4f(q, ns, vbase + (long)k * ld + i, x, pow2f(-ew[k]));
+  }
+}
+
+__global__ void v_slice_full_kernel(const float* Cv, int W, int M, int ns, Q q, long ld, const int* e) {
+  const long n = 2L * W * M * ld;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const long k = t % ld, r = t / ld;  // r = (w * 2 + c) * M + i
+    const long i = r % M, wc2 = r / M, c = wc2 % 2, w = wc2 / 2;
+    const float x = k < M ? Cv[(c * W + w) * (long)M * M + i * M + k] : 0.f;
+    int a, b, d;
+    slice_value_f(x, pow2f(-e[w * M + i]), ns, a, b, d);
+    q.p[0][t] = int8_t(a);
+    if (ns > 1) q.p[1][t] = int8_t(b);
+    if (ns > 2) q.p[2][t] = int8_t(d);
+  }
+}
+
+// planar FP32 C[c][w][a][j] -> SM[w][j][a] complex, 32 x 32 tiles through shared memory
+__global__ void to_walkers_kernel(const float* C, const float* S, int W, int M, int N, cplx* SM) {
+  __shared__ double2 tile[32][33];
+  const int w = blockIdx.z, a0 = blockIdx.y * 32, j0 = blockIdx.x * 32;
+  const long R = (long)W * N;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int a = a0 + r, j = j0 + threadIdx.x;
+    if (a < N && j < M) {
+      const long i = ((long)w * N + a) * M + j;
+      double re = double(C[i]), im = double(C[R * M + i]);
+      if (S) {
+        re += double(S[i]);
+        im += double(S[R * M + i]);
+      }
+      tile[r][threadIdx.x] = make_double2(re, im);
+    }
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = j0 + r, a = a0 + threadIdx.x;
+    if (a < N && j < M) {
+      const double2 z = tile[threadIdx.x][r];
+      SM[((long)w * M + j) * N + a] = mk(z.x, z.y);
+    }
+  }
+}
+
+inline int grid_for(long n) {
+  long g = (n + 255) / 256;
+  if (g > 148L * 32) g = 148L * 32;
+  return int(g < 1 ? 1 : g);
+}
+
+int check_slices(int ns, int8_t* const* q, long ld) {
+  if (ns < 2 || ns > 3) return record_error(SFQ_ERR_ARG, "islice: 2 or 3 slices");
+  for (int s = 0; s < ns; ++s)
+    if (!q[s]) return record_error(SFQ_ERR_ARG, "islice: slice %d missing", s);
+  if (ld % 16) return record_error(SFQ_ERR_SHAPE, "islice: row stride %ld is not a multiple of 16", ld);
+  return SFQ_OK;
+}
+
+}  // namespace
+
+int islice_rows_real(const double* src, long R, long K, long lds, int nslices, int8_t* const* q, long ld, int* e,
+                     cudaStream_t st) {
+  if (int rc = check_slices(nslices, q, ld)) return rc;
+  if (R <= 0) return SFQ_OK;
+  if (ld < K || R > 2147483647L) return record_error(SFQ_ERR_SHAPE, "islice_rows_real: sizes");
+  rows_real_kernel<<<unsigned(R), ld <= 512 ? 128 : 256, 0, st>>>(src, K, lds, nslices, qptrs(q), ld, e);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int islice_rows_planar(const cplx* src, long R, long K, int nslices, int8_t* const* q, long ld, int* e,
+                       cudaStream_t st) {
+  if (int rc = check_slices(nslices, q, ld)) return rc;
+  if (R <= 0) return SFQ_OK;
+  if (ld < K || R > 2147483647L) return record_error(SFQ_ERR_SHAPE, "islice_rows_planar: sizes");
+  rows_planar_kernel<<<unsigned(R), K >= 4096 ? 512 : 256, 0, st>>>(src, R, K, nslices, qptrs(q), ld, e);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int islice_rows_real_f32(const float* src, long R, long K, long lds, int nslices, int8_t* const* q, long ld, int* e,
+                         cudaStream_t st) {
+  if (int rc = check_slices(nslices, q, ld)) return rc;
+  if (R <= 0) return SFQ_OK;
+  if (ld < K || R > 2147483647L) return record_error(SFQ_ERR_SHAPE, "islice_rows_real_f32: sizes");
+  const int bs = K >= 8192 ? 512 : 256;
+  if (K % 4 == 0 && lds % 4 == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0)
+    rows_real_f32_kernel<true><<<unsigned(R), bs, 0, st>>>(src, K, lds, nslices, qptrs(q), ld, e);
+  else
+    rows_real_f32_kernel<false><<<unsigned(R), bs, 0, st>>>(src, K, lds, nslices, qptrs(q), ld, e);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int islice_tblk(const cplx* Tinv, int W, int N, int nslices, int8_t* const* q, long ld, int* e, cudaStream_t st) {
+  if (int rc = check_slices(nslices, q, ld)) return rc;
+  if (ld < 2L * N || W > 65535) return record_error(SFQ_ERR_SHAPE, "islice_tblk: sizes");
+  tblk_slices_kernel<<<dim3(unsigned(N), unsigned(W)), 128, 0, st>>>(Tinv, N, nslices, qptrs(q), ld, e);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int islice_walkers(const cplx* SM, int W, int M, int N, int nslices, int8_t* const* q, long ld, int* e,
+                   float* planar, cudaStream_t st) {
+  if (int rc = check_slices(nslices, q, ld)) return rc;
+  if (ld < M || W > 65535) return record_error(SFQ_ERR_SHAPE, "islice_walkers: sizes");
+  walkers_max_kernel<<<dim3(unsigned((N + 31) / 32), unsigned(W)), dim3(32, 8), 0, st>>>(SM, M, N, e);
+  SFQ_LAUNCHED();
+  walkers_slice_kernel<<<dim3(unsigned((N + 31) / 32), unsigned((ld + 31) / 32), unsigned(W)), dim3(32, 8), 0, st>>>(
+      SM, W, M, N, nslices, qptrs(q), ld, e, planar);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int islice_taylor_update(const float* C, float* S, long R, int M, int k, bool slice_sum, int nslices,
+                         int8_t* const* q, int8_t* const* qn, long ld, int* e, cudaStream_t st) {
+  if (int rc = check_slices(nslices, q, ld)) return rc;
+  if (ld < M || ld > 32L * kMaxPerLane) return record_error(SFQ_ERR_SHAPE, "islice_taylor_update: M=%d too large", M);
+  if (k > 0 && !C) return record_error(SFQ_ERR_ARG, "islice_taylor_update: product missing");
+  int8_t* none[3] = {nullptr, nullptr, nullptr};
+  const int wpb = 8;
+  if (M % 4 == 0) {
+    taylor_update4_kernel<<<unsigned((R + wpb - 1) / wpb), 32 * wpb, 0, st>>>(
+        C, S, R, M, k, slice_sum ? 1 : 0, nslices, qptrs(q), qptrs(qn ? qn : none), ld, e);
+  } else {
+    taylor_update_kernel<<<unsigned((R + wpb - 1) / wpb), 32 * wpb, 0, st>>>(
+        C, S, R, M, k, slice_sum ? 1 : 0, nslices, qptrs(q), qptrs(qn ? qn : none), ld, e);
+  }
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int islice_build_v(const float* Cv, int W, int M, bool packed, int nslices, int8_t* const* q, long ld, int* e,
+                   int* emax, cudaStream_t st) {
+  if (int rc = check_slices(nslices, q, ld)) return rc;
+  if (ld < M || 2L * W > 65535) return record_error(SFQ_ERR_SHAPE, "islice_build_v: sizes");
+  SFQ_CUDA_TRY(cudaMemsetAsync(emax, 0, sizeof(int) * (size_t)W * M, st));
+  const int T = (M + kVT - 1) / kVT;
+  if (packed) {
+    v_max_packed_kernel<<<dim3(unsigned(T * (T + 1) / 2), unsigned(2 * W)), 256, 0, st>>>(Cv, W, M, T, emax);
+  } else {
+    v_max_full_kernel<<<unsigned((2L * W * M + 7) / 8), 256, 0, st>>>(Cv, W, M, emax);
+  }
+  SFQ_LAUNCHED();
+  v_exponent_kernel<<<grid_for((long)W * M), 256, 0, st>>>(emax, (long)W * M, e);
+  SFQ_LAUNCHED();
+  if (packed) {
+    if (ld > (long)T * kVT) return record_error(SFQ_ERR_SHAPE, "islice_build_v: row stride beyond the tiles");
+    const dim3 grid(unsigned(T * (T + 1) / 2), unsigned(2 * W));
+    if (M % 4 == 0)  // groups of four orbitals
+      v_slice_packed_kernel<true><<<grid, 256, 0, st>>>(Cv, W, M, T, nslices, qptrs(q), ld, e);
+    else
+      v_slice_packed_kernel<false><<<grid, 256, 0, st>>>(Cv, W, M, T, nslices, qptrs(q), ld, e);
+  } else {
+    v_slice_full_kernel<<<grid_for(2L * W * M * ld), 256, 0, st>>>(Cv, W, M, nslices, qptrs(q), ld, e);
+  }
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int islice_to_walkers(const float* C, const float* S, int W, int M, int N, cplx* SM, cudaStream_t st) {
+  if (W > 65535) return record_error(SFQ_ERR_SHAPE, "islice_to_walkers: too many walkers");
+  to_walkers_kernel<<<dim3(unsigned((M + 31) / 32), unsigned((N + 31) / 32), unsigned(W)), dim3(32, 8), 0, st>>>(
+      C, S, W, M, N, SM);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+}  // namespace sfq

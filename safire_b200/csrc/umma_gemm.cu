@@ -4,16 +4,46 @@
 #include <cstring>
 #include <mutex>
 
+#include "tc_common.cuh"
 #include "umma_gemm.cuh"
 
 namespace sfq {
+namespace tc {
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+int sm_count() {
+  static int counts[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!counts[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    counts[dev] = n;
+  }
+  return counts[dev];
+}
+
+}  // namespace tc
+
 namespace umma {
+using namespace tc;
 
 constexpr int BM = 128;                  // UMMA M (one CTA, accumulator rows = TMEM lanes)
 constexpr int BK = 64;                   // bf16 elements per K slice = one 128-byte swizzle row
 constexpr int kWarps = 6;                // 0: TMA producer, 1: TMEM owner + MMA issuer, 2-5: epilogue
 constexpr int kThreads = kWarps * 32;
-constexpr unsigned long long kWaitNs = 2000000000ull;  // bounded waits: 2 s
+constexpr unsigned long long kWaitNs = 2000000000ull;  // limit of one wait: 2 s without progress
 
 struct KParams {
   int M, N, K;
@@ -27,6 +57,7 @@ struct KParams {
   float alpha, beta;
   UmmaEpilogue e;
   int* err;
+  unsigned long long wait_ns;  // limit of one mbarrier wait
 };
 
 // products (plane of A, plane of B) kept for NP planes: the pairs of combined order < NP, listed
@@ -34,64 +65,6 @@ struct KParams {
 __host__ __device__ constexpr int n_terms(int np) { return np == 1 ? 1 : np == 2 ? 3 : 6; }
 __host__ __device__ constexpr int term_a(int t) { return t < 2 ? 0 : t == 2 ? 1 : t == 3 ? 0 : t == 4 ? 1 : 2; }
 __host__ __device__ constexpr int term_b(int t) { return t == 0 ? 0 : t == 1 ? 1 : t == 2 ? 0 : t == 3 ? 2 : t == 4 ? 1 : 0; }
-
-__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(su32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ unsigned long long gtimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-// Bounded wait for the phase with the given parity; false when the deadline passes.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long deadline) {
-  uint32_t spins = 0;
-  while (!mbar_try_wait(bar, parity)) {
-    if ((++spins & 255u) == 0u && gtimer() > deadline) return false;
-  }
-  return true;
-}
-
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
-      ::"r"(su32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(su32(bar)), "r"(c0), "r"(c1), "r"(c2)
-      : "memory");
-}
-
-__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// K-major operand tile, 128-byte swizzle: rows of 128 bytes, 8-row groups 1024 bytes apart.
-__device__ __forceinline__ uint64_t smem_desc(const void* tile) {
-  const uint64_t addr = su32(tile);
-  uint64_t d = 0;
-  d |= (addr & 0x3FFFFull) >> 4;        // start address
-  d |= uint64_t(1) << 16;               // leading byte offset (unused for swizzled K-major)
-  d |= uint64_t(1024 >> 4) << 32;       // stride byte offset: next 8-row group
-  d |= uint64_t(1) << 46;               // descriptor version (sm_100)
-  d |= uint64_t(2) << 61;               // SWIZZLE_128B
-  return d;
-}
 
 template <int BN>
 __host__ __device__ constexpr uint32_t instr_desc() {
@@ -111,23 +84,6 @@ __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint6
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
       ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2),
         "r"(mask3));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 template <int BN>
@@ -375,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
   __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_slot;
-  const unsigned long long deadline = gtimer() + kWaitNs;
+  const unsigned long long wait_ns = p.wait_ns;  // each wait may take this long from its own start
 
   if (warp == 0) {
     if (lane == 0) {  // TMA producer
@@ -390,7 +346,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
         for (int kt = kb; kt < ke; ++kt, ++it) {
           const int s = int(it % STAGES);
           const uint32_t ph = (it / STAGES) & 1;
-          if (!mbar_wait(&empty[s], ph ^ 1, deadline) || *s_abort) {
+          if (!mbar_wait_for(&empty[s], ph ^ 1, wait_ns) || *s_abort) {
             *s_abort = 1;
             stop = true;
             break;
@@ -434,7 +390,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
       }
       // drain: every issued stage must have landed before the CTA may exit
       for (uint32_t j = (it > uint32_t(STAGES) ? it - STAGES : 0u); j < it; ++j)
-        mbar_wait(&full[j % STAGES], (j / STAGES) & 1, gtimer() + kWaitNs);
+        mbar_wait_for(&full[j % STAGES], (j / STAGES) & 1, kWaitNs);
     }
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
@@ -445,7 +401,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
       for (long t = blockIdx.x; t < p.tiles && !stop; t += gridDim.x, ++lt) {
         const int b = lt & 1;
         const uint32_t aph = (uint32_t(lt) >> 1) & 1;
-        if (*s_abort || !mbar_wait(&acc_empty[b], aph ^ 1, deadline)) {
+        if (*s_abort || !mbar_wait_for(&acc_empty[b], aph ^ 1, wait_ns)) {
           *s_abort = 1;
           break;
         }
@@ -457,7 +413,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
         for (int kt = kb; kt < ke; ++kt, ++it) {
           const int s = int(it % STAGES);
           const uint32_t ph = (it / STAGES) & 1;
-          if (*s_abort || !mbar_wait(&full[s], ph, deadline)) {
+          if (*s_abort || !mbar_wait_for(&full[s], ph, wait_ns)) {
             *s_abort = 1;
             stop = true;
             break;
@@ -529,7 +485,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
       }
       // every MMA issued has completed before the tensor memory may be released
       umma_commit(done);
-      mbar_wait(done, 0, gtimer() + kWaitNs);
+      mbar_wait_for(done, 0, kWaitNs);
     }
   } else {  // epilogue warps 2..5 -> TMEM lane quarters 2,3,0,1
     const int q = warp & 3;
@@ -538,7 +494,7 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
     for (long t = blockIdx.x; t < p.tiles; t += gridDim.x, ++lt) {
       const int b = lt & 1;
       const uint32_t aph = (uint32_t(lt) >> 1) & 1;
-      const bool ok = mbar_wait(&acc_full[b], aph, deadline);
+      const bool ok = mbar_wait_for(&acc_full[b], aph, wait_ns);
       // tcgen05.ld is warp-collective: the whole warp goes on, or stops, together
       const bool go = __all_sync(0xffffffffu, ok) && !__any_sync(0xffffffffu, *s_abort != 0);
       if (!go) {
@@ -563,23 +519,6 @@ __global__ void __launch_bounds__(kThreads, 1) umma_gemm_kernel(const __grid_con
 }
 
 // ---- host side: tensor maps ---------------------------------------------------------------
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  });
-  return fn;
-}
-
 int make_map(CUtensorMap* m, const void* base, long rows, long K, long ld, long batch, long bstride, int box_rows) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return record_error(SFQ_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
@@ -600,18 +539,6 @@ int make_map(CUtensorMap* m, const void* base, long rows, long K, long ld, long 
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return record_error(SFQ_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
   return SFQ_OK;
-}
-
-int sm_count() {
-  static int counts[64] = {0};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-  if (!counts[dev]) {
-    int n = 0;
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
-    counts[dev] = n;
-  }
-  return counts[dev];
 }
 
 template <int BN, int STAGES, int NP, bool JOINT = false>
@@ -676,6 +603,7 @@ int launch(const UmmaGemmDesc& d, cudaStream_t st) {
   kp.C = d.C; kp.ldc = d.ldc; kp.sCb = d.sCb; kp.sCk = d.sCk; kp.alpha = d.alpha; kp.beta = d.beta;
   kp.e = e;
   kp.err = d.err;
+  kp.wait_ns = d.wait_ns ? d.wait_ns : kWaitNs;
   if (JOINT && !cb) return record_error(SFQ_ERR_ARG, "umma_gemm: the joint layout is for complex B only");
   auto k = umma_gemm_kernel<BN, STAGES, NP, JOINT>;
   SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));

@@ -18,8 +18,9 @@
 // thread issues tcgen05.mma (M = 128, N = BN, K = 16) on the smem descriptors and commits each
 // stage back to the TMA producer; the accumulator is double-buffered in tensor memory, so four
 // epilogue warps drain tile i (tcgen05.ld) while the tensor core computes tile i + 1.  Every
-// mbarrier wait is bounded: on expiry the kernel records SFQ_ERR_TIMEOUT in *err, waits for its
-// own TMA loads and MMAs, frees its tensor memory and returns.
+// mbarrier wait is bounded, each from its own start (a launch that keeps making progress may run
+// for any time): on expiry the kernel records SFQ_ERR_TIMEOUT in *err, waits for its own TMA
+// loads and MMAs, frees its tensor memory and returns.
 //
 // The epilogue is selectable, so that the elementwise work around the products of the mixed
 // propagation happens while the tile is still on chip:
@@ -90,6 +91,7 @@ struct UmmaGemmDesc {
   int cplx_half = 0, cplx_nmo = 0, cplx_ldh = 0;
   UmmaEpilogue epi;
   int* err = nullptr;     // device flag, SFQ_ERR_TIMEOUT on an expired wait (may be null)
+  unsigned long long wait_ns = 0;  // limit of one mbarrier wait without progress (0: 2 s)
 };
 
 int umma_gemm(const UmmaGemmDesc& d, cudaStream_t st);
