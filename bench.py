@@ -5,16 +5,17 @@ A "step" is one iteration of run_afqmc's loop in its equilibration phase: Propag
 walker (force bias, fields, vHS, P1 + order-6 Taylor exp, overlap, walker update, weight bound),
 orthogonalization every 5 steps and comb population control every 20 steps amortised into the
 steps they fall on, and the Eshift relaxation from the growth estimator.  Workload (default): synthetic dense-Cholesky
-system M=400, N=100+100 (closed shell), Nchol=2400, 256 walkers, dt=0.005, Philox fields.
+system M=400, N=100+100 (closed shell), Nchol=2400, 256 walkers, dt=0.0005, Philox fields, the
+products from int8 slices with exact accumulation (INT8X3), against the FP64 drop-in in the same run.
 
   value       device time (CUDA events on the engine stream), inputs resident in HBM
   e2e         the same steps through sfq_engine_propagate_host: the step's field uniforms are
               copied from pinned host memory and the walker properties read back every step
-  roofline    the dominant kernel (the vHS GEMM) timed with CUDA events inside this run
+  roofline    the dominant kernel (one Taylor-term product) timed with CUDA events inside this run
   cpu_baseline the FP64 oracle (numpy + LAPACK/BLAS) on a bounded walker sample, on host cores
 
 --impl reference times the CPU restatement of the reference's path (the oracle) on the same
-configuration, with all host threads.  Under torchrun every rank runs an independent walker
+configuration, walkers split over all host threads with one BLAS thread each.  Under torchrun every rank runs an independent walker
 population of the same system (replicas; weak scaling); timings are max over ranks.
 """
 import argparse
@@ -36,12 +37,15 @@ sys.path.insert(0, ROOT)
 # walker within a few steps (the oracle shows it; the reference's comb then aborts), so those
 # systems run at the dt where |vHS| ~ 0.5-0.7 per step.  The work per step does not depend on dt.
 CONFIGS = {
-    "large": dict(spec="CFG_LARGE", nwalk=256, cpu_walkers=32, dt=0.0005),
+    "large": dict(spec="CFG_LARGE", nwalk=256, cpu_walkers=64, dt=0.0005),
     "medium": dict(spec="CFG_MEDIUM", nwalk=1024, cpu_walkers=64, dt=0.002),
     "small": dict(spec="CFG_SMALL", nwalk=32, cpu_walkers=32, dt=0.005),
 }
 ORTHO_EVERY = 5
 POP_EVERY = 20
+# DRAM bytes (read + write) of one Taylor-term int8 product at 64 walkers, M = 400, N = 100, from an
+# ncu capture (profiles/islice_taylor_M400_N100_W64_full.md); None until captured
+TAYLOR_DRAM_BYTES_64 = None
 EQUIL_STEPS = 100  # run_afqmc relaxes Eshift every step for the first equilibration_steps
 RELAX = 1.0 - math.exp(-10.0 / EQUIL_STEPS)
 
@@ -49,6 +53,12 @@ RELAX = 1.0 - math.exp(-10.0 / EQUIL_STEPS)
 def step_flops(M, N, Nc):
     """Algorithmic flops per walker-step (complex multiply-add = 8 real flops)."""
     return 8 * N * M * Nc + 4 * M * M * Nc + 64 * M * M * N + 24 * N * N * M + (32 / 3) * N ** 3
+
+
+def taylor_flops(M, N, W):
+    """Algorithmic flops of one Taylor-term launch: every walker's complex (M x M) vHS times its
+    complex (M x N) term, 8 real flops per complex multiply-add."""
+    return 8.0 * M * M * N * W
 
 
 def vhs_flops(M, Nc, W, packed):
@@ -147,71 +157,78 @@ def fp64_gemm_peak_tflops(dev):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def cpu_baseline(cfg, steps=2, warm=1):
-    """The FP64 oracle on a bounded walker sample of the same system, on this host's cores."""
-    from oracle import afqmc_oracle as O
-    from safire_b200 import synthetic
-    spec = getattr(synthetic, cfg["spec"])
-    s = synthetic.make_system(spec)
-    Ws = cfg["cpu_walkers"]
-    ham = O.Hamiltonian(s.hcore, s.Likn, s.PsiT)
-    dt = cfg["dt"]
-    prop = O.Propagator(ham, dt, seed=0)
-    wo = O.Walkers(s.initial_walkers(Ws))
-    Esh = O.init_walkers(ham, wo)
-    for st in range(warm):
-        prop.propagate(wo, Esh, st)
-    t0 = time.perf_counter()
-    for st in range(warm, warm + steps):
-        prop.propagate(wo, Esh, st)
-        if st % ORTHO_EVERY == 0:
-            prop.orthogonalize(wo)
-        Esh += RELAX * (O.average_pseudo_energy(wo, dt) - Esh)
-    t = time.perf_counter() - t0
-    return dict(value=Ws * steps / t, unit="walker-steps/s", cores=os.cpu_count(), kind="port",
-                sample=f"{Ws} walkers x {steps} steps of {spec.name} (after {warm} warm-up), FP64 numpy/OpenBLAS")
+def workload_config(cfg, spec, precision, world):
+    """The workload both arms report (the same dict, so their lines describe the same config)."""
+    return {"workload": f"AFQMC propagation {spec.name}: dense real Cholesky, closed shell, "
+                        f"{cfg['nwalk']} walkers per GPU",
+            "M": spec.M, "N": spec.N, "Nchol": spec.Nc, "walkers_per_gpu": cfg["nwalk"], "dt": cfg["dt"],
+            "precision": precision, "eshift": "relaxed every step (equilibration phase of run_afqmc)",
+            "taylor_order": 6, "ortho_every": ORTHO_EVERY, "popcontrol_every": POP_EVERY,
+            "l2": "inputs larger than L2 (Likn alone is %.2f GB)" % (spec.M ** 2 * spec.Nc * 8 / 1e9),
+            "parallelism": f"replicas x{world}"}
 
 
-def run_reference(args, cfg):
-    """--impl reference: the oracle (CPU restatement of the reference path), all host threads."""
+def cpu_port_rate(cfg, steps=5, warm=2, walkers=None, with_popcontrol=False):
+    """The FP64 oracle (numpy/LAPACK restatement of the reference path) on a bounded walker sample of
+    the same system, as the reference runs on CPUs: walkers split over one worker per host core
+    (execute.cpp:140, one thread per rank), each worker's BLAS on one thread
+    (threading.cpp:27-36).  2 warm-up steps, then `steps` timed steps (orthogonalization every 5,
+    Eshift relaxed; the comb only with with_popcontrol, global over the sample)."""
+    import concurrent.futures as cf
+    from threadpoolctl import threadpool_limits
     from oracle import afqmc_oracle as O
     from oracle import philox
     from safire_b200 import synthetic
     spec = getattr(synthetic, cfg["spec"])
     s = synthetic.make_system(spec)
-    Ws = cfg["cpu_walkers"]
+    Ws = walkers or cfg["cpu_walkers"]
+    cores = os.cpu_count() or 1
+    nthr = max(1, min(cores, Ws))
     ham = O.Hamiltonian(s.hcore, s.Likn, s.PsiT)
     dt = cfg["dt"]
-    prop = O.Propagator(ham, dt, seed=0)
-    wo = O.Walkers(s.initial_walkers(Ws))
-    state = {"Esh": O.init_walkers(ham, wo)}
+    shards = [Ws // nthr + (1 if r < Ws % nthr else 0) for r in range(nthr)]
+    props = [O.Propagator(ham, dt, seed=r) for r in range(nthr)]
+    wsets = [O.Walkers(s.initial_walkers(n)) for n in shards]
+    Esh = [O.init_walkers(ham, w) for w in wsets]
 
-    def one(st):
-        prop.propagate(wo, state["Esh"], st)
+    def shard_step(r, st):
+        props[r].propagate(wsets[r], Esh[r], st)
         if st % ORTHO_EVERY == 0:
-            prop.orthogonalize(wo)
-        if st % POP_EVERY == 0:
-            O.population_control(wo, philox.comb_uniform(0, st))
-        state["Esh"] += RELAX * (O.average_pseudo_energy(wo, dt) - state["Esh"])
+            props[r].orthogonalize(wsets[r])
+        Esh[r] += RELAX * (O.average_pseudo_energy(wsets[r], dt) - Esh[r])
 
-    for st in range(args.warmup):
-        one(st)
-    t0 = time.perf_counter()
-    for st in range(args.warmup, args.warmup + args.steps):
-        one(st)
-    t = time.perf_counter() - t0
-    value = Ws * args.steps / t
-    unit = "walker-steps/s"
+    with threadpool_limits(limits=1), cf.ThreadPoolExecutor(max_workers=nthr) as ex:
+        def step(st):
+            list(ex.map(lambda r: shard_step(r, st), range(nthr)))
+            if with_popcontrol and st % POP_EVERY == 0:
+                for r in range(nthr):
+                    O.population_control(wsets[r], philox.comb_uniform(r, st))
+
+        for st in range(warm):
+            step(st)
+        t0 = time.perf_counter()
+        for st in range(warm, warm + steps):
+            step(st)
+        t = time.perf_counter() - t0
+    return dict(value=Ws * steps / t, unit="walker-steps/s", cores=nthr, kind="port",
+                sample=f"{Ws} walkers of {spec.name} split over {nthr} host threads (BLAS 1 thread each), "
+                       f"{steps} timed steps after {warm} warm-up; FP64 numpy/LAPACK restatement of the "
+                       "reference path", seconds=t)
+
+
+def run_reference(args, cfg):
+    """--impl reference: the reference's path on the host cores (the oracle port, since the reference
+    itself cannot be built here), on the same workload; each step a bounded walker sample."""
+    from safire_b200 import synthetic
+    spec = getattr(synthetic, cfg["spec"])
+    r = cpu_port_rate(cfg, steps=args.steps, warm=args.warmup, with_popcontrol=True)
+    value, unit = r["value"], r["unit"]
     line = {"impl": "reference", "metric": "walker-steps/s", "value": value, "unit": unit, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"AFQMC propagation {spec.name} (dense real Cholesky, closed shell, "
-                                   f"{cfg['nwalk']} walkers; CPU sample {Ws} walkers per step)",
-                       "M": spec.M, "N": spec.N, "Nchol": spec.Nc, "walkers": cfg["nwalk"], "dt": dt,
-                       "ortho_every": ORTHO_EVERY, "popcontrol_every": POP_EVERY},
-            "cpu_baseline": {"value": value, "unit": unit, "cores": os.cpu_count(), "kind": "port",
-                             "sample": f"{Ws} walkers per step, {args.steps} timed steps after {args.warmup} warm-up; "
-                                       "oracle = FP64 numpy/LAPACK restatement of the reference path"},
+            "config": workload_config(cfg, spec, args.precision, args.gpus),
+            "cpu_baseline": {"value": value, "unit": unit, "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -239,6 +256,26 @@ def step_errors(eng, eng64, W, spec, Eshift, step):
             "local_energy_E1": rel(E[:, 0], E64[:, 0]), "local_energy_EXX": rel(E[:, 1], E64[:, 1]),
             "local_energy_EJ": rel(E[:, 2], E64[:, 2]), "local_energy": rel(E.sum(1), E64.sum(1)),
             "how": "one step of both engines from identical walkers and seeded fields; max |mixed - fp64| / max |fp64|"}
+
+
+def seeded_block_delta(s, W, DT, prec, seed, steps):
+    """Block energy difference (mHa) of `prec` against the FP64 drop-in after `steps` steps of the
+    benchmark's schedule from the same seed (untimed)."""
+    from safire_b200 import afqmc, capi
+    E = {}
+    for p in (capi.PRECISION_FP64, prec):
+        eng = afqmc.AfqmcEngine(s, W, dt=DT, seed=seed, device=0, precision=p)
+        Esh = eng.init()
+        for st in range(steps):
+            eng.propagate(Esh, st)
+            if st % ORTHO_EVERY == 0:
+                eng.orthogonalize()
+            if st % POP_EVERY == 0:
+                eng.population_control(st)
+            Esh += RELAX * (eng.averages()[0] - Esh)
+        E[p] = eng.measure()["Energy"].real
+        eng.close()
+    return 1e3 * (E[prec] - E[capi.PRECISION_FP64])
 
 
 def run_engine(args, cfg, spec, s, W, DT, prec, rank, local, profile_pass=True, e2e=True):
@@ -331,11 +368,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="large", choices=sorted(CONFIGS))
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed-fp32"])
+    ap.add_argument("--precision", default="int8x3", choices=["fp64", "int8x3", "int8x2", "mixed", "mixed-fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 drop-in comparison run")
     ap.add_argument("--no-autotune", action="store_true", help="keep the built-in tile widths")
+    ap.add_argument("--compare-seeds", type=int, default=5,
+                    help="further seeds for the block-energy comparison against FP64 (untimed)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -360,8 +399,8 @@ def main():
     W = cfg["nwalk"]
     DT = cfg["dt"]
     s = synthetic.make_system(spec)
-    prec = {"fp64": capi.PRECISION_FP64, "mixed": capi.PRECISION_MIXED,
-            "mixed-fp32": capi.PRECISION_MIXED_FP32}[args.precision]
+    prec = {"fp64": capi.PRECISION_FP64, "mixed": capi.PRECISION_MIXED, "mixed-fp32": capi.PRECISION_MIXED_FP32,
+            "int8x3": capi.PRECISION_INT8X3, "int8x2": capi.PRECISION_INT8X2}[args.precision]
     if dist:
         dist.barrier()
     eng, m = run_engine(args, cfg, spec, s, W, DT, prec, rank, local, e2e=not args.no_e2e)
@@ -394,52 +433,87 @@ def main():
                    "block_energy_delta_rel": (m["energy"] - m64["energy"]) / abs(m64["energy"]),
                    "block": f"energy measured after the {args.warmup}+{args.steps} steps of each timed run",
                    "step_errors": errors}
+        if args.compare_seeds > 0 and rank == 0:
+            # the same comparison from further seeds (untimed): the fixed-point slices' noise moves
+            # one seeded block either way; a bias would show in the mean
+            ds = [compare["block_energy_delta_mHa"]]
+            for sd in range(1, args.compare_seeds + 1):
+                ds.append(seeded_block_delta(s, W, DT, prec, sd, args.warmup + args.steps))
+            d = np.array(ds)
+            compare["seeds"] = {"seeds": [replicas.seed_for(rank)] + list(range(1, args.compare_seeds + 1)),
+                                "block_energy_delta_mHa": [float(x) for x in d],
+                                "mean_mHa": float(d.mean()),
+                                "sem_mHa": float(d.std(ddof=1) / math.sqrt(len(d))),
+                                "max_abs_mHa": float(np.max(np.abs(d)))}
     eng.close()
     del eng
 
-    # ---- roofline of the dominant kernel: the vHS product ---------------------------------
+    # ---- roofline of the dominant kernel: the Taylor-term product --------------------------
     ph = m["phases"]
-    g_ms, g_n = ph["vHS_gemm"]
-    launch_ms = g_ms / max(g_n, 1)
-    alg = vhs_flops(spec.M, spec.Nc, W, m["vhs_packed"])
-    achieved = alg / (launch_ms * 1e-3) / 1e12
     peaks = measured_peaks()
+    t_ms, t_n = ph["taylor_gemm"]
+    launch_ms = t_ms / max(t_n, 1)
+    alg = taylor_flops(spec.M, spec.N, W)
+    achieved = alg / (launch_ms * 1e-3) / 1e12
+    v_ms, v_n = ph["vHS_gemm"]
+    v_launch = v_ms / max(v_n, 1)
+    v_alg = vhs_flops(spec.M, spec.Nc, W, m["vhs_packed"])
     if prec == capi.PRECISION_FP64:
         peak = fp64_gemm_peak_tflops(local)
-        roofline = {"bound": "tensor", "kernel": "gemm_f64_kernel (vHS: complex X x real Likn, DMMA m8n8k4)",
+        roofline = {"bound": "tensor", "kernel": "gemm_f64_kernel (Taylor term: complex vHS x complex walkers, DMMA)",
                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in the peaks file)"}
     else:
-        nprod = 3 if prec == capi.PRECISION_MIXED else 6
         peak = peaks.get("bf16_tflops_sustained") or 1400.0
-        src = "MEASURED_PEAKS.json bf16_tflops_sustained (kernel timed inside a long step)" \
-            if peaks.get("bf16_tflops_sustained") else "fallback 1.4 PFLOP/s sustained"
-        roofline = {"bound": "tensor",
-                    "kernel": f"umma_gemm_kernel (vHS: split-BF16 tcgen05, {nprod} tensor-core products per real product)",
-                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                    "executed_tflops": achieved * nprod, "executed_frac": achieved * nprod / peak,
-                    "peak_source": src}
+        src = ("MEASURED_PEAKS.json bf16_tflops_sustained, of measured (kernel timed inside a long step)"
+               if peaks.get("bf16_tflops_sustained") else "fallback 1.4 PFLOP/s sustained")
+        if prec in (capi.PRECISION_INT8X3, capi.PRECISION_INT8X2):
+            ns = 3 if prec == capi.PRECISION_INT8X3 else 2
+            npairs = 6 if ns == 3 else 3
+            # the complex product runs as [re|im] += A_re [Vr;Vi]^T, re += (-A_im) Vi^T, im += A_im Vr^T:
+            # 2 real products' worth of work per complex one, times the slice pairs, on rows padded
+            # to 128 and orbitals to the tile
+            rows = 128 * ((spec.N + 127) // 128)
+            kpad = 32 * ((spec.M + 31) // 32)
+            executed = 2.0 * 2 * rows * (2 * spec.M) * kpad * W * npairs
+            roofline = {"bound": "tensor",
+                        "kernel": f"islice_gemm_kernel (Taylor term: int8 slices x{ns}, tcgen05 kind::i8, exact "
+                                  f"int32 accumulation, {npairs} int8 products per real product)",
+                        "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                        "executed_int8_tops": executed / (launch_ms * 1e-3) / 1e12,
+                        "executed_frac_of_int8": executed / (launch_ms * 1e-3) / 1e12 / (2 * peak),
+                        "int8_peak_note": "int8 tensor rate taken as twice the measured bf16 rate (B200's ratio)",
+                        "peak_source": src}
+        else:
+            nprod = 3 if prec == capi.PRECISION_MIXED else 6
+            roofline = {"bound": "tensor",
+                        "kernel": f"umma_gemm_kernel (Taylor term: split-BF16 tcgen05, {nprod} tensor-core products "
+                                  "per real product)",
+                        "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                        "executed_tflops": achieved * nprod * 2, "peak_source": src}
     traffic = None
-    if prec == capi.PRECISION_MIXED and m["vhs_packed"] and W == 256 and spec.Nc == 2400:
-        # dram__bytes_read.sum + dram__bytes_write.sum of this kernel in one ncu capture of the same
-        # product with 80089 rows, 256 walkers, Nc = 2400
-        # (profiles/umma_gemm_vhs_packed_rows80089_W256_Nc2400_full.md: 779.1 + 153.2 MB), scaled
-        # by the rows of this system (both operand and result bytes grow with the rows)
-        rows = spec.M * (spec.M + 1) // 2
-        traffic = (779.1e6 + 153.2e6) * rows / 80089.0
+    if prec == capi.PRECISION_INT8X3 and spec.M == 400 and spec.N == 100:
+        # dram__bytes_read.sum + dram__bytes_write.sum of the Taylor product in one ncu capture of
+        # sfq_gemm_int8_cplx_b at 64 walkers, M = 400, N = 100 (the same kernel and tile),
+        # scaled to this launch's walkers: every byte moved is per walker
+        traffic = TAYLOR_DRAM_BYTES_64 * W / 64.0 if TAYLOR_DRAM_BYTES_64 else None
         roofline.update({"traffic_unit": "bytes per launch",
-                         "traffic_source": "ncu capture of the same product (80089 rows), scaled to this system's rows",
-                         "algorithmic_bytes_per_launch": 2 * 2.0 * rows * spec.Nc + 2 * 2.0 * 2 * W * spec.Nc
-                         + 4.0 * 2 * W * rows})
-    roofline.update({"algorithmic_flops_per_launch": alg, "launch_ms": launch_ms, "traffic": traffic,
-                     "vhs_columns": "packed upper triangle M(M+1)/2" if m["vhs_packed"] else "full M*M"})
-    tot = sum(v[0] for k, v in ph.items() if k != "vHS_gemm")
+                         "traffic_source": "ncu capture of the same product at 64 walkers, scaled by walkers",
+                         "algorithmic_bytes_per_launch": W * (3.0 * 2 * spec.M * spec.M + 3.0 * 3 * spec.N * spec.M
+                                                              + 4.0 * 2 * spec.N * spec.M)})
+    roofline.update({"algorithmic_flops_per_launch": alg, "launch_ms": launch_ms, "launches_timed": t_n,
+                     "traffic": traffic,
+                     "vhs_product": {"launch_ms": v_launch, "algorithmic_flops_per_launch": v_alg,
+                                     "achieved": v_alg / (v_launch * 1e-3) / 1e12 if v_launch else None,
+                                     "columns": "packed upper triangle M(M+1)/2" if m["vhs_packed"] else "full M*M"}})
+    tot = sum(v[0] for k, v in ph.items() if k not in ("vHS_gemm", "taylor_gemm"))
     phases = {k: {"ms_per_step": v[0] / args.steps, "share": v[0] / tot if tot else None}
-              for k, v in ph.items() if v[1] > 0 and k != "vHS_gemm"}
+              for k, v in ph.items() if v[1] > 0 and k not in ("vHS_gemm", "taylor_gemm")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(cfg)
+        cpu = cpu_port_rate(cfg)
+        cpu.pop("seconds", None)
 
     if dist:
         dist.barrier()
@@ -447,17 +521,12 @@ def main():
     if rank != 0:
         return
     dtype = {"fp64": "f64", "mixed": "bf16x3 split (fp32 accumulate) + f64", "mixed-fp32":
-             "bf16x6 split (fp32 accumulate) + f64"}[args.precision]
+             "bf16x6 split (fp32 accumulate) + f64", "int8x3": "int8 slices x3 (exact int32 accumulate) + f64",
+             "int8x2": "int8 slices x2 (exact int32 accumulate) + f64"}[args.precision]
     line = {"metric": "walker-steps/s", "value": value, "unit": "walker-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
-            "config": {"workload": f"AFQMC propagation {spec.name}: dense real Cholesky, closed shell, "
-                                   f"{W} walkers per GPU, precision {args.precision}",
-                       "M": spec.M, "N": spec.N, "Nchol": spec.Nc, "walkers_per_gpu": W, "dt": DT,
-                       "eshift": "relaxed every step (equilibration phase of run_afqmc)",
-                       "taylor_order": 6, "ortho_every": ORTHO_EVERY, "popcontrol_every": POP_EVERY,
-                       "l2": "inputs larger than L2 (Likn alone is %.2f GB)" % (spec.M ** 2 * spec.Nc * 8 / 1e9),
-                       "parallelism": f"replicas x{world}", "tiles": m.get("tiles")},
+            "config": workload_config(cfg, spec, args.precision, world), "tiles": m.get("tiles"),
             "algorithmic_tflops": step_flops(spec.M, spec.N, spec.Nc) * W * args.steps * world / (ms * 1e-3) / 1e12,
             "gpu_launches": m["launches"], "clocks": m["clocks"], "e2e": e2e, "roofline": roofline,
             "fp64_comparison": compare, "phases": phases, "cpu_baseline": cpu}

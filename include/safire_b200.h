@@ -476,7 +476,8 @@ enum sfq_phase {
   SFQ_PH_POPCONTROL = 8,  /* comb + walker copies */
   SFQ_PH_ENERGY = 9,      /* local energy */
   SFQ_PH_VHS_GEMM = 10,   /* the vHS matrix product alone (inside SFQ_PH_VHS) */
-  SFQ_NUM_PHASES = 11
+  SFQ_PH_TAYLOR_GEMM = 11, /* the Taylor terms' matrix products alone (inside SFQ_PH_PROPAGATE), one per term */
+  SFQ_NUM_PHASES = 12
 };
 int sfq_engine_profile(sfq_engine_t e, int enable);
 /* synchronizes; ms[ph] = summed device time since the last call, counts[ph] = intervals (either may be NULL) */

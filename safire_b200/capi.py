@@ -17,7 +17,7 @@ OP_MIXED_DENSITY_MATRIX, OP_LOG_OVERLAP, OP_PROPAGATE, OP_ORTHOGONALIZE, OP_ENER
 # walker property columns, in the order the engine stores them (WalkerConfig.hpp:28-48 names)
 PROPS = ("WEIGHT", "PHASE", "PSEUDO_ELOC_", "E1_", "EXX_", "EJ_", "OVLP", "THETA")
 PHASES = ("density", "vbias", "fields", "vHS", "propagate", "overlap", "update", "ortho", "popcontrol", "energy",
-          "vHS_gemm")
+          "vHS_gemm", "taylor_gemm")
 
 
 class SafireError(RuntimeError):

@@ -409,9 +409,8 @@ struct Engine {
   int8_t* Xq_q[3] = {};  int* Xq_e = nullptr;   // fields, planar rows (c, w) over n
   int8_t* V_q[3] = {};   int* V_e = nullptr;  int* V_emax = nullptr;  // V[w][c][i][k], exponent per (w, i)
   int8_t* A_q[2][3] = {};  int8_t* A_n[2][3] = {};  int* A_e[2] = {};  // walker operand: rows (c, r); -im rows r
-  int8_t* Tb_q[3] = {};  int* Tb_e = nullptr;   // [[Tr, -Ti], [Ti, Tr]] of the inverse overlaps, rows (w, c, a)
-  int8_t* Ws_q[3] = {};  int* Ws_e = nullptr;   // the walkers read as reals, rows (w, k) over (b, c')
-  long ld_2n = 0;
+  cplx* GT_c = nullptr;  // the trial's own G (N, M) and force bias (Nc), FP64
+  cplx* vbT = nullptr;
   float* Cp = nullptr;  // FP32 output of the walker-shaped products, planar (2 W N, M)
   int i8_vb_bn = 160, i8_vb_ks = 1, i8_bn = 160, i8_half = 80;
   double* h_pinned = nullptr;  // pinned host staging for e2e calls
@@ -578,8 +577,6 @@ struct Engine {
           mx.push_back({(void**)&A_q[b][q], (size_t)2 * R * ld_m});
           mx.push_back({(void**)&A_n[b][q], (size_t)R * ld_m});
         }
-        mx.push_back({(void**)&Tb_q[q], (size_t)W * 2 * N * ld_2n});
-        mx.push_back({(void**)&Ws_q[q], (size_t)W * M * ld_2n});
       }
       const size_t ie = sizeof(int);
       std::vector<Item> mx2 = {
@@ -587,7 +584,7 @@ struct Engine {
           {(void**)&P1_e, ie * M}, {(void**)&Gv_e, ie * 2 * W}, {(void**)&Ge_e, ie * 2 * R},
           {(void**)&Xq_e, ie * 2 * W}, {(void**)&V_e, ie * W * M}, {(void**)&V_emax, ie * W * M},
           {(void**)&A_e[0], ie * R}, {(void**)&A_e[1], ie * R},
-          {(void**)&Tb_e, ie * 2 * R}, {(void**)&Ws_e, ie * W * M},
+          {(void**)&GT_c, c * (size_t)N * M}, {(void**)&vbT, c * (size_t)Nc},
           {(void**)&Cvb, sizeof(float) * i8_vb_ks * 2 * (size_t)W * Nc},
           {(void**)&Cv, sizeof(float) * 2 * W * vrows},
           {(void**)&Sacc, sizeof(float) * 2 * R * M},
@@ -807,9 +804,23 @@ struct Engine {
         if ((rc = threshold_real(P1, MM, 1e-8, st))) return rc;
       }
     }
-    // exact-accumulation mode: int8 slices of the resident real tensors
+    // exact-accumulation mode: int8 slices of the resident real tensors, and the trial's own G and
+    // force bias (NOMSD::vMF before its real part is taken)
     if (mixed && nslices) {
       const long NM = (long)N * M;
+      {
+        std::vector<cplx> psi(size_t(M) * N);  // PsiT^H (M x N)
+        for (int a = 0; a < N; ++a)
+          for (int i = 0; i < M; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * M + i]);
+        SFQ_CUDA_TRY(cudaMemcpyAsync(SM2, psi.data(), sizeof(cplx) * M * N, cudaMemcpyHostToDevice, st));
+        if ((rc = ops::overlap_matrix(PsiT, true, SM2, T, 1, M, N, st))) return rc;
+        if ((rc = lu_logdet(T, (long)N * N, 1, N, ovtmp, false, 1.0, true, st))) return rc;
+        if ((rc = ops::green_compact(T, SM2, G, 1, M, N, st))) return rc;
+        SFQ_CUDA_TRY(cudaMemcpyAsync(GT_c, G, sizeof(cplx) * NM, cudaMemcpyDeviceToDevice, st));
+        if ((rc = ops::vbias(G, Lnak, false, X, 1, N, M, Nc, vb_scale(), st))) return rc;
+        SFQ_CUDA_TRY(cudaMemcpyAsync(vbT, X, sizeof(cplx) * Nc, cudaMemcpyDeviceToDevice, st));
+        SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+      }
       const double* Ln = (const double*)Lnak;
       if ((rc = islice_rows_real(Ln, Nc, NM, NM, nslices, Lv_q, ld_nm, Lv_e, st))) return rc;
       if ((rc = islice_rows_real(Ln, (long)Nc * N, M, M, nslices, Le_q, ld_m, Le_e, st))) return rc;
@@ -1598,7 +1609,6 @@ struct Engine {
     ld_m = round16(M);
     ld_nm = round16((long)N * M);
     ld_nc = round16(Nc);
-    ld_2n = round16(2L * N);
     int best = 0;
     long best_pad = 1L << 40;
     for (int h : {32, 64, 80}) {
@@ -1666,35 +1676,18 @@ struct Engine {
     return islice_gemm(d, st);
   }
 
-  // the force bias's G = (W Tinv)^T from int8 slices: rows (c, a) of [[Tr, -Ti], [Ti, Tr]] of the
-  // (cached FP64) inverse overlaps against each walker read as reals (K = (b, c')), written planar
-  // (c, w, a, k) in FP32 and sliced as the force bias's rows (c, w) over (a, k)
-  int density_i8() {
-    int rc;
-    if ((rc = ensure_inverse(nullptr))) return rc;
-    if ((rc = islice_tblk(T, W, N, nslices, Tb_q, ld_2n, Tb_e, st))) return rc;
-    if ((rc = islice_rows_real(reinterpret_cast<const double*>(SM), (long)W * M, 2L * N, 2L * N, nslices, Ws_q,
-                               ld_2n, Ws_e, st)))
-      return rc;
-    IsliceGemmDesc d = i8_desc();
-    d.M = 2 * N; d.N = M; d.K = 2 * N; d.batch = W;
-    d.A = i8_operand(Tb_q, 2L * N, ld_2n, Tb_e, 2L * N * ld_2n, 2L * N);
-    d.B = i8_operand(Ws_q, M, ld_2n, Ws_e, (long)M * ld_2n, M);
-    d.bn = i8_bn;
-    d.C = Cp; d.ldc = M; d.sCb = (long)N * M; d.row_split = N; d.sCc = (long)W * N * M;
-    if ((rc = islice_gemm(d, st))) return rc;
-    return islice_rows_real_f32(Cp, 2L * W, (long)N * M, (long)N * M, nslices, Gv_q, ld_nm, Gv_e, st);
-  }
-
-  // AFQMCBasePropagator::Propagate with the products from int8 slices (exact accumulation): G,
-  // force bias, vHS, P1 and the Taylor terms on the tensor cores; the elementwise steps between them
-  // (T = (i/k) C, S += T, slicing) round to nearest; LU / overlaps / walker update in FP64.
+  // AFQMCBasePropagator::Propagate with the products from int8 slices (exact accumulation): force
+  // bias, vHS, P1 and the Taylor terms on the tensor cores; the elementwise steps between them
+  // (T = (i/k) C, S += T, slicing) round to nearest; G, LU / overlaps and the walker update in FP64.
+  // The force bias is the trial's own (FP64, setup) plus that of G - G_trial from slices: G's rows
+  // are dominated by entries near the trial's, which would set the fixed-point scale of the rest.
   int propagate_i8(double Eshift, unsigned long long step, const double* uniforms) {
     int rc;
     const long R = (long)W * N;
     const double sdt = std::sqrt(p.dt);
     ph_begin(SFQ_PH_DENSITY);
-    if ((rc = density_i8())) return rc;
+    if ((rc = density(nullptr))) return rc;
+    if ((rc = islice_rows_planar(G, W, (long)N * M, nslices, Gv_q, ld_nm, Gv_e, st, GT_c))) return rc;
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
     const long part = 2L * W * Nc;
@@ -1707,7 +1700,7 @@ struct Engine {
       d.C = Cvb; d.ldc = Nc;
       if ((rc = islice_gemm(d, st))) return rc;
     }
-    if ((rc = mixed_reduce_planar_to_cplx(Cvb, i8_vb_ks, part, W, Nc, 2.0 * sdt, X, st))) return rc;
+    if ((rc = mixed_reduce_planar_to_cplx(Cvb, i8_vb_ks, part, W, Nc, 2.0 * sdt, X, st, vbT))) return rc;
     ph_end(SFQ_PH_VBIAS);
     ph_begin(SFQ_PH_FIELDS);
     FieldParams fp;
@@ -1739,12 +1732,13 @@ struct Engine {
     inv_cached = false;
     // S = P1 W = W + (P1 - I) W; then T_k = (i/k) V T_{k-1}, S += T_k for k = 1..order; SM = S + (P1 - I) S
     if ((rc = islice_walkers(SM, W, M, N, nslices, A_q[0], ld_m, A_e[0], Sacc, st))) return rc;
-    if ((rc = i8_p1(0, Sacc, true))) return rc;
-    if ((rc = islice_taylor_update(nullptr, Sacc, R, M, 0, true, nslices, A_q[1], A_n[1], ld_m, A_e[1], st)))
-      return rc;
+    if ((rc = i8_p1(0, Cp, false))) return rc;
+    if ((rc = islice_taylor_update(Cp, Sacc, R, M, 0, true, nslices, A_q[1], A_n[1], ld_m, A_e[1], st))) return rc;
     int cur = 1;
     for (int k = 1; k <= p.taylor_order; ++k) {
+      ph_begin(SFQ_PH_TAYLOR_GEMM);
       if ((rc = i8_taylor(cur))) return rc;
+      ph_end(SFQ_PH_TAYLOR_GEMM);
       const bool last = k == p.taylor_order;
       if ((rc = islice_taylor_update(Cp, Sacc, R, M, k, last, nslices, A_q[1 - cur], last ? nullptr : A_n[1 - cur],
                                      ld_m, A_e[1 - cur], st)))
@@ -1871,7 +1865,9 @@ struct Engine {
       et.write = k < p.taylor_order ? 1 : 2;
       for (int q = 0; q < 3; ++q) et.out[q] = nxt[q];
       et.out_planes = nplanes;
+      ph_begin(SFQ_PH_TAYLOR_GEMM);
       if ((rc = umma_gemm(d, st))) return rc;
+      ph_end(SFQ_PH_TAYLOR_GEMM);
       std::swap(cur, nxt);
     }
     UmmaEpilogue ew;
@@ -2465,9 +2461,9 @@ int sfq_engine_create_nomsd(sfq_engine_t* out, const sfq_engine_params_t* p, con
     return record_error(SFQ_ERR_UNSUPPORTED,
                         "engine: COLLINEAR and NONCOLLINEAR walkers and multi-determinant trials run in FP64");
   }
-  if (e.nslices && !e.trial_real) {
+  if (e.nslices && (!e.trial_real || e.M > 1024)) {
     delete h;
-    return record_error(SFQ_ERR_UNSUPPORTED, "engine: the int8-slice products need a real trial");
+    return record_error(SFQ_ERR_UNSUPPORTED, "engine: the int8-slice products need a real trial and nmo <= 1024");
   }
   if (e.mixed && !e.nslices && (!e.trial_real || e.M % 8 || e.Nc % 8)) {
     delete h;

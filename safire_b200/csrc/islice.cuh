@@ -61,7 +61,6 @@ struct IsliceGemmDesc {
   const int8_t* a_nim[3] = {nullptr, nullptr, nullptr};
   float* C = nullptr;                  // FP32 output, row-major: C[s*sCk + batch*sCb + row*ldc + col]
   long ldc = 0, sCb = 0, sCc = 0;      // sCc: complex B, elements between the re and im outputs
-  int row_split = 0;                   // plain products: row r at (r / row_split) * sCc + (r % row_split) * ldc
   double alpha = 1.0;
   bool accumulate = false;             // C += alpha A B^T (one FP32 round to nearest) instead of C =
   int* err = nullptr;                  // device flag: SFQ_ERR_TIMEOUT on an expired wait (may be null)
@@ -78,25 +77,19 @@ int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st);
 // real rows: x[r][k] = src[r * lds + k]
 int islice_rows_real(const double* src, long R, long K, long lds, int nslices, int8_t* const* q, long ld, int* e,
                      cudaStream_t st);
-// FP32 real rows: x[r][k] = src[r * lds + k]
-int islice_rows_real_f32(const float* src, long R, long K, long lds, int nslices, int8_t* const* q, long ld, int* e,
-                         cudaStream_t st);
-// inverse overlaps Tinv (W, N, N) complex -> rows (w, c, a) over (b, c') of the real block
-// [[Tr, -Ti], [Ti, Tr]] at Tinv[b][a] (ld >= 2N), one exponent per (w, a): e[(w * 2 + c) * N + a]
-int islice_tblk(const cplx* Tinv, int W, int N, int nslices, int8_t* const* q, long ld, int* e, cudaStream_t st);
-// complex rows split into planar rows: row c * R + r holds part c (0 re, 1 im) of src[r * K + k],
-// with its own exponent
+// complex rows split into planar rows: row c * R + r holds part c (0 re, 1 im) of src[r * K + k]
+// (minus sub[k] when sub is given), with its own exponent
 int islice_rows_planar(const cplx* src, long R, long K, int nslices, int8_t* const* q, long ld, int* e,
-                       cudaStream_t st);
+                       cudaStream_t st, const cplx* sub = nullptr);
 // walkers SM (W, M, N) complex -> rows (c, w, a) over orbitals j (the P1 product's A operand), one
 // exponent per (w, a) for both parts: e[w * N + a]; planar (may be null): the same rows in FP32,
 // row stride M
 int islice_walkers(const cplx* SM, int W, int M, int N, int nslices, int8_t* const* q, long ld, int* e,
                    float* planar, cudaStream_t st);
-// FP32 planar walker-shaped rows S[c][r][j] (r < R = W N, j < M): with k > 0 first
-// T = (i / k) C (T_re = -C_im / k, T_im = C_re / k) and S += T; then the slices of T (k > 0 and
-// !slice_sum) or of S into q (rows (c, r)) and into the negated imaginary rows qn (rows r; may be
-// null), one exponent per r
+// planar walker-shaped FP32 rows (r < R = W N, j < M, M <= 1024), the product C[c][r][j] into the
+// sum S[c][r][j]: k = 0: S += C; k > 0: T = (i / k) C (T_re = -C_im / k, T_im = C_re / k) and
+// S += T; then the slices of S (slice_sum; required for k = 0) or of T into q (rows (c, r)) and
+// into the negated imaginary rows qn (rows r; may be null), one exponent per r
 int islice_taylor_update(const float* C, float* S, long R, int M, int k, bool slice_sum, int nslices,
                          int8_t* const* q, int8_t* const* qn, long ld, int* e, cudaStream_t st);
 // vHS (planar rows c * W + w over the packed upper triangle, or over M * M) -> V slices

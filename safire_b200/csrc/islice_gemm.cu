@@ -11,8 +11,11 @@ using namespace tc;
 constexpr int BM = 128;                  // MMA M: accumulator rows = TMEM lanes
 constexpr int BK = 128;                  // int8 elements per K slice = one 128-byte swizzle row
 constexpr int KSTEP = 32;                // K of one kind::i8 MMA
-constexpr int kWarps = 6;                // 0: TMA producer, 1: TMEM owner + MMA issuer, 2-5: epilogue
+// warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2-9 epilogue (two per TMEM lane quarter, taking
+// alternate 16-column chunks of the tile)
+constexpr int kWarps = 10;
 constexpr int kThreads = kWarps * 32;
+constexpr int kEpiThreads = 256;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // limit of one wait: 2 s without progress
 
 // slice pairs kept for NS slices, listed by group: g0 (0,0) | g1 (0,1) (1,0) | g2 (0,2) (1,1) (2,0)
@@ -67,7 +70,6 @@ struct KParams {
   const int* eb; long eb_bs, eb_mod;
   float* C;
   long ldc, sCb, sCc, sCk;
-  int row_split;
   double alpha;
   int accumulate;      // C += the product (one FP32 round to nearest) instead of C = the product
   int* err;
@@ -90,15 +92,16 @@ __device__ __forceinline__ double pow2(int e) {
   return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
-// one tile's accumulator groups at taddr (group g at column g * BN) -> FP32 output, row `row`
+// the 16-column chunks c0, c0 + 32, ... of one tile's accumulator groups at taddr (group g at column
+// g * BN) -> FP32 output, row `row`
 template <int BN, int NS>
 __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, int row, int mt, int nt, int bz,
-                                              int ks) {
+                                              int ks, int c0) {
   const int gm = mt * BM + row;
   const bool live = gm < p.M;
   const int ea = live ? p.ea[(long)bz * p.ea_bs + (p.ea_mod ? gm % p.ea_mod : gm)] : 0;
 #pragma unroll 1
-  for (int c = 0; c < BN; c += 16) {
+  for (int c = c0; c < BN; c += 32) {
     uint32_t acc[3][16];
     __syncwarp();
 #pragma unroll
@@ -116,9 +119,7 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
       col0 = nt * BN + c;
       if (col0 >= p.N) continue;
       valid = p.N - col0 < 16 ? p.N - col0 : 16;
-      const long orow = p.row_split ? (long)(gm / p.row_split) * p.sCc + (long)(gm % p.row_split) * p.ldc
-                                    : (long)gm * p.ldc;
-      obase = (long)ks * p.sCk + (long)bz * p.sCb + orow + col0;
+      obase = (long)ks * p.sCk + (long)bz * p.sCb + (long)gm * p.ldc + col0;
     }
     float v[16];
 #pragma unroll
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 128);
+      mbar_init(&acc_empty[b], kEpiThreads);
     }
     mbar_init(done, 1);
     *s_abort = 0;
@@ -319,9 +320,10 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
       umma_commit(done);
       mbar_wait_for(done, 0, kWaitNs);
     }
-  } else {  // epilogue warps 2..5 -> TMEM lane quarters 2,3,0,1
+  } else {  // epilogue warps 2..9 -> TMEM lane quarters 2,3,0,1 (a warp reaches only its quarter)
     const int q = warp & 3;
     const int row = q * 32 + lane;
+    const int c0 = 16 * ((warp - 2) >> 2);  // the two warps of a quarter take alternate 16-column chunks
     int lt = 0;
     for (long t = blockIdx.x; t < p.tiles; t += gridDim.x, ++lt) {
       const int b = BUFS == 2 ? (lt & 1) : 0;
@@ -335,7 +337,7 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
       fence_after();
       int mt, nt, bz, ks;
       decode(p, t, mt, nt, bz, ks);
-      epilogue_tile<BN, NS>(p, tmem + (uint32_t(q * 32) << 16) + uint32_t(b) * GCOLS, row, mt, nt, bz, ks);
+      epilogue_tile<BN, NS>(p, tmem + (uint32_t(q * 32) << 16) + uint32_t(b) * GCOLS, row, mt, nt, bz, ks, c0);
       fence_before();
       mbar_arrive(&acc_empty[b]);
     }
@@ -375,6 +377,7 @@ int make_map_i8(CUtensorMap* m, const void* base, long rows, long K, long ld, lo
 template <int BN, int STAGES, int NS>
 int launch(const IsliceGemmDesc& d, cudaStream_t st) {
   using L = Smem<BN, STAGES, NS>;
+  static_assert(BN % 16 == 0, "the epilogue drains whole 16-column chunks");
   constexpr int BUFS = (2 * NS * BN <= 512) ? 2 : 1;
   static_assert(L::TOTAL <= 232448, "shared memory budget");
   static_assert(NS * BN * BUFS <= 512, "accumulator groups must fit in tensor memory");
@@ -430,7 +433,6 @@ int launch(const IsliceGemmDesc& d, cudaStream_t st) {
   kp.ea = d.A.e; kp.ea_bs = d.A.e_bs; kp.ea_mod = d.A.e_mod;
   kp.eb = d.B.e; kp.eb_bs = d.B.e_bs; kp.eb_mod = cb ? 0 : d.B.e_mod;  // complex B: indexed by orbital
   kp.C = d.C; kp.ldc = d.ldc; kp.sCb = d.sCb; kp.sCc = d.sCc; kp.sCk = d.sCk;
-  kp.row_split = cb ? 0 : d.row_split;
   kp.alpha = d.alpha;
   kp.accumulate = d.accumulate ? 1 : 0;
   kp.err = d.err;
@@ -455,6 +457,7 @@ int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st) {
     case 2128: return islice::launch<128, 3, 2>(d, st);
     case 2160: return islice::launch<160, 3, 2>(d, st);
     case 3064: return islice::launch<64, 3, 3>(d, st);
+    case 3080: return islice::launch<80, 2, 3>(d, st);
     case 3128: return islice::launch<128, 2, 3>(d, st);
     case 3160: return islice::launch<160, 2, 3>(d, st);
     default:
@@ -467,10 +470,11 @@ int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st) {
 // ---- C ABI: the int8-slice products on caller operands (tests and benchmarks) ---------------
 namespace sfq {
 namespace {
-__global__ void cplx_to_planar_f32_kernel(const cplx* src, long n, float* re, float* im) {
+template <typename T>
+__global__ void cplx_to_planar_f32_kernel(const cplx* src, long n, T* re, T* im) {
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    re[t] = float(src[t].x);
-    im[t] = float(src[t].y);
+    re[t] = T(float(src[t].x));
+    im[t] = T(float(src[t].y));
   }
 }
 }  // namespace
@@ -483,7 +487,7 @@ int sfq_gemm_int8_slices(const double* A, const double* B, float* C, int M, int 
   using namespace sfq;
   if (nslices < 2 || nslices > 3) return record_error(SFQ_ERR_ARG, "nslices must be 2 or 3");
   if (M <= 0 || N <= 0 || K <= 0) return record_error(SFQ_ERR_SHAPE, "gemm_int8_slices: empty product");
-  if (tile_n != 0 && tile_n != 64 && tile_n != 128 && tile_n != 160)
+  if (tile_n != 0 && tile_n != 64 && tile_n != 80 && tile_n != 128 && tile_n != 160)
     return record_error(SFQ_ERR_ARG, "gemm_int8_slices: tile width %d not built", tile_n);
   if (!A || !B || !C) return record_error(SFQ_ERR_ARG, "gemm_int8_slices: null operand");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -535,17 +539,19 @@ int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, i
   if (half != 32 && half != 64 && half != 80)
     return record_error(SFQ_ERR_ARG, "gemm_int8_cplx_b: %d orbitals per tile not built", half);
   if (!A || !V || !C) return record_error(SFQ_ERR_ARG, "gemm_int8_cplx_b: null operand");
-  if (32L * 32 < M) return record_error(SFQ_ERR_SHAPE, "gemm_int8_cplx_b: M=%d too large", M);
+  if (M > 1024) return record_error(SFQ_ERR_SHAPE, "gemm_int8_cplx_b: M=%d above 1024", M);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const long ld = (M + 15) / 16 * 16, R = (long)W * N, MM = (long)M * M;
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-  const size_t sa = al(sizeof(float) * 2 * R * M), sv = al(sizeof(float) * 2 * W * MM);
+  const size_t sa = al(sizeof(float) * 2 * R * M), sz = al(sizeof(float) * 2 * R * M),
+               sv = al(sizeof(float) * 2 * W * MM);
   const size_t qa = al((size_t)2 * R * ld), qn = al((size_t)R * ld), qv = al((size_t)W * 2 * M * ld);
   const size_t ea = al(sizeof(int) * R), ev = al(sizeof(int) * W * M);
   char* buf = nullptr;
-  SFQ_CUDA_TRY(cudaMallocAsync((void**)&buf, sa + sv + nslices * (qa + qn + qv) + ea + 2 * ev, st));
+  SFQ_CUDA_TRY(cudaMallocAsync((void**)&buf, sa + sz + sv + nslices * (qa + qn + qv) + ea + 2 * ev, st));
   char* o = buf;
   float* S = reinterpret_cast<float*>(o); o += sa;
+  float* Cz = reinterpret_cast<float*>(o); o += sz;
   float* Cv = reinterpret_cast<float*>(o); o += sv;
   int8_t *aq[3] = {}, *an[3] = {}, *vq[3] = {};
   for (int s = 0; s < nslices; ++s) {
@@ -556,15 +562,17 @@ int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, i
   int* eA = reinterpret_cast<int*>(o); o += ea;
   int* eV = reinterpret_cast<int*>(o); o += ev;
   int* eVmax = reinterpret_cast<int*>(o);
-  // A as FP32 planar rows (c, w, a); V[w][j][i] as the planar rows (c * W + w, j * M + i) of a full vHS
+  // A through FP32 as the planar rows (c, w, a) of a sum S (plus a zero product); V[w][j][i] as the
+  // planar rows (c * W + w, j * M + i) of a full vHS
   cplx_to_planar_f32_kernel<<<148 * 8, 256, 0, st>>>(static_cast<const cplx*>(A), R * M, S, S + R * M);
   SFQ_LAUNCHED();
+  SFQ_CUDA_TRY(cudaMemsetAsync(Cz, 0, sz, st));
   for (int w = 0; w < W; ++w) {
     cplx_to_planar_f32_kernel<<<148, 256, 0, st>>>(static_cast<const cplx*>(V) + w * MM, MM, Cv + w * MM,
                                                    Cv + (W + w) * MM);
     SFQ_LAUNCHED();
   }
-  int rc = islice_taylor_update(nullptr, S, R, M, 0, true, nslices, aq, an, ld, eA, st);
+  int rc = islice_taylor_update(Cz, S, R, M, 0, true, nslices, aq, an, ld, eA, st);
   if (!rc) rc = islice_build_v(Cv, W, M, false, nslices, vq, ld, eV, eVmax, st);
   if (!rc) {
     IsliceGemmDesc d;

@@ -148,13 +148,13 @@ __global__ void rows_real_kernel(const double* src, long K, long lds, int ns, Q 
 }
 
 // one block per complex row r: planar rows r (re) and R + r (im)
-__global__ void rows_planar_kernel(const cplx* src, long R, long K, int ns, Q q, long ld, int* e) {
+__global__ void rows_planar_kernel(const cplx* src, long R, long K, int ns, Q q, long ld, int* e, const cplx* sub) {
   __shared__ double sh[32];
   const long r = blockIdx.x;
   const cplx* x = src + r * K;
   double mr = 0.0, mi = 0.0;
   for (long k = threadIdx.x; k < K; k += blockDim.x) {
-    const cplx z = x[k];
+    const cplx z = sub ? csub(x[k], sub[k]) : x[k];
     mr = fmax(mr, fabs(z.x));
     mi = fmax(mi, fabs(z.y));
   }
@@ -167,71 +167,9 @@ __global__ void rows_planar_kernel(const cplx* src, long R, long K, int ns, Q q,
   }
   const double sr = pow2d(-er), si = pow2d(-ei);
   for (long k = threadIdx.x; k < ld; k += blockDim.x) {
-    const cplx z = k < K ? x[k] : mk(0.0, 0.0);
+    const cplx z = k < K ? (sub ? csub(x[k], sub[k]) : x[k]) : mk(0.0, 0.0);
     put(q, ns, r * ld + k, z.x, sr);
     put(q, ns, (R + r) * ld + k, z.y, si);
-  }
-}
-
-// FP32 rows (four values per thread when K is a multiple of 4): one block per row
-template <bool VEC>
-__global__ void rows_real_f32_kernel(const float* src, long K, long lds, int ns, Q q, long ld, int* e) {
-  __shared__ double sh[32];
-  const long r = blockIdx.x;
-  const float* x = src + r * lds;
-  float m = 0.f;
-  if (VEC) {
-    for (long k = 4 * threadIdx.x; k < K; k += 4 * blockDim.x) {
-      const float4 v = *reinterpret_cast<const float4*>(x + k);
-      m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
-    }
-  } else {
-    for (long k = threadIdx.x; k < K; k += blockDim.x) m = fmaxf(m, fabsf(x[k]));
-  }
-  const int ex = row_exponent(block_max(double(m), sh));
-  if (threadIdx.x == 0) e[r] = ex;
-  const float sc = pow2f(-ex);
-  if (VEC) {
-    for (long k = 4 * threadIdx.x; k < ld; k += 4 * blockDim.x) {
-      float v[4] = {0.f, 0.f, 0.f, 0.f};
-      if (k < K) {
-        const float4 u = *reinterpret_cast<const float4*>(x + k);
-        v[0] = u.x; v[1] = u.y; v[2] = u.z; v[3] = u.w;
-      }
-      put4f(q, ns, r * ld + k, v, sc);
-    }
-  } else {
-    for (long k = threadIdx.x; k < ld; k += blockDim.x) put1f(q, ns, r * ld + k, k < K ? x[k] : 0.f, sc);
-  }
-}
-
-// inverse overlaps Tinv (W, N, N) complex -> the rows (w, c, a) over (b, c') of the real block
-// [[Tr, -Ti], [Ti, Tr]] at Tinv[b][a] (the A operand of G = (W Tinv)^T), one exponent per (w, a)
-// shared by both rows; one block per (w, a), thread b
-__global__ void tblk_slices_kernel(const cplx* Tinv, int N, int ns, Q q, long ld, int* e) {
-  __shared__ double sh[32];
-  const int w = blockIdx.y, a = blockIdx.x;
-  const cplx* T = Tinv + (long)w * N * N;
-  double m = 0.0;
-  for (int b = threadIdx.x; b < N; b += blockDim.x) {
-    const cplx z = T[(long)b * N + a];
-    m = fmax(m, fmax(fabs(z.x), fabs(z.y)));
-  }
-  const int ex = row_exponent(block_max(m, sh));
-  const long r0 = ((long)w * 2) * N + a, r1 = r0 + N;  // rows (w, 0, a) and (w, 1, a)
-  if (threadIdx.x == 0) {
-    e[r0] = ex;
-    e[r1] = ex;
-  }
-  const double sc = pow2d(-ex);
-  for (int b = threadIdx.x; 2 * b < ld; b += blockDim.x) {
-    const cplx z = b < N ? T[(long)b * N + a] : mk(0.0, 0.0);
-    if (2 * b + 1 < ld) {
-      put(q, ns, r0 * ld + 2 * b, z.x, sc);
-      put(q, ns, r0 * ld + 2 * b + 1, -z.y, sc);
-      put(q, ns, r1 * ld + 2 * b, z.y, sc);
-      put(q, ns, r1 * ld + 2 * b + 1, z.x, sc);
-    }
   }
 }
 
@@ -279,93 +217,72 @@ __global__ void walkers_slice_kernel(const cplx* SM, int W, int M, int N, int ns
   }
 }
 
-// Taylor update, one warp per row r; each lane keeps its <= kMaxPerLane values per part in registers
-constexpr int kMaxPerLane = 32;
-__global__ void taylor_update_kernel(const float* C, float* S, long R, int M, int k, int slice_sum, int ns, Q q,
-                                     Q qn, long ld, int* e) {
-  const long r = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (r >= R) return;
-  float v[2][kMaxPerLane];
-  double m = 0.0;
-  const float fk = float(k);
+// Taylor update, one warp per row r of the planar walker-shaped arrays (FP32):
+//   k = 0: S += C                    (S = W + (P1 - I) W = P1 W)
+//   k > 0: T = (i / k) C (T_re = -C_im / k, T_im = C_re / k), S += T
+// then the slices of S (SUM) or of T, one exponent per row over both parts.  Each lane keeps its
+// values in registers between the pass that updates S and finds the row's largest entry and the
+// pass that slices: four consecutive orbitals per group, kMaxQuads groups per lane (M <= 1024).
+constexpr int kMaxQuads = 8;
+template <bool VEC>
+__device__ __forceinline__ void ld4(const float* p, float (&v)[4], int valid) {
+  if (VEC) {
+    const float4 u = *reinterpret_cast<const float4*>(p);
+    v[0] = u.x; v[1] = u.y; v[2] = u.z; v[3] = u.w;
+  } else {
 #pragma unroll
-  for (int t = 0; t < kMaxPerLane; ++t) {
-    const int j = lane + 32 * t;
-    if (j >= M) break;
-    const long i0 = r * M + j, i1 = (R + r) * M + j;
-    float sr = S[i0], si = S[i1];
-    if (k > 0) {
-      const float tr = -C[i1] / fk, ti = C[i0] / fk;  // T_{k} = (i / k) C
-      sr += tr;
-      si += ti;
-      S[i0] = sr;
-      S[i1] = si;
-      v[0][t] = slice_sum ? sr : tr;
-      v[1][t] = slice_sum ? si : ti;
-    } else {
-      v[0][t] = sr;
-      v[1][t] = si;
-    }
-    m = fmax(m, fmax(fabs(double(v[0][t])), fabs(double(v[1][t]))));
-  }
-#pragma unroll
-  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  const int ex = row_exponent(m);
-  if (lane == 0) e[r] = ex;
-  const double s = pow2d(-ex);
-#pragma unroll
-  for (int t = 0; t < kMaxPerLane; ++t) {
-    const int j = lane + 32 * t;
-    if (j >= ld) break;
-    const double xr = j < M ? double(v[0][t]) : 0.0, xi = j < M ? double(v[1][t]) : 0.0;
-    put(q, ns, r * ld + j, xr, s);
-    put(q, ns, (R + r) * ld + j, xi, s);
-    if (qn.p[0]) put(qn, ns, r * ld + j, -xi, s);
+    for (int u = 0; u < 4; ++u) v[u] = u < valid ? p[u] : 0.f;
   }
 }
-
-// the same, four consecutive orbitals per lane (M a multiple of 4: 16-byte rows of C and S)
-constexpr int kMaxQuadsPerLane = 8;  // M <= 1024
-__global__ void taylor_update4_kernel(const float* C, float* S, long R, int M, int k, int slice_sum, int ns, Q q,
-                                      Q qn, long ld, int* e) {
+template <bool VEC>
+__device__ __forceinline__ void st4(float* p, const float (&v)[4], int valid) {
+  if (VEC) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (u < valid) p[u] = v[u];
+  }
+}
+template <bool SUM, bool VEC>
+__global__ void taylor_update_kernel(const float* C, float* S, long R, int M, int k, int ns, Q q, Q qn, long ld,
+                                     int* e) {
   const long r = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (r >= R) return;
-  const int M4 = M >> 2;
-  float v[2][kMaxQuadsPerLane][4];
+  const int G4 = (M + 3) >> 2;
+  float v[2][kMaxQuads][4];
   float m = 0.f;
   const float fk = float(k);
 #pragma unroll
-  for (int t = 0; t < kMaxQuadsPerLane; ++t) {
+  for (int t = 0; t < kMaxQuads; ++t) {
     const int g = lane + 32 * t;
-    if (g >= M4) break;
+    if (g >= G4) break;
+    const int valid = M - 4 * g < 4 ? M - 4 * g : 4;
     const long i0 = r * M + 4 * g, i1 = (R + r) * M + 4 * g;
-    float4 sr = *reinterpret_cast<const float4*>(S + i0), si = *reinterpret_cast<const float4*>(S + i1);
-    float xr[4] = {sr.x, sr.y, sr.z, sr.w}, xi[4] = {si.x, si.y, si.z, si.w};
-    if (k > 0) {
-      const float4 cr = *reinterpret_cast<const float4*>(C + i0), ci = *reinterpret_cast<const float4*>(C + i1);
-      const float c0[4] = {cr.x, cr.y, cr.z, cr.w}, c1[4] = {ci.x, ci.y, ci.z, ci.w};
+    float sr[4], si[4], cr[4], ci[4];
+    ld4<VEC>(S + i0, sr, valid);
+    ld4<VEC>(S + i1, si, valid);
+    ld4<VEC>(C + i0, cr, valid);
+    ld4<VEC>(C + i1, ci, valid);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const float tr = -c1[u] / fk, ti = c0[u] / fk;  // T_k = (i / k) C
-        const float nr = xr[u] + tr, ni = xi[u] + ti;
-        v[0][t][u] = slice_sum ? nr : tr;
-        v[1][t][u] = slice_sum ? ni : ti;
-        xr[u] = nr;
-        xi[u] = ni;
+    for (int u = 0; u < 4; ++u) {
+      float tr, ti;
+      if (k == 0) {
+        tr = cr[u];
+        ti = ci[u];
+      } else {
+        tr = -ci[u] / fk;
+        ti = cr[u] / fk;
       }
-      *reinterpret_cast<float4*>(S + i0) = make_float4(xr[0], xr[1], xr[2], xr[3]);
-      *reinterpret_cast<float4*>(S + i1) = make_float4(xi[0], xi[1], xi[2], xi[3]);
-    } else {
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        v[0][t][u] = xr[u];
-        v[1][t][u] = xi[u];
-      }
+      sr[u] += tr;
+      si[u] += ti;
+      v[0][t][u] = SUM ? sr[u] : tr;
+      v[1][t][u] = SUM ? si[u] : ti;
+      m = fmaxf(m, fmaxf(fabsf(v[0][t][u]), fabsf(v[1][t][u])));
     }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) m = fmaxf(m, fmaxf(fabsf(v[0][t][u]), fabsf(v[1][t][u])));
+    st4<VEC>(S + i0, sr, valid);
+    st4<VEC>(S + i1, si, valid);
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -373,13 +290,13 @@ __global__ void taylor_update4_kernel(const float* C, float* S, long R, int M, i
   if (lane == 0) e[r] = ex;
   const float sc = pow2f(-ex);
 #pragma unroll
-  for (int t = 0; t < kMaxQuadsPerLane; ++t) {
+  for (int t = 0; t < kMaxQuads; ++t) {
     const int g = lane + 32 * t;
     if (4 * g >= ld) break;
     float xr[4], xi[4], xn[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      const bool in = g < M4;
+      const bool in = 4 * g + u < M;
       xr[u] = in ? v[0][t][u] : 0.f;
       xi[u] = in ? v[1][t][u] : 0.f;
       xn[u] = -xi[u];
@@ -585,33 +502,11 @@ int islice_rows_real(const double* src, long R, long K, long lds, int nslices, i
 }
 
 int islice_rows_planar(const cplx* src, long R, long K, int nslices, int8_t* const* q, long ld, int* e,
-                       cudaStream_t st) {
+                       cudaStream_t st, const cplx* sub) {
   if (int rc = check_slices(nslices, q, ld)) return rc;
   if (R <= 0) return SFQ_OK;
   if (ld < K || R > 2147483647L) return record_error(SFQ_ERR_SHAPE, "islice_rows_planar: sizes");
-  rows_planar_kernel<<<unsigned(R), K >= 4096 ? 512 : 256, 0, st>>>(src, R, K, nslices, qptrs(q), ld, e);
-  SFQ_LAUNCHED();
-  return SFQ_OK;
-}
-
-int islice_rows_real_f32(const float* src, long R, long K, long lds, int nslices, int8_t* const* q, long ld, int* e,
-                         cudaStream_t st) {
-  if (int rc = check_slices(nslices, q, ld)) return rc;
-  if (R <= 0) return SFQ_OK;
-  if (ld < K || R > 2147483647L) return record_error(SFQ_ERR_SHAPE, "islice_rows_real_f32: sizes");
-  const int bs = K >= 8192 ? 512 : 256;
-  if (K % 4 == 0 && lds % 4 == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0)
-    rows_real_f32_kernel<true><<<unsigned(R), bs, 0, st>>>(src, K, lds, nslices, qptrs(q), ld, e);
-  else
-    rows_real_f32_kernel<false><<<unsigned(R), bs, 0, st>>>(src, K, lds, nslices, qptrs(q), ld, e);
-  SFQ_LAUNCHED();
-  return SFQ_OK;
-}
-
-int islice_tblk(const cplx* Tinv, int W, int N, int nslices, int8_t* const* q, long ld, int* e, cudaStream_t st) {
-  if (int rc = check_slices(nslices, q, ld)) return rc;
-  if (ld < 2L * N || W > 65535) return record_error(SFQ_ERR_SHAPE, "islice_tblk: sizes");
-  tblk_slices_kernel<<<dim3(unsigned(N), unsigned(W)), 128, 0, st>>>(Tinv, N, nslices, qptrs(q), ld, e);
+  rows_planar_kernel<<<unsigned(R), K >= 4096 ? 512 : 256, 0, st>>>(src, R, K, nslices, qptrs(q), ld, e, sub);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
@@ -631,16 +526,20 @@ int islice_walkers(const cplx* SM, int W, int M, int N, int nslices, int8_t* con
 int islice_taylor_update(const float* C, float* S, long R, int M, int k, bool slice_sum, int nslices,
                          int8_t* const* q, int8_t* const* qn, long ld, int* e, cudaStream_t st) {
   if (int rc = check_slices(nslices, q, ld)) return rc;
-  if (ld < M || ld > 32L * kMaxPerLane) return record_error(SFQ_ERR_SHAPE, "islice_taylor_update: M=%d too large", M);
-  if (k > 0 && !C) return record_error(SFQ_ERR_ARG, "islice_taylor_update: product missing");
+  if (ld < M || ld > 128L * kMaxQuads) return record_error(SFQ_ERR_SHAPE, "islice_taylor_update: M=%d", M);
+  if (!C || !S) return record_error(SFQ_ERR_ARG, "islice_taylor_update: product or sum missing");
+  if (k == 0 && !slice_sum) return record_error(SFQ_ERR_ARG, "islice_taylor_update: k = 0 slices the sum");
   int8_t* none[3] = {nullptr, nullptr, nullptr};
   const int wpb = 8;
+  const unsigned grid = unsigned((R + wpb - 1) / wpb);
+  const Q qq = qptrs(q), qnn = qptrs(qn ? qn : none);
+  // four consecutive orbitals per group: 16-byte rows when M is a multiple of 4
   if (M % 4 == 0) {
-    taylor_update4_kernel<<<unsigned((R + wpb - 1) / wpb), 32 * wpb, 0, st>>>(
-        C, S, R, M, k, slice_sum ? 1 : 0, nslices, qptrs(q), qptrs(qn ? qn : none), ld, e);
+    if (slice_sum) taylor_update_kernel<true, true><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, nslices, qq, qnn, ld, e);
+    else taylor_update_kernel<false, true><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, nslices, qq, qnn, ld, e);
   } else {
-    taylor_update_kernel<<<unsigned((R + wpb - 1) / wpb), 32 * wpb, 0, st>>>(
-        C, S, R, M, k, slice_sum ? 1 : 0, nslices, qptrs(q), qptrs(qn ? qn : none), ld, e);
+    if (slice_sum) taylor_update_kernel<true, false><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, nslices, qq, qnn, ld, e);
+    else taylor_update_kernel<false, false><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, nslices, qq, qnn, ld, e);
   }
   SFQ_LAUNCHED();
   return SFQ_OK;

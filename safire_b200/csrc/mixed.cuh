@@ -7,9 +7,10 @@ namespace sfq {
 
 // `pl` points at 3 plane pointers (p0, p1, p2); unused planes are null
 int mixed_split_planar(const cplx* src, int W, long E, void* const* pl, cudaStream_t st);
-// out[w][e] = alpha * (sum_s C_s[w][e], sum_s C_s[W + w][e]), the KS partial sums C_s = C + s * sk
+// out[w][e] = add[e] + alpha * (sum_s C_s[w][e], sum_s C_s[W + w][e]), the KS partial sums
+// C_s = C + s * sk (add may be null)
 int mixed_reduce_planar_to_cplx(const float* C, int KS, long sk, int W, long E, double alpha, cplx* out,
-                                cudaStream_t st);
+                                cudaStream_t st, const cplx* add = nullptr);
 // Cv: (2W, M*M) planar, or (2W, M(M+1)/2) with packed (upper triangle of a symmetric vHS) ->
 // split planes V[w][c][i][k] (Vr, Vi)
 int mixed_build_v(const float* Cv, int W, int M, bool packed, void* const* pl, cudaStream_t st);

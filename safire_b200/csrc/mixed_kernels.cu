@@ -72,7 +72,7 @@ __global__ void split_planar_kernel(const cplx* src, int W, long E, Planes P) {
 // KS partial sums of planar fp32 rows (c*W + w), split s at C + s * sk -> complex fp64 (W, E),
 // times alpha; the splits are added in order, in double precision
 __global__ void reduce_planar_to_cplx_kernel(const float* C, int KS, long sk, int W, long E, double alpha,
-                                             cplx* out) {
+                                             cplx* out, const cplx* add) {
   const long total = (long)W * E;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
     const long w = t / E, e = t % E;
@@ -97,7 +97,7 @@ __global__ void reduce_planar_to_cplx_kernel(const float* C, int KS, long sk, in
       re += double(cr[s * sk]);
       im += double(ci[s * sk]);
     }
-    out[t] = mk(alpha * re, alpha * im);
+    out[t] = add ? mk(add[e].x + alpha * re, add[e].y + alpha * im) : mk(alpha * re, alpha * im);
   }
 }
 
@@ -340,8 +340,8 @@ int mixed_split_planar(const cplx* src, int W, long E, void* const* pl, cudaStre
 }
 
 int mixed_reduce_planar_to_cplx(const float* C, int KS, long sk, int W, long E, double alpha, cplx* out,
-                                cudaStream_t st) {
-  reduce_planar_to_cplx_kernel<<<grid_for((long)W * E), 256, 0, st>>>(C, KS, sk, W, E, alpha, out);
+                                cudaStream_t st, const cplx* add) {
+  reduce_planar_to_cplx_kernel<<<grid_for((long)W * E), 256, 0, st>>>(C, KS, sk, W, E, alpha, out, add);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
