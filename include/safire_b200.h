@@ -206,6 +206,12 @@ int sfq_gemm_int8_slices(const double* A, const double* B, float* C, int M, int 
  * FP32 (2, W, N, M)); half: 32, 64 or 80 orbitals per tile. */
 int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, int N, int nslices, int half,
                          void* stream);
+/* Failure-path self test of the tensor-core kernels' bounded waits, no reference counterpart: one
+ * small int8-slice product whose loads are held back by a device flag nothing sets, every
+ * mbarrier wait limited to wait_ns (1 ns .. 1 s).  Each wait expires; the kernel records
+ * SFQ_ERR_TIMEOUT, has no copy or MMA in flight, frees its tensor memory and returns.  Returns the
+ * status the kernel recorded (SFQ_ERR_TIMEOUT), or an error of its own. */
+int sfq_selftest_wait_expiry(unsigned long long wait_ns, void* stream);
 
 /* ---------------------------------------------------------------------------------------
  * Resident engine: HamiltonianOperations + NOMSD trial + WalkerSet + AFQMCBasePropagator
@@ -504,8 +510,25 @@ typedef struct {
   void* new_ovlp;     /* (nwalk) complex */
   unsigned long long bound_stats[5]; /* eloc total/upper/lower, weight total/upper */
   int vhs_packed;     /* 1: the Cholesky vectors are symmetric and vHS comes from their upper triangle */
+  void* hcore;        /* (nmo, nmo) real */
 } sfq_engine_info_t;
 int sfq_engine_info(sfq_engine_t e, sfq_engine_info_t* info);
+
+/* WalkerSet::copy_walker (WalkerSetBase.h:413-415): every field of the walker in slot `from` (its
+ * Slater matrix and property columns) into slot `to`. */
+int sfq_engine_copy_walker(sfq_engine_t e, int from, int to);
+/* WalkerSet::resize (WalkerSetBase.h:195): the engine is rebuilt for nwalk walkers (the resident
+ * tensors recomputed from its Hamiltonian and trial, tiles back to their defaults, back propagation
+ * off), and its walkers are carried over, new slots filled from the existing walkers in
+ * round-robin order, slot w from slot w mod the old count.  *e is replaced by the new engine. */
+int sfq_engine_resize(sfq_engine_t* e, int nwalk);
+
+/* HamiltonianOperations::getOneBodyPropagatorMatrix (Real3IndexFactorization.hpp:99-124,
+ * add_one_body_shifts one_body.hpp:64-82): H1 = dt (hcore + v0) + sqrt(dt) sum_n L_n vMF_n, the
+ * matrix generateP1 exponentiates.  hcore, v0 (nmo x nmo) and Likn (nmo, nmo, nchol) on the device;
+ * vMF (nchol, the real mean field) and H1 (nmo x nmo, real) in host memory. */
+int sfq_one_body_matrix(const double* hcore, const double* v0, const double* Likn, const double* vMF, int nmo,
+                        int nchol, double dt, double* H1, void* stream);
 
 #ifdef __cplusplus
 }

@@ -11,9 +11,11 @@
 // matching utils::check's throw-on-failure semantics (src/utilities/check.hpp:36-46).
 #pragma once
 
+#include <algorithm>
 #include <complex>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -32,8 +34,32 @@ inline void check(int rc) {
   if (rc != SFQ_OK) throw Error(rc, sfq_last_error());
 }
 
-// walker_data columns kept by the engine (WalkerConfig.hpp:28-48 names)
-enum walker_data { WEIGHT = 0, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, THETA };
+// walker_data (WalkerConfig.hpp:28-48): the reference's names with the reference's values
+enum walker_data {
+  SM, UR, DR, VR, WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, LOGSCL_UP, LOGSCL_DN, IS_UNITARY, SMN,
+  FIELDS, WEIGHT_FAC, WEIGHT_HISTORY, THETA,
+};
+// the engine's property column of a walker_data id (sfq_engine_get_walkers order); the fields the
+// engine does not keep as a property column are refused
+inline int property_column(walker_data id) {
+  switch (id) {
+    case WEIGHT: return 0;
+    case PHASE: return 1;
+    case PSEUDO_ELOC_: return 2;
+    case E1_: return 3;
+    case EXX_: return 4;
+    case EJ_: return 5;
+    case OVLP: return 6;
+    case THETA: return 7;
+    default: throw Error(SFQ_ERR_ARG, "walker_data " + std::to_string(int(id)) + " is not a property column");
+  }
+}
+// PropagatorTypes (propagator_types.hpp:13-20) and HamiltonianType (config.h:158-164)
+enum PropagatorTypes {
+  ContinuousChargePropagator, ContinuousSpinPropagator, DiscreteChargePropagator, DiscreteSpinPropagator,
+  UndefinedPropagator,
+};
+enum class HamiltonianType { thc, kpthc, kp_factorized, real_dense_factorized, model_hamiltonian };
 
 namespace det_ops {
 
@@ -123,9 +149,31 @@ class HamiltonianOperations {
                         const ComplexType* haj, double E0)
       : nmo_(nmo), nel_(nel), nchol_(nchol), Likn_(Likn), Lnak_(Lnak), lnak_complex_(lnak_complex), haj_(haj),
         E0_(E0) {}
+  // with the one-body tensors too (device hcore and v0, nmo x nmo), for getOneBodyPropagatorMatrix
+  HamiltonianOperations(int nmo, int nel, int nchol, const double* Likn, const void* Lnak, bool lnak_complex,
+                        const ComplexType* haj, double E0, const double* hcore, const double* v0)
+      : HamiltonianOperations(nmo, nel, nchol, Likn, Lnak, lnak_complex, haj, E0) {
+    hcore_ = hcore;
+    v0_ = v0;
+  }
 
   int number_of_cholesky_vectors() const { return nchol_; }
+  int number_of_ke_vectors() const { return nchol_; }
   double energy_offset() const { return E0_; }
+  // (spin blocks, polarizations) of vHS: one of each for CLOSED walkers (Real3IndexFactorization.hpp:430-434)
+  std::tuple<int, int> vHS_dims() const { return std::make_tuple(1, 1); }
+  HamiltonianType getHamType() const { return HamiltonianType::real_dense_factorized; }
+  // every Cholesky vector is a continuous charge field (Real3IndexFactorization.hpp:129-133)
+  std::vector<int> getFieldTypes() const { return std::vector<int>(size_t(nchol_), int(ContinuousChargePropagator)); }
+  // H1 = dt (h + v0) + vHS(vMF, dt) as a host [1][nmo][nmo] array (Real3IndexFactorization.hpp:99-124)
+  std::vector<ComplexType> getOneBodyPropagatorMatrix(double dt, const std::vector<ComplexType>& vMF) const {
+    if (!hcore_ || !v0_) throw Error(SFQ_ERR_ARG, "getOneBodyPropagatorMatrix: constructed without hcore and v0");
+    if (long(vMF.size()) != nchol_) throw Error(SFQ_ERR_SHAPE, "getOneBodyPropagatorMatrix: Size mismatch");
+    std::vector<double> v(vMF.size()), h(size_t(nmo_) * nmo_);
+    for (size_t n = 0; n < vMF.size(); ++n) v[n] = vMF[n].real();
+    check(sfq_one_body_matrix(hcore_, v0_, Likn_, v.data(), nmo_, nchol_, dt, h.data(), nullptr));
+    return std::vector<ComplexType>(h.begin(), h.end());
+  }
 
   // vbias(G, v, dt): v[W, nchol] = 2 sqrt(dt) G Lnak^T
   void vbias(const ComplexType* G, ComplexType* v, int nwalk, double dt, void* stream = nullptr) const {
@@ -149,6 +197,8 @@ class HamiltonianOperations {
   bool lnak_complex_;
   const ComplexType* haj_;
   double E0_;
+  const double* hcore_ = nullptr;
+  const double* v0_ = nullptr;
 };
 
 // The resident system: HamOps + NOMSD trial + WalkerSet + AFQMCBasePropagator on one GPU.
@@ -169,6 +219,11 @@ class Engine {
   Engine& operator=(const Engine&) = delete;
   sfq_engine_t handle() const { return h_; }
   const sfq_engine_params_t& params() const { return p_; }
+  // WalkerSet::resize: the engine rebuilt for n walkers, its walkers carried over round robin
+  void resize(int n) {
+    check(sfq_engine_resize(&h_, n));
+    p_.nwalk = n;
+  }
 
   // run_afqmc's loop as one device-resident block replayed from a CUDA graph (sfq_engine_block);
   // returns the measurements (10 doubles each), Eshift in/out
@@ -276,15 +331,41 @@ class Server {
   sfq_server_t s_ = nullptr;
 };
 
-// WalkerSet view of an engine (WalkerSetBase.h): size, properties, Slater matrices
+// the auxiliary-field generator of an engine: counter-based Philox draws keyed by (seed, step,
+// walker, vector), the stream sampleUniformFields stands for (Random.hpp:37-118)
+class RandomGenerator {
+ public:
+  RandomGenerator(unsigned long long seed, int nwalk, int nchol) : seed_(seed), nwalk_(nwalk), nchol_(nchol) {}
+  unsigned long long seed() const { return seed_; }
+  // the uniforms of one step into a device buffer of nwalk x nchol doubles
+  void sampleUniformFields(double* dev, unsigned long long step, void* stream = nullptr) const {
+    check(sfq_field_uniforms(dev, seed_, step, nwalk_, nchol_, stream));
+  }
+
+ private:
+  unsigned long long seed_;
+  int nwalk_, nchol_;
+};
+
+// WalkerSet view of an engine (WalkerSetBase.h:51-572): size, properties, Slater matrices, copies
 class WalkerSet {
  public:
   explicit WalkerSet(Engine& e) : e_(e) {}
   int size() const { return e_.params().nwalk; }
   std::vector<ComplexType> getProperty(walker_data id) const {
+    const int col = property_column(id);
     std::vector<ComplexType> props(size_t(8) * size());
     check(sfq_engine_get_walkers(e_.handle(), nullptr, props.data()));
-    return std::vector<ComplexType>(props.begin() + size_t(id) * size(), props.begin() + size_t(id + 1) * size());
+    return std::vector<ComplexType>(props.begin() + size_t(col) * size(), props.begin() + size_t(col + 1) * size());
+  }
+  // setProperty (WalkerSetBase.h:476-481): v holds at least size() values
+  void setProperty(walker_data id, const std::vector<ComplexType>& v) {
+    const int col = property_column(id);
+    if (long(v.size()) < size()) throw Error(SFQ_ERR_SHAPE, "setProperty: Shape mismatch");
+    std::vector<ComplexType> props(size_t(8) * size());
+    check(sfq_engine_get_walkers(e_.handle(), nullptr, props.data()));
+    std::copy(v.begin(), v.begin() + size(), props.begin() + size_t(col) * size());
+    check(sfq_engine_set_walkers(e_.handle(), nullptr, props.data()));
   }
   std::vector<ComplexType> SlaterMatrices() const {
     const auto& p = e_.params();
@@ -292,25 +373,42 @@ class WalkerSet {
     check(sfq_engine_get_walkers(e_.handle(), sm.data(), nullptr));
     return sm;
   }
+  void copy_walker(int from, int to) { check(sfq_engine_copy_walker(e_.handle(), from, to)); }
+  void resize(int n) { e_.resize(n); }
+  RandomGenerator getRNG() const {
+    const auto& p = e_.params();
+    return RandomGenerator(p.seed, p.nwalk, p.nchol);
+  }
   Engine& engine() { return e_; }
 
  private:
   Engine& e_;
 };
 
-// AFQMCBasePropagator: Propagate(wset, Eshift) / Orthogonalize(wset)
+// AFQMCBasePropagator (AFQMCBasePropagator.h:51-172): Propagate / Orthogonalize on the engine
 class AFQMCBasePropagator {
  public:
   explicit AFQMCBasePropagator(Engine& e) : e_(e) {}
-  void Propagate(WalkerSet& wset, double Eshift) {
+  // nt is the time slice of finite-temperature walkers (WalkerSet::setTauStep); zero-temperature
+  // walkers ignore it.  The fields of each call are those of the next step of the generator.
+  void Propagate(WalkerSet& wset, double Eshift, int nt = 0) {
+    (void)nt;
     check(sfq_engine_propagate(wset.engine().handle(), Eshift, step_++, nullptr));
   }
   void Orthogonalize(WalkerSet& wset) { check(sfq_engine_orthogonalize(wset.engine().handle())); }
   bool stores_local_energy() const { return false; }  // hybrid propagation
+  // uniforms drawn per walker (at least nchol, AFQMCBasePropagator.cpp:708): the counter-based fields
+  // are keyed per (walker, vector), so the block size changes no field
+  void set_rng_block_size(int sz) {
+    if (sz < e_.params().nchol) throw Error(SFQ_ERR_ARG, "set_rng_block_size: rng_block_size < nCV");
+    rng_block_size_ = sz;
+  }
+  int rng_block_size() const { return rng_block_size_; }
 
  private:
   Engine& e_;
   unsigned long long step_ = 0;
+  int rng_block_size_ = 0;
 };
 
 }  // namespace safire_b200

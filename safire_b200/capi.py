@@ -52,7 +52,7 @@ class EngineInfo(ctypes.Structure):
                [("lnak_complex", ctypes.c_int)] + \
                [(n, ctypes.c_void_p) for n in ("Likn", "haj", "v0", "vmf", "P1", "G", "X", "vHS", "hw", "mf",
                                                "new_ovlp")] + \
-               [("bound_stats", ctypes.c_ulonglong * 5), ("vhs_packed", ctypes.c_int)]
+               [("bound_stats", ctypes.c_ulonglong * 5), ("vhs_packed", ctypes.c_int), ("hcore", ctypes.c_void_p)]
 
 
 class Tiles(ctypes.Structure):
@@ -104,6 +104,10 @@ _SIGS = {
                               ctypes.c_long, ctypes.c_float, ctypes.c_float, _I, _VP], _I),
     "sfq_split_bf16": ([_VP, ctypes.c_long, _VP, _VP, _VP, _VP], _I),
     "sfq_gemm_int8_slices": ([_VP, _VP, _VP, _I, _I, _I, _I, _I, _I, _VP], _I),
+    "sfq_engine_copy_walker": ([_VP, _I, _I], _I),
+    "sfq_selftest_wait_expiry": ([_U64, _VP], _I),
+    "sfq_engine_resize": ([_VP, _I], _I),
+    "sfq_one_body_matrix": ([_VP, _VP, _VP, _VP, _I, _I, _D, _VP, _VP], _I),
     "sfq_gemm_int8_cplx_b": ([_VP, _VP, _VP, _I, _I, _I, _I, _I, _VP], _I),
     "sfq_engine_params_default": ([ctypes.POINTER(EngineParams)], None),
     "sfq_engine_create": ([ctypes.POINTER(_VP), ctypes.POINTER(EngineParams), _VP, _VP, _VP], _I),

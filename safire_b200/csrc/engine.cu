@@ -2887,9 +2887,68 @@ int sfq_engine_phase_times(sfq_engine_t h, double* ms, int* counts, int nphase) 
   return h->e.phase_times(ms, counts, nphase);
 }
 
+int sfq_engine_copy_walker(sfq_engine_t h, int from, int to) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  if (from < 0 || from >= e.W || to < 0 || to >= e.W)
+    return record_error(SFQ_ERR_ARG, "copy_walker: slots %d, %d of %d", from, to, e.W);
+  if (from == to) return SFQ_OK;
+  const long mn = (long)e.Mr * e.N;
+  SFQ_CUDA_TRY(cudaMemcpyAsync(e.SM + to * mn, e.SM + from * mn, sizeof(cplx) * mn, cudaMemcpyDeviceToDevice, e.st));
+  SFQ_CUDA_TRY(cudaMemcpy2DAsync(e.props + to, sizeof(cplx) * e.W, e.props + from, sizeof(cplx) * e.W, sizeof(cplx),
+                                 kNumProps, cudaMemcpyDeviceToDevice, e.st));
+  e.inv_cached = false;
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+int sfq_engine_resize(sfq_engine_t* ph, int nwalk) {
+  if (!ph || !*ph) return record_error(SFQ_ERR_ARG, "null engine");
+  if (nwalk <= 0) return record_error(SFQ_ERR_ARG, "resize: %d walkers", nwalk);
+  Engine& e = (*ph)->e;
+  SFQ_CUDA_TRY(cudaSetDevice(e.p.device));
+  if (nwalk == e.W) return SFQ_OK;
+  // the inputs the engine was built from, back from the device
+  const long MM = (long)e.M * e.M, RN = e.det_elems();
+  std::vector<double> hc(MM), L(size_t(MM) * e.Nc);
+  std::vector<cplx> ps(size_t(e.ndet) * RN);
+  SFQ_CUDA_TRY(cudaMemcpyAsync(hc.data(), e.hcore, sizeof(double) * MM, cudaMemcpyDeviceToHost, e.st));
+  SFQ_CUDA_TRY(cudaMemcpyAsync(L.data(), e.Likn, sizeof(double) * L.size(), cudaMemcpyDeviceToHost, e.st));
+  SFQ_CUDA_TRY(cudaMemcpyAsync(ps.data(), e.PsiT, sizeof(cplx) * ps.size(), cudaMemcpyDeviceToHost, e.st));
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  sfq_engine_params_t p = e.p;
+  p.nwalk = nwalk;
+  sfq_engine_t nh = nullptr;
+  int rc = e.ndet > 1 ? sfq_engine_create_nomsd(&nh, &p, hc.data(), L.data(), e.ndet, ps.data(), e.ci_h.data())
+                      : sfq_engine_create(&nh, &p, hc.data(), L.data(), ps.data());
+  if (rc) return rc;
+  Engine& n = nh->e;
+  const long mn = (long)e.Mr * e.N;
+  for (int w = 0; w < nwalk && !rc; ++w) {  // slot w from slot w mod the old count
+    const int src = w % e.W;
+    cudaError_t ce = cudaMemcpyAsync(n.SM + w * mn, e.SM + src * mn, sizeof(cplx) * mn, cudaMemcpyDeviceToDevice, n.st);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpy2DAsync(n.props + w, sizeof(cplx) * n.W, e.props + src, sizeof(cplx) * e.W, sizeof(cplx),
+                             kNumProps, cudaMemcpyDeviceToDevice, n.st);
+    if (ce != cudaSuccess) rc = record_cuda(ce, "resize: walker copy", __FILE__, __LINE__);
+  }
+  if (!rc) {
+    const cudaError_t ce = cudaStreamSynchronize(n.st);
+    if (ce != cudaSuccess) rc = record_cuda(ce, "resize", __FILE__, __LINE__);
+  }
+  if (rc) {
+    sfq_engine_destroy(nh);
+    return rc;
+  }
+  sfq_engine_destroy(*ph);
+  *ph = nh;
+  return SFQ_OK;
+}
+
 int sfq_engine_info(sfq_engine_t h, sfq_engine_info_t* info) {
   if (!h || !info) return record_error(SFQ_ERR_ARG, "null pointer");
   Engine& e = h->e;
+  info->hcore = e.hcore;
   info->SM = e.SM;
   info->props = e.props;
   info->PsiT = e.PsiT;

@@ -20,8 +20,9 @@
 // A^-1[a][p_k] = B[p_a][k] / U_aa (p_k: pivot row of step k) is scattered straight to the output
 // with INVERT; without it only the log det is written.  A zero pivot marks the matrix singular: the
 // step is skipped and the inverse is written as zeros (getri_or_zero,
-// src/numerics/nda_functions.hpp:422-438).  The pivot warp's wait is bounded (2 s); if it ever
-// expired the matrix would be reported as singular with a NaN log det.
+// src/numerics/nda_functions.hpp:422-438).  The pivot warp's wait for each column is bounded (2 s
+// from the start of that wait); if one ever expired the matrix would be reported as singular with a
+// NaN log det.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -221,7 +222,6 @@ __global__ void __launch_bounds__(((LPC * LPC * R + 31) / 32) * 32 + 32)
   }
   __syncthreads();
 
-  const unsigned long long deadline = gtimer() + kGjWaitNs;
   for (int k = 0; k < N; ++k) {
     const int buf = k & 1, nb = buf ^ 1;
     const int p = s_p[buf];
@@ -276,11 +276,14 @@ __global__ void __launch_bounds__(((LPC * LPC * R + 31) / 32) * 32 + 32)
     if (pivot_warp && k + 1 < N) {
       // wait (bounded) for column k+1, then its pivot
       bool ok = true;
-      uint32_t spins = 0;
-      while (!mbar_try_wait(&col_ready, uint32_t(k & 1))) {
-        if ((++spins & 255u) == 0u && gtimer() > deadline) {
-          ok = false;
-          break;
+      if (!mbar_try_wait(&col_ready, uint32_t(k & 1))) {
+        const unsigned long long deadline = gtimer() + kGjWaitNs;  // from the start of this wait
+        uint32_t spins = 0;
+        while (!mbar_try_wait(&col_ready, uint32_t(k & 1))) {
+          if ((++spins & 255u) == 0u && gtimer() > deadline) {
+            ok = false;
+            break;
+          }
         }
       }
       if (__all_sync(0xffffffffu, ok)) {

@@ -106,7 +106,6 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
     __syncwarp();
 #pragma unroll
     for (int g = 0; g < NS; ++g) tmem_ld16_u32(taddr + uint32_t(g * BN + c), acc[g]);
-    if (!live) continue;
     long obase;
     int col0, valid;
     if (p.half) {  // complex B: [re | im] halves of `half` orbitals
@@ -121,17 +120,26 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
       valid = p.N - col0 < 16 ? p.N - col0 : 16;
       obase = (long)ks * p.sCk + (long)bz * p.sCb + (long)gm * p.ldc + col0;
     }
+    // (col0 is the same for the whole warp; every lane takes part in the broadcast below, rows past
+    // M included, whose results are dropped)
+    // the chunk's 16 column exponents: one load by lanes 0-15, then broadcast
+    const int lane = threadIdx.x & 31;
+    int ebl = 0;
+    {
+      const int col = col0 + (lane & 15) < p.N ? col0 + (lane & 15) : p.N - 1;
+      ebl = p.eb[(long)bz * p.eb_bs + (p.eb_mod ? col % p.eb_mod : col)];
+    }
     float v[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-      const int col = col0 + j < p.N ? col0 + j : p.N - 1;
-      const int eb = p.eb[(long)bz * p.eb_bs + (p.eb_mod ? col % p.eb_mod : col)];
+      const int eb = __shfl_sync(0xffffffffu, ebl, j);
       // acc0 2^16 + acc1 2^8 + acc2: exact in int64 (< 2^48) and in its conversion to FP64 (< 2^53)
       long long s = (long long)int(acc[0][j]) << (8 * (NS - 1));
       if (NS > 1) s += (long long)int(acc[1][j]) << (8 * (NS - 2));
       if (NS > 2) s += (long long)int(acc[2][j]);
       v[j] = __double2float_rn(double(s) * pow2(ea + eb - 8 * (NS - 1)) * p.alpha);
     }
+    if (!live) continue;
     float* out = p.C + obase;
     const bool vec = valid == 16 && (obase % 4) == 0;
     if (p.accumulate) {
@@ -529,6 +537,41 @@ int sfq_gemm_int8_slices(const double* A, const double* B, float* C, int M, int 
   }
   cudaFreeAsync(buf, st);
   return rc;
+}
+
+int sfq_selftest_wait_expiry(unsigned long long wait_ns, void* stream) {
+  using namespace sfq;
+  if (wait_ns == 0 || wait_ns > 1000000000ull) return record_error(SFQ_ERR_ARG, "selftest: wait of 1 ns .. 1 s");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  constexpr int n = 128;
+  const size_t qb = (size_t)n * n, ebytes = sizeof(int) * n;
+  char* buf = nullptr;
+  const size_t total = 6 * qb + 2 * ebytes + sizeof(float) * n * n + 256;
+  SFQ_CUDA_TRY(cudaMallocAsync((void**)&buf, total, st));
+  SFQ_CUDA_TRY(cudaMemsetAsync(buf, 0, total, st));
+  IsliceGemmDesc d;
+  d.M = n; d.N = n; d.K = n; d.nslices = 3; d.bn = 128;
+  for (int q = 0; q < 3; ++q) {
+    d.A.q[q] = reinterpret_cast<int8_t*>(buf + q * qb);
+    d.B.q[q] = reinterpret_cast<int8_t*>(buf + (3 + q) * qb);
+  }
+  d.A.rows = n; d.A.ld = n; d.A.e = reinterpret_cast<int*>(buf + 6 * qb);
+  d.B.rows = n; d.B.ld = n; d.B.e = reinterpret_cast<int*>(buf + 6 * qb + ebytes);
+  d.C = reinterpret_cast<float*>(buf + 6 * qb + 2 * ebytes);
+  d.ldc = n;
+  int* flags = reinterpret_cast<int*>(buf + total - 256);  // [0] the kernel's status, [1] the hold flag (0)
+  d.err = flags;
+  d.hold = flags + 1;
+  d.wait_ns = wait_ns;
+  int rc = islice_gemm(d, st);
+  int status = SFQ_OK;
+  if (!rc) {
+    cudaError_t ce = cudaMemcpyAsync(&status, flags, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) rc = record_cuda(ce, "selftest", __FILE__, __LINE__);
+  }
+  cudaFreeAsync(buf, st);
+  return rc ? rc : status;
 }
 
 int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, int N, int nslices, int half,

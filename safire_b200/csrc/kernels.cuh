@@ -89,6 +89,9 @@ int permute_lnak(const void* tmp, void* Lnak, int nel, int nmo, int nchol, int e
 // H[i][k] = -0.5 * herm(dt*h + dt*v0 + Re vhs)  (real symmetric one-body matrix of P1)
 int build_h1(const double* h, const double* v0, const cplx* vhs, double dt, double* H, int nmo, cudaStream_t st);
 int add_identity(double* P, int nmo, double v, cudaStream_t st);
+// H = dt (h + v0) + Re vhs  (add_one_body_shifts)
+int one_body_shift(const double* h, const double* v0, const cplx* vhs, double dt, double* H, int nmo,
+                   cudaStream_t st);
 int threshold_real(double* P, long n, double drop, cudaStream_t st);
 int real_of(const cplx* z, double* r, long n, cudaStream_t st);
 int fill_cplx(cplx* p, long n, cplx v, cudaStream_t st);

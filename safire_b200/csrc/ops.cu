@@ -7,6 +7,7 @@
 #include <string>
 
 #include "ops.cuh"
+#include <vector>
 #include "umma_gemm.cuh"
 
 namespace sfq {
@@ -437,6 +438,40 @@ int sfq_vhs(const double* Likn, const void* X, void* vHS, int nwalk, int nmo, in
   if (nwalk == 0 || nmo == 0) return SFQ_OK;
   if (!Likn || !X || !vHS) return record_error(SFQ_ERR_ARG, "null pointer");
   return ops::vhs(Likn, (const cplx*)X, (cplx*)vHS, nwalk, nmo, nchol, std::sqrt(dt), S(stream));
+}
+
+int sfq_one_body_matrix(const double* hcore, const double* v0, const double* Likn, const double* vMF, int nmo,
+                        int nchol, double dt, double* H1, void* stream) {
+  if (nmo <= 0 || nchol < 0) return record_error(SFQ_ERR_SHAPE, "one_body_matrix: sizes");
+  if (!hcore || !v0 || !Likn || !H1 || (nchol > 0 && !vMF)) return record_error(SFQ_ERR_ARG, "null pointer");
+  cudaStream_t st = S(stream);
+  const long MM = (long)nmo * nmo;
+  char* buf = nullptr;
+  const size_t bx = (sizeof(cplx) * (nchol > 0 ? nchol : 1) + 255) & ~size_t(255);
+  const size_t bv = (sizeof(cplx) * MM + 255) & ~size_t(255);
+  SFQ_CUDA_TRY(cudaMallocAsync((void**)&buf, bx + bv + sizeof(double) * MM, st));
+  cplx* X = reinterpret_cast<cplx*>(buf);
+  cplx* V = reinterpret_cast<cplx*>(buf + bx);
+  double* H = reinterpret_cast<double*>(buf + bx + bv);
+  std::vector<cplx> xv(nchol > 0 ? nchol : 1);
+  for (int n = 0; n < nchol; ++n) xv[n] = mk(vMF[n], 0.0);
+  int rc = SFQ_OK;
+  cudaError_t ce = cudaMemcpyAsync(X, xv.data(), sizeof(cplx) * xv.size(), cudaMemcpyHostToDevice, st);
+  if (ce != cudaSuccess) rc = record_cuda(ce, "one_body_matrix: vMF", __FILE__, __LINE__);
+  // the mean-field shift vHS(vMF) = sqrt(dt) sum_n L_n vMF_n (real for real Cholesky vectors)
+  if (!rc && nchol > 0) rc = ops::vhs(Likn, X, V, 1, nmo, nchol, std::sqrt(dt), st);
+  if (!rc && nchol == 0) {
+    ce = cudaMemsetAsync(V, 0, sizeof(cplx) * MM, st);
+    if (ce != cudaSuccess) rc = record_cuda(ce, "one_body_matrix", __FILE__, __LINE__);
+  }
+  if (!rc) rc = one_body_shift(hcore, v0, V, dt, H, nmo, st);
+  if (!rc) {
+    ce = cudaMemcpyAsync(H1, H, sizeof(double) * MM, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) rc = record_cuda(ce, "one_body_matrix: H1", __FILE__, __LINE__);
+  }
+  cudaFreeAsync(buf, st);
+  return rc;
 }
 
 int sfq_energy(void* E, const void* G, const void* haj, const void* Lnak, int lnak_complex, double E0, int nwalk,

@@ -380,6 +380,13 @@ __global__ void build_h1_kernel(const double* h, const double* v0, const cplx* v
   }
 }
 
+// add_one_body_shifts (one_body.hpp:64-82): H = dt (h + v0) + the mean-field shift's real part
+__global__ void one_body_shift_kernel(const double* h, const double* v0, const cplx* vhs, double dt, double* H,
+                                      long total) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x)
+    H[e] = dt * h[e] + dt * v0[e] + vhs[e].x;
+}
+
 __global__ void add_identity_kernel(double* P, int M, double v) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < M) P[(long)i * M + i] += v;
@@ -605,6 +612,13 @@ int permute_lnak(const void* tmp, void* Lnak, int nel, int nmo, int nchol, int e
 
 int build_h1(const double* h, const double* v0, const cplx* vhs, double dt, double* H, int nmo, cudaStream_t st) {
   build_h1_kernel<<<grid_for((long)nmo * nmo), 256, 0, st>>>(h, v0, vhs, dt, H, nmo);
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+int one_body_shift(const double* h, const double* v0, const cplx* vhs, double dt, double* H, int nmo,
+                   cudaStream_t st) {
+  one_body_shift_kernel<<<grid_for((long)nmo * nmo), 256, 0, st>>>(h, v0, vhs, dt, H, (long)nmo * nmo);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

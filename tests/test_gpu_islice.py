@@ -154,3 +154,14 @@ def test_int8x3_engine_one_step_vs_oracle(spec):
     assert _rel(E[:, 0], Eo[:, 0]) < 1e-10
     assert _rel(E, Eo) < 2e-6
     eng.close()
+
+
+def test_bounded_waits_expire_and_report_timeout():
+    """The product's loads are held back by a flag nothing sets and every wait is limited to 1 ms:
+    each wait expires, the kernel reports SFQ_ERR_TIMEOUT with nothing in flight and its tensor
+    memory freed, and the next product on the same context runs and is exact."""
+    L = capi.lib()
+    assert L.sfq_selftest_wait_expiry(1_000_000, None) == 8  # SFQ_ERR_TIMEOUT
+    A, B = _operands(200, 150, 400, seed=9)
+    assert np.array_equal(_int8_gemm(A, B, 3, 128)[0], R.gemm(A, B, 3))
+    assert L.sfq_selftest_wait_expiry(0, None) == 2  # no limit is no test

@@ -297,6 +297,48 @@ def test_engine_full_run_small():
     eng.close()
 
 
+def test_engine_configs1_full_population():
+    """The FP64 drop-in at M=128, N=32+32, Nchol=640 with all 1024 walkers: run_afqmc's loop for 21
+    steps (orthogonalization every 5, combs at steps 0 and 20, Eshift relaxed every step) against
+    the oracle on the same Philox fields; weights, overlaps and walkers at 1e-10, the combs
+    bit-exact (the same walkers in the same slots).  dt = 0.002: at 0.005 these walkers collapse
+    within a few steps, in the oracle as well."""
+    s, ham, eng, prop, wo = _engine_pair(synthetic.CFG_MEDIUM, 1024, dt=0.002, seed=7)
+    Esh_o = O.init_walkers(ham, wo)
+    Esh = eng.init()
+    assert abs(Esh - Esh_o) < REL * abs(Esh_o)
+    Esh_o, _ = O.run(ham, wo, prop, 21, Esh_o, ortho_interval=5, pop_interval=20)
+    Esh, _ = eng.run(21, Esh, ortho_interval=5, pop_interval=20)
+    assert abs(Esh - Esh_o) < REL * abs(Esh_o)
+    SM, pr = eng.walkers()
+    assert rel(pr["WEIGHT"], wo.weight) < REL
+    assert rel(pr["OVLP"], wo.ovlp) < REL
+    assert rel(SM, wo.SM) < REL
+    # the comb picked the same parents: every slot holds the oracle's walker, not merely a close one
+    assert np.max(np.abs(SM - wo.SM)) < 1e-9 * np.max(np.abs(wo.SM))
+    eng.close()
+
+
+def test_engine_configs2_fp64_step_on_a_sample():
+    """The FP64 drop-in at M=400, N=100+100, Nchol=2400 on a 16-walker sample: one step and the
+    local energy of the propagated walkers against the oracle at 1e-10."""
+    s, ham, eng, prop, wo = _engine_pair(synthetic.CFG_LARGE, 16, dt=0.0005, seed=1000)
+    Esh_o = O.init_walkers(ham, wo)
+    Esh = eng.init()
+    assert abs(Esh - Esh_o) < REL * abs(Esh_o)
+    dbg = prop.propagate(wo, Esh_o, 0)
+    eng.propagate(Esh, 0)
+    assert rel(eng.fetch("X", (16, s.Nc), np.complex128), dbg["X"]) < REL
+    SM, pr = eng.walkers()
+    assert rel(SM, wo.SM) < REL
+    assert rel(pr["WEIGHT"], wo.weight) < REL
+    assert rel(pr["OVLP"], wo.ovlp) < REL
+    E = eng.energy()
+    Eo, _ = O.wfn_energy_noupdate(ham, wo)
+    assert rel(E, Eo) < REL
+    eng.close()
+
+
 def test_engine_host_step_matches_device_step():
     s = synthetic.make_system(synthetic.CFG_SMALL)
     e1 = A.AfqmcEngine(s, 8, seed=3)
