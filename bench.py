@@ -43,9 +43,9 @@ CONFIGS = {
 }
 ORTHO_EVERY = 5
 POP_EVERY = 20
-# DRAM bytes (read + write) of one Taylor-term int8 product at 64 walkers, M = 400, N = 100, from an
-# ncu capture (profiles/islice_taylor_M400_N100_W64_full.md); None until captured
-TAYLOR_DRAM_BYTES_64 = None
+# DRAM bytes (read + write) of one Taylor-term int8 product at 256 walkers, M = 400, N = 100, from an
+# ncu capture of the same kernel and tile (profiles/islice_taylor_M400_N100_W256_full.md)
+TAYLOR_DRAM_BYTES_256 = 339.224064e6 + 62.147584e6
 EQUIL_STEPS = 100  # run_afqmc relaxes Eshift every step for the first equilibration_steps
 RELAX = 1.0 - math.exp(-10.0 / EQUIL_STEPS)
 
@@ -494,11 +494,11 @@ def main():
     traffic = None
     if prec == capi.PRECISION_INT8X3 and spec.M == 400 and spec.N == 100:
         # dram__bytes_read.sum + dram__bytes_write.sum of the Taylor product in one ncu capture of
-        # sfq_gemm_int8_cplx_b at 64 walkers, M = 400, N = 100 (the same kernel and tile),
-        # scaled to this launch's walkers: every byte moved is per walker
-        traffic = TAYLOR_DRAM_BYTES_64 * W / 64.0 if TAYLOR_DRAM_BYTES_64 else None
+        # sfq_gemm_int8_cplx_b at 256 walkers, M = 400, N = 100 (the same kernel and tile), scaled
+        # to this launch's walkers: every byte moved is per walker
+        traffic = TAYLOR_DRAM_BYTES_256 * W / 256.0
         roofline.update({"traffic_unit": "bytes per launch",
-                         "traffic_source": "ncu capture of the same product at 64 walkers, scaled by walkers",
+                         "traffic_source": "ncu capture of the same product (256 walkers), scaled by walkers",
                          "algorithmic_bytes_per_launch": W * (3.0 * 2 * spec.M * spec.M + 3.0 * 3 * spec.N * spec.M
                                                               + 4.0 * 2 * spec.N * spec.M)})
     roofline.update({"algorithmic_flops_per_launch": alg, "launch_ms": launch_ms, "launches_timed": t_n,
