@@ -4,10 +4,12 @@ continuous batching on the GPU; and its benchmark.
     python -m safire_b200.serve            # 40 systems, Poisson arrivals, p50/p99 block latency
 
 The benchmark builds 40 synthetic systems (M uniform in [32, 400] on a multiple of 16, N = M/4,
-Nchol = 6M, 128 walkers each, mixed precision), measures batch-mode capacity (blocks of all systems
-submitted at once, repeatedly), then drives Poisson arrivals at fractions of that capacity, each
-request a block of 20 steps plus one local-energy measurement for a uniformly chosen system, and
-prints one JSON line with p50/p99 block latency and walker-steps/s per arrival rate.
+Nchol = 6M, 128 walkers each, INT8X3 precision as the headline's), measures batch-mode capacity in a
+steady state (many rounds of blocks of every system submitted at once and drained, so the tail of
+the last blocks is a small part of the time), then drives Poisson arrivals at fractions of that
+capacity, each request a block of 20 steps plus one local-energy measurement for a uniformly chosen
+system, a fixed number of requests per rate (1000 by default, so that p99 is a percentile and not
+the maximum), and prints one JSON line with p50/p99 block latency and walker-steps/s per rate.
 """
 import argparse
 import ctypes
@@ -121,9 +123,10 @@ def _systems(count, seed):
 def system_dt(M):
     """Timestep of a serving system: these synthetic systems' force bias grows as the walkers move
     away from the (poor) trial, and the walkers of the larger ones die out after a few hundred steps
-    at dt = 5e-4 (in FP64 as in mixed precision); dt ~ 1/M keeps every system alive for the whole
-    run.  The work per step does not depend on dt."""
-    return float(min(max(1e-4 * 256.0 / M, 5e-5), 1e-3))
+    at dt = 5e-4; with dt = 5e-5 * 256 / M every system (M = 48 .. 400, 128 walkers) survives 250
+    blocks of 20 steps, the benchmark's length, while 1e-4 * 256 / M lost M = 320 and 400 after 60-70
+    blocks.  The work per step does not depend on dt."""
+    return float(min(max(5e-5 * 256.0 / M, 2.5e-5), 5e-4))
 
 
 def _percentile(x, q):
@@ -138,23 +141,25 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--inflight", type=int, default=8)
     ap.add_argument("--rates", default="0.1,0.3,0.5,0.7,0.9,1.0,1.2")
-    ap.add_argument("--seconds", type=float, default=8.0, help="arrival window per rate")
-    ap.add_argument("--batch-rounds", type=int, default=3)
+    ap.add_argument("--requests", type=int, default=1000, help="requests per rate")
+    ap.add_argument("--batch-rounds", type=int, default=12)
+    ap.add_argument("--precision", default="int8x3", choices=["int8x3", "mixed", "fp64"])
     a = ap.parse_args()
+    prec = {"int8x3": capi.PRECISION_INT8X3, "mixed": capi.PRECISION_MIXED, "fp64": capi.PRECISION_FP64}[a.precision]
     systems = _systems(a.systems, 7)
     srv = Server(a.budget_gb, a.inflight)
-    ids = [srv.add_system(s, a.walkers, dt=system_dt(s.M), seed=1000 + i, precision=capi.PRECISION_MIXED)
+    ids = [srv.add_system(s, a.walkers, dt=system_dt(s.M), seed=1000 + i, precision=prec)
            for i, s in enumerate(systems)]
     t0 = time.time()
     for sid in ids:
         srv.warm(sid)
     build_s = time.time() - t0
     blk = dict(BLOCK, steps=a.steps)
-    # one warm block per system (graph capture), then batch mode: every system at once, repeatedly
+    # one warm block per system (graph capture), then batch mode: batch_rounds blocks of every system
+    # submitted at once and drained (the server runs them max_inflight at a time)
     srv.drain([srv.submit(sid, **blk) for sid in ids])
     t0 = srv.clock()
-    for _ in range(a.batch_rounds):
-        srv.drain([srv.submit(sid, **blk) for sid in ids])
+    srv.drain([srv.submit(sid, **blk) for _ in range(a.batch_rounds) for sid in ids])
     batch_s = srv.clock() - t0
     nblocks = a.batch_rounds * len(ids)
     ws_block = a.walkers * a.steps
@@ -164,8 +169,7 @@ def main():
     rows = []
     for f in [float(x) for x in a.rates.split(",")]:
         lam = f * cap_rps
-        arrivals = np.cumsum(rng.exponential(1.0 / lam, size=int(lam * a.seconds * 1.5) + 4))
-        arrivals = arrivals[arrivals < a.seconds]
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, size=a.requests))
         picks = rng.integers(0, len(ids), size=len(arrivals))
         rids = []
         base = srv.clock()
@@ -190,8 +194,9 @@ def main():
     srv.close()
     print(json.dumps({
         "metric": "serving block latency", "unit": "ms", "systems": len(ids), "walkers_per_system": a.walkers,
-        "block": f"{a.steps} steps + 1 local-energy measurement", "precision": "mixed (2 BF16 planes)",
-        "dt": "1e-4 * 256 / M, clipped to [5e-5, 1e-3]", "max_inflight": a.inflight, "hbm_budget_gb": a.budget_gb, "resident_bytes": st["used_bytes"],
+        "block": f"{a.steps} steps + 1 local-energy measurement", "precision": a.precision,
+        "requests_per_rate": a.requests, "batch_blocks": nblocks,
+        "dt": "5e-5 * 256 / M, clipped to [2.5e-5, 5e-4]", "max_inflight": a.inflight, "hbm_budget_gb": a.budget_gb, "resident_bytes": st["used_bytes"],
         "build_seconds": build_s, "batch_walker_steps_per_s": batch_ws, "batch_blocks_per_s": cap_rps,
         "rates": rows, "data": "synthetic (M uniform in [32, 400] on multiples of 16, N = M/4, Nchol = 6M)"}))
 

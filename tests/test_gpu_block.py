@@ -79,8 +79,9 @@ def test_block_async_query_result():
     b.close()
 
 
-def test_mixed_block_matches_host_loop():
-    host, dev = _pair(prec=capi.PRECISION_MIXED, spec=synthetic.CFG_MEDIUM, W=16, seed=2)
+@pytest.mark.parametrize("prec", [capi.PRECISION_MIXED, capi.PRECISION_INT8X3])
+def test_mixed_block_matches_host_loop(prec):
+    host, dev = _pair(prec=prec, spec=synthetic.CFG_MEDIUM, W=16, seed=2)
     E0 = host.init()
     dev.init()
     sched = dict(ortho_interval=5, pop_interval=20, equilibration_steps=0, measure_interval=10)
