@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 9 */
+int sfq_abi_version(void); /* 10 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -74,8 +74,9 @@ int sfq_mixed_density_matrix(const void* A, int a_complex, const void* B, void* 
  * device-wide synchronisation).  Scratch is a fixed array of sfq_noalloc_scratch_bytes() (16 MiB)
  * compiled into the library and held on every GPU that loads it until the process exits; calls
  * with nwalk * nel * nel * 16 bytes above that return SFQ_ERR_WORKSPACE.  All calls on a device
- * share the array, so calls that overlap on the GPU race; the first call on each device looks up
- * the array's address and should come before any stream capture. */
+ * share the array, so calls that overlap on the GPU race; the first call in each context looks up
+ * the array's address and should come before any stream capture; the address is kept with the
+ * context's id, so a context created anew (after cudaDeviceReset) is looked up again. */
 int sfq_mixed_density_matrix_noalloc(const void* A, int a_complex, const void* B, void* C, void* ovlp, int nwalk,
                                      int nmo, int nel, void* stream);
 size_t sfq_noalloc_scratch_bytes(void);
@@ -517,6 +518,20 @@ int sfq_engine_info(sfq_engine_t e, sfq_engine_info_t* info);
 /* WalkerSet::copy_walker (WalkerSetBase.h:413-415): every field of the walker in slot `from` (its
  * Slater matrix and property columns) into slot `to`. */
 int sfq_engine_copy_walker(sfq_engine_t e, int from, int to);
+/* The sharded walker exchange on device buffers (swap_walkers_async, population_control.hpp:143-209;
+ * the plan from sfq_walker_moves).  A row is one walker: its Slater matrix followed by its 8 property
+ * values (the column order of sfq_engine_set_walkers), sfq_engine_walker_row_elems complex values in
+ * all (negative: an error code).  pack writes walker slots[r] into row r of `rows` (device memory,
+ * n rows), unpack writes row r into walker slots[r]; copy_walkers first sets every weight to
+ * w / |w| when normalize_weights != 0 (population_control.hpp:238-241), then copies walker
+ * pairs[2k] into walker pairs[2k+1], k < n (destinations distinct and none a source).  slots and
+ * pairs are host arrays.  Each call runs on the engine stream and returns after it has finished, so
+ * the rows are ready for a send on another stream.  Engines with back propagation on are refused
+ * (the rows do not carry its history). */
+long sfq_engine_walker_row_elems(sfq_engine_t e);
+int sfq_engine_pack_walkers(sfq_engine_t e, const int* slots, int n, void* rows);
+int sfq_engine_unpack_walkers(sfq_engine_t e, const int* slots, int n, const void* rows);
+int sfq_engine_copy_walkers(sfq_engine_t e, const int* pairs, int n, int normalize_weights);
 /* WalkerSet::resize (WalkerSetBase.h:195): the engine is rebuilt for nwalk walkers (the resident
  * tensors recomputed from its Hamiltonian and trial, tiles back to their defaults, back propagation
  * off), and its walkers are carried over, new slots filled from the existing walkers in

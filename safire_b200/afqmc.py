@@ -221,6 +221,47 @@ class AfqmcEngine:
         check(lib().sfq_engine_set_walkers(self.h, None if sm is None else sm.ctypes.data,
                                            None if pr is None else pr.ctypes.data))
 
+    def properties(self):
+        """The property columns alone (WEIGHT, PHASE, ...: W values each), without the Slater matrices."""
+        pr = np.empty((len(capi.PROPS), self.W), np.complex128)
+        check(lib().sfq_engine_get_walkers(self.h, None, pr.ctypes.data))
+        return {k: pr[i].copy() for i, k in enumerate(capi.PROPS)}
+
+    # the sharded walker exchange on device rows (sfq_engine_pack_walkers / unpack_walkers / copy_walkers)
+    @property
+    def exchange_device(self):
+        import torch
+        return torch.device("cuda", int(self.params.device))
+
+    def walker_row_elems(self):
+        n = int(lib().sfq_engine_walker_row_elems(self.h))
+        if n < 0:
+            check(-n)
+        return n
+
+    def _rows(self, rows, n):
+        import torch
+        if n and (not isinstance(rows, torch.Tensor) or rows.device != self.exchange_device or not rows.is_contiguous()
+                  or rows.dtype != torch.float64 or rows.numel() < n * 2 * self.walker_row_elems()):
+            raise capi.SafireError(2, "walker rows: a contiguous float64 tensor of (n, 2 * walker_row_elems()) "
+                                      "on the engine's device")
+        return ctypes.c_void_p(rows.data_ptr() if n else 0)
+
+    def pack_walkers(self, slots, rows):
+        """rows[r] <- walker slots[r] (Slater matrix, then the 8 property values)."""
+        sl = np.ascontiguousarray(np.asarray(slots, np.int32).reshape(-1))
+        check(lib().sfq_engine_pack_walkers(self.h, sl.ctypes.data, sl.size, self._rows(rows, sl.size)))
+
+    def unpack_walkers(self, slots, rows):
+        """walker slots[r] <- rows[r]."""
+        sl = np.ascontiguousarray(np.asarray(slots, np.int32).reshape(-1))
+        check(lib().sfq_engine_unpack_walkers(self.h, sl.ctypes.data, sl.size, self._rows(rows, sl.size)))
+
+    def copy_walkers(self, pairs, normalize=True):
+        """Every weight to w / |w| (normalize), then walker dst <- walker src for (src, dst) in pairs."""
+        pr = np.ascontiguousarray(np.asarray(pairs, np.int32).reshape(-1, 2))
+        check(lib().sfq_engine_copy_walkers(self.h, pr.ctypes.data, len(pr), int(bool(normalize))))
+
     def walker_buffer(self):
         rows = np.empty((self.W, self.Mr * self.N + 11), np.complex128)
         check(lib().sfq_engine_export_walker_buffer(self.h, rows.ctypes.data))

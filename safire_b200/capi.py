@@ -105,6 +105,10 @@ _SIGS = {
     "sfq_split_bf16": ([_VP, ctypes.c_long, _VP, _VP, _VP, _VP], _I),
     "sfq_gemm_int8_slices": ([_VP, _VP, _VP, _I, _I, _I, _I, _I, _I, _VP], _I),
     "sfq_engine_copy_walker": ([_VP, _I, _I], _I),
+    "sfq_engine_walker_row_elems": ([_VP], ctypes.c_long),
+    "sfq_engine_pack_walkers": ([_VP, _VP, _I, _VP], _I),
+    "sfq_engine_unpack_walkers": ([_VP, _VP, _I, _VP], _I),
+    "sfq_engine_copy_walkers": ([_VP, _VP, _I, _I], _I),
     "sfq_selftest_wait_expiry": ([_U64, _VP], _I),
     "sfq_engine_resize": ([_VP, _I], _I),
     "sfq_one_body_matrix": ([_VP, _VP, _VP, _VP, _I, _I, _D, _VP, _VP], _I),

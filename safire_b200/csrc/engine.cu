@@ -34,7 +34,7 @@ namespace sfq {
 
 namespace {
 
-constexpr int kNumProps = 8;  // WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, THETA
+constexpr int kNumProps = kWalkerProps;  // WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, THETA
 enum { P_WEIGHT = 0, P_PHASE, P_PSEUDO, P_E1, P_EXX, P_EJ, P_OVLP, P_THETA };
 constexpr long kEnergyChunkElems = 1L << 27;
 
@@ -407,8 +407,8 @@ struct Engine {
   int8_t* Gv_q[3] = {};  int* Gv_e = nullptr;   // G, planar rows (c, w) over (a, k)
   int8_t* Ge_q[3] = {};  int* Ge_e = nullptr;   // G, planar rows (c, w, a) over k
   int8_t* Xq_q[3] = {};  int* Xq_e = nullptr;   // fields, planar rows (c, w) over n
-  int8_t* V_q[3] = {};   int* V_e = nullptr;  int* V_emax = nullptr;  // V[w][c][i][k], exponent per (w, i)
-  int8_t* A_q[2][3] = {};  int8_t* A_n[2][3] = {};  int* A_e[2] = {};  // walker operand: rows (c, r); -im rows r
+  int8_t* V_q[3] = {};   int* V_e = nullptr;  int* V_emax = nullptr;  // V[w][c][i][k]: Vr, Vi, -Vi; e per (w, i)
+  int8_t* A_q[2][3] = {};  int* A_e[2] = {};  // walker operand: rows (c, r)
   cplx* GT_c = nullptr;  // the trial's own G (N, M) and force bias (Nc), FP64
   cplx* vbT = nullptr;
   float* Cp = nullptr;  // FP32 output of the walker-shaped products, planar (2 W N, M)
@@ -572,11 +572,8 @@ struct Engine {
         mx.push_back({(void**)&Gv_q[q], (size_t)2 * W * ld_nm});
         mx.push_back({(void**)&Ge_q[q], (size_t)2 * R * ld_m});
         mx.push_back({(void**)&Xq_q[q], (size_t)2 * W * ld_nc});
-        mx.push_back({(void**)&V_q[q], (size_t)W * 2 * M * ld_m});
-        for (int b = 0; b < 2; ++b) {
-          mx.push_back({(void**)&A_q[b][q], (size_t)2 * R * ld_m});
-          mx.push_back({(void**)&A_n[b][q], (size_t)R * ld_m});
-        }
+        mx.push_back({(void**)&V_q[q], (size_t)W * 3 * M * ld_m});
+        for (int b = 0; b < 2; ++b) mx.push_back({(void**)&A_q[b][q], (size_t)2 * R * ld_m});
       }
       const size_t ie = sizeof(int);
       std::vector<Item> mx2 = {
@@ -1666,11 +1663,8 @@ struct Engine {
     IsliceGemmDesc d = i8_desc();
     d.M = N; d.N = M; d.K = M; d.batch = W;
     d.A = i8_operand(A_q[buf], N, ld_m, A_e[buf], (long)N * ld_m, N);
-    for (int s2 = 0; s2 < 3; ++s2) {
-      d.a_im[s2] = A_q[buf][s2] ? A_q[buf][s2] + R * ld_m : nullptr;
-      d.a_nim[s2] = A_n[buf][s2];
-    }
-    d.B = i8_operand(V_q, 2L * M, ld_m, V_e, 2L * M * ld_m, M);
+    for (int s2 = 0; s2 < 3; ++s2) d.a_im[s2] = A_q[buf][s2] ? A_q[buf][s2] + R * ld_m : nullptr;
+    d.B = i8_operand(V_q, 3L * M, ld_m, V_e, 3L * M * ld_m, M);
     d.cplx_half = i8_half;
     d.C = Cp; d.ldc = M; d.sCc = R * M;
     return islice_gemm(d, st);
@@ -1733,15 +1727,14 @@ struct Engine {
     // S = P1 W = W + (P1 - I) W; then T_k = (i/k) V T_{k-1}, S += T_k for k = 1..order; SM = S + (P1 - I) S
     if ((rc = islice_walkers(SM, W, M, N, nslices, A_q[0], ld_m, A_e[0], Sacc, st))) return rc;
     if ((rc = i8_p1(0, Cp, false))) return rc;
-    if ((rc = islice_taylor_update(Cp, Sacc, R, M, 0, true, nslices, A_q[1], A_n[1], ld_m, A_e[1], st))) return rc;
+    if ((rc = islice_taylor_update(Cp, Sacc, R, M, 0, true, nslices, A_q[1], ld_m, A_e[1], st))) return rc;
     int cur = 1;
     for (int k = 1; k <= p.taylor_order; ++k) {
       ph_begin(SFQ_PH_TAYLOR_GEMM);
       if ((rc = i8_taylor(cur))) return rc;
       ph_end(SFQ_PH_TAYLOR_GEMM);
       const bool last = k == p.taylor_order;
-      if ((rc = islice_taylor_update(Cp, Sacc, R, M, k, last, nslices, A_q[1 - cur], last ? nullptr : A_n[1 - cur],
-                                     ld_m, A_e[1 - cur], st)))
+      if ((rc = islice_taylor_update(Cp, Sacc, R, M, k, last, nslices, A_q[1 - cur], ld_m, A_e[1 - cur], st)))
         return rc;
       cur = 1 - cur;
     }
@@ -2898,6 +2891,58 @@ int sfq_engine_copy_walker(sfq_engine_t h, int from, int to) {
   SFQ_CUDA_TRY(cudaMemcpy2DAsync(e.props + to, sizeof(cplx) * e.W, e.props + from, sizeof(cplx) * e.W, sizeof(cplx),
                                  kNumProps, cudaMemcpyDeviceToDevice, e.st));
   e.inv_cached = false;
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+long sfq_engine_walker_row_elems(sfq_engine_t h) {
+  if (!h) return -record_error(SFQ_ERR_ARG, "null engine");
+  return (long)h->e.Mr * h->e.N + kNumProps;
+}
+
+namespace {
+int exchange_checks(sfq_engine_t h, const void* list, int n, const void* rows, bool need_rows) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  if (n < 0) return record_error(SFQ_ERR_ARG, "walker exchange: %d rows", n);
+  if (n > 0 && (!list || (need_rows && !rows))) return record_error(SFQ_ERR_ARG, "walker exchange: null pointer");
+  if (h->e.nbp)
+    return record_error(SFQ_ERR_UNSUPPORTED, "walker exchange: the rows do not carry back-propagation history");
+  return SFQ_OK;
+}
+}  // namespace
+
+int sfq_engine_pack_walkers(sfq_engine_t h, const int* slots, int n, void* rows) {
+  int rc;
+  if ((rc = exchange_checks(h, slots, n, rows, true))) return rc;
+  Engine& e = h->e;
+  SFQ_CUDA_TRY(cudaSetDevice(e.p.device));
+  if ((rc = pack_walker_rows(e.SM, e.props, e.W, (long)e.Mr * e.N, slots, n, static_cast<cplx*>(rows), e.st)))
+    return record_error(rc, "pack_walkers: a slot outside [0, %d)", e.W);
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+int sfq_engine_unpack_walkers(sfq_engine_t h, const int* slots, int n, const void* rows) {
+  int rc;
+  if ((rc = exchange_checks(h, slots, n, rows, true))) return rc;
+  Engine& e = h->e;
+  SFQ_CUDA_TRY(cudaSetDevice(e.p.device));
+  e.inv_cached = false;
+  if ((rc = unpack_walker_rows(e.SM, e.props, e.W, (long)e.Mr * e.N, slots, n, static_cast<const cplx*>(rows), e.st)))
+    return record_error(rc, "unpack_walkers: a slot outside [0, %d)", e.W);
+  SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
+  return SFQ_OK;
+}
+
+int sfq_engine_copy_walkers(sfq_engine_t h, const int* pairs, int n, int normalize_weights) {
+  int rc;
+  if ((rc = exchange_checks(h, pairs, n, nullptr, false))) return rc;
+  Engine& e = h->e;
+  SFQ_CUDA_TRY(cudaSetDevice(e.p.device));
+  e.inv_cached = false;
+  if ((rc = copy_walker_pairs(e.SM, e.props, e.W, (long)e.Mr * e.N, pairs, n, normalize_weights, e.st)))
+    return record_error(rc, "copy_walkers: pairs must lie in [0, %d), with distinct destinations that are no source",
+                        e.W);
   SFQ_CUDA_TRY(cudaStreamSynchronize(e.st));
   return SFQ_OK;
 }

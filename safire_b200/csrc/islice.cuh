@@ -20,17 +20,17 @@
 //
 // Persistent kernel: one CTA per SM walks a static list of 128 x BN output tiles; warp 0 issues
 // TMA loads of 128-byte K slices (128 int8 elements) into a ring of stages, one thread of warp 1
-// issues tcgen05.mma.kind::i8 (M = 128, N = BN, K = 32) and commits each stage, four epilogue
+// issues tcgen05.mma.kind::i8 (M = 128, N = BN, K = 32) and commits each stage, eight epilogue
 // warps drain the group accumulators.  K tails are zero-filled by TMA and their MMA steps skipped.
 // Every mbarrier wait is bounded from its own start; on expiry the kernel records SFQ_ERR_TIMEOUT,
 // waits for its own copies and MMAs, frees its tensor memory and returns.
 //
 // Complex B (cplx_half > 0), the Taylor product C = A [[Vr, -Vi], [Vi, Vr]]^T of one walker:
-// B holds the rows Vr (i < nmo) and Vi (nmo + i) sharing one exponent per orbital i; A has three
-// arrays of the same shape, the real parts (a.q), the imaginary parts (a_im) and the negated
-// imaginary parts (a_nim), one exponent per row.  Output tile t holds [re | im] over orbitals
-// t * half ... + half:  [re | im] += A_re [Vr; Vi]^T,  re += (-A_im) Vi^T,  im += A_im Vr^T
-// (int8 products have no negate bit, hence the negated copy), written planar:
+// B holds the rows Vr (i < nmo), Vi (nmo + i) and -Vi (2 nmo + i) sharing one exponent per
+// orbital i; A has two arrays of the same shape, the real parts (a.q) and the imaginary parts
+// (a_im), one exponent per row.  Output tile t holds [re | im] over orbitals t * half ... + half,
+// two full-width MMAs per K step:  [re | im] += A_re [Vr; Vi]^T  and  [re | im] += A_im [-Vi; Vr]^T
+// (int8 products have no negate bit, hence the negated rows of V), written planar:
 // C[c * sCc + (batch * M + row) * ldc + i].
 #pragma once
 #include <cstdint>
@@ -58,7 +58,6 @@ struct IsliceGemmDesc {
   IsliceOperand A, B;
   int cplx_half = 0;                   // complex B (see above): orbitals per tile
   const int8_t* a_im[3] = {nullptr, nullptr, nullptr};
-  const int8_t* a_nim[3] = {nullptr, nullptr, nullptr};
   float* C = nullptr;                  // FP32 output, row-major: C[s*sCk + batch*sCb + row*ldc + col]
   long ldc = 0, sCb = 0, sCc = 0;      // sCc: complex B, elements between the re and im outputs
   double alpha = 1.0;
@@ -88,12 +87,13 @@ int islice_walkers(const cplx* SM, int W, int M, int N, int nslices, int8_t* con
                    float* planar, cudaStream_t st);
 // planar walker-shaped FP32 rows (r < R = W N, j < M, M <= 1024), the product C[c][r][j] into the
 // sum S[c][r][j]: k = 0: S += C; k > 0: T = (i / k) C (T_re = -C_im / k, T_im = C_re / k) and
-// S += T; then the slices of S (slice_sum; required for k = 0) or of T into q (rows (c, r)) and
-// into the negated imaginary rows qn (rows r; may be null), one exponent per r
+// S += T; then the slices of S (slice_sum; required for k = 0) or of T into q (rows (c, r)), one
+// exponent per r
 int islice_taylor_update(const float* C, float* S, long R, int M, int k, bool slice_sum, int nslices,
-                         int8_t* const* q, int8_t* const* qn, long ld, int* e, cudaStream_t st);
+                         int8_t* const* q, long ld, int* e, cudaStream_t st);
 // vHS (planar rows c * W + w over the packed upper triangle, or over M * M) -> V slices
-// V[w][c][i][k] with one exponent per (w, i) shared by Vr and Vi rows; emax: W * M scratch ints
+// V[w][c][i][k], c = 0, 1, 2 for Vr, Vi, -Vi (the negation sliced as itself), with one exponent per
+// (w, i) shared by the three rows; emax: W * M scratch ints
 int islice_build_v(const float* Cv, int W, int M, bool packed, int nslices, int8_t* const* q, long ld, int* e,
                    int* emax, cudaStream_t st);
 // planar FP32 rows C[c][w][a][j] (+ S[c][w][a][j] when S is given, added in FP64) -> SM[w][j][a]

@@ -57,13 +57,13 @@ struct Smem {
 };
 
 struct Maps {
-  CUtensorMap a[3], b[3], aim[3], anim[3];
+  CUtensorMap a[3], b[3], aim[3];
 };
 
 struct KParams {
   int M, N, K, batch;
   int a_batched, b_batched;
-  int MT, NT, KS, KT;  // tiles along M, N; K splits; K slices (complex B: 3 per 128 orbitals)
+  int MT, NT, KS, KT;  // tiles along M, N; K splits; K slices (complex B: 2 per 128 orbitals)
   long tiles;
   int half;            // complex B: orbitals per tile (0: plain product)
   const int* ea; long ea_bs, ea_mod;
@@ -234,21 +234,16 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
           }
           unsigned char* stg = smem + s * L::STAGE;
           if (cb) {
-            const int part = kt % 3, k0 = (kt / 3) * BK, i0 = nt * p.half;
-            const uint32_t bbytes = uint32_t((part == 0 ? 2 : 1) * p.half * BK);
-            mbar_expect_tx(&full[s], uint32_t(NS) * (uint32_t(L::A_BYTES) + bbytes));
+            // part 0: A_re with the rows [Vr; Vi] of the tile's orbitals; part 1: A_im with [-Vi; Vr]
+            const int part = kt & 1, k0 = (kt >> 1) * BK, i0 = nt * p.half;
+            mbar_expect_tx(&full[s], uint32_t(L::STAGE));
 #pragma unroll
             for (int q = 0; q < NS; ++q) {
               unsigned char* at = stg + q * L::A_BYTES;
               unsigned char* bt = stg + NS * L::A_BYTES + q * L::B_BYTES;
-              const CUtensorMap* am = part == 0 ? &maps.a[q] : part == 1 ? &maps.anim[q] : &maps.aim[q];
-              tma_load_3d(at, am, &full[s], k0, m0, ab);
-              if (part == 0) {  // [Vr; Vi] rows of the tile's orbitals
-                tma_load_3d(bt, &maps.b[q], &full[s], k0, i0, bb);
-                tma_load_3d(bt + p.half * BK, &maps.b[q], &full[s], k0, p.N + i0, bb);
-              } else {          // Vi (for -A_im) or Vr (for A_im)
-                tma_load_3d(bt, &maps.b[q], &full[s], k0, (part == 1 ? p.N : 0) + i0, bb);
-              }
+              tma_load_3d(at, part == 0 ? &maps.a[q] : &maps.aim[q], &full[s], k0, m0, ab);
+              tma_load_3d(bt, &maps.b[q], &full[s], k0, (part == 0 ? 0 : 2 * p.N) + i0, bb);
+              tma_load_3d(bt + p.half * BK, &maps.b[q], &full[s], k0, (part == 0 ? p.N : 0) + i0, bb);
             }
           } else {
             const int k0 = kt * BK, n0 = nt * BN;
@@ -298,26 +293,17 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
             ad[q] = smem_desc(stg + q * L::A_BYTES);
             bd[q] = smem_desc(stg + NS * L::A_BYTES + q * L::B_BYTES);
           }
-          const int part = cb ? kt % 3 : 0;
-          const int k0 = cb ? (kt / 3) * BK : kt * BK;
+          const int k0 = cb ? (kt >> 1) * BK : kt * BK;
           const int rem = Kv - k0;
           const int nk = rem >= BK ? BK / KSTEP : (rem + KSTEP - 1) / KSTEP;  // K tail: skip all-zero steps
-          uint32_t idesc, coff;
-          if (!cb || part == 0) {
-            idesc = idesc_i8(uint32_t(BN));
-            coff = 0;
-          } else {
-            idesc = idesc_i8(uint32_t(p.half));
-            coff = part == 1 ? 0u : uint32_t(p.half);  // -A_im Vi^T into re, A_im Vr^T into im
-          }
+          const uint32_t idesc = idesc_i8(uint32_t(BN));
           const bool first_slice = kt == kb;  // complex B: part 0 of the first K block initialises
           for (int kk = 0; kk < nk; ++kk) {
             const uint64_t off = uint64_t(kk * KSTEP) >> 4;  // 32 bytes along the swizzled row
 #pragma unroll
             for (int t2 = 0; t2 < NP; ++t2) {
               const uint32_t accum = (first_slice && kk == 0 && pair_first(t2)) ? 0u : 1u;
-              umma_i8(d_tmem + uint32_t(pair_g(t2) * BN) + coff, ad[pair_a(t2)] + off, bd[pair_b(t2)] + off, idesc,
-                      accum);
+              umma_i8(d_tmem + uint32_t(pair_g(t2) * BN), ad[pair_a(t2)] + off, bd[pair_b(t2)] + off, idesc, accum);
             }
           }
           umma_commit(&empty[s]);
@@ -399,19 +385,16 @@ int launch(const IsliceGemmDesc& d, cudaStream_t st) {
     if ((rc = make_map_i8(&maps.b[q], d.B.q[q], d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, cb ? d.cplx_half : BN)))
       return rc;
     if (cb) {
-      if (!d.a_im[q] || !d.a_nim[q]) return record_error(SFQ_ERR_ARG, "islice_gemm: complex B needs a_im and a_nim");
+      if (!d.a_im[q]) return record_error(SFQ_ERR_ARG, "islice_gemm: complex B needs a_im");
       if ((rc = make_map_i8(&maps.aim[q], d.a_im[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
-      if ((rc = make_map_i8(&maps.anim[q], d.a_nim[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
     } else {
       maps.aim[q] = maps.a[q];
-      maps.anim[q] = maps.a[q];
     }
   }
   for (int q = NS; q < 3; ++q) {
     maps.a[q] = maps.a[0];
     maps.b[q] = maps.b[0];
     maps.aim[q] = maps.aim[0];
-    maps.anim[q] = maps.anim[0];
   }
   if (!d.A.e || !d.B.e || !d.C) return record_error(SFQ_ERR_ARG, "islice_gemm: exponents and output required");
   KParams kp;
@@ -419,11 +402,11 @@ int launch(const IsliceGemmDesc& d, cudaStream_t st) {
   kp.a_batched = d.A.batch_stride != 0; kp.b_batched = d.B.batch_stride != 0;
   kp.MT = (d.M + BM - 1) / BM;
   if (cb) {
-    if (d.cplx_half * 2 != BN || d.cplx_half % 16 || d.K != d.N || d.B.rows != 2L * d.N || d.ksplit > 1)
+    if (d.cplx_half * 2 != BN || d.cplx_half % 16 || d.K != d.N || d.B.rows != 3L * d.N || d.ksplit > 1)
       return record_error(SFQ_ERR_ARG, "islice_gemm: complex B needs BN = 2 half, half %% 16 == 0, K = N = nmo, "
-                                       "B rows = 2 nmo and no K split");
+                                       "B rows = 3 nmo and no K split");
     kp.NT = (d.N + d.cplx_half - 1) / d.cplx_half;
-    kp.KT = 3 * ((d.K + BK - 1) / BK);
+    kp.KT = 2 * ((d.K + BK - 1) / BK);
     kp.KS = 1;
   } else {
     kp.NT = (d.N + BN - 1) / BN;
@@ -588,18 +571,17 @@ int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, i
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t sa = al(sizeof(float) * 2 * R * M), sz = al(sizeof(float) * 2 * R * M),
                sv = al(sizeof(float) * 2 * W * MM);
-  const size_t qa = al((size_t)2 * R * ld), qn = al((size_t)R * ld), qv = al((size_t)W * 2 * M * ld);
+  const size_t qa = al((size_t)2 * R * ld), qv = al((size_t)W * 3 * M * ld);
   const size_t ea = al(sizeof(int) * R), ev = al(sizeof(int) * W * M);
   char* buf = nullptr;
-  SFQ_CUDA_TRY(cudaMallocAsync((void**)&buf, sa + sz + sv + nslices * (qa + qn + qv) + ea + 2 * ev, st));
+  SFQ_CUDA_TRY(cudaMallocAsync((void**)&buf, sa + sz + sv + nslices * (qa + qv) + ea + 2 * ev, st));
   char* o = buf;
   float* S = reinterpret_cast<float*>(o); o += sa;
   float* Cz = reinterpret_cast<float*>(o); o += sz;
   float* Cv = reinterpret_cast<float*>(o); o += sv;
-  int8_t *aq[3] = {}, *an[3] = {}, *vq[3] = {};
+  int8_t *aq[3] = {}, *vq[3] = {};
   for (int s = 0; s < nslices; ++s) {
     aq[s] = reinterpret_cast<int8_t*>(o); o += qa;
-    an[s] = reinterpret_cast<int8_t*>(o); o += qn;
     vq[s] = reinterpret_cast<int8_t*>(o); o += qv;
   }
   int* eA = reinterpret_cast<int*>(o); o += ea;
@@ -615,7 +597,7 @@ int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, i
                                                    Cv + (W + w) * MM);
     SFQ_LAUNCHED();
   }
-  int rc = islice_taylor_update(Cz, S, R, M, 0, true, nslices, aq, an, ld, eA, st);
+  int rc = islice_taylor_update(Cz, S, R, M, 0, true, nslices, aq, ld, eA, st);
   if (!rc) rc = islice_build_v(Cv, W, M, false, nslices, vq, ld, eV, eVmax, st);
   if (!rc) {
     IsliceGemmDesc d;
@@ -623,11 +605,10 @@ int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, i
     for (int s = 0; s < 3; ++s) {
       d.A.q[s] = aq[s];
       d.a_im[s] = aq[s] ? aq[s] + R * ld : nullptr;
-      d.a_nim[s] = an[s];
       d.B.q[s] = vq[s];
     }
     d.A.rows = N; d.A.ld = ld; d.A.batch_stride = (long)N * ld; d.A.e = eA; d.A.e_bs = N;
-    d.B.rows = 2L * M; d.B.ld = ld; d.B.batch_stride = 2L * M * ld; d.B.e = eV; d.B.e_bs = M;
+    d.B.rows = 3L * M; d.B.ld = ld; d.B.batch_stride = 3L * M * ld; d.B.e = eV; d.B.e_bs = M;
     d.cplx_half = half;
     d.C = C; d.ldc = M; d.sCc = R * M;
     rc = islice_gemm(d, st);

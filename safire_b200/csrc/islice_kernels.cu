@@ -220,12 +220,14 @@ __global__ void walkers_slice_kernel(const cplx* SM, int W, int M, int N, int ns
 // Taylor update, one warp per row r of the planar walker-shaped arrays (FP32):
 //   k = 0: S += C                    (S = W + (P1 - I) W = P1 W)
 //   k > 0: T = (i / k) C (T_re = -C_im / k, T_im = C_re / k), S += T
-// then the slices of S (SUM) or of T, one exponent per row over both parts.  Each lane keeps its
-// values in registers between the pass that updates S and finds the row's largest entry and the
-// pass that slices: four consecutive orbitals per group, kMaxQuads groups per lane (M <= 1024).
+// then the slices of S (SUM) or of T, one exponent per row over both parts.  Each lane holds QPL
+// groups of four consecutive orbitals (lane + 32 t, t < QPL; QPL * 128 >= the slice row stride,
+// at most kMaxQuads): every load of the row is issued before the first store, and the values stay
+// in registers between the pass that updates S and finds the row's largest entry and the pass
+// that slices.
 constexpr int kMaxQuads = 8;
 template <bool VEC>
-__device__ __forceinline__ void ld4(const float* p, float (&v)[4], int valid) {
+__device__ __forceinline__ void ld4(const float* __restrict__ p, float (&v)[4], int valid) {
   if (VEC) {
     const float4 u = *reinterpret_cast<const float4*>(p);
     v[0] = u.x; v[1] = u.y; v[2] = u.z; v[3] = u.w;
@@ -235,7 +237,7 @@ __device__ __forceinline__ void ld4(const float* p, float (&v)[4], int valid) {
   }
 }
 template <bool VEC>
-__device__ __forceinline__ void st4(float* p, const float (&v)[4], int valid) {
+__device__ __forceinline__ void st4(float* __restrict__ p, const float (&v)[4], int valid) {
   if (VEC) {
     *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
   } else {
@@ -244,45 +246,55 @@ __device__ __forceinline__ void st4(float* p, const float (&v)[4], int valid) {
       if (u < valid) p[u] = v[u];
   }
 }
-template <bool SUM, bool VEC>
-__global__ void taylor_update_kernel(const float* C, float* S, long R, int M, int k, int ns, Q q, Q qn, long ld,
-                                     int* e) {
+template <bool SUM, bool VEC, int QPL>
+__global__ void __launch_bounds__(256) taylor_update_kernel(const float* __restrict__ C, float* __restrict__ S,
+                                                            long R, int M, int k, int ns, Q q, long ld, int* e) {
   const long r = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (r >= R) return;
   const int G4 = (M + 3) >> 2;
-  float v[2][kMaxQuads][4];
+  float sr[QPL][4], si[QPL][4], vr[QPL][4], vi[QPL][4];
+#pragma unroll
+  for (int t = 0; t < QPL; ++t) {
+    const int g = lane + 32 * t;
+    const int valid = g < G4 ? (M - 4 * g < 4 ? M - 4 * g : 4) : 0;
+    if (valid) {
+      const long i0 = r * M + 4 * g, i1 = (R + r) * M + 4 * g;
+      ld4<VEC>(S + i0, sr[t], valid);
+      ld4<VEC>(S + i1, si[t], valid);
+      ld4<VEC>(C + i0, vr[t], valid);
+      ld4<VEC>(C + i1, vi[t], valid);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) sr[t][u] = si[t][u] = vr[t][u] = vi[t][u] = 0.f;
+    }
+  }
   float m = 0.f;
   const float fk = float(k);
 #pragma unroll
-  for (int t = 0; t < kMaxQuads; ++t) {
-    const int g = lane + 32 * t;
-    if (g >= G4) break;
-    const int valid = M - 4 * g < 4 ? M - 4 * g : 4;
-    const long i0 = r * M + 4 * g, i1 = (R + r) * M + 4 * g;
-    float sr[4], si[4], cr[4], ci[4];
-    ld4<VEC>(S + i0, sr, valid);
-    ld4<VEC>(S + i1, si, valid);
-    ld4<VEC>(C + i0, cr, valid);
-    ld4<VEC>(C + i1, ci, valid);
+  for (int t = 0; t < QPL; ++t) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      float tr, ti;
-      if (k == 0) {
-        tr = cr[u];
-        ti = ci[u];
-      } else {
-        tr = -ci[u] / fk;
-        ti = cr[u] / fk;
+      float tr = vr[t][u], ti = vi[t][u];
+      if (k != 0) {
+        tr = -vi[t][u] / fk;
+        ti = vr[t][u] / fk;
       }
-      sr[u] += tr;
-      si[u] += ti;
-      v[0][t][u] = SUM ? sr[u] : tr;
-      v[1][t][u] = SUM ? si[u] : ti;
-      m = fmaxf(m, fmaxf(fabsf(v[0][t][u]), fabsf(v[1][t][u])));
+      sr[t][u] += tr;
+      si[t][u] += ti;
+      vr[t][u] = SUM ? sr[t][u] : tr;
+      vi[t][u] = SUM ? si[t][u] : ti;
+      m = fmaxf(m, fmaxf(fabsf(vr[t][u]), fabsf(vi[t][u])));
     }
-    st4<VEC>(S + i0, sr, valid);
-    st4<VEC>(S + i1, si, valid);
+  }
+#pragma unroll
+  for (int t = 0; t < QPL; ++t) {
+    const int g = lane + 32 * t;
+    const int valid = g < G4 ? (M - 4 * g < 4 ? M - 4 * g : 4) : 0;
+    if (valid) {
+      st4<VEC>(S + r * M + 4 * g, sr[t], valid);
+      st4<VEC>(S + (R + r) * M + 4 * g, si[t], valid);
+    }
   }
 #pragma unroll
   for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -290,20 +302,33 @@ __global__ void taylor_update_kernel(const float* C, float* S, long R, int M, in
   if (lane == 0) e[r] = ex;
   const float sc = pow2f(-ex);
 #pragma unroll
-  for (int t = 0; t < kMaxQuads; ++t) {
+  for (int t = 0; t < QPL; ++t) {
     const int g = lane + 32 * t;
     if (4 * g >= ld) break;
-    float xr[4], xi[4], xn[4];
+    float xr[4], xi[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 4; ++u) {  // zeros past M (the padding up to ld)
       const bool in = 4 * g + u < M;
-      xr[u] = in ? v[0][t][u] : 0.f;
-      xi[u] = in ? v[1][t][u] : 0.f;
-      xn[u] = -xi[u];
+      xr[u] = in ? vr[t][u] : 0.f;
+      xi[u] = in ? vi[t][u] : 0.f;
     }
     put4f(q, ns, r * ld + 4 * g, xr, sc);
     put4f(q, ns, (R + r) * ld + 4 * g, xi, sc);
-    if (qn.p[0]) put4f(qn, ns, r * ld + 4 * g, xn, sc);
+  }
+}
+
+template <int QPL>
+void launch_taylor_update(const float* C, float* S, long R, int M, int k, bool slice_sum, int ns, const Q& q, long ld,
+                          int* e, cudaStream_t st) {
+  const int wpb = 8;
+  const unsigned grid = unsigned((R + wpb - 1) / wpb);
+  // four consecutive orbitals per group: 16-byte rows when M is a multiple of 4
+  if (M % 4 == 0) {
+    if (slice_sum) taylor_update_kernel<true, true, QPL><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, ns, q, ld, e);
+    else taylor_update_kernel<false, true, QPL><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, ns, q, ld, e);
+  } else {
+    if (slice_sum) taylor_update_kernel<true, false, QPL><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, ns, q, ld, e);
+    else taylor_update_kernel<false, false, QPL><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, ns, q, ld, e);
   }
 }
 
@@ -366,7 +391,8 @@ __global__ void v_exponent_kernel(const int* emax, long n, int* e) {
     e[t] = row_exponent(double(__int_as_float(emax[t])));
 }
 
-// V slices: one block per 64 x 64 tile pair of one planar row, V[w][c][i][k] and its mirror
+// V slices: one block per 64 x 64 tile pair of one planar row, V[w][c][i][k] and its mirror; the
+// imaginary row (c = 1) also as its negation, block c = 2 (sliced as -x, the same exponent)
 template <bool VEC>
 __global__ void __launch_bounds__(256) v_slice_packed_kernel(const float* Cv, int W, int M, int T, int ns, Q q,
                                                                long ld, const int* e) {
@@ -381,7 +407,8 @@ __global__ void __launch_bounds__(256) v_slice_packed_kernel(const float* Cv, in
   const int kb = ib + t;
   const int i0 = ib * kVT, k0 = kb * kVT;
   const float* src = Cv + (long)wc * ((long)M * (M + 1) / 2);
-  const long vbase = ((long)w * 2 + c) * M * ld;
+  const long vbase = ((long)w * 3 + c) * M * ld;
+  const long nbase = c == 1 ? vbase + (long)M * ld : -1;  // -Vi
   const int* ew = e + (long)w * M;
   const int tid = threadIdx.x;
   {
@@ -399,7 +426,9 @@ __global__ void __launch_bounds__(256) v_slice_packed_kernel(const float* Cv, in
       const int r = el / kVT, g = el % kVT;
       const int i = i0 + r, k = k0 + g;
       if (i >= M || k >= ld) continue;
-      put1f(q, ns, vbase + (long)i * ld + k, k >= M ? 0.f : (i <= k ? tile[r][g] : tile[g][r]), pow2f(-ew[i]));
+      const float x = k >= M ? 0.f : (i <= k ? tile[r][g] : tile[g][r]);
+      put1f(q, ns, vbase + (long)i * ld + k, x, pow2f(-ew[i]));
+      if (nbase >= 0) put1f(q, ns, nbase + (long)i * ld + k, -x, pow2f(-ew[i]));
     }
     if (ib == kb) return;
     for (int el = tid; el < kVT * kVT; el += 256) {
@@ -407,6 +436,7 @@ __global__ void __launch_bounds__(256) v_slice_packed_kernel(const float* Cv, in
       const int k = k0 + r, i = i0 + g;
       if (k >= M || i >= M) continue;
       put1f(q, ns, vbase + (long)k * ld + i, tile[g][r], pow2f(-ew[k]));
+      if (nbase >= 0) put1f(q, ns, nbase + (long)k * ld + i, -tile[g][r], pow2f(-ew[k]));
     }
     return;
   }
@@ -421,6 +451,11 @@ __global__ void __launch_bounds__(256) v_slice_packed_kernel(const float* Cv, in
     for (int u = 0; u < 4; ++u)  // the diagonal tile's lower half mirrored; zeros past M
       x[u] = k + u >= M ? 0.f : (i <= k + u ? tile[r][g + u] : tile[g + u][r]);
     put4f(q, ns, vbase + (long)i * ld + k, x, pow2f(-ew[i]));
+    if (nbase >= 0) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = -x[u];
+      put4f(q, ns, nbase + (long)i * ld + k, x, pow2f(-ew[i]));
+    }
   }
   if (ib == kb) return;
   for (int el = tid; el < kVT * kVT / 4; el += 256) {
@@ -431,15 +466,21 @@ __global__ void __launch_bounds__(256) v_slice_packed_kernel(const float* Cv, in
 #pragma unroll
     for (int u = 0; u < 4; ++u) x[u] = tile[g + u][r];
     put4f(q, ns, vbase + (long)k * ld + i, x, pow2f(-ew[k]));
+    if (nbase >= 0) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = -x[u];
+      put4f(q, ns, nbase + (long)k * ld + i, x, pow2f(-ew[k]));
+    }
   }
 }
 
 __global__ void v_slice_full_kernel(const float* Cv, int W, int M, int ns, Q q, long ld, const int* e) {
-  const long n = 2L * W * M * ld;
+  const long n = 3L * W * M * ld;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const long k = t % ld, r = t / ld;  // r = (w * 2 + c) * M + i
-    const long i = r % M, wc2 = r / M, c = wc2 % 2, w = wc2 / 2;
-    const float x = k < M ? Cv[(c * W + w) * (long)M * M + i * M + k] : 0.f;
+    const long k = t % ld, r = t / ld;  // r = (w * 3 + c) * M + i; block c = 2 is -Vi
+    const long i = r % M, wc3 = r / M, c = wc3 % 3, w = wc3 / 3;
+    const float v = k < M ? Cv[((c ? 1 : 0) * W + w) * (long)M * M + i * M + k] : 0.f;
+    const float x = c == 2 ? -v : v;
     int a, b, d;
     slice_value_f(x, pow2f(-e[w * M + i]), ns, a, b, d);
     q.p[0][t] = int8_t(a);
@@ -524,22 +565,22 @@ int islice_walkers(const cplx* SM, int W, int M, int N, int nslices, int8_t* con
 }
 
 int islice_taylor_update(const float* C, float* S, long R, int M, int k, bool slice_sum, int nslices,
-                         int8_t* const* q, int8_t* const* qn, long ld, int* e, cudaStream_t st) {
+                         int8_t* const* q, long ld, int* e, cudaStream_t st) {
   if (int rc = check_slices(nslices, q, ld)) return rc;
   if (ld < M || ld > 128L * kMaxQuads) return record_error(SFQ_ERR_SHAPE, "islice_taylor_update: M=%d", M);
   if (!C || !S) return record_error(SFQ_ERR_ARG, "islice_taylor_update: product or sum missing");
   if (k == 0 && !slice_sum) return record_error(SFQ_ERR_ARG, "islice_taylor_update: k = 0 slices the sum");
-  int8_t* none[3] = {nullptr, nullptr, nullptr};
-  const int wpb = 8;
-  const unsigned grid = unsigned((R + wpb - 1) / wpb);
-  const Q qq = qptrs(q), qnn = qptrs(qn ? qn : none);
-  // four consecutive orbitals per group: 16-byte rows when M is a multiple of 4
-  if (M % 4 == 0) {
-    if (slice_sum) taylor_update_kernel<true, true><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, nslices, qq, qnn, ld, e);
-    else taylor_update_kernel<false, true><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, nslices, qq, qnn, ld, e);
-  } else {
-    if (slice_sum) taylor_update_kernel<true, false><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, nslices, qq, qnn, ld, e);
-    else taylor_update_kernel<false, false><<<grid, 32 * wpb, 0, st>>>(C, S, R, M, k, nslices, qq, qnn, ld, e);
+  if (R <= 0) return SFQ_OK;
+  const Q qq = qptrs(q);
+  switch ((ld + 127) / 128) {  // quads per lane covering the slice row
+    case 1: launch_taylor_update<1>(C, S, R, M, k, slice_sum, nslices, qq, ld, e, st); break;
+    case 2: launch_taylor_update<2>(C, S, R, M, k, slice_sum, nslices, qq, ld, e, st); break;
+    case 3: launch_taylor_update<3>(C, S, R, M, k, slice_sum, nslices, qq, ld, e, st); break;
+    case 4: launch_taylor_update<4>(C, S, R, M, k, slice_sum, nslices, qq, ld, e, st); break;
+    case 5: launch_taylor_update<5>(C, S, R, M, k, slice_sum, nslices, qq, ld, e, st); break;
+    case 6: launch_taylor_update<6>(C, S, R, M, k, slice_sum, nslices, qq, ld, e, st); break;
+    case 7: launch_taylor_update<7>(C, S, R, M, k, slice_sum, nslices, qq, ld, e, st); break;
+    default: launch_taylor_update<8>(C, S, R, M, k, slice_sum, nslices, qq, ld, e, st); break;
   }
   SFQ_LAUNCHED();
   return SFQ_OK;
@@ -567,7 +608,7 @@ int islice_build_v(const float* Cv, int W, int M, bool packed, int nslices, int8
     else
       v_slice_packed_kernel<false><<<grid, 256, 0, st>>>(Cv, W, M, T, nslices, qptrs(q), ld, e);
   } else {
-    v_slice_full_kernel<<<grid_for(2L * W * M * ld), 256, 0, st>>>(Cv, W, M, nslices, qptrs(q), ld, e);
+    v_slice_full_kernel<<<grid_for(3L * W * M * ld), 256, 0, st>>>(Cv, W, M, nslices, qptrs(q), ld, e);
   }
   SFQ_LAUNCHED();
   return SFQ_OK;

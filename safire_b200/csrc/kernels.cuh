@@ -62,6 +62,19 @@ struct PopWork {
 };
 // the rows of A (elems per walker) copied along the population-control plan pw (after population_control)
 int copy_walker_rows(cplx* A, long elems, const PopWork& pw, int nwalk, cudaStream_t st);
+// property columns of a walker table: WEIGHT, PHASE, PSEUDO_ELOC_, E1_, EXX_, EJ_, OVLP, THETA
+constexpr int kWalkerProps = 8;
+// Walker rows of the sharded exchange: row r = [Slater matrix of walker slots[r] (elems complex),
+// its kWalkerProps property values] (props (kWalkerProps, nwalk) column-major by walker).
+// pack: rows[r] <- walker slots[r]; unpack: walker slots[r] <- rows[r]; slots are host values.
+int pack_walker_rows(const cplx* SM, const cplx* props, int nwalk, long elems, const int* slots, int n, cplx* rows,
+                     cudaStream_t st);
+int unpack_walker_rows(cplx* SM, cplx* props, int nwalk, long elems, const int* slots, int n, const cplx* rows,
+                       cudaStream_t st);
+// every weight w <- w / |w| (normalize != 0), then walker pairs[2k+1] <- walker pairs[2k] (Slater matrix
+// and properties) for k < n; pairs are host values, no destination may also be a source
+int copy_walker_pairs(cplx* SM, cplx* props, int nwalk, long elems, const int* pairs, int n, int normalize,
+                      cudaStream_t st);
 // call_dev: when set, the comb's call index is read from device memory
 int population_control(cplx* SM, long walker_elems, const WalkerProps& w, int nwalk, double r_uniform,
                        unsigned long long seed, unsigned long long call, int use_philox, const PopWork& pw,

@@ -15,8 +15,12 @@
 //    has to start at zero, because the overlap GEMM overwrites the whole region it uses;
 //  * two calls whose work overlaps on the GPU (different streams, or threads issuing at the same
 //    time) race on the array: serialise them;
-//  * the first call on each device looks up the array's device address (cudaGetSymbolAddress
-//    with that device current); make that first call before any stream capture.
+//  * the first call in each CUDA context looks up the array's device address
+//    (cudaGetSymbolAddress with that device current); make that first call before any stream
+//    capture.  The address is kept per device together with the context's unique id
+//    (cuCtxGetId), so a context created anew on the device (after cudaDeviceReset, or after
+//    the primary context was released) makes the next call look the address up again instead
+//    of writing through one from the old context.
 #include <mutex>
 
 #include "ops.cuh"
@@ -32,20 +36,53 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 std::mutex g_scratch_mu;
 void* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
 
-// Device address of g_noalloc_scratch on the current device, looked up once per device.
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points (no link to libcuda).
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+
+template <class Fn>
+Fn driver_fn(const char* name) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return reinterpret_cast<Fn>(p);
+}
+
+// Unique id of the calling thread's current context; 0 when there is none or the driver has no
+// cuCtxGetId (the address is then looked up on every call).
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    get_current = driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+    get_id = driver_fn<CtxGetIdFn>("cuCtxGetId");
+  });
+  if (!get_current || !get_id) return 0;
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+// Device address of g_noalloc_scratch in the current context, looked up once per context.
 int scratch_address(void** out) {
   int dev = 0;
   SFQ_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices)
     return record_error(SFQ_ERR_UNSUPPORTED, "no-alloc scratch: device ordinal %d out of range", dev);
   std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
+  const unsigned long long ctx = current_context_id();
+  if (!g_scratch_addr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return record_cuda(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
     if (!p) return record_error(SFQ_ERR_INTERNAL, "no-alloc scratch: null device address");
     g_scratch_addr[dev] = p;
+    g_scratch_ctx[dev] = current_context_id();  // the lookup made the primary context current
   }
   *out = g_scratch_addr[dev];
   return SFQ_OK;

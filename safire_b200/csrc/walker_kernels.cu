@@ -1,5 +1,7 @@
 // Elementwise / per-walker kernels of the propagation step: field assembly, walker update and
 // weight bound, comb population control, energy reductions, and small layout helpers.
+#include <vector>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "philox.cuh"
@@ -472,6 +474,107 @@ int copy_walker_rows(cplx* A, long elems, const PopWork& pw, int nwalk, cudaStre
   if (gx > 8) gx = 8;
   copy_rows_kernel<<<dim3(gx, nwalk - 1), 256, 0, st>>>(A, elems, pw.pairs, pw.npairs);
   SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+namespace {
+// Slot lists travel in the kernel parameters, kSlotChunk at a time (no device allocation).
+constexpr int kSlotChunk = 512;
+struct SlotChunk {
+  int v[2 * kSlotChunk];
+};
+
+// blockIdx.y: row within the chunk; DIR 0 packs walker -> row, 1 unpacks row -> walker
+template <int DIR>
+__global__ void walker_rows_kernel(cplx* SM, cplx* props, int nwalk, long elems, SlotChunk sl, int r0, cplx* rows) {
+  const int r = blockIdx.y;
+  const int w = sl.v[r];
+  cplx* wr = SM + (long)w * elems;
+  cplx* row = rows + (long)(r0 + r) * (elems + kWalkerProps);
+  for (long e = blockIdx.x * blockDim.x + threadIdx.x; e < elems; e += (long)gridDim.x * blockDim.x) {
+    if (DIR == 0) row[e] = wr[e];
+    else wr[e] = row[e];
+  }
+  if (blockIdx.x == 0 && threadIdx.x < kWalkerProps) {
+    if (DIR == 0) row[elems + threadIdx.x] = props[(long)threadIdx.x * nwalk + w];
+    else props[(long)threadIdx.x * nwalk + w] = row[elems + threadIdx.x];
+  }
+}
+
+__global__ void normalize_weights_kernel(cplx* weight, int nwalk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nwalk) return;
+  const cplx w = weight[i];
+  const double a = hypot(w.x, w.y);
+  weight[i] = mk(w.x / a, w.y / a);
+}
+
+__global__ void copy_pairs_kernel(cplx* SM, cplx* props, int nwalk, long elems, SlotChunk pr) {
+  const int src = pr.v[2 * blockIdx.y], dst = pr.v[2 * blockIdx.y + 1];
+  const cplx* s = SM + (long)src * elems;
+  cplx* d = SM + (long)dst * elems;
+  for (long e = blockIdx.x * blockDim.x + threadIdx.x; e < elems; e += (long)gridDim.x * blockDim.x) d[e] = s[e];
+  if (blockIdx.x == 0 && threadIdx.x < kWalkerProps)
+    props[(long)threadIdx.x * nwalk + dst] = props[(long)threadIdx.x * nwalk + src];
+}
+
+int row_grid_x(long elems) {
+  long gx = (elems + 255) / 256;
+  return int(gx < 1 ? 1 : (gx > 16 ? 16 : gx));
+}
+
+template <int DIR>
+int walker_rows(cplx* SM, cplx* props, int nwalk, long elems, const int* slots, int n, cplx* rows, cudaStream_t st) {
+  if (n < 0 || elems < 0) return SFQ_ERR_SHAPE;
+  for (int r0 = 0; r0 < n; r0 += kSlotChunk) {
+    const int m = n - r0 < kSlotChunk ? n - r0 : kSlotChunk;
+    SlotChunk sl;
+    for (int r = 0; r < m; ++r) {
+      if (slots[r0 + r] < 0 || slots[r0 + r] >= nwalk) return SFQ_ERR_ARG;
+      sl.v[r] = slots[r0 + r];
+    }
+    walker_rows_kernel<DIR><<<dim3(row_grid_x(elems), m), 256, 0, st>>>(SM, props, nwalk, elems, sl, r0, rows);
+    SFQ_LAUNCHED();
+  }
+  return SFQ_OK;
+}
+}  // namespace
+
+int pack_walker_rows(const cplx* SM, const cplx* props, int nwalk, long elems, const int* slots, int n, cplx* rows,
+                     cudaStream_t st) {
+  return walker_rows<0>(const_cast<cplx*>(SM), const_cast<cplx*>(props), nwalk, elems, slots, n, rows, st);
+}
+
+int unpack_walker_rows(cplx* SM, cplx* props, int nwalk, long elems, const int* slots, int n, const cplx* rows,
+                       cudaStream_t st) {
+  return walker_rows<1>(SM, props, nwalk, elems, slots, n, const_cast<cplx*>(rows), st);
+}
+
+int copy_walker_pairs(cplx* SM, cplx* props, int nwalk, long elems, const int* pairs, int n, int normalize,
+                      cudaStream_t st) {
+  if (n < 0 || elems < 0) return SFQ_ERR_SHAPE;
+  std::vector<char> is_dst(size_t(nwalk > 0 ? nwalk : 0), 0);
+  for (int k = 0; k < n; ++k) {
+    const int s = pairs[2 * k], d = pairs[2 * k + 1];
+    if (s < 0 || s >= nwalk || d < 0 || d >= nwalk || s == d || is_dst[d]) return SFQ_ERR_ARG;
+    is_dst[d] = 1;
+  }
+  for (int k = 0; k < n; ++k)
+    if (is_dst[pairs[2 * k]]) return SFQ_ERR_ARG;  // a source overwritten by another copy
+  if (normalize && nwalk > 0) {
+    normalize_weights_kernel<<<(nwalk + 255) / 256, 256, 0, st>>>(props, nwalk);  // WEIGHT is column 0
+    SFQ_LAUNCHED();
+  }
+  for (int k0 = 0; k0 < n; k0 += kSlotChunk) {
+    const int m = n - k0 < kSlotChunk ? n - k0 : kSlotChunk;
+    SlotChunk pr;
+    for (int k = 0; k < m; ++k) {
+      pr.v[2 * k] = pairs[2 * (k0 + k)];
+      pr.v[2 * k + 1] = pairs[2 * (k0 + k) + 1];
+    }
+    copy_pairs_kernel<<<dim3(row_grid_x(elems), m), 256, 0, st>>>(SM, props, nwalk, elems, pr);
+    SFQ_LAUNCHED();
+  }
   return SFQ_OK;
 }
 

@@ -18,6 +18,13 @@ sfq_plan_walker_exchange, sfq_walker_moves), which needs no device; the data mov
 torch.distributed.  Within one rank the copies fill the slots of walkers that leave, in the order
 swap_walkers_async fills them (population_control.hpp:143-209), so one rank reproduces the
 single-rank comb exactly.
+
+engine_population_control runs the same steps on an engine's resident walker table without taking
+it off the device: only the |w| column (8 bytes per walker) goes to the host for the gather and the
+comb; the walkers that leave are packed on the device into rows (sfq_engine_pack_walkers), the rows
+cross ranks as device tensors (NCCL send/recv; through the host under gloo), arrive in a device
+buffer and are scattered into the free slots (sfq_engine_unpack_walkers), and the local copies and
+the weight normalisation run as one device call (sfq_engine_copy_walkers).
 """
 import numpy as np
 
@@ -96,14 +103,13 @@ def comm_device(dist, group=None):
     return torch.device("cpu")
 
 
-def population_control(dist, SM, props, r, group=None):
-    """The collective population control on this rank's walker table (SM (nw, rows, cols) complex,
-    props (8, nw) complex); r is the root's comb uniform (ignored elsewhere).  Returns the new table:
-    walkers copied and exchanged along the plan, weights w / |w|.  With dist None: one rank."""
+def global_offspring(dist, w, r, group=None):
+    """The collective part of population_control (population_control.hpp:219-236): the ranks' walker
+    counts and |w| are gathered, the root combs the whole population with its uniform r, and every
+    rank receives the offspring.  w: this rank's |w| (host).  Returns (offspring, counts, rank)."""
     import torch
-    SM = np.array(SM, dtype=np.complex128)
-    props = np.array(props, dtype=np.complex128)
-    nw = SM.shape[0]
+    w = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+    nw = w.size
     rank = dist.get_rank(group) if dist else 0
     size = dist.get_world_size(group) if dist else 1
     dev = comm_device(dist, group)
@@ -111,10 +117,6 @@ def population_control(dist, SM, props, r, group=None):
         cnt = [torch.zeros(1, dtype=torch.int64, device=dev) for _ in range(size)]
         dist.all_gather(cnt, torch.tensor([nw], dtype=torch.int64, device=dev), group=group)
         counts = [int(c.item()) for c in cnt]
-    else:
-        counts = [nw]
-    w = np.abs(props[WEIGHT])
-    if dist:
         mx = max(counts)
         buf = torch.zeros(mx, dtype=torch.float64)
         buf[:nw] = torch.from_numpy(w)
@@ -122,6 +124,7 @@ def population_control(dist, SM, props, r, group=None):
         dist.all_gather(allw, buf.to(dev), group=group)
         weights = np.concatenate([a.cpu().numpy()[:c] for a, c in zip(allw, counts)])
     else:
+        counts = [nw]
         weights = w
     off = torch.zeros(sum(counts), dtype=torch.int64)
     if rank == 0:
@@ -129,7 +132,19 @@ def population_control(dist, SM, props, r, group=None):
     if dist:
         off = off.to(dev)
         dist.broadcast(off, 0, group=group)
-    offspring = off.cpu().numpy()
+    return off.cpu().numpy(), counts, rank
+
+
+def population_control(dist, SM, props, r, group=None):
+    """The collective population control on this rank's walker table (SM (nw, rows, cols) complex,
+    props (8, nw) complex, host arrays); r is the root's comb uniform (ignored elsewhere).  Returns
+    the new table: walkers copied and exchanged along the plan, weights w / |w|.  With dist None:
+    one rank."""
+    import torch
+    SM = np.array(SM, dtype=np.complex128)
+    props = np.array(props, dtype=np.complex128)
+    dev = comm_device(dist, group)
+    offspring, counts, rank = global_offspring(dist, np.abs(props[WEIGHT]), r, group)
     sends, recvs, copies = local_moves(offspring, counts, rank)
     sm_elems = int(np.prod(SM.shape[1:]))  # a rank may hold no walkers
     row = lambda i: torch.from_numpy(np.concatenate([SM[i].reshape(-1), props[:, i]]).view(np.float64)).to(dev)
@@ -151,8 +166,14 @@ def population_control(dist, SM, props, r, group=None):
 
 
 def engine_population_control(dist, engine, r, group=None):
-    """population_control for an AfqmcEngine whose walkers are this rank's share of the population:
-    the engine's walker table goes through the collective comb and exchange and back (set_walkers).
+    """population_control for an engine whose walkers are this rank's share of the population, with
+    the walker table kept on the engine's device.
+
+    Engine interface: properties() (the property columns, host), and the row calls of the walker
+    exchange -- exchange_device (where its rows live), walker_row_elems(), pack_walkers(slots, rows),
+    unpack_walkers(slots, rows), copy_walkers(pairs, normalize) -- as AfqmcEngine has them over
+    sfq_engine_pack_walkers / unpack_walkers / copy_walkers.  Rows are float64 tensors (n, 2 *
+    walker_row_elems()) on exchange_device: a walker's Slater matrix then its 8 property values.
 
     Only the Slater matrices and the property columns travel.  An engine that keeps back-propagation
     history (enable_back_propagation) also holds per-walker field rings, weight factors and anchored
@@ -162,7 +183,31 @@ def engine_population_control(dist, engine, r, group=None):
     if getattr(engine, "nbp", 0) > 0:
         raise capi.SafireError(3, "sharded population control does not move back-propagation history; "
                                   "run back propagation on one rank (engine.population_control)")
-    SM, pr = engine.walkers()
-    props = np.stack([pr[k] for k in capi.PROPS])
-    SM, props = population_control(dist, SM, props, r, group)
-    engine.set_walkers(SM, {k: props[i] for i, k in enumerate(capi.PROPS)})
+    import torch
+    pr = engine.properties()
+    offspring, counts, rank = global_offspring(dist, np.abs(np.asarray(pr["WEIGHT"])), r, group)
+    sends, recvs, copies = local_moves(offspring, counts, rank)
+    edev = engine.exchange_device
+    cdev = comm_device(dist, group)
+    width = 2 * int(engine.walker_row_elems())
+    # a rank either sends or receives; both ends post in plan order (MPI's non-overtaking rule there)
+    if sends:
+        rows = torch.empty((len(sends), width), dtype=torch.float64, device=edev)
+        engine.pack_walkers([w for w, _ in sends], rows)
+        for i, (_, dst) in enumerate(sends):
+            dist.send(rows[i] if cdev == edev else rows[i].to(cdev), dst, group=group)
+    if recvs:
+        rows = torch.empty((len(recvs), width), dtype=torch.float64, device=edev)
+        for i, (_, src) in enumerate(recvs):
+            if cdev == edev:
+                dist.recv(rows[i], src, group=group)
+            else:
+                t = torch.empty(width, dtype=torch.float64, device=cdev)
+                dist.recv(t, src, group=group)
+                rows[i].copy_(t)
+        if edev.type == "cuda":
+            torch.cuda.current_stream(edev).synchronize()  # the receives land before the engine stream reads
+        engine.unpack_walkers([slot for slot, _ in recvs], rows)
+    if sends and edev.type == "cuda":
+        torch.cuda.current_stream(edev).synchronize()  # the sends have read their rows
+    engine.copy_walkers(copies, normalize=True)

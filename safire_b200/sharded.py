@@ -9,8 +9,9 @@ rank-local calls; what crosses ranks is what the reference reduces or exchanges 
   * the energy estimator's MeasurementOutput (Measurements.hpp:96-130): every observable's weighted
     sum all-reduced and divided by the all-reduced total weight.
 
-The engine interface used: walkers(), set_walkers(), propagate / propagate_host, orthogonalize(),
-measure() (AfqmcEngine's), and dt.
+The engine interface used: properties(), propagate / propagate_host, orthogonalize(), measure(),
+dt, and the row calls of the walker exchange (exchange_device, walker_row_elems(), pack_walkers(),
+unpack_walkers(), copy_walkers()) -- AfqmcEngine's, which keep the walker table on the device.
 """
 import math
 
@@ -32,7 +33,7 @@ def _allreduce(dist, values, group=None):
 
 def global_pseudo_energy(dist, engine, group=None):
     """averagePseudoEnergy over the ranks: log(Re(sum w e^{dt eloc} / sum w)) / dt."""
-    _, pr = engine.walkers()
+    pr = engine.properties()
     w, el = pr["WEIGHT"], pr["PSEUDO_ELOC_"]
     s = _allreduce(dist, [np.sum(w * np.exp(engine.dt * el)), np.sum(w)], group)
     return math.log((s[0] / s[1]).real) / engine.dt

@@ -88,9 +88,9 @@ def cplx_b(A, V, ns):
     for w in range(W):
         ea = row_exponent(np.maximum(np.max(np.abs(Ar[w]), axis=1), np.max(np.abs(Ai[w]), axis=1)))
         ev = row_exponent(np.maximum(np.max(np.abs(Vr[w]), axis=1), np.max(np.abs(Vi[w]), axis=1)))
-        qre, qim, qnim = slices_at(Ar[w], ea, ns), slices_at(Ai[w], ea, ns), slices_at(-Ai[w], ea, ns)
-        qvr, qvi = slices_at(Vr[w], ev, ns), slices_at(Vi[w], ev, ns)
-        gre = groups_of(qre, qvr, ns) + groups_of(qnim, qvi, ns)
+        qre, qim = slices_at(Ar[w], ea, ns), slices_at(Ai[w], ea, ns)
+        qvr, qvi, qnvi = slices_at(Vr[w], ev, ns), slices_at(Vi[w], ev, ns), slices_at(-Vi[w], ev, ns)
+        gre = groups_of(qre, qvr, ns) + groups_of(qim, qnvi, ns)
         gim = groups_of(qre, qvi, ns) + groups_of(qim, qvr, ns)
         out[0, w] = combine(gre, ea, ev)
         out[1, w] = combine(gim, ea, ev)

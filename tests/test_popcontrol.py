@@ -166,6 +166,8 @@ def test_engine_with_back_propagation_is_refused():
         def walkers(self):
             raise AssertionError("the walkers must not be read")
 
+        properties = walkers
+
     with pytest.raises(capi.SafireError) as ei:
         P.engine_population_control(None, FakeEngine(), 0.5)
     assert ei.value.code == 3

@@ -10,6 +10,7 @@ import socket
 
 import numpy as np
 import pytest
+import torch
 import torch.multiprocessing as mp
 
 from oracle import afqmc_oracle as O
@@ -40,6 +41,36 @@ class OracleEngine:
         self.w.SM = np.array(SM)
         for k, f in FIELDS.items():
             setattr(self.w, f, np.array(props[k]))
+
+    def properties(self):
+        return {k: getattr(self.w, f).copy() for k, f in FIELDS.items()}
+
+    # the walker-exchange rows, on the host: Slater matrix then the 8 properties
+    exchange_device = torch.device("cpu")
+
+    def walker_row_elems(self):
+        return self.w.SM[0].size + len(FIELDS)
+
+    def pack_walkers(self, slots, rows):
+        v = rows.numpy().view(np.complex128)
+        for r, i in enumerate(slots):
+            v[r] = np.concatenate([self.w.SM[i].ravel(), [getattr(self.w, f)[i] for f in FIELDS.values()]])
+
+    def unpack_walkers(self, slots, rows):
+        v = rows.numpy().view(np.complex128)
+        n = self.w.SM[0].size
+        for r, i in enumerate(slots):
+            self.w.SM[i] = v[r, :n].reshape(self.w.SM.shape[1:])
+            for j, f in enumerate(FIELDS.values()):
+                getattr(self.w, f)[i] = v[r, n + j]
+
+    def copy_walkers(self, pairs, normalize=True):
+        if normalize:
+            self.w.weight = self.w.weight / np.abs(self.w.weight)
+        for src, dst in pairs:
+            self.w.SM[dst] = self.w.SM[src]
+            for f in FIELDS.values():
+                getattr(self.w, f)[dst] = getattr(self.w, f)[src]
 
     def propagate_host(self, Eshift, step, uniforms_host):
         self.prop.propagate(self.w, Eshift, step, target_population=self.target, uniforms=uniforms_host)
