@@ -45,7 +45,7 @@ ORTHO_EVERY = 5
 POP_EVERY = 20
 # DRAM bytes (read + write) of one Taylor-term int8 product at 256 walkers, M = 400, N = 100, from an
 # ncu capture of the same kernel and tile (profiles/islice_taylor_M400_N100_W256_full.md)
-TAYLOR_DRAM_BYTES_256 = 339.224064e6 + 62.147584e6
+TAYLOR_DRAM_BYTES_256 = 432.294656e6 + 67.308544e6
 EQUIL_STEPS = 100  # run_afqmc relaxes Eshift every step for the first equilibration_steps
 RELAX = 1.0 - math.exp(-10.0 / EQUIL_STEPS)
 
@@ -499,7 +499,8 @@ def main():
         traffic = TAYLOR_DRAM_BYTES_256 * W / 256.0
         roofline.update({"traffic_unit": "bytes per launch",
                          "traffic_source": "ncu capture of the same product (256 walkers), scaled by walkers",
-                         "algorithmic_bytes_per_launch": W * (3.0 * 2 * spec.M * spec.M + 3.0 * 3 * spec.N * spec.M
+                         # V slices [Vr; Vi; -Vi] (3 x 3 M^2 bytes), A slices (3 x 2 N M), C in FP32 (8 N M)
+                         "algorithmic_bytes_per_launch": W * (3.0 * 3 * spec.M * spec.M + 3.0 * 2 * spec.N * spec.M
                                                               + 4.0 * 2 * spec.N * spec.M)})
     roofline.update({"algorithmic_flops_per_launch": alg, "launch_ms": launch_ms, "launches_timed": t_n,
                      "traffic": traffic,

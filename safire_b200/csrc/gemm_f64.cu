@@ -28,9 +28,10 @@ template <bool AC, bool BC, bool CONJA, bool AK, bool BK>
 int pick_tile(const GemmDesc& d, cudaStream_t st) {
   if constexpr (AC || BC) {
     if (d.N <= 32) return launch<AC, BC, CONJA, AK, BK, 128, 32, 4, 1, 3>(d, st);
-    // per-walker products (overlaps, CholeskyQR, propagation): 8 warps per 64 x 64 tile hide
-    // more of the DMMA latency on their short K loops (measured 4-6 % faster at N = 100)
-    if (d.batch > 1 && d.N <= 128) return launch<AC, BC, CONJA, AK, BK, 64, 64, 4, 2, 3>(d, st);
+    // per-walker products (overlaps, CholeskyQR, propagation, the Green's function): 8 warps per
+    // 64 x 64 tile hide more of the DMMA latency on their short K loops (measured 4-6 % faster at
+    // N = 100)
+    if (d.batch > 1 && (d.N <= 128 || d.K <= 128)) return launch<AC, BC, CONJA, AK, BK, 64, 64, 4, 2, 3>(d, st);
     return launch<AC, BC, CONJA, AK, BK, 64, 64, 2, 2, 3>(d, st);
   } else {
     return launch<AC, BC, CONJA, AK, BK, 128, 64, 4, 2, 3>(d, st);

@@ -22,6 +22,7 @@ def _flops(op, M, N, Nc, W):
         "vbias": 8.0 * N * M * Nc * W,
         "propagate": 64.0 * M * M * N * W,
         "density": (8.0 * N * N * M + 8.0 * N * N * M + 8.0 * N ** 3) * W,
+        "inverse": 8.0 * N ** 3 * W,
         "energy": 8.0 * N * N * M * Nc * W,
         "orthogonalize": 2 * (8.0 * N * N * M * 2) * W,
         "umma_vhs": 2.0 * (2 * W) * M * M * Nc,   # one real product of the split GEMM
@@ -83,6 +84,10 @@ def run(op, M, N, Nc, W, reps, warm=2, real_lnak=True):
         A = torch.randn(N, M, generator=g, device="cuda", dtype=torch.float64)
         B = crand(W, M, N)
         fn = lambda: afqmc.MixedDensityMatrix(A, B)  # noqa: E731
+    elif op == "inverse":
+        # the per-walker overlap matrices' inverse and log det (Gauss-Jordan), N x N
+        A = crand(W, N, N) + 4.0 * torch.eye(N, dtype=torch.complex128, device="cuda")
+        fn = lambda: afqmc.inverse_logdet(A)  # noqa: E731
     elif op == "energy":
         G = crand(W, N, M) * 0.01
         haj = crand(N, M)
