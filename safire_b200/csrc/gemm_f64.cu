@@ -28,6 +28,19 @@ template <bool AC, bool BC, bool CONJA, bool AK, bool BK>
 int pick_tile(const GemmDesc& d, cudaStream_t st) {
   if constexpr (AC || BC) {
     if (d.N <= 32) return launch<AC, BC, CONJA, AK, BK, 128, 32, 4, 1, 3>(d, st);
+    // per-walker products with 65-112 rows, a short K and many columns (the Green's function at
+    // N = 100: 100 x 400 per walker, K = 100): one tile row of 104 or 112 pads 100 rows 1.04x or
+    // 1.12x instead of the 1.28x of two 64-row tiles, 80 columns divide 400; one 8 x 40 warp
+    // tile per warp.  At N = 100, 256 walkers: 386 us against 463 us with 64 x 64 tiles (same bits)
+    if (d.batch > 1 && d.M > 64 && d.M <= 104 && d.N >= 160 && d.K <= 128)
+      return launch<AC, BC, CONJA, AK, BK, 104, 80, 13, 2, 3>(d, st);
+    if (d.batch > 1 && d.M > 64 && d.M <= 112 && d.N >= 160 && d.K <= 128)
+      return launch<AC, BC, CONJA, AK, BK, 112, 80, 14, 2, 2>(d, st);
+    // per-walker 65-112 square products of a real A over a long K (the overlap PsiT W with a real
+    // trial at N = 100, K = 400): 56 x 56 tiles of 7 warps, four stages.  232 us against 256 us
+    // with 64 x 64 tiles; with a complex A (W^H W) they were slower
+    if (!AC && d.batch > 1 && d.M > 64 && d.M <= 112 && d.N > 64 && d.N <= 112 && d.K >= 256)
+      return launch<AC, BC, CONJA, AK, BK, 56, 56, 7, 1, 4>(d, st);
     // per-walker products (overlaps, CholeskyQR, propagation, the Green's function): 8 warps per
     // 64 x 64 tile hide more of the DMMA latency on their short K loops (measured 4-6 % faster at
     // N = 100)
