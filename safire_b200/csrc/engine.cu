@@ -811,6 +811,7 @@ struct Engine {
           for (int i = 0; i < M; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * M + i]);
         SFQ_CUDA_TRY(cudaMemcpyAsync(SM2, psi.data(), sizeof(cplx) * M * N, cudaMemcpyHostToDevice, st));
         if ((rc = ops::overlap_matrix(PsiT, true, SM2, T, 1, M, N, st))) return rc;
+        if (collinear && (rc = ops::mask_cross_spin(T, 1, N, spin_split(), st))) return rc;
         if ((rc = lu_logdet(T, (long)N * N, 1, N, ovtmp, false, 1.0, true, st))) return rc;
         if ((rc = ops::green_compact(T, SM2, G, 1, M, N, st))) return rc;
         SFQ_CUDA_TRY(cudaMemcpyAsync(GT_c, G, sizeof(cplx) * NM, cudaMemcpyDeviceToDevice, st));
@@ -1694,7 +1695,7 @@ struct Engine {
       d.C = Cvb; d.ldc = Nc;
       if ((rc = islice_gemm(d, st))) return rc;
     }
-    if ((rc = mixed_reduce_planar_to_cplx(Cvb, i8_vb_ks, part, W, Nc, 2.0 * sdt, X, st, vbT))) return rc;
+    if ((rc = mixed_reduce_planar_to_cplx(Cvb, i8_vb_ks, part, W, Nc, vb_scale(), X, st, vbT))) return rc;
     ph_end(SFQ_PH_VBIAS);
     ph_begin(SFQ_PH_FIELDS);
     FieldParams fp;
@@ -1763,7 +1764,7 @@ struct Engine {
     int rc;
     ph_begin(SFQ_PH_ENERGY);
     if ((rc = density(ovtmp))) return rc;
-    const double scl = 2.0;
+    const double scl = closed() ? 2.0 : 1.0;  // CLOSED counts each orbital twice
     if ((rc = energy_e1(G, haj, E3, W, N, M, p.E0, scl, 1, st))) return rc;
     const long R = (long)W * N;
     if ((rc = islice_rows_planar(G, R, M, nslices, Ge_q, ld_m, Ge_e, st))) return rc;
@@ -1784,7 +1785,7 @@ struct Engine {
       d.bn = i8_bn;
       d.C = Tf; d.ldc = ldc;
       if ((rc = islice_gemm(d, st))) return rc;
-      if ((rc = energy_exx_reduce_f32(Tf, W, N, nv, n0, Nc, ldc, exxn, kl, st))) return rc;
+      if ((rc = energy_exx_reduce_f32(Tf, W, N, nv, n0, Nc, ldc, exxn, kl, st, spin_split()))) return rc;
     }
     if ((rc = energy_finish(exxn, kl, E3, W, Nc, scl, 1, 1, st))) return rc;
     ph_end(SFQ_PH_ENERGY);
@@ -2449,10 +2450,11 @@ int sfq_engine_create_nomsd(sfq_engine_t* out, const sfq_engine_params_t* p, con
     delete h;
     return record_error(SFQ_ERR_ARG, "engine: unknown precision %d", p->precision);
   }
-  if (e.mixed && (coll || npol > 1 || ndet > 1)) {
+  if (e.mixed && ((coll && !e.nslices) || npol > 1 || ndet > 1)) {
     delete h;
     return record_error(SFQ_ERR_UNSUPPORTED,
-                        "engine: COLLINEAR and NONCOLLINEAR walkers and multi-determinant trials run in FP64");
+                        "engine: NONCOLLINEAR walkers and multi-determinant trials run in FP64, COLLINEAR walkers in "
+                        "FP64 or the int8-slice precisions");
   }
   if (e.nslices && (!e.trial_real || e.M > 1024)) {
     delete h;

@@ -91,7 +91,7 @@ int energy_exx_reduce(const cplx* T, int nwalk, int nel, int nv, int n0, int nch
                       cudaStream_t st, int nup = -1);
 // the same from FP32 planar T of the split-BF16 product: rows (c*W + w)*nel + a, columns n*nel + b
 int energy_exx_reduce_f32(const float* C, int nwalk, int nel, int nv, int n0, int nchol, long ldc, cplx* exxn,
-                          cplx* kl, cudaStream_t st);
+                          cplx* kl, cudaStream_t st, int nup = -1);
 // E3[:,1] += -0.5*scl*sum_n exxn; E3[:,2] += (CLOSED ? 2 : 0.5) * sum_n kl^2
 int energy_finish(const cplx* exxn, const cplx* kl, cplx* E3, int nwalk, int nchol, double scl, int addEXX,
                   int addEJ, cudaStream_t st);

@@ -313,8 +313,9 @@ __global__ void __launch_bounds__(RT) energy_exx_kernel(const cplx* T, int nel, 
 
 // the same from the split-BF16 product: T planar in FP32, T[a][n][b] = (C[w*nel + a][n*nel + b],
 // C[(W + w)*nel + a][n*nel + b]), sums in FP64
+// nup < nel: COLLINEAR walkers, the exchange pairs orbitals of one spin only (as energy_exx_kernel)
 __global__ void __launch_bounds__(RT) energy_exx_f32_kernel(const float* C, int W, int nel, int nv, int n0, int nchol,
-                                                            long ldc, cplx* exxn, cplx* kl) {
+                                                            long ldc, cplx* exxn, cplx* kl, int nup) {
   __shared__ cplx red[RT / 32];
   const int n = blockIdx.x, w = blockIdx.y;
   const float* Cr = C + (long)w * nel * ldc + (long)n * nel;
@@ -324,9 +325,10 @@ __global__ void __launch_bounds__(RT) energy_exx_f32_kernel(const float* C, int 
   for (int e = threadIdx.x; e < nn; e += RT) {
     const int a = e / nel, b = e % nel;
     const cplx tab = mk(Cr[(long)a * ldc + b], Ci[(long)a * ldc + b]);
+    if (a == b) tr = cadd(tr, tab);
+    if ((a < nup) != (b < nup)) continue;
     const cplx tba = mk(Cr[(long)b * ldc + a], Ci[(long)b * ldc + a]);
     acc = cadd(acc, cmul(tab, tba));
-    if (a == b) tr = cadd(tr, tab);
   }
   cplx s = block_sum<RT>(acc, red);
   cplx t = block_sum<RT>(tr, red);
@@ -619,10 +621,10 @@ int energy_exx_reduce(const cplx* T, int nwalk, int nel, int nv, int n0, int nch
 }
 
 int energy_exx_reduce_f32(const float* C, int nwalk, int nel, int nv, int n0, int nchol, long ldc, cplx* exxn,
-                          cplx* kl, cudaStream_t st) {
+                          cplx* kl, cudaStream_t st, int nup) {
   if (nwalk <= 0 || nv <= 0) return SFQ_OK;
   dim3 grid(nv, nwalk);
-  energy_exx_f32_kernel<<<grid, RT, 0, st>>>(C, nwalk, nel, nv, n0, nchol, ldc, exxn, kl);
+  energy_exx_f32_kernel<<<grid, RT, 0, st>>>(C, nwalk, nel, nv, n0, nchol, ldc, exxn, kl, nup < 0 ? nel : nup);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }

@@ -5,7 +5,8 @@ walkers) -- dense Cholesky, 96 ranks x 16 walkers, 48000 steps of 0.01, 3000 of 
 with a relaxing Eshift, population control, orthogonalization and a measurement every 10 steps --
 recorded the mean and error of each energy.  The engine runs the same schedule on one GPU for the same
 1536 walkers, with its own Philox fields and comb, as device-resident blocks; its means must agree
-with the recorded ones under the reference's own statistical comparison.
+with the recorded ones under the reference's own statistical comparison -- in FP64, and with the
+int8-slice products (INT8X3) on both fixtures.
 """
 import numpy as np
 import pytest
@@ -20,11 +21,12 @@ pytestmark = pytest.mark.gpu
 KEYS = ("Energy", "OnebodyEnergy", "ExchangeEnergy", "CoulombEnergy")
 
 
+@pytest.mark.parametrize("prec", [capi.PRECISION_FP64, capi.PRECISION_INT8X3], ids=["fp64", "int8x3"])
 @pytest.mark.parametrize("case", ["bh_rhf_closed", "li_rohf_collinear"])
-def test_engine_agrees_with_reference_statistics(case):
+def test_engine_agrees_with_reference_statistics(case, prec):
     snap, stat = snapshot(case), bh_statistical(case)
     assert snap["settings"]["walker_type"] == stat["walker_type"]
-    eng = A.AfqmcEngine(engine_system(snap), stat["nwalk"], dt=stat["dt"], seed=2024, precision=capi.PRECISION_FP64)
+    eng = A.AfqmcEngine(engine_system(snap), stat["nwalk"], dt=stat["dt"], seed=2024, precision=prec)
     Eshift = eng.init()
     block = 50 * stat["measure_interval"]  # 50 measurements per device-resident block
     assert stat["steps"] % block == 0
@@ -44,6 +46,6 @@ def test_engine_agrees_with_reference_statistics(case):
         mean, err = O.rebinned_average(series, 50)  # bins of 500 steps, longer than the correlation time
         ok, d, tol = statistically_equal(mean, err, *stat["recorded"][k])
         rm, re_ = stat["recorded"][k]
-        print(f"{case} {k}: {mean.real:.6f} +- {abs(err):.6f} vs recorded {rm.real:.6f} +- {abs(re_):.6f}, "
+        print(f"{case} {prec} {k}: {mean.real:.6f} +- {abs(err):.6f} vs recorded {rm.real:.6f} +- {abs(re_):.6f}, "
               f"|d| = {d:.2e} <= {tol:.2e}")
         assert ok, (k, mean, err, stat["recorded"][k], d, tol)
