@@ -268,7 +268,7 @@ typedef struct {
  * biases every product by the same relative shrink; these carry no such bias.  The force bias, the
  * fields, vHS, the P1 products and Taylor terms, and the exchange tensor of the energy run this way;
  * the Green's function, LU / log det, overlaps, orthogonalization, walker update and all sums stay
- * FP64.  Needs a real trial; any nmo and nchol. */
+ * FP64.  Needs a real trial and nmo <= 1024; any nchol; CLOSED or COLLINEAR walkers. */
 #define SFQ_PRECISION_INT8X3 3     /* 3 slices: 2^-24 of each row's largest entry, 6 int8 products */
 #define SFQ_PRECISION_INT8X2 4     /* 2 slices: 2^-16 of each row's largest entry, 3 int8 products */
 
