@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 10 */
+int sfq_abi_version(void); /* 11 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -325,6 +325,24 @@ int sfq_engine_population_control(sfq_engine_t e, unsigned long long call);
  * folded diagonal two-body RDM, nmo (2 nmo - 1) complex values (CLOSED: nmo (2 nmo - 1) - nmo (nmo - 1) / 2).
  * Both divided by the total weight, as recorded per measurement; host pointers, either may be NULL. */
 int sfq_engine_measure_rdm(sfq_engine_t e, void* one_rdm, void* diag_two_rdm);
+
+/* The other observables of MixedEstimator (sfq_engine_measure_observables) and BackPropEstimator
+ * (sfq_engine_measure_bp_observables, the arguments of sfq_engine_measure_bp_rdm), FP64 engines with a
+ * single-determinant trial, divided by the total weight as the RDMs are; host pointers, NULL skips:
+ *  - two_rdm: TwoRDM (Observables/twordm.hpp:29-77), (nspin + 1, nmo, nmo, nmo, nmo) complex as
+ *    [block][i][k][j][l] = sum_w c_w (G_ik G_jl - G_il G_jk) within a spin, G_ik G_jl across, blocks
+ *    (a,a,a,a), (a,a,b,b), (b,b,b,b) (CLOSED: the first two); CLOSED and COLLINEAR walkers, nmo^4 * 16
+ *    bytes per block at most 1 GiB;
+ *  - spin_corr: SpinCorr (Observables/spincorr.hpp:25-136), (2, nmo (nmo + 1) / 2) complex, the XY
+ *    then the Z channel of <S_i . S_j> over i <= j, i-major; every walker type;
+ *  - pair_corr: PairCorr (Observables/paircorr.hpp:31-152), (npair, npair, nmo, nmo) complex for the
+ *    orbital pair maps pair_maps (npair, nmo) int (a negative partner leaves the orbital out);
+ *    COLLINEAR (j > i) and NONCOLLINEAR (every j) walkers. */
+int sfq_engine_measure_observables(sfq_engine_t e, void* two_rdm, void* spin_corr, int npair, const int* pair_maps,
+                                   void* pair_corr);
+int sfq_engine_measure_bp_observables(sfq_engine_t e, int nsteps, int ortho_interval, int path_restoration,
+                                      void* two_rdm, void* spin_corr, int npair, const int* pair_maps,
+                                      void* pair_corr);
 
 /* Back propagation (BackPropEstimator.hpp, AFQMCBasePropagator.cpp:404-526), FP64 engines.
  * enable: every later step keeps, per walker, its fields in a ring of nbp slots and its weight factor

@@ -1156,6 +1156,90 @@ def _rdm_reduce(parts, coeffs, w, wt, M):
     return one, np.array(out, np.complex128)
 
 
+def _observables_reduce(parts, coeffs, w, wt, M, two_rdm=True, spin_corr=True, pair_maps=None):
+    """TwoRDM, SpinCorr and PairCorr (Observables/twordm.hpp:41-77, spincorr.hpp:36-136,
+    paircorr.hpp:62-152) from per-reference full G's (W, nspin, R, R) and walker coefficients,
+    divided by sum_w w.  TwoRDM: [block][i][k][j][l], blocks (a,a,a,a), (a,a,b,b), (b,b,b,b) (CLOSED:
+    two); SpinCorr: (2, M(M+1)/2), the XY then the Z channel over i <= j; PairCorr: (npair, npair, M,
+    M) for the maps (npair, M)."""
+    out = {}
+    den = np.sum(w)
+    nspin = parts[0].shape[1]
+    if two_rdm and wt != "NONCOLLINEAR":  # twordm.hpp:34-36
+        avg = np.zeros((nspin + 1, M, M, M, M), np.complex128)
+        for G, c in zip(parts, coeffs):
+            XwG = (w * c)[:, None, None, None] * G
+            for sp in range(nspin):
+                avg[2 * sp] += np.einsum('wik,wjl->ikjl', XwG[:, sp], G[:, sp])
+                avg[2 * sp] -= np.einsum('wil,wjk->ikjl', XwG[:, sp], G[:, sp])
+            avg[1] += np.einsum('wik,wjl->ikjl', XwG[:, 0], G[:, nspin - 1])
+        out["TwoRDM"] = avg / den
+    if spin_corr:  # spincorr.hpp:58-124, term by term
+        avg = np.zeros((2, M * (M + 1) // 2), np.complex128)
+        for G, c in zip(parts, coeffs):
+            Xw = w * c
+            idx = 0
+            for i in range(M):
+                for j in range(i, M):
+                    if wt in ("CLOSED", "COLLINEAR"):
+                        Gu = G[:, 0]
+                        Gd = G[:, 1] if wt == "COLLINEAR" else G[:, 0]
+                        if j == i:
+                            z = Gu[:, i, i] * (1.0 - Gd[:, j, j]) + Gd[:, i, i] * (1.0 - Gu[:, j, j])
+                            xy = Gu[:, i, j] * (1.0 - Gd[:, j, i]) + Gd[:, i, j] * (1.0 - Gu[:, j, i])
+                        else:
+                            z = (Gu[:, i, i] * (Gu[:, j, j] - Gd[:, j, j]) + Gd[:, i, i] * (Gd[:, j, j] - Gu[:, j, j])
+                                 - Gu[:, i, j] * Gu[:, j, i] - Gd[:, i, j] * Gd[:, j, i])
+                            xy = Gu[:, i, j] * (-Gd[:, j, i]) + Gd[:, i, j] * (-Gu[:, j, i])
+                    else:
+                        g = G[:, 0]
+                        I, J = i + M, j + M
+                        if j == i:
+                            z = (g[:, i, i] * (1.0 - g[:, J, J]) + g[:, I, I] * (1.0 - g[:, j, j])
+                                 - g[:, i, J] * (-g[:, J, i]) - g[:, I, j] * (-g[:, j, I]))
+                            xy = (g[:, i, j] * (1.0 - g[:, J, I]) + g[:, I, J] * (1.0 - g[:, j, i])
+                                  + g[:, J, j] * g[:, i, I] + g[:, j, J] * g[:, I, i])
+                        else:
+                            z = (g[:, i, i] * (g[:, j, j] - g[:, J, J]) + g[:, I, I] * (g[:, J, J] - g[:, j, j])
+                                 - g[:, i, j] * g[:, j, i] - g[:, I, J] * g[:, J, I]
+                                 - g[:, i, J] * (-g[:, J, i]) - g[:, I, j] * (-g[:, j, I]))
+                            xy = (g[:, i, j] * (-g[:, J, I]) + g[:, I, J] * -g[:, j, i]
+                                  + g[:, J, j] * g[:, i, I] + g[:, j, J] * g[:, I, i])
+                    avg[1, idx] += np.sum(Xw / 4.0 * z)
+                    avg[0, idx] += np.sum(Xw / 2.0 * xy)
+                    idx += 1
+        out["SpinCorr"] = avg / den
+    if pair_maps is not None and wt != "CLOSED":  # paircorr.hpp:37-40, 80-135
+        maps = np.asarray(pair_maps, dtype=np.int64)
+        n = maps.shape[0]
+        avg = np.zeros((n, n, M, M), np.complex128)
+        for G, c in zip(parts, coeffs):
+            Xw = w * c
+            for a in range(n):
+                for b in range(n):
+                    for i in range(M):
+                        ib = maps[a, i]
+                        if ib < 0:
+                            continue
+                        for j in (range(i + 1, M) if wt == "COLLINEAR" else range(M)):
+                            jb = maps[b, j]
+                            if jb < 0:
+                                continue
+                            if wt == "COLLINEAR":
+                                Gup, Gdn = G[:, 0], G[:, 1]
+                                cc = (Gup[:, i, j] * Gdn[:, ib, jb] + Gup[:, i, jb] * Gdn[:, ib, j]
+                                      + Gdn[:, i, jb] * Gup[:, ib, j] + Gdn[:, i, j] * Gup[:, ib, jb])
+                            else:
+                                g = G[:, 0]
+                                cc = (g[:, i, j] * g[:, M + ib, M + jb] - g[:, i, M + jb] * g[:, M + ib, j])
+                                cc = cc + (g[:, i, jb] * g[:, M + ib, M + j] - g[:, i, M + j] * g[:, M + ib, jb])
+                                cc = cc + (g[:, M + i, M + jb] * g[:, ib, j] - g[:, M + i, j] * g[:, ib, M + jb])
+                                cc = cc + (g[:, M + i, M + j] * g[:, ib, jb] - g[:, M + i, jb] * g[:, ib, M + j])
+                            avg[a, b, i, j] += np.sum(0.5 * Xw * cc)
+        out["PairCorr"] = avg / den
+    return out
+
+
 class BackPropEstimator:
     """BackPropEstimator with the OneRDM and DiagonalTwoRDM observables (BackPropEstimator.hpp:36-275,
     AFQMCBasePropagator::BackPropagate :404-526), one rank.
@@ -1171,8 +1255,9 @@ class BackPropEstimator:
     conj(logdetR_d)) / sum (CLOSED: both doubled).  The anchor moves to the current step once bp
     reaches the longest length."""
 
-    def __init__(self, ham, prop, wset, steps=(2,), ortho_interval=10, path_restoration=True):
+    def __init__(self, ham, prop, wset, steps=(2,), ortho_interval=10, path_restoration=True, observables=None):
         self.ham, self.prop = ham, prop
+        self.observables = observables  # keyword arguments of _observables_reduce, or None
         self.steps = sorted(int(k) for k in steps)
         self.ortho = int(ortho_interval)
         self.path_restoration = path_restoration
@@ -1226,10 +1311,15 @@ class BackPropEstimator:
         tot = np.sum(es, axis=0)
         one, two = _rdm_reduce(parts, [e / tot for e in es], weights, _walker_kind(dets[0]), ham.M)
         pre = f"BackPropEstimator/Steps={nb}"
-        return {f"{pre}/OneRDM": one, f"{pre}/DiagonalTwoRDM": two}
+        out = {f"{pre}/OneRDM": one, f"{pre}/DiagonalTwoRDM": two}
+        if self.observables:
+            obs = _observables_reduce(parts, [e / tot for e in es], weights, _walker_kind(dets[0]), ham.M,
+                                      **self.observables)
+            out.update({f"{pre}/{k}": v for k, v in obs.items()})
+        return out
 
 
-def measure_mixed_rdms(ham, wset):
+def measure_mixed_rdms(ham, wset, observables=None):
     """MixedEstimator::measure with the OneRDM and DiagonalTwoRDM observables (MixedEstimator.hpp:37-147),
     one rank: per reference determinant d the full mixed G_d and its log overlap (one determinant per
     spin, not doubled for CLOSED) give refCoeff_d = conj(c_d) exp(ov_d - OVLP) / sum_d' (...); the
@@ -1239,17 +1329,23 @@ def measure_mixed_rdms(ham, wset):
     e = [np.conj(ci[k]) * np.exp(ov - wset.ovlp) for k, (_, ov) in enumerate(parts)]
     tot = np.sum(e, axis=0)
     one, two = _rdm_reduce([G for G, _ in parts], [x / tot for x in e], wset.weight, _walker_kind(dets[0]), ham.M)
-    return {"MixedEstimator/OneRDM": one, "MixedEstimator/DiagonalTwoRDM": two}
+    out = {"MixedEstimator/OneRDM": one, "MixedEstimator/DiagonalTwoRDM": two}
+    if observables:  # TwoRDM, SpinCorr, PairCorr (keyword arguments of _observables_reduce)
+        obs = _observables_reduce([G for G, _ in parts], [x / tot for x in e], wset.weight, _walker_kind(dets[0]),
+                                  ham.M, **observables)
+        out.update({f"MixedEstimator/{k}": v for k, v in obs.items()})
+    return out
 
 
 def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, measure_interval=10,
                equilibration_steps=0, relax=None, rank=0, mixed_interval=None, bp_steps=None, bp_ortho_interval=None,
-               **prop_args):
+               observables=None, **prop_args):
     """execute_simulation + run_afqmc for one stage with HostRandomGenerator streams: walkers from
     the trial (NOMSD::initial_guess), Energy + seedPseudoEnergy, Eshift = averageEnergy, then the
     step loop.  Fields come from stream 1 (nwalk x nchol uniforms per step), the comb from stream 0.
     With mixed_interval the mixed estimator's one-body and diagonal two-body RDMs are measured too,
-    with bp_steps (back propagation lengths) the back-propagated ones.
+    with bp_steps (back propagation lengths) the back-propagated ones; observables (keyword
+    arguments of _observables_reduce) adds TwoRDM, SpinCorr and PairCorr to both estimators.
     Returns (initial Eshift, final Eshift, {observable: list of bins})."""
     from .mt19937 import HostRandomGenerator, split_seed
     walker_rng = HostRandomGenerator(split_seed(seed, rank, 0))
@@ -1259,7 +1355,8 @@ def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, 
     Eshift = init_walkers(ham, wset)
     E_init = Eshift
     prop = Propagator(ham, dt, **prop_args)
-    bp = BackPropEstimator(ham, prop, wset, bp_steps, bp_ortho_interval or ortho_interval) if bp_steps else None
+    bp = BackPropEstimator(ham, prop, wset, bp_steps, bp_ortho_interval or ortho_interval,
+                           observables=observables) if bp_steps else None
     if relax is None:
         relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
     series = {}
@@ -1275,7 +1372,7 @@ def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, 
                 for k, v in measure_step(ham, wset, step, dt).items():
                     series.setdefault(k, []).append(v)
             if mixed_interval and step % mixed_interval == 0:
-                for k, v in measure_mixed_rdms(ham, wset).items():
+                for k, v in measure_mixed_rdms(ham, wset, observables).items():
                     series.setdefault(k, []).append(v)
             if bp is not None:
                 for k, v in bp.measure(wset, step).items():

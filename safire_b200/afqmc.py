@@ -336,16 +336,53 @@ class AfqmcEngine:
         pre = f"BackPropEstimator/Steps={int(nsteps)}"
         return {f"{pre}/OneRDM": one, f"{pre}/DiagonalTwoRDM": two}
 
+    def _obs_buffers(self, two_rdm, spin_corr, pair_maps):
+        M = self.M
+        ns = 2 if self.params.walker_type == capi.WALKER_COLLINEAR else 1
+        two = np.empty((ns + 1, M, M, M, M), np.complex128) if two_rdm else None
+        spin = np.empty((2, M * (M + 1) // 2), np.complex128) if spin_corr else None
+        maps = None if pair_maps is None else np.ascontiguousarray(np.asarray(pair_maps, np.int32))
+        pair = None if maps is None else np.empty((len(maps), len(maps), M, M), np.complex128)
+        p = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+        return (two, spin, maps, pair), (p(two), p(spin), 0 if maps is None else len(maps), p(maps), p(pair))
+
+    @staticmethod
+    def _obs_dict(pre, two, spin, pair):
+        out = {}
+        if two is not None:
+            out[f"{pre}/TwoRDM"] = two
+        if spin is not None:
+            out[f"{pre}/SpinCorr"] = spin
+        if pair is not None:
+            out[f"{pre}/PairCorr"] = pair
+        return out
+
+    def measure_observables(self, two_rdm=True, spin_corr=True, pair_maps=None):
+        """MixedEstimator's TwoRDM, SpinCorr and PairCorr (pair_maps (npair, nmo): each orbital's
+        partner, negative for none) of the current walkers (sfq_engine_measure_observables)."""
+        (two, spin, _, pair), args = self._obs_buffers(two_rdm, spin_corr, pair_maps)
+        check(lib().sfq_engine_measure_observables(self.h, *args))
+        return self._obs_dict("MixedEstimator", two, spin, pair)
+
+    def measure_bp_observables(self, nsteps, ortho_interval=10, path_restoration=True, two_rdm=True, spin_corr=True,
+                               pair_maps=None):
+        """BackPropEstimator's TwoRDM, SpinCorr and PairCorr over the last nsteps."""
+        (two, spin, _, pair), args = self._obs_buffers(two_rdm, spin_corr, pair_maps)
+        check(lib().sfq_engine_measure_bp_observables(self.h, int(nsteps), int(ortho_interval),
+                                                      int(bool(path_restoration)), *args))
+        return self._obs_dict(f"BackPropEstimator/Steps={int(nsteps)}", two, spin, pair)
+
     def run_with_streams(self, steps, Eshift, field_uniforms, comb_uniform, ortho_interval=10, pop_interval=10,
                          equilibration_steps=100, measure_interval=10, relax=None, step0=0, mixed_interval=None,
-                         bp_steps=None, bp_ortho_interval=None, path_restoration=True):
+                         bp_steps=None, bp_ortho_interval=None, path_restoration=True, observables=None):
         """run_afqmc's step loop (run_afqmc.cpp:69-104) with the caller's random streams at the
         reference's two injection points: field_uniforms(n) returns the n = nwalk * nchol uniforms
         of a step (walker-major, assemble_X's sampleUniformFields) and comb_uniform() the comb's
         uniform (population_control.hpp:41-42).  Given the reference's own generators it replays
         a reference run.  Every measurement records EnergyEstimator::measure's observables
         (EnergyEstimator.h:51-100), every mixed_interval steps the mixed estimator's RDMs, and with
-        bp_steps the back-propagated ones.
+        bp_steps the back-propagated ones; observables (keyword arguments of measure_observables) adds
+        TwoRDM, SpinCorr and PairCorr to both estimators.
         Returns (Eshift, {observable: list of bins})."""
         if relax is None:
             relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
@@ -376,11 +413,18 @@ class AfqmcEngine:
                 if mixed_interval and step % mixed_interval == 0:
                     for k, v in self.measure_mixed_rdms().items():
                         series.setdefault(k, []).append(v)
+                    if observables:
+                        for k, v in self.measure_observables(**observables).items():
+                            series.setdefault(k, []).append(v)
                 if bp_steps:
                     if step - bp_pos in bp_steps:
                         for k, v in self.measure_bp_rdms(step - bp_pos, bp_ortho_interval or ortho_interval,
                                                          path_restoration).items():
                             series.setdefault(k, []).append(v)
+                        if observables:
+                            for k, v in self.measure_bp_observables(step - bp_pos, bp_ortho_interval or ortho_interval,
+                                                                    path_restoration, **observables).items():
+                                series.setdefault(k, []).append(v)
                     if step - bp_pos >= bp_steps[-1]:
                         self.bp_anchor()
                         bp_pos = step

@@ -255,6 +255,111 @@ __global__ void bp_ov_kernel(cplx* ov, const cplx* ld, double f, int W) {
   if (w < W) ov[w] = cadd(cscale(ov[w], f), cconj(cscale(ld[w], f)));
 }
 
+// ---- TwoRDM, SpinCorr, PairCorr observables (Observables/twordm.hpp, spincorr.hpp, paircorr.hpp) ----
+// XwG[w][s][x] = wc[w] Gf[w][s][x]
+__global__ void scale_walker_rows_kernel(const cplx* Gf, const cplx* wc, long per_walker, int W, cplx* out) {
+  const long n = per_walker * W;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+    out[e] = cmul(wc[e / per_walker], Gf[e]);
+}
+// avg[i][k][j][l] += C[(i,k)][(j,l)] - [same spin] C[(i,l)][(j,k)], C = sum_w XwG_s[w] (x) G_s'[w]
+// (twordm.hpp:57-71: (ikjl) = G_ik G_jl - G_il G_jk for one spin, G_ik G_jl across the spins)
+__global__ void twordm_block_kernel(const cplx* C, int M, int same, cplx* avg) {
+  const long MM = (long)M * M, n = MM * MM;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const long x = e / MM, y = e % MM;  // x = (i, k), y = (j, l)
+    cplx v = C[e];
+    if (same) {
+      const long i = x / M, k = x % M, j = y / M, l = y % M;
+      v = csub(v, C[(i * M + l) * MM + j * M + k]);
+    }
+    avg[e] = cadd(avg[e], v);
+  }
+}
+// <S_i . S_j> for i <= j in the order i-major (spincorr.hpp:58-124): out[0] the XY channel, out[1] Z.
+// kind 0 CLOSED (one block), 1 COLLINEAR (up, down blocks of M x M), 2 NONCOLLINEAR (one 2M x 2M block)
+__global__ void spincorr_kernel(const cplx* Gf, const cplx* wc, int W, int M, int kind, cplx* out) {
+  const int i = blockIdx.y, j = i + blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= M) return;
+  const long P = (long)M * (M + 1) / 2;
+  const long idx = (long)i * M - (long)i * (i - 1) / 2 + (j - i);
+  const int R = kind == 2 ? 2 * M : M;
+  const long blk = (long)R * R;
+  const int ns = kind == 1 ? 2 : 1;
+  cplx xy = mk(0.0, 0.0), z = mk(0.0, 0.0);
+  const cplx one = mk(1.0, 0.0);
+  for (int w = 0; w < W; ++w) {
+    const cplx* G = Gf + (long)w * ns * blk;
+    auto g = [&](int s, int a, int b) { return G[s * blk + (long)a * R + b]; };
+    cplx cz, cxy;
+    if (kind != 2) {
+      const int d = kind == 1 ? 1 : 0;  // CLOSED: the down block is the up block
+      if (j == i) {
+        cz = cadd(cmul(g(0, i, i), csub(one, g(d, j, j))), cmul(g(d, i, i), csub(one, g(0, j, j))));
+        cxy = cadd(cmul(g(0, i, j), csub(one, g(d, j, i))), cmul(g(d, i, j), csub(one, g(0, j, i))));
+      } else {
+        cz = csub(csub(cadd(cmul(g(0, i, i), csub(g(0, j, j), g(d, j, j))), cmul(g(d, i, i), csub(g(d, j, j), g(0, j, j)))),
+                       cmul(g(0, i, j), g(0, j, i))),
+                  cmul(g(d, i, j), g(d, j, i)));
+        cxy = cadd(cmul(g(0, i, j), cscale(g(d, j, i), -1.0)), cmul(g(d, i, j), cscale(g(0, j, i), -1.0)));
+      }
+    } else {
+      const int I = i + M, J = j + M;
+      if (j == i) {
+        cz = cadd(cadd(cmul(g(0, i, i), csub(one, g(0, J, J))), cmul(g(0, I, I), csub(one, g(0, j, j)))),
+                  cadd(cmul(g(0, i, J), g(0, J, i)), cmul(g(0, I, j), g(0, j, I))));
+        cxy = cadd(cadd(cmul(g(0, i, j), csub(one, g(0, J, I))), cmul(g(0, I, J), csub(one, g(0, j, i)))),
+                   cadd(cmul(g(0, J, j), g(0, i, I)), cmul(g(0, j, J), g(0, I, i))));
+      } else {
+        cz = cadd(cmul(g(0, i, i), csub(g(0, j, j), g(0, J, J))), cmul(g(0, I, I), csub(g(0, J, J), g(0, j, j))));
+        cz = csub(cz, cmul(g(0, i, j), g(0, j, i)));
+        cz = csub(cz, cmul(g(0, I, J), g(0, J, I)));
+        cz = cadd(cz, cmul(g(0, i, J), g(0, J, i)));
+        cz = cadd(cz, cmul(g(0, I, j), g(0, j, I)));
+        cxy = cadd(cmul(g(0, i, j), cscale(g(0, J, I), -1.0)), cmul(g(0, I, J), cscale(g(0, j, i), -1.0)));
+        cxy = cadd(cxy, cadd(cmul(g(0, J, j), g(0, i, I)), cmul(g(0, j, J), g(0, I, i))));
+      }
+    }
+    z = cadd(z, cmul(wc[w], cscale(cz, 0.25)));
+    xy = cadd(xy, cmul(wc[w], cscale(cxy, 0.5)));
+  }
+  out[idx] = cadd(out[idx], xy);
+  out[P + idx] = cadd(out[P + idx], z);
+}
+// P_ab(i, j) for the pair maps a, b (paircorr.hpp:80-135): kind 1 COLLINEAR (j > i), 2 NONCOLLINEAR
+// (every j); maps (npair, M), a negative partner leaves the entry out; out (npair, npair, M, M)
+__global__ void paircorr_kernel(const cplx* Gf, const cplx* wc, int W, int M, int kind, int npair, const int* maps,
+                                cplx* out) {
+  const long n = (long)npair * npair * M * M;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const int j = int(e % M), i = int((e / M) % M);
+    const int b = int((e / ((long)M * M)) % npair), a = int(e / ((long)M * M * npair));
+    if (kind == 1 && j <= i) continue;
+    const int ib = maps[(long)a * M + i], jb = maps[(long)b * M + j];
+    if (ib < 0 || jb < 0) continue;
+    const int R = kind == 2 ? 2 * M : M;
+    const long blk = (long)R * R;
+    const int ns = kind == 1 ? 2 : 1;
+    cplx acc = mk(0.0, 0.0);
+    for (int w = 0; w < W; ++w) {
+      const cplx* G = Gf + (long)w * ns * blk;
+      auto g = [&](int s, int x, int y) { return G[s * blk + (long)x * R + y]; };
+      cplx c;
+      if (kind == 1) {
+        c = cadd(cadd(cmul(g(0, i, j), g(1, ib, jb)), cmul(g(0, i, jb), g(1, ib, j))),
+                 cadd(cmul(g(1, i, jb), g(0, ib, j)), cmul(g(1, i, j), g(0, ib, jb))));
+      } else {
+        c = csub(cmul(g(0, i, j), g(0, M + ib, M + jb)), cmul(g(0, i, M + jb), g(0, M + ib, j)));
+        c = cadd(c, csub(cmul(g(0, i, jb), g(0, M + ib, M + j)), cmul(g(0, i, M + j), g(0, M + ib, jb))));
+        c = cadd(c, csub(cmul(g(0, M + i, M + jb), g(0, ib, j)), cmul(g(0, M + i, j), g(0, ib, M + jb))));
+        c = cadd(c, csub(cmul(g(0, M + i, M + j), g(0, ib, jb)), cmul(g(0, M + i, jb), g(0, ib, M + j))));
+      }
+      acc = cadd(acc, cmul(wc[w], cscale(c, 0.5)));
+    }
+    out[e] = cadd(out[e], acc);
+  }
+}
+
 // ---- the mixed estimator's RDMs (MixedEstimator.hpp:37-147) ---------------------------------
 // tot[w] = sum_d conj(ci_d) exp(ov_d[w] - shift[w]) over the reference determinants
 __global__ void rdm_tot_kernel(const cplx* ov, const cplx* cic, const cplx* shift, int ndet, int W, cplx* tot) {
@@ -1006,6 +1111,13 @@ struct Engine {
     return SFQ_OK;
   }
 
+  // the other observables of the mixed and back-propagated estimators, when asked for (results divided by the total weight)
+  struct ObsSpec {
+    bool two_rdm = false, spin_corr = false;
+    int npair = 0;
+    const int* maps = nullptr;  // host (npair, M)
+    std::vector<cplx> two, spin, pair;
+  };
   // --- back propagation (WalkerSetBase::resize_bp, BackPropEstimator) ---------------------------
   // per walker: the anchored walkers, a ring of the last nbp steps' fields (slot hist_pos % nbp),
   // the weight factors of the last 3 nbp steps (slot hist_pos); all travel with population control
@@ -1038,7 +1150,8 @@ struct Engine {
   }
   // BackPropagate over the last nb steps and the BackPropEstimator's RDMs (one (nspin, Mr, Mr), two
   // before folding (nblk, Mr, Mr)), divided by the sum of the restored weights
-  int measure_bp(int nb, int ortho, bool restore, std::vector<cplx>& one, std::vector<cplx>& two) {
+  int measure_bp(int nb, int ortho, bool restore, std::vector<cplx>& one, std::vector<cplx>& two,
+                 ObsSpec* obs = nullptr) {
     int rc;
     if (!nbp) return record_error(SFQ_ERR_ARG, "back propagation is not enabled");
     if (nb <= 0 || nb > nbp || ortho <= 0) return record_error(SFQ_ERR_ARG, "back propagation over %d steps (ring %d)", nb, nbp);
@@ -1081,7 +1194,7 @@ struct Engine {
         SFQ_LAUNCHED();
       }
     }
-    return rdm_measure(bp_wt, true, one, two);
+    return rdm_measure(bp_wt, true, one, two, obs);
   }
 
   // --- MixedEstimator with the OneRDM and DiagonalTwoRDM observables -------------------------
@@ -1090,17 +1203,34 @@ struct Engine {
   int rdm_nblk() const { return collinear ? 3 : (npol == 2 ? 1 : 2); }
   // one (rdm_nspin, Mr, Mr) and the diagonal two-body RDM before folding (rdm_nblk, Mr, Mr), both divided
   // by the total weight, on the host (MixedEstimator.hpp:37-147)
-  int measure_rdm(std::vector<cplx>& one, std::vector<cplx>& two) {
+  int measure_rdm(std::vector<cplx>& one, std::vector<cplx>& two, ObsSpec* obs = nullptr) {
     if (mixed) return record_error(SFQ_ERR_UNSUPPORTED, "the mixed estimator's RDMs are measured in FP64 engines");
     inv_cached = false;
-    return rdm_measure(props + (long)P_WEIGHT * W, false, one, two);
+    return rdm_measure(props + (long)P_WEIGHT * W, false, one, two, obs);
+  }
+  // which observables this engine's walkers support, as the reference's constructors check them
+  int check_obs(const ObsSpec& o) const {
+    if (ndet > 1 && (o.two_rdm || o.spin_corr || o.npair))
+      return record_error(SFQ_ERR_UNSUPPORTED, "TwoRDM, SpinCorr and PairCorr are measured for single determinants");
+    if (o.two_rdm && npol == 2)
+      return record_error(SFQ_ERR_UNSUPPORTED, "TwoRDM is only implemented for closed and collinear walkers");
+    if (o.two_rdm && (double)M * M * M * M * 16.0 > double(1L << 30))
+      return record_error(SFQ_ERR_UNSUPPORTED, "TwoRDM of %d orbitals: more than 1 GiB per block", M);
+    if (o.npair && closed())
+      return record_error(SFQ_ERR_UNSUPPORTED, "PairCorr is not implemented for closed walkers");
+    if (o.npair < 0 || (o.npair && !o.maps)) return record_error(SFQ_ERR_ARG, "PairCorr: %d maps", o.npair);
+    for (long t = 0; t < (long)o.npair * M; ++t)
+      if (o.maps[t] >= M) return record_error(SFQ_ERR_ARG, "PairCorr: partner %d of %d orbitals", o.maps[t], M);
+    return SFQ_OK;
   }
   // the RDM reduction shared by the mixed estimator (bp false: the trial's references against the
   // walkers, coefficients relative to the walkers' log overlaps) and the back-propagated one (bp true:
   // each walker's propagated references against its anchored matrix, the overlaps with conj of the
   // references' QR log dets, constructBPMeasurementInputs, BackPropEstimator.hpp:36-110)
-  int rdm_measure(const cplx* weight, bool bp, std::vector<cplx>& one, std::vector<cplx>& two) {
+  int rdm_measure(const cplx* weight, bool bp, std::vector<cplx>& one, std::vector<cplx>& two,
+                  ObsSpec* obs = nullptr) {
     int rc;
+    if (obs && (rc = check_obs(*obs))) return rc;
     const int ns = rdm_nspin(), nb = rdm_nblk();
     const long MM = (long)Mr * Mr, RN = det_elems();
     const size_t elems = (size_t)W * ns * MM + ns * MM + nb * MM + 2 * (size_t)W + (size_t)ndet * W;
@@ -1112,6 +1242,39 @@ struct Engine {
     cplx* tot = wc + W;
     cplx* ovd = tot + W;
     SFQ_CUDA_TRY(cudaMemsetAsync(o1, 0, sizeof(cplx) * (ns + nb) * MM, st));
+    // observables' device buffers: TwoRDM (ns + 1 blocks of M^4) and its product scratch, the weighted
+    // walker G's, SpinCorr (2, M(M+1)/2), PairCorr (npair^2 M^2) and the pair maps
+    // (sized by the orbitals M: NONCOLLINEAR G blocks are 2M x 2M, the observables M x M)
+    const int kind = npol == 2 ? 2 : (collinear ? 1 : 0);
+    const long Mo2 = (long)M * M, M4 = Mo2 * Mo2, Ptri = (long)M * (M + 1) / 2;
+    const long n2 = obs && obs->two_rdm ? (ns + 1) * M4 : 0, ns_sp = obs && obs->spin_corr ? 2 * Ptri : 0;
+    const long npr = obs ? (long)obs->npair * obs->npair * Mo2 : 0;
+    cplx *d_two = nullptr, *d_C = nullptr, *d_xwg = nullptr, *d_spin = nullptr, *d_pair = nullptr;
+    int* d_maps = nullptr;
+    if (n2) {
+      SFQ_CUDA_TRY(cudaMallocAsync((void**)&d_two, sizeof(cplx) * n2, st));
+      SFQ_CUDA_TRY(cudaMallocAsync((void**)&d_C, sizeof(cplx) * M4, st));
+      SFQ_CUDA_TRY(cudaMallocAsync((void**)&d_xwg, sizeof(cplx) * (size_t)W * ns * MM, st));
+      SFQ_CUDA_TRY(cudaMemsetAsync(d_two, 0, sizeof(cplx) * n2, st));
+    }
+    if (ns_sp) {
+      SFQ_CUDA_TRY(cudaMallocAsync((void**)&d_spin, sizeof(cplx) * ns_sp, st));
+      SFQ_CUDA_TRY(cudaMemsetAsync(d_spin, 0, sizeof(cplx) * ns_sp, st));
+    }
+    if (npr) {
+      SFQ_CUDA_TRY(cudaMallocAsync((void**)&d_pair, sizeof(cplx) * npr, st));
+      SFQ_CUDA_TRY(cudaMemsetAsync(d_pair, 0, sizeof(cplx) * npr, st));
+      SFQ_CUDA_TRY(cudaMallocAsync((void**)&d_maps, sizeof(int) * (size_t)obs->npair * M, st));
+      SFQ_CUDA_TRY(cudaMemcpyAsync(d_maps, obs->maps, sizeof(int) * (size_t)obs->npair * M, cudaMemcpyHostToDevice, st));
+    }
+    struct StreamFree {  // the observables' buffers go back to the pool on every way out
+      cudaStream_t st;
+      std::vector<void*> p;
+      ~StreamFree() {
+        for (void* q : p)
+          if (q) cudaFreeAsync(q, st);
+      }
+    } obs_bufs{st, {d_two, d_C, d_xwg, d_spin, d_pair, d_maps}};
     const cplx* shift = bp ? nullptr : props + (long)P_OVLP * W;
     const cplx* B = bp ? bp_SMN : SM;
     std::vector<cplx> cic(ndet, mk(1.0, 0.0));
@@ -1177,6 +1340,39 @@ struct Engine {
       const long tot2 = nb * MM;
       rdm_two_kernel<<<int(std::min<long>((tot2 + 127) / 128, 1184)), 128, 0, st>>>(Gf, wc, W, ns, Mr, nb, o2);
       SFQ_LAUNCHED();
+      if (n2) {  // avg blocks (a,a,a,a), (a,a,b,b), (b,b,b,b): C = sum_w (wc G_s)[w] (x) G_s'[w], one GEMM each
+        scale_walker_rows_kernel<<<1184, 256, 0, st>>>(Gf, wc, ns * MM, W, d_xwg);
+        SFQ_LAUNCHED();
+        for (int blk = 0; blk <= ns; ++blk) {  // (TwoRDM runs for npol = 1 only: MM = M^2 here)
+          const bool same = blk % 2 == 0;
+          const int s1 = same ? blk / 2 : 0, s2 = same ? blk / 2 : ns - 1;
+          GemmDesc g;
+          g.M = int(MM); g.N = int(MM); g.K = W; g.batch = 1;
+          g.A = d_xwg + s1 * MM; g.sAm = 1; g.sAk = ns * MM; g.a_cplx = true;
+          g.B = Gf + s2 * MM; g.sBk = ns * MM; g.sBn = 1; g.b_cplx = true;
+          g.C = d_C; g.sCm = MM; g.sCn = 1;
+          if ((rc = gemm_f64(g, st))) return rc;
+          twordm_block_kernel<<<1184, 256, 0, st>>>(d_C, M, same ? 1 : 0, d_two + blk * M4);
+          SFQ_LAUNCHED();
+        }
+      }
+      if (ns_sp) {
+        spincorr_kernel<<<dim3((M + 127) / 128, M), 128, 0, st>>>(Gf, wc, W, M, kind, d_spin);
+        SFQ_LAUNCHED();
+      }
+      if (npr) {
+        paircorr_kernel<<<int(std::min<long>((npr + 127) / 128, 1184)), 128, 0, st>>>(Gf, wc, W, M, kind, obs->npair,
+                                                                                       d_maps, d_pair);
+        SFQ_LAUNCHED();
+      }
+    }
+    if (obs) {
+      obs->two.assign(n2, mk(0.0, 0.0));
+      obs->spin.assign(ns_sp, mk(0.0, 0.0));
+      obs->pair.assign(npr, mk(0.0, 0.0));
+      if (n2) SFQ_CUDA_TRY(cudaMemcpyAsync(obs->two.data(), d_two, sizeof(cplx) * n2, cudaMemcpyDeviceToHost, st));
+      if (ns_sp) SFQ_CUDA_TRY(cudaMemcpyAsync(obs->spin.data(), d_spin, sizeof(cplx) * ns_sp, cudaMemcpyDeviceToHost, st));
+      if (npr) SFQ_CUDA_TRY(cudaMemcpyAsync(obs->pair.data(), d_pair, sizeof(cplx) * npr, cudaMemcpyDeviceToHost, st));
     }
     one.resize(ns * MM);
     two.resize(nb * MM);
@@ -1193,6 +1389,11 @@ struct Engine {
     };
     divide(one);
     divide(two);
+    if (obs) {
+      divide(obs->two);
+      divide(obs->spin);
+      divide(obs->pair);
+    }
     return SFQ_OK;
   }
 
@@ -2646,6 +2847,50 @@ int sfq_engine_measure_rdm(sfq_engine_t h, void* one_rdm, void* diag_two_rdm) {
   int rc;
   if ((rc = e.measure_rdm(one, two))) return rc;
   return fold_rdms(e, one, two, one_rdm, diag_two_rdm);
+}
+
+namespace {
+int obs_request(Engine& e, Engine::ObsSpec& o, void* two_rdm, void* spin_corr, int npair, const int* pair_maps,
+                void* pair_corr) {
+  o.two_rdm = two_rdm != nullptr;
+  o.spin_corr = spin_corr != nullptr;
+  o.npair = pair_corr ? npair : 0;
+  o.maps = pair_maps;
+  if (e.mixed) return record_error(SFQ_ERR_UNSUPPORTED, "the estimators' observables are measured in FP64 engines");
+  return e.check_obs(o);
+}
+void obs_out(const Engine::ObsSpec& o, void* two_rdm, void* spin_corr, void* pair_corr) {
+  if (two_rdm) std::memcpy(two_rdm, o.two.data(), sizeof(cplx) * o.two.size());
+  if (spin_corr) std::memcpy(spin_corr, o.spin.data(), sizeof(cplx) * o.spin.size());
+  if (pair_corr) std::memcpy(pair_corr, o.pair.data(), sizeof(cplx) * o.pair.size());
+}
+}  // namespace
+
+int sfq_engine_measure_observables(sfq_engine_t h, void* two_rdm, void* spin_corr, int npair, const int* pair_maps,
+                                   void* pair_corr) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  Engine::ObsSpec o;
+  int rc;
+  if ((rc = obs_request(e, o, two_rdm, spin_corr, npair, pair_maps, pair_corr))) return rc;
+  std::vector<cplx> one, two;
+  if ((rc = e.measure_rdm(one, two, &o))) return rc;
+  obs_out(o, two_rdm, spin_corr, pair_corr);
+  return SFQ_OK;
+}
+
+int sfq_engine_measure_bp_observables(sfq_engine_t h, int nsteps, int ortho_interval, int path_restoration,
+                                      void* two_rdm, void* spin_corr, int npair, const int* pair_maps,
+                                      void* pair_corr) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  Engine::ObsSpec o;
+  int rc;
+  if ((rc = obs_request(e, o, two_rdm, spin_corr, npair, pair_maps, pair_corr))) return rc;
+  std::vector<cplx> one, two;
+  if ((rc = e.measure_bp(nsteps, ortho_interval, path_restoration != 0, one, two, &o))) return rc;
+  obs_out(o, two_rdm, spin_corr, pair_corr);
+  return SFQ_OK;
 }
 
 static int fold_rdms(Engine& e, const std::vector<cplx>& one, const std::vector<cplx>& two, void* one_rdm,

@@ -1,0 +1,76 @@
+"""TwoRDM, SpinCorr and PairCorr of the mixed and back-propagated estimators on the B200
+(sfq_engine_measure_observables / sfq_engine_measure_bp_observables) against the oracle's
+restatement of Observables/twordm.hpp, spincorr.hpp and paircorr.hpp, measured along the replay of
+the reference's seeded BH runs (the same schedule as the recorded one- and two-body RDMs): CLOSED,
+COLLINEAR and NONCOLLINEAR walkers, each observable where the reference measures it."""
+import numpy as np
+import pytest
+
+from oracle import afqmc_oracle as O
+from oracle.mt19937 import HostRandomGenerator, split_seed
+from safire_b200 import afqmc as A
+from safire_b200 import capi
+from tests.golden_io import engine_system, oracle_hamiltonian, snapshot
+
+pytestmark = pytest.mark.gpu
+
+
+def _maps(M):
+    return np.array([[(i + 1) % M if i % 3 != 2 else -1 for i in range(M)], [M - 1 - i for i in range(M)]])
+
+
+CASES = [("bh_rhf_closed", True, True, False), ("bh_uhf_collinear", True, True, True),
+         ("bh_uhf_noncollinear", False, True, True)]
+
+
+@pytest.mark.parametrize("case,two,spin,pair", CASES)
+def test_observables_match_the_oracle_along_the_seeded_replay(case, two, spin, pair):
+    snap = snapshot(case)
+    st = snap["settings"]
+    M = snap["hcore"].shape[0]
+    obs = dict(two_rdm=two, spin_corr=spin, pair_maps=_maps(M) if pair else None)
+    eng = A.AfqmcEngine(engine_system(snap), st["nwalk"], dt=st["dt"], seed=0, precision=capi.PRECISION_FP64)
+    walker_rng = HostRandomGenerator(split_seed(st["seed"], 0, 0))
+    field_rng = HostRandomGenerator(split_seed(st["seed"], 0, 1))
+    _, series = eng.run_with_streams(st["steps"], eng.init(), field_rng.uniforms, lambda: walker_rng.uniforms(1)[0],
+                                     ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
+                                     equilibration_steps=st["equilibration_steps"],
+                                     measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"],
+                                     bp_steps=snap["bp_steps"], bp_ortho_interval=snap["bp_ortho_interval"],
+                                     observables=obs)
+    eng.close()
+    _, _, oracle = O.run_seeded(oracle_hamiltonian(snap), st["nwalk"], st["dt"], st["steps"], st["seed"],
+                                ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"],
+                                measure_interval=st["measure_interval"], mixed_interval=snap["mixed_interval"],
+                                bp_steps=snap["bp_steps"], bp_ortho_interval=snap["bp_ortho_interval"],
+                                observables=obs)
+    names = [k for k in series if k.endswith(("TwoRDM", "SpinCorr", "PairCorr")) and "Diagonal" not in k]
+    expect = (2 if two else 0) + (2 if spin else 0) + (2 if pair else 0)  # mixed and back-propagated
+    assert len(names) == expect, names
+    for k in names:
+        a, b = np.asarray(series[k]), np.asarray(oracle[k])
+        assert a.shape == b.shape, k
+        assert np.max(np.abs(a - b)) <= 1e-11 * max(1.0, float(np.max(np.abs(b)))), k
+
+
+def test_observables_refused_where_the_reference_refuses_them():
+    closed = engine_system(snapshot("bh_rhf_closed"))
+    nonc = engine_system(snapshot("bh_uhf_noncollinear"))
+    e = A.AfqmcEngine(closed, 8, dt=0.01, seed=1, precision=capi.PRECISION_FP64)
+    e.init()
+    with pytest.raises(capi.SafireError) as ex:
+        e.measure_observables(two_rdm=False, spin_corr=False, pair_maps=_maps(closed.M))  # paircorr.hpp:37-40
+    assert ex.value.code == 3
+    e.close()
+    e = A.AfqmcEngine(nonc, 8, dt=0.01, seed=1, precision=capi.PRECISION_FP64)
+    e.init()
+    with pytest.raises(capi.SafireError) as ex:
+        e.measure_observables(two_rdm=True, spin_corr=False)  # twordm.hpp:34-36
+    assert ex.value.code == 3
+    e.close()
+    e = A.AfqmcEngine(closed, 8, dt=0.01, seed=1, precision=capi.PRECISION_INT8X3)
+    e.init()
+    with pytest.raises(capi.SafireError) as ex:
+        e.measure_observables(two_rdm=True, spin_corr=True)  # the estimators are FP64
+    assert ex.value.code == 3
+    e.close()
