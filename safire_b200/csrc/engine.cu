@@ -116,6 +116,18 @@ __global__ void measure_kernel(const double* o, double* out) {
   out[9] = o[3];
 }
 __global__ void step_add_kernel(unsigned long long* step) { *step += 1ull; }
+// back propagation in device-resident blocks: the history position lives in device memory (d_step[1])
+__global__ void set_hist_kernel(unsigned long long* pos, unsigned long long v) { *pos = v; }
+__global__ void hist_advance_kernel(unsigned long long* pos, int nhist) { *pos = (*pos + 1ull) % (unsigned long long)nhist; }
+// storeFields into the ring slot pos % nbp: ring[w][slot][n] = X[w][n]
+__global__ void store_fields_kernel(const cplx* X, cplx* ring, int nbp, int Nc, int W, const unsigned long long* pos) {
+  const long slot = long(*pos % (unsigned long long)nbp);
+  const long n = (long)W * Nc;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const long w = e / Nc, c = e % Nc;
+    ring[(w * nbp + slot) * Nc + c] = X[e];
+  }
+}
 __global__ void set_block_state_kernel(unsigned long long* step, unsigned long long s0, double* eshift, double e0) {
   *step = s0;
   *eshift = e0;
@@ -1467,9 +1479,14 @@ struct Engine {
       uni_wait = nullptr;
     }
     if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
-    if (nbp)  // storeFields (AFQMCBasePropagator.cpp:342-344): the fields into the ring slot
+    if (nbp && dev_mode) {  // storeFields (AFQMCBasePropagator.cpp:342-344): the fields into the ring slot
+      store_fields_kernel<<<int(std::min<long>(((long)W * Nc + 255) / 256, 1184)), 256, 0, st>>>(X, bp_fields, nbp, Nc, W,
+                                                                                                 d_step + 1);
+      SFQ_LAUNCHED();
+    } else if (nbp) {
       SFQ_CUDA_TRY(cudaMemcpy2DAsync(bp_fields + (long)(hist_pos % nbp) * Nc, sizeof(cplx) * nbp * Nc, X,
                                      sizeof(cplx) * Nc, sizeof(cplx) * Nc, W, cudaMemcpyDeviceToDevice, st));
+    }
     ph_end(SFQ_PH_FIELDS);
     ph_begin(SFQ_PH_VHS);
     ph_begin(SFQ_PH_VHS_GEMM);
@@ -1496,11 +1513,17 @@ struct Engine {
     up.hybrid = 1; up.free_projection = p.free_projection; up.use_cp_constraint = 0;
     up.Eshift_dev = dev_mode ? d_eshift : nullptr;
     if (nbp) {  // the step's weight factors into the history slot (WalkerSetUpdate.hpp:184-188)
-      up.wfac = bp_wfac + hist_pos;
+      up.wfac = bp_wfac + (dev_mode ? 0 : hist_pos);
+      up.wfac_pos = dev_mode ? d_step + 1 : nullptr;
       up.wfac_stride = nhist;
     }
     if ((rc = walker_update(wprops(), newov, mf, hw, E3, up, stats, st))) return rc;
-    if (nbp) hist_pos = (hist_pos + 1) % nhist;  // advanceHistoryPos
+    if (nbp && dev_mode) {  // advanceHistoryPos; a block's host position moves when it is launched
+      hist_advance_kernel<<<1, 1, 0, st>>>(d_step + 1, nhist);
+      SFQ_LAUNCHED();
+    } else if (nbp) {
+      hist_pos = (hist_pos + 1) % nhist;
+    }
     ph_end(SFQ_PH_UPDATE);
     return SFQ_OK;
   }
@@ -2317,6 +2340,11 @@ struct Engine {
     const BlockGraph& bg = it->second;
     set_block_state_kernel<<<1, 1, 0, st>>>(d_step, rp.step0, d_eshift, Eshift);
     SFQ_LAUNCHED();
+    if (nbp) {  // the block's steps store their fields and weight factors from here on
+      set_hist_kernel<<<1, 1, 0, st>>>(d_step + 1, (unsigned long long)hist_pos);
+      SFQ_LAUNCHED();
+      hist_pos = int((hist_pos + (long)rp.steps) % nhist);
+    }
     SFQ_CUDA_TRY(cudaGraphLaunch(bg.exec, st));
     inv_cached = bg.inv_after;
     inv_ov = bg.inv_ov_after;
@@ -3006,8 +3034,6 @@ int sfq_engine_run(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, d
 int sfq_engine_block(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift, double* meas, int max_meas,
                      int* nmeas) {
   if (!h || !rp || !Eshift) return record_error(SFQ_ERR_ARG, "null pointer");
-  if (h->e.nbp)
-    return record_error(SFQ_ERR_UNSUPPORTED, "device-resident blocks do not keep the back-propagation history");
   int rc;
   if ((rc = h->e.block_async(*rp, *Eshift))) return rc;
   return h->e.block_result(Eshift, meas, max_meas, nmeas);
@@ -3015,8 +3041,6 @@ int sfq_engine_block(sfq_engine_t h, const sfq_run_params_t* rp, double* Eshift,
 
 int sfq_engine_block_async(sfq_engine_t h, const sfq_run_params_t* rp, double Eshift) {
   if (!h || !rp) return record_error(SFQ_ERR_ARG, "null pointer");
-  if (h->e.nbp)
-    return record_error(SFQ_ERR_UNSUPPORTED, "device-resident blocks do not keep the back-propagation history");
   return h->e.block_async(*rp, Eshift);
 }
 

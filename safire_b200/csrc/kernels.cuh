@@ -43,6 +43,7 @@ struct UpdateParams {
   // of walker i goes to wfac[i * wfac_stride] when wfac is set
   cplx* wfac = nullptr;
   long wfac_stride = 1;
+  const unsigned long long* wfac_pos = nullptr;  // when set, the history slot *wfac_pos is added to wfac
 };
 struct WalkerProps {  // columns of the walker set (SoA), each nwalk complex
   cplx *weight, *phase, *pseudo_eloc, *e1, *exx, *ej, *ovlp, *theta;

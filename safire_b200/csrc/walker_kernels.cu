@@ -132,7 +132,7 @@ __global__ void walker_update_kernel(WalkerProps wp, const cplx* new_ovlp, const
     phase = cmul(phase, mk(wf.x / aw, wf.y / aw));
     if (fabs(scale) > 2.2250738585072014e-308) wfac = mk(wf.x / aw / scale, wf.y / aw / scale);
   }
-  if (p.wfac) p.wfac[(long)i * p.wfac_stride] = wfac;
+  if (p.wfac) p.wfac[(p.wfac_pos ? (long)*p.wfac_pos : 0L) + (long)i * p.wfac_stride] = wfac;
   // bound_walker_weights
   const double a = hypot(weight.x, weight.y);
   if (stats) atomicAdd(&stats[3], 1ull);

@@ -87,18 +87,34 @@ def test_collinear_with_identical_spins_is_closed():
         assert np.max(np.abs(a - b)) < 1e-10 * np.max(np.abs(a)), k
 
 
-def test_back_propagation_refused_by_blocks():
+def test_back_propagation_inside_device_blocks_matches_the_host_loop():
+    """Blocks keep the back-propagation history on the device (field ring and weight-factor slots
+    from a device-side position): anchored after 4 steps, 4 more steps with a comb inside, the
+    back-propagated RDMs and observables equal the host loop's."""
     snap = bh_snapshot()
-    eng = A.AfqmcEngine(_system(snap), 8, dt=0.01, precision=capi.PRECISION_FP64)
-    E0 = eng.init()
-    eng.enable_back_propagation(2)
-    with pytest.raises(capi.SafireError) as ex:
-        eng.run_block(4, E0, ortho_interval=2, pop_interval=2, equilibration_steps=0, measure_interval=2)
-    assert ex.value.code == 3
-    with pytest.raises(capi.SafireError) as ex:
-        eng.measure_bp_rdms(3)  # longer than the ring
-    assert ex.value.code == 2
-    eng.close()
+    sched = dict(ortho_interval=2, pop_interval=3, equilibration_steps=0, measure_interval=2)
+    out = []
+    for use_block in (False, True):
+        eng = A.AfqmcEngine(_system(snap), 16, dt=0.01, seed=9, precision=capi.PRECISION_FP64)
+        E = eng.init()
+        eng.enable_back_propagation(4)
+        for b in range(2):
+            run = eng.run_block if use_block else eng.run
+            E, _ = run(4, E, step0=4 * b, **sched)
+            if b == 0:
+                eng.bp_anchor()
+        r = eng.measure_bp_rdms(4, ortho_interval=2)
+        r.update(eng.measure_bp_observables(4, ortho_interval=2))
+        out.append((r, eng.walkers()[0]))
+        with pytest.raises(capi.SafireError) as ex:
+            eng.measure_bp_rdms(5)  # longer than the ring
+        assert ex.value.code == 2
+        eng.close()
+    (rh, Sh), (rd, Sd) = out
+    assert np.max(np.abs(Sh - Sd)) <= 1e-12 * np.max(np.abs(Sh))
+    assert rh.keys() == rd.keys() and len(rh) == 4
+    for k in rh:
+        assert np.max(np.abs(rh[k] - rd[k])) <= 1e-11 * max(1.0, float(np.max(np.abs(rh[k])))), k
 
 
 @pytest.mark.parametrize("case", ["bh_uhf_collinear", "bh_ghf_noncollinear", "bh_rcasci_rhf_closed"])
