@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 11 */
+int sfq_abi_version(void); /* 12 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -343,6 +343,25 @@ int sfq_engine_measure_observables(sfq_engine_t e, void* two_rdm, void* spin_cor
 int sfq_engine_measure_bp_observables(sfq_engine_t e, int nsteps, int ortho_interval, int path_restoration,
                                       void* two_rdm, void* spin_corr, int npair, const int* pair_maps,
                                       void* pair_corr);
+
+/* TimeEvolvedBPEstimator (TimeEvolvedBPEstimator.hpp:42-300, PropagateOperators
+ * AFQMCBasePropagator.cpp:538-654), FP64 engines, single determinant; needs the back-propagation ring
+ * (sfq_engine_enable_back_propagation with nbp >= the longest length).  Per walker and spin the
+ * operator states X, Y (identity at the anchor) and M (zero) evolve forward: te_evolve(nsteps) replays
+ * the last nsteps stored fields oldest first (X <- P1 e^{i vHS} P1 X, Y <- P1^-1 e^{i vHS^H} P1^-1 Y)
+ * and regularizes against the walkers' current Slater matrices S (Y <- S S^H Y, M += Y^H X,
+ * X <- X - S S^H X).  The measurements take the dressed Green's functions
+ * M + (PsiT X)^T (Gc conj(Y)) with the walker weights restored over restore_steps history steps
+ * (the caller passes bp, or 2 bp with extra path restoration, or 0), and the output layouts of
+ * sfq_engine_measure_rdm / sfq_engine_measure_observables.  The schedule (evolve the segment since
+ * the previous length, measure, re-anchor after the longest) is the caller's, as the reference's
+ * measure() does it. */
+int sfq_engine_enable_time_evolved_bp(sfq_engine_t e);
+int sfq_engine_te_anchor(sfq_engine_t e);
+int sfq_engine_te_evolve(sfq_engine_t e, int nsteps);
+int sfq_engine_measure_te_rdm(sfq_engine_t e, int restore_steps, void* one_rdm, void* diag_two_rdm);
+int sfq_engine_measure_te_observables(sfq_engine_t e, int restore_steps, void* two_rdm, void* spin_corr, int npair,
+                                      const int* pair_maps, void* pair_corr);
 
 /* Back propagation (BackPropEstimator.hpp, AFQMCBasePropagator.cpp:404-526), FP64 engines.
  * enable: every later step keeps, per walker, its fields in a ring of nbp slots and its weight factor

@@ -645,6 +645,16 @@ def build_P1(ham, vmf, dt, dense=False, drop=1e-8):
     return P
 
 
+def build_P1_inv(ham, vmf, dt, dense=False, drop=1e-8):
+    """generateP1(Pinv = true) (AFQMCBasePropagator.cpp:148-172): exp(+1/2 herm(H1)), the inverse
+    of P1 before the thresholding, thresholded like P1."""
+    H1 = hermitize(ham.one_body_propagator_matrix(dt, vmf)) * 0.5
+    P = exp_hermitian(H1)
+    if not dense:
+        P = np.where(np.abs(P) < drop, 0.0, P)
+    return P
+
+
 # --------------------------------------------------------------------------------------------
 # Fields (construct_X_kernel.hpp:34-87; probit.h:58-136; AFQMCBasePropagator.cpp:324-336)
 # --------------------------------------------------------------------------------------------
@@ -985,6 +995,7 @@ class Propagator:
         self.wfloor = weight_bound_floor
         self.wfrac = weight_bound_fraction
         self.vmf = vMF(ham, dt) if subtractMF else np.zeros(ham.Nc, np.complex128)
+        self.denseP1 = denseP1
         self.P1 = build_P1(ham, self.vmf, dt, dense=denseP1)
 
     def propagate(self, wset, Eshift, step, target_population=None, uniforms=None):
@@ -1319,6 +1330,103 @@ class BackPropEstimator:
         return out
 
 
+def _spin_trials(ham):
+    """Each spin block's trial (PsiT_s in the herm form) and its walker columns [c0, c1)."""
+    if isinstance(ham, CollinearHamiltonian):
+        return [(ham.PsiT_up, 0, ham.nup), (ham.PsiT_dn, ham.nup, ham.N)]
+    return [(ham.PsiT, 0, ham.PsiT.shape[0])]
+
+
+class TimeEvolvedBPEstimator:
+    """TimeEvolvedBPEstimator with the mixed estimator's observables (TimeEvolvedBPEstimator.hpp:42-300,
+    AFQMCBasePropagator::PropagateOperators :538-654), one rank, a single-determinant trial.
+
+    Per walker and spin, operator states X (-> c^+), Y (-> c) start from the identity and M from zero
+    at the anchor.  At a measurement length bp the segment since the previous length is replayed from
+    the stored fields, oldest first: X <- P1 e^{i vHS} P1 X and Y <- P1^-1 e^{i vHS^H} P1^-1 Y (the
+    adjoint of the inverse propagator), then, with the walkers' current Slater matrices S:
+    Y <- S S^H Y, M += Y^H X, X <- X - S S^H X.  The observables are measured on the dressed Green's
+    functions G_s = M_s + (PsiT_s X_s)^T (Gc_s conj(Y_s)), Gc_s the walkers' compact mixed density
+    matrix, with the walker weights restored over bp (2 bp with extra path restoration) steps and
+    coefficient 1 (one determinant).  The anchor moves to the current step once bp reaches the
+    longest length."""
+
+    def __init__(self, ham, prop, wset, steps=(2,), path_restoration=True, extra_path_restoration=False,
+                 observables=None):
+        self.ham, self.prop = ham, prop
+        self.steps = sorted(int(k) for k in steps)
+        self.restore = path_restoration or extra_path_restoration
+        self.extra = extra_path_restoration
+        self.observables = observables
+        wset.enable_back_propagation(self.steps[-1], ham.Nc)
+        self.P1inv = build_P1_inv(ham, prop.vmf, prop.dt, dense=prop.denseP1)
+        self.anchor(wset, -1)
+
+    def anchor(self, wset, step):
+        W, R = wset.size(), wset.SM.shape[1]
+        ns = len(_spin_trials(self.ham))
+        self.X = np.tile(np.eye(R, dtype=np.complex128), (ns, W, 1, 1))
+        self.Y = self.X.copy()
+        self.Mac = np.zeros_like(self.X)
+        self.bp_pos = step
+
+    def measure(self, wset, step):
+        bp = step - self.bp_pos
+        out = {}
+        if bp in self.steps:
+            i = self.steps.index(bp)
+            self.evolve(wset, bp - (self.steps[i - 1] if i > 0 else 0))
+            out = self._measure(wset, bp)
+        if bp >= self.steps[-1]:
+            self.anchor(wset, step)
+        return out
+
+    def evolve(self, wset, nsteps):
+        ham, prop = self.ham, self.prop
+        slot = (wset.hist_pos % wset.nbp + wset.nbp - nsteps) % wset.nbp
+        for _ in range(nsteps):
+            V = ham.vHS(wset.fields[:, slot], prop.dt)
+            Vh = np.conj(np.transpose(V, (0, 2, 1)))
+            for q in range(len(self.X)):
+                self.X[q] = ham.propagate(self.X[q], prop.P1, V, prop.order)
+                self.Y[q] = ham.propagate(self.Y[q], self.P1inv, Vh, prop.order)
+            slot = (slot + 1) % wset.nbp
+        for q, (_, c0, c1) in enumerate(_spin_trials(ham)):
+            if c1 == c0:  # an empty sector: S S^H = 0
+                self.Y[q] = 0.0
+                continue
+            S = wset.SM[:, :, c0:c1]
+            Sh = np.conj(np.transpose(S, (0, 2, 1)))
+            self.Y[q] = S @ (Sh @ self.Y[q])
+            self.Mac[q] += np.conj(np.transpose(self.Y[q], (0, 2, 1))) @ self.X[q]
+            self.X[q] = self.X[q] - S @ (Sh @ self.X[q])
+
+    def _measure(self, wset, bp):
+        ham = self.ham
+        weights = wset.weight.copy()
+        if self.restore:
+            hpos = wset.hist_pos
+            for _ in range(bp * (2 if self.extra else 1)):
+                hpos = wset.nhist - 1 if hpos == 0 else hpos - 1
+                weights = weights * wset.wfac[:, hpos]
+        blocks = []
+        for q, (P, c0, c1) in enumerate(_spin_trials(ham)):
+            G = self.Mac[q].copy()
+            if c1 > c0:
+                Gc, _ = mixed_density_matrix(P, wset.SM[:, :, c0:c1], compact=True)
+                G = G + np.transpose(P @ self.X[q], (0, 2, 1)) @ (Gc @ np.conj(self.Y[q]))
+            blocks.append(G)
+        G = np.stack(blocks, axis=1)
+        ones = np.ones(wset.size(), np.complex128)
+        one, two = _rdm_reduce([G], [ones], weights, _walker_kind(ham), ham.M)
+        pre = f"TimeEvolvedBP/Steps={bp}"
+        out = {f"{pre}/OneRDM": one, f"{pre}/DiagonalTwoRDM": two}
+        if self.observables:
+            obs = _observables_reduce([G], [ones], weights, _walker_kind(ham), ham.M, **self.observables)
+            out.update({f"{pre}/{k}": v for k, v in obs.items()})
+        return out
+
+
 def measure_mixed_rdms(ham, wset, observables=None):
     """MixedEstimator::measure with the OneRDM and DiagonalTwoRDM observables (MixedEstimator.hpp:37-147),
     one rank: per reference determinant d the full mixed G_d and its log overlap (one determinant per
@@ -1339,13 +1447,14 @@ def measure_mixed_rdms(ham, wset, observables=None):
 
 def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, measure_interval=10,
                equilibration_steps=0, relax=None, rank=0, mixed_interval=None, bp_steps=None, bp_ortho_interval=None,
-               observables=None, **prop_args):
+               observables=None, te_steps=None, te_extra_path_restoration=False, **prop_args):
     """execute_simulation + run_afqmc for one stage with HostRandomGenerator streams: walkers from
     the trial (NOMSD::initial_guess), Energy + seedPseudoEnergy, Eshift = averageEnergy, then the
     step loop.  Fields come from stream 1 (nwalk x nchol uniforms per step), the comb from stream 0.
     With mixed_interval the mixed estimator's one-body and diagonal two-body RDMs are measured too,
     with bp_steps (back propagation lengths) the back-propagated ones; observables (keyword
-    arguments of _observables_reduce) adds TwoRDM, SpinCorr and PairCorr to both estimators.
+    arguments of _observables_reduce) adds TwoRDM, SpinCorr and PairCorr to both estimators; with
+    te_steps the time-evolved back-propagation estimator runs (instead of bp_steps).
     Returns (initial Eshift, final Eshift, {observable: list of bins})."""
     from .mt19937 import HostRandomGenerator, split_seed
     walker_rng = HostRandomGenerator(split_seed(seed, rank, 0))
@@ -1357,6 +1466,9 @@ def run_seeded(ham, nwalk, dt, steps, seed, ortho_interval=10, pop_interval=10, 
     prop = Propagator(ham, dt, **prop_args)
     bp = BackPropEstimator(ham, prop, wset, bp_steps, bp_ortho_interval or ortho_interval,
                            observables=observables) if bp_steps else None
+    if te_steps:
+        bp = TimeEvolvedBPEstimator(ham, prop, wset, te_steps, extra_path_restoration=te_extra_path_restoration,
+                                    observables=observables)
     if relax is None:
         relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
     series = {}

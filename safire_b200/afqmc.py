@@ -372,9 +372,33 @@ class AfqmcEngine:
                                                       int(bool(path_restoration)), *args))
         return self._obs_dict(f"BackPropEstimator/Steps={int(nsteps)}", two, spin, pair)
 
+    # TimeEvolvedBPEstimator (sfq_engine_*_te_*): the operators evolve through the back-propagation ring
+    def enable_time_evolved_bp(self):
+        check(lib().sfq_engine_enable_time_evolved_bp(self.h))
+
+    def te_anchor(self):
+        check(lib().sfq_engine_te_anchor(self.h))
+
+    def te_evolve(self, nsteps):
+        check(lib().sfq_engine_te_evolve(self.h, int(nsteps)))
+
+    def measure_te_rdms(self, steps, restore_steps):
+        """The one-body and folded diagonal two-body RDMs of the evolved operators, the weights
+        restored over restore_steps (0: none)."""
+        one, two = self._rdm_buffers()
+        check(lib().sfq_engine_measure_te_rdm(self.h, int(restore_steps), one.ctypes.data, two.ctypes.data))
+        pre = f"TimeEvolvedBP/Steps={int(steps)}"
+        return {f"{pre}/OneRDM": one, f"{pre}/DiagonalTwoRDM": two}
+
+    def measure_te_observables(self, steps, restore_steps, two_rdm=True, spin_corr=True, pair_maps=None):
+        (two, spin, _, pair), args = self._obs_buffers(two_rdm, spin_corr, pair_maps)
+        check(lib().sfq_engine_measure_te_observables(self.h, int(restore_steps), *args))
+        return self._obs_dict(f"TimeEvolvedBP/Steps={int(steps)}", two, spin, pair)
+
     def run_with_streams(self, steps, Eshift, field_uniforms, comb_uniform, ortho_interval=10, pop_interval=10,
                          equilibration_steps=100, measure_interval=10, relax=None, step0=0, mixed_interval=None,
-                         bp_steps=None, bp_ortho_interval=None, path_restoration=True, observables=None):
+                         bp_steps=None, bp_ortho_interval=None, path_restoration=True, observables=None,
+                         te_steps=None, te_extra_path_restoration=False):
         """run_afqmc's step loop (run_afqmc.cpp:69-104) with the caller's random streams at the
         reference's two injection points: field_uniforms(n) returns the n = nwalk * nchol uniforms
         of a step (walker-major, assemble_X's sampleUniformFields) and comb_uniform() the comb's
@@ -382,7 +406,8 @@ class AfqmcEngine:
         a reference run.  Every measurement records EnergyEstimator::measure's observables
         (EnergyEstimator.h:51-100), every mixed_interval steps the mixed estimator's RDMs, and with
         bp_steps the back-propagated ones; observables (keyword arguments of measure_observables) adds
-        TwoRDM, SpinCorr and PairCorr to both estimators.
+        TwoRDM, SpinCorr and PairCorr to both estimators; te_steps runs TimeEvolvedBPEstimator's schedule
+        (TimeEvolvedBPEstimator.hpp:199-220) instead of bp_steps.
         Returns (Eshift, {observable: list of bins})."""
         if relax is None:
             relax = 1 - math.exp(-10.0 / equilibration_steps) if equilibration_steps > 1 else 1.0
@@ -391,6 +416,11 @@ class AfqmcEngine:
             bp_steps = sorted(int(k) for k in bp_steps)
             self.enable_back_propagation(bp_steps[-1])
             bp_pos = step0 - 1
+        if te_steps:
+            te_steps = sorted(int(k) for k in te_steps)
+            self.enable_back_propagation(te_steps[-1])
+            self.enable_time_evolved_bp()
+            te_pos = step0 - 1
         for step in range(step0, step0 + steps):
             u = np.ascontiguousarray(np.asarray(field_uniforms(self.W * self.Nc), np.float64).reshape(self.W, self.Nc))
             self.propagate_host(Eshift, step, uniforms_host=u)
@@ -428,6 +458,20 @@ class AfqmcEngine:
                     if step - bp_pos >= bp_steps[-1]:
                         self.bp_anchor()
                         bp_pos = step
+                if te_steps:
+                    bp = step - te_pos
+                    if bp in te_steps:
+                        i = te_steps.index(bp)
+                        self.te_evolve(bp - (te_steps[i - 1] if i > 0 else 0))
+                        restore = bp * (2 if te_extra_path_restoration else 1) if path_restoration else 0
+                        for k, v in self.measure_te_rdms(bp, restore).items():
+                            series.setdefault(k, []).append(v)
+                        if observables:
+                            for k, v in self.measure_te_observables(bp, restore, **observables).items():
+                                series.setdefault(k, []).append(v)
+                    if bp >= te_steps[-1]:
+                        self.te_anchor()
+                        te_pos = step
             else:
                 Eshift += relax * (self.averages()[0] - Eshift)
         return Eshift, series

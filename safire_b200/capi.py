@@ -107,6 +107,11 @@ _SIGS = {
     "sfq_engine_copy_walker": ([_VP, _I, _I], _I),
     "sfq_engine_walker_row_elems": ([_VP], ctypes.c_long),
     "sfq_engine_measure_observables": ([_VP, _VP, _VP, _I, _VP, _VP], _I),
+    "sfq_engine_enable_time_evolved_bp": ([_VP], _I),
+    "sfq_engine_te_anchor": ([_VP], _I),
+    "sfq_engine_te_evolve": ([_VP, _I], _I),
+    "sfq_engine_measure_te_rdm": ([_VP, _I, _VP, _VP], _I),
+    "sfq_engine_measure_te_observables": ([_VP, _I, _VP, _VP, _I, _VP, _VP], _I),
     "sfq_engine_measure_bp_observables": ([_VP, _I, _I, _I, _VP, _VP, _I, _VP, _VP], _I),
     "sfq_engine_pack_walkers": ([_VP, _VP, _I, _VP], _I),
     "sfq_engine_unpack_walkers": ([_VP, _VP, _I, _VP], _I),

@@ -234,6 +234,33 @@ __global__ void bp_init_refs_kernel(const cplx* PsiT, int ndet, int W, int Mr, i
   }
 }
 // V[w] <- -V[w]^H in place: exp(i (-V^H)) = exp(-i V^H), the adjoint Taylor propagator (propagate.hpp:56-57)
+// time-evolved back propagation helpers: X[b] = I (R x R) for every matrix b; out = conj(in)
+__global__ void set_identity_batched_kernel(cplx* X, long nmat, int R) {
+  const long n = nmat * R * R;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const long k = e % ((long)R * R);
+    X[e] = mk(k / R == k % R ? 1.0 : 0.0, 0.0);
+  }
+}
+__global__ void conj_copy_kernel(const cplx* in, cplx* out, long n) {
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+    out[e] = cconj(in[e]);
+}
+// V[w] <- V[w]^H (M x M, in place)
+__global__ void adjoint_kernel(cplx* V, int M) {
+  cplx* Vw = V + (long)blockIdx.y * M * M;
+  const long npairs = (long)M * (M + 1) / 2;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < npairs; e += (long)gridDim.x * blockDim.x) {
+    int i = int((sqrt(8.0 * e + 1.0) - 1.0) / 2.0);
+    while ((long)i * (i + 1) / 2 > e) --i;
+    while ((long)(i + 1) * (i + 2) / 2 <= e) ++i;
+    const int j = int(e - (long)i * (i + 1) / 2);  // j <= i
+    const cplx a = Vw[(long)i * M + j], b = Vw[(long)j * M + i];
+    Vw[(long)i * M + j] = cconj(b);
+    Vw[(long)j * M + i] = cconj(a);
+  }
+}
+
 __global__ void neg_adjoint_kernel(cplx* V, int M) {
   cplx* Vw = V + (long)blockIdx.y * M * M;
   const long npairs = (long)M * (M + 1) / 2;
@@ -463,6 +490,8 @@ struct Engine {
   double* v0 = nullptr;
   double* vmf = nullptr;
   double* P1 = nullptr;
+  double* H1m = nullptr;    // -1/2 herm(H1): P1 = exp(H1m)
+  double* P1inv = nullptr;  // exp(-H1m), built when the time-evolved back propagation is enabled
   // walkers
   cplx* SM = nullptr;
   cplx* props = nullptr;
@@ -913,6 +942,8 @@ struct Engine {
         std::swap(cur, nxt);
       }
       SFQ_CUDA_TRY(cudaMemcpyAsync(P1, cur, sizeof(double) * MM, cudaMemcpyDeviceToDevice, st));
+      if (!H1m) SFQ_CUDA_TRY(cudaMalloc(&H1m, sizeof(double) * MM));  // for P1^-1 (time-evolved BP)
+      SFQ_CUDA_TRY(cudaMemcpyAsync(H1m, H, sizeof(double) * MM, cudaMemcpyDeviceToDevice, st));
       SFQ_CUDA_TRY(cudaFreeAsync(scr, st));
       if (!p.denseP1) {
         if ((rc = threshold_real(P1, MM, 1e-8, st))) return rc;
@@ -1130,6 +1161,218 @@ struct Engine {
     const int* maps = nullptr;  // host (npair, M)
     std::vector<cplx> two, spin, pair;
   };
+  // --- time-evolved back propagation (TimeEvolvedBPEstimator.hpp, PropagateOperators
+  // AFQMCBasePropagator.cpp:538-654) ----------------------------------------------------------
+  // the operator states X (-> c^+), Y (-> c) and the stabilization sums M per spin and walker,
+  // (ns, W, R, R) with R = npol M, evolved forward through the fields the back-propagation ring keeps
+  cplx *te_X = nullptr, *te_Y = nullptr, *te_M = nullptr, *te_scr = nullptr;
+  // out = exp(sgn H) by scaling and squaring (Taylor to order 18 at norm <= 1/4), as P1 is built
+  int expm_real(const double* H, double sgn, double* out) {
+    int rc;
+    const long MM = (long)M * M;
+    std::vector<double> hh(MM);
+    SFQ_CUDA_TRY(cudaMemcpyAsync(hh.data(), H, sizeof(double) * MM, cudaMemcpyDeviceToHost, st));
+    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    double norm1 = 0.0;
+    for (int k = 0; k < M; ++k) {
+      double a = 0.0;
+      for (int i = 0; i < M; ++i) a += std::fabs(hh[size_t(i) * M + k]);
+      norm1 = std::fmax(norm1, a);
+    }
+    int sq = 0;
+    while (norm1 / std::ldexp(1.0, sq) > 0.25) ++sq;
+    const double scale = sgn * std::ldexp(1.0, -sq);
+    double* scr = nullptr;
+    SFQ_CUDA_TRY(cudaMallocAsync((void**)&scr, sizeof(double) * 4 * MM, st));
+    double *Pa = scr, *Pb = scr + MM, *ta = scr + 2 * MM, *tb = scr + 3 * MM;
+    SFQ_CUDA_TRY(cudaMemsetAsync(Pa, 0, sizeof(double) * MM, st));
+    SFQ_CUDA_TRY(cudaMemsetAsync(ta, 0, sizeof(double) * MM, st));
+    if ((rc = add_identity(Pa, M, 1.0, st)) || (rc = add_identity(ta, M, 1.0, st))) return rc;
+    for (int k = 1; k <= 18; ++k) {
+      GemmDesc d;  // tb = (scale/k) H ta; Pa += tb
+      d.M = M; d.N = M; d.K = M;
+      d.A = H; d.sAm = M; d.sAk = 1;
+      d.B = ta; d.sBk = M; d.sBn = 1;
+      d.C = tb; d.sCm = M; d.sCn = 1;
+      d.S = Pa;
+      d.alpha = mk(scale / double(k), 0.0);
+      if ((rc = gemm_f64(d, st))) return rc;
+      std::swap(ta, tb);
+    }
+    double* cur = Pa;
+    double* nxt = Pb;
+    for (int q = 0; q < sq; ++q) {
+      GemmDesc d;
+      d.M = M; d.N = M; d.K = M;
+      d.A = cur; d.sAm = M; d.sAk = 1;
+      d.B = cur; d.sBk = M; d.sBn = 1;
+      d.C = nxt; d.sCm = M; d.sCn = 1;
+      if ((rc = gemm_f64(d, st))) return rc;
+      std::swap(cur, nxt);
+    }
+    SFQ_CUDA_TRY(cudaMemcpyAsync(out, cur, sizeof(double) * MM, cudaMemcpyDeviceToDevice, st));
+    SFQ_CUDA_TRY(cudaFreeAsync(scr, st));
+    if (!p.denseP1 && (rc = threshold_real(out, MM, 1e-8, st))) return rc;
+    return SFQ_OK;
+  }
+  int te_enable() {
+    int rc;
+    if (!nbp) return record_error(SFQ_ERR_ARG, "time-evolved back propagation needs the field ring: enable back propagation first");
+    if (ndet > 1) return record_error(SFQ_ERR_UNSUPPORTED, "time-evolved back propagation is measured for single determinants");
+    if (te_X) return SFQ_OK;
+    const long RR = (long)Mr * Mr, nmat = (long)rdm_nspin() * W;
+    SFQ_CUDA_TRY(cudaMalloc(&te_X, sizeof(cplx) * nmat * RR));
+    SFQ_CUDA_TRY(cudaMalloc(&te_Y, sizeof(cplx) * nmat * RR));
+    SFQ_CUDA_TRY(cudaMalloc(&te_M, sizeof(cplx) * nmat * RR));
+    SFQ_CUDA_TRY(cudaMalloc(&te_scr, sizeof(cplx) * 4 * (size_t)W * RR));
+    SFQ_CUDA_TRY(cudaMalloc(&P1inv, sizeof(double) * (size_t)M * M));
+    if ((rc = expm_real(H1m, -1.0, P1inv))) return rc;  // generateP1(true): exp(+1/2 herm(H1))
+    return te_anchor();
+  }
+  // setAnchor (TimeEvolvedBPEstimator.hpp:282-287): X = Y = I, M = 0
+  int te_anchor() {
+    if (!te_X) return record_error(SFQ_ERR_ARG, "time-evolved back propagation is not enabled");
+    const long RR = (long)Mr * Mr, nmat = (long)rdm_nspin() * W;
+    set_identity_batched_kernel<<<1184, 256, 0, st>>>(te_X, nmat, Mr);
+    SFQ_LAUNCHED();
+    set_identity_batched_kernel<<<1184, 256, 0, st>>>(te_Y, nmat, Mr);
+    SFQ_LAUNCHED();
+    SFQ_CUDA_TRY(cudaMemsetAsync(te_M, 0, sizeof(cplx) * nmat * RR, st));
+    return SFQ_OK;
+  }
+  // columns [c0, c0 + nel) of the walkers' Slater matrices: the spin block s
+  void spin_cols(int s, int& c0, int& nel) const {
+    c0 = (collinear && s == 1) ? nup : 0;
+    nel = collinear ? (s == 0 ? nup : N - nup) : N;
+  }
+  // PropagateOperators over the last nsteps stored fields, oldest first: X <- P1 e^{i vHS} P1 X,
+  // Y <- P1^-1 e^{i vHS^H} P1^-1 Y (the adjoint of the inverse step), then per spin with the walkers'
+  // Slater matrices S: Y <- S S^H Y, M += Y^H X, X <- X - S S^H X
+  int te_evolve(int nsteps) {
+    int rc;
+    if (!te_X) return record_error(SFQ_ERR_ARG, "time-evolved back propagation is not enabled");
+    if (nsteps <= 0 || nsteps > nbp) return record_error(SFQ_ERR_ARG, "operators evolved over %d steps (ring %d)", nsteps, nbp);
+    const long MM = (long)M * M, RR = (long)Mr * Mr;
+    const int ns = rdm_nspin();
+    cplx* TM = te_scr;
+    cplx* T1x = te_scr + (size_t)W * RR;
+    cplx* T2x = te_scr + 2 * (size_t)W * RR;
+    int slot = (hist_pos % nbp + nbp - nsteps) % nbp;
+    for (int i = 0; i < nsteps; ++i, slot = (slot + 1) % nbp) {
+      SFQ_CUDA_TRY(cudaMemcpy2DAsync(X, sizeof(cplx) * Nc, bp_fields + (long)slot * Nc, sizeof(cplx) * nbp * Nc,
+                                     sizeof(cplx) * Nc, W, cudaMemcpyDeviceToDevice, st));
+      if (sym) {
+        if ((rc = ops::vhs_rows(Lp, P, X, Vp, W, Nc, std::sqrt(p.dt), st))) return rc;
+        if ((rc = unpack_symmetric(Vp, W, M, V, st))) return rc;
+      } else if ((rc = ops::vhs(Likn, X, V, W, M, Nc, std::sqrt(p.dt), st))) {
+        return rc;
+      }
+      for (int q = 0; q < ns; ++q)
+        if ((rc = ops::propagate(te_X + (size_t)q * W * RR, P1, false, V, W, M, Mr, p.taylor_order, TM, T1x, T2x, st,
+                                 npol)))
+          return rc;
+      adjoint_kernel<<<dim3(md_grid(MM / 2 + M), W), 256, 0, st>>>(V, M);
+      SFQ_LAUNCHED();
+      for (int q = 0; q < ns; ++q)
+        if ((rc = ops::propagate(te_Y + (size_t)q * W * RR, P1inv, false, V, W, M, Mr, p.taylor_order, TM, T1x, T2x,
+                                 st, npol)))
+          return rc;
+    }
+    for (int q = 0; q < ns; ++q) {
+      int c0, nel;
+      spin_cols(q, c0, nel);
+      cplx* Xs = te_X + (size_t)q * W * RR;
+      cplx* Ys = te_Y + (size_t)q * W * RR;
+      cplx* Ms = te_M + (size_t)q * W * RR;
+      if (nel == 0) {  // an empty sector: S S^H = 0
+        SFQ_CUDA_TRY(cudaMemsetAsync(Ys, 0, sizeof(cplx) * W * RR, st));
+        continue;
+      }
+      cplx* SY = TM;  // (W, nel, R)
+      auto sh = [&](const cplx* B) {  // SY = S^H B
+        GemmDesc g;
+        g.M = nel; g.N = Mr; g.K = Mr; g.batch = W;
+        g.A = SM + c0; g.sAm = 1; g.sAk = N; g.sAb = (long)Mr * N; g.a_cplx = true; g.conj_a = true;
+        g.B = B; g.sBk = Mr; g.sBn = 1; g.sBb = RR; g.b_cplx = true;
+        g.C = SY; g.sCm = Mr; g.sCn = 1; g.sCb = (long)nel * Mr;
+        return gemm_f64(g, st);
+      };
+      auto s_sy = [&](cplx* C, cplx alpha, cplx beta) {  // C = alpha S SY + beta C
+        GemmDesc g;
+        g.M = Mr; g.N = Mr; g.K = nel; g.batch = W;
+        g.A = SM + c0; g.sAm = N; g.sAk = 1; g.sAb = (long)Mr * N; g.a_cplx = true;
+        g.B = SY; g.sBk = Mr; g.sBn = 1; g.sBb = (long)nel * Mr; g.b_cplx = true;
+        g.C = C; g.sCm = Mr; g.sCn = 1; g.sCb = RR;
+        g.alpha = alpha; g.beta = beta;
+        return gemm_f64(g, st);
+      };
+      if ((rc = sh(Ys)) || (rc = s_sy(Ys, mk(1.0, 0.0), mk(0.0, 0.0)))) return rc;
+      GemmDesc g;  // M += Y^H X
+      g.M = Mr; g.N = Mr; g.K = Mr; g.batch = W;
+      g.A = Ys; g.sAm = 1; g.sAk = Mr; g.sAb = RR; g.a_cplx = true; g.conj_a = true;
+      g.B = Xs; g.sBk = Mr; g.sBn = 1; g.sBb = RR; g.b_cplx = true;
+      g.C = Ms; g.sCm = Mr; g.sCn = 1; g.sCb = RR; g.beta = mk(1.0, 0.0);
+      if ((rc = gemm_f64(g, st))) return rc;
+      if ((rc = sh(Xs)) || (rc = s_sy(Xs, mk(-1.0, 0.0), mk(1.0, 0.0)))) return rc;
+    }
+    return SFQ_OK;
+  }
+  // the Green's functions the evolved operators dress (constructTimeEvolvedMeasurementInputs,
+  // TimeEvolvedBPEstimator.hpp:42-140): Gf[w][s] = M_s + (PsiT_s X_s)^T (Gc_s conj(Y_s)), Gc the
+  // walkers' compact mixed density matrix
+  int te_green(cplx* Gf) {
+    int rc;
+    const long RR = (long)Mr * Mr;
+    const int ns = rdm_nspin();
+    if ((rc = density(ovtmp))) return rc;
+    cplx* Yc = te_scr;                        // conj(Y_s) (W, R, R)
+    cplx* XR = te_scr + (size_t)W * RR;       // PsiT_s X_s (W, nel, R)
+    cplx* GY = te_scr + 2 * (size_t)W * RR;   // Gc_s conj(Y_s) (W, nel, R)
+    for (int q = 0; q < ns; ++q) {
+      int c0, nel;
+      spin_cols(q, c0, nel);
+      SFQ_CUDA_TRY(cudaMemcpy2DAsync(Gf + q * RR, sizeof(cplx) * ns * RR, te_M + (size_t)q * W * RR,
+                                     sizeof(cplx) * RR, sizeof(cplx) * RR, W, cudaMemcpyDeviceToDevice, st));
+      if (nel == 0) continue;
+      conj_copy_kernel<<<1184, 256, 0, st>>>(te_Y + (size_t)q * W * RR, Yc, (long)W * RR);
+      SFQ_LAUNCHED();
+      GemmDesc g;  // GY = Gc_s conj(Y_s)
+      g.M = nel; g.N = Mr; g.K = Mr; g.batch = W;
+      g.A = G + (long)c0 * Mr; g.sAm = Mr; g.sAk = 1; g.sAb = (long)N * Mr; g.a_cplx = true;
+      g.B = Yc; g.sBk = Mr; g.sBn = 1; g.sBb = RR; g.b_cplx = true;
+      g.C = GY; g.sCm = Mr; g.sCn = 1; g.sCb = (long)nel * Mr;
+      if ((rc = gemm_f64(g, st))) return rc;
+      GemmDesc h;  // XR = PsiT_s X_s
+      h.M = nel; h.N = Mr; h.K = Mr; h.batch = W;
+      h.A = PsiT + (long)c0 * Mr; h.sAm = Mr; h.sAk = 1; h.sAb = 0; h.a_cplx = true;
+      h.B = te_X + (size_t)q * W * RR; h.sBk = Mr; h.sBn = 1; h.sBb = RR; h.b_cplx = true;
+      h.C = XR; h.sCm = Mr; h.sCn = 1; h.sCb = (long)nel * Mr;
+      if ((rc = gemm_f64(h, st))) return rc;
+      GemmDesc k;  // Gf_s += XR^T GY
+      k.M = Mr; k.N = Mr; k.K = nel; k.batch = W;
+      k.A = XR; k.sAm = 1; k.sAk = Mr; k.sAb = (long)nel * Mr; k.a_cplx = true;
+      k.B = GY; k.sBk = Mr; k.sBn = 1; k.sBb = (long)nel * Mr; k.b_cplx = true;
+      k.C = Gf + q * RR; k.sCm = Mr; k.sCn = 1; k.sCb = ns * RR; k.beta = mk(1.0, 0.0);
+      if ((rc = gemm_f64(k, st))) return rc;
+    }
+    return SFQ_OK;
+  }
+  // the measurement: the weights restored over restore steps (TimeEvolvedBPEstimator.hpp:245-256),
+  // the RDMs and observables of the dressed Green's functions, divided by their sum
+  int te_measure(int restore, std::vector<cplx>& one, std::vector<cplx>& two, ObsSpec* obs) {
+    if (!te_X) return record_error(SFQ_ERR_ARG, "time-evolved back propagation is not enabled");
+    if (restore < 0 || restore > nhist) return record_error(SFQ_ERR_ARG, "weights restored over %d steps (history %d)", restore, nhist);
+    inv_cached = false;
+    SFQ_CUDA_TRY(cudaMemcpyAsync(bp_wt, props + (long)P_WEIGHT * W, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
+    int h = hist_pos;
+    for (int k = 0; k < restore; ++k) {
+      h = h == 0 ? nhist - 1 : h - 1;
+      bp_restore_kernel<<<(W + 127) / 128, 128, 0, st>>>(bp_wt, bp_wfac + h, nhist, W);
+      SFQ_LAUNCHED();
+    }
+    return rdm_measure(bp_wt, false, one, two, obs, true);
+  }
+
   // --- back propagation (WalkerSetBase::resize_bp, BackPropEstimator) ---------------------------
   // per walker: the anchored walkers, a ring of the last nbp steps' fields (slot hist_pos % nbp),
   // the weight factors of the last 3 nbp steps (slot hist_pos); all travel with population control
@@ -1240,7 +1483,7 @@ struct Engine {
   // each walker's propagated references against its anchored matrix, the overlaps with conj of the
   // references' QR log dets, constructBPMeasurementInputs, BackPropEstimator.hpp:36-110)
   int rdm_measure(const cplx* weight, bool bp, std::vector<cplx>& one, std::vector<cplx>& two,
-                  ObsSpec* obs = nullptr) {
+                  ObsSpec* obs = nullptr, bool te = false) {
     int rc;
     if (obs && (rc = check_obs(*obs))) return rc;
     const int ns = rdm_nspin(), nb = rdm_nblk();
@@ -1307,9 +1550,9 @@ struct Engine {
       SFQ_LAUNCHED();
       return SFQ_OK;
     };
-    for (int d = 0; d < ndet; ++d)
+    for (int d = 0; d < ndet && !te; ++d)
       if ((rc = factor(d, false))) return rc;
-    {
+    if (!te) {
       cplx* dcic = nullptr;
       SFQ_CUDA_TRY(cudaMallocAsync((void**)&dcic, sizeof(cplx) * ndet, st));
       SFQ_CUDA_TRY(cudaMemcpyAsync(dcic, cic.data(), sizeof(cplx) * ndet, cudaMemcpyHostToDevice, st));
@@ -1319,11 +1562,15 @@ struct Engine {
       SFQ_CUDA_TRY(cudaStreamSynchronize(st));  // cic lives until the copy is done
     }
     for (int d = 0; d < ndet; ++d) {
-      if ((rc = factor(d, true))) return rc;
-      if ((rc = ops::green_compact(T, B, G, W, Mr, N, st))) return rc;
+      if (te) {  // the operators' dressed G, a single determinant: coefficient 1
+        if ((rc = te_green(Gf))) return rc;
+        SFQ_CUDA_TRY(cudaMemcpyAsync(wc, weight, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
+      }
+      if (!te && (rc = factor(d, true))) return rc;
+      if (!te && (rc = ops::green_compact(T, B, G, W, Mr, N, st))) return rc;
       // the full G of each spin block: Gf[w][s] = Aeff[rows s]^T Gc[w][rows s] (density_matrix.hpp:580-600),
       // Aeff = PsiT_d (shared) or the walker's conj(Refs^T)
-      for (int s = 0; s < ns; ++s) {
+      for (int s = 0; s < ns && !te; ++s) {
         const int r0 = collinear ? (s == 0 ? 0 : nup) : 0, r1 = collinear ? (s == 0 ? nup : N) : N;
         if (r1 == r0) {  // an empty spin sector has a zero G
           SFQ_CUDA_TRY(cudaMemset2DAsync(Gf + s * MM, sizeof(cplx) * ns * MM, 0, sizeof(cplx) * MM, W, st));
@@ -1341,8 +1588,10 @@ struct Engine {
         g.C = Gf + s * MM; g.sCm = Mr; g.sCn = 1; g.sCb = ns * MM;
         if ((rc = gemm_f64(g, st))) return rc;
       }
-      rdm_coeff_kernel<<<(W + 127) / 128, 128, 0, st>>>(ovd + (long)d * W, cic[d], shift, tot, weight, W, wc);
-      SFQ_LAUNCHED();
+      if (!te) {
+        rdm_coeff_kernel<<<(W + 127) / 128, 128, 0, st>>>(ovd + (long)d * W, cic[d], shift, tot, weight, W, wc);
+        SFQ_LAUNCHED();
+      }
       GemmDesc g;  // one[s,i,j] += sum_w wc[w] Gf[w,s,i,j] (onerdm.hpp:56-61)
       g.M = 1; g.N = int(ns * MM); g.K = W; g.batch = 1;
       g.A = wc; g.sAm = W; g.sAk = 1; g.a_cplx = true;
@@ -2729,7 +2978,8 @@ int sfq_engine_destroy(sfq_engine_t h) {
   if (e.h_pinned) cudaFreeHost(e.h_pinned);
   if (e.rdm_buf) cudaFree(e.rdm_buf);
   for (void* q : {(void*)e.bp_SMN, (void*)e.bp_fields, (void*)e.bp_wfac, (void*)e.bp_refs, (void*)e.bp_ldet,
-                  (void*)e.bp_wt})
+                  (void*)e.bp_wt, (void*)e.te_X, (void*)e.te_Y, (void*)e.te_M, (void*)e.te_scr, (void*)e.P1inv,
+                  (void*)e.H1m})
     if (q) cudaFree(q);
   if (e.st) cudaStreamDestroy(e.st);
   delete h;
@@ -2850,6 +3100,21 @@ int sfq_engine_enable_back_propagation(sfq_engine_t h, int nbp) {
   return h->e.enable_bp(nbp);
 }
 
+int sfq_engine_enable_time_evolved_bp(sfq_engine_t h) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.te_enable();
+}
+
+int sfq_engine_te_anchor(sfq_engine_t h) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.te_anchor();
+}
+
+int sfq_engine_te_evolve(sfq_engine_t h, int nsteps) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  return h->e.te_evolve(nsteps);
+}
+
 int sfq_engine_bp_anchor(sfq_engine_t h) {
   if (!h) return record_error(SFQ_ERR_ARG, "null engine");
   return h->e.bp_anchor();
@@ -2865,6 +3130,15 @@ int sfq_engine_measure_bp_rdm(sfq_engine_t h, int nsteps, int ortho_interval, in
   std::vector<cplx> one, two;
   int rc;
   if ((rc = e.measure_bp(nsteps, ortho_interval, path_restoration != 0, one, two))) return rc;
+  return fold_rdms(e, one, two, one_rdm, diag_two_rdm);
+}
+
+int sfq_engine_measure_te_rdm(sfq_engine_t h, int restore_steps, void* one_rdm, void* diag_two_rdm) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  std::vector<cplx> one, two;
+  int rc;
+  if ((rc = e.te_measure(restore_steps, one, two, nullptr))) return rc;
   return fold_rdms(e, one, two, one_rdm, diag_two_rdm);
 }
 
@@ -2917,6 +3191,19 @@ int sfq_engine_measure_bp_observables(sfq_engine_t h, int nsteps, int ortho_inte
   if ((rc = obs_request(e, o, two_rdm, spin_corr, npair, pair_maps, pair_corr))) return rc;
   std::vector<cplx> one, two;
   if ((rc = e.measure_bp(nsteps, ortho_interval, path_restoration != 0, one, two, &o))) return rc;
+  obs_out(o, two_rdm, spin_corr, pair_corr);
+  return SFQ_OK;
+}
+
+int sfq_engine_measure_te_observables(sfq_engine_t h, int restore_steps, void* two_rdm, void* spin_corr, int npair,
+                                      const int* pair_maps, void* pair_corr) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null engine");
+  Engine& e = h->e;
+  Engine::ObsSpec o;
+  int rc;
+  if ((rc = obs_request(e, o, two_rdm, spin_corr, npair, pair_maps, pair_corr))) return rc;
+  std::vector<cplx> one, two;
+  if ((rc = e.te_measure(restore_steps, one, two, &o))) return rc;
   obs_out(o, two_rdm, spin_corr, pair_corr);
   return SFQ_OK;
 }

@@ -2,7 +2,8 @@
 (sfq_engine_measure_observables / sfq_engine_measure_bp_observables) against the oracle's
 restatement of Observables/twordm.hpp, spincorr.hpp and paircorr.hpp, measured along the replay of
 the reference's seeded BH runs (the same schedule as the recorded one- and two-body RDMs): CLOSED,
-COLLINEAR and NONCOLLINEAR walkers, each observable where the reference measures it."""
+COLLINEAR and NONCOLLINEAR walkers, each observable where the reference measures it; and the
+time-evolved back-propagation estimator (sfq_engine_te_*) against the oracle's restatement."""
 import numpy as np
 import pytest
 
@@ -74,3 +75,33 @@ def test_observables_refused_where_the_reference_refuses_them():
         e.measure_observables(two_rdm=True, spin_corr=True)  # the estimators are FP64
     assert ex.value.code == 3
     e.close()
+
+
+@pytest.mark.parametrize("case,extra", [("bh_rhf_closed", False), ("bh_uhf_collinear", True),
+                                        ("bh_uhf_noncollinear", False)])
+def test_time_evolved_back_propagation_matches_the_oracle(case, extra):
+    """TimeEvolvedBPEstimator over lengths 2 and 4 (two segments per window, combs and
+    orthogonalizations inside it) along the seeded BH replay: the one-body and diagonal two-body
+    RDMs and the other observables of the dressed Green's functions, against the oracle's
+    restatement (with extra path restoration for the collinear case)."""
+    snap = snapshot(case)
+    st = snap["settings"]
+    M = snap["hcore"].shape[0]
+    nonc = st["walker_type"] == "NONCOLLINEAR"
+    obs = dict(two_rdm=not nonc, spin_corr=True, pair_maps=_maps(M) if st["walker_type"] != "CLOSED" else None)
+    kw = dict(ortho_interval=st["ortho_interval"], pop_interval=3, measure_interval=st["measure_interval"])
+    eng = A.AfqmcEngine(engine_system(snap), st["nwalk"], dt=st["dt"], seed=0, precision=capi.PRECISION_FP64)
+    walker_rng = HostRandomGenerator(split_seed(st["seed"], 0, 0))
+    field_rng = HostRandomGenerator(split_seed(st["seed"], 0, 1))
+    _, series = eng.run_with_streams(12, eng.init(), field_rng.uniforms, lambda: walker_rng.uniforms(1)[0],
+                                     equilibration_steps=0, te_steps=[2, 4], te_extra_path_restoration=extra,
+                                     observables=obs, **kw)
+    eng.close()
+    _, _, oracle = O.run_seeded(oracle_hamiltonian(snap), st["nwalk"], st["dt"], 12, st["seed"], te_steps=[2, 4],
+                                te_extra_path_restoration=extra, observables=obs, **kw)
+    names = [k for k in series if k.startswith("TimeEvolvedBP/")]
+    assert len(names) == 2 * (2 + sum(1 for v in (obs["two_rdm"], obs["spin_corr"], obs["pair_maps"] is not None) if v))
+    for k in names:
+        a, b = np.asarray(series[k]), np.asarray(oracle[k])
+        assert a.shape == b.shape and len(a) == 3, k  # lengths 2 and 4 of windows at steps 1, 5, 9
+        assert np.max(np.abs(a - b)) <= 1e-10 * max(1.0, float(np.max(np.abs(b)))), k
