@@ -3,9 +3,9 @@
     python -m safire_b200.batched        # 24 systems, M = 48, 64, ..., 320 (cycled), N = M/4,
                                          # Nchol = 5M, walkers log-uniform in [64, 512]
 
-Every system gets a resident mixed-precision engine (3 BF16 planes: FP32-class products, the
-LU / log det / QR / weights in FP64) whose tile widths are chosen by the autotuner
-(sfq_engine_autotune).  The engines form one group (sfq_group_*): one block of every system is one
+Every system gets a resident engine of the chosen precision (default INT8X3: int8-slice products
+with exact integer accumulation; `--precision mixed-fp32`: 3 BF16 planes, its tile widths chosen
+by the autotuner, sfq_engine_autotune), the LU / log det / QR / weights in FP64.  The engines form one group (sfq_group_*): one block of every system is one
 CUDA graph launch, the systems' blocks arranged in lanes that run side by side (members of a lane
 in turn), the lane count picked by timing real blocks (EngineGroup.tune_lanes).  The block is 20
 steps (orthogonalization every 5, population control and one local-energy measurement at the end,
@@ -79,11 +79,14 @@ def main():
     ap.add_argument("--lanes", default="1,2,3,4,6,8,0", help="lane counts the schedule tuner tries (0: all)")
     ap.add_argument("--no-tune", action="store_true", help="keep the built-in tiles")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--precision", default="int8x3", choices=["int8x3", "mixed-fp32", "mixed"])
     a = ap.parse_args()
     specs, walkers = uneven_specs(a.systems)
     blk = dict(ortho_interval=BLOCK["ortho_interval"], pop_interval=a.steps, equilibration_steps=0,
                measure_interval=a.steps, relax=BLOCK["relax"], steer=True)
-    prec = capi.PRECISION_MIXED_FP32
+    prec = {"int8x3": capi.PRECISION_INT8X3, "mixed-fp32": capi.PRECISION_MIXED_FP32,
+            "mixed": capi.PRECISION_MIXED}[a.precision]
+    tunable = prec != capi.PRECISION_INT8X3  # the int8-slice products run fixed tiles
 
     # resident mixed engines, autotuned
     t0 = time.time()
@@ -91,7 +94,7 @@ def main():
     for i, (spec, W) in enumerate(zip(specs, walkers)):
         e = _make_engine(spec, W, 1000 + i, prec)
         Esh.append(e.init())
-        if not a.no_tune:
+        if tunable and not a.no_tune:
             t = e.autotune()
             tiles.append(t.choice())
             w = (1, 1, 1, 6, 1)  # per step: G, vbias, vHS, six Taylor terms, the P1 pair
@@ -173,7 +176,8 @@ def main():
                     f"[64, 512] (total {sum(walkers)}); blocks of {a.steps} steps (ortho every "
                     f"{blk['ortho_interval']}, population control + 1 measurement per block, steered Eshift)",
         "systems": [{"M": s.M, "N": s.N, "Nc": s.Nc, "W": w} for s, w in zip(specs, walkers)],
-        "precision": "mixed: 3 BF16 planes (FP32-class products), LU/log det/QR/weights FP64",
+        "precision": {"int8x3": "int8 slices x3 (exact int32 accumulation)", "mixed-fp32": "3 BF16 planes",
+                      "mixed": "2 BF16 planes"}[a.precision] + "; LU/log det/QR/weights FP64",
         "group": {"value": rate(group_s), "ms_per_block": 1e3 * group_s / a.blocks, "lanes": lanes,
                   "lane_seconds_per_block": {str(k): v for k, v in lane_times.items()},
                   "how": "one CUDA graph per block; members in `lanes` chains side by side (0: one per member)"},
