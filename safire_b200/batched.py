@@ -189,7 +189,7 @@ def main():
                      "step_products_us_tuned": tune["us_tuned"]} if not a.no_tune else None,
         "accuracy": acc, "max_abs_energy_same_walkers_mHa": max((abs(r["energy_same_walkers_mHa"]) for r in acc),
                                                                 default=None),
-        "resident_bytes": foot, "build_seconds": build_s, "dt": "1e-4 * 256 / M, clipped to [5e-5, 1e-3]",
+        "resident_bytes": foot, "build_seconds": build_s, "dt": "5e-5 * 256 / M, clipped to [2.5e-5, 5e-4]",
         "data": "synthetic (seeded random Cholesky tensors and trial)",
         "timing": "host clock around the timed blocks, each ending with its results on the host",
     }
