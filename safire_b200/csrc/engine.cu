@@ -555,6 +555,7 @@ struct Engine {
   int8_t* Xq_q[3] = {};  int* Xq_e = nullptr;   // fields, planar rows (c, w) over n
   int8_t* V_q[3] = {};   int* V_e = nullptr;  int* V_emax = nullptr;  // V[w][c][i][k]: Vr, Vi, -Vi; e per (w, i)
   int8_t* A_q[2][3] = {};  int* A_e[2] = {};  // walker operand: rows (c, r)
+  unsigned long long* pl_emax = nullptr;  // 2W scratch row maxima for slicing G - G_T
   cplx* GT_c = nullptr;  // the trial's own G (N, M) and force bias (Nc), FP64
   cplx* vbT = nullptr;
   float* Cp = nullptr;  // FP32 output of the walker-shaped products, planar (2 W N, M)
@@ -728,6 +729,7 @@ struct Engine {
           {(void**)&Xq_e, ie * 2 * W}, {(void**)&V_e, ie * W * M}, {(void**)&V_emax, ie * W * M},
           {(void**)&A_e[0], ie * R}, {(void**)&A_e[1], ie * R},
           {(void**)&GT_c, c * (size_t)N * M}, {(void**)&vbT, c * (size_t)Nc},
+          {(void**)&pl_emax, sizeof(unsigned long long) * 2 * (size_t)W},
           {(void**)&Cvb, sizeof(float) * i8_vb_ks * 2 * (size_t)W * Nc},
           {(void**)&Cv, sizeof(float) * 2 * W * vrows},
           {(void**)&Sacc, sizeof(float) * 2 * R * M},
@@ -2155,7 +2157,7 @@ struct Engine {
     const double sdt = std::sqrt(p.dt);
     ph_begin(SFQ_PH_DENSITY);
     if ((rc = density(nullptr))) return rc;
-    if ((rc = islice_rows_planar(G, W, (long)N * M, nslices, Gv_q, ld_nm, Gv_e, st, GT_c))) return rc;
+    if ((rc = islice_rows_planar(G, W, (long)N * M, nslices, Gv_q, ld_nm, Gv_e, st, GT_c, pl_emax))) return rc;
     ph_end(SFQ_PH_DENSITY);
     ph_begin(SFQ_PH_VBIAS);
     const long part = 2L * W * Nc;

@@ -77,9 +77,11 @@ int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st);
 int islice_rows_real(const double* src, long R, long K, long lds, int nslices, int8_t* const* q, long ld, int* e,
                      cudaStream_t st);
 // complex rows split into planar rows: row c * R + r holds part c (0 re, 1 im) of src[r * K + k]
-// (minus sub[k] when sub is given), with its own exponent
+// (minus sub[k] when sub is given), with its own exponent; with emax (2 R scratch values) rows longer
+// than 8192 are spread over blocks (a max pass, then a slicing pass), else one block per row
 int islice_rows_planar(const cplx* src, long R, long K, int nslices, int8_t* const* q, long ld, int* e,
-                       cudaStream_t st, const cplx* sub = nullptr);
+                       cudaStream_t st, const cplx* sub = nullptr,
+                       unsigned long long* emax = nullptr);
 // walkers SM (W, M, N) complex -> rows (c, w, a) over orbitals j (the P1 product's A operand), one
 // exponent per (w, a) for both parts: e[w * N + a]; planar (may be null): the same rows in FP32,
 // row stride M

@@ -214,6 +214,48 @@ __global__ void rows_planar_kernel(const cplx* src, long R, long K, int ns, Q q,
   }
 }
 
+// long rows split over blocks: pass 1, each chunk's largest |re| and |im| into the row's maxima
+// (non-negative doubles order like their bits, so a 64-bit atomic max is exact); pass 2 slices
+constexpr long kPlanarChunk = 4096;
+__global__ void __launch_bounds__(256) planar_max_kernel(const cplx* src, long R, long K, const cplx* sub,
+                                                         unsigned long long* emax) {
+  __shared__ double sh[32];
+  const long r = blockIdx.y, k0 = blockIdx.x * kPlanarChunk;
+  const long k1 = k0 + kPlanarChunk < K ? k0 + kPlanarChunk : K;
+  const cplx* x = src + r * K;
+  double mr = 0.0, mi = 0.0;
+  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    const cplx z = sub ? csub(x[k], sub[k]) : x[k];
+    mr = fmax(mr, fabs(z.x));
+    mi = fmax(mi, fabs(z.y));
+  }
+  mr = block_max(mr, sh);
+  mi = block_max(mi, sh);
+  if (threadIdx.x == 0) {
+    atomicMax(emax + r, (unsigned long long)__double_as_longlong(mr));
+    atomicMax(emax + R + r, (unsigned long long)__double_as_longlong(mi));
+  }
+}
+__global__ void __launch_bounds__(256) planar_slice_kernel(const cplx* src, long R, long K, const cplx* sub,
+                                                           const unsigned long long* emax, int ns, Q q, long ld,
+                                                           int* e) {
+  const long r = blockIdx.y, k0 = blockIdx.x * kPlanarChunk;
+  const long k1 = k0 + kPlanarChunk < ld ? k0 + kPlanarChunk : ld;
+  const int er = row_exponent(__longlong_as_double((long long)emax[r]));
+  const int ei = row_exponent(__longlong_as_double((long long)emax[R + r]));
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    e[r] = er;
+    e[R + r] = ei;
+  }
+  const double sr = pow2d(-er), si = pow2d(-ei);
+  const cplx* x = src + r * K;
+  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    const cplx z = k < K ? (sub ? csub(x[k], sub[k]) : x[k]) : mk(0.0, 0.0);
+    put(q, ns, r * ld + k, z.x, sr);
+    put(q, ns, (R + r) * ld + k, z.y, si);
+  }
+}
+
 // walkers: the largest |re|, |im| of each (w, a) over the orbitals (threads along a: coalesced)
 __global__ void walkers_max_kernel(const cplx* SM, int M, int N, int* e) {
   __shared__ double sh[8][33];
@@ -578,10 +620,20 @@ int islice_rows_real(const double* src, long R, long K, long lds, int nslices, i
 }
 
 int islice_rows_planar(const cplx* src, long R, long K, int nslices, int8_t* const* q, long ld, int* e,
-                       cudaStream_t st, const cplx* sub) {
+                       cudaStream_t st, const cplx* sub, unsigned long long* emax) {
   if (int rc = check_slices(nslices, q, ld)) return rc;
   if (R <= 0) return SFQ_OK;
   if (ld < K || R > 2147483647L) return record_error(SFQ_ERR_SHAPE, "islice_rows_planar: sizes");
+  if (emax && K > 2 * kPlanarChunk && R <= 65535) {  // long rows: spread each row over blocks
+    SFQ_CUDA_TRY(cudaMemsetAsync(emax, 0, sizeof(unsigned long long) * 2 * R, st));
+    planar_max_kernel<<<dim3(unsigned((K + kPlanarChunk - 1) / kPlanarChunk), unsigned(R)), 256, 0, st>>>(src, R, K,
+                                                                                                           sub, emax);
+    SFQ_LAUNCHED();
+    planar_slice_kernel<<<dim3(unsigned((ld + kPlanarChunk - 1) / kPlanarChunk), unsigned(R)), 256, 0, st>>>(
+        src, R, K, sub, emax, nslices, qptrs(q), ld, e);
+    SFQ_LAUNCHED();
+    return SFQ_OK;
+  }
   rows_planar_kernel<<<unsigned(R), K >= 4096 ? 512 : 256, 0, st>>>(src, R, K, nslices, qptrs(q), ld, e, sub);
   SFQ_LAUNCHED();
   return SFQ_OK;
