@@ -38,7 +38,7 @@ extern "C" {
 #define SFQ_ERR_RANK 11           /* CholeskyQR: a walker lost rank (non-positive pivot) */
 
 /* version of this ABI */
-int sfq_abi_version(void); /* 12 */
+int sfq_abi_version(void); /* 13 */
 const char* sfq_last_error(void);
 /* kernels this library has launched in this process (all threads, all devices) */
 unsigned long long sfq_launch_count(void);
@@ -268,7 +268,8 @@ typedef struct {
  * biases every product by the same relative shrink; these carry no such bias.  The force bias, the
  * fields, vHS, the P1 products and Taylor terms, and the exchange tensor of the energy run this way;
  * the Green's function, LU / log det, overlaps, orthogonalization, walker update and all sums stay
- * FP64.  Needs a real trial and nmo <= 1024; any nchol; CLOSED or COLLINEAR walkers. */
+ * FP64.  Needs a real trial and nmo <= 1024; any nchol; CLOSED, COLLINEAR or NONCOLLINEAR walkers (a
+ * spinor walker's two (nmo, nel) components share its vHS and P1). */
 #define SFQ_PRECISION_INT8X3 3     /* 3 slices: 2^-24 of each row's largest entry, 6 int8 products */
 #define SFQ_PRECISION_INT8X2 4     /* 2 slices: 2^-16 of each row's largest entry, 3 int8 products */
 
@@ -457,6 +458,12 @@ int sfq_engine_tiles(sfq_engine_t e, sfq_tiles_t* tiles);
  * status[i] (0, SFQ_ERR_WEIGHT_COLLAPSE, SFQ_ERR_TIMEOUT), nmeas[i] measurements of 10 doubles at
  * meas + 10 * max_meas * i.  The call returns the first member error.  The engines stay usable on
  * their own between group blocks; one block of a group runs at a time (_async, then _result).
+ * sfq_group_set_fused(g, 1) (members in one int8-slice precision, SFQ_PRECISION_INT8X3 or _INT8X2,
+ * on one block schedule) instead interleaves the members' steps stage by stage: each stage's
+ * tensor-core products of ALL members (force bias, vHS, the P1 products and Taylor terms, the
+ * exchange tensor's chunks) run as ONE persistent grouped launch over their concatenated tile
+ * lists, the work between them on the members' streams side by side.  Each tile is computed as the
+ * member's own launch computes it: the results equal the members' blocks run alone, bit for bit.
  * No counterpart in the reference, which runs one system per process. */
 typedef struct sfq_group_s* sfq_group_t;
 int sfq_group_create(sfq_group_t* g, const sfq_engine_t* engines, int n);
@@ -466,6 +473,7 @@ int sfq_group_block(sfq_group_t g, const sfq_run_params_t* rps, double* Eshift, 
 int sfq_group_block_async(sfq_group_t g, const sfq_run_params_t* rps, const double* Eshift);
 int sfq_group_block_query(sfq_group_t g);
 int sfq_group_set_lanes(sfq_group_t g, int lanes);
+int sfq_group_set_fused(sfq_group_t g, int fused);
 int sfq_group_block_result(sfq_group_t g, double* Eshift, int* status, double* meas, int max_meas, int* nmeas);
 
 /* ---- serving loop: continuous batching of propagation blocks over resident systems -----------

@@ -574,6 +574,7 @@ class EngineGroup:
         check(lib().sfq_group_create(ctypes.byref(h), arr, len(self.engines)))
         self.h = h
         self.lanes = 0
+        self.fused = False
 
     def close(self):
         if self.h:
@@ -632,20 +633,37 @@ class EngineGroup:
         check(lib().sfq_group_set_lanes(self.h, int(lanes)))
         self.lanes = int(lanes)
 
-    def tune_lanes(self, steps, Eshift, step0=0, candidates=(1, 2, 3, 4, 6, 8, 0), **kw):
-        """Schedule autotuner: run real blocks with each lane count (one to capture its graph, one
-        timed) and keep the fastest.  Returns (Eshift, next step0, {lanes: seconds per block})."""
+    def set_fused(self, on=True):
+        """Fused schedule (int8-slice members on one block schedule): the members' steps stage by
+        stage, each stage's tensor-core products of all members as one grouped launch."""
+        check(lib().sfq_group_set_fused(self.h, 1 if on else 0))
+        self.fused = bool(on)
+
+    def _schedule(self, c):
+        if c == "fused":
+            self.set_fused(True)
+        else:
+            self.set_fused(False)
+            self.set_lanes(c)
+
+    def tune_lanes(self, steps, Eshift, step0=0, candidates=("fused", 1, 2, 3, 4, 6, 8, 0), **kw):
+        """Schedule autotuner: run real blocks with each schedule ("fused" where every member runs an
+        int8-slice precision, else a lane count), one to capture its graph and one timed, and keep
+        the fastest.  Returns (Eshift, next step0, {schedule: seconds per block})."""
         times = {}
         es = Eshift
-        for L in candidates:
-            if L > len(self.engines):
+        int8 = all(e.params.precision in (capi.PRECISION_INT8X3, capi.PRECISION_INT8X2) for e in self.engines)
+        for c in candidates:
+            if c == "fused" and not int8:
                 continue
-            self.set_lanes(L)
+            if c != "fused" and c > len(self.engines):
+                continue
+            self._schedule(c)
             es, _st, _m = self.run_block(steps, es, step0=step0, **kw)
             step0 += steps
             t0 = time.perf_counter()
             es, _st, _m = self.run_block(steps, es, step0=step0, **kw)
-            times[L] = time.perf_counter() - t0
+            times[c] = time.perf_counter() - t0
             step0 += steps
-        self.set_lanes(min(times, key=times.get))
+        self._schedule(min(times, key=times.get))
         return es, step0, times

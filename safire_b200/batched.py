@@ -5,9 +5,11 @@
 
 Every system gets a resident engine of the chosen precision (default INT8X3: int8-slice products
 with exact integer accumulation; `--precision mixed-fp32`: 3 BF16 planes, its tile widths chosen
-by the autotuner, sfq_engine_autotune), the LU / log det / QR / weights in FP64.  The engines form one group (sfq_group_*): one block of every system is one
-CUDA graph launch, the systems' blocks arranged in lanes that run side by side (members of a lane
-in turn), the lane count picked by timing real blocks (EngineGroup.tune_lanes).  The block is 20
+by the autotuner, sfq_engine_autotune), the LU / log det / QR / weights in FP64.  The engines form
+one group (sfq_group_*): one block of every system is one CUDA graph launch, scheduled either fused
+(INT8X3: the systems' steps stage by stage, each stage's tensor-core products of all systems as ONE
+grouped launch) or in lanes that run side by side (members of a lane in turn), the schedule picked
+by timing real blocks (EngineGroup.tune_lanes).  The block is 20
 steps (orthogonalization every 5, population control and one local-energy measurement at the end,
 Eshift steered every step).  Three timings of the same blocks:
 
@@ -76,7 +78,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20, help="steps per block")
     ap.add_argument("--blocks", type=int, default=3, help="timed blocks")
     ap.add_argument("--warmup", type=int, default=2, help="untimed blocks per timing (the first captures graphs)")
-    ap.add_argument("--lanes", default="1,2,3,4,6,8,0", help="lane counts the schedule tuner tries (0: all)")
+    ap.add_argument("--lanes", default="fused,1,2,3,4,6,8,0",
+                    help="schedules the tuner tries: 'fused' (int8-slice precisions: each stage's products of all "
+                         "systems as one grouped launch) and lane counts (0: one lane per system)")
     ap.add_argument("--no-tune", action="store_true", help="keep the built-in tiles")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--precision", default="int8x3", choices=["int8x3", "mixed-fp32", "mixed"])
@@ -130,11 +134,13 @@ def main():
     es = np.asarray(Esh0, np.float64)
     step0 = 0
     lane_times = {}
-    cands = [int(x) for x in a.lanes.split(",")]
+    cands = [x if x == "fused" else int(x) for x in a.lanes.split(",")]
+    if a.precision != "int8x3":
+        cands = [c for c in cands if c != "fused"]
     if len(cands) > 1:
         es, step0, lane_times = grp.tune_lanes(a.steps, es, step0=step0, candidates=cands, **blk)
     else:
-        grp.set_lanes(cands[0])
+        grp._schedule(cands[0])
     for _ in range(a.warmup):
         es, st, _m = grp.run_block(a.steps, es, step0=step0, **blk)
         step0 += a.steps
@@ -143,7 +149,7 @@ def main():
         es, st, _m = grp.run_block(a.steps, es, step0=step0, **blk)
         step0 += a.steps
     group_s = time.perf_counter() - t0
-    lanes = grp.lanes
+    lanes = "fused" if grp.fused else grp.lanes
     grp.close()
 
     # FP64 engines one at a time: timing, then accuracy against the mixed engine
@@ -180,7 +186,9 @@ def main():
                       "mixed": "2 BF16 planes"}[a.precision] + "; LU/log det/QR/weights FP64",
         "group": {"value": rate(group_s), "ms_per_block": 1e3 * group_s / a.blocks, "lanes": lanes,
                   "lane_seconds_per_block": {str(k): v for k, v in lane_times.items()},
-                  "how": "one CUDA graph per block; members in `lanes` chains side by side (0: one per member)"},
+                  "how": "one CUDA graph per block; 'fused': the members' steps stage by stage, each stage's "
+                         "int8-slice products of all members as one grouped launch; else members in `lanes` "
+                         "chains side by side (0: one per member)"},
         "mixed_serial": {"value": rate(serial_s), "ms_per_block": 1e3 * serial_s / a.blocks},
         "fp64_serial": {"value": rate(fp64_s), "ms_per_block": 1e3 * fp64_s / a.blocks} if fp64_s else None,
         "speedup_group_vs_fp64_serial": fp64_s / group_s if fp64_s else None,

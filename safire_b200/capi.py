@@ -156,6 +156,7 @@ _SIGS = {
     "sfq_group_block_async": ([_VP, ctypes.POINTER(RunParams), _VP], _I),
     "sfq_group_block_query": ([_VP], _I),
     "sfq_group_set_lanes": ([_VP, _I], _I),
+    "sfq_group_set_fused": ([_VP, _I], _I),
     "sfq_group_block_result": ([_VP, _VP, _VP, _VP, _I, _VP], _I),
     "sfq_server_create": ([ctypes.POINTER(_VP), ctypes.POINTER(ServerParams)], _I),
     "sfq_server_destroy": ([_VP], _I),

@@ -543,9 +543,11 @@ struct Engine {
   int ldh = 0;          // padded half of the walker operand rows (re, im): M rounded up to 64
   int* gemm_err = nullptr;
   // exact-accumulation mode (nslices > 0): int8 fixed-point slices of every tensor-core operand, one
-  // exponent per row (islice.cuh); rows of the walker-shaped arrays are r = w * N + a
+  // exponent per row (islice.cuh); rows of the walker-shaped arrays are r = (w npol + q) N + a (the
+  // spinor components q of a NONCOLLINEAR walker are two (M, N) blocks that V and P1 act on alike),
+  // and k runs over the Mr = npol M rows of the G-shaped arrays
   int nslices = 0;
-  long ld_m = 0, ld_nm = 0, ld_nc = 0;  // slice row strides (bytes): M, N*M, Nc rounded up to 16
+  long ld_m = 0, ld_mr = 0, ld_nm = 0, ld_nc = 0;  // slice row strides (bytes): M, Mr, N*Mr, Nc rounded up to 16
   int8_t* Lv_q[3] = {};  int* Lv_e = nullptr;   // Lnak, rows n over (a, k): the force bias's B
   int8_t* Le_q[3] = {};  int* Le_e = nullptr;   // Lnak, rows (n, a) over k: the exchange tensor's B
   int8_t* Lh_q[3] = {};  int* Lh_e = nullptr;   // L, rows (i, k) (packed pairs when symmetric) over n: vHS's B
@@ -556,7 +558,7 @@ struct Engine {
   int8_t* V_q[3] = {};   int* V_e = nullptr;  int* V_emax = nullptr;  // V[w][c][i][k]: Vr, Vi, -Vi; e per (w, i)
   int8_t* A_q[2][3] = {};  int* A_e[2] = {};  // walker operand: rows (c, r)
   unsigned long long* pl_emax = nullptr;  // 2W scratch row maxima for slicing G - G_T
-  cplx* GT_c = nullptr;  // the trial's own G (N, M) and force bias (Nc), FP64
+  cplx* GT_c = nullptr;  // the trial's own G (N, Mr) and force bias (Nc), FP64
   cplx* vbT = nullptr;
   float* Cp = nullptr;  // FP32 output of the walker-shaped products, planar (2 W N, M)
   int i8_vb_bn = 160, i8_vb_ks = 1, i8_bn = 160, i8_half = 80;
@@ -709,15 +711,15 @@ struct Engine {
     }
     if (mixed && nslices) {
       plan_i8();
-      const long R = (long)W * N, vrows = sym ? P : MM;
+      const long R = (long)W * npol * N, RG = (long)W * N, vrows = sym ? P : MM;
       std::vector<Item> mx;
       for (int q = 0; q < nslices; ++q) {
         mx.push_back({(void**)&Lv_q[q], (size_t)Nc * ld_nm});
-        mx.push_back({(void**)&Le_q[q], (size_t)Nc * N * ld_m});
+        mx.push_back({(void**)&Le_q[q], (size_t)Nc * N * ld_mr});
         mx.push_back({(void**)&Lh_q[q], (size_t)vrows * ld_nc});
         mx.push_back({(void**)&P1_q[q], (size_t)M * ld_m});
         mx.push_back({(void**)&Gv_q[q], (size_t)2 * W * ld_nm});
-        mx.push_back({(void**)&Ge_q[q], (size_t)2 * R * ld_m});
+        mx.push_back({(void**)&Ge_q[q], (size_t)2 * RG * ld_mr});
         mx.push_back({(void**)&Xq_q[q], (size_t)2 * W * ld_nc});
         mx.push_back({(void**)&V_q[q], (size_t)W * 3 * M * ld_m});
         for (int b = 0; b < 2; ++b) mx.push_back({(void**)&A_q[b][q], (size_t)2 * R * ld_m});
@@ -725,10 +727,10 @@ struct Engine {
       const size_t ie = sizeof(int);
       std::vector<Item> mx2 = {
           {(void**)&Lv_e, ie * Nc}, {(void**)&Le_e, ie * Nc * N}, {(void**)&Lh_e, ie * vrows},
-          {(void**)&P1_e, ie * M}, {(void**)&Gv_e, ie * 2 * W}, {(void**)&Ge_e, ie * 2 * R},
+          {(void**)&P1_e, ie * M}, {(void**)&Gv_e, ie * 2 * W}, {(void**)&Ge_e, ie * 2 * RG},
           {(void**)&Xq_e, ie * 2 * W}, {(void**)&V_e, ie * W * M}, {(void**)&V_emax, ie * W * M},
           {(void**)&A_e[0], ie * R}, {(void**)&A_e[1], ie * R},
-          {(void**)&GT_c, c * (size_t)N * M}, {(void**)&vbT, c * (size_t)Nc},
+          {(void**)&GT_c, c * (size_t)N * Mr}, {(void**)&vbT, c * (size_t)Nc},
           {(void**)&pl_emax, sizeof(unsigned long long) * 2 * (size_t)W},
           {(void**)&Cvb, sizeof(float) * i8_vb_ks * 2 * (size_t)W * Nc},
           {(void**)&Cv, sizeof(float) * 2 * W * vrows},
@@ -954,24 +956,24 @@ struct Engine {
     // exact-accumulation mode: int8 slices of the resident real tensors, and the trial's own G and
     // force bias (NOMSD::vMF before its real part is taken)
     if (mixed && nslices) {
-      const long NM = (long)N * M;
+      const long NM = (long)N * Mr;
       {
-        std::vector<cplx> psi(size_t(M) * N);  // PsiT^H (M x N)
+        std::vector<cplx> psi(size_t(Mr) * N);  // PsiT^H (Mr x N)
         for (int a = 0; a < N; ++a)
-          for (int i = 0; i < M; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * M + i]);
-        SFQ_CUDA_TRY(cudaMemcpyAsync(SM2, psi.data(), sizeof(cplx) * M * N, cudaMemcpyHostToDevice, st));
-        if ((rc = ops::overlap_matrix(PsiT, true, SM2, T, 1, M, N, st))) return rc;
+          for (int i = 0; i < Mr; ++i) psi[size_t(i) * N + a] = cconj(h_PsiT[size_t(a) * Mr + i]);
+        SFQ_CUDA_TRY(cudaMemcpyAsync(SM2, psi.data(), sizeof(cplx) * NM, cudaMemcpyHostToDevice, st));
+        if ((rc = ops::overlap_matrix(PsiT, true, SM2, T, 1, Mr, N, st))) return rc;
         if (collinear && (rc = ops::mask_cross_spin(T, 1, N, spin_split(), st))) return rc;
         if ((rc = lu_logdet(T, (long)N * N, 1, N, ovtmp, false, 1.0, true, st))) return rc;
-        if ((rc = ops::green_compact(T, SM2, G, 1, M, N, st))) return rc;
+        if ((rc = ops::green_compact(T, SM2, G, 1, Mr, N, st))) return rc;
         SFQ_CUDA_TRY(cudaMemcpyAsync(GT_c, G, sizeof(cplx) * NM, cudaMemcpyDeviceToDevice, st));
-        if ((rc = ops::vbias(G, Lnak, false, X, 1, N, M, Nc, vb_scale(), st))) return rc;
+        if ((rc = ops::vbias(G, Lnak, false, X, 1, N, Mr, Nc, vb_scale(), st))) return rc;
         SFQ_CUDA_TRY(cudaMemcpyAsync(vbT, X, sizeof(cplx) * Nc, cudaMemcpyDeviceToDevice, st));
         SFQ_CUDA_TRY(cudaStreamSynchronize(st));
       }
       const double* Ln = (const double*)Lnak;
       if ((rc = islice_rows_real(Ln, Nc, NM, NM, nslices, Lv_q, ld_nm, Lv_e, st))) return rc;
-      if ((rc = islice_rows_real(Ln, (long)Nc * N, M, M, nslices, Le_q, ld_m, Le_e, st))) return rc;
+      if ((rc = islice_rows_real(Ln, (long)Nc * N, Mr, Mr, nslices, Le_q, ld_mr, Le_e, st))) return rc;
       if (sym) {
         double* packed = nullptr;
         SFQ_CUDA_TRY(cudaMallocAsync(&packed, sizeof(double) * P * Nc, st));
@@ -2080,7 +2082,8 @@ struct Engine {
   // M, then the widest), the force bias split along K to fill whole waves of SMs
   void plan_i8() {
     ld_m = round16(M);
-    ld_nm = round16((long)N * M);
+    ld_mr = round16(Mr);
+    ld_nm = round16((long)N * Mr);
     ld_nc = round16(Nc);
     int best = 0;
     long best_pad = 1L << 40;
@@ -2095,7 +2098,7 @@ struct Engine {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device);
     const long tiles = (long)((2 * W + 127) / 128) * ((Nc + i8_vb_bn - 1) / i8_vb_bn);
-    const long kt = ((long)N * M + 127) / 128;
+    const long kt = ((long)N * Mr + 127) / 128;
     double best_eff = 0.0;
     i8_vb_ks = 1;
     for (int ks = 1; ks <= 64 && ks * 4 <= kt; ++ks) {
@@ -2123,27 +2126,28 @@ struct Engine {
   }
   // C (2R, M) planar (+)= A (rows (c, r), one exponent per r) times (P1 - I)^T: the two P1 products,
   // whose identity part the caller adds
-  int i8_p1(int buf, float* C, bool accumulate) {
-    const long R = (long)W * N;
+  IsliceGemmDesc i8_p1(int buf, float* C, bool accumulate) const {
+    const long R = (long)W * npol * N;
     IsliceGemmDesc d = i8_desc();
     d.M = int(2 * R); d.N = M; d.K = M;
     d.A = i8_operand(A_q[buf], 2 * R, ld_m, A_e[buf], 0, 0, R);
     d.B = i8_operand(P1_q, M, ld_m, P1_e);
     d.bn = i8_bn;
     d.C = C; d.ldc = M; d.accumulate = accumulate;
-    return islice_gemm(d, st);
+    return d;
   }
-  // one Taylor product of every walker: Cp = A [[Vr, -Vi], [Vi, Vr]]^T, planar [c][w][a][j]
-  int i8_taylor(int buf) {
-    const long R = (long)W * N;
+  // one Taylor product of every walker: Cp = A [[Vr, -Vi], [Vi, Vr]]^T, planar [c][w][(q, a)][j]
+  // (a NONCOLLINEAR walker's two components are one batch item of 2N rows against its V)
+  IsliceGemmDesc i8_taylor(int buf) const {
+    const long Nw = (long)npol * N, R = W * Nw;
     IsliceGemmDesc d = i8_desc();
-    d.M = N; d.N = M; d.K = M; d.batch = W;
-    d.A = i8_operand(A_q[buf], N, ld_m, A_e[buf], (long)N * ld_m, N);
+    d.M = int(Nw); d.N = M; d.K = M; d.batch = W;
+    d.A = i8_operand(A_q[buf], Nw, ld_m, A_e[buf], Nw * ld_m, Nw);
     for (int s2 = 0; s2 < 3; ++s2) d.a_im[s2] = A_q[buf][s2] ? A_q[buf][s2] + R * ld_m : nullptr;
     d.B = i8_operand(V_q, 3L * M, ld_m, V_e, 3L * M * ld_m, M);
     d.cplx_half = i8_half;
     d.C = Cp; d.ldc = M; d.sCc = R * M;
-    return islice_gemm(d, st);
+    return d;
   }
 
   // AFQMCBasePropagator::Propagate with the products from int8 slices (exact accumulation): force
@@ -2151,71 +2155,93 @@ struct Engine {
   // (T = (i/k) C, S += T, slicing) round to nearest; G, LU / overlaps and the walker update in FP64.
   // The force bias is the trial's own (FP64, setup) plus that of G - G_trial from slices: G's rows
   // are dominated by entries near the trial's, which would set the fixed-point scale of the rest.
-  int propagate_i8(double Eshift, unsigned long long step, const double* uniforms) {
+  //
+  // Written as stages s = 0, 1, ...: stage s records its work on the stream and hands back, in *d,
+  // the int8-slice product that follows it (not launched), *more = false after the last stage.  Run
+  // alone, each product is launched right after its stage; a group of engines runs stage s of
+  // every member, then all their products as one launch (Group::record_fused).
+  int i8_cur = 0;  // Taylor operand buffer between stages
+  int propagate_i8_stage(int s, double Eshift, unsigned long long step, const double* uniforms, IsliceGemmDesc* d,
+                         bool* more) {
     int rc;
-    const long R = (long)W * N;
-    const double sdt = std::sqrt(p.dt);
-    ph_begin(SFQ_PH_DENSITY);
-    if ((rc = density(nullptr))) return rc;
-    if ((rc = islice_rows_planar(G, W, (long)N * M, nslices, Gv_q, ld_nm, Gv_e, st, GT_c, pl_emax))) return rc;
-    ph_end(SFQ_PH_DENSITY);
-    ph_begin(SFQ_PH_VBIAS);
-    const long part = 2L * W * Nc;
-    {
-      IsliceGemmDesc d = i8_desc();
-      d.M = 2 * W; d.N = Nc; d.K = int((long)N * M);
-      d.A = i8_operand(Gv_q, 2L * W, ld_nm, Gv_e);
-      d.B = i8_operand(Lv_q, Nc, ld_nm, Lv_e);
-      d.bn = i8_vb_bn; d.ksplit = i8_vb_ks; d.sCk = part;
-      d.C = Cvb; d.ldc = Nc;
-      if ((rc = islice_gemm(d, st))) return rc;
+    const int Wb = W * npol;  // (M, N) walker blocks
+    const long R = (long)Wb * N;
+    const int order = p.taylor_order;
+    *more = true;
+    if (s == 0) {
+      ph_begin(SFQ_PH_DENSITY);
+      if ((rc = density(nullptr))) return rc;
+      if ((rc = islice_rows_planar(G, W, (long)N * Mr, nslices, Gv_q, ld_nm, Gv_e, st, GT_c, pl_emax))) return rc;
+      ph_end(SFQ_PH_DENSITY);
+      ph_begin(SFQ_PH_VBIAS);
+      *d = i8_desc();
+      d->M = 2 * W; d->N = Nc; d->K = int((long)N * Mr);
+      d->A = i8_operand(Gv_q, 2L * W, ld_nm, Gv_e);
+      d->B = i8_operand(Lv_q, Nc, ld_nm, Lv_e);
+      d->bn = i8_vb_bn; d->ksplit = i8_vb_ks; d->sCk = 2L * W * Nc;
+      d->C = Cvb; d->ldc = Nc;
+      return SFQ_OK;
     }
-    if ((rc = mixed_reduce_planar_to_cplx(Cvb, i8_vb_ks, part, W, Nc, vb_scale(), X, st, vbT))) return rc;
-    ph_end(SFQ_PH_VBIAS);
-    ph_begin(SFQ_PH_FIELDS);
-    FieldParams fp;
-    fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
-    fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms; fp.step_dev = dev_mode ? d_step : nullptr;
-    if (uni_wait) {
-      SFQ_CUDA_TRY(cudaStreamWaitEvent(st, uni_wait, 0));
-      uni_wait = nullptr;
+    if (s == 1) {
+      if ((rc = mixed_reduce_planar_to_cplx(Cvb, i8_vb_ks, 2L * W * Nc, W, Nc, vb_scale(), X, st, vbT))) return rc;
+      ph_end(SFQ_PH_VBIAS);
+      ph_begin(SFQ_PH_FIELDS);
+      FieldParams fp;
+      fp.nwalk = W; fp.nchol = Nc; fp.vbias_bound = p.vbias_bound; fp.free_projection = p.free_projection;
+      fp.seed = p.seed; fp.step = step; fp.uniforms = uniforms; fp.step_dev = dev_mode ? d_step : nullptr;
+      if (uni_wait) {
+        SFQ_CUDA_TRY(cudaStreamWaitEvent(st, uni_wait, 0));
+        uni_wait = nullptr;
+      }
+      if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
+      ph_end(SFQ_PH_FIELDS);
+      ph_begin(SFQ_PH_VHS);
+      if ((rc = islice_rows_planar(X, W, Nc, nslices, Xq_q, ld_nc, Xq_e, st))) return rc;
+      ph_begin(SFQ_PH_VHS_GEMM);
+      const long vcols = sym ? P : (long)M * M;
+      *d = i8_desc();
+      d->M = 2 * W; d->N = int(vcols); d->K = Nc;
+      d->A = i8_operand(Xq_q, 2L * W, ld_nc, Xq_e);
+      d->B = i8_operand(Lh_q, vcols, ld_nc, Lh_e);
+      d->bn = i8_bn;
+      d->C = Cv; d->ldc = vcols; d->alpha = std::sqrt(p.dt);
+      return SFQ_OK;
     }
-    if ((rc = assemble_x(X, vmf, hw, mf, fp, st))) return rc;
-    ph_end(SFQ_PH_FIELDS);
-    ph_begin(SFQ_PH_VHS);
-    if ((rc = islice_rows_planar(X, W, Nc, nslices, Xq_q, ld_nc, Xq_e, st))) return rc;
-    ph_begin(SFQ_PH_VHS_GEMM);
-    const long vcols = sym ? P : (long)M * M;
-    {
-      IsliceGemmDesc d = i8_desc();
-      d.M = 2 * W; d.N = int(vcols); d.K = Nc;
-      d.A = i8_operand(Xq_q, 2L * W, ld_nc, Xq_e);
-      d.B = i8_operand(Lh_q, vcols, ld_nc, Lh_e);
-      d.bn = i8_bn;
-      d.C = Cv; d.ldc = vcols; d.alpha = sdt;
-      if ((rc = islice_gemm(d, st))) return rc;
+    if (s == 2) {
+      ph_end(SFQ_PH_VHS_GEMM);
+      if ((rc = islice_build_v(Cv, W, M, sym, nslices, V_q, ld_m, V_e, V_emax, st))) return rc;
+      ph_end(SFQ_PH_VHS);
+      ph_begin(SFQ_PH_PROPAGATE);
+      inv_cached = false;
+      // S = P1 W = W + (P1 - I) W; then T_k = (i/k) V T_{k-1}, S += T_k for k = 1..order; SM = S + (P1 - I) S
+      if ((rc = islice_walkers(SM, Wb, M, N, nslices, A_q[0], ld_m, A_e[0], Sacc, st))) return rc;
+      *d = i8_p1(0, Cp, false);
+      return SFQ_OK;
     }
-    ph_end(SFQ_PH_VHS_GEMM);
-    if ((rc = islice_build_v(Cv, W, M, sym, nslices, V_q, ld_m, V_e, V_emax, st))) return rc;
-    ph_end(SFQ_PH_VHS);
-    ph_begin(SFQ_PH_PROPAGATE);
-    inv_cached = false;
-    // S = P1 W = W + (P1 - I) W; then T_k = (i/k) V T_{k-1}, S += T_k for k = 1..order; SM = S + (P1 - I) S
-    if ((rc = islice_walkers(SM, W, M, N, nslices, A_q[0], ld_m, A_e[0], Sacc, st))) return rc;
-    if ((rc = i8_p1(0, Cp, false))) return rc;
-    if ((rc = islice_taylor_update(Cp, Sacc, R, M, 0, true, nslices, A_q[1], ld_m, A_e[1], st))) return rc;
-    int cur = 1;
-    for (int k = 1; k <= p.taylor_order; ++k) {
+    if (s == 3) {
+      if ((rc = islice_taylor_update(Cp, Sacc, R, M, 0, true, nslices, A_q[1], ld_m, A_e[1], st))) return rc;
+      i8_cur = 1;
       ph_begin(SFQ_PH_TAYLOR_GEMM);
-      if ((rc = i8_taylor(cur))) return rc;
+      *d = i8_taylor(i8_cur);  // T_1
+      return SFQ_OK;
+    }
+    if (s <= 3 + order) {  // after the product of T_k, k = s - 3
+      const int k = s - 3, cur = i8_cur;
       ph_end(SFQ_PH_TAYLOR_GEMM);
-      const bool last = k == p.taylor_order;
+      const bool last = k == order;
       if ((rc = islice_taylor_update(Cp, Sacc, R, M, k, last, nslices, A_q[1 - cur], ld_m, A_e[1 - cur], st)))
         return rc;
-      cur = 1 - cur;
+      i8_cur = 1 - cur;
+      if (last) {
+        *d = i8_p1(i8_cur, Cp, false);
+      } else {
+        ph_begin(SFQ_PH_TAYLOR_GEMM);
+        *d = i8_taylor(i8_cur);  // T_{k+1}
+      }
+      return SFQ_OK;
     }
-    if ((rc = i8_p1(cur, Cp, false))) return rc;
-    if ((rc = islice_to_walkers(Cp, Sacc, W, M, N, SM, st))) return rc;
+    *more = false;
+    if ((rc = islice_to_walkers(Cp, Sacc, Wb, M, N, SM, st))) return rc;
     ph_end(SFQ_PH_PROPAGATE);
     ph_begin(SFQ_PH_OVERLAP);
     if ((rc = log_overlap(newov))) return rc;
@@ -2231,39 +2257,80 @@ struct Engine {
     ph_end(SFQ_PH_UPDATE);
     return SFQ_OK;
   }
+  int propagate_i8(double Eshift, unsigned long long step, const double* uniforms) {
+    int rc;
+    IsliceGemmDesc d;
+    bool more = true;
+    for (int s = 0; more; ++s) {
+      if ((rc = propagate_i8_stage(s, Eshift, step, uniforms, &d, &more))) return rc;
+      if (more && (rc = islice_gemm(d, st))) return rc;
+    }
+    return SFQ_OK;
+  }
 
   // NOMSD::Energy in the exact-accumulation mode: E1 from the FP64 G; the exchange tensor
   // T[(c,w,b)][(n,a)] = sum_k G_c[w,b,k] Lnak[n,a,k] from int8 slices in chunks of Cholesky vectors
-  // (FP32, one rounding), its contractions summed in FP64
-  int energy_i8() {
-    int rc;
-    ph_begin(SFQ_PH_ENERGY);
-    if ((rc = density(ovtmp))) return rc;
-    const double scl = closed() ? 2.0 : 1.0;  // CLOSED counts each orbital twice
-    if ((rc = energy_e1(G, haj, E3, W, N, M, p.E0, scl, 1, st))) return rc;
-    const long R = (long)W * N;
-    if ((rc = islice_rows_planar(G, R, M, nslices, Ge_q, ld_m, Ge_e, st))) return rc;
+  // (FP32, one rounding), its contractions summed in FP64.  Stages as propagate_i8_stage: stage 0
+  // ends in the product of the first chunk, stage s > 0 reduces chunk s - 1 and ends in the next.
+  int i8_n0 = 0;  // first Cholesky vector of the chunk in flight
+  long i8_chunk() const {
     const long per_n = 2L * W * N * N;
     long nv_max = (2L * tchunk_elems) / per_n;
     if (nv_max < 1) nv_max = 1;
     if (nv_max > Nc) nv_max = Nc;
-    float* Tf = reinterpret_cast<float*>(Tchunk);
-    for (int n0 = 0; n0 < Nc; n0 += int(nv_max)) {
-      const int nv = (Nc - n0) < nv_max ? (Nc - n0) : int(nv_max);
-      const long ldc = (long)nv * N;
-      int8_t* Lc[3];
-      for (int q = 0; q < 3; ++q) Lc[q] = Le_q[q] ? Le_q[q] + (long)n0 * N * ld_m : nullptr;
-      IsliceGemmDesc d = i8_desc();
-      d.M = int(2 * R); d.N = int(ldc); d.K = M;
-      d.A = i8_operand(Ge_q, 2 * R, ld_m, Ge_e);
-      d.B = i8_operand(Lc, ldc, ld_m, Le_e + (long)n0 * N);
-      d.bn = i8_bn;
-      d.C = Tf; d.ldc = ldc;
-      if ((rc = islice_gemm(d, st))) return rc;
-      if ((rc = energy_exx_reduce_f32(Tf, W, N, nv, n0, Nc, ldc, exxn, kl, st, spin_split()))) return rc;
+    return nv_max;
+  }
+  void i8_exchange_desc(int n0, IsliceGemmDesc* d) const {
+    const long R = (long)W * N;
+    const long nv_max = i8_chunk();
+    const int nv = (Nc - n0) < nv_max ? (Nc - n0) : int(nv_max);
+    const long ldc = (long)nv * N;
+    int8_t* Lc[3];
+    for (int q = 0; q < 3; ++q) Lc[q] = Le_q[q] ? Le_q[q] + (long)n0 * N * ld_mr : nullptr;
+    *d = i8_desc();
+    d->M = int(2 * R); d->N = int(ldc); d->K = Mr;
+    d->A = i8_operand(Ge_q, 2 * R, ld_mr, Ge_e);
+    d->B = i8_operand(Lc, ldc, ld_mr, Le_e + (long)n0 * N);
+    d->bn = i8_bn;
+    d->C = reinterpret_cast<float*>(Tchunk); d->ldc = ldc;
+  }
+  int energy_i8_stage(int s, IsliceGemmDesc* d, bool* more) {
+    int rc;
+    const double scl = closed() ? 2.0 : 1.0;  // CLOSED counts each orbital twice
+    *more = true;
+    if (s == 0) {
+      ph_begin(SFQ_PH_ENERGY);
+      if ((rc = density(ovtmp))) return rc;
+      if ((rc = energy_e1(G, haj, E3, W, N, Mr, p.E0, scl, 1, st))) return rc;
+      if ((rc = islice_rows_planar(G, (long)W * N, Mr, nslices, Ge_q, ld_mr, Ge_e, st))) return rc;
+      i8_n0 = 0;
+      i8_exchange_desc(0, d);
+      return SFQ_OK;
     }
+    const long nv_max = i8_chunk();
+    const int n0 = i8_n0;
+    const int nv = (Nc - n0) < nv_max ? (Nc - n0) : int(nv_max);
+    if ((rc = energy_exx_reduce_f32(reinterpret_cast<float*>(Tchunk), W, N, nv, n0, Nc, (long)nv * N, exxn, kl, st,
+                                    spin_split())))
+      return rc;
+    i8_n0 = n0 + nv;
+    if (i8_n0 < Nc) {
+      i8_exchange_desc(i8_n0, d);
+      return SFQ_OK;
+    }
+    *more = false;
     if ((rc = energy_finish(exxn, kl, E3, W, Nc, scl, 1, 1, st))) return rc;
     ph_end(SFQ_PH_ENERGY);
+    return SFQ_OK;
+  }
+  int energy_i8() {
+    int rc;
+    IsliceGemmDesc d;
+    bool more = true;
+    for (int s = 0; more; ++s) {
+      if ((rc = energy_i8_stage(s, &d, &more))) return rc;
+      if (more && (rc = islice_gemm(d, st))) return rc;
+    }
     return SFQ_OK;
   }
 
@@ -2488,27 +2555,41 @@ struct Engine {
     for (char ch : sched) {
       const int c = ch - 'a';
       if ((rc = propagate(0.0, 0, nullptr))) return rc;  // step and Eshift come from the device
-      if ((c & 1) && (rc = orthogonalize())) return rc;
-      if ((c & 2) && (rc = population_control(0))) return rc;
+      if ((rc = block_after_propagate(c))) return rc;
       if (c & 8) {
         if (slot >= kMeasCap) return record_error(SFQ_ERR_ARG, "block: more than %d measurements", kMeasCap);
         if ((rc = energy_only())) return rc;
-        averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, E3, red);
-        SFQ_LAUNCHED();
-        measure_kernel<<<1, 1, 0, st>>>(red, d_meas + 10 * slot);
-        SFQ_LAUNCHED();
-        ++slot;
+        if ((rc = block_measure(&slot))) return rc;
       }
-      if (c & 4) {
-        averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, nullptr, red);
-        SFQ_LAUNCHED();
-        eshift_relax_kernel<<<1, 1, 0, st>>>(red, p.dt, relax, d_eshift);
-        SFQ_LAUNCHED();
-      }
-      step_add_kernel<<<1, 1, 0, st>>>(d_step);
-      SFQ_LAUNCHED();
+      if ((rc = block_step_end(c, relax))) return rc;
     }
     *nmeas = slot;
+    return SFQ_OK;
+  }
+  // the pieces of one block step around the propagation and the energy (record_block's order)
+  int block_after_propagate(int c) {
+    int rc;
+    if ((c & 1) && (rc = orthogonalize())) return rc;
+    if ((c & 2) && (rc = population_control(0))) return rc;
+    return SFQ_OK;
+  }
+  int block_measure(int* slot) {  // after the energy
+    averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, E3, red);
+    SFQ_LAUNCHED();
+    measure_kernel<<<1, 1, 0, st>>>(red, d_meas + 10 * *slot);
+    SFQ_LAUNCHED();
+    ++*slot;
+    return SFQ_OK;
+  }
+  int block_step_end(int c, double relax) {
+    if (c & 4) {
+      averages_kernel<<<1, 1024, 0, st>>>(props, W, p.dt, nullptr, red);
+      SFQ_LAUNCHED();
+      eshift_relax_kernel<<<1, 1, 0, st>>>(red, p.dt, relax, d_eshift);
+      SFQ_LAUNCHED();
+    }
+    step_add_kernel<<<1, 1, 0, st>>>(d_step);
+    SFQ_LAUNCHED();
     return SFQ_OK;
   }
 
@@ -2535,21 +2616,30 @@ struct Engine {
   // the step counter and Eshift from the group's input row, the block, then the results into the
   // group's output row (4 + 10 kMeasCap doubles)
   int record_group_part(const sfq_run_params_t& rp, const unsigned long long* in, double* out, int* nmeas) {
-    int rc;
-    const bool prof = profile;
+    int rc = group_part_begin(in);
+    if (!rc) rc = record_block(block_schedule(rp), block_relax(rp), nmeas);
+    if (!rc) rc = group_part_results(out, *nmeas);
+    group_part_end();
+    return rc;
+  }
+  bool saved_profile = false;
+  int group_part_begin(const unsigned long long* in) {
+    saved_profile = profile;
     profile = false;
     dev_mode = true;
+    inv_cached = false;
     load_block_state_kernel<<<1, 1, 0, st>>>(in, d_step, d_eshift);
     SFQ_LAUNCHED();
-    rc = record_block(block_schedule(rp), block_relax(rp), nmeas);
-    if (!rc) {
-      store_block_result_kernel<<<1, 128, 0, st>>>(d_eshift, pw.flag, mixed ? gemm_err : nullptr, d_meas, *nmeas,
-                                                   out);
-      SFQ_LAUNCHED();
-    }
+    return SFQ_OK;
+  }
+  int group_part_results(double* out, int nmeas) {
+    store_block_result_kernel<<<1, 128, 0, st>>>(d_eshift, pw.flag, mixed ? gemm_err : nullptr, d_meas, nmeas, out);
+    SFQ_LAUNCHED();
+    return SFQ_OK;
+  }
+  void group_part_end() {
     dev_mode = false;
-    profile = prof;
-    return rc;
+    profile = saved_profile;
   }
 
   // enqueue one block: its graph (captured on first use of its schedule), then the copies of
@@ -2677,6 +2767,18 @@ struct Group {
   std::map<std::string, Captured> graphs;
   const Captured* pending = nullptr;
   int lanes = 0;  // 0: one lane per member
+  // fused mode (int8-slice members on one block schedule): the members' steps interleaved stage by
+  // stage, each stage's int8-slice products of all members as ONE grouped launch on the group
+  // stream, the work between them on the members' streams side by side
+  bool fused = false;
+  struct Table {
+    void* dev = nullptr;  // the grouped launch's table in device memory
+    IsliceGroupPlan plan;
+  };
+  std::map<std::string, Table> tables;  // by stage and members; the same for every step and block
+  std::vector<std::string> new_tables;  // created in the capture under way, to be copied to the device
+  cudaEvent_t ev_prod = nullptr;        // after the last grouped launch
+  std::vector<cudaEvent_t> ev_stage;
 
   // lane of each member, and the members of each lane in order
   std::vector<std::vector<int>> plan_lanes(const sfq_run_params_t* rps) const {
@@ -2708,11 +2810,14 @@ struct Group {
     SFQ_CUDA_TRY(cudaStreamCreateWithFlags(&gst, cudaStreamNonBlocking));
     SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+    SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_prod, cudaEventDisableTiming));
     ev_join.assign(n, nullptr);
     ev_pre.assign(n, nullptr);
+    ev_stage.assign(n, nullptr);
     for (size_t i = 0; i < n; ++i) {
       SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_join[i], cudaEventDisableTiming));
       SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_pre[i], cudaEventDisableTiming));
+      SFQ_CUDA_TRY(cudaEventCreateWithFlags(&ev_stage[i], cudaEventDisableTiming));
     }
     SFQ_CUDA_TRY(cudaMalloc(&d_in, sizeof(unsigned long long) * 2 * n));
     SFQ_CUDA_TRY(cudaMalloc(&d_out, sizeof(double) * kOut * n));
@@ -2726,9 +2831,13 @@ struct Group {
     for (auto& kv : graphs)
       if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     graphs.clear();
-    for (auto* v : {&ev_join, &ev_pre})
+    for (auto& kv : tables)
+      if (kv.second.dev) cudaFree(kv.second.dev);
+    tables.clear();
+    for (auto* v : {&ev_join, &ev_pre, &ev_stage})
       for (auto& x : *v)
         if (x) cudaEventDestroy(x);
+    if (ev_prod) cudaEventDestroy(ev_prod);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_done) cudaEventDestroy(ev_done);
     if (d_in) cudaFree(d_in);
@@ -2776,10 +2885,156 @@ struct Group {
     return SFQ_OK;
   }
 
+  int set_fused(bool on) {
+    if (on) {
+      for (Engine* e : es)
+        if (!e->nslices || e->nslices != es[0]->nslices)
+          return record_error(SFQ_ERR_UNSUPPORTED, "group: fused products need int8-slice members of one precision");
+    }
+    fused = on;
+    return SFQ_OK;
+  }
+
+  // K slices of one output tile of a product (its tiles' length)
+  static long tile_k(const IsliceGemmDesc& d) {
+    const long kt = (d.K + 127) / 128;
+    if (d.cplx_half > 0) return 2 * kt;
+    const long ks = d.ksplit < 1 ? 1 : d.ksplit;
+    return (kt + ks - 1) / ks;
+  }
+
+  // stage s = 0, 1, ... of every member still running: its work on its own stream (after the
+  // previous grouped launch), then all their products as one launch on the group stream
+  template <typename StageFn>
+  int grouped_stages(const char* kind, StageFn stage) {
+    const int n = int(es.size());
+    std::vector<char> more(size_t(n), 1);
+    for (int s = 0;; ++s) {
+      std::vector<IsliceGemmDesc> ds;
+      std::vector<int> who;
+      for (int i = 0; i < n; ++i) {
+        if (!more[size_t(i)]) continue;
+        Engine& e = *es[size_t(i)];
+        if (s > 0) SFQ_CUDA_TRY(cudaStreamWaitEvent(e.st, ev_prod, 0));
+        IsliceGemmDesc d;
+        bool m = false;
+        int rc = stage(e, s, &d, &m);
+        if (rc) return rc;
+        more[size_t(i)] = m ? 1 : 0;
+        if (!m) continue;
+        ds.push_back(d);
+        who.push_back(i);
+        SFQ_CUDA_TRY(cudaEventRecord(ev_stage[size_t(i)], e.st));
+        SFQ_CUDA_TRY(cudaStreamWaitEvent(gst, ev_stage[size_t(i)], 0));
+      }
+      if (ds.empty()) return SFQ_OK;
+      // the longest tiles first: the persistent CTAs take the tiles in list order
+      std::vector<size_t> ord(ds.size());
+      for (size_t j = 0; j < ord.size(); ++j) ord[j] = j;
+      std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return tile_k(ds[a]) > tile_k(ds[b]); });
+      std::string key = std::string(kind) + std::to_string(s);
+      for (size_t j : ord) key += "," + std::to_string(who[j]);
+      auto it = tables.find(key);
+      if (it == tables.end()) {
+        std::vector<IsliceGemmDesc> sorted;
+        for (size_t j : ord) sorted.push_back(ds[j]);
+        Table t;
+        int rc = islice_gemm_group_plan(sorted.data(), int(sorted.size()), &t.plan);
+        if (rc) return rc;
+        SFQ_CUDA_TRY(cudaMalloc(&t.dev, t.plan.image.size()));
+        it = tables.emplace(key, std::move(t)).first;
+        new_tables.push_back(key);
+      }
+      int rc = islice_gemm_group_launch(it->second.dev, it->second.plan, gst);
+      if (rc) return rc;
+      SFQ_CUDA_TRY(cudaEventRecord(ev_prod, gst));
+    }
+  }
+
+  // the members' blocks as one graph in fused mode (the steps of record_block, stage by stage)
+  int capture_fused(const sfq_run_params_t* rps, Captured* c) {
+    const size_t n = es.size();
+    const std::string sched = Engine::block_schedule(rps[0]);
+    for (size_t i = 1; i < n; ++i)
+      if (Engine::block_schedule(rps[i]) != sched)
+        return record_error(SFQ_ERR_ARG, "group: fused products need every member on one block schedule");
+    int nmeas = 0;
+    for (char ch : sched)
+      if ((ch - 'a') & 8) ++nmeas;
+    if (nmeas > Engine::kMeasCap) return record_error(SFQ_ERR_ARG, "block: more than %d measurements", Engine::kMeasCap);
+    c->nmeas.assign(n, 0);
+    c->inv_after.assign(n, 0);
+    c->inv_ov_after.assign(n, nullptr);
+    new_tables.clear();
+    SFQ_CUDA_TRY(cudaStreamBeginCapture(gst, cudaStreamCaptureModeRelaxed));
+    int rc = SFQ_OK;
+    cudaError_t ce = cudaEventRecord(ev_fork, gst);
+    std::vector<char> forked(n, 0), begun(n, 0);
+    for (size_t i = 0; i < n && ce == cudaSuccess; ++i) {
+      ce = cudaStreamWaitEvent(es[i]->st, ev_fork, 0);
+      if (ce != cudaSuccess) break;
+      forked[i] = 1;
+      if (!rc) {
+        rc = es[i]->group_part_begin(d_in + 2 * i);
+        begun[i] = 1;
+      }
+    }
+    std::vector<int> slot(n, 0);
+    for (char ch : sched) {
+      if (rc || ce != cudaSuccess) break;
+      const int cc = ch - 'a';
+      rc = grouped_stages("p", [](Engine& e, int s, IsliceGemmDesc* d, bool* m) {
+        return e.propagate_i8_stage(s, 0.0, 0, nullptr, d, m);  // step and Eshift come from the device
+      });
+      for (size_t i = 0; i < n && !rc; ++i) rc = es[i]->block_after_propagate(cc);
+      if (!rc && (cc & 8)) {
+        rc = grouped_stages("e", [](Engine& e, int s, IsliceGemmDesc* d, bool* m) { return e.energy_i8_stage(s, d, m); });
+        for (size_t i = 0; i < n && !rc; ++i) rc = es[i]->block_measure(&slot[i]);
+      }
+      for (size_t i = 0; i < n && !rc; ++i) rc = es[i]->block_step_end(cc, Engine::block_relax(rps[i]));
+    }
+    for (size_t i = 0; i < n; ++i) {
+      if (!rc && begun[i]) rc = es[i]->group_part_results(d_out + (size_t)kOut * i, slot[i]);
+      c->nmeas[i] = slot[i];
+      c->inv_after[i] = es[i]->inv_cached ? 1 : 0;
+      c->inv_ov_after[i] = es[i]->inv_ov;
+      if (begun[i]) es[i]->group_part_end();
+      if (forked[i] && ce == cudaSuccess) {  // close every forked branch, also after an error
+        ce = cudaEventRecord(ev_join[i], es[i]->st);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(gst, ev_join[i], 0);
+      }
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(gst, &g);
+    if (rc || ce != cudaSuccess || ee != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      for (const std::string& k : new_tables) {  // never copied: drop them
+        auto it = tables.find(k);
+        if (it != tables.end()) {
+          cudaFree(it->second.dev);
+          tables.erase(it);
+        }
+      }
+      new_tables.clear();
+      if (rc) return rc;
+      return record_cuda(ce != cudaSuccess ? ce : ee, "group capture", __FILE__, __LINE__);
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&c->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return record_cuda(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+    // the new tables reach the device on the group stream, ahead of the graph's first launch there
+    for (const std::string& k : new_tables) {
+      const Table& t = tables[k];
+      SFQ_CUDA_TRY(cudaMemcpyAsync(t.dev, t.plan.image.data(), t.plan.image.size(), cudaMemcpyHostToDevice, gst));
+    }
+    new_tables.clear();
+    return SFQ_OK;
+  }
+
   int block_async(const sfq_run_params_t* rps, const double* Eshift) {
     const size_t n = es.size();
     if (pending) return record_error(SFQ_ERR_ARG, "group: the previous block's results were not taken");
-    std::string key = std::to_string(lanes) + "#";
+    std::string key = (fused ? std::string("F") : std::to_string(lanes)) + "#";
     for (size_t i = 0; i < n; ++i) {
       if (rps[i].steps <= 0) return record_error(SFQ_ERR_ARG, "group: steps must be positive");
       key += Engine::block_key(rps[i]);
@@ -2788,7 +3043,7 @@ struct Group {
     auto it = graphs.find(key);
     if (it == graphs.end()) {
       Captured c;
-      int rc = capture(rps, &c);
+      int rc = fused ? capture_fused(rps, &c) : capture(rps, &c);
       if (rc) return rc;
       it = graphs.emplace(key, std::move(c)).first;
     }
@@ -2930,11 +3185,11 @@ int sfq_engine_create_nomsd(sfq_engine_t* out, const sfq_engine_params_t* p, con
     delete h;
     return record_error(SFQ_ERR_ARG, "engine: unknown precision %d", p->precision);
   }
-  if (e.mixed && ((coll && !e.nslices) || npol > 1 || ndet > 1)) {
+  if (e.mixed && (((coll || npol > 1) && !e.nslices) || ndet > 1)) {
     delete h;
     return record_error(SFQ_ERR_UNSUPPORTED,
-                        "engine: NONCOLLINEAR walkers and multi-determinant trials run in FP64, COLLINEAR walkers in "
-                        "FP64 or the int8-slice precisions");
+                        "engine: multi-determinant trials run in FP64, COLLINEAR and NONCOLLINEAR walkers in FP64 or "
+                        "the int8-slice precisions");
   }
   if (e.nslices && (!e.trial_real || e.M > 1024)) {
     delete h;
@@ -3385,6 +3640,12 @@ int sfq_group_set_lanes(sfq_group_t h, int lanes) {
   if (h->g.pending) return record_error(SFQ_ERR_ARG, "group: a block is running");
   h->g.lanes = lanes;
   return SFQ_OK;
+}
+
+int sfq_group_set_fused(sfq_group_t h, int fused) {
+  if (!h) return record_error(SFQ_ERR_ARG, "null group");
+  if (h->g.pending) return record_error(SFQ_ERR_ARG, "group: a block is running");
+  return h->g.set_fused(fused != 0);
 }
 
 int sfq_group_block_query(sfq_group_t h) {

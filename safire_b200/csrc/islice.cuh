@@ -34,6 +34,7 @@
 // C[c * sCc + (batch * M + row) * ldc + i].
 #pragma once
 #include <cstdint>
+#include <vector>
 
 #include "common.cuh"
 
@@ -68,6 +69,22 @@ struct IsliceGemmDesc {
 };
 
 int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st);
+
+// Several products (the same slice count; plain ones of tile width 160, complex-B ones of any
+// half <= 80) as ONE persistent launch over the concatenated tile lists, each tile computed as its
+// own product's launch computes it (the results are the same bit for bit).  The plan is a host
+// image of the launch's table (per product: tensor maps and parameters; then the tile offsets)
+// that the caller copies to device memory (128-byte aligned) before the launch runs, and keeps
+// there for as long as the launch may run (a graph holding it may be replayed).
+struct IsliceGroupPlan {
+  std::vector<char> image;
+  size_t start_off = 0;  // byte offset of the nprob + 1 tile offsets in the image
+  int nprob = 0, nslices = 0;
+  long tiles = 0;
+  unsigned long long wait_ns = 0;
+};
+int islice_gemm_group_plan(const IsliceGemmDesc* ds, int n, IsliceGroupPlan* out);
+int islice_gemm_group_launch(const void* table, const IsliceGroupPlan& plan, cudaStream_t st);
 
 // ---- slicing (islice_kernels.cu) ------------------------------------------------------------
 // Every slicer writes nslices int8 arrays (rows, ld) at q[s] and one exponent per row (or per row

@@ -1,4 +1,5 @@
 // Exact-accumulation int8-slice products on the tensor cores (see islice.cuh).
+#include <cstddef>
 #include <cstring>
 
 #include "islice.cuh"
@@ -77,6 +78,47 @@ struct KParams {
   const int* hold;
 };
 
+// a grouped launch: the products of several problems (the members of a group of systems) as one
+// persistent tile list; problem i owns tiles [start[i], start[i+1]), its tensor maps and parameters
+// in device memory (written before the launch)
+struct alignas(128) GroupProb {
+  Maps maps;
+  KParams kp;
+};
+static_assert(sizeof(GroupProb) % 128 == 0 && offsetof(GroupProb, maps) == 0,
+              "tensor maps in the table keep their 64-byte alignment");
+struct GroupTab {
+  const GroupProb* prob = nullptr;
+  const long* start = nullptr;  // nprob + 1 tile offsets
+  int nprob = 0;
+  long tiles = 0;
+};
+__device__ __forceinline__ int find_prob(const GroupTab& g, long t) {
+  int lo = 0, hi = g.nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (g.start[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+// the problem of tile t (global index) and its local tile index
+template <bool GROUP>
+__device__ __forceinline__ int locate(const GroupTab& g, long t, long& lt) {
+  if (!GROUP) {
+    lt = t;
+    return 0;
+  }
+  const int pi = find_prob(g, t);
+  lt = t - g.start[pi];
+  return pi;
+}
+// a tensor map in device memory, written before the launch, is read by the tensor-map proxy
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(m))
+               : "memory");
+}
+
 __device__ __forceinline__ void decode(const KParams& p, long t, int& mt, int& nt, int& bz, int& ks) {
   mt = int(t % p.MT);
   long r = t / p.MT;
@@ -100,8 +142,9 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
   const int gm = mt * BM + row;
   const bool live = gm < p.M;
   const int ea = live ? p.ea[(long)bz * p.ea_bs + (p.ea_mod ? gm % p.ea_mod : gm)] : 0;
+  const int width = p.half ? 2 * p.half : BN;  // complex B: the [re | im] halves may be narrower than BN
 #pragma unroll 1
-  for (int c = c0; c < BN; c += 32) {
+  for (int c = c0; c < width; c += 32) {
     uint32_t acc[3][16];
     __syncwarp();
 #pragma unroll
@@ -159,9 +202,10 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
   }
 }
 
-template <int BN, int STAGES, int NS, int BUFS>
-__global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_constant__ Maps maps,
-                                                                  const __grid_constant__ KParams p) {
+template <int BN, int STAGES, int NS, int BUFS, bool GROUP>
+__global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_constant__ Maps maps0,
+                                                                  const __grid_constant__ KParams p0,
+                                                                  const __grid_constant__ GroupTab g) {
   using L = Smem<BN, STAGES, NS>;
   constexpr uint32_t GCOLS = uint32_t(NS * BN);               // columns of one tile's groups
   constexpr uint32_t ALLOC = pow2_ceil(GCOLS * BUFS);
@@ -177,8 +221,7 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
   volatile int* s_abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const bool cb = p.half > 0;
-  const int Kv = cb ? p.N : p.K;  // valid K elements (complex B: the orbitals)
+  const long total = GROUP ? g.tiles : p0.tiles;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -202,15 +245,15 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
   __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_slot;
-  const unsigned long long wait_ns = p.wait_ns;
+  const unsigned long long wait_ns = p0.wait_ns;
 
   if (warp == 0) {
     if (lane == 0) {  // TMA producer
       uint32_t it = 0;
       bool stop = false;
-      if (p.hold) {  // start only once *hold is set (bounded like every wait)
+      if (!GROUP && p0.hold) {  // start only once *hold is set (bounded like every wait)
         const unsigned long long t0 = gtimer();
-        while (*reinterpret_cast<const volatile int*>(p.hold) == 0) {
+        while (*reinterpret_cast<const volatile int*>(p0.hold) == 0) {
           if (gtimer() - t0 > wait_ns) {
             *s_abort = 1;
             stop = true;
@@ -218,9 +261,26 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
           }
         }
       }
-      for (long t = blockIdx.x; t < p.tiles && !stop; t += gridDim.x) {
+      int last_pi = -1;
+      for (long t = blockIdx.x; t < total && !stop; t += gridDim.x) {
+        long lt;
+        const int pi = locate<GROUP>(g, t, lt);
+        const KParams& p = GROUP ? g.prob[pi].kp : p0;
+        const Maps& maps = GROUP ? g.prob[pi].maps : maps0;
+        const bool cb = p.half > 0;
+        if (GROUP && pi != last_pi) {
+#pragma unroll
+          for (int q = 0; q < NS; ++q) {
+            tensormap_acquire(&maps.a[q]);
+            tensormap_acquire(&maps.b[q]);
+            if (cb) tensormap_acquire(&maps.aim[q]);
+          }
+          last_pi = pi;
+        }
+        // bytes of one stage: complex B loads two half-tiles of `half` rows of B
+        const uint32_t stage_bytes = cb ? uint32_t(NS * (L::A_BYTES + 2 * p.half * BK)) : uint32_t(L::STAGE);
         int mt, nt, bz, ks;
-        decode(p, t, mt, nt, bz, ks);
+        decode(p, lt, mt, nt, bz, ks);
         const int m0 = mt * BM;
         const int ab = p.a_batched ? bz : 0, bb = p.b_batched ? bz : 0;
         const int kb = k_begin(p.KT, p.KS, ks), ke = k_begin(p.KT, p.KS, ks + 1);
@@ -233,10 +293,10 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
             break;
           }
           unsigned char* stg = smem + s * L::STAGE;
+          mbar_expect_tx(&full[s], stage_bytes);
           if (cb) {
             // part 0: A_re with the rows [Vr; Vi] of the tile's orbitals; part 1: A_im with [-Vi; Vr]
             const int part = kt & 1, k0 = (kt >> 1) * BK, i0 = nt * p.half;
-            mbar_expect_tx(&full[s], uint32_t(L::STAGE));
 #pragma unroll
             for (int q = 0; q < NS; ++q) {
               unsigned char* at = stg + q * L::A_BYTES;
@@ -247,7 +307,6 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
             }
           } else {
             const int k0 = kt * BK, n0 = nt * BN;
-            mbar_expect_tx(&full[s], uint32_t(L::STAGE));
 #pragma unroll
             for (int q = 0; q < NS; ++q) {
               tma_load_3d(stg + q * L::A_BYTES, &maps.a[q], &full[s], k0, m0, ab);
@@ -263,20 +322,26 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
       uint32_t it = 0;
-      int lt = 0;
+      int lt_n = 0;
       bool stop = false;
-      for (long t = blockIdx.x; t < p.tiles && !stop; t += gridDim.x, ++lt) {
-        const int b = BUFS == 2 ? (lt & 1) : 0;
-        const uint32_t aph = BUFS == 2 ? ((uint32_t(lt) >> 1) & 1) : (uint32_t(lt) & 1);
+      for (long t = blockIdx.x; t < total && !stop; t += gridDim.x, ++lt_n) {
+        const int b = BUFS == 2 ? (lt_n & 1) : 0;
+        const uint32_t aph = BUFS == 2 ? ((uint32_t(lt_n) >> 1) & 1) : (uint32_t(lt_n) & 1);
         if (*s_abort || !mbar_wait_for(&acc_empty[b], aph ^ 1, wait_ns)) {
           *s_abort = 1;
           break;
         }
         fence_after();
         const uint32_t d_tmem = tmem + uint32_t(b) * GCOLS;
+        long lt;
+        const int pi = locate<GROUP>(g, t, lt);
+        const KParams& p = GROUP ? g.prob[pi].kp : p0;
+        const bool cb = p.half > 0;
+        const int Kv = cb ? p.N : p.K;  // valid K elements (complex B: the orbitals)
         int mt, nt, bz, ks;
-        decode(p, t, mt, nt, bz, ks);
+        decode(p, lt, mt, nt, bz, ks);
         const int kb = k_begin(p.KT, p.KS, ks), ke = k_begin(p.KT, p.KS, ks + 1);
+        const uint32_t idesc = idesc_i8(uint32_t(cb ? 2 * p.half : BN));
         for (int kt = kb; kt < ke; ++kt, ++it) {
           const int s = int(it % STAGES);
           const uint32_t ph = (it / STAGES) & 1;
@@ -296,7 +361,6 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
           const int k0 = cb ? (kt >> 1) * BK : kt * BK;
           const int rem = Kv - k0;
           const int nk = rem >= BK ? BK / KSTEP : (rem + KSTEP - 1) / KSTEP;  // K tail: skip all-zero steps
-          const uint32_t idesc = idesc_i8(uint32_t(BN));
           const bool first_slice = kt == kb;  // complex B: part 0 of the first K block initialises
           for (int kk = 0; kk < nk; ++kk) {
             const uint64_t off = uint64_t(kk * KSTEP) >> 4;  // 32 bytes along the swizzled row
@@ -318,10 +382,10 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
     const int q = warp & 3;
     const int row = q * 32 + lane;
     const int c0 = 16 * ((warp - 2) >> 2);  // the two warps of a quarter take alternate 16-column chunks
-    int lt = 0;
-    for (long t = blockIdx.x; t < p.tiles; t += gridDim.x, ++lt) {
-      const int b = BUFS == 2 ? (lt & 1) : 0;
-      const uint32_t aph = BUFS == 2 ? ((uint32_t(lt) >> 1) & 1) : (uint32_t(lt) & 1);
+    int lt_n = 0;
+    for (long t = blockIdx.x; t < total; t += gridDim.x, ++lt_n) {
+      const int b = BUFS == 2 ? (lt_n & 1) : 0;
+      const uint32_t aph = BUFS == 2 ? ((uint32_t(lt_n) >> 1) & 1) : (uint32_t(lt_n) & 1);
       const bool ok = mbar_wait_for(&acc_full[b], aph, wait_ns);
       const bool go = __all_sync(0xffffffffu, ok) && !__any_sync(0xffffffffu, *s_abort != 0);
       if (!go) {
@@ -329,8 +393,11 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
         break;
       }
       fence_after();
+      long lt;
+      const int pi = locate<GROUP>(g, t, lt);
+      const KParams& p = GROUP ? g.prob[pi].kp : p0;
       int mt, nt, bz, ks;
-      decode(p, t, mt, nt, bz, ks);
+      decode(p, lt, mt, nt, bz, ks);
       epilogue_tile<BN, NS>(p, tmem + (uint32_t(q * 32) << 16) + uint32_t(b) * GCOLS, row, mt, nt, bz, ks, c0);
       fence_before();
       mbar_arrive(&acc_empty[b]);
@@ -338,7 +405,14 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
   }
   fence_before();
   __syncthreads();
-  if (threadIdx.x == 0 && *s_abort && p.err) atomicExch(p.err, SFQ_ERR_TIMEOUT);
+  if (threadIdx.x == 0 && *s_abort) {
+    if (GROUP) {
+      for (int i = 0; i < g.nprob; ++i)
+        if (g.prob[i].kp.err) atomicExch(g.prob[i].kp.err, SFQ_ERR_TIMEOUT);
+    } else if (p0.err) {
+      atomicExch(p0.err, SFQ_ERR_TIMEOUT);
+    }
+  }
   if (warp == 1) {
     fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ALLOC));
@@ -368,43 +442,41 @@ int make_map_i8(CUtensorMap* m, const void* base, long rows, long K, long ld, lo
   return SFQ_OK;
 }
 
+// the tensor maps and kernel parameters of one product; `group`: a member of a grouped launch of
+// tile width BN, whose complex-B products may use narrower halves
 template <int BN, int STAGES, int NS>
-int launch(const IsliceGemmDesc& d, cudaStream_t st) {
-  using L = Smem<BN, STAGES, NS>;
-  static_assert(BN % 16 == 0, "the epilogue drains whole 16-column chunks");
-  constexpr int BUFS = (2 * NS * BN <= 512) ? 2 : 1;
-  static_assert(L::TOTAL <= 232448, "shared memory budget");
-  static_assert(NS * BN * BUFS <= 512, "accumulator groups must fit in tensor memory");
+int prepare(const IsliceGemmDesc& d, Maps* maps, KParams* kp_out, bool group) {
   const bool cb = d.cplx_half > 0;
-  Maps maps;
   int rc;
   const long ab = d.A.batch_stride ? d.batch : 1, bb = d.B.batch_stride ? d.batch : 1;
   for (int q = 0; q < NS; ++q) {
     if (!d.A.q[q] || !d.B.q[q]) return record_error(SFQ_ERR_ARG, "islice_gemm: slice %d missing", q);
-    if ((rc = make_map_i8(&maps.a[q], d.A.q[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
-    if ((rc = make_map_i8(&maps.b[q], d.B.q[q], d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, cb ? d.cplx_half : BN)))
+    if ((rc = make_map_i8(&maps->a[q], d.A.q[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
+    if ((rc = make_map_i8(&maps->b[q], d.B.q[q], d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, cb ? d.cplx_half : BN)))
       return rc;
     if (cb) {
       if (!d.a_im[q]) return record_error(SFQ_ERR_ARG, "islice_gemm: complex B needs a_im");
-      if ((rc = make_map_i8(&maps.aim[q], d.a_im[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
+      if ((rc = make_map_i8(&maps->aim[q], d.a_im[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
     } else {
-      maps.aim[q] = maps.a[q];
+      maps->aim[q] = maps->a[q];
     }
   }
   for (int q = NS; q < 3; ++q) {
-    maps.a[q] = maps.a[0];
-    maps.b[q] = maps.b[0];
-    maps.aim[q] = maps.aim[0];
+    maps->a[q] = maps->a[0];
+    maps->b[q] = maps->b[0];
+    maps->aim[q] = maps->aim[0];
   }
   if (!d.A.e || !d.B.e || !d.C) return record_error(SFQ_ERR_ARG, "islice_gemm: exponents and output required");
-  KParams kp;
+  KParams& kp = *kp_out;
+  kp = KParams{};
   kp.M = d.M; kp.N = d.N; kp.K = d.K; kp.batch = d.batch;
   kp.a_batched = d.A.batch_stride != 0; kp.b_batched = d.B.batch_stride != 0;
   kp.MT = (d.M + BM - 1) / BM;
   if (cb) {
-    if (d.cplx_half * 2 != BN || d.cplx_half % 16 || d.K != d.N || d.B.rows != 3L * d.N || d.ksplit > 1)
-      return record_error(SFQ_ERR_ARG, "islice_gemm: complex B needs BN = 2 half, half %% 16 == 0, K = N = nmo, "
-                                       "B rows = 3 nmo and no K split");
+    const bool width_ok = group ? d.cplx_half * 2 <= BN : d.cplx_half * 2 == BN;
+    if (!width_ok || d.cplx_half % 16 || d.K != d.N || d.B.rows != 3L * d.N || d.ksplit > 1)
+      return record_error(SFQ_ERR_ARG, "islice_gemm: complex B needs BN = 2 half (a grouped launch: <=), half %% 16 "
+                                       "== 0, K = N = nmo, B rows = 3 nmo and no K split");
     kp.NT = (d.N + d.cplx_half - 1) / d.cplx_half;
     kp.KT = 2 * ((d.K + BK - 1) / BK);
     kp.KS = 1;
@@ -428,11 +500,87 @@ int launch(const IsliceGemmDesc& d, cudaStream_t st) {
   kp.accumulate = d.accumulate ? 1 : 0;
   kp.err = d.err;
   kp.wait_ns = d.wait_ns ? d.wait_ns : kWaitNs;
-  kp.hold = d.hold;
-  auto k = islice_gemm_kernel<BN, STAGES, NS, BUFS>;
-  SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL));
+  kp.hold = group ? nullptr : d.hold;
+  return SFQ_OK;
+}
+
+template <int BN, int STAGES, int NS>
+struct Config {
+  using L = Smem<BN, STAGES, NS>;
+  static_assert(BN % 16 == 0, "the epilogue drains whole 16-column chunks");
+  static constexpr int BUFS = (2 * NS * BN <= 512) ? 2 : 1;
+  static_assert(L::TOTAL <= 232448, "shared memory budget");
+  static_assert(NS * BN * BUFS <= 512, "accumulator groups must fit in tensor memory");
+};
+
+template <int BN, int STAGES, int NS>
+int launch(const IsliceGemmDesc& d, cudaStream_t st) {
+  using C = Config<BN, STAGES, NS>;
+  Maps maps;
+  KParams kp;
+  int rc;
+  if ((rc = prepare<BN, STAGES, NS>(d, &maps, &kp, false))) return rc;
+  auto k = islice_gemm_kernel<BN, STAGES, NS, C::BUFS, false>;
+  SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, C::L::TOTAL));
   const long grid = kp.tiles < sm_count() ? kp.tiles : sm_count();
-  k<<<unsigned(grid), kThreads, L::TOTAL, st>>>(maps, kp);
+  k<<<unsigned(grid), kThreads, C::L::TOTAL, st>>>(maps, kp, GroupTab{});
+  SFQ_LAUNCHED();
+  return SFQ_OK;
+}
+
+// the grouped launches' tile widths: every plain product of a group has tile width kGroupBN
+constexpr int kGroupBN = 160;
+constexpr int group_stages(int ns) { return ns == 2 ? 3 : 2; }
+
+template <int NS>
+int group_plan(const IsliceGemmDesc* ds, int n, IsliceGroupPlan* out) {
+  constexpr int ST = group_stages(NS);
+  std::vector<GroupProb> probs(static_cast<size_t>(n));
+  std::vector<long> start(size_t(n) + 1, 0);
+  int rc;
+  for (int i = 0; i < n; ++i) {
+    const IsliceGemmDesc& d = ds[i];
+    if (d.nslices != NS) return record_error(SFQ_ERR_ARG, "islice_gemm_group: members differ in slices");
+    if (d.cplx_half == 0 && d.bn != kGroupBN)
+      return record_error(SFQ_ERR_ARG, "islice_gemm_group: plain products need tile width %d", kGroupBN);
+    if (d.hold) return record_error(SFQ_ERR_ARG, "islice_gemm_group: no held launches");
+    if (d.M <= 0 || d.N <= 0 || d.batch <= 0 || d.K <= 0)
+      return record_error(SFQ_ERR_SHAPE, "islice_gemm_group: empty member %d", i);
+    GroupProb* pr = probs.data() + i;
+    Maps* mp = &pr->maps;
+    KParams* kq = &pr->kp;
+    rc = prepare<kGroupBN, ST, NS>(d, mp, kq, true);
+    if (rc) return rc;
+    start[size_t(i) + 1] = start[size_t(i)] + kq->tiles;
+  }
+  out->nprob = n;
+  out->nslices = NS;
+  out->tiles = start[size_t(n)];
+  out->wait_ns = n ? probs[0].kp.wait_ns : kWaitNs;
+  out->start_off = sizeof(GroupProb) * size_t(n);
+  out->image.assign(out->start_off + sizeof(long) * (size_t(n) + 1), 0);
+  std::memcpy(out->image.data(), probs.data(), out->start_off);
+  std::memcpy(out->image.data() + out->start_off, start.data(), sizeof(long) * (size_t(n) + 1));
+  return SFQ_OK;
+}
+
+template <int NS>
+int group_launch(const void* table, const IsliceGroupPlan& plan, cudaStream_t st) {
+  constexpr int ST = group_stages(NS);
+  using C = Config<kGroupBN, ST, NS>;
+  if (reinterpret_cast<uintptr_t>(table) & 127)
+    return record_error(SFQ_ERR_ARG, "islice_gemm_group: the table needs 128-byte alignment");
+  GroupTab g;
+  g.prob = static_cast<const GroupProb*>(table);
+  g.start = reinterpret_cast<const long*>(static_cast<const char*>(table) + plan.start_off);
+  g.nprob = plan.nprob;
+  g.tiles = plan.tiles;
+  KParams kp{};
+  kp.wait_ns = plan.wait_ns;
+  auto k = islice_gemm_kernel<kGroupBN, ST, NS, C::BUFS, true>;
+  SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, C::L::TOTAL));
+  const long grid = plan.tiles < sm_count() ? plan.tiles : sm_count();
+  k<<<unsigned(grid), kThreads, C::L::TOTAL, st>>>(Maps{}, kp, g);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
@@ -454,6 +602,20 @@ int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st) {
     default:
       return record_error(SFQ_ERR_ARG, "islice_gemm: %d slices with tile width %d not built", d.nslices, bn);
   }
+}
+
+int islice_gemm_group_plan(const IsliceGemmDesc* ds, int n, IsliceGroupPlan* out) {
+  if (n <= 0 || !ds || !out) return record_error(SFQ_ERR_ARG, "islice_gemm_group: no members");
+  if (ds[0].nslices == 2) return islice::group_plan<2>(ds, n, out);
+  if (ds[0].nslices == 3) return islice::group_plan<3>(ds, n, out);
+  return record_error(SFQ_ERR_ARG, "islice_gemm_group: %d slices not built", ds[0].nslices);
+}
+
+int islice_gemm_group_launch(const void* table, const IsliceGroupPlan& plan, cudaStream_t st) {
+  if (plan.nprob <= 0 || plan.tiles <= 0) return SFQ_OK;
+  if (plan.nslices == 2) return islice::group_launch<2>(table, plan, st);
+  if (plan.nslices == 3) return islice::group_launch<3>(table, plan, st);
+  return record_error(SFQ_ERR_ARG, "islice_gemm_group: %d slices not built", plan.nslices);
 }
 
 }  // namespace sfq

@@ -305,7 +305,7 @@ constexpr long kEnergyChunkElems = 1L << 27;  // 2 GiB of complex T per chunk at
 
 extern "C" {
 
-int sfq_abi_version(void) { return 12; }
+int sfq_abi_version(void) { return 13; }
 
 unsigned long long sfq_launch_count(void) { return g_launches.load(); }
 

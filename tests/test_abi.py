@@ -44,7 +44,7 @@ def test_binding_covers_header():
 def test_last_error_and_version(lib):
     from safire_b200 import capi
     L = capi.lib()
-    assert L.sfq_abi_version() == 12
+    assert L.sfq_abi_version() == 13
     assert isinstance(L.sfq_last_error(), bytes)
 
 
@@ -187,7 +187,7 @@ int main(void) {
   double w[12];
   int off[12], counts[3] = {4, 5, 3}, plan[4 * 15], n = 0, i;
   for (i = 0; i < 12; ++i) w[i] = (i == 2 || i == 9) ? 0.0 : 0.5 + 0.375 * ((i * 5) % 7);
-  if (sfq_abi_version() != 12) return 3;
+  if (sfq_abi_version() != 13) return 3;
   if (sfq_comb_host(w, 0.71, 12, 12, off) != SFQ_OK) return 4;
   for (i = 0; i < 12; ++i) printf("%d ", off[i]);
   printf("\n");

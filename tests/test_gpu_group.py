@@ -63,6 +63,77 @@ def test_group_block_equals_each_member_alone(lanes):
         e.close()
 
 
+def _int8_engines(seed0=200):
+    """INT8X3 members whose products differ in every shape: synthetic CLOSED systems (Taylor tiles of
+    64 and 80 orbitals), the reference's Li COLLINEAR and BH GHF NONCOLLINEAR fixtures (tiles of 32)."""
+    from tests.golden_io import engine_system, snapshot
+    systems = [(synthetic.make_system(spec), W) for spec, W, _p in MEMBERS]
+    systems += [(engine_system(snapshot("li_rohf_collinear")), 40), (engine_system(snapshot("bh_ghf_noncollinear")), 50)]
+    return [A.AfqmcEngine(s, W, dt=2e-4, seed=seed0 + i, precision=capi.PRECISION_INT8X3)
+            for i, (s, W) in enumerate(systems)]
+
+
+def test_fused_group_block_equals_each_member_alone():
+    """Fused schedule: every stage's int8-slice products of all members (force bias, vHS, P1, Taylor
+    terms, the exchange tensor's chunks) run as ONE grouped launch; each member's blocks, its
+    measurements and walkers equal its blocks run alone bit for bit, captured and replayed."""
+    grouped, alone = _int8_engines(), _int8_engines()
+    E0 = np.array([e.init() for e in grouped])
+    for e in alone:
+        e.init()
+    grp = A.EngineGroup(grouped)
+    grp.set_fused(True)
+    Eg, st, mg = grp.run_block(20, E0, step0=0, **BLK)
+    Eg2, st2, mg2 = grp.run_block(20, Eg, step0=20, **BLK)  # the replayed graph
+    assert not st.any() and not st2.any()
+    for i, e in enumerate(alone):
+        Ea, ma = e.run_block(20, E0[i], step0=0, **BLK)
+        Ea2, ma2 = e.run_block(20, Ea, step0=20, **BLK)
+        assert Eg[i] == Ea and Eg2[i] == Ea2, i
+        assert len(mg[i]) == len(ma) == 2 and np.array_equal(mg[i], ma) and np.array_equal(mg2[i], ma2), i
+        S1, p1 = grouped[i].walkers()
+        S2, p2 = e.walkers()
+        assert np.array_equal(S1, S2), i
+        for k in ("WEIGHT", "OVLP", "PHASE"):
+            assert np.array_equal(p1[k], p2[k]), (i, k)
+    # back to lanes: the same members, a block each way again equal
+    grp.set_fused(False)
+    grp.set_lanes(1)
+    Eg3, st3, _m = grp.run_block(10, Eg2, step0=40, **BLK)
+    for i, e in enumerate(alone):
+        Ea3, _m = e.run_block(10, Eg2[i], step0=40, **BLK)
+        assert Eg3[i] == Ea3
+    grp.close()
+    for e in grouped + alone:
+        e.close()
+
+
+def test_fused_group_refusals():
+    es = _engines()[:2]  # split-BF16 members: no int8-slice products to group
+    grp = A.EngineGroup(es)
+    with pytest.raises(capi.SafireError) as ex:
+        grp.set_fused(True)
+    assert ex.value.code == 3
+    grp.close()
+    for e in es:
+        e.close()
+    es = _int8_engines()[:2]
+    grp = A.EngineGroup(es)
+    grp.set_fused(True)
+    E0 = np.array([e.init() for e in es])
+    rps_a = dict(BLK)
+    rps_b = dict(BLK, ortho_interval=4)
+    grp.block_async(10, E0, **rps_a)
+    grp.block_result()
+    # one member on another block schedule: refused before anything runs
+    with pytest.raises(capi.SafireError) as ex:
+        grp.block_async(10, E0, step0=[0, 3], **rps_b)
+    assert ex.value.code == 2
+    grp.close()
+    for e in es:
+        e.close()
+
+
 def test_group_rejects_bad_use():
     es = _engines()[:2]
     with pytest.raises(capi.SafireError):

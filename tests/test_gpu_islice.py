@@ -186,6 +186,40 @@ def test_int8x3_collinear_walkers_vs_fp64_engine():
     e8.close()
 
 
+@pytest.mark.parametrize("case", ["bh_ghf_noncollinear", "bh_uhf_noncollinear"])
+def test_int8x3_noncollinear_walkers_vs_fp64_engine(case):
+    """NONCOLLINEAR walkers (the reference's BH spinor fixtures, M=19 in 2M=38 spinor rows, N=6,
+    Nc=78; the GHF trial mixes the components) in INT8X3 against the FP64 engine, which reproduces
+    the reference's recorded runs: the trial's energy, the energies of identical walkers, and three
+    steps from identical walkers and seeded fields, at the 3-slice bounds of the closed-shell test."""
+    from tests.golden_io import engine_system, snapshot
+    s = engine_system(snapshot(case))
+    W, dt = 32, 0.01
+    e64 = afqmc.AfqmcEngine(s, W, dt=dt, seed=5, precision=capi.PRECISION_FP64)
+    e8 = afqmc.AfqmcEngine(s, W, dt=dt, seed=5, precision=capi.PRECISION_INT8X3)
+    E64, E8 = e64.init(), e8.init()
+    assert abs(E8 - E64) < 2e-6 * abs(E64)
+    for st in range(3):  # walkers away from the trial
+        e64.propagate(E64, st)
+    SM, pr = e64.walkers()
+    assert SM.shape == (W, 2 * s.M, s.N)
+    e8.set_walkers(SM, pr)
+    assert _rel(e8.energy(), e64.energy()) < 2e-6
+    for st in (7, 8, 9):
+        e64.propagate(E64, st)
+        e8.propagate(E64, st)
+        X8, X64 = (e.fetch("X", (W, s.Nc), np.complex128) for e in (e8, e64))
+        assert _rel(X8, X64) < 1e-6 * (st - 6)
+    S8, p8 = e8.walkers()
+    S64, p64 = e64.walkers()
+    assert _rel(S8, S64) < 6e-6
+    assert _rel(p8["OVLP"], p64["OVLP"]) < 1.5e-5
+    assert _rel(p8["WEIGHT"], p64["WEIGHT"]) < 6e-5
+    assert _rel(e8.energy(), e64.energy()) < 2e-6
+    e64.close()
+    e8.close()
+
+
 def test_bounded_waits_expire_and_report_timeout():
     """The product's loads are held back by a flag nothing sets and every wait is limited to 1 ms:
     each wait expires, the kernel reports SFQ_ERR_TIMEOUT with nothing in flight and its tensor
