@@ -421,7 +421,7 @@ int sfq_engine_block_result(sfq_engine_t e, double* Eshift, double* meas, int ma
 /* bytes of device memory the engine holds (its arena and packed tensors) */
 int sfq_engine_footprint(sfq_engine_t e, size_t* bytes);
 
-/* ---- tile autotuner (mixed precision only) ----------------------------------------------------
+/* ---- tile autotuner (the tensor-core precisions) -----------------------------------------------
  * The tensor-core products are tiled in output tiles of 128 rows by a width the kernel is built
  * for (64, 128, 160 with any plane count; 208, 256 with at most 2 planes).  sfq_engine_autotune
  * times every built width of each product on the engine's own operands (the current walkers; only
@@ -435,7 +435,10 @@ int sfq_engine_footprint(sfq_engine_t e, size_t* bytes);
  * engines given the same tiles (sfq_engine_set_tiles; 0 = the built-in choice) produce identical
  * results.  Setting tiles drops the engine's captured block graphs.  us_builtin / us_tuned: median
  * time of each product (G, force bias, vHS, one Taylor term, both P1 products) with the built-in
- * and the chosen tiles (0 when a product was not timed).  No counterpart in the reference. */
+ * and the chosen tiles (0 when a product was not timed).  The int8-slice precisions tile only the
+ * Taylor terms by choice (taylor_half 32, 64 or 80; the other widths are fixed and reported, g_bn = 0
+ * as G is FP64): their exact integer accumulation gives the same results bit for bit at every
+ * width, and the tuner times the three on the engine's operands.  No counterpart in the reference. */
 typedef struct {
   int g_bn, vbias_bn, vhs_bn, taylor_half, p1_bn;
   int vbias_ksplit; /* force-bias K split; set_tiles: 0 = planned from vbias_bn */

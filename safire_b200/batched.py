@@ -90,7 +90,7 @@ def main():
                measure_interval=a.steps, relax=BLOCK["relax"], steer=True)
     prec = {"int8x3": capi.PRECISION_INT8X3, "mixed-fp32": capi.PRECISION_MIXED_FP32,
             "mixed": capi.PRECISION_MIXED}[a.precision]
-    tunable = prec != capi.PRECISION_INT8X3  # the int8-slice products run fixed tiles
+    tunable = True  # split-BF16: every product's width; int8 slices: the Taylor term's orbitals per tile
 
     # resident mixed engines, autotuned
     t0 = time.time()

@@ -547,7 +547,7 @@ struct Engine {
   // spinor components q of a NONCOLLINEAR walker are two (M, N) blocks that V and P1 act on alike),
   // and k runs over the Mr = npol M rows of the G-shaped arrays
   int nslices = 0;
-  long ld_m = 0, ld_mr = 0, ld_nm = 0, ld_nc = 0;  // slice row strides (bytes): M, Mr, N*Mr, Nc rounded up to 16
+  long ld_m = 0, ld_mr = 0, ld_nm = 0, ld_nc = 0;  // slice row strides (bytes): M, Mr, N*Mr, Nc rounded up to 64
   int8_t* Lv_q[3] = {};  int* Lv_e = nullptr;   // Lnak, rows n over (a, k): the force bias's B
   int8_t* Le_q[3] = {};  int* Le_e = nullptr;   // Lnak, rows (n, a) over k: the exchange tensor's B
   int8_t* Lh_q[3] = {};  int* Lh_e = nullptr;   // L, rows (i, k) (packed pairs when symmetric) over n: vHS's B
@@ -561,7 +561,7 @@ struct Engine {
   cplx* GT_c = nullptr;  // the trial's own G (N, Mr) and force bias (Nc), FP64
   cplx* vbT = nullptr;
   float* Cp = nullptr;  // FP32 output of the walker-shaped products, planar (2 W N, M)
-  int i8_vb_bn = 160, i8_vb_ks = 1, i8_bn = 160, i8_half = 80;
+  int i8_vb_bn = 160, i8_vb_ks = 1, i8_bn = 160, i8_half = 80, i8_half_req = 0;
   double* h_pinned = nullptr;  // pinned host staging for e2e calls
   size_t h_pinned_bytes = 0;
   // device-resident block driver: Eshift, the step counter and the block's measurements in device
@@ -1865,7 +1865,7 @@ struct Engine {
   // set the tiles (0: the built-in choice); the captured block graphs are dropped
   int set_tiles(int gbn, int vbbn, int vhsbn, int half, int p1bn, int vbks = 0) {
     if (!mixed) return record_error(SFQ_ERR_UNSUPPORTED, "tiles: only the mixed-precision products are tiled");
-    if (nslices) return record_error(SFQ_ERR_UNSUPPORTED, "tiles: the int8-slice products keep their planned tiles");
+    if (nslices) return set_tiles_i8(gbn, vbbn, vhsbn, half, p1bn, vbks);
     for (int bn : {gbn, vbbn, vhsbn, p1bn})
       if (bn && !tile_built(bn))
         return record_error(SFQ_ERR_ARG, "tiles: width %d is not built for %d planes", bn, nplanes);
@@ -1892,7 +1892,30 @@ struct Engine {
     graphs.clear();
   }
 
+  // the int8-slice products: only the Taylor term's orbitals per tile are a choice (32, 64 or 80;
+  // 0 = the planned one, the least padding of M); the other widths are fixed (0 or their value)
+  int set_tiles_i8(int gbn, int vbbn, int vhsbn, int half, int p1bn, int vbks) {
+    if (gbn || (vbbn && vbbn != i8_vb_bn) || (vhsbn && vhsbn != i8_bn) || (p1bn && p1bn != i8_bn) ||
+        (vbks && vbks != i8_vb_ks))
+      return record_error(SFQ_ERR_ARG, "tiles: the int8-slice products only tile the Taylor term (orbitals per tile)");
+    if (half && half != 32 && half != 64 && half != 80)
+      return record_error(SFQ_ERR_ARG, "tiles: Taylor half %d not built for int8 slices", half);
+    i8_half_req = half;
+    plan_i8();
+    drop_graphs();
+    return SFQ_OK;
+  }
+
   void get_tiles(sfq_tiles_t* t) const {
+    if (nslices) {
+      t->g_bn = 0;  // G is FP64
+      t->vbias_bn = i8_vb_bn;
+      t->vhs_bn = i8_bn;
+      t->taylor_half = i8_half;
+      t->p1_bn = i8_bn;
+      t->vbias_ksplit = i8_vb_ks;
+      return;
+    }
     t->g_bn = g_tile();
     t->vbias_bn = vb_bn;
     t->vhs_bn = vhs_bn ? vhs_bn : 128;
@@ -1997,15 +2020,51 @@ struct Engine {
   // walkers, their weights and overlaps are not modified (only scratch buffers are written)
   int autotune(int reps, sfq_tiles_t* out) {
     if (!mixed) return record_error(SFQ_ERR_UNSUPPORTED, "autotune: only the mixed-precision products are tiled");
-    if (nslices) {  // the int8-slice products keep their planned tiles
-      if (out) get_tiles(out);
-      return SFQ_OK;
-    }
     const bool prof = profile;
     profile = false;
-    const int rc = autotune_run(reps < 1 ? 9 : reps, out);
+    const int rc = nslices ? autotune_i8(reps < 1 ? 9 : reps, out) : autotune_run(reps < 1 ? 9 : reps, out);
     profile = prof;
     return rc;
+  }
+
+  // the int8-slice Taylor product at each built width (exact accumulation: every width gives the
+  // same results bit for bit), on real operands: the step's stages up to the first Taylor term
+  // (they write only per-step scratch, not the walkers or their properties)
+  int autotune_i8(int reps, sfq_tiles_t* out) {
+    int rc;
+    IsliceGemmDesc d;
+    bool more = true;
+    for (int s = 0; s < 4 && more; ++s) {
+      if ((rc = propagate_i8_stage(s, 0.0, 0, nullptr, &d, &more))) return rc;
+      if (s < 3 && (rc = islice_gemm(d, st))) return rc;
+    }
+    const int planned = i8_half;
+    double t_cur = 0.0, best = 1e300;
+    int chosen = planned;
+    for (int h : {32, 64, 80}) {
+      i8_half = h;
+      const IsliceGemmDesc dt = i8_taylor(i8_cur);
+      double us = 0.0;
+      if ((rc = time_median([&] { return islice_gemm(dt, st); }, reps, &us))) {
+        i8_half = planned;
+        return rc;
+      }
+      if (h == planned) t_cur = us;
+      if (us < best) {
+        best = us;
+        chosen = h;
+      }
+    }
+    i8_half = planned;
+    if ((rc = sync_checked())) return rc;
+    if ((rc = set_tiles_i8(0, 0, 0, chosen, 0, 0))) return rc;
+    if (out) {
+      get_tiles(out);
+      for (int i = 0; i < kTunedProducts; ++i) out->us_builtin[i] = out->us_tuned[i] = 0.0;
+      out->us_builtin[3] = t_cur;
+      out->us_tuned[3] = best;
+    }
+    return SFQ_OK;
   }
 
   int autotune_run(int reps, sfq_tiles_t* out) {
@@ -2077,14 +2136,16 @@ struct Engine {
   }
 
   // ---- exact-accumulation mode (int8 slices) ------------------------------------------------
-  static long round16(long x) { return (x + 15) / 16 * 16; }
+  // slice rows start on 64-byte boundaries: a product's 64-byte K slice of a row is then exactly two
+  // 32-byte sectors (rows 16 bytes apart made three of every such load)
+  static long round64(long x) { return (x + 63) / 64 * 64; }
   // tile shapes of the int8-slice products: Taylor tiles of `half` orbitals (the least padding of
   // M, then the widest), the force bias split along K to fill whole waves of SMs
   void plan_i8() {
-    ld_m = round16(M);
-    ld_mr = round16(Mr);
-    ld_nm = round16((long)N * Mr);
-    ld_nc = round16(Nc);
+    ld_m = round64(M);
+    ld_mr = round64(Mr);
+    ld_nm = round64((long)N * Mr);
+    ld_nc = round64(Nc);
     int best = 0;
     long best_pad = 1L << 40;
     for (int h : {32, 64, 80}) {
@@ -2094,7 +2155,7 @@ struct Engine {
         best_pad = pad;
       }
     }
-    i8_half = best;
+    i8_half = i8_half_req ? i8_half_req : best;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device);
     const long tiles = (long)((2 * W + 127) / 128) * ((Nc + i8_vb_bn - 1) / i8_vb_bn);

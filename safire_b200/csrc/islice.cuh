@@ -19,8 +19,8 @@
 // products at twice the rate); 2 slices: 3.
 //
 // Persistent kernel: one CTA per SM walks a static list of 128 x BN output tiles; warp 0 issues
-// TMA loads of 128-byte K slices (128 int8 elements) into a ring of stages, one thread of warp 1
-// issues tcgen05.mma.kind::i8 (M = 128, N = BN, K = 32) and commits each stage, eight epilogue
+// TMA loads of 64-byte K slices (64 int8 elements, 64-byte swizzle) into a ring of 4 to 8 stages,
+// one thread of warp 1 issues tcgen05.mma.kind::i8 (M = 128, N = BN, K = 32) and commits each stage, eight epilogue
 // warps drain the group accumulators.  K tails are zero-filled by TMA and their MMA steps skipped.
 // Every mbarrier wait is bounded from its own start; on expiry the kernel records SFQ_ERR_TIMEOUT,
 // waits for its own copies and MMAs, frees its tensor memory and returns.

@@ -10,7 +10,7 @@ namespace islice {
 using namespace tc;
 
 constexpr int BM = 128;                  // MMA M: accumulator rows = TMEM lanes
-constexpr int BK = 128;                  // int8 elements per K slice = one 128-byte swizzle row
+constexpr int BK = 64;                   // int8 elements per K slice = one 64-byte swizzle row
 constexpr int KSTEP = 32;                // K of one kind::i8 MMA
 // warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2-9 epilogue (two per TMEM lane quarter, taking
 // alternate 16-column chunks of the tile)
@@ -40,6 +40,18 @@ __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t adesc, uint64_
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
       ::"r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2),
         "r"(mask3));
+}
+
+// K-major operand tile, 64-byte swizzle: rows of 64 bytes (one K slice), 8-row groups 512 bytes apart
+__device__ __forceinline__ uint64_t smem_desc_k64(const void* tile) {
+  const uint64_t addr = su32(tile);
+  uint64_t d = 0;
+  d |= (addr & 0x3FFFFull) >> 4;        // start address
+  d |= uint64_t(1) << 16;               // leading byte offset (unused for swizzled K-major)
+  d |= uint64_t(512 >> 4) << 32;        // stride byte offset: next 8-row group
+  d |= uint64_t(1) << 46;               // descriptor version (sm_100)
+  d |= uint64_t(4) << 61;               // SWIZZLE_64B
+  return d;
 }
 
 __host__ __device__ constexpr uint32_t pow2_ceil(uint32_t x) {
@@ -134,6 +146,36 @@ __device__ __forceinline__ double pow2(int e) {
   return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
+// tensor-memory loads of a chunk's groups issued back to back, then one wait; the wait names the
+// registers so that nothing reads them before it
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld(uint32_t* r) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
+}
+
+// first output column of the tile's chunk at accumulator column c (complex B: and its part, re or
+// im); the same for the whole warp
+template <int BN>
+__device__ __forceinline__ int chunk_col0(const KParams& p, int nt, int c, int* part) {
+  if (p.half) {  // complex B: [re | im] halves of `half` orbitals
+    const int pt = c >= p.half ? 1 : 0;
+    *part = pt;
+    return nt * p.half + (c - pt * p.half);
+  }
+  *part = 0;
+  return nt * BN + c;
+}
+
 // the 16-column chunks c0, c0 + 32, ... of one tile's accumulator groups at taddr (group g at column
 // g * BN) -> FP32 output, row `row`
 template <int BN, int NS>
@@ -141,63 +183,76 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
                                               int ks, int c0) {
   const int gm = mt * BM + row;
   const bool live = gm < p.M;
-  const int ea = live ? p.ea[(long)bz * p.ea_bs + (p.ea_mod ? gm % p.ea_mod : gm)] : 0;
   const int width = p.half ? 2 * p.half : BN;  // complex B: the [re | im] halves may be narrower than BN
+  const int lane = threadIdx.x & 31;
+  // the column exponents of all of this thread's chunks c0 + 32 j, loaded before the first one:
+  // lanes 0-15 hold chunk 2m's 16 columns in eb2[m], lanes 16-31 chunk 2m + 1's
+  constexpr int NPAIR = ((BN + 31) / 32 + 1) / 2;
+  int eb2[NPAIR];
+#pragma unroll
+  for (int m = 0; m < NPAIR; ++m) {
+    const int c = c0 + 32 * (2 * m + (lane >> 4));
+    int e = 0;
+    if (c < width) {
+      int part;
+      const int col0 = chunk_col0<BN>(p, nt, c, &part);
+      if (col0 < p.N) {
+        const int col = col0 + (lane & 15) < p.N ? col0 + (lane & 15) : p.N - 1;
+        e = p.eb[(long)bz * p.eb_bs + (p.eb_mod ? col % p.eb_mod : col)];
+      }
+    }
+    eb2[m] = e;
+  }
+  const int ea = live ? p.ea[(long)bz * p.ea_bs + (p.ea_mod ? gm % p.ea_mod : gm)] : 0;
 #pragma unroll 1
-  for (int c = c0; c < width; c += 32) {
+  for (int j = 0;; ++j) {
+    const int c = c0 + 32 * j;
+    if (c >= width) break;
     uint32_t acc[3][16];
     __syncwarp();
 #pragma unroll
-    for (int g = 0; g < NS; ++g) tmem_ld16_u32(taddr + uint32_t(g * BN + c), acc[g]);
-    long obase;
-    int col0, valid;
-    if (p.half) {  // complex B: [re | im] halves of `half` orbitals
-      const int part = c >= p.half ? 1 : 0;
-      col0 = nt * p.half + (c - part * p.half);
-      if (col0 >= p.N) continue;
-      valid = p.N - col0 < 16 ? p.N - col0 : 16;
-      obase = (long)part * p.sCc + ((long)bz * p.M + gm) * p.ldc + col0;
-    } else {
-      col0 = nt * BN + c;
-      if (col0 >= p.N) continue;
-      valid = p.N - col0 < 16 ? p.N - col0 : 16;
-      obase = (long)ks * p.sCk + (long)bz * p.sCb + (long)gm * p.ldc + col0;
-    }
+    for (int g = 0; g < NS; ++g) tmem_ld16_nowait(taddr + uint32_t(g * BN + c), acc[g]);
+#pragma unroll
+    for (int g = 0; g < NS; ++g) tmem_wait_ld(acc[g]);
+    int part;
+    const int col0 = chunk_col0<BN>(p, nt, c, &part);
+    if (col0 >= p.N) continue;
+    const int valid = p.N - col0 < 16 ? p.N - col0 : 16;
+    const long obase = p.half ? (long)part * p.sCc + ((long)bz * p.M + gm) * p.ldc + col0
+                              : (long)ks * p.sCk + (long)bz * p.sCb + (long)gm * p.ldc + col0;
     // (col0 is the same for the whole warp; every lane takes part in the broadcast below, rows past
     // M included, whose results are dropped)
-    // the chunk's 16 column exponents: one load by lanes 0-15, then broadcast
-    const int lane = threadIdx.x & 31;
-    int ebl = 0;
-    {
-      const int col = col0 + (lane & 15) < p.N ? col0 + (lane & 15) : p.N - 1;
-      ebl = p.eb[(long)bz * p.eb_bs + (p.eb_mod ? col % p.eb_mod : col)];
-    }
+    int ebs = eb2[0];
+#pragma unroll
+    for (int m = 1; m < NPAIR; ++m)
+      if ((j >> 1) == m) ebs = eb2[m];
+    const int src = (j & 1) << 4;
     float v[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int eb = __shfl_sync(0xffffffffu, ebl, j);
+    for (int jj = 0; jj < 16; ++jj) {
+      const int eb = __shfl_sync(0xffffffffu, ebs, src + jj);
       // acc0 2^16 + acc1 2^8 + acc2: exact in int64 (< 2^48) and in its conversion to FP64 (< 2^53)
-      long long s = (long long)int(acc[0][j]) << (8 * (NS - 1));
-      if (NS > 1) s += (long long)int(acc[1][j]) << (8 * (NS - 2));
-      if (NS > 2) s += (long long)int(acc[2][j]);
-      v[j] = __double2float_rn(double(s) * pow2(ea + eb - 8 * (NS - 1)) * p.alpha);
+      long long sum = (long long)int(acc[0][jj]) << (8 * (NS - 1));
+      if (NS > 1) sum += (long long)int(acc[1][jj]) << (8 * (NS - 2));
+      if (NS > 2) sum += (long long)int(acc[2][jj]);
+      v[jj] = __double2float_rn(double(sum) * pow2(ea + eb - 8 * (NS - 1)) * p.alpha);
     }
     if (!live) continue;
     float* out = p.C + obase;
     const bool vec = valid == 16 && (obase % 4) == 0;
     if (p.accumulate) {
 #pragma unroll
-      for (int j = 0; j < 16; ++j)
-        if (j < valid) v[j] = __fadd_rn(v[j], out[j]);
+      for (int jj = 0; jj < 16; ++jj)
+        if (jj < valid) v[jj] = __fadd_rn(v[jj], out[jj]);
     }
     if (vec) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        reinterpret_cast<float4*>(out)[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+      for (int jj = 0; jj < 4; ++jj)
+        reinterpret_cast<float4*>(out)[jj] = make_float4(v[4 * jj], v[4 * jj + 1], v[4 * jj + 2], v[4 * jj + 3]);
     } else {
 #pragma unroll
-      for (int j = 0; j < 16; ++j)
-        if (j < valid) out[j] = v[j];
+      for (int jj = 0; jj < 16; ++jj)
+        if (jj < valid) out[jj] = v[jj];
     }
   }
 }
@@ -355,8 +410,8 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
           uint64_t ad[NS], bd[NS];
 #pragma unroll
           for (int q = 0; q < NS; ++q) {
-            ad[q] = smem_desc(stg + q * L::A_BYTES);
-            bd[q] = smem_desc(stg + NS * L::A_BYTES + q * L::B_BYTES);
+            ad[q] = smem_desc_k64(stg + q * L::A_BYTES);
+            bd[q] = smem_desc_k64(stg + NS * L::A_BYTES + q * L::B_BYTES);
           }
           const int k0 = cb ? (kt >> 1) * BK : kt * BK;
           const int rem = Kv - k0;
@@ -436,7 +491,7 @@ int make_map_i8(CUtensorMap* m, const void* base, long rows, long K, long ld, lo
   cuuint32_t box[3] = {cuuint32_t(BK), cuuint32_t(box_rows), 1};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return record_error(SFQ_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
   return SFQ_OK;
@@ -530,7 +585,7 @@ int launch(const IsliceGemmDesc& d, cudaStream_t st) {
 
 // the grouped launches' tile widths: every plain product of a group has tile width kGroupBN
 constexpr int kGroupBN = 160;
-constexpr int group_stages(int ns) { return ns == 2 ? 3 : 2; }
+constexpr int group_stages(int ns) { return ns == 2 ? 6 : 4; }
 
 template <int NS>
 int group_plan(const IsliceGemmDesc* ds, int n, IsliceGroupPlan* out) {
@@ -592,13 +647,13 @@ int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st) {
   if (d.K <= 0) return record_error(SFQ_ERR_SHAPE, "islice_gemm: K must be positive");
   const int bn = d.cplx_half > 0 ? 2 * d.cplx_half : (d.bn ? d.bn : (d.N <= 64 ? 64 : 128));
   switch (d.nslices * 1000 + bn) {
-    case 2064: return islice::launch<64, 4, 2>(d, st);
-    case 2128: return islice::launch<128, 3, 2>(d, st);
-    case 2160: return islice::launch<160, 3, 2>(d, st);
-    case 3064: return islice::launch<64, 3, 3>(d, st);
-    case 3080: return islice::launch<80, 2, 3>(d, st);
-    case 3128: return islice::launch<128, 2, 3>(d, st);
-    case 3160: return islice::launch<160, 2, 3>(d, st);
+    case 2064: return islice::launch<64, 8, 2>(d, st);
+    case 2128: return islice::launch<128, 6, 2>(d, st);
+    case 2160: return islice::launch<160, 6, 2>(d, st);
+    case 3064: return islice::launch<64, 6, 3>(d, st);
+    case 3080: return islice::launch<80, 5, 3>(d, st);
+    case 3128: return islice::launch<128, 4, 3>(d, st);
+    case 3160: return islice::launch<160, 4, 3>(d, st);
     default:
       return record_error(SFQ_ERR_ARG, "islice_gemm: %d slices with tile width %d not built", d.nslices, bn);
   }

@@ -208,6 +208,43 @@ def test_tile_choices_keep_mixed_accuracy(tiles):
     e64.close()
 
 
+def test_int8_taylor_tiles_tuned_and_exact():
+    """INT8X3: the Taylor term's orbitals per tile (32, 64, 80) change only the tiling of an exact
+    integer product, so blocks at every width are equal bit for bit; the tuner picks one of them
+    from timings on the engine's operands and writes no walker state."""
+    spec = synthetic.SystemSpec(M=144, N=36, Nc=720, decay=144.0, seed=43)
+    s = synthetic.make_system(spec)
+    W = 96
+    out = []
+    for h in (32, 64, 80):
+        e = A.AfqmcEngine(s, W, dt=2e-4, seed=6, precision=capi.PRECISION_INT8X3)
+        E0 = e.init()
+        e.set_tiles(taylor_half=h)
+        assert e.tiles()["taylor_half"] == h
+        out.append((e.run_block(10, E0, step0=0, **BLK), e.walkers()))
+        e.close()
+    for (Eb, mb), (S, p) in out[1:]:
+        assert Eb == out[0][0][0] and np.array_equal(mb, out[0][0][1])
+        assert np.array_equal(S, out[0][1][0]) and np.array_equal(p["WEIGHT"], out[0][1][1]["WEIGHT"])
+    e = A.AfqmcEngine(s, W, dt=2e-4, seed=6, precision=capi.PRECISION_INT8X3)
+    E0 = e.init()
+    SM0, pr0 = e.walkers()
+    t = e.autotune(repeats=5)
+    ch = t.choice()
+    assert ch["taylor_half"] in (32, 64, 80) and ch["g_bn"] == 0
+    assert 0.0 < t.us_tuned[3] <= t.us_builtin[3] * 1.0000001
+    SM1, pr1 = e.walkers()
+    assert np.array_equal(SM0, SM1) and np.array_equal(pr0["WEIGHT"], pr1["WEIGHT"])
+    assert e.run_block(10, E0, step0=0, **BLK)[0] == out[0][0][0]
+    with pytest.raises(capi.SafireError) as ex:
+        e.set_tiles(taylor_half=48)
+    assert ex.value.code == 2
+    with pytest.raises(capi.SafireError) as ex:
+        e.set_tiles(g_bn=64)
+    assert ex.value.code == 2
+    e.close()
+
+
 def test_tiles_rejected():
     s = synthetic.make_system(synthetic.SystemSpec(M=48, N=12, Nc=240, decay=48.0, seed=42))
     e = A.AfqmcEngine(s, 32, dt=2e-4, seed=1, precision=capi.PRECISION_MIXED_FP32)
