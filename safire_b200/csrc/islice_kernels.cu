@@ -217,6 +217,16 @@ __global__ void rows_planar_kernel(const cplx* src, long R, long K, int ns, Q q,
 // long rows split over blocks: pass 1, each chunk's largest |re| and |im| into the row's maxima
 // (non-negative doubles order like their bits, so a 64-bit atomic max is exact); pass 2 slices
 constexpr long kPlanarChunk = 4096;
+// four consecutive elements of row x (minus sub) from k: zeros past K
+__device__ __forceinline__ void load4c(const cplx* x, const cplx* sub, long k, long K, cplx (&z)[4]) {
+#pragma unroll
+  for (int u = 0; u < 4; ++u) z[u] = k + u < K ? x[k + u] : mk(0.0, 0.0);
+  if (sub) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (k + u < K) z[u] = csub(z[u], sub[k + u]);
+  }
+}
 __global__ void __launch_bounds__(256) planar_max_kernel(const cplx* src, long R, long K, const cplx* sub,
                                                          unsigned long long* emax) {
   __shared__ double sh[32];
@@ -224,10 +234,14 @@ __global__ void __launch_bounds__(256) planar_max_kernel(const cplx* src, long R
   const long k1 = k0 + kPlanarChunk < K ? k0 + kPlanarChunk : K;
   const cplx* x = src + r * K;
   double mr = 0.0, mi = 0.0;
-  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-    const cplx z = sub ? csub(x[k], sub[k]) : x[k];
-    mr = fmax(mr, fabs(z.x));
-    mi = fmax(mi, fabs(z.y));
+  for (long k = k0 + 4 * threadIdx.x; k < k1; k += 4 * blockDim.x) {  // four elements in flight per thread
+    cplx z[4];
+    load4c(x, sub, k, k1, z);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      mr = fmax(mr, fabs(z[u].x));
+      mi = fmax(mi, fabs(z[u].y));
+    }
   }
   mr = block_max(mr, sh);
   mi = block_max(mi, sh);
@@ -235,6 +249,15 @@ __global__ void __launch_bounds__(256) planar_max_kernel(const cplx* src, long R
     atomicMax(emax + r, (unsigned long long)__double_as_longlong(mr));
     atomicMax(emax + R + r, (unsigned long long)__double_as_longlong(mi));
   }
+}
+// four consecutive values -> one 4-byte word per slice at idx (a multiple of 4)
+__device__ __forceinline__ void put4d(const Q& q, int ns, long idx, const double (&x)[4], double s) {
+  int a[4], b[4], c[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) slice_value(x[u], s, ns, a[u], b[u], c[u]);
+  *reinterpret_cast<char4*>(q.p[0] + idx) = make_char4(char(a[0]), char(a[1]), char(a[2]), char(a[3]));
+  if (ns > 1) *reinterpret_cast<char4*>(q.p[1] + idx) = make_char4(char(b[0]), char(b[1]), char(b[2]), char(b[3]));
+  if (ns > 2) *reinterpret_cast<char4*>(q.p[2] + idx) = make_char4(char(c[0]), char(c[1]), char(c[2]), char(c[3]));
 }
 __global__ void __launch_bounds__(256) planar_slice_kernel(const cplx* src, long R, long K, const cplx* sub,
                                                            const unsigned long long* emax, int ns, Q q, long ld,
@@ -249,10 +272,17 @@ __global__ void __launch_bounds__(256) planar_slice_kernel(const cplx* src, long
   }
   const double sr = pow2d(-er), si = pow2d(-ei);
   const cplx* x = src + r * K;
-  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-    const cplx z = k < K ? (sub ? csub(x[k], sub[k]) : x[k]) : mk(0.0, 0.0);
-    put(q, ns, r * ld + k, z.x, sr);
-    put(q, ns, (R + r) * ld + k, z.y, si);
+  for (long k = k0 + 4 * threadIdx.x; k < k1; k += 4 * blockDim.x) {  // ld and k0 are multiples of 4
+    cplx z[4];
+    load4c(x, sub, k, K, z);
+    double xr[4], xi[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      xr[u] = z[u].x;
+      xi[u] = z[u].y;
+    }
+    put4d(q, ns, r * ld + k, xr, sr);
+    put4d(q, ns, (R + r) * ld + k, xi, si);
   }
 }
 
@@ -417,44 +447,93 @@ void launch_taylor_update(const float* C, float* S, long R, int M, int k, bool s
   }
 }
 
-// vHS row maxima over k and both parts, per (w, i), as float bits (non-negative floats order as ints)
-constexpr int kVT = 64;
-__global__ void __launch_bounds__(256) v_max_packed_kernel(const float* Cv, int W, int M, int T, int* emax) {
-  __shared__ float tile[kVT][kVT + 1];
-  const int wc = blockIdx.y, w = wc % W;
-  int t = blockIdx.x, ib = 0;
-  while (ib < T && t >= T - ib) {
-    t -= T - ib;
-    ++ib;
-  }
-  const int kb = ib + t;
-  const int i0 = ib * kVT, k0 = kb * kVT;
-  const float* src = Cv + (long)wc * ((long)M * (M + 1) / 2);
-  const int tid = threadIdx.x;
-  {
-    const int qc = tid % kVT, r0 = tid / kVT;
+// V slices from the packed vHS, one block per (walker, strip of rs <= 32 rows): both parts' full rows
+// V[w][c][i][0..M) in shared memory, from the stored upper triangle (packed row i holds k >= i) and
+// its mirror (k < i: packed row k, column i; the strip's columns lie side by side in every earlier
+// packed row, so both are read in whole rows); each row's exponent from its maximum over both parts;
+// then whole rows of the slices of Vr, Vi and -Vi (zeros past M up to ld), four orbitals per thread
+__global__ void __launch_bounds__(512) v_strip_kernel(const float* Cv, int W, int M, int rs, int lds, int ns, Q q,
+                                                      long ld, int* e) {
+  extern __shared__ float vs[];  // [2][rs][lds]
+  __shared__ float scale[32];
+  const int w = blockIdx.y, i0 = blockIdx.x * rs;
+  const int rows = M - i0 < rs ? M - i0 : rs;
+  const long P = (long)M * (M + 1) / 2;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int c = 0; c < 2; ++c) {
+    const float* src = Cv + ((long)c * W + w) * P;
+    float* t = vs + c * rs * lds;
+    for (int r = warp; r < rows; r += nw) {  // the strip's rows, k >= i: four loads in flight per lane
+      const int i = i0 + r;
+      const float* row = src + (long)i * M - (long)i * (i + 1) / 2;
+      for (int k = i + lane; k < M; k += 128) {
+        float v[4];
 #pragma unroll
-    for (int s = 0; s < kVT / 4; ++s) {
-      const int r = r0 + 4 * s;
-      const long i = i0 + r, k = k0 + qc;
-      tile[r][qc] = (i < M && k < M && i <= k) ? fabsf(src[i * M - i * (i + 1) / 2 + k]) : 0.f;
+        for (int u = 0; u < 4; ++u) v[u] = k + 32 * u < M ? row[k + 32 * u] : 0.f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (k + 32 * u < M) t[r * lds + k + 32 * u] = v[u];
+      }
+    }
+    // earlier rows k < i0: their columns i0 .. i0 + rows - 1, four rows in flight per warp
+    for (int k = warp; k < i0; k += 4 * nw) {
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int kk = k + u * nw;
+        v[u] = (kk < i0 && lane < rows) ? src[(long)kk * M - (long)kk * (kk + 1) / 2 + i0 + lane] : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int kk = k + u * nw;
+        if (kk < i0 && lane < rows) t[lane * lds + kk] = v[u];
+      }
     }
   }
   __syncthreads();
-  if (tid < kVT) {  // row i0 + tid: V[i][k] over the tile's k
+  for (int c = 0; c < 2; ++c) {  // the strip's own lower triangle, i0 <= k < i
+    float* t = vs + c * rs * lds;
+    for (int el = threadIdx.x; el < rows * rows; el += blockDim.x) {
+      const int r = el / rows, rk = el - r * rows;
+      if (rk < r) t[r * lds + i0 + rk] = t[rk * lds + i0 + r];
+    }
+  }
+  __syncthreads();
+  for (int r = warp; r < rows; r += nw) {
     float m = 0.f;
-    for (int c = 0; c < kVT; ++c) m = fmaxf(m, tile[tid][c]);
-    if (i0 + tid < M) atomicMax(emax + (long)w * M + i0 + tid, __float_as_int(m));
-  } else if (tid < 2 * kVT && ib != kb) {  // row k0 + c: the mirrored V[k][i] over the tile's i
-    const int c = tid - kVT;
-    float m = 0.f;
-    for (int r = 0; r < kVT; ++r) m = fmaxf(m, tile[r][c]);
-    if (k0 + c < M) atomicMax(emax + (long)w * M + k0 + c, __float_as_int(m));
-  } else if (tid < 2 * kVT) {  // diagonal tile: the lower half mirrored into row k0 + c
-    const int c = tid - kVT;
-    float m = 0.f;
-    for (int r = 0; r < c; ++r) m = fmaxf(m, tile[r][c]);
-    if (k0 + c < M) atomicMax(emax + (long)w * M + k0 + c, __float_as_int(m));
+    for (int c = 0; c < 2; ++c)
+      for (int k = lane; k < M; k += 32) m = fmaxf(m, fabsf(vs[(c * rs + r) * lds + k]));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const int ex = row_exponent(double(m));
+    if (lane == 0) {
+      e[(long)w * M + i0 + r] = ex;
+      scale[r] = pow2f(-ex);
+    }
+  }
+  __syncthreads();
+  const long vb = (long)w * 3 * M * ld;
+  for (int r = warp; r < rows; r += nw) {
+    const long i = i0 + r;
+    const float sc = scale[r];
+    const float* tr = vs + r * lds;
+    const float* ti = vs + (rs + r) * lds;
+    for (int k = 4 * lane; k < ld; k += 128) {
+      float xr[4], xi[4];
+      if (k + 3 < M) {
+        const float4 a = *reinterpret_cast<const float4*>(tr + k), b = *reinterpret_cast<const float4*>(ti + k);
+        xr[0] = a.x; xr[1] = a.y; xr[2] = a.z; xr[3] = a.w;
+        xi[0] = b.x; xi[1] = b.y; xi[2] = b.z; xi[3] = b.w;
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          xr[u] = k + u < M ? tr[k + u] : 0.f;
+          xi[u] = k + u < M ? ti[k + u] : 0.f;
+        }
+      }
+      put4f(q, ns, vb + i * ld + k, xr, sc);
+      put4f_pm(q, ns, vb + ((long)M + i) * ld + k, vb + (2L * M + i) * ld + k, xi, sc);
+    }
   }
 }
 
@@ -474,81 +553,6 @@ __global__ void v_max_full_kernel(const float* Cv, int W, int M, int* emax) {
 __global__ void v_exponent_kernel(const int* emax, long n, int* e) {
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
     e[t] = row_exponent(double(__int_as_float(emax[t])));
-}
-
-// V slices: one block per 64 x 64 tile pair of one planar row, V[w][c][i][k] and its mirror; the
-// imaginary row (c = 1) also as its negation, block c = 2 (sliced as -x, the same exponent)
-template <bool VEC>
-__global__ void __launch_bounds__(256) v_slice_packed_kernel(const float* Cv, int W, int M, int T, int ns, Q q,
-                                                               long ld, const int* e) {
-  __shared__ float tile[kVT][kVT + 1];
-  const int wc = blockIdx.y;
-  const int c = wc / W, w = wc - c * W;
-  int t = blockIdx.x, ib = 0;
-  while (ib < T && t >= T - ib) {
-    t -= T - ib;
-    ++ib;
-  }
-  const int kb = ib + t;
-  const int i0 = ib * kVT, k0 = kb * kVT;
-  const float* src = Cv + (long)wc * ((long)M * (M + 1) / 2);
-  const long vbase = ((long)w * 3 + c) * M * ld;
-  const long nbase = c == 1 ? vbase + (long)M * ld : -1;  // -Vi
-  const int* ew = e + (long)w * M;
-  const int tid = threadIdx.x;
-  {
-    const int qc = tid % kVT, r0 = tid / kVT;
-#pragma unroll
-    for (int s = 0; s < kVT / 4; ++s) {
-      const int r = r0 + 4 * s;
-      const long i = i0 + r, k = k0 + qc;
-      tile[r][qc] = (i < M && k < M && i <= k) ? src[i * M - i * (i + 1) / 2 + k] : 0.f;
-    }
-  }
-  __syncthreads();
-  if (!VEC) {  // M not a multiple of 4: one value at a time
-    for (int el = tid; el < kVT * kVT; el += 256) {
-      const int r = el / kVT, g = el % kVT;
-      const int i = i0 + r, k = k0 + g;
-      if (i >= M || k >= ld) continue;
-      const float x = k >= M ? 0.f : (i <= k ? tile[r][g] : tile[g][r]);
-      put1f(q, ns, vbase + (long)i * ld + k, x, pow2f(-ew[i]));
-      if (nbase >= 0) put1f(q, ns, nbase + (long)i * ld + k, -x, pow2f(-ew[i]));
-    }
-    if (ib == kb) return;
-    for (int el = tid; el < kVT * kVT; el += 256) {
-      const int r = el / kVT, g = el % kVT;
-      const int k = k0 + r, i = i0 + g;
-      if (k >= M || i >= M) continue;
-      put1f(q, ns, vbase + (long)k * ld + i, tile[g][r], pow2f(-ew[k]));
-      if (nbase >= 0) put1f(q, ns, nbase + (long)k * ld + i, -tile[g][r], pow2f(-ew[k]));
-    }
-    return;
-  }
-  // four consecutive columns per thread (ld is a multiple of 16 and k0 of 64: a group lies inside
-  // the row's [0, ld) or wholly past it)
-  for (int el = tid; el < kVT * kVT / 4; el += 256) {
-    const int r = el / (kVT / 4), g = 4 * (el % (kVT / 4));
-    const int i = i0 + r, k = k0 + g;
-    if (i >= M || k >= ld) continue;
-    float x[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u)  // the diagonal tile's lower half mirrored; zeros past M
-      x[u] = k + u >= M ? 0.f : (i <= k + u ? tile[r][g + u] : tile[g + u][r]);
-    if (nbase >= 0) put4f_pm(q, ns, vbase + (long)i * ld + k, nbase + (long)i * ld + k, x, pow2f(-ew[i]));
-    else put4f(q, ns, vbase + (long)i * ld + k, x, pow2f(-ew[i]));
-  }
-  if (ib == kb) return;
-  for (int el = tid; el < kVT * kVT / 4; el += 256) {
-    const int r = el / (kVT / 4), g = 4 * (el % (kVT / 4));
-    const int k = k0 + r, i = i0 + g;
-    if (k >= M || i >= M) continue;  // i < M and M a multiple of 4 (else the full path): i + 3 < M
-    float x[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) x[u] = tile[g + u][r];
-    if (nbase >= 0) put4f_pm(q, ns, vbase + (long)k * ld + i, nbase + (long)k * ld + i, x, pow2f(-ew[k]));
-    else put4f(q, ns, vbase + (long)k * ld + i, x, pow2f(-ew[k]));
-  }
 }
 
 __global__ void v_slice_full_kernel(const float* Cv, int W, int M, int ns, Q q, long ld, const int* e) {
@@ -677,26 +681,26 @@ int islice_build_v(const float* Cv, int W, int M, bool packed, int nslices, int8
                    int* emax, cudaStream_t st) {
   if (int rc = check_slices(nslices, q, ld)) return rc;
   if (ld < M || 2L * W > 65535) return record_error(SFQ_ERR_SHAPE, "islice_build_v: sizes");
-  SFQ_CUDA_TRY(cudaMemsetAsync(emax, 0, sizeof(int) * (size_t)W * M, st));
-  const int T = (M + kVT - 1) / kVT;
   if (packed) {
-    v_max_packed_kernel<<<dim3(unsigned(T * (T + 1) / 2), unsigned(2 * W)), 256, 0, st>>>(Cv, W, M, T, emax);
-  } else {
-    v_max_full_kernel<<<unsigned((2L * W * M + 7) / 8), 256, 0, st>>>(Cv, W, M, emax);
+    // strips of up to 32 rows whose two parts fit 200 KB of shared memory; rows padded to a multiple
+    // of four floats (16-byte row starts for the slicing pass's vector reads)
+    const int lds = (M + 3) / 4 * 4;
+    int rs = int((200L * 1024) / (2L * lds * sizeof(float)));
+    if (rs > 32) rs = 32;
+    if (rs < 1) return record_error(SFQ_ERR_SHAPE, "islice_build_v: nmo %d too large for a strip", M);
+    const size_t smem = 2 * sizeof(float) * (size_t)rs * lds;
+    SFQ_CUDA_TRY(cudaFuncSetAttribute(v_strip_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    v_strip_kernel<<<dim3(unsigned((M + rs - 1) / rs), unsigned(W)), 512, smem, st>>>(Cv, W, M, rs, lds, nslices,
+                                                                                       qptrs(q), ld, e);
+    SFQ_LAUNCHED();
+    return SFQ_OK;
   }
+  SFQ_CUDA_TRY(cudaMemsetAsync(emax, 0, sizeof(int) * (size_t)W * M, st));
+  v_max_full_kernel<<<unsigned((2L * W * M + 7) / 8), 256, 0, st>>>(Cv, W, M, emax);
   SFQ_LAUNCHED();
   v_exponent_kernel<<<grid_for((long)W * M), 256, 0, st>>>(emax, (long)W * M, e);
   SFQ_LAUNCHED();
-  if (packed) {
-    if (ld > (long)T * kVT) return record_error(SFQ_ERR_SHAPE, "islice_build_v: row stride beyond the tiles");
-    const dim3 grid(unsigned(T * (T + 1) / 2), unsigned(2 * W));
-    if (M % 4 == 0)  // groups of four orbitals
-      v_slice_packed_kernel<true><<<grid, 256, 0, st>>>(Cv, W, M, T, nslices, qptrs(q), ld, e);
-    else
-      v_slice_packed_kernel<false><<<grid, 256, 0, st>>>(Cv, W, M, T, nslices, qptrs(q), ld, e);
-  } else {
-    v_slice_full_kernel<<<grid_for(3L * W * M * ld), 256, 0, st>>>(Cv, W, M, nslices, qptrs(q), ld, e);
-  }
+  v_slice_full_kernel<<<grid_for(3L * W * M * ld), 256, 0, st>>>(Cv, W, M, nslices, qptrs(q), ld, e);
   SFQ_LAUNCHED();
   return SFQ_OK;
 }
