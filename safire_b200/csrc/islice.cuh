@@ -19,9 +19,11 @@
 // products at twice the rate); 2 slices: 3.
 //
 // Persistent kernel: one CTA per SM walks a static list of 128 x BN output tiles; warp 0 issues
-// TMA loads of 64-byte K slices (64 int8 elements, 64-byte swizzle) into a ring of 4 to 8 stages,
-// one thread of warp 1 issues tcgen05.mma.kind::i8 (M = 128, N = BN, K = 32) and commits each stage, eight epilogue
-// warps drain the group accumulators.  K tails are zero-filled by TMA and their MMA steps skipped.
+// TMA loads of K slices into a ring of stages (64 int8 elements per slice, 64-byte swizzle, where a
+// tile's K range is short; 128 elements, 128-byte swizzle, half the stages, where it reaches 1024),
+// one thread of warp 1 issues tcgen05.mma.kind::i8 (M = 128, N = BN, K = 32) and commits each
+// stage, eight epilogue warps drain the group accumulators.  K tails are zero-filled by TMA and
+// their MMA steps skipped; K splits fall on multiples of 128 elements at either slice width.
 // Every mbarrier wait is bounded from its own start; on expiry the kernel records SFQ_ERR_TIMEOUT,
 // waits for its own copies and MMAs, frees its tensor memory and returns.
 //
@@ -80,6 +82,7 @@ struct IsliceGroupPlan {
   std::vector<char> image;
   size_t start_off = 0;  // byte offset of the nprob + 1 tile offsets in the image
   int nprob = 0, nslices = 0;
+  int bk = 64;  // K slice width of the launch
   long tiles = 0;
   unsigned long long wait_ns = 0;
 };
@@ -112,7 +115,7 @@ int islice_taylor_update(const float* C, float* S, long R, int M, int k, bool sl
                          int8_t* const* q, long ld, int* e, cudaStream_t st);
 // vHS (planar rows c * W + w over the packed upper triangle, or over M * M) -> V slices
 // V[w][c][i][k], c = 0, 1, 2 for Vr, Vi, -Vi (the negation sliced as itself), with one exponent per
-// (w, i) shared by the three rows; emax: W * M scratch ints
+// (w, i) shared by the three rows; emax: W * M scratch ints (the full M * M form only)
 int islice_build_v(const float* Cv, int W, int M, bool packed, int nslices, int8_t* const* q, long ld, int* e,
                    int* emax, cudaStream_t st);
 // planar FP32 rows C[c][w][a][j] (+ S[c][w][a][j] when S is given, added in FP64) -> SM[w][j][a]

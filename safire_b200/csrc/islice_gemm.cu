@@ -10,7 +10,8 @@ namespace islice {
 using namespace tc;
 
 constexpr int BM = 128;                  // MMA M: accumulator rows = TMEM lanes
-constexpr int BK = 64;                   // int8 elements per K slice = one 64-byte swizzle row
+// int8 elements per K slice (BK, a template parameter): 64 (one 64-byte swizzle row) for products
+// whose tiles run over short K ranges, 128 (one 128-byte swizzle row, half the stages) for long ones
 constexpr int KSTEP = 32;                // K of one kind::i8 MMA
 // warps: 0 TMA producer, 1 TMEM owner + MMA issuer, 2-9 epilogue (two per TMEM lane quarter, taking
 // alternate 16-column chunks of the tile)
@@ -42,15 +43,18 @@ __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t adesc, uint64_
         "r"(mask3));
 }
 
-// K-major operand tile, 64-byte swizzle: rows of 64 bytes (one K slice), 8-row groups 512 bytes apart
-__device__ __forceinline__ uint64_t smem_desc_k64(const void* tile) {
+// K-major operand tile, BK-byte swizzle (64 or 128): rows of BK bytes (one K slice), 8-row groups
+// 8 BK bytes apart
+template <int BK>
+__device__ __forceinline__ uint64_t smem_desc_k(const void* tile) {
+  static_assert(BK == 64 || BK == 128, "K slice width");
   const uint64_t addr = su32(tile);
   uint64_t d = 0;
-  d |= (addr & 0x3FFFFull) >> 4;        // start address
-  d |= uint64_t(1) << 16;               // leading byte offset (unused for swizzled K-major)
-  d |= uint64_t(512 >> 4) << 32;        // stride byte offset: next 8-row group
-  d |= uint64_t(1) << 46;               // descriptor version (sm_100)
-  d |= uint64_t(4) << 61;               // SWIZZLE_64B
+  d |= (addr & 0x3FFFFull) >> 4;                  // start address
+  d |= uint64_t(1) << 16;                         // leading byte offset (unused for swizzled K-major)
+  d |= uint64_t((8 * BK) >> 4) << 32;             // stride byte offset: next 8-row group
+  d |= uint64_t(1) << 46;                         // descriptor version (sm_100)
+  d |= uint64_t(BK == 128 ? 2 : 4) << 61;         // SWIZZLE_128B or SWIZZLE_64B
   return d;
 }
 
@@ -58,7 +62,7 @@ __host__ __device__ constexpr uint32_t pow2_ceil(uint32_t x) {
   return x <= 32 ? 32 : x <= 64 ? 64 : x <= 128 ? 128 : x <= 256 ? 256 : 512;
 }
 
-template <int BN, int STAGES, int NS>
+template <int BN, int STAGES, int NS, int BK>
 struct Smem {
   static constexpr int A_BYTES = BM * BK;
   static constexpr int B_BYTES = BN * BK;
@@ -139,7 +143,15 @@ __device__ __forceinline__ void decode(const KParams& p, long t, int& mt, int& n
   bz = int(r % p.batch);
   ks = int(r / p.batch);
 }
-__device__ __forceinline__ int k_begin(int KT, int KS, int s) { return int((long)KT * s / KS); }
+// first K slice of split s of KS over KT slices of BK elements: the boundaries fall on multiples of
+// 128 elements whatever BK, so a product's partial sums do not depend on the slice width
+template <int BK>
+__device__ __forceinline__ int k_begin(int KT, int KS, int s) {
+  constexpr int per = 128 / BK;
+  const int kt128 = (KT + per - 1) / per;
+  const int b = int((long)kt128 * s / KS) * per;
+  return b < KT ? b : KT;
+}
 
 __device__ __forceinline__ double pow2(int e) {
   e = e < -1022 ? -1022 : (e > 1023 ? 1023 : e);
@@ -257,11 +269,11 @@ __device__ __forceinline__ void epilogue_tile(const KParams& p, uint32_t taddr, 
   }
 }
 
-template <int BN, int STAGES, int NS, int BUFS, bool GROUP>
+template <int BN, int STAGES, int NS, int BUFS, bool GROUP, int BK>
 __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_constant__ Maps maps0,
                                                                   const __grid_constant__ KParams p0,
                                                                   const __grid_constant__ GroupTab g) {
-  using L = Smem<BN, STAGES, NS>;
+  using L = Smem<BN, STAGES, NS, BK>;
   constexpr uint32_t GCOLS = uint32_t(NS * BN);               // columns of one tile's groups
   constexpr uint32_t ALLOC = pow2_ceil(GCOLS * BUFS);
   constexpr int NP = n_pairs(NS);
@@ -338,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
         decode(p, lt, mt, nt, bz, ks);
         const int m0 = mt * BM;
         const int ab = p.a_batched ? bz : 0, bb = p.b_batched ? bz : 0;
-        const int kb = k_begin(p.KT, p.KS, ks), ke = k_begin(p.KT, p.KS, ks + 1);
+        const int kb = k_begin<BK>(p.KT, p.KS, ks), ke = k_begin<BK>(p.KT, p.KS, ks + 1);
         for (int kt = kb; kt < ke; ++kt, ++it) {
           const int s = int(it % STAGES);
           const uint32_t ph = (it / STAGES) & 1;
@@ -395,7 +407,7 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
         const int Kv = cb ? p.N : p.K;  // valid K elements (complex B: the orbitals)
         int mt, nt, bz, ks;
         decode(p, lt, mt, nt, bz, ks);
-        const int kb = k_begin(p.KT, p.KS, ks), ke = k_begin(p.KT, p.KS, ks + 1);
+        const int kb = k_begin<BK>(p.KT, p.KS, ks), ke = k_begin<BK>(p.KT, p.KS, ks + 1);
         const uint32_t idesc = idesc_i8(uint32_t(cb ? 2 * p.half : BN));
         for (int kt = kb; kt < ke; ++kt, ++it) {
           const int s = int(it % STAGES);
@@ -410,8 +422,8 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
           uint64_t ad[NS], bd[NS];
 #pragma unroll
           for (int q = 0; q < NS; ++q) {
-            ad[q] = smem_desc_k64(stg + q * L::A_BYTES);
-            bd[q] = smem_desc_k64(stg + NS * L::A_BYTES + q * L::B_BYTES);
+            ad[q] = smem_desc_k<BK>(stg + q * L::A_BYTES);
+            bd[q] = smem_desc_k<BK>(stg + NS * L::A_BYTES + q * L::B_BYTES);
           }
           const int k0 = cb ? (kt >> 1) * BK : kt * BK;
           const int rem = Kv - k0;
@@ -475,7 +487,8 @@ __global__ void __launch_bounds__(kThreads, 1) islice_gemm_kernel(const __grid_c
 }
 
 // ---- host side -------------------------------------------------------------------------------
-int make_map_i8(CUtensorMap* m, const void* base, long rows, long K, long ld, long batch, long bstride, int box_rows) {
+int make_map_i8(CUtensorMap* m, const void* base, long rows, long K, long ld, long batch, long bstride, int box_rows,
+                int bk) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return record_error(SFQ_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld % 16) || ld < K)
@@ -488,10 +501,11 @@ int make_map_i8(CUtensorMap* m, const void* base, long rows, long K, long ld, lo
   }
   cuuint64_t dims[3] = {cuuint64_t(K), cuuint64_t(rows), cuuint64_t(batch)};
   cuuint64_t strides[2] = {cuuint64_t(ld), cuuint64_t(bstride)};
-  cuuint32_t box[3] = {cuuint32_t(BK), cuuint32_t(box_rows), 1};
+  cuuint32_t box[3] = {cuuint32_t(bk), cuuint32_t(box_rows), 1};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, bk == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return record_error(SFQ_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
   return SFQ_OK;
@@ -499,19 +513,20 @@ int make_map_i8(CUtensorMap* m, const void* base, long rows, long K, long ld, lo
 
 // the tensor maps and kernel parameters of one product; `group`: a member of a grouped launch of
 // tile width BN, whose complex-B products may use narrower halves
-template <int BN, int STAGES, int NS>
+template <int BN, int STAGES, int NS, int BK>
 int prepare(const IsliceGemmDesc& d, Maps* maps, KParams* kp_out, bool group) {
   const bool cb = d.cplx_half > 0;
   int rc;
   const long ab = d.A.batch_stride ? d.batch : 1, bb = d.B.batch_stride ? d.batch : 1;
   for (int q = 0; q < NS; ++q) {
     if (!d.A.q[q] || !d.B.q[q]) return record_error(SFQ_ERR_ARG, "islice_gemm: slice %d missing", q);
-    if ((rc = make_map_i8(&maps->a[q], d.A.q[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
-    if ((rc = make_map_i8(&maps->b[q], d.B.q[q], d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, cb ? d.cplx_half : BN)))
+    if ((rc = make_map_i8(&maps->a[q], d.A.q[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM, BK))) return rc;
+    if ((rc = make_map_i8(&maps->b[q], d.B.q[q], d.B.rows, d.K, d.B.ld, bb, d.B.batch_stride, cb ? d.cplx_half : BN,
+                           BK)))
       return rc;
     if (cb) {
       if (!d.a_im[q]) return record_error(SFQ_ERR_ARG, "islice_gemm: complex B needs a_im");
-      if ((rc = make_map_i8(&maps->aim[q], d.a_im[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM))) return rc;
+      if ((rc = make_map_i8(&maps->aim[q], d.a_im[q], d.A.rows, d.K, d.A.ld, ab, d.A.batch_stride, BM, BK))) return rc;
     } else {
       maps->aim[q] = maps->a[q];
     }
@@ -538,12 +553,13 @@ int prepare(const IsliceGemmDesc& d, Maps* maps, KParams* kp_out, bool group) {
   } else {
     kp.NT = (d.N + BN - 1) / BN;
     kp.KT = (d.K + BK - 1) / BK;
-    kp.KS = d.ksplit < 1 ? 1 : (d.ksplit > kp.KT ? kp.KT : d.ksplit);
+    const int kt128 = (d.K + 127) / 128;  // split boundaries fall on multiples of 128 elements
+    kp.KS = d.ksplit < 1 ? 1 : (d.ksplit > kt128 ? kt128 : d.ksplit);
     if (kp.KS > 1 && d.sCk <= 0) return record_error(SFQ_ERR_ARG, "islice_gemm: K splits need a partial-sum stride");
   }
   // int32 exactness: a group sums at most 3 pairs of |q| <= 128 products over one K range (complex
   // B: each output sums both halves, 2 nmo terms)
-  const long krange = cb ? 2L * d.K : (long)((kp.KT + kp.KS - 1) / kp.KS) * BK;
+  const long krange = cb ? 2L * d.K : (long)(((d.K + 127) / 128 + kp.KS - 1) / kp.KS) * 128;
   if (krange > 43000)
     return record_error(SFQ_ERR_SHAPE, "islice_gemm: K range of %ld too long for exact int32 accumulation", krange);
   kp.tiles = (long)kp.MT * kp.NT * d.batch * kp.KS;
@@ -559,23 +575,23 @@ int prepare(const IsliceGemmDesc& d, Maps* maps, KParams* kp_out, bool group) {
   return SFQ_OK;
 }
 
-template <int BN, int STAGES, int NS>
+template <int BN, int STAGES, int NS, int BK>
 struct Config {
-  using L = Smem<BN, STAGES, NS>;
+  using L = Smem<BN, STAGES, NS, BK>;
   static_assert(BN % 16 == 0, "the epilogue drains whole 16-column chunks");
   static constexpr int BUFS = (2 * NS * BN <= 512) ? 2 : 1;
   static_assert(L::TOTAL <= 232448, "shared memory budget");
   static_assert(NS * BN * BUFS <= 512, "accumulator groups must fit in tensor memory");
 };
 
-template <int BN, int STAGES, int NS>
+template <int BN, int STAGES, int NS, int BK>
 int launch(const IsliceGemmDesc& d, cudaStream_t st) {
-  using C = Config<BN, STAGES, NS>;
+  using C = Config<BN, STAGES, NS, BK>;
   Maps maps;
   KParams kp;
   int rc;
-  if ((rc = prepare<BN, STAGES, NS>(d, &maps, &kp, false))) return rc;
-  auto k = islice_gemm_kernel<BN, STAGES, NS, C::BUFS, false>;
+  if ((rc = prepare<BN, STAGES, NS, BK>(d, &maps, &kp, false))) return rc;
+  auto k = islice_gemm_kernel<BN, STAGES, NS, C::BUFS, false, BK>;
   SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, C::L::TOTAL));
   const long grid = kp.tiles < sm_count() ? kp.tiles : sm_count();
   k<<<unsigned(grid), kThreads, C::L::TOTAL, st>>>(maps, kp, GroupTab{});
@@ -585,11 +601,11 @@ int launch(const IsliceGemmDesc& d, cudaStream_t st) {
 
 // the grouped launches' tile widths: every plain product of a group has tile width kGroupBN
 constexpr int kGroupBN = 160;
-constexpr int group_stages(int ns) { return ns == 2 ? 6 : 4; }
+constexpr int group_stages(int ns, int bk) { return (ns == 2 ? 6 : 4) * 64 / bk; }
 
-template <int NS>
+template <int NS, int BK>
 int group_plan(const IsliceGemmDesc* ds, int n, IsliceGroupPlan* out) {
-  constexpr int ST = group_stages(NS);
+  constexpr int ST = group_stages(NS, BK);
   std::vector<GroupProb> probs(static_cast<size_t>(n));
   std::vector<long> start(size_t(n) + 1, 0);
   int rc;
@@ -604,12 +620,13 @@ int group_plan(const IsliceGemmDesc* ds, int n, IsliceGroupPlan* out) {
     GroupProb* pr = probs.data() + i;
     Maps* mp = &pr->maps;
     KParams* kq = &pr->kp;
-    rc = prepare<kGroupBN, ST, NS>(d, mp, kq, true);
+    rc = prepare<kGroupBN, ST, NS, BK>(d, mp, kq, true);
     if (rc) return rc;
     start[size_t(i) + 1] = start[size_t(i)] + kq->tiles;
   }
   out->nprob = n;
   out->nslices = NS;
+  out->bk = BK;
   out->tiles = start[size_t(n)];
   out->wait_ns = n ? probs[0].kp.wait_ns : kWaitNs;
   out->start_off = sizeof(GroupProb) * size_t(n);
@@ -619,10 +636,10 @@ int group_plan(const IsliceGemmDesc* ds, int n, IsliceGroupPlan* out) {
   return SFQ_OK;
 }
 
-template <int NS>
+template <int NS, int BK>
 int group_launch(const void* table, const IsliceGroupPlan& plan, cudaStream_t st) {
-  constexpr int ST = group_stages(NS);
-  using C = Config<kGroupBN, ST, NS>;
+  constexpr int ST = group_stages(NS, BK);
+  using C = Config<kGroupBN, ST, NS, BK>;
   if (reinterpret_cast<uintptr_t>(table) & 127)
     return record_error(SFQ_ERR_ARG, "islice_gemm_group: the table needs 128-byte alignment");
   GroupTab g;
@@ -632,12 +649,19 @@ int group_launch(const void* table, const IsliceGroupPlan& plan, cudaStream_t st
   g.tiles = plan.tiles;
   KParams kp{};
   kp.wait_ns = plan.wait_ns;
-  auto k = islice_gemm_kernel<kGroupBN, ST, NS, C::BUFS, true>;
+  auto k = islice_gemm_kernel<kGroupBN, ST, NS, C::BUFS, true, BK>;
   SFQ_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, C::L::TOTAL));
   const long grid = plan.tiles < sm_count() ? plan.tiles : sm_count();
   k<<<unsigned(grid), kThreads, C::L::TOTAL, st>>>(Maps{}, kp, g);
   SFQ_LAUNCHED();
   return SFQ_OK;
+}
+
+// the K slice width for a product: 128 elements where its tiles run over 1024 or more K elements
+// (half as many stages, each twice as long), else 64
+inline int k_slice_width(const IsliceGemmDesc& d) {
+  const long k = d.cplx_half > 0 ? 2L * d.K : (d.K + (d.ksplit > 1 ? d.ksplit : 1) - 1) / (d.ksplit > 1 ? d.ksplit : 1);
+  return k >= 1024 ? 128 : 64;
 }
 
 }  // namespace islice
@@ -646,14 +670,16 @@ int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st) {
   if (d.M <= 0 || d.N <= 0 || d.batch <= 0) return SFQ_OK;
   if (d.K <= 0) return record_error(SFQ_ERR_SHAPE, "islice_gemm: K must be positive");
   const int bn = d.cplx_half > 0 ? 2 * d.cplx_half : (d.bn ? d.bn : (d.N <= 64 ? 64 : 128));
+  const bool k128 = islice::k_slice_width(d) == 128;
+  // stages: as many as about 216 KB of shared memory holds
   switch (d.nslices * 1000 + bn) {
-    case 2064: return islice::launch<64, 8, 2>(d, st);
-    case 2128: return islice::launch<128, 6, 2>(d, st);
-    case 2160: return islice::launch<160, 6, 2>(d, st);
-    case 3064: return islice::launch<64, 6, 3>(d, st);
-    case 3080: return islice::launch<80, 5, 3>(d, st);
-    case 3128: return islice::launch<128, 4, 3>(d, st);
-    case 3160: return islice::launch<160, 4, 3>(d, st);
+    case 2064: return k128 ? islice::launch<64, 4, 2, 128>(d, st) : islice::launch<64, 8, 2, 64>(d, st);
+    case 2128: return k128 ? islice::launch<128, 3, 2, 128>(d, st) : islice::launch<128, 6, 2, 64>(d, st);
+    case 2160: return k128 ? islice::launch<160, 3, 2, 128>(d, st) : islice::launch<160, 6, 2, 64>(d, st);
+    case 3064: return k128 ? islice::launch<64, 3, 3, 128>(d, st) : islice::launch<64, 6, 3, 64>(d, st);
+    case 3080: return k128 ? islice::launch<80, 2, 3, 128>(d, st) : islice::launch<80, 5, 3, 64>(d, st);
+    case 3128: return k128 ? islice::launch<128, 2, 3, 128>(d, st) : islice::launch<128, 4, 3, 64>(d, st);
+    case 3160: return k128 ? islice::launch<160, 2, 3, 128>(d, st) : islice::launch<160, 4, 3, 64>(d, st);
     default:
       return record_error(SFQ_ERR_ARG, "islice_gemm: %d slices with tile width %d not built", d.nslices, bn);
   }
@@ -661,15 +687,22 @@ int islice_gemm(const IsliceGemmDesc& d, cudaStream_t st) {
 
 int islice_gemm_group_plan(const IsliceGemmDesc* ds, int n, IsliceGroupPlan* out) {
   if (n <= 0 || !ds || !out) return record_error(SFQ_ERR_ARG, "islice_gemm_group: no members");
-  if (ds[0].nslices == 2) return islice::group_plan<2>(ds, n, out);
-  if (ds[0].nslices == 3) return islice::group_plan<3>(ds, n, out);
+  // one K slice width for the launch: the widest any member would take alone (the results do not
+  // depend on it)
+  bool k128 = false;
+  for (int i = 0; i < n; ++i) k128 = k128 || islice::k_slice_width(ds[i]) == 128;
+  if (ds[0].nslices == 2) return k128 ? islice::group_plan<2, 128>(ds, n, out) : islice::group_plan<2, 64>(ds, n, out);
+  if (ds[0].nslices == 3) return k128 ? islice::group_plan<3, 128>(ds, n, out) : islice::group_plan<3, 64>(ds, n, out);
   return record_error(SFQ_ERR_ARG, "islice_gemm_group: %d slices not built", ds[0].nslices);
 }
 
 int islice_gemm_group_launch(const void* table, const IsliceGroupPlan& plan, cudaStream_t st) {
   if (plan.nprob <= 0 || plan.tiles <= 0) return SFQ_OK;
-  if (plan.nslices == 2) return islice::group_launch<2>(table, plan, st);
-  if (plan.nslices == 3) return islice::group_launch<3>(table, plan, st);
+  const bool k128 = plan.bk == 128;
+  if (plan.nslices == 2)
+    return k128 ? islice::group_launch<2, 128>(table, plan, st) : islice::group_launch<2, 64>(table, plan, st);
+  if (plan.nslices == 3)
+    return k128 ? islice::group_launch<3, 128>(table, plan, st) : islice::group_launch<3, 64>(table, plan, st);
   return record_error(SFQ_ERR_ARG, "islice_gemm_group: %d slices not built", plan.nslices);
 }
 

@@ -217,16 +217,6 @@ __global__ void rows_planar_kernel(const cplx* src, long R, long K, int ns, Q q,
 // long rows split over blocks: pass 1, each chunk's largest |re| and |im| into the row's maxima
 // (non-negative doubles order like their bits, so a 64-bit atomic max is exact); pass 2 slices
 constexpr long kPlanarChunk = 4096;
-// four consecutive elements of row x (minus sub) from k: zeros past K
-__device__ __forceinline__ void load4c(const cplx* x, const cplx* sub, long k, long K, cplx (&z)[4]) {
-#pragma unroll
-  for (int u = 0; u < 4; ++u) z[u] = k + u < K ? x[k + u] : mk(0.0, 0.0);
-  if (sub) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (k + u < K) z[u] = csub(z[u], sub[k + u]);
-  }
-}
 __global__ void __launch_bounds__(256) planar_max_kernel(const cplx* src, long R, long K, const cplx* sub,
                                                          unsigned long long* emax) {
   __shared__ double sh[32];
@@ -234,14 +224,10 @@ __global__ void __launch_bounds__(256) planar_max_kernel(const cplx* src, long R
   const long k1 = k0 + kPlanarChunk < K ? k0 + kPlanarChunk : K;
   const cplx* x = src + r * K;
   double mr = 0.0, mi = 0.0;
-  for (long k = k0 + 4 * threadIdx.x; k < k1; k += 4 * blockDim.x) {  // four elements in flight per thread
-    cplx z[4];
-    load4c(x, sub, k, k1, z);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      mr = fmax(mr, fabs(z[u].x));
-      mi = fmax(mi, fabs(z[u].y));
-    }
+  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    const cplx z = sub ? csub(x[k], sub[k]) : x[k];
+    mr = fmax(mr, fabs(z.x));
+    mi = fmax(mi, fabs(z.y));
   }
   mr = block_max(mr, sh);
   mi = block_max(mi, sh);
@@ -249,15 +235,6 @@ __global__ void __launch_bounds__(256) planar_max_kernel(const cplx* src, long R
     atomicMax(emax + r, (unsigned long long)__double_as_longlong(mr));
     atomicMax(emax + R + r, (unsigned long long)__double_as_longlong(mi));
   }
-}
-// four consecutive values -> one 4-byte word per slice at idx (a multiple of 4)
-__device__ __forceinline__ void put4d(const Q& q, int ns, long idx, const double (&x)[4], double s) {
-  int a[4], b[4], c[4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u) slice_value(x[u], s, ns, a[u], b[u], c[u]);
-  *reinterpret_cast<char4*>(q.p[0] + idx) = make_char4(char(a[0]), char(a[1]), char(a[2]), char(a[3]));
-  if (ns > 1) *reinterpret_cast<char4*>(q.p[1] + idx) = make_char4(char(b[0]), char(b[1]), char(b[2]), char(b[3]));
-  if (ns > 2) *reinterpret_cast<char4*>(q.p[2] + idx) = make_char4(char(c[0]), char(c[1]), char(c[2]), char(c[3]));
 }
 __global__ void __launch_bounds__(256) planar_slice_kernel(const cplx* src, long R, long K, const cplx* sub,
                                                            const unsigned long long* emax, int ns, Q q, long ld,
@@ -272,17 +249,10 @@ __global__ void __launch_bounds__(256) planar_slice_kernel(const cplx* src, long
   }
   const double sr = pow2d(-er), si = pow2d(-ei);
   const cplx* x = src + r * K;
-  for (long k = k0 + 4 * threadIdx.x; k < k1; k += 4 * blockDim.x) {  // ld and k0 are multiples of 4
-    cplx z[4];
-    load4c(x, sub, k, K, z);
-    double xr[4], xi[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      xr[u] = z[u].x;
-      xi[u] = z[u].y;
-    }
-    put4d(q, ns, r * ld + k, xr, sr);
-    put4d(q, ns, (R + r) * ld + k, xi, si);
+  for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    const cplx z = k < K ? (sub ? csub(x[k], sub[k]) : x[k]) : mk(0.0, 0.0);
+    put(q, ns, r * ld + k, z.x, sr);
+    put(q, ns, (R + r) * ld + k, z.y, si);
   }
 }
 

@@ -60,15 +60,15 @@ def test_int8_slice_product_is_bit_exact(ns, K, bn):
 
 
 def test_int8_slice_product_k_split_partials():
-    """K split into ranges of whole 64-element K blocks (the kernel's stage): each partial product is
-    the exact product over its range."""
+    """K split into ranges of whole 128-element blocks (at either K slice width of the kernel): each
+    partial product is the exact product over its range."""
     A, B = _operands(200, 170, 2400, seed=11)
-    ks = 5
-    C = _int8_gemm(A, B, 3, 160, ks)
-    KT = (2400 + 63) // 64
-    for s in range(ks):
-        k0, k1 = 64 * (KT * s // ks), min(2400, 64 * (KT * (s + 1) // ks))
-        assert np.array_equal(C[s], R.gemm(A, B, 3, k0=k0, k1=k1)), s
+    for ks in (5, 2):  # 480 and 1200 elements per range: 64- and 128-element K slices
+        C = _int8_gemm(A, B, 3, 160, ks)
+        KT = (2400 + 127) // 128
+        for s in range(ks):
+            k0, k1 = 128 * (KT * s // ks), min(2400, 128 * (KT * (s + 1) // ks))
+            assert np.array_equal(C[s], R.gemm(A, B, 3, k0=k0, k1=k1)), (ks, s)
 
 
 def test_int8_slices_carry_no_accumulation_bias():
