@@ -65,21 +65,23 @@ __device__ __forceinline__ void pivot_step(int k, int N, const cplx (&v)[kGjMaxN
       }
     }
   }
-  bool tie = cnt > 1;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const long long ob = __shfl_xor_sync(0xffffffffu, best, off);
-    const int orow = __shfl_xor_sync(0xffffffffu, brow, off);
-    const int otie = __shfl_xor_sync(0xffffffffu, int(tie), off);
-    if (ob > best) {
-      best = ob;
-      brow = orow;
-      tie = otie != 0;
-    } else if (ob == best && ob >= 0) {
-      tie = true;
-    }
+  // the warp's largest key: keys + 1 as unsigned (no candidate, -1, becomes the least), reduced by
+  // its high word, then by its low word among the lanes that hold the largest high word (two
+  // redux.sync instead of a shuffle tree); the lanes holding the maximum are the ballot's
+  {
+    const unsigned long long u = (unsigned long long)(best + 1);
+    const unsigned hi = unsigned(u >> 32), lo = unsigned(u);
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    const unsigned win = __ballot_sync(0xffffffffu, hi == mhi && lo == mlo);
+    best = (long long)(((unsigned long long)mhi << 32) | mlo) - 1;
+    const bool any = best >= 0;
+    // a tie: two lanes with the maximum, or one lane with it in two of its rows
+    const bool tie = any && (__popc(win) > 1 || __any_sync(0xffffffffu, ((win >> lane) & 1u) && cnt > 1));
+    brow = any ? __shfl_sync(0xffffffffu, brow, __ffs(win) - 1) : (1 << 30);
+    cnt = tie ? 2 : 1;
   }
-  if (__any_sync(0xffffffffu, tie)) {
+  if (cnt > 1) {
     // exact zgetrf rule among the tied maxima: the lowest LAPACK position
     int bpos = 1 << 30, prow_ = 1 << 30;
 #pragma unroll

@@ -92,6 +92,20 @@ def test_kat_orthogonalize(kats):
     assert rel(Qh, Qo) < REL
 
 
+@pytest.mark.parametrize("N", [40, 100])
+def test_inverse_logdet_with_tied_pivots(N):
+    """Entries of modulus |re| + |im| = 1 (+-1, +-i): every pivot search starts among exactly tied
+    candidates, which zgetrf resolves by the first in its row order; the inverse and log det against
+    the oracle's LAPACK factorization."""
+    rng = np.random.default_rng(N)
+    T = rng.choice(np.array([1, -1, 1j, -1j]), size=(4, N, N))
+    assert all(abs(np.linalg.det(t)) > 1e-6 for t in T)
+    inv, ld = A.inverse_logdet(cu(T))
+    io, lo = O.inverse_logdet(T)
+    assert rel(host(inv), io) < 1e-9
+    assert np.max(np.abs(host(ld) - lo)) < 1e-9 * np.max(np.abs(lo))
+
+
 def test_singular_overlap_zero_inverse():
     T = np.zeros((2, 3, 3), np.complex128)
     T[:, 0, 0] = 1.0
