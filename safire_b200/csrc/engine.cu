@@ -235,6 +235,25 @@ __global__ void bp_init_refs_kernel(const cplx* PsiT, int ndet, int W, int Mr, i
 }
 // V[w] <- -V[w]^H in place: exp(i (-V^H)) = exp(-i V^H), the adjoint Taylor propagator (propagate.hpp:56-57)
 // time-evolved back propagation helpers: X[b] = I (R x R) for every matrix b; out = conj(in)
+// dst[c][r] = src[r * cols + c0 + c] for r < rows, c < nc: a block of columns of a row-major matrix,
+// transposed through 32 x 32 shared-memory tiles
+__global__ void transpose_cols_kernel(const double* src, long rows, long cols, long c0, int nc, double* dst) {
+  __shared__ double tile[32][33];
+  const long r0 = (long)blockIdx.x * 32;
+  const int cb = blockIdx.y * 32;
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const long r = r0 + y;
+    const int c = cb + threadIdx.x;
+    tile[y][threadIdx.x] = (r < rows && c < nc) ? src[r * cols + c0 + c] : 0.0;
+  }
+  __syncthreads();
+  for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+    const int c = cb + y;
+    const long r = r0 + threadIdx.x;
+    if (c < nc && r < rows) dst[(long)c * rows + r] = tile[threadIdx.x][y];
+  }
+}
+
 __global__ void set_identity_batched_kernel(cplx* X, long nmat, int R) {
   const long n = nmat * R * R;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
@@ -549,7 +568,13 @@ struct Engine {
   int nslices = 0;
   long ld_m = 0, ld_mr = 0, ld_nm = 0, ld_nc = 0;  // slice row strides (bytes): M, Mr, N*Mr, Nc rounded up to 64
   int8_t* Lv_q[3] = {};  int* Lv_e = nullptr;   // Lnak, rows n over (a, k): the force bias's B
-  int8_t* Le_q[3] = {};  int* Le_e = nullptr;   // Lnak, rows (n, a) over k: the exchange tensor's B
+  int8_t* Le_q[3] = {};  int* Le_e = nullptr;   // Lnak, rows (n, a) over k: the exchange tensor's B (per determinant)
+  // multi-determinant trials: the force bias contracts the ci-weighted full G (M x M) with L
+  int8_t* Lf_q[3] = {};  int* Lf_e = nullptr;   // L, rows n over (i, k)
+  int8_t* Gf_q[3] = {};  int* Gf_e = nullptr;   // full G minus the trial's, planar rows (c, w) over (i, k)
+  cplx* RT_md = nullptr;                         // the trial's ci-weighted full G (M x M), FP64
+  long ld_mm = 0;
+  int i8_md_ks = 1;                              // K splits of that product (exact int32 per range)
   int8_t* Lh_q[3] = {};  int* Lh_e = nullptr;   // L, rows (i, k) (packed pairs when symmetric) over n: vHS's B
   int8_t* P1_q[3] = {};  int* P1_e = nullptr;   // P1, rows j over i
   int8_t* Gv_q[3] = {};  int* Gv_e = nullptr;   // G, planar rows (c, w) over (a, k)
@@ -712,13 +737,18 @@ struct Engine {
     if (mixed && nslices) {
       plan_i8();
       const long R = (long)W * npol * N, RG = (long)W * N, vrows = sym ? P : MM;
+      const bool md = ndet > 1;  // the force bias from the full G: no slices of Lnak over (a, k) nor of G
       std::vector<Item> mx;
       for (int q = 0; q < nslices; ++q) {
-        mx.push_back({(void**)&Lv_q[q], (size_t)Nc * ld_nm});
-        mx.push_back({(void**)&Le_q[q], (size_t)Nc * N * ld_mr});
+        mx.push_back({(void**)&Lv_q[q], md ? 0 : (size_t)Nc * ld_nm});
+        mx.push_back({(void**)&Le_q[q], (size_t)ndet * Nc * N * ld_mr});
+        if (md) {
+          mx.push_back({(void**)&Lf_q[q], (size_t)Nc * ld_mm});
+          mx.push_back({(void**)&Gf_q[q], (size_t)2 * W * ld_mm});
+        }
         mx.push_back({(void**)&Lh_q[q], (size_t)vrows * ld_nc});
         mx.push_back({(void**)&P1_q[q], (size_t)M * ld_m});
-        mx.push_back({(void**)&Gv_q[q], (size_t)2 * W * ld_nm});
+        mx.push_back({(void**)&Gv_q[q], md ? 0 : (size_t)2 * W * ld_nm});
         mx.push_back({(void**)&Ge_q[q], (size_t)2 * RG * ld_mr});
         mx.push_back({(void**)&Xq_q[q], (size_t)2 * W * ld_nc});
         mx.push_back({(void**)&V_q[q], (size_t)W * 3 * M * ld_m});
@@ -726,18 +756,22 @@ struct Engine {
       }
       const size_t ie = sizeof(int);
       std::vector<Item> mx2 = {
-          {(void**)&Lv_e, ie * Nc}, {(void**)&Le_e, ie * Nc * N}, {(void**)&Lh_e, ie * vrows},
+          {(void**)&Lv_e, ie * Nc}, {(void**)&Le_e, ie * ndet * Nc * N}, {(void**)&Lh_e, ie * vrows},
           {(void**)&P1_e, ie * M}, {(void**)&Gv_e, ie * 2 * W}, {(void**)&Ge_e, ie * 2 * RG},
           {(void**)&Xq_e, ie * 2 * W}, {(void**)&V_e, ie * W * M}, {(void**)&V_emax, ie * W * M},
           {(void**)&A_e[0], ie * R}, {(void**)&A_e[1], ie * R},
           {(void**)&GT_c, c * (size_t)N * Mr}, {(void**)&vbT, c * (size_t)Nc},
           {(void**)&pl_emax, sizeof(unsigned long long) * 2 * (size_t)W},
-          {(void**)&Cvb, sizeof(float) * i8_vb_ks * 2 * (size_t)W * Nc},
+          {(void**)&Cvb, sizeof(float) * std::max(i8_vb_ks, i8_md_ks) * 2 * (size_t)W * Nc},
           {(void**)&Cv, sizeof(float) * 2 * W * vrows},
           {(void**)&Sacc, sizeof(float) * 2 * R * M},
           {(void**)&Cp, sizeof(float) * 2 * R * M},
           {(void**)&gemm_err, sizeof(int) * 4},
       };
+      if (md) {
+        std::vector<Item> mx3 = {{(void**)&Lf_e, ie * Nc}, {(void**)&Gf_e, ie * 2 * W}, {(void**)&RT_md, c * MM}};
+        mx2.insert(mx2.end(), mx3.begin(), mx3.end());
+      }
       items.insert(items.end(), mx.begin(), mx.end());
       items.insert(items.end(), mx2.begin(), mx2.end());
     } else if (mixed) {
@@ -780,6 +814,69 @@ struct Engine {
   }
 
   // --- setup: RealDenseHamiltonian::getHamiltonianOperations + NOMSD::vMF + generateP1 --------
+  // the int8-slice setup shared by single- and multi-determinant trials: vHS's B (L over n, the
+  // packed pairs when symmetric) and the P1 slices
+  int setup_i8_common() {
+    int rc;
+    const long MM = (long)M * M;
+    if (sym) {
+      double* packed = nullptr;
+      SFQ_CUDA_TRY(cudaMallocAsync(&packed, sizeof(double) * P * Nc, st));
+      if ((rc = pack_upper(Likn, M, Nc, packed, st))) return rc;
+      if ((rc = islice_rows_real(packed, P, Nc, Nc, nslices, Lh_q, ld_nc, Lh_e, st))) return rc;
+      SFQ_CUDA_TRY(cudaFreeAsync(packed, st));
+    } else {
+      if ((rc = islice_rows_real(Likn, MM, Nc, Nc, nslices, Lh_q, ld_nc, Lh_e, st))) return rc;
+    }
+    // P1 = I + Q with Q of order dt: the slices hold Q (each row's entries at their own scale, not
+    // at the diagonal's), and the identity part is added exactly where the products are used
+    double* q1 = nullptr;
+    SFQ_CUDA_TRY(cudaMallocAsync((void**)&q1, sizeof(double) * MM, st));
+    SFQ_CUDA_TRY(cudaMemcpyAsync(q1, P1, sizeof(double) * MM, cudaMemcpyDeviceToDevice, st));
+    if ((rc = add_identity(q1, M, -1.0, st))) return rc;
+    if ((rc = islice_rows_real(q1, M, M, M, nslices, P1_q, ld_m, P1_e, st))) return rc;
+    SFQ_CUDA_TRY(cudaFreeAsync(q1, st));
+    SFQ_CUDA_TRY(cudaMemsetAsync(gemm_err, 0, sizeof(int) * 4, st));
+    return SFQ_OK;
+  }
+  // multi-determinant trials in the int8-slice mode: the trial's ci-weighted full G (the reference
+  // the walkers' full G is sliced against) and its force bias, the slices of L as rows n over (i, k)
+  // (L transposed in blocks of Cholesky vectors), and every determinant's exchange slices
+  int setup_i8_md(const cplx* h_PsiT) {
+    int rc;
+    const long MM = (long)M * M;
+    if ((rc = md_trial_green(h_PsiT))) return rc;
+    SFQ_CUDA_TRY(cudaMemcpyAsync(RT_md, Racc, sizeof(cplx) * MM, cudaMemcpyDeviceToDevice, st));
+    if ((rc = vbias_full(RT_md, 1, X))) return rc;
+    SFQ_CUDA_TRY(cudaMemcpyAsync(vbT, X, sizeof(cplx) * Nc, cudaMemcpyDeviceToDevice, st));
+    const long cap = (64L << 20) / MM;  // Cholesky vectors per block: at most 512 MB of FP64
+    const int blk = int(cap < 1 ? 1 : (cap > Nc ? Nc : cap));
+    double* tmp = nullptr;
+    SFQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(double) * blk * MM, st));
+    for (int n0 = 0; n0 < Nc; n0 += blk) {
+      const int nb = Nc - n0 < blk ? Nc - n0 : blk;
+      transpose_cols_kernel<<<dim3(unsigned((MM + 31) / 32), unsigned((nb + 31) / 32)), dim3(32, 8), 0, st>>>(
+          Likn, MM, Nc, n0, nb, tmp);
+      SFQ_LAUNCHED();
+      int8_t* q[3];
+      for (int t = 0; t < 3; ++t) q[t] = Lf_q[t] ? Lf_q[t] + (long)n0 * ld_mm : nullptr;
+      if ((rc = islice_rows_real(tmp, nb, MM, MM, nslices, q, ld_mm, Lf_e + n0, st))) {
+        cudaFreeAsync(tmp, st);
+        return rc;
+      }
+    }
+    SFQ_CUDA_TRY(cudaFreeAsync(tmp, st));
+    const long o = det_elems();
+    for (int d = 0; d < ndet; ++d) {
+      const double* Ld = (const double*)Lnak + (size_t)d * Nc * o;
+      int8_t* q[3];
+      for (int t = 0; t < 3; ++t) q[t] = Le_q[t] ? Le_q[t] + (long)d * Nc * N * ld_mr : nullptr;
+      if ((rc = islice_rows_real(Ld, (long)Nc * N, Mr, Mr, nslices, q, ld_mr, Le_e + (long)d * Nc * N, st))) return rc;
+    }
+    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    return setup_i8_common();
+  }
+
   int setup(const double* h_hcore, const double* h_Likn, const cplx* h_PsiT) {
     int rc;
     const long MM = (long)M * M;
@@ -955,7 +1052,9 @@ struct Engine {
     }
     // exact-accumulation mode: int8 slices of the resident real tensors, and the trial's own G and
     // force bias (NOMSD::vMF before its real part is taken)
-    if (mixed && nslices) {
+    if (mixed && nslices && ndet > 1) {
+      if ((rc = setup_i8_md(h_PsiT))) return rc;
+    } else if (mixed && nslices) {
       const long NM = (long)N * Mr;
       {
         std::vector<cplx> psi(size_t(Mr) * N);  // PsiT^H (Mr x N)
@@ -974,24 +1073,7 @@ struct Engine {
       const double* Ln = (const double*)Lnak;
       if ((rc = islice_rows_real(Ln, Nc, NM, NM, nslices, Lv_q, ld_nm, Lv_e, st))) return rc;
       if ((rc = islice_rows_real(Ln, (long)Nc * N, Mr, Mr, nslices, Le_q, ld_mr, Le_e, st))) return rc;
-      if (sym) {
-        double* packed = nullptr;
-        SFQ_CUDA_TRY(cudaMallocAsync(&packed, sizeof(double) * P * Nc, st));
-        if ((rc = pack_upper(Likn, M, Nc, packed, st))) return rc;
-        if ((rc = islice_rows_real(packed, P, Nc, Nc, nslices, Lh_q, ld_nc, Lh_e, st))) return rc;
-        SFQ_CUDA_TRY(cudaFreeAsync(packed, st));
-      } else {
-        if ((rc = islice_rows_real(Likn, MM, Nc, Nc, nslices, Lh_q, ld_nc, Lh_e, st))) return rc;
-      }
-      // P1 = I + Q with Q of order dt: the slices hold Q (each row's entries at their own scale, not
-      // at the diagonal's), and the identity part is added exactly where the products are used
-      double* q1 = nullptr;
-      SFQ_CUDA_TRY(cudaMallocAsync((void**)&q1, sizeof(double) * MM, st));
-      SFQ_CUDA_TRY(cudaMemcpyAsync(q1, P1, sizeof(double) * MM, cudaMemcpyDeviceToDevice, st));
-      if ((rc = add_identity(q1, M, -1.0, st))) return rc;
-      if ((rc = islice_rows_real(q1, M, M, M, nslices, P1_q, ld_m, P1_e, st))) return rc;
-      SFQ_CUDA_TRY(cudaFreeAsync(q1, st));
-      SFQ_CUDA_TRY(cudaMemsetAsync(gemm_err, 0, sizeof(int) * 4, st));
+      if ((rc = setup_i8_common())) return rc;
     } else if (mixed) {  // mixed precision: bf16 hi/lo planes of the resident real tensors
       if (sym) {
         double* packed = nullptr;
@@ -1087,6 +1169,16 @@ struct Engine {
   // NOMSD::vMF, ndet > 1 (NOMSD.cpp:466-512): the pairs q >= p of the trial's own determinants
   int mean_field_md(const cplx* h_PsiT) {
     int rc;
+    if ((rc = md_trial_green(h_PsiT))) return rc;
+    if ((rc = vbias_full(Racc, 1, X))) return rc;
+    if ((rc = real_of(X, vmf, Nc, st))) return rc;
+    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
+    return SFQ_OK;
+  }
+  // the trial's own ci-weighted full G (M x M) into Racc (first walker slot): the pairs q >= p of
+  // its determinants, normalised (NOMSD.cpp:466-512 before the force bias is taken)
+  int md_trial_green(const cplx* h_PsiT) {
+    int rc;
     const long MM = (long)M * M;
     bool first = true;
     std::vector<cplx> psi(size_t(Mr) * N);
@@ -1108,13 +1200,16 @@ struct Engine {
     }
     md_normalize_kernel<<<dim3(md_grid(MM), 1), 256, 0, st>>>(Racc, wsum, MM);
     SFQ_LAUNCHED();
-    if ((rc = vbias_full(Racc, 1, X))) return rc;
-    if ((rc = real_of(X, vmf, Nc, st))) return rc;
-    SFQ_CUDA_TRY(cudaStreamSynchronize(st));
     return SFQ_OK;
   }
   // NOMSD::vbias with ndet > 1 (NOMSD.cpp:39-61,238-278): the ci-weighted full G, then vbias on it
   int vbias_md(cplx* out) {
+    int rc;
+    if ((rc = md_full_green())) return rc;
+    return vbias_full(Racc, W, out);
+  }
+  // every walker's ci-weighted full G (W, M, M) into Racc, the determinants' log overlaps in md_ov
+  int md_full_green() {
     int rc;
     const long MM = (long)M * M;
     const cplx* lm = props + (long)P_OVLP * W;
@@ -1128,7 +1223,7 @@ struct Engine {
     }
     md_normalize_kernel<<<dim3(md_grid(MM), W), 256, 0, st>>>(Racc, wsum, MM);
     SFQ_LAUNCHED();
-    return vbias_full(Racc, W, out);
+    return SFQ_OK;
   }
   // NOMSD::Log_Overlap with ndet > 1 into ov (W)
   int log_overlap_md(cplx* ov) {
@@ -2146,6 +2241,7 @@ struct Engine {
     ld_mr = round64(Mr);
     ld_nm = round64((long)N * Mr);
     ld_nc = round64(Nc);
+    ld_mm = round64((long)M * M);
     int best = 0;
     long best_pad = 1L << 40;
     for (int h : {32, 64, 80}) {
@@ -2170,6 +2266,23 @@ struct Engine {
         i8_vb_ks = ks;
       }
       if (eff > 0.999) break;
+    }
+    // multi-determinant force bias: K = M * M, split into ranges of at most 335 blocks of 128 (exact
+    // int32 accumulation), then as for the single-determinant one to fill whole waves of SMs
+    i8_md_ks = 1;
+    if (ndet > 1) {
+      const long ktm = ((long)M * M + 127) / 128;
+      const int ks_min = int((ktm + 334) / 335);
+      double be = -1.0;
+      for (int ks = ks_min; ks <= 64 || ks == ks_min; ++ks) {
+        const double units = double(tiles) * ks;
+        const double eff = units / (std::ceil(units / sms) * sms);
+        if (eff > be + 1e-9) {
+          be = eff;
+          i8_md_ks = ks;
+        }
+        if (eff > 0.999 || ks * 4 > ktm) break;
+      }
     }
   }
   IsliceOperand i8_operand(int8_t* const* q, long rows, long ld, const int* e, long bstride = 0, long e_bs = 0,
@@ -2229,6 +2342,20 @@ struct Engine {
     const long R = (long)Wb * N;
     const int order = p.taylor_order;
     *more = true;
+    if (s == 0 && ndet > 1) {
+      // NOMSD::vbias with ndet > 1: the ci-weighted full G (FP64), its difference from the trial's
+      // sliced as planar rows over (i, k), against L; the trial's own force bias added back
+      ph_begin(SFQ_PH_VBIAS);
+      if ((rc = md_full_green())) return rc;
+      if ((rc = islice_rows_planar(Racc, W, (long)M * M, nslices, Gf_q, ld_mm, Gf_e, st, RT_md, pl_emax))) return rc;
+      *d = i8_desc();
+      d->M = 2 * W; d->N = Nc; d->K = int((long)M * M);
+      d->A = i8_operand(Gf_q, 2L * W, ld_mm, Gf_e);
+      d->B = i8_operand(Lf_q, Nc, ld_mm, Lf_e);
+      d->bn = i8_vb_bn; d->ksplit = i8_md_ks; d->sCk = 2L * W * Nc;
+      d->C = Cvb; d->ldc = Nc;
+      return SFQ_OK;
+    }
     if (s == 0) {
       ph_begin(SFQ_PH_DENSITY);
       if ((rc = density(nullptr))) return rc;
@@ -2244,7 +2371,8 @@ struct Engine {
       return SFQ_OK;
     }
     if (s == 1) {
-      if ((rc = mixed_reduce_planar_to_cplx(Cvb, i8_vb_ks, 2L * W * Nc, W, Nc, vb_scale(), X, st, vbT))) return rc;
+      const int ks = ndet > 1 ? i8_md_ks : i8_vb_ks;
+      if ((rc = mixed_reduce_planar_to_cplx(Cvb, ks, 2L * W * Nc, W, Nc, vb_scale(), X, st, vbT))) return rc;
       ph_end(SFQ_PH_VBIAS);
       ph_begin(SFQ_PH_FIELDS);
       FieldParams fp;
@@ -2305,7 +2433,7 @@ struct Engine {
     if ((rc = islice_to_walkers(Cp, Sacc, Wb, M, N, SM, st))) return rc;
     ph_end(SFQ_PH_PROPAGATE);
     ph_begin(SFQ_PH_OVERLAP);
-    if ((rc = log_overlap(newov))) return rc;
+    if ((rc = ndet > 1 ? log_overlap_md(newov) : log_overlap(newov))) return rc;
     ph_end(SFQ_PH_OVERLAP);
     ph_begin(SFQ_PH_UPDATE);
     UpdateParams up;
@@ -2341,21 +2469,73 @@ struct Engine {
     if (nv_max > Nc) nv_max = Nc;
     return nv_max;
   }
-  void i8_exchange_desc(int n0, IsliceGemmDesc* d) const {
+  void i8_exchange_desc(int n0, IsliceGemmDesc* d, int det = 0) const {
     const long R = (long)W * N;
     const long nv_max = i8_chunk();
     const int nv = (Nc - n0) < nv_max ? (Nc - n0) : int(nv_max);
     const long ldc = (long)nv * N;
+    const long row0 = (long)det * Nc * N + (long)n0 * N;  // determinant det's Lnak rows (n0, 0)
     int8_t* Lc[3];
-    for (int q = 0; q < 3; ++q) Lc[q] = Le_q[q] ? Le_q[q] + (long)n0 * N * ld_mr : nullptr;
+    for (int q = 0; q < 3; ++q) Lc[q] = Le_q[q] ? Le_q[q] + row0 * ld_mr : nullptr;
     *d = i8_desc();
     d->M = int(2 * R); d->N = int(ldc); d->K = Mr;
     d->A = i8_operand(Ge_q, 2 * R, ld_mr, Ge_e);
-    d->B = i8_operand(Lc, ldc, ld_mr, Le_e + (long)n0 * N);
+    d->B = i8_operand(Lc, ldc, ld_mr, Le_e + row0);
     d->bn = i8_bn;
     d->C = reinterpret_cast<float*>(Tchunk); d->ldc = ldc;
   }
+  int i8_det = 0;  // multi-determinant trials: the determinant whose exchange is in flight
+  // determinant det's G (FP64, its own overlap factors), one-body energy and G slices
+  int energy_md_i8_prep(int det) {
+    int rc;
+    const long o = det_elems();
+    const double scl = closed() ? 2.0 : 1.0;
+    if ((rc = md_factor(det, SM, W, md_ov + (long)det * W, true, ov_scale()))) return rc;
+    if ((rc = ops::green_compact(T, SM, G, W, Mr, N, st))) return rc;
+    if ((rc = energy_e1(G, haj + det * o, md_E + (long)det * W * 3, W, N, Mr, p.E0, scl, 1, st))) return rc;
+    return islice_rows_planar(G, (long)W * N, Mr, nslices, Ge_q, ld_mr, Ge_e, st);
+  }
+  // NOMSD::Energy with ndet > 1 in stages: each determinant's exchange chunks in turn (its G, one-body
+  // energy and slices before its first chunk, its sums after its last), then the ci-weighted ratio
+  int energy_md_i8_stage(int s, IsliceGemmDesc* d, bool* more) {
+    int rc;
+    const double scl = closed() ? 2.0 : 1.0;
+    *more = true;
+    if (s == 0) {
+      ph_begin(SFQ_PH_ENERGY);
+      inv_cached = false;
+      i8_det = 0;
+      i8_n0 = 0;
+      if ((rc = energy_md_i8_prep(0))) return rc;
+      i8_exchange_desc(0, d, 0);
+      return SFQ_OK;
+    }
+    const long nv_max = i8_chunk();
+    const int n0 = i8_n0;
+    const int nv = (Nc - n0) < nv_max ? (Nc - n0) : int(nv_max);
+    if ((rc = energy_exx_reduce_f32(reinterpret_cast<float*>(Tchunk), W, N, nv, n0, Nc, (long)nv * N, exxn, kl, st,
+                                    spin_split())))
+      return rc;
+    i8_n0 = n0 + nv;
+    if (i8_n0 < Nc) {
+      i8_exchange_desc(i8_n0, d, i8_det);
+      return SFQ_OK;
+    }
+    if ((rc = energy_finish(exxn, kl, md_E + (long)i8_det * W * 3, W, Nc, scl, 1, 1, st))) return rc;
+    if (++i8_det < ndet) {
+      i8_n0 = 0;
+      if ((rc = energy_md_i8_prep(i8_det))) return rc;
+      i8_exchange_desc(0, d, i8_det);
+      return SFQ_OK;
+    }
+    *more = false;
+    md_energy_kernel<<<(W + 127) / 128, 128, 0, st>>>(md_ov, md_E, md_cic, ndet, W, E3, ovtmp);
+    SFQ_LAUNCHED();
+    ph_end(SFQ_PH_ENERGY);
+    return SFQ_OK;
+  }
   int energy_i8_stage(int s, IsliceGemmDesc* d, bool* more) {
+    if (ndet > 1) return energy_md_i8_stage(s, d, more);
     int rc;
     const double scl = closed() ? 2.0 : 1.0;  // CLOSED counts each orbital twice
     *more = true;
@@ -3246,11 +3426,11 @@ int sfq_engine_create_nomsd(sfq_engine_t* out, const sfq_engine_params_t* p, con
     delete h;
     return record_error(SFQ_ERR_ARG, "engine: unknown precision %d", p->precision);
   }
-  if (e.mixed && (((coll || npol > 1) && !e.nslices) || ndet > 1)) {
+  if (e.mixed && !e.nslices && (coll || npol > 1 || ndet > 1)) {
     delete h;
     return record_error(SFQ_ERR_UNSUPPORTED,
-                        "engine: multi-determinant trials run in FP64, COLLINEAR and NONCOLLINEAR walkers in FP64 or "
-                        "the int8-slice precisions");
+                        "engine: COLLINEAR and NONCOLLINEAR walkers and multi-determinant trials run in FP64 or the "
+                        "int8-slice precisions");
   }
   if (e.nslices && (!e.trial_real || e.M > 1024)) {
     delete h;

@@ -65,10 +65,12 @@ def test_group_block_equals_each_member_alone(lanes):
 
 def _int8_engines(seed0=200):
     """INT8X3 members whose products differ in every shape: synthetic CLOSED systems (Taylor tiles of
-    64 and 80 orbitals), the reference's Li COLLINEAR and BH GHF NONCOLLINEAR fixtures (tiles of 32)."""
+    64 and 80 orbitals), the reference's Li COLLINEAR and BH GHF NONCOLLINEAR fixtures (tiles of 32)
+    and its 34-determinant BH CASCI trial (the force bias from the full G)."""
     from tests.golden_io import engine_system, snapshot
     systems = [(synthetic.make_system(spec), W) for spec, W, _p in MEMBERS]
-    systems += [(engine_system(snapshot("li_rohf_collinear")), 40), (engine_system(snapshot("bh_ghf_noncollinear")), 50)]
+    systems += [(engine_system(snapshot("li_rohf_collinear")), 40), (engine_system(snapshot("bh_ghf_noncollinear")), 50),
+                (engine_system(snapshot("bh_rcasci_uhf_collinear")), 24)]
     return [A.AfqmcEngine(s, W, dt=2e-4, seed=seed0 + i, precision=capi.PRECISION_INT8X3)
             for i, (s, W) in enumerate(systems)]
 

@@ -222,6 +222,41 @@ def test_int8x3_noncollinear_walkers_vs_fp64_engine(case):
     e8.close()
 
 
+@pytest.mark.parametrize("case", ["bh_rcasci_rhf_closed", "bh_rcasci_uhf_collinear", "bh_rcasci_ghf_noncollinear"])
+def test_int8x3_multi_determinant_trials_vs_fp64_engine(case):
+    """Multi-determinant NOMSD trials (the reference's BH CASCI fixtures, 34 determinants; CLOSED,
+    COLLINEAR and NONCOLLINEAR walkers) in INT8X3 against the FP64 engine, which reproduces the
+    reference's recorded CASCI runs: the force bias from the ci-weighted full G minus the trial's,
+    sliced against L over (i, k); every determinant's exchange from its own slices.  The trial's
+    energy, the energies of identical walkers and three steps from identical walkers and seeded
+    fields, at the bounds of the single-determinant tests."""
+    from tests.golden_io import engine_system, snapshot
+    s = engine_system(snapshot(case))
+    W, dt = 32, 0.01
+    e64 = afqmc.AfqmcEngine(s, W, dt=dt, seed=5, precision=capi.PRECISION_FP64)
+    e8 = afqmc.AfqmcEngine(s, W, dt=dt, seed=5, precision=capi.PRECISION_INT8X3)
+    E64, E8 = e64.init(), e8.init()
+    assert abs(E8 - E64) < 2e-6 * abs(E64)
+    for st in range(3):  # walkers away from the trial
+        e64.propagate(E64, st)
+    SM, pr = e64.walkers()
+    e8.set_walkers(SM, pr)
+    assert _rel(e8.energy(), e64.energy()) < 2e-6
+    for st in (7, 8, 9):
+        e64.propagate(E64, st)
+        e8.propagate(E64, st)
+        X8, X64 = (e.fetch("X", (W, s.Nc), np.complex128) for e in (e8, e64))
+        assert _rel(X8, X64) < 1e-6 * (st - 6)
+    S8, p8 = e8.walkers()
+    S64, p64 = e64.walkers()
+    assert _rel(S8, S64) < 6e-6
+    assert _rel(p8["OVLP"], p64["OVLP"]) < 1.5e-5
+    assert _rel(p8["WEIGHT"], p64["WEIGHT"]) < 6e-5
+    assert _rel(e8.energy(), e64.energy()) < 2e-6
+    e64.close()
+    e8.close()
+
+
 def test_bounded_waits_expire_and_report_timeout():
     """The product's loads are held back by a flag nothing sets and every wait is limited to 1 ms:
     each wait expires, the kernel reports SFQ_ERR_TIMEOUT with nothing in flight and its tensor
