@@ -268,10 +268,11 @@ typedef struct {
  * biases every product by the same relative shrink; these carry no such bias.  The force bias, the
  * fields, vHS, the P1 products and Taylor terms, and the exchange tensor of the energy run this way;
  * the Green's function, LU / log det, overlaps, orthogonalization, walker update and all sums stay
- * FP64.  Needs a real trial and nmo <= 1024; any nchol; CLOSED, COLLINEAR or NONCOLLINEAR walkers (a
- * spinor walker's two (nmo, nel) components share its vHS and P1); single- or multi-determinant trials
- * (with ndet > 1 the force bias contracts the ci-weighted full G, minus the trial's, with L over (i, k),
- * and each determinant's exchange uses its own slices of its Lnak). */
+ * FP64.  Needs nmo <= 1024; any nchol; CLOSED, COLLINEAR or NONCOLLINEAR walkers (a spinor walker's
+ * two (nmo, nel) components share its vHS and P1); single- or multi-determinant trials (with ndet > 1
+ * the force bias contracts the ci-weighted full G, minus the trial's, with L over (i, k), and each
+ * determinant's exchange uses its own slices of its Lnak); real or complex trials (a complex trial's
+ * Lnak adds the products with its imaginary rows to the force bias and the exchange tensor). */
 #define SFQ_PRECISION_INT8X3 3     /* 3 slices: 2^-24 of each row's largest entry, 6 int8 products */
 #define SFQ_PRECISION_INT8X2 4     /* 2 slices: 2^-16 of each row's largest entry, 3 int8 products */
 

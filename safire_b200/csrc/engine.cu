@@ -738,10 +738,11 @@ struct Engine {
       plan_i8();
       const long R = (long)W * npol * N, RG = (long)W * N, vrows = sym ? P : MM;
       const bool md = ndet > 1;  // the force bias from the full G: no slices of Lnak over (a, k) nor of G
+      const long lp = trial_real ? 1 : 2;  // a complex trial's Lnak: planar rows, real parts then imaginary
       std::vector<Item> mx;
       for (int q = 0; q < nslices; ++q) {
-        mx.push_back({(void**)&Lv_q[q], md ? 0 : (size_t)Nc * ld_nm});
-        mx.push_back({(void**)&Le_q[q], (size_t)ndet * Nc * N * ld_mr});
+        mx.push_back({(void**)&Lv_q[q], md ? 0 : (size_t)lp * Nc * ld_nm});
+        mx.push_back({(void**)&Le_q[q], (size_t)lp * ndet * Nc * N * ld_mr});
         if (md) {
           mx.push_back({(void**)&Lf_q[q], (size_t)Nc * ld_mm});
           mx.push_back({(void**)&Gf_q[q], (size_t)2 * W * ld_mm});
@@ -756,7 +757,7 @@ struct Engine {
       }
       const size_t ie = sizeof(int);
       std::vector<Item> mx2 = {
-          {(void**)&Lv_e, ie * Nc}, {(void**)&Le_e, ie * ndet * Nc * N}, {(void**)&Lh_e, ie * vrows},
+          {(void**)&Lv_e, ie * lp * Nc}, {(void**)&Le_e, ie * lp * ndet * Nc * N}, {(void**)&Lh_e, ie * vrows},
           {(void**)&P1_e, ie * M}, {(void**)&Gv_e, ie * 2 * W}, {(void**)&Ge_e, ie * 2 * RG},
           {(void**)&Xq_e, ie * 2 * W}, {(void**)&V_e, ie * W * M}, {(void**)&V_emax, ie * W * M},
           {(void**)&A_e[0], ie * R}, {(void**)&A_e[1], ie * R},
@@ -866,12 +867,18 @@ struct Engine {
       }
     }
     SFQ_CUDA_TRY(cudaFreeAsync(tmp, st));
-    const long o = det_elems();
-    for (int d = 0; d < ndet; ++d) {
-      const double* Ld = (const double*)Lnak + (size_t)d * Nc * o;
+    const long o = det_elems(), lp = trial_real ? 1 : 2;
+    for (int d = 0; d < ndet; ++d) {  // determinant d's rows at d lp Nc N (planar for a complex trial)
       int8_t* q[3];
-      for (int t = 0; t < 3; ++t) q[t] = Le_q[t] ? Le_q[t] + (long)d * Nc * N * ld_mr : nullptr;
-      if ((rc = islice_rows_real(Ld, (long)Nc * N, Mr, Mr, nslices, q, ld_mr, Le_e + (long)d * Nc * N, st))) return rc;
+      for (int t = 0; t < 3; ++t) q[t] = Le_q[t] ? Le_q[t] + lp * d * Nc * N * ld_mr : nullptr;
+      int* ed = Le_e + lp * d * Nc * N;
+      if (trial_real) {
+        const double* Ld = (const double*)Lnak + (size_t)d * Nc * o;
+        if ((rc = islice_rows_real(Ld, (long)Nc * N, Mr, Mr, nslices, q, ld_mr, ed, st))) return rc;
+      } else {
+        const cplx* Ld = (const cplx*)Lnak + (size_t)d * Nc * o;
+        if ((rc = islice_rows_planar(Ld, (long)Nc * N, Mr, nslices, q, ld_mr, ed, st))) return rc;
+      }
     }
     SFQ_CUDA_TRY(cudaStreamSynchronize(st));
     return setup_i8_common();
@@ -1066,13 +1073,19 @@ struct Engine {
         if ((rc = lu_logdet(T, (long)N * N, 1, N, ovtmp, false, 1.0, true, st))) return rc;
         if ((rc = ops::green_compact(T, SM2, G, 1, Mr, N, st))) return rc;
         SFQ_CUDA_TRY(cudaMemcpyAsync(GT_c, G, sizeof(cplx) * NM, cudaMemcpyDeviceToDevice, st));
-        if ((rc = ops::vbias(G, Lnak, false, X, 1, N, Mr, Nc, vb_scale(), st))) return rc;
+        if ((rc = ops::vbias(G, Lnak, !trial_real, X, 1, N, Mr, Nc, vb_scale(), st))) return rc;
         SFQ_CUDA_TRY(cudaMemcpyAsync(vbT, X, sizeof(cplx) * Nc, cudaMemcpyDeviceToDevice, st));
         SFQ_CUDA_TRY(cudaStreamSynchronize(st));
       }
-      const double* Ln = (const double*)Lnak;
-      if ((rc = islice_rows_real(Ln, Nc, NM, NM, nslices, Lv_q, ld_nm, Lv_e, st))) return rc;
-      if ((rc = islice_rows_real(Ln, (long)Nc * N, Mr, Mr, nslices, Le_q, ld_mr, Le_e, st))) return rc;
+      if (trial_real) {
+        const double* Ln = (const double*)Lnak;
+        if ((rc = islice_rows_real(Ln, Nc, NM, NM, nslices, Lv_q, ld_nm, Lv_e, st))) return rc;
+        if ((rc = islice_rows_real(Ln, (long)Nc * N, Mr, Mr, nslices, Le_q, ld_mr, Le_e, st))) return rc;
+      } else {  // planar rows: Lr (rows r), Li (rows R + r)
+        const cplx* Lc = (const cplx*)Lnak;
+        if ((rc = islice_rows_planar(Lc, Nc, NM, nslices, Lv_q, ld_nm, Lv_e, st))) return rc;
+        if ((rc = islice_rows_planar(Lc, (long)Nc * N, Mr, nslices, Le_q, ld_mr, Le_e, st))) return rc;
+      }
       if ((rc = setup_i8_common())) return rc;
     } else if (mixed) {  // mixed precision: bf16 hi/lo planes of the resident real tensors
       if (sym) {
@@ -2129,9 +2142,10 @@ struct Engine {
     int rc;
     IsliceGemmDesc d;
     bool more = true;
-    for (int s = 0; s < 4 && more; ++s) {
-      if ((rc = propagate_i8_stage(s, 0.0, 0, nullptr, &d, &more))) return rc;
-      if (s < 3 && (rc = islice_gemm(d, st))) return rc;
+    for (int s = 0; more; ++s) {  // up to the first Taylor product
+      if ((rc = propagate_i8_next(s, 0.0, 0, nullptr, &d, &more))) return rc;
+      if (d.cplx_half > 0) break;
+      if (more && (rc = islice_gemm(d, st))) return rc;
     }
     const int planned = i8_half;
     double t_cur = 0.0, best = 1e300;
@@ -2335,6 +2349,54 @@ struct Engine {
   // alone, each product is launched right after its stage; a group of engines runs stage s of
   // every member, then all their products as one launch (Group::record_fused).
   int i8_cur = 0;  // Taylor operand buffer between stages
+  // follow-up products of a stage, launched before the next stage: with a complex trial, Lnak's
+  // imaginary rows Li make a force bias or exchange product C = [A_re; A_im] Lr^T complete only with
+  // C_re -= A_im Li^T and C_im += A_re Li^T (accumulated into the same output, the same K splits)
+  IsliceGemmDesc i8_queue[2];
+  int i8_qn = 0, i8_qh = 0, i8_pst = 0, i8_est = 0;
+  void i8_queue_cplx(const IsliceGemmDesc& d, long h, const IsliceOperand& Bi) {
+    IsliceGemmDesc a = d, b = d;
+    a.M = b.M = int(h);
+    a.A.rows = b.A.rows = h;
+    for (int t = 0; t < 3; ++t) a.A.q[t] = d.A.q[t] ? d.A.q[t] + h * d.A.ld : nullptr;  // A_im rows
+    a.A.e = d.A.e + h;
+    a.B = b.B = Bi;
+    a.alpha = -d.alpha;
+    a.accumulate = b.accumulate = true;
+    b.C = d.C + h * d.ldc;
+    i8_queue[0] = a;
+    i8_queue[1] = b;
+    i8_qh = 0;
+    i8_qn = 2;
+  }
+  // the step's and the energy's products in order (stages and their follow-ups): call k = 0, 1, ...
+  int propagate_i8_next(int k, double Eshift, unsigned long long step, const double* uniforms, IsliceGemmDesc* d,
+                        bool* more) {
+    if (k == 0) {
+      i8_qn = 0;
+      i8_pst = 0;
+    }
+    if (i8_qn > 0) {
+      *d = i8_queue[i8_qh++];
+      --i8_qn;
+      *more = true;
+      return SFQ_OK;
+    }
+    return propagate_i8_stage(i8_pst++, Eshift, step, uniforms, d, more);
+  }
+  int energy_i8_next(int k, IsliceGemmDesc* d, bool* more) {
+    if (k == 0) {
+      i8_qn = 0;
+      i8_est = 0;
+    }
+    if (i8_qn > 0) {
+      *d = i8_queue[i8_qh++];
+      --i8_qn;
+      *more = true;
+      return SFQ_OK;
+    }
+    return energy_i8_stage(i8_est++, d, more);
+  }
   int propagate_i8_stage(int s, double Eshift, unsigned long long step, const double* uniforms, IsliceGemmDesc* d,
                          bool* more) {
     int rc;
@@ -2368,6 +2430,11 @@ struct Engine {
       d->B = i8_operand(Lv_q, Nc, ld_nm, Lv_e);
       d->bn = i8_vb_bn; d->ksplit = i8_vb_ks; d->sCk = 2L * W * Nc;
       d->C = Cvb; d->ldc = Nc;
+      if (!trial_real) {  // Lnak's imaginary rows follow its real ones
+        int8_t* qi[3];
+        for (int t = 0; t < 3; ++t) qi[t] = Lv_q[t] ? Lv_q[t] + (long)Nc * ld_nm : nullptr;
+        i8_queue_cplx(*d, W, i8_operand(qi, Nc, ld_nm, Lv_e + Nc));
+      }
       return SFQ_OK;
     }
     if (s == 1) {
@@ -2451,7 +2518,7 @@ struct Engine {
     IsliceGemmDesc d;
     bool more = true;
     for (int s = 0; more; ++s) {
-      if ((rc = propagate_i8_stage(s, Eshift, step, uniforms, &d, &more))) return rc;
+      if ((rc = propagate_i8_next(s, Eshift, step, uniforms, &d, &more))) return rc;
       if (more && (rc = islice_gemm(d, st))) return rc;
     }
     return SFQ_OK;
@@ -2469,12 +2536,13 @@ struct Engine {
     if (nv_max > Nc) nv_max = Nc;
     return nv_max;
   }
-  void i8_exchange_desc(int n0, IsliceGemmDesc* d, int det = 0) const {
+  void i8_exchange_desc(int n0, IsliceGemmDesc* d, int det = 0) {
     const long R = (long)W * N;
     const long nv_max = i8_chunk();
     const int nv = (Nc - n0) < nv_max ? (Nc - n0) : int(nv_max);
     const long ldc = (long)nv * N;
-    const long row0 = (long)det * Nc * N + (long)n0 * N;  // determinant det's Lnak rows (n0, 0)
+    const long lp = trial_real ? 1 : 2;
+    const long row0 = lp * det * Nc * N + (long)n0 * N;  // determinant det's Lnak rows (n0, 0)
     int8_t* Lc[3];
     for (int q = 0; q < 3; ++q) Lc[q] = Le_q[q] ? Le_q[q] + row0 * ld_mr : nullptr;
     *d = i8_desc();
@@ -2483,6 +2551,11 @@ struct Engine {
     d->B = i8_operand(Lc, ldc, ld_mr, Le_e + row0);
     d->bn = i8_bn;
     d->C = reinterpret_cast<float*>(Tchunk); d->ldc = ldc;
+    if (!trial_real) {  // the imaginary rows of these Lnak rows: Nc N rows further
+      int8_t* qi[3];
+      for (int q = 0; q < 3; ++q) qi[q] = Le_q[q] ? Le_q[q] + (row0 + (long)Nc * N) * ld_mr : nullptr;
+      i8_queue_cplx(*d, R, i8_operand(qi, ldc, ld_mr, Le_e + row0 + (long)Nc * N));
+    }
   }
   int i8_det = 0;  // multi-determinant trials: the determinant whose exchange is in flight
   // determinant det's G (FP64, its own overlap factors), one-body energy and G slices
@@ -2569,7 +2642,7 @@ struct Engine {
     IsliceGemmDesc d;
     bool more = true;
     for (int s = 0; more; ++s) {
-      if ((rc = energy_i8_stage(s, &d, &more))) return rc;
+      if ((rc = energy_i8_next(s, &d, &more))) return rc;
       if (more && (rc = islice_gemm(d, st))) return rc;
     }
     return SFQ_OK;
@@ -3225,11 +3298,11 @@ struct Group {
       if (rc || ce != cudaSuccess) break;
       const int cc = ch - 'a';
       rc = grouped_stages("p", [](Engine& e, int s, IsliceGemmDesc* d, bool* m) {
-        return e.propagate_i8_stage(s, 0.0, 0, nullptr, d, m);  // step and Eshift come from the device
+        return e.propagate_i8_next(s, 0.0, 0, nullptr, d, m);  // step and Eshift come from the device
       });
       for (size_t i = 0; i < n && !rc; ++i) rc = es[i]->block_after_propagate(cc);
       if (!rc && (cc & 8)) {
-        rc = grouped_stages("e", [](Engine& e, int s, IsliceGemmDesc* d, bool* m) { return e.energy_i8_stage(s, d, m); });
+        rc = grouped_stages("e", [](Engine& e, int s, IsliceGemmDesc* d, bool* m) { return e.energy_i8_next(s, d, m); });
         for (size_t i = 0; i < n && !rc; ++i) rc = es[i]->block_measure(&slot[i]);
       }
       for (size_t i = 0; i < n && !rc; ++i) rc = es[i]->block_step_end(cc, Engine::block_relax(rps[i]));
@@ -3432,9 +3505,9 @@ int sfq_engine_create_nomsd(sfq_engine_t* out, const sfq_engine_params_t* p, con
                         "engine: COLLINEAR and NONCOLLINEAR walkers and multi-determinant trials run in FP64 or the "
                         "int8-slice precisions");
   }
-  if (e.nslices && (!e.trial_real || e.M > 1024)) {
+  if (e.nslices && e.M > 1024) {
     delete h;
-    return record_error(SFQ_ERR_UNSUPPORTED, "engine: the int8-slice products need a real trial and nmo <= 1024");
+    return record_error(SFQ_ERR_UNSUPPORTED, "engine: the int8-slice products need nmo <= 1024");
   }
   if (e.mixed && !e.nslices && (!e.trial_real || e.M % 8 || e.Nc % 8)) {
     delete h;

@@ -158,6 +158,37 @@ def test_int8x3_engine_one_step_vs_oracle(spec):
     eng.close()
 
 
+@pytest.mark.parametrize("spec", [synthetic.CFG_SMALL, synthetic.SystemSpec(M=19, N=3, Nc=78, decay=19.0)])
+def test_int8x3_complex_trial_one_step_vs_oracle(spec):
+    """A complex trial (the orbitals given phases e^{i theta_j}): Lnak is complex, so the force bias and
+    the exchange tensor are completed by the products with its imaginary rows (accumulated into the
+    same outputs).  One step against the FP64 oracle at the closed-shell test's bounds."""
+    s = synthetic.make_system(spec)
+    s.PsiT = s.PsiT * np.exp(1j * np.linspace(0.0, 1.0, s.M))[None, :]
+    W, dt = 16, 0.005
+    eng = afqmc.AfqmcEngine(s, W, dt=dt, seed=3, precision=capi.PRECISION_INT8X3)
+    assert eng.info().lnak_complex == 1
+    ham = O.Hamiltonian(s.hcore, s.Likn, s.PsiT)
+    prop = O.Propagator(ham, dt, seed=3)
+    wo = O.Walkers(s.initial_walkers(W))
+    Esh_o = O.init_walkers(ham, wo)
+    Esh = eng.init()
+    assert abs(Esh - Esh_o) < 5e-6 * abs(Esh_o)
+    dbg = prop.propagate(wo, Esh_o, 0)
+    eng.propagate(Esh, 0)
+    X = eng.fetch("X", (W, s.Nc), np.complex128)
+    assert _rel(X, dbg["X"]) < 1e-6
+    SM, pr = eng.walkers()
+    assert _rel(SM, wo.SM) < 2e-6
+    assert _rel(pr["OVLP"], wo.ovlp) < 5e-6
+    assert _rel(pr["WEIGHT"], wo.weight) < 2e-5
+    E = eng.energy()
+    Eo, _ = O.wfn_energy_noupdate(ham, O.Walkers(SM))
+    assert _rel(E[:, 0], Eo[:, 0]) < 1e-10
+    assert _rel(E, Eo) < 2e-6
+    eng.close()
+
+
 def test_int8x3_collinear_walkers_vs_fp64_engine():
     """COLLINEAR walkers (the reference's Li ROHF fixture, M=14, 2 up + 1 down, Nc=70) in INT8X3
     against the FP64 engine, which reproduces the reference's recorded Li runs: the trial's energy,
@@ -222,16 +253,20 @@ def test_int8x3_noncollinear_walkers_vs_fp64_engine(case):
     e8.close()
 
 
-@pytest.mark.parametrize("case", ["bh_rcasci_rhf_closed", "bh_rcasci_uhf_collinear", "bh_rcasci_ghf_noncollinear"])
-def test_int8x3_multi_determinant_trials_vs_fp64_engine(case):
+@pytest.mark.parametrize("case,phased", [("bh_rcasci_rhf_closed", False), ("bh_rcasci_uhf_collinear", False),
+                                         ("bh_rcasci_ghf_noncollinear", False), ("bh_rcasci_rhf_closed", True)])
+def test_int8x3_multi_determinant_trials_vs_fp64_engine(case, phased):
     """Multi-determinant NOMSD trials (the reference's BH CASCI fixtures, 34 determinants; CLOSED,
     COLLINEAR and NONCOLLINEAR walkers) in INT8X3 against the FP64 engine, which reproduces the
     reference's recorded CASCI runs: the force bias from the ci-weighted full G minus the trial's,
     sliced against L over (i, k); every determinant's exchange from its own slices.  The trial's
     energy, the energies of identical walkers and three steps from identical walkers and seeded
-    fields, at the bounds of the single-determinant tests."""
+    fields, at the bounds of the single-determinant tests.  Phased: every determinant's orbitals given
+    phases e^{i theta_j}, a complex trial (complex Lnak per determinant)."""
     from tests.golden_io import engine_system, snapshot
     s = engine_system(snapshot(case))
+    if phased:
+        s.PsiT = s.PsiT * np.exp(1j * np.linspace(0.0, 1.0, s.PsiT.shape[-1]))
     W, dt = 32, 0.01
     e64 = afqmc.AfqmcEngine(s, W, dt=dt, seed=5, precision=capi.PRECISION_FP64)
     e8 = afqmc.AfqmcEngine(s, W, dt=dt, seed=5, precision=capi.PRECISION_INT8X3)
