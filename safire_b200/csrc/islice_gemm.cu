@@ -732,7 +732,7 @@ int sfq_gemm_int8_slices(const double* A, const double* B, float* C, int M, int 
     return record_error(SFQ_ERR_ARG, "gemm_int8_slices: tile width %d not built", tile_n);
   if (!A || !B || !C) return record_error(SFQ_ERR_ARG, "gemm_int8_slices: null operand");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const long ld = (K + 15) / 16 * 16;
+  const long ld = (K + 63) / 64 * 64;  // slice rows on 64-byte boundaries, as the engine lays them out
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t qa = al((size_t)M * ld), qb = al((size_t)N * ld), ea = al(sizeof(int) * M), eb = al(sizeof(int) * N);
   const int ks = ksplit < 1 ? 1 : ksplit;
@@ -817,7 +817,7 @@ int sfq_gemm_int8_cplx_b(const void* A, const void* V, float* C, int W, int M, i
   if (!A || !V || !C) return record_error(SFQ_ERR_ARG, "gemm_int8_cplx_b: null operand");
   if (M > 1024) return record_error(SFQ_ERR_SHAPE, "gemm_int8_cplx_b: M=%d above 1024", M);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const long ld = (M + 15) / 16 * 16, R = (long)W * N, MM = (long)M * M;
+  const long ld = (M + 63) / 64 * 64, R = (long)W * N, MM = (long)M * M;  // 64-byte slice rows, as in the engine
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t sa = al(sizeof(float) * 2 * R * M), sz = al(sizeof(float) * 2 * R * M),
                sv = al(sizeof(float) * 2 * W * MM);
