@@ -331,8 +331,10 @@ int sfq_engine_population_control(sfq_engine_t e, unsigned long long call);
 int sfq_engine_measure_rdm(sfq_engine_t e, void* one_rdm, void* diag_two_rdm);
 
 /* The other observables of MixedEstimator (sfq_engine_measure_observables) and BackPropEstimator
- * (sfq_engine_measure_bp_observables, the arguments of sfq_engine_measure_bp_rdm), FP64 engines with a
- * single-determinant trial, divided by the total weight as the RDMs are; host pointers, NULL skips:
+ * (sfq_engine_measure_bp_observables, the arguments of sfq_engine_measure_bp_rdm), FP64 engines, single- or
+ * multi-determinant trials (summed over the references, each determinant's G with its coefficient, as
+ * the reference's referenceLoop does), divided by the total weight as the RDMs are; host pointers,
+ * NULL skips:
  *  - two_rdm: TwoRDM (Observables/twordm.hpp:29-77), (nspin + 1, nmo, nmo, nmo, nmo) complex as
  *    [block][i][k][j][l] = sum_w c_w (G_ik G_jl - G_il G_jk) within a spin, G_ik G_jl across, blocks
  *    (a,a,a,a), (a,a,b,b), (b,b,b,b) (CLOSED: the first two); CLOSED and COLLINEAR walkers, nmo^4 * 16

@@ -1577,8 +1577,6 @@ struct Engine {
   }
   // which observables this engine's walkers support, as the reference's constructors check them
   int check_obs(const ObsSpec& o) const {
-    if (ndet > 1 && (o.two_rdm || o.spin_corr || o.npair))
-      return record_error(SFQ_ERR_UNSUPPORTED, "TwoRDM, SpinCorr and PairCorr are measured for single determinants");
     if (o.two_rdm && npol == 2)
       return record_error(SFQ_ERR_UNSUPPORTED, "TwoRDM is only implemented for closed and collinear walkers");
     if (o.two_rdm && (double)M * M * M * M * 16.0 > double(1L << 30))

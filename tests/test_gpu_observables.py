@@ -54,6 +54,37 @@ def test_observables_match_the_oracle_along_the_seeded_replay(case, two, spin, p
         assert np.max(np.abs(a - b)) <= 1e-11 * max(1.0, float(np.max(np.abs(b)))), k
 
 
+@pytest.mark.parametrize("case,two,pair", [("bh_rcasci_rhf_closed", True, False), ("bh_rcasci_uhf_collinear", True, True),
+                                           ("bh_rcasci_ghf_noncollinear", False, True)])
+def test_multi_determinant_observables_match_the_oracle(case, two, pair):
+    """The reference's 34-determinant BH CASCI trials: TwoRDM, SpinCorr and PairCorr of the mixed and
+    back-propagated estimators summed over the references (each determinant's G with its
+    coefficient, the referenceLoop of twordm.hpp / spincorr.hpp / paircorr.hpp), along 8 steps of
+    the seeded replay, against the oracle's restatement."""
+    snap = snapshot(case)
+    st = snap["settings"]
+    M = snap["hcore"].shape[0]
+    steps = 8
+    obs = dict(two_rdm=two, spin_corr=True, pair_maps=_maps(M) if pair else None)
+    kw = dict(ortho_interval=st["ortho_interval"], pop_interval=st["pop_interval"], measure_interval=st["measure_interval"],
+              mixed_interval=snap.get("mixed_interval") or 2, bp_steps=snap.get("bp_steps") or [2],
+              bp_ortho_interval=snap.get("bp_ortho_interval") or 10)
+    eng = A.AfqmcEngine(engine_system(snap), st["nwalk"], dt=st["dt"], seed=0, precision=capi.PRECISION_FP64)
+    walker_rng = HostRandomGenerator(split_seed(st["seed"], 0, 0))
+    field_rng = HostRandomGenerator(split_seed(st["seed"], 0, 1))
+    _, series = eng.run_with_streams(steps, eng.init(), field_rng.uniforms, lambda: walker_rng.uniforms(1)[0],
+                                     equilibration_steps=st["equilibration_steps"], observables=obs, **kw)
+    eng.close()
+    _, _, oracle = O.run_seeded(oracle_hamiltonian(snap), st["nwalk"], st["dt"], steps, st["seed"], observables=obs,
+                                equilibration_steps=st["equilibration_steps"], **kw)
+    names = [k for k in series if k.endswith(("TwoRDM", "SpinCorr", "PairCorr")) and "Diagonal" not in k]
+    assert len(names) == (2 if two else 0) + 2 + (2 if pair else 0), names
+    for k in names:
+        a, b = np.asarray(series[k]), np.asarray(oracle[k])
+        assert a.shape == b.shape and len(a) > 0, k
+        assert np.max(np.abs(a - b)) <= 1e-11 * max(1.0, float(np.max(np.abs(b)))), k
+
+
 def test_observables_refused_where_the_reference_refuses_them():
     closed = engine_system(snapshot("bh_rhf_closed"))
     nonc = engine_system(snapshot("bh_uhf_noncollinear"))
