@@ -351,13 +351,14 @@ int sfq_engine_measure_bp_observables(sfq_engine_t e, int nsteps, int ortho_inte
                                       void* pair_corr);
 
 /* TimeEvolvedBPEstimator (TimeEvolvedBPEstimator.hpp:42-300, PropagateOperators
- * AFQMCBasePropagator.cpp:538-654), FP64 engines, single determinant; needs the back-propagation ring
+ * AFQMCBasePropagator.cpp:538-654), FP64 engines, single- or multi-determinant trials; needs the back-propagation ring
  * (sfq_engine_enable_back_propagation with nbp >= the longest length).  Per walker and spin the
  * operator states X, Y (identity at the anchor) and M (zero) evolve forward: te_evolve(nsteps) replays
  * the last nsteps stored fields oldest first (X <- P1 e^{i vHS} P1 X, Y <- P1^-1 e^{i vHS^H} P1^-1 Y)
  * and regularizes against the walkers' current Slater matrices S (Y <- S S^H Y, M += Y^H X,
  * X <- X - S S^H X).  The measurements take the dressed Green's functions
- * M + (PsiT X)^T (Gc conj(Y)) with the walker weights restored over restore_steps history steps
+ * M + (PsiT X)^T (Gc conj(Y)) (per reference determinant with its PsiT_d and Gc_d, weighted by
+ * conj(c_d) exp(ov_d - OVLP) / sum, CLOSED overlaps counted twice) with the walker weights restored over restore_steps history steps
  * (the caller passes bp, or 2 bp with extra path restoration, or 0), and the output layouts of
  * sfq_engine_measure_rdm / sfq_engine_measure_observables.  The schedule (evolve the segment since
  * the previous length, measure, re-anchor after the longest) is the caller's, as the reference's

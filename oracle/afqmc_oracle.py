@@ -1339,7 +1339,7 @@ def _spin_trials(ham):
 
 class TimeEvolvedBPEstimator:
     """TimeEvolvedBPEstimator with the mixed estimator's observables (TimeEvolvedBPEstimator.hpp:42-300,
-    AFQMCBasePropagator::PropagateOperators :538-654), one rank, a single-determinant trial.
+    AFQMCBasePropagator::PropagateOperators :538-654), one rank, single- or multi-determinant trials.
 
     Per walker and spin, operator states X (-> c^+), Y (-> c) start from the identity and M from zero
     at the anchor.  At a measurement length bp the segment since the previous length is replayed from
@@ -1347,9 +1347,11 @@ class TimeEvolvedBPEstimator:
     adjoint of the inverse propagator), then, with the walkers' current Slater matrices S:
     Y <- S S^H Y, M += Y^H X, X <- X - S S^H X.  The observables are measured on the dressed Green's
     functions G_s = M_s + (PsiT_s X_s)^T (Gc_s conj(Y_s)), Gc_s the walkers' compact mixed density
-    matrix, with the walker weights restored over bp (2 bp with extra path restoration) steps and
-    coefficient 1 (one determinant).  The anchor moves to the current step once bp reaches the
-    longest length."""
+    matrix, per reference determinant d with its PsiT_d (constructTimeEvolvedMeasurementInputs,
+    :48-140), with the walker weights restored over bp (2 bp with extra path restoration) steps and
+    the coefficients conj(c_d) exp(f ov_d - OVLP) / sum_d' (...) (f = 2 for CLOSED, ov_d the sum
+    over spins of the determinant's log overlaps with the current walkers): 1 for one determinant.
+    The anchor moves to the current step once bp reaches the longest length."""
 
     def __init__(self, ham, prop, wset, steps=(2,), path_restoration=True, extra_path_restoration=False,
                  observables=None):
@@ -1364,7 +1366,7 @@ class TimeEvolvedBPEstimator:
 
     def anchor(self, wset, step):
         W, R = wset.size(), wset.SM.shape[1]
-        ns = len(_spin_trials(self.ham))
+        ns = len(_spin_trials(_references(self.ham)[0][0]))
         self.X = np.tile(np.eye(R, dtype=np.complex128), (ns, W, 1, 1))
         self.Y = self.X.copy()
         self.Mac = np.zeros_like(self.X)
@@ -1391,7 +1393,7 @@ class TimeEvolvedBPEstimator:
                 self.X[q] = ham.propagate(self.X[q], prop.P1, V, prop.order)
                 self.Y[q] = ham.propagate(self.Y[q], self.P1inv, Vh, prop.order)
             slot = (slot + 1) % wset.nbp
-        for q, (_, c0, c1) in enumerate(_spin_trials(ham)):
+        for q, (_, c0, c1) in enumerate(_spin_trials(_references(ham)[0][0])):
             if c1 == c0:  # an empty sector: S S^H = 0
                 self.Y[q] = 0.0
                 continue
@@ -1409,20 +1411,28 @@ class TimeEvolvedBPEstimator:
             for _ in range(bp * (2 if self.extra else 1)):
                 hpos = wset.nhist - 1 if hpos == 0 else hpos - 1
                 weights = weights * wset.wfac[:, hpos]
-        blocks = []
-        for q, (P, c0, c1) in enumerate(_spin_trials(ham)):
-            G = self.Mac[q].copy()
-            if c1 > c0:
-                Gc, _ = mixed_density_matrix(P, wset.SM[:, :, c0:c1], compact=True)
-                G = G + np.transpose(P @ self.X[q], (0, 2, 1)) @ (Gc @ np.conj(self.Y[q]))
-            blocks.append(G)
-        G = np.stack(blocks, axis=1)
-        ones = np.ones(wset.size(), np.complex128)
-        one, two = _rdm_reduce([G], [ones], weights, _walker_kind(ham), ham.M)
+        dets, ci = _references(ham)
+        parts, es = [], []
+        for d, det in enumerate(dets):
+            blocks = []
+            ov = np.zeros(wset.size(), np.complex128)
+            for q, (P, c0, c1) in enumerate(_spin_trials(det)):
+                G = self.Mac[q].copy()
+                if c1 > c0:
+                    Gc, ovq = mixed_density_matrix(P, wset.SM[:, :, c0:c1], compact=True)
+                    G = G + np.transpose(P @ self.X[q], (0, 2, 1)) @ (Gc @ np.conj(self.Y[q]))
+                    ov = ov + ovq
+                blocks.append(G)
+            parts.append(np.stack(blocks, axis=1))
+            es.append(np.conj(ci[d]) * np.exp(det.ov_factor * ov - wset.ovlp))
+        tot = np.sum(es, axis=0)
+        coeffs = [e / tot for e in es]
+        kind = _walker_kind(dets[0])
+        one, two = _rdm_reduce(parts, coeffs, weights, kind, ham.M)
         pre = f"TimeEvolvedBP/Steps={bp}"
         out = {f"{pre}/OneRDM": one, f"{pre}/DiagonalTwoRDM": two}
         if self.observables:
-            obs = _observables_reduce([G], [ones], weights, _walker_kind(ham), ham.M, **self.observables)
+            obs = _observables_reduce(parts, coeffs, weights, kind, ham.M, **self.observables)
             out.update({f"{pre}/{k}": v for k, v in obs.items()})
         return out
 

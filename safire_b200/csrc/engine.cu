@@ -1330,7 +1330,6 @@ struct Engine {
   int te_enable() {
     int rc;
     if (!nbp) return record_error(SFQ_ERR_ARG, "time-evolved back propagation needs the field ring: enable back propagation first");
-    if (ndet > 1) return record_error(SFQ_ERR_UNSUPPORTED, "time-evolved back propagation is measured for single determinants");
     if (te_X) return SFQ_OK;
     const long RR = (long)Mr * Mr, nmat = (long)rdm_nspin() * W;
     SFQ_CUDA_TRY(cudaMalloc(&te_X, sizeof(cplx) * nmat * RR));
@@ -1432,11 +1431,14 @@ struct Engine {
   // the Green's functions the evolved operators dress (constructTimeEvolvedMeasurementInputs,
   // TimeEvolvedBPEstimator.hpp:42-140): Gf[w][s] = M_s + (PsiT_s X_s)^T (Gc_s conj(Y_s)), Gc the
   // walkers' compact mixed density matrix
-  int te_green(cplx* Gf) {
+  // det < 0: the single-determinant trial's G from density(); det >= 0: reference det's, its compact
+  // G already in G (from its overlap factors) and its PsiT_d in the dressing
+  int te_green(cplx* Gf, int det = -1) {
     int rc;
     const long RR = (long)Mr * Mr;
     const int ns = rdm_nspin();
-    if ((rc = density(ovtmp))) return rc;
+    if (det < 0 && (rc = density(ovtmp))) return rc;
+    const cplx* Pd = PsiT + (det < 0 ? 0 : (long)det * det_elems());
     cplx* Yc = te_scr;                        // conj(Y_s) (W, R, R)
     cplx* XR = te_scr + (size_t)W * RR;       // PsiT_s X_s (W, nel, R)
     cplx* GY = te_scr + 2 * (size_t)W * RR;   // Gc_s conj(Y_s) (W, nel, R)
@@ -1456,7 +1458,7 @@ struct Engine {
       if ((rc = gemm_f64(g, st))) return rc;
       GemmDesc h;  // XR = PsiT_s X_s
       h.M = nel; h.N = Mr; h.K = Mr; h.batch = W;
-      h.A = PsiT + (long)c0 * Mr; h.sAm = Mr; h.sAk = 1; h.sAb = 0; h.a_cplx = true;
+      h.A = Pd + (long)c0 * Mr; h.sAm = Mr; h.sAk = 1; h.sAb = 0; h.a_cplx = true;
       h.B = te_X + (size_t)q * W * RR; h.sBk = Mr; h.sBn = 1; h.sBb = RR; h.b_cplx = true;
       h.C = XR; h.sCm = Mr; h.sCn = 1; h.sCb = (long)nel * Mr;
       if ((rc = gemm_f64(h, st))) return rc;
@@ -1644,9 +1646,11 @@ struct Engine {
     const cplx* B = bp ? bp_SMN : SM;
     std::vector<cplx> cic(ndet, mk(1.0, 0.0));
     for (int d = 0; d < ndet && ndet > 1; ++d) cic[d] = cconj(ci_h[d]);
-    // determinant d's overlap matrices (one determinant per spin, not doubled), inverses in T
+    // determinant d's overlap matrices (one determinant per spin, not doubled; the time-evolved
+    // estimator doubles CLOSED ones, TimeEvolvedBPEstimator.hpp:84-92), inverses in T
+    const bool te_md = te && ndet > 1;
     auto factor = [&](int d, bool invert) -> int {
-      if (!bp) return md_factor(d, SM, W, ovd + (long)d * W, invert, 1.0);
+      if (!bp) return md_factor(d, SM, W, ovd + (long)d * W, invert, te ? ov_scale() : 1.0);
       GemmDesc g;  // T = Refs^H SMN, per walker (density_matrix.hpp:158-195)
       g.M = N; g.N = N; g.K = Mr; g.batch = W;
       g.A = bp_refs + (long)d * W * RN; g.sAm = 1; g.sAk = N; g.sAb = RN; g.a_cplx = true; g.conj_a = true;
@@ -1660,9 +1664,9 @@ struct Engine {
       SFQ_LAUNCHED();
       return SFQ_OK;
     };
-    for (int d = 0; d < ndet && !te; ++d)
+    for (int d = 0; d < ndet && (!te || te_md); ++d)
       if ((rc = factor(d, false))) return rc;
-    if (!te) {
+    if (!te || te_md) {
       cplx* dcic = nullptr;
       SFQ_CUDA_TRY(cudaMallocAsync((void**)&dcic, sizeof(cplx) * ndet, st));
       SFQ_CUDA_TRY(cudaMemcpyAsync(dcic, cic.data(), sizeof(cplx) * ndet, cudaMemcpyHostToDevice, st));
@@ -1672,12 +1676,17 @@ struct Engine {
       SFQ_CUDA_TRY(cudaStreamSynchronize(st));  // cic lives until the copy is done
     }
     for (int d = 0; d < ndet; ++d) {
-      if (te) {  // the operators' dressed G, a single determinant: coefficient 1
+      if (te && !te_md) {  // the operators' dressed G, a single determinant: coefficient 1
         if ((rc = te_green(Gf))) return rc;
         SFQ_CUDA_TRY(cudaMemcpyAsync(wc, weight, sizeof(cplx) * W, cudaMemcpyDeviceToDevice, st));
       }
-      if (!te && (rc = factor(d, true))) return rc;
-      if (!te && (rc = ops::green_compact(T, B, G, W, Mr, N, st))) return rc;
+      if ((!te || te_md) && (rc = factor(d, true))) return rc;
+      if ((!te || te_md) && (rc = ops::green_compact(T, B, G, W, Mr, N, st))) return rc;
+      if (te_md) {  // reference d's dressed G (constructTimeEvolvedMeasurementInputs) and coefficient
+        if ((rc = te_green(Gf, d))) return rc;
+        rdm_coeff_kernel<<<(W + 127) / 128, 128, 0, st>>>(ovd + (long)d * W, cic[d], shift, tot, weight, W, wc);
+        SFQ_LAUNCHED();
+      }
       // the full G of each spin block: Gf[w][s] = Aeff[rows s]^T Gc[w][rows s] (density_matrix.hpp:580-600),
       // Aeff = PsiT_d (shared) or the walker's conj(Refs^T)
       for (int s = 0; s < ns && !te; ++s) {

@@ -109,12 +109,14 @@ def test_observables_refused_where_the_reference_refuses_them():
 
 
 @pytest.mark.parametrize("case,extra", [("bh_rhf_closed", False), ("bh_uhf_collinear", True),
-                                        ("bh_uhf_noncollinear", False)])
+                                        ("bh_uhf_noncollinear", False), ("bh_rcasci_rhf_closed", False),
+                                        ("bh_rcasci_uhf_collinear", False), ("bh_rcasci_ghf_noncollinear", False)])
 def test_time_evolved_back_propagation_matches_the_oracle(case, extra):
     """TimeEvolvedBPEstimator over lengths 2 and 4 (two segments per window, combs and
     orthogonalizations inside it) along the seeded BH replay: the one-body and diagonal two-body
     RDMs and the other observables of the dressed Green's functions, against the oracle's
-    restatement (with extra path restoration for the collinear case)."""
+    restatement (with extra path restoration for the collinear case); the CASCI trials dress every
+    reference's G and weight it by its coefficient (CLOSED overlaps doubled)."""
     snap = snapshot(case)
     st = snap["settings"]
     M = snap["hcore"].shape[0]
