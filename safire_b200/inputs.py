@@ -18,8 +18,9 @@ Layouts (read with safire_b200.h5read):
 
 The reference's readers: RealDenseHamiltonian::getHamiltonianOperations
 (RealDenseHamiltonian.cpp:77-134) and read_wavefunction_info / HDF2CSR (readWfn.cpp:50-131,
-csr_utils.hpp:372-420).  Only what the CLOSED, single-determinant, dense-Cholesky path uses is
-accepted; anything else raises InputError with the reason, as utils::check aborts there.
+csr_utils.hpp:372-420).  Only what the dense real-Cholesky path uses is accepted (CLOSED, COLLINEAR and
+NONCOLLINEAR walkers over a spin-independent Hamiltonian; NOMSD trials of one or several
+determinants); anything else raises InputError with the reason, as utils::check aborts there.
 """
 import numpy as np
 
@@ -176,19 +177,40 @@ def load_nomsd_trial(path, walker_type="CLOSED"):
 
 
 def load_system(hamiltonian_path, wavefunction_path, walker_type="CLOSED"):
-    """The engine's System (hcore, Likn, PsiT, E0 and sizes) from a Hamiltonian and a trial file; for
-    COLLINEAR walkers PsiT stacks the up rows over the down rows and nel_dn counts the latter."""
+    """The engine's System (hcore, Likn, PsiT, E0 and sizes) from a Hamiltonian and a NOMSD trial file,
+    for CLOSED, COLLINEAR and NONCOLLINEAR walkers and single- or multi-determinant trials, as
+    getHamiltonianOperations and read_nomsd_wavefunction take them (RealDenseHamiltonian.cpp:77-134,
+    readWfn.h:90-153): COLLINEAR PsiT stacks the up rows over the down rows and nel_dn counts the
+    latter; NONCOLLINEAR PsiT holds the (N, 2 nmo) spinor orbitals (npol 2); a trial of several
+    determinants gives PsiT (ndet, rows, cols) and the coefficients ci.  E0 counts the electrons as
+    read_energy_offset does for the walker type."""
     from .synthetic import System, SystemSpec
     wt = walker_type.upper()
-    _check(wt in ("CLOSED", "COLLINEAR"), f"the engine runs CLOSED and COLLINEAR walkers, not {wt}")
-    wfn = load_nomsd_trial(wavefunction_path, wt)
+    dets, ci, _ = load_nomsd_determinants(wavefunction_path, wt)
+    d0 = dets[0]
+    kw = {}
     if wt == "COLLINEAR":
-        ham = load_dense_hamiltonian(hamiltonian_path, wfn["nup"], wfn["ndn"])
-        _check(wfn["nmo"] == ham["nmo"], f"trial has {wfn['nmo']} orbitals, Hamiltonian {ham['nmo']}")
-        PsiT = np.concatenate([wfn["PsiT_up"], wfn["PsiT_dn"]])
-        spec = SystemSpec(M=ham["nmo"], N=PsiT.shape[0], Nc=ham["nchol"], decay=0.0)
-        return System(spec, ham["hcore"], ham["Likn"], PsiT, ham["E0"], nel_dn=wfn["ndn"])
-    ham = load_dense_hamiltonian(hamiltonian_path, wfn["nup"])
-    _check(wfn["nmo"] == ham["nmo"], f"trial has {wfn['nmo']} orbitals, Hamiltonian {ham['nmo']}")
-    spec = SystemSpec(M=ham["nmo"], N=wfn["nup"], Nc=ham["nchol"], decay=0.0)
-    return System(spec, ham["hcore"], ham["Likn"], wfn["PsiT"], ham["E0"])
+        ham = load_dense_hamiltonian(hamiltonian_path, d0["nup"], d0["ndn"])
+        for d in dets:
+            _check((d["nup"], d["ndn"]) == (d0["nup"], d0["ndn"]),
+                   f"determinants with {d['nup']} + {d['ndn']} and {d0['nup']} + {d0['ndn']} electrons")
+        mats = [np.concatenate([d["PsiT_up"], d["PsiT_dn"]]) for d in dets]
+        kw["nel_dn"] = d0["ndn"]
+    elif wt == "NONCOLLINEAR":
+        ham = load_dense_hamiltonian(hamiltonian_path, d0["nup"], 0)
+        mats = [d["PsiT"] for d in dets]
+        kw["npol"] = 2
+    else:
+        ham = load_dense_hamiltonian(hamiltonian_path, d0["nup"])
+        mats = [d["PsiT"] for d in dets]
+    _check(d0["nmo"] == ham["nmo"], f"trial has {d0['nmo']} orbitals, Hamiltonian {ham['nmo']}")
+    for m in mats:
+        _check(m.shape == mats[0].shape, f"determinants of shapes {m.shape} and {mats[0].shape}")
+    N = mats[0].shape[0]
+    if len(mats) > 1:
+        PsiT = np.stack(mats)
+        kw["ci"] = ci
+    else:
+        PsiT = mats[0]
+    spec = SystemSpec(M=ham["nmo"], N=N, Nc=ham["nchol"], decay=0.0)
+    return System(spec, ham["hcore"], ham["Likn"], PsiT, ham["E0"], **kw)

@@ -118,6 +118,43 @@ def test_loaders_read_reference_files():
         load_dense_hamiltonian(f"{REF}/afqmc_inputs/BH/afqmc_H_rhf_noncollinear.h5", 3)
 
 
+LOAD_CASES = [("bh_rhf_closed", "BH", "afqmc_H_rhf_closed.h5", "afqmc_rhf_nomsd.h5"),
+              ("bh_rhf_collinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_rhf_nomsd.h5"),
+              ("bh_uhf_collinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_uhf_nomsd.h5"),
+              ("bh_rhf_noncollinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_rhf_nomsd.h5"),
+              ("bh_uhf_noncollinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_uhf_nomsd.h5"),
+              ("bh_ghf_noncollinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_ghf_nomsd.h5"),
+              ("bh_rcasci_rhf_closed", "BH", "afqmc_H_rhf_closed.h5", "afqmc_casci_rhf_nomsd.h5"),
+              ("bh_rcasci_rhf_collinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_casci_rhf_nomsd.h5"),
+              ("bh_rcasci_uhf_collinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_casci_uhf_nomsd.h5"),
+              ("bh_rcasci_rhf_noncollinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_casci_rhf_nomsd.h5"),
+              ("bh_rcasci_uhf_noncollinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_casci_uhf_nomsd.h5"),
+              ("bh_rcasci_ghf_noncollinear", "BH", "afqmc_H_rhf_closed.h5", "afqmc_casci_ghf_nomsd.h5"),
+              ("li_rohf_collinear", "Li", "hamil_closed.h5", "rohf_nomsd_polarized.h5")]
+
+
+@pytest.mark.skipif(not (REF and os.path.isdir(REF)),
+                    reason="SAFIRE_REFERENCE_ROOT does not name the reference tree on this machine")
+@pytest.mark.parametrize("case,system,ham,wfn", LOAD_CASES)
+def test_load_system_reads_every_walker_type_and_trial(case, system, ham, wfn):
+    """load_system builds, from the reference's own input files, the same System the snapshot case's
+    fixture gives the engine: CLOSED, COLLINEAR and NONCOLLINEAR walkers, single-determinant and the
+    34-determinant CASCI trials, BH and Li."""
+    from safire_b200.inputs import load_system
+    from tests.golden_io import engine_system
+    snap = snapshot(case)
+    wt = snap["settings"]["walker_type"]
+    got = load_system(f"{REF}/afqmc_inputs/{system}/{ham}", f"{REF}/afqmc_inputs/{system}/{wfn}", wt)
+    want = engine_system(snap)
+    assert (got.M, got.N, got.Nc, got.nel_dn, got.npol) == (want.M, want.N, want.Nc, want.nel_dn, want.npol)
+    assert got.E0 == want.E0
+    for k in ("hcore", "Likn", "PsiT"):
+        assert np.array_equal(getattr(got, k), getattr(want, k)), k
+    assert (got.ci is None) == (want.ci is None)
+    if want.ci is not None:
+        assert np.array_equal(got.ci, want.ci)
+
+
 def test_collinear_with_identical_spins_is_closed():
     """COLLINEAR walkers whose up and down trials are the same RHF orbitals follow the CLOSED walk:
     same fields, overlaps (two equal determinants) and energies."""
