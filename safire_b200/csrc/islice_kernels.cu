@@ -417,11 +417,21 @@ void launch_taylor_update(const float* C, float* S, long R, int M, int k, bool s
   }
 }
 
+// 4-byte asynchronous global -> shared copy (L1-allocating); no register holds the value, so a
+// thread may have all of its copies in flight at once
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
+  const unsigned s = unsigned(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // V slices from the packed vHS, one block per (walker, strip of rs <= 32 rows): both parts' full rows
 // V[w][c][i][0..M) in shared memory, from the stored upper triangle (packed row i holds k >= i) and
 // its mirror (k < i: packed row k, column i; the strip's columns lie side by side in every earlier
 // packed row, so both are read in whole rows); each row's exponent from its maximum over both parts;
-// then whole rows of the slices of Vr, Vi and -Vi (zeros past M up to ld), four orbitals per thread
+// then whole rows of the slices of Vr, Vi and -Vi (zeros past M up to ld), four orbitals per thread.
+// The loads are asynchronous copies, every one of a block in flight together; the row stride lds is
+// four times an odd number of floats, so the mirrored columns' 32 rows fall in 8 banks, not 2.
 __global__ void __launch_bounds__(512) v_strip_kernel(const float* Cv, int W, int M, int rs, int lds, int ns, Q q,
                                                       long ld, int* e) {
   extern __shared__ float vs[];  // [2][rs][lds]
@@ -433,33 +443,16 @@ __global__ void __launch_bounds__(512) v_strip_kernel(const float* Cv, int W, in
   for (int c = 0; c < 2; ++c) {
     const float* src = Cv + ((long)c * W + w) * P;
     float* t = vs + c * rs * lds;
-    for (int r = warp; r < rows; r += nw) {  // the strip's rows, k >= i: four loads in flight per lane
+    for (int r = warp; r < rows; r += nw) {  // the strip's rows, k >= i
       const int i = i0 + r;
       const float* row = src + (long)i * M - (long)i * (i + 1) / 2;
-      for (int k = i + lane; k < M; k += 128) {
-        float v[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) v[u] = k + 32 * u < M ? row[k + 32 * u] : 0.f;
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (k + 32 * u < M) t[r * lds + k + 32 * u] = v[u];
-      }
+      for (int k = i + lane; k < M; k += 32) cp_async4(t + r * lds + k, row + k);
     }
-    // earlier rows k < i0: their columns i0 .. i0 + rows - 1, four rows in flight per warp
-    for (int k = warp; k < i0; k += 4 * nw) {
-      float v[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int kk = k + u * nw;
-        v[u] = (kk < i0 && lane < rows) ? src[(long)kk * M - (long)kk * (kk + 1) / 2 + i0 + lane] : 0.f;
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int kk = k + u * nw;
-        if (kk < i0 && lane < rows) t[lane * lds + kk] = v[u];
-      }
-    }
+    // earlier rows k < i0: their columns i0 .. i0 + rows - 1
+    if (lane < rows)
+      for (int k = warp; k < i0; k += nw) cp_async4(t + lane * lds + k, src + (long)k * M - (long)k * (k + 1) / 2 + i0 + lane);
   }
+  cp_async_wait_all();
   __syncthreads();
   for (int c = 0; c < 2; ++c) {  // the strip's own lower triangle, i0 <= k < i
     float* t = vs + c * rs * lds;
@@ -652,9 +645,11 @@ int islice_build_v(const float* Cv, int W, int M, bool packed, int nslices, int8
   if (int rc = check_slices(nslices, q, ld)) return rc;
   if (ld < M || 2L * W > 65535) return record_error(SFQ_ERR_SHAPE, "islice_build_v: sizes");
   if (packed) {
-    // strips of up to 32 rows whose two parts fit 200 KB of shared memory; rows padded to a multiple
-    // of four floats (16-byte row starts for the slicing pass's vector reads)
-    const int lds = (M + 3) / 4 * 4;
+    // strips of up to 32 rows whose two parts fit 200 KB of shared memory; rows padded to four times
+    // an odd number of floats (16-byte row starts for the slicing pass's vector reads, and the
+    // mirrored columns' stores spread over 8 banks)
+    const int l4 = (M + 3) / 4;
+    const int lds = 4 * (l4 | 1);
     int rs = int((200L * 1024) / (2L * lds * sizeof(float)));
     if (rs > 32) rs = 32;
     if (rs < 1) return record_error(SFQ_ERR_SHAPE, "islice_build_v: nmo %d too large for a strip", M);
