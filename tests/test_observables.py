@@ -4,7 +4,8 @@ RDMs of the same estimator (which the oracle reproduces from the reference's see
 
 * TwoRDM[(a,a,a,a)][i][i][j][j] and TwoRDM[(a,a,b,b)][i][i][j][j] are the diagonal two-body RDM's
   blocks; contracting TwoRDM over its last pair gives (N_s - 1) times the one-body RDM within a
-  spin and N_other times it across (each walker's mixed G is idempotent with trace N_s).
+  spin and N_other times it across (each walker's mixed G is idempotent with trace N_s; with a
+  multi-determinant trial each reference's G is, and the references' coefficients sum to one).
 * SpinCorr's Z channel off the diagonal is a combination of the diagonal two-body RDM's blocks:
   CLOSED  -(1/2) (D_ab - D_aa)[i][j];  COLLINEAR  (1/4) (D_aa + D_bb - D_ab - D_ab^T)[i][j].
 * PairCorr has no such link; it is pinned only by restating paircorr.hpp term by term, and the
@@ -45,7 +46,9 @@ def _unfold(diag, M, wt):
     return D
 
 
-@pytest.mark.parametrize("case,wt,nel", [("bh_rhf_closed", "CLOSED", (3, 3)), ("li_rohf_collinear", "COLLINEAR", (3, 0))])
+@pytest.mark.parametrize("case,wt,nel", [("bh_rhf_closed", "CLOSED", (3, 3)), ("li_rohf_collinear", "COLLINEAR", (3, 0)),
+                                         ("bh_rcasci_rhf_closed", "CLOSED", (3, 3)),
+                                         ("bh_rcasci_uhf_collinear", "COLLINEAR", (3, 3))])
 def test_two_rdm_and_spin_corr_follow_the_diagonal_and_one_body_rdms(case, wt, nel):
     ham, series = _run(case, dict(two_rdm=True, spin_corr=True))
     M = ham.M
