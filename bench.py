@@ -157,6 +157,20 @@ def fp64_gemm_peak_tflops(dev):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+L2_BYTES = 126e6  # B200 L2
+
+
+def l2_note(spec, nwalk):
+    """Whether a step's inputs (the Cholesky tensor and the walkers' Slater matrices) outgrow L2, so
+    that no flush is needed between timed steps, or fit in it."""
+    likn = spec.M ** 2 * spec.Nc * 8
+    walkers = nwalk * spec.M * spec.N * 16
+    if likn + walkers > L2_BYTES:
+        return "inputs larger than L2 (Likn %.2f GB + walkers %.2f GB)" % (likn / 1e9, walkers / 1e9)
+    return "inputs fit in L2 (Likn %.4f GB + walkers %.4f GB), not flushed between steps" % (
+        likn / 1e9, walkers / 1e9)
+
+
 def workload_config(cfg, spec, precision, world):
     """The workload both arms report (the same dict, so their lines describe the same config)."""
     return {"workload": f"AFQMC propagation {spec.name}: dense real Cholesky, closed shell, "
@@ -164,7 +178,7 @@ def workload_config(cfg, spec, precision, world):
             "M": spec.M, "N": spec.N, "Nchol": spec.Nc, "walkers_per_gpu": cfg["nwalk"], "dt": cfg["dt"],
             "precision": precision, "eshift": "relaxed every step (equilibration phase of run_afqmc)",
             "taylor_order": 6, "ortho_every": ORTHO_EVERY, "popcontrol_every": POP_EVERY,
-            "l2": "inputs larger than L2 (Likn alone is %.2f GB)" % (spec.M ** 2 * spec.Nc * 8 / 1e9),
+            "l2": l2_note(spec, cfg["nwalk"]),
             "parallelism": f"replicas x{world}"}
 
 
