@@ -187,7 +187,8 @@ def cpu_port_rate(cfg, steps=5, warm=2, walkers=None, with_popcontrol=False):
     the same system, as the reference runs on CPUs: walkers split over one worker per host core
     (execute.cpp:140, one thread per rank), each worker's BLAS on one thread
     (threading.cpp:27-36).  2 warm-up steps, then `steps` timed steps (orthogonalization every 5,
-    Eshift relaxed; the comb only with with_popcontrol, global over the sample)."""
+    Eshift relaxed; with with_popcontrol, the comb at the GPU arm's interval, each worker's shard
+    combed on its own)."""
     import concurrent.futures as cf
     from threadpoolctl import threadpool_limits
     from oracle import afqmc_oracle as O
