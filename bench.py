@@ -45,7 +45,7 @@ ORTHO_EVERY = 5
 POP_EVERY = 20
 # DRAM bytes (read + write) of one Taylor-term int8 product at 256 walkers, M = 400, N = 100, from an
 # ncu capture of the same kernel and tile (profiles/islice_taylor_M400_N100_W256_full.md)
-TAYLOR_DRAM_BYTES_256 = 432.294656e6 + 67.308544e6
+TAYLOR_DRAM_BYTES_256 = 485.248512e6 + 68.982528e6
 EQUIL_STEPS = 100  # run_afqmc relaxes Eshift every step for the first equilibration_steps
 RELAX = 1.0 - math.exp(-10.0 / EQUIL_STEPS)
 
